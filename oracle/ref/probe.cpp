@@ -1,0 +1,158 @@
+/*
+ * probe.cpp -- driver for the CPU oracle binary oracle/_ref/tpsc_ref_probe.
+ *
+ * TEST INFRASTRUCTURE.  It is compiled together with the UNMODIFIED reference
+ * sources (src/*.cpp of dbergeron1/TPSC_conductivity, read in place) and the
+ * FFTW shim in this folder.  It derives from the reference's cond_opt class
+ * only to reach the protected result arrays, runs the reference's own public
+ * methods in the order src/tpsc_main.cpp:61-75 uses, times them with
+ * omp_get_wtime, and dumps the results as raw little-endian doubles.
+ *
+ * usage: tpsc_ref_probe OUTDIR MODE U tp tpp t3 n T nk0 Nw0
+ *   MODE chi0   chi0::calc_chiqw_FFT_spline(nk0, Nw0)            (chi0.cpp:279)
+ *        solve  green::calc_Self_FFT_spline(); traceSelfG(); find_mu()
+ *               (green.cpp:1673, 3001, 3185) -- the full TPSC solve
+ *        cond   solve + cond_opt::calc_chijj_vertex_corr_all_optim(false,3,1,NULL,0)
+ *               (cond_opt.cpp:2537)
+ * The reference writes its own text files into the current directory; the
+ * probe chdir()s into OUTDIR/work first so they land there.
+ */
+#include "cond_opt.h"
+
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <sstream>
+#include <string>
+
+class tpsc_probe : public cond_opt {
+public:
+    tpsc_probe(int nk0, int Nw0, double n, double T, double eta, double *p)
+        : cond_opt(nk0, Nw0, n, T, eta, p) {}
+
+    int nk8() const { return (nbq * (nbq + 1)) / 2; }
+
+    void dump_chi0(FILE *meta, const std::string &dir) {
+        const long n8 = nk8();
+        const long nw = nwmax + 1;
+        fprintf(meta, "nbq %d\nnwmax %d\nmu0 %.17g\nchi0max %.17g\nqmax0 %d\nqmax1 %d\n", nbq,
+                nwmax, mu0, chi0max, qmax[0], qmax[1]);
+        write(dir + "/chiqw.bin", chiqw_array, n8 * nw);
+        write(dir + "/chi0_inf.bin", chi0_inf, n8);
+        write(dir + "/chi0_inf2.bin", chi0_inf2, n8);
+        write(dir + "/dtau_chirt0.bin", dtau_chirt0, n8);
+        write(dir + "/dtau_Grt0p.bin", dtau_Grt0p, n8);
+        if (chirt) write(dir + "/chirt.bin", chirt, n8 * nw);
+        write(dir + "/ek.bin", ek, (long)nbk * nbk);
+    }
+
+    void dump_solve(FILE *meta, const std::string &dir) {
+        const long n8 = nk8();
+        fprintf(meta, "Usp %.17g\nUch %.17g\ndblOcc %.17g\nSigma_inf %.17g\nmu %.17g\nnbw %d\n",
+                Usp, Uch, dblOcc, Sigma_inf, mu, nbw);
+        write(dir + "/vertex_rt.bin", vertex_rt_array, n8 * (nwmax + 1));
+        write(dir + "/self.bin", reinterpret_cast<double *>(Self_kw_array), 2 * n8 * (nbw / 2));
+        write(dir + "/sigma_inf2.bin", Sigma_inf2, n8);
+        write(dir + "/sigma_inf3.bin", Sigma_inf3, n8);
+        write(dir + "/sigma_inf4.bin", Sigma_inf4, n8);
+    }
+
+    void dump_cond(FILE *meta, const std::string &dir) {
+        fprintf(meta, "kx0 %.17g\n", kx0);
+        write(dir + "/chijj1.bin", chijj1_qn, nbw / 2 + 1);
+        write(dir + "/chijj2.bin", chijj2_qn, nbw / 2 + 1);
+    }
+
+private:
+    static void write(const std::string &path, const double *p, long n) {
+        if (!p) return;
+        FILE *f = fopen(path.c_str(), "wb");
+        if (!f) {
+            perror(path.c_str());
+            exit(2);
+        }
+        fwrite(p, sizeof(double), n, f);
+        fclose(f);
+    }
+};
+
+int main(int argc, char **argv) {
+    if (argc != 11) {
+        fprintf(stderr, "usage: %s OUTDIR MODE U tp tpp t3 n T nk0 Nw0\n", argv[0]);
+        return 1;
+    }
+    std::string dir = argv[1];
+    std::string mode = argv[2];
+    double U = atof(argv[3]), tp = atof(argv[4]), tpp = atof(argv[5]), t3 = atof(argv[6]);
+    double n = atof(argv[7]), T = atof(argv[8]);
+    int nk0 = atoi(argv[9]), Nw0 = atoi(argv[10]);
+    double params[] = {tp, tpp, t3, U};
+
+    mkdir(dir.c_str(), 0755);
+    std::string work = dir + "/work";
+    mkdir(work.c_str(), 0755);
+    char cwd[4096];
+    if (!getcwd(cwd, sizeof cwd)) return 2;
+    std::string absdir = dir[0] == '/' ? dir : std::string(cwd) + "/" + dir;
+    if (chdir(work.c_str())) return 2;
+
+    // capture the reference's stdout (it prints the sum-rule traces there)
+    std::stringstream captured;
+    std::streambuf *orig = std::cout.rdbuf(captured.rdbuf());
+    std::cout << std::setprecision(17);
+
+    double t0 = omp_get_wtime();
+    tpsc_probe *g = new tpsc_probe(nk0, Nw0, n, T, 0.1, params);
+    double t_ctor = omp_get_wtime() - t0;
+
+    FILE *meta = fopen((absdir + "/meta.txt").c_str(), "w");
+    fprintf(meta, "mode %s\nU %.17g\ntp %.17g\ntpp %.17g\nt3 %.17g\nn %.17g\nT %.17g\nnk0 %d\nNw0 %d\n",
+            mode.c_str(), U, tp, tpp, t3, n, T, nk0, Nw0);
+    fprintf(meta, "omp_threads %d\nt_ctor %.6f\n", omp_get_max_threads(), t_ctor);
+
+    if (mode == "chi0") {
+        g->set_keep_chirt(true);
+        t0 = omp_get_wtime();
+        g->calc_chiqw_FFT_spline(nk0, Nw0);
+        fprintf(meta, "t_chi0 %.6f\n", omp_get_wtime() - t0);
+        g->dump_chi0(meta, absdir);
+    } else if (mode == "solve" || mode == "cond") {
+        g->set_keep_chiqw(true);
+        t0 = omp_get_wtime();
+        g->calc_Self_FFT_spline();
+        double t_self = omp_get_wtime() - t0;
+        std::cout << std::setprecision(17);
+        t0 = omp_get_wtime();
+        g->traceSelfG();
+        double t_tr = omp_get_wtime() - t0;
+        std::cout << std::setprecision(17);
+        t0 = omp_get_wtime();
+        g->find_mu();
+        double t_mu = omp_get_wtime() - t0;
+        fprintf(meta, "t_self %.6f\nt_traceSelfG %.6f\nt_find_mu %.6f\n", t_self, t_tr, t_mu);
+        g->dump_chi0(meta, absdir);
+        g->dump_solve(meta, absdir);
+        if (mode == "cond") {
+            std::cout << std::setprecision(17);
+            t0 = omp_get_wtime();
+            g->calc_chijj_vertex_corr_all_optim(false, 3, 1, NULL, 0);
+            fprintf(meta, "t_cond %.6f\n", omp_get_wtime() - t0);
+            g->dump_cond(meta, absdir);
+        }
+    } else {
+        fprintf(stderr, "unknown mode %s\n", mode.c_str());
+        return 1;
+    }
+    fclose(meta);
+    delete g;
+
+    std::cout.rdbuf(orig);
+    FILE *log = fopen((absdir + "/stdout.txt").c_str(), "w");
+    std::string s = captured.str();
+    fwrite(s.data(), 1, s.size(), log);
+    fclose(log);
+    return 0;
+}

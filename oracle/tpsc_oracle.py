@@ -1,0 +1,672 @@
+"""CPU oracle for the TPSC hot path -- TEST INFRASTRUCTURE ONLY.
+
+This module is a plain numpy/scipy restatement of the reference algorithm
+(dbergeron1/TPSC_conductivity, C++), written from reading its sources.  Only
+``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg may
+import it, and only as the checker: the product (``tpsc_conductivity_b200``)
+never calls into it and fails loudly when its CUDA library is missing.
+
+Parity is pinned: ``tests/test_oracle_golden.py`` checks every function here
+against golden vectors produced by the unmodified reference sources compiled
+in this repository (``oracle/ref/Makefile`` -> ``oracle/_ref/tpsc_ref_probe``;
+fixtures and the script that made them live in ``tests/golden/``).
+
+Conventions follow the reference:
+  * lattice side ``nk0`` (L), quadrant side ``nbk = L/2+1``, octant index
+    ``m + l(l+1)/2`` with ``m <= l`` (src/chi0.cpp:341);
+  * ``Nw0`` = total fermionic frequency count, ``nw = Nw0/2+1`` bosonic
+    n >= 0 frequencies == tau nodes on [0, beta/2];
+  * 2D DCT-I == FFTW ``REDFT00`` on the nbk x nbk quadrant (unnormalised);
+  * FFT of the spline third derivative uses FFTW_BACKWARD, exp(+2 pi i jk/N).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.fft as sfft
+import scipy.linalg as sla
+
+EPS = np.finfo(np.float64).eps
+PI = math.acos(-1.0)
+
+
+# ----------------------------------------------------------------------------
+# lattice tables (src/hamiltonien.cpp)
+# ----------------------------------------------------------------------------
+def dispersion(nbk: int, tp: float, tpp: float, t3: float) -> np.ndarray:
+    """eps_k on the quadrant grid k = l pi/(nbk-1); ``ek[l, m]`` with l the kx
+    index (src/hamiltonien.cpp:358-375, dispk at :428-431)."""
+    k = np.arange(nbk) * PI / (nbk - 1)
+    kx = k[:, None]
+    ky = k[None, :]
+    return (-2.0 * (np.cos(kx) + np.cos(ky)) - 4.0 * tp * np.cos(kx) * np.cos(ky)
+            - 2.0 * tpp * (np.cos(2 * kx) + np.cos(2 * ky))
+            - 4 * t3 * (np.cos(2 * kx) * np.cos(ky) + np.cos(2 * ky) * np.cos(kx)))
+
+
+def octant_index(nbk: int):
+    """(l, m) arrays of the octant m <= l in storage order m + l(l+1)/2."""
+    ls, ms = [], []
+    for l in range(nbk):
+        for m in range(l + 1):
+            ls.append(l)
+            ms.append(m)
+    return np.array(ls), np.array(ms)
+
+
+def hopping_octant(nbk: int, tp: float, tpp: float, t3: float) -> np.ndarray:
+    """er[] = -t at octant sites (1,0),(1,1),(2,0),(2,1) (src/hamiltonien.cpp:17-30)."""
+    n8 = nbk * (nbk + 1) // 2
+    er = np.zeros(n8)
+    er[1] = -1.0
+    er[2] = -tp
+    er[3] = -tpp
+    er[4] = -t3
+    return er
+
+
+def octant_weights(nbk: int, base: int) -> np.ndarray:
+    """Multiplicity weights of octant points: ``base`` halved on the l or m
+    edges and on the diagonal (e.g. src/green0.cpp:193-196, src/chi.cpp:755-759)."""
+    l, m = octant_index(nbk)
+    w = np.full(l.shape, base, dtype=np.int64)
+    w = np.where((l == 0) | (l == nbk - 1), w // 2, w)
+    w = np.where((m == 0) | (m == nbk - 1), w // 2, w)
+    w = np.where(m == l, w // 2, w)
+    return w.astype(np.float64)
+
+
+def to_octant(full: np.ndarray) -> np.ndarray:
+    l, m = octant_index(full.shape[-1])
+    return full[..., l, m]
+
+
+def from_octant(oct_vals: np.ndarray, nbk: int) -> np.ndarray:
+    """Symmetric nbk x nbk array from octant values (the chir_tmp fill pattern
+    of src/chi0.cpp:349-358)."""
+    l, m = octant_index(nbk)
+    full = np.zeros(oct_vals.shape[:-1] + (nbk, nbk))
+    full[..., l, m] = oct_vals
+    full[..., m, l] = oct_vals
+    return full
+
+
+def dct2(full: np.ndarray) -> np.ndarray:
+    """2D DCT-I over the last two axes, FFTW REDFT00 x REDFT00 (unnormalised)."""
+    return sfft.dct(sfft.dct(full, type=1, axis=-1), type=1, axis=-2)
+
+
+# ----------------------------------------------------------------------------
+# root finder (src/generique.cpp:604-913 and the bounded variant :917-1234)
+# ----------------------------------------------------------------------------
+class RootNotFound(RuntimeError):
+    pass
+
+
+def _cdiv(a, b):
+    """IEEE division as C does it (x/0 -> +-inf or nan, no exception)."""
+    with np.errstate(all="ignore"):
+        return float(np.float64(a) / np.float64(b))
+
+
+def find_zero(func, init, lims=None):
+    """Bracketing inverse-quadratic / secant / bisection root search with the
+    reference's control flow: tol 1e-16 and 20 iterations
+    (src/generique.cpp:604-913); with ``lims`` the bounded variant, tol 1e-15,
+    12 iterations and eps = 2 machine epsilons (src/generique.cpp:917-1234).
+    Returns (root, number_of_evaluations)."""
+    if lims is None:
+        tol, tol2, eps, itmax = 1.0e-16, 1.0e-10, 10.0 * EPS, 20
+    else:
+        tol, tol2, eps, itmax = 1.0e-15, 1.0e-10, 2.0 * EPS, 12
+    nev = [0]
+
+    def f(x):
+        nev[0] += 1
+        return func(x)
+
+    nbiter = 0
+    dytol = 0.01
+    x0, xmin, xmax = init
+    ymin = f(xmin)
+    ymax = f(xmax)
+    x = [x0, xmin, xmax]
+    y = [0.0, ymin, ymax]
+    if abs(ymin) < tol:
+        return xmin, nev[0]
+    if abs(ymax) < tol:
+        return xmax, nev[0]
+    if ymin * ymax > 0:
+        y[0] = f(x[0])
+        if abs(y[0]) < tol:
+            return x[0], nev[0]
+        if y[0] * y[2] < 0:
+            xtmp = x[0]
+            x[0] = (x[0] + x[2]) / 2
+            x[1] = xtmp
+            y[1] = y[0]
+        else:
+            ytmp = y[0]
+            xtmp = x[0]
+            if abs(y[1]) < abs(ytmp):
+                ytmp, xtmp = y[1], x[1]
+            if abs(y[2]) < abs(ytmp):
+                ytmp, xtmp = y[2], x[2]
+            xtmp1 = xtmp + 10 * eps
+            ytmp1 = f(xtmp1)
+            xtmp1 = xtmp - ytmp * _cdiv(xtmp1 - xtmp, ytmp1 - ytmp)
+            ytmp1 = f(xtmp1)
+            nbiter += 1
+            while abs(ytmp1) > tol and nbiter < itmax and ytmp1 * ytmp > 0 and math.isfinite(xtmp1):
+                xtmp, ytmp = xtmp1, ytmp1
+                xtmp1 = xtmp + 10 * eps
+                ytmp1 = f(xtmp1)
+                xtmp1 = xtmp - ytmp * _cdiv(xtmp1 - xtmp, ytmp1 - ytmp)
+                ytmp1 = f(xtmp1)
+                nbiter += 1
+            if abs(ytmp1) < tol:
+                return xtmp1, nev[0]
+            if ytmp1 * ytmp < 0:
+                x[0] = (xtmp + xtmp1) / 2
+                x[1], y[1] = xtmp, ytmp
+                x[2], y[2] = xtmp1, ytmp1
+            if nbiter >= itmax:
+                raise RootNotFound("iteration limit in the secant search")
+            if not math.isfinite(xtmp1):
+                raise RootNotFound("non-finite iterate")
+    if lims is not None:
+        if x[1] < lims[0] or x[1] > lims[1] or x[2] < lims[0] or x[2] > lims[1]:
+            raise RootNotFound("no root inside the limits")
+    if abs(xmax - xmin) < eps:
+        return xmin, nev[0]
+    y[0] = f(x[0])
+    if abs(y[0]) < tol:
+        return x[0], nev[0]
+
+    def classify():
+        if y[0] * y[1] > 0:
+            i1, i2 = 0, 1
+        elif y[0] * y[2] > 0:
+            i1, i2 = 0, 2
+        else:
+            i1, i2 = 1, 2
+        i3 = 3 - i1 - i2
+        if x[i3] > x[i1]:
+            if x[i1] > x[i2]:
+                far, mid = i2, i1
+            else:
+                far, mid = i1, i2
+            im, ip = mid, i3
+        else:
+            if x[i1] < x[i2]:
+                far, mid = i2, i1
+            else:
+                far, mid = i1, i2
+            im, ip = i3, mid
+        return i3, far, mid, im, ip
+
+    i3, far, mid, _, _ = classify()
+    x[far] = -y[mid] * _cdiv(x[i3] - x[mid], y[i3] - y[mid]) + x[mid]
+    y[far] = f(x[far])
+    dy = y[far]
+    a = b = c = 0.0
+    while abs(dy) > tol and nbiter < itmax:
+        i3, far, mid, im, ip = classify()
+        denom = (-x[0] * x[0] * x[2] + x[0] * x[0] * x[1] - x[0] * x[1] * x[1]
+                 + x[0] * x[2] * x[2] - x[2] * x[2] * x[1] + x[2] * x[1] * x[1])
+        if abs(denom) > 0.0:
+            a = (x[0] * y[2] - x[0] * y[1] + x[2] * y[1] - y[2] * x[1] - y[0] * x[2] + y[0] * x[1]) / denom
+            b = -(-y[2] * x[1] * x[1] + x[1] * x[1] * y[0] - x[2] * x[2] * y[0] - y[1] * x[0] * x[0]
+                  + y[2] * x[0] * x[0] + y[1] * x[2] * x[2]) / denom
+            c = (y[2] * x[0] * x[0] * x[1] - y[1] * x[0] * x[0] * x[2] - x[1] * x[1] * x[0] * y[2]
+                 + x[2] * x[2] * x[0] * y[1] + x[1] * x[1] * y[0] * x[2] - x[2] * x[2] * y[0] * x[1]) / denom
+        if (b * b - 4.0 * a * c) > 0.0 and abs(denom) > 0.0:
+            sq = math.sqrt(b * b - 4.0 * a * c)
+            xp = _cdiv(-b + sq, 2 * a)
+            xm = _cdiv(-b - sq, 2 * a)
+            if x[im] < xp < x[ip]:
+                x[far] = xp
+            elif x[im] < xm < x[ip]:
+                x[far] = xm
+            elif abs(y[i3] - y[mid]) > tol:
+                x[far] = -y[mid] * (x[i3] - x[mid]) / (y[i3] - y[mid]) + x[mid]
+            else:
+                return x[mid], nev[0]
+        else:
+            if abs(y[i3] - y[mid]) > tol:
+                x[far] = -y[mid] * (x[i3] - x[mid]) / (y[i3] - y[mid]) + x[mid]
+            else:
+                return x[mid], nev[0]
+        y[far] = f(x[far])
+        dyprec = abs(dy)
+        dy = y[far]
+        if abs(dyprec - abs(dy)) < dytol * dyprec or dyprec < abs(dy):
+            x[far] = (x[i3] + x[mid]) / 2.0
+            y[far] = f(x[far])
+            dy = y[far]
+        nbiter += 1
+    best = 0
+    root = x[0]
+    if abs(y[1]) < abs(y[best]):
+        root = x[1]
+        best = 1
+    if abs(y[2]) < abs(y[best]):
+        root = x[2]
+    return root, nev[0]
+
+
+# ----------------------------------------------------------------------------
+# clamped cubic spline on a uniform grid (src/generique.cpp:214-322)
+# ----------------------------------------------------------------------------
+def clamped_spline(V: np.ndarray, h: float, d0, dN):
+    """Clamped cubic spline through V[0..N] (axis 0; extra axes are independent
+    columns) with end slopes d0, dN.  Returns (a, b, c, d) per interval with
+    S_j(x) = a (x-x_j)^3 + b (x-x_j)^2 + c (x-x_j) + d, the layout of
+    generique::spline_coeffs_rel (src/generique.cpp:214-322).  The reference
+    solves the 3N-1 banded system for (a,b,c) with LAPACK dgbsv; this restates
+    the same interpolant through the node second derivatives M_j (tridiagonal
+    1-4-1 system with clamped end rows), which is algebraically identical."""
+    V = np.asarray(V, dtype=np.float64)
+    N = V.shape[0] - 1
+    rhs = np.empty_like(V)
+    rhs[1:N] = 6.0 / (h * h) * (V[2:] - 2.0 * V[1:N] + V[:N - 1])
+    rhs[0] = 6.0 / h * ((V[1] - V[0]) / h - d0)
+    rhs[N] = 6.0 / h * (dN - (V[N] - V[N - 1]) / h)
+    ab = np.zeros((3, N + 1))
+    ab[0, 1:] = 1.0
+    ab[1, :] = 4.0
+    ab[1, 0] = 2.0
+    ab[1, N] = 2.0
+    ab[2, :-1] = 1.0
+    M = sla.solve_banded((1, 1), ab, rhs.reshape(N + 1, -1)).reshape(V.shape)
+    a = (M[1:] - M[:-1]) / (6.0 * h)
+    b = M[:-1] / 2.0
+    c = (V[1:] - V[:-1]) / h - h * (2.0 * M[:-1] + M[1:]) / 6.0
+    d = V[:-1]
+    return a, b, c, d
+
+
+# ----------------------------------------------------------------------------
+# green0: mu0 on the finite lattice (src/green0.cpp:182-203, 240-262)
+# ----------------------------------------------------------------------------
+def mu0_finite(ek: np.ndarray, n: float, T: float, tp=0.0, tpp=0.0):
+    if n == 1.0 and tp == 0 and tpp == 0:
+        return 0.0
+    nbk = ek.shape[0]
+    w = octant_weights(nbk, 8)
+    eo = to_octant(ek)
+    nk2 = 4 * (nbk - 1) * (nbk - 1)
+
+    def dens(mup):
+        return float(np.sum(2 * w / ((np.exp((eo - mup) / T) + 1.0) * nk2))) - n
+
+    root, _ = find_zero(dens, (0.0, -8.0, 8.0))
+    return root
+
+
+# ----------------------------------------------------------------------------
+# chi0 (src/chi0.cpp:279-718)
+# ----------------------------------------------------------------------------
+@dataclass
+class Chi0Result:
+    chiqw: np.ndarray          # [nw, N8]  chi0(q, iqn), n = 0..Nw0/2
+    chirt: np.ndarray          # [nw, N8]  chi0(r, tau_j)
+    chi0_inf: np.ndarray       # [N8]      coefficient of 1/qn^2
+    chi0_inf2: np.ndarray      # [N8]      coefficient of 1/qn^4
+    dtau_chirt0: np.ndarray    # [N8]      d/dtau chi0(r, 0)
+    dtau_Grt0p: np.ndarray     # [N8]      d/dtau G(r, 0+)
+    dtau_chiqt0: np.ndarray    # [N8]      d/dtau chi0(q, 0)
+    chi0max: float
+    qmax: tuple
+
+
+def chi0_fft_spline(ek: np.ndarray, mu0: float, T: float, er: np.ndarray, nw0: int) -> Chi0Result:
+    """chi0::calc_chiqw_FFT_spline (src/chi0.cpp:279-718)."""
+    nk = ek.shape[0]
+    nq0 = 2 * (nk - 1)
+    nk02 = float(nq0 * nq0)
+    nw = nw0 // 2 + 1
+    n8 = nk * (nk + 1) // 2
+    beta = 1.0 / T
+    ekmu = to_octant(ek) - mu0                                   # :341
+    Gkt = -1.0 / (np.exp(-ekmu / T) + 1.0)                       # :342
+
+    # d/dtau G(r, 0-) and d/dtau G(r, 0+) (:323-367)
+    dG0m = er.copy()
+    dG0m[0] = -mu0
+    tmp = to_octant(dct2(from_octant(-ekmu * Gkt / nk02, nk)))
+    dG0m = dG0m - tmp
+    dG0p = tmp
+
+    # G(r, 0+) and chi0(r, 0) (:375-418)
+    G0 = to_octant(dct2(from_octant(Gkt / nk02, nk)))
+    chir = -2.0 * G0 * G0
+    chir[0] = -2.0 * G0[0] * (G0[0] + 1.0)
+    chirt = np.empty((nw, n8))
+    chiqt = np.empty((nw, n8))
+    chirt[0] = chir
+    chiqt[0] = to_octant(dct2(from_octant(chir, nk)))
+
+    # d/dtau chi0(r, 0) (:424-447)
+    dchir = -2.0 * (dG0p * G0 + dG0m * G0)
+    dchir[0] = -2.0 * (dG0p[0] * (1.0 + G0[0]) + dG0m[0] * G0[0])
+    dtau_chiqt0 = to_octant(dct2(from_octant(dchir, nk)))
+
+    # 0 < tau < beta/2 (:454-519)
+    pos = ekmu >= 0.0
+    ex = np.exp(ekmu / T)
+    for j in range(1, nw - 1):
+        t = j / (nw0 * T)
+        gp = np.where(pos, np.exp(-t * ekmu) * Gkt / nk02,
+                      -np.exp((beta - t) * ekmu) / (ex + 1.0) / nk02)
+        gm = np.where(pos, -np.exp((t - beta) * ekmu) * Gkt / nk02,
+                      np.exp(t * ekmu) / ((ex + 1.0) * nk02))
+        Gp = to_octant(dct2(from_octant(gp, nk)))
+        Gm = to_octant(dct2(from_octant(gm, nk)))
+        chir = -2.0 * Gm * Gp
+        chirt[j] = chir
+        chiqt[j] = to_octant(dct2(from_octant(chir, nk)))
+    # tau = beta/2 (:527-559)
+    j = nw - 1
+    t = 1.0 / (2.0 * T)
+    gp = np.where(pos, np.exp(-t * ekmu) * Gkt / nk02,
+                  -np.exp((beta - t) * ekmu) / ((ex + 1.0) * nk02))
+    Gp = to_octant(dct2(from_octant(gp, nk)))
+    chir = 2.0 * Gp * Gp
+    chirt[j] = chir
+    chiqt[j] = to_octant(dct2(from_octant(chir, nk)))
+
+    # per q: clamped spline along tau, FFT of 6 a_j, tails (:586-690)
+    h = 1.0 / (nw0 * T)
+    a, b, c, d = clamped_spline(chiqt, h, dtau_chiqt0, np.zeros(n8))
+    f = np.empty((nw0, n8))
+    f[: nw0 // 2] = 6.0 * a
+    f[nw0 // 2:] = -f[: nw0 // 2][::-1]
+    F = np.fft.ifft(f, axis=0) * nw0                            # FFTW_BACKWARD
+    x = h
+    integ = np.sum(a * x ** 4 / 4.0 + b * x ** 3 / 3.0 + c * x ** 2 / 2.0 + d * x, axis=0)
+    chiqw = np.empty((nw, n8))
+    chiqw[0] = 2 * integ
+    chi0_inf = -2.0 * dtau_chiqt0
+    jj = np.arange(1, nw)[:, None]
+    wn = 2 * jj * PI * T
+    th = 2 * jj * PI / nw0
+    chiqw[1:] = chi0_inf / (wn * wn) + ((1.0 - np.cos(th)) * F[1:nw].real
+                                        + np.sin(th) * F[1:nw].imag) / (wn ** 4)
+    chi0_inf2 = 2.0 * F[nw - 1].real
+    chi0_inf[0] = 0.0
+    chi0_inf2[0] = 0.0
+    chiqw[1:, 0] = 0.0
+
+    # chi0max and its wave vector (:703-717): scan l down, m down, strict >
+    chi0max = 0.0
+    qmax = (0, 0)
+    for l in range(nk - 1, -1, -1):
+        for m in range(l, -1, -1):
+            v = chiqw[0, m + l * (l + 1) // 2]
+            if v > chi0max:
+                chi0max = v
+                qmax = (l, m)
+    return Chi0Result(chiqw, chirt, chi0_inf, chi0_inf2, dchir, dG0p, dtau_chiqt0, chi0max, qmax)
+
+
+def trace_chi0(r: Chi0Result, n: float, T: float):
+    """chi0::traceChi0 (src/chi0.cpp:1498-1584) -> (raw trace, extrapolated)."""
+    nw, n8 = r.chiqw.shape
+    nk = int(round((math.sqrt(8 * n8 + 1) - 1) / 2))
+    nwmax = nw - 1
+    Nq = 4 * (nk - 1) ** 2
+    w = octant_weights(nk, 16)
+    wj = np.ones(nw)
+    wj[0] = 0.5
+    wj[nwmax] = 0.5
+    tr1 = float(np.sum(wj[:, None] * w[None, :] * T * r.chiqw / Nq))
+    jj = np.arange(nwmax + 1, 2 * nwmax)[:, None]
+    wn = 2 * PI * jj * T
+    c = r.chi0_inf / (wn * wn) + r.chi0_inf2 / wn ** 4
+    tr = tr1 + float(np.sum(w * T * c / Nq))
+    N1 = nwmax + 1
+    tr_corr = tr + N1 * (tr1 - tr) / (N1 - 2 * nwmax)
+    return tr, tr_corr
+
+
+# ----------------------------------------------------------------------------
+# chi: sum rules and Usp, Uch (src/chi.cpp:738-876, 210-371)
+# ----------------------------------------------------------------------------
+def trace_diff_chi(r: Chi0Result, Uv: float, sign: float, T: float) -> float:
+    """traceDiffChispChi0 (sign=-1) / traceDiffChichChi0 (sign=+1)
+    (src/chi.cpp:738-830): sum of chi0/(1 + sign*U chi0/2) - chi0, stored
+    frequencies n <= Nw0/2 plus tails Nw0/2 < n <= Nw0."""
+    nw, n8 = r.chiqw.shape
+    nk = int(round((math.sqrt(8 * n8 + 1) - 1) / 2))
+    nwmax = nw - 1
+    Nq = 4 * (nk - 1) ** 2
+    w = octant_weights(nk, 16)
+    jj = np.arange(nwmax + 1, 2 * nwmax + 1)[:, None]
+    wn = 2 * jj * PI * T
+    c = r.chi0_inf / (wn * wn) + r.chi0_inf2 / (wn * wn * wn * wn)
+    tail = np.sum(w * T / Nq * (c / (1 + sign * Uv * c / 2.0) - c))
+    wj = np.ones(nw)
+    wj[0] = 0.5
+    c = r.chiqw
+    main = np.sum(wj[:, None] * w[None, :] * T / Nq * (c / (1 + sign * Uv * c / 2.0) - c))
+    return float(main + tail)
+
+
+@dataclass
+class UResult:
+    Usp: float
+    Uch: float
+    dblOcc: float
+    evals_sp: int
+    evals_ch: int
+
+
+def find_Usp_Uch(r: Chi0Result, U: float, n: float, T: float) -> UResult:
+    """chi::find_Usp_Uch(nq0, nw0, Usc) on one grid (src/chi.cpp:846-876) and
+    the double occupancy ansatz (src/chi.cpp:370-371)."""
+    nsr = 2.0 - n if n > 1.0 else n
+
+    def rsp(Us):
+        return trace_diff_chi(r, Us, -1.0, T) + n - n * n / 2.0 - nsr + Us * nsr * nsr / (2.0 * U)
+
+    Usp, ev1 = find_zero(rsp, (U / 2.0, 0.0, 2.0 / r.chi0max - 2 * EPS))
+
+    def rch(Uc):
+        return trace_diff_chi(r, Uc, 1.0, T) + n - n * n / 2.0 - (nsr + Usp * nsr * nsr / (2.0 * U) - nsr * nsr)
+
+    Uch, ev2 = find_zero(rch, (0.0, 0.0, 1000.0 * U))
+    if n > 1.0:
+        D = Usp / U * nsr * nsr / 4.0 + 1.0 - nsr
+    else:
+        D = Usp / U * nsr * nsr / 4.0
+    return UResult(Usp, Uch, D, ev1, ev2)
+
+
+def vertex_rt(r: Chi0Result, U: float, Usp: float, Uch: float, T: float) -> np.ndarray:
+    """chi::calc_chirt (src/chi.cpp:37-170): V(r, tau_j), j = 0..Nw0/2."""
+    nw, n8 = r.chiqw.shape
+    nk = int(round((math.sqrt(8 * n8 + 1) - 1) / 2))
+    nq0 = 2 * (nk - 1)
+    normFact = T / (nq0 * nq0)
+    c0 = r.chiqw
+    csp = c0 / (1.0 - Usp * c0 / 2.0)
+    cch = c0 / (1.0 + Uch * c0 / 2.0)
+    vq = normFact * U * (3.0 * Usp * (csp - c0) + Uch * (cch - c0)) / 8.0
+    vr = to_octant(dct2(from_octant(vq, nk)))
+    vr = sfft.dct(vr, type=1, axis=0)
+    return vr + U * (3.0 * Usp + Uch) / 8.0 * r.chirt
+
+
+# ----------------------------------------------------------------------------
+# green: self-energy (src/green.cpp:1673-2025)
+# ----------------------------------------------------------------------------
+@dataclass
+class SelfResult:
+    S: np.ndarray            # [Nw0/2, N8] complex: coefficient of 1/z^4
+    Sigma_inf: float         # coefficient of 1/z (k-independent)
+    Sigma_inf2: np.ndarray   # [N8] coefficient of 1/z^2
+    Sigma_inf3: np.ndarray   # [N8] coefficient of 1/z^3
+    Sigma_inf4: np.ndarray   # [N8] Re S at the last stored frequency
+    sigma_tau: np.ndarray = field(repr=False, default=None)   # [Nw0+1, N8]
+
+    def sigma(self, T: float) -> np.ndarray:
+        """Full Sigma(k, i w_n) for n < Nw0/2 (src/green.cpp:3039)."""
+        nj = self.S.shape[0]
+        z = 1j * (2 * np.arange(nj)[:, None] + 1) * PI * T
+        return (self.Sigma_inf / z + self.Sigma_inf2 / (z * z) + self.Sigma_inf3 / (z * z * z)
+                + self.S / (z * z * z * z))
+
+
+def self_energy(ek, mu0, T, er, r: Chi0Result, V: np.ndarray, U, Usp, Uch, nbw) -> SelfResult:
+    """green::calc_Self_FFT_spline, stages after calc_chirt (src/green.cpp:1741-2025)."""
+    nk = ek.shape[0]
+    nk0 = 2 * (nk - 1)
+    nk02 = float(nk0 * nk0)
+    n8 = nk * (nk + 1) // 2
+    nw = nbw // 2 + 1
+    ekmu = ek - mu0
+    fact = U * (3.0 * Usp + Uch) / 8.0
+
+    # d/dtau Sigma(k, 0) and d/dtau Sigma(k, beta) (:1745-1817)
+    g = to_octant(dct2(-1.0 / (np.exp(-ekmu / T) + 1.0) / nk02))
+    s0 = (fact * r.dtau_chirt0) * g + V[0] * r.dtau_Grt0p
+    d0 = to_octant(dct2(from_octant(s0, nk)))
+    g = to_octant(dct2(-1.0 / (np.exp(ekmu / T) + 1.0) / nk02))
+    xi = er.copy()
+    xi[0] = -mu0
+    sb = (-fact * r.dtau_chirt0) * g + V[0] * (-r.dtau_Grt0p + xi)
+    dN = to_octant(dct2(from_octant(sb, nk)))
+
+    # Sigma(k, tau_j), j = 0..Nw0 (:1822-1885)
+    st = np.empty((nbw + 1, n8))
+    pos = ekmu > 0
+    e1 = np.exp(-ekmu / T) + 1.0
+    e2 = np.exp(ekmu / T) + 1.0
+    for j in range(nbw + 1):
+        t = j / (nbw * T)
+        gk = np.where(pos, -np.exp(-t * ekmu) / e1 / nk02, -np.exp((1.0 / T - t) * ekmu) / e2 / nk02)
+        gr = to_octant(dct2(gk))
+        vr = V[j] if j < nw else V[nbw - j]
+        st[j] = to_octant(dct2(from_octant(gr * vr, nk)))
+
+    # per k: spline over [0, beta], FFT, tails (:1935-2017)
+    h = 1.0 / (nbw * T)
+    a, b, c, d = clamped_spline(st, h, d0, dN)
+    d2S0 = 2 * b[0]
+    d2Sb = 6.0 * a[nbw - 1] / (nbw * T) + 2.0 * b[nbw - 1]
+    jj = np.arange(nbw)[:, None]
+    f = np.exp(1j * jj * PI / nbw) * 6.0 * a
+    F = np.fft.ifft(f, axis=0) * nbw
+    coeff1 = st[0] + st[nbw]
+    Sigma_inf = float(-coeff1[0])
+    S2 = d0 + dN
+    S3 = -(d2S0 + d2Sb)
+    jh = np.arange(nbw // 2)[:, None]
+    S = (1.0 - np.exp(1j * (2 * jh + 1) * PI / nbw)) * F[: nbw // 2]
+    S4 = S[nbw // 2 - 1].real.copy()
+    return SelfResult(S, Sigma_inf, S2, S3, S4, st)
+
+
+def _sigma_parts(sr: SelfResult, T: float):
+    sig = sr.sigma(T)
+    return sig.real, sig.imag
+
+
+def trace_self_G(ek, mu0, sr: SelfResult, T: float):
+    """green::traceSelfG (src/green.cpp:3001-3089) -> (sum, sum + asymptotic)."""
+    nk = ek.shape[0]
+    nk02 = 4 * (nk - 1) ** 2
+    w = octant_weights(nk, 8)
+    eo = to_octant(ek)
+    nj = sr.S.shape[0]
+    wn = (2 * np.arange(nj)[:, None] + 1) * PI * T
+    rS, iS = _sigma_parts(sr, T)
+    tmp = w * T * 2 / (nk02 * (wn * wn + (eo - mu0) ** 2))
+    s = float(np.sum(tmp * (rS * (mu0 - eo) + iS * wn)))
+    s2 = float(np.sum(w * sr.Sigma_inf * T * 2 / (nk02 * (wn * wn + (eo - mu0) ** 2))))
+    x = eo - mu0
+    big = np.abs(x) > 1.0e-12
+    ek_ = np.where(x < 0, np.exp(x / T), np.exp(-x / T))
+    s2 += float(np.sum(np.where(big, w * sr.Sigma_inf * (1.0 / (np.exp(x / T) + 1.0) - 0.5) / np.where(big, x, 1.0) / nk02,
+                                -w * sr.Sigma_inf * ek_ / ((ek_ + 1.0) * (ek_ + 1.0) * nk02 * T))))
+    return s, s + s2
+
+
+def trace_diff_G(ek, mu0, sr: SelfResult, T: float, pmu: float) -> float:
+    """green::traceDiffG (src/green.cpp:3108-3182): Tr(G - G0) at chemical
+    potential pmu, stored frequencies plus the analytic tail up to j = Nw0."""
+    nk = ek.shape[0]
+    w = octant_weights(nk, 16)
+    eo = to_octant(ek)
+    nj = sr.S.shape[0]
+    nbw = 2 * nj
+    jt = np.arange(nbw // 2, nbw + 1)[:, None]
+    wn = (2 * jt + 1) * PI * T
+    rS = -sr.Sigma_inf2 / (wn * wn) + sr.Sigma_inf4 / (wn * wn * wn * wn)
+    iS = -sr.Sigma_inf / wn + sr.Sigma_inf3 / (wn * wn * wn)
+    tmp = w / (((wn - iS) ** 2 + (eo - pmu + rS) ** 2) * (wn * wn + (eo - mu0) ** 2))
+    s1 = np.sum(tmp * ((mu0 - pmu + rS) * (eo - pmu + rS) * (eo - mu0) + iS * (iS - 2 * wn) * (eo - mu0)
+                       - wn * wn * (mu0 - pmu + rS)))
+    wn = (2 * np.arange(nj)[:, None] + 1) * PI * T
+    rS, iS = _sigma_parts(sr, T)
+    tmp = w / (((wn - iS) ** 2 + (eo - pmu + rS) ** 2) * (wn * wn + (eo - mu0) ** 2))
+    s = np.sum(tmp * ((mu0 - pmu + rS) * (eo - pmu + rS) * (eo - mu0) + iS * (iS - 2 * wn) * (eo - mu0)
+                      - wn * wn * (mu0 - pmu + rS)))
+    return float(s + s1)
+
+
+def find_mu(ek, mu0, sr: SelfResult, T: float):
+    """green::find_mu (src/green.cpp:3185-3259)."""
+    return find_zero(lambda m: trace_diff_G(ek, mu0, sr, T, m), (0.0, -10.0, 10.0), lims=(-20.0, 20.0))
+
+
+def trace_self_G2(ek, mu, sr: SelfResult, T: float, U: float, n: float):
+    """green::traceSelfG2 (src/green.cpp:2929-2980) -> (trace, double occupancy)."""
+    nk = ek.shape[0]
+    nk02 = 4 * (nk - 1) ** 2
+    w = octant_weights(nk, 8)
+    eo = to_octant(ek)
+    nj = sr.S.shape[0]
+    wn = (2 * np.arange(nj)[:, None] + 1) * PI * T
+    rS, iS = _sigma_parts(sr, T)
+    tmp = w * T * 2 / (nk02 * ((wn - iS) ** 2 + (eo - mu + rS) ** 2))
+    s = float(np.sum(tmp * (iS * wn - iS * iS - (eo - mu) * rS - rS * rS)))
+    return s, (s + U * n * n / 4.0) / U
+
+
+# ----------------------------------------------------------------------------
+# one full solve in the reference's order (src/tpsc_main.cpp:61-75)
+# ----------------------------------------------------------------------------
+@dataclass
+class Solve:
+    nk0: int
+    Nw0: int
+    mu0: float
+    chi0: Chi0Result
+    U: UResult
+    V: np.ndarray
+    sigma: SelfResult
+    mu: float
+    trace_self_G: tuple
+    trace_self_G2: tuple
+
+
+def solve(U, tp, tpp, t3, n, T, nk0, Nw0) -> Solve:
+    """Full-grid TPSC solve: chi0 -> Usp, Uch -> V(r,tau) -> Sigma -> mu.  The
+    reference's half-grid Usp/Uch pre-pass (src/chi.cpp:285-297) only feeds the
+    difRel diagnostics, so it is not part of the solve."""
+    nbk = nk0 // 2 + 1
+    ek = dispersion(nbk, tp, tpp, t3)
+    er = hopping_octant(nbk, tp, tpp, t3)
+    mu0 = mu0_finite(ek, n, T, tp, tpp)
+    c0 = chi0_fft_spline(ek, mu0, T, er, Nw0)
+    ur = find_Usp_Uch(c0, U, n, T)
+    V = vertex_rt(c0, U, ur.Usp, ur.Uch, T)
+    sr = self_energy(ek, mu0, T, er, c0, V, U, ur.Usp, ur.Uch, Nw0)
+    tsg = trace_self_G(ek, mu0, sr, T)
+    mu, _ = find_mu(ek, mu0, sr, T)
+    tsg2 = trace_self_G2(ek, mu, sr, T, U, n)
+    return Solve(nk0, Nw0, mu0, c0, ur, V, sr, mu, tsg, tsg2)

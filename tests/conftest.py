@@ -1,0 +1,37 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+    config.addinivalue_line("markers", "slow: CPU test that takes more than a few seconds")
+
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def load_golden(name):
+    import numpy as np
+
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    d = {k: z[k] for k in z.files}
+    names = [str(s) for s in d["scalars_names"]]
+    d["s"] = dict(zip(names, d["scalars"].tolist()))
+    U, tp, tpp, t3, n, T, nk0, Nw0 = d["params"].tolist()
+    d["p"] = dict(U=U, tp=tp, tpp=tpp, t3=t3, n=n, T=T, nk0=int(nk0), Nw0=int(Nw0))
+    return d
+
+
+def golden_names():
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+
+
+@pytest.fixture
+def golden():
+    return load_golden

@@ -1,0 +1,122 @@
+"""Regenerate the golden fixtures in this folder from the reference itself.
+
+Runs ``oracle/_ref/tpsc_ref_probe`` -- the UNMODIFIED reference sources
+compiled by ``oracle/ref/Makefile`` (``make -C oracle/ref``) -- on a set of
+small lattices and stores what it computed as ``<name>.npz``.  Needs the
+reference checkout to build the probe; the fixtures themselves travel with the
+repository and are all the tests read.
+
+usage: python tests/golden/make_golden.py [--threads 8] [--only name ...]
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+PROBE = os.path.join(ROOT, "oracle", "_ref", "tpsc_ref_probe")
+
+# name: (mode, U, tp, tpp, t3, n, T, nk0, Nw0, keep_full_arrays)
+CASES = {
+    # tiny lattice, half-grid pre-pass exercised, conductivity too
+    "l16_w64_u2": ("cond", 2.0, 0.0, 0.0, 0.0, 0.875, 0.25, 16, 64, True),
+    # the 32x32 plain-TPSC case: t'=0, U=2, n=0.875, T=0.25, 256 positive iwn
+    "l32_w512_u2": ("cond", 2.0, 0.0, 0.0, 0.0, 0.875, 0.25, 32, 512, True),
+    # next-nearest and third-neighbour hoppings
+    "l32_w256_u4_tp": ("cond", 4.0, -0.15, 0.05, 0.02, 0.875, 0.1, 32, 256, True),
+    # electron doping n > 1 (nsr = 2 - n branch, src/chi.cpp:18, 370)
+    "l16_w128_n110": ("cond", 3.0, -0.2, 0.1, 0.0, 1.1, 0.2, 16, 128, True),
+    # half filling, particle-hole symmetric: mu0 = 0 shortcut (src/green0.cpp:18-23)
+    "l16_w64_half": ("cond", 2.0, 0.0, 0.0, 0.0, 1.0, 0.3, 16, 64, True),
+    # larger lattice, lower temperature
+    "l64_w1024_u4": ("solve", 4.0, -0.15, 0.0, 0.0, 0.875, 0.05, 64, 1024, False),
+    # the 256x256, 2048 positive iwn case: scalars and sampled columns only
+    "l256_w4096_u4": ("solve", 4.0, -0.15, 0.0, 0.0, 0.875, 0.05, 256, 4096, False),
+}
+
+
+def read_meta(path):
+    meta = {}
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 2:
+                meta[parts[0]] = parts[1]
+    return meta
+
+
+def run_case(name, spec, threads):
+    mode, U, tp, tpp, t3, n, T, nk0, Nw0, full = spec
+    with tempfile.TemporaryDirectory() as d:
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        args = [PROBE, d, mode] + [repr(v) for v in (U, tp, tpp, t3, n, T)] + [str(nk0), str(Nw0)]
+        subprocess.run(args, check=True, env=env)
+        meta = read_meta(os.path.join(d, "meta.txt"))
+        nbk = nk0 // 2 + 1
+        n8 = nbk * (nbk + 1) // 2
+        nw = Nw0 // 2 + 1
+
+        def rd(fname, shape=None, cplx=False):
+            a = np.fromfile(os.path.join(d, fname), dtype=np.float64)
+            if cplx:
+                a = a[0::2] + 1j * a[1::2]
+            return a.reshape(shape) if shape else a
+
+        out = {
+            "params": np.array([U, tp, tpp, t3, n, T, nk0, Nw0], dtype=np.float64),
+            "scalars_names": np.array(["mu0", "chi0max", "qmax0", "qmax1", "Usp", "Uch", "dblOcc",
+                                       "Sigma_inf", "mu"]),
+            "scalars": np.array([float(meta[k]) for k in ["mu0", "chi0max", "qmax0", "qmax1", "Usp",
+                                                         "Uch", "dblOcc", "Sigma_inf", "mu"]]),
+            "chi0_inf": rd("chi0_inf.bin"),
+            "chi0_inf2": rd("chi0_inf2.bin"),
+            "dtau_chirt0": rd("dtau_chirt0.bin"),
+            "sigma_inf2": rd("sigma_inf2.bin"),
+            "sigma_inf3": rd("sigma_inf3.bin"),
+            "sigma_inf4": rd("sigma_inf4.bin"),
+            "ref_seconds": np.array([float(meta.get(k, 0.0)) for k in
+                                     ["t_self", "t_traceSelfG", "t_find_mu"]]),
+            "ref_threads": np.array(int(meta["omp_threads"])),
+        }
+        chiqw = rd("chiqw.bin", (nw, n8))
+        V = rd("vertex_rt.bin", (nw, n8))
+        S = rd("self.bin", (Nw0 // 2, n8), cplx=True)
+        if full:
+            out["chiqw"] = chiqw
+            out["vertex_rt"] = V
+            out["self"] = S
+        else:
+            cols = np.unique(np.linspace(0, n8 - 1, 12).astype(np.int64))
+            out["cols"] = cols
+            out["chiqw_cols"] = chiqw[:, cols]
+            out["vertex_rt_cols"] = V[:, cols]
+            out["self_cols"] = S[:, cols]
+            out["chiqw_w0"] = chiqw[0]
+        if mode == "cond":
+            out["kx0"] = np.array(float(meta["kx0"]))
+            out["chijj1"] = rd("chijj1.bin")
+            out["chijj2"] = rd("chijj2.bin")
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        print(name, "done", {k: meta.get(k) for k in ("Usp", "Uch", "mu")})
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--threads", type=int, default=os.cpu_count())
+    ap.add_argument("--only", nargs="*")
+    a = ap.parse_args()
+    if not os.path.exists(PROBE):
+        raise SystemExit("build the reference probe first: make -C oracle/ref")
+    for name, spec in CASES.items():
+        if a.only and name not in a.only:
+            continue
+        run_case(name, spec, a.threads)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,84 @@
+"""Pin the numpy oracle to the reference: every golden fixture was produced by
+the unmodified reference sources (tests/golden/make_golden.py); the oracle must
+reproduce them.  Tolerances are relative to the array's max magnitude; the
+reference's own run-to-run noise (OpenMP reduction order) is ~1e-12 on Usp,
+Uch and mu at L=256."""
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden
+from oracle import tpsc_oracle as O
+
+SMALL = [n for n in golden_names() if not n.startswith("l256")]
+
+
+def full_sigma(g, S, T, cols=None):
+    """Sigma(k, iw_n) = Sigma_inf/z + C2/z^2 + C3/z^3 + S/z^4 (src/green.cpp:3039)."""
+    s2, s3 = g["sigma_inf2"], g["sigma_inf3"]
+    if cols is not None:
+        s2, s3 = s2[cols], s3[cols]
+    z = 1j * (2 * np.arange(S.shape[0])[:, None] + 1) * np.pi * T
+    return g["s"]["Sigma_inf"] / z + s2 / z ** 2 + s3 / z ** 3 + S / z ** 4
+
+
+def rel(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_oracle_matches_reference(name):
+    g = load_golden(name)
+    p, s = g["p"], g["s"]
+    r = O.solve(p["U"], p["tp"], p["tpp"], p["t3"], p["n"], p["T"], p["nk0"], p["Nw0"])
+    assert abs(r.mu0 - s["mu0"]) <= 1e-12 * max(1.0, abs(s["mu0"]))
+    assert r.chi0.qmax == (int(s["qmax0"]), int(s["qmax1"]))
+    assert rel(r.chi0.chi0max, s["chi0max"]) < 1e-12
+    assert rel(r.chi0.chi0_inf, g["chi0_inf"]) < 1e-12
+    # Nyquist component of the spline third derivative: an alternating sum, so
+    # two exact spline solvers differ here at ~1e-9 of the max (it only weights
+    # the 1/qn^4 tail beyond the stored frequencies)
+    assert rel(r.chi0.chi0_inf2, g["chi0_inf2"]) < 1e-8
+    assert rel(r.chi0.dtau_chirt0, g["dtau_chirt0"]) < 1e-12
+    if "chiqw" in g:
+        assert rel(r.chi0.chiqw, g["chiqw"]) < 1e-11
+        assert rel(r.V, g["vertex_rt"]) < 1e-11
+        # S multiplies 1/z^4: its high-frequency end is an alternating sum of
+        # spline third derivatives and carries ~1e-9 (of max) solver noise
+        assert rel(r.sigma.S, g["self"]) < 1e-8
+        assert rel(r.sigma.sigma(p["T"]), full_sigma(g, g["self"], p["T"])) < 1e-11
+    else:
+        c = g["cols"]
+        assert rel(r.chi0.chiqw[:, c], g["chiqw_cols"]) < 1e-11
+        assert rel(r.chi0.chiqw[0], g["chiqw_w0"]) < 1e-11
+        assert rel(r.V[:, c], g["vertex_rt_cols"]) < 1e-11
+        assert rel(r.sigma.S[:, c], g["self_cols"]) < 1e-8
+        assert rel(r.sigma.sigma(p["T"])[:, c], full_sigma(g, g["self_cols"], p["T"], c)) < 1e-11
+    assert rel(r.U.Usp, s["Usp"]) < 1e-10
+    assert rel(r.U.Uch, s["Uch"]) < 1e-10
+    assert rel(r.U.dblOcc, s["dblOcc"]) < 1e-10
+    assert rel(r.sigma.Sigma_inf, s["Sigma_inf"]) < 1e-10
+    assert rel(r.sigma.Sigma_inf2, g["sigma_inf2"]) < 1e-10
+    assert rel(r.sigma.Sigma_inf3, g["sigma_inf3"]) < 1e-9
+    assert rel(r.sigma.Sigma_inf4, g["sigma_inf4"]) < 1e-8
+    assert abs(r.mu - s["mu"]) < 1e-10 * max(1.0, abs(s["mu"]))
+
+
+def test_spline_matches_definition():
+    """The M-form clamped spline interpolates, is C2 and has the end slopes."""
+    rng = np.random.default_rng(1)
+    V = rng.standard_normal((33, 3))
+    h = 0.1
+    d0, dN = rng.standard_normal(3), rng.standard_normal(3)
+    a, b, c, d = O.clamped_spline(V, h, d0, dN)
+    assert np.allclose(a * h ** 3 + b * h * h + c * h + d, V[1:], atol=1e-12)
+    assert np.allclose(3 * a[:-1] * h * h + 2 * b[:-1] * h + c[:-1], c[1:], atol=1e-11)
+    assert np.allclose(6 * a[:-1] * h + 2 * b[:-1], 2 * b[1:], atol=1e-9)
+    assert np.allclose(c[0], d0)
+    assert np.allclose(3 * a[-1] * h * h + 2 * b[-1] * h + c[-1], dN, atol=1e-11)
+
+
+def test_find_zero_quadratic():
+    root, nev = O.find_zero(lambda x: x * x - 2.0, (1.0, 0.0, 3.0))
+    assert abs(root - np.sqrt(2.0)) < 1e-15
+    root, nev = O.find_zero(lambda x: x - 0.3, (0.0, -10.0, 10.0), lims=(-20, 20))
+    assert abs(root - 0.3) < 1e-15
