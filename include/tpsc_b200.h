@@ -1,0 +1,146 @@
+/*
+ * tpsc_b200.h -- C ABI of the B200 (sm_100a) TPSC engine.
+ *
+ * The reference (dbergeron1/TPSC_conductivity) has no FFI: its interface is a
+ * chain of C++ classes (hamiltonien -> green0 -> chi0 -> chi -> green ->
+ * cond_opt) whose methods run OpenMP loops over FFTW and LAPACK.  Each entry
+ * point below replaces one of those methods (cited as path:line in the
+ * reference checkout) and is what a drop-in of those classes binds.
+ *
+ * Conventions
+ *  - plain C types only; every call returns a tpsc_status (0 = OK);
+ *  - one context owns one CUDA stream and all device arrays of its grids; a
+ *    context is not thread-safe (the reference's objects are not either);
+ *  - host output buffers use the reference's layouts: octant index
+ *    o = m + l(l+1)/2 (m <= l < nbk = nk0/2+1), frequency-major arrays
+ *    [j * N8 + o], complex numbers as interleaved (re, im) doubles;
+ *  - "the current grid" is the (nk0, Nw0) of the last tpsc_chi0 call, as
+ *    chi0::calc_chiqw_FFT_spline re-grids the reference object (set_grid,
+ *    src/green0.h:44).
+ */
+#ifndef TPSC_B200_H
+#define TPSC_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct tpsc_ctx tpsc_ctx;
+
+enum tpsc_status {
+    TPSC_OK = 0,
+    TPSC_ERR_ARG = 1,        /* bad argument or unsupported size */
+    TPSC_ERR_CUDA = 2,       /* CUDA runtime error (message in tpsc_last_error) */
+    TPSC_ERR_OOM = 3,        /* device allocation failed */
+    TPSC_ERR_NO_ROOT = 4,    /* root search failed (find_zero returned false) */
+    TPSC_ERR_STATE = 5,      /* a prerequisite stage has not run */
+    TPSC_ERR_NONFINITE = 6   /* non-finite result */
+};
+
+/* Scalar results, index into tpsc_get_scalars(). */
+enum tpsc_scalar {
+    TPSC_S_MU0 = 0,        /* green0::mu0 (src/green0.cpp:240-262) */
+    TPSC_S_CHI0MAX,        /* chi0::chi0max (src/chi0.cpp:703-717) */
+    TPSC_S_QMAX0,          /* chi0::qmax[0] */
+    TPSC_S_QMAX1,          /* chi0::qmax[1] */
+    TPSC_S_USP,            /* chi::Usp */
+    TPSC_S_UCH,            /* chi::Uch */
+    TPSC_S_DBLOCC,         /* chi::dblOcc ansatz (src/chi.cpp:370-371) */
+    TPSC_S_DIFRELSP,       /* half grid vs full grid (src/chi.cpp:308-309) */
+    TPSC_S_DIFRELCH,
+    TPSC_S_SIGMA_INF,      /* green::Sigma_inf */
+    TPSC_S_MU,             /* green::mu */
+    TPSC_S_TR_SG,          /* traceSelfG raw sum (src/green.cpp:3088) */
+    TPSC_S_TR_SG_ASYMP,    /* traceSelfG with asymptotic correction (:3089) */
+    TPSC_S_TR_SG2,         /* traceSelfG2 (src/green.cpp:2979) */
+    TPSC_S_DBLOCC_SG2,     /* double occupancy from Tr Sigma G (:2980) */
+    TPSC_S_TR_CHI0,        /* traceChi0 raw (src/chi0.cpp:1578) */
+    TPSC_S_TR_CHI0_CORR,   /* traceChi0 extrapolated (src/chi0.cpp:1580) */
+    TPSC_S_EVALS_SP,       /* sum-rule evaluations spent on Usp */
+    TPSC_S_EVALS_CH,       /* ... on Uch */
+    TPSC_S_EVALS_MU,       /* Tr(G-G0) evaluations spent on mu */
+    TPSC_S_COUNT
+};
+
+/* Create a context on CUDA device `device`.  Returns NULL and sets *status on
+ * failure (no CUDA device, driver error). */
+tpsc_ctx *tpsc_create(int device, int *status);
+void tpsc_destroy(tpsc_ctx *ctx);
+/* Last error message of the context (static storage if ctx is NULL). */
+const char *tpsc_last_error(const tpsc_ctx *ctx);
+
+/* Model of the green(nk0, Nw0, n, T, eta, {tp, tpp, t3, U}) constructor
+ * (src/green.h:26, src/hamiltonien.cpp:13-30, src/green0.cpp:13-23):
+ * lattice side nk0 (power of two, 8..256), Nw0 total fermionic frequencies
+ * (power of two, 16..4096), density n in (0,2), temperature T > 0.
+ * Computes eps_k and mu0 of the finite lattice on the device. */
+int tpsc_set_model(tpsc_ctx *ctx, int nk0, int Nw0, double n, double T, double tp, double tpp, double t3,
+                   double U);
+
+/* chi0::calc_chiqw_FFT_spline(nq0, nw0) (src/chi0.cpp:279-718): switches the
+ * current grid to (nq0, nw0) -- re-deriving eps_k and mu0 as set_grid does --
+ * and computes chi0(q, iqn), n = 0..nw0/2, with its tail coefficients. */
+int tpsc_chi0(tpsc_ctx *ctx, int nq0, int nw0);
+
+/* chi0::traceChi0 (src/chi0.cpp:1498-1584): out[0] raw trace, out[1]
+ * extrapolated trace; both compare to n - n^2/2. */
+int tpsc_trace_chi0(tpsc_ctx *ctx, double out[2]);
+
+/* chi::traceDiffChispChi0 (channel 0) / traceDiffChichChi0 (channel 1)
+ * (src/chi.cpp:738-830) at vertex Uv; *dtrace = d trace / d Uv. */
+int tpsc_trace_diff_chi(tpsc_ctx *ctx, int channel, double Uv, double *trace, double *dtrace);
+
+/* chi::find_Usp_Uch(nq0, nw0, Usc) (src/chi.cpp:846-876): chi0 on the grid,
+ * then the spin and charge sum-rule roots; Usc = {Usp, Uch}. */
+int tpsc_find_Usp_Uch_grid(tpsc_ctx *ctx, int nq0, int nw0, double Usc[2]);
+
+/* chi::find_Usp_Uch() (src/chi.cpp:210-371): half grid, then full grid,
+ * difRel diagnostics and the double occupancy ansatz. */
+int tpsc_find_Usp_Uch(tpsc_ctx *ctx);
+
+/* chi::calc_chirt (src/chi.cpp:37-170): V(r, tau) on tau in [0, beta/2]. */
+int tpsc_vertex(tpsc_ctx *ctx);
+
+/* green::calc_Self_FFT_spline, stages after calc_chirt (src/green.cpp:1741-2025):
+ * Sigma(k, i w_n) = Sigma_inf/z + C2/z^2 + C3/z^3 + S/z^4, z = i w_n. */
+int tpsc_self_energy(tpsc_ctx *ctx);
+
+/* green::traceSelfG (src/green.cpp:3001-3104). */
+int tpsc_trace_self_G(tpsc_ctx *ctx, double out[2]);
+
+/* green::traceDiffG (src/green.cpp:3108-3182): Tr(G - G0) at chemical potential mu. */
+int tpsc_trace_diff_G(tpsc_ctx *ctx, double mu, double *trace);
+
+/* green::find_mu (src/green.cpp:3185-3282): mu from Tr(G - G0) = 0, then traceSelfG2. */
+int tpsc_find_mu(tpsc_ctx *ctx);
+
+/* One full TPSC solve on the model's grid: chi0 -> Usp, Uch -> V -> Sigma ->
+ * traceSelfG -> mu -> traceSelfG2, i.e. green::calc_Self_FFT_spline +
+ * traceSelfG + find_mu (src/tpsc_main.cpp:71-75) without the half-grid
+ * Usp/Uch pre-pass (which only feeds the difRel diagnostics) and without
+ * file output. */
+int tpsc_solve(tpsc_ctx *ctx);
+
+/* ---- results ------------------------------------------------------------ */
+/* n doubles of the scalar table (enum tpsc_scalar order). */
+int tpsc_get_scalars(tpsc_ctx *ctx, double *out, int n);
+/* grid of the context: dims = {nk0, Nw0, nbk, N8}. */
+int tpsc_get_dims(tpsc_ctx *ctx, int dims[4]);
+/* eps_k on the quadrant, ek[m + l*nbk] (src/hamiltonien.cpp:358-375). */
+int tpsc_get_ek(tpsc_ctx *ctx, double *ek);
+/* chiqw_array [ (Nw0/2+1) * N8 ] (any pointer may be NULL). */
+int tpsc_get_chi0(tpsc_ctx *ctx, double *chiqw, double *chi0_inf, double *chi0_inf2, double *dtau_chirt0);
+/* vertex_rt_array [ (Nw0/2+1) * N8 ]. */
+int tpsc_get_vertex(tpsc_ctx *ctx, double *vertex_rt);
+/* Self_kw_array [ (Nw0/2) * N8 ] complex (interleaved), Sigma_inf2/3/4 [N8]. */
+int tpsc_get_self(tpsc_ctx *ctx, double *self_kw, double *sigma_inf2, double *sigma_inf3, double *sigma_inf4);
+
+/* Device time of the last tpsc_solve per stage in ms:
+ * {chi0, sum rules, vertex, self energy, traces + mu}; n <= 5. */
+int tpsc_stage_times(tpsc_ctx *ctx, double *ms, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TPSC_B200_H */

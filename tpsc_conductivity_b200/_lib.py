@@ -1,0 +1,84 @@
+"""ctypes binding of the C ABI in include/tpsc_b200.h.
+
+The shared library is the in-tree ``libtpsc_b200.so`` built by
+``tpsc_conductivity_b200.build``.  There is no fallback: if the library is
+missing or no CUDA device is present, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libtpsc_b200.so")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+# (name, restype, argtypes) -- the exact exports of include/tpsc_b200.h
+SIGNATURES = [
+    ("tpsc_create", C.c_void_p, [C.c_int, _ip]),
+    ("tpsc_destroy", None, [C.c_void_p]),
+    ("tpsc_last_error", C.c_char_p, [C.c_void_p]),
+    ("tpsc_set_model", C.c_int, [C.c_void_p, C.c_int, C.c_int] + [C.c_double] * 6),
+    ("tpsc_chi0", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("tpsc_trace_chi0", C.c_int, [C.c_void_p, _dp]),
+    ("tpsc_trace_diff_chi", C.c_int, [C.c_void_p, C.c_int, C.c_double, _dp, _dp]),
+    ("tpsc_find_Usp_Uch_grid", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),
+    ("tpsc_find_Usp_Uch", C.c_int, [C.c_void_p]),
+    ("tpsc_vertex", C.c_int, [C.c_void_p]),
+    ("tpsc_self_energy", C.c_int, [C.c_void_p]),
+    ("tpsc_trace_self_G", C.c_int, [C.c_void_p, _dp]),
+    ("tpsc_trace_diff_G", C.c_int, [C.c_void_p, C.c_double, _dp]),
+    ("tpsc_find_mu", C.c_int, [C.c_void_p]),
+    ("tpsc_solve", C.c_int, [C.c_void_p]),
+    ("tpsc_get_scalars", C.c_int, [C.c_void_p, _dp, C.c_int]),
+    ("tpsc_get_dims", C.c_int, [C.c_void_p, _ip]),
+    ("tpsc_get_ek", C.c_int, [C.c_void_p, _dp]),
+    ("tpsc_get_chi0", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    ("tpsc_get_vertex", C.c_int, [C.c_void_p, _dp]),
+    ("tpsc_get_self", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    ("tpsc_stage_times", C.c_int, [C.c_void_p, _dp, C.c_int]),
+]
+
+STATUS = {0: "OK", 1: "bad argument", 2: "CUDA error", 3: "out of device memory",
+          4: "root not found", 5: "stage prerequisite missing", 6: "non-finite result"}
+
+# enum tpsc_scalar
+SCALARS = ["mu0", "chi0max", "qmax0", "qmax1", "Usp", "Uch", "dblOcc", "difRelsp", "difRelch",
+           "Sigma_inf", "mu", "trSG", "trSG_asymp", "trSG2", "dblOcc_SG2", "trChi0", "trChi0_corr",
+           "evals_sp", "evals_ch", "evals_mu"]
+
+
+class TPSCError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def load(path: str | None = None) -> C.CDLL:
+    """Load (once) the CUDA library; raises if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"{p} is missing: build it with `python -m tpsc_conductivity_b200.build` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(p)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(lib, ctx, status: int):
+    if status != 0:
+        msg = lib.tpsc_last_error(ctx)
+        raise TPSCError(status, msg.decode() if msg else "")

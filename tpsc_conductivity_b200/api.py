@@ -1,0 +1,174 @@
+"""Python mirror of the reference's TPSC class interface over the C ABI.
+
+``Green(nk0, Nw0, n, T, eta, params)`` takes the arguments of the reference's
+``green`` constructor (src/green.h:26; params = {tp, tpp, t3, U}) and offers
+its hot-path methods under the same names: ``calc_chiqw_FFT_spline``,
+``find_Usp_Uch``, ``calc_chirt``, ``calc_Self_FFT_spline``, ``traceSelfG``,
+``find_mu``, ``traceSelfG2``, ``traceChi0``.  Results come back as numpy
+arrays in the reference's layouts (octant index m + l(l+1)/2, frequency
+major).  Every computation runs in the CUDA library; a missing library or
+device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+class Context:
+    """One CUDA stream and the device arrays of every grid it has used."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        st = C.c_int(0)
+        self.h = self.lib.tpsc_create(device, C.byref(st))
+        if not self.h:
+            raise _lib.TPSCError(st.value, self.lib.tpsc_last_error(None).decode())
+
+    def call(self, name, *args):
+        _lib.check(self.lib, self.h, getattr(self.lib, name)(self.h, *args))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tpsc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Green:
+    """Drop-in for the reference's ``green`` object on the TPSC hot path."""
+
+    def __init__(self, nk0=8, Nw0=32, n=1.0, T=1.0, eta=0.1, params=None, device=0, ctx=None):
+        tp, tpp, t3, U = (params if params is not None else (0.0, 0.0, 0.0, 1.0))
+        self.nk0, self.Nw0, self.density, self.tem, self.eta = nk0, Nw0, n, T, eta
+        self.tp, self.tpp, self.t3, self.U = tp, tpp, t3, U
+        self.ctx = ctx or Context(device)
+        self.ctx.call("tpsc_set_model", nk0, Nw0, n, T, tp, tpp, t3, U)
+
+    # ---- stages (reference method names) ---------------------------------
+    def calc_chiqw_FFT_spline(self, nq0=None, nw0=None):
+        """chi0::calc_chiqw_FFT_spline (src/chi0.cpp:279)."""
+        self.ctx.call("tpsc_chi0", nq0 or self.nk0, nw0 or self.Nw0)
+
+    def traceChi0(self):
+        """chi0::traceChi0 (src/chi0.cpp:1498): (raw, extrapolated)."""
+        out = np.zeros(2)
+        self.ctx.call("tpsc_trace_chi0", _dptr(out))
+        return float(out[0]), float(out[1])
+
+    def traceDiffChi(self, channel, Uv):
+        """traceDiffChispChi0 (channel 0) / traceDiffChichChi0 (channel 1), src/chi.cpp:738-830."""
+        t, dt = C.c_double(), C.c_double()
+        self.ctx.call("tpsc_trace_diff_chi", channel, Uv, C.byref(t), C.byref(dt))
+        return t.value, dt.value
+
+    def find_Usp_Uch_grid(self, nq0, nw0):
+        """chi::find_Usp_Uch(nq0, nw0, Usc) (src/chi.cpp:846)."""
+        out = np.zeros(2)
+        self.ctx.call("tpsc_find_Usp_Uch_grid", nq0, nw0, _dptr(out))
+        return float(out[0]), float(out[1])
+
+    def find_Usp_Uch(self):
+        """chi::find_Usp_Uch() (src/chi.cpp:210): half grid, full grid, dblOcc."""
+        self.ctx.call("tpsc_find_Usp_Uch")
+
+    def calc_chirt(self):
+        """chi::calc_chirt (src/chi.cpp:37)."""
+        self.ctx.call("tpsc_vertex")
+
+    def calc_self_energy(self):
+        """green::calc_Self_FFT_spline after calc_chirt (src/green.cpp:1741-2025)."""
+        self.ctx.call("tpsc_self_energy")
+
+    def calc_Self_FFT_spline(self):
+        """green::calc_Self_FFT_spline (src/green.cpp:1673): find_Usp_Uch (two
+        grids), calc_chirt, then the self-energy."""
+        self.find_Usp_Uch()
+        self.calc_chirt()
+        self.calc_self_energy()
+
+    def traceSelfG(self):
+        """green::traceSelfG (src/green.cpp:3001): (sum, sum with asymptotic correction)."""
+        out = np.zeros(2)
+        self.ctx.call("tpsc_trace_self_G", _dptr(out))
+        return float(out[0]), float(out[1])
+
+    def traceDiffG(self, mu):
+        """green::traceDiffG (src/green.cpp:3108)."""
+        t = C.c_double()
+        self.ctx.call("tpsc_trace_diff_G", mu, C.byref(t))
+        return t.value
+
+    def find_mu(self):
+        """green::find_mu (src/green.cpp:3185), followed by traceSelfG2."""
+        self.ctx.call("tpsc_find_mu")
+
+    def solve(self):
+        """One full TPSC solve on the model grid (no half-grid pre-pass)."""
+        self.ctx.call("tpsc_solve")
+
+    # ---- results ----------------------------------------------------------
+    def scalars(self) -> dict:
+        out = np.zeros(len(_lib.SCALARS))
+        self.ctx.call("tpsc_get_scalars", _dptr(out), len(out))
+        return dict(zip(_lib.SCALARS, out.tolist()))
+
+    def dims(self):
+        d = (C.c_int * 4)()
+        self.ctx.call("tpsc_get_dims", d)
+        return tuple(d)
+
+    def ek(self):
+        nk0, nw0, nbk, n8 = self.dims()
+        out = np.zeros(nbk * nbk)
+        self.ctx.call("tpsc_get_ek", _dptr(out))
+        return out.reshape(nbk, nbk)
+
+    def chi0(self, full=True):
+        nk0, nw0, nbk, n8 = self.dims()
+        nb = nw0 // 2 + 1
+        cq = np.zeros((nb, n8)) if full else None
+        ci, ci2, dc = np.zeros(n8), np.zeros(n8), np.zeros(n8)
+        self.ctx.call("tpsc_get_chi0", _dptr(cq), _dptr(ci), _dptr(ci2), _dptr(dc))
+        return dict(chiqw=cq, chi0_inf=ci, chi0_inf2=ci2, dtau_chirt0=dc)
+
+    def vertex(self):
+        nk0, nw0, nbk, n8 = self.dims()
+        out = np.zeros((nw0 // 2 + 1, n8))
+        self.ctx.call("tpsc_get_vertex", _dptr(out))
+        return out
+
+    def self_energy(self, out=None):
+        """S (coefficient of 1/z^4) as complex [Nw0/2, N8] plus Sigma_inf2/3/4."""
+        nk0, nw0, nbk, n8 = self.dims()
+        if out is None:
+            out = np.zeros((nw0 // 2, n8), dtype=np.complex128)
+        s2, s3, s4 = np.zeros(n8), np.zeros(n8), np.zeros(n8)
+        self.ctx.call("tpsc_get_self", _dptr(out.view(np.float64)), _dptr(s2), _dptr(s3), _dptr(s4))
+        return dict(S=out, Sigma_inf2=s2, Sigma_inf3=s3, Sigma_inf4=s4)
+
+    def sigma(self):
+        """Full Sigma(k, i w_n), n < Nw0/2 (src/green.cpp:3039)."""
+        r = self.self_energy()
+        sc = self.scalars()
+        nj = r["S"].shape[0]
+        z = 1j * (2 * np.arange(nj)[:, None] + 1) * np.pi * self.tem
+        return (sc["Sigma_inf"] / z + r["Sigma_inf2"] / z ** 2 + r["Sigma_inf3"] / z ** 3
+                + r["S"] / z ** 4)
+
+    def stage_times(self):
+        out = np.zeros(5)
+        self.ctx.call("tpsc_stage_times", _dptr(out), 5)
+        return dict(zip(["chi0", "sumrules", "vertex", "self", "mu"], out.tolist()))

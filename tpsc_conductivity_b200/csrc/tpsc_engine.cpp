@@ -1,0 +1,936 @@
+// tpsc_engine.cpp -- host side of the C ABI (include/tpsc_b200.h).
+//
+// Owns the device arrays of each (nk0, Nw0) grid, builds the lattice and FFT
+// tables, sequences the kernels of tpsc_kernels.cu on one CUDA stream and
+// runs the root searches of the reference (generique::find_zero) with every
+// function evaluation a device reduction.  Only scalars cross PCIe during a
+// solve.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/tpsc_b200.h"
+#include "tpsc_kernels.cuh"
+
+using namespace tpsc;
+
+namespace {
+
+const double PI = std::acos(-1.0);
+const double EPS = std::numeric_limits<double>::epsilon();
+
+// ---------------------------------------------------------------------------
+// Root search with the control flow of generique::find_zero: bracketing
+// inverse-quadratic interpolation with secant and bisection fallbacks, tol
+// 1e-16 and 20 iterations (src/generique.cpp:604-913); with lims, the bounded
+// variant: tol 1e-15, 12 iterations, eps = 2 machine epsilons
+// (src/generique.cpp:917-1234).  The evaluator returns false on a device
+// error, which aborts the search.
+// ---------------------------------------------------------------------------
+template <typename F>
+bool find_zero(F &&func, const double init[3], double *root, const double *lims, int *nev, bool *dev_err) {
+    double tol, eps;
+    int itmax;
+    if (!lims) {
+        tol = 1.0e-16;
+        eps = 10.0 * EPS;
+        itmax = 20;
+    } else {
+        tol = 1.0e-15;
+        eps = 2.0 * EPS;
+        itmax = 12;
+    }
+    *nev = 0;
+    *dev_err = false;
+    auto f = [&](double x, double &y) -> bool {
+        ++*nev;
+        if (!func(x, y)) {
+            *dev_err = true;
+            return false;
+        }
+        return true;
+    };
+    int nbiter = 0;
+    const double dytol = 0.01;
+    double x0 = init[0], xmin = init[1], xmax = init[2];
+    double ymin, ymax;
+    if (!f(xmin, ymin) || !f(xmax, ymax)) return false;
+    double x[3] = {x0, xmin, xmax}, y[3] = {0.0, ymin, ymax};
+    if (std::fabs(ymin) < tol) {
+        *root = xmin;
+        return true;
+    }
+    if (std::fabs(ymax) < tol) {
+        *root = xmax;
+        return true;
+    }
+    if (ymin * ymax > 0) {
+        if (!f(x[0], y[0])) return false;
+        if (std::fabs(y[0]) < tol) {
+            *root = x[0];
+            return true;
+        }
+        if (y[0] * y[2] < 0) {
+            const double xt = x[0];
+            x[0] = (x[0] + x[2]) / 2;
+            x[1] = xt;
+            y[1] = y[0];
+        } else {
+            double ytmp = y[0], xtmp = x[0], xtmp1, ytmp1;
+            if (std::fabs(y[1]) < std::fabs(ytmp)) ytmp = y[1], xtmp = x[1];
+            if (std::fabs(y[2]) < std::fabs(ytmp)) ytmp = y[2], xtmp = x[2];
+            xtmp1 = xtmp + 10 * eps;
+            if (!f(xtmp1, ytmp1)) return false;
+            xtmp1 = xtmp - ytmp * ((xtmp1 - xtmp) / (ytmp1 - ytmp));
+            if (!f(xtmp1, ytmp1)) return false;
+            nbiter++;
+            while (std::fabs(ytmp1) > tol && nbiter < itmax && ytmp1 * ytmp > 0 && std::isfinite(xtmp1)) {
+                xtmp = xtmp1;
+                ytmp = ytmp1;
+                xtmp1 = xtmp + 10 * eps;
+                if (!f(xtmp1, ytmp1)) return false;
+                xtmp1 = xtmp - ytmp * ((xtmp1 - xtmp) / (ytmp1 - ytmp));
+                if (!f(xtmp1, ytmp1)) return false;
+                nbiter++;
+            }
+            if (std::fabs(ytmp1) < tol) {
+                *root = xtmp1;
+                return true;
+            }
+            if (ytmp1 * ytmp < 0) {
+                x[0] = (xtmp + xtmp1) / 2;
+                x[1] = xtmp;
+                y[1] = ytmp;
+                x[2] = xtmp1;
+                y[2] = ytmp1;
+            }
+            if (nbiter >= itmax) return false;
+            if (!std::isfinite(xtmp1)) return false;
+        }
+    }
+    if (lims) {
+        if (x[1] < lims[0] || x[1] > lims[1] || x[2] < lims[0] || x[2] > lims[1]) return false;
+    }
+    if (std::fabs(xmax - xmin) < eps) {
+        *root = xmin;
+        return true;
+    }
+    if (!f(x[0], y[0])) return false;
+    if (std::fabs(y[0]) < tol) {
+        *root = x[0];
+        return true;
+    }
+    int ind1, ind2, ind3, indm = 0, indp = 0, indfar, indmid;
+    auto classify = [&]() {
+        if (y[0] * y[1] > 0)
+            ind1 = 0, ind2 = 1;
+        else if (y[0] * y[2] > 0)
+            ind1 = 0, ind2 = 2;
+        else
+            ind1 = 1, ind2 = 2;
+        ind3 = 3 - ind1 - ind2;
+        if (x[ind3] > x[ind1]) {
+            if (x[ind1] > x[ind2])
+                indfar = ind2, indmid = ind1;
+            else
+                indfar = ind1, indmid = ind2;
+            indm = indmid, indp = ind3;
+        } else {
+            if (x[ind1] < x[ind2])
+                indfar = ind2, indmid = ind1;
+            else
+                indfar = ind1, indmid = ind2;
+            indm = ind3, indp = indmid;
+        }
+    };
+    classify();
+    x[indfar] = -y[indmid] * (x[ind3] - x[indmid]) / (y[ind3] - y[indmid]) + x[indmid];
+    if (!f(x[indfar], y[indfar])) return false;
+    double dy = y[indfar], dyprec;
+    double a = 0.0, b = 0.0, c = 0.0;
+    while (std::fabs(dy) > tol && nbiter < itmax) {
+        classify();
+        const double denom = -x[0] * x[0] * x[2] + x[0] * x[0] * x[1] - x[0] * x[1] * x[1] + x[0] * x[2] * x[2] -
+                             x[2] * x[2] * x[1] + x[2] * x[1] * x[1];
+        if (std::fabs(denom) > 0.0) {
+            a = (x[0] * y[2] - x[0] * y[1] + x[2] * y[1] - y[2] * x[1] - y[0] * x[2] + y[0] * x[1]) / denom;
+            b = -(-y[2] * x[1] * x[1] + x[1] * x[1] * y[0] - x[2] * x[2] * y[0] - y[1] * x[0] * x[0] +
+                  y[2] * x[0] * x[0] + y[1] * x[2] * x[2]) /
+                denom;
+            c = (y[2] * x[0] * x[0] * x[1] - y[1] * x[0] * x[0] * x[2] - x[1] * x[1] * x[0] * y[2] +
+                 x[2] * x[2] * x[0] * y[1] + x[1] * x[1] * y[0] * x[2] - x[2] * x[2] * y[0] * x[1]) /
+                denom;
+        }
+        if ((b * b - 4.0 * a * c) > 0.0 && std::fabs(denom) > 0.0) {
+            const double sq = std::sqrt(b * b - 4.0 * a * c);
+            const double xp = (-b + sq) / (2 * a), xm = (-b - sq) / (2 * a);
+            if (xp > x[indm] && xp < x[indp])
+                x[indfar] = xp;
+            else if (xm > x[indm] && xm < x[indp])
+                x[indfar] = xm;
+            else if (std::fabs(y[ind3] - y[indmid]) > tol)
+                x[indfar] = -y[indmid] * (x[ind3] - x[indmid]) / (y[ind3] - y[indmid]) + x[indmid];
+            else {
+                *root = x[indmid];
+                return true;
+            }
+        } else {
+            if (std::fabs(y[ind3] - y[indmid]) > tol)
+                x[indfar] = -y[indmid] * (x[ind3] - x[indmid]) / (y[ind3] - y[indmid]) + x[indmid];
+            else {
+                *root = x[indmid];
+                return true;
+            }
+        }
+        if (!f(x[indfar], y[indfar])) return false;
+        dyprec = std::fabs(dy);
+        dy = y[indfar];
+        if (std::fabs(dyprec - std::fabs(dy)) < dytol * dyprec || dyprec < std::fabs(dy)) {
+            x[indfar] = (x[ind3] + x[indmid]) / 2.0;
+            if (!f(x[indfar], y[indfar])) return false;
+            dy = y[indfar];
+        }
+        nbiter++;
+    }
+    int best = 0;
+    *root = x[0];
+    if (std::fabs(y[1]) < std::fabs(y[best])) {
+        *root = x[1];
+        best = 1;
+    }
+    if (std::fabs(y[2]) < std::fabs(y[best])) *root = x[2];
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// one (nk0, Nw0) grid: tables and arrays
+// ---------------------------------------------------------------------------
+struct Grid {
+    GridDev d;
+    std::vector<double> ek_host;  // [nbk * nbk], ek[m + l*nbk]
+    double mu0 = 0.0;
+    double *Grt = nullptr;        // [(Nw0+1) * n8]      G(r, tau_j)
+    double *chirt = nullptr;      // blocked nb          chi0(r, tau_j)
+    double *chiq = nullptr;       // blocked nb          chi0(q, tau_j) -> chi0(q, iqn)
+    double *dG0p = nullptr, *dchirt0 = nullptr, *dchiqt0 = nullptr;  // [n8]
+    double *cinf = nullptr, *cinf2 = nullptr;                        // [n8]
+    double *V = nullptr;          // blocked nb          V(r, iqn) -> V(r, tau_j)
+    double *dS = nullptr;         // [2 n8p]             Sigma'(k, 0), Sigma'(k, beta)
+    double *sigt = nullptr;       // blocked Nw0+1       Sigma(k, tau_j)
+    double2 *S = nullptr;         // blocked Nw0/2       coefficient of 1/z^4
+    double *s2 = nullptr, *s3 = nullptr, *s4 = nullptr, *sinf = nullptr;
+    bool have_chi0 = false, have_V = false, have_S = false;
+    std::vector<void *> allocs;
+};
+
+}  // namespace
+
+struct tpsc_ctx {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    Reduce red;
+    double *h_res = nullptr;  // pinned, 8 doubles
+    // model
+    bool have_model = false;
+    int nk0 = 0, Nw0 = 0;
+    double n = 0, T = 0, tp = 0, tpp = 0, t3 = 0, U = 0, nsr = 0;
+    double Usp = 0, Uch = 0;
+    std::map<std::pair<int, int>, Grid *> grids;
+    Grid *cur = nullptr;
+    double scal[TPSC_S_COUNT] = {0};
+    double stage_ms[5] = {0};
+    cudaEvent_t ev[6] = {};
+    void *stage = nullptr;
+    size_t stage_bytes = 0;
+    std::string err;
+};
+
+namespace {
+
+std::string g_static_err;
+
+int fail(tpsc_ctx *c, int code, const std::string &msg) {
+    if (c)
+        c->err = msg;
+    else
+        g_static_err = msg;
+    return code;
+}
+
+int cuda_fail(tpsc_ctx *c, cudaError_t e, const char *where) {
+    return fail(c, e == cudaErrorMemoryAllocation ? TPSC_ERR_OOM : TPSC_ERR_CUDA,
+                std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                  \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);  \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(Grid *g, T **p, size_t count) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 16);
+    if (e != cudaSuccess) return e;
+    g->allocs.push_back(q);
+    *p = static_cast<T *>(q);
+    return cudaMemset(q, 0, count * sizeof(T) + 16);
+}
+
+void free_grid(Grid *g) {
+    for (void *p : g->allocs) cudaFree(p);
+    delete g;
+}
+
+// eps_k = -2(cx + cy) - 4 t' cx cy - 2 t''(c2x + c2y) - 4 t3 (c2x cy + c2y cx) on
+// k = l pi/(nbk-1) (hamiltonien::calc_ek / dispk, src/hamiltonien.cpp:358-375, 428-431)
+double dispk(double kx, double ky, double tp, double tpp, double t3) {
+    return -2.0 * (std::cos(kx) + std::cos(ky)) - 4.0 * tp * std::cos(kx) * std::cos(ky) -
+           2.0 * tpp * (std::cos(2 * kx) + std::cos(2 * ky)) -
+           4 * t3 * (std::cos(2 * kx) * std::cos(ky) + std::cos(2 * ky) * std::cos(kx));
+}
+
+// Thomas-algorithm tables of the clamped-spline system with NJ nodes:
+// invp[i] = 1/pivot_i, cp[i] = superdiagonal / pivot (cp[NJ-1] = 0).
+void spline_tables(int NJ, std::vector<double> &out) {
+    out.assign(2 * NJ, 0.0);
+    const int N = NJ - 1;
+    long double cpv = 0.0L;
+    for (int i = 0; i <= N; ++i) {
+        long double p;
+        if (i == 0)
+            p = 2.0L;
+        else if (i < N)
+            p = 4.0L - cpv;
+        else
+            p = 2.0L - cpv;
+        out[i] = (double)(1.0L / p);
+        cpv = (i < N) ? 1.0L / p : 0.0L;
+        out[NJ + i] = (double)cpv;
+    }
+}
+
+void twiddles(int N, long double sign, long double scale, std::vector<double2> &out) {
+    out.resize(N);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int m = 0; m < N; ++m) {
+        const long double a = sign * scale * pi * m / N;
+        out[m] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+}
+
+template <typename T>
+cudaError_t upload(Grid *g, T **dst, const std::vector<T> &src) {
+    cudaError_t e = dalloc(g, dst, src.size());
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
+    auto key = std::make_pair(nk0, nw0);
+    auto it = ctx->grids.find(key);
+    if (it != ctx->grids.end()) {
+        *out = it->second;
+        return TPSC_OK;
+    }
+    if (!supported_grid(nk0, nw0))
+        return fail(ctx, TPSC_ERR_ARG, "unsupported grid nk0=" + std::to_string(nk0) +
+                                           " Nw0=" + std::to_string(nw0) +
+                                           " (nk0 in {8,16,32,64,128,256}, Nw0 power of two in [16, 4096])");
+    Grid *g = new Grid;
+    GridDev &d = g->d;
+    d.nk0 = nk0;
+    d.nbk = nk0 / 2 + 1;
+    d.n8 = d.nbk * (d.nbk + 1) / 2;
+    d.n8p = (d.n8 + 3) & ~3;
+    d.nw0 = nw0;
+    d.nb = nw0 / 2 + 1;
+    std::vector<uint32_t> lm(d.n8);
+    for (int l = 0; l < d.nbk; ++l)
+        for (int m = 0; m <= l; ++m) lm[m + l * (l + 1) / 2] = ((uint32_t)l << 16) | (uint32_t)m;
+    std::vector<double2> twk, tww, htw;
+    twiddles(nk0, -2.0L, 1.0L, twk);
+    twiddles(nw0, -2.0L, 1.0L, tww);
+    twiddles(nw0, 1.0L, 1.0L, htw);
+    std::vector<double> sh, sf;
+    spline_tables(d.nb, sh);
+    spline_tables(nw0 + 1, sf);
+    cudaError_t e = cudaSuccess;
+    const size_t n8 = d.n8, n8p = d.n8p, nb = d.nb, nw = nw0;
+#define A(x)                                       \
+    if (e == cudaSuccess) {                        \
+        e = (x);                                   \
+    }
+    A(upload(g, &d.lm, lm));
+    A(upload(g, &d.tw_k, twk));
+    A(upload(g, &d.tw_w, tww));
+    A(upload(g, &d.ht_w, htw));
+    A(upload(g, &d.spl_half, sh));
+    A(upload(g, &d.spl_full, sf));
+    A(dalloc(g, &d.ek, n8));
+    A(dalloc(g, &d.er, n8));
+    A(dalloc(g, &g->Grt, (nw + 1) * n8));
+    A(dalloc(g, &g->chirt, nb * n8p));
+    A(dalloc(g, &g->chiq, nb * n8p));
+    A(dalloc(g, &g->dG0p, n8));
+    A(dalloc(g, &g->dchirt0, n8));
+    A(dalloc(g, &g->dchiqt0, n8));
+    A(dalloc(g, &g->cinf, n8));
+    A(dalloc(g, &g->cinf2, n8));
+    A(dalloc(g, &g->V, nb * n8p));
+    A(dalloc(g, &g->dS, 2 * n8p));
+    A(dalloc(g, &g->sigt, (nw + 1) * n8p));
+    A(dalloc(g, &g->S, (nw / 2) * n8p));
+    A(dalloc(g, &g->s2, n8));
+    A(dalloc(g, &g->s3, n8));
+    A(dalloc(g, &g->s4, n8));
+    A(dalloc(g, &g->sinf, 1));
+#undef A
+    if (e != cudaSuccess) {
+        free_grid(g);
+        return cuda_fail(ctx, e, "grid allocation");
+    }
+    ctx->grids[key] = g;
+    *out = g;
+    return TPSC_OK;
+}
+
+// device scalar readback after a reduction launched on ctx->st
+int read_result(tpsc_ctx *ctx, int count, double *out) {
+    CK(cudaMemcpyAsync(ctx->h_res, ctx->red.result, count * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (int i = 0; i < count; ++i) out[i] = ctx->h_res[i];
+    return TPSC_OK;
+}
+
+// eps_k tables of the grid for the current model, then mu0 by the density
+// root of green0::find_mu (src/green0.cpp:240-262)
+int grid_set_model(tpsc_ctx *ctx, Grid *g) {
+    GridDev &d = g->d;
+    g->ek_host.assign((size_t)d.nbk * d.nbk, 0.0);
+    for (int l = 0; l < d.nbk; ++l) {
+        const double kx = l * PI / (d.nbk - 1);
+        for (int m = 0; m < d.nbk; ++m) {
+            const double ky = m * PI / (d.nbk - 1);
+            g->ek_host[m + l * d.nbk] = dispk(kx, ky, ctx->tp, ctx->tpp, ctx->t3);
+        }
+    }
+    std::vector<double> eo(d.n8), er(d.n8, 0.0);
+    for (int l = 0; l < d.nbk; ++l)
+        for (int m = 0; m <= l; ++m) eo[m + l * (l + 1) / 2] = g->ek_host[m + l * d.nbk];
+    er[1] = -1;
+    er[2] = -ctx->tp;
+    er[3] = -ctx->tpp;
+    er[4] = -ctx->t3;
+    CK(cudaMemcpyAsync(d.ek, eo.data(), d.n8 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(d.er, er.data(), d.n8 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    g->have_chi0 = g->have_V = g->have_S = false;
+    if (ctx->n == 1.0 && ctx->tp == 0 && ctx->tpp == 0) {
+        g->mu0 = 0.0;
+        return TPSC_OK;
+    }
+    int rc = TPSC_OK;
+    auto dens = [&](double mu, double &y) -> bool {
+        cudaError_t e = launch_density(d, mu, ctx->n, ctx->T, ctx->red, ctx->st);
+        if (e != cudaSuccess) {
+            rc = cuda_fail(ctx, e, "launch_density");
+            return false;
+        }
+        rc = read_result(ctx, 1, &y);
+        return rc == TPSC_OK;
+    };
+    const double init[3] = {0.0, -8.0, 8.0};
+    double root = 0;
+    int nev;
+    bool derr;
+    if (!find_zero(dens, init, &root, nullptr, &nev, &derr)) {
+        if (derr) return rc;
+        return fail(ctx, TPSC_ERR_NO_ROOT, "mu0 not found");
+    }
+    g->mu0 = root;
+    return TPSC_OK;
+}
+
+int switch_grid(tpsc_ctx *ctx, int nk0, int nw0) {
+    Grid *g = nullptr;
+    int rc = build_grid(ctx, nk0, nw0, &g);
+    if (rc) return rc;
+    rc = grid_set_model(ctx, g);
+    if (rc) return rc;
+    ctx->cur = g;
+    ctx->scal[TPSC_S_MU0] = g->mu0;
+    return TPSC_OK;
+}
+
+int need_model(tpsc_ctx *ctx) {
+    if (!ctx) return fail(nullptr, TPSC_ERR_ARG, "null context");
+    if (!ctx->have_model) return fail(ctx, TPSC_ERR_STATE, "tpsc_set_model has not been called");
+    return TPSC_OK;
+}
+
+int run_chi0(tpsc_ctx *ctx) {
+    Grid *g = ctx->cur;
+    const GridDev &d = g->d;
+    CK(launch_gslice(d, g->Grt, g->mu0, ctx->T, ctx->st));
+    CK(launch_chi0_boundary(d, g->Grt, g->mu0, ctx->T, g->dG0p, g->dchirt0, g->dchiqt0, ctx->st));
+    CK(launch_chi0_slice(d, g->Grt, g->chirt, g->chiq, ctx->st));
+    CK(launch_chi0_tau(d, g->chiq, g->dchiqt0, g->cinf, g->cinf2, ctx->T, ctx->st));
+    CK(launch_chi0max(d, g->chiq, ctx->red, ctx->st));
+    double r[3];
+    int rc = read_result(ctx, 3, r);
+    if (rc) return rc;
+    ctx->scal[TPSC_S_CHI0MAX] = r[0];
+    ctx->scal[TPSC_S_QMAX0] = r[1];
+    ctx->scal[TPSC_S_QMAX1] = r[2];
+    g->have_chi0 = true;
+    g->have_V = g->have_S = false;
+    if (!std::isfinite(r[0]) || r[0] <= 0.0) return fail(ctx, TPSC_ERR_NONFINITE, "chi0(q, 0) has no positive maximum");
+    return TPSC_OK;
+}
+
+int sumrule(tpsc_ctx *ctx, int channel, double Uv, double *tr, double *dtr) {
+    Grid *g = ctx->cur;
+    CK(launch_sumrule(g->d, g->chiq, g->cinf, g->cinf2, Uv, channel == 0 ? -1.0 : 1.0, ctx->T, ctx->red, ctx->st));
+    double r[2];
+    int rc = read_result(ctx, 2, r);
+    if (rc) return rc;
+    *tr = r[0];
+    if (dtr) *dtr = r[1];
+    return TPSC_OK;
+}
+
+// chi::find_Usp_Uch(nq0, nw0, Usc) on the current grid after chi0 (src/chi.cpp:850-876)
+int roots_Usp_Uch(tpsc_ctx *ctx, double Usc[2]) {
+    const double n = ctx->n, U = ctx->U, nsr = ctx->nsr;
+    int rc = TPSC_OK;
+    auto rsp = [&](double Us, double &y) -> bool {
+        double tr;
+        rc = sumrule(ctx, 0, Us, &tr, nullptr);
+        if (rc) return false;
+        y = tr + n - n * n / 2.0 - nsr + Us * nsr * nsr / (2.0 * U);
+        return true;
+    };
+    const double init_sp[3] = {U / 2.0, 0.0, 2.0 / ctx->scal[TPSC_S_CHI0MAX] - 2 * EPS};
+    int nev;
+    bool derr;
+    double root = 0;
+    if (!find_zero(rsp, init_sp, &root, nullptr, &nev, &derr)) {
+        if (derr) return rc;
+        return fail(ctx, TPSC_ERR_NO_ROOT, "Usp not found");
+    }
+    ctx->scal[TPSC_S_EVALS_SP] = nev;
+    Usc[0] = root;
+    ctx->Usp = root;
+    auto rch = [&](double Uc, double &y) -> bool {
+        double tr;
+        rc = sumrule(ctx, 1, Uc, &tr, nullptr);
+        if (rc) return false;
+        y = tr + n - n * n / 2.0 - (nsr + ctx->Usp * nsr * nsr / (2.0 * U) - nsr * nsr);
+        return true;
+    };
+    const double init_ch[3] = {0.0, 0.0, 1000.0 * U};
+    if (!find_zero(rch, init_ch, &root, nullptr, &nev, &derr)) {
+        if (derr) return rc;
+        return fail(ctx, TPSC_ERR_NO_ROOT, "Uch not found");
+    }
+    ctx->scal[TPSC_S_EVALS_CH] = nev;
+    Usc[1] = root;
+    ctx->Uch = root;
+    ctx->scal[TPSC_S_USP] = ctx->Usp;
+    ctx->scal[TPSC_S_UCH] = ctx->Uch;
+    return TPSC_OK;
+}
+
+void set_dblocc(tpsc_ctx *ctx) {
+    const double nsr = ctx->nsr;
+    double D = ctx->Usp / ctx->U * nsr * nsr / 4.0;
+    if (ctx->n > 1.0) D += 1.0 - nsr;
+    ctx->scal[TPSC_S_DBLOCC] = D;
+}
+
+int run_vertex(tpsc_ctx *ctx) {
+    Grid *g = ctx->cur;
+    if (!g || !g->have_chi0) return fail(ctx, TPSC_ERR_STATE, "chi0 has not been computed on the current grid");
+    const double fact = ctx->U * (3.0 * ctx->Usp + ctx->Uch) / 8.0;
+    CK(launch_vertex_q(g->d, g->chiq, g->V, ctx->U, ctx->Usp, ctx->Uch, ctx->T, ctx->st));
+    CK(launch_vertex_tau(g->d, g->V, g->chirt, fact, ctx->st));
+    g->have_V = true;
+    return TPSC_OK;
+}
+
+int run_self(tpsc_ctx *ctx) {
+    Grid *g = ctx->cur;
+    if (!g || !g->have_V) return fail(ctx, TPSC_ERR_STATE, "the vertex V(r, tau) has not been computed");
+    const double fact = ctx->U * (3.0 * ctx->Usp + ctx->Uch) / 8.0;
+    const GridDev &d = g->d;
+    CK(launch_sigma_boundary(d, g->Grt, g->V, g->dchirt0, g->dG0p, g->mu0, fact, g->dS, ctx->st));
+    CK(launch_sigma_slice(d, g->Grt, g->V, g->sigt, ctx->st));
+    CK(launch_sigma_tau(d, g->sigt, g->dS, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->T, ctx->st));
+    CK(cudaMemcpyAsync(ctx->h_res, g->sinf, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->scal[TPSC_S_SIGMA_INF] = ctx->h_res[0];
+    g->have_S = true;
+    return TPSC_OK;
+}
+
+int trace_self_G(tpsc_ctx *ctx, double out[2]) {
+    Grid *g = ctx->cur;
+    if (!g || !g->have_S) return fail(ctx, TPSC_ERR_STATE, "the self-energy has not been computed");
+    CK(launch_trace_self_G(g->d, g->S, g->s2, g->s3, g->sinf, g->mu0, ctx->T, ctx->red, ctx->st));
+    double r[2];
+    int rc = read_result(ctx, 2, r);
+    if (rc) return rc;
+    out[0] = r[0];
+    out[1] = r[0] + r[1];
+    ctx->scal[TPSC_S_TR_SG] = out[0];
+    ctx->scal[TPSC_S_TR_SG_ASYMP] = out[1];
+    return TPSC_OK;
+}
+
+int trace_diff_G(tpsc_ctx *ctx, double pmu, double *tr) {
+    Grid *g = ctx->cur;
+    CK(launch_trace_diff_G(g->d, g->S, g->s2, g->s3, g->s4, g->sinf, g->mu0, pmu, ctx->T, ctx->red, ctx->st));
+    return read_result(ctx, 1, tr);
+}
+
+int find_mu(tpsc_ctx *ctx) {
+    Grid *g = ctx->cur;
+    if (!g || !g->have_S) return fail(ctx, TPSC_ERR_STATE, "the self-energy has not been computed");
+    int rc = TPSC_OK;
+    auto f = [&](double m, double &y) -> bool {
+        rc = trace_diff_G(ctx, m, &y);
+        return rc == TPSC_OK;
+    };
+    const double init[3] = {0.0, -10.0, 10.0}, lims[2] = {-20.0, 20.0};
+    double root = 0;
+    int nev;
+    bool derr;
+    if (!find_zero(f, init, &root, lims, &nev, &derr)) {
+        if (derr) return rc;
+        return fail(ctx, TPSC_ERR_NO_ROOT, "mu not found");
+    }
+    ctx->scal[TPSC_S_EVALS_MU] = nev;
+    ctx->scal[TPSC_S_MU] = root;
+    // traceSelfG2 at the new mu (src/green.cpp:3281)
+    CK(launch_trace_self_G2(g->d, g->S, g->s2, g->s3, g->sinf, root, ctx->T, ctx->red, ctx->st));
+    double r;
+    rc = read_result(ctx, 1, &r);
+    if (rc) return rc;
+    ctx->scal[TPSC_S_TR_SG2] = r;
+    ctx->scal[TPSC_S_DBLOCC_SG2] = (r + ctx->U * ctx->n * ctx->n / 4.0) / ctx->U;
+    return TPSC_OK;
+}
+
+int ensure_stage(tpsc_ctx *ctx, size_t bytes) {
+    if (ctx->stage_bytes >= bytes) return TPSC_OK;
+    if (ctx->stage) cudaFree(ctx->stage);
+    ctx->stage = nullptr;
+    ctx->stage_bytes = 0;
+    CK(cudaMalloc(&ctx->stage, bytes));
+    ctx->stage_bytes = bytes;
+    return TPSC_OK;
+}
+
+int copy_out(tpsc_ctx *ctx, void *host, const void *dev, size_t bytes) {
+    CK(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, ctx->st));
+    return TPSC_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+tpsc_ctx *tpsc_create(int device, int *status) {
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        g_static_err = std::string("no CUDA device: ") + cudaGetErrorString(e);
+        if (status) *status = TPSC_ERR_CUDA;
+        return nullptr;
+    }
+    if (device < 0 || device >= ndev) {
+        g_static_err = "device index out of range";
+        if (status) *status = TPSC_ERR_ARG;
+        return nullptr;
+    }
+    tpsc_ctx *ctx = new tpsc_ctx;
+    ctx->device = device;
+    auto bad = [&](cudaError_t er) {
+        g_static_err = cudaGetErrorString(er);
+        if (status) *status = TPSC_ERR_CUDA;
+        tpsc_destroy(ctx);
+        return (tpsc_ctx *)nullptr;
+    };
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return bad(e);
+    if ((e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking)) != cudaSuccess) return bad(e);
+    if ((e = cudaMalloc(&ctx->red.partial, 4 * kMaxBlocks * sizeof(double))) != cudaSuccess) return bad(e);
+    if ((e = cudaMalloc(&ctx->red.result, 8 * sizeof(double))) != cudaSuccess) return bad(e);
+    if ((e = cudaMallocHost(&ctx->h_res, 8 * sizeof(double))) != cudaSuccess) return bad(e);
+    for (auto &ev : ctx->ev)
+        if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bad(e);
+    if (status) *status = TPSC_OK;
+    return ctx;
+}
+
+void tpsc_destroy(tpsc_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    for (auto &kv : ctx->grids) free_grid(kv.second);
+    if (ctx->red.partial) cudaFree(ctx->red.partial);
+    if (ctx->red.result) cudaFree(ctx->red.result);
+    if (ctx->h_res) cudaFreeHost(ctx->h_res);
+    if (ctx->stage) cudaFree(ctx->stage);
+    for (auto &ev : ctx->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->st) cudaStreamDestroy(ctx->st);
+    delete ctx;
+}
+
+const char *tpsc_last_error(const tpsc_ctx *ctx) { return ctx ? ctx->err.c_str() : g_static_err.c_str(); }
+
+int tpsc_set_model(tpsc_ctx *ctx, int nk0, int Nw0, double n, double T, double tp, double tpp, double t3,
+                   double U) {
+    if (!ctx) return fail(nullptr, TPSC_ERR_ARG, "null context");
+    if (!(n > 0.0 && n < 2.0) || !(T > 0.0) || !std::isfinite(U) || !(U > 0.0) || !std::isfinite(tp) ||
+        !std::isfinite(tpp) || !std::isfinite(t3))
+        return fail(ctx, TPSC_ERR_ARG, "need 0 < n < 2, T > 0, U > 0 and finite hoppings");
+    if (!supported_grid(nk0, Nw0))
+        return fail(ctx, TPSC_ERR_ARG, "unsupported grid nk0=" + std::to_string(nk0) + " Nw0=" + std::to_string(Nw0));
+    cudaSetDevice(ctx->device);
+    ctx->nk0 = nk0;
+    ctx->Nw0 = Nw0;
+    ctx->n = n;
+    ctx->T = T;
+    ctx->tp = tp;
+    ctx->tpp = tpp;
+    ctx->t3 = t3;
+    ctx->U = U;
+    ctx->nsr = n > 1.0 ? 2.0 - n : n;  // src/chi.cpp:18-19
+    ctx->Usp = ctx->Uch = 0.0;
+    for (double &s : ctx->scal) s = 0.0;
+    for (auto &kv : ctx->grids) kv.second->have_chi0 = kv.second->have_V = kv.second->have_S = false;
+    ctx->have_model = true;
+    return switch_grid(ctx, nk0, Nw0);
+}
+
+int tpsc_chi0(tpsc_ctx *ctx, int nq0, int nw0) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    rc = switch_grid(ctx, nq0, nw0);
+    if (rc) return rc;
+    return run_chi0(ctx);
+}
+
+int tpsc_trace_chi0(tpsc_ctx *ctx, double out[2]) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    Grid *g = ctx->cur;
+    if (!g->have_chi0) return fail(ctx, TPSC_ERR_STATE, "chi0 has not been computed");
+    CK(launch_trace_chi0(g->d, g->chiq, g->cinf, g->cinf2, ctx->T, ctx->red, ctx->st));
+    double r[2];
+    rc = read_result(ctx, 2, r);
+    if (rc) return rc;
+    const double tr1 = r[0], tr = r[0] + r[1];
+    const double N1 = g->d.nb;
+    out[0] = tr;
+    out[1] = tr + N1 * (tr1 - tr) / (N1 - 2.0 * (g->d.nb - 1));  // src/chi0.cpp:1580
+    ctx->scal[TPSC_S_TR_CHI0] = out[0];
+    ctx->scal[TPSC_S_TR_CHI0_CORR] = out[1];
+    return TPSC_OK;
+}
+
+int tpsc_trace_diff_chi(tpsc_ctx *ctx, int channel, double Uv, double *trace, double *dtrace) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    if (!ctx->cur->have_chi0) return fail(ctx, TPSC_ERR_STATE, "chi0 has not been computed");
+    if (channel != 0 && channel != 1) return fail(ctx, TPSC_ERR_ARG, "channel must be 0 (spin) or 1 (charge)");
+    return sumrule(ctx, channel, Uv, trace, dtrace);
+}
+
+int tpsc_find_Usp_Uch_grid(tpsc_ctx *ctx, int nq0, int nw0, double Usc[2]) {
+    int rc = tpsc_chi0(ctx, nq0, nw0);
+    if (rc) return rc;
+    return roots_Usp_Uch(ctx, Usc);
+}
+
+int tpsc_find_Usp_Uch(tpsc_ctx *ctx) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    double Us_half[2], Us_full[2];
+    // src/chi.cpp:285-306: (nbq-1, nwmax) then twice that
+    rc = tpsc_find_Usp_Uch_grid(ctx, ctx->nk0 / 2, ctx->Nw0 / 2, Us_half);
+    if (rc) return rc;
+    rc = tpsc_find_Usp_Uch_grid(ctx, ctx->nk0, ctx->Nw0, Us_full);
+    if (rc) return rc;
+    ctx->scal[TPSC_S_DIFRELSP] = std::fabs((Us_full[0] - Us_half[0]) / Us_full[0]);
+    ctx->scal[TPSC_S_DIFRELCH] = std::fabs((Us_full[1] - Us_half[1]) / Us_full[1]);
+    set_dblocc(ctx);
+    return TPSC_OK;
+}
+
+int tpsc_vertex(tpsc_ctx *ctx) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    return run_vertex(ctx);
+}
+
+int tpsc_self_energy(tpsc_ctx *ctx) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    return run_self(ctx);
+}
+
+int tpsc_trace_self_G(tpsc_ctx *ctx, double out[2]) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    return trace_self_G(ctx, out);
+}
+
+int tpsc_trace_diff_G(tpsc_ctx *ctx, double mu, double *trace) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    if (!ctx->cur->have_S) return fail(ctx, TPSC_ERR_STATE, "the self-energy has not been computed");
+    return trace_diff_G(ctx, mu, trace);
+}
+
+int tpsc_find_mu(tpsc_ctx *ctx) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    return find_mu(ctx);
+}
+
+int tpsc_solve(tpsc_ctx *ctx) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    rc = switch_grid(ctx, ctx->nk0, ctx->Nw0);
+    if (rc) return rc;
+    rc = run_chi0(ctx);
+    if (rc) return rc;
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    double Usc[2];
+    rc = roots_Usp_Uch(ctx, Usc);
+    if (rc) return rc;
+    set_dblocc(ctx);
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    rc = run_vertex(ctx);
+    if (rc) return rc;
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    rc = run_self(ctx);
+    if (rc) return rc;
+    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    double tsg[2];
+    rc = trace_self_G(ctx, tsg);
+    if (rc) return rc;
+    rc = find_mu(ctx);
+    if (rc) return rc;
+    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    CK(cudaEventSynchronize(ctx->ev[5]));
+    for (int i = 0; i < 5; ++i) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ctx->ev[i], ctx->ev[i + 1]));
+        ctx->stage_ms[i] = ms;
+    }
+    for (int i = 0; i < TPSC_S_COUNT; ++i)
+        if (!std::isfinite(ctx->scal[i])) return fail(ctx, TPSC_ERR_NONFINITE, "non-finite scalar result");
+    return TPSC_OK;
+}
+
+int tpsc_get_scalars(tpsc_ctx *ctx, double *out, int n) {
+    if (!ctx || !out || n < 0) return fail(ctx, TPSC_ERR_ARG, "bad arguments");
+    for (int i = 0; i < n && i < TPSC_S_COUNT; ++i) out[i] = ctx->scal[i];
+    return TPSC_OK;
+}
+
+int tpsc_get_dims(tpsc_ctx *ctx, int dims[4]) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    const GridDev &d = ctx->cur->d;
+    dims[0] = d.nk0;
+    dims[1] = d.nw0;
+    dims[2] = d.nbk;
+    dims[3] = d.n8;
+    return TPSC_OK;
+}
+
+int tpsc_get_ek(tpsc_ctx *ctx, double *ek) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    std::memcpy(ek, ctx->cur->ek_host.data(), ctx->cur->ek_host.size() * sizeof(double));
+    return TPSC_OK;
+}
+
+int tpsc_get_chi0(tpsc_ctx *ctx, double *chiqw, double *chi0_inf, double *chi0_inf2, double *dtau_chirt0) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    Grid *g = ctx->cur;
+    if (!g->have_chi0) return fail(ctx, TPSC_ERR_STATE, "chi0 has not been computed");
+    const GridDev &d = g->d;
+    if (chiqw) {
+        const size_t bytes = (size_t)d.nb * d.n8 * sizeof(double);
+        if ((rc = ensure_stage(ctx, bytes))) return rc;
+        CK(launch_unblock(g->chiq, (double *)ctx->stage, d.nb, d.nb, d.n8, ctx->st));
+        if ((rc = copy_out(ctx, chiqw, ctx->stage, bytes))) return rc;
+    }
+    if (chi0_inf && (rc = copy_out(ctx, chi0_inf, g->cinf, d.n8 * sizeof(double)))) return rc;
+    if (chi0_inf2 && (rc = copy_out(ctx, chi0_inf2, g->cinf2, d.n8 * sizeof(double)))) return rc;
+    if (dtau_chirt0 && (rc = copy_out(ctx, dtau_chirt0, g->dchirt0, d.n8 * sizeof(double)))) return rc;
+    CK(cudaStreamSynchronize(ctx->st));
+    return TPSC_OK;
+}
+
+int tpsc_get_vertex(tpsc_ctx *ctx, double *vertex_rt) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    Grid *g = ctx->cur;
+    if (!g->have_V) return fail(ctx, TPSC_ERR_STATE, "the vertex has not been computed");
+    const GridDev &d = g->d;
+    const size_t bytes = (size_t)d.nb * d.n8 * sizeof(double);
+    if ((rc = ensure_stage(ctx, bytes))) return rc;
+    CK(launch_unblock(g->V, (double *)ctx->stage, d.nb, d.nb, d.n8, ctx->st));
+    if ((rc = copy_out(ctx, vertex_rt, ctx->stage, bytes))) return rc;
+    CK(cudaStreamSynchronize(ctx->st));
+    return TPSC_OK;
+}
+
+int tpsc_get_self(tpsc_ctx *ctx, double *self_kw, double *s2, double *s3, double *s4) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    Grid *g = ctx->cur;
+    if (!g->have_S) return fail(ctx, TPSC_ERR_STATE, "the self-energy has not been computed");
+    const GridDev &d = g->d;
+    if (self_kw) {
+        const size_t bytes = (size_t)(d.nw0 / 2) * d.n8 * sizeof(double2);
+        if ((rc = ensure_stage(ctx, bytes))) return rc;
+        CK(launch_unblock_c(g->S, (double2 *)ctx->stage, d.nw0 / 2, d.nw0 / 2, d.n8, ctx->st));
+        if ((rc = copy_out(ctx, self_kw, ctx->stage, bytes))) return rc;
+    }
+    if (s2 && (rc = copy_out(ctx, s2, g->s2, d.n8 * sizeof(double)))) return rc;
+    if (s3 && (rc = copy_out(ctx, s3, g->s3, d.n8 * sizeof(double)))) return rc;
+    if (s4 && (rc = copy_out(ctx, s4, g->s4, d.n8 * sizeof(double)))) return rc;
+    CK(cudaStreamSynchronize(ctx->st));
+    return TPSC_OK;
+}
+
+int tpsc_stage_times(tpsc_ctx *ctx, double *ms, int n) {
+    if (!ctx || !ms) return fail(ctx, TPSC_ERR_ARG, "bad arguments");
+    for (int i = 0; i < n && i < 5; ++i) ms[i] = ctx->stage_ms[i];
+    return TPSC_OK;
+}
+
+}  // extern "C"

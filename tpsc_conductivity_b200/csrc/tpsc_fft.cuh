@@ -1,0 +1,247 @@
+// tpsc_fft.cuh -- FP64 FFT building blocks for sm_100a.
+//
+// * in-register radix-2/4/8/16 DFTs (exact constants, standard split-radix
+//   style recursion);
+// * a Stockham auto-sort FFT executed by a group of G threads, each thread
+//   holding 16 points, over a padded shared-memory buffer;
+// * a 2D DCT-I of a symmetric nbk x nbk slice held in shared memory.  Two
+//   real rows (columns) are packed into one complex FFT of their even
+//   extension of length L = 2(nbk-1): a real even sequence has a real
+//   spectrum, so Re/Im of the packed transform are the two DCT-I outputs.
+//
+// DCT-I here is FFTW's REDFT00 (unnormalised):
+//   Y_k = X_0 + (-1)^k X_{n-1} + 2 sum_{j=1}^{n-2} X_j cos(pi j k/(n-1)).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tpsc {
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+// multiply by -i (SIGN = -1) or +i (SIGN = +1)
+template <int SIGN>
+__device__ __forceinline__ double2 mul_i(double2 a) {
+    return SIGN < 0 ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
+}
+
+// exp(sign * 2 pi i m / 16) for the constant twiddles of the radix-8/16
+// kernels; m is a compile-time constant after unrolling, so the switch folds.
+__device__ __forceinline__ double2 w16(int m, int sign) {
+    const double c1 = 0.92387953251128675613;  // cos(pi/8)
+    const double s1 = 0.38268343236508977173;  // sin(pi/8)
+    const double c2 = 0.70710678118654752440;  // cos(pi/4)
+    double c, s;
+    switch (m & 15) {
+        case 0: c = 1; s = 0; break;
+        case 1: c = c1; s = s1; break;
+        case 2: c = c2; s = c2; break;
+        case 3: c = s1; s = c1; break;
+        case 4: c = 0; s = 1; break;
+        case 5: c = -s1; s = c1; break;
+        case 6: c = -c2; s = c2; break;
+        case 7: c = -c1; s = s1; break;
+        case 8: c = -1; s = 0; break;
+        case 9: c = -c1; s = -s1; break;
+        case 10: c = -c2; s = -c2; break;
+        case 11: c = -s1; s = -c1; break;
+        case 12: c = 0; s = -1; break;
+        case 13: c = s1; s = -c1; break;
+        case 14: c = c2; s = -c2; break;
+        default: c = c1; s = -s1; break;
+    }
+    return make_double2(c, sign * s);
+}
+
+// In-register DFT of length R on v[0..R) with stride S inside the array
+// (elements v[OFF + k*S]).  X_k = sum_j x_j exp(SIGN 2 pi i jk/R).
+template <int SIGN, int R, int S = 1, int OFF = 0, int NV>
+__device__ __forceinline__ void dft(double2 (&v)[NV]) {
+    if constexpr (R == 1) {
+        return;
+    } else if constexpr (R == 2) {
+        double2 a = v[OFF], b = v[OFF + S];
+        v[OFF] = cadd(a, b);
+        v[OFF + S] = csub(a, b);
+    } else if constexpr (R == 4) {
+        double2 a = v[OFF], b = v[OFF + S], c = v[OFF + 2 * S], d = v[OFF + 3 * S];
+        double2 t0 = cadd(a, c), t1 = csub(a, c), t2 = cadd(b, d), t3 = mul_i<SIGN>(csub(b, d));
+        v[OFF] = cadd(t0, t2);
+        v[OFF + 2 * S] = csub(t0, t2);
+        v[OFF + S] = cadd(t1, t3);
+        v[OFF + 3 * S] = csub(t1, t3);
+    } else {
+        // radix-2 decimation in time: even/odd halves are DFTs of length R/2
+        // taken on the sub-sequences at stride 2S; results interleaved back.
+        constexpr int H = R / 2;
+        double2 e[H], o[H];
+#pragma unroll
+        for (int k = 0; k < H; ++k) {
+            e[k] = v[OFF + (2 * k) * S];
+            o[k] = v[OFF + (2 * k + 1) * S];
+        }
+        dft<SIGN, H, 1, 0>(e);
+        dft<SIGN, H, 1, 0>(o);
+#pragma unroll
+        for (int k = 0; k < H; ++k) {
+            const double2 w = w16((16 / R) * k, SIGN);
+            double2 t = cmul(o[k], w);
+            v[OFF + k * S] = cadd(e[k], t);
+            v[OFF + (k + H) * S] = csub(e[k], t);
+        }
+    }
+}
+
+// padded index into an FFT scratch buffer: one complex of padding every 16
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr int padded_len(int n) { return n + n / 16; }
+
+// Group barrier: G threads with consecutive thread ids starting at a multiple
+// of G.  Groups inside one warp use a lane mask; a group spanning the whole
+// block uses __syncthreads; otherwise a named barrier per group.
+template <int G>
+__device__ __forceinline__ void group_sync(int grp) {
+    if constexpr (G < 32) {
+        const unsigned lane0 = (threadIdx.x & 31) & ~(G - 1);
+        const unsigned mask = ((G == 32) ? 0xffffffffu : ((1u << G) - 1u)) << lane0;
+        __syncwarp(mask);
+    } else if constexpr (G == 32) {
+        __syncwarp();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"r"(grp + 1), "r"(G) : "memory");
+    }
+}
+
+// One Stockham pass of radix R over x[0..N) (padded layout), performed by a
+// group of G threads holding E points each; thread t does E/R butterflies
+// b = t + G u.  tw[m] = exp(-2 pi i m / N), m < N.
+template <int N, int G, int R, int SIGN, int E>
+__device__ __forceinline__ void stockham_pass(double2 *x, int t, int Ns, const double2 *__restrict__ tw,
+                                              int grp) {
+    constexpr int NB = E / R;  // butterflies per thread
+    double2 v[E];
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+        const int b = t + G * u;
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[u * R + q] = x[pidx(b + q * (N / R))];
+    }
+    group_sync<G>(grp);
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+        const int b = t + G * u;
+        const int k = b % Ns;
+        if (Ns > 1) {
+            // twiddle exp(SIGN 2 pi i k q / (Ns R)) = tw[k q N/(Ns R)] (conjugated for SIGN>0)
+            const int step = k * (N / (Ns * R));
+#pragma unroll
+            for (int q = 1; q < R; ++q) {
+                double2 w = __ldg(&tw[(step * q) & (N - 1)]);
+                if (SIGN > 0) w.y = -w.y;
+                v[u * R + q] = cmul(v[u * R + q], w);
+            }
+        }
+        double2 r[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) r[q] = v[u * R + q];
+        dft<SIGN, R>(r);
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[u * R + q] = r[q];
+    }
+#pragma unroll
+    for (int u = 0; u < NB; ++u) {
+        const int b = t + G * u;
+        const int k = b % Ns;
+        const int base = (b / Ns) * Ns * R + k;
+#pragma unroll
+        for (int q = 0; q < R; ++q) x[pidx(base + q * Ns)] = v[u * R + q];
+    }
+    group_sync<G>(grp);
+}
+
+template <int N>
+struct FftPlan {
+    // radix-16 passes followed by one pass of radix N / 16^P16 (if > 1);
+    // each of the G threads holds E = min(16, N) points
+    static constexpr int log2n() {
+        int l = 0;
+        while ((1 << l) < N) ++l;
+        return l;
+    }
+    static constexpr int P16 = log2n() / 4;
+    static constexpr int RLAST = 1 << (log2n() % 4);
+    static constexpr int E = N < 16 ? N : 16;
+    static constexpr int G = N / E;
+};
+
+// In-place FFT of x[0..N) (padded layout) by a group of G = FftPlan<N>::G
+// threads.  Must be called by all G threads of the group; x is synchronised
+// within the group on exit.
+template <int N, int SIGN>
+__device__ __forceinline__ void group_fft(double2 *x, int t, const double2 *__restrict__ tw, int grp) {
+    static_assert(N >= 4 && (N & (N - 1)) == 0, "power of two >= 4");
+    constexpr int G = FftPlan<N>::G;
+    constexpr int E = FftPlan<N>::E;
+    int Ns = 1;
+#pragma unroll
+    for (int p = 0; p < FftPlan<N>::P16; ++p) {
+        stockham_pass<N, G, 16, SIGN, E>(x, t, Ns, tw, grp);
+        Ns *= 16;
+    }
+    if constexpr (FftPlan<N>::RLAST > 1) {
+        stockham_pass<N, G, FftPlan<N>::RLAST, SIGN, E>(x, t, Ns, tw, grp);
+    }
+}
+
+// 2D DCT-I (REDFT00 x REDFT00) in place on a symmetric NBK x NBK slice S
+// (row-major, leading dimension NBK, which is odd so that column accesses
+// are bank-conflict free).  scr: per-group FFT scratch, group g at
+// scr + g * padded_len(L).  All threads of the block must call.
+template <int NBK>
+__device__ void dct2_slice(double *S, double2 *scr, const double2 *__restrict__ tw) {
+    constexpr int L = 2 * (NBK - 1);
+    constexpr int G = FftPlan<L>::G;
+    constexpr int NPAIR = (NBK + 1) / 2;
+    const int tid = threadIdx.x;
+    const int grp = tid / G;
+    const int t = tid % G;
+    const int ngrp = blockDim.x / G;
+    double2 *x = scr + grp * padded_len(L);
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+        // pass 0: rows (stride 1 along the line, NBK between lines)
+        // pass 1: columns (stride NBK along the line, 1 between lines)
+        const int es = pass == 0 ? 1 : NBK;
+        const int ls = pass == 0 ? NBK : 1;
+#pragma unroll 1
+        for (int p = grp; p < NPAIR; p += ngrp) {
+            const int r0 = 2 * p, r1 = 2 * p + 1;
+            const bool two = r1 < NBK;
+            const double *a = S + r0 * ls;
+            const double *b = S + r1 * ls;
+#pragma unroll 4
+            for (int j = t; j < L; j += G) {
+                const int c = j < NBK ? j : L - j;
+                x[pidx(j)] = make_double2(a[c * es], two ? b[c * es] : 0.0);
+            }
+            group_sync<G>(grp);
+            group_fft<L, -1>(x, t, tw, grp);
+            double *ao = S + r0 * ls;
+            double *bo = S + r1 * ls;
+#pragma unroll 4
+            for (int k = t; k < NBK; k += G) {
+                const double2 z = x[pidx(k)];
+                ao[k * es] = z.x;
+                if (two) bo[k * es] = z.y;
+            }
+            group_sync<G>(grp);
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace tpsc

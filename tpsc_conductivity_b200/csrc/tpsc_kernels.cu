@@ -1,0 +1,1228 @@
+// tpsc_kernels.cu -- sm_100a kernels of the TPSC hot path (FP64).
+//
+// Two kernel families do the transforms:
+//  * slice kernels: one CTA per imaginary-time (or bosonic-frequency) slice.
+//    The symmetric nbk x nbk quadrant of the slice lives in shared memory and
+//    is transformed by a 2D DCT-I (tpsc_fft.cuh).  They replace the OpenMP
+//    tau loops of chi0::calc_chiqw_FFT_spline (src/chi0.cpp:454-559),
+//    chi::calc_chirt (src/chi.cpp:85-119) and green::calc_Self_FFT_spline
+//    (src/green.cpp:1822-1892), which call FFTW REDFT00 per slice.
+//  * tau kernels: one CTA per block of four octant columns.  The column data
+//    (contiguous in the column-block layout) is staged in shared memory, the
+//    clamped cubic spline along tau is solved in place, and the FFT of the
+//    spline's third derivative gives the Matsubara values.  They replace the
+//    per-q / per-k loops of src/chi0.cpp:586-690 and src/green.cpp:1925-2017
+//    (LAPACK dgbsv + FFTW dft) and the 1D DCT-I over n of src/chi.cpp:129-144.
+// Reductions (sum rules, traces) are two-pass and deterministic.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tpsc_fft.cuh"
+#include "tpsc_kernels.cuh"
+
+namespace tpsc {
+
+namespace {
+
+constexpr double kPi = 3.141592653589793;  // == acos(-1.0) in double
+constexpr int kSliceThreads = 256;
+constexpr int kTauThreads = 256;
+constexpr int kWarm = 40;  // spline sweep warm-up: carry error <= 0.268^40
+
+__device__ __forceinline__ void oct_lm(const uint32_t *lm, int o, int &l, int &m) {
+    const uint32_t v = __ldg(&lm[o]);
+    l = (int)(v >> 16);
+    m = (int)(v & 0xffffu);
+}
+
+// integer multiplicity weight of octant point (l, m) as in the reference
+// loops: `base` halved on the l edges, m edges and the diagonal
+__device__ __forceinline__ int oct_weight(int base, int l, int m, int nbk) {
+    int w = base;
+    if (l == 0 || l == nbk - 1) w /= 2;
+    if (m == 0 || m == nbk - 1) w /= 2;
+    if (m == l) w /= 2;
+    return w;
+}
+
+// ---------------------------------------------------------------------------
+// reductions: per-thread compensated (Kahan-Babuska) sums -> warp -> block ->
+// per-block partials -> one block finishes in a fixed order
+// ---------------------------------------------------------------------------
+struct KSum {
+    double s = 0.0, c = 0.0;
+    __device__ __forceinline__ void add(double x) {
+        const double t = s + x;
+        if (fabs(s) >= fabs(x))
+            c += (s - t) + x;
+        else
+            c += (x - t) + s;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return s + c; }
+};
+
+template <int NV>
+__device__ void block_store(double (&v)[NV], double *partial) {
+    __shared__ double red[32][NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) red[warp][k] = v[k];
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double x = lane < nw ? red[lane][k] : 0.0;
+            for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+            if (lane == 0) partial[k * kMaxBlocks + blockIdx.x] = x;
+        }
+    }
+}
+
+template <int NV>
+__global__ void k_finish(const double *partial, int nblocks, double *result, double offset0) {
+    KSum acc[NV];
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[k].add(partial[k * kMaxBlocks + b]);
+    // every thread's compensated partial, added by one thread in a fixed
+    // order: deterministic from run to run
+    __shared__ double all[256][NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) all[threadIdx.x][k] = acc[k].value();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            KSum s;
+            for (int i = 0; i < (int)blockDim.x; ++i) s.add(all[i][k]);
+            result[k] = s.value() + (k == 0 ? offset0 : 0.0);
+        }
+    }
+}
+
+int grid_for(long long total, int threads) {
+    long long b = (total + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > kMaxBlocks) b = kMaxBlocks;
+    return (int)b;
+}
+
+template <int NV>
+cudaError_t finish(Reduce r, int nblocks, double offset0, cudaStream_t st) {
+    k_finish<NV><<<1, 256, 0, st>>>(r.partial, nblocks, r.result, offset0);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// mu0 of the finite lattice: sum_o w 2 f(eps - mu) / L^2 - n
+// (green0::ddensity_mu_PBC, src/green0.cpp:182-203)
+// ---------------------------------------------------------------------------
+__global__ void k_density(const double *__restrict__ ek, const uint32_t *__restrict__ lm, int n8, int nbk,
+                          double mu, double T, double nk2, double *partial) {
+    KSum acc;
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n8; o += gridDim.x * blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        const int w = oct_weight(8, l, m, nbk);
+        acc.add(2 * w / ((exp((ek[o] - mu) / T) + 1.0) * nk2));
+    }
+    double v[1] = {acc.value()};
+    block_store<1>(v, partial);
+}
+
+// ---------------------------------------------------------------------------
+// slice kernels
+// ---------------------------------------------------------------------------
+template <int NBK>
+struct SliceSmem {
+    static constexpr int L = 2 * (NBK - 1);
+    static constexpr int G = FftPlan<L>::G;
+    static constexpr int NGRP = kSliceThreads / G;
+    static constexpr size_t slice_bytes = (size_t)NBK * NBK * sizeof(double);
+    static constexpr size_t scr_off = (slice_bytes + 15) & ~(size_t)15;
+    static constexpr size_t bytes = scr_off + (size_t)NGRP * padded_len(L) * sizeof(double2);
+};
+
+template <int NBK>
+__device__ __forceinline__ double2 *slice_scratch(double *S) {
+    return reinterpret_cast<double2 *>(reinterpret_cast<char *>(S) + SliceSmem<NBK>::scr_off);
+}
+
+// write octant value v of point (l, m) into both triangles of the slice
+template <int NBK>
+__device__ __forceinline__ void put_sym(double *S, int l, int m, double v) {
+    S[l * NBK + m] = v;
+    S[m * NBK + l] = v;
+}
+
+// G(r, tau_j) = DCT-I[ G0(k, tau_j) / L^2 ], tau_j = j / (Nw0 T), j = 0..Nw0,
+// with the overflow-safe branches of src/green.cpp:1834-1837.  The chi0 stage
+// needs G(r, tau) and G(r, -tau) (src/chi0.cpp:462-495); G(r,-tau) =
+// -G(r, beta - tau), so one table serves both stages.  Plain layout
+// Grt[j * n8 + o].
+template <int NBK>
+__global__ void __launch_bounds__(kSliceThreads, 1)
+    k_gslice(const double *__restrict__ ek, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
+             double mu0, int n8, int nw0, double T, double nk02, double *__restrict__ Grt) {
+    extern __shared__ __align__(16) double S[];
+    const int j = blockIdx.x;
+    const double t = j / (nw0 * T);
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        const double x = ek[o] - mu0;
+        double g;
+        if (x > 0)
+            g = -exp(-t * x) / (exp(-x / T) + 1.0) / nk02;
+        else
+            g = -exp((1.0 / T - t) * x) / (exp(x / T) + 1.0) / nk02;
+        put_sym<NBK>(S, l, m, g);
+    }
+    __syncthreads();
+    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tw);
+    double *out = Grt + (size_t)j * n8;
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        out[o] = S[l * NBK + m];
+    }
+}
+
+// chi0(r, tau_j) = -2 G(r, tau_j) G(r, -tau_j) and its DCT-I chi0(q, tau_j),
+// j = 0..Nw0/2 (src/chi0.cpp:393-418, 497-517, 545-558).  tau = 0 uses
+// G(r,0-) = G(r,0+) + delta_r0, tau = beta/2 uses 2 G^2.
+template <int NBK>
+__global__ void __launch_bounds__(kSliceThreads, 1)
+    k_chi0_slice(const double *__restrict__ Grt, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
+                 int n8, int nw0, double *__restrict__ chirt, double *__restrict__ chiq) {
+    extern __shared__ __align__(16) double S[];
+    const int j = blockIdx.x;
+    const int nb = nw0 / 2 + 1;
+    const double *gp = Grt + (size_t)j * n8;
+    const double *gm = Grt + (size_t)(nw0 - j) * n8;
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        const double a = gp[o];
+        double c;
+        if (j == 0)
+            c = (o == 0) ? -2.0 * a * (a + 1.0) : -2.0 * a * a;
+        else if (j == nb - 1)
+            c = 2.0 * a * a;
+        else
+            c = -2.0 * (-gm[o]) * a;
+        chirt[bidx(j, o, nb)] = c;
+        put_sym<NBK>(S, l, m, c);
+    }
+    __syncthreads();
+    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tw);
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        chiq[bidx(j, o, nb)] = S[l * NBK + m];
+    }
+}
+
+// d/dtau G(r,0+-) and d/dtau chi0(r,0), d/dtau chi0(q,0): the spline's left
+// end condition (src/chi0.cpp:323-367, 420-447).  One CTA.
+template <int NBK>
+__global__ void __launch_bounds__(kSliceThreads, 1)
+    k_chi0_boundary(const double *__restrict__ ek, const double *__restrict__ er, const uint32_t *__restrict__ lm,
+                    const double2 *__restrict__ tw, const double *__restrict__ Grt, int n8, double mu0, double T,
+                    double nk02, double *__restrict__ dG0p, double *__restrict__ dtau_chirt0,
+                    double *__restrict__ dtau_chiqt0) {
+    extern __shared__ __align__(16) double S[];
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        const double x = ek[o] - mu0;
+        const double gkt = -1.0 / (exp(-x / T) + 1.0);
+        put_sym<NBK>(S, l, m, -x * gkt / nk02);
+    }
+    __syncthreads();
+    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tw);
+    // every thread handles the same octant points in both loops, so the
+    // first loop's S reads complete before its second-loop writes
+    double dp_[(NBK * (NBK + 1) / 2 + kSliceThreads - 1) / kSliceThreads];
+    double dc_[(NBK * (NBK + 1) / 2 + kSliceThreads - 1) / kSliceThreads];
+    int k = 0;
+    for (int o = threadIdx.x; o < n8; o += blockDim.x, ++k) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        const double dp = S[l * NBK + m];
+        const double dm = ((o == 0) ? -mu0 : er[o]) - dp;
+        const double g0 = Grt[o];
+        const double dc = (o == 0) ? -2.0 * (dp * (1.0 + g0) + dm * g0) : -2.0 * (dp * g0 + dm * g0);
+        dp_[k] = dp;
+        dc_[k] = dc;
+    }
+    __syncthreads();
+    k = 0;
+    for (int o = threadIdx.x; o < n8; o += blockDim.x, ++k) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        dG0p[o] = dp_[k];
+        dtau_chirt0[o] = dc_[k];
+        put_sym<NBK>(S, l, m, dc_[k]);
+    }
+    __syncthreads();
+    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tw);
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        dtau_chiqt0[o] = S[l * NBK + m];
+    }
+}
+
+// V(q, iqn) = (T/L^2) U [3 Usp (chisp - chi0) + Uch (chich - chi0)] / 8 and
+// its DCT-I over q, one bosonic frequency per CTA (src/chi.cpp:89-115).
+template <int NBK>
+__global__ void __launch_bounds__(kSliceThreads, 1)
+    k_vertex_q(const double *__restrict__ chiq, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
+               int n8, int nb, double normFact, double U, double Usp, double Uch, double *__restrict__ Vr) {
+    extern __shared__ __align__(16) double S[];
+    const int j = blockIdx.x;
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        const double c0 = chiq[bidx(j, o, nb)];
+        const double sp = c0 / (1.0 - Usp * c0 / 2.0);
+        const double ch = c0 / (1.0 + Uch * c0 / 2.0);
+        put_sym<NBK>(S, l, m, normFact * U * (3.0 * Usp * (sp - c0) + Uch * (ch - c0)) / 8.0);
+    }
+    __syncthreads();
+    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tw);
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        Vr[bidx(j, o, nb)] = S[l * NBK + m];
+    }
+}
+
+// d/dtau Sigma(k, 0) and d/dtau Sigma(k, beta): the spline end conditions of
+// the self-energy (src/green.cpp:1743-1817).  One CTA, two 2D DCT-I.
+template <int NBK>
+__global__ void __launch_bounds__(kSliceThreads, 1)
+    k_sigma_boundary(const double *__restrict__ er, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
+                     const double *__restrict__ Grt, const double *__restrict__ V, const double *__restrict__ dtau_chirt0,
+                     const double *__restrict__ dG0p, int n8, int nw0, int n8p, double mu0, double fact,
+                     double *__restrict__ dS) {
+    extern __shared__ __align__(16) double S[];
+    const int nb = nw0 / 2 + 1;
+#pragma unroll 1
+    for (int side = 0; side < 2; ++side) {
+        const double *g = Grt + (side == 0 ? 0 : (size_t)nw0 * n8);
+        for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+            int l, m;
+            oct_lm(lm, o, l, m);
+            const double v0 = V[bidx(0, o, nb)];
+            double val;
+            if (side == 0) {
+                val = (fact * dtau_chirt0[o]) * g[o] + v0 * dG0p[o];
+            } else {
+                const double xi = (o == 0) ? -mu0 : er[o];
+                val = (-fact * dtau_chirt0[o]) * g[o] + v0 * (-dG0p[o] + xi);
+            }
+            put_sym<NBK>(S, l, m, val);
+        }
+        __syncthreads();
+        dct2_slice<NBK>(S, slice_scratch<NBK>(S), tw);
+        for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+            int l, m;
+            oct_lm(lm, o, l, m);
+            dS[side * n8p + o] = S[l * NBK + m];
+        }
+        __syncthreads();
+    }
+}
+
+// Sigma(k, tau_j) = DCT-I[ G(r, tau_j) V(r, tau_j) ], j = 0..Nw0, with
+// V(r, tau_j) = V(r, beta - tau_j) for tau_j > beta/2 (src/green.cpp:1822-1885).
+template <int NBK>
+__global__ void __launch_bounds__(kSliceThreads, 1)
+    k_sigma_slice(const double *__restrict__ Grt, const double *__restrict__ V, const uint32_t *__restrict__ lm,
+                  const double2 *__restrict__ tw, int n8, int nw0, double *__restrict__ sigt) {
+    extern __shared__ __align__(16) double S[];
+    const int j = blockIdx.x;
+    const int nb = nw0 / 2 + 1;
+    const int jv = j < nb ? j : nw0 - j;
+    const double *g = Grt + (size_t)j * n8;
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        put_sym<NBK>(S, l, m, g[o] * V[bidx(jv, o, nb)]);
+    }
+    __syncthreads();
+    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tw);
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        sigt[bidx(j, o, nw0 + 1)] = S[l * NBK + m];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// tau kernels
+// ---------------------------------------------------------------------------
+
+// Clamped cubic spline through y[0..NJ) on a uniform grid of step h with end
+// slopes d0, dN: on exit y holds the node second derivatives M_j.  Solves
+//   2 M_0 + M_1 = 6/h ((V_1 - V_0)/h - d0)
+//   M_{i-1} + 4 M_i + M_{i+1} = 6/h^2 (V_{i+1} - 2 V_i + V_{i-1})
+//   M_{N-1} + 2 M_N = 6/h (dN - (V_N - V_{N-1})/h)
+// -- the same interpolant as generique::spline_coeffs_rel
+// (src/generique.cpp:214-322), S_j''' = 6 a_j = (M_{j+1} - M_j)/h -- by the
+// Thomas algorithm with pivots invp = 1/p_i and multipliers cp_i (cp_N = 0)
+// precomputed on the host.  The sweeps are split over TPC threads per column:
+// each chunk starts its carry kWarm rows early from zero; the carry decays
+// by 1/p_i <= 1/(2+sqrt3) per row, so the truncation error is below 1e-22 of
+// the local magnitude.  All threads of the block must call.
+__device__ void spline_second_derivatives(double *A, int lda, int NJ, double h, const double *d0, const double *dN,
+                                          const double *__restrict__ invp, const double *__restrict__ cp) {
+    const int TPC = blockDim.x / 4;
+    const int c = threadIdx.x / TPC, k = threadIdx.x % TPC;
+    double *y = A + c * lda;
+    const int C = (NJ + TPC - 1) / TPC;
+    const int s = min(k * C, NJ), e = min(s + C, NJ);
+    const int N = NJ - 1;
+    const double a6 = 6.0 / (h * h), b6 = 6.0 / h;
+    const double dl = d0[c], dr = dN[c];
+    auto rhs = [&](int i, double vm, double v0, double vp) -> double {
+        if (i == 0) return b6 * ((vp - v0) / h - dl);
+        if (i == N) return b6 * (dr - (v0 - vm) / h);
+        return a6 * (vp - 2.0 * v0 + vm);
+    };
+    double carry = 0.0, vm_h = 0.0, vs_h = 0.0, ve_h = 0.0;
+    if (s < e) {
+        if (s > 0) {
+            const int i0 = max(0, s - kWarm);
+            double cc = 0.0;
+            double vm = i0 > 0 ? y[i0 - 1] : 0.0, v0 = y[i0];
+            for (int i = i0; i < s; ++i) {
+                const double vp = y[i + 1];
+                cc = (rhs(i, vm, v0, vp) - cc) * __ldg(&invp[i]);
+                vm = v0;
+                v0 = vp;
+            }
+            carry = cc;
+            vm_h = y[s - 1];
+        }
+        vs_h = y[s];
+        ve_h = e < NJ ? y[e] : 0.0;
+    }
+    __syncthreads();
+    if (s < e) {
+        double vm = vm_h, v0 = vs_h;
+        for (int i = s; i < e; ++i) {
+            const double vp = (i + 1 < e) ? y[i + 1] : ve_h;
+            const double dp = (rhs(i, vm, v0, vp) - carry) * __ldg(&invp[i]);
+            y[i] = dp;
+            carry = dp;
+            vm = v0;
+            v0 = vp;
+        }
+    }
+    __syncthreads();
+    double mc = 0.0;
+    if (s < e && e < NJ) {
+        const int i1 = min(N, e - 1 + kWarm);
+        double mm = 0.0;
+        for (int i = i1; i >= e; --i) mm = y[i] - __ldg(&cp[i]) * mm;
+        mc = mm;
+    }
+    __syncthreads();
+    if (s < e) {
+        double mm = mc;
+        for (int i = e - 1; i >= s; --i) {
+            mm = y[i] - __ldg(&cp[i]) * mm;
+            y[i] = mm;
+        }
+    }
+    __syncthreads();
+}
+
+// per-column sum of y[i0..i1) over the TPC threads of each column -> out[c]
+__device__ void column_sums(const double *A, int lda, int i0, int i1, double *out) {
+    const int TPC = blockDim.x / 4;
+    const int c = threadIdx.x / TPC, k = threadIdx.x % TPC;
+    KSum acc;
+    for (int i = i0 + k; i < i1; i += TPC) acc.add(A[c * lda + i]);
+    __shared__ double part[1024];
+    part[threadIdx.x] = acc.value();
+    __syncthreads();
+    if (k == 0) {
+        KSum s;
+        for (int q = 0; q < TPC; ++q) s.add(part[c * TPC + q]);
+        out[c] = s.value();
+    }
+    __syncthreads();
+}
+
+template <int N>
+struct TauSmem {
+    static constexpr int threads = (N / 16) > kTauThreads ? (N / 16) : kTauThreads;
+    static size_t bytes(int NJ) {
+        size_t a = ((size_t)4 * NJ * sizeof(double) + 15) & ~(size_t)15;
+        return a + (size_t)padded_len(N) * sizeof(double2);
+    }
+};
+
+__device__ __forceinline__ void stage_in(double *A, const double *g, int NJ) {
+    for (int i = threadIdx.x; i < 4 * NJ; i += blockDim.x) A[(i & 3) * NJ + (i >> 2)] = g[i];
+}
+__device__ __forceinline__ void stage_out(const double *A, double *g, int NJ) {
+    for (int i = threadIdx.x; i < 4 * NJ; i += blockDim.x) g[i] = A[(i & 3) * NJ + (i >> 2)];
+}
+
+// chi0(q, iqn) from chi0(q, tau_j), j = 0..Nw0/2, for the four columns of one
+// block, in place (src/chi0.cpp:586-690): clamped spline with slopes
+// d/dtau chi0(q,0) and 0 at beta/2; FFT_{Nw0}[6 a_j antisymmetrised]
+// (exp(+2 pi i jk/N)); chi0(q,0) = 2 * integral of the spline;
+// chi0(q,iqn) = c2/qn^2 + [(1 - cos th) Re F + sin th Im F]/qn^4.
+template <int N>
+__global__ void __launch_bounds__(TauSmem<N>::threads, 1)
+    k_chi0_tau(double *__restrict__ chiq, const double *__restrict__ dtau_chiqt0, double *__restrict__ chi0_inf,
+               double *__restrict__ chi0_inf2, const double *__restrict__ spl, const double2 *__restrict__ tw,
+               double T, int n8) {
+    constexpr int NJ = N / 2 + 1;
+    extern __shared__ __align__(16) double A[];
+    double2 *X = reinterpret_cast<double2 *>(A + ((4 * NJ + 1) & ~1));
+    __shared__ double d0[4], dN[4], V0[4], VN[4], sV[4], sM[4], integ[4];
+    const int o0 = 4 * blockIdx.x;
+    double *g = chiq + (size_t)blockIdx.x * 4 * NJ;
+    stage_in(A, g, NJ);
+    if (threadIdx.x < 4) {
+        const int o = o0 + threadIdx.x;
+        d0[threadIdx.x] = o < n8 ? dtau_chiqt0[o] : 0.0;
+        dN[threadIdx.x] = 0.0;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        V0[threadIdx.x] = A[threadIdx.x * NJ];
+        VN[threadIdx.x] = A[threadIdx.x * NJ + NJ - 1];
+    }
+    column_sums(A, NJ, 0, NJ, sV);
+    const double h = 1.0 / (N * T);
+    spline_second_derivatives(A, NJ, NJ, h, d0, dN, spl, spl + NJ);
+    column_sums(A, NJ, 0, NJ, sM);
+    if (threadIdx.x < 4) {
+        const int c = threadIdx.x;
+        const double M0 = A[c * NJ], MN = A[c * NJ + NJ - 1];
+        // sum_j [h (V_j + V_{j+1})/2 - h^3 (M_j + M_{j+1})/24]
+        integ[c] = h * (sV[c] - 0.5 * (V0[c] + VN[c])) - h * h * h / 24.0 * (2.0 * sM[c] - M0 - MN);
+    }
+    __syncthreads();
+    constexpr int G = FftPlan<N>::G;
+#pragma unroll 1
+    for (int pr = 0; pr < 2; ++pr) {
+        const double *Ma = A + (2 * pr) * NJ;
+        const double *Mb = A + (2 * pr + 1) * NJ;
+        for (int j = threadIdx.x; j < N; j += blockDim.x) {
+            const bool lo = j < N / 2;
+            const int jj = lo ? j : N - 1 - j;
+            const double sg = lo ? 1.0 : -1.0;
+            X[pidx(j)] = make_double2(sg * (Ma[jj + 1] - Ma[jj]) / h, sg * (Mb[jj + 1] - Mb[jj]) / h);
+        }
+        __syncthreads();
+        if (threadIdx.x < G) group_fft<N, +1>(X, threadIdx.x, tw, 0);
+        __syncthreads();
+        for (int n = threadIdx.x + 1; n < NJ; n += blockDim.x) {
+            const double2 Z = X[pidx(n)];
+            const double2 Zc = X[pidx(N - n)];
+            // split the packed transform: F_a = (Z_n + conj Z_{N-n})/2, F_b = (Z_n - conj Z_{N-n})/(2i)
+            const double2 Fa = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
+            const double2 Fb = make_double2(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
+            const double wn = 2 * n * kPi * T;
+            const double2 w = __ldg(&tw[n]);
+            const double cth = w.x, sth = -w.y;  // cos, sin of 2 pi n / N
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int c = 2 * pr + q;
+                const int o = o0 + c;
+                const double2 F = q == 0 ? Fa : Fb;
+                const double cinf = -2.0 * d0[c];
+                double val = cinf / (wn * wn) + ((1.0 - cth) * F.x + sth * F.y) / (wn * wn * wn * wn);
+                if (o == 0) val = 0.0;
+                A[c * NJ + n] = val;
+                if (n == NJ - 1 && o < n8) chi0_inf2[o] = (o == 0) ? 0.0 : 2.0 * F.x;
+            }
+        }
+        if (threadIdx.x < 2) A[(2 * pr + threadIdx.x) * NJ] = 2.0 * integ[2 * pr + threadIdx.x];
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) {
+        const int o = o0 + threadIdx.x;
+        if (o < n8) chi0_inf[o] = (o == 0) ? 0.0 : -2.0 * d0[threadIdx.x];
+    }
+    stage_out(A, g, NJ);
+}
+
+// V(r, tau_j) = DCT-I_n[ V(r, iqn) ] + U(3 Usp + Uch)/8 chi0(r, tau_j), in
+// place on one column block (src/chi.cpp:129-166).
+template <int N>
+__global__ void __launch_bounds__(TauSmem<N>::threads, 1)
+    k_vertex_tau(double *__restrict__ Vr, const double *__restrict__ chirt, const double2 *__restrict__ tw,
+                 double fact) {
+    constexpr int NJ = N / 2 + 1;
+    extern __shared__ __align__(16) double A[];
+    double2 *X = reinterpret_cast<double2 *>(A + ((4 * NJ + 1) & ~1));
+    double *g = Vr + (size_t)blockIdx.x * 4 * NJ;
+    const double *cr = chirt + (size_t)blockIdx.x * 4 * NJ;
+    stage_in(A, g, NJ);
+    __syncthreads();
+    constexpr int G = FftPlan<N>::G;
+#pragma unroll 1
+    for (int pr = 0; pr < 2; ++pr) {
+        double *a = A + (2 * pr) * NJ;
+        double *b = A + (2 * pr + 1) * NJ;
+        for (int j = threadIdx.x; j < N; j += blockDim.x) {
+            const int jj = j < NJ ? j : N - j;
+            X[pidx(j)] = make_double2(a[jj], b[jj]);
+        }
+        __syncthreads();
+        if (threadIdx.x < G) group_fft<N, -1>(X, threadIdx.x, tw, 0);
+        __syncthreads();
+        for (int n = threadIdx.x; n < NJ; n += blockDim.x) {
+            const double2 Z = X[pidx(n)];
+            a[n] = Z.x;
+            b[n] = Z.y;
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < 4 * NJ; i += blockDim.x) g[i] = A[(i & 3) * NJ + (i >> 2)] + fact * cr[i];
+}
+
+// Sigma(k, i w_n) coefficients from Sigma(k, tau_j), j = 0..Nw0, for one
+// column block (src/green.cpp:1935-2017): clamped spline with the two end
+// slopes; F_n = sum_j exp(i pi j (2n+1)/N) 6 a_j (pre-twiddled FFT,
+// exp(+2 pi i jk/N)); S_n = (1 - exp(i (2n+1) pi/N)) F_n for n < N/2.
+// Sigma_inf2 = S'(0)+S'(beta), Sigma_inf3 = -(S''(0)+S''(beta)),
+// Sigma_inf4 = Re S_{N/2-1}, Sigma_inf = -(S(0)+S(beta)) at k = 0.
+template <int N>
+__global__ void __launch_bounds__(TauSmem<N>::threads, 1)
+    k_sigma_tau(const double *__restrict__ sigt, const double *__restrict__ dS, double2 *__restrict__ Sout,
+                double *__restrict__ s2, double *__restrict__ s3, double *__restrict__ s4, double *__restrict__ sinf,
+                const double *__restrict__ spl, const double2 *__restrict__ tw, const double2 *__restrict__ ht,
+                double T, int n8, int n8p) {
+    constexpr int NJ = N + 1;
+    constexpr int NO = N / 2;
+    extern __shared__ __align__(16) double A[];
+    double2 *X = reinterpret_cast<double2 *>(A + ((4 * NJ + 1) & ~1));
+    __shared__ double d0[4], dN[4];
+    const int o0 = 4 * blockIdx.x;
+    stage_in(A, sigt + (size_t)blockIdx.x * 4 * NJ, NJ);
+    if (threadIdx.x < 4) {
+        const int o = o0 + threadIdx.x;
+        d0[threadIdx.x] = dS[o];
+        dN[threadIdx.x] = dS[n8p + o];
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        const int o = o0 + threadIdx.x;
+        if (o == 0) sinf[0] = -(A[0] + A[NJ - 1]);
+        if (o < n8) s2[o] = d0[threadIdx.x] + dN[threadIdx.x];
+    }
+    const double h = 1.0 / (N * T);
+    spline_second_derivatives(A, NJ, NJ, h, d0, dN, spl, spl + NJ);
+    if (threadIdx.x < 4) {
+        const int o = o0 + threadIdx.x;
+        const int c = threadIdx.x;
+        if (o < n8) s3[o] = -(A[c * NJ] + A[c * NJ + N]);
+    }
+    constexpr int G = FftPlan<N>::G;
+#pragma unroll 1
+    for (int pr = 0; pr < 2; ++pr) {
+        const double *Ma = A + (2 * pr) * NJ;
+        const double *Mb = A + (2 * pr + 1) * NJ;
+        for (int j = threadIdx.x; j < N; j += blockDim.x) {
+            const double fa = (Ma[j + 1] - Ma[j]) / h;
+            const double fb = (Mb[j + 1] - Mb[j]) / h;
+            X[pidx(j)] = cmul(__ldg(&ht[j]), make_double2(fa, fb));
+        }
+        __syncthreads();
+        if (threadIdx.x < G) group_fft<N, +1>(X, threadIdx.x, tw, 0);
+        __syncthreads();
+        for (int n = threadIdx.x; n < NO; n += blockDim.x) {
+            const double2 Z = X[pidx(n)];
+            const double2 Zr = X[pidx(N - 1 - n)];
+            // F_a = (Z_n + conj Z_{N-1-n})/2, F_b = (Z_n - conj Z_{N-1-n})/(2i)
+            const double2 Fa = make_double2(0.5 * (Z.x + Zr.x), 0.5 * (Z.y - Zr.y));
+            const double2 Fb = make_double2(0.5 * (Z.y + Zr.y), -0.5 * (Z.x - Zr.x));
+            const double2 e = __ldg(&ht[2 * n + 1]);
+            const double2 f = make_double2(1.0 - e.x, -e.y);
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int c = 2 * pr + q;
+                const int o = o0 + c;
+                const double2 Sv = cmul(f, q == 0 ? Fa : Fb);
+                Sout[bidx(n, o, NO)] = Sv;
+                if (n == NO - 1 && o < n8) s4[o] = Sv.x;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// sum rules and traces
+// ---------------------------------------------------------------------------
+
+// sum_{q, n <= Nw0/2} w T/Nq [chi/(1 + s U chi/2) - chi] plus the tail
+// Nw0/2 < n <= Nw0 with chi = c2/qn^2 + c4/qn^4, and its U derivative
+// (chi::traceDiffChispChi0 s = -1, traceDiffChichChi0 s = +1,
+// src/chi.cpp:738-830)
+__global__ void k_sumrule(const double *__restrict__ chiq, const double *__restrict__ cinf,
+                          const double *__restrict__ cinf2, const uint32_t *__restrict__ lm, int n8, int n8p, int nb,
+                          int nbk, double Uv, double sgn, double T, double Nq, double *partial) {
+    KSum v, dv;
+    const long long main_total = (long long)n8p * nb;
+    const int nwmax = nb - 1;
+    const long long tail_total = (long long)n8 * nwmax;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < main_total + tail_total; i += stride) {
+        double c;
+        int w, o;
+        if (i < main_total) {
+            const long long blk = i / (4LL * nb);
+            const int rem = (int)(i - blk * 4LL * nb);
+            const int j = rem >> 2;
+            o = (int)(blk * 4) + (rem & 3);
+            if (o >= n8) continue;
+            int l, m;
+            oct_lm(lm, o, l, m);
+            w = 16;
+            if (j == 0) w /= 2;
+            w = oct_weight(w, l, m, nbk);
+            c = chiq[i];
+        } else {
+            const long long t = i - main_total;
+            o = (int)(t % n8);
+            const int jt = nwmax + 1 + (int)(t / n8);
+            int l, m;
+            oct_lm(lm, o, l, m);
+            w = oct_weight(16, l, m, nbk);
+            const double wn = 2 * jt * kPi * T;
+            c = cinf[o] / (wn * wn) + cinf2[o] / (wn * wn * wn * wn);
+        }
+        const double den = 1 + sgn * Uv * c / 2.0;
+        const double f = w * T / Nq;
+        v.add(f * (c / den - c));
+        dv.add(f * (-sgn * c * c / 2.0 / (den * den)));
+    }
+    double out[2] = {v.value(), dv.value()};
+    block_store<2>(out, partial);
+}
+
+// raw and tail parts of chi0::traceChi0 (src/chi0.cpp:1498-1584)
+__global__ void k_trace_chi0(const double *__restrict__ chiq, const double *__restrict__ cinf,
+                             const double *__restrict__ cinf2, const uint32_t *__restrict__ lm, int n8, int n8p, int nb,
+                             int nbk, double T, double Nq, double *partial) {
+    KSum v, vt;
+    const long long main_total = (long long)n8p * nb;
+    const int nwmax = nb - 1;
+    const long long tail_total = (long long)n8 * (nwmax - 1);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < main_total + tail_total; i += stride) {
+        if (i < main_total) {
+            const long long blk = i / (4LL * nb);
+            const int rem = (int)(i - blk * 4LL * nb);
+            const int j = rem >> 2;
+            const int o = (int)(blk * 4) + (rem & 3);
+            if (o >= n8) continue;
+            int l, m;
+            oct_lm(lm, o, l, m);
+            int w = 16;
+            if (j == 0 || j == nwmax) w /= 2;
+            w = oct_weight(w, l, m, nbk);
+            v.add(w * T * chiq[i] / Nq);
+        } else {
+            const long long t = i - main_total;
+            const int o = (int)(t % n8);
+            const int jt = nwmax + 1 + (int)(t / n8);
+            int l, m;
+            oct_lm(lm, o, l, m);
+            const int w = oct_weight(16, l, m, nbk);
+            const double wn = 2 * kPi * jt * T;
+            vt.add(w * T * (cinf[o] / (wn * wn) + cinf2[o] / (wn * wn * wn * wn)) / Nq);
+        }
+    }
+    double out[2] = {v.value(), vt.value()};
+    block_store<2>(out, partial);
+}
+
+// full Sigma(k, i w_n) = Sinf/z + C2/z^2 + C3/z^3 + S/z^4, z = i w_n
+__device__ __forceinline__ void sigma_full(double wn, double sinf, double c2, double c3, double2 Sv, double &rS,
+                                           double &iS) {
+    const double w2 = wn * wn, w4 = w2 * w2;
+    rS = -c2 / w2 + Sv.x / w4;
+    iS = -sinf / wn + c3 / (w2 * wn) + Sv.y / w4;
+}
+
+// Tr(G - G0) at chemical potential pmu (green::traceDiffG, src/green.cpp:3108-3182)
+__global__ void k_trace_diff_G(const double2 *__restrict__ S, const double *__restrict__ s2,
+                               const double *__restrict__ s3, const double *__restrict__ s4,
+                               const double *__restrict__ sinfp, const double *__restrict__ ek,
+                               const uint32_t *__restrict__ lm, int n8, int n8p, int nw0, int nbk, double mu0,
+                               double pmu, double T, double *partial) {
+    KSum v;
+    const int NO = nw0 / 2;
+    const double sinf = sinfp[0];
+    const long long main_total = (long long)n8p * NO;
+    const long long tail_total = (long long)n8 * (nw0 / 2 + 1);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < main_total + tail_total; i += stride) {
+        int o, j;
+        double rS, iS;
+        if (i < main_total) {
+            const long long blk = i / (4LL * NO);
+            const int rem = (int)(i - blk * 4LL * NO);
+            j = rem >> 2;
+            o = (int)(blk * 4) + (rem & 3);
+            if (o >= n8) continue;
+            const double wn = (2 * j + 1) * kPi * T;
+            sigma_full(wn, sinf, s2[o], s3[o], S[i], rS, iS);
+        } else {
+            const long long t = i - main_total;
+            o = (int)(t % n8);
+            j = NO + (int)(t / n8);
+            const double wn = (2 * j + 1) * kPi * T;
+            rS = -s2[o] / (wn * wn) + s4[o] / (wn * wn * wn * wn);
+            iS = -sinf / wn + s3[o] / (wn * wn * wn);
+        }
+        int l, m;
+        oct_lm(lm, o, l, m);
+        const int w = oct_weight(16, l, m, nbk);
+        const double wn = (2 * j + 1) * kPi * T;
+        const double e = ek[o];
+        const double tmp = ((double)w) / (((wn - iS) * (wn - iS) + (e - pmu + rS) * (e - pmu + rS)) *
+                                          (wn * wn + (e - mu0) * (e - mu0)));
+        v.add(tmp * ((mu0 - pmu + rS) * (e - pmu + rS) * (e - mu0) + iS * (iS - 2 * wn) * (e - mu0) -
+                     wn * wn * (mu0 - pmu + rS)));
+    }
+    double out[1] = {v.value()};
+    block_store<1>(out, partial);
+}
+
+// Tr Sigma G0 and its asymptotic correction (green::traceSelfG, src/green.cpp:3001-3084)
+__global__ void k_trace_self_G(const double2 *__restrict__ S, const double *__restrict__ s2,
+                               const double *__restrict__ s3, const double *__restrict__ sinfp,
+                               const double *__restrict__ ek, const uint32_t *__restrict__ lm, int n8, int n8p,
+                               int nw0, int nbk, double mu0, double T, double nk02, double *partial) {
+    KSum v, v2;
+    const int NO = nw0 / 2;
+    const double sinf = sinfp[0];
+    const long long main_total = (long long)n8p * NO;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < main_total + n8; i += stride) {
+        if (i < main_total) {
+            const long long blk = i / (4LL * NO);
+            const int rem = (int)(i - blk * 4LL * NO);
+            const int j = rem >> 2;
+            const int o = (int)(blk * 4) + (rem & 3);
+            if (o >= n8) continue;
+            int l, m;
+            oct_lm(lm, o, l, m);
+            const int w = oct_weight(8, l, m, nbk);
+            const double wn = (2 * j + 1) * kPi * T;
+            double rS, iS;
+            sigma_full(wn, sinf, s2[o], s3[o], S[i], rS, iS);
+            const double e = ek[o];
+            const double tmp = w * T * 2 / (nk02 * (wn * wn + (e - mu0) * (e - mu0)));
+            v.add(tmp * (rS * (mu0 - e) + iS * wn));
+            v2.add(w * sinf * T * 2 / (nk02 * (wn * wn + (e - mu0) * (e - mu0))));
+        } else {
+            const int o = (int)(i - main_total);
+            int l, m;
+            oct_lm(lm, o, l, m);
+            const int w = oct_weight(8, l, m, nbk);
+            const double x = ek[o] - mu0;
+            if (fabs(x) > 1.0e-12) {
+                v2.add(w * sinf * (1.0 / (exp(x / T) + 1.0) - 0.5) / x / nk02);
+            } else {
+                const double ex = (x < 0) ? exp(x / T) : exp(-x / T);
+                v2.add(-w * sinf * ex / ((ex + 1.0) * (ex + 1.0) * nk02 * T));
+            }
+        }
+    }
+    double out[2] = {v.value(), v2.value()};
+    block_store<2>(out, partial);
+}
+
+// Tr Sigma G (green::traceSelfG2, src/green.cpp:2929-2976)
+__global__ void k_trace_self_G2(const double2 *__restrict__ S, const double *__restrict__ s2,
+                                const double *__restrict__ s3, const double *__restrict__ sinfp,
+                                const double *__restrict__ ek, const uint32_t *__restrict__ lm, int n8, int n8p,
+                                int nw0, int nbk, double mu, double T, double nk02, double *partial) {
+    KSum v;
+    const int NO = nw0 / 2;
+    const double sinf = sinfp[0];
+    const long long main_total = (long long)n8p * NO;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < main_total; i += stride) {
+        const long long blk = i / (4LL * NO);
+        const int rem = (int)(i - blk * 4LL * NO);
+        const int j = rem >> 2;
+        const int o = (int)(blk * 4) + (rem & 3);
+        if (o >= n8) continue;
+        int l, m;
+        oct_lm(lm, o, l, m);
+        const int w = oct_weight(8, l, m, nbk);
+        const double wn = (2 * j + 1) * kPi * T;
+        double rS, iS;
+        sigma_full(wn, sinf, s2[o], s3[o], S[i], rS, iS);
+        const double e = ek[o];
+        const double tmp = w * T * 2 / (nk02 * ((wn - iS) * (wn - iS) + (e - mu + rS) * (e - mu + rS)));
+        v.add(tmp * (iS * wn - iS * iS - (e - mu) * rS - rS * rS));
+    }
+    double out[1] = {v.value()};
+    block_store<1>(out, partial);
+}
+
+// chi0max and its wave vector (src/chi0.cpp:703-717): the reference scans l
+// and then m downwards keeping the first strict maximum, i.e. among equal
+// maxima the largest l, then the largest m.  One block.
+__global__ void k_chi0max(const double *__restrict__ chiq, const uint32_t *__restrict__ lm, int n8, int nb,
+                          double *result) {
+    double best = 0.0;
+    int bl = 0, bm = 0;
+    bool have = false;
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        const double v = chiq[bidx(0, o, nb)];
+        if (!(v > 0.0)) continue;  // the scan starts from chi0max = 0
+        if (!have || v > best || (v == best && (l > bl || (l == bl && m > bm)))) {
+            best = v;
+            bl = l;
+            bm = m;
+            have = true;
+        }
+    }
+    __shared__ double sv[1024];
+    __shared__ int sl[1024], sm[1024], sh[1024];
+    sv[threadIdx.x] = best;
+    sl[threadIdx.x] = bl;
+    sm[threadIdx.x] = bm;
+    sh[threadIdx.x] = have;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        int L = 0, M = 0;
+        bool h = false;
+        for (int i = 0; i < (int)blockDim.x; ++i) {
+            if (!sh[i]) continue;
+            const double v = sv[i];
+            if (!h || v > b || (v == b && (sl[i] > L || (sl[i] == L && sm[i] > M)))) {
+                b = v;
+                L = sl[i];
+                M = sm[i];
+                h = true;
+            }
+        }
+        result[0] = b;
+        result[1] = L;
+        result[2] = M;
+    }
+}
+
+// blocked -> [j][o]
+__global__ void k_unblock(const double *__restrict__ src, double *__restrict__ dst, int NJ, int nrows, int n8) {
+    const long long total = (long long)nrows * n8;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(i / n8), o = (int)(i % n8);
+        dst[i] = src[bidx(j, o, NJ)];
+    }
+}
+__global__ void k_unblock_c(const double2 *__restrict__ src, double2 *__restrict__ dst, int NJ, int nrows, int n8) {
+    const long long total = (long long)nrows * n8;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(i / n8), o = (int)(i % n8);
+        dst[i] = src[bidx(j, o, NJ)];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// dispatch over the compiled sizes
+// ---------------------------------------------------------------------------
+template <template <int> class F, typename... Args>
+cudaError_t dispatch_nbk(int nbk, Args... args) {
+    switch (nbk) {
+        case 5: return F<5>::run(args...);
+        case 9: return F<9>::run(args...);
+        case 17: return F<17>::run(args...);
+        case 33: return F<33>::run(args...);
+        case 65: return F<65>::run(args...);
+        case 129: return F<129>::run(args...);
+        default: return cudaErrorInvalidValue;
+    }
+}
+template <template <int> class F, typename... Args>
+cudaError_t dispatch_nw(int nw0, Args... args) {
+    switch (nw0) {
+        case 16: return F<16>::run(args...);
+        case 32: return F<32>::run(args...);
+        case 64: return F<64>::run(args...);
+        case 128: return F<128>::run(args...);
+        case 256: return F<256>::run(args...);
+        case 512: return F<512>::run(args...);
+        case 1024: return F<1024>::run(args...);
+        case 2048: return F<2048>::run(args...);
+        case 4096: return F<4096>::run(args...);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename K>
+cudaError_t set_smem(K kernel, size_t bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <int NBK>
+struct RunGslice {
+    static cudaError_t run(const GridDev *g, double *Grt, double mu0, double T, cudaStream_t st) {
+        const size_t sm = SliceSmem<NBK>::bytes;
+        cudaError_t e = set_smem(k_gslice<NBK>, sm);
+        if (e != cudaSuccess) return e;
+        const double nk02 = (double)g->nk0 * g->nk0;
+        k_gslice<NBK><<<g->nw0 + 1, kSliceThreads, sm, st>>>(g->ek, g->lm, g->tw_k, mu0, g->n8, g->nw0, T, nk02,
+                                                              Grt);
+        return cudaGetLastError();
+    }
+};
+template <int NBK>
+struct RunChi0Boundary {
+    static cudaError_t run(const GridDev *g, const double *Grt, double mu0, double T, double *dG0p, double *dchirt0,
+                           double *dchiqt0, cudaStream_t st) {
+        const size_t sm = SliceSmem<NBK>::bytes;
+        cudaError_t e = set_smem(k_chi0_boundary<NBK>, sm);
+        if (e != cudaSuccess) return e;
+        const double nk02 = (double)g->nk0 * g->nk0;
+        k_chi0_boundary<NBK><<<1, kSliceThreads, sm, st>>>(g->ek, g->er, g->lm, g->tw_k, Grt, g->n8, mu0, T, nk02,
+                                                            dG0p, dchirt0, dchiqt0);
+        return cudaGetLastError();
+    }
+};
+template <int NBK>
+struct RunChi0Slice {
+    static cudaError_t run(const GridDev *g, const double *Grt, double *chirt, double *chiq, cudaStream_t st) {
+        const size_t sm = SliceSmem<NBK>::bytes;
+        cudaError_t e = set_smem(k_chi0_slice<NBK>, sm);
+        if (e != cudaSuccess) return e;
+        k_chi0_slice<NBK><<<g->nb, kSliceThreads, sm, st>>>(Grt, g->lm, g->tw_k, g->n8, g->nw0, chirt, chiq);
+        return cudaGetLastError();
+    }
+};
+template <int NBK>
+struct RunVertexQ {
+    static cudaError_t run(const GridDev *g, const double *chiq, double *Vr, double U, double Usp, double Uch, double T,
+                           cudaStream_t st) {
+        const size_t sm = SliceSmem<NBK>::bytes;
+        cudaError_t e = set_smem(k_vertex_q<NBK>, sm);
+        if (e != cudaSuccess) return e;
+        const double normFact = T / ((double)g->nk0 * g->nk0);
+        k_vertex_q<NBK><<<g->nb, kSliceThreads, sm, st>>>(chiq, g->lm, g->tw_k, g->n8, g->nb, normFact, U, Usp, Uch,
+                                                          Vr);
+        return cudaGetLastError();
+    }
+};
+template <int NBK>
+struct RunSigmaBoundary {
+    static cudaError_t run(const GridDev *g, const double *Grt, const double *V, const double *dchirt0,
+                           const double *dG0p, double mu0, double fact, double *dS, cudaStream_t st) {
+        const size_t sm = SliceSmem<NBK>::bytes;
+        cudaError_t e = set_smem(k_sigma_boundary<NBK>, sm);
+        if (e != cudaSuccess) return e;
+        k_sigma_boundary<NBK><<<1, kSliceThreads, sm, st>>>(g->er, g->lm, g->tw_k, Grt, V, dchirt0, dG0p, g->n8,
+                                                             g->nw0, g->n8p, mu0, fact, dS);
+        return cudaGetLastError();
+    }
+};
+template <int NBK>
+struct RunSigmaSlice {
+    static cudaError_t run(const GridDev *g, const double *Grt, const double *V, double *sigt, cudaStream_t st) {
+        const size_t sm = SliceSmem<NBK>::bytes;
+        cudaError_t e = set_smem(k_sigma_slice<NBK>, sm);
+        if (e != cudaSuccess) return e;
+        k_sigma_slice<NBK><<<g->nw0 + 1, kSliceThreads, sm, st>>>(Grt, V, g->lm, g->tw_k, g->n8, g->nw0, sigt);
+        return cudaGetLastError();
+    }
+};
+
+template <int N>
+struct RunChi0Tau {
+    static cudaError_t run(const GridDev *g, double *chiq, const double *dchiqt0, double *cinf, double *cinf2,
+                           double T, cudaStream_t st) {
+        const size_t sm = TauSmem<N>::bytes(N / 2 + 1);
+        cudaError_t e = set_smem(k_chi0_tau<N>, sm);
+        if (e != cudaSuccess) return e;
+        k_chi0_tau<N><<<g->n8p / 4, TauSmem<N>::threads, sm, st>>>(chiq, dchiqt0, cinf, cinf2, g->spl_half, g->tw_w,
+                                                                    T, g->n8);
+        return cudaGetLastError();
+    }
+};
+template <int N>
+struct RunVertexTau {
+    static cudaError_t run(const GridDev *g, double *Vr, const double *chirt, double fact, cudaStream_t st) {
+        const size_t sm = TauSmem<N>::bytes(N / 2 + 1);
+        cudaError_t e = set_smem(k_vertex_tau<N>, sm);
+        if (e != cudaSuccess) return e;
+        k_vertex_tau<N><<<g->n8p / 4, TauSmem<N>::threads, sm, st>>>(Vr, chirt, g->tw_w, fact);
+        return cudaGetLastError();
+    }
+};
+template <int N>
+struct RunSigmaTau {
+    static cudaError_t run(const GridDev *g, const double *sigt, const double *dS, double2 *S, double *s2, double *s3,
+                           double *s4, double *sinf, double T, cudaStream_t st) {
+        const size_t sm = TauSmem<N>::bytes(N + 1);
+        cudaError_t e = set_smem(k_sigma_tau<N>, sm);
+        if (e != cudaSuccess) return e;
+        k_sigma_tau<N><<<g->n8p / 4, TauSmem<N>::threads, sm, st>>>(sigt, dS, S, s2, s3, s4, sinf, g->spl_full,
+                                                                     g->tw_w, g->ht_w, T, g->n8, g->n8p);
+        return cudaGetLastError();
+    }
+};
+
+}  // namespace
+
+bool supported_grid(int nk0, int nw0) {
+    const int nbk = nk0 / 2 + 1;
+    const bool k_ok = nbk == 5 || nbk == 9 || nbk == 17 || nbk == 33 || nbk == 65 || nbk == 129;
+    const bool w_ok = nw0 >= 16 && nw0 <= 4096 && (nw0 & (nw0 - 1)) == 0;
+    return k_ok && w_ok && nk0 == 2 * (nbk - 1);
+}
+
+cudaError_t launch_density(const GridDev &g, double mu, double n, double T, Reduce r, cudaStream_t st) {
+    const int nb = grid_for(g.n8, 256);
+    k_density<<<nb, 256, 0, st>>>(g.ek, g.lm, g.n8, g.nbk, mu, T, 4.0 * (g.nbk - 1) * (g.nbk - 1), r.partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return finish<1>(r, nb, -n, st);
+}
+
+cudaError_t launch_gslice(const GridDev &g, double *Grt, double mu0, double T, cudaStream_t st) {
+    return dispatch_nbk<RunGslice>(g.nbk, &g, Grt, mu0, T, st);
+}
+
+cudaError_t launch_chi0_boundary(const GridDev &g, const double *Grt, double mu0, double T, double *dG0p,
+                                 double *dtau_chirt0, double *dtau_chiqt0, cudaStream_t st) {
+    return dispatch_nbk<RunChi0Boundary>(g.nbk, &g, Grt, mu0, T, dG0p, dtau_chirt0, dtau_chiqt0, st);
+}
+
+cudaError_t launch_chi0_slice(const GridDev &g, const double *Grt, double *chirt, double *chiq, cudaStream_t st) {
+    return dispatch_nbk<RunChi0Slice>(g.nbk, &g, Grt, chirt, chiq, st);
+}
+
+cudaError_t launch_chi0_tau(const GridDev &g, double *chiq, const double *dtau_chiqt0, double *chi0_inf,
+                            double *chi0_inf2, double T, cudaStream_t st) {
+    return dispatch_nw<RunChi0Tau>(g.nw0, &g, chiq, dtau_chiqt0, chi0_inf, chi0_inf2, T, st);
+}
+
+cudaError_t launch_sumrule(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
+                           double Uv, double sign, double T, Reduce r, cudaStream_t st) {
+    const long long total = (long long)g.n8p * g.nb + (long long)g.n8 * (g.nb - 1);
+    const int nb = grid_for(total, 256);
+    const double Nq = 4.0 * (g.nbk - 1) * (g.nbk - 1);
+    k_sumrule<<<nb, 256, 0, st>>>(chiq, chi0_inf, chi0_inf2, g.lm, g.n8, g.n8p, g.nb, g.nbk, Uv, sign, T, Nq,
+                                  r.partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return finish<2>(r, nb, 0.0, st);
+}
+
+cudaError_t launch_trace_chi0(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
+                              double T, Reduce r, cudaStream_t st) {
+    const long long total = (long long)g.n8p * g.nb + (long long)g.n8 * (g.nb - 2);
+    const int nb = grid_for(total, 256);
+    const double Nq = 4.0 * (g.nbk - 1) * (g.nbk - 1);
+    k_trace_chi0<<<nb, 256, 0, st>>>(chiq, chi0_inf, chi0_inf2, g.lm, g.n8, g.n8p, g.nb, g.nbk, T, Nq, r.partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return finish<2>(r, nb, 0.0, st);
+}
+
+cudaError_t launch_vertex_q(const GridDev &g, const double *chiq, double *Vr, double U, double Usp, double Uch,
+                            double T, cudaStream_t st) {
+    return dispatch_nbk<RunVertexQ>(g.nbk, &g, chiq, Vr, U, Usp, Uch, T, st);
+}
+
+cudaError_t launch_vertex_tau(const GridDev &g, double *Vr, const double *chirt, double fact, cudaStream_t st) {
+    return dispatch_nw<RunVertexTau>(g.nw0, &g, Vr, chirt, fact, st);
+}
+
+cudaError_t launch_sigma_boundary(const GridDev &g, const double *Grt, const double *V, const double *dtau_chirt0,
+                                  const double *dG0p, double mu0, double fact, double *dS, cudaStream_t st) {
+    return dispatch_nbk<RunSigmaBoundary>(g.nbk, &g, Grt, V, dtau_chirt0, dG0p, mu0, fact, dS, st);
+}
+
+cudaError_t launch_sigma_slice(const GridDev &g, const double *Grt, const double *V, double *sigt, cudaStream_t st) {
+    return dispatch_nbk<RunSigmaSlice>(g.nbk, &g, Grt, V, sigt, st);
+}
+
+cudaError_t launch_sigma_tau(const GridDev &g, const double *sigt, const double *dS, double2 *S, double *s2,
+                             double *s3, double *s4, double *sinf, double T, cudaStream_t st) {
+    return dispatch_nw<RunSigmaTau>(g.nw0, &g, sigt, dS, S, s2, s3, s4, sinf, T, st);
+}
+
+cudaError_t launch_trace_diff_G(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                                const double *s4, const double *sinf, double mu0, double pmu, double T, Reduce r,
+                                cudaStream_t st) {
+    const long long total = (long long)g.n8p * (g.nw0 / 2) + (long long)g.n8 * (g.nw0 / 2 + 1);
+    const int nb = grid_for(total, 256);
+    k_trace_diff_G<<<nb, 256, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.lm, g.n8, g.n8p, g.nw0, g.nbk, mu0, pmu, T,
+                                       r.partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return finish<1>(r, nb, 0.0, st);
+}
+
+cudaError_t launch_trace_self_G(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                                const double *sinf, double mu0, double T, Reduce r, cudaStream_t st) {
+    const long long total = (long long)g.n8p * (g.nw0 / 2) + g.n8;
+    const int nb = grid_for(total, 256);
+    const double nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
+    k_trace_self_G<<<nb, 256, 0, st>>>(S, s2, s3, sinf, g.ek, g.lm, g.n8, g.n8p, g.nw0, g.nbk, mu0, T, nk02,
+                                       r.partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return finish<2>(r, nb, 0.0, st);
+}
+
+cudaError_t launch_trace_self_G2(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                                 const double *sinf, double mu, double T, Reduce r, cudaStream_t st) {
+    const long long total = (long long)g.n8p * (g.nw0 / 2);
+    const int nb = grid_for(total, 256);
+    const double nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
+    k_trace_self_G2<<<nb, 256, 0, st>>>(S, s2, s3, sinf, g.ek, g.lm, g.n8, g.n8p, g.nw0, g.nbk, mu, T, nk02,
+                                        r.partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return finish<1>(r, nb, 0.0, st);
+}
+
+cudaError_t launch_chi0max(const GridDev &g, const double *chiq, Reduce r, cudaStream_t st) {
+    k_chi0max<<<1, 1024, 0, st>>>(chiq, g.lm, g.n8, g.nb, r.result);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unblock(const double *src, double *dst, int NJ, int nrows, int n8, cudaStream_t st) {
+    const int nb = grid_for((long long)nrows * n8, 256);
+    k_unblock<<<nb, 256, 0, st>>>(src, dst, NJ, nrows, n8);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unblock_c(const double2 *src, double2 *dst, int NJ, int nrows, int n8, cudaStream_t st) {
+    const int nb = grid_for((long long)nrows * n8, 256);
+    k_unblock_c<<<nb, 256, 0, st>>>(src, dst, NJ, nrows, n8);
+    return cudaGetLastError();
+}
+
+}  // namespace tpsc

@@ -1,0 +1,84 @@
+// tpsc_kernels.cuh -- launchers of the sm_100a kernels of the TPSC hot path.
+// Host-side declarations shared by tpsc_kernels.cu and tpsc_engine.cpp.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tpsc {
+
+// Device tables of one lattice / frequency grid.
+struct GridDev {
+    int nk0 = 0;        // lattice side L
+    int nbk = 0;        // quadrant side L/2 + 1
+    int n8 = 0;         // octant size nbk (nbk + 1) / 2
+    int n8p = 0;        // n8 rounded up to a multiple of 4 (column blocks)
+    int nw0 = 0;        // Nw0: fermionic frequencies (+ and -)
+    int nb = 0;         // Nw0/2 + 1: bosonic n >= 0 == tau nodes on [0, beta/2]
+    uint32_t *lm = nullptr;        // [n8] (l << 16) | m of octant point o
+    double *ek = nullptr;          // [n8] eps_k on the octant
+    double *er = nullptr;          // [n8] real-space hopping table
+    double2 *tw_k = nullptr;       // [L]   exp(-2 pi i m / L)
+    double2 *tw_w = nullptr;       // [Nw0] exp(-2 pi i m / Nw0)
+    double2 *ht_w = nullptr;       // [Nw0] exp(+i pi m / Nw0)
+    double *spl_half = nullptr;    // [2 nb]       spline LU tables, nb nodes
+    double *spl_full = nullptr;    // [2 (Nw0+1)]  spline LU tables, Nw0+1 nodes
+};
+
+// Column-block layout of the (tau or frequency) x octant arrays: element
+// (j, o) of an array with NJ rows sits at ((o / 4) NJ + j) 4 + o % 4, so the
+// four columns of a block are contiguous along j (32-byte granules).
+__host__ __device__ inline size_t bidx(int j, int o, int NJ) {
+    return ((size_t)(o >> 2) * NJ + j) * 4 + (o & 3);
+}
+
+struct Reduce {
+    double *partial = nullptr;  // [2 * kMaxBlocks]
+    double *result = nullptr;   // [4]
+};
+constexpr int kMaxBlocks = 1184;  // 8 blocks per SM on 148 SMs
+
+// ---- launchers (all asynchronous on `st`) ---------------------------------
+cudaError_t launch_density(const GridDev &g, double mu, double n, double T, Reduce r, cudaStream_t st);
+
+cudaError_t launch_gslice(const GridDev &g, double *Grt, double mu0, double T, cudaStream_t st);
+cudaError_t launch_chi0_boundary(const GridDev &g, const double *Grt, double mu0, double T,
+                                 double *dG0p, double *dtau_chirt0, double *dtau_chiqt0, cudaStream_t st);
+cudaError_t launch_chi0_slice(const GridDev &g, const double *Grt, double *chirt, double *chiq, cudaStream_t st);
+cudaError_t launch_chi0_tau(const GridDev &g, double *chiq, const double *dtau_chiqt0, double *chi0_inf,
+                            double *chi0_inf2, double T, cudaStream_t st);
+
+// chi0max, qmax -> r.result[0..2]
+cudaError_t launch_chi0max(const GridDev &g, const double *chiq, Reduce r, cudaStream_t st);
+
+cudaError_t launch_sumrule(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
+                           double Uv, double sign, double T, Reduce r, cudaStream_t st);
+cudaError_t launch_trace_chi0(const GridDev &g, const double *chiq, const double *chi0_inf,
+                              const double *chi0_inf2, double T, Reduce r, cudaStream_t st);
+
+cudaError_t launch_vertex_q(const GridDev &g, const double *chiq, double *Vr, double U, double Usp, double Uch,
+                            double T, cudaStream_t st);
+cudaError_t launch_vertex_tau(const GridDev &g, double *Vr, const double *chirt, double fact, cudaStream_t st);
+
+cudaError_t launch_sigma_boundary(const GridDev &g, const double *Grt, const double *V, const double *dtau_chirt0,
+                                  const double *dG0p, double mu0, double fact, double *dS, cudaStream_t st);
+cudaError_t launch_sigma_slice(const GridDev &g, const double *Grt, const double *V, double *sigt, cudaStream_t st);
+cudaError_t launch_sigma_tau(const GridDev &g, const double *sigt, const double *dS, double2 *S, double *s2,
+                             double *s3, double *s4, double *sinf, double T, cudaStream_t st);
+
+cudaError_t launch_trace_diff_G(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                                const double *s4, const double *sinf, double mu0, double pmu, double T, Reduce r,
+                                cudaStream_t st);
+cudaError_t launch_trace_self_G(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                                const double *sinf, double mu0, double T, Reduce r, cudaStream_t st);
+cudaError_t launch_trace_self_G2(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                                 const double *sinf, double mu, double T, Reduce r, cudaStream_t st);
+
+// ---- layout conversion for the getters ------------------------------------
+// blocked (NJ rows) -> reference layout [j][o], j < nrows
+cudaError_t launch_unblock(const double *src, double *dst, int NJ, int nrows, int n8, cudaStream_t st);
+cudaError_t launch_unblock_c(const double2 *src, double2 *dst, int NJ, int nrows, int n8, cudaStream_t st);
+
+// the FFT lengths the build instantiates
+bool supported_grid(int nk0, int nw0);
+
+}  // namespace tpsc
