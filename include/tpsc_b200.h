@@ -139,6 +139,30 @@ int tpsc_get_self(tpsc_ctx *ctx, double *self_kw, double *sigma_inf2, double *si
  * {chi0, sum rules, vertex, self energy, traces + mu}; n <= 5. */
 int tpsc_stage_times(tpsc_ctx *ctx, double *ms, int n);
 
+/* ---- instrumentation (no counterpart in the reference) ------------------ */
+/* The context's CUDA stream (a cudaStream_t), so callers can record timing
+ * events on the stream the kernels run on. */
+int tpsc_get_stream(tpsc_ctx *ctx, void **stream);
+
+/* Re-launch the kernel(s) of one stage on the current grid's state,
+ * asynchronously on the context stream (for timing and profiling):
+ *  0 G(r,tau) slices   1 chi0 slices   2 chi0 tau transform
+ *  3 V q-slices        4 V tau transform   5 Sigma slices
+ *  6 Sigma tau transform  7 one spin sum-rule evaluation at Usp
+ *  8 one Tr(G-G0) evaluation at mu   9 stages 1 and 2 back to back.
+ * Requires a completed tpsc_solve.  Stages 2 and 4 transform in place and
+ * expect stage 1 (resp. 3) to have run just before; launching the stages in
+ * increasing order leaves the state as the solve left it. */
+int tpsc_run_kernel(tpsc_ctx *ctx, int which);
+
+/* Algorithmic HBM bytes of one launch of tpsc_run_kernel(which) on the current
+ * grid: every distinct input read once plus every output written once. */
+int tpsc_kernel_bytes(tpsc_ctx *ctx, int which, double *bytes);
+
+/* Number of CUDA kernels the library has launched (all contexts) since it was
+ * loaded. */
+int tpsc_launch_count(tpsc_ctx *ctx, long long *count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -14,6 +14,7 @@
  *               (green.cpp:1673, 3001, 3185) -- the full TPSC solve
  *        cond   solve + cond_opt::calc_chijj_vertex_corr_all_optim(false,3,1,NULL,0)
  *               (cond_opt.cpp:2537)
+ *        bench  timings only: the half-grid pre-pass alone, then the solve
  * The reference writes its own text files into the current directory; the
  * probe chdir()s into OUTDIR/work first so they land there.
  */
@@ -119,6 +120,27 @@ int main(int argc, char **argv) {
         g->calc_chiqw_FFT_spline(nk0, Nw0);
         fprintf(meta, "t_chi0 %.6f\n", omp_get_wtime() - t0);
         g->dump_chi0(meta, absdir);
+    } else if (mode == "bench") {
+        // timing only: the solve exactly as src/tpsc_main.cpp:71-75 runs it, then
+        // the half-grid Usp/Uch pass that calc_Self_FFT_spline runs first
+        // (src/chi.cpp:285-297) timed on its own so it can be subtracted (it
+        // re-grids the object, so it must come after the solve)
+        double Usc[2] = {0, 0};
+        g->set_keep_chiqw(false);
+        t0 = omp_get_wtime();
+        g->calc_Self_FFT_spline();
+        double t_self = omp_get_wtime() - t0;
+        t0 = omp_get_wtime();
+        g->traceSelfG();
+        double t_tr = omp_get_wtime() - t0;
+        t0 = omp_get_wtime();
+        g->find_mu();
+        double t_mu = omp_get_wtime() - t0;
+        fprintf(meta, "t_self %.6f\nt_traceSelfG %.6f\nt_find_mu %.6f\n", t_self, t_tr, t_mu);
+        fprintf(meta, "mu %.17g\n", g->get_mu());
+        t0 = omp_get_wtime();
+        g->find_Usp_Uch(nk0 / 2, Nw0 / 2, Usc);
+        fprintf(meta, "t_half %.6f\n", omp_get_wtime() - t0);
     } else if (mode == "solve" || mode == "cond") {
         g->set_keep_chiqw(true);
         t0 = omp_get_wtime();

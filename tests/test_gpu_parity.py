@@ -127,6 +127,22 @@ def test_l256_scalars_match_reference(ctx):
     assert rel(se["S"][:, cols], g["self_cols"]) < 1e-7
 
 
+@pytest.mark.parametrize("name", ["l64_w1024_u4", "l32_w256_u4_tp"])
+def test_repeated_solves_are_bit_identical(ctx, name):
+    """State left by one solve (including the padding columns of the column
+    blocks) must not leak into the next: three solves, identical bits."""
+    g = load_golden(name)
+    gr = make(ctx, g["p"])
+    runs = []
+    for _ in range(3):
+        gr.solve()
+        runs.append((gr.scalars(), gr.self_energy()["S"].copy(), gr.vertex().copy()))
+    for sc, S, V in runs[1:]:
+        assert sc == runs[0][0]
+        assert np.array_equal(S, runs[0][1])
+        assert np.array_equal(V, runs[0][2])
+
+
 def test_bad_arguments_raise(ctx):
     from tpsc_conductivity_b200._lib import TPSCError
     from tpsc_conductivity_b200.api import Green

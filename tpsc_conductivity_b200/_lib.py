@@ -39,7 +39,15 @@ SIGNATURES = [
     ("tpsc_get_vertex", C.c_int, [C.c_void_p, _dp]),
     ("tpsc_get_self", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     ("tpsc_stage_times", C.c_int, [C.c_void_p, _dp, C.c_int]),
+    ("tpsc_get_stream", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("tpsc_run_kernel", C.c_int, [C.c_void_p, C.c_int]),
+    ("tpsc_kernel_bytes", C.c_int, [C.c_void_p, C.c_int, _dp]),
+    ("tpsc_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
 ]
+
+# tpsc_run_kernel stage ids
+KERNELS = ["gslice", "chi0_slice", "chi0_tau", "vertex_q", "vertex_tau", "sigma_slice", "sigma_tau",
+           "sumrule", "trace_diff_G"]
 
 STATUS = {0: "OK", 1: "bad argument", 2: "CUDA error", 3: "out of device memory",
           4: "root not found", 5: "stage prerequisite missing", 6: "non-finite result"}

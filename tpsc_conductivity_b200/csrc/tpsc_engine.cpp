@@ -933,4 +933,76 @@ int tpsc_stage_times(tpsc_ctx *ctx, double *ms, int n) {
     return TPSC_OK;
 }
 
+int tpsc_launch_count(tpsc_ctx *ctx, long long *count) {
+    if (!count) return fail(ctx, TPSC_ERR_ARG, "bad arguments");
+    *count = launches_total();
+    return TPSC_OK;
+}
+
+int tpsc_get_stream(tpsc_ctx *ctx, void **stream) {
+    if (!ctx || !stream) return fail(ctx, TPSC_ERR_ARG, "bad arguments");
+    *stream = (void *)ctx->st;
+    return TPSC_OK;
+}
+
+int tpsc_run_kernel(tpsc_ctx *ctx, int which) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    Grid *g = ctx->cur;
+    if (!g->have_S) return fail(ctx, TPSC_ERR_STATE, "run tpsc_solve first");
+    const GridDev &d = g->d;
+    const double fact = ctx->U * (3.0 * ctx->Usp + ctx->Uch) / 8.0;
+    switch (which) {
+        case 0: CK(launch_gslice(d, g->Grt, g->mu0, ctx->T, ctx->st)); break;
+        case 1: CK(launch_chi0_slice(d, g->Grt, g->chirt, g->chiq, ctx->st)); break;
+        case 2: CK(launch_chi0_tau(d, g->chiq, g->dchiqt0, g->cinf, g->cinf2, ctx->T, ctx->st)); break;
+        case 3: CK(launch_vertex_q(d, g->chiq, g->V, ctx->U, ctx->Usp, ctx->Uch, ctx->T, ctx->st)); break;
+        case 4: CK(launch_vertex_tau(d, g->V, g->chirt, fact, ctx->st)); break;
+        case 5: CK(launch_sigma_slice(d, g->Grt, g->V, g->sigt, ctx->st)); break;
+        case 6:
+            CK(launch_sigma_tau(d, g->sigt, g->dS, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->T, ctx->st));
+            break;
+        case 7:
+            CK(launch_sumrule(d, g->chiq, g->cinf, g->cinf2, ctx->Usp, -1.0, ctx->T, ctx->red, ctx->st));
+            break;
+        case 8:
+            CK(launch_trace_diff_G(d, g->S, g->s2, g->s3, g->s4, g->sinf, g->mu0, ctx->scal[TPSC_S_MU], ctx->T,
+                                   ctx->red, ctx->st));
+            break;
+        case 9:
+            // chi0 slices followed by the in-place chi0 tau transform
+            CK(launch_chi0_slice(d, g->Grt, g->chirt, g->chiq, ctx->st));
+            CK(launch_chi0_tau(d, g->chiq, g->dchiqt0, g->cinf, g->cinf2, ctx->T, ctx->st));
+            break;
+        default: return fail(ctx, TPSC_ERR_ARG, "unknown stage");
+    }
+    return TPSC_OK;
+}
+
+int tpsc_kernel_bytes(tpsc_ctx *ctx, int which, double *bytes) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    const GridDev &d = ctx->cur->d;
+    const double s = sizeof(double), n8 = d.n8, nb = d.nb, nw = d.nw0;
+    const double tau = (nw + 1) * n8 * s;   // one (Nw0+1) x N8 real array
+    const double half = nb * n8 * s;        // one (Nw0/2+1) x N8 real array
+    const double cplx = (nw / 2) * n8 * 2 * s;
+    double b;
+    switch (which) {
+        case 0: b = tau; break;                       // write G(r, tau)
+        case 1: b = tau + 2 * half; break;            // read G, write chi0(r,tau), chi0(q,tau)
+        case 2: b = 2 * half; break;                  // read + write chi0(q, .)
+        case 3: b = 2 * half; break;                  // read chi0(q, iqn), write V(r, iqn)
+        case 4: b = 3 * half; break;                  // read V, chi0(r, tau); write V
+        case 5: b = tau + half + tau; break;          // read G, V; write Sigma(k, tau)
+        case 6: b = tau + cplx; break;                // read Sigma(k, tau); write S
+        case 7: b = half; break;                      // read chi0(q, iqn)
+        case 8: b = cplx; break;                      // read S
+        case 9: b = tau + 2 * half + 2 * half; break; // stages 1 and 2
+        default: return fail(ctx, TPSC_ERR_ARG, "unknown stage");
+    }
+    *bytes = b;
+    return TPSC_OK;
+}
+
 }  // extern "C"

@@ -17,6 +17,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "tpsc_fft.cuh"
 #include "tpsc_kernels.cuh"
 
@@ -28,6 +30,13 @@ constexpr double kPi = 3.141592653589793;  // == acos(-1.0) in double
 constexpr int kSliceThreads = 256;
 constexpr int kTauThreads = 256;
 constexpr int kWarm = 40;  // spline sweep warm-up: carry error <= 0.268^40
+
+// kernels launched by this library (all contexts), for the instrumentation ABI
+std::atomic<long long> g_launches{0};
+inline cudaError_t launched(int n = 1) {
+    g_launches.fetch_add(n, std::memory_order_relaxed);
+    return cudaGetLastError();
+}
 
 __device__ __forceinline__ void oct_lm(const uint32_t *lm, int o, int &l, int &m) {
     const uint32_t v = __ldg(&lm[o]);
@@ -116,7 +125,7 @@ int grid_for(long long total, int threads) {
 template <int NV>
 cudaError_t finish(Reduce r, int nblocks, double offset0, cudaStream_t st) {
     k_finish<NV><<<1, 256, 0, st>>>(r.partial, nblocks, r.result, offset0);
-    return cudaGetLastError();
+    return launched();
 }
 
 // ---------------------------------------------------------------------------
@@ -473,8 +482,12 @@ struct TauSmem {
     }
 };
 
-__device__ __forceinline__ void stage_in(double *A, const double *g, int NJ) {
-    for (int i = threadIdx.x; i < 4 * NJ; i += blockDim.x) A[(i & 3) * NJ + (i >> 2)] = g[i];
+// Load one column block into shared memory, column-major.  Padding columns
+// (octant index >= n8, present because N8 is rounded up to a multiple of 4)
+// load as zeros: they share packed FFTs with real columns, so stale values
+// there would leak into real outputs through rounding.
+__device__ __forceinline__ void stage_in(double *A, const double *g, int NJ, int nvalid) {
+    for (int i = threadIdx.x; i < 4 * NJ; i += blockDim.x) A[(i & 3) * NJ + (i >> 2)] = (i & 3) < nvalid ? g[i] : 0.0;
 }
 __device__ __forceinline__ void stage_out(const double *A, double *g, int NJ) {
     for (int i = threadIdx.x; i < 4 * NJ; i += blockDim.x) g[i] = A[(i & 3) * NJ + (i >> 2)];
@@ -496,7 +509,7 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
     __shared__ double d0[4], dN[4], V0[4], VN[4], sV[4], sM[4], integ[4];
     const int o0 = 4 * blockIdx.x;
     double *g = chiq + (size_t)blockIdx.x * 4 * NJ;
-    stage_in(A, g, NJ);
+    stage_in(A, g, NJ, n8 - o0);
     if (threadIdx.x < 4) {
         const int o = o0 + threadIdx.x;
         d0[threadIdx.x] = o < n8 ? dtau_chiqt0[o] : 0.0;
@@ -568,13 +581,13 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
 template <int N>
 __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
     k_vertex_tau(double *__restrict__ Vr, const double *__restrict__ chirt, const double2 *__restrict__ tw,
-                 double fact) {
+                 double fact, int n8) {
     constexpr int NJ = N / 2 + 1;
     extern __shared__ __align__(16) double A[];
     double2 *X = reinterpret_cast<double2 *>(A + ((4 * NJ + 1) & ~1));
     double *g = Vr + (size_t)blockIdx.x * 4 * NJ;
     const double *cr = chirt + (size_t)blockIdx.x * 4 * NJ;
-    stage_in(A, g, NJ);
+    stage_in(A, g, NJ, n8 - 4 * (int)blockIdx.x);
     __syncthreads();
     constexpr int G = FftPlan<N>::G;
 #pragma unroll 1
@@ -595,7 +608,9 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
         }
         __syncthreads();
     }
-    for (int i = threadIdx.x; i < 4 * NJ; i += blockDim.x) g[i] = A[(i & 3) * NJ + (i >> 2)] + fact * cr[i];
+    const int nvalid = n8 - 4 * (int)blockIdx.x;
+    for (int i = threadIdx.x; i < 4 * NJ; i += blockDim.x)
+        g[i] = (i & 3) < nvalid ? A[(i & 3) * NJ + (i >> 2)] + fact * cr[i] : 0.0;
 }
 
 // Sigma(k, i w_n) coefficients from Sigma(k, tau_j), j = 0..Nw0, for one
@@ -616,7 +631,7 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
     double2 *X = reinterpret_cast<double2 *>(A + ((4 * NJ + 1) & ~1));
     __shared__ double d0[4], dN[4];
     const int o0 = 4 * blockIdx.x;
-    stage_in(A, sigt + (size_t)blockIdx.x * 4 * NJ, NJ);
+    stage_in(A, sigt + (size_t)blockIdx.x * 4 * NJ, NJ, n8 - o0);
     if (threadIdx.x < 4) {
         const int o = o0 + threadIdx.x;
         d0[threadIdx.x] = dS[o];
@@ -994,7 +1009,7 @@ struct RunGslice {
         const double nk02 = (double)g->nk0 * g->nk0;
         k_gslice<NBK><<<g->nw0 + 1, kSliceThreads, sm, st>>>(g->ek, g->lm, g->tw_k, mu0, g->n8, g->nw0, T, nk02,
                                                               Grt);
-        return cudaGetLastError();
+        return launched();
     }
 };
 template <int NBK>
@@ -1007,7 +1022,7 @@ struct RunChi0Boundary {
         const double nk02 = (double)g->nk0 * g->nk0;
         k_chi0_boundary<NBK><<<1, kSliceThreads, sm, st>>>(g->ek, g->er, g->lm, g->tw_k, Grt, g->n8, mu0, T, nk02,
                                                             dG0p, dchirt0, dchiqt0);
-        return cudaGetLastError();
+        return launched();
     }
 };
 template <int NBK>
@@ -1017,7 +1032,7 @@ struct RunChi0Slice {
         cudaError_t e = set_smem(k_chi0_slice<NBK>, sm);
         if (e != cudaSuccess) return e;
         k_chi0_slice<NBK><<<g->nb, kSliceThreads, sm, st>>>(Grt, g->lm, g->tw_k, g->n8, g->nw0, chirt, chiq);
-        return cudaGetLastError();
+        return launched();
     }
 };
 template <int NBK>
@@ -1030,7 +1045,7 @@ struct RunVertexQ {
         const double normFact = T / ((double)g->nk0 * g->nk0);
         k_vertex_q<NBK><<<g->nb, kSliceThreads, sm, st>>>(chiq, g->lm, g->tw_k, g->n8, g->nb, normFact, U, Usp, Uch,
                                                           Vr);
-        return cudaGetLastError();
+        return launched();
     }
 };
 template <int NBK>
@@ -1042,7 +1057,7 @@ struct RunSigmaBoundary {
         if (e != cudaSuccess) return e;
         k_sigma_boundary<NBK><<<1, kSliceThreads, sm, st>>>(g->er, g->lm, g->tw_k, Grt, V, dchirt0, dG0p, g->n8,
                                                              g->nw0, g->n8p, mu0, fact, dS);
-        return cudaGetLastError();
+        return launched();
     }
 };
 template <int NBK>
@@ -1052,7 +1067,7 @@ struct RunSigmaSlice {
         cudaError_t e = set_smem(k_sigma_slice<NBK>, sm);
         if (e != cudaSuccess) return e;
         k_sigma_slice<NBK><<<g->nw0 + 1, kSliceThreads, sm, st>>>(Grt, V, g->lm, g->tw_k, g->n8, g->nw0, sigt);
-        return cudaGetLastError();
+        return launched();
     }
 };
 
@@ -1065,7 +1080,7 @@ struct RunChi0Tau {
         if (e != cudaSuccess) return e;
         k_chi0_tau<N><<<g->n8p / 4, TauSmem<N>::threads, sm, st>>>(chiq, dchiqt0, cinf, cinf2, g->spl_half, g->tw_w,
                                                                     T, g->n8);
-        return cudaGetLastError();
+        return launched();
     }
 };
 template <int N>
@@ -1074,8 +1089,8 @@ struct RunVertexTau {
         const size_t sm = TauSmem<N>::bytes(N / 2 + 1);
         cudaError_t e = set_smem(k_vertex_tau<N>, sm);
         if (e != cudaSuccess) return e;
-        k_vertex_tau<N><<<g->n8p / 4, TauSmem<N>::threads, sm, st>>>(Vr, chirt, g->tw_w, fact);
-        return cudaGetLastError();
+        k_vertex_tau<N><<<g->n8p / 4, TauSmem<N>::threads, sm, st>>>(Vr, chirt, g->tw_w, fact, g->n8);
+        return launched();
     }
 };
 template <int N>
@@ -1087,11 +1102,13 @@ struct RunSigmaTau {
         if (e != cudaSuccess) return e;
         k_sigma_tau<N><<<g->n8p / 4, TauSmem<N>::threads, sm, st>>>(sigt, dS, S, s2, s3, s4, sinf, g->spl_full,
                                                                      g->tw_w, g->ht_w, T, g->n8, g->n8p);
-        return cudaGetLastError();
+        return launched();
     }
 };
 
 }  // namespace
+
+long long launches_total() { return g_launches.load(); }
 
 bool supported_grid(int nk0, int nw0) {
     const int nbk = nk0 / 2 + 1;
@@ -1103,7 +1120,7 @@ bool supported_grid(int nk0, int nw0) {
 cudaError_t launch_density(const GridDev &g, double mu, double n, double T, Reduce r, cudaStream_t st) {
     const int nb = grid_for(g.n8, 256);
     k_density<<<nb, 256, 0, st>>>(g.ek, g.lm, g.n8, g.nbk, mu, T, 4.0 * (g.nbk - 1) * (g.nbk - 1), r.partial);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launched();
     if (e != cudaSuccess) return e;
     return finish<1>(r, nb, -n, st);
 }
@@ -1133,7 +1150,7 @@ cudaError_t launch_sumrule(const GridDev &g, const double *chiq, const double *c
     const double Nq = 4.0 * (g.nbk - 1) * (g.nbk - 1);
     k_sumrule<<<nb, 256, 0, st>>>(chiq, chi0_inf, chi0_inf2, g.lm, g.n8, g.n8p, g.nb, g.nbk, Uv, sign, T, Nq,
                                   r.partial);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launched();
     if (e != cudaSuccess) return e;
     return finish<2>(r, nb, 0.0, st);
 }
@@ -1144,7 +1161,7 @@ cudaError_t launch_trace_chi0(const GridDev &g, const double *chiq, const double
     const int nb = grid_for(total, 256);
     const double Nq = 4.0 * (g.nbk - 1) * (g.nbk - 1);
     k_trace_chi0<<<nb, 256, 0, st>>>(chiq, chi0_inf, chi0_inf2, g.lm, g.n8, g.n8p, g.nb, g.nbk, T, Nq, r.partial);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launched();
     if (e != cudaSuccess) return e;
     return finish<2>(r, nb, 0.0, st);
 }
@@ -1179,7 +1196,7 @@ cudaError_t launch_trace_diff_G(const GridDev &g, const double2 *S, const double
     const int nb = grid_for(total, 256);
     k_trace_diff_G<<<nb, 256, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.lm, g.n8, g.n8p, g.nw0, g.nbk, mu0, pmu, T,
                                        r.partial);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launched();
     if (e != cudaSuccess) return e;
     return finish<1>(r, nb, 0.0, st);
 }
@@ -1191,7 +1208,7 @@ cudaError_t launch_trace_self_G(const GridDev &g, const double2 *S, const double
     const double nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
     k_trace_self_G<<<nb, 256, 0, st>>>(S, s2, s3, sinf, g.ek, g.lm, g.n8, g.n8p, g.nw0, g.nbk, mu0, T, nk02,
                                        r.partial);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launched();
     if (e != cudaSuccess) return e;
     return finish<2>(r, nb, 0.0, st);
 }
@@ -1203,26 +1220,26 @@ cudaError_t launch_trace_self_G2(const GridDev &g, const double2 *S, const doubl
     const double nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
     k_trace_self_G2<<<nb, 256, 0, st>>>(S, s2, s3, sinf, g.ek, g.lm, g.n8, g.n8p, g.nw0, g.nbk, mu, T, nk02,
                                         r.partial);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launched();
     if (e != cudaSuccess) return e;
     return finish<1>(r, nb, 0.0, st);
 }
 
 cudaError_t launch_chi0max(const GridDev &g, const double *chiq, Reduce r, cudaStream_t st) {
     k_chi0max<<<1, 1024, 0, st>>>(chiq, g.lm, g.n8, g.nb, r.result);
-    return cudaGetLastError();
+    return launched();
 }
 
 cudaError_t launch_unblock(const double *src, double *dst, int NJ, int nrows, int n8, cudaStream_t st) {
     const int nb = grid_for((long long)nrows * n8, 256);
     k_unblock<<<nb, 256, 0, st>>>(src, dst, NJ, nrows, n8);
-    return cudaGetLastError();
+    return launched();
 }
 
 cudaError_t launch_unblock_c(const double2 *src, double2 *dst, int NJ, int nrows, int n8, cudaStream_t st) {
     const int nb = grid_for((long long)nrows * n8, 256);
     k_unblock_c<<<nb, 256, 0, st>>>(src, dst, NJ, nrows, n8);
-    return cudaGetLastError();
+    return launched();
 }
 
 }  // namespace tpsc

@@ -78,6 +78,9 @@ cudaError_t launch_trace_self_G2(const GridDev &g, const double2 *S, const doubl
 cudaError_t launch_unblock(const double *src, double *dst, int NJ, int nrows, int n8, cudaStream_t st);
 cudaError_t launch_unblock_c(const double2 *src, double2 *dst, int NJ, int nrows, int n8, cudaStream_t st);
 
+// kernels launched by the library so far
+long long launches_total();
+
 // the FFT lengths the build instantiates
 bool supported_grid(int nk0, int nw0);
 
