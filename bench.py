@@ -338,7 +338,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nk0", type=int, default=None, help="lattice side override (profiling only)")
+    ap.add_argument("--nw0", type=int, default=None, help="Nw0 override (profiling only)")
     a = ap.parse_args()
+    if a.nk0 or a.nw0:
+        global WORKLOAD_NAME
+        WORKLOAD["nk0"] = a.nk0 or WORKLOAD["nk0"]
+        WORKLOAD["Nw0"] = a.nw0 or WORKLOAD["Nw0"]
+        WORKLOAD_NAME = f"PROFILING OVERRIDE nk0={WORKLOAD['nk0']} Nw0={WORKLOAD['Nw0']} (not the headline)"
+        a.no_cpu_baseline = True
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -227,6 +227,8 @@ struct Grid {
     double2 *S = nullptr;         // blocked Nw0/2       coefficient of 1/z^4
     double *s2 = nullptr, *s3 = nullptr, *s4 = nullptr, *sinf = nullptr;
     bool have_chi0 = false, have_V = false, have_S = false;
+    double tailq_T = -1.0;         // temperature the tail power sums were built for
+    double tailq_host[kTailQ] = {0};
     std::vector<void *> allocs;
 };
 
@@ -354,8 +356,18 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
     d.nw0 = nw0;
     d.nb = nw0 / 2 + 1;
     std::vector<uint32_t> lm(d.n8);
+    std::vector<double> w16(d.n8p, 0.0);
     for (int l = 0; l < d.nbk; ++l)
-        for (int m = 0; m <= l; ++m) lm[m + l * (l + 1) / 2] = ((uint32_t)l << 16) | (uint32_t)m;
+        for (int m = 0; m <= l; ++m) {
+            lm[m + l * (l + 1) / 2] = ((uint32_t)l << 16) | (uint32_t)m;
+            // multiplicity of octant point (l, m): 16 halved on the l edges, the m
+            // edges and the diagonal (src/chi.cpp:755-759)
+            int w = 16;
+            if (l == 0 || l == d.nbk - 1) w /= 2;
+            if (m == 0 || m == d.nbk - 1) w /= 2;
+            if (m == l) w /= 2;
+            w16[m + l * (l + 1) / 2] = w;
+        }
     std::vector<double2> twk, tww, htw;
     twiddles(nk0, -2.0L, 1.0L, twk);
     twiddles(nw0, -2.0L, 1.0L, tww);
@@ -370,12 +382,15 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
         e = (x);                                   \
     }
     A(upload(g, &d.lm, lm));
+    A(upload(g, &d.w16, w16));
     A(upload(g, &d.tw_k, twk));
     A(upload(g, &d.tw_w, tww));
     A(upload(g, &d.ht_w, htw));
     A(upload(g, &d.spl_half, sh));
     A(upload(g, &d.spl_full, sf));
     A(dalloc(g, &d.ek, n8));
+    A(dalloc(g, &d.gk, n8));
+    A(dalloc(g, &d.tailq, (size_t)kTailQ));
     A(dalloc(g, &d.er, n8));
     A(dalloc(g, &g->Grt, (nw + 1) * n8));
     A(dalloc(g, &g->chirt, nb * n8p));
@@ -432,6 +447,21 @@ int grid_set_model(tpsc_ctx *ctx, Grid *g) {
     er[4] = -ctx->t3;
     CK(cudaMemcpyAsync(d.ek, eo.data(), d.n8 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(d.er, er.data(), d.n8 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    // power sums Q_k = sum_{n = Nw0/2+1}^{Nw0} qn^(-2k), qn = 2 pi n T, for the
+    // sum-rule tail series (smallest terms first, long double)
+    if (g->tailq_T != ctx->T) {
+        std::vector<long double> acc(kTailQ, 0.0L);
+        const int nwmax = d.nb - 1;
+        for (int j = 2 * nwmax; j > nwmax; --j) {
+            const long double wn = 2.0L * 3.141592653589793238462643383279502884L * j * (long double)ctx->T;
+            const long double x = 1.0L / (wn * wn);
+            long double xp = x;
+            for (int k = 1; k < kTailQ; ++k, xp *= x) acc[k] += xp;
+        }
+        for (int k = 0; k < kTailQ; ++k) g->tailq_host[k] = (double)acc[k];
+        CK(cudaMemcpyAsync(d.tailq, g->tailq_host, kTailQ * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+        g->tailq_T = ctx->T;
+    }
     CK(cudaStreamSynchronize(ctx->st));
     g->have_chi0 = g->have_V = g->have_S = false;
     if (ctx->n == 1.0 && ctx->tp == 0 && ctx->tpp == 0) {
@@ -677,6 +707,8 @@ tpsc_ctx *tpsc_create(int device, int *status) {
     if ((e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking)) != cudaSuccess) return bad(e);
     if ((e = cudaMalloc(&ctx->red.partial, 4 * kMaxBlocks * sizeof(double))) != cudaSuccess) return bad(e);
     if ((e = cudaMalloc(&ctx->red.result, 8 * sizeof(double))) != cudaSuccess) return bad(e);
+    if ((e = cudaMalloc(&ctx->red.ticket, sizeof(unsigned))) != cudaSuccess) return bad(e);
+    if ((e = cudaMemset(ctx->red.ticket, 0, sizeof(unsigned))) != cudaSuccess) return bad(e);
     if ((e = cudaMallocHost(&ctx->h_res, 8 * sizeof(double))) != cudaSuccess) return bad(e);
     for (auto &ev : ctx->ev)
         if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bad(e);
@@ -691,6 +723,7 @@ void tpsc_destroy(tpsc_ctx *ctx) {
     for (auto &kv : ctx->grids) free_grid(kv.second);
     if (ctx->red.partial) cudaFree(ctx->red.partial);
     if (ctx->red.result) cudaFree(ctx->red.result);
+    if (ctx->red.ticket) cudaFree(ctx->red.ticket);
     if (ctx->h_res) cudaFreeHost(ctx->h_res);
     if (ctx->stage) cudaFree(ctx->stage);
     for (auto &ev : ctx->ev)

@@ -116,21 +116,35 @@ __device__ __forceinline__ void group_sync(int grp) {
     }
 }
 
-// One Stockham pass of radix R over x[0..N) (padded layout), performed by a
-// group of G threads holding E points each; thread t does E/R butterflies
-// b = t + G u.  tw[m] = exp(-2 pi i m / N), m < N.
-template <int N, int G, int R, int SIGN, int E>
-__device__ __forceinline__ void stockham_pass(double2 *x, int t, int Ns, const double2 *__restrict__ tw,
-                                              int grp) {
+// Loaders / storers for the first and last FFT pass.  `In` returns input
+// element j of the sequence; `Out` receives output element k.
+struct ScratchIO {
+    double2 *x;
+    __device__ __forceinline__ double2 operator()(int j) const { return x[pidx(j)]; }
+    __device__ __forceinline__ void operator()(int k, double2 v) const { x[pidx(k)] = v; }
+};
+
+// One Stockham pass of radix R over a length-N sequence, performed by a group
+// of G threads holding E points each; thread t does E/R butterflies
+// b = t + G u.  tw[m] = exp(-2 pi i m / N), m < N.  The first pass reads its
+// inputs through `in` (FIRST), the last pass hands its outputs, in natural
+// order, to `out` (LAST); every other pass reads and writes the padded
+// scratch x in place, with group barriers around the writes.
+template <int N, int G, int R, int SIGN, int E, bool SMEM_TW, bool FIRST, bool LAST, class In, class Out>
+__device__ __forceinline__ void stockham_pass(double2 *x, int t, int Ns, const double2 *__restrict__ tw, int grp,
+                                              const In &in, const Out &out) {
     constexpr int NB = E / R;  // butterflies per thread
     double2 v[E];
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
         const int b = t + G * u;
 #pragma unroll
-        for (int q = 0; q < R; ++q) v[u * R + q] = x[pidx(b + q * (N / R))];
+        for (int q = 0; q < R; ++q) {
+            const int j = b + q * (N / R);
+            v[u * R + q] = FIRST ? in(j) : x[pidx(j)];
+        }
     }
-    group_sync<G>(grp);
+    if (!FIRST) group_sync<G>(grp);
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
         const int b = t + G * u;
@@ -140,7 +154,7 @@ __device__ __forceinline__ void stockham_pass(double2 *x, int t, int Ns, const d
             const int step = k * (N / (Ns * R));
 #pragma unroll
             for (int q = 1; q < R; ++q) {
-                double2 w = __ldg(&tw[(step * q) & (N - 1)]);
+                double2 w = SMEM_TW ? tw[(step * q) & (N - 1)] : __ldg(&tw[(step * q) & (N - 1)]);
                 if (SIGN > 0) w.y = -w.y;
                 v[u * R + q] = cmul(v[u * R + q], w);
             }
@@ -158,9 +172,14 @@ __device__ __forceinline__ void stockham_pass(double2 *x, int t, int Ns, const d
         const int k = b % Ns;
         const int base = (b / Ns) * Ns * R + k;
 #pragma unroll
-        for (int q = 0; q < R; ++q) x[pidx(base + q * Ns)] = v[u * R + q];
+        for (int q = 0; q < R; ++q) {
+            if (LAST)
+                out(base + q * Ns, v[u * R + q]);
+            else
+                x[pidx(base + q * Ns)] = v[u * R + q];
+        }
     }
-    group_sync<G>(grp);
+    if (!LAST) group_sync<G>(grp);
 }
 
 template <int N>
@@ -176,33 +195,55 @@ struct FftPlan {
     static constexpr int RLAST = 1 << (log2n() % 4);
     static constexpr int E = N < 16 ? N : 16;
     static constexpr int G = N / E;
+    static constexpr int NPASS = P16 + (RLAST > 1 ? 1 : 0);
 };
 
-// In-place FFT of x[0..N) (padded layout) by a group of G = FftPlan<N>::G
-// threads.  Must be called by all G threads of the group; x is synchronised
-// within the group on exit.
-template <int N, int SIGN>
-__device__ __forceinline__ void group_fft(double2 *x, int t, const double2 *__restrict__ tw, int grp) {
-    static_assert(N >= 4 && (N & (N - 1)) == 0, "power of two >= 4");
+template <int N, int SIGN, bool SMEM_TW, int P, class In, class Out>
+__device__ __forceinline__ void fft_passes(double2 *x, int t, int Ns, const double2 *__restrict__ tw, int grp,
+                                           const In &in, const Out &out) {
     constexpr int G = FftPlan<N>::G;
     constexpr int E = FftPlan<N>::E;
-    int Ns = 1;
-#pragma unroll
-    for (int p = 0; p < FftPlan<N>::P16; ++p) {
-        stockham_pass<N, G, 16, SIGN, E>(x, t, Ns, tw, grp);
-        Ns *= 16;
+    constexpr int NP = FftPlan<N>::NPASS;
+    constexpr int R = (P < FftPlan<N>::P16) ? 16 : FftPlan<N>::RLAST;
+    if constexpr (N <= 16) {
+        // one in-register DFT, single pass
+        stockham_pass<N, G, N, SIGN, E, SMEM_TW, true, true>(x, t, 1, tw, grp, in, out);
+    } else {
+        stockham_pass<N, G, R, SIGN, E, SMEM_TW, P == 0, P == NP - 1>(x, t, Ns, tw, grp, in, out);
+        if constexpr (P + 1 < NP) fft_passes<N, SIGN, SMEM_TW, P + 1>(x, t, Ns * R, tw, grp, in, out);
     }
-    if constexpr (FftPlan<N>::RLAST > 1) {
-        stockham_pass<N, G, FftPlan<N>::RLAST, SIGN, E>(x, t, Ns, tw, grp);
-    }
+}
+
+// FFT of a length-N sequence by a group of G = FftPlan<N>::G threads: inputs
+// from in(j), outputs (natural order) to out(k, value); x is the group's
+// padded scratch of padded_len(N) complex.  All G threads must call.  When
+// the FFT has more than one pass, x is free again when the call returns.
+template <int N, int SIGN, bool SMEM_TW = false, class In, class Out>
+__device__ __forceinline__ void group_fft_io(double2 *x, int t, const double2 *__restrict__ tw, int grp,
+                                             const In &in, const Out &out) {
+    static_assert(N >= 4 && (N & (N - 1)) == 0, "power of two >= 4");
+    fft_passes<N, SIGN, SMEM_TW, 0>(x, t, 1, tw, grp, in, out);
+    if constexpr (FftPlan<N>::NPASS > 1) group_sync<FftPlan<N>::G>(grp);
+}
+
+// In-place FFT of x[0..N) (padded layout).
+template <int N, int SIGN, bool SMEM_TW = false>
+__device__ __forceinline__ void group_fft(double2 *x, int t, const double2 *__restrict__ tw, int grp) {
+    const ScratchIO io{x};
+    // the first pass reads x into registers before the barrier that precedes
+    // any write of x, so in-place is safe
+    group_fft_io<N, SIGN, SMEM_TW>(x, t, tw, grp, io, io);
 }
 
 // 2D DCT-I (REDFT00 x REDFT00) in place on a symmetric NBK x NBK slice S
 // (row-major, leading dimension NBK, which is odd so that column accesses
 // are bank-conflict free).  scr: per-group FFT scratch, group g at
-// scr + g * padded_len(L).  All threads of the block must call.
+// scr + g * padded_len(L); tw: the L twiddles, in shared memory.  All
+// threads of the block must call.  Two lines (rows, then columns) go through
+// one complex FFT of their even extension; the first FFT pass reads the
+// lines straight from S and the last pass writes outputs k < NBK back.
 template <int NBK>
-__device__ void dct2_slice(double *S, double2 *scr, const double2 *__restrict__ tw) {
+__device__ void dct2_slice(double *S, double2 *scr, const double2 *tw) {
     constexpr int L = 2 * (NBK - 1);
     constexpr int G = FftPlan<L>::G;
     constexpr int NPAIR = (NBK + 1) / 2;
@@ -221,24 +262,20 @@ __device__ void dct2_slice(double *S, double2 *scr, const double2 *__restrict__ 
         for (int p = grp; p < NPAIR; p += ngrp) {
             const int r0 = 2 * p, r1 = 2 * p + 1;
             const bool two = r1 < NBK;
-            const double *a = S + r0 * ls;
-            const double *b = S + r1 * ls;
-#pragma unroll 4
-            for (int j = t; j < L; j += G) {
+            double *a = S + r0 * ls;
+            double *b = S + (two ? r1 : r0) * ls;
+            auto in = [&](int j) -> double2 {
                 const int c = j < NBK ? j : L - j;
-                x[pidx(j)] = make_double2(a[c * es], two ? b[c * es] : 0.0);
-            }
-            group_sync<G>(grp);
-            group_fft<L, -1>(x, t, tw, grp);
-            double *ao = S + r0 * ls;
-            double *bo = S + r1 * ls;
-#pragma unroll 4
-            for (int k = t; k < NBK; k += G) {
-                const double2 z = x[pidx(k)];
-                ao[k * es] = z.x;
-                if (two) bo[k * es] = z.y;
-            }
-            group_sync<G>(grp);
+                return make_double2(a[c * es], two ? b[c * es] : 0.0);
+            };
+            auto out = [&](int k, double2 z) {
+                if (k < NBK) {
+                    a[k * es] = z.x;
+                    if (two) b[k * es] = z.y;
+                }
+            };
+            group_fft_io<L, -1, true>(x, t, tw, grp, in, out);
+            if constexpr (FftPlan<L>::NPASS == 1) group_sync<G>(grp);
         }
         __syncthreads();
     }

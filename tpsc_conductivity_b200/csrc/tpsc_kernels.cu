@@ -155,12 +155,22 @@ struct SliceSmem {
     static constexpr int NGRP = kSliceThreads / G;
     static constexpr size_t slice_bytes = (size_t)NBK * NBK * sizeof(double);
     static constexpr size_t scr_off = (slice_bytes + 15) & ~(size_t)15;
-    static constexpr size_t bytes = scr_off + (size_t)NGRP * padded_len(L) * sizeof(double2);
+    static constexpr size_t tw_off = scr_off + (size_t)NGRP * padded_len(L) * sizeof(double2);
+    static constexpr size_t bytes = tw_off + (size_t)L * sizeof(double2);
 };
 
 template <int NBK>
 __device__ __forceinline__ double2 *slice_scratch(double *S) {
     return reinterpret_cast<double2 *>(reinterpret_cast<char *>(S) + SliceSmem<NBK>::scr_off);
+}
+
+// the L-point twiddle table staged in shared memory behind the FFT scratch;
+// the first __syncthreads of the kernel publishes it
+template <int NBK>
+__device__ __forceinline__ const double2 *slice_twiddles(double *S, const double2 *__restrict__ tw) {
+    double2 *t = reinterpret_cast<double2 *>(reinterpret_cast<char *>(S) + SliceSmem<NBK>::tw_off);
+    for (int i = threadIdx.x; i < SliceSmem<NBK>::L; i += blockDim.x) t[i] = __ldg(&tw[i]);
+    return t;
 }
 
 // write octant value v of point (l, m) into both triangles of the slice
@@ -170,6 +180,19 @@ __device__ __forceinline__ void put_sym(double *S, int l, int m, double v) {
     S[m * NBK + l] = v;
 }
 
+// Per-octant constants of G0(k, tau)/L^2 (src/green.cpp:1834-1837):
+//   x = eps_k - mu0 > 0:  -exp(-tau x) / (exp(-x/T) + 1) / L^2
+//   x <= 0:               -exp((beta - tau) x) / (exp(x/T) + 1) / L^2
+// gk[o] = (x, prefactor), so one exp per element remains per slice.
+__global__ void k_gk_table(const double *__restrict__ ek, int n8, double mu0, double T, double nk02,
+                           double2 *__restrict__ gk) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n8) return;
+    const double x = ek[o] - mu0;
+    const double pre = x > 0 ? -1.0 / (exp(-x / T) + 1.0) / nk02 : -1.0 / (exp(x / T) + 1.0) / nk02;
+    gk[o] = make_double2(x, pre);
+}
+
 // G(r, tau_j) = DCT-I[ G0(k, tau_j) / L^2 ], tau_j = j / (Nw0 T), j = 0..Nw0,
 // with the overflow-safe branches of src/green.cpp:1834-1837.  The chi0 stage
 // needs G(r, tau) and G(r, -tau) (src/chi0.cpp:462-495); G(r,-tau) =
@@ -177,24 +200,23 @@ __device__ __forceinline__ void put_sym(double *S, int l, int m, double v) {
 // Grt[j * n8 + o].
 template <int NBK>
 __global__ void __launch_bounds__(kSliceThreads, 1)
-    k_gslice(const double *__restrict__ ek, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
-             double mu0, int n8, int nw0, double T, double nk02, double *__restrict__ Grt) {
+    k_gslice(const double2 *__restrict__ gk, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
+             int n8, int nw0, double T, double *__restrict__ Grt) {
     extern __shared__ __align__(16) double S[];
+    const double2 *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
     const double t = j / (nw0 * T);
+    const double bt = 1.0 / T - t;
+#pragma unroll 4
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
         oct_lm(lm, o, l, m);
-        const double x = ek[o] - mu0;
-        double g;
-        if (x > 0)
-            g = -exp(-t * x) / (exp(-x / T) + 1.0) / nk02;
-        else
-            g = -exp((1.0 / T - t) * x) / (exp(x / T) + 1.0) / nk02;
+        const double2 c = __ldg(&gk[o]);
+        const double g = c.y * exp((c.x > 0 ? -t : bt) * c.x);
         put_sym<NBK>(S, l, m, g);
     }
     __syncthreads();
-    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tw);
+    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     double *out = Grt + (size_t)j * n8;
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
@@ -211,6 +233,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     k_chi0_slice(const double *__restrict__ Grt, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
                  int n8, int nw0, double *__restrict__ chirt, double *__restrict__ chiq) {
     extern __shared__ __align__(16) double S[];
+    const double2 *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
     const int nb = nw0 / 2 + 1;
     const double *gp = Grt + (size_t)j * n8;
@@ -230,7 +253,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
         put_sym<NBK>(S, l, m, c);
     }
     __syncthreads();
-    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tw);
+    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
         oct_lm(lm, o, l, m);
@@ -247,6 +270,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
                     double nk02, double *__restrict__ dG0p, double *__restrict__ dtau_chirt0,
                     double *__restrict__ dtau_chiqt0) {
     extern __shared__ __align__(16) double S[];
+    const double2 *tws = slice_twiddles<NBK>(S, tw);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
         oct_lm(lm, o, l, m);
@@ -255,7 +279,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
         put_sym<NBK>(S, l, m, -x * gkt / nk02);
     }
     __syncthreads();
-    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tw);
+    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     // every thread handles the same octant points in both loops, so the
     // first loop's S reads complete before its second-loop writes
     double dp_[(NBK * (NBK + 1) / 2 + kSliceThreads - 1) / kSliceThreads];
@@ -281,7 +305,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
         put_sym<NBK>(S, l, m, dc_[k]);
     }
     __syncthreads();
-    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tw);
+    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
         oct_lm(lm, o, l, m);
@@ -296,6 +320,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     k_vertex_q(const double *__restrict__ chiq, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
                int n8, int nb, double normFact, double U, double Usp, double Uch, double *__restrict__ Vr) {
     extern __shared__ __align__(16) double S[];
+    const double2 *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
@@ -306,7 +331,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
         put_sym<NBK>(S, l, m, normFact * U * (3.0 * Usp * (sp - c0) + Uch * (ch - c0)) / 8.0);
     }
     __syncthreads();
-    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tw);
+    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
         oct_lm(lm, o, l, m);
@@ -323,6 +348,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
                      const double *__restrict__ dG0p, int n8, int nw0, int n8p, double mu0, double fact,
                      double *__restrict__ dS) {
     extern __shared__ __align__(16) double S[];
+    const double2 *tws = slice_twiddles<NBK>(S, tw);
     const int nb = nw0 / 2 + 1;
 #pragma unroll 1
     for (int side = 0; side < 2; ++side) {
@@ -341,7 +367,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
             put_sym<NBK>(S, l, m, val);
         }
         __syncthreads();
-        dct2_slice<NBK>(S, slice_scratch<NBK>(S), tw);
+        dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
         for (int o = threadIdx.x; o < n8; o += blockDim.x) {
             int l, m;
             oct_lm(lm, o, l, m);
@@ -358,6 +384,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     k_sigma_slice(const double *__restrict__ Grt, const double *__restrict__ V, const uint32_t *__restrict__ lm,
                   const double2 *__restrict__ tw, int n8, int nw0, double *__restrict__ sigt) {
     extern __shared__ __align__(16) double S[];
+    const double2 *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
     const int nb = nw0 / 2 + 1;
     const int jv = j < nb ? j : nw0 - j;
@@ -368,7 +395,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
         put_sym<NBK>(S, l, m, g[o] * V[bidx(jv, o, nb)]);
     }
     __syncthreads();
-    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tw);
+    dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
         oct_lm(lm, o, l, m);
@@ -536,14 +563,14 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
     for (int pr = 0; pr < 2; ++pr) {
         const double *Ma = A + (2 * pr) * NJ;
         const double *Mb = A + (2 * pr + 1) * NJ;
-        for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        // FFT input: 6 a_j = (M_{j+1} - M_j)/h, antisymmetrised over [N/2, N)
+        auto in = [&](int j) -> double2 {
             const bool lo = j < N / 2;
             const int jj = lo ? j : N - 1 - j;
             const double sg = lo ? 1.0 : -1.0;
-            X[pidx(j)] = make_double2(sg * (Ma[jj + 1] - Ma[jj]) / h, sg * (Mb[jj + 1] - Mb[jj]) / h);
-        }
-        __syncthreads();
-        if (threadIdx.x < G) group_fft<N, +1>(X, threadIdx.x, tw, 0);
+            return make_double2(sg * (Ma[jj + 1] - Ma[jj]) / h, sg * (Mb[jj + 1] - Mb[jj]) / h);
+        };
+        if (threadIdx.x < G) group_fft_io<N, +1>(X, threadIdx.x, tw, 0, in, ScratchIO{X});
         __syncthreads();
         for (int n = threadIdx.x + 1; n < NJ; n += blockDim.x) {
             const double2 Z = X[pidx(n)];
@@ -594,12 +621,12 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
     for (int pr = 0; pr < 2; ++pr) {
         double *a = A + (2 * pr) * NJ;
         double *b = A + (2 * pr + 1) * NJ;
-        for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        // even extension of the two columns: a DCT-I each, packed as Re/Im
+        auto in = [&](int j) -> double2 {
             const int jj = j < NJ ? j : N - j;
-            X[pidx(j)] = make_double2(a[jj], b[jj]);
-        }
-        __syncthreads();
-        if (threadIdx.x < G) group_fft<N, -1>(X, threadIdx.x, tw, 0);
+            return make_double2(a[jj], b[jj]);
+        };
+        if (threadIdx.x < G) group_fft_io<N, -1>(X, threadIdx.x, tw, 0, in, ScratchIO{X});
         __syncthreads();
         for (int n = threadIdx.x; n < NJ; n += blockDim.x) {
             const double2 Z = X[pidx(n)];
@@ -655,13 +682,13 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
     for (int pr = 0; pr < 2; ++pr) {
         const double *Ma = A + (2 * pr) * NJ;
         const double *Mb = A + (2 * pr + 1) * NJ;
-        for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        // FFT input: exp(i pi j/N) 6 a_j, two columns packed as Re/Im
+        auto in = [&](int j) -> double2 {
             const double fa = (Ma[j + 1] - Ma[j]) / h;
             const double fb = (Mb[j + 1] - Mb[j]) / h;
-            X[pidx(j)] = cmul(__ldg(&ht[j]), make_double2(fa, fb));
-        }
-        __syncthreads();
-        if (threadIdx.x < G) group_fft<N, +1>(X, threadIdx.x, tw, 0);
+            return cmul(__ldg(&ht[j]), make_double2(fa, fb));
+        };
+        if (threadIdx.x < G) group_fft_io<N, +1>(X, threadIdx.x, tw, 0, in, ScratchIO{X});
         __syncthreads();
         for (int n = threadIdx.x; n < NO; n += blockDim.x) {
             const double2 Z = X[pidx(n)];
@@ -688,215 +715,341 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
 // sum rules and traces
 // ---------------------------------------------------------------------------
 
-// sum_{q, n <= Nw0/2} w T/Nq [chi/(1 + s U chi/2) - chi] plus the tail
-// Nw0/2 < n <= Nw0 with chi = c2/qn^2 + c4/qn^4, and its U derivative
-// (chi::traceDiffChispChi0 s = -1, traceDiffChichChi0 s = +1,
-// src/chi.cpp:738-830)
-__global__ void k_sumrule(const double *__restrict__ chiq, const double *__restrict__ cinf,
-                          const double *__restrict__ cinf2, const uint32_t *__restrict__ lm, int n8, int n8p, int nb,
-                          int nbk, double Uv, double sgn, double T, double Nq, double *partial) {
-    KSum v, dv;
-    const long long main_total = (long long)n8p * nb;
-    const int nwmax = nb - 1;
-    const long long tail_total = (long long)n8 * nwmax;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < main_total + tail_total; i += stride) {
-        double c;
-        int w, o;
-        if (i < main_total) {
-            const long long blk = i / (4LL * nb);
-            const int rem = (int)(i - blk * 4LL * nb);
-            const int j = rem >> 2;
-            o = (int)(blk * 4) + (rem & 3);
-            if (o >= n8) continue;
-            int l, m;
-            oct_lm(lm, o, l, m);
-            w = 16;
-            if (j == 0) w /= 2;
-            w = oct_weight(w, l, m, nbk);
-            c = chiq[i];
-        } else {
-            const long long t = i - main_total;
-            o = (int)(t % n8);
-            const int jt = nwmax + 1 + (int)(t / n8);
-            int l, m;
-            oct_lm(lm, o, l, m);
-            w = oct_weight(16, l, m, nbk);
-            const double wn = 2 * jt * kPi * T;
-            c = cinf[o] / (wn * wn) + cinf2[o] / (wn * wn * wn * wn);
+// Deterministic grid reduction for the column-block reducers: every block
+// stores NV partial sums, the last block to arrive (ticket counter) adds all
+// partials in block order with compensated summation and resets the ticket.
+// Partials are read with ld.global.cg, so the other blocks' stores (fenced
+// before the ticket increment) are seen.
+template <int NV>
+__device__ void grid_finish(double (&v)[NV], Reduce r, double offset0) {
+    __shared__ double red[32][NV];
+    __shared__ bool last;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) red[warp][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = blockDim.x >> 5;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double x = 0.0;
+            for (int w = 0; w < nw; ++w) x += red[w][k];
+            r.partial[k * kMaxBlocks + blockIdx.x] = x;
         }
-        const double den = 1 + sgn * Uv * c / 2.0;
-        const double f = w * T / Nq;
-        v.add(f * (c / den - c));
-        dv.add(f * (-sgn * c * c / 2.0 / (den * den)));
+        __threadfence();
+        const unsigned t = atomicAdd(r.ticket, 1u);
+        last = (t == gridDim.x - 1);
     }
-    double out[2] = {v.value(), dv.value()};
-    block_store<2>(out, partial);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    KSum acc[NV];
+    // thread t owns the contiguous slice [t*per, (t+1)*per) of the partials
+    const int nb = gridDim.x;
+    const int per = (nb + blockDim.x - 1) / blockDim.x;
+    for (int b = threadIdx.x * per; b < min(nb, (int)(threadIdx.x + 1) * per); ++b)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[k].add(__ldcg(&r.partial[k * kMaxBlocks + b]));
+    __shared__ double all[1024][NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) all[threadIdx.x][k] = acc[k].value();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            KSum s;
+            for (int i = 0; i < (int)blockDim.x; ++i) s.add(all[i][k]);
+            r.result[k] = s.value() + (k == 0 ? offset0 : 0.0);
+        }
+        *r.ticket = 0u;
+    }
 }
 
-// raw and tail parts of chi0::traceChi0 (src/chi0.cpp:1498-1584)
-__global__ void k_trace_chi0(const double *__restrict__ chiq, const double *__restrict__ cinf,
-                             const double *__restrict__ cinf2, const uint32_t *__restrict__ lm, int n8, int n8p, int nb,
-                             int nbk, double T, double Nq, double *partial) {
-    KSum v, vt;
-    const long long main_total = (long long)n8p * nb;
-    const int nwmax = nb - 1;
-    const long long tail_total = (long long)n8 * (nwmax - 1);
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < main_total + tail_total; i += stride) {
-        if (i < main_total) {
-            const long long blk = i / (4LL * nb);
-            const int rem = (int)(i - blk * 4LL * nb);
-            const int j = rem >> 2;
-            const int o = (int)(blk * 4) + (rem & 3);
-            if (o >= n8) continue;
-            int l, m;
-            oct_lm(lm, o, l, m);
-            int w = 16;
-            if (j == 0 || j == nwmax) w /= 2;
-            w = oct_weight(w, l, m, nbk);
-            v.add(w * T * chiq[i] / Nq);
-        } else {
-            const long long t = i - main_total;
-            const int o = (int)(t % n8);
-            const int jt = nwmax + 1 + (int)(t / n8);
-            int l, m;
-            oct_lm(lm, o, l, m);
-            const int w = oct_weight(16, l, m, nbk);
-            const double wn = 2 * kPi * jt * T;
-            vt.add(w * T * (cinf[o] / (wn * wn) + cinf2[o] / (wn * wn * wn * wn)) / Nq);
-        }
-    }
-    double out[2] = {v.value(), vt.value()};
-    block_store<2>(out, partial);
+constexpr int kRedThreads = 256;
+
+// streaming (evict-first) load of 32 bytes as two 16-byte loads
+__device__ __forceinline__ double4 ld_stream4(const double4 *p) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    const double2 a = __ldcs(q), b = __ldcs(q + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
 }
 
-// full Sigma(k, i w_n) = Sinf/z + C2/z^2 + C3/z^3 + S/z^4, z = i w_n
-__device__ __forceinline__ void sigma_full(double wn, double sinf, double c2, double c3, double2 Sv, double &rS,
+// chi::traceDiffChispChi0 (sgn = -1) / traceDiffChichChi0 (sgn = +1)
+// (src/chi.cpp:738-830): sum over q and n <= Nw0/2 of w T/Nq [chi/(1 + sgn U
+// chi/2) - chi], plus the tail Nw0/2 < n <= Nw0 with chi = c2/qn^2 + c4/qn^4,
+// and d/dU of the same sum.  One CTA per block of four octant columns: the
+// block's rows are contiguous 32-byte loads.  w16 holds the octant weights
+// (16 halved on edges and diagonal; 0 on padding columns); the row n = 0
+// carries an extra factor 1/2.
+//
+// Tail: with x_n = 1/qn^2, chi_n = a x_n + b x_n^2 and h = sgn U/2,
+//   chi/(1 + h chi) - chi = sum_{m>=1} (-h)^m chi^{m+1},
+//   sum_n chi_n^{m+1} = sum_i C(m+1, i) a^{m+1-i} b^i Q_{m+1+i},
+// with the U-independent power sums Q_k = sum_n x_n^k (tailq[k], k <= 2 kTailM + 2).
+// A column whose |h chi_max| >= kTailSeriesMax is summed term by term.
+constexpr int kTailM = 8;
+constexpr double kTailSeriesMax = 0.004;  // (0.004)^8 < 1e-19: series truncation below rounding
+
+__device__ __forceinline__ void tail_series(double a, double b, double h, const double *__restrict__ Q, double &f,
+                                           double &dfdh) {
+    double ap[kTailM + 2], bp[kTailM + 2];
+    ap[0] = bp[0] = 1.0;
+#pragma unroll
+    for (int k = 1; k < kTailM + 2; ++k) {
+        ap[k] = ap[k - 1] * a;
+        bp[k] = bp[k - 1] * b;
+    }
+    f = 0.0;
+    dfdh = 0.0;
+    double hm = 1.0;  // (-h)^(m-1)
+#pragma unroll
+    for (int m = 1; m <= kTailM; ++m) {
+        const int p = m + 1;
+        double Sp = 0.0, coef = 1.0;  // coef = C(p, i)
+#pragma unroll
+        for (int i = 0; i <= p; ++i) {
+            Sp += coef * ap[p - i] * bp[i] * __ldg(&Q[p + i]);
+            coef = coef * (p - i) / (i + 1);
+        }
+        f += (-h) * hm * Sp;           // (-h)^m S_p
+        dfdh += -m * hm * Sp;          // d/dh (-h)^m = -m (-h)^(m-1)
+        hm *= -h;
+    }
+}
+
+__global__ void __launch_bounds__(kRedThreads)
+    k_sumrule(const double4 *__restrict__ chiq, const double *__restrict__ cinf, const double *__restrict__ cinf2,
+              const double *__restrict__ w16, const double *__restrict__ tailq, int nb, double Uv, double sgn,
+              double T, double scale, Reduce r) {
+    const int blk = blockIdx.x;
+    const int o0 = 4 * blk;
+    const double4 w = *reinterpret_cast<const double4 *>(w16 + o0);
+    const double ww[4] = {w.x, w.y, w.z, w.w};
+    const double hu = sgn * Uv / 2.0;
+    double v = 0.0, dv = 0.0;
+    const double4 *col = chiq + (size_t)blk * nb;
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+        const double4 x = ld_stream4(&col[j]);
+        const double f = j == 0 ? 0.5 : 1.0;
+        const double xs[4] = {x.x, x.y, x.z, x.w};
+        double sv = 0.0, sd = 0.0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double q = xs[c] / (1.0 + hu * xs[c]);
+            sv += ww[c] * (q - xs[c]);
+            sd += ww[c] * q * q;
+        }
+        v += f * sv;
+        dv += f * sd;
+    }
+    dv *= -0.5 * sgn;
+    // tail: n = nwmax+1 .. 2 nwmax
+    const int nwmax = nb - 1;
+    const double tw = 2.0 * 3.141592653589793 * T;
+    const double wn1 = (nwmax + 1) * tw;
+    const double x1 = 1.0 / (wn1 * wn1);
+    double tv = 0.0, tdv = 0.0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        if (ww[c] == 0.0) continue;
+        const double a = cinf[o0 + c], b = cinf2[o0 + c];
+        const double cmax = fabs(a) * x1 + fabs(b) * x1 * x1;
+        if (fabs(hu) * cmax < kTailSeriesMax) {
+            if (threadIdx.x == c) {
+                double f, dfdh;
+                tail_series(a, b, hu, tailq, f, dfdh);
+                tv += ww[c] * f;
+                tdv += ww[c] * dfdh * (0.5 * sgn);
+            }
+        } else {
+            for (int t = threadIdx.x; t < nwmax; t += blockDim.x) {
+                const double wn = (nwmax + 1 + t) * tw;
+                const double i2 = 1.0 / (wn * wn);
+                const double xv = a * i2 + b * i2 * i2;
+                const double q = xv / (1.0 + hu * xv);
+                tv += ww[c] * (q - xv);
+                tdv += ww[c] * (-0.5 * sgn) * q * q;
+            }
+        }
+    }
+    double out[2] = {scale * (v + tv), scale * (dv + tdv)};
+    grid_finish<2>(out, r, 0.0);
+}
+
+// full Sigma(k, i w_n) = Sinf/z + C2/z^2 + C3/z^3 + S/z^4, z = i w_n, from the
+// reciprocal powers of w_n
+__device__ __forceinline__ void sigma_full(double i1, double sinf, double c2, double c3, double2 Sv, double &rS,
                                            double &iS) {
-    const double w2 = wn * wn, w4 = w2 * w2;
-    rS = -c2 / w2 + Sv.x / w4;
-    iS = -sinf / wn + c3 / (w2 * wn) + Sv.y / w4;
+    const double i2 = i1 * i1, i4 = i2 * i2;
+    rS = -c2 * i2 + Sv.x * i4;
+    iS = -sinf * i1 + c3 * i2 * i1 + Sv.y * i4;
 }
 
-// Tr(G - G0) at chemical potential pmu (green::traceDiffG, src/green.cpp:3108-3182)
-__global__ void k_trace_diff_G(const double2 *__restrict__ S, const double *__restrict__ s2,
-                               const double *__restrict__ s3, const double *__restrict__ s4,
-                               const double *__restrict__ sinfp, const double *__restrict__ ek,
-                               const uint32_t *__restrict__ lm, int n8, int n8p, int nw0, int nbk, double mu0,
-                               double pmu, double T, double *partial) {
-    KSum v;
-    const int NO = nw0 / 2;
+// Tr(G - G0) at chemical potential pmu (green::traceDiffG,
+// src/green.cpp:3108-3182): stored frequencies j < Nw0/2 with the full Sigma,
+// tail Nw0/2 <= j <= Nw0 with its asymptotic form.  One CTA per column block.
+__device__ __forceinline__ double trdiff_term(double wn, double rS, double iS, double e, double mu0, double pmu) {
+    const double a = e - pmu + rS, d = e - mu0, g = mu0 - pmu + rS;
+    const double tmp = 1.0 / (((wn - iS) * (wn - iS) + a * a) * (wn * wn + d * d));
+    return tmp * (g * a * d + iS * (iS - 2 * wn) * d - wn * wn * g);
+}
+
+__global__ void __launch_bounds__(kRedThreads)
+    k_trace_diff_G(const double2 *__restrict__ S, const double *__restrict__ s2, const double *__restrict__ s3,
+                   const double *__restrict__ s4, const double *__restrict__ sinfp, const double *__restrict__ ek,
+                   const double *__restrict__ w16, int nw0, double mu0, double pmu, double T, Reduce r) {
+    const int blk = blockIdx.x, o0 = 4 * blk, NO = nw0 / 2;
     const double sinf = sinfp[0];
-    const long long main_total = (long long)n8p * NO;
-    const long long tail_total = (long long)n8 * (nw0 / 2 + 1);
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < main_total + tail_total; i += stride) {
-        int o, j;
-        double rS, iS;
-        if (i < main_total) {
-            const long long blk = i / (4LL * NO);
-            const int rem = (int)(i - blk * 4LL * NO);
-            j = rem >> 2;
-            o = (int)(blk * 4) + (rem & 3);
-            if (o >= n8) continue;
-            const double wn = (2 * j + 1) * kPi * T;
-            sigma_full(wn, sinf, s2[o], s3[o], S[i], rS, iS);
-        } else {
-            const long long t = i - main_total;
-            o = (int)(t % n8);
-            j = NO + (int)(t / n8);
-            const double wn = (2 * j + 1) * kPi * T;
-            rS = -s2[o] / (wn * wn) + s4[o] / (wn * wn * wn * wn);
-            iS = -sinf / wn + s3[o] / (wn * wn * wn);
-        }
-        int l, m;
-        oct_lm(lm, o, l, m);
-        const int w = oct_weight(16, l, m, nbk);
-        const double wn = (2 * j + 1) * kPi * T;
-        const double e = ek[o];
-        const double tmp = ((double)w) / (((wn - iS) * (wn - iS) + (e - pmu + rS) * (e - pmu + rS)) *
-                                          (wn * wn + (e - mu0) * (e - mu0)));
-        v.add(tmp * ((mu0 - pmu + rS) * (e - pmu + rS) * (e - mu0) + iS * (iS - 2 * wn) * (e - mu0) -
-                     wn * wn * (mu0 - pmu + rS)));
+    double ww[4], e[4], c2[4], c3[4], c4[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        ww[c] = w16[o0 + c];
+        const bool ok = ww[c] != 0.0;
+        e[c] = ok ? ek[o0 + c] : 0.0;
+        c2[c] = ok ? s2[o0 + c] : 0.0;
+        c3[c] = ok ? s3[o0 + c] : 0.0;
+        c4[c] = ok ? s4[o0 + c] : 0.0;
     }
-    double out[1] = {v.value()};
-    block_store<1>(out, partial);
+    const double pt = 3.141592653589793 * T;
+    double v = 0.0;
+    const double4 *row = reinterpret_cast<const double4 *>(S + (size_t)blk * 4 * NO);
+    for (int j = threadIdx.x; j < NO; j += blockDim.x) {
+        const double wn = (2 * j + 1) * pt;
+        const double i1 = 1.0 / wn;
+        const double4 p = ld_stream4(&row[2 * j]), q = ld_stream4(&row[2 * j + 1]);
+        const double2 sv[4] = {make_double2(p.x, p.y), make_double2(p.z, p.w), make_double2(q.x, q.y),
+                               make_double2(q.z, q.w)};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (ww[c] == 0.0) continue;
+            double rS, iS;
+            sigma_full(i1, sinf, c2[c], c3[c], sv[c], rS, iS);
+            v += ww[c] * trdiff_term(wn, rS, iS, e[c], mu0, pmu);
+        }
+    }
+    for (int t = threadIdx.x; t <= NO; t += blockDim.x) {
+        const int j = NO + t;
+        const double wn = (2 * j + 1) * pt;
+        const double i1 = 1.0 / wn, i2 = i1 * i1;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (ww[c] == 0.0) continue;
+            const double rS = -c2[c] * i2 + c4[c] * i2 * i2;
+            const double iS = -sinf * i1 + c3[c] * i2 * i1;
+            v += ww[c] * trdiff_term(wn, rS, iS, e[c], mu0, pmu);
+        }
+    }
+    double out[1] = {v};
+    grid_finish<1>(out, r, 0.0);
 }
 
-// Tr Sigma G0 and its asymptotic correction (green::traceSelfG, src/green.cpp:3001-3084)
-__global__ void k_trace_self_G(const double2 *__restrict__ S, const double *__restrict__ s2,
-                               const double *__restrict__ s3, const double *__restrict__ sinfp,
-                               const double *__restrict__ ek, const uint32_t *__restrict__ lm, int n8, int n8p,
-                               int nw0, int nbk, double mu0, double T, double nk02, double *partial) {
-    KSum v, v2;
-    const int NO = nw0 / 2;
+// Tr Sigma G0 and its asymptotic correction (green::traceSelfG,
+// src/green.cpp:3001-3084); w8 = w16 / 2.
+__global__ void __launch_bounds__(kRedThreads)
+    k_trace_self_G(const double2 *__restrict__ S, const double *__restrict__ s2, const double *__restrict__ s3,
+                   const double *__restrict__ sinfp, const double *__restrict__ ek, const double *__restrict__ w16,
+                   int nw0, double mu0, double T, double nk02, Reduce r) {
+    const int blk = blockIdx.x, o0 = 4 * blk, NO = nw0 / 2;
     const double sinf = sinfp[0];
-    const long long main_total = (long long)n8p * NO;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < main_total + n8; i += stride) {
-        if (i < main_total) {
-            const long long blk = i / (4LL * NO);
-            const int rem = (int)(i - blk * 4LL * NO);
-            const int j = rem >> 2;
-            const int o = (int)(blk * 4) + (rem & 3);
-            if (o >= n8) continue;
-            int l, m;
-            oct_lm(lm, o, l, m);
-            const int w = oct_weight(8, l, m, nbk);
-            const double wn = (2 * j + 1) * kPi * T;
+    const double pt = 3.141592653589793 * T;
+    KSum v, v2;
+    const double4 *row = reinterpret_cast<const double4 *>(S + (size_t)blk * 4 * NO);
+    for (int j = threadIdx.x; j < NO; j += blockDim.x) {
+        const double wn = (2 * j + 1) * pt;
+        const double i1 = 1.0 / wn;
+        const double4 p = ld_stream4(&row[2 * j]), q = ld_stream4(&row[2 * j + 1]);
+        const double2 sv[4] = {make_double2(p.x, p.y), make_double2(p.z, p.w), make_double2(q.x, q.y),
+                               make_double2(q.z, q.w)};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double w8 = 0.5 * w16[o0 + c];
+            if (w8 == 0.0) continue;
             double rS, iS;
-            sigma_full(wn, sinf, s2[o], s3[o], S[i], rS, iS);
-            const double e = ek[o];
-            const double tmp = w * T * 2 / (nk02 * (wn * wn + (e - mu0) * (e - mu0)));
-            v.add(tmp * (rS * (mu0 - e) + iS * wn));
-            v2.add(w * sinf * T * 2 / (nk02 * (wn * wn + (e - mu0) * (e - mu0))));
-        } else {
-            const int o = (int)(i - main_total);
-            int l, m;
-            oct_lm(lm, o, l, m);
-            const int w = oct_weight(8, l, m, nbk);
-            const double x = ek[o] - mu0;
+            sigma_full(i1, sinf, s2[o0 + c], s3[o0 + c], sv[c], rS, iS);
+            const double x = ek[o0 + c] - mu0;
+            const double tmp = w8 * T * 2 / (nk02 * (wn * wn + x * x));
+            v.add(tmp * (rS * (-x) + iS * wn));
+            v2.add(w8 * sinf * T * 2 / (nk02 * (wn * wn + x * x)));
+        }
+    }
+    if (threadIdx.x < 4) {
+        const int c = threadIdx.x;
+        const double w8 = 0.5 * w16[o0 + c];
+        if (w8 != 0.0) {
+            const double x = ek[o0 + c] - mu0;
             if (fabs(x) > 1.0e-12) {
-                v2.add(w * sinf * (1.0 / (exp(x / T) + 1.0) - 0.5) / x / nk02);
+                v2.add(w8 * sinf * (1.0 / (exp(x / T) + 1.0) - 0.5) / x / nk02);
             } else {
                 const double ex = (x < 0) ? exp(x / T) : exp(-x / T);
-                v2.add(-w * sinf * ex / ((ex + 1.0) * (ex + 1.0) * nk02 * T));
+                v2.add(-w8 * sinf * ex / ((ex + 1.0) * (ex + 1.0) * nk02 * T));
             }
         }
     }
     double out[2] = {v.value(), v2.value()};
-    block_store<2>(out, partial);
+    grid_finish<2>(out, r, 0.0);
 }
 
 // Tr Sigma G (green::traceSelfG2, src/green.cpp:2929-2976)
-__global__ void k_trace_self_G2(const double2 *__restrict__ S, const double *__restrict__ s2,
-                                const double *__restrict__ s3, const double *__restrict__ sinfp,
-                                const double *__restrict__ ek, const uint32_t *__restrict__ lm, int n8, int n8p,
-                                int nw0, int nbk, double mu, double T, double nk02, double *partial) {
-    KSum v;
-    const int NO = nw0 / 2;
+__global__ void __launch_bounds__(kRedThreads)
+    k_trace_self_G2(const double2 *__restrict__ S, const double *__restrict__ s2, const double *__restrict__ s3,
+                    const double *__restrict__ sinfp, const double *__restrict__ ek, const double *__restrict__ w16,
+                    int nw0, double mu, double T, double nk02, Reduce r) {
+    const int blk = blockIdx.x, o0 = 4 * blk, NO = nw0 / 2;
     const double sinf = sinfp[0];
-    const long long main_total = (long long)n8p * NO;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < main_total; i += stride) {
-        const long long blk = i / (4LL * NO);
-        const int rem = (int)(i - blk * 4LL * NO);
-        const int j = rem >> 2;
-        const int o = (int)(blk * 4) + (rem & 3);
-        if (o >= n8) continue;
-        int l, m;
-        oct_lm(lm, o, l, m);
-        const int w = oct_weight(8, l, m, nbk);
-        const double wn = (2 * j + 1) * kPi * T;
-        double rS, iS;
-        sigma_full(wn, sinf, s2[o], s3[o], S[i], rS, iS);
-        const double e = ek[o];
-        const double tmp = w * T * 2 / (nk02 * ((wn - iS) * (wn - iS) + (e - mu + rS) * (e - mu + rS)));
-        v.add(tmp * (iS * wn - iS * iS - (e - mu) * rS - rS * rS));
+    const double pt = 3.141592653589793 * T;
+    KSum v;
+    const double4 *row = reinterpret_cast<const double4 *>(S + (size_t)blk * 4 * NO);
+    for (int j = threadIdx.x; j < NO; j += blockDim.x) {
+        const double wn = (2 * j + 1) * pt;
+        const double i1 = 1.0 / wn;
+        const double4 p = ld_stream4(&row[2 * j]), q = ld_stream4(&row[2 * j + 1]);
+        const double2 sv[4] = {make_double2(p.x, p.y), make_double2(p.z, p.w), make_double2(q.x, q.y),
+                               make_double2(q.z, q.w)};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double w8 = 0.5 * w16[o0 + c];
+            if (w8 == 0.0) continue;
+            double rS, iS;
+            sigma_full(i1, sinf, s2[o0 + c], s3[o0 + c], sv[c], rS, iS);
+            const double a = ek[o0 + c] - mu + rS;
+            const double tmp = w8 * T * 2 / (nk02 * ((wn - iS) * (wn - iS) + a * a));
+            v.add(tmp * (iS * wn - iS * iS - (ek[o0 + c] - mu) * rS - rS * rS));
+        }
     }
     double out[1] = {v.value()};
-    block_store<1>(out, partial);
+    grid_finish<1>(out, r, 0.0);
+}
+
+// raw and tail parts of chi0::traceChi0 (src/chi0.cpp:1498-1584)
+__global__ void __launch_bounds__(kRedThreads)
+    k_trace_chi0(const double4 *__restrict__ chiq, const double *__restrict__ cinf, const double *__restrict__ cinf2,
+                 const double *__restrict__ w16, int nb, double T, double Nq, Reduce r) {
+    const int blk = blockIdx.x, o0 = 4 * blk, nwmax = nb - 1;
+    const double4 w = *reinterpret_cast<const double4 *>(w16 + o0);
+    const double ww[4] = {w.x, w.y, w.z, w.w};
+    KSum v, vt;
+    const double4 *col = chiq + (size_t)blk * nb;
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+        const double4 x = col[j];
+        const double f = (j == 0 || j == nwmax) ? 0.5 : 1.0;
+        const double xs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            if (ww[c] != 0.0) v.add(f * ww[c] * T * xs[c] / Nq);
+    }
+    for (int t = threadIdx.x; t < nwmax - 1; t += blockDim.x) {
+        const double wn = 2 * 3.141592653589793 * (nwmax + 1 + t) * T;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            if (ww[c] != 0.0)
+                vt.add(ww[c] * T * (cinf[o0 + c] / (wn * wn) + cinf2[o0 + c] / (wn * wn * wn * wn)) / Nq);
+    }
+    double out[2] = {v.value(), vt.value()};
+    grid_finish<2>(out, r, 0.0);
 }
 
 // chi0max and its wave vector (src/chi0.cpp:703-717): the reference scans l
@@ -1007,8 +1160,9 @@ struct RunGslice {
         cudaError_t e = set_smem(k_gslice<NBK>, sm);
         if (e != cudaSuccess) return e;
         const double nk02 = (double)g->nk0 * g->nk0;
-        k_gslice<NBK><<<g->nw0 + 1, kSliceThreads, sm, st>>>(g->ek, g->lm, g->tw_k, mu0, g->n8, g->nw0, T, nk02,
-                                                              Grt);
+        k_gk_table<<<(g->n8 + 255) / 256, 256, 0, st>>>(g->ek, g->n8, mu0, T, nk02, g->gk);
+        if ((e = launched()) != cudaSuccess) return e;
+        k_gslice<NBK><<<g->nw0 + 1, kSliceThreads, sm, st>>>(g->gk, g->lm, g->tw_k, g->n8, g->nw0, T, Grt);
         return launched();
     }
 };
@@ -1145,25 +1299,18 @@ cudaError_t launch_chi0_tau(const GridDev &g, double *chiq, const double *dtau_c
 
 cudaError_t launch_sumrule(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
                            double Uv, double sign, double T, Reduce r, cudaStream_t st) {
-    const long long total = (long long)g.n8p * g.nb + (long long)g.n8 * (g.nb - 1);
-    const int nb = grid_for(total, 256);
     const double Nq = 4.0 * (g.nbk - 1) * (g.nbk - 1);
-    k_sumrule<<<nb, 256, 0, st>>>(chiq, chi0_inf, chi0_inf2, g.lm, g.n8, g.n8p, g.nb, g.nbk, Uv, sign, T, Nq,
-                                  r.partial);
-    cudaError_t e = launched();
-    if (e != cudaSuccess) return e;
-    return finish<2>(r, nb, 0.0, st);
+    k_sumrule<<<g.n8p / 4, kRedThreads, 0, st>>>(reinterpret_cast<const double4 *>(chiq), chi0_inf, chi0_inf2,
+                                                  g.w16, g.tailq, g.nb, Uv, sign, T, T / Nq, r);
+    return launched();
 }
 
 cudaError_t launch_trace_chi0(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
                               double T, Reduce r, cudaStream_t st) {
-    const long long total = (long long)g.n8p * g.nb + (long long)g.n8 * (g.nb - 2);
-    const int nb = grid_for(total, 256);
     const double Nq = 4.0 * (g.nbk - 1) * (g.nbk - 1);
-    k_trace_chi0<<<nb, 256, 0, st>>>(chiq, chi0_inf, chi0_inf2, g.lm, g.n8, g.n8p, g.nb, g.nbk, T, Nq, r.partial);
-    cudaError_t e = launched();
-    if (e != cudaSuccess) return e;
-    return finish<2>(r, nb, 0.0, st);
+    k_trace_chi0<<<g.n8p / 4, kRedThreads, 0, st>>>(reinterpret_cast<const double4 *>(chiq), chi0_inf, chi0_inf2,
+                                                     g.w16, g.nb, T, Nq, r);
+    return launched();
 }
 
 cudaError_t launch_vertex_q(const GridDev &g, const double *chiq, double *Vr, double U, double Usp, double Uch,
@@ -1192,37 +1339,22 @@ cudaError_t launch_sigma_tau(const GridDev &g, const double *sigt, const double 
 cudaError_t launch_trace_diff_G(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                                 const double *s4, const double *sinf, double mu0, double pmu, double T, Reduce r,
                                 cudaStream_t st) {
-    const long long total = (long long)g.n8p * (g.nw0 / 2) + (long long)g.n8 * (g.nw0 / 2 + 1);
-    const int nb = grid_for(total, 256);
-    k_trace_diff_G<<<nb, 256, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.lm, g.n8, g.n8p, g.nw0, g.nbk, mu0, pmu, T,
-                                       r.partial);
-    cudaError_t e = launched();
-    if (e != cudaSuccess) return e;
-    return finish<1>(r, nb, 0.0, st);
+    k_trace_diff_G<<<g.n8p / 4, kRedThreads, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.nw0, mu0, pmu, T, r);
+    return launched();
 }
 
 cudaError_t launch_trace_self_G(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                                 const double *sinf, double mu0, double T, Reduce r, cudaStream_t st) {
-    const long long total = (long long)g.n8p * (g.nw0 / 2) + g.n8;
-    const int nb = grid_for(total, 256);
     const double nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
-    k_trace_self_G<<<nb, 256, 0, st>>>(S, s2, s3, sinf, g.ek, g.lm, g.n8, g.n8p, g.nw0, g.nbk, mu0, T, nk02,
-                                       r.partial);
-    cudaError_t e = launched();
-    if (e != cudaSuccess) return e;
-    return finish<2>(r, nb, 0.0, st);
+    k_trace_self_G<<<g.n8p / 4, kRedThreads, 0, st>>>(S, s2, s3, sinf, g.ek, g.w16, g.nw0, mu0, T, nk02, r);
+    return launched();
 }
 
 cudaError_t launch_trace_self_G2(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                                  const double *sinf, double mu, double T, Reduce r, cudaStream_t st) {
-    const long long total = (long long)g.n8p * (g.nw0 / 2);
-    const int nb = grid_for(total, 256);
     const double nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
-    k_trace_self_G2<<<nb, 256, 0, st>>>(S, s2, s3, sinf, g.ek, g.lm, g.n8, g.n8p, g.nw0, g.nbk, mu, T, nk02,
-                                        r.partial);
-    cudaError_t e = launched();
-    if (e != cudaSuccess) return e;
-    return finish<1>(r, nb, 0.0, st);
+    k_trace_self_G2<<<g.n8p / 4, kRedThreads, 0, st>>>(S, s2, s3, sinf, g.ek, g.w16, g.nw0, mu, T, nk02, r);
+    return launched();
 }
 
 cudaError_t launch_chi0max(const GridDev &g, const double *chiq, Reduce r, cudaStream_t st) {

@@ -16,7 +16,10 @@ struct GridDev {
     int nb = 0;         // Nw0/2 + 1: bosonic n >= 0 == tau nodes on [0, beta/2]
     uint32_t *lm = nullptr;        // [n8] (l << 16) | m of octant point o
     double *ek = nullptr;          // [n8] eps_k on the octant
+    double2 *gk = nullptr;         // [n8] (eps_k - mu0, G0 prefactor) for the G(r, tau) slices
     double *er = nullptr;          // [n8] real-space hopping table
+    double *w16 = nullptr;         // [n8p] octant weight: 16 halved on edges and diagonal, 0 on padding
+    double *tailq = nullptr;       // [kTailQ] sum-rule tail power sums Q_k = sum_n qn^-2k (T dependent)
     double2 *tw_k = nullptr;       // [L]   exp(-2 pi i m / L)
     double2 *tw_w = nullptr;       // [Nw0] exp(-2 pi i m / Nw0)
     double2 *ht_w = nullptr;       // [Nw0] exp(+i pi m / Nw0)
@@ -31,11 +34,13 @@ __host__ __device__ inline size_t bidx(int j, int o, int NJ) {
     return ((size_t)(o >> 2) * NJ + j) * 4 + (o & 3);
 }
 
+constexpr int kMaxBlocks = 4096;
+constexpr int kTailQ = 20;  // Q_k for k < kTailQ (the series uses k <= 18)  // >= column blocks of the largest grid (2097)
 struct Reduce {
-    double *partial = nullptr;  // [2 * kMaxBlocks]
-    double *result = nullptr;   // [4]
+    double *partial = nullptr;   // [4 * kMaxBlocks]
+    double *result = nullptr;    // [8]
+    unsigned *ticket = nullptr;  // arrival counter of the last-block finish (0 between launches)
 };
-constexpr int kMaxBlocks = 1184;  // 8 blocks per SM on 148 SMs
 
 // ---- launchers (all asynchronous on `st`) ---------------------------------
 cudaError_t launch_density(const GridDev &g, double mu, double n, double T, Reduce r, cudaStream_t st);
