@@ -135,6 +135,22 @@ int tpsc_get_vertex(tpsc_ctx *ctx, double *vertex_rt);
 /* Self_kw_array [ (Nw0/2) * N8 ] complex (interleaved), Sigma_inf2/3/4 [N8]. */
 int tpsc_get_self(tpsc_ctx *ctx, double *self_kw, double *sigma_inf2, double *sigma_inf3, double *sigma_inf4);
 
+/* ---- real-frequency continuation (needs tpsc_find_mu) -------------------- */
+/* Sigma(k, z) and A(k, z) = -Im 1/(z - eps_k + mu - Sigma(k, z)) / pi for every
+ * octant k at the Nz complex energies z (interleaved re, im), from Sigma
+ * sampled at z_j = i (2 n_idx[j] + 1) pi T, j < Nn (2 <= Nn <= 32), read at
+ * the stored frequency j as green::MDC does (src/green.cpp:986-993).
+ * mode 0: Vidberg-Serene continued-fraction Pade (generique::
+ * pade_cont_frac_coef_rec and pade, src/generique.cpp:1605-1663);
+ * mode 1: Lagrange polynomial through the Nn samples (src/green.cpp:887-897).
+ * out_sigma [N8][Nz] complex (may be NULL), out_A [N8][Nz]. */
+int tpsc_pade_sigma(tpsc_ctx *ctx, const int *n_idx, int Nn, const double *z, int Nz, int mode,
+                    double *out_sigma, double *out_A);
+
+/* green::Gwn_local (src/green.cpp:209-266): local G(i w_n), n < Nw0/2,
+ * out [Nw0/2] complex interleaved. */
+int tpsc_gwn_local(tpsc_ctx *ctx, double *out);
+
 /* Device time of the last tpsc_solve per stage in ms:
  * {chi0, sum rules, vertex, self energy, traces + mu}; n <= 5. */
 int tpsc_stage_times(tpsc_ctx *ctx, double *ms, int n);

@@ -14,6 +14,8 @@
  *               (green.cpp:1673, 3001, 3185) -- the full TPSC solve
  *        cond   solve + cond_opt::calc_chijj_vertex_corr_all_optim(false,3,1,NULL,0)
  *               (cond_opt.cpp:2537)
+ *        post   solve + find_FS_inter, MDC(10 points, w=0, 4 etas), Gwn_local
+ *               (src/tpsc_main.cpp:77-114)
  *        bench  timings only: the half-grid pre-pass alone, then the solve
  * The reference writes its own text files into the current directory; the
  * probe chdir()s into OUTDIR/work first so they land there.
@@ -141,7 +143,7 @@ int main(int argc, char **argv) {
         t0 = omp_get_wtime();
         g->find_Usp_Uch(nk0 / 2, Nw0 / 2, Usc);
         fprintf(meta, "t_half %.6f\n", omp_get_wtime() - t0);
-    } else if (mode == "solve" || mode == "cond") {
+    } else if (mode == "solve" || mode == "post" || mode == "cond") {
         g->set_keep_chiqw(true);
         t0 = omp_get_wtime();
         g->calc_Self_FFT_spline();
@@ -157,6 +159,17 @@ int main(int argc, char **argv) {
         fprintf(meta, "t_self %.6f\nt_traceSelfG %.6f\nt_find_mu %.6f\n", t_self, t_tr, t_mu);
         g->dump_chi0(meta, absdir);
         g->dump_solve(meta, absdir);
+        if (mode == "post" || mode == "cond") {
+            // the post-processing tpsc_main.cpp runs after find_mu (lines 77-114)
+            g->find_FS_inter();
+            int NP = 10;
+            double eta_p[] = {0.01, 0.001, 0.0001, 0.00001};
+            int *n_qn = new int[Nw0 / 2];
+            for (int j = 0; j < Nw0 / 2; j++) n_qn[j] = j;
+            g->MDC(n_qn, NP, 0.0, eta_p, 4, true);
+            delete[] n_qn;
+            g->Gwn_local();
+        }
         if (mode == "cond") {
             std::cout << std::setprecision(17);
             t0 = omp_get_wtime();

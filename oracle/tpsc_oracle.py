@@ -670,3 +670,99 @@ def solve(U, tp, tpp, t3, n, T, nk0, Nw0) -> Solve:
     mu, _ = find_mu(ek, mu0, sr, T)
     tsg2 = trace_self_G2(ek, mu, sr, T, U, n)
     return Solve(nk0, Nw0, mu0, c0, ur, V, sr, mu, tsg, tsg2)
+
+
+# ----------------------------------------------------------------------------
+# real-frequency continuation and local G (src/generique.cpp:1605-1663,
+# src/green.cpp:209-266, 814-1068, 2210-2341)
+# ----------------------------------------------------------------------------
+def pade_coefficients(f, x):
+    """Vidberg-Serene continued-fraction coefficients
+    (generique::pade_cont_frac_coef_rec / pade_recursion, src/generique.cpp:1649-1663):
+    g_0(l) = f_l, g_m(l) = (g_{m-1}(m-1) - g_{m-1}(l)) / ((x_l - x_{m-1}) g_{m-1}(l)),
+    coef_m = g_m(m)."""
+    N = len(f)
+    g = np.array(f, dtype=np.complex128)
+    coef = np.zeros(N, dtype=np.complex128)
+    coef[0] = g[0]
+    for m in range(1, N):
+        gm = g[m - 1]
+        g[m:] = (gm - g[m:]) / ((x[m:] - x[m - 1]) * g[m:])
+        coef[m] = g[m]
+    return coef
+
+
+def pade_eval(z, x0, coef):
+    """generique::pade (src/generique.cpp:1628-1646)."""
+    n = len(coef)
+    A = 1.0 + 0j
+    B = 1.0 + (z - x0[0]) * coef[1]
+    q = A / B
+    for j in range(3, n + 1):
+        A = 1.0 + (z - x0[j - 2]) * coef[j - 1] / A
+        B = 1.0 + (z - x0[j - 2]) * coef[j - 1] / B
+        q = q * A / B
+    return q * coef[0]
+
+
+def lagrange_eval(z, x0, f):
+    s = 0j
+    for j in range(len(f)):
+        t = f[j]
+        for i in range(len(f)):
+            if i != j:
+                t = t * (z - x0[i]) / (x0[j] - x0[i])
+        s += t
+    return s
+
+
+def pade_sigma(ek, mu, sr: SelfResult, T, z, n_idx, Nn, mode=0):
+    """Sigma(k, z) and A(k, z) for every octant k from Nn Matsubara samples read at
+    the stored frequency j with z_j = i (2 n_idx[j] + 1) pi T (green::MDC,
+    src/green.cpp:986-1003): mode 0 Pade, mode 1 Lagrange polynomial."""
+    eo = to_octant(ek)
+    sig = sr.sigma(T)
+    x0 = 1j * (2 * np.asarray(n_idx[:Nn]) + 1) * PI * T
+    z = np.atleast_1d(np.asarray(z, dtype=np.complex128))
+    out_s = np.zeros((eo.size, z.size), dtype=np.complex128)
+    out_A = np.zeros((eo.size, z.size))
+    for o in range(eo.size):
+        f = sig[:Nn, o]
+        coef = pade_coefficients(f, x0) if mode == 0 else None
+        for iz, zz in enumerate(z):
+            s = pade_eval(zz, x0, coef) if mode == 0 else lagrange_eval(zz, x0, f)
+            out_s[o, iz] = s
+            out_A[o, iz] = -(1.0 / (zz - (eo[o] - mu) - s)).imag / PI
+    return out_s, out_A
+
+
+def fs_inter(ek, mu, sr: SelfResult, T):
+    """green::find_FS_inter (src/green.cpp:2210-2341): along each line
+    (l + m, m) of the quadrant, the m maximising A(k, w = 0 + i 1e-6) from a
+    3-point polynomial and from a 4-point Pade; rows (l + m*, m*, A*)."""
+    nbk = ek.shape[0]
+    z = 1e-6j
+    _, A_poly = pade_sigma(ek, mu, sr, T, [z], np.arange(3), 3, mode=1)
+    _, A_pade = pade_sigma(ek, mu, sr, T, [z], np.arange(4), 4, mode=0)
+    res_poly, res_pade = [], []
+    for l in range(nbk):
+        for A, res in ((A_poly, res_poly), (A_pade, res_pade)):
+            best, bm = 0.0, 0
+            for m in range(nbk - l):
+                x, y = l + m, m
+                a = A[y + x * (x + 1) // 2, 0]
+                if a > best:
+                    best, bm = a, m
+            res.append((l + bm, bm, best))
+    return np.array(res_poly), np.array(res_pade)
+
+
+def gwn_local(ek, mu, sr: SelfResult, T):
+    """green::Gwn_local (src/green.cpp:209-266)."""
+    nbk = ek.shape[0]
+    nk02 = 4 * (nbk - 1) ** 2
+    w = octant_weights(nbk, 8)
+    eo = to_octant(ek)
+    sig = sr.sigma(T)
+    z = 1j * (2 * np.arange(sig.shape[0])[:, None] + 1) * PI * T
+    return np.sum((w / nk02) / (z - eo + mu - sig), axis=1)

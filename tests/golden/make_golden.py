@@ -101,6 +101,23 @@ def run_case(name, spec, threads):
             out["kx0"] = np.array(float(meta["kx0"]))
             out["chijj1"] = rd("chijj1.bin")
             out["chijj2"] = rd("chijj2.bin")
+            # text outputs of find_FS_inter, MDC (10 points, w = 0, 4 etas) and
+            # Gwn_local as the reference writes them (src/green.cpp:2227-2330,
+            # 1020-1060, 226-263); the probe runs them as tpsc_main.cpp does
+            work = os.path.join(d, "work")
+
+            def table(prefix, exclude=None):
+                f = [x for x in os.listdir(work)
+                     if x.startswith(prefix) and not (exclude and x.startswith(exclude))]
+                return np.loadtxt(os.path.join(work, f[0]), ndmin=2)
+
+            out["mdc_A"] = table("Akw_Pade_k_")[:, 2:]
+            sp = table("Self_Pade_k_")[:, 2:]
+            out["mdc_sigma"] = sp[:, 0::2] + 1j * sp[:, 1::2]
+            g = table("Gwn_loc_")
+            out["gwn_local"] = g[:, 1] + 1j * g[:, 2]
+            out["fs_inter"] = table("FS_inter_AkF_", exclude="FS_inter_AkF_Pade_")
+            out["fs_inter_pade"] = table("FS_inter_AkF_Pade_")
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
         print(name, "done", {k: meta.get(k) for k in ("Usp", "Uch", "mu")})
 

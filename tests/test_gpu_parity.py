@@ -127,6 +127,37 @@ def test_l256_scalars_match_reference(ctx):
     assert rel(se["S"][:, cols], g["self_cols"]) < 1e-7
 
 
+@pytest.mark.parametrize("name", ["l32_w512_u2", "l16_w128_n110", "l16_w64_half"])
+def test_continuation_matches_reference(ctx, name):
+    """Pade / polynomial continuation (green::MDC, find_FS_inter) and
+    Gwn_local against the reference's own text output."""
+    g = load_golden(name)
+    p = g["p"]
+    gr = make(ctx, p)
+    gr.solve()
+    etas = np.array([0.01, 0.001, 0.0001, 0.00001])
+    s, A = gr.pade_sigma(1j * etas, np.arange(10), 10, mode=0)
+    assert np.allclose(A, g["mdc_A"], rtol=1e-6, atol=1e-11)
+    assert np.allclose(s, g["mdc_sigma"], rtol=1e-6, atol=1e-11)
+    assert np.allclose(gr.Gwn_local(), g["gwn_local"], rtol=1e-8, atol=1e-11)
+    nbk = p["nk0"] // 2 + 1
+    for Nn, mode, key in ((3, 1, "fs_inter"), (4, 0, "fs_inter_pade")):
+        _, a = gr.pade_sigma([1e-6j], np.arange(Nn), Nn, mode=mode)
+        rows = []
+        for l in range(nbk):
+            best, bm = 0.0, 0
+            for m in range(nbk - l):
+                x, y = l + m, m
+                if a[y + x * (x + 1) // 2, 0] > best:
+                    best, bm = a[y + x * (x + 1) // 2, 0], m
+            rows.append((l + bm, bm, best))
+        rows = np.array(rows)
+        assert np.allclose(rows[:, 2], g[key][:, 2], rtol=1e-6)
+        for r_, ref in zip(rows, g[key]):
+            if r_[1] != ref[1]:
+                assert abs(r_[2] - ref[2]) <= 1e-6 * abs(ref[2])
+
+
 @pytest.mark.parametrize("name", ["l64_w1024_u4", "l32_w256_u4_tp"])
 def test_repeated_solves_are_bit_identical(ctx, name):
     """State left by one solve (including the padding columns of the column

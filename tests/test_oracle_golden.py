@@ -82,3 +82,35 @@ def test_find_zero_quadratic():
     assert abs(root - np.sqrt(2.0)) < 1e-15
     root, nev = O.find_zero(lambda x: x - 0.3, (0.0, -10.0, 10.0), lims=(-20, 20))
     assert abs(root - 0.3) < 1e-15
+
+
+CONT = [n for n in SMALL if "mdc_A" in load_golden(n)]
+
+
+def check_fs(mine, ref):
+    """Rows (l + m*, m*, A*) of find_FS_inter.  The maxima must agree; the
+    arg-max may differ only where the line has two equal maxima (symmetric
+    points about a particle-hole symmetric Fermi surface), where rounding
+    decides."""
+    assert np.allclose(mine[:, 2], ref[:, 2], rtol=1e-6)
+    for a, b in zip(mine, ref):
+        if a[1] != b[1]:
+            assert abs(a[2] - b[2]) <= 1e-6 * abs(b[2])
+
+
+@pytest.mark.parametrize("name", CONT)
+def test_oracle_continuation_matches_reference(name):
+    """MDC (10-point Pade at w = 0, 4 etas), find_FS_inter and Gwn_local against
+    the reference's own text output (written with 8-12 significant digits)."""
+    g = load_golden(name)
+    p = g["p"]
+    r = O.solve(p["U"], p["tp"], p["tpp"], p["t3"], p["n"], p["T"], p["nk0"], p["Nw0"])
+    ek = O.dispersion(p["nk0"] // 2 + 1, p["tp"], p["tpp"], p["t3"])
+    etas = np.array([0.01, 0.001, 0.0001, 0.00001])
+    s, A = O.pade_sigma(ek, r.mu, r.sigma, p["T"], 1j * etas, np.arange(10), 10, mode=0)
+    assert np.allclose(A, g["mdc_A"], rtol=1e-6, atol=1e-11)
+    assert np.allclose(s, g["mdc_sigma"], rtol=1e-6, atol=1e-11)
+    poly, pade = O.fs_inter(ek, r.mu, r.sigma, p["T"])
+    check_fs(poly, g["fs_inter"])
+    check_fs(pade, g["fs_inter_pade"])
+    assert np.allclose(O.gwn_local(ek, r.mu, r.sigma, p["T"]), g["gwn_local"], rtol=1e-8, atol=1e-11)

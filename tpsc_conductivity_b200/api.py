@@ -168,6 +168,26 @@ class Green:
         return (sc["Sigma_inf"] / z + r["Sigma_inf2"] / z ** 2 + r["Sigma_inf3"] / z ** 3
                 + r["S"] / z ** 4)
 
+    def pade_sigma(self, z, n_idx=None, Nn=10, mode=0):
+        """Sigma(k, z) and A(k, z) at complex energies z for every octant k, from
+        Nn Matsubara samples (mode 0 Pade, 1 Lagrange polynomial), as
+        green::MDC / find_FS_inter do (src/green.cpp:814-1068, 2210-2341)."""
+        nk0, nw0, nbk, n8 = self.dims()
+        z = np.ascontiguousarray(np.atleast_1d(np.asarray(z, dtype=np.complex128)))
+        idx = np.ascontiguousarray(np.arange(Nn) if n_idx is None else np.asarray(n_idx), dtype=np.int32)
+        sig = np.zeros((n8, z.size), dtype=np.complex128)
+        A = np.zeros((n8, z.size))
+        self.ctx.call("tpsc_pade_sigma", idx.ctypes.data_as(C.POINTER(C.c_int)), int(idx.size),
+                      _dptr(z.view(np.float64)), int(z.size), int(mode), _dptr(sig.view(np.float64)), _dptr(A))
+        return sig, A
+
+    def Gwn_local(self):
+        """green::Gwn_local (src/green.cpp:209): local G(i w_n), n < Nw0/2."""
+        nk0, nw0, nbk, n8 = self.dims()
+        out = np.zeros(nw0 // 2, dtype=np.complex128)
+        self.ctx.call("tpsc_gwn_local", _dptr(out.view(np.float64)))
+        return out
+
     def stage_times(self):
         out = np.zeros(5)
         self.ctx.call("tpsc_stage_times", _dptr(out), 5)

@@ -960,6 +960,48 @@ int tpsc_get_self(tpsc_ctx *ctx, double *self_kw, double *s2, double *s3, double
     return TPSC_OK;
 }
 
+int tpsc_pade_sigma(tpsc_ctx *ctx, const int *n_idx, int Nn, const double *z, int Nz, int mode, double *out_sigma,
+                    double *out_A) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    Grid *g = ctx->cur;
+    if (!g->have_S || ctx->scal[TPSC_S_EVALS_MU] == 0)
+        return fail(ctx, TPSC_ERR_STATE, "the self-energy and mu must be computed first");
+    if (!n_idx || !z || !out_A || Nn < 2 || Nn > 32 || Nn > g->d.nw0 / 2 || Nz < 1 || (mode != 0 && mode != 1))
+        return fail(ctx, TPSC_ERR_ARG, "need 2 <= Nn <= min(32, Nw0/2), Nz >= 1, mode 0 (Pade) or 1 (polynomial)");
+    const size_t n8 = g->d.n8;
+    const size_t bytes = Nn * sizeof(int) + 16 + Nz * sizeof(double2) + n8 * Nz * (sizeof(double2) + sizeof(double));
+    if ((rc = ensure_stage(ctx, bytes))) return rc;
+    char *base = (char *)ctx->stage;
+    double2 *dz = (double2 *)base;
+    double2 *dsig = dz + Nz;
+    double *dA = (double *)(dsig + n8 * Nz);
+    int *didx = (int *)(dA + n8 * Nz);
+    CK(cudaMemcpyAsync(didx, n_idx, Nn * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(dz, z, Nz * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+    CK(launch_pade_sigma(g->d, g->S, g->s2, g->s3, g->sinf, didx, Nn, dz, Nz, mode, ctx->scal[TPSC_S_MU], ctx->T,
+                         dsig, dA, ctx->st));
+    if (out_sigma) CK(cudaMemcpyAsync(out_sigma, dsig, n8 * Nz * sizeof(double2), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(out_A, dA, n8 * Nz * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return TPSC_OK;
+}
+
+int tpsc_gwn_local(tpsc_ctx *ctx, double *out) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    Grid *g = ctx->cur;
+    if (!g->have_S || ctx->scal[TPSC_S_EVALS_MU] == 0)
+        return fail(ctx, TPSC_ERR_STATE, "the self-energy and mu must be computed first");
+    const size_t bytes = (size_t)(g->d.nw0 / 2) * sizeof(double2);
+    if ((rc = ensure_stage(ctx, bytes))) return rc;
+    CK(launch_gwn_local(g->d, g->S, g->s2, g->s3, g->sinf, ctx->scal[TPSC_S_MU], ctx->T, (double2 *)ctx->stage,
+                        ctx->st));
+    CK(cudaMemcpyAsync(out, ctx->stage, bytes, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return TPSC_OK;
+}
+
 int tpsc_stage_times(tpsc_ctx *ctx, double *ms, int n) {
     if (!ctx || !ms) return fail(ctx, TPSC_ERR_ARG, "bad arguments");
     for (int i = 0; i < n && i < 5; ++i) ms[i] = ctx->stage_ms[i];

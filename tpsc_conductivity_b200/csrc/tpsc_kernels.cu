@@ -1099,6 +1099,129 @@ __global__ void k_chi0max(const double *__restrict__ chiq, const uint32_t *__res
     }
 }
 
+// ---------------------------------------------------------------------------
+// real-frequency continuation on Matsubara samples of Sigma (row a12)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+    // Smith's algorithm
+    if (fabs(b.x) >= fabs(b.y)) {
+        const double r = b.y / b.x, d = b.x + b.y * r;
+        return make_double2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+    } else {
+        const double r = b.x / b.y, d = b.y + b.x * r;
+        return make_double2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+    }
+}
+
+constexpr int kPadeMax = 32;
+
+// Per octant k: Sigma(k, z_j) at z_j = i (2 n_j + 1) pi T with the stored
+// frequency j (green::MDC and find_FS_inter read Self_kw_array at j while
+// z_j uses n[j], src/green.cpp:992, 2276), then either
+//  mode 0: Vidberg-Serene continued-fraction Pade (pade_cont_frac_coef_rec
+//          and pade, src/generique.cpp:1605-1663) at the Nz energies z;
+//  mode 1: Lagrange polynomial through the Nn samples (src/green.cpp:2297-2299).
+// out_sig [N8][Nz] (complex, may be null), out_A [N8][Nz] with
+// A = -Im 1/(z - (eps_k - mu) - Sigma)/pi.
+__global__ void k_pade_sigma(const double2 *__restrict__ S, const double *__restrict__ s2,
+                             const double *__restrict__ s3, const double *__restrict__ sinfp,
+                             const double *__restrict__ ek, const int *__restrict__ nidx, int Nn,
+                             const double2 *__restrict__ z, int Nz, int mode, int n8, int nw0, double mu, double T,
+                             double2 *__restrict__ out_sig, double *__restrict__ out_A) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n8) return;
+    const int NO = nw0 / 2;
+    const double sinf = sinfp[0];
+    double2 f[kPadeMax], x0[kPadeMax], coef[kPadeMax];
+    for (int j = 0; j < Nn; ++j) {
+        x0[j] = make_double2(0.0, (2 * nidx[j] + 1) * 3.141592653589793 * T);
+        const double wn = (2 * j + 1) * 3.141592653589793 * T;
+        const double i1 = 1.0 / wn, i2 = i1 * i1, i4 = i2 * i2;
+        const double2 Sv = S[bidx(j, o, NO)];
+        // Sigma(k, i w_j) = Sinf/z + C2/z^2 + C3/z^3 + S/z^4 at z = i w_j
+        f[j] = make_double2(-s2[o] * i2 + Sv.x * i4, -sinf * i1 + s3[o] * i2 * i1 + Sv.y * i4);
+    }
+    if (mode == 0) {
+        // continued-fraction coefficients: g_0(l) = f_l,
+        // g_m(l) = (g_{m-1}(m-1) - g_{m-1}(l)) / ((x_l - x_{m-1}) g_{m-1}(l)), coef_m = g_m(m)
+        double2 g[kPadeMax];
+        for (int l = 0; l < Nn; ++l) g[l] = f[l];
+        coef[0] = g[0];
+        for (int m = 1; m < Nn; ++m) {
+            const double2 gm = g[m - 1];
+            for (int l = m; l < Nn; ++l) {
+                const double2 dx = make_double2(x0[l].x - x0[m - 1].x, x0[l].y - x0[m - 1].y);
+                g[l] = cdiv(csub(gm, g[l]), cmul(dx, g[l]));
+            }
+            coef[m] = g[m];
+        }
+    }
+    const double e = ek[o] - mu;
+    for (int iz = 0; iz < Nz; ++iz) {
+        const double2 zz = z[iz];
+        double2 sig;
+        if (mode == 0) {
+            double2 A = make_double2(1.0, 0.0);
+            double2 B = cadd(make_double2(1.0, 0.0), cmul(csub(zz, x0[0]), coef[1]));
+            double2 q = cdiv(A, B);
+            for (int j = 3; j <= Nn; ++j) {
+                const double2 t = cmul(csub(zz, x0[j - 2]), coef[j - 1]);
+                A = cadd(make_double2(1.0, 0.0), cdiv(t, A));
+                B = cadd(make_double2(1.0, 0.0), cdiv(t, B));
+                q = cdiv(cmul(q, A), B);
+            }
+            sig = cmul(q, coef[0]);
+        } else {
+            sig = make_double2(0.0, 0.0);
+            for (int j = 0; j < Nn; ++j) {
+                double2 term = f[j];
+                for (int i = 0; i < Nn; ++i)
+                    if (i != j) term = cmul(term, cdiv(csub(zz, x0[i]), csub(x0[j], x0[i])));
+                sig = cadd(sig, term);
+            }
+        }
+        const double2 d = make_double2(zz.x - e - sig.x, zz.y - sig.y);
+        const double2 gz = cdiv(make_double2(1.0, 0.0), d);
+        if (out_sig) out_sig[(size_t)o * Nz + iz] = sig;
+        out_A[(size_t)o * Nz + iz] = -gz.y / 3.141592653589793;
+    }
+}
+
+// green::Gwn_local (src/green.cpp:209-266): G_loc(i w_j) = sum_k w/L^2
+// 1/(z - eps_k + mu - Sigma(k, z)), w = 8 halved on edges and diagonal.
+// One block per frequency j.
+__global__ void k_gwn_local(const double2 *__restrict__ S, const double *__restrict__ s2,
+                            const double *__restrict__ s3, const double *__restrict__ sinfp,
+                            const double *__restrict__ ek, const double *__restrict__ w16, int n8, int nw0, double mu,
+                            double T, double nk02, double2 *__restrict__ out) {
+    const int j = blockIdx.x, NO = nw0 / 2;
+    const double sinf = sinfp[0];
+    const double wn = (2 * j + 1) * 3.141592653589793 * T;
+    const double i1 = 1.0 / wn, i2 = i1 * i1, i4 = i2 * i2;
+    double re = 0.0, im = 0.0;
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        const double2 Sv = S[bidx(j, o, NO)];
+        const double rS = -s2[o] * i2 + Sv.x * i4;
+        const double iS = -sinf * i1 + s3[o] * i2 * i1 + Sv.y * i4;
+        const double2 g = cdiv(make_double2(0.5 * w16[o] / nk02, 0.0),
+                               make_double2(-ek[o] + mu - rS, wn - iS));
+        re += g.x;
+        im += g.y;
+    }
+    __shared__ double sr[1024], si[1024];
+    sr[threadIdx.x] = re;
+    si[threadIdx.x] = im;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int i = 0; i < (int)blockDim.x; ++i) {
+            a += sr[i];
+            b += si[i];
+        }
+        out[j] = make_double2(a, b);
+    }
+}
+
 // blocked -> [j][o]
 __global__ void k_unblock(const double *__restrict__ src, double *__restrict__ dst, int NJ, int nrows, int n8) {
     const long long total = (long long)nrows * n8;
@@ -1354,6 +1477,22 @@ cudaError_t launch_trace_self_G2(const GridDev &g, const double2 *S, const doubl
                                  const double *sinf, double mu, double T, Reduce r, cudaStream_t st) {
     const double nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
     k_trace_self_G2<<<g.n8p / 4, kRedThreads, 0, st>>>(S, s2, s3, sinf, g.ek, g.w16, g.nw0, mu, T, nk02, r);
+    return launched();
+}
+
+cudaError_t launch_pade_sigma(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                              const double *sinf, const int *nidx, int Nn, const double2 *z, int Nz, int mode,
+                              double mu, double T, double2 *out_sig, double *out_A, cudaStream_t st) {
+    if (Nn < 2 || Nn > kPadeMax || Nn > g.nw0 / 2) return cudaErrorInvalidValue;
+    k_pade_sigma<<<(g.n8 + 127) / 128, 128, 0, st>>>(S, s2, s3, sinf, g.ek, nidx, Nn, z, Nz, mode, g.n8, g.nw0, mu, T,
+                                                      out_sig, out_A);
+    return launched();
+}
+
+cudaError_t launch_gwn_local(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                             const double *sinf, double mu, double T, double2 *out, cudaStream_t st) {
+    const double nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
+    k_gwn_local<<<g.nw0 / 2, 256, 0, st>>>(S, s2, s3, sinf, g.ek, g.w16, g.n8, g.nw0, mu, T, nk02, out);
     return launched();
 }
 

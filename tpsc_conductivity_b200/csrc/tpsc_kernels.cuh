@@ -78,6 +78,13 @@ cudaError_t launch_trace_self_G(const GridDev &g, const double2 *S, const double
 cudaError_t launch_trace_self_G2(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                                  const double *sinf, double mu, double T, Reduce r, cudaStream_t st);
 
+// ---- real-frequency continuation (Pade / Lagrange) and local G ---------------
+cudaError_t launch_pade_sigma(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                              const double *sinf, const int *nidx, int Nn, const double2 *z, int Nz, int mode,
+                              double mu, double T, double2 *out_sig, double *out_A, cudaStream_t st);
+cudaError_t launch_gwn_local(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                             const double *sinf, double mu, double T, double2 *out, cudaStream_t st);
+
 // ---- layout conversion for the getters ------------------------------------
 // blocked (NJ rows) -> reference layout [j][o], j < nrows
 cudaError_t launch_unblock(const double *src, double *dst, int NJ, int nrows, int n8, cudaStream_t st);

@@ -1,0 +1,460 @@
+// tpsc_dropin.cpp -- the drop-in classes of tpsc_dropin.h over the C ABI.
+//
+// Result files keep the reference's names (sprintf formats) and column
+// layouts so that tools reading the reference's output read these too:
+// TPSC_infos_* / TPSCparams_* (src/chi.cpp:375-415), the traces
+// (src/green.cpp:3091-3102, 2982-2995), mu0_mu_D_* (src/green.cpp:3272-3279),
+// FS_inter_* (src/green.cpp:2227-2330), Akw/Self_Pade_k_* and *_poly_k_*
+// (src/green.cpp:838-1060), Gwn_loc_* (src/green.cpp:225-263) and the chi0
+// dumps (src/chi0.cpp:720-742).
+#include "tpsc_dropin.h"
+
+#include <vector>
+
+namespace {
+
+int device_from_env() {
+    const char *d = getenv("TPSC_DEVICE");
+    return d ? atoi(d) : 0;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+hamiltonien::hamiltonien(int nk0, double n, double T, double params[]) {
+    nbk = nk0 / 2 + 1;
+    density = n;
+    tem = T;
+    if (params) {
+        tp = params[0];
+        tpp = params[1];
+        t3 = params[2];
+        U = params[3];
+    } else {
+        tp = tpp = t3 = 0;
+        U = 1;
+    }
+}
+
+void hamiltonien::get_params() const {
+    cout << setiosflags(ios::left) << "U: " << setw(10) << U << "tp: " << setw(10) << tp << "tpp: " << setw(10)
+         << tpp << "t3: " << setw(10) << t3 << "density: " << setw(10) << density << "T: " << tem << endl;
+}
+
+// ---------------------------------------------------------------------------
+green0::green0(int nk0, int Nw0, double n, double T, double params[]) : hamiltonien(nk0, n, T, params) {
+    nbw = Nw0;
+    nwmax = (nbw - 2) / 2;
+    mu0 = 0.0;
+    for (double &s : scal_) s = 0.0;
+    int st = 0;
+    ctx_ = tpsc_create(device_from_env(), &st);
+    if (!ctx_) {
+        cout << "tpsc: no CUDA context (" << tpsc_last_error(NULL) << ")" << endl;
+        return;
+    }
+    if (check(tpsc_set_model(ctx_, nk0, Nw0, n, T, tp, tpp, t3, U), "tpsc_set_model")) {
+        refresh();
+        mu0 = scal_[TPSC_S_MU0];
+        cout << "mu0 du systeme fini: " << mu0 << endl;
+    }
+}
+
+green0::~green0() {
+    if (ctx_) tpsc_destroy(ctx_);
+}
+
+bool green0::check(int status, const char *what) const {
+    if (status == TPSC_OK) return true;
+    cout << what << ": " << tpsc_last_error(ctx_) << " (status " << status << ")" << endl;
+    return false;
+}
+
+void green0::refresh() {
+    if (ctx_) tpsc_get_scalars(ctx_, scal_, TPSC_S_COUNT);
+}
+
+void green0::get_params() const {
+    hamiltonien::get_params();
+    cout << "mu0: " << mu0 << '\n';
+}
+
+// ---------------------------------------------------------------------------
+chi0::chi0(int nk0, int Nw0, double n, double T, double params[]) : green0(nk0, Nw0, n, T, params) {
+    nbq = nk0 / 2 + 1;
+    nwmax = Nw0 / 2;
+    keep_chirt = keep_chiqw = save_chi0_q = save_chi0_to_file = true;
+    chi0max = 0.0;
+    qmax[0] = qmax[1] = 0;
+}
+
+void chi0::calc_chiqw_FFT_spline(int nq0, int nw0) {
+    cout << "calcul de chi0 par calc_chiqw_FFT_spline()\n";
+    if (!ctx_ || !check(tpsc_chi0(ctx_, nq0, nw0), "calc_chiqw_FFT_spline")) return;
+    nbq = nbk = nq0 / 2 + 1;
+    nbw = nw0;
+    nwmax = nw0 / 2;
+    refresh();
+    mu0 = scal_[TPSC_S_MU0];
+    chi0max = scal_[TPSC_S_CHI0MAX];
+    qmax[0] = (int)scal_[TPSC_S_QMAX0];
+    qmax[1] = (int)scal_[TPSC_S_QMAX1];
+    cout << "qxmax, qymax: " << qmax[0] << ",  " << qmax[1] << '\n';
+    if (save_chi0_q) {
+        const int nw = nwmax + 1, n8 = nbq * (nbq + 1) / 2;
+        std::vector<double> c((size_t)nw * n8);
+        if (check(tpsc_get_chi0(ctx_, c.data(), NULL, NULL, NULL), "tpsc_get_chi0")) {
+            char name[300];
+            fstream file;
+            int l = qmax[0], m = qmax[1];
+            sprintf(name, "./chi0_qmax_wn_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%d_%d_%d_%d.dat", tp, tpp, t3, density, tem,
+                    nq0, nw0, l, m);
+            file.open(name, ios::out);
+            file << setiosflags(ios::left) << setprecision(16);
+            for (int j = 0; j < nw; j++) file << setw(10) << j << c[m + (l * (l + 1)) / 2 + (size_t)j * n8] << '\n';
+            file.close();
+            sprintf(name, "./chi0_wn0_q_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%d_%d.dat", tp, tpp, t3, density, tem, nq0,
+                    nw0);
+            file.open(name, ios::out);
+            file << setiosflags(ios::left) << setprecision(16);
+            for (l = 0; l < nbq; l++)
+                for (m = 0; m <= l; m++) file << setw(10) << l << setw(10) << m << c[m + (l * (l + 1)) / 2] << '\n';
+            file.close();
+        }
+    }
+    traceChi0();
+}
+
+void chi0::traceChi0() {
+    double tr[2];
+    if (!ctx_ || !check(tpsc_trace_chi0(ctx_, tr), "traceChi0")) return;
+    const double ex = density - density * density / 2.0;
+    cout << setprecision(14);
+    cout << "trace(chi0(q,iwn)):   " << tr[0] << "\tn-n^2/2:   " << ex << "\tdifference relative:  "
+         << (ex - tr[0]) / ex << '\n';
+    cout << "trace(chi0(q,iwn))(+correction asymptotique):   " << tr[1] << "\tn-n^2/2:   " << ex
+         << "\tdifference relative:  " << (ex - tr[1]) / ex << '\n';
+}
+
+// ---------------------------------------------------------------------------
+chi::chi(int nk0, int Nw0, double n, double T, double *params) : chi0(nk0, Nw0, n, T, params) {
+    nsr = n > 1.0 ? 2.0 - n : n;
+    Usp = Uch = dblOcc = 0.0;
+    paramsFileName[0] = 0;
+}
+
+void chi::get_params() const { green0::get_params(); }
+
+void chi::find_Usp_Uch(int nq0, int nw0, double Usc[]) {
+    double u[2];
+    if (!ctx_ || !check(tpsc_find_Usp_Uch_grid(ctx_, nq0, nw0, u), "find_Usp_Uch")) return;
+    nbq = nbk = nq0 / 2 + 1;
+    nbw = nw0;
+    nwmax = nw0 / 2;
+    refresh();
+    mu0 = scal_[TPSC_S_MU0];
+    chi0max = scal_[TPSC_S_CHI0MAX];
+    qmax[0] = (int)scal_[TPSC_S_QMAX0];
+    qmax[1] = (int)scal_[TPSC_S_QMAX1];
+    Usc[0] = Usp = u[0];
+    Usc[1] = u[1];
+    cout << "Usp: " << Usc[0] << '\n' << "Uch: " << Usc[1] << '\n';
+}
+
+void chi::find_Usp_Uch() {
+    cout << "calcul de Usp et Uch\n";
+    if (!ctx_ || !check(tpsc_find_Usp_Uch(ctx_), "find_Usp_Uch")) return;
+    refresh();
+    nbq = nbk;
+    nwmax = nbw / 2;
+    mu0 = scal_[TPSC_S_MU0];
+    chi0max = scal_[TPSC_S_CHI0MAX];
+    qmax[0] = (int)scal_[TPSC_S_QMAX0];
+    qmax[1] = (int)scal_[TPSC_S_QMAX1];
+    Usp = scal_[TPSC_S_USP];
+    Uch = scal_[TPSC_S_UCH];
+    dblOcc = scal_[TPSC_S_DBLOCC];
+    const double difRelsp = scal_[TPSC_S_DIFRELSP], difRelch = scal_[TPSC_S_DIFRELCH];
+    cout << "iteration q: 1  difRelsp: " << difRelsp << "  difRelch: " << difRelch << '\n';
+    if (save_chi0_to_file) {
+        // the full-grid chi0 dumps calc_chiqw_FFT_spline writes on the second grid
+        const bool keep = save_chi0_q;
+        save_chi0_q = true;
+        const int nq0 = 2 * (nbq - 1), nw0 = 2 * nwmax;
+        const int nw = nwmax + 1, n8 = nbq * (nbq + 1) / 2;
+        std::vector<double> c((size_t)nw * n8);
+        if (check(tpsc_get_chi0(ctx_, c.data(), NULL, NULL, NULL), "tpsc_get_chi0")) {
+            char name[300];
+            fstream file;
+            int l = qmax[0], m = qmax[1];
+            sprintf(name, "./chi0_qmax_wn_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%d_%d_%d_%d.dat", tp, tpp, t3, density, tem,
+                    nq0, nw0, l, m);
+            file.open(name, ios::out);
+            file << setiosflags(ios::left) << setprecision(16);
+            for (int j = 0; j < nw; j++) file << setw(10) << j << c[m + (l * (l + 1)) / 2 + (size_t)j * n8] << '\n';
+            file.close();
+            sprintf(name, "./chi0_wn0_q_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%d_%d.dat", tp, tpp, t3, density, tem, nq0,
+                    nw0);
+            file.open(name, ios::out);
+            file << setiosflags(ios::left) << setprecision(16);
+            for (l = 0; l < nbq; l++)
+                for (m = 0; m <= l; m++) file << setw(10) << l << setw(10) << m << c[m + (l * (l + 1)) / 2] << '\n';
+            file.close();
+        }
+        save_chi0_q = keep;
+    }
+    const double chispmax = chi0max / (1.0 - Usp * chi0max / 2.0);
+    char name[300];
+    sprintf(name, "./TPSC_infos_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%d_%d.dat", U, tp, tpp, t3, density, tem,
+            2 * (nbq - 1), 2 * nwmax);
+    fstream infos;
+    infos << setprecision(16);
+    infos.open(name, ios::out);
+    infos << "Usp:  " << Usp << "   difRelsp:  " << difRelsp << '\n';
+    infos << "Uch:  " << Uch << "   difRelch:  " << difRelch << '\n';
+    infos << "chi0max: " << chi0max << "   chispmax: " << chispmax << "   rapport: " << chispmax / chi0max << '\n';
+    infos << "double occupation (ansatz): " << dblOcc << '\n';
+    infos << "qxmax, qymax:   " << qmax[0] << ",  " << qmax[1] << '\n';
+    infos.close();
+    cout << "chi0max: " << chi0max << "  chispmax: " << chispmax << "  rapport: " << chispmax / chi0max << '\n';
+    cout << "double occupation: " << dblOcc << '\n';
+    sprintf(paramsFileName, "./TPSCparams_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%d_%d.dat", U, tp, tpp, t3, density,
+            tem, 2 * (nbq - 1), 2 * nwmax);
+    fstream params;
+    params.open(paramsFileName, ios::out);
+    if (!params) {
+        cout << "echec de creation du fichier de parametres\n";
+        return;
+    }
+    params << setprecision(16);
+    params << "Usp  " << Usp << "   difRelsp:  " << difRelsp << '\n';
+    params << "Uch  " << Uch << "   difRelch:  " << difRelch << '\n';
+    params << "nbq  " << nbq << '\n';
+    params << "nbw  " << nwmax + 1 << '\n';
+    params << "dblOcc_ansatz  " << dblOcc << '\n';
+    params << "qxmax  " << qmax[0] << '\n';
+    params << "qymax  " << qmax[1] << '\n';
+    params << "chispmax_over_chi0max  " << chispmax / chi0max << '\n';
+    params << "mu0  " << mu0 << '\n';
+    params.close();
+}
+
+void chi::sp_corr_length() {
+    // needs the infinite-lattice Fermi surface (green0::find_FS, adaptive
+    // quadrature), which this build does not reproduce
+    cout << "sp_corr_length(): not available in this build\n";
+}
+
+void chi::calc_chirt() {
+    cout << "calcul de vertex_rt_array\n";
+    if (!ctx_) return;
+    check(tpsc_vertex(ctx_), "calc_chirt");
+}
+
+// ---------------------------------------------------------------------------
+green::green(int nk0, int Nw0, double n, double T, double eta0, double *params) : chi(nk0, Nw0, n, T, params) {
+    eta = eta0;
+    mu = 0;
+    Sigma_inf = 0;
+    mu_calcule = have_self = false;
+}
+
+void green::get_params() const {
+    chi::get_params();
+    cout << "mu: " << mu << '\n';
+}
+
+void green::calc_Self_FFT_spline() {
+    find_Usp_Uch();
+    calc_chirt();
+    cout << "calcul de la self-energie par calc_Self_FFT_spline()\n";
+    if (!ctx_ || !check(tpsc_self_energy(ctx_), "calc_Self_FFT_spline")) return;
+    refresh();
+    Sigma_inf = scal_[TPSC_S_SIGMA_INF];
+    have_self = true;
+    cout << "self-energie calculee\n";
+}
+
+void green::traceSelfG() {
+    double tr[2];
+    if (!ctx_ || !check(tpsc_trace_self_G(ctx_, tr), "traceSelfG")) return;
+    const double ud = U * dblOcc - U * density * density / 4.0;
+    cout << "U*dblOcc-U*n^2/4:  " << ud << '\n';
+    cout << "trace Self*G: " << tr[0] << '\n';
+    cout << "trace Self*G (avec correction asymptotique): " << tr[1] << '\n';
+    char name[300];
+    sprintf(name, "./TPSC_infos_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat", U, tp, tpp, t3, density, tem,
+            2 * (nbk - 1), nbw);
+    fstream f;
+    f.open(name, ios::out | ios::app);
+    f << setprecision(16);
+    f << "U*dblOcc-U*n^2/4:   " << ud << '\n';
+    f << "trace Self*G:  " << tr[0] << '\n';
+    f.close();
+}
+
+void green::traceSelfG2() {
+    refresh();
+    const double sum = scal_[TPSC_S_TR_SG2];
+    cout << "trace Self*G2: " << sum << "  U*dblOcc-U*n^2/4:  " << U * dblOcc - U * density * density / 4.0 << '\n';
+    cout << "double occupation (Self*G2): " << (sum + U * density * density / 4.0) / U << '\n';
+    char name[300];
+    sprintf(name, "./TPSC_infos_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat", U, tp, tpp, t3, density, tem,
+            2 * (nbk - 1), nbw);
+    fstream f;
+    f.open(name, ios::out | ios::app);
+    f << setprecision(16);
+    f << "trace Self*G2:  " << sum << '\n';
+    f << "double occupation (Self*G2): " << (sum + U * density * density / 4.0) / U << '\n';
+    f << "mu0:  " << mu0 << '\n';
+    f << "mu:  " << mu << '\n';
+    f.close();
+}
+
+void green::find_mu() {
+    if (!ctx_) return;
+    if (check(tpsc_find_mu(ctx_), "find_mu")) {
+        refresh();
+        mu = scal_[TPSC_S_MU];
+        mu_calcule = true;
+        cout << "mu:  " << mu << '\n';
+    } else {
+        cout << "Attention! mu non calcule!\n";
+    }
+    char pname[300], mname[300];
+    sprintf(pname, "./TPSCparams_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat", U, tp, tpp, t3, density, tem,
+            2 * (nbk - 1), nbw);
+    sprintf(mname, "./mu0_mu_D_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat", U, tp, tpp, t3, density, tem,
+            2 * (nbk - 1), nbw);
+    fstream pf;
+    pf.open(pname, ios::out | ios::app);
+    if (pf) {
+        pf << setprecision(14);
+        pf << "mu  " << mu << '\n';
+        pf.close();
+    } else {
+        cout << "echec d'ouverture du fichier de parametres\n";
+    }
+    fstream mf;
+    mf.open(mname, ios::out);
+    if (mf) {
+        mf << setprecision(15) << setiosflags(ios::left);
+        mf << setw(25) << mu0 << setw(25) << mu << dblOcc << '\n';
+        mf.close();
+    }
+    if (mu_calcule) traceSelfG2();
+}
+
+void green::find_FS_inter() {
+    cout << "calcul des coordonnees de la surface de Fermi avec interaction\n";
+    if (!have_self) {
+        cout << "find_FS_inter(): self-energy non calculee\n";
+        return;
+    }
+    if (!mu_calcule) {
+        cout << "find_FS_inter(): mu n'a pas ete calcule\n";
+        return;
+    }
+    const int n8 = nbk * (nbk + 1) / 2;
+    const double z[2] = {0.0, 0.000001};
+    int idx[4] = {0, 1, 2, 3};
+    std::vector<double> Apoly(n8), Apade(n8);
+    if (!check(tpsc_pade_sigma(ctx_, idx, 3, z, 1, 1, NULL, Apoly.data()), "find_FS_inter")) return;
+    if (!check(tpsc_pade_sigma(ctx_, idx, 4, z, 1, 0, NULL, Apade.data()), "find_FS_inter")) return;
+    const char *forms[4] = {"./FS_inter_AkF_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat",
+                            "./FS_inter_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat",
+                            "./FS_inter_AkF_Pade_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat",
+                            "./FS_inter_Pade_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat"};
+    fstream f[4];
+    for (int i = 0; i < 4; ++i) {
+        char name[300];
+        sprintf(name, forms[i], U, tp, tpp, t3, density, tem, 2 * (nbk - 1), nbw);
+        f[i].open(name, ios::out);
+        f[i] << setiosflags(ios::left) << setprecision(8);
+    }
+    for (int l = 0; l < nbk; l++) {
+        double best[2] = {0, 0};
+        int bm[2] = {0, 0};
+        for (int m = 0; m < nbk - l; m++) {
+            const int x = l + m, y = m;
+            const double a[2] = {Apoly[y + (x * (x + 1)) / 2], Apade[y + (x * (x + 1)) / 2]};
+            for (int k = 0; k < 2; ++k)
+                if (a[k] > best[k]) {
+                    best[k] = a[k];
+                    bm[k] = m;
+                }
+        }
+        f[0] << setw(10) << l + bm[0] << setw(10) << bm[0] << best[0] << endl;
+        f[1] << setw(10) << l + bm[0] << setw(10) << bm[0] << endl;
+        f[2] << setw(10) << l + bm[1] << setw(10) << bm[1] << best[1] << endl;
+        f[3] << setw(10) << l + bm[1] << setw(10) << bm[1] << endl;
+    }
+    for (auto &x : f) x.close();
+}
+
+void green::MDC(int *n, int Nn, double w, double *eta_p, int Neta, bool use_Pade) {
+    if (!have_self) {
+        cout << "MDC(): la self-energie n'a pas ete calculee\n";
+        return;
+    }
+    if (Nn < 2) Nn = 2;
+    const int npts = use_Pade ? Nn : (Nn >= 4 ? 4 : 3);
+    const int n8 = nbk * (nbk + 1) / 2;
+    std::vector<double> z(2 * Neta), sig((size_t)2 * n8 * Neta), A((size_t)n8 * Neta);
+    for (int j = 0; j < Neta; ++j) {
+        z[2 * j] = w;
+        z[2 * j + 1] = eta_p[j];
+    }
+    if (!check(tpsc_pade_sigma(ctx_, n, npts, z.data(), Neta, use_Pade ? 0 : 1, sig.data(), A.data()), "MDC"))
+        return;
+    char name[300];
+    fstream af, sf;
+    sprintf(name,
+            use_Pade ? "Akw_Pade_k_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%5.3e_%1d_%1d.dat"
+                     : "Akw_poly_k_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%5.3e_%1d_%1d.dat",
+            U, tp, tpp, t3, density, tem, w, 2 * (nbk - 1), nbw);
+    af.open(name, ios::out);
+    af << setprecision(12) << setiosflags(ios::left);
+    sprintf(name,
+            use_Pade ? "Self_Pade_k_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%5.3e_%1d_%1d.dat"
+                     : "Self_poly_k_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%5.3e_%1d_%1d.dat",
+            U, tp, tpp, t3, density, tem, w, 2 * (nbk - 1), nbw);
+    sf.open(name, ios::out);
+    sf << setprecision(12) << setiosflags(ios::left);
+    for (int l = 0; l < nbk; l++)
+        for (int m = 0; m <= l; m++) {
+            const size_t o = m + (l * (l + 1)) / 2;
+            sf << setw(10) << l << setw(20) << m << setw(20) << sig[2 * (o * Neta)] << setw(25)
+               << sig[2 * (o * Neta) + 1];
+            af << setw(10) << l << setw(20) << m << setw(20) << A[o * Neta];
+            for (int j = 1; j < Neta; j++) {
+                sf << setw(20) << sig[2 * (o * Neta + j)] << setw(25) << sig[2 * (o * Neta + j) + 1];
+                af << setw(20) << A[o * Neta + j];
+            }
+            sf << endl;
+            af << endl;
+        }
+    sf.close();
+    af.close();
+}
+
+void green::Gwn_local() {
+    if (!mu_calcule || !have_self) {
+        cout << "G_local(): mu non calcule ou Self_kw_array inexistant\n";
+        return;
+    }
+    std::vector<double> g(nbw);
+    if (!check(tpsc_gwn_local(ctx_, g.data()), "Gwn_local")) return;
+    char name[300];
+    sprintf(name, "./Gwn_loc_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%d_%d.dat", U, tp, tpp, t3, density, tem,
+            2 * (nbk - 1), nbw);
+    fstream file;
+    file.open(name, ios::out);
+    file << setprecision(10) << setiosflags(ios::left);
+    for (int j = 0; j < nbw / 2; j++) file << setw(10) << j << setw(25) << g[2 * j] << g[2 * j + 1] << endl;
+    file.close();
+}
+
+// ---------------------------------------------------------------------------
+cond_opt::cond_opt(int nk0, int Nw0, double n, double T, double eta0, double *params)
+    : green(nk0, Nw0, n, T, eta0, params) {}

@@ -1,0 +1,132 @@
+// tpsc_dropin.h -- C++ drop-in for the reference's TPSC class chain.
+//
+// The reference (dbergeron1/TPSC_conductivity) exposes its computation as the
+// classes generique -> hamiltonien -> green0 -> chi0 -> chi -> green ->
+// cond_opt.  These classes keep those names, that inheritance order and the
+// public member functions a driver calls (src/tpsc_main.cpp and the
+// commented-out blocks there), with the same argument meaning, so the
+// reference's tpsc_main.cpp compiles unchanged against this directory.  Every
+// computation goes through the C ABI of include/tpsc_b200.h on a CUDA device;
+// the result files keep the reference's names and column layouts.
+//
+// Error behaviour follows the reference: failures print a message and the
+// member function returns (the reference prints French messages and returns).
+#ifndef TPSC_B200_DROPIN_H
+#define TPSC_B200_DROPIN_H
+
+#include <sys/stat.h>
+
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <limits>
+#include <string>
+
+#include "../../include/tpsc_b200.h"
+
+using namespace std;
+
+typedef complex<double> dcomplex;
+
+// numerical routines base class (root search, spline, Pade live in the engine)
+class generique {
+public:
+    generique() {}
+};
+
+// lattice and model parameters (src/hamiltonien.h:24-57)
+class hamiltonien : public generique {
+public:
+    hamiltonien(int nk0 = 8, double n = 1.0, double T = 1.0, double params[] = NULL);
+    void set_U(double Up) { U = Up; }
+    void set_tem(double T) { tem = T; }
+    void set_density(double n) { density = n; }
+    void get_params() const;
+
+protected:
+    double density, U, tp, tpp, t3, tem;
+    int nbk;
+};
+
+// non-interacting Green's function; owns the device context (src/green0.h)
+class green0 : public hamiltonien {
+public:
+    green0(int nk0 = 8, int Nw0 = 32, double n = 0.0, double T = 1.0, double params[] = NULL);
+    virtual ~green0();
+    void get_params() const;
+    double get_mu() const { return mu0; }
+
+protected:
+    bool check(int status, const char *what) const;
+    tpsc_ctx *ctx_;
+    double mu0;
+    int nbw, nwmax;
+    double scal_[TPSC_S_COUNT];
+    void refresh();
+};
+
+// Lindhard function (src/chi0.h)
+class chi0 : public green0 {
+public:
+    chi0(int nk0 = 8, int Nw0 = 32, double n = 1.0, double T = 1.0, double params[] = NULL);
+    void set_keep_chirt(bool v) { keep_chirt = v; }
+    void set_keep_chiqw(bool v) { keep_chiqw = v; }
+    void set_save_chi0_q(bool v) { save_chi0_q = v; }
+    void set_save_chi0_to_file(bool v) { save_chi0_to_file = v; }
+    void calc_chiqw_FFT_spline(int nq0, int nw0);
+    void traceChi0();
+
+protected:
+    bool keep_chirt, keep_chiqw, save_chi0_q, save_chi0_to_file;
+    double chi0max;
+    int qmax[2];
+    int nbq;
+};
+
+// spin and charge response, Usp and Uch (src/chi.h)
+class chi : public chi0 {
+public:
+    chi(int nk0 = 8, int Nw0 = 32, double n = 0.0, double T = 1.0, double *params = NULL);
+    void get_params() const;
+    void find_Usp_Uch();
+    void find_Usp_Uch(int nq0, int nw0, double Usc[]);
+    void sp_corr_length();
+
+protected:
+    void calc_chirt();
+    double Uch, Usp, dblOcc, nsr;
+    char paramsFileName[200];
+};
+
+// interacting Green's function (src/green.h)
+class green : public chi {
+public:
+    green(int nk0 = 8, int Nw0 = 32, double n = 1.0, double T = 1.0, double eta = 0.1, double *params = NULL);
+    void get_params() const;
+    double get_mu() { return mu; }
+    void calc_Self_FFT_spline();
+    void traceSelfG();
+    void traceSelfG2();
+    void find_mu();
+    void find_FS_inter();
+    void MDC(int *n, int Nn, double w, double *eta, int Neta, bool use_Pade = false);
+    void Gwn_local();
+
+protected:
+    double eta, mu, Sigma_inf;
+    bool mu_calcule, have_self;
+};
+
+// optical conductivity (src/cond_opt.h)
+class cond_opt : public green {
+public:
+    cond_opt(int nk0 = 8, int Nw0 = 256, double n = 1.0, double T = 1.0, double eta = 0.1, double *params = NULL);
+};
+
+#endif
