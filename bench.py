@@ -197,29 +197,36 @@ def our_arm(a, world, rank, local_rank):
         ctx.call("tpsc_launch_count", C.byref(c))
         return c.value
 
-    for _ in range(a.warmup):
-        g.solve()
-    torch.cuda.synchronize()
-    barrier(world)
-
-    # ---- device-resident solves --------------------------------------------
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
-    l0 = launches()
-    with ClockSampler(dev) as clk:
-        torch.cuda.synchronize()
-        for i in range(a.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            ev[i][0].record(stream)
+    def timed_solves(form):
+        """K solves of one root-search form, each bracketed by CUDA events on
+        the library stream after an L2 flush; returns total ms (max over
+        ranks), kernels launched, the clock record, scalars and stage times."""
+        g.set_form(form)
+        for _ in range(a.warmup):
             g.solve()
-            ev[i][1].record(stream)
         torch.cuda.synchronize()
-    n_launch = launches() - l0
-    ms = sum(s.elapsed_time(e) for s, e in ev)
-    ms = allreduce_max(ms, world, dev)
+        barrier(world)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+        l0 = launches()
+        with ClockSampler(dev) as clk:
+            torch.cuda.synchronize()
+            for i in range(a.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                ev[i][0].record(stream)
+                g.solve()
+                ev[i][1].record(stream)
+            torch.cuda.synchronize()
+        n = launches() - l0
+        t = allreduce_max(sum(s.elapsed_time(e) for s, e in ev), world, dev)
+        return t, n, clk.summary(), g.scalars(), g.stage_times()
+
+    # ---- device-resident solves: the FP64 drop-in with the reference's root
+    # searches, then the Newton form (the headline) -----------------------------
+    ms_ref, _, _, sc_ref, stages_ref = timed_solves(_lib.FORM_REFERENCE)
+    ms, n_launch, clocks, sc, stages = timed_solves(_lib.FORM_NEWTON)
     value = world * a.steps / (ms / 1e3)
-    sc = g.scalars()
-    stages = g.stage_times()
+    value_ref = world * a.steps / (ms_ref / 1e3)
 
     # ---- end to end through the public API ------------------------------------
     nk0, nw0, nbk, n8 = g.dims()
@@ -274,17 +281,24 @@ def our_arm(a, world, rank, local_rank):
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (model parameters; no dataset)",
-        "config": {"workload": WORKLOAD_NAME, "form": "fp64 drop-in (reference root searches)",
+        "config": {"workload": WORKLOAD_NAME, "form": "fp64 transforms + Newton root searches",
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "512 MB flush before every step; working set ~2.4 GB per solve",
                    "sumrule_evals": counts["sumrule"], "mu_evals": counts["trace_diff_G"]},
+        "forms": {"fp64_newton": {"solves_per_s": value, "ms_per_step": ms / a.steps, "stage_ms": stages},
+                  "fp64_reference_roots": {"solves_per_s": value_ref, "ms_per_step": ms_ref / a.steps,
+                                           "stage_ms": stages_ref,
+                                           "sumrule_evals": int(sc_ref["evals_sp"] + sc_ref["evals_ch"]),
+                                           "mu_evals": int(sc_ref["evals_mu"])},
+                  "max_rel_diff_roots": max(abs(sc[k] - sc_ref[k]) / abs(sc_ref[k])
+                                            for k in ("Usp", "Uch", "mu"))},
         "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                      "algorithmic_bytes": kb.value, "launch_ms": per_ms[dom]},
         "kernels_ms": per_ms, "kernel_launches_per_solve": counts, "stage_ms": stages,
         "gpu_launches": n_launch,
-        "clocks": clk.summary(),
+        "clocks": clocks,
         "results": {k: sc[k] for k in ("Usp", "Uch", "dblOcc", "mu", "Sigma_inf")},
     }
     if world == 1 and not a.no_cpu_baseline:

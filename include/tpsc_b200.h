@@ -62,6 +62,17 @@ enum tpsc_scalar {
     TPSC_S_COUNT
 };
 
+/* How a solve finds its roots (tpsc_set_form).
+ *  TPSC_FORM_REFERENCE: the reference's find_zero control flow for Usp, Uch
+ *    and mu (src/generique.cpp:604-1234) -- the FP64 drop-in, same roots and
+ *    the same number of function evaluations as the reference;
+ *  TPSC_FORM_NEWTON: safeguarded Newton steps inside the reference's search
+ *    intervals, with the derivative from the same device pass as the value
+ *    (d trace/dU of the sum rules, d Tr(G-G0)/d mu); mu starts at mu0.
+ *    Same roots to ~1e-14, several times fewer passes.  No counterpart in
+ *    the reference. */
+enum tpsc_form { TPSC_FORM_REFERENCE = 0, TPSC_FORM_NEWTON = 1 };
+
 /* Create a context on CUDA device `device`.  Returns NULL and sets *status on
  * failure (no CUDA device, driver error). */
 tpsc_ctx *tpsc_create(int device, int *status);
@@ -76,6 +87,10 @@ const char *tpsc_last_error(const tpsc_ctx *ctx);
  * Computes eps_k and mu0 of the finite lattice on the device. */
 int tpsc_set_model(tpsc_ctx *ctx, int nk0, int Nw0, double n, double T, double tp, double tpp, double t3,
                    double U);
+
+/* Root-search form of the following solves (enum tpsc_form); default
+ * TPSC_FORM_REFERENCE. */
+int tpsc_set_form(tpsc_ctx *ctx, int form);
 
 /* chi0::calc_chiqw_FFT_spline(nq0, nw0) (src/chi0.cpp:279-718): switches the
  * current grid to (nq0, nw0) -- re-deriving eps_k and mu0 as set_grid does --
@@ -108,8 +123,9 @@ int tpsc_self_energy(tpsc_ctx *ctx);
 /* green::traceSelfG (src/green.cpp:3001-3104). */
 int tpsc_trace_self_G(tpsc_ctx *ctx, double out[2]);
 
-/* green::traceDiffG (src/green.cpp:3108-3182): Tr(G - G0) at chemical potential mu. */
-int tpsc_trace_diff_G(tpsc_ctx *ctx, double mu, double *trace);
+/* green::traceDiffG (src/green.cpp:3108-3182): Tr(G - G0) at chemical potential
+ * mu; *dtrace (may be NULL) = d Tr(G - G0) / d mu from the same pass. */
+int tpsc_trace_diff_G(tpsc_ctx *ctx, double mu, double *trace, double *dtrace);
 
 /* green::find_mu (src/green.cpp:3185-3282): mu from Tr(G - G0) = 0, then traceSelfG2. */
 int tpsc_find_mu(tpsc_ctx *ctx);

@@ -127,6 +127,27 @@ def test_l256_scalars_match_reference(ctx):
     assert rel(se["S"][:, cols], g["self_cols"]) < 1e-7
 
 
+@pytest.mark.parametrize("name", ["l32_w256_u4_tp", "l16_w128_n110", "l16_w64_half", "l256_w4096_u4"])
+def test_newton_form_same_roots(ctx, name):
+    """The Newton form reaches the reference's Usp, Uch and mu (to the
+    rounding of the sum rules) with far fewer device passes."""
+    from tpsc_conductivity_b200 import _lib
+
+    g = load_golden(name)
+    p, s = g["p"], g["s"]
+    gr = make(ctx, p)
+    try:
+        gr.set_form(_lib.FORM_NEWTON)
+        gr.solve()
+        sc = gr.scalars()
+    finally:
+        gr.set_form(_lib.FORM_REFERENCE)
+    for k in ("Usp", "Uch", "dblOcc"):
+        assert rel(sc[k], s[k]) < 1e-9, (k, sc[k], s[k])
+    assert abs(sc["mu"] - s["mu"]) < 1e-9 * max(1, abs(s["mu"]))
+    assert sc["evals_sp"] + sc["evals_ch"] <= 20 and sc["evals_mu"] <= 12
+
+
 @pytest.mark.parametrize("name", ["l32_w512_u2", "l16_w128_n110", "l16_w64_half"])
 def test_continuation_matches_reference(ctx, name):
     """Pade / polynomial continuation (green::MDC, find_FS_inter) and

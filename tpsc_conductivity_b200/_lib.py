@@ -29,7 +29,7 @@ SIGNATURES = [
     ("tpsc_vertex", C.c_int, [C.c_void_p]),
     ("tpsc_self_energy", C.c_int, [C.c_void_p]),
     ("tpsc_trace_self_G", C.c_int, [C.c_void_p, _dp]),
-    ("tpsc_trace_diff_G", C.c_int, [C.c_void_p, C.c_double, _dp]),
+    ("tpsc_trace_diff_G", C.c_int, [C.c_void_p, C.c_double, _dp, _dp]),
     ("tpsc_find_mu", C.c_int, [C.c_void_p]),
     ("tpsc_solve", C.c_int, [C.c_void_p]),
     ("tpsc_get_scalars", C.c_int, [C.c_void_p, _dp, C.c_int]),
@@ -45,7 +45,11 @@ SIGNATURES = [
     ("tpsc_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
     ("tpsc_pade_sigma", C.c_int, [C.c_void_p, _ip, C.c_int, _dp, C.c_int, C.c_int, _dp, _dp]),
     ("tpsc_gwn_local", C.c_int, [C.c_void_p, _dp]),
+    ("tpsc_set_form", C.c_int, [C.c_void_p, C.c_int]),
 ]
+
+# enum tpsc_form
+FORM_REFERENCE, FORM_NEWTON = 0, 1
 
 # tpsc_run_kernel stage ids
 KERNELS = ["gslice", "chi0_slice", "chi0_tau", "vertex_q", "vertex_tau", "sigma_slice", "sigma_tau",

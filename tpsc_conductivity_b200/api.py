@@ -57,6 +57,11 @@ class Green:
         self.ctx = ctx or Context(device)
         self.ctx.call("tpsc_set_model", nk0, Nw0, n, T, tp, tpp, t3, U)
 
+    def set_form(self, form):
+        """Root-search form of the context: _lib.FORM_REFERENCE (the reference's
+        find_zero) or _lib.FORM_NEWTON (safeguarded Newton)."""
+        self.ctx.call("tpsc_set_form", int(form))
+
     # ---- stages (reference method names) ---------------------------------
     def calc_chiqw_FFT_spline(self, nq0=None, nw0=None):
         """chi0::calc_chiqw_FFT_spline (src/chi0.cpp:279)."""
@@ -105,11 +110,12 @@ class Green:
         self.ctx.call("tpsc_trace_self_G", _dptr(out))
         return float(out[0]), float(out[1])
 
-    def traceDiffG(self, mu):
-        """green::traceDiffG (src/green.cpp:3108)."""
-        t = C.c_double()
-        self.ctx.call("tpsc_trace_diff_G", mu, C.byref(t))
-        return t.value
+    def traceDiffG(self, mu, derivative=False):
+        """green::traceDiffG (src/green.cpp:3108); with derivative=True also
+        d Tr(G - G0)/d mu from the same pass."""
+        t, dt = C.c_double(), C.c_double()
+        self.ctx.call("tpsc_trace_diff_G", mu, C.byref(t), C.byref(dt))
+        return (t.value, dt.value) if derivative else t.value
 
     def find_mu(self):
         """green::find_mu (src/green.cpp:3185), followed by traceSelfG2."""

@@ -7,6 +7,7 @@
 // solve.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -210,6 +211,61 @@ bool find_zero(F &&func, const double init[3], double *root, const double *lims,
 }
 
 // ---------------------------------------------------------------------------
+// Safeguarded Newton root search for the Newton form: f returns the value and
+// the derivative (from the same device pass).  [lo, hi] is the reference's
+// search interval; it shrinks to the side of each evaluation that the
+// derivative's sign and the value's sign rule out, and a Newton step that
+// leaves it is replaced by the midpoint.  Converged when |f| is below tol,
+// when the step is below 1e-14 relative, or when the step stops shrinking
+// (at most half the previous one) while already below 1e-10 relative: f is
+// then at its rounding-noise floor and further steps only dither.
+// ---------------------------------------------------------------------------
+template <typename F>
+bool newton_root(F &&func, double x0, double lo, double hi, double tol, double *root, int *nev, bool *dev_err) {
+    *nev = 0;
+    *dev_err = false;
+    // the start must lie strictly inside the interval (the spin sum rule has
+    // its pole at the upper end: U/2 can lie beyond it)
+    double x = (x0 > lo && x0 < hi) ? x0 : 0.5 * (lo + hi), prev_step = 0.0;
+    for (int it = 0; it < 60; ++it) {
+        double y, dy;
+        ++*nev;
+        if (!func(x, y, dy)) {
+            *dev_err = true;
+            return false;
+        }
+        if (!std::isfinite(y) || !std::isfinite(dy)) return false;
+        if (std::fabs(y) < tol) {
+            *root = x;
+            return true;
+        }
+        // the root lies on the side where f changes sign
+        if ((y > 0) == (dy > 0))
+            hi = std::min(hi, x);
+        else
+            lo = std::max(lo, x);
+        const double scale = std::max(1.0, std::fabs(x));
+        double xn = (dy != 0.0) ? x - y / dy : 0.5 * (lo + hi);
+        // convergence is judged on the Newton step itself, before the bracket
+        // safeguard: at the root the step rounds to (or next to) x, which may
+        // coincide with the bracket end just moved to x
+        if (dy != 0.0 && std::fabs(xn - x) <= 1e-14 * scale) {
+            *root = xn;
+            return true;
+        }
+        if (!(xn >= lo && xn <= hi)) xn = 0.5 * (lo + hi);
+        const double step = std::fabs(xn - x);
+        if (it >= 2 && step < 1e-10 * scale && step > 0.5 * prev_step) {
+            *root = xn;
+            return true;
+        }
+        prev_step = step;
+        x = xn;
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------
 // one (nk0, Nw0) grid: tables and arrays
 // ---------------------------------------------------------------------------
 struct Grid {
@@ -236,6 +292,7 @@ struct Grid {
 
 struct tpsc_ctx {
     int device = 0;
+    int form = TPSC_FORM_REFERENCE;
     cudaStream_t st = nullptr;
     Reduce red;
     double *h_res = nullptr;  // pinned, 8 doubles
@@ -541,34 +598,53 @@ int sumrule(tpsc_ctx *ctx, int channel, double Uv, double *tr, double *dtr) {
 // chi::find_Usp_Uch(nq0, nw0, Usc) on the current grid after chi0 (src/chi.cpp:850-876)
 int roots_Usp_Uch(tpsc_ctx *ctx, double Usc[2]) {
     const double n = ctx->n, U = ctx->U, nsr = ctx->nsr;
+    const bool newton = (ctx->form & TPSC_FORM_NEWTON) != 0;
     int rc = TPSC_OK;
-    auto rsp = [&](double Us, double &y) -> bool {
-        double tr;
-        rc = sumrule(ctx, 0, Us, &tr, nullptr);
+    // R_sp(Us) = trace + n - n^2/2 - nsr + Us nsr^2/(2U)  (chi::sum_rule_sp, src/chi.cpp:833-836)
+    auto rsp = [&](double Us, double &y, double &dy) -> bool {
+        double tr, dtr;
+        rc = sumrule(ctx, 0, Us, &tr, &dtr);
         if (rc) return false;
         y = tr + n - n * n / 2.0 - nsr + Us * nsr * nsr / (2.0 * U);
+        dy = dtr + nsr * nsr / (2.0 * U);
         return true;
+    };
+    auto rsp1 = [&](double Us, double &y) -> bool {
+        double dy;
+        return rsp(Us, y, dy);
     };
     const double init_sp[3] = {U / 2.0, 0.0, 2.0 / ctx->scal[TPSC_S_CHI0MAX] - 2 * EPS};
     int nev;
-    bool derr;
+    bool derr, ok;
     double root = 0;
-    if (!find_zero(rsp, init_sp, &root, nullptr, &nev, &derr)) {
+    ok = newton ? newton_root(rsp, init_sp[0], init_sp[1], init_sp[2], 1e-16, &root, &nev, &derr)
+                : find_zero(rsp1, init_sp, &root, nullptr, &nev, &derr);
+    if (!ok) {
         if (derr) return rc;
         return fail(ctx, TPSC_ERR_NO_ROOT, "Usp not found");
     }
     ctx->scal[TPSC_S_EVALS_SP] = nev;
     Usc[0] = root;
     ctx->Usp = root;
-    auto rch = [&](double Uc, double &y) -> bool {
-        double tr;
-        rc = sumrule(ctx, 1, Uc, &tr, nullptr);
+    // R_ch(Uc) = trace + n - n^2/2 - (nsr + Usp nsr^2/(2U) - nsr^2)  (src/chi.cpp:840-843)
+    auto rch = [&](double Uc, double &y, double &dy) -> bool {
+        double tr, dtr;
+        rc = sumrule(ctx, 1, Uc, &tr, &dtr);
         if (rc) return false;
         y = tr + n - n * n / 2.0 - (nsr + ctx->Usp * nsr * nsr / (2.0 * U) - nsr * nsr);
+        dy = dtr;
         return true;
     };
+    auto rch1 = [&](double Uc, double &y) -> bool {
+        double dy;
+        return rch(Uc, y, dy);
+    };
     const double init_ch[3] = {0.0, 0.0, 1000.0 * U};
-    if (!find_zero(rch, init_ch, &root, nullptr, &nev, &derr)) {
+    // the Newton form starts the charge search at U (the interval's lower end
+    // is not an interior point)
+    ok = newton ? newton_root(rch, U, init_ch[1], init_ch[2], 1e-16, &root, &nev, &derr)
+                : find_zero(rch1, init_ch, &root, nullptr, &nev, &derr);
+    if (!ok) {
         if (derr) return rc;
         return fail(ctx, TPSC_ERR_NO_ROOT, "Uch not found");
     }
@@ -626,10 +702,15 @@ int trace_self_G(tpsc_ctx *ctx, double out[2]) {
     return TPSC_OK;
 }
 
-int trace_diff_G(tpsc_ctx *ctx, double pmu, double *tr) {
+int trace_diff_G(tpsc_ctx *ctx, double pmu, double *tr, double *dtr = nullptr) {
     Grid *g = ctx->cur;
     CK(launch_trace_diff_G(g->d, g->S, g->s2, g->s3, g->s4, g->sinf, g->mu0, pmu, ctx->T, ctx->red, ctx->st));
-    return read_result(ctx, 1, tr);
+    double r[2];
+    int rc = read_result(ctx, 2, r);
+    if (rc) return rc;
+    *tr = r[0];
+    if (dtr) *dtr = r[1];
+    return TPSC_OK;
 }
 
 int find_mu(tpsc_ctx *ctx) {
@@ -640,11 +721,19 @@ int find_mu(tpsc_ctx *ctx) {
         rc = trace_diff_G(ctx, m, &y);
         return rc == TPSC_OK;
     };
+    auto fd = [&](double m, double &y, double &dy) -> bool {
+        rc = trace_diff_G(ctx, m, &y, &dy);
+        return rc == TPSC_OK;
+    };
     const double init[3] = {0.0, -10.0, 10.0}, lims[2] = {-20.0, 20.0};
     double root = 0;
     int nev;
     bool derr;
-    if (!find_zero(f, init, &root, lims, &nev, &derr)) {
+    // the Newton form starts from mu0, the non-interacting chemical potential
+    const bool ok = (ctx->form & TPSC_FORM_NEWTON)
+                        ? newton_root(fd, g->mu0, init[1], init[2], 1e-15, &root, &nev, &derr)
+                        : find_zero(f, init, &root, lims, &nev, &derr);
+    if (!ok) {
         if (derr) return rc;
         return fail(ctx, TPSC_ERR_NO_ROOT, "mu not found");
     }
@@ -833,11 +922,11 @@ int tpsc_trace_self_G(tpsc_ctx *ctx, double out[2]) {
     return trace_self_G(ctx, out);
 }
 
-int tpsc_trace_diff_G(tpsc_ctx *ctx, double mu, double *trace) {
+int tpsc_trace_diff_G(tpsc_ctx *ctx, double mu, double *trace, double *dtrace) {
     int rc = need_model(ctx);
     if (rc) return rc;
     if (!ctx->cur->have_S) return fail(ctx, TPSC_ERR_STATE, "the self-energy has not been computed");
-    return trace_diff_G(ctx, mu, trace);
+    return trace_diff_G(ctx, mu, trace, dtrace);
 }
 
 int tpsc_find_mu(tpsc_ctx *ctx) {
@@ -1011,6 +1100,14 @@ int tpsc_stage_times(tpsc_ctx *ctx, double *ms, int n) {
 int tpsc_launch_count(tpsc_ctx *ctx, long long *count) {
     if (!count) return fail(ctx, TPSC_ERR_ARG, "bad arguments");
     *count = launches_total();
+    return TPSC_OK;
+}
+
+int tpsc_set_form(tpsc_ctx *ctx, int form) {
+    if (!ctx) return fail(nullptr, TPSC_ERR_ARG, "null context");
+    if (form != TPSC_FORM_REFERENCE && form != TPSC_FORM_NEWTON)
+        return fail(ctx, TPSC_ERR_ARG, "unknown form");
+    ctx->form = form;
     return TPSC_OK;
 }
 

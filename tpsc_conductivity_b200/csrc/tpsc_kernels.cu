@@ -892,10 +892,15 @@ __device__ __forceinline__ void sigma_full(double i1, double sinf, double c2, do
 // Tr(G - G0) at chemical potential pmu (green::traceDiffG,
 // src/green.cpp:3108-3182): stored frequencies j < Nw0/2 with the full Sigma,
 // tail Nw0/2 <= j <= Nw0 with its asymptotic form.  One CTA per column block.
-__device__ __forceinline__ double trdiff_term(double wn, double rS, double iS, double e, double mu0, double pmu) {
+// one term of Tr(G - G0) and its derivative with respect to pmu
+__device__ __forceinline__ void trdiff_term(double wn, double rS, double iS, double e, double mu0, double pmu,
+                                            double w, double &v, double &dv) {
     const double a = e - pmu + rS, d = e - mu0, g = mu0 - pmu + rS;
-    const double tmp = 1.0 / (((wn - iS) * (wn - iS) + a * a) * (wn * wn + d * d));
-    return tmp * (g * a * d + iS * (iS - 2 * wn) * d - wn * wn * g);
+    const double A2 = (wn - iS) * (wn - iS) + a * a;
+    const double num = g * a * d + iS * (iS - 2 * wn) * d - wn * wn * g;
+    const double inv = w / (A2 * (wn * wn + d * d));
+    v += inv * num;
+    dv += inv * (wn * wn - (a + g) * d + num * 2.0 * a / A2);
 }
 
 __global__ void __launch_bounds__(kRedThreads)
@@ -915,7 +920,7 @@ __global__ void __launch_bounds__(kRedThreads)
         c4[c] = ok ? s4[o0 + c] : 0.0;
     }
     const double pt = 3.141592653589793 * T;
-    double v = 0.0;
+    double v = 0.0, dv = 0.0;
     const double4 *row = reinterpret_cast<const double4 *>(S + (size_t)blk * 4 * NO);
     for (int j = threadIdx.x; j < NO; j += blockDim.x) {
         const double wn = (2 * j + 1) * pt;
@@ -928,7 +933,7 @@ __global__ void __launch_bounds__(kRedThreads)
             if (ww[c] == 0.0) continue;
             double rS, iS;
             sigma_full(i1, sinf, c2[c], c3[c], sv[c], rS, iS);
-            v += ww[c] * trdiff_term(wn, rS, iS, e[c], mu0, pmu);
+            trdiff_term(wn, rS, iS, e[c], mu0, pmu, ww[c], v, dv);
         }
     }
     for (int t = threadIdx.x; t <= NO; t += blockDim.x) {
@@ -940,11 +945,11 @@ __global__ void __launch_bounds__(kRedThreads)
             if (ww[c] == 0.0) continue;
             const double rS = -c2[c] * i2 + c4[c] * i2 * i2;
             const double iS = -sinf * i1 + c3[c] * i2 * i1;
-            v += ww[c] * trdiff_term(wn, rS, iS, e[c], mu0, pmu);
+            trdiff_term(wn, rS, iS, e[c], mu0, pmu, ww[c], v, dv);
         }
     }
-    double out[1] = {v};
-    grid_finish<1>(out, r, 0.0);
+    double out[2] = {v, dv};
+    grid_finish<2>(out, r, 0.0);
 }
 
 // Tr Sigma G0 and its asymptotic correction (green::traceSelfG,
