@@ -195,6 +195,30 @@ int tpsc_kernel_bytes(tpsc_ctx *ctx, int which, double *bytes);
  * loaded. */
 int tpsc_launch_count(tpsc_ctx *ctx, long long *count);
 
+/* ---- allocation-free sum rule (no counterpart in the reference) ----------
+ * The spin (channel 0) or charge (channel 1) sum-rule trace and its U
+ * derivative, as tpsc_trace_diff_chi computes them, for callers that cannot
+ * allocate device memory at the point of the call: code running inside a
+ * memory pool or arena that owns the device memory, callbacks from a
+ * framework that forbids allocation on its hot path, solver loops that must
+ * not call cudaMalloc/cudaFree because they synchronise the device.  It
+ * needs no context and allocates nothing: the caller passes device pointers
+ * to chi0(q, iqn) in the reference's layout ([(Nw0/2+1) * N8], octant index
+ * m + l(l+1)/2), chi0_inf and chi0_inf2 ([N8]) and out (2 doubles: trace,
+ * d trace/dU), and the work runs asynchronously on `stream` (a cudaStream_t,
+ * NULL for the default stream) of the current device.
+ *
+ * Its per-block partial sums live in a fixed device array of the library
+ * (about 33 KB), which every GPU that loads the library holds until the
+ * process exits.  That array bounds the lattice: nk0 up to 256 (N8 up to
+ * 8385); larger lattices return TPSC_ERR_ARG.  The first call on each device
+ * looks up the array's address with that device current; make that first
+ * call before any stream capture.  All calls on a device share the array and
+ * it keeps the last call's contents; calls whose work overlaps on the GPU
+ * race on it, so order them (one stream, or events). */
+int tpsc_sumrule_noalloc(const double *chiqw, const double *chi0_inf, const double *chi0_inf2, int nk0, int Nw0,
+                         double T, int channel, double Uv, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
