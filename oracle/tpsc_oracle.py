@@ -766,3 +766,274 @@ def gwn_local(ek, mu, sr: SelfResult, T):
     sig = sr.sigma(T)
     z = 1j * (2 * np.arange(sig.shape[0])[:, None] + 1) * PI * T
     return np.sum((w / nk02) / (z - eo + mu - sig), axis=1)
+
+
+# ----------------------------------------------------------------------------
+# current-current correlator: bubble + Maki-Thompson and kx0
+# (cond_opt::calc_chijj_vertex_corr_all_optim with chi3 = false,
+# src/cond_opt.cpp:2537-4286)
+# ----------------------------------------------------------------------------
+def grad_ek_x(kx, ky, tp, tpp, t3):
+    """d eps/d kx (hamiltonien::grad_ek dir 0, src/hamiltonien.cpp:411-419)."""
+    return (2.0 * np.sin(kx) + 4.0 * tp * np.sin(kx) * np.cos(ky) + 4.0 * tpp * np.sin(2 * kx)
+            + 4 * t3 * (2.0 * np.sin(2 * kx) * np.cos(ky) + np.cos(2 * ky) * np.sin(kx)))
+
+
+def hessian_ek_xx(kx, ky, tp, tpp, t3):
+    """d2 eps/d kx2 (hamiltonien::Hessian_ek (0,0), src/hamiltonien.cpp:428-433)."""
+    return (2.0 * np.cos(kx) + 4.0 * tp * np.cos(kx) * np.cos(ky) + 8.0 * tpp * np.cos(2 * kx)
+            + 4 * t3 * (4.0 * np.cos(2 * kx) * np.cos(ky) + np.cos(2 * ky) * np.cos(kx)))
+
+
+def dst_dct(a):
+    """FFTW RODFT00 along axis -2 and REDFT00 along axis -1 (unnormalised)."""
+    return sfft.dst(sfft.dct(a, type=1, axis=-1), type=1, axis=-2)
+
+
+def find_roots_2pol(A, B, C):
+    """generique::find_roots_2pol (src/generique.cpp:1666-1727): roots of
+    A z^2 + B z + C, then Newton polish (tol 1e-16, <= 10 steps), elementwise."""
+    R = np.sqrt(B * B - 4.0 * A * C + 0j)
+    roots = [(-B - R) / (2.0 * A), (-B + R) / (2.0 * A)]
+    out = []
+    for r0 in roots:
+        x = np.array(r0, dtype=np.complex128)
+        y = A * x * x + B * x + C
+        p = 2.0 * A * x + B
+        y0 = y.copy()
+        for _ in range(10):
+            act = (np.abs(p) > 0) & (np.abs(y) > 1e-16)
+            if not np.any(act):
+                break
+            x2, y2 = x.copy(), y.copy()
+            c = y - p * x
+            xn = np.where(act, -c / np.where(act, p, 1), x)
+            yn = A * xn * xn + B * xn + C
+            worse = act & (np.abs(y2) < np.abs(yn))
+            xn = np.where(worse, 0.5 * (xn + x2), xn)
+            x = xn
+            y = A * x * x + B * x + C
+            p = 2.0 * A * x + B
+        out.append(np.where(np.abs(y) < np.abs(y0), x, r0))
+    return out
+
+
+@dataclass
+class CondResult:
+    chijj1: np.ndarray   # [Nw0/2 + 1] bubble chi_jj(iqn)
+    chijj2: np.ndarray   # [Nw0/2 + 1] Maki-Thompson correction
+    kx0: float           # diamagnetic term <-kx> (f-sum: chijj1(0)+chijj2(0) = -kx0)
+
+
+def conductivity(sv: Solve, tp, tpp, t3, U, T) -> CondResult:
+    nk0, nbw = sv.nk0, sv.Nw0
+    nbk = nk0 // 2 + 1
+    n8 = nbk * (nbk + 1) // 2
+    nw = nbw // 2
+    ek = dispersion(nbk, tp, tpp, t3)
+    mu0, mu = sv.mu0, sv.mu
+    sr, V, c0 = sv.sigma, sv.V, sv.chi0
+    Usp, Uch = sv.U.Usp, sv.U.Uch
+    normFact = 1.0 / (nk0 * nk0)
+    kq = np.arange(nbk) * PI / (nbk - 1)
+    # tables (src/cond_opt.cpp:2588-2611)
+    d2ek = hessian_ek_xx(kq[:, None], kq[None, :], tp, tpp, t3)                 # [nbk, nbk]
+    dek = grad_ek_x(kq[1:nbk - 1, None], kq[None, :], tp, tpp, t3)              # [nbk-2, nbk]
+    xk = ek[1:nbk - 1, :] - mu0                                                # eps - mu0 on K4
+    pos = xk > 0
+    # h(r, tau_j) (:2696-2735)
+    h = np.empty((nbw + 1, nbk - 2, nbk))
+    for j in range(nbw + 1):
+        t = j / (T * nbw)
+        fr = np.where(pos, normFact * dek * np.exp(-xk * t) / (np.exp(-xk / T) + 1.0),
+                      normFact * dek * np.exp(xk * (1.0 / T - t)) / (np.exp(xk / T) + 1.0))
+        h[j] = dst_dct(fr)
+    # dh at tau = 0, beta (:2744-2783)
+    dh0 = dst_dct(np.where(pos, -normFact * dek * xk / (np.exp(-xk / T) + 1.0),
+                           -normFact * dek * xk * np.exp(xk / T) / (np.exp(xk / T) + 1.0)))
+    dhb = dst_dct(np.where(pos, -normFact * dek * xk * np.exp(-xk / T) / (np.exp(-xk / T) + 1.0),
+                           -normFact * dek * xk / (np.exp(xk / T) + 1.0)))
+    # f0(r, tau_j) (:2794-2827)
+    f0 = np.empty_like(h)
+    ekp = np.exp(-xk / T)
+    ekn = np.exp(xk / T)
+    for j in range(nbw + 1):
+        t = j / (T * nbw)
+        fr = np.where(pos,
+                      normFact * dek * np.exp(-xk * t) * (t / (ekp + 1.0) - ekp / (T * (ekp + 1.0) ** 2)),
+                      normFact * dek * np.exp(xk * (1.0 / T - t)) * (t / (ekn + 1.0) - 1.0 / (T * (ekn + 1.0) ** 2)))
+        f0[j] = dst_dct(fr)
+    # df0 at tau = 0, beta (:2835-2887)
+    df00 = dst_dct(np.where(pos, normFact * dek * (xk * ekp / (T * (ekp + 1.0) ** 2) + 1.0 / (ekp + 1.0)),
+                            normFact * dek * ekn * (xk / (T * (ekn + 1.0) ** 2) + 1.0 / (ekn + 1.0))))
+    df0b = dst_dct(np.where(pos, normFact * dek * ekp * ((-xk) * (1.0 / (T * (ekp + 1.0)) - ekp / (T * (ekp + 1.0) ** 2))
+                                                        + 1.0 / (ekp + 1.0)),
+                            normFact * dek * ((-xk) * (1.0 / (T * (ekn + 1.0)) - 1.0 / (T * (ekn + 1.0) ** 2))
+                                              + 1.0 / (ekn + 1.0))))
+    # vertex on the K4-shaped r grid: r = (l+1, m) folded into the octant (:2892-2908)
+    lx = np.arange(1, nbk - 1)[:, None] * np.ones((1, nbk), dtype=int)
+    my = np.ones((nbk - 2, 1), dtype=int) * np.arange(nbk)[None, :]
+    xo = np.maximum(lx, my)
+    yo = np.minimum(lx, my)
+    oidx = yo + xo * (xo + 1) // 2
+    fact = U * (3.0 * Usp + Uch) / 4
+    V0 = V[0][oidx]
+    dchi = c0.dtau_chirt0[oidx]
+    dhV0 = dst_dct(2.0 * dh0 * V0 + h[0] * fact * dchi)
+    dhVb = dst_dct(2.0 * dhb * V0 - h[nbw] * fact * dchi)
+    df0V0 = dst_dct(2.0 * df00 * V0 + f0[0] * fact * dchi)
+    df0Vb = dst_dct(2.0 * df0b * V0 - f0[nbw] * fact * dchi)
+    for j in range(nbw + 1):
+        wn = j if j <= nbw // 2 else nbw - j
+        h[j] = dst_dct(2.0 * h[j] * V[wn][oidx])
+        f0[j] = dst_dct(2.0 * f0[j] * V[wn][oidx])
+    # per k (:3179-3871), vectorised over the K4 grid; axis 0 = tau or frequency
+    K = (nbk - 2) * nbk
+    hk = h.reshape(nbw + 1, K)
+    f0k = f0.reshape(nbw + 1, K)
+    ok = oidx.reshape(K)
+    e = ek[1:nbk - 1, :].reshape(K)
+    wt = np.where((my == 0) | (my == nbk - 1), 2.0, 4.0).reshape(K)
+    dk = dek.reshape(K)
+    hdt = 1.0 / (nbw * T)
+    jj = np.arange(nbw)[:, None]
+
+    def spline_to_matsubara(vals, d0, dN):
+        """J(i k_n) for the nbw fermionic frequencies in the reference's
+        ordering (index p <-> n = p - nbw/2) (:3204-3234)."""
+        a, b, c, d = clamped_spline(vals, hdt, d0, dN)
+        F = np.fft.ifft(np.exp(1j * jj * PI / nbw) * 6.0 * a, axis=0) * nbw
+        C1 = -vals[0] - vals[nbw]
+        C2_ = d0 + dN
+        d2J0 = 2 * b[0]
+        d2Jb = 6.0 * a[nbw - 1] / (nbw * T) + 2.0 * b[nbw - 1]
+        C3_ = -d2J0 - d2Jb
+        out = np.empty((nbw, K), dtype=np.complex128)
+        jpos = np.arange(nbw // 2)[:, None]
+        kn = (2 * jpos + 1) * PI * T
+        out[jpos[:, 0] + nbw // 2] = (-1j * C1 / kn - C2_ / kn ** 2 + 1j * C3_ / kn ** 3
+                                      + (1.0 - np.exp(1j * (2 * jpos + 1) * PI / nbw)) * F[:nbw // 2] / kn ** 4)
+        jneg = np.arange(nbw // 2, nbw)[:, None]
+        kn = (2 * (jneg - nbw) + 1) * PI * T
+        out[jneg[:, 0] - nbw // 2] = (-1j * C1 / kn - C2_ / kn ** 2 + 1j * C3_ / kn ** 3
+                                      + (1.0 - np.exp(1j * (2 * (jneg - nbw) + 1) * PI / nbw)) * F[nbw // 2:] / kn ** 4)
+        return out, C1
+
+    Jt, CJ1 = spline_to_matsubara(hk, dhV0.reshape(K), dhVb.reshape(K))
+    J0t, _ = spline_to_matsubara(f0k, df0V0.reshape(K), df0Vb.reshape(K))
+    # G(k, i k_n) on the same frequency ordering (:3309-3347)
+    sig = sr.sigma(T)[:, ok]                                   # [nw, K] positive frequencies
+    p = np.arange(nbw)[:, None]
+    kn = (2.0 * (p - nw) + 1) * PI * T
+    sigfull = np.where(p < nw, np.conj(sig[np.clip(nw - p[:, 0] - 1, 0, nw - 1)]), sig[np.clip(p[:, 0] - nw, 0, nw - 1)])
+    G = T / (1j * kn - e + mu - sigfull)
+    Jt = G * Jt
+    chijj2_qn0 = np.sum(G * G * J0t / T, axis=0)
+    Gtail = T / ((-e + mu) + 1j * (kn + sr.Sigma_inf / kn))
+    G = G - Gtail
+    Jt = Jt - Gtail * (-1j * CJ1 / kn)
+    k0 = np.sum(G, axis=0)
+    dGp = np.sum(kn * G.imag, axis=0)
+    dJ0 = -np.sum(kn * Jt.imag, axis=0)
+    r1, r2 = find_roots_2pol(np.ones(K, dtype=np.complex128), (-e + mu) + 0j, -sr.Sigma_inf + 0j * e)
+    a1, a2 = r1 / (r1 - r2), r2 / (r2 - r1)
+    b1 = CJ1 / (r1 - r2)
+    b2 = -b1
+
+    def branch(r, a, b):
+        big = r.real > 0
+        ex = np.where(big, np.exp(-r / T), np.exp(r / T))
+        den = ex + 1.0
+        fp = np.where(big, a / den, a * ex / den)
+        fm = np.where(big, a * ex / den, a / den)
+        fj = np.where(big, r * b * ex / den, r * b / den)
+        fjb = np.where(big, r * b / den, r * b * ex / den)
+        return den, fp, fm, fj, fjb
+
+    den1, f1p, f1m, fj1, fj1b = branch(r1, a1, b1)
+    den2, f2p, f2m, fj2, fj2b = branch(r2, a2, b2)
+    k0 = k0 + (f1m + f2m).real
+    dGm = -dGp
+    dGp = dGp + (r1 * f1p + r2 * f2p).real
+    dGm = dGm + (r1 * f1m + r2 * f2m).real
+    dJb = -dJ0
+    dJ0 = dJ0 + (fj1 + fj2).real
+    dJb = dJb + (fj1b + fj2b).real
+    # back to tau, analytic tails added (:3545-3620)
+    Gt = np.fft.fft(G, axis=0)
+    Gbeta = Gt[0].copy()
+    Jtt = np.fft.ifft(Jt, axis=0) * nbw
+    Jbeta = Jtt[0].copy()
+    t = jj / (nbw * T)
+
+    def tails(tt):
+        e1 = np.where(r1.real > 0, np.exp(-tt * r1), np.exp((1.0 / T - tt) * r1))
+        j1 = np.where(r1.real > 0, np.exp(r1 * (tt - 1.0 / T)), np.exp(r1 * tt))
+        e2 = np.where(r2.real > 0, np.exp(-tt * r2), np.exp((1.0 / T - tt) * r2))
+        j2 = np.where(r2.real > 0, np.exp(r2 * (tt - 1.0 / T)), np.exp(r2 * tt))
+        G0t = (-a1 * e1 / den1 - a2 * e2 / den2).real
+        Jinf = (b1 * j1 / den1 + b2 * j2 / den2).real
+        return G0t, Jinf
+
+    G0t, Jinf = tails(t)
+    ph = np.exp(1j * (jj * PI * (nbw - 1)) / nbw)
+    Gt = ph * Gt + G0t
+    Jtt = Jtt / ph + Jinf
+    G0b, Jinfb = tails(np.full((1, K), 1.0 / T))
+    phb = np.exp(1j * PI * (nbw - 1))
+    Gbeta = phb * Gbeta + G0b[0]
+    Jbeta = Jbeta / phb + Jinfb[0]
+    # GJ(tau) spline -> J(i q_n) (:3622-3660)
+    gj = np.empty((nbw + 1, K))
+    gj[:nbw] = (Gt * Jtt).real
+    gj[nbw] = ((-Gt[0] - 1.0) * Jbeta).real
+    d0 = (dGp * Jtt[0] + Gt[0] * dJ0).real
+    dN = (dGm * Jbeta - (Gt[0] + 1.0) * dJb).real
+    CJ1b = gj[0] - gj[nbw]
+    a, b, c, d = clamped_spline(gj, hdt, d0, dN)
+    d2J0 = 2 * b[0]
+    d2Jb = 6.0 * a[nbw - 1] / (nbw * T) + 2.0 * b[nbw - 1]
+    CJ3b = d2J0 - d2Jb
+    J0f = np.fft.fft(6.0 * a, axis=0)
+    jq = np.arange(1, nw + 1)[:, None]
+    wq = 2 * jq * PI * T
+    Jq = (-2.0j * CJ1b / wq + 2.0j * CJ3b / wq ** 3
+          + 2.0j * ((1.0 - np.exp(-2j * jq * PI / nbw)) * J0f[1:nw + 1] / wq ** 4).imag)
+    # bubble -G(tau)G(beta - tau) (:3662-3700)
+    GG = np.empty((nw + 1, K))
+    GG[0] = (Gt[0] * (Gt[0] + 1.0)).real
+    GG[1:] = (-Gt[1:nw + 1] * Gt[nbw - np.arange(1, nw + 1)]).real
+    dchi_b = dGp * (Gt[0].real + 1.0) + Gt[0].real * dGm
+    a, b, c, d = clamped_spline(GG, hdt, dchi_b, np.zeros(K))
+    fb = np.empty((nbw, K))
+    fb[:nw] = 6.0 * a
+    fb[nw:] = -fb[:nw][::-1]
+    Fb = np.fft.fft(fb, axis=0)
+    integ = np.sum(a * hdt ** 4 / 4.0 + b * hdt ** 3 / 3.0 + c * hdt ** 2 / 2.0 + d * hdt, axis=0)
+    bub = np.empty((nw + 1, K))
+    bub[0] = 2 * integ
+    bub[1:] = -2.0 * dchi_b / wq ** 2 + ((1.0 - np.exp(-2j * jq * PI / nbw)) * Fb[1:nw + 1] / wq ** 4).real
+    chijj1 = -np.sum(2.0 * wt * normFact * dk * dk * bub, axis=1)
+    chijj2 = np.empty(nw + 1)
+    chijj2[0] = -np.sum(normFact * wt * dk * chijj2_qn0.real)
+    chijj2[1:] = -np.sum(normFact * wt * dk * Jq.imag / wq, axis=1)
+    k0sum = -np.sum(2.0 * wt * normFact * d2ek[1:nbk - 1, :].reshape(K) * k0)
+    # kx = 0 and kx = pi lines (:3993-4173)
+    for l in (0, nbk - 1):
+        mm = np.arange(nbk)
+        xo2 = np.maximum(l, mm)
+        yo2 = np.minimum(l, mm)
+        o2 = yo2 + xo2 * (xo2 + 1) // 2
+        e2 = ek[l, :]
+        s2 = sr.sigma(T)[:, o2]
+        sfull = np.where(p < nw, np.conj(s2[np.clip(nw - p[:, 0] - 1, 0, nw - 1)]), s2[np.clip(p[:, 0] - nw, 0, nw - 1)])
+        G2 = T / (1j * kn - e2 + mu - sfull) - T / ((-e2 + mu) + 1j * (kn + sr.Sigma_inf / kn))
+        kk = np.sum(G2, axis=0)
+        q1, q2 = find_roots_2pol(np.ones(nbk, dtype=np.complex128), (-e2 + mu) + 0j, -sr.Sigma_inf + 0j * e2)
+        aa1, aa2 = q1 / (q1 - q2), q2 / (q2 - q1)
+        fm = (np.where(q1.real > 0, aa1 * np.exp(-q1 / T) / (np.exp(-q1 / T) + 1.0), aa1 / (np.exp(q1 / T) + 1.0))
+              + np.where(q2.real > 0, aa2 * np.exp(-q2 / T) / (np.exp(-q2 / T) + 1.0), aa2 / (np.exp(q2 / T) + 1.0)))
+        kk = kk + fm.real
+        w2 = np.where((mm == 0) | (mm == nbk - 1), 1.0, 2.0)
+        k0sum -= np.sum(2.0 * w2 * normFact * d2ek[l, :] * kk)
+    return CondResult(chijj1, chijj2, float(k0sum.real))

@@ -114,3 +114,19 @@ def test_oracle_continuation_matches_reference(name):
     check_fs(poly, g["fs_inter"])
     check_fs(pade, g["fs_inter_pade"])
     assert np.allclose(O.gwn_local(ek, r.mu, r.sigma, p["T"]), g["gwn_local"], rtol=1e-8, atol=1e-11)
+
+
+@pytest.mark.parametrize("name", CONT)
+def test_oracle_conductivity_matches_reference(name):
+    """Bubble chi_jj, the Maki-Thompson correction and kx0
+    (cond_opt::calc_chijj_vertex_corr_all_optim, src/cond_opt.cpp:2537-4286)
+    against the reference's own arrays."""
+    g = load_golden(name)
+    p = g["p"]
+    r = O.solve(p["U"], p["tp"], p["tpp"], p["t3"], p["n"], p["T"], p["nk0"], p["Nw0"])
+    c = O.conductivity(r, p["tp"], p["tpp"], p["t3"], p["U"], p["T"])
+    scale1 = np.max(np.abs(g["chijj1"]))
+    scale2 = np.max(np.abs(g["chijj2"]))
+    assert np.max(np.abs(c.chijj1 - g["chijj1"])) <= 1e-11 * scale1
+    assert np.max(np.abs(c.chijj2 - g["chijj2"])) <= 1e-11 * scale2
+    assert abs(c.kx0 - float(g["kx0"])) <= 1e-12 * abs(float(g["kx0"]))
