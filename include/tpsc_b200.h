@@ -167,8 +167,25 @@ int tpsc_pade_sigma(tpsc_ctx *ctx, const int *n_idx, int Nn, const double *z, in
  * out [Nw0/2] complex interleaved. */
 int tpsc_gwn_local(tpsc_ctx *ctx, double *out);
 
+/* ---- current-current correlator (needs tpsc_find_mu) -------------------- */
+/* cond_opt::calc_chijj_vertex_corr_all_optim(false, mmin, n_theta, NULL, 0),
+ * the bubble + Maki-Thompson branch (src/cond_opt.cpp:2537-4286), on the
+ * context's solve: chi_jj1(iq_n) (bubble) and chi_jj2(iq_n) (Maki-Thompson
+ * vertex correction), n = 0..Nw0/2, the diamagnetic term kx0, and both
+ * chi_jj resolved into n_theta >= 1 bins of the angle
+ * theta_k = atan((L/2 - m)/(L/2 - kx index)) (N_theta_k of the reference).
+ * Needs nk0 >= 8. */
+int tpsc_chijj(tpsc_ctx *ctx, int n_theta);
+/* Results of the last tpsc_chijj (any pointer may be NULL): chijj1, chijj2
+ * [Nw0/2+1]; kx0 [1]; chijj1_k, chijj2_k [(Nw0/2+1) * n_theta] in the
+ * reference's layout p + j * n_theta. */
+int tpsc_get_chijj(tpsc_ctx *ctx, double *chijj1, double *chijj2, double *kx0, double *chijj1_k,
+                   double *chijj2_k);
+
 /* Device time of the last tpsc_solve per stage in ms:
- * {chi0, sum rules, vertex, self energy, traces + mu}; n <= 5. */
+ * {chi0, sum rules, vertex, self energy, traces + mu}, then of the last
+ * tpsc_chijj: {h V / f0 V slices + end conditions, per-k tau kernel,
+ * kx lines + final sums}; n <= 8. */
 int tpsc_stage_times(tpsc_ctx *ctx, double *ms, int n);
 
 /* ---- instrumentation (no counterpart in the reference) ------------------ */

@@ -12,8 +12,8 @@
  *   MODE chi0   chi0::calc_chiqw_FFT_spline(nk0, Nw0)            (chi0.cpp:279)
  *        solve  green::calc_Self_FFT_spline(); traceSelfG(); find_mu()
  *               (green.cpp:1673, 3001, 3185) -- the full TPSC solve
- *        cond   solve + cond_opt::calc_chijj_vertex_corr_all_optim(false,3,1,NULL,0)
- *               (cond_opt.cpp:2537)
+ *        cond   solve + cond_opt::calc_chijj_vertex_corr_all_optim(false,3,N,NULL,0)
+ *               (cond_opt.cpp:2537), N = $TPSC_PROBE_NTHETA (default 1) angle bins
  *        post   solve + find_FS_inter, MDC(10 points, w=0, 4 etas), Gwn_local
  *               (src/tpsc_main.cpp:77-114)
  *        bench  timings only: the half-grid pre-pass alone, then the solve
@@ -173,7 +173,10 @@ int main(int argc, char **argv) {
         if (mode == "cond") {
             std::cout << std::setprecision(17);
             t0 = omp_get_wtime();
-            g->calc_chijj_vertex_corr_all_optim(false, 3, 1, NULL, 0);
+            const char *nt = getenv("TPSC_PROBE_NTHETA");
+            const int ntheta = nt ? atoi(nt) : 1;
+            fprintf(meta, "ntheta %d\n", ntheta);
+            g->calc_chijj_vertex_corr_all_optim(false, 3, ntheta, NULL, 0);
             fprintf(meta, "t_cond %.6f\n", omp_get_wtime() - t0);
             g->dump_cond(meta, absdir);
         }

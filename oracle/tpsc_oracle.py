@@ -774,13 +774,13 @@ def gwn_local(ek, mu, sr: SelfResult, T):
 # src/cond_opt.cpp:2537-4286)
 # ----------------------------------------------------------------------------
 def grad_ek_x(kx, ky, tp, tpp, t3):
-    """d eps/d kx (hamiltonien::grad_ek dir 0, src/hamiltonien.cpp:411-419)."""
+    """d eps/d kx (hamiltonien::grad_ek dir 0, src/hamiltonien.cpp:134-142)."""
     return (2.0 * np.sin(kx) + 4.0 * tp * np.sin(kx) * np.cos(ky) + 4.0 * tpp * np.sin(2 * kx)
             + 4 * t3 * (2.0 * np.sin(2 * kx) * np.cos(ky) + np.cos(2 * ky) * np.sin(kx)))
 
 
 def hessian_ek_xx(kx, ky, tp, tpp, t3):
-    """d2 eps/d kx2 (hamiltonien::Hessian_ek (0,0), src/hamiltonien.cpp:428-433)."""
+    """d2 eps/d kx2 (hamiltonien::Hessian_ek (0,0), src/hamiltonien.cpp:145-155)."""
     return (2.0 * np.cos(kx) + 4.0 * tp * np.cos(kx) * np.cos(ky) + 8.0 * tpp * np.cos(2 * kx)
             + 4 * t3 * (4.0 * np.cos(2 * kx) * np.cos(ky) + np.cos(2 * ky) * np.cos(kx)))
 
@@ -823,9 +823,11 @@ class CondResult:
     chijj1: np.ndarray   # [Nw0/2 + 1] bubble chi_jj(iqn)
     chijj2: np.ndarray   # [Nw0/2 + 1] Maki-Thompson correction
     kx0: float           # diamagnetic term <-kx> (f-sum: chijj1(0)+chijj2(0) = -kx0)
+    chijj1_k: np.ndarray = None   # [Nw0/2 + 1, ntheta] angle-resolved
+    chijj2_k: np.ndarray = None
 
 
-def conductivity(sv: Solve, tp, tpp, t3, U, T) -> CondResult:
+def conductivity(sv: Solve, tp, tpp, t3, U, T, ntheta=1) -> CondResult:
     nk0, nbw = sv.nk0, sv.Nw0
     nbk = nk0 // 2 + 1
     n8 = nbk * (nbk + 1) // 2
@@ -1013,10 +1015,19 @@ def conductivity(sv: Solve, tp, tpp, t3, U, T) -> CondResult:
     bub = np.empty((nw + 1, K))
     bub[0] = 2 * integ
     bub[1:] = -2.0 * dchi_b / wq ** 2 + ((1.0 - np.exp(-2j * jq * PI / nbw)) * Fb[1:nw + 1] / wq ** 4).real
-    chijj1 = -np.sum(2.0 * wt * normFact * dk * dk * bub, axis=1)
-    chijj2 = np.empty(nw + 1)
-    chijj2[0] = -np.sum(normFact * wt * dk * chijj2_qn0.real)
-    chijj2[1:] = -np.sum(normFact * wt * dk * Jq.imag / wq, axis=1)
+    c1 = -2.0 * wt * normFact * dk * dk * bub                      # [nw + 1, K] per-k terms
+    c2 = np.empty((nw + 1, K))
+    c2[0] = -normFact * wt * dk * chijj2_qn0.real
+    c2[1:] = -normFact * wt * dk * Jq.imag / wq
+    chijj1, chijj2 = c1.sum(axis=1), c2.sum(axis=1)
+    # angle bins theta_k = atan((nk0/2 - m)/(nk0/2 - l - 1)) (:3174, 3790-3796)
+    theta = np.arctan((nk0 / 2 - my) / (nk0 / 2 - lx)).reshape(K)
+    ib = np.floor(theta / (PI / (2.0 * ntheta))).astype(int)
+    chijj1_k = np.zeros((nw + 1, ntheta))
+    chijj2_k = np.zeros((nw + 1, ntheta))
+    for b in range(ntheta):
+        chijj1_k[:, b] = c1[:, ib == b].sum(axis=1)
+        chijj2_k[:, b] = c2[:, ib == b].sum(axis=1)
     k0sum = -np.sum(2.0 * wt * normFact * d2ek[1:nbk - 1, :].reshape(K) * k0)
     # kx = 0 and kx = pi lines (:3993-4173)
     for l in (0, nbk - 1):
@@ -1036,4 +1047,4 @@ def conductivity(sv: Solve, tp, tpp, t3, U, T) -> CondResult:
         kk = kk + fm.real
         w2 = np.where((mm == 0) | (mm == nbk - 1), 1.0, 2.0)
         k0sum -= np.sum(2.0 * w2 * normFact * d2ek[l, :] * kk)
-    return CondResult(chijj1, chijj2, float(k0sum.real))
+    return CondResult(chijj1, chijj2, float(k0sum.real), chijj1_k, chijj2_k)

@@ -21,7 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 PROBE = os.path.join(ROOT, "oracle", "_ref", "tpsc_ref_probe")
 
-# name: (mode, U, tp, tpp, t3, n, T, nk0, Nw0, keep_full_arrays)
+# name: (mode, U, tp, tpp, t3, n, T, nk0, Nw0, keep_full_arrays[, angle bins of chi_jj])
 CASES = {
     # tiny lattice, half-grid pre-pass exercised, conductivity too
     "l16_w64_u2": ("cond", 2.0, 0.0, 0.0, 0.0, 0.875, 0.25, 16, 64, True),
@@ -33,6 +33,11 @@ CASES = {
     "l16_w128_n110": ("cond", 3.0, -0.2, 0.1, 0.0, 1.1, 0.2, 16, 128, True),
     # half filling, particle-hole symmetric: mu0 = 0 shortcut (src/green0.cpp:18-23)
     "l16_w64_half": ("cond", 2.0, 0.0, 0.0, 0.0, 1.0, 0.3, 16, 64, True),
+    # chi_jj resolved into 3 angle bins (N_theta_k)
+    "l32_w256_theta3": ("cond", 3.0, -0.1, 0.0, 0.0, 0.9, 0.1, 32, 256, True, 3),
+    # the optical-conductivity case: 128x128, U=3, n=0.9, T=0.1, 1024 positive
+    # fermionic frequencies; scalars, sampled columns, chi_jj and 4 angle bins
+    "l128_w2048_cond": ("cond", 3.0, 0.0, 0.0, 0.0, 0.9, 0.1, 128, 2048, False, 4),
     # larger lattice, lower temperature
     "l64_w1024_u4": ("solve", 4.0, -0.15, 0.0, 0.0, 0.875, 0.05, 64, 1024, False),
     # the 256x256, 2048 positive iwn case: scalars and sampled columns only
@@ -51,9 +56,10 @@ def read_meta(path):
 
 
 def run_case(name, spec, threads):
-    mode, U, tp, tpp, t3, n, T, nk0, Nw0, full = spec
+    mode, U, tp, tpp, t3, n, T, nk0, Nw0, full = spec[:10]
+    ntheta = spec[10] if len(spec) > 10 else 1
     with tempfile.TemporaryDirectory() as d:
-        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), TPSC_PROBE_NTHETA=str(ntheta))
         args = [PROBE, d, mode] + [repr(v) for v in (U, tp, tpp, t3, n, T)] + [str(nk0), str(Nw0)]
         subprocess.run(args, check=True, env=env)
         meta = read_meta(os.path.join(d, "meta.txt"))
@@ -111,6 +117,11 @@ def run_case(name, spec, threads):
                      if x.startswith(prefix) and not (exclude and x.startswith(exclude))]
                 return np.loadtxt(os.path.join(work, f[0]), ndmin=2)
 
+            if ntheta > 1:
+                # chijj1_k_qn_* / chijj2_k_qn_*: lines "j  p+1  value" (src/cond_opt.cpp:3931-3941)
+                for key, prefix in (("chijj1_k", "chijj1_k_qn_"), ("chijj2_k", "chijj2_k_qn_")):
+                    t = table(prefix)
+                    out[key] = t[:, 2].reshape(nw, ntheta)
             out["mdc_A"] = table("Akw_Pade_k_")[:, 2:]
             sp = table("Self_Pade_k_")[:, 2:]
             out["mdc_sigma"] = sp[:, 0::2] + 1j * sp[:, 1::2]

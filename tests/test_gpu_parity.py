@@ -15,7 +15,7 @@ from conftest import golden_names, load_golden
 
 pytestmark = pytest.mark.gpu
 
-SMALL = [n for n in golden_names() if not n.startswith("l256")]
+SMALL = [n for n in golden_names() if not n.startswith(("l256", "l128"))]
 
 
 def rel(a, b):

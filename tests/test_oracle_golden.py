@@ -9,7 +9,7 @@ import pytest
 from conftest import golden_names, load_golden
 from oracle import tpsc_oracle as O
 
-SMALL = [n for n in golden_names() if not n.startswith("l256")]
+SMALL = [n for n in golden_names() if not n.startswith(("l256", "l128"))]
 
 
 def full_sigma(g, S, T, cols=None):
@@ -116,17 +116,20 @@ def test_oracle_continuation_matches_reference(name):
     assert np.allclose(O.gwn_local(ek, r.mu, r.sigma, p["T"]), g["gwn_local"], rtol=1e-8, atol=1e-11)
 
 
-@pytest.mark.parametrize("name", CONT)
-def test_oracle_conductivity_matches_reference(name):
-    """Bubble chi_jj, the Maki-Thompson correction and kx0
-    (cond_opt::calc_chijj_vertex_corr_all_optim, src/cond_opt.cpp:2537-4286)
+@pytest.mark.parametrize("name,ntheta", [(n, 1) for n in CONT] + [("l32_w256_theta3", 3)])
+def test_oracle_conductivity_matches_reference(name, ntheta):
+    """Bubble chi_jj, the Maki-Thompson correction, kx0 and the angle-resolved
+    sums (cond_opt::calc_chijj_vertex_corr_all_optim, src/cond_opt.cpp:2537-4286)
     against the reference's own arrays."""
     g = load_golden(name)
     p = g["p"]
     r = O.solve(p["U"], p["tp"], p["tpp"], p["t3"], p["n"], p["T"], p["nk0"], p["Nw0"])
-    c = O.conductivity(r, p["tp"], p["tpp"], p["t3"], p["U"], p["T"])
+    c = O.conductivity(r, p["tp"], p["tpp"], p["t3"], p["U"], p["T"], ntheta)
     scale1 = np.max(np.abs(g["chijj1"]))
     scale2 = np.max(np.abs(g["chijj2"]))
     assert np.max(np.abs(c.chijj1 - g["chijj1"])) <= 1e-11 * scale1
     assert np.max(np.abs(c.chijj2 - g["chijj2"])) <= 1e-11 * scale2
     assert abs(c.kx0 - float(g["kx0"])) <= 1e-12 * abs(float(g["kx0"]))
+    if ntheta > 1:
+        assert np.max(np.abs(c.chijj1_k - g["chijj1_k"])) <= 1e-11 * scale1
+        assert np.max(np.abs(c.chijj2_k - g["chijj2_k"])) <= 1e-11 * scale2

@@ -195,6 +195,58 @@ class Green:
         return out
 
     def stage_times(self):
-        out = np.zeros(5)
-        self.ctx.call("tpsc_stage_times", _dptr(out), 5)
-        return dict(zip(["chi0", "sumrules", "vertex", "self", "mu"], out.tolist()))
+        out = np.zeros(8)
+        self.ctx.call("tpsc_stage_times", _dptr(out), 8)
+        return dict(zip(["chi0", "sumrules", "vertex", "self", "mu", "cond_slices", "cond_tau", "cond_finish"],
+                        out.tolist()))
+
+
+class CondOpt(Green):
+    """Drop-in for the reference's ``cond_opt`` (src/cond_opt.h:25), a ``green``
+    with the current-current correlator."""
+
+    def __init__(self, nk0=8, Nw0=32, n=1.0, T=1.0, eta=0.1, params=None, device=0, ctx=None):
+        super().__init__(nk0, Nw0, n, T, eta, params, device, ctx)
+
+    def calc_chijj_vertex_corr_all_optim(self, chi3=False, mmin=3, N_theta_k=1, k_chijj=None, nk_chijj=0):
+        """cond_opt::calc_chijj_vertex_corr_all_optim (src/cond_opt.cpp:2537-4286),
+        bubble + Maki-Thompson branch.  Computes Sigma and mu first when they are
+        missing, as the reference does (src/cond_opt.cpp:2550-2560).  ``mmin``,
+        ``k_chijj`` and ``nk_chijj`` do not change chi_jj in the reference and
+        are accepted for the signature's sake.  Returns chijj1, chijj2
+        [Nw0/2+1], kx0 and the angle-resolved chijj1_k, chijj2_k [Nw0/2+1,
+        N_theta_k]."""
+        if chi3:
+            raise NotImplementedError("the second vertex correction (chi3 = true) is not part of this build")
+        self._nbins = int(N_theta_k)
+        try:
+            self.ctx.call("tpsc_chijj", int(N_theta_k))
+        except _lib.TPSCError as e:
+            if e.status != 5:
+                raise
+            self.calc_Self_FFT_spline()
+            self.traceSelfG()
+            self.find_mu()
+            self.ctx.call("tpsc_chijj", int(N_theta_k))
+        return self.chijj()
+
+    def chijj(self):
+        """Results of the last calc_chijj_vertex_corr_all_optim."""
+        nk0, nw0, nbk, n8 = self.dims()
+        NB = nw0 // 2 + 1
+        c1, c2, kx0 = np.zeros(NB), np.zeros(NB), np.zeros(1)
+        self.ctx.call("tpsc_get_chijj", _dptr(c1), _dptr(c2), _dptr(kx0), None, None)
+        nb = getattr(self, "_nbins", 1)
+        k1, k2 = np.zeros(NB * nb), np.zeros(NB * nb)
+        self.ctx.call("tpsc_get_chijj", None, None, None, _dptr(k1), _dptr(k2))
+        return {"chijj1": c1, "chijj2": c2, "kx0": float(kx0[0]), "chijj1_k": k1.reshape(NB, nb),
+                "chijj2_k": k2.reshape(NB, nb)}
+
+    def sigma_qn(self, nq=None):
+        """sigma(iq_n) = (-kx0 - chi_jj(iq_n)) / q_n, n = 1..nq (the Kubo form;
+        the reference stops at chi_jj and kx0)."""
+        r = self.chijj()
+        chi = r["chijj1"] + r["chijj2"]
+        nq = len(chi) - 1 if nq is None else nq
+        qn = 2 * np.pi * np.arange(1, nq + 1) * self.tem
+        return (-r["kx0"] - chi[1:nq + 1]) / qn

@@ -16,8 +16,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libtpsc_b200.so")
-SOURCES = ["tpsc_kernels.cu", "tpsc_engine.cpp", "tpsc_noalloc.cu"]
-HEADERS = ["tpsc_fft.cuh", "tpsc_kernels.cuh"]
+SOURCES = ["tpsc_kernels.cu", "tpsc_cond.cu", "tpsc_engine.cpp", "tpsc_noalloc.cu"]
+HEADERS = ["tpsc_fft.cuh", "tpsc_kernels.cuh", "tpsc_device.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -48,13 +48,28 @@ def _stale() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
-    cmd = [nvcc_path(), *ARCH, *host_compiler(), "-std=c++17", "-O3", "-lineinfo", "-shared",
-           "-Xcompiler", "-fPIC", "-cudart", "static", "-I", os.path.join(ROOT, "include"),
-           *[os.path.join(CSRC, f) for f in SOURCES], "-o", LIB + ".tmp"]
+    from concurrent.futures import ThreadPoolExecutor
+
+    objdir = os.path.join(PKG, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    common = [nvcc_path(), *ARCH, *host_compiler(), "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC",
+              "-I", os.path.join(ROOT, "include")]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        common.insert(1, "-Xptxas=-v")
+
+    def compile_one(src: str) -> str:
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        cmd = [*common, "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        return obj
+
+    # the translation units compile independently (one nvcc each), then one link
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as pool:
+        objs = list(pool.map(compile_one, SOURCES))
+    subprocess.run([nvcc_path(), *ARCH, *host_compiler(), "-shared", "-cudart", "static", *objs, "-o", LIB + ".tmp"],
+                   check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -1,0 +1,267 @@
+// tpsc_device.cuh -- device helpers shared by the kernel translation units
+// (tpsc_kernels.cu: chi0, vertex, self-energy, traces; tpsc_cond.cu: the
+// current-current correlator).  Everything here is internal to the library.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tpsc_fft.cuh"
+#include "tpsc_kernels.cuh"
+
+namespace tpsc {
+
+// counts one (or n) kernel launches for the instrumentation ABI and returns
+// the launch status
+cudaError_t launched(int n = 1);
+
+namespace {
+
+constexpr double kPi = 3.141592653589793;  // == acos(-1.0) in double
+constexpr int kSliceThreads = 256;
+constexpr int kTauThreads = 256;
+constexpr int kWarm = 40;  // spline sweep warm-up: carry error <= 0.268^40
+
+__device__ __forceinline__ void oct_lm(const uint32_t *lm, int o, int &l, int &m) {
+    const uint32_t v = __ldg(&lm[o]);
+    l = (int)(v >> 16);
+    m = (int)(v & 0xffffu);
+}
+
+// integer multiplicity weight of octant point (l, m) as in the reference
+// loops: `base` halved on the l edges, m edges and the diagonal
+__device__ __forceinline__ int oct_weight(int base, int l, int m, int nbk) {
+    int w = base;
+    if (l == 0 || l == nbk - 1) w /= 2;
+    if (m == 0 || m == nbk - 1) w /= 2;
+    if (m == l) w /= 2;
+    return w;
+}
+
+// ---------------------------------------------------------------------------
+// compensated (Kahan-Babuska) summation
+// ---------------------------------------------------------------------------
+struct KSum {
+    double s = 0.0, c = 0.0;
+    __device__ __forceinline__ void add(double x) {
+        const double t = s + x;
+        if (fabs(s) >= fabs(x))
+            c += (s - t) + x;
+        else
+            c += (x - t) + s;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return s + c; }
+};
+
+// ---------------------------------------------------------------------------
+// slice kernels: shared-memory plan of one nbk x nbk slice + FFT scratch
+// ---------------------------------------------------------------------------
+template <int NBK>
+struct SliceSmem {
+    static constexpr int L = 2 * (NBK - 1);
+    static constexpr int G = FftPlan<L>::G;
+    static constexpr int NGRP = kSliceThreads / G;
+    static constexpr size_t slice_bytes = (size_t)NBK * NBK * sizeof(double);
+    static constexpr size_t scr_off = (slice_bytes + 15) & ~(size_t)15;
+    static constexpr size_t tw_off = scr_off + (size_t)NGRP * padded_len(L) * sizeof(double2);
+    static constexpr size_t bytes = tw_off + (size_t)L * sizeof(double2);
+};
+
+template <int NBK>
+__device__ __forceinline__ double2 *slice_scratch(double *S) {
+    return reinterpret_cast<double2 *>(reinterpret_cast<char *>(S) + SliceSmem<NBK>::scr_off);
+}
+
+// the L-point twiddle table staged in shared memory behind the FFT scratch;
+// the first __syncthreads of the kernel publishes it
+template <int NBK>
+__device__ __forceinline__ const double2 *slice_twiddles(double *S, const double2 *__restrict__ tw) {
+    double2 *t = reinterpret_cast<double2 *>(reinterpret_cast<char *>(S) + SliceSmem<NBK>::tw_off);
+    for (int i = threadIdx.x; i < SliceSmem<NBK>::L; i += blockDim.x) t[i] = __ldg(&tw[i]);
+    return t;
+}
+
+// write octant value v of point (l, m) into both triangles of the slice
+template <int NBK>
+__device__ __forceinline__ void put_sym(double *S, int l, int m, double v) {
+    S[l * NBK + m] = v;
+    S[m * NBK + l] = v;
+}
+
+// ---------------------------------------------------------------------------
+// tau kernels: clamped spline along a column, staging
+// ---------------------------------------------------------------------------
+// Clamped cubic spline through y[0..NJ) on a uniform grid of step h with end
+// slopes d0, dN: on exit y holds the node second derivatives M_j.  Solves
+//   2 M_0 + M_1 = 6/h ((V_1 - V_0)/h - d0)
+//   M_{i-1} + 4 M_i + M_{i+1} = 6/h^2 (V_{i+1} - 2 V_i + V_{i-1})
+//   M_{N-1} + 2 M_N = 6/h (dN - (V_N - V_{N-1})/h)
+// -- the same interpolant as generique::spline_coeffs_rel
+// (src/generique.cpp:214-322), S_j''' = 6 a_j = (M_{j+1} - M_j)/h -- by the
+// Thomas algorithm with pivots invp = 1/p_i and multipliers cp_i (cp_N = 0)
+// precomputed on the host.  The sweeps are split over TPC threads per column:
+// each chunk starts its carry kWarm rows early from zero; the carry decays
+// by 1/p_i <= 1/(2+sqrt3) per row, so the truncation error is below 1e-22 of
+// the local magnitude.  All threads of the block must call.
+template <int NC = 4>
+__device__ void spline_second_derivatives(double *A, int lda, int NJ, double h, const double *d0, const double *dN,
+                                          const double *__restrict__ invp, const double *__restrict__ cp) {
+    const int TPC = blockDim.x / NC;
+    const int c = threadIdx.x / TPC, k = threadIdx.x % TPC;
+    double *y = A + c * lda;
+    const int C = (NJ + TPC - 1) / TPC;
+    const int s = min(k * C, NJ), e = min(s + C, NJ);
+    const int N = NJ - 1;
+    const double a6 = 6.0 / (h * h), b6 = 6.0 / h;
+    const double dl = d0[c], dr = dN[c];
+    auto rhs = [&](int i, double vm, double v0, double vp) -> double {
+        if (i == 0) return b6 * ((vp - v0) / h - dl);
+        if (i == N) return b6 * (dr - (v0 - vm) / h);
+        return a6 * (vp - 2.0 * v0 + vm);
+    };
+    double carry = 0.0, vm_h = 0.0, vs_h = 0.0, ve_h = 0.0;
+    if (s < e) {
+        if (s > 0) {
+            const int i0 = max(0, s - kWarm);
+            double cc = 0.0;
+            double vm = i0 > 0 ? y[i0 - 1] : 0.0, v0 = y[i0];
+            for (int i = i0; i < s; ++i) {
+                const double vp = y[i + 1];
+                cc = (rhs(i, vm, v0, vp) - cc) * __ldg(&invp[i]);
+                vm = v0;
+                v0 = vp;
+            }
+            carry = cc;
+            vm_h = y[s - 1];
+        }
+        vs_h = y[s];
+        ve_h = e < NJ ? y[e] : 0.0;
+    }
+    __syncthreads();
+    if (s < e) {
+        double vm = vm_h, v0 = vs_h;
+        for (int i = s; i < e; ++i) {
+            const double vp = (i + 1 < e) ? y[i + 1] : ve_h;
+            const double dp = (rhs(i, vm, v0, vp) - carry) * __ldg(&invp[i]);
+            y[i] = dp;
+            carry = dp;
+            vm = v0;
+            v0 = vp;
+        }
+    }
+    __syncthreads();
+    double mc = 0.0;
+    if (s < e && e < NJ) {
+        const int i1 = min(N, e - 1 + kWarm);
+        double mm = 0.0;
+        for (int i = i1; i >= e; --i) mm = y[i] - __ldg(&cp[i]) * mm;
+        mc = mm;
+    }
+    __syncthreads();
+    if (s < e) {
+        double mm = mc;
+        for (int i = e - 1; i >= s; --i) {
+            mm = y[i] - __ldg(&cp[i]) * mm;
+            y[i] = mm;
+        }
+    }
+    __syncthreads();
+}
+
+// per-column sum of y[i0..i1) over the TPC threads of each column -> out[c]
+template <int NC = 4>
+__device__ void column_sums(const double *A, int lda, int i0, int i1, double *out) {
+    const int TPC = blockDim.x / NC;
+    const int c = threadIdx.x / TPC, k = threadIdx.x % TPC;
+    KSum acc;
+    for (int i = i0 + k; i < i1; i += TPC) acc.add(A[c * lda + i]);
+    __shared__ double part[1024];
+    part[threadIdx.x] = acc.value();
+    __syncthreads();
+    if (k == 0) {
+        KSum s;
+        for (int q = 0; q < TPC; ++q) s.add(part[c * TPC + q]);
+        out[c] = s.value();
+    }
+    __syncthreads();
+}
+
+template <int N>
+struct TauSmem {
+    static constexpr int threads = (N / 16) > kTauThreads ? (N / 16) : kTauThreads;
+    static size_t bytes(int NJ) {
+        size_t a = ((size_t)4 * NJ * sizeof(double) + 15) & ~(size_t)15;
+        return a + (size_t)padded_len(N) * sizeof(double2);
+    }
+};
+
+// Load one column block into shared memory, column-major.  Padding columns
+// (octant index >= n8, present because N8 is rounded up to a multiple of 4)
+// load as zeros: they share packed FFTs with real columns, so stale values
+// there would leak into real outputs through rounding.
+__device__ __forceinline__ void stage_in(double *A, const double *g, int NJ, int nvalid) {
+    for (int i = threadIdx.x; i < 4 * NJ; i += blockDim.x) A[(i & 3) * NJ + (i >> 2)] = (i & 3) < nvalid ? g[i] : 0.0;
+}
+__device__ __forceinline__ void stage_out(const double *A, double *g, int NJ) {
+    for (int i = threadIdx.x; i < 4 * NJ; i += blockDim.x) g[i] = A[(i & 3) * NJ + (i >> 2)];
+}
+
+// full Sigma(k, i w_n) = Sinf/z + C2/z^2 + C3/z^3 + S/z^4, z = i w_n, from the
+// reciprocal powers of w_n
+__device__ __forceinline__ void sigma_full(double i1, double sinf, double c2, double c3, double2 Sv, double &rS,
+                                           double &iS) {
+    const double i2 = i1 * i1, i4 = i2 * i2;
+    rS = -c2 * i2 + Sv.x * i4;
+    iS = -sinf * i1 + c3 * i2 * i1 + Sv.y * i4;
+}
+
+// complex division
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+    // Smith's algorithm
+    if (fabs(b.x) >= fabs(b.y)) {
+        const double r = b.y / b.x, d = b.x + b.y * r;
+        return make_double2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+    } else {
+        const double r = b.x / b.y, d = b.y + b.x * r;
+        return make_double2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// dispatch over the compiled sizes
+// ---------------------------------------------------------------------------
+template <template <int> class F, typename... Args>
+cudaError_t dispatch_nbk(int nbk, Args... args) {
+    switch (nbk) {
+        case 5: return F<5>::run(args...);
+        case 9: return F<9>::run(args...);
+        case 17: return F<17>::run(args...);
+        case 33: return F<33>::run(args...);
+        case 65: return F<65>::run(args...);
+        case 129: return F<129>::run(args...);
+        default: return cudaErrorInvalidValue;
+    }
+}
+template <template <int> class F, typename... Args>
+cudaError_t dispatch_nw(int nw0, Args... args) {
+    switch (nw0) {
+        case 16: return F<16>::run(args...);
+        case 32: return F<32>::run(args...);
+        case 64: return F<64>::run(args...);
+        case 128: return F<128>::run(args...);
+        case 256: return F<256>::run(args...);
+        case 512: return F<512>::run(args...);
+        case 1024: return F<1024>::run(args...);
+        case 2048: return F<2048>::run(args...);
+        case 4096: return F<4096>::run(args...);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename K>
+cudaError_t set_smem(K kernel, size_t bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+}  // namespace
+}  // namespace tpsc

@@ -286,6 +286,13 @@ struct Grid {
     double tailq_T = -1.0;         // temperature the tail power sums were built for
     double tailq_host[kTailQ] = {0};
     std::vector<void *> allocs;
+    // current-current correlator: device state (allocated on first use) and
+    // the last result, [n_theta 2 NB] binned, [2 NB] totals, kx0
+    CondDev cond;
+    bool cond_alloc = false;
+    size_t cond_part_cap = 0, cond_out_cap = 0;  // doubles in cond.partial, cond.out
+    std::vector<double> cond_host;
+    int cond_bins = 0;                            // n_theta of cond_host (0: none yet)
 };
 
 }  // namespace
@@ -304,7 +311,7 @@ struct tpsc_ctx {
     std::map<std::pair<int, int>, Grid *> grids;
     Grid *cur = nullptr;
     double scal[TPSC_S_COUNT] = {0};
-    double stage_ms[5] = {0};
+    double stage_ms[8] = {0};
     cudaEvent_t ev[6] = {};
     void *stage = nullptr;
     size_t stage_bytes = 0;
@@ -346,6 +353,8 @@ cudaError_t dalloc(Grid *g, T **p, size_t count) {
 
 void free_grid(Grid *g) {
     for (void *p : g->allocs) cudaFree(p);
+    if (g->cond.partial) cudaFree(g->cond.partial);
+    if (g->cond.out) cudaFree(g->cond.out);
     delete g;
 }
 
@@ -355,6 +364,17 @@ double dispk(double kx, double ky, double tp, double tpp, double t3) {
     return -2.0 * (std::cos(kx) + std::cos(ky)) - 4.0 * tp * std::cos(kx) * std::cos(ky) -
            2.0 * tpp * (std::cos(2 * kx) + std::cos(2 * ky)) -
            4 * t3 * (std::cos(2 * kx) * std::cos(ky) + std::cos(2 * ky) * std::cos(kx));
+}
+
+// d eps/d kx and d2 eps/d kx2 (hamiltonien::grad_ek direction 0 and
+// Hessian_ek (0, 0), src/hamiltonien.cpp:134-155)
+double grad_ek_x(double kx, double ky, double tp, double tpp, double t3) {
+    return 2.0 * std::sin(kx) + 4.0 * tp * std::sin(kx) * std::cos(ky) + 4.0 * tpp * std::sin(2 * kx) +
+           4 * t3 * (2.0 * std::sin(2 * kx) * std::cos(ky) + std::cos(2 * ky) * std::sin(kx));
+}
+double hessian_ek_xx(double kx, double ky, double tp, double tpp, double t3) {
+    return 2.0 * std::cos(kx) + 4.0 * tp * std::cos(kx) * std::cos(ky) + 8.0 * tpp * std::cos(2 * kx) +
+           4 * t3 * (4.0 * std::cos(2 * kx) * std::cos(ky) + std::cos(2 * ky) * std::cos(kx));
 }
 
 // Thomas-algorithm tables of the clamped-spline system with NJ nodes:
@@ -749,6 +769,123 @@ int find_mu(tpsc_ctx *ctx) {
     return TPSC_OK;
 }
 
+// Device state of the correlator on grid g for n_theta bins: the K4 arrays
+// once, the per-CTA partial rows and the output when n_theta grows, and the
+// eps-derivative tables (model dependent) and angle bins on every call.
+int ensure_cond(tpsc_ctx *ctx, Grid *g, int nbins) {
+    CondDev &c = g->cond;
+    const GridDev &d = g->d;
+    const int nbk = d.nbk;
+    if (!g->cond_alloc) {
+        c.K4 = (nbk - 2) * nbk;
+        c.K4p = (c.K4 + 1) & ~1;
+        int nblk = 0;
+        CK(cond_blocks(d, &nblk));
+        c.nblk = std::max(1, std::min(nblk, c.K4p / 2));
+        const size_t K4 = c.K4, K4p = c.K4p, NJ = d.nw0 + 1;
+        cudaError_t e = cudaSuccess;
+#define A(x)                \
+    if (e == cudaSuccess) { \
+        e = (x);            \
+    }
+        A(dalloc(g, &c.dek, K4));
+        A(dalloc(g, &c.d2ek, K4));
+        A(dalloc(g, &c.d2line, (size_t)2 * nbk));
+        A(dalloc(g, &c.bin, K4));
+        A(dalloc(g, &c.tab, 4 * K4));
+        A(dalloc(g, &c.hV, K4p * NJ));
+        A(dalloc(g, &c.f0V, K4p * NJ));
+        A(dalloc(g, &c.pre, 4 * K4p));
+        A(dalloc(g, &c.dbound, 4 * K4p));
+        A(dalloc(g, &c.lines, (size_t)2 * nbk));
+#undef A
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "conductivity allocation");
+        g->cond_alloc = true;
+    }
+    const int NB = d.nw0 / 2 + 1;
+    c.nbins = nbins;
+    c.pw = nbins * 2 * NB + 1;
+    const size_t need_part = (size_t)c.nblk * c.pw, need_out = (size_t)nbins * 2 * NB + 2 * NB + 1;
+    if (need_part > g->cond_part_cap) {
+        if (c.partial) cudaFree(c.partial);
+        c.partial = nullptr;
+        g->cond_part_cap = 0;
+        CK(cudaMalloc(&c.partial, need_part * sizeof(double)));
+        g->cond_part_cap = need_part;
+    }
+    if (need_out > g->cond_out_cap) {
+        if (c.out) cudaFree(c.out);
+        c.out = nullptr;
+        g->cond_out_cap = 0;
+        CK(cudaMalloc(&c.out, need_out * sizeof(double)));
+        g->cond_out_cap = need_out;
+    }
+    // tables on k = (l+1, m) pi/(nbk-1) (src/cond_opt.cpp:2588-2611) and on
+    // the kx = 0, pi lines; the angle bin theta_k = atan((L/2 - m)/(L/2 - l - 1)),
+    // floor(theta_k / (pi / (2 n_theta))) (src/cond_opt.cpp:3174, 3790-3793)
+    std::vector<double> dek(c.K4), d2(c.K4), d2l(2 * nbk);
+    std::vector<int> bins(c.K4, 0);
+    const int nk0 = d.nk0;
+    const double Dtheta = PI / (2.0 * nbins);
+    for (int l = 0; l < nbk - 2; ++l) {
+        const double kx = (l + 1) * PI / (nbk - 1);
+        for (int m = 0; m < nbk; ++m) {
+            const double ky = m * PI / (nbk - 1);
+            dek[m + l * nbk] = grad_ek_x(kx, ky, ctx->tp, ctx->tpp, ctx->t3);
+            d2[m + l * nbk] = hessian_ek_xx(kx, ky, ctx->tp, ctx->tpp, ctx->t3);
+            if (nbins > 1) {
+                const double th = std::atan((1.0 * (nk0 / 2 - m)) / (nk0 / 2 - l - 1));
+                bins[m + l * nbk] = std::min(nbins - 1, std::max(0, (int)std::floor(th / Dtheta)));
+            }
+        }
+    }
+    for (int side = 0; side < 2; ++side) {
+        const double kx = side == 0 ? 0.0 : (nbk - 1) * PI / (nbk - 1);
+        for (int m = 0; m < nbk; ++m)
+            d2l[side * nbk + m] = hessian_ek_xx(kx, m * PI / (nbk - 1), ctx->tp, ctx->tpp, ctx->t3);
+    }
+    CK(cudaMemcpyAsync(c.dek, dek.data(), c.K4 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(c.d2ek, d2.data(), c.K4 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(c.d2line, d2l.data(), 2 * nbk * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(c.bin, bins.data(), c.K4 * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    // the host vectors are released when this function returns
+    CK(cudaStreamSynchronize(ctx->st));
+    return TPSC_OK;
+}
+
+// cond_opt::calc_chijj_vertex_corr_all_optim, bubble + Maki-Thompson branch,
+// on the current grid after Sigma and mu (src/cond_opt.cpp:2537-4286)
+int run_cond(tpsc_ctx *ctx, int nbins) {
+    Grid *g = ctx->cur;
+    int rc = ensure_cond(ctx, g, nbins);
+    if (rc) return rc;
+    const GridDev &d = g->d;
+    const CondDev &c = g->cond;
+    const double mu = ctx->scal[TPSC_S_MU];
+    const double fact = ctx->U * (3.0 * ctx->Usp + ctx->Uch) / 4.0;  // TPSC_fact (src/cond_opt.cpp:2892)
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    CK(launch_cond_slices(d, c, g->V, g->dchirt0, g->mu0, ctx->T, fact, ctx->st));
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    CK(launch_cond_tau(d, c, g->S, g->s2, g->s3, g->sinf, mu, ctx->T, ctx->st));
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    CK(launch_cond_finish(d, c, g->S, g->s2, g->s3, g->sinf, mu, ctx->T, ctx->st));
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    const int NB = d.nw0 / 2 + 1;
+    g->cond_host.assign((size_t)nbins * 2 * NB + 2 * NB + 1, 0.0);
+    CK(cudaMemcpyAsync(g->cond_host.data(), c.out, g->cond_host.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (int i = 0; i < 3; ++i) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ctx->ev[i], ctx->ev[i + 1]));
+        ctx->stage_ms[5 + i] = ms;
+    }
+    g->cond_bins = nbins;
+    for (double v : g->cond_host)
+        if (!std::isfinite(v)) return fail(ctx, TPSC_ERR_NONFINITE, "non-finite chi_jj");
+    return TPSC_OK;
+}
+
 int ensure_stage(tpsc_ctx *ctx, size_t bytes) {
     if (ctx->stage_bytes >= bytes) return TPSC_OK;
     if (ctx->stage) cudaFree(ctx->stage);
@@ -1091,9 +1228,40 @@ int tpsc_gwn_local(tpsc_ctx *ctx, double *out) {
     return TPSC_OK;
 }
 
+int tpsc_chijj(tpsc_ctx *ctx, int n_theta) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    Grid *g = ctx->cur;
+    if (!g->have_S || ctx->scal[TPSC_S_EVALS_MU] == 0)
+        return fail(ctx, TPSC_ERR_STATE, "the self-energy and mu must be computed first");
+    if (n_theta < 1 || n_theta > 64) return fail(ctx, TPSC_ERR_ARG, "need 1 <= n_theta <= 64");
+    if (g->d.nk0 < 8) return fail(ctx, TPSC_ERR_ARG, "need nk0 >= 8");
+    g->cond_bins = 0;
+    return run_cond(ctx, n_theta);
+}
+
+int tpsc_get_chijj(tpsc_ctx *ctx, double *chijj1, double *chijj2, double *kx0, double *chijj1_k, double *chijj2_k) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    const Grid *g = ctx->cur;
+    if (g->cond_bins == 0) return fail(ctx, TPSC_ERR_STATE, "tpsc_chijj has not been run on the current grid");
+    const int NB = g->d.nw0 / 2 + 1, nb = g->cond_bins;
+    const double *tot = g->cond_host.data() + (size_t)nb * 2 * NB;
+    if (chijj1) std::memcpy(chijj1, tot, NB * sizeof(double));
+    if (chijj2) std::memcpy(chijj2, tot + NB, NB * sizeof(double));
+    if (kx0) *kx0 = tot[2 * NB];
+    for (int j = 0; j < NB; ++j)
+        for (int p = 0; p < nb; ++p) {
+            if (chijj1_k) chijj1_k[p + j * nb] = g->cond_host[(size_t)p * 2 * NB + j];
+            if (chijj2_k) chijj2_k[p + j * nb] = g->cond_host[(size_t)p * 2 * NB + NB + j];
+        }
+    return TPSC_OK;
+}
+
 int tpsc_stage_times(tpsc_ctx *ctx, double *ms, int n) {
     if (!ctx || !ms) return fail(ctx, TPSC_ERR_ARG, "bad arguments");
-    for (int i = 0; i < n && i < 5; ++i) ms[i] = ctx->stage_ms[i];
+    for (int i = 0; i < n && i < 8; ++i) ms[i] = ctx->stage_ms[i];
     return TPSC_OK;
 }
 

@@ -129,8 +129,11 @@ struct ScratchIO {
 // b = t + G u.  tw[m] = exp(-2 pi i m / N), m < N.  The first pass reads its
 // inputs through `in` (FIRST), the last pass hands its outputs, in natural
 // order, to `out` (LAST); every other pass reads and writes the padded
-// scratch x in place, with group barriers around the writes.
-template <int N, int G, int R, int SIGN, int E, bool SMEM_TW, bool FIRST, bool LAST, class In, class Out>
+// scratch x in place, with group barriers around the writes.  SYNC_IN puts
+// a barrier between the first pass's reads and its writes, for an `in` that
+// reads x itself.
+template <int N, int G, int R, int SIGN, int E, bool SMEM_TW, bool FIRST, bool LAST, bool SYNC_IN, class In,
+          class Out>
 __device__ __forceinline__ void stockham_pass(double2 *x, int t, int Ns, const double2 *__restrict__ tw, int grp,
                                               const In &in, const Out &out) {
     constexpr int NB = E / R;  // butterflies per thread
@@ -144,7 +147,7 @@ __device__ __forceinline__ void stockham_pass(double2 *x, int t, int Ns, const d
             v[u * R + q] = FIRST ? in(j) : x[pidx(j)];
         }
     }
-    if (!FIRST) group_sync<G>(grp);
+    if (!FIRST || SYNC_IN) group_sync<G>(grp);
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
         const int b = t + G * u;
@@ -198,7 +201,7 @@ struct FftPlan {
     static constexpr int NPASS = P16 + (RLAST > 1 ? 1 : 0);
 };
 
-template <int N, int SIGN, bool SMEM_TW, int P, class In, class Out>
+template <int N, int SIGN, bool SMEM_TW, bool INPLACE, int P, class In, class Out>
 __device__ __forceinline__ void fft_passes(double2 *x, int t, int Ns, const double2 *__restrict__ tw, int grp,
                                            const In &in, const Out &out) {
     constexpr int G = FftPlan<N>::G;
@@ -207,10 +210,11 @@ __device__ __forceinline__ void fft_passes(double2 *x, int t, int Ns, const doub
     constexpr int R = (P < FftPlan<N>::P16) ? 16 : FftPlan<N>::RLAST;
     if constexpr (N <= 16) {
         // one in-register DFT, single pass
-        stockham_pass<N, G, N, SIGN, E, SMEM_TW, true, true>(x, t, 1, tw, grp, in, out);
+        stockham_pass<N, G, N, SIGN, E, SMEM_TW, true, true, INPLACE>(x, t, 1, tw, grp, in, out);
     } else {
-        stockham_pass<N, G, R, SIGN, E, SMEM_TW, P == 0, P == NP - 1>(x, t, Ns, tw, grp, in, out);
-        if constexpr (P + 1 < NP) fft_passes<N, SIGN, SMEM_TW, P + 1>(x, t, Ns * R, tw, grp, in, out);
+        stockham_pass<N, G, R, SIGN, E, SMEM_TW, P == 0, P == NP - 1, INPLACE && P == 0>(x, t, Ns, tw, grp, in,
+                                                                                        out);
+        if constexpr (P + 1 < NP) fft_passes<N, SIGN, SMEM_TW, INPLACE, P + 1>(x, t, Ns * R, tw, grp, in, out);
     }
 }
 
@@ -218,11 +222,13 @@ __device__ __forceinline__ void fft_passes(double2 *x, int t, int Ns, const doub
 // from in(j), outputs (natural order) to out(k, value); x is the group's
 // padded scratch of padded_len(N) complex.  All G threads must call.  When
 // the FFT has more than one pass, x is free again when the call returns.
-template <int N, int SIGN, bool SMEM_TW = false, class In, class Out>
+// INPLACE: `in` reads x (the first pass then holds its writes back until
+// every thread of the group has read its inputs).
+template <int N, int SIGN, bool SMEM_TW = false, bool INPLACE = false, class In, class Out>
 __device__ __forceinline__ void group_fft_io(double2 *x, int t, const double2 *__restrict__ tw, int grp,
                                              const In &in, const Out &out) {
     static_assert(N >= 4 && (N & (N - 1)) == 0, "power of two >= 4");
-    fft_passes<N, SIGN, SMEM_TW, 0>(x, t, 1, tw, grp, in, out);
+    fft_passes<N, SIGN, SMEM_TW, INPLACE, 0>(x, t, 1, tw, grp, in, out);
     if constexpr (FftPlan<N>::NPASS > 1) group_sync<FftPlan<N>::G>(grp);
 }
 
@@ -230,9 +236,7 @@ __device__ __forceinline__ void group_fft_io(double2 *x, int t, const double2 *_
 template <int N, int SIGN, bool SMEM_TW = false>
 __device__ __forceinline__ void group_fft(double2 *x, int t, const double2 *__restrict__ tw, int grp) {
     const ScratchIO io{x};
-    // the first pass reads x into registers before the barrier that precedes
-    // any write of x, so in-place is safe
-    group_fft_io<N, SIGN, SMEM_TW>(x, t, tw, grp, io, io);
+    group_fft_io<N, SIGN, SMEM_TW, true>(x, t, tw, grp, io, io);
 }
 
 // 2D DCT-I (REDFT00 x REDFT00) in place on a symmetric NBK x NBK slice S
@@ -279,6 +283,70 @@ __device__ void dct2_slice(double *S, double2 *scr, const double2 *tw) {
         }
         __syncthreads();
     }
+}
+
+// 2D RODFT00 x REDFT00 in place on an (NBK-2) x NBK slice S (row l, column
+// m, leading dimension NBK): DCT-I of length NBK along m, DST-I of length
+// NBK-2 along l -- the transform of functions odd in kx and even in ky on the
+// interior kx points (FFTW's RODFT00: Y_k = 2 sum_j X_j sin(pi (j+1)(k+1)/(n+1))).
+// Both lengths use complex FFTs of L = 2(NBK-1): the DCT through the even
+// extension of two packed lines, the DST through the odd extension
+// z = [0, X, 0, -reverse(X)], whose transform is -i Y_a + Y_b for the packed
+// pair a + i b.  Same calling rules as dct2_slice.
+template <int NBK>
+__device__ void dst_dct_slice(double *S, double2 *scr, const double2 *tw) {
+    constexpr int L = 2 * (NBK - 1);
+    constexpr int NR = NBK - 2;
+    constexpr int G = FftPlan<L>::G;
+    const int tid = threadIdx.x;
+    const int grp = tid / G;
+    const int t = tid % G;
+    const int ngrp = blockDim.x / G;
+    double2 *x = scr + grp * padded_len(L);
+    // rows: DCT-I along m, NR lines
+#pragma unroll 1
+    for (int p = grp; p < (NR + 1) / 2; p += ngrp) {
+        const int r0 = 2 * p, r1 = 2 * p + 1;
+        const bool two = r1 < NR;
+        double *a = S + r0 * NBK;
+        double *b = S + (two ? r1 : r0) * NBK;
+        auto in = [&](int j) -> double2 {
+            const int c = j < NBK ? j : L - j;
+            return make_double2(a[c], two ? b[c] : 0.0);
+        };
+        auto out = [&](int k, double2 z) {
+            if (k < NBK) {
+                a[k] = z.x;
+                if (two) b[k] = z.y;
+            }
+        };
+        group_fft_io<L, -1, true>(x, t, tw, grp, in, out);
+        if constexpr (FftPlan<L>::NPASS == 1) group_sync<G>(grp);
+    }
+    __syncthreads();
+    // columns: DST-I along l, NBK lines
+#pragma unroll 1
+    for (int p = grp; p < (NBK + 1) / 2; p += ngrp) {
+        const int c0 = 2 * p, c1 = 2 * p + 1;
+        const bool two = c1 < NBK;
+        double *a = S + c0;
+        double *b = S + (two ? c1 : c0);
+        auto in = [&](int j) -> double2 {
+            if (j == 0 || j == NR + 1) return make_double2(0.0, 0.0);
+            if (j <= NR) return make_double2(a[(j - 1) * NBK], two ? b[(j - 1) * NBK] : 0.0);
+            const int r = L - j - 1;
+            return make_double2(-a[r * NBK], two ? -b[r * NBK] : 0.0);
+        };
+        auto out = [&](int k, double2 z) {
+            if (k >= 1 && k <= NR) {
+                a[(k - 1) * NBK] = -z.y;
+                if (two) b[(k - 1) * NBK] = z.x;
+            }
+        };
+        group_fft_io<L, -1, true>(x, t, tw, grp, in, out);
+        if constexpr (FftPlan<L>::NPASS == 1) group_sync<G>(grp);
+    }
+    __syncthreads();
 }
 
 }  // namespace tpsc

@@ -85,6 +85,40 @@ cudaError_t launch_pade_sigma(const GridDev &g, const double2 *S, const double *
 cudaError_t launch_gwn_local(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                              const double *sinf, double mu, double T, double2 *out, cudaStream_t st);
 
+// ---- current-current correlator (bubble + Maki-Thompson) and kx0 -----------
+// K4 = (nbk - 2) nbk interior-kx points, c = l nbk + m for kx = (l+1) pi/(nbk-1),
+// ky = m pi/(nbk-1).
+struct CondDev {
+    int K4 = 0;             // interior-kx points
+    int K4p = 0;            // K4 rounded up to even (column pairs)
+    int nbins = 1;          // angular bins of the k-resolved sums (N_theta_k)
+    int nblk = 0;           // CTAs of the persistent tau kernel
+    int pw = 0;             // partial row width: nbins 2 (Nw0/2+1) + 1
+    double *dek = nullptr;     // [K4]  d eps/d kx
+    double *d2ek = nullptr;    // [K4]  d2 eps/d kx2
+    double *d2line = nullptr;  // [2 nbk] d2 eps/d kx2 on kx = 0, then kx = pi
+    int *bin = nullptr;        // [K4]  angular bin of each point
+    double *tab = nullptr;     // [4 K4] (eps - mu0, A, B, 0) of the h, f0 slices
+    double *hV = nullptr;      // [K4p (Nw0+1)] h V(r, tau), two-column blocks
+    double *f0V = nullptr;     // [K4p (Nw0+1)] f0 V(r, tau), two-column blocks
+    double *pre = nullptr;     // [4 K4p] transformed h, f0 at tau = 0, beta
+    double *dbound = nullptr;  // [4 K4p] dhV(0), dhV(beta), df0V(0), df0V(beta)
+    double *partial = nullptr; // [nblk pw] per-CTA sums
+    double *lines = nullptr;   // [2 nbk] kx0 terms of the kx = 0, pi lines
+    double *out = nullptr;     // [nbins 2 NB] binned, [2 NB] totals, kx0 (NB = Nw0/2+1)
+};
+
+cudaError_t cond_blocks(const GridDev &g, int *blocks);
+// table + h V, f0 V slices + end conditions (fact = U (3 Usp + Uch)/4)
+cudaError_t launch_cond_slices(const GridDev &g, const CondDev &c, const double *V, const double *dtau_chirt0,
+                               double mu0, double T, double fact, cudaStream_t st);
+// per-k pairs -> c.partial (zeroed first)
+cudaError_t launch_cond_tau(const GridDev &g, const CondDev &c, const double2 *S, const double *s2, const double *s3,
+                            const double *sinf, double mu, double T, cudaStream_t st);
+// kx = 0, pi lines and the ordered sum of the partial rows -> c.out
+cudaError_t launch_cond_finish(const GridDev &g, const CondDev &c, const double2 *S, const double *s2,
+                               const double *s3, const double *sinf, double mu, double T, cudaStream_t st);
+
 // ---- layout conversion for the getters ------------------------------------
 // blocked (NJ rows) -> reference layout [j][o], j < nrows
 cudaError_t launch_unblock(const double *src, double *dst, int NJ, int nrows, int n8, cudaStream_t st);
