@@ -182,6 +182,24 @@ int tpsc_chijj(tpsc_ctx *ctx, int n_theta);
 int tpsc_get_chijj(tpsc_ctx *ctx, double *chijj1, double *chijj2, double *kx0, double *chijj1_k,
                    double *chijj2_k);
 
+/* Optical conductivity on the bosonic Matsubara axis from the last tpsc_chijj
+ * (no counterpart in the reference, which stops at chi_jj and kx0):
+ * sigma(iq_n) = (-kx0 - chi_jj(iq_n)) / q_n, q_n = 2 pi n T, n = 1..nq, with
+ * chi_jj = chijj1 + chijj2 (sigma, with vertex correction) and chi_jj =
+ * chijj1 (sigma_bubble).  nq <= Nw0/2; either pointer may be NULL. */
+int tpsc_sigma_iqn(tpsc_ctx *ctx, int nq, double *sigma, double *sigma_bubble);
+/* Continued-fraction Pade continuation of sigma(iq_n), n = 1..Nn, and of
+ * sigma_bubble to z = w + i eta for the Nw real frequencies w:
+ * out [2][Nw] complex interleaved (sigma, then sigma_bubble). */
+int tpsc_sigma_pade(tpsc_ctx *ctx, int Nn, const double *w, int Nw, double eta, double *out);
+/* Batched continued-fraction Pade (the recursion of
+ * generique::pade_cont_frac_coef_rec and generique::pade,
+ * src/generique.cpp:1628-1663): nf functions sampled at x[f][j] with values
+ * y[f][j] (j < Nn, 2 <= Nn <= 4096, complex interleaved) evaluated at the Nz
+ * complex points z: out [nf][Nz] complex interleaved. */
+int tpsc_pade_batch(tpsc_ctx *ctx, int nf, int Nn, const double *x, const double *y, int Nz, const double *z,
+                    double *out);
+
 /* Device time of the last tpsc_solve per stage in ms:
  * {chi0, sum rules, vertex, self energy, traces + mu}, then of the last
  * tpsc_chijj: {h V / f0 V slices + end conditions, per-k tau kernel,

@@ -96,3 +96,66 @@ def test_chijj_bad_arguments():
         c.ctx.call("tpsc_chijj", 0)
     with pytest.raises(NotImplementedError):
         c.calc_chijj_vertex_corr_all_optim(True)
+
+
+def test_sigma_iqn_is_the_kubo_form_of_chijj():
+    g = load_golden("l128_w2048_cond")
+    p = g["p"]
+    c = _cond(p)
+    c.solve()
+    r = c.calc_chijj_vertex_corr_all_optim(False, 3, 1)
+    s, sb = c.sigma_qn(256)
+    qn = 2 * np.pi * np.arange(1, 257) * p["T"]
+    assert np.allclose(s, (-r["kx0"] - r["chijj1"][1:257] - r["chijj2"][1:257]) / qn, rtol=1e-14, atol=0)
+    assert np.allclose(sb, (-r["kx0"] - r["chijj1"][1:257]) / qn, rtol=1e-14, atol=0)
+    # against the reference's chi_jj and kx0
+    ref = (-float(g["kx0"]) - g["chijj1"][1:257] - g["chijj2"][1:257]) / qn
+    scale = np.max(np.abs(g["chijj1"])) / qn
+    assert np.all(np.abs(s - ref) <= 1e-10 * scale)
+
+
+def test_pade_batch_reproduces_rational_functions():
+    """A rational function with three poles is its own Pade approximant: the
+    batched continuation recovers it on the real axis, and matches the oracle's
+    restatement of generique::pade_cont_frac_coef_rec / pade."""
+    from oracle import tpsc_oracle as O
+    from tpsc_conductivity_b200.api import pade_batch
+
+    T = 0.1
+    poles = [np.array([0.3 - 0.2j, -1.1 - 0.5j, 2.0 - 0.1j]), np.array([0.7 - 0.3j, 1.5 - 0.05j, -0.4 - 1.0j])]
+    res = [np.array([1.0, 0.5 + 0.2j, 0.25]), np.array([0.3, 0.1 - 0.1j, 2.0])]
+
+    def f(k, z):
+        return np.sum(res[k][:, None] / (z[None, :] - poles[k][:, None]), axis=0)
+
+    z = np.linspace(0.0, 10.0, 2000) + 0.05j
+    for Nn in (8, 16, 32):
+        x = 1j * 2 * np.pi * np.arange(1, Nn + 1) * T
+        y = np.stack([f(0, x), f(1, x)])
+        out = pade_batch(x, y, z)
+        for k in range(2):
+            exact = f(k, z)
+            assert np.max(np.abs(out[k] - exact)) <= 1e-9 * np.max(np.abs(exact)), (Nn, k)
+            coef = O.pade_coefficients(y[k], x)
+            ora = np.array([O.pade_eval(zz, x, coef) for zz in z[::50]])
+            assert np.max(np.abs(out[k][::50] - ora)) <= 1e-9 * np.max(np.abs(ora)), (Nn, k)
+
+
+def test_sigma_pade_interpolates_the_matsubara_data():
+    from tpsc_conductivity_b200.api import pade_batch
+
+    g = load_golden("l32_w256_u4_tp")
+    p = g["p"]
+    c = _cond(p)
+    c.solve()
+    c.calc_chijj_vertex_corr_all_optim()
+    Nn = 64
+    s, sb = c.sigma_qn(Nn)
+    x = 1j * 2 * np.pi * np.arange(1, Nn + 1) * p["T"]
+    back = pade_batch(x, np.stack([s, sb]).astype(complex), x)
+    assert np.max(np.abs(back[0] - s) / np.abs(s)) <= 1e-11
+    assert np.max(np.abs(back[1] - sb) / np.abs(sb)) <= 1e-11
+    w = np.linspace(0.0, 10.0, 2000)
+    sw, sbw = c.sigma_pade(w, Nn, 0.05)
+    ref = pade_batch(x, np.stack([s, sb]).astype(complex), w + 0.05j)
+    assert np.array_equal(sw, ref[0]) and np.array_equal(sbw, ref[1])

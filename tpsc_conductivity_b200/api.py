@@ -243,10 +243,34 @@ class CondOpt(Green):
                 "chijj2_k": k2.reshape(NB, nb)}
 
     def sigma_qn(self, nq=None):
-        """sigma(iq_n) = (-kx0 - chi_jj(iq_n)) / q_n, n = 1..nq (the Kubo form;
-        the reference stops at chi_jj and kx0)."""
-        r = self.chijj()
-        chi = r["chijj1"] + r["chijj2"]
-        nq = len(chi) - 1 if nq is None else nq
-        qn = 2 * np.pi * np.arange(1, nq + 1) * self.tem
-        return (-r["kx0"] - chi[1:nq + 1]) / qn
+        """sigma(iq_n) = (-kx0 - chi_jj(iq_n)) / q_n, n = 1..nq, with and without
+        the vertex correction (the Kubo form; the reference stops at chi_jj and
+        kx0).  Returns (sigma, sigma_bubble)."""
+        nk0, nw0, nbk, n8 = self.dims()
+        nq = nw0 // 2 if nq is None else int(nq)
+        s, sb = np.zeros(nq), np.zeros(nq)
+        self.ctx.call("tpsc_sigma_iqn", nq, _dptr(s), _dptr(sb))
+        return s, sb
+
+    def sigma_pade(self, w, Nn=64, eta=0.0):
+        """Pade continuation of sigma(iq_n), n = 1..Nn, to w + i eta:
+        (sigma(w), sigma_bubble(w)) complex arrays."""
+        w = np.ascontiguousarray(np.atleast_1d(np.asarray(w, dtype=np.float64)))
+        out = np.zeros((2, w.size), dtype=np.complex128)
+        self.ctx.call("tpsc_sigma_pade", int(Nn), _dptr(w), int(w.size), float(eta), _dptr(out.view(np.float64)))
+        return out[0], out[1]
+
+
+def pade_batch(x, y, z, ctx=None):
+    """Batched continued-fraction Pade on the GPU: functions sampled at x[f, j]
+    with values y[f, j], evaluated at the points z; returns [nf, len(z)]."""
+    ctx = ctx or Context()
+    x = np.ascontiguousarray(np.atleast_2d(np.asarray(x, dtype=np.complex128)))
+    y = np.ascontiguousarray(np.atleast_2d(np.asarray(y, dtype=np.complex128)))
+    z = np.ascontiguousarray(np.atleast_1d(np.asarray(z, dtype=np.complex128)))
+    nf, Nn = y.shape
+    x = np.ascontiguousarray(np.broadcast_to(x, (nf, Nn)))
+    out = np.zeros((nf, z.size), dtype=np.complex128)
+    ctx.call("tpsc_pade_batch", nf, Nn, _dptr(x.view(np.float64)), _dptr(y.view(np.float64)), int(z.size),
+             _dptr(z.view(np.float64)), _dptr(out.view(np.float64)))
+    return out

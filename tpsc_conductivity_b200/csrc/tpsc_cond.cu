@@ -702,6 +702,46 @@ __global__ void k_cond_finish(const double *__restrict__ partial, int nblk, int 
 }
 
 // ---------------------------------------------------------------------------
+// batched continued-fraction Pade (Vidberg-Serene), one CTA per function:
+// g_0(l) = y_l, g_m(l) = (g_{m-1}(m-1) - g_{m-1}(l)) / ((x_l - x_{m-1}) g_{m-1}(l)),
+// a_m = g_m(m) (generique::pade_cont_frac_coef_rec, src/generique.cpp:1649-1663),
+// computed in shared memory, one barrier per order m; then every thread
+// evaluates the continued fraction at its energies with the recurrence of
+// generique::pade (src/generique.cpp:1628-1646).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+    k_pade_batch(const double2 *__restrict__ x, const double2 *__restrict__ y, int Nn, const double2 *__restrict__ z,
+                 int Nz, double2 *__restrict__ out) {
+    extern __shared__ __align__(16) double2 sp[];
+    double2 *xs = sp, *g = sp + Nn;
+    const int f = blockIdx.x;
+    for (int l = threadIdx.x; l < Nn; l += blockDim.x) {
+        xs[l] = x[(size_t)f * Nn + l];
+        g[l] = y[(size_t)f * Nn + l];
+    }
+    __syncthreads();
+    for (int m = 1; m < Nn; ++m) {
+        const double2 gm = g[m - 1], xm = xs[m - 1];
+        for (int l = m + threadIdx.x; l < Nn; l += blockDim.x)
+            g[l] = cdiv(csub(gm, g[l]), cmul(csub(xs[l], xm), g[l]));
+        __syncthreads();
+    }
+    for (int iz = threadIdx.x; iz < Nz; iz += blockDim.x) {
+        const double2 zz = z[iz];
+        double2 A = make_double2(1.0, 0.0);
+        double2 B = cadd(make_double2(1.0, 0.0), cmul(csub(zz, xs[0]), g[1]));
+        double2 q = cdiv(A, B);
+        for (int j = 3; j <= Nn; ++j) {
+            const double2 t = cmul(csub(zz, xs[j - 2]), g[j - 1]);
+            A = cadd(make_double2(1.0, 0.0), cdiv(t, A));
+            B = cadd(make_double2(1.0, 0.0), cdiv(t, B));
+            q = cdiv(cmul(q, A), B);
+        }
+        out[(size_t)f * Nz + iz] = cmul(q, g[0]);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // launch wrappers per compiled size
 // ---------------------------------------------------------------------------
 template <int NBK>
@@ -790,6 +830,16 @@ cudaError_t launch_cond_slices(const GridDev &g, const CondDev &c, const double 
 cudaError_t launch_cond_tau(const GridDev &g, const CondDev &c, const double2 *S, const double *s2, const double *s3,
                             const double *sinf, double mu, double T, cudaStream_t st) {
     return dispatch_nw<RunCondTau>(g.nw0, &g, &c, S, s2, s3, sinf, mu, T, st);
+}
+
+cudaError_t launch_pade_batch(const double2 *x, const double2 *y, int nf, int Nn, const double2 *z, int Nz,
+                              double2 *out, cudaStream_t st) {
+    if (nf < 1 || Nn < 2 || Nn > kPadeBatchMax || Nz < 1) return cudaErrorInvalidValue;
+    const size_t sm = (size_t)2 * Nn * sizeof(double2);
+    cudaError_t e = set_smem(k_pade_batch, sm);
+    if (e != cudaSuccess) return e;
+    k_pade_batch<<<nf, 256, sm, st>>>(x, y, Nn, z, Nz, out);
+    return launched();
 }
 
 cudaError_t launch_cond_finish(const GridDev &g, const CondDev &c, const double2 *S, const double *s2,

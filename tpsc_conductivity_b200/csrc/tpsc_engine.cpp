@@ -1259,6 +1259,69 @@ int tpsc_get_chijj(tpsc_ctx *ctx, double *chijj1, double *chijj2, double *kx0, d
     return TPSC_OK;
 }
 
+int tpsc_sigma_iqn(tpsc_ctx *ctx, int nq, double *sigma, double *sigma_bubble) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    const Grid *g = ctx->cur;
+    if (g->cond_bins == 0) return fail(ctx, TPSC_ERR_STATE, "tpsc_chijj has not been run on the current grid");
+    const int NB = g->d.nw0 / 2 + 1;
+    if (nq < 1 || nq > NB - 1) return fail(ctx, TPSC_ERR_ARG, "need 1 <= nq <= Nw0/2");
+    const double *tot = g->cond_host.data() + (size_t)g->cond_bins * 2 * NB;
+    const double kx0 = tot[2 * NB];
+    for (int n = 1; n <= nq; ++n) {
+        const double qn = 2.0 * PI * n * ctx->T;
+        if (sigma) sigma[n - 1] = (-kx0 - (tot[n] + tot[NB + n])) / qn;
+        if (sigma_bubble) sigma_bubble[n - 1] = (-kx0 - tot[n]) / qn;
+    }
+    return TPSC_OK;
+}
+
+int pade_batch(tpsc_ctx *ctx, int nf, int Nn, const double *x, const double *y, int Nz, const double *z,
+               double *out) {
+    const size_t bx = (size_t)nf * Nn * sizeof(double2), bz = (size_t)Nz * sizeof(double2),
+                 bo = (size_t)nf * Nz * sizeof(double2);
+    int rc = ensure_stage(ctx, 2 * bx + bz + bo);
+    if (rc) return rc;
+    char *base = (char *)ctx->stage;
+    double2 *dx = (double2 *)base, *dy = (double2 *)(base + bx), *dz = (double2 *)(base + 2 * bx),
+            *dout = (double2 *)(base + 2 * bx + bz);
+    CK(cudaMemcpyAsync(dx, x, bx, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(dy, y, bx, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(dz, z, bz, cudaMemcpyHostToDevice, ctx->st));
+    CK(launch_pade_batch(dx, dy, nf, Nn, dz, Nz, dout, ctx->st));
+    CK(cudaMemcpyAsync(out, dout, bo, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return TPSC_OK;
+}
+
+int tpsc_pade_batch(tpsc_ctx *ctx, int nf, int Nn, const double *x, const double *y, int Nz, const double *z,
+                    double *out) {
+    if (!ctx) return fail(nullptr, TPSC_ERR_ARG, "null context");
+    if (!x || !y || !z || !out || nf < 1 || Nn < 2 || Nn > kPadeBatchMax || Nz < 1)
+        return fail(ctx, TPSC_ERR_ARG, "need nf >= 1, 2 <= Nn <= 4096, Nz >= 1 and non-NULL arrays");
+    cudaSetDevice(ctx->device);
+    return pade_batch(ctx, nf, Nn, x, y, Nz, z, out);
+}
+
+int tpsc_sigma_pade(tpsc_ctx *ctx, int Nn, const double *w, int Nw, double eta, double *out) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    if (!w || !out || Nw < 1 || Nn < 2) return fail(ctx, TPSC_ERR_ARG, "need Nn >= 2, Nw >= 1");
+    std::vector<double> s(Nn), sb(Nn);
+    if ((rc = tpsc_sigma_iqn(ctx, Nn, s.data(), sb.data()))) return rc;
+    std::vector<double2> x(2 * Nn), y(2 * Nn), z(Nw);
+    for (int j = 0; j < Nn; ++j) {
+        const double qn = 2.0 * PI * (j + 1) * ctx->T;
+        x[j] = x[Nn + j] = make_double2(0.0, qn);
+        y[j] = make_double2(s[j], 0.0);
+        y[Nn + j] = make_double2(sb[j], 0.0);
+    }
+    for (int i = 0; i < Nw; ++i) z[i] = make_double2(w[i], eta);
+    cudaSetDevice(ctx->device);
+    return pade_batch(ctx, 2, Nn, (const double *)x.data(), (const double *)y.data(), Nw, (const double *)z.data(),
+                      out);
+}
+
 int tpsc_stage_times(tpsc_ctx *ctx, double *ms, int n) {
     if (!ctx || !ms) return fail(ctx, TPSC_ERR_ARG, "bad arguments");
     for (int i = 0; i < n && i < 8; ++i) ms[i] = ctx->stage_ms[i];

@@ -119,6 +119,12 @@ cudaError_t launch_cond_tau(const GridDev &g, const CondDev &c, const double2 *S
 cudaError_t launch_cond_finish(const GridDev &g, const CondDev &c, const double2 *S, const double *s2,
                                const double *s3, const double *sinf, double mu, double T, cudaStream_t st);
 
+// Batched continued-fraction Pade of nf functions sampled at Nn points
+// (x, y: [nf][Nn]) evaluated at Nz shared points: out [nf][Nz].
+constexpr int kPadeBatchMax = 4096;
+cudaError_t launch_pade_batch(const double2 *x, const double2 *y, int nf, int Nn, const double2 *z, int Nz,
+                              double2 *out, cudaStream_t st);
+
 // ---- layout conversion for the getters ------------------------------------
 // blocked (NJ rows) -> reference layout [j][o], j < nrows
 cudaError_t launch_unblock(const double *src, double *dst, int NJ, int nrows, int n8, cudaStream_t st);
