@@ -47,3 +47,52 @@ def test_reference_main_runs_on_the_dropin(tmp_path):
     assert np.allclose(A[:, 2:], g["mdc_A"], rtol=1e-6, atol=1e-11)
     fs = np.loadtxt(glob.glob(str(run / "FS_inter_AkF_Pade_*"))[0])
     assert np.allclose(fs[:, 2], g["fs_inter_pade"][:, 2], rtol=1e-6)
+
+
+COND_BIN = os.path.join(ROOT, "tpsc_conductivity_b200", "dropin", "_build", "cond_main_b200")
+
+
+@pytest.mark.gpu
+def test_conductivity_block_writes_the_reference_files(tmp_path):
+    """The conductivity block of src/tpsc_main.cpp (cond_opt +
+    calc_chijj_vertex_corr_all_optim) on the drop-in classes writes
+    chijj1_qn_*, chijj2_qn_*, chijj_with_vc1_qn_*, kx0_*, kx0_bin_* and the
+    angle-resolved chijj*_k_qn_* / chijj*_k_tot_qn_* with the reference's
+    numbers."""
+    if not os.path.exists(COND_BIN):
+        pytest.skip("cond_main_b200 is built by make -C tpsc_conductivity_b200/dropin")
+    g = load_golden("l32_w256_theta3")
+    p = g["p"]
+    nt = g["chijj1_k"].shape[1]
+    run = tmp_path / "a" / "b"
+    run.mkdir(parents=True)
+    (tmp_path / "input.dat").write_text(
+        f"{p['U']} {p['tp']} {p['tpp']} {p['t3']} {p['n']} {p['T']} {p['nk0']} {p['Nw0']} 0 3 {nt}\n")
+    r = subprocess.run([COND_BIN], cwd=run, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "difference relative avec -k0" in r.stdout
+
+    def one(prefix):
+        return glob.glob(str(run / prefix))[0]
+
+    s1, s2 = np.max(np.abs(g["chijj1"])), np.max(np.abs(g["chijj2"]))
+    c1 = np.loadtxt(one("chijj1_qn_*"))
+    c2 = np.loadtxt(one("chijj2_qn_*"))
+    cv = np.loadtxt(one("chijj_with_vc1_qn_*"))
+    assert np.array_equal(c1[:, 0], np.arange(p["Nw0"] // 2 + 1))
+    assert np.max(np.abs(c1[:, 1] - g["chijj1"])) <= 1e-10 * s1
+    assert np.max(np.abs(c2[:, 1] - g["chijj2"])) <= 1e-10 * s2
+    assert np.max(np.abs(cv[:, 1] - (g["chijj1"] + g["chijj2"]))) <= 1e-10 * s1
+    kx0 = float(open(one("kx0_[0-9]*")).read())
+    assert abs(kx0 - float(g["kx0"])) <= 1e-10 * abs(float(g["kx0"]))
+    kb = np.fromfile(one("kx0_bin_*"), dtype=np.float64)
+    assert kb.size == 1 and kb[0] == kx0
+    k1 = np.loadtxt(one("chijj1_k_qn_*"))
+    k2 = np.loadtxt(one("chijj2_k_qn_*"))
+    assert np.array_equal(k1[:nt, 1], np.arange(1, nt + 1))
+    assert np.max(np.abs(k1[:, 2].reshape(-1, nt) - g["chijj1_k"])) <= 1e-10 * s1
+    assert np.max(np.abs(k2[:, 2].reshape(-1, nt) - g["chijj2_k"])) <= 1e-10 * s2
+    t1 = np.loadtxt(one("chijj1_k_tot_qn_*"))
+    assert np.allclose(t1[:, 1], t1[:, 2], rtol=1e-12, atol=0)
+    # the Fermi-surface files of find_FS_inter come first, as in the reference
+    assert glob.glob(str(run / "FS_inter_AkF_Pade_*"))

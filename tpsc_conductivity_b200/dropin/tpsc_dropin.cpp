@@ -455,6 +455,153 @@ void green::Gwn_local() {
     file.close();
 }
 
+// Sigma(k, i k_n) at the listed k points, n <= Nwn (green::save_self_ikn,
+// src/green.cpp:127-180)
+void green::save_self_ikn(int *k_save, int nk_save, int Nwn) {
+    if (!have_self) {
+        set_keep_chiqw(false);
+        calc_Self_FFT_spline();
+        traceSelfG();
+        green::find_mu();
+    }
+    if (!have_self) return;
+    const size_t n8 = (size_t)nbk * (nbk + 1) / 2;
+    std::vector<double> S((size_t)2 * n8 * (nbw / 2)), c2(n8), c3(n8);
+    if (!check(tpsc_get_self(ctx_, S.data(), c2.data(), c3.data(), NULL), "save_self_ikn")) return;
+    char name[200];
+    sprintf(name, "./self_k_ikn_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat", U, tp, tpp, t3, density, tem,
+            2 * (nbk - 1), nbw);
+    fstream file;
+    file.open(name, ios::out);
+    file << setprecision(16) << setiosflags(ios::left) << setiosflags(ios::scientific);
+    const double pi = acos(-1.0);
+    for (int j = 0; j <= Nwn && j < nbw / 2; j++) {
+        const double kn = (2.0 * j + 1) * pi * tem;
+        for (int p = 0; p < nk_save; p++) {
+            long x = k_save[2 * p], y = k_save[2 * p + 1];
+            if (y > x) std::swap(x, y);
+            if (x >= 0 && x < nbk && y >= 0) {
+                const size_t o = y + (x * (x + 1)) / 2;
+                const double re = -c2[o] / (kn * kn) + S[2 * (o + j * n8)] / (kn * kn * kn * kn);
+                const double im = -Sigma_inf / kn + c3[o] / (kn * kn * kn) + S[2 * (o + j * n8) + 1] / (kn * kn * kn * kn);
+                file << setw(10) << j << setw(10) << x << setw(10) << y << setw(25) << re << im << endl;
+            }
+        }
+    }
+    file.close();
+}
+
 // ---------------------------------------------------------------------------
 cond_opt::cond_opt(int nk0, int Nw0, double n, double T, double eta0, double *params)
-    : green(nk0, Nw0, n, T, eta0, params) {}
+    : green(nk0, Nw0, n, T, eta0, params), chijj1_qn(NULL), chijj2_qn(NULL), kx0(0.0) {}
+
+cond_opt::~cond_opt() {
+    delete[] chijj1_qn;
+    delete[] chijj2_qn;
+}
+
+// cond_opt::calc_chijj_vertex_corr_all_optim (src/cond_opt.cpp:2537-4286):
+// Sigma and mu first when missing, Sigma at the listed k points, the Fermi
+// surface files, then chi_jj on the device and the reference's result files
+// (chijj*_k_qn_*, chijj*_k_tot_qn_*, kx0_*, kx0_bin_*, chijj1_qn_*,
+// chijj_with_vc1_qn_*, chijj2_qn_*) with its column layouts and stdout lines.
+// mmin does not enter the bubble + Maki-Thompson result in the reference.
+void cond_opt::calc_chijj_vertex_corr_all_optim(bool chi3, int mmin, int N_theta_k, int *k_chijj, int nk_chijj) {
+    (void)mmin;
+    cout << "calcul de chijj par calc_chijj_vertex_corr_all_optim()\n";
+    const int nw = nbw / 2, nk0 = 2 * (nbk - 1);
+    if (!have_self) {
+        calc_Self_FFT_spline();
+        traceSelfG();
+        green::find_mu();
+    }
+    if (!mu_calcule) {
+        cout << "calc_chijj_vertex_corr_all_optim(): mu non calcule\n";
+        return;
+    }
+    if (k_chijj && nk_chijj) save_self_ikn(k_chijj, nk_chijj, nw / 16);
+    find_FS_inter();
+    if (N_theta_k < 1) N_theta_k = 1;
+    if (!check(tpsc_chijj(ctx_, N_theta_k), "calc_chijj_vertex_corr_all_optim")) return;
+    delete[] chijj1_qn;
+    delete[] chijj2_qn;
+    chijj1_qn = new double[nw + 1];
+    chijj2_qn = new double[nw + 1];
+    std::vector<double> k1((size_t)(nw + 1) * N_theta_k), k2((size_t)(nw + 1) * N_theta_k);
+    if (!check(tpsc_get_chijj(ctx_, chijj1_qn, chijj2_qn, &kx0, k1.data(), k2.data()), "tpsc_get_chijj")) return;
+
+    char name[200];
+    fstream file, file2, file3, file4;
+    const double dn = density;
+    sprintf(name, "./chijj1_k_qn_%5.3f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat", U, tp, tpp, t3, dn, tem, nk0, nbw);
+    file.open(name, ios::out);
+    file << setprecision(16) << setiosflags(ios::left) << setiosflags(ios::scientific);
+    sprintf(name, "./chijj1_k_tot_qn_%5.3f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat", U, tp, tpp, t3, dn, tem, nk0,
+            nbw);
+    file2.open(name, ios::out);
+    file2 << setprecision(16) << setiosflags(ios::left) << setiosflags(ios::scientific);
+    sprintf(name, "./chijj2_k_qn_%5.3f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat", U, tp, tpp, t3, dn, tem, nk0, nbw);
+    file3.open(name, ios::out);
+    file3 << setprecision(16) << setiosflags(ios::left) << setiosflags(ios::scientific);
+    sprintf(name, "./chijj2_k_tot_qn_%5.3f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat", U, tp, tpp, t3, dn, tem, nk0,
+            nbw);
+    file4.open(name, ios::out);
+    file4 << setprecision(16) << setiosflags(ios::left) << setiosflags(ios::scientific);
+    for (int j = 0; j <= nw; j++) {
+        double t1 = 0, t2 = 0;
+        for (int p = 0; p < N_theta_k; p++) {
+            t1 += k1[p + (size_t)j * N_theta_k];
+            t2 += k2[p + (size_t)j * N_theta_k];
+        }
+        file2 << setw(10) << j << setw(30) << t1 << setw(30) << chijj1_qn[j] << t1 / chijj1_qn[j] << '\n';
+        file4 << setw(10) << j << setw(30) << t2 << setw(30) << chijj2_qn[j] << t2 / chijj2_qn[j] << '\n';
+        for (int p = 0; p < N_theta_k; p++) {
+            file << setw(10) << j << setw(10) << p + 1 << k1[p + (size_t)j * N_theta_k] << '\n';
+            file3 << setw(10) << j << setw(10) << p + 1 << k2[p + (size_t)j * N_theta_k] << '\n';
+        }
+    }
+    file.close();
+    file2.close();
+    file3.close();
+    file4.close();
+
+    sprintf(name, "kx0_%5.3f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat", U, tp, tpp, t3, dn, tem, nk0, nbw);
+    file.open(name, ios::out);
+    file << setprecision(16) << setiosflags(ios::left) << setiosflags(ios::scientific) << kx0 << '\n';
+    file.close();
+    sprintf(name, "kx0_bin_%5.3f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat", U, tp, tpp, t3, dn, tem, nk0, nbw);
+    file.open(name, ios::out | ios::binary);
+    file.write((char *)&kx0, sizeof(kx0));
+    file.close();
+
+    for (int j = 0; j <= nw; j++)
+        if (chijj1_qn[j] < 0.0) {
+            cout << "attention! valeur non-physique de chi_jj\n";
+            cout << setw(30) << chijj1_qn[j] << '\n';
+            break;
+        }
+    sprintf(name, "./chijj1_qn_%5.3f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat", U, tp, tpp, t3, dn, tem, nk0, nbw);
+    file.open(name, ios::out);
+    file << setprecision(16) << setiosflags(ios::left) << setiosflags(ios::scientific);
+    sprintf(name, "./chijj_with_vc1_qn_%5.3f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat", U, tp, tpp, t3, dn, tem,
+            nk0, nbw);
+    file2.open(name, ios::out);
+    file2 << setprecision(16) << setiosflags(ios::left) << setiosflags(ios::scientific);
+    sprintf(name, "./chijj2_qn_%5.3f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d.dat", U, tp, tpp, t3, dn, tem, nk0, nbw);
+    file4.open(name, ios::out);
+    file4 << setprecision(16) << setiosflags(ios::left) << setiosflags(ios::scientific);
+    for (int j = 0; j <= nw; j++) {
+        file << setw(10) << j << chijj1_qn[j] << '\n';
+        file4 << setw(10) << j << chijj2_qn[j] << '\n';
+        file2 << setw(10) << j << chijj1_qn[j] + chijj2_qn[j] << '\n';
+    }
+    file.close();
+    file2.close();
+    file4.close();
+    cout << "-k0:  " << -kx0 << '\n';
+    cout << "chijj1(iqn=0):  " << chijj1_qn[0] << '\n';
+    cout << "chijj2(iqn=0):  " << chijj2_qn[0] << '\n';
+    cout << "chijj1(iqn=0)+chijj2(iqn=0):  " << chijj1_qn[0] + chijj2_qn[0] << '\n';
+    cout << "difference relative avec -k0:  " << (chijj1_qn[0] + chijj2_qn[0] + kx0) / kx0 << '\n';
+    if (chi3) cout << "calc_chijj_vertex_corr_all_optim(): la seconde correction de vertex (chi3) n'est pas disponible\n";
+}

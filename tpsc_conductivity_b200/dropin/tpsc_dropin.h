@@ -117,6 +117,7 @@ public:
     void find_FS_inter();
     void MDC(int *n, int Nn, double w, double *eta, int Neta, bool use_Pade = false);
     void Gwn_local();
+    void save_self_ikn(int *k_save, int nk_save, int Nwn);
 
 protected:
     double eta, mu, Sigma_inf;
@@ -127,6 +128,14 @@ protected:
 class cond_opt : public green {
 public:
     cond_opt(int nk0 = 8, int Nw0 = 256, double n = 1.0, double T = 1.0, double eta = 0.1, double *params = NULL);
+    virtual ~cond_opt();
+    // bubble + Maki-Thompson branch; chi3 = true (second vertex correction)
+    // prints that it is not available after the bubble + Maki-Thompson files
+    void calc_chijj_vertex_corr_all_optim(bool chi3, int mmin, int N_theta_k, int *k_chijj, int nk_chijj);
+
+protected:
+    double *chijj1_qn, *chijj2_qn;  // [Nw0/2 + 1]
+    double kx0;
 };
 
 #endif
