@@ -148,6 +148,30 @@ def test_newton_form_same_roots(ctx, name):
     assert sc["evals_sp"] + sc["evals_ch"] <= 20 and sc["evals_mu"] <= 12
 
 
+@pytest.mark.parametrize("name", ["l32_w256_u4_tp", "l64_w1024_u4", "l128_w2048_cond"])
+def test_newton_series_sum_rule_equals_full_sum(ctx, name):
+    """The Newton form sums the high frequencies of the sum rule as a power
+    series in U from precomputed moments of chi0; it agrees with the term-by-
+    term sum (the reference form) to rounding, across the whole spin bracket
+    and well beyond the charge root."""
+    from tpsc_conductivity_b200 import _lib
+
+    g = load_golden(name)
+    p, s = g["p"], g["s"]
+    gr = make(ctx, p)
+    gr.calc_chiqw_FFT_spline()
+    umax = 2.0 / gr.scalars()["chi0max"]
+    cases = [(0, f * umax) for f in (0.0, 0.01, 0.3, 0.9, 0.999)] + [(1, f * s["Uch"]) for f in (0.0, 0.2, 1.0, 5.0)]
+    for ch, U in cases:
+        gr.set_form(_lib.FORM_REFERENCE)
+        t0, d0 = gr.traceDiffChi(ch, U)
+        gr.set_form(_lib.FORM_NEWTON)
+        t1, d1 = gr.traceDiffChi(ch, U)
+        gr.set_form(_lib.FORM_REFERENCE)
+        assert abs(t1 - t0) <= 1e-13 * max(abs(t0), 1e-3), (ch, U, t0, t1)
+        assert abs(d1 - d0) <= 1e-12 * abs(d0), (ch, U, d0, d1)
+
+
 @pytest.mark.parametrize("name", ["l32_w512_u2", "l16_w128_n110", "l16_w64_half"])
 def test_continuation_matches_reference(ctx, name):
     """Pade / polynomial continuation (green::MDC, find_FS_inter) and

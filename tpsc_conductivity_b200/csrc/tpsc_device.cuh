@@ -17,7 +17,7 @@ cudaError_t launched(int n = 1);
 namespace {
 
 constexpr double kPi = 3.141592653589793;  // == acos(-1.0) in double
-constexpr int kSliceThreads = 256;
+constexpr int kSliceThreads = 352;  // 22 groups of 16: the 65 line pairs of a 129-point pass in 3 rounds
 constexpr int kTauThreads = 256;
 constexpr int kWarm = 40;  // spline sweep warm-up: carry error <= 0.268^40
 
@@ -64,7 +64,11 @@ struct SliceSmem {
     static constexpr size_t slice_bytes = (size_t)NBK * NBK * sizeof(double);
     static constexpr size_t scr_off = (slice_bytes + 15) & ~(size_t)15;
     static constexpr size_t tw_off = scr_off + (size_t)NGRP * padded_len(L) * sizeof(double2);
-    static constexpr size_t bytes = tw_off + (size_t)L * sizeof(double2);
+    // the twiddles stay in global memory (read through L1) when shared memory
+    // is full: the slice and the groups' FFT scratch come first
+    static constexpr bool smem_tw = tw_off + (size_t)L * sizeof(double2) <= 232448;
+    static constexpr size_t bytes = tw_off + (smem_tw ? (size_t)L * sizeof(double2) : 0);
+    static_assert(bytes <= 232448, "slice does not fit in shared memory");
 };
 
 template <int NBK>
@@ -72,10 +76,11 @@ __device__ __forceinline__ double2 *slice_scratch(double *S) {
     return reinterpret_cast<double2 *>(reinterpret_cast<char *>(S) + SliceSmem<NBK>::scr_off);
 }
 
-// the L-point twiddle table staged in shared memory behind the FFT scratch;
-// the first __syncthreads of the kernel publishes it
+// the L-point twiddle table staged in shared memory behind the FFT scratch
+// (the first __syncthreads of the kernel publishes it), or the global table
 template <int NBK>
 __device__ __forceinline__ const double2 *slice_twiddles(double *S, const double2 *__restrict__ tw) {
+    if constexpr (!SliceSmem<NBK>::smem_tw) return tw;
     double2 *t = reinterpret_cast<double2 *>(reinterpret_cast<char *>(S) + SliceSmem<NBK>::tw_off);
     for (int i = threadIdx.x; i < SliceSmem<NBK>::L; i += blockDim.x) t[i] = __ldg(&tw[i]);
     return t;

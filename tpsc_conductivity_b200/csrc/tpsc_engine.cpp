@@ -283,6 +283,13 @@ struct Grid {
     double2 *S = nullptr;         // blocked Nw0/2       coefficient of 1/z^4
     double *s2 = nullptr, *s3 = nullptr, *s4 = nullptr, *sinf = nullptr;
     bool have_chi0 = false, have_V = false, have_S = false;
+    // Newton form: moments of chi0 for the high-frequency sum-rule series
+    double *mom = nullptr, *cmax = nullptr;  // device [nb][kMomP], [nb]
+    bool have_mom = false;
+    std::vector<long double> mom_suf;        // [(nb + 1) kMomP] sums over frequencies >= j
+    std::vector<double> cmax_suf;            // [nb + 1] max |chi| over frequencies >= j
+    long double tail_mom[kMomP] = {0};       // the same moments of the Matsubara tail n > Nw0/2
+    double tail_max = 0.0;                   // max |chi| over the tail
     double tailq_T = -1.0;         // temperature the tail power sums were built for
     double tailq_host[kTailQ] = {0};
     std::vector<void *> allocs;
@@ -302,7 +309,8 @@ struct tpsc_ctx {
     int form = TPSC_FORM_REFERENCE;
     cudaStream_t st = nullptr;
     Reduce red;
-    double *h_res = nullptr;  // pinned, 8 doubles
+    Reduce redm;              // moment sums: partial [(2 kMomP + 1) kMaxBlocks], result [32]
+    double *h_res = nullptr;  // pinned, 32 doubles
     // model
     bool have_model = false;
     int nk0 = 0, Nw0 = 0;
@@ -485,6 +493,8 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
     A(dalloc(g, &g->s3, n8));
     A(dalloc(g, &g->s4, n8));
     A(dalloc(g, &g->sinf, 1));
+    A(dalloc(g, &g->mom, nb * kMomP));
+    A(dalloc(g, &g->cmax, nb));
 #undef A
     if (e != cudaSuccess) {
         free_grid(g);
@@ -496,8 +506,9 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
 }
 
 // device scalar readback after a reduction launched on ctx->st
-int read_result(tpsc_ctx *ctx, int count, double *out) {
-    CK(cudaMemcpyAsync(ctx->h_res, ctx->red.result, count * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+int read_result(tpsc_ctx *ctx, int count, double *out, const double *src = nullptr) {
+    CK(cudaMemcpyAsync(ctx->h_res, src ? src : ctx->red.result, count * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     for (int i = 0; i < count; ++i) out[i] = ctx->h_res[i];
     return TPSC_OK;
@@ -599,17 +610,78 @@ int run_chi0(tpsc_ctx *ctx) {
     ctx->scal[TPSC_S_QMAX0] = r[1];
     ctx->scal[TPSC_S_QMAX1] = r[2];
     g->have_chi0 = true;
-    g->have_V = g->have_S = false;
+    g->have_V = g->have_S = g->have_mom = false;
     if (!std::isfinite(r[0]) || r[0] <= 0.0) return fail(ctx, TPSC_ERR_NONFINITE, "chi0(q, 0) has no positive maximum");
     return TPSC_OK;
 }
 
+// Per-frequency moments of chi0 and their sums over the frequencies >= j
+// (long double), for the high-frequency series of the Newton-form sum rule.
+int ensure_moments(tpsc_ctx *ctx, Grid *g) {
+    if (g->have_mom) return TPSC_OK;
+    const GridDev &d = g->d;
+    const int nb = d.nb;
+    CK(launch_chi0_moments(d, g->chiq, g->mom, g->cmax, ctx->st));
+    std::vector<double> m((size_t)nb * kMomP), c(nb);
+    CK(cudaMemcpyAsync(m.data(), g->mom, m.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(c.data(), g->cmax, c.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    g->mom_suf.assign((size_t)(nb + 1) * kMomP, 0.0L);
+    g->cmax_suf.assign(nb + 1, 0.0);
+    for (int j = nb - 1; j >= 0; --j) {
+        for (int k = 0; k < kMomP; ++k)
+            g->mom_suf[(size_t)j * kMomP + k] = g->mom_suf[(size_t)(j + 1) * kMomP + k] + m[(size_t)j * kMomP + k];
+        g->cmax_suf[j] = std::max(g->cmax_suf[j + 1], c[j]);
+    }
+    CK(launch_tail_moments(d, g->cinf, g->cinf2, ctx->T, ctx->redm, ctx->st));
+    double tm[kMomP + 2];
+    int rc = read_result(ctx, kMomP + 2, tm, ctx->redm.result);
+    if (rc) return rc;
+    for (int k = 0; k < kMomP; ++k) g->tail_mom[k] = tm[k];
+    g->tail_max = tm[kMomP + 1];
+    g->have_mom = true;
+    return TPSC_OK;
+}
+
+// Sum-rule trace and its derivative in U (the reference's traceDiffChispChi0 /
+// traceDiffChichChi0, src/chi.cpp:738-830).  The Newton form sums the stored
+// frequencies j < jdir term by term and the rest as the series
+//   sum_{q, j >= jdir} w [chi/(1 + h chi) - chi] = sum_{m=1}^{kMomP} (-h)^m M_{m+1}(jdir),
+// h = -+ U/2, where jdir is the first frequency from which |h chi| < kMomSeriesMax
+// for every q (truncation below (kMomSeriesMax)^kMomP relative).
 int sumrule(tpsc_ctx *ctx, int channel, double Uv, double *tr, double *dtr) {
     Grid *g = ctx->cur;
-    CK(launch_sumrule(g->d, g->chiq, g->cinf, g->cinf2, Uv, channel == 0 ? -1.0 : 1.0, ctx->T, ctx->red, ctx->st));
+    const GridDev &d = g->d;
+    const double sgn = channel == 0 ? -1.0 : 1.0;
+    const bool series = (ctx->form & TPSC_FORM_NEWTON) != 0;
+    int jdir = d.nb, tail = 1;
+    if (series) {
+        int rc = ensure_moments(ctx, g);
+        if (rc) return rc;
+        const double ah = std::fabs(Uv) / 2.0;
+        jdir = 0;
+        while (jdir < d.nb && ah * g->cmax_suf[jdir] >= kMomSeriesMax) ++jdir;
+        tail = (ah * g->tail_max < kMomSeriesMax) ? 0 : 1;
+    }
+    CK(launch_sumrule(d, g->chiq, g->cinf, g->cinf2, Uv, sgn, ctx->T, ctx->red, ctx->st, jdir, tail));
     double r[2];
     int rc = read_result(ctx, 2, r);
     if (rc) return rc;
+    if (series && (jdir < d.nb || !tail)) {
+        long double M[kMomP];
+        for (int k = 0; k < kMomP; ++k)
+            M[k] = (jdir < d.nb ? g->mom_suf[(size_t)jdir * kMomP + k] : 0.0L) + (tail ? 0.0L : g->tail_mom[k]);
+        const long double h = sgn * Uv / 2.0;
+        long double S = 0.0L, dS = 0.0L, hm1 = 1.0L;  // hm1 = (-h)^(m-1)
+        for (int m = 1; m <= kMomP; ++m) {
+            S += -h * hm1 * M[m - 1];
+            dS += -m * hm1 * M[m - 1];
+            hm1 *= -h;
+        }
+        const long double scale = (long double)ctx->T / (4.0L * (d.nbk - 1) * (d.nbk - 1));
+        r[0] += (double)(scale * S);
+        r[1] += (double)(scale * 0.5L * sgn * dS);
+    }
     *tr = r[0];
     if (dtr) *dtr = r[1];
     return TPSC_OK;
@@ -741,9 +813,53 @@ int find_mu(tpsc_ctx *ctx) {
         rc = trace_diff_G(ctx, m, &y);
         return rc == TPSC_OK;
     };
+    // Newton form: the frequencies with w_n >= w_c enter as the series
+    //   Re sum_m (mu0 - mu)^m C_m - G0,  C_m = sum w (i w_n - eps + mu0 - Sigma)^-(m+1)
+    // of k_trdiff_moments, valid while |mu - mu0| <= dmax = kMomSeriesMax |z|_min;
+    // only the frequencies below w_c are summed per evaluation.  |z| >= w_n -
+    // |Im Sigma| >= w_n - 2 Sigma_inf / w_n bounds |z| on the series set.
+    const GridDev &d = g->d;
+    const int NO = d.nw0 / 2;
+    const double pt = PI * ctx->T;
+    int jc = (int)std::ceil((kMomMuRange / kMomSeriesMax / pt - 1.0) / 2.0);
+    jc = std::max(0, std::min(jc, NO));
+    const double wc = (2 * jc + 1) * pt;
+    const double zmin = wc - 2.0 * std::fabs(ctx->scal[TPSC_S_SIGMA_INF]) / wc;
+    const double dmax = zmin > 0 ? kMomSeriesMax * zmin : 0.0;
+    double Cm[2 * kMomP + 1] = {0};
+    const bool newton = (ctx->form & TPSC_FORM_NEWTON) != 0;
+    if (newton && dmax > 0) {
+        CK(launch_trdiff_moments(d, g->S, g->s2, g->s3, g->s4, g->sinf, g->mu0, g->mu0, ctx->T, jc, ctx->redm,
+                                 ctx->st));
+        if ((rc = read_result(ctx, 2 * kMomP + 1, Cm, ctx->redm.result))) return rc;
+    }
     auto fd = [&](double m, double &y, double &dy) -> bool {
-        rc = trace_diff_G(ctx, m, &y, &dy);
-        return rc == TPSC_OK;
+        const double delta = m - g->mu0;
+        if (!(newton && std::fabs(delta) <= dmax)) {
+            rc = trace_diff_G(ctx, m, &y, &dy);
+            return rc == TPSC_OK;
+        }
+        rc = TPSC_OK;
+        cudaError_t e = launch_trace_diff_G(d, g->S, g->s2, g->s3, g->s4, g->sinf, g->mu0, m, ctx->T, ctx->red,
+                                            ctx->st, jc);
+        if (e != cudaSuccess) {
+            rc = cuda_fail(ctx, e, "launch_trace_diff_G");
+            return false;
+        }
+        double r[2];
+        if ((rc = read_result(ctx, 2, r))) return false;
+        // Re sum_m (-delta)^m C_m and its delta derivative, in long double
+        long double sr = 0.0L, dsr = 0.0L;
+        long double pr = 1.0L, pi = 0.0L;  // (-delta)^m as a real power
+        for (int k = 0; k < kMomP; ++k) {
+            sr += pr * Cm[2 * k];
+            if (k > 0) dsr += -k * pi * Cm[2 * k];  // d/d delta (-delta)^k = -k (-delta)^(k-1)
+            pi = pr;
+            pr *= -(long double)delta;
+        }
+        y = r[0] + (double)(sr - Cm[2 * kMomP]);
+        dy = r[1] + (double)dsr;
+        return true;
     };
     const double init[3] = {0.0, -10.0, 10.0}, lims[2] = {-20.0, 20.0};
     double root = 0;
@@ -935,7 +1051,10 @@ tpsc_ctx *tpsc_create(int device, int *status) {
     if ((e = cudaMalloc(&ctx->red.result, 8 * sizeof(double))) != cudaSuccess) return bad(e);
     if ((e = cudaMalloc(&ctx->red.ticket, sizeof(unsigned))) != cudaSuccess) return bad(e);
     if ((e = cudaMemset(ctx->red.ticket, 0, sizeof(unsigned))) != cudaSuccess) return bad(e);
-    if ((e = cudaMallocHost(&ctx->h_res, 8 * sizeof(double))) != cudaSuccess) return bad(e);
+    if ((e = cudaMalloc(&ctx->redm.partial, (2 * kMomP + 2) * kMaxBlocks * sizeof(double))) != cudaSuccess)
+        return bad(e);
+    if ((e = cudaMalloc(&ctx->redm.result, 32 * sizeof(double))) != cudaSuccess) return bad(e);
+    if ((e = cudaMallocHost(&ctx->h_res, 32 * sizeof(double))) != cudaSuccess) return bad(e);
     for (auto &ev : ctx->ev)
         if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bad(e);
     if (status) *status = TPSC_OK;
@@ -950,6 +1069,8 @@ void tpsc_destroy(tpsc_ctx *ctx) {
     if (ctx->red.partial) cudaFree(ctx->red.partial);
     if (ctx->red.result) cudaFree(ctx->red.result);
     if (ctx->red.ticket) cudaFree(ctx->red.ticket);
+    if (ctx->redm.partial) cudaFree(ctx->redm.partial);
+    if (ctx->redm.result) cudaFree(ctx->redm.result);
     if (ctx->h_res) cudaFreeHost(ctx->h_res);
     if (ctx->stage) cudaFree(ctx->stage);
     for (auto &ev : ctx->ev)

@@ -242,7 +242,7 @@ __device__ __forceinline__ void group_fft(double2 *x, int t, const double2 *__re
 // 2D DCT-I (REDFT00 x REDFT00) in place on a symmetric NBK x NBK slice S
 // (row-major, leading dimension NBK, which is odd so that column accesses
 // are bank-conflict free).  scr: per-group FFT scratch, group g at
-// scr + g * padded_len(L); tw: the L twiddles, in shared memory.  All
+// scr + g * padded_len(L); tw: the L twiddles (shared or global memory).  All
 // threads of the block must call.  Two lines (rows, then columns) go through
 // one complex FFT of their even extension; the first FFT pass reads the
 // lines straight from S and the last pass writes outputs k < NBK back.

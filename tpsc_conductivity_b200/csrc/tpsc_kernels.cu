@@ -59,26 +59,25 @@ __device__ void block_store(double (&v)[NV], double *partial) {
     }
 }
 
+// Sum of the per-block partials in a fixed order: warp k adds value k with
+// lane-strided compensated sums and a shuffle tree (deterministic).
 template <int NV>
 __global__ void k_finish(const double *partial, int nblocks, double *result, double offset0) {
-    KSum acc[NV];
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
-#pragma unroll
-        for (int k = 0; k < NV; ++k) acc[k].add(partial[k * kMaxBlocks + b]);
-    // every thread's compensated partial, added by one thread in a fixed
-    // order: deterministic from run to run
-    __shared__ double all[256][NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k) all[threadIdx.x][k] = acc[k].value();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            KSum s;
-            for (int i = 0; i < (int)blockDim.x; ++i) s.add(all[i][k]);
-            result[k] = s.value() + (k == 0 ? offset0 : 0.0);
-        }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int k = warp; k < NV; k += blockDim.x >> 5) {
+        KSum acc;
+        for (int b = lane; b < nblocks; b += 32) acc.add(partial[k * kMaxBlocks + b]);
+        double v = acc.value();
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) result[k] = v + (k == 0 ? offset0 : 0.0);
     }
+}
+
+__global__ void k_max_finish(const double *partial, int nblocks, double *result) {
+    double m = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += 32) m = fmax(m, partial[b]);
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+    if (threadIdx.x == 0) result[0] = m;
 }
 
 int grid_for(long long total, int threads) {
@@ -90,7 +89,7 @@ int grid_for(long long total, int threads) {
 
 template <int NV>
 cudaError_t finish(Reduce r, int nblocks, double offset0, cudaStream_t st) {
-    k_finish<NV><<<1, 256, 0, st>>>(r.partial, nblocks, r.result, offset0);
+    k_finish<NV><<<1, 32 * (NV < 32 ? NV : 32), 0, st>>>(r.partial, nblocks, r.result, offset0);
     return launched();
 }
 
@@ -569,26 +568,17 @@ __device__ void grid_finish(double (&v)[NV], Reduce r, double offset0) {
     __syncthreads();
     if (!last) return;
     __threadfence();
-    KSum acc[NV];
-    // thread t owns the contiguous slice [t*per, (t+1)*per) of the partials
+    // warp k adds value k over the blocks: lane-strided compensated sums and a
+    // shuffle tree, a fixed order (deterministic)
     const int nb = gridDim.x;
-    const int per = (nb + blockDim.x - 1) / blockDim.x;
-    for (int b = threadIdx.x * per; b < min(nb, (int)(threadIdx.x + 1) * per); ++b)
-#pragma unroll
-        for (int k = 0; k < NV; ++k) acc[k].add(__ldcg(&r.partial[k * kMaxBlocks + b]));
-    __shared__ double all[1024][NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k) all[threadIdx.x][k] = acc[k].value();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            KSum s;
-            for (int i = 0; i < (int)blockDim.x; ++i) s.add(all[i][k]);
-            r.result[k] = s.value() + (k == 0 ? offset0 : 0.0);
-        }
-        *r.ticket = 0u;
+    for (int k = warp; k < NV; k += blockDim.x >> 5) {
+        KSum acc;
+        for (int b = lane; b < nb; b += 32) acc.add(__ldcg(&r.partial[k * kMaxBlocks + b]));
+        double x = acc.value();
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+        if (lane == 0) r.result[k] = x + (k == 0 ? offset0 : 0.0);
     }
+    if (threadIdx.x == 0) *r.ticket = 0u;
 }
 
 constexpr int kRedThreads = 256;
@@ -643,10 +633,13 @@ __device__ __forceinline__ void tail_series(double a, double b, double h, const 
     }
 }
 
+// Stored frequencies j < jdir are summed term by term (jdir = nb: all of
+// them); the Newton form passes jdir < nb and adds the frequencies above as a
+// power series in h from the moments of k_chi0_moments.
 __global__ void __launch_bounds__(kRedThreads)
     k_sumrule(const double4 *__restrict__ chiq, const double *__restrict__ cinf, const double *__restrict__ cinf2,
-              const double *__restrict__ w16, const double *__restrict__ tailq, int nb, double Uv, double sgn,
-              double T, double scale, Reduce r) {
+              const double *__restrict__ w16, const double *__restrict__ tailq, int nb, int jdir, int tail, double Uv,
+              double sgn, double T, double scale, Reduce r) {
     const int blk = blockIdx.x;
     const int o0 = 4 * blk;
     const double4 w = *reinterpret_cast<const double4 *>(w16 + o0);
@@ -654,7 +647,7 @@ __global__ void __launch_bounds__(kRedThreads)
     const double hu = sgn * Uv / 2.0;
     double v = 0.0, dv = 0.0;
     const double4 *col = chiq + (size_t)blk * nb;
-    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+    for (int j = threadIdx.x; j < jdir; j += blockDim.x) {
         const double4 x = ld_stream4(&col[j]);
         const double f = j == 0 ? 0.5 : 1.0;
         const double xs[4] = {x.x, x.y, x.z, x.w};
@@ -677,7 +670,7 @@ __global__ void __launch_bounds__(kRedThreads)
     double tv = 0.0, tdv = 0.0;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-        if (ww[c] == 0.0) continue;
+        if (ww[c] == 0.0 || !tail) continue;
         const double a = cinf[o0 + c], b = cinf2[o0 + c];
         const double cmax = fabs(a) * x1 + fabs(b) * x1 * x1;
         if (fabs(hu) * cmax < kTailSeriesMax) {
@@ -703,6 +696,118 @@ __global__ void __launch_bounds__(kRedThreads)
 }
 
 
+// Per-frequency moments of chi0 for the sum-rule series of the Newton form:
+// mom[j][k] = sum_q w_q f_j chi(q, iq_j)^(k+2), k < kMomP (f_0 = 1/2, else 1),
+// and cmax[j] = max_q |chi(q, iq_j)|.  One block per frequency j, a fixed
+// reduction order (deterministic).  With |h chi| < kTailSeriesMax for every
+// q at frequencies j >= jdir,
+//   sum_{q, j >= jdir} w f [chi/(1 + h chi) - chi] = sum_{m=1}^{kMomP} (-h)^m M_{m+1}
+// up to a relative (kTailSeriesMax)^kMomP.
+__global__ void __launch_bounds__(256)
+    k_chi0_moments(const double4 *__restrict__ chiq, const double *__restrict__ w16, int nb, int nblk,
+                   double *__restrict__ mom, double *__restrict__ cmax) {
+    const int j = blockIdx.x;
+    const double f = j == 0 ? 0.5 : 1.0;
+    double acc[kMomP + 1];
+#pragma unroll
+    for (int k = 0; k <= kMomP; ++k) acc[k] = 0.0;
+    double mx = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+        const double4 x = chiq[(size_t)b * nb + j];
+        const double4 w = *reinterpret_cast<const double4 *>(w16 + 4 * b);
+        const double xs[4] = {x.x, x.y, x.z, x.w}, ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (ws[c] == 0.0) continue;
+            const double v = xs[c];
+            mx = fmax(mx, fabs(v));
+            double pw = ws[c] * f * v * v;
+#pragma unroll
+            for (int k = 0; k < kMomP; ++k) {
+                acc[k] += pw;
+                pw *= v;
+            }
+        }
+    }
+    acc[kMomP] = mx;
+    __shared__ double red[8][kMomP + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k <= kMomP; ++k)
+        for (int off = 16; off > 0; off >>= 1) {
+            const double o = __shfl_down_sync(0xffffffffu, acc[k], off);
+            acc[k] = (k == kMomP) ? fmax(acc[k], o) : acc[k] + o;
+        }
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k <= kMomP; ++k) red[warp][k] = acc[k];
+    __syncthreads();
+    if (threadIdx.x <= kMomP) {
+        const int k = threadIdx.x;
+        double x = red[0][k];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) x = (k == kMomP) ? fmax(x, red[w][k]) : x + red[w][k];
+        if (k == kMomP)
+            cmax[j] = x;
+        else
+            mom[(size_t)j * kMomP + k] = x;
+    }
+}
+
+// Moments of the Matsubara tail of the sum rule (n = Nw0/2+1 .. Nw0, where
+// chi0 = a/qn^2 + b/qn^4, a = chi0_inf, b = chi0_inf2): per column the
+// U-independent S_p = sum_n chi_n^p from the power sums Q_k = sum_n qn^-2k,
+// S_p = sum_i C(p,i) a^(p-i) b^i Q_(p+i), weighted and summed over the
+// columns -> partial for block_store, value k = sum w S_(k+2), k < kMomP, and
+// value kMomP = max over columns of |chi| at the first tail frequency.
+__global__ void __launch_bounds__(256)
+    k_tail_moments(const double *__restrict__ cinf, const double *__restrict__ cinf2, const double *__restrict__ w16,
+                   const double *__restrict__ tailq, int n8, int nb, double T, double *partial) {
+    constexpr int NV = kMomP + 1;
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    const int nwmax = nb - 1;
+    const double wn1 = (nwmax + 1) * 2.0 * 3.141592653589793 * T;
+    const double x1 = 1.0 / (wn1 * wn1);
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n8; o += gridDim.x * blockDim.x) {
+        const double w = w16[o];
+        if (w == 0.0) continue;
+        const double a = cinf[o], b = cinf2[o];
+        double ap[2 * kMomP + 2], bp[2 * kMomP + 2];
+        ap[0] = bp[0] = 1.0;
+#pragma unroll
+        for (int k = 1; k < kMomP + 2; ++k) {
+            ap[k] = ap[k - 1] * a;
+            bp[k] = bp[k - 1] * b;
+        }
+#pragma unroll
+        for (int m = 1; m <= kMomP; ++m) {
+            const int p = m + 1;
+            double Sp = 0.0, coef = 1.0;
+#pragma unroll
+            for (int i = 0; i <= p; ++i) {
+                Sp += coef * ap[p - i] * bp[i] * __ldg(&tailq[p + i]);
+                coef = coef * (p - i) / (i + 1);
+            }
+            acc[m - 1] += w * Sp;
+        }
+        acc[kMomP] = fmax(acc[kMomP], fabs(a) * x1 + fabs(b) * x1 * x1);
+    }
+    // the max enters block_store's sum: keep it in a separate shared slot
+    __shared__ double mx[32];
+    double m = acc[kMomP];
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+    if ((threadIdx.x & 31) == 0) mx[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double x = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) x = fmax(x, mx[i]);
+        partial[(2 * kMomP + 1) * kMaxBlocks + blockIdx.x] = x;
+    }
+    acc[kMomP] = 0.0;
+    block_store<NV>(acc, partial);
+}
+
 // Tr(G - G0) at chemical potential pmu (green::traceDiffG,
 // src/green.cpp:3108-3182): stored frequencies j < Nw0/2 with the full Sigma,
 // tail Nw0/2 <= j <= Nw0 with its asymptotic form.  One CTA per column block.
@@ -717,10 +822,14 @@ __device__ __forceinline__ void trdiff_term(double wn, double rS, double iS, dou
     dv += inv * (wn * wn - (a + g) * d + num * 2.0 * a / A2);
 }
 
+// Stored frequencies j < jdir term by term (jdir = Nw0/2: all), and the
+// tail Nw0/2 <= j <= Nw0 when `tail` is set; the Newton form covers the
+// rest with the series of k_trdiff_moments.
 __global__ void __launch_bounds__(kRedThreads)
     k_trace_diff_G(const double2 *__restrict__ S, const double *__restrict__ s2, const double *__restrict__ s3,
                    const double *__restrict__ s4, const double *__restrict__ sinfp, const double *__restrict__ ek,
-                   const double *__restrict__ w16, int nw0, double mu0, double pmu, double T, Reduce r) {
+                   const double *__restrict__ w16, int nw0, double mu0, double pmu, double T, int jdir, int tail,
+                   Reduce r) {
     const int blk = blockIdx.x, o0 = 4 * blk, NO = nw0 / 2;
     const double sinf = sinfp[0];
     double ww[4], e[4], c2[4], c3[4], c4[4];
@@ -736,7 +845,7 @@ __global__ void __launch_bounds__(kRedThreads)
     const double pt = 3.141592653589793 * T;
     double v = 0.0, dv = 0.0;
     const double4 *row = reinterpret_cast<const double4 *>(S + (size_t)blk * 4 * NO);
-    for (int j = threadIdx.x; j < NO; j += blockDim.x) {
+    for (int j = threadIdx.x; j < jdir; j += blockDim.x) {
         const double wn = (2 * j + 1) * pt;
         const double i1 = 1.0 / wn;
         const double4 p = ld_stream4(&row[2 * j]), q = ld_stream4(&row[2 * j + 1]);
@@ -750,7 +859,7 @@ __global__ void __launch_bounds__(kRedThreads)
             trdiff_term(wn, rS, iS, e[c], mu0, pmu, ww[c], v, dv);
         }
     }
-    for (int t = threadIdx.x; t <= NO; t += blockDim.x) {
+    for (int t = threadIdx.x; tail && t <= NO; t += blockDim.x) {
         const int j = NO + t;
         const double wn = (2 * j + 1) * pt;
         const double i1 = 1.0 / wn, i2 = i1 * i1;
@@ -764,6 +873,60 @@ __global__ void __launch_bounds__(kRedThreads)
     }
     double out[2] = {v, dv};
     grid_finish<2>(out, r, 0.0);
+}
+
+// Moments of the high-frequency part of Tr(G - G0) for the Newton form of
+// find_mu.  With z = i w_n - eps_k + mu_r - Sigma(k, i w_n) over every octant
+// k and the frequencies jc <= n < Nw0/2 (stored Sigma) and Nw0/2 <= n <= Nw0
+// (asymptotic Sigma, as k_trace_diff_G sums them):
+//   v[2m], v[2m+1] = Re, Im sum w z^-(m+1),  m < kMomP
+//   v[2 kMomP]     = sum w Re 1/(i w_n - eps_k + mu0)
+// so that this part of the trace at mu is Re sum_m (mu_r - mu)^m C_m - v[2 kMomP]
+// while |mu - mu_r| |z|^-1 < kMomSeriesMax.  Per-block partials (block_store).
+__global__ void __launch_bounds__(kRedThreads)
+    k_trdiff_moments(const double2 *__restrict__ S, const double *__restrict__ s2, const double *__restrict__ s3,
+                     const double *__restrict__ s4, const double *__restrict__ sinfp, const double *__restrict__ ek,
+                     const double *__restrict__ w16, int nw0, double mu0, double mu_r, double T, int jc,
+                     double *partial) {
+    constexpr int NV = 2 * kMomP + 1;
+    const int blk = blockIdx.x, o0 = 4 * blk, NO = nw0 / 2;
+    const double sinf = sinfp[0];
+    const double pt = 3.141592653589793 * T;
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    auto add = [&](double wn, double rS, double iS, double e, double w) {
+        const double zx = mu_r - e - rS, zy = wn - iS;
+        const double rr = 1.0 / (zx * zx + zy * zy);  // |z| >= w_n: no overflow or underflow here
+        const double2 zi = make_double2(zx * rr, -zy * rr);
+        double2 zp = zi;
+#pragma unroll
+        for (int m = 0; m < kMomP; ++m) {
+            acc[2 * m] += w * zp.x;
+            acc[2 * m + 1] += w * zp.y;
+            zp = cmul(zp, zi);
+        }
+        const double d = mu0 - e;
+        acc[2 * kMomP] += w * d / (d * d + wn * wn);
+    };
+    for (int c = 0; c < 4; ++c) {
+        const double w = w16[o0 + c];
+        if (w == 0.0) continue;
+        const int o = o0 + c;
+        const double e = ek[o], c2 = s2[o], c3 = s3[o], c4 = s4[o];
+        for (int j = jc + threadIdx.x; j < NO; j += blockDim.x) {
+            const double wn = (2 * j + 1) * pt, i1 = 1.0 / wn;
+            double rS, iS;
+            sigma_full(i1, sinf, c2, c3, S[bidx(j, o, NO)], rS, iS);
+            add(wn, rS, iS, e, w);
+        }
+        for (int t = threadIdx.x; t <= NO; t += blockDim.x) {
+            const double wn = (2 * (NO + t) + 1) * pt;
+            const double i1 = 1.0 / wn, i2 = i1 * i1;
+            add(wn, -c2 * i2 + c4 * i2 * i2, -sinf * i1 + c3 * i2 * i1, e, w);
+        }
+    }
+    block_store<NV>(acc, partial);
 }
 
 // Tr Sigma G0 and its asymptotic correction (green::traceSelfG,
@@ -1196,10 +1359,30 @@ cudaError_t launch_chi0_tau(const GridDev &g, double *chiq, const double *dtau_c
 }
 
 cudaError_t launch_sumrule(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
-                           double Uv, double sign, double T, Reduce r, cudaStream_t st) {
+                           double Uv, double sign, double T, Reduce r, cudaStream_t st, int jdir, int tail) {
     const double Nq = 4.0 * (g.nbk - 1) * (g.nbk - 1);
+    if (jdir < 0 || jdir > g.nb) jdir = g.nb;
     k_sumrule<<<g.n8p / 4, kRedThreads, 0, st>>>(reinterpret_cast<const double4 *>(chiq), chi0_inf, chi0_inf2,
-                                                  g.w16, g.tailq, g.nb, Uv, sign, T, T / Nq, r);
+                                                  g.w16, g.tailq, g.nb, jdir, tail, Uv, sign, T, T / Nq, r);
+    return launched();
+}
+
+cudaError_t launch_tail_moments(const GridDev &g, const double *chi0_inf, const double *chi0_inf2, double T,
+                                Reduce r, cudaStream_t st) {
+    constexpr int NV = kMomP + 1;
+    const int nblk = grid_for(g.n8, 256);
+    k_tail_moments<<<nblk, 256, 0, st>>>(chi0_inf, chi0_inf2, g.w16, g.tailq, g.n8, g.nb, T, r.partial);
+    cudaError_t e = launched();
+    if (e != cudaSuccess) return e;
+    e = finish<NV>(r, nblk, 0.0, st);
+    if (e != cudaSuccess) return e;
+    // the per-block maxima -> result[NV]
+    k_max_finish<<<1, 32, 0, st>>>(r.partial + (2 * kMomP + 1) * kMaxBlocks, nblk, r.result + NV);
+    return launched();
+}
+
+cudaError_t launch_chi0_moments(const GridDev &g, const double *chiq, double *mom, double *cmax, cudaStream_t st) {
+    k_chi0_moments<<<g.nb, 256, 0, st>>>(reinterpret_cast<const double4 *>(chiq), g.w16, g.nb, g.n8p / 4, mom, cmax);
     return launched();
 }
 
@@ -1236,9 +1419,25 @@ cudaError_t launch_sigma_tau(const GridDev &g, const double *sigt, const double 
 
 cudaError_t launch_trace_diff_G(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                                 const double *s4, const double *sinf, double mu0, double pmu, double T, Reduce r,
-                                cudaStream_t st) {
-    k_trace_diff_G<<<g.n8p / 4, kRedThreads, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.nw0, mu0, pmu, T, r);
+                                cudaStream_t st, int jdir) {
+    const int NO = g.nw0 / 2;
+    const int tail = (jdir < 0) ? 1 : 0;
+    if (jdir < 0 || jdir > NO) jdir = NO;
+    k_trace_diff_G<<<g.n8p / 4, kRedThreads, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.nw0, mu0, pmu, T, jdir,
+                                                       tail, r);
     return launched();
+}
+
+cudaError_t launch_trdiff_moments(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                                  const double *s4, const double *sinf, double mu0, double mu_r, double T, int jc,
+                                  Reduce r, cudaStream_t st) {
+    constexpr int NV = 2 * kMomP + 1;
+    const int nblk = g.n8p / 4;
+    k_trdiff_moments<<<nblk, kRedThreads, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.nw0, mu0, mu_r, T, jc,
+                                                    r.partial);
+    cudaError_t e = launched();
+    if (e != cudaSuccess) return e;
+    return finish<NV>(r, nblk, 0.0, st);
 }
 
 cudaError_t launch_trace_self_G(const GridDev &g, const double2 *S, const double *s2, const double *s3,

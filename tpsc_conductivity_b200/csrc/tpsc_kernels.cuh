@@ -55,8 +55,20 @@ cudaError_t launch_chi0_tau(const GridDev &g, double *chiq, const double *dtau_c
 // chi0max, qmax -> r.result[0..2]
 cudaError_t launch_chi0max(const GridDev &g, const double *chiq, Reduce r, cudaStream_t st);
 
+// sum-rule trace and its U derivative -> r.result[0..1]; stored frequencies
+// j < jdir term by term (jdir = -1: all)
 cudaError_t launch_sumrule(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
-                           double Uv, double sign, double T, Reduce r, cudaStream_t st);
+                           double Uv, double sign, double T, Reduce r, cudaStream_t st, int jdir = -1,
+                           int tail = 1);
+// Matsubara-tail moments sum_q w S_(k+2) -> r.result[0..kMomP), max tail |chi| ->
+// r.result[kMomP + 1] (r.partial must hold (2 kMomP + 2) kMaxBlocks doubles)
+cudaError_t launch_tail_moments(const GridDev &g, const double *chi0_inf, const double *chi0_inf2, double T,
+                                Reduce r, cudaStream_t st);
+// per-frequency moments sum_q w f chi^(k+2), k < kMomP -> mom [nb][kMomP]; max_q |chi| -> cmax [nb]
+constexpr int kMomP = 8;
+constexpr double kMomSeriesMax = 0.004;  // |h chi| bound of the series terms: 0.004^8 < 1e-19
+constexpr double kMomMuRange = 0.35;     // |mu - mu0| the find_mu series is built to cover
+cudaError_t launch_chi0_moments(const GridDev &g, const double *chiq, double *mom, double *cmax, cudaStream_t st);
 cudaError_t launch_trace_chi0(const GridDev &g, const double *chiq, const double *chi0_inf,
                               const double *chi0_inf2, double T, Reduce r, cudaStream_t st);
 
@@ -70,9 +82,16 @@ cudaError_t launch_sigma_slice(const GridDev &g, const double *Grt, const double
 cudaError_t launch_sigma_tau(const GridDev &g, const double *sigt, const double *dS, double2 *S, double *s2,
                              double *s3, double *s4, double *sinf, double T, cudaStream_t st);
 
+// Tr(G - G0) at pmu and its pmu derivative -> r.result[0..1]; jdir = -1: all
+// frequencies (stored and tail), else stored j < jdir only
 cudaError_t launch_trace_diff_G(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                                 const double *s4, const double *sinf, double mu0, double pmu, double T, Reduce r,
-                                cudaStream_t st);
+                                cudaStream_t st, int jdir = -1);
+// series moments of the frequencies j >= jc (and the tail) around mu_r ->
+// r.result[0 .. 2 kMomP] (r.partial must hold (2 kMomP + 1) kMaxBlocks doubles)
+cudaError_t launch_trdiff_moments(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                                  const double *s4, const double *sinf, double mu0, double mu_r, double T, int jc,
+                                  Reduce r, cudaStream_t st);
 cudaError_t launch_trace_self_G(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                                 const double *sinf, double mu0, double T, Reduce r, cudaStream_t st);
 cudaError_t launch_trace_self_G2(const GridDev &g, const double2 *S, const double *s2, const double *s3,
