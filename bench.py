@@ -9,7 +9,9 @@ T = 0.05): chi0 -> Usp, Uch (sum-rule roots) -> V(r, tau) -> Sigma(k, i w_n)
 -> Tr Sigma G -> mu (root of Tr(G - G0)) -> Tr Sigma G at mu.  The inputs are
 model parameters (synthetic; no dataset exists for this path).
 
-* value: device-resident solves/s, each step timed with CUDA events on the
+* value: device-resident solves/s of the mixed-precision + Newton form
+  (FP32 G, chi0 and V slice transforms; FP64 for the rest), Sigma compared
+  with the FP64 forms' (reported), each step timed with CUDA events on the
   library's own stream, L2 flushed (512 MB write) before every step; with
   N > 1 every rank solves its own replica (weak scaling, no collective on the
   data path) and the time is the max over ranks.
@@ -39,7 +41,7 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(nk0=256, Nw0=4096, U=4.0, tp=-0.15, tpp=0.0, t3=0.0, n=0.875, T=0.05)
 WORKLOAD_NAME = ("TPSC solve, 256x256 lattice, 2048 positive fermionic iwn (Nw0=4096), "
-                 "t'=-0.15, U=4, n=0.875, T=0.05, FP64")
+                 "t'=-0.15, U=4, n=0.875, T=0.05")
 METRIC = "TPSC solves/s at 256²×2048 iωn: mixed+Newton vs FP64 GPU at ≤1e-6 ΔΣ; HBM GB/s"
 PROBE = os.path.join(ROOT, "oracle", "_ref", "tpsc_ref_probe")
 FALLBACK_HBM = 6650.0
@@ -222,11 +224,18 @@ def our_arm(a, world, rank, local_rank):
         return t, n, clk.summary(), g.scalars(), g.stage_times()
 
     # ---- device-resident solves: the FP64 drop-in with the reference's root
-    # searches, then the Newton form (the headline) -----------------------------
+    # searches, the FP64 Newton form, then mixed precision + Newton (the
+    # headline); Sigma of the two Newton forms compared ------------------------
     ms_ref, _, _, sc_ref, stages_ref = timed_solves(_lib.FORM_REFERENCE)
-    ms, n_launch, clocks, sc, stages = timed_solves(_lib.FORM_NEWTON)
+    ms_n64, _, _, sc_n64, stages_n64 = timed_solves(_lib.FORM_NEWTON)
+    sigma64 = g.sigma()
+    MIXED = _lib.FORM_NEWTON | _lib.FORM_MIXED
+    ms, n_launch, clocks, sc, stages = timed_solves(MIXED)
+    dsigma = float(np.max(np.abs(g.sigma() - sigma64)) / np.max(np.abs(sigma64)))
+    del sigma64
     value = world * a.steps / (ms / 1e3)
     value_ref = world * a.steps / (ms_ref / 1e3)
+    value_n64 = world * a.steps / (ms_n64 / 1e3)
 
     # ---- end to end through the public API ------------------------------------
     nk0, nw0, nbk, n8 = g.dims()
@@ -240,6 +249,7 @@ def our_arm(a, world, rank, local_rank):
         torch.cuda.synchronize()
         ev2[i][0].record(stream)
         g2 = Green(w["nk0"], w["Nw0"], w["n"], w["T"], 0.1, (w["tp"], w["tpp"], w["t3"], w["U"]), ctx=ctx)
+        g2.set_form(MIXED)
         g2.solve()
         g2.self_energy(out=S_c)
         g2.scalars()
@@ -248,13 +258,17 @@ def our_arm(a, world, rank, local_rank):
     ms2 = allreduce_max(sum(s.elapsed_time(e) for s, e in ev2), world, dev)
     e2e = world * a.steps / (ms2 / 1e3)
 
-    # ---- per-kernel timing (stages re-launched alone, in order) -------------
+    # ---- per-kernel timing (stages re-launched alone, in order, as the
+    # mixed + Newton solve runs them) -------------------------------------------
+    g.set_form(MIXED)
     g.solve()
     torch.cuda.synchronize()
     reps = 3
     per = {}
     for rep in range(reps):
         for k, name in enumerate(_lib.KERNELS):
+            if name == "chi0_slice+tau":
+                continue
             flush.zero_()
             torch.cuda.synchronize()
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -264,9 +278,13 @@ def our_arm(a, world, rank, local_rank):
             torch.cuda.synchronize()
             per.setdefault(name, []).append(s.elapsed_time(e))
     per_ms = {k: min(v) for k, v in per.items()}
+    # launches per mixed + Newton solve: the root searches run the restricted
+    # (Newton-form) evaluations, never the full ones
     counts = {k: 1 for k in per_ms}
-    counts["sumrule"] = int(sc["evals_sp"] + sc["evals_ch"])
-    counts["trace_diff_G"] = int(sc["evals_mu"])
+    counts["sumrule"] = 0
+    counts["trace_diff_G"] = 0
+    counts["sumrule_newton"] = int(sc["evals_sp"] + sc["evals_ch"])
+    counts["trace_diff_G_newton"] = int(sc["evals_mu"])
     share = {k: per_ms[k] * counts[k] for k in per_ms}
     dom = max(share, key=share.get)
     kb = C.c_double()
@@ -280,18 +298,26 @@ def our_arm(a, world, rank, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (model parameters; no dataset)",
-        "config": {"workload": WORKLOAD_NAME, "form": "fp64 transforms + Newton root searches",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (model parameters; no dataset)",
+        "config": {"workload": WORKLOAD_NAME,
+                   "form": "mixed precision (FP32 G/chi0/V slice transforms, compensated twiddles; FP64 Sigma "
+                           "transforms, tau transforms, sums, roots) + Newton root searches with moment series",
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "512 MB flush before every step; working set ~2.4 GB per solve",
-                   "sumrule_evals": counts["sumrule"], "mu_evals": counts["trace_diff_G"]},
-        "forms": {"fp64_newton": {"solves_per_s": value, "ms_per_step": ms / a.steps, "stage_ms": stages},
+                   "sumrule_evals": counts["sumrule_newton"], "mu_evals": counts["trace_diff_G_newton"]},
+        "forms": {"mixed_newton": {"solves_per_s": value, "ms_per_step": ms / a.steps, "stage_ms": stages,
+                                   "max_rel_dSigma_vs_fp64": dsigma},
+                  "fp64_newton": {"solves_per_s": value_n64, "ms_per_step": ms_n64 / a.steps,
+                                  "stage_ms": stages_n64},
                   "fp64_reference_roots": {"solves_per_s": value_ref, "ms_per_step": ms_ref / a.steps,
                                            "stage_ms": stages_ref,
                                            "sumrule_evals": int(sc_ref["evals_sp"] + sc_ref["evals_ch"]),
                                            "mu_evals": int(sc_ref["evals_mu"])},
-                  "max_rel_diff_roots": max(abs(sc[k] - sc_ref[k]) / abs(sc_ref[k])
-                                            for k in ("Usp", "Uch", "mu"))},
+                  "mixed_newton_over_fp64_reference_roots": value / value_ref,
+                  "max_rel_diff_roots_fp64_newton": max(abs(sc_n64[k] - sc_ref[k]) / abs(sc_ref[k])
+                                                        for k in ("Usp", "Uch", "mu")),
+                  "max_rel_diff_roots_mixed": max(abs(sc[k] - sc_ref[k]) / abs(sc_ref[k])
+                                                  for k in ("Usp", "Uch", "mu"))},
         "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,

@@ -62,16 +62,23 @@ enum tpsc_scalar {
     TPSC_S_COUNT
 };
 
-/* How a solve finds its roots (tpsc_set_form).
- *  TPSC_FORM_REFERENCE: the reference's find_zero control flow for Usp, Uch
- *    and mu (src/generique.cpp:604-1234) -- the FP64 drop-in, same roots and
- *    the same number of function evaluations as the reference;
- *  TPSC_FORM_NEWTON: safeguarded Newton steps inside the reference's search
- *    intervals, with the derivative from the same device pass as the value
- *    (d trace/dU of the sum rules, d Tr(G-G0)/d mu); mu starts at mu0.
- *    Same roots to ~1e-14, several times fewer passes.  No counterpart in
- *    the reference. */
-enum tpsc_form { TPSC_FORM_REFERENCE = 0, TPSC_FORM_NEWTON = 1 };
+/* How a solve computes (tpsc_set_form); the flags combine.
+ *  TPSC_FORM_REFERENCE (0): FP64 throughout and the reference's find_zero
+ *    control flow for mu0, Usp, Uch and mu (src/generique.cpp:604-1234) --
+ *    the FP64 drop-in, same roots and the same number of function
+ *    evaluations as the reference;
+ *  TPSC_FORM_NEWTON (1): safeguarded Newton steps inside the reference's
+ *    search intervals, with the derivative from the same device pass as the
+ *    value (d trace/dU of the sum rules, d Tr(G-G0)/d mu, dn/d mu0); the
+ *    high frequencies of the sum rules and of Tr(G-G0) enter as power series
+ *    from moments computed once per search (truncation below 1e-19 of the
+ *    leading term).  Same roots to ~1e-14, several times fewer passes;
+ *  TPSC_FORM_MIXED (2): the G(r, tau), chi0(q, tau) and V(q) slice transforms
+ *    in FP32 with compensated twiddles (G stored in FP32); Sigma's
+ *    transforms, every tau transform, the sum rules, traces, roots and the
+ *    continuation in FP64.  Sigma within ~1e-6 of the FP64 forms.
+ * Neither NEWTON nor MIXED has a counterpart in the reference. */
+enum tpsc_form { TPSC_FORM_REFERENCE = 0, TPSC_FORM_NEWTON = 1, TPSC_FORM_MIXED = 2 };
 
 /* Create a context on CUDA device `device`.  Returns NULL and sets *status on
  * failure (no CUDA device, driver error). */
@@ -216,7 +223,9 @@ int tpsc_get_stream(tpsc_ctx *ctx, void **stream);
  *  0 G(r,tau) slices   1 chi0 slices   2 chi0 tau transform
  *  3 V q-slices        4 V tau transform   5 Sigma slices
  *  6 Sigma tau transform  7 one spin sum-rule evaluation at Usp
- *  8 one Tr(G-G0) evaluation at mu   9 stages 1 and 2 back to back.
+ *  8 one Tr(G-G0) evaluation at mu   9 stages 1 and 2 back to back
+ *  10 one Newton-form sum-rule evaluation at Usp (stored frequencies below
+ *     the series cut)   11 one Newton-form Tr(G-G0) evaluation at mu.
  * Requires a completed tpsc_solve.  Stages 2 and 4 transform in place and
  * expect stage 1 (resp. 3) to have run just before; launching the stages in
  * increasing order leaves the state as the solve left it. */

@@ -56,12 +56,12 @@ SIGNATURES = [
       C.c_void_p]),
 ]
 
-# enum tpsc_form
-FORM_REFERENCE, FORM_NEWTON = 0, 1
+# enum tpsc_form (flags)
+FORM_REFERENCE, FORM_NEWTON, FORM_MIXED = 0, 1, 2
 
 # tpsc_run_kernel stage ids
 KERNELS = ["gslice", "chi0_slice", "chi0_tau", "vertex_q", "vertex_tau", "sigma_slice", "sigma_tau",
-           "sumrule", "trace_diff_G"]
+           "sumrule", "trace_diff_G", "chi0_slice+tau", "sumrule_newton", "trace_diff_G_newton"]
 
 STATUS = {0: "OK", 1: "bad argument", 2: "CUDA error", 3: "out of device memory",
           4: "root not found", 5: "stage prerequisite missing", 6: "non-finite result"}

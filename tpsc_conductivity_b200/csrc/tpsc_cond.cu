@@ -312,7 +312,14 @@ __device__ __forceinline__ void tails(const ColState &q, double tau, double beta
 // Stage the two columns of pair p (contiguous in the two-column-block layout)
 // column-major into R; a padding column loads zeros.
 __device__ __forceinline__ void stage_pair(double *R, const double *g, int NJ, bool two) {
-    for (int i = threadIdx.x; i < 2 * NJ; i += blockDim.x) R[(i & 1) * NJ + (i >> 1)] = ((i & 1) && !two) ? 0.0 : g[i];
+    for (int i = threadIdx.x; i < 2 * NJ; i += blockDim.x) {
+        double *dst = &R[(i & 1) * NJ + (i >> 1)];
+        if ((i & 1) && !two)
+            *dst = 0.0;
+        else
+            cp_async8(dst, g + i);
+    }
+    cp_async_wait_all();
 }
 
 template <int N>

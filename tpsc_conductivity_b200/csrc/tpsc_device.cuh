@@ -200,12 +200,30 @@ struct TauSmem {
     }
 };
 
-// Load one column block into shared memory, column-major.  Padding columns
-// (octant index >= n8, present because N8 is rounded up to a multiple of 4)
-// load as zeros: they share packed FFTs with real columns, so stale values
-// there would leak into real outputs through rounding.
+// Asynchronous 8-byte global -> shared copy (cp.async); the issuing thread
+// waits for its own copies with cp_async_wait_all, a barrier then publishes
+// them.  A thread keeps all its copies in flight at once, which is what
+// streams a column block in at HBM speed with one CTA per SM.
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Load one column block into shared memory, column-major (the caller's next
+// __syncthreads publishes it).  Padding columns (octant index >= n8, present
+// because N8 is rounded up to a multiple of 4) load as zeros: they share
+// packed FFTs with real columns, so stale values there would leak into real
+// outputs through rounding.
 __device__ __forceinline__ void stage_in(double *A, const double *g, int NJ, int nvalid) {
-    for (int i = threadIdx.x; i < 4 * NJ; i += blockDim.x) A[(i & 3) * NJ + (i >> 2)] = (i & 3) < nvalid ? g[i] : 0.0;
+    for (int i = threadIdx.x; i < 4 * NJ; i += blockDim.x) {
+        double *dst = &A[(i & 3) * NJ + (i >> 2)];
+        if ((i & 3) < nvalid)
+            cp_async8(dst, g + i);
+        else
+            *dst = 0.0;
+    }
+    cp_async_wait_all();
 }
 __device__ __forceinline__ void stage_out(const double *A, double *g, int NJ) {
     for (int i = threadIdx.x; i < 4 * NJ; i += blockDim.x) g[i] = A[(i & 3) * NJ + (i >> 2)];

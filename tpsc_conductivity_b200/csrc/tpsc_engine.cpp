@@ -273,6 +273,7 @@ struct Grid {
     std::vector<double> ek_host;  // [nbk * nbk], ek[m + l*nbk]
     double mu0 = 0.0;
     double *Grt = nullptr;        // [(Nw0+1) * n8]      G(r, tau_j)
+    float *Grt32 = nullptr;       // [(Nw0+1) * n8]      G(r, tau_j) in FP32 (mixed form; allocated on first use)
     double *chirt = nullptr;      // blocked nb          chi0(r, tau_j)
     double *chiq = nullptr;       // blocked nb          chi0(q, tau_j) -> chi0(q, iqn)
     double *dG0p = nullptr, *dchirt0 = nullptr, *dchiqt0 = nullptr;  // [n8]
@@ -283,6 +284,7 @@ struct Grid {
     double2 *S = nullptr;         // blocked Nw0/2       coefficient of 1/z^4
     double *s2 = nullptr, *s3 = nullptr, *s4 = nullptr, *sinf = nullptr;
     bool have_chi0 = false, have_V = false, have_S = false;
+    bool g_mixed = false;         // G(r, tau) of the last chi0 stage is Grt32
     // Newton form: moments of chi0 for the high-frequency sum-rule series
     double *mom = nullptr, *cmax = nullptr;  // device [nb][kMomP], [nb]
     bool have_mom = false;
@@ -414,6 +416,19 @@ void twiddles(int N, long double sign, long double scale, std::vector<double2> &
     }
 }
 
+// FP32 twiddles exp(-2 pi i m / N) as (cos_hi, sin_hi, cos_lo, sin_lo):
+// hi = float(x), lo = float(x - hi), from long double
+void twiddles32(int N, std::vector<float4> &out) {
+    out.resize(N);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int m = 0; m < N; ++m) {
+        const long double a = -2.0L * pi * m / N;
+        const long double c = cosl(a), s = sinl(a);
+        const float ch = (float)c, sh = (float)s;
+        out[m] = make_float4(ch, sh, (float)(c - ch), (float)(s - sh));
+    }
+}
+
 template <typename T>
 cudaError_t upload(Grid *g, T **dst, const std::vector<T> &src) {
     cudaError_t e = dalloc(g, dst, src.size());
@@ -454,6 +469,8 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
             w16[m + l * (l + 1) / 2] = w;
         }
     std::vector<double2> twk, tww, htw;
+    std::vector<float4> twk32;
+    twiddles32(nk0, twk32);
     twiddles(nk0, -2.0L, 1.0L, twk);
     twiddles(nw0, -2.0L, 1.0L, tww);
     twiddles(nw0, 1.0L, 1.0L, htw);
@@ -469,6 +486,7 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
     A(upload(g, &d.lm, lm));
     A(upload(g, &d.w16, w16));
     A(upload(g, &d.tw_k, twk));
+    A(upload(g, &d.tw_k32, twk32));
     A(upload(g, &d.tw_w, tww));
     A(upload(g, &d.ht_w, htw));
     A(upload(g, &d.spl_half, sh));
@@ -557,6 +575,14 @@ int grid_set_model(tpsc_ctx *ctx, Grid *g) {
         return TPSC_OK;
     }
     int rc = TPSC_OK;
+    if (ctx->form & TPSC_FORM_NEWTON) {
+        CK(launch_mu0_newton(d, ctx->n, ctx->T, ctx->red, ctx->st));
+        double r[2];
+        if ((rc = read_result(ctx, 2, r))) return rc;
+        if (!std::isfinite(r[0]) || r[1] >= 200) return fail(ctx, TPSC_ERR_NO_ROOT, "mu0 not found");
+        g->mu0 = r[0];
+        return TPSC_OK;
+    }
     auto dens = [&](double mu, double &y) -> bool {
         cudaError_t e = launch_density(d, mu, ctx->n, ctx->T, ctx->red, ctx->st);
         if (e != cudaSuccess) {
@@ -595,12 +621,24 @@ int need_model(tpsc_ctx *ctx) {
     return TPSC_OK;
 }
 
+bool mixed(const tpsc_ctx *ctx) { return (ctx->form & TPSC_FORM_MIXED) != 0; }
+
 int run_chi0(tpsc_ctx *ctx) {
     Grid *g = ctx->cur;
     const GridDev &d = g->d;
-    CK(launch_gslice(d, g->Grt, g->mu0, ctx->T, ctx->st));
-    CK(launch_chi0_boundary(d, g->Grt, g->mu0, ctx->T, g->dG0p, g->dchirt0, g->dchiqt0, ctx->st));
-    CK(launch_chi0_slice(d, g->Grt, g->chirt, g->chiq, ctx->st));
+    if (mixed(ctx)) {
+        if (!g->Grt32) CK(dalloc(g, &g->Grt32, (size_t)(d.nw0 + 1) * d.n8));
+        CK(launch_gslice32(d, g->Grt32, g->mu0, ctx->T, ctx->st));
+        CK(launch_chi0_boundary(d, (const float *)g->Grt32, g->mu0, ctx->T, g->dG0p, g->dchirt0, g->dchiqt0,
+                                ctx->st));
+        CK(launch_chi0_slice32(d, g->Grt32, g->chirt, g->chiq, ctx->st));
+    } else {
+        CK(launch_gslice(d, g->Grt, g->mu0, ctx->T, ctx->st));
+        CK(launch_chi0_boundary(d, (const double *)g->Grt, g->mu0, ctx->T, g->dG0p, g->dchirt0, g->dchiqt0,
+                                ctx->st));
+        CK(launch_chi0_slice(d, g->Grt, g->chirt, g->chiq, ctx->st));
+    }
+    g->g_mixed = mixed(ctx);
     CK(launch_chi0_tau(d, g->chiq, g->dchiqt0, g->cinf, g->cinf2, ctx->T, ctx->st));
     CK(launch_chi0max(d, g->chiq, ctx->red, ctx->st));
     double r[3];
@@ -643,6 +681,16 @@ int ensure_moments(tpsc_ctx *ctx, Grid *g) {
     return TPSC_OK;
 }
 
+// First stored frequency from which |U/2 chi| < kMomSeriesMax for every q, and
+// whether the Matsubara tail needs the term-by-term sum (tail = 1).
+void series_cut(const Grid *g, double Uv, int *jdir, int *tail) {
+    const double ah = std::fabs(Uv) / 2.0;
+    int j = 0;
+    while (j < g->d.nb && ah * g->cmax_suf[j] >= kMomSeriesMax) ++j;
+    *jdir = j;
+    *tail = (ah * g->tail_max < kMomSeriesMax) ? 0 : 1;
+}
+
 // Sum-rule trace and its derivative in U (the reference's traceDiffChispChi0 /
 // traceDiffChichChi0, src/chi.cpp:738-830).  The Newton form sums the stored
 // frequencies j < jdir term by term and the rest as the series
@@ -658,10 +706,7 @@ int sumrule(tpsc_ctx *ctx, int channel, double Uv, double *tr, double *dtr) {
     if (series) {
         int rc = ensure_moments(ctx, g);
         if (rc) return rc;
-        const double ah = std::fabs(Uv) / 2.0;
-        jdir = 0;
-        while (jdir < d.nb && ah * g->cmax_suf[jdir] >= kMomSeriesMax) ++jdir;
-        tail = (ah * g->tail_max < kMomSeriesMax) ? 0 : 1;
+        series_cut(g, Uv, &jdir, &tail);
     }
     CK(launch_sumrule(d, g->chiq, g->cinf, g->cinf2, Uv, sgn, ctx->T, ctx->red, ctx->st, jdir, tail));
     double r[2];
@@ -759,7 +804,10 @@ int run_vertex(tpsc_ctx *ctx) {
     Grid *g = ctx->cur;
     if (!g || !g->have_chi0) return fail(ctx, TPSC_ERR_STATE, "chi0 has not been computed on the current grid");
     const double fact = ctx->U * (3.0 * ctx->Usp + ctx->Uch) / 8.0;
-    CK(launch_vertex_q(g->d, g->chiq, g->V, ctx->U, ctx->Usp, ctx->Uch, ctx->T, ctx->st));
+    if (mixed(ctx))
+        CK(launch_vertex_q32(g->d, g->chiq, g->V, ctx->U, ctx->Usp, ctx->Uch, ctx->T, ctx->st));
+    else
+        CK(launch_vertex_q(g->d, g->chiq, g->V, ctx->U, ctx->Usp, ctx->Uch, ctx->T, ctx->st));
     CK(launch_vertex_tau(g->d, g->V, g->chirt, fact, ctx->st));
     g->have_V = true;
     return TPSC_OK;
@@ -770,8 +818,16 @@ int run_self(tpsc_ctx *ctx) {
     if (!g || !g->have_V) return fail(ctx, TPSC_ERR_STATE, "the vertex V(r, tau) has not been computed");
     const double fact = ctx->U * (3.0 * ctx->Usp + ctx->Uch) / 8.0;
     const GridDev &d = g->d;
-    CK(launch_sigma_boundary(d, g->Grt, g->V, g->dchirt0, g->dG0p, g->mu0, fact, g->dS, ctx->st));
-    CK(launch_sigma_slice(d, g->Grt, g->V, g->sigt, ctx->st));
+    // G(r, tau) as the chi0 stage left it (FP32 in the mixed form)
+    if (g->g_mixed) {
+        CK(launch_sigma_boundary(d, (const float *)g->Grt32, g->V, g->dchirt0, g->dG0p, g->mu0, fact, g->dS,
+                                 ctx->st));
+        CK(launch_sigma_slice(d, (const float *)g->Grt32, g->V, g->sigt, ctx->st));
+    } else {
+        CK(launch_sigma_boundary(d, (const double *)g->Grt, g->V, g->dchirt0, g->dG0p, g->mu0, fact, g->dS,
+                                 ctx->st));
+        CK(launch_sigma_slice(d, (const double *)g->Grt, g->V, g->sigt, ctx->st));
+    }
     CK(launch_sigma_tau(d, g->sigt, g->dS, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->T, ctx->st));
     CK(cudaMemcpyAsync(ctx->h_res, g->sinf, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
@@ -805,6 +861,20 @@ int trace_diff_G(tpsc_ctx *ctx, double pmu, double *tr, double *dtr = nullptr) {
     return TPSC_OK;
 }
 
+// The find_mu series covers the frequencies from jc = first n with
+// w_n >= kMomMuRange / kMomSeriesMax (capped at Nw0/2: then only the tail),
+// valid for |mu - mu0| <= dmax.
+void mu_series_cut(const tpsc_ctx *ctx, int *jc_out, double *dmax) {
+    const int NO = ctx->cur->d.nw0 / 2;
+    const double pt = PI * ctx->T;
+    int jc = (int)std::ceil((kMomMuRange / kMomSeriesMax / pt - 1.0) / 2.0);
+    jc = std::max(0, std::min(jc, NO));
+    const double wc = (2 * jc + 1) * pt;
+    const double zmin = wc - 2.0 * std::fabs(ctx->scal[TPSC_S_SIGMA_INF]) / wc;
+    *dmax = zmin > 0 ? kMomSeriesMax * zmin : 0.0;
+    *jc_out = jc;
+}
+
 int find_mu(tpsc_ctx *ctx) {
     Grid *g = ctx->cur;
     if (!g || !g->have_S) return fail(ctx, TPSC_ERR_STATE, "the self-energy has not been computed");
@@ -819,13 +889,9 @@ int find_mu(tpsc_ctx *ctx) {
     // only the frequencies below w_c are summed per evaluation.  |z| >= w_n -
     // |Im Sigma| >= w_n - 2 Sigma_inf / w_n bounds |z| on the series set.
     const GridDev &d = g->d;
-    const int NO = d.nw0 / 2;
-    const double pt = PI * ctx->T;
-    int jc = (int)std::ceil((kMomMuRange / kMomSeriesMax / pt - 1.0) / 2.0);
-    jc = std::max(0, std::min(jc, NO));
-    const double wc = (2 * jc + 1) * pt;
-    const double zmin = wc - 2.0 * std::fabs(ctx->scal[TPSC_S_SIGMA_INF]) / wc;
-    const double dmax = zmin > 0 ? kMomSeriesMax * zmin : 0.0;
+    int jc;
+    double dmax;
+    mu_series_cut(ctx, &jc, &dmax);
     double Cm[2 * kMomP + 1] = {0};
     const bool newton = (ctx->form & TPSC_FORM_NEWTON) != 0;
     if (newton && dmax > 0) {
@@ -1457,8 +1523,7 @@ int tpsc_launch_count(tpsc_ctx *ctx, long long *count) {
 
 int tpsc_set_form(tpsc_ctx *ctx, int form) {
     if (!ctx) return fail(nullptr, TPSC_ERR_ARG, "null context");
-    if (form != TPSC_FORM_REFERENCE && form != TPSC_FORM_NEWTON)
-        return fail(ctx, TPSC_ERR_ARG, "unknown form");
+    if (form < 0 || form > (TPSC_FORM_NEWTON | TPSC_FORM_MIXED)) return fail(ctx, TPSC_ERR_ARG, "unknown form");
     ctx->form = form;
     return TPSC_OK;
 }
@@ -1477,12 +1542,32 @@ int tpsc_run_kernel(tpsc_ctx *ctx, int which) {
     const GridDev &d = g->d;
     const double fact = ctx->U * (3.0 * ctx->Usp + ctx->Uch) / 8.0;
     switch (which) {
-        case 0: CK(launch_gslice(d, g->Grt, g->mu0, ctx->T, ctx->st)); break;
-        case 1: CK(launch_chi0_slice(d, g->Grt, g->chirt, g->chiq, ctx->st)); break;
+        case 0:
+            if (g->g_mixed)
+                CK(launch_gslice32(d, g->Grt32, g->mu0, ctx->T, ctx->st));
+            else
+                CK(launch_gslice(d, g->Grt, g->mu0, ctx->T, ctx->st));
+            break;
+        case 1:
+            if (g->g_mixed)
+                CK(launch_chi0_slice32(d, g->Grt32, g->chirt, g->chiq, ctx->st));
+            else
+                CK(launch_chi0_slice(d, g->Grt, g->chirt, g->chiq, ctx->st));
+            break;
         case 2: CK(launch_chi0_tau(d, g->chiq, g->dchiqt0, g->cinf, g->cinf2, ctx->T, ctx->st)); break;
-        case 3: CK(launch_vertex_q(d, g->chiq, g->V, ctx->U, ctx->Usp, ctx->Uch, ctx->T, ctx->st)); break;
+        case 3:
+            if (g->g_mixed)
+                CK(launch_vertex_q32(d, g->chiq, g->V, ctx->U, ctx->Usp, ctx->Uch, ctx->T, ctx->st));
+            else
+                CK(launch_vertex_q(d, g->chiq, g->V, ctx->U, ctx->Usp, ctx->Uch, ctx->T, ctx->st));
+            break;
         case 4: CK(launch_vertex_tau(d, g->V, g->chirt, fact, ctx->st)); break;
-        case 5: CK(launch_sigma_slice(d, g->Grt, g->V, g->sigt, ctx->st)); break;
+        case 5:
+            if (g->g_mixed)
+                CK(launch_sigma_slice(d, (const float *)g->Grt32, g->V, g->sigt, ctx->st));
+            else
+                CK(launch_sigma_slice(d, (const double *)g->Grt, g->V, g->sigt, ctx->st));
+            break;
         case 6:
             CK(launch_sigma_tau(d, g->sigt, g->dS, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->T, ctx->st));
             break;
@@ -1495,9 +1580,30 @@ int tpsc_run_kernel(tpsc_ctx *ctx, int which) {
             break;
         case 9:
             // chi0 slices followed by the in-place chi0 tau transform
-            CK(launch_chi0_slice(d, g->Grt, g->chirt, g->chiq, ctx->st));
+            if (g->g_mixed)
+                CK(launch_chi0_slice32(d, g->Grt32, g->chirt, g->chiq, ctx->st));
+            else
+                CK(launch_chi0_slice(d, g->Grt, g->chirt, g->chiq, ctx->st));
             CK(launch_chi0_tau(d, g->chiq, g->dchiqt0, g->cinf, g->cinf2, ctx->T, ctx->st));
             break;
+        case 10: {
+            // one Newton-form sum-rule evaluation at Usp: low frequencies, series above
+            int rc2 = ensure_moments(ctx, g);
+            if (rc2) return rc2;
+            int jdir, tail;
+            series_cut(g, ctx->Usp, &jdir, &tail);
+            CK(launch_sumrule(d, g->chiq, g->cinf, g->cinf2, ctx->Usp, -1.0, ctx->T, ctx->red, ctx->st, jdir, tail));
+            break;
+        }
+        case 11: {
+            // one Newton-form Tr(G - G0) evaluation at mu: frequencies below the series
+            int jc;
+            double dmax;
+            mu_series_cut(ctx, &jc, &dmax);
+            CK(launch_trace_diff_G(d, g->S, g->s2, g->s3, g->s4, g->sinf, g->mu0, ctx->scal[TPSC_S_MU], ctx->T,
+                                   ctx->red, ctx->st, jc));
+            break;
+        }
         default: return fail(ctx, TPSC_ERR_ARG, "unknown stage");
     }
     return TPSC_OK;
@@ -1509,20 +1615,38 @@ int tpsc_kernel_bytes(tpsc_ctx *ctx, int which, double *bytes) {
     const GridDev &d = ctx->cur->d;
     const double s = sizeof(double), n8 = d.n8, nb = d.nb, nw = d.nw0;
     const double tau = (nw + 1) * n8 * s;   // one (Nw0+1) x N8 real array
+    // G(r, tau) as the last solve stored it (FP32 in the mixed form)
+    const double gtau = ctx->cur->g_mixed ? tau / 2 : tau;
     const double half = nb * n8 * s;        // one (Nw0/2+1) x N8 real array
     const double cplx = (nw / 2) * n8 * 2 * s;
     double b;
     switch (which) {
-        case 0: b = tau; break;                       // write G(r, tau)
-        case 1: b = tau + 2 * half; break;            // read G, write chi0(r,tau), chi0(q,tau)
+        case 0: b = gtau; break;                      // write G(r, tau)
+        case 1: b = gtau + 2 * half; break;           // read G, write chi0(r,tau), chi0(q,tau)
         case 2: b = 2 * half; break;                  // read + write chi0(q, .)
         case 3: b = 2 * half; break;                  // read chi0(q, iqn), write V(r, iqn)
         case 4: b = 3 * half; break;                  // read V, chi0(r, tau); write V
-        case 5: b = tau + half + tau; break;          // read G, V; write Sigma(k, tau)
+        case 5: b = gtau + half + tau; break;         // read G, V; write Sigma(k, tau)
         case 6: b = tau + cplx; break;                // read Sigma(k, tau); write S
         case 7: b = half; break;                      // read chi0(q, iqn)
         case 8: b = cplx; break;                      // read S
-        case 9: b = tau + 2 * half + 2 * half; break; // stages 1 and 2
+        case 9: b = gtau + 2 * half + 2 * half; break; // stages 1 and 2
+        case 10: {                                     // read chi0(q, iqn), j < jdir
+            Grid *g = ctx->cur;
+            int rc2 = ensure_moments(ctx, g);
+            if (rc2) return rc2;
+            int jdir, tail;
+            series_cut(g, ctx->Usp, &jdir, &tail);
+            b = (double)jdir * d.n8 * s + (tail ? 2 * d.n8 * s : 0.0);
+            break;
+        }
+        case 11: {                                     // read S, j < jc
+            int jc;
+            double dmax;
+            mu_series_cut(ctx, &jc, &dmax);
+            b = (double)jc * d.n8 * 2 * s;
+            break;
+        }
         default: return fail(ctx, TPSC_ERR_ARG, "unknown stage");
     }
     *bytes = b;

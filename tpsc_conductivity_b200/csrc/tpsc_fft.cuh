@@ -1,4 +1,5 @@
-// tpsc_fft.cuh -- FP64 FFT building blocks for sm_100a.
+// tpsc_fft.cuh -- FFT building blocks for sm_100a, FP64 (double2) and FP32
+// (float2) complex data.
 //
 // * in-register radix-2/4/8/16 DFTs (exact constants, standard split-radix
 //   style recursion);
@@ -11,6 +12,12 @@
 //
 // DCT-I here is FFTW's REDFT00 (unnormalised):
 //   Y_k = X_0 + (-1)^k X_{n-1} + 2 sum_{j=1}^{n-2} X_j cos(pi j k/(n-1)).
+//
+// FP32 transforms take their inter-pass twiddles from a float4 table
+// (cos_hi, sin_hi, cos_lo, sin_lo) with hi + lo the twiddle to ~48 bits and
+// form the twiddle product with FMAs around the lo correction, so the
+// twiddle enters to full FP32 accuracy of the product (compensated twiddles);
+// the radix-16 constants and the butterfly sums are plain FP32.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -23,10 +30,49 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
 }
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 // multiply by -i (SIGN = -1) or +i (SIGN = +1)
-template <int SIGN>
-__device__ __forceinline__ double2 mul_i(double2 a) {
-    return SIGN < 0 ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
+template <int SIGN, class C>
+__device__ __forceinline__ C mul_i(C a) {
+    return SIGN < 0 ? C{a.y, -a.x} : C{-a.y, a.x};
+}
+
+// real type of a complex type
+template <class C>
+struct real_of;
+template <>
+struct real_of<double2> {
+    using type = double;
+};
+template <>
+struct real_of<float2> {
+    using type = float;
+};
+
+// the twiddle product v * w (conj(w) for SIGN > 0), w from the table of the
+// transform's precision: double2 for FP64; float4 (hi, lo) for FP32
+template <int SIGN, bool SMEM>
+__device__ __forceinline__ double2 twiddle(double2 v, const double2 *__restrict__ tw, int m) {
+    double2 w = SMEM ? tw[m] : __ldg(&tw[m]);
+    if (SIGN > 0) w.y = -w.y;
+    return cmul(v, w);
+}
+template <int SIGN, bool SMEM>
+__device__ __forceinline__ float2 twiddle(float2 v, const float4 *__restrict__ tw, int m) {
+    float4 w = SMEM ? tw[m] : __ldg(&tw[m]);
+    if (SIGN > 0) {
+        w.y = -w.y;
+        w.w = -w.w;
+    }
+    // (a + i b)(c + i d) with c = w.x + w.z, d = w.y + w.w: the lo parts as a
+    // correction term, the hi parts fused into it
+    const float cr = fmaf(v.x, w.z, -v.y * w.w), ci = fmaf(v.x, w.w, v.y * w.z);
+    return make_float2(fmaf(v.x, w.x, fmaf(-v.y, w.y, cr)), fmaf(v.x, w.y, fmaf(v.y, w.x, ci)));
 }
 
 // exp(sign * 2 pi i m / 16) for the constant twiddles of the radix-8/16
@@ -57,19 +103,26 @@ __device__ __forceinline__ double2 w16(int m, int sign) {
     return make_double2(c, sign * s);
 }
 
+template <class C>
+__device__ __forceinline__ C w16c(int m, int sign) {
+    const double2 w = w16(m, sign);
+    using T = typename real_of<C>::type;
+    return C{(T)w.x, (T)w.y};
+}
+
 // In-register DFT of length R on v[0..R) with stride S inside the array
 // (elements v[OFF + k*S]).  X_k = sum_j x_j exp(SIGN 2 pi i jk/R).
-template <int SIGN, int R, int S = 1, int OFF = 0, int NV>
-__device__ __forceinline__ void dft(double2 (&v)[NV]) {
+template <int SIGN, int R, int S = 1, int OFF = 0, int NV, class C>
+__device__ __forceinline__ void dft(C (&v)[NV]) {
     if constexpr (R == 1) {
         return;
     } else if constexpr (R == 2) {
-        double2 a = v[OFF], b = v[OFF + S];
+        C a = v[OFF], b = v[OFF + S];
         v[OFF] = cadd(a, b);
         v[OFF + S] = csub(a, b);
     } else if constexpr (R == 4) {
-        double2 a = v[OFF], b = v[OFF + S], c = v[OFF + 2 * S], d = v[OFF + 3 * S];
-        double2 t0 = cadd(a, c), t1 = csub(a, c), t2 = cadd(b, d), t3 = mul_i<SIGN>(csub(b, d));
+        C a = v[OFF], b = v[OFF + S], c = v[OFF + 2 * S], d = v[OFF + 3 * S];
+        C t0 = cadd(a, c), t1 = csub(a, c), t2 = cadd(b, d), t3 = mul_i<SIGN>(csub(b, d));
         v[OFF] = cadd(t0, t2);
         v[OFF + 2 * S] = csub(t0, t2);
         v[OFF + S] = cadd(t1, t3);
@@ -78,7 +131,7 @@ __device__ __forceinline__ void dft(double2 (&v)[NV]) {
         // radix-2 decimation in time: even/odd halves are DFTs of length R/2
         // taken on the sub-sequences at stride 2S; results interleaved back.
         constexpr int H = R / 2;
-        double2 e[H], o[H];
+        C e[H], o[H];
 #pragma unroll
         for (int k = 0; k < H; ++k) {
             e[k] = v[OFF + (2 * k) * S];
@@ -88,8 +141,8 @@ __device__ __forceinline__ void dft(double2 (&v)[NV]) {
         dft<SIGN, H, 1, 0>(o);
 #pragma unroll
         for (int k = 0; k < H; ++k) {
-            const double2 w = w16((16 / R) * k, SIGN);
-            double2 t = cmul(o[k], w);
+            const C w = w16c<C>((16 / R) * k, SIGN);
+            C t = cmul(o[k], w);
             v[OFF + k * S] = cadd(e[k], t);
             v[OFF + (k + H) * S] = csub(e[k], t);
         }
@@ -118,11 +171,13 @@ __device__ __forceinline__ void group_sync(int grp) {
 
 // Loaders / storers for the first and last FFT pass.  `In` returns input
 // element j of the sequence; `Out` receives output element k.
-struct ScratchIO {
-    double2 *x;
-    __device__ __forceinline__ double2 operator()(int j) const { return x[pidx(j)]; }
-    __device__ __forceinline__ void operator()(int k, double2 v) const { x[pidx(k)] = v; }
+template <class C>
+struct ScratchIOT {
+    C *x;
+    __device__ __forceinline__ C operator()(int j) const { return x[pidx(j)]; }
+    __device__ __forceinline__ void operator()(int k, C v) const { x[pidx(k)] = v; }
 };
+using ScratchIO = ScratchIOT<double2>;
 
 // One Stockham pass of radix R over a length-N sequence, performed by a group
 // of G threads holding E points each; thread t does E/R butterflies
@@ -133,11 +188,11 @@ struct ScratchIO {
 // a barrier between the first pass's reads and its writes, for an `in` that
 // reads x itself.
 template <int N, int G, int R, int SIGN, int E, bool SMEM_TW, bool FIRST, bool LAST, bool SYNC_IN, class In,
-          class Out>
-__device__ __forceinline__ void stockham_pass(double2 *x, int t, int Ns, const double2 *__restrict__ tw, int grp,
-                                              const In &in, const Out &out) {
+          class Out, class C, class TW>
+__device__ __forceinline__ void stockham_pass(C *x, int t, int Ns, const TW *__restrict__ tw, int grp, const In &in,
+                                              const Out &out) {
     constexpr int NB = E / R;  // butterflies per thread
-    double2 v[E];
+    C v[E];
 #pragma unroll
     for (int u = 0; u < NB; ++u) {
         const int b = t + G * u;
@@ -156,13 +211,9 @@ __device__ __forceinline__ void stockham_pass(double2 *x, int t, int Ns, const d
             // twiddle exp(SIGN 2 pi i k q / (Ns R)) = tw[k q N/(Ns R)] (conjugated for SIGN>0)
             const int step = k * (N / (Ns * R));
 #pragma unroll
-            for (int q = 1; q < R; ++q) {
-                double2 w = SMEM_TW ? tw[(step * q) & (N - 1)] : __ldg(&tw[(step * q) & (N - 1)]);
-                if (SIGN > 0) w.y = -w.y;
-                v[u * R + q] = cmul(v[u * R + q], w);
-            }
+            for (int q = 1; q < R; ++q) v[u * R + q] = twiddle<SIGN, SMEM_TW>(v[u * R + q], tw, (step * q) & (N - 1));
         }
-        double2 r[R];
+        C r[R];
 #pragma unroll
         for (int q = 0; q < R; ++q) r[q] = v[u * R + q];
         dft<SIGN, R>(r);
@@ -201,9 +252,9 @@ struct FftPlan {
     static constexpr int NPASS = P16 + (RLAST > 1 ? 1 : 0);
 };
 
-template <int N, int SIGN, bool SMEM_TW, bool INPLACE, int P, class In, class Out>
-__device__ __forceinline__ void fft_passes(double2 *x, int t, int Ns, const double2 *__restrict__ tw, int grp,
-                                           const In &in, const Out &out) {
+template <int N, int SIGN, bool SMEM_TW, bool INPLACE, int P, class In, class Out, class C, class TW>
+__device__ __forceinline__ void fft_passes(C *x, int t, int Ns, const TW *__restrict__ tw, int grp, const In &in,
+                                           const Out &out) {
     constexpr int G = FftPlan<N>::G;
     constexpr int E = FftPlan<N>::E;
     constexpr int NP = FftPlan<N>::NPASS;
@@ -224,18 +275,18 @@ __device__ __forceinline__ void fft_passes(double2 *x, int t, int Ns, const doub
 // the FFT has more than one pass, x is free again when the call returns.
 // INPLACE: `in` reads x (the first pass then holds its writes back until
 // every thread of the group has read its inputs).
-template <int N, int SIGN, bool SMEM_TW = false, bool INPLACE = false, class In, class Out>
-__device__ __forceinline__ void group_fft_io(double2 *x, int t, const double2 *__restrict__ tw, int grp,
-                                             const In &in, const Out &out) {
+template <int N, int SIGN, bool SMEM_TW = false, bool INPLACE = false, class In, class Out, class C, class TW>
+__device__ __forceinline__ void group_fft_io(C *x, int t, const TW *__restrict__ tw, int grp, const In &in,
+                                             const Out &out) {
     static_assert(N >= 4 && (N & (N - 1)) == 0, "power of two >= 4");
     fft_passes<N, SIGN, SMEM_TW, INPLACE, 0>(x, t, 1, tw, grp, in, out);
     if constexpr (FftPlan<N>::NPASS > 1) group_sync<FftPlan<N>::G>(grp);
 }
 
 // In-place FFT of x[0..N) (padded layout).
-template <int N, int SIGN, bool SMEM_TW = false>
-__device__ __forceinline__ void group_fft(double2 *x, int t, const double2 *__restrict__ tw, int grp) {
-    const ScratchIO io{x};
+template <int N, int SIGN, bool SMEM_TW = false, class C, class TW>
+__device__ __forceinline__ void group_fft(C *x, int t, const TW *__restrict__ tw, int grp) {
+    const ScratchIOT<C> io{x};
     group_fft_io<N, SIGN, SMEM_TW, true>(x, t, tw, grp, io, io);
 }
 
@@ -246,8 +297,8 @@ __device__ __forceinline__ void group_fft(double2 *x, int t, const double2 *__re
 // threads of the block must call.  Two lines (rows, then columns) go through
 // one complex FFT of their even extension; the first FFT pass reads the
 // lines straight from S and the last pass writes outputs k < NBK back.
-template <int NBK>
-__device__ void dct2_slice(double *S, double2 *scr, const double2 *tw) {
+template <int NBK, class T, class C, class TW>
+__device__ void dct2_slice(T *S, C *scr, const TW *tw) {
     constexpr int L = 2 * (NBK - 1);
     constexpr int G = FftPlan<L>::G;
     constexpr int NPAIR = (NBK + 1) / 2;
@@ -255,7 +306,7 @@ __device__ void dct2_slice(double *S, double2 *scr, const double2 *tw) {
     const int grp = tid / G;
     const int t = tid % G;
     const int ngrp = blockDim.x / G;
-    double2 *x = scr + grp * padded_len(L);
+    C *x = scr + grp * padded_len(L);
 #pragma unroll 1
     for (int pass = 0; pass < 2; ++pass) {
         // pass 0: rows (stride 1 along the line, NBK between lines)
@@ -266,13 +317,13 @@ __device__ void dct2_slice(double *S, double2 *scr, const double2 *tw) {
         for (int p = grp; p < NPAIR; p += ngrp) {
             const int r0 = 2 * p, r1 = 2 * p + 1;
             const bool two = r1 < NBK;
-            double *a = S + r0 * ls;
-            double *b = S + (two ? r1 : r0) * ls;
-            auto in = [&](int j) -> double2 {
+            T *a = S + r0 * ls;
+            T *b = S + (two ? r1 : r0) * ls;
+            auto in = [&](int j) -> C {
                 const int c = j < NBK ? j : L - j;
-                return make_double2(a[c * es], two ? b[c * es] : 0.0);
+                return C{a[c * es], two ? b[c * es] : (T)0};
             };
-            auto out = [&](int k, double2 z) {
+            auto out = [&](int k, C z) {
                 if (k < NBK) {
                     a[k * es] = z.x;
                     if (two) b[k * es] = z.y;

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <atomic>
 
 #include "tpsc_device.cuh"
@@ -197,10 +198,10 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
 
 // d/dtau G(r,0+-) and d/dtau chi0(r,0), d/dtau chi0(q,0): the spline's left
 // end condition (src/chi0.cpp:323-367, 420-447).  One CTA.
-template <int NBK>
+template <int NBK, class GT>
 __global__ void __launch_bounds__(kSliceThreads, 1)
     k_chi0_boundary(const double *__restrict__ ek, const double *__restrict__ er, const uint32_t *__restrict__ lm,
-                    const double2 *__restrict__ tw, const double *__restrict__ Grt, int n8, double mu0, double T,
+                    const double2 *__restrict__ tw, const GT *__restrict__ Grt, int n8, double mu0, double T,
                     double nk02, double *__restrict__ dG0p, double *__restrict__ dtau_chirt0,
                     double *__restrict__ dtau_chiqt0) {
     extern __shared__ __align__(16) double S[];
@@ -275,10 +276,10 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
 
 // d/dtau Sigma(k, 0) and d/dtau Sigma(k, beta): the spline end conditions of
 // the self-energy (src/green.cpp:1743-1817).  One CTA, two 2D DCT-I.
-template <int NBK>
+template <int NBK, class GT>
 __global__ void __launch_bounds__(kSliceThreads, 1)
     k_sigma_boundary(const double *__restrict__ er, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
-                     const double *__restrict__ Grt, const double *__restrict__ V, const double *__restrict__ dtau_chirt0,
+                     const GT *__restrict__ Grt, const double *__restrict__ V, const double *__restrict__ dtau_chirt0,
                      const double *__restrict__ dG0p, int n8, int nw0, int n8p, double mu0, double fact,
                      double *__restrict__ dS) {
     extern __shared__ __align__(16) double S[];
@@ -286,7 +287,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     const int nb = nw0 / 2 + 1;
 #pragma unroll 1
     for (int side = 0; side < 2; ++side) {
-        const double *g = Grt + (side == 0 ? 0 : (size_t)nw0 * n8);
+        const GT *g = Grt + (side == 0 ? 0 : (size_t)nw0 * n8);
         for (int o = threadIdx.x; o < n8; o += blockDim.x) {
             int l, m;
             oct_lm(lm, o, l, m);
@@ -313,20 +314,22 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
 
 // Sigma(k, tau_j) = DCT-I[ G(r, tau_j) V(r, tau_j) ], j = 0..Nw0, with
 // V(r, tau_j) = V(r, beta - tau_j) for tau_j > beta/2 (src/green.cpp:1822-1885).
-template <int NBK>
+// G in FP64, or in FP32 in the mixed-precision form (the product and the
+// transform in FP64 either way).
+template <int NBK, class GT>
 __global__ void __launch_bounds__(kSliceThreads, 1)
-    k_sigma_slice(const double *__restrict__ Grt, const double *__restrict__ V, const uint32_t *__restrict__ lm,
+    k_sigma_slice(const GT *__restrict__ Grt, const double *__restrict__ V, const uint32_t *__restrict__ lm,
                   const double2 *__restrict__ tw, int n8, int nw0, double *__restrict__ sigt) {
     extern __shared__ __align__(16) double S[];
     const double2 *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
     const int nb = nw0 / 2 + 1;
     const int jv = j < nb ? j : nw0 - j;
-    const double *g = Grt + (size_t)j * n8;
+    const GT *g = Grt + (size_t)j * n8;
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
         oct_lm(lm, o, l, m);
-        put_sym<NBK>(S, l, m, g[o] * V[bidx(jv, o, nb)]);
+        put_sym<NBK>(S, l, m, (double)g[o] * V[bidx(jv, o, nb)]);
     }
     __syncthreads();
     dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
@@ -640,12 +643,12 @@ __global__ void __launch_bounds__(kRedThreads)
     k_sumrule(const double4 *__restrict__ chiq, const double *__restrict__ cinf, const double *__restrict__ cinf2,
               const double *__restrict__ w16, const double *__restrict__ tailq, int nb, int jdir, int tail, double Uv,
               double sgn, double T, double scale, Reduce r) {
+    const double hu = sgn * Uv / 2.0;
+    double v = 0.0, dv = 0.0, tv = 0.0, tdv = 0.0;
     const int blk = blockIdx.x;
     const int o0 = 4 * blk;
     const double4 w = *reinterpret_cast<const double4 *>(w16 + o0);
     const double ww[4] = {w.x, w.y, w.z, w.w};
-    const double hu = sgn * Uv / 2.0;
-    double v = 0.0, dv = 0.0;
     const double4 *col = chiq + (size_t)blk * nb;
     for (int j = threadIdx.x; j < jdir; j += blockDim.x) {
         const double4 x = ld_stream4(&col[j]);
@@ -661,13 +664,11 @@ __global__ void __launch_bounds__(kRedThreads)
         v += f * sv;
         dv += f * sd;
     }
-    dv *= -0.5 * sgn;
     // tail: n = nwmax+1 .. 2 nwmax
     const int nwmax = nb - 1;
     const double tw = 2.0 * 3.141592653589793 * T;
     const double wn1 = (nwmax + 1) * tw;
     const double x1 = 1.0 / (wn1 * wn1);
-    double tv = 0.0, tdv = 0.0;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
         if (ww[c] == 0.0 || !tail) continue;
@@ -691,7 +692,36 @@ __global__ void __launch_bounds__(kRedThreads)
             }
         }
     }
+    dv *= -0.5 * sgn;
     double out[2] = {scale * (v + tv), scale * (dv + tdv)};
+    grid_finish<2>(out, r, 0.0);
+}
+
+// The Newton form's sum-rule evaluation: only the stored frequencies
+// j < jdir (the rest enters as the moment series on the host), over a
+// flattened (column block, j) index so that every thread has independent
+// loads in flight; a short grid.
+__global__ void __launch_bounds__(kRedThreads)
+    k_sumrule_low(const double4 *__restrict__ chiq, const double *__restrict__ w16, int nb, int nblk, int jdir,
+                  double Uv, double sgn, double scale, Reduce r) {
+    const double hu = sgn * Uv / 2.0;
+    double v = 0.0, dv = 0.0;
+    const long long total = (long long)nblk * jdir;
+    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < total;
+         it += (long long)gridDim.x * blockDim.x) {
+        const int blk = (int)(it / jdir), j = (int)(it - (long long)blk * jdir);
+        const double4 x = ld_stream4(&chiq[(size_t)blk * nb + j]);
+        const double4 w = reinterpret_cast<const double4 *>(w16)[blk];
+        const double f = j == 0 ? 0.5 : 1.0;
+        const double xs[4] = {x.x, x.y, x.z, x.w}, ww[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double q = xs[c] / (1.0 + hu * xs[c]);
+            v += f * ww[c] * (q - xs[c]);
+            dv += f * ww[c] * q * q;
+        }
+    }
+    double out[2] = {scale * v, scale * (-0.5 * sgn) * dv};
     grid_finish<2>(out, r, 0.0);
 }
 
@@ -830,8 +860,11 @@ __global__ void __launch_bounds__(kRedThreads)
                    const double *__restrict__ s4, const double *__restrict__ sinfp, const double *__restrict__ ek,
                    const double *__restrict__ w16, int nw0, double mu0, double pmu, double T, int jdir, int tail,
                    Reduce r) {
-    const int blk = blockIdx.x, o0 = 4 * blk, NO = nw0 / 2;
+    const int NO = nw0 / 2;
     const double sinf = sinfp[0];
+    double v = 0.0, dv = 0.0;
+    const int blk = blockIdx.x;
+    const int o0 = 4 * blk;
     double ww[4], e[4], c2[4], c3[4], c4[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
@@ -843,7 +876,6 @@ __global__ void __launch_bounds__(kRedThreads)
         c4[c] = ok ? s4[o0 + c] : 0.0;
     }
     const double pt = 3.141592653589793 * T;
-    double v = 0.0, dv = 0.0;
     const double4 *row = reinterpret_cast<const double4 *>(S + (size_t)blk * 4 * NO);
     for (int j = threadIdx.x; j < jdir; j += blockDim.x) {
         const double wn = (2 * j + 1) * pt;
@@ -869,6 +901,40 @@ __global__ void __launch_bounds__(kRedThreads)
             const double rS = -c2[c] * i2 + c4[c] * i2 * i2;
             const double iS = -sinf * i1 + c3[c] * i2 * i1;
             trdiff_term(wn, rS, iS, e[c], mu0, pmu, ww[c], v, dv);
+        }
+    }
+    double out[2] = {v, dv};
+    grid_finish<2>(out, r, 0.0);
+}
+
+// The Newton form's Tr(G - G0) evaluation: only the stored frequencies
+// j < jdir, over a flattened (column block, j) index, a short grid.
+__global__ void __launch_bounds__(kRedThreads)
+    k_trace_diff_G_low(const double2 *__restrict__ S, const double *__restrict__ s2, const double *__restrict__ s3,
+                       const double *__restrict__ sinfp, const double *__restrict__ ek,
+                       const double *__restrict__ w16, int nw0, int nblk, double mu0, double pmu, double T, int jdir,
+                       Reduce r) {
+    const int NO = nw0 / 2;
+    const double sinf = sinfp[0];
+    const double pt = 3.141592653589793 * T;
+    double v = 0.0, dv = 0.0;
+    const long long total = (long long)nblk * jdir;
+    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < total;
+         it += (long long)gridDim.x * blockDim.x) {
+        const int blk = (int)(it / jdir), j = (int)(it - (long long)blk * jdir);
+        const int o0 = 4 * blk;
+        const double4 *row = reinterpret_cast<const double4 *>(S + (size_t)blk * 4 * NO);
+        const double4 p = ld_stream4(&row[2 * j]), q = ld_stream4(&row[2 * j + 1]);
+        const double2 sv[4] = {make_double2(p.x, p.y), make_double2(p.z, p.w), make_double2(q.x, q.y),
+                               make_double2(q.z, q.w)};
+        const double wn = (2 * j + 1) * pt, i1 = 1.0 / wn;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double w = __ldg(&w16[o0 + c]);
+            if (w == 0.0) continue;
+            double rS, iS;
+            sigma_full(i1, sinf, __ldg(&s2[o0 + c]), __ldg(&s3[o0 + c]), sv[c], rS, iS);
+            trdiff_term(wn, rS, iS, __ldg(&ek[o0 + c]), mu0, pmu, w, v, dv);
         }
     }
     double out[2] = {v, dv};
@@ -1036,48 +1102,111 @@ __global__ void __launch_bounds__(kRedThreads)
 
 // chi0max and its wave vector (src/chi0.cpp:703-717): the reference scans l
 // and then m downwards keeping the first strict maximum, i.e. among equal
-// maxima the largest l, then the largest m.  One block.
-__global__ void k_chi0max(const double *__restrict__ chiq, const uint32_t *__restrict__ lm, int n8, int nb,
-                          double *result) {
-    double best = 0.0;
-    int bl = 0, bm = 0;
-    bool have = false;
+// maxima the largest l, then the largest m.  That is the maximum of the
+// total order (value, l, m), so any reduction tree gives the reference's
+// point: per-thread scans, then shuffle trees.  One block.
+struct MaxPt {
+    double v;
+    int l, m;
+};
+__device__ __forceinline__ bool better(const MaxPt &a, const MaxPt &b) {
+    return a.v > b.v || (a.v == b.v && (a.l > b.l || (a.l == b.l && a.m > b.m)));
+}
+__device__ __forceinline__ MaxPt max_shfl(MaxPt a, int off) {
+    MaxPt b;
+    b.v = __shfl_down_sync(0xffffffffu, a.v, off);
+    b.l = __shfl_down_sync(0xffffffffu, a.l, off);
+    b.m = __shfl_down_sync(0xffffffffu, a.m, off);
+    return better(b, a) ? b : a;
+}
+__global__ void __launch_bounds__(1024)
+    k_chi0max(const double *__restrict__ chiq, const uint32_t *__restrict__ lm, int n8, int nb, double *result) {
+    // values <= 0 never win: the reference's scan starts from chi0max = 0
+    MaxPt best{0.0, -1, -1};
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
         oct_lm(lm, o, l, m);
-        const double v = chiq[bidx(0, o, nb)];
-        if (!(v > 0.0)) continue;  // the scan starts from chi0max = 0
-        if (!have || v > best || (v == best && (l > bl || (l == bl && m > bm)))) {
-            best = v;
-            bl = l;
-            bm = m;
-            have = true;
+        const MaxPt c{chiq[bidx(0, o, nb)], l, m};
+        if (c.v > 0.0 && better(c, best)) best = c;
+    }
+    for (int off = 16; off > 0; off >>= 1) best = max_shfl(best, off);
+    __shared__ MaxPt w[32];
+    if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        best = threadIdx.x < (int)(blockDim.x >> 5) ? w[threadIdx.x] : MaxPt{0.0, -1, -1};
+        for (int off = 16; off > 0; off >>= 1) best = max_shfl(best, off);
+        if (threadIdx.x == 0) {
+            result[0] = best.l < 0 ? 0.0 : best.v;
+            result[1] = best.l < 0 ? 0 : best.l;
+            result[2] = best.m < 0 ? 0 : best.m;
         }
     }
-    __shared__ double sv[1024];
-    __shared__ int sl[1024], sm[1024], sh[1024];
-    sv[threadIdx.x] = best;
-    sl[threadIdx.x] = bl;
-    sm[threadIdx.x] = bm;
-    sh[threadIdx.x] = have;
-    __syncthreads();
+}
+
+// mu0 of the finite lattice by safeguarded Newton on the density
+// n(mu) = sum_o w 2 f(eps_o - mu) / L^2 (the function of green0::find_mu /
+// ddensity_mu_PBC, src/green0.cpp:182-262) in one block: each iteration is a
+// block reduction of n(mu) - n and dn/dmu in a fixed order; the Newton step
+// is kept inside the bracket [-8, 8] that the sign of n - n0 shrinks, a
+// bisection otherwise; stops when the step is below 1e-15 (1 + |mu|).
+// The Newton form's replacement of the host root search.
+__global__ void __launch_bounds__(1024)
+    k_mu0_newton(const double *__restrict__ ek, const uint32_t *__restrict__ lm, int n8, int nbk, double n, double T,
+                 double nk2, double *result) {
+    __shared__ double red[32][2];
+    __shared__ double s_mu;
+    __shared__ int s_done, s_it;
+    double lo = -8.0, hi = 8.0, mu = 0.0;
     if (threadIdx.x == 0) {
-        double b = 0.0;
-        int L = 0, M = 0;
-        bool h = false;
-        for (int i = 0; i < (int)blockDim.x; ++i) {
-            if (!sh[i]) continue;
-            const double v = sv[i];
-            if (!h || v > b || (v == b && (sl[i] > L || (sl[i] == L && sm[i] > M)))) {
-                b = v;
-                L = sl[i];
-                M = sm[i];
-                h = true;
-            }
+        s_mu = 0.0;
+        s_done = 0;
+    }
+    __syncthreads();
+    for (int it = 0; it < 200; ++it) {
+        mu = s_mu;
+        double v = 0.0, dv = 0.0;
+        for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+            int l, m;
+            oct_lm(lm, o, l, m);
+            const int w = oct_weight(8, l, m, nbk);
+            const double f = 1.0 / (exp((ek[o] - mu) / T) + 1.0);
+            v += 2 * w * f / nk2;
+            dv += 2 * w * f * (1.0 - f) / (T * nk2);
         }
-        result[0] = b;
-        result[1] = L;
-        result[2] = M;
+        for (int off = 16; off > 0; off >>= 1) {
+            v += __shfl_down_sync(0xffffffffu, v, off);
+            dv += __shfl_down_sync(0xffffffffu, dv, off);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            red[threadIdx.x >> 5][0] = v;
+            red[threadIdx.x >> 5][1] = dv;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double V = 0.0, D = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+                V += red[w][0];
+                D += red[w][1];
+            }
+            const double F = V - n;
+            if (F > 0)
+                hi = mu;
+            else
+                lo = mu;
+            double mn = (D > 0) ? mu - F / D : 0.5 * (lo + hi);
+            if (!(mn > lo && mn < hi)) mn = 0.5 * (lo + hi);
+            const bool done = F == 0.0 || fabs(mn - mu) <= 1e-15 * (1.0 + fabs(mu));
+            s_mu = done && F == 0.0 ? mu : mn;
+            s_done = done;
+            s_it = it + 1;
+        }
+        __syncthreads();
+        if (s_done) break;
+    }
+    if (threadIdx.x == 0) {
+        result[0] = s_mu;
+        result[1] = s_it;
     }
 }
 
@@ -1229,14 +1358,15 @@ struct RunGslice {
 };
 template <int NBK>
 struct RunChi0Boundary {
-    static cudaError_t run(const GridDev *g, const double *Grt, double mu0, double T, double *dG0p, double *dchirt0,
+    template <class GT>
+    static cudaError_t run(const GridDev *g, const GT *Grt, double mu0, double T, double *dG0p, double *dchirt0,
                            double *dchiqt0, cudaStream_t st) {
         const size_t sm = SliceSmem<NBK>::bytes;
-        cudaError_t e = set_smem(k_chi0_boundary<NBK>, sm);
+        cudaError_t e = set_smem(k_chi0_boundary<NBK, GT>, sm);
         if (e != cudaSuccess) return e;
         const double nk02 = (double)g->nk0 * g->nk0;
-        k_chi0_boundary<NBK><<<1, kSliceThreads, sm, st>>>(g->ek, g->er, g->lm, g->tw_k, Grt, g->n8, mu0, T, nk02,
-                                                            dG0p, dchirt0, dchiqt0);
+        k_chi0_boundary<NBK, GT><<<1, kSliceThreads, sm, st>>>(g->ek, g->er, g->lm, g->tw_k, Grt, g->n8, mu0, T,
+                                                                nk02, dG0p, dchirt0, dchiqt0);
         return launched();
     }
 };
@@ -1265,23 +1395,25 @@ struct RunVertexQ {
 };
 template <int NBK>
 struct RunSigmaBoundary {
-    static cudaError_t run(const GridDev *g, const double *Grt, const double *V, const double *dchirt0,
+    template <class GT>
+    static cudaError_t run(const GridDev *g, const GT *Grt, const double *V, const double *dchirt0,
                            const double *dG0p, double mu0, double fact, double *dS, cudaStream_t st) {
         const size_t sm = SliceSmem<NBK>::bytes;
-        cudaError_t e = set_smem(k_sigma_boundary<NBK>, sm);
+        cudaError_t e = set_smem(k_sigma_boundary<NBK, GT>, sm);
         if (e != cudaSuccess) return e;
-        k_sigma_boundary<NBK><<<1, kSliceThreads, sm, st>>>(g->er, g->lm, g->tw_k, Grt, V, dchirt0, dG0p, g->n8,
-                                                             g->nw0, g->n8p, mu0, fact, dS);
+        k_sigma_boundary<NBK, GT><<<1, kSliceThreads, sm, st>>>(g->er, g->lm, g->tw_k, Grt, V, dchirt0, dG0p, g->n8,
+                                                                 g->nw0, g->n8p, mu0, fact, dS);
         return launched();
     }
 };
 template <int NBK>
 struct RunSigmaSlice {
-    static cudaError_t run(const GridDev *g, const double *Grt, const double *V, double *sigt, cudaStream_t st) {
+    template <class GT>
+    static cudaError_t run(const GridDev *g, const GT *Grt, const double *V, double *sigt, cudaStream_t st) {
         const size_t sm = SliceSmem<NBK>::bytes;
-        cudaError_t e = set_smem(k_sigma_slice<NBK>, sm);
+        cudaError_t e = set_smem(k_sigma_slice<NBK, GT>, sm);
         if (e != cudaSuccess) return e;
-        k_sigma_slice<NBK><<<g->nw0 + 1, kSliceThreads, sm, st>>>(Grt, V, g->lm, g->tw_k, g->n8, g->nw0, sigt);
+        k_sigma_slice<NBK, GT><<<g->nw0 + 1, kSliceThreads, sm, st>>>(Grt, V, g->lm, g->tw_k, g->n8, g->nw0, sigt);
         return launched();
     }
 };
@@ -1348,6 +1480,15 @@ cudaError_t launch_chi0_boundary(const GridDev &g, const double *Grt, double mu0
                                  double *dtau_chirt0, double *dtau_chiqt0, cudaStream_t st) {
     return dispatch_nbk<RunChi0Boundary>(g.nbk, &g, Grt, mu0, T, dG0p, dtau_chirt0, dtau_chiqt0, st);
 }
+cudaError_t launch_chi0_boundary(const GridDev &g, const float *Grt, double mu0, double T, double *dG0p,
+                                 double *dtau_chirt0, double *dtau_chiqt0, cudaStream_t st) {
+    return dispatch_nbk<RunChi0Boundary>(g.nbk, &g, Grt, mu0, T, dG0p, dtau_chirt0, dtau_chiqt0, st);
+}
+
+cudaError_t launch_gk_table(const GridDev &g, double mu0, double T, cudaStream_t st) {
+    k_gk_table<<<(g.n8 + 255) / 256, 256, 0, st>>>(g.ek, g.n8, mu0, T, (double)g.nk0 * g.nk0, g.gk);
+    return launched();
+}
 
 cudaError_t launch_chi0_slice(const GridDev &g, const double *Grt, double *chirt, double *chiq, cudaStream_t st) {
     return dispatch_nbk<RunChi0Slice>(g.nbk, &g, Grt, chirt, chiq, st);
@@ -1362,8 +1503,16 @@ cudaError_t launch_sumrule(const GridDev &g, const double *chiq, const double *c
                            double Uv, double sign, double T, Reduce r, cudaStream_t st, int jdir, int tail) {
     const double Nq = 4.0 * (g.nbk - 1) * (g.nbk - 1);
     if (jdir < 0 || jdir > g.nb) jdir = g.nb;
-    k_sumrule<<<g.n8p / 4, kRedThreads, 0, st>>>(reinterpret_cast<const double4 *>(chiq), chi0_inf, chi0_inf2,
-                                                  g.w16, g.tailq, g.nb, jdir, tail, Uv, sign, T, T / Nq, r);
+    const int nblk = g.n8p / 4;
+    if (jdir < g.nb && !tail) {
+        // low frequencies only: a short grid over the flattened (block, j) index
+        const int grid = (int)std::min<long long>(2 * 148, ((long long)nblk * jdir + kRedThreads - 1) / kRedThreads);
+        k_sumrule_low<<<std::max(grid, 1), kRedThreads, 0, st>>>(reinterpret_cast<const double4 *>(chiq), g.w16,
+                                                                  g.nb, nblk, jdir, Uv, sign, T / Nq, r);
+        return launched();
+    }
+    k_sumrule<<<nblk, kRedThreads, 0, st>>>(reinterpret_cast<const double4 *>(chiq), chi0_inf, chi0_inf2, g.w16,
+                                            g.tailq, g.nb, jdir, tail, Uv, sign, T, T / Nq, r);
     return launched();
 }
 
@@ -1407,8 +1556,15 @@ cudaError_t launch_sigma_boundary(const GridDev &g, const double *Grt, const dou
                                   const double *dG0p, double mu0, double fact, double *dS, cudaStream_t st) {
     return dispatch_nbk<RunSigmaBoundary>(g.nbk, &g, Grt, V, dtau_chirt0, dG0p, mu0, fact, dS, st);
 }
+cudaError_t launch_sigma_boundary(const GridDev &g, const float *Grt, const double *V, const double *dtau_chirt0,
+                                  const double *dG0p, double mu0, double fact, double *dS, cudaStream_t st) {
+    return dispatch_nbk<RunSigmaBoundary>(g.nbk, &g, Grt, V, dtau_chirt0, dG0p, mu0, fact, dS, st);
+}
 
 cudaError_t launch_sigma_slice(const GridDev &g, const double *Grt, const double *V, double *sigt, cudaStream_t st) {
+    return dispatch_nbk<RunSigmaSlice>(g.nbk, &g, Grt, V, sigt, st);
+}
+cudaError_t launch_sigma_slice(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st) {
     return dispatch_nbk<RunSigmaSlice>(g.nbk, &g, Grt, V, sigt, st);
 }
 
@@ -1423,8 +1579,15 @@ cudaError_t launch_trace_diff_G(const GridDev &g, const double2 *S, const double
     const int NO = g.nw0 / 2;
     const int tail = (jdir < 0) ? 1 : 0;
     if (jdir < 0 || jdir > NO) jdir = NO;
-    k_trace_diff_G<<<g.n8p / 4, kRedThreads, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.nw0, mu0, pmu, T, jdir,
-                                                       tail, r);
+    const int nblk = g.n8p / 4;
+    if (!tail) {
+        const int grid = (int)std::min<long long>(2 * 148, ((long long)nblk * jdir + kRedThreads - 1) / kRedThreads);
+        k_trace_diff_G_low<<<std::max(grid, 1), kRedThreads, 0, st>>>(S, s2, s3, sinf, g.ek, g.w16, g.nw0, nblk, mu0,
+                                                                       pmu, T, jdir, r);
+        return launched();
+    }
+    k_trace_diff_G<<<nblk, kRedThreads, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.nw0, mu0, pmu, T, jdir, tail,
+                                                  r);
     return launched();
 }
 
@@ -1467,6 +1630,11 @@ cudaError_t launch_gwn_local(const GridDev &g, const double2 *S, const double *s
                              const double *sinf, double mu, double T, double2 *out, cudaStream_t st) {
     const double nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
     k_gwn_local<<<g.nw0 / 2, 256, 0, st>>>(S, s2, s3, sinf, g.ek, g.w16, g.n8, g.nw0, mu, T, nk02, out);
+    return launched();
+}
+
+cudaError_t launch_mu0_newton(const GridDev &g, double n, double T, Reduce r, cudaStream_t st) {
+    k_mu0_newton<<<1, 1024, 0, st>>>(g.ek, g.lm, g.n8, g.nbk, n, T, 4.0 * (g.nbk - 1) * (g.nbk - 1), r.result);
     return launched();
 }
 

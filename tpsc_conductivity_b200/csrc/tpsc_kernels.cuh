@@ -21,6 +21,7 @@ struct GridDev {
     double *w16 = nullptr;         // [n8p] octant weight: 16 halved on edges and diagonal, 0 on padding
     double *tailq = nullptr;       // [kTailQ] sum-rule tail power sums Q_k = sum_n qn^-2k (T dependent)
     double2 *tw_k = nullptr;       // [L]   exp(-2 pi i m / L)
+    float4 *tw_k32 = nullptr;      // [L]   the same as (cos, sin) rounded to float, then the float remainders
     double2 *tw_w = nullptr;       // [Nw0] exp(-2 pi i m / Nw0)
     double2 *ht_w = nullptr;       // [Nw0] exp(+i pi m / Nw0)
     double *spl_half = nullptr;    // [2 nb]       spline LU tables, nb nodes
@@ -45,13 +46,24 @@ struct Reduce {
 // ---- launchers (all asynchronous on `st`) ---------------------------------
 cudaError_t launch_density(const GridDev &g, double mu, double n, double T, Reduce r, cudaStream_t st);
 
+// per-octant (eps - mu0, G0 prefactor) into g.gk
+cudaError_t launch_gk_table(const GridDev &g, double mu0, double T, cudaStream_t st);
 cudaError_t launch_gslice(const GridDev &g, double *Grt, double mu0, double T, cudaStream_t st);
 cudaError_t launch_chi0_boundary(const GridDev &g, const double *Grt, double mu0, double T,
                                  double *dG0p, double *dtau_chirt0, double *dtau_chiqt0, cudaStream_t st);
+cudaError_t launch_chi0_boundary(const GridDev &g, const float *Grt, double mu0, double T,
+                                 double *dG0p, double *dtau_chirt0, double *dtau_chiqt0, cudaStream_t st);
+// the mixed-precision form's FP32 slice transforms (tpsc_mixed.cu)
+cudaError_t launch_gslice32(const GridDev &g, float *Grt, double mu0, double T, cudaStream_t st);
+cudaError_t launch_chi0_slice32(const GridDev &g, const float *Grt, double *chirt, double *chiq, cudaStream_t st);
+cudaError_t launch_vertex_q32(const GridDev &g, const double *chiq, double *Vr, double U, double Usp, double Uch,
+                              double T, cudaStream_t st);
 cudaError_t launch_chi0_slice(const GridDev &g, const double *Grt, double *chirt, double *chiq, cudaStream_t st);
 cudaError_t launch_chi0_tau(const GridDev &g, double *chiq, const double *dtau_chiqt0, double *chi0_inf,
                             double *chi0_inf2, double T, cudaStream_t st);
 
+// mu0 by safeguarded Newton in one block -> r.result[0] (iterations in r.result[1])
+cudaError_t launch_mu0_newton(const GridDev &g, double n, double T, Reduce r, cudaStream_t st);
 // chi0max, qmax -> r.result[0..2]
 cudaError_t launch_chi0max(const GridDev &g, const double *chiq, Reduce r, cudaStream_t st);
 
@@ -78,7 +90,10 @@ cudaError_t launch_vertex_tau(const GridDev &g, double *Vr, const double *chirt,
 
 cudaError_t launch_sigma_boundary(const GridDev &g, const double *Grt, const double *V, const double *dtau_chirt0,
                                   const double *dG0p, double mu0, double fact, double *dS, cudaStream_t st);
+cudaError_t launch_sigma_boundary(const GridDev &g, const float *Grt, const double *V, const double *dtau_chirt0,
+                                  const double *dG0p, double mu0, double fact, double *dS, cudaStream_t st);
 cudaError_t launch_sigma_slice(const GridDev &g, const double *Grt, const double *V, double *sigt, cudaStream_t st);
+cudaError_t launch_sigma_slice(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st);
 cudaError_t launch_sigma_tau(const GridDev &g, const double *sigt, const double *dS, double2 *S, double *s2,
                              double *s3, double *s4, double *sinf, double T, cudaStream_t st);
 

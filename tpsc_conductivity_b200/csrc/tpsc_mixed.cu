@@ -1,0 +1,198 @@
+// tpsc_mixed.cu -- the FP32 slice transforms of the mixed-precision form.
+//
+// The G(r, tau), chi0 and V(q) stages of the solve transform in FP32 (the
+// slice and its DCT-I in float, twiddles compensated, see tpsc_fft.cuh);
+// their inputs are formed and their outputs kept in FP64 where the next
+// stage needs it: chi0(r, tau) and chi0(q, tau) feed the FP64 tau
+// transforms and sum rules, V(r, tau) the FP64 self-energy.  G(r, tau) is
+// stored in FP32 (half the bytes) and read by the FP64 Sigma slices.  The
+// Sigma slices, every tau transform, the tail moments, the sum rules, the
+// root searches and the continuation stay FP64: Sigma's own 2D transform in
+// FP32 would cost ~6e-6 of Sigma, the other three stages together ~3e-7.
+//
+// Each FP32 slice needs ~105 KB of shared memory (the 129 x 129 float slice,
+// 16 groups' float2 FFT scratch and the hi/lo twiddles), so two CTAs run on
+// an SM where the FP64 slice kernels fit one.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tpsc_device.cuh"
+
+namespace tpsc {
+
+namespace {
+
+constexpr int kSlice32Threads = 256;
+
+template <int NBK>
+struct Slice32Smem {
+    static constexpr int L = 2 * (NBK - 1);
+    static constexpr int G = FftPlan<L>::G;
+    static constexpr int NGRP = kSlice32Threads / G;
+    static constexpr size_t slice_bytes = (size_t)NBK * NBK * sizeof(float);
+    static constexpr size_t scr_off = (slice_bytes + 15) & ~(size_t)15;
+    static constexpr size_t tw_off = scr_off + (size_t)NGRP * padded_len(L) * sizeof(float2);
+    static constexpr size_t bytes = tw_off + (size_t)L * sizeof(float4);
+};
+
+template <int NBK>
+__device__ __forceinline__ float2 *scratch32(float *S) {
+    return reinterpret_cast<float2 *>(reinterpret_cast<char *>(S) + Slice32Smem<NBK>::scr_off);
+}
+
+// the hi/lo twiddles in shared memory; the kernel's first barrier publishes them
+template <int NBK>
+__device__ __forceinline__ const float4 *twiddles32(float *S, const float4 *__restrict__ tw) {
+    float4 *t = reinterpret_cast<float4 *>(reinterpret_cast<char *>(S) + Slice32Smem<NBK>::tw_off);
+    for (int i = threadIdx.x; i < Slice32Smem<NBK>::L; i += blockDim.x) t[i] = __ldg(&tw[i]);
+    return t;
+}
+
+template <int NBK>
+__device__ __forceinline__ void put_sym32(float *S, int l, int m, float v) {
+    S[l * NBK + m] = v;
+    S[m * NBK + l] = v;
+}
+
+// G(r, tau_j) = DCT-I[ G0(k, tau_j) / L^2 ] in FP32 (the FP64 k_gslice's
+// stage, src/green.cpp:1830-1841 and src/chi0.cpp:462-495): G0 formed in
+// FP64, rounded once to float; Grt32[j * n8 + o].
+template <int NBK>
+__global__ void __launch_bounds__(kSlice32Threads, 2)
+    k_gslice32(const double2 *__restrict__ gk, const uint32_t *__restrict__ lm, const float4 *__restrict__ tw,
+               int n8, int nw0, double T, float *__restrict__ Grt) {
+    extern __shared__ __align__(16) float S32[];
+    const float4 *tws = twiddles32<NBK>(S32, tw);
+    const int j = blockIdx.x;
+    const double t = j / (nw0 * T);
+    const double bt = 1.0 / T - t;
+#pragma unroll 4
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        const double2 c = __ldg(&gk[o]);
+        put_sym32<NBK>(S32, l, m, (float)(c.y * exp((c.x > 0 ? -t : bt) * c.x)));
+    }
+    __syncthreads();
+    dct2_slice<NBK>(S32, scratch32<NBK>(S32), tws);
+    float *out = Grt + (size_t)j * n8;
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        out[o] = S32[l * NBK + m];
+    }
+}
+
+// chi0(r, tau_j) = -2 G(r, tau_j) G(r, -tau_j) from the FP32 G (the product
+// is exact in FP64 and kept there for the tau transforms), its DCT-I in FP32
+// -> chi0(q, tau_j) in FP64 (src/chi0.cpp:393-418, 497-517, 545-558).
+template <int NBK>
+__global__ void __launch_bounds__(kSlice32Threads, 2)
+    k_chi0_slice32(const float *__restrict__ Grt, const uint32_t *__restrict__ lm, const float4 *__restrict__ tw,
+                   int n8, int nw0, double *__restrict__ chirt, double *__restrict__ chiq) {
+    extern __shared__ __align__(16) float S32[];
+    const float4 *tws = twiddles32<NBK>(S32, tw);
+    const int j = blockIdx.x;
+    const int nb = nw0 / 2 + 1;
+    const float *gp = Grt + (size_t)j * n8;
+    const float *gm = Grt + (size_t)(nw0 - j) * n8;
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        const double a = gp[o];
+        double c;
+        if (j == 0)
+            c = (o == 0) ? -2.0 * a * (a + 1.0) : -2.0 * a * a;
+        else if (j == nb - 1)
+            c = 2.0 * a * a;
+        else
+            c = -2.0 * (-(double)gm[o]) * a;
+        chirt[bidx(j, o, nb)] = c;
+        put_sym32<NBK>(S32, l, m, (float)c);
+    }
+    __syncthreads();
+    dct2_slice<NBK>(S32, scratch32<NBK>(S32), tws);
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        chiq[bidx(j, o, nb)] = S32[l * NBK + m];
+    }
+}
+
+// V(q, iqn) in FP64 from chi0(q, iqn), its DCT-I over q in FP32
+// (src/chi.cpp:89-115).
+template <int NBK>
+__global__ void __launch_bounds__(kSlice32Threads, 2)
+    k_vertex_q32(const double *__restrict__ chiq, const uint32_t *__restrict__ lm, const float4 *__restrict__ tw,
+                 int n8, int nb, double normFact, double U, double Usp, double Uch, double *__restrict__ Vr) {
+    extern __shared__ __align__(16) float S32[];
+    const float4 *tws = twiddles32<NBK>(S32, tw);
+    const int j = blockIdx.x;
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        const double c0 = chiq[bidx(j, o, nb)];
+        const double sp = c0 / (1.0 - Usp * c0 / 2.0);
+        const double ch = c0 / (1.0 + Uch * c0 / 2.0);
+        put_sym32<NBK>(S32, l, m, (float)(normFact * U * (3.0 * Usp * (sp - c0) + Uch * (ch - c0)) / 8.0));
+    }
+    __syncthreads();
+    dct2_slice<NBK>(S32, scratch32<NBK>(S32), tws);
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(lm, o, l, m);
+        Vr[bidx(j, o, nb)] = S32[l * NBK + m];
+    }
+}
+
+template <int NBK>
+struct RunGslice32 {
+    static cudaError_t run(const GridDev *g, float *Grt, double mu0, double T, cudaStream_t st) {
+        const size_t sm = Slice32Smem<NBK>::bytes;
+        cudaError_t e = set_smem(k_gslice32<NBK>, sm);
+        if (e != cudaSuccess) return e;
+        if ((e = launch_gk_table(*g, mu0, T, st)) != cudaSuccess) return e;
+        k_gslice32<NBK><<<g->nw0 + 1, kSlice32Threads, sm, st>>>(g->gk, g->lm, g->tw_k32, g->n8, g->nw0, T, Grt);
+        return launched();
+    }
+};
+template <int NBK>
+struct RunChi0Slice32 {
+    static cudaError_t run(const GridDev *g, const float *Grt, double *chirt, double *chiq, cudaStream_t st) {
+        const size_t sm = Slice32Smem<NBK>::bytes;
+        cudaError_t e = set_smem(k_chi0_slice32<NBK>, sm);
+        if (e != cudaSuccess) return e;
+        k_chi0_slice32<NBK><<<g->nb, kSlice32Threads, sm, st>>>(Grt, g->lm, g->tw_k32, g->n8, g->nw0, chirt, chiq);
+        return launched();
+    }
+};
+template <int NBK>
+struct RunVertexQ32 {
+    static cudaError_t run(const GridDev *g, const double *chiq, double *Vr, double U, double Usp, double Uch,
+                           double T, cudaStream_t st) {
+        const size_t sm = Slice32Smem<NBK>::bytes;
+        cudaError_t e = set_smem(k_vertex_q32<NBK>, sm);
+        if (e != cudaSuccess) return e;
+        const double normFact = T / ((double)g->nk0 * g->nk0);
+        k_vertex_q32<NBK><<<g->nb, kSlice32Threads, sm, st>>>(chiq, g->lm, g->tw_k32, g->n8, g->nb, normFact, U, Usp,
+                                                              Uch, Vr);
+        return launched();
+    }
+};
+
+}  // namespace
+
+cudaError_t launch_gslice32(const GridDev &g, float *Grt, double mu0, double T, cudaStream_t st) {
+    return dispatch_nbk<RunGslice32>(g.nbk, &g, Grt, mu0, T, st);
+}
+
+cudaError_t launch_chi0_slice32(const GridDev &g, const float *Grt, double *chirt, double *chiq, cudaStream_t st) {
+    return dispatch_nbk<RunChi0Slice32>(g.nbk, &g, Grt, chirt, chiq, st);
+}
+
+cudaError_t launch_vertex_q32(const GridDev &g, const double *chiq, double *Vr, double U, double Usp, double Uch,
+                              double T, cudaStream_t st) {
+    return dispatch_nbk<RunVertexQ32>(g.nbk, &g, chiq, Vr, U, Usp, Uch, T, st);
+}
+
+}  // namespace tpsc
