@@ -232,7 +232,8 @@ struct CondTauSmem {
     static constexpr int threads = TauSmem<N>::threads;
     static constexpr size_t r_bytes = ((size_t)2 * (N + 1) * sizeof(double) + 15) & ~(size_t)15;
     static constexpr size_t x_bytes = (size_t)padded_len(N) * sizeof(double2);
-    static constexpr size_t bytes = r_bytes + 2 * x_bytes;
+    static constexpr size_t tables_off = r_bytes + 2 * x_bytes;
+    static constexpr size_t bytes = tables_off + 2 * sizeof(TwoLevelTw);
 };
 
 struct CondTauArgs {
@@ -329,6 +330,9 @@ __global__ void __launch_bounds__(CondTauSmem<N>::threads, 1) k_cond_tau(const C
     extern __shared__ __align__(16) double R[];
     double2 *X1 = reinterpret_cast<double2 *>(reinterpret_cast<char *>(R) + CondTauSmem<N>::r_bytes);
     double2 *X2 = X1 + padded_len(N);
+    TwoLevelTw *tw2 = reinterpret_cast<TwoLevelTw *>(reinterpret_cast<char *>(R) + CondTauSmem<N>::tables_off);
+    const TwoLevelTw *ht2 = tw2 + 1;
+    tau_tables(tw2, tw2 + 1, a.tw, a.ht, N);  // published by the first barrier of the pair loop
     __shared__ ColState cs[2];
     __shared__ double d0s[2], dNs[2], sums[8], sV[2], sM[2];
     const int tid = threadIdx.x, NT = blockDim.x;
@@ -351,9 +355,9 @@ __global__ void __launch_bounds__(CondTauSmem<N>::threads, 1) k_cond_tau(const C
         if (tid < G) {
             const double *Ma = R, *Mb = R + NJ;
             auto in = [&](int j) -> double2 {
-                return cmul(__ldg(&a.ht[j]), make_double2((Ma[j + 1] - Ma[j]) / h, (Mb[j + 1] - Mb[j]) / h));
+                return cmul(tw_at(ht2, j), make_double2((Ma[j + 1] - Ma[j]) / h, (Mb[j + 1] - Mb[j]) / h));
             };
-            group_fft_io<N, +1>(X1, tid, a.tw, 0, in, ScratchIO{X1});
+            group_fft_io<N, +1>(X1, tid, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X1});
         }
         __syncthreads();
     };
@@ -396,7 +400,7 @@ __global__ void __launch_bounds__(CondTauSmem<N>::threads, 1) k_cond_tau(const C
                 split_real(X1[pidx(n)], X1[pidx(N - 1 - n)], F[0], F[1]);
                 // the pre-twiddled split: F_b = (Z_n - conj Z_{N-1-n}) / (2i)
                 const double kn = (2 * n + 1) * pT, ik = 1.0 / kn;
-                const double2 e = __ldg(&a.ht[2 * n + 1]);
+                const double2 e = tw_at(ht2, 2 * n + 1);
                 const double2 f = make_double2(1.0 - e.x, -e.y);
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
@@ -428,7 +432,7 @@ __global__ void __launch_bounds__(CondTauSmem<N>::threads, 1) k_cond_tau(const C
                 double2 F[2];
                 split_real(X1[pidx(n)], X1[pidx(N - 1 - n)], F[0], F[1]);
                 const double kn = (2 * n + 1) * pT, ik = 1.0 / kn;
-                const double2 e = __ldg(&a.ht[2 * n + 1]);
+                const double2 e = tw_at(ht2, 2 * n + 1);
                 const double2 f = make_double2(1.0 - e.x, -e.y);
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
@@ -499,7 +503,7 @@ __global__ void __launch_bounds__(CondTauSmem<N>::threads, 1) k_cond_tau(const C
                 }
                 return make_double2(A.x - B.y, A.y + B.x);
             };
-            group_fft_io<N, -1, false, true>(X2, tid, a.tw, 0, inG, ScratchIO{X2});
+            group_fft_io<N, -1, false, true>(X2, tid, (const TwoLevelTw *)tw2, 0, inG, ScratchIO{X2});
             auto inJ = [&](int k) -> double2 {
                 double2 A, B;
                 if (k < NO) {
@@ -511,13 +515,13 @@ __global__ void __launch_bounds__(CondTauSmem<N>::threads, 1) k_cond_tau(const C
                 }
                 return make_double2(A.x - B.y, A.y + B.x);
             };
-            group_fft_io<N, +1, false, true>(X1, tid, a.tw, 0, inJ, ScratchIO{X1});
+            group_fft_io<N, +1, false, true>(X1, tid, (const TwoLevelTw *)tw2, 0, inJ, ScratchIO{X1});
         }
         __syncthreads();
         // ---- G J(tau) into R; G(tau) kept in X2 for the bubble
         for (int j = tid; j < N; j += NT) {
             const double tau = j * h;
-            const double2 ph = __ldg(&a.ht[j]);
+            const double2 ph = tw_at(ht2, j);
             const double2 g = cmul(cconj(ph), X2[pidx(j)]);
             const double2 jr = cmul(ph, X1[pidx(j)]);
             double g0a, jia, g0b, jib;
@@ -556,14 +560,14 @@ __global__ void __launch_bounds__(CondTauSmem<N>::threads, 1) k_cond_tau(const C
             auto in = [&](int j) -> double2 {
                 return make_double2((Ma[j + 1] - Ma[j]) / h, (Mb[j + 1] - Mb[j]) / h);
             };
-            group_fft_io<N, -1>(X1, tid, a.tw, 0, in, ScratchIO{X1});
+            group_fft_io<N, -1>(X1, tid, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X1});
         }
         __syncthreads();
         for (int n = 1 + tid; n <= NO; n += NT) {
             double2 F[2];
             split_real(X1[pidx(n)], X1[pidx(N - n)], F[0], F[1]);
             const double wq = 2 * n * pT, iw = 1.0 / wq, iw2 = iw * iw;
-            const double2 e = __ldg(&a.tw[n]);
+            const double2 e = tw_at(tw2, n);
             const double2 f = make_double2(1.0 - e.x, -e.y);
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
@@ -615,14 +619,14 @@ __global__ void __launch_bounds__(CondTauSmem<N>::threads, 1) k_cond_tau(const C
                 const double sg = lo ? 1.0 : -1.0;
                 return make_double2(sg * (Ma[jj + 1] - Ma[jj]) / h, sg * (Mb[jj + 1] - Mb[jj]) / h);
             };
-            group_fft_io<N, -1>(X1, tid, a.tw, 0, in, ScratchIO{X1});
+            group_fft_io<N, -1>(X1, tid, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X1});
         }
         __syncthreads();
         for (int n = 1 + tid; n <= NO; n += NT) {
             double2 F[2];
             split_real(X1[pidx(n)], X1[pidx(N - n)], F[0], F[1]);
             const double wq = 2 * n * pT, iw = 1.0 / wq, iw2 = iw * iw;
-            const double2 e = __ldg(&a.tw[n]);
+            const double2 e = tw_at(tw2, n);
             const double2 f = make_double2(1.0 - e.x, -e.y);
 #pragma unroll
             for (int q = 0; q < 2; ++q) {

@@ -194,11 +194,28 @@ __device__ void column_sums(const double *A, int lda, int i0, int i1, double *ou
 template <int N>
 struct TauSmem {
     static constexpr int threads = (N / 16) > kTauThreads ? (N / 16) : kTauThreads;
-    static size_t bytes(int NJ) {
-        size_t a = ((size_t)4 * NJ * sizeof(double) + 15) & ~(size_t)15;
-        return a + (size_t)padded_len(N) * sizeof(double2);
+    // four staged columns, the FFT scratch, then the two-level twiddle tables
+    __host__ __device__ static size_t tables_off(int NJ) {
+        return (((size_t)4 * NJ * sizeof(double) + 15) & ~(size_t)15) + (size_t)padded_len(N) * sizeof(double2);
     }
+    __host__ __device__ static size_t bytes(int NJ) { return tables_off(NJ) + 2 * sizeof(TwoLevelTw); }
 };
+
+// Two-level tables (shared memory) of the N-point FFT twiddles tw[m] =
+// exp(-2 pi i m/N) and of the pre-twiddles ht[m] = exp(+i pi m/N), m < N,
+// from the global tables; entry m is hi[m >> 6] * lo[m & 63].  The caller's
+// next barrier publishes them.
+__device__ __forceinline__ void tau_tables(TwoLevelTw *tw2, TwoLevelTw *ht2, const double2 *__restrict__ tw,
+                                           const double2 *__restrict__ ht, int N) {
+    for (int t = threadIdx.x; t < 64; t += blockDim.x) {
+        const double2 one = make_double2(1.0, 0.0);
+        tw2->hi[t] = 64 * t < N ? __ldg(&tw[64 * t]) : one;
+        tw2->lo[t] = t < N ? __ldg(&tw[t]) : one;
+        ht2->hi[t] = 64 * t < N ? __ldg(&ht[64 * t]) : one;
+        ht2->lo[t] = t < N ? __ldg(&ht[t]) : one;
+    }
+}
+__device__ __forceinline__ double2 tw_at(const TwoLevelTw *t, int m) { return cmul(t->hi[m >> 6], t->lo[m & 63]); }
 
 // Asynchronous 8-byte global -> shared copy (cp.async); the issuing thread
 // waits for its own copies with cp_async_wait_all, a barrier then publishes

@@ -292,6 +292,7 @@ struct Grid {
     std::vector<double> cmax_suf;            // [nb + 1] max |chi| over frequencies >= j
     long double tail_mom[kMomP] = {0};       // the same moments of the Matsubara tail n > Nw0/2
     double tail_max = 0.0;                   // max |chi| over the tail
+    double *d_mom_suf = nullptr, *d_cmax_suf = nullptr, *d_tailm = nullptr;  // device copies (FP64)
     double tailq_T = -1.0;         // temperature the tail power sums were built for
     double tailq_host[kTailQ] = {0};
     std::vector<void *> allocs;
@@ -312,6 +313,7 @@ struct tpsc_ctx {
     cudaStream_t st = nullptr;
     Reduce red;
     Reduce redm;              // moment sums: partial [(2 kMomP + 1) kMaxBlocks], result [32]
+    RootScratch roots;        // the device root searches' state
     double *h_res = nullptr;  // pinned, 32 doubles
     // model
     bool have_model = false;
@@ -513,6 +515,9 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
     A(dalloc(g, &g->sinf, 1));
     A(dalloc(g, &g->mom, nb * kMomP));
     A(dalloc(g, &g->cmax, nb));
+    A(dalloc(g, &g->d_mom_suf, (nb + 1) * kMomP));
+    A(dalloc(g, &g->d_cmax_suf, nb + 1));
+    A(dalloc(g, &g->d_tailm, (size_t)kMomP + 1));
 #undef A
     if (e != cudaSuccess) {
         free_grid(g);
@@ -677,6 +682,15 @@ int ensure_moments(tpsc_ctx *ctx, Grid *g) {
     if (rc) return rc;
     for (int k = 0; k < kMomP; ++k) g->tail_mom[k] = tm[k];
     g->tail_max = tm[kMomP + 1];
+    // FP64 copies for the device root search
+    std::vector<double> ms(g->mom_suf.begin(), g->mom_suf.end()), tl(kMomP + 1);
+    for (int k = 0; k < kMomP; ++k) tl[k] = (double)g->tail_mom[k];
+    tl[kMomP] = g->tail_max;
+    CK(cudaMemcpyAsync(g->d_mom_suf, ms.data(), ms.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(g->d_cmax_suf, g->cmax_suf.data(), g->cmax_suf.size() * sizeof(double),
+                       cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(g->d_tailm, tl.data(), tl.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));  // the host vectors above are released on return
     g->have_mom = true;
     return TPSC_OK;
 }
@@ -737,6 +751,27 @@ int roots_Usp_Uch(tpsc_ctx *ctx, double Usc[2]) {
     const double n = ctx->n, U = ctx->U, nsr = ctx->nsr;
     const bool newton = (ctx->form & TPSC_FORM_NEWTON) != 0;
     int rc = TPSC_OK;
+    if (newton) {
+        // both roots in one cooperative launch (tpsc_roots.cu)
+        Grid *g = ctx->cur;
+        if ((rc = ensure_moments(ctx, g))) return rc;
+        CK(launch_sumrule_roots(g->d, g->chiq, g->cinf, g->cinf2, g->d_mom_suf, g->d_cmax_suf, g->d_tailm, ctx->T,
+                                n, nsr, U, 2.0 / ctx->scal[TPSC_S_CHI0MAX] - 2 * EPS, ctx->roots, ctx->st));
+        double r[6];
+        if ((rc = read_result(ctx, 6, r, ctx->roots.out))) return rc;
+        unsigned flags[4];
+        CK(cudaMemcpy(flags, ctx->roots.bar, sizeof(flags), cudaMemcpyDeviceToHost));
+        if (flags[2]) return fail(ctx, TPSC_ERR_CUDA, "device root search: grid barrier timed out");
+        if (r[4] != 1.0) return fail(ctx, TPSC_ERR_NO_ROOT, "Usp not found");
+        if (r[5] != 1.0) return fail(ctx, TPSC_ERR_NO_ROOT, "Uch not found");
+        ctx->Usp = Usc[0] = r[0];
+        ctx->Uch = Usc[1] = r[1];
+        ctx->scal[TPSC_S_EVALS_SP] = r[2];
+        ctx->scal[TPSC_S_EVALS_CH] = r[3];
+        ctx->scal[TPSC_S_USP] = ctx->Usp;
+        ctx->scal[TPSC_S_UCH] = ctx->Uch;
+        return TPSC_OK;
+    }
     // R_sp(Us) = trace + n - n^2/2 - nsr + Us nsr^2/(2U)  (chi::sum_rule_sp, src/chi.cpp:833-836)
     auto rsp = [&](double Us, double &y, double &dy) -> bool {
         double tr, dtr;
@@ -1120,6 +1155,10 @@ tpsc_ctx *tpsc_create(int device, int *status) {
     if ((e = cudaMalloc(&ctx->redm.partial, (2 * kMomP + 2) * kMaxBlocks * sizeof(double))) != cudaSuccess)
         return bad(e);
     if ((e = cudaMalloc(&ctx->redm.result, 32 * sizeof(double))) != cudaSuccess) return bad(e);
+    if ((e = cudaMalloc(&ctx->roots.partial, 2 * kRootMaxBlocks * sizeof(double))) != cudaSuccess) return bad(e);
+    if ((e = cudaMalloc(&ctx->roots.bar, 4 * sizeof(unsigned))) != cudaSuccess) return bad(e);
+    if ((e = cudaMalloc(&ctx->roots.ctl, 8 * sizeof(double))) != cudaSuccess) return bad(e);
+    if ((e = cudaMalloc(&ctx->roots.out, 8 * sizeof(double))) != cudaSuccess) return bad(e);
     if ((e = cudaMallocHost(&ctx->h_res, 32 * sizeof(double))) != cudaSuccess) return bad(e);
     for (auto &ev : ctx->ev)
         if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bad(e);
@@ -1137,6 +1176,10 @@ void tpsc_destroy(tpsc_ctx *ctx) {
     if (ctx->red.ticket) cudaFree(ctx->red.ticket);
     if (ctx->redm.partial) cudaFree(ctx->redm.partial);
     if (ctx->redm.result) cudaFree(ctx->redm.result);
+    if (ctx->roots.partial) cudaFree(ctx->roots.partial);
+    if (ctx->roots.bar) cudaFree(ctx->roots.bar);
+    if (ctx->roots.ctl) cudaFree(ctx->roots.ctl);
+    if (ctx->roots.out) cudaFree(ctx->roots.out);
     if (ctx->h_res) cudaFreeHost(ctx->h_res);
     if (ctx->stage) cudaFree(ctx->stage);
     for (auto &ev : ctx->ev)

@@ -75,6 +75,20 @@ __device__ __forceinline__ float2 twiddle(float2 v, const float4 *__restrict__ t
     return make_float2(fmaf(v.x, w.x, fmaf(-v.y, w.y, cr)), fmaf(v.x, w.y, fmaf(v.y, w.x, ci)));
 }
 
+// Two-level twiddle table for FFT lengths N <= 4096 kept in shared memory:
+// exp(-2 pi i m / N) = hi[m >> 6] * lo[m & 63] with hi[a] = exp(-2 pi i 64 a/N)
+// and lo[b] = exp(-2 pi i b/N) (2 KB instead of 16 N bytes; the product adds
+// about one ulp to the twiddle).
+struct TwoLevelTw {
+    double2 hi[64], lo[64];
+};
+template <int SIGN, bool SMEM>
+__device__ __forceinline__ double2 twiddle(double2 v, const TwoLevelTw *__restrict__ tw, int m) {
+    double2 w = cmul(tw->hi[m >> 6], tw->lo[m & 63]);
+    if (SIGN > 0) w.y = -w.y;
+    return cmul(v, w);
+}
+
 // exp(sign * 2 pi i m / 16) for the constant twiddles of the radix-8/16
 // kernels; m is a compile-time constant after unrolling, so the switch folds.
 __device__ __forceinline__ double2 w16(int m, int sign) {

@@ -357,9 +357,11 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
     constexpr int NJ = N / 2 + 1;
     extern __shared__ __align__(16) double A[];
     double2 *X = reinterpret_cast<double2 *>(A + ((4 * NJ + 1) & ~1));
+    TwoLevelTw *tw2 = reinterpret_cast<TwoLevelTw *>(reinterpret_cast<char *>(A) + TauSmem<N>::tables_off(NJ));
     __shared__ double d0[4], dN[4], V0[4], VN[4], sV[4], sM[4], integ[4];
     const int o0 = 4 * blockIdx.x;
     double *g = chiq + (size_t)blockIdx.x * 4 * NJ;
+    tau_tables(tw2, tw2 + 1, tw, tw, N);
     stage_in(A, g, NJ, n8 - o0);
     if (threadIdx.x < 4) {
         const int o = o0 + threadIdx.x;
@@ -394,7 +396,7 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
             const double sg = lo ? 1.0 : -1.0;
             return make_double2(sg * (Ma[jj + 1] - Ma[jj]) / h, sg * (Mb[jj + 1] - Mb[jj]) / h);
         };
-        if (threadIdx.x < G) group_fft_io<N, +1>(X, threadIdx.x, tw, 0, in, ScratchIO{X});
+        if (threadIdx.x < G) group_fft_io<N, +1>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
         __syncthreads();
         for (int n = threadIdx.x + 1; n < NJ; n += blockDim.x) {
             const double2 Z = X[pidx(n)];
@@ -403,7 +405,7 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
             const double2 Fa = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
             const double2 Fb = make_double2(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
             const double wn = 2 * n * kPi * T;
-            const double2 w = __ldg(&tw[n]);
+            const double2 w = tw_at(tw2, n);
             const double cth = w.x, sth = -w.y;  // cos, sin of 2 pi n / N
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
@@ -436,8 +438,10 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
     constexpr int NJ = N / 2 + 1;
     extern __shared__ __align__(16) double A[];
     double2 *X = reinterpret_cast<double2 *>(A + ((4 * NJ + 1) & ~1));
+    TwoLevelTw *tw2 = reinterpret_cast<TwoLevelTw *>(reinterpret_cast<char *>(A) + TauSmem<N>::tables_off(NJ));
     double *g = Vr + (size_t)blockIdx.x * 4 * NJ;
     const double *cr = chirt + (size_t)blockIdx.x * 4 * NJ;
+    tau_tables(tw2, tw2 + 1, tw, tw, N);
     stage_in(A, g, NJ, n8 - 4 * (int)blockIdx.x);
     __syncthreads();
     constexpr int G = FftPlan<N>::G;
@@ -450,7 +454,7 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
             const int jj = j < NJ ? j : N - j;
             return make_double2(a[jj], b[jj]);
         };
-        if (threadIdx.x < G) group_fft_io<N, -1>(X, threadIdx.x, tw, 0, in, ScratchIO{X});
+        if (threadIdx.x < G) group_fft_io<N, -1>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
         __syncthreads();
         for (int n = threadIdx.x; n < NJ; n += blockDim.x) {
             const double2 Z = X[pidx(n)];
@@ -480,8 +484,11 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
     constexpr int NO = N / 2;
     extern __shared__ __align__(16) double A[];
     double2 *X = reinterpret_cast<double2 *>(A + ((4 * NJ + 1) & ~1));
+    TwoLevelTw *tw2 = reinterpret_cast<TwoLevelTw *>(reinterpret_cast<char *>(A) + TauSmem<N>::tables_off(NJ));
+    const TwoLevelTw *ht2 = tw2 + 1;
     __shared__ double d0[4], dN[4];
     const int o0 = 4 * blockIdx.x;
+    tau_tables(tw2, tw2 + 1, tw, ht, N);
     stage_in(A, sigt + (size_t)blockIdx.x * 4 * NJ, NJ, n8 - o0);
     if (threadIdx.x < 4) {
         const int o = o0 + threadIdx.x;
@@ -510,9 +517,9 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
         auto in = [&](int j) -> double2 {
             const double fa = (Ma[j + 1] - Ma[j]) / h;
             const double fb = (Mb[j + 1] - Mb[j]) / h;
-            return cmul(__ldg(&ht[j]), make_double2(fa, fb));
+            return cmul(tw_at(ht2, j), make_double2(fa, fb));
         };
-        if (threadIdx.x < G) group_fft_io<N, +1>(X, threadIdx.x, tw, 0, in, ScratchIO{X});
+        if (threadIdx.x < G) group_fft_io<N, +1>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
         __syncthreads();
         for (int n = threadIdx.x; n < NO; n += blockDim.x) {
             const double2 Z = X[pidx(n)];
@@ -520,7 +527,7 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
             // F_a = (Z_n + conj Z_{N-1-n})/2, F_b = (Z_n - conj Z_{N-1-n})/(2i)
             const double2 Fa = make_double2(0.5 * (Z.x + Zr.x), 0.5 * (Z.y - Zr.y));
             const double2 Fb = make_double2(0.5 * (Z.y + Zr.y), -0.5 * (Z.x - Zr.x));
-            const double2 e = __ldg(&ht[2 * n + 1]);
+            const double2 e = tw_at(ht2, 2 * n + 1);
             const double2 f = make_double2(1.0 - e.x, -e.y);
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
@@ -532,6 +539,215 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
             }
         }
         __syncthreads();
+    }
+}
+
+// The same transform for ONE pair of columns per CTA, two CTAs per SM: the
+// pair is staged in a buffer of padded_len(N) complex and the FFT runs in
+// place in it (its first pass reads the spline's third derivatives before the
+// group barrier that precedes its writes), so a CTA needs ~74 KB of shared
+// memory and at most 128 registers per thread.
+template <int N>
+struct Tau2Smem {
+    static constexpr size_t buf = (size_t)padded_len(N) * sizeof(double2);
+    static constexpr size_t bytes = buf + 2 * sizeof(TwoLevelTw);
+};
+
+template <int N>
+__global__ void __launch_bounds__(256, 2)
+    k_sigma_tau2(const double *__restrict__ sigt, const double *__restrict__ dS, double2 *__restrict__ Sout,
+                 double *__restrict__ s2, double *__restrict__ s3, double *__restrict__ s4, double *__restrict__ sinf,
+                 const double *__restrict__ spl, const double2 *__restrict__ tw, const double2 *__restrict__ ht,
+                 double T, int n8, int n8p) {
+    constexpr int NJ = N + 1;
+    constexpr int NO = N / 2;
+    static_assert(2 * NJ * sizeof(double) <= Tau2Smem<N>::buf, "pair must fit the FFT buffer");
+    extern __shared__ __align__(16) double A[];
+    double2 *X = reinterpret_cast<double2 *>(A);
+    TwoLevelTw *tw2 = reinterpret_cast<TwoLevelTw *>(reinterpret_cast<char *>(A) + Tau2Smem<N>::buf);
+    const TwoLevelTw *ht2 = tw2 + 1;
+    __shared__ double d0[2], dN[2];
+    const int pair = blockIdx.x, blk = pair >> 1, half = pair & 1;
+    const int o0 = 2 * pair;
+    tau_tables(tw2, tw2 + 1, tw, ht, N);
+    // the pair's two columns of the four-column block, column-major
+    const double *g = sigt + (size_t)blk * 4 * NJ + 2 * half;
+    for (int i = threadIdx.x; i < 2 * NJ; i += blockDim.x) {
+        const int c = i & 1, j = i >> 1;
+        double *dst = &A[c * NJ + j];
+        if (o0 + c < n8)
+            cp_async8(dst, g + 4 * j + c);
+        else
+            *dst = 0.0;
+    }
+    cp_async_wait_all();
+    if (threadIdx.x < 2) {
+        d0[threadIdx.x] = dS[o0 + threadIdx.x];
+        dN[threadIdx.x] = dS[n8p + o0 + threadIdx.x];
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        const int o = o0 + threadIdx.x;
+        if (o == 0) sinf[0] = -(A[0] + A[NJ - 1]);
+        if (o < n8) s2[o] = d0[threadIdx.x] + dN[threadIdx.x];
+    }
+    const double h = 1.0 / (N * T);
+    spline_second_derivatives<2>(A, NJ, NJ, h, d0, dN, spl, spl + NJ);
+    if (threadIdx.x < 2) {
+        const int o = o0 + threadIdx.x;
+        if (o < n8) s3[o] = -(A[threadIdx.x * NJ] + A[threadIdx.x * NJ + N]);
+    }
+    constexpr int G = FftPlan<N>::G;
+    if (threadIdx.x < G) {
+        const double *Ma = A, *Mb = A + NJ;
+        auto in = [&](int j) -> double2 {
+            const double fa = (Ma[j + 1] - Ma[j]) / h;
+            const double fb = (Mb[j + 1] - Mb[j]) / h;
+            return cmul(tw_at(ht2, j), make_double2(fa, fb));
+        };
+        group_fft_io<N, +1, false, true>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
+    }
+    __syncthreads();
+    for (int n = threadIdx.x; n < NO; n += blockDim.x) {
+        const double2 Z = X[pidx(n)];
+        const double2 Zr = X[pidx(N - 1 - n)];
+        const double2 Fa = make_double2(0.5 * (Z.x + Zr.x), 0.5 * (Z.y - Zr.y));
+        const double2 Fb = make_double2(0.5 * (Z.y + Zr.y), -0.5 * (Z.x - Zr.x));
+        const double2 e = tw_at(ht2, 2 * n + 1);
+        const double2 f = make_double2(1.0 - e.x, -e.y);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int o = o0 + q;
+            const double2 Sv = cmul(f, q == 0 ? Fa : Fb);
+            Sout[bidx(n, o, NO)] = Sv;
+            if (n == NO - 1 && o < n8) s4[o] = Sv.x;
+        }
+    }
+}
+
+// Stage the two columns 2 half, 2 half + 1 of a four-column block (NJ rows)
+// column-major into A; columns >= n8 as zeros.  The caller's barrier
+// publishes them.
+__device__ __forceinline__ void stage_pair4(double *A, const double *blk4, int NJ, int half, int o0, int n8) {
+    const double *g = blk4 + 2 * half;
+    for (int i = threadIdx.x; i < 2 * NJ; i += blockDim.x) {
+        const int c = i & 1, j = i >> 1;
+        double *dst = &A[c * NJ + j];
+        if (o0 + c < n8)
+            cp_async8(dst, g + 4 * j + c);
+        else
+            *dst = 0.0;
+    }
+    cp_async_wait_all();
+}
+
+// k_chi0_tau for one pair per CTA (in-place FFT, two CTAs per SM); results
+// go straight back to chiq.
+template <int N>
+__global__ void __launch_bounds__(256, 2)
+    k_chi0_tau2(double *__restrict__ chiq, const double *__restrict__ dtau_chiqt0, double *__restrict__ chi0_inf,
+                double *__restrict__ chi0_inf2, const double *__restrict__ spl, const double2 *__restrict__ tw,
+                double T, int n8) {
+    constexpr int NJ = N / 2 + 1;
+    static_assert(2 * NJ * sizeof(double) <= Tau2Smem<N>::buf, "pair must fit the FFT buffer");
+    extern __shared__ __align__(16) double A[];
+    double2 *X = reinterpret_cast<double2 *>(A);
+    TwoLevelTw *tw2 = reinterpret_cast<TwoLevelTw *>(reinterpret_cast<char *>(A) + Tau2Smem<N>::buf);
+    __shared__ double d0[2], dN[2], V0[2], VN[2], sV[2], sM[2], integ[2];
+    const int pair = blockIdx.x, blk = pair >> 1, half = pair & 1;
+    const int o0 = 2 * pair;
+    double *g = chiq + (size_t)blk * 4 * NJ + 2 * half;
+    tau_tables(tw2, tw2 + 1, tw, tw, N);
+    stage_pair4(A, chiq + (size_t)blk * 4 * NJ, NJ, half, o0, n8);
+    if (threadIdx.x < 2) {
+        const int o = o0 + threadIdx.x;
+        d0[threadIdx.x] = o < n8 ? dtau_chiqt0[o] : 0.0;
+        dN[threadIdx.x] = 0.0;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        V0[threadIdx.x] = A[threadIdx.x * NJ];
+        VN[threadIdx.x] = A[threadIdx.x * NJ + NJ - 1];
+    }
+    column_sums<2>(A, NJ, 0, NJ, sV);
+    const double h = 1.0 / (N * T);
+    spline_second_derivatives<2>(A, NJ, NJ, h, d0, dN, spl, spl + NJ);
+    column_sums<2>(A, NJ, 0, NJ, sM);
+    if (threadIdx.x < 2) {
+        const int c = threadIdx.x;
+        const double M0 = A[c * NJ], MN = A[c * NJ + NJ - 1];
+        integ[c] = h * (sV[c] - 0.5 * (V0[c] + VN[c])) - h * h * h / 24.0 * (2.0 * sM[c] - M0 - MN);
+    }
+    constexpr int G = FftPlan<N>::G;
+    if (threadIdx.x < G) {
+        const double *Ma = A, *Mb = A + NJ;
+        auto in = [&](int j) -> double2 {
+            const bool lo = j < N / 2;
+            const int jj = lo ? j : N - 1 - j;
+            const double sg = lo ? 1.0 : -1.0;
+            return make_double2(sg * (Ma[jj + 1] - Ma[jj]) / h, sg * (Mb[jj + 1] - Mb[jj]) / h);
+        };
+        group_fft_io<N, +1, false, true>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
+    }
+    __syncthreads();
+    for (int n = threadIdx.x + 1; n < NJ; n += blockDim.x) {
+        const double2 Z = X[pidx(n)];
+        const double2 Zc = X[pidx(N - n)];
+        const double2 Fa = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
+        const double2 Fb = make_double2(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
+        const double wn = 2 * n * kPi * T;
+        const double2 w = tw_at(tw2, n);
+        const double cth = w.x, sth = -w.y;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int o = o0 + q;
+            const double2 F = q == 0 ? Fa : Fb;
+            const double cinf = -2.0 * d0[q];
+            double val = cinf / (wn * wn) + ((1.0 - cth) * F.x + sth * F.y) / (wn * wn * wn * wn);
+            if (o == 0) val = 0.0;
+            g[4 * n + q] = val;
+            if (n == NJ - 1 && o < n8) chi0_inf2[o] = (o == 0) ? 0.0 : 2.0 * F.x;
+        }
+    }
+    if (threadIdx.x < 2) {
+        const int o = o0 + threadIdx.x;
+        g[threadIdx.x] = 2.0 * integ[threadIdx.x];
+        if (o < n8) chi0_inf[o] = (o == 0) ? 0.0 : -2.0 * d0[threadIdx.x];
+    }
+}
+
+// k_vertex_tau for one pair per CTA (in-place FFT, two CTAs per SM).
+template <int N>
+__global__ void __launch_bounds__(256, 2)
+    k_vertex_tau2(double *__restrict__ Vr, const double *__restrict__ chirt, const double2 *__restrict__ tw,
+                  double fact, int n8) {
+    constexpr int NJ = N / 2 + 1;
+    static_assert(2 * NJ * sizeof(double) <= Tau2Smem<N>::buf, "pair must fit the FFT buffer");
+    extern __shared__ __align__(16) double A[];
+    double2 *X = reinterpret_cast<double2 *>(A);
+    TwoLevelTw *tw2 = reinterpret_cast<TwoLevelTw *>(reinterpret_cast<char *>(A) + Tau2Smem<N>::buf);
+    const int pair = blockIdx.x, blk = pair >> 1, half = pair & 1;
+    const int o0 = 2 * pair;
+    tau_tables(tw2, tw2 + 1, tw, tw, N);
+    stage_pair4(A, Vr + (size_t)blk * 4 * NJ, NJ, half, o0, n8);
+    __syncthreads();
+    constexpr int G = FftPlan<N>::G;
+    if (threadIdx.x < G) {
+        const double *a = A, *b = A + NJ;
+        // even extension of the two columns: a DCT-I each, packed as Re/Im
+        auto in = [&](int j) -> double2 {
+            const int jj = j < NJ ? j : N - j;
+            return make_double2(a[jj], b[jj]);
+        };
+        group_fft_io<N, -1, false, true>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
+    }
+    __syncthreads();
+    double *g = Vr + (size_t)blk * 4 * NJ + 2 * half;
+    const double *cr = chirt + (size_t)blk * 4 * NJ + 2 * half;
+    for (int n = threadIdx.x; n < NJ; n += blockDim.x) {
+        const double2 Z = X[pidx(n)];
+        g[4 * n] = (o0 < n8) ? Z.x + fact * cr[4 * n] : 0.0;
+        g[4 * n + 1] = (o0 + 1 < n8) ? Z.y + fact * cr[4 * n + 1] : 0.0;
     }
 }
 
@@ -1422,8 +1638,15 @@ template <int N>
 struct RunChi0Tau {
     static cudaError_t run(const GridDev *g, double *chiq, const double *dchiqt0, double *cinf, double *cinf2,
                            double T, cudaStream_t st) {
+        cudaError_t e;
+        if constexpr (N / 16 <= 256) {
+            const size_t sm = Tau2Smem<N>::bytes;
+            if ((e = set_smem(k_chi0_tau2<N>, sm)) != cudaSuccess) return e;
+            k_chi0_tau2<N><<<g->n8p / 2, 256, sm, st>>>(chiq, dchiqt0, cinf, cinf2, g->spl_half, g->tw_w, T, g->n8);
+            return launched();
+        }
         const size_t sm = TauSmem<N>::bytes(N / 2 + 1);
-        cudaError_t e = set_smem(k_chi0_tau<N>, sm);
+        e = set_smem(k_chi0_tau<N>, sm);
         if (e != cudaSuccess) return e;
         k_chi0_tau<N><<<g->n8p / 4, TauSmem<N>::threads, sm, st>>>(chiq, dchiqt0, cinf, cinf2, g->spl_half, g->tw_w,
                                                                     T, g->n8);
@@ -1433,8 +1656,15 @@ struct RunChi0Tau {
 template <int N>
 struct RunVertexTau {
     static cudaError_t run(const GridDev *g, double *Vr, const double *chirt, double fact, cudaStream_t st) {
+        cudaError_t e;
+        if constexpr (N / 16 <= 256) {
+            const size_t sm = Tau2Smem<N>::bytes;
+            if ((e = set_smem(k_vertex_tau2<N>, sm)) != cudaSuccess) return e;
+            k_vertex_tau2<N><<<g->n8p / 2, 256, sm, st>>>(Vr, chirt, g->tw_w, fact, g->n8);
+            return launched();
+        }
         const size_t sm = TauSmem<N>::bytes(N / 2 + 1);
-        cudaError_t e = set_smem(k_vertex_tau<N>, sm);
+        e = set_smem(k_vertex_tau<N>, sm);
         if (e != cudaSuccess) return e;
         k_vertex_tau<N><<<g->n8p / 4, TauSmem<N>::threads, sm, st>>>(Vr, chirt, g->tw_w, fact, g->n8);
         return launched();
@@ -1444,9 +1674,17 @@ template <int N>
 struct RunSigmaTau {
     static cudaError_t run(const GridDev *g, const double *sigt, const double *dS, double2 *S, double *s2, double *s3,
                            double *s4, double *sinf, double T, cudaStream_t st) {
+        cudaError_t e;
+        if constexpr (N / 16 <= 256) {
+            // one pair per CTA, two CTAs per SM
+            const size_t sm = Tau2Smem<N>::bytes;
+            if ((e = set_smem(k_sigma_tau2<N>, sm)) != cudaSuccess) return e;
+            k_sigma_tau2<N><<<g->n8p / 2, 256, sm, st>>>(sigt, dS, S, s2, s3, s4, sinf, g->spl_full, g->tw_w,
+                                                         g->ht_w, T, g->n8, g->n8p);
+            return launched();
+        }
         const size_t sm = TauSmem<N>::bytes(N + 1);
-        cudaError_t e = set_smem(k_sigma_tau<N>, sm);
-        if (e != cudaSuccess) return e;
+        if ((e = set_smem(k_sigma_tau<N>, sm)) != cudaSuccess) return e;
         k_sigma_tau<N><<<g->n8p / 4, TauSmem<N>::threads, sm, st>>>(sigt, dS, S, s2, s3, s4, sinf, g->spl_full,
                                                                      g->tw_w, g->ht_w, T, g->n8, g->n8p);
         return launched();

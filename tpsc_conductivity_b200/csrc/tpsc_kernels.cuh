@@ -112,6 +112,20 @@ cudaError_t launch_trace_self_G(const GridDev &g, const double2 *S, const double
 cudaError_t launch_trace_self_G2(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                                  const double *sinf, double mu, double T, Reduce r, cudaStream_t st);
 
+// ---- the Newton form's root searches on the device (tpsc_roots.cu) ----------
+constexpr int kRootMaxBlocks = 1024;
+struct RootScratch {
+    double *partial = nullptr;  // [2 kRootMaxBlocks]
+    unsigned *bar = nullptr;    // [4]: barrier arrivals, generation, error flag
+    double *ctl = nullptr;      // [8] Newton state
+    double *out = nullptr;      // [8] results
+};
+// Usp then Uch by safeguarded Newton with the moment series, one cooperative
+// launch -> rs.out = {Usp, Uch, evals_sp, evals_ch, ok_sp, ok_ch}
+cudaError_t launch_sumrule_roots(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
+                                 const double *mom_suf, const double *cmax_suf, const double *tailm, double T,
+                                 double n, double nsr, double U, double hi_sp, RootScratch rs, cudaStream_t st);
+
 // ---- real-frequency continuation (Pade / Lagrange) and local G ---------------
 cudaError_t launch_pade_sigma(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                               const double *sinf, const int *nidx, int Nn, const double2 *z, int Nz, int mode,
