@@ -54,6 +54,58 @@ struct KSum {
 };
 
 // ---------------------------------------------------------------------------
+// two-pass reductions: per-block partials, then one block adds them in order
+// ---------------------------------------------------------------------------
+template <int NV>
+__device__ void block_store(double (&v)[NV], double *partial) {
+    __shared__ double red[32][NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) red[warp][k] = v[k];
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double x = lane < nw ? red[lane][k] : 0.0;
+            for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+            if (lane == 0) partial[k * kMaxBlocks + blockIdx.x] = x;
+        }
+    }
+}
+
+// Sum of the per-block partials in a fixed order: warp k adds value k with
+// lane-strided compensated sums and a shuffle tree (deterministic).
+template <int NV>
+__global__ void k_finish(const double *partial, int nblocks, double *result, double offset0) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int k = warp; k < NV; k += blockDim.x >> 5) {
+        KSum acc;
+        for (int b = lane; b < nblocks; b += 32) acc.add(partial[k * kMaxBlocks + b]);
+        double v = acc.value();
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) result[k] = v + (k == 0 ? offset0 : 0.0);
+    }
+}
+
+__global__ void k_max_finish(const double *partial, int nblocks, double *result) {
+    double m = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += 32) m = fmax(m, partial[b]);
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+    if (threadIdx.x == 0) result[0] = m;
+}
+
+template <int NV>
+cudaError_t finish(Reduce r, int nblocks, double offset0, cudaStream_t st) {
+    k_finish<NV><<<1, 32 * (NV < 32 ? NV : 32), 0, st>>>(r.partial, nblocks, r.result, offset0);
+    return launched();
+}
+
+// ---------------------------------------------------------------------------
 // slice kernels: shared-memory plan of one nbk x nbk slice + FFT scratch
 // ---------------------------------------------------------------------------
 template <int NBK>
@@ -253,6 +305,26 @@ __device__ __forceinline__ void sigma_full(double i1, double sinf, double c2, do
     const double i2 = i1 * i1, i4 = i2 * i2;
     rS = -c2 * i2 + Sv.x * i4;
     iS = -sinf * i1 + c3 * i2 * i1 + Sv.y * i4;
+}
+
+// 32-byte streaming load (two 16-byte evict-first loads)
+__device__ __forceinline__ double4 ld_stream4(const double4 *p) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    const double2 a = __ldcs(q), b = __ldcs(q + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// one term of Tr(G - G0) (green::traceDiffG, src/green.cpp:3108-3182) and its
+// derivative with respect to the chemical potential pmu: w Re[G - G0] with
+// G = 1/(i w_n - e + pmu - Sigma), G0 = 1/(i w_n - e + mu0)
+__device__ __forceinline__ void trdiff_term(double wn, double rS, double iS, double e, double mu0, double pmu,
+                                            double w, double &v, double &dv) {
+    const double a = e - pmu + rS, d = e - mu0, g = mu0 - pmu + rS;
+    const double A2 = (wn - iS) * (wn - iS) + a * a;
+    const double num = g * a * d + iS * (iS - 2 * wn) * d - wn * wn * g;
+    const double inv = w / (A2 * (wn * wn + d * d));
+    v += inv * num;
+    dv += inv * (wn * wn - (a + g) * d + num * 2.0 * a / A2);
 }
 
 // complex division

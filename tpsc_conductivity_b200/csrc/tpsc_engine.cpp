@@ -897,80 +897,65 @@ int trace_diff_G(tpsc_ctx *ctx, double pmu, double *tr, double *dtr = nullptr) {
 }
 
 // The find_mu series covers the frequencies from jc = first n with
-// w_n >= kMomMuRange / kMomSeriesMax (capped at Nw0/2: then only the tail),
-// valid for |mu - mu0| <= dmax.
+// w_n >= kMomMuRange / kMuSeriesMax (capped at Nw0/2: then only the tail),
+// valid for |mu - mu0| <= dmax = kMuSeriesMax |z|_min, where |z| >= w_n -
+// |Im Sigma| >= w_n - 2 Sigma_inf / w_n bounds |z| on the series set.
 void mu_series_cut(const tpsc_ctx *ctx, int *jc_out, double *dmax) {
     const int NO = ctx->cur->d.nw0 / 2;
     const double pt = PI * ctx->T;
-    int jc = (int)std::ceil((kMomMuRange / kMomSeriesMax / pt - 1.0) / 2.0);
+    int jc = (int)std::ceil((kMomMuRange / kMuSeriesMax / pt - 1.0) / 2.0);
     jc = std::max(0, std::min(jc, NO));
     const double wc = (2 * jc + 1) * pt;
     const double zmin = wc - 2.0 * std::fabs(ctx->scal[TPSC_S_SIGMA_INF]) / wc;
-    *dmax = zmin > 0 ? kMomSeriesMax * zmin : 0.0;
+    *dmax = zmin > 0 ? kMuSeriesMax * zmin : 0.0;
     *jc_out = jc;
+}
+
+// The Newton form of traceSelfG + find_mu + traceSelfG2: one pass over Sigma
+// for Tr Sigma G0 and the series moments (k_sigma_moments), then the Newton
+// search and Tr Sigma G at mu in one cooperative launch (k_mu_roots), one
+// readback for all of it.
+int self_traces_and_mu_newton(tpsc_ctx *ctx) {
+    Grid *g = ctx->cur;
+    const GridDev &d = g->d;
+    int jc;
+    double dmax;
+    mu_series_cut(ctx, &jc, &dmax);
+    CK(launch_sigma_moments(d, g->S, g->s2, g->s3, g->s4, g->sinf, g->mu0, ctx->T, jc, ctx->redm, ctx->st));
+    CK(launch_mu_roots(d, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->redm.result, g->mu0, ctx->T, jc, dmax, ctx->roots,
+                       ctx->st));
+    CK(cudaMemcpyAsync(ctx->h_res, ctx->redm.result, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(ctx->h_res + 2, ctx->roots.out, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(ctx->h_res + 6, ctx->roots.bar + 2, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    int err;
+    std::memcpy(&err, ctx->h_res + 6, sizeof(int));
+    if (err) return fail(ctx, TPSC_ERR_CUDA, "device mu search: grid barrier timed out");
+    const double *r = ctx->h_res;
+    ctx->scal[TPSC_S_TR_SG] = r[0];
+    ctx->scal[TPSC_S_TR_SG_ASYMP] = r[0] + r[1];
+    if (r[4] != 1.0) return fail(ctx, TPSC_ERR_NO_ROOT, "mu not found");
+    ctx->scal[TPSC_S_MU] = r[2];
+    ctx->scal[TPSC_S_EVALS_MU] = r[3];
+    ctx->scal[TPSC_S_TR_SG2] = r[5];
+    ctx->scal[TPSC_S_DBLOCC_SG2] = (r[5] + ctx->U * ctx->n * ctx->n / 4.0) / ctx->U;
+    return TPSC_OK;
 }
 
 int find_mu(tpsc_ctx *ctx) {
     Grid *g = ctx->cur;
     if (!g || !g->have_S) return fail(ctx, TPSC_ERR_STATE, "the self-energy has not been computed");
+    if (ctx->form & TPSC_FORM_NEWTON) return self_traces_and_mu_newton(ctx);
     int rc = TPSC_OK;
     auto f = [&](double m, double &y) -> bool {
         rc = trace_diff_G(ctx, m, &y);
         return rc == TPSC_OK;
     };
-    // Newton form: the frequencies with w_n >= w_c enter as the series
-    //   Re sum_m (mu0 - mu)^m C_m - G0,  C_m = sum w (i w_n - eps + mu0 - Sigma)^-(m+1)
-    // of k_trdiff_moments, valid while |mu - mu0| <= dmax = kMomSeriesMax |z|_min;
-    // only the frequencies below w_c are summed per evaluation.  |z| >= w_n -
-    // |Im Sigma| >= w_n - 2 Sigma_inf / w_n bounds |z| on the series set.
-    const GridDev &d = g->d;
-    int jc;
-    double dmax;
-    mu_series_cut(ctx, &jc, &dmax);
-    double Cm[2 * kMomP + 1] = {0};
-    const bool newton = (ctx->form & TPSC_FORM_NEWTON) != 0;
-    if (newton && dmax > 0) {
-        CK(launch_trdiff_moments(d, g->S, g->s2, g->s3, g->s4, g->sinf, g->mu0, g->mu0, ctx->T, jc, ctx->redm,
-                                 ctx->st));
-        if ((rc = read_result(ctx, 2 * kMomP + 1, Cm, ctx->redm.result))) return rc;
-    }
-    auto fd = [&](double m, double &y, double &dy) -> bool {
-        const double delta = m - g->mu0;
-        if (!(newton && std::fabs(delta) <= dmax)) {
-            rc = trace_diff_G(ctx, m, &y, &dy);
-            return rc == TPSC_OK;
-        }
-        rc = TPSC_OK;
-        cudaError_t e = launch_trace_diff_G(d, g->S, g->s2, g->s3, g->s4, g->sinf, g->mu0, m, ctx->T, ctx->red,
-                                            ctx->st, jc);
-        if (e != cudaSuccess) {
-            rc = cuda_fail(ctx, e, "launch_trace_diff_G");
-            return false;
-        }
-        double r[2];
-        if ((rc = read_result(ctx, 2, r))) return false;
-        // Re sum_m (-delta)^m C_m and its delta derivative, in long double
-        long double sr = 0.0L, dsr = 0.0L;
-        long double pr = 1.0L, pi = 0.0L;  // (-delta)^m as a real power
-        for (int k = 0; k < kMomP; ++k) {
-            sr += pr * Cm[2 * k];
-            if (k > 0) dsr += -k * pi * Cm[2 * k];  // d/d delta (-delta)^k = -k (-delta)^(k-1)
-            pi = pr;
-            pr *= -(long double)delta;
-        }
-        y = r[0] + (double)(sr - Cm[2 * kMomP]);
-        dy = r[1] + (double)dsr;
-        return true;
-    };
     const double init[3] = {0.0, -10.0, 10.0}, lims[2] = {-20.0, 20.0};
     double root = 0;
     int nev;
     bool derr;
-    // the Newton form starts from mu0, the non-interacting chemical potential
-    const bool ok = (ctx->form & TPSC_FORM_NEWTON)
-                        ? newton_root(fd, g->mu0, init[1], init[2], 1e-15, &root, &nev, &derr)
-                        : find_zero(f, init, &root, lims, &nev, &derr);
-    if (!ok) {
+    if (!find_zero(f, init, &root, lims, &nev, &derr)) {
         if (derr) return rc;
         return fail(ctx, TPSC_ERR_NO_ROOT, "mu not found");
     }
@@ -1152,12 +1137,12 @@ tpsc_ctx *tpsc_create(int device, int *status) {
     if ((e = cudaMalloc(&ctx->red.result, 8 * sizeof(double))) != cudaSuccess) return bad(e);
     if ((e = cudaMalloc(&ctx->red.ticket, sizeof(unsigned))) != cudaSuccess) return bad(e);
     if ((e = cudaMemset(ctx->red.ticket, 0, sizeof(unsigned))) != cudaSuccess) return bad(e);
-    if ((e = cudaMalloc(&ctx->redm.partial, (2 * kMomP + 2) * kMaxBlocks * sizeof(double))) != cudaSuccess)
+    if ((e = cudaMalloc(&ctx->redm.partial, (size_t)std::max(2 * kMomP + 2, kSigmaMomNV) * kMaxBlocks *
+                                                 sizeof(double))) != cudaSuccess)
         return bad(e);
     if ((e = cudaMalloc(&ctx->redm.result, 32 * sizeof(double))) != cudaSuccess) return bad(e);
-    if ((e = cudaMalloc(&ctx->roots.partial, 2 * kRootMaxBlocks * sizeof(double))) != cudaSuccess) return bad(e);
+    if ((e = cudaMalloc(&ctx->roots.partial, 4 * kRootMaxBlocks * sizeof(double))) != cudaSuccess) return bad(e);
     if ((e = cudaMalloc(&ctx->roots.bar, 4 * sizeof(unsigned))) != cudaSuccess) return bad(e);
-    if ((e = cudaMalloc(&ctx->roots.ctl, 8 * sizeof(double))) != cudaSuccess) return bad(e);
     if ((e = cudaMalloc(&ctx->roots.out, 8 * sizeof(double))) != cudaSuccess) return bad(e);
     if ((e = cudaMallocHost(&ctx->h_res, 32 * sizeof(double))) != cudaSuccess) return bad(e);
     for (auto &ev : ctx->ev)
@@ -1178,7 +1163,6 @@ void tpsc_destroy(tpsc_ctx *ctx) {
     if (ctx->redm.result) cudaFree(ctx->redm.result);
     if (ctx->roots.partial) cudaFree(ctx->roots.partial);
     if (ctx->roots.bar) cudaFree(ctx->roots.bar);
-    if (ctx->roots.ctl) cudaFree(ctx->roots.ctl);
     if (ctx->roots.out) cudaFree(ctx->roots.out);
     if (ctx->h_res) cudaFreeHost(ctx->h_res);
     if (ctx->stage) cudaFree(ctx->stage);
@@ -1323,9 +1307,12 @@ int tpsc_solve(tpsc_ctx *ctx) {
     rc = run_self(ctx);
     if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[4], ctx->st));
-    double tsg[2];
-    rc = trace_self_G(ctx, tsg);
-    if (rc) return rc;
+    // the Newton form computes traceSelfG in the same Sigma pass as the find_mu moments
+    if (!(ctx->form & TPSC_FORM_NEWTON)) {
+        double tsg[2];
+        rc = trace_self_G(ctx, tsg);
+        if (rc) return rc;
+    }
     rc = find_mu(ctx);
     if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[5], ctx->st));

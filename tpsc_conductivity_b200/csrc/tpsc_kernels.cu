@@ -38,49 +38,6 @@ namespace {
 // per-block partials -> one block finishes in a fixed order
 // ---------------------------------------------------------------------------
 
-template <int NV>
-__device__ void block_store(double (&v)[NV], double *partial) {
-    __shared__ double red[32][NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k)
-        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0)
-#pragma unroll
-        for (int k = 0; k < NV; ++k) red[warp][k] = v[k];
-    __syncthreads();
-    if (warp == 0) {
-        const int nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            double x = lane < nw ? red[lane][k] : 0.0;
-            for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
-            if (lane == 0) partial[k * kMaxBlocks + blockIdx.x] = x;
-        }
-    }
-}
-
-// Sum of the per-block partials in a fixed order: warp k adds value k with
-// lane-strided compensated sums and a shuffle tree (deterministic).
-template <int NV>
-__global__ void k_finish(const double *partial, int nblocks, double *result, double offset0) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int k = warp; k < NV; k += blockDim.x >> 5) {
-        KSum acc;
-        for (int b = lane; b < nblocks; b += 32) acc.add(partial[k * kMaxBlocks + b]);
-        double v = acc.value();
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        if (lane == 0) result[k] = v + (k == 0 ? offset0 : 0.0);
-    }
-}
-
-__global__ void k_max_finish(const double *partial, int nblocks, double *result) {
-    double m = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += 32) m = fmax(m, partial[b]);
-    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
-    if (threadIdx.x == 0) result[0] = m;
-}
-
 int grid_for(long long total, int threads) {
     long long b = (total + threads - 1) / threads;
     if (b < 1) b = 1;
@@ -88,11 +45,6 @@ int grid_for(long long total, int threads) {
     return (int)b;
 }
 
-template <int NV>
-cudaError_t finish(Reduce r, int nblocks, double offset0, cudaStream_t st) {
-    k_finish<NV><<<1, 32 * (NV < 32 ? NV : 32), 0, st>>>(r.partial, nblocks, r.result, offset0);
-    return launched();
-}
 
 // ---------------------------------------------------------------------------
 // mu0 of the finite lattice: sum_o w 2 f(eps - mu) / L^2 - n
@@ -802,13 +754,6 @@ __device__ void grid_finish(double (&v)[NV], Reduce r, double offset0) {
 
 constexpr int kRedThreads = 256;
 
-// streaming (evict-first) load of 32 bytes as two 16-byte loads
-__device__ __forceinline__ double4 ld_stream4(const double4 *p) {
-    const double2 *q = reinterpret_cast<const double2 *>(p);
-    const double2 a = __ldcs(q), b = __ldcs(q + 1);
-    return make_double4(a.x, a.y, b.x, b.y);
-}
-
 // chi::traceDiffChispChi0 (sgn = -1) / traceDiffChichChi0 (sgn = +1)
 // (src/chi.cpp:738-830): sum over q and n <= Nw0/2 of w T/Nq [chi/(1 + sgn U
 // chi/2) - chi], plus the tail Nw0/2 < n <= Nw0 with chi = c2/qn^2 + c4/qn^4,
@@ -1057,20 +1002,10 @@ __global__ void __launch_bounds__(256)
 // Tr(G - G0) at chemical potential pmu (green::traceDiffG,
 // src/green.cpp:3108-3182): stored frequencies j < Nw0/2 with the full Sigma,
 // tail Nw0/2 <= j <= Nw0 with its asymptotic form.  One CTA per column block.
-// one term of Tr(G - G0) and its derivative with respect to pmu
-__device__ __forceinline__ void trdiff_term(double wn, double rS, double iS, double e, double mu0, double pmu,
-                                            double w, double &v, double &dv) {
-    const double a = e - pmu + rS, d = e - mu0, g = mu0 - pmu + rS;
-    const double A2 = (wn - iS) * (wn - iS) + a * a;
-    const double num = g * a * d + iS * (iS - 2 * wn) * d - wn * wn * g;
-    const double inv = w / (A2 * (wn * wn + d * d));
-    v += inv * num;
-    dv += inv * (wn * wn - (a + g) * d + num * 2.0 * a / A2);
-}
 
 // Stored frequencies j < jdir term by term (jdir = Nw0/2: all), and the
 // tail Nw0/2 <= j <= Nw0 when `tail` is set; the Newton form covers the
-// rest with the series of k_trdiff_moments.
+// rest with the series of k_sigma_moments.
 __global__ void __launch_bounds__(kRedThreads)
     k_trace_diff_G(const double2 *__restrict__ S, const double *__restrict__ s2, const double *__restrict__ s3,
                    const double *__restrict__ s4, const double *__restrict__ sinfp, const double *__restrict__ ek,
@@ -1155,60 +1090,6 @@ __global__ void __launch_bounds__(kRedThreads)
     }
     double out[2] = {v, dv};
     grid_finish<2>(out, r, 0.0);
-}
-
-// Moments of the high-frequency part of Tr(G - G0) for the Newton form of
-// find_mu.  With z = i w_n - eps_k + mu_r - Sigma(k, i w_n) over every octant
-// k and the frequencies jc <= n < Nw0/2 (stored Sigma) and Nw0/2 <= n <= Nw0
-// (asymptotic Sigma, as k_trace_diff_G sums them):
-//   v[2m], v[2m+1] = Re, Im sum w z^-(m+1),  m < kMomP
-//   v[2 kMomP]     = sum w Re 1/(i w_n - eps_k + mu0)
-// so that this part of the trace at mu is Re sum_m (mu_r - mu)^m C_m - v[2 kMomP]
-// while |mu - mu_r| |z|^-1 < kMomSeriesMax.  Per-block partials (block_store).
-__global__ void __launch_bounds__(kRedThreads)
-    k_trdiff_moments(const double2 *__restrict__ S, const double *__restrict__ s2, const double *__restrict__ s3,
-                     const double *__restrict__ s4, const double *__restrict__ sinfp, const double *__restrict__ ek,
-                     const double *__restrict__ w16, int nw0, double mu0, double mu_r, double T, int jc,
-                     double *partial) {
-    constexpr int NV = 2 * kMomP + 1;
-    const int blk = blockIdx.x, o0 = 4 * blk, NO = nw0 / 2;
-    const double sinf = sinfp[0];
-    const double pt = 3.141592653589793 * T;
-    double acc[NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
-    auto add = [&](double wn, double rS, double iS, double e, double w) {
-        const double zx = mu_r - e - rS, zy = wn - iS;
-        const double rr = 1.0 / (zx * zx + zy * zy);  // |z| >= w_n: no overflow or underflow here
-        const double2 zi = make_double2(zx * rr, -zy * rr);
-        double2 zp = zi;
-#pragma unroll
-        for (int m = 0; m < kMomP; ++m) {
-            acc[2 * m] += w * zp.x;
-            acc[2 * m + 1] += w * zp.y;
-            zp = cmul(zp, zi);
-        }
-        const double d = mu0 - e;
-        acc[2 * kMomP] += w * d / (d * d + wn * wn);
-    };
-    for (int c = 0; c < 4; ++c) {
-        const double w = w16[o0 + c];
-        if (w == 0.0) continue;
-        const int o = o0 + c;
-        const double e = ek[o], c2 = s2[o], c3 = s3[o], c4 = s4[o];
-        for (int j = jc + threadIdx.x; j < NO; j += blockDim.x) {
-            const double wn = (2 * j + 1) * pt, i1 = 1.0 / wn;
-            double rS, iS;
-            sigma_full(i1, sinf, c2, c3, S[bidx(j, o, NO)], rS, iS);
-            add(wn, rS, iS, e, w);
-        }
-        for (int t = threadIdx.x; t <= NO; t += blockDim.x) {
-            const double wn = (2 * (NO + t) + 1) * pt;
-            const double i1 = 1.0 / wn, i2 = i1 * i1;
-            add(wn, -c2 * i2 + c4 * i2 * i2, -sinf * i1 + c3 * i2 * i1, e, w);
-        }
-    }
-    block_store<NV>(acc, partial);
 }
 
 // Tr Sigma G0 and its asymptotic correction (green::traceSelfG,
@@ -1827,18 +1708,6 @@ cudaError_t launch_trace_diff_G(const GridDev &g, const double2 *S, const double
     k_trace_diff_G<<<nblk, kRedThreads, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.nw0, mu0, pmu, T, jdir, tail,
                                                   r);
     return launched();
-}
-
-cudaError_t launch_trdiff_moments(const GridDev &g, const double2 *S, const double *s2, const double *s3,
-                                  const double *s4, const double *sinf, double mu0, double mu_r, double T, int jc,
-                                  Reduce r, cudaStream_t st) {
-    constexpr int NV = 2 * kMomP + 1;
-    const int nblk = g.n8p / 4;
-    k_trdiff_moments<<<nblk, kRedThreads, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.nw0, mu0, mu_r, T, jc,
-                                                    r.partial);
-    cudaError_t e = launched();
-    if (e != cudaSuccess) return e;
-    return finish<NV>(r, nblk, 0.0, st);
 }
 
 cudaError_t launch_trace_self_G(const GridDev &g, const double2 *S, const double *s2, const double *s3,

@@ -80,6 +80,8 @@ cudaError_t launch_tail_moments(const GridDev &g, const double *chi0_inf, const 
 constexpr int kMomP = 8;
 constexpr double kMomSeriesMax = 0.004;  // |h chi| bound of the series terms: 0.004^8 < 1e-19
 constexpr double kMomMuRange = 0.35;     // |mu - mu0| the find_mu series is built to cover
+constexpr int kMuMomP = 12;              // terms of the find_mu series
+constexpr double kMuSeriesMax = 0.03;    // |mu - mu0| / |z| bound of its terms: 0.03^12 < 1e-18
 cudaError_t launch_chi0_moments(const GridDev &g, const double *chiq, double *mom, double *cmax, cudaStream_t st);
 cudaError_t launch_trace_chi0(const GridDev &g, const double *chiq, const double *chi0_inf,
                               const double *chi0_inf2, double T, Reduce r, cudaStream_t st);
@@ -102,11 +104,6 @@ cudaError_t launch_sigma_tau(const GridDev &g, const double *sigt, const double 
 cudaError_t launch_trace_diff_G(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                                 const double *s4, const double *sinf, double mu0, double pmu, double T, Reduce r,
                                 cudaStream_t st, int jdir = -1);
-// series moments of the frequencies j >= jc (and the tail) around mu_r ->
-// r.result[0 .. 2 kMomP] (r.partial must hold (2 kMomP + 1) kMaxBlocks doubles)
-cudaError_t launch_trdiff_moments(const GridDev &g, const double2 *S, const double *s2, const double *s3,
-                                  const double *s4, const double *sinf, double mu0, double mu_r, double T, int jc,
-                                  Reduce r, cudaStream_t st);
 cudaError_t launch_trace_self_G(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                                 const double *sinf, double mu0, double T, Reduce r, cudaStream_t st);
 cudaError_t launch_trace_self_G2(const GridDev &g, const double2 *S, const double *s2, const double *s3,
@@ -115,11 +112,26 @@ cudaError_t launch_trace_self_G2(const GridDev &g, const double2 *S, const doubl
 // ---- the Newton form's root searches on the device (tpsc_roots.cu) ----------
 constexpr int kRootMaxBlocks = 1024;
 struct RootScratch {
-    double *partial = nullptr;  // [2 kRootMaxBlocks]
+    double *partial = nullptr;  // [4 kRootMaxBlocks]
     unsigned *bar = nullptr;    // [4]: barrier arrivals, generation, error flag
-    double *ctl = nullptr;      // [8] Newton state
     double *out = nullptr;      // [8] results
 };
+// The Newton form's Sigma pass: Tr Sigma G0 (green::traceSelfG) and the
+// find_mu series moments around mu0 over the frequencies n >= jc and the tail
+// -> r.result[0..1] = (trace, asymptotic correction), r.result[2 + 2m],
+// r.result[3 + 2m] = Re, Im sum w (i w_n - eps + mu0 - Sigma)^-(m+1), m < kMuMomP,
+// r.result[2 + 2 kMuMomP] = sum w Re 1/(i w_n - eps + mu0).  r.partial must
+// hold (2 kMuMomP + 3) kMaxBlocks doubles.
+constexpr int kSigmaMomNV = 2 * kMuMomP + 3;
+cudaError_t launch_sigma_moments(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                                 const double *s4, const double *sinf, double mu0, double T, int jc, Reduce r,
+                                 cudaStream_t st);
+// mu by safeguarded Newton from mu0 (the series of the moments `mom` for
+// |mu - mu0| <= dmax, the full sum beyond), then Tr Sigma G at mu; one
+// cooperative launch -> rs.out = {mu, evals, ok, Tr Sigma G}
+cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2, const double *s3, const double *s4,
+                            const double *sinf, const double *mom, double mu0, double T, int jc, double dmax,
+                            RootScratch rs, cudaStream_t st);
 // Usp then Uch by safeguarded Newton with the moment series, one cooperative
 // launch -> rs.out = {Usp, Uch, evals_sp, evals_ch, ok_sp, ok_ch}
 cudaError_t launch_sumrule_roots(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,

@@ -2,10 +2,10 @@
 //
 // The sum-rule roots Usp and Uch (chi::find_Usp_Uch(nq0, nw0, Usc),
 // src/chi.cpp:846-876) as one cooperative kernel: every block sums its share
-// of the stored frequencies below the series cut, a grid barrier, block 0
-// adds the high-frequency moment series and takes the safeguarded Newton
-// step, a grid barrier, and so on until both roots have converged.  One
-// launch and one readback replace a host round trip per evaluation.
+// of the stored frequencies below the series cut, a grid barrier, then every
+// block adds the partials and the high-frequency moment series and takes the
+// same safeguarded Newton step, until both roots have converged.  One launch
+// and one readback replace a host round trip per evaluation.
 //
 // The grid barrier spins on a generation counter with an iteration bound:
 // the launch is cooperative (every block resident), so the bound only ends
@@ -69,10 +69,9 @@ struct SumRootArgs {
     const double *tailm;     // [kMomP] tail moments, [kMomP] = max |chi| over the tail
     int nb, nblk, n8;
     double T, scale, n, nsr, U, hi_sp;
-    double *partial;  // [2 gridDim.x]
+    double *partial;  // [2][2 kRootMaxBlocks]: two buffers of (value, derivative) per block
     unsigned *bar;    // [2], zero at launch
     int *err;         // zero at launch
-    RootCtl *ctl;     // [1]
     double *out;      // Usp, Uch, evals_sp, evals_ch, ok_sp, ok_ch
 };
 
@@ -139,35 +138,35 @@ __device__ void newton_update(RootCtl &c, double y, double dy, double tol) {
     }
 }
 
+// One barrier per evaluation: every block writes its partial sums into the
+// buffer of the iteration's parity, waits at the barrier, then adds ALL
+// partials in the same order and takes the same Newton step on its own copy
+// of the state (identical in every block).  A buffer is rewritten two
+// iterations later, after a barrier that every reader of it has passed.
 __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
-    __shared__ int s_jdir, s_tail, s_done;
-    __shared__ double s_x;
+    __shared__ RootCtl sc;
+    __shared__ int s_jdir, s_tail;
     const int nwmax = a.nb - 1;
     const double tw = 2.0 * 3.141592653589793 * a.T;
     double Usp = 0.0;
+    int parity = 0;
 #pragma unroll 1
     for (int phase = 0; phase < 2; ++phase) {
         const double sgn = phase == 0 ? -1.0 : 1.0;
-        // every block has read the previous phase's result before it is overwritten
-        if (phase > 0 && !grid_sync(a.bar, a.err)) return;
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            RootCtl &c = *a.ctl;
-            c.lo = 0.0;
-            c.hi = phase == 0 ? a.hi_sp : 1000.0 * a.U;
+        if (threadIdx.x == 0) {
+            sc.lo = 0.0;
+            sc.hi = phase == 0 ? a.hi_sp : 1000.0 * a.U;
             // spin: U/2 (clamped inside the interval); charge: U
             const double x0 = phase == 0 ? a.U / 2.0 : a.U;
-            c.x = (x0 > c.lo && x0 < c.hi) ? x0 : 0.5 * (c.lo + c.hi);
-            c.prev_step = 0.0;
-            c.nev = c.it = c.done = c.ok = 0;
+            sc.x = (x0 > sc.lo && x0 < sc.hi) ? x0 : 0.5 * (sc.lo + sc.hi);
+            sc.prev_step = 0.0;
+            sc.nev = sc.it = sc.done = sc.ok = 0;
         }
+        __syncthreads();
 #pragma unroll 1
-        for (;;) {
-            if (!grid_sync(a.bar, a.err)) return;
+        while (!sc.done) {
             if (threadIdx.x == 0) {
-                const volatile RootCtl *c = a.ctl;
-                s_x = c->x;
-                s_done = c->done;
-                const double ah = fabs(s_x) / 2.0;
+                const double ah = fabs(sc.x) / 2.0;
                 // first frequency of the series (cmax_suf does not increase)
                 int lo = 0, hi = a.nb;
                 while (lo < hi) {
@@ -181,8 +180,7 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
                 s_tail = ah * a.tailm[kMomP] >= kMomSeriesMax;
             }
             __syncthreads();
-            if (s_done) break;
-            const double x = s_x, hu = sgn * x / 2.0;
+            const double x = sc.x, hu = sgn * x / 2.0;
             const int jdir = s_jdir;
             double v = 0.0, dv = 0.0;
             const long long total = (long long)a.nblk * jdir;
@@ -217,13 +215,15 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
                     }
                 }
             }
-            block_pair_sum(v, dv, a.partial + 2 * blockIdx.x);
+            double *part = a.partial + (size_t)parity * 2 * kRootMaxBlocks;
+            block_pair_sum(v, dv, part + 2 * blockIdx.x);
             if (!grid_sync(a.bar, a.err)) return;
-            if (blockIdx.x == 0 && threadIdx.x < 32) {
+            parity ^= 1;
+            if (threadIdx.x < 32) {
                 double pv = 0.0, pd = 0.0;
                 for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) {
-                    pv += __ldcg(&a.partial[2 * b]);
-                    pd += __ldcg(&a.partial[2 * b + 1]);
+                    pv += __ldcg(&part[2 * b]);
+                    pd += __ldcg(&part[2 * b + 1]);
                 }
                 for (int off = 16; off > 0; off >>= 1) {
                     pv += __shfl_down_sync(0xffffffffu, pv, off);
@@ -252,39 +252,329 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
                         y = tr + n - n * n / 2.0 - (nsr + Usp * nsr * nsr / (2.0 * U) - nsr * nsr);
                         dy = dtr;
                     }
-                    RootCtl c = *a.ctl;
-                    newton_update(c, y, dy, 1e-16);
-                    *a.ctl = c;
-                    __threadfence();
+                    newton_update(sc, y, dy, 1e-16);
                 }
             }
+            __syncthreads();
         }
-        // every block leaves the loop on the same done flag; record the root
-        const volatile RootCtl *vc = a.ctl;
-        const double root = vc->root;
-        const int nev = vc->nev, ok = vc->ok;
-        if (phase == 0) Usp = root;
+        if (phase == 0) Usp = sc.root;
         if (blockIdx.x == 0 && threadIdx.x == 0) {
-            a.out[phase] = root;
-            a.out[2 + phase] = nev;
-            a.out[4 + phase] = ok;
+            a.out[phase] = sc.root;
+            a.out[2 + phase] = sc.nev;
+            a.out[4 + phase] = sc.ok;
         }
-        if (!ok) return;
+        if (!sc.ok) return;
+        __syncthreads();
     }
 }
 
-}  // namespace
+// ---------------------------------------------------------------------------
+// chemical potential
+// ---------------------------------------------------------------------------
 
-cudaError_t launch_sumrule_roots(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
-                                 const double *mom_suf, const double *cmax_suf, const double *tailm, double T,
-                                 double n, double nsr, double U, double hi_sp, RootScratch rs, cudaStream_t st) {
+// One pass over Sigma for the Newton form: Tr Sigma G0 with its asymptotic
+// correction (green::traceSelfG, src/green.cpp:3001-3084) over the stored
+// frequencies, and the moments of the find_mu series over the stored
+// frequencies n >= jc and the tail Nw0/2 <= n <= Nw0 (asymptotic Sigma, as
+// green::traceDiffG sums them):
+//   C_m = sum w z^-(m+1),  z = i w_n - eps + mu0 - Sigma,  m < kMuMomP,
+//   G0  = sum w Re 1/(i w_n - eps + mu0),
+// so that this part of Tr(G - G0) at mu is Re sum_m (mu0 - mu)^m C_m - G0 to
+// a relative kMuSeriesMax^kMuMomP while |mu - mu0| <= kMuSeriesMax |z|.
+// One CTA per column block, per-block partials (block_store).
+__global__ void __launch_bounds__(256)
+    k_sigma_moments(const double2 *__restrict__ S, const double *__restrict__ s2, const double *__restrict__ s3,
+                    const double *__restrict__ s4, const double *__restrict__ sinfp, const double *__restrict__ ek,
+                    const double *__restrict__ w16, int nw0, double mu0, double T, double nk02, int jc,
+                    double *partial) {
+    constexpr int NV = kSigmaMomNV;
+    const int blk = blockIdx.x, o0 = 4 * blk, NO = nw0 / 2;
+    const double sinf = sinfp[0];
+    const double pt = 3.141592653589793 * T;
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    double ww[4], e[4], c2[4], c3[4], c4[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        ww[c] = w16[o0 + c];
+        const bool ok = ww[c] != 0.0;
+        e[c] = ok ? ek[o0 + c] : 0.0;
+        c2[c] = ok ? s2[o0 + c] : 0.0;
+        c3[c] = ok ? s3[o0 + c] : 0.0;
+        c4[c] = ok ? s4[o0 + c] : 0.0;
+    }
+    auto moments = [&](double wn, double rS, double iS, double ec, double w) {
+        const double zx = mu0 - ec - rS, zy = wn - iS;
+        const double rr = 1.0 / (zx * zx + zy * zy);  // |z| >= w_n > 0
+        const double2 zi = make_double2(zx * rr, -zy * rr);
+        double2 zp = zi;
+#pragma unroll
+        for (int m = 0; m < kMuMomP; ++m) {
+            acc[2 + 2 * m] += w * zp.x;
+            acc[3 + 2 * m] += w * zp.y;
+            zp = cmul(zp, zi);
+        }
+        const double d = mu0 - ec;
+        acc[2 + 2 * kMuMomP] += w * d / (d * d + wn * wn);
+    };
+    const double4 *row = reinterpret_cast<const double4 *>(S + (size_t)blk * 4 * NO);
+    for (int j = threadIdx.x; j < NO; j += blockDim.x) {
+        const double wn = (2 * j + 1) * pt, i1 = 1.0 / wn;
+        const double4 p = ld_stream4(&row[2 * j]), q = ld_stream4(&row[2 * j + 1]);
+        const double2 sv[4] = {make_double2(p.x, p.y), make_double2(p.z, p.w), make_double2(q.x, q.y),
+                               make_double2(q.z, q.w)};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (ww[c] == 0.0) continue;
+            double rS, iS;
+            sigma_full(i1, sinf, c2[c], c3[c], sv[c], rS, iS);
+            const double w8 = 0.5 * ww[c], x = e[c] - mu0;
+            const double tmp = w8 * T * 2 / (nk02 * (wn * wn + x * x));
+            acc[0] += tmp * (rS * (-x) + iS * wn);
+            acc[1] += w8 * sinf * T * 2 / (nk02 * (wn * wn + x * x));
+            if (j >= jc) moments(wn, rS, iS, e[c], ww[c]);
+        }
+    }
+    for (int t = threadIdx.x; t <= NO; t += blockDim.x) {
+        const double wn = (2 * (NO + t) + 1) * pt, i1 = 1.0 / wn, i2 = i1 * i1;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (ww[c] == 0.0) continue;
+            moments(wn, -c2[c] * i2 + c4[c] * i2 * i2, -sinf * i1 + c3[c] * i2 * i1, e[c], ww[c]);
+        }
+    }
+    // traceSelfG's Fermi-function term per octant point
+    if (threadIdx.x < 4) {
+        const int c = threadIdx.x;
+        const double w8 = 0.5 * ww[c];
+        if (w8 != 0.0) {
+            const double x = e[c] - mu0;
+            if (fabs(x) > 1.0e-12) {
+                acc[1] += w8 * sinf * (1.0 / (exp(x / T) + 1.0) - 0.5) / x / nk02;
+            } else {
+                const double ex = (x < 0) ? exp(x / T) : exp(-x / T);
+                acc[1] += -w8 * sinf * ex / ((ex + 1.0) * (ex + 1.0) * nk02 * T);
+            }
+        }
+    }
+    block_store<NV>(acc, partial);
+}
+
+struct MuRootArgs {
+    const double2 *S;
+    const double *s2, *s3, *s4, *sinf, *ek, *w16;
+    const double *mom;  // the k_sigma_moments results
+    int nw0, nblk, jc;
+    double mu0, T, nk02, dmax;
+    double *partial;  // [2][2 kRootMaxBlocks]
+    unsigned *bar;
+    int *err;
+    double *out;  // mu, evals, ok, Tr Sigma G at mu
+};
+
+// find_mu by safeguarded Newton (the host routine newton_root's steps) from
+// mu0 inside [-10, 10] with tolerance 1e-15, one barrier per evaluation as in
+// k_sumrule_roots; then green::traceSelfG2 (src/green.cpp:2929-2976) at mu.
+__global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
+    __shared__ RootCtl sc;
+    const int NO = a.nw0 / 2;
+    const double sinf = a.sinf[0];
+    const double pt = 3.141592653589793 * a.T;
+    int parity = 0;
+    if (threadIdx.x == 0) {
+        sc.lo = -10.0;
+        sc.hi = 10.0;
+        sc.x = (a.mu0 > sc.lo && a.mu0 < sc.hi) ? a.mu0 : 0.0;
+        sc.prev_step = 0.0;
+        sc.nev = sc.it = sc.done = sc.ok = 0;
+    }
+    __syncthreads();
+#pragma unroll 1
+    while (!sc.done) {
+        const double pmu = sc.x, delta = pmu - a.mu0;
+        const bool series = fabs(delta) <= a.dmax;
+        const int jhi = series ? a.jc : NO;
+        double v = 0.0, dv = 0.0;
+        const long long total = (long long)a.nblk * jhi;
+        for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < total;
+             it += (long long)gridDim.x * blockDim.x) {
+            const int blk = (int)(it / jhi), j = (int)(it - (long long)blk * jhi);
+            const int o0 = 4 * blk;
+            const double4 *row = reinterpret_cast<const double4 *>(a.S + (size_t)blk * 4 * NO);
+            const double4 p = ld_stream4(&row[2 * j]), q = ld_stream4(&row[2 * j + 1]);
+            const double2 sv[4] = {make_double2(p.x, p.y), make_double2(p.z, p.w), make_double2(q.x, q.y),
+                                   make_double2(q.z, q.w)};
+            const double wn = (2 * j + 1) * pt, i1 = 1.0 / wn;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const double w = __ldg(&a.w16[o0 + c]);
+                if (w == 0.0) continue;
+                double rS, iS;
+                sigma_full(i1, sinf, __ldg(&a.s2[o0 + c]), __ldg(&a.s3[o0 + c]), sv[c], rS, iS);
+                trdiff_term(wn, rS, iS, __ldg(&a.ek[o0 + c]), a.mu0, pmu, w, v, dv);
+            }
+        }
+        if (!series) {
+            // the tail Nw0/2 <= n <= Nw0 with the asymptotic Sigma, term by term
+            const long long ttot = (long long)a.nblk * 4 * (NO + 1);
+            for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < ttot;
+                 it += (long long)gridDim.x * blockDim.x) {
+                const int o = (int)(it / (NO + 1)), t = (int)(it - (long long)o * (NO + 1));
+                const double w = __ldg(&a.w16[o]);
+                if (w == 0.0) continue;
+                const double wn = (2 * (NO + t) + 1) * pt, i1 = 1.0 / wn, i2 = i1 * i1;
+                const double rS = -__ldg(&a.s2[o]) * i2 + __ldg(&a.s4[o]) * i2 * i2;
+                const double iS = -sinf * i1 + __ldg(&a.s3[o]) * i2 * i1;
+                trdiff_term(wn, rS, iS, __ldg(&a.ek[o]), a.mu0, pmu, w, v, dv);
+            }
+        }
+        double *part = a.partial + (size_t)parity * 2 * kRootMaxBlocks;
+        block_pair_sum(v, dv, part + 2 * blockIdx.x);
+        if (!grid_sync(a.bar, a.err)) return;
+        parity ^= 1;
+        if (threadIdx.x < 32) {
+            double pv = 0.0, pd = 0.0;
+            for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) {
+                pv += __ldcg(&part[2 * b]);
+                pd += __ldcg(&part[2 * b + 1]);
+            }
+            for (int off = 16; off > 0; off >>= 1) {
+                pv += __shfl_down_sync(0xffffffffu, pv, off);
+                pd += __shfl_down_sync(0xffffffffu, pd, off);
+            }
+            if (threadIdx.x == 0) {
+                if (series) {
+                    // Re sum_m (-delta)^m C_m - G0 and its delta derivative
+                    double sr = 0.0, dsr = 0.0, pr = 1.0, pm = 0.0;  // (-delta)^m, (-delta)^(m-1)
+                    for (int m = 0; m < kMuMomP; ++m) {
+                        sr += pr * a.mom[2 + 2 * m];
+                        if (m > 0) dsr += -m * pm * a.mom[2 + 2 * m];
+                        pm = pr;
+                        pr *= -delta;
+                    }
+                    pv += sr - a.mom[2 + 2 * kMuMomP];
+                    pd += dsr;
+                }
+                newton_update(sc, pv, pd, 1e-15);
+            }
+        }
+        __syncthreads();
+    }
+    if (!sc.ok) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            a.out[0] = sc.x;
+            a.out[1] = sc.nev;
+            a.out[2] = 0.0;
+            a.out[3] = 0.0;
+        }
+        return;
+    }
+    // Tr Sigma G at mu over the stored frequencies
+    const double mu = sc.root;
+    double v = 0.0, dummy = 0.0;
+    const long long total = (long long)a.nblk * NO;
+    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < total;
+         it += (long long)gridDim.x * blockDim.x) {
+        const int blk = (int)(it / NO), j = (int)(it - (long long)blk * NO);
+        const int o0 = 4 * blk;
+        const double4 *row = reinterpret_cast<const double4 *>(a.S + (size_t)blk * 4 * NO);
+        const double4 p = ld_stream4(&row[2 * j]), q = ld_stream4(&row[2 * j + 1]);
+        const double2 sv[4] = {make_double2(p.x, p.y), make_double2(p.z, p.w), make_double2(q.x, q.y),
+                               make_double2(q.z, q.w)};
+        const double wn = (2 * j + 1) * pt, i1 = 1.0 / wn;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double w8 = 0.5 * __ldg(&a.w16[o0 + c]);
+            if (w8 == 0.0) continue;
+            double rS, iS;
+            sigma_full(i1, sinf, __ldg(&a.s2[o0 + c]), __ldg(&a.s3[o0 + c]), sv[c], rS, iS);
+            const double ec = __ldg(&a.ek[o0 + c]);
+            const double aa = ec - mu + rS;
+            const double tmp = w8 * a.T * 2 / (a.nk02 * ((wn - iS) * (wn - iS) + aa * aa));
+            v += tmp * (iS * wn - iS * iS - (ec - mu) * rS - rS * rS);
+        }
+    }
+    double *part = a.partial + (size_t)parity * 2 * kRootMaxBlocks;
+    block_pair_sum(v, dummy, part + 2 * blockIdx.x);
+    if (!grid_sync(a.bar, a.err)) return;
+    if (blockIdx.x == 0 && threadIdx.x < 32) {
+        double pv = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) pv += __ldcg(&part[2 * b]);
+        for (int off = 16; off > 0; off >>= 1) pv += __shfl_down_sync(0xffffffffu, pv, off);
+        if (threadIdx.x == 0) {
+            a.out[0] = mu;
+            a.out[1] = sc.nev;
+            a.out[2] = 1.0;
+            a.out[3] = pv;
+        }
+    }
+}
+
+// the cooperative grid of the root searches: up to two blocks per SM
+template <typename K>
+cudaError_t root_grid(K kernel, int *grid) {
     int dev = 0, sms = 0, per = 0;
     cudaError_t e;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sumrule_roots, kRootThreads, 0)) != cudaSuccess)
-        return e;
-    const int grid = std::min(sms * std::max(1, std::min(per, 2)), kRootMaxBlocks);
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kRootThreads, 0)) != cudaSuccess) return e;
+    *grid = std::min(sms * std::max(1, std::min(per, 2)), kRootMaxBlocks);
+    return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t launch_sigma_moments(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                                 const double *s4, const double *sinf, double mu0, double T, int jc, Reduce r,
+                                 cudaStream_t st) {
+    const int nblk = g.n8p / 4;
+    const double nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
+    k_sigma_moments<<<nblk, 256, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.nw0, mu0, T, nk02, jc, r.partial);
+    cudaError_t e = launched();
+    if (e != cudaSuccess) return e;
+    return finish<kSigmaMomNV>(r, nblk, 0.0, st);
+}
+
+cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2, const double *s3, const double *s4,
+                            const double *sinf, const double *mom, double mu0, double T, int jc, double dmax,
+                            RootScratch rs, cudaStream_t st) {
+    int grid = 0;
+    cudaError_t e = root_grid(k_mu_roots, &grid);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(rs.bar, 0, 2 * sizeof(unsigned) + sizeof(int), st)) != cudaSuccess) return e;
+    MuRootArgs a;
+    a.S = S;
+    a.s2 = s2;
+    a.s3 = s3;
+    a.s4 = s4;
+    a.sinf = sinf;
+    a.ek = g.ek;
+    a.w16 = g.w16;
+    a.mom = mom;
+    a.nw0 = g.nw0;
+    a.nblk = g.n8p / 4;
+    a.jc = jc;
+    a.mu0 = mu0;
+    a.T = T;
+    a.nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
+    a.dmax = dmax;
+    a.partial = rs.partial;
+    a.bar = rs.bar;
+    a.err = reinterpret_cast<int *>(rs.bar + 2);
+    a.out = rs.out;
+    void *args[] = {&a};
+    e = cudaLaunchCooperativeKernel((const void *)k_mu_roots, dim3(grid), dim3(kRootThreads), args, 0, st);
+    if (e != cudaSuccess) return e;
+    return launched();
+}
+
+cudaError_t launch_sumrule_roots(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
+                                 const double *mom_suf, const double *cmax_suf, const double *tailm, double T,
+                                 double n, double nsr, double U, double hi_sp, RootScratch rs, cudaStream_t st) {
+    int grid = 0;
+    cudaError_t e = root_grid(k_sumrule_roots, &grid);
+    if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(rs.bar, 0, 2 * sizeof(unsigned) + sizeof(int), st)) != cudaSuccess) return e;
     SumRootArgs a;
     a.chiq = reinterpret_cast<const double4 *>(chiq);
@@ -307,7 +597,6 @@ cudaError_t launch_sumrule_roots(const GridDev &g, const double *chiq, const dou
     a.partial = rs.partial;
     a.bar = rs.bar;
     a.err = reinterpret_cast<int *>(rs.bar + 2);
-    a.ctl = reinterpret_cast<RootCtl *>(rs.ctl);
     a.out = rs.out;
     void *args[] = {&a};
     e = cudaLaunchCooperativeKernel((const void *)k_sumrule_roots, dim3(grid), dim3(kRootThreads), args, 0, st);
