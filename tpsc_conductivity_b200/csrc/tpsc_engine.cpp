@@ -285,6 +285,7 @@ struct Grid {
     double *s2 = nullptr, *s3 = nullptr, *s4 = nullptr, *sinf = nullptr;
     bool have_chi0 = false, have_V = false, have_S = false;
     bool g_mixed = false;         // G(r, tau) of the last chi0 stage is Grt32
+    long long model_id = -1;      // the model (tpsc_set_model call) the eps_k tables and mu0 belong to
     // Newton form: moments of chi0 for the high-frequency sum-rule series
     double *mom = nullptr, *cmax = nullptr;  // device [nb][kMomP], [nb]
     bool have_mom = false;
@@ -311,12 +312,15 @@ struct tpsc_ctx {
     int device = 0;
     int form = TPSC_FORM_REFERENCE;
     cudaStream_t st = nullptr;
+    cudaStream_t st2 = nullptr;   // side stream: the single-CTA boundary transforms, overlapped with the slices
+    cudaEvent_t evf[4] = {};      // fork / join events of the side stream
     Reduce red;
     Reduce redm;              // moment sums: partial [(2 kMomP + 1) kMaxBlocks], result [32]
     RootScratch roots;        // the device root searches' state
     double *h_res = nullptr;  // pinned, 32 doubles
     // model
     bool have_model = false;
+    long long model_id = 0;   // incremented by every tpsc_set_model
     int nk0 = 0, Nw0 = 0;
     double n = 0, T = 0, tp = 0, tpp = 0, t3 = 0, U = 0, nsr = 0;
     double Usp = 0, Uch = 0;
@@ -609,12 +613,20 @@ int grid_set_model(tpsc_ctx *ctx, Grid *g) {
     return TPSC_OK;
 }
 
+// Make (nk0, nw0) the current grid with the model's eps_k tables and mu0;
+// those are computed once per model and grid, as the reference computes them
+// once in its constructors (src/hamiltonien.cpp:328-394, src/green0.cpp:18-23),
+// not by every solve.
 int switch_grid(tpsc_ctx *ctx, int nk0, int nw0) {
     Grid *g = nullptr;
     int rc = build_grid(ctx, nk0, nw0, &g);
     if (rc) return rc;
-    rc = grid_set_model(ctx, g);
-    if (rc) return rc;
+    if (g->model_id != ctx->model_id) {
+        rc = grid_set_model(ctx, g);
+        if (rc) return rc;
+        g->model_id = ctx->model_id;
+    }
+    g->have_chi0 = g->have_V = g->have_S = g->have_mom = false;
     ctx->cur = g;
     ctx->scal[TPSC_S_MU0] = g->mu0;
     return TPSC_OK;
@@ -628,26 +640,45 @@ int need_model(tpsc_ctx *ctx) {
 
 bool mixed(const tpsc_ctx *ctx) { return (ctx->form & TPSC_FORM_MIXED) != 0; }
 
+// The side stream st2 takes over after everything queued on st so far
+// (fork), and st waits for what st2 queued (join).
+int fork_side(tpsc_ctx *ctx, int k) {
+    CK(cudaEventRecord(ctx->evf[2 * k], ctx->st));
+    CK(cudaStreamWaitEvent(ctx->st2, ctx->evf[2 * k], 0));
+    return TPSC_OK;
+}
+int join_side(tpsc_ctx *ctx, int k) {
+    CK(cudaEventRecord(ctx->evf[2 * k + 1], ctx->st2));
+    CK(cudaStreamWaitEvent(ctx->st, ctx->evf[2 * k + 1], 0));
+    return TPSC_OK;
+}
+
 int run_chi0(tpsc_ctx *ctx) {
     Grid *g = ctx->cur;
     const GridDev &d = g->d;
+    int rc;
+    // the chi0 boundary (one CTA: G(r, 0) -> d/dtau chi0) runs beside the
+    // chi0 slices; both need only G(r, tau)
     if (mixed(ctx)) {
         if (!g->Grt32) CK(dalloc(g, &g->Grt32, (size_t)(d.nw0 + 1) * d.n8));
         CK(launch_gslice32(d, g->Grt32, g->mu0, ctx->T, ctx->st));
+        if ((rc = fork_side(ctx, 0))) return rc;
         CK(launch_chi0_boundary(d, (const float *)g->Grt32, g->mu0, ctx->T, g->dG0p, g->dchirt0, g->dchiqt0,
-                                ctx->st));
+                                ctx->st2));
         CK(launch_chi0_slice32(d, g->Grt32, g->chirt, g->chiq, ctx->st));
     } else {
         CK(launch_gslice(d, g->Grt, g->mu0, ctx->T, ctx->st));
+        if ((rc = fork_side(ctx, 0))) return rc;
         CK(launch_chi0_boundary(d, (const double *)g->Grt, g->mu0, ctx->T, g->dG0p, g->dchirt0, g->dchiqt0,
-                                ctx->st));
+                                ctx->st2));
         CK(launch_chi0_slice(d, g->Grt, g->chirt, g->chiq, ctx->st));
     }
+    if ((rc = join_side(ctx, 0))) return rc;
     g->g_mixed = mixed(ctx);
     CK(launch_chi0_tau(d, g->chiq, g->dchiqt0, g->cinf, g->cinf2, ctx->T, ctx->st));
     CK(launch_chi0max(d, g->chiq, ctx->red, ctx->st));
     double r[3];
-    int rc = read_result(ctx, 3, r);
+    rc = read_result(ctx, 3, r);
     if (rc) return rc;
     ctx->scal[TPSC_S_CHI0MAX] = r[0];
     ctx->scal[TPSC_S_QMAX0] = r[1];
@@ -853,16 +884,20 @@ int run_self(tpsc_ctx *ctx) {
     if (!g || !g->have_V) return fail(ctx, TPSC_ERR_STATE, "the vertex V(r, tau) has not been computed");
     const double fact = ctx->U * (3.0 * ctx->Usp + ctx->Uch) / 8.0;
     const GridDev &d = g->d;
-    // G(r, tau) as the chi0 stage left it (FP32 in the mixed form)
+    // G(r, tau) as the chi0 stage left it (FP32 in the mixed form); the two
+    // boundary CTAs run beside the Sigma slices
+    int rc = fork_side(ctx, 1);
+    if (rc) return rc;
     if (g->g_mixed) {
         CK(launch_sigma_boundary(d, (const float *)g->Grt32, g->V, g->dchirt0, g->dG0p, g->mu0, fact, g->dS,
-                                 ctx->st));
+                                 ctx->st2));
         CK(launch_sigma_slice(d, (const float *)g->Grt32, g->V, g->sigt, ctx->st));
     } else {
         CK(launch_sigma_boundary(d, (const double *)g->Grt, g->V, g->dchirt0, g->dG0p, g->mu0, fact, g->dS,
-                                 ctx->st));
+                                 ctx->st2));
         CK(launch_sigma_slice(d, (const double *)g->Grt, g->V, g->sigt, ctx->st));
     }
+    if ((rc = join_side(ctx, 1))) return rc;
     CK(launch_sigma_tau(d, g->sigt, g->dS, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->T, ctx->st));
     CK(cudaMemcpyAsync(ctx->h_res, g->sinf, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
@@ -1133,6 +1168,9 @@ tpsc_ctx *tpsc_create(int device, int *status) {
     };
     if ((e = cudaSetDevice(device)) != cudaSuccess) return bad(e);
     if ((e = cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking)) != cudaSuccess) return bad(e);
+    if ((e = cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking)) != cudaSuccess) return bad(e);
+    for (auto &ev : ctx->evf)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return bad(e);
     if ((e = cudaMalloc(&ctx->red.partial, 4 * kMaxBlocks * sizeof(double))) != cudaSuccess) return bad(e);
     if ((e = cudaMalloc(&ctx->red.result, 8 * sizeof(double))) != cudaSuccess) return bad(e);
     if ((e = cudaMalloc(&ctx->red.ticket, sizeof(unsigned))) != cudaSuccess) return bad(e);
@@ -1168,6 +1206,9 @@ void tpsc_destroy(tpsc_ctx *ctx) {
     if (ctx->stage) cudaFree(ctx->stage);
     for (auto &ev : ctx->ev)
         if (ev) cudaEventDestroy(ev);
+    for (auto &ev : ctx->evf)
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->st2) cudaStreamDestroy(ctx->st2);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
 }
@@ -1196,6 +1237,7 @@ int tpsc_set_model(tpsc_ctx *ctx, int nk0, int Nw0, double n, double T, double t
     for (double &s : ctx->scal) s = 0.0;
     for (auto &kv : ctx->grids) kv.second->have_chi0 = kv.second->have_V = kv.second->have_S = false;
     ctx->have_model = true;
+    ++ctx->model_id;
     return switch_grid(ctx, nk0, Nw0);
 }
 

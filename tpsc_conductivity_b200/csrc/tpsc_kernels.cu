@@ -227,7 +227,8 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
 }
 
 // d/dtau Sigma(k, 0) and d/dtau Sigma(k, beta): the spline end conditions of
-// the self-energy (src/green.cpp:1743-1817).  One CTA, two 2D DCT-I.
+// the self-energy (src/green.cpp:1743-1817).  Two CTAs, one 2D DCT-I each
+// (blockIdx.x = 0: tau = 0, 1: tau = beta).
 template <int NBK, class GT>
 __global__ void __launch_bounds__(kSliceThreads, 1)
     k_sigma_boundary(const double *__restrict__ er, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
@@ -237,8 +238,8 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     extern __shared__ __align__(16) double S[];
     const double2 *tws = slice_twiddles<NBK>(S, tw);
     const int nb = nw0 / 2 + 1;
-#pragma unroll 1
-    for (int side = 0; side < 2; ++side) {
+    {
+        const int side = blockIdx.x;
         const GT *g = Grt + (side == 0 ? 0 : (size_t)nw0 * n8);
         for (int o = threadIdx.x; o < n8; o += blockDim.x) {
             int l, m;
@@ -1498,7 +1499,7 @@ struct RunSigmaBoundary {
         const size_t sm = SliceSmem<NBK>::bytes;
         cudaError_t e = set_smem(k_sigma_boundary<NBK, GT>, sm);
         if (e != cudaSuccess) return e;
-        k_sigma_boundary<NBK, GT><<<1, kSliceThreads, sm, st>>>(g->er, g->lm, g->tw_k, Grt, V, dchirt0, dG0p, g->n8,
+        k_sigma_boundary<NBK, GT><<<2, kSliceThreads, sm, st>>>(g->er, g->lm, g->tw_k, Grt, V, dchirt0, dG0p, g->n8,
                                                                  g->nw0, g->n8p, mu0, fact, dS);
         return launched();
     }
