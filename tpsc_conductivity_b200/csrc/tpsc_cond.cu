@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
                  double *__restrict__ pre) {
     constexpr int K4 = (NBK - 2) * NBK;
     extern __shared__ __align__(16) double S[];
-    const double2 *tws = slice_twiddles<NBK>(S, tw);
+    const auto *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x, y = blockIdx.y;
     const int nb = nw0 / 2 + 1;
     const double t = j / (nw0 * T);
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
                     int nw0, int K4p, double mu0, double T, double nf, double fact, double *__restrict__ dbound) {
     constexpr int K4 = (NBK - 2) * NBK;
     extern __shared__ __align__(16) double S[];
-    const double2 *tws = slice_twiddles<NBK>(S, tw);
+    const auto *tws = slice_twiddles<NBK>(S, tw);
     const int kind = blockIdx.x;
     const int nb = nw0 / 2 + 1;
     for (int c = threadIdx.x; c < K4; c += blockDim.x) {

@@ -116,10 +116,10 @@ struct SliceSmem {
     static constexpr size_t slice_bytes = (size_t)NBK * NBK * sizeof(double);
     static constexpr size_t scr_off = (slice_bytes + 15) & ~(size_t)15;
     static constexpr size_t tw_off = scr_off + (size_t)NGRP * padded_len(L) * sizeof(double2);
-    // the twiddles stay in global memory (read through L1) when shared memory
-    // is full: the slice and the groups' FFT scratch come first
+    // the full L-point twiddle table when it fits behind the slice and the
+    // groups' FFT scratch, else the two-level table (2 KB)
     static constexpr bool smem_tw = tw_off + (size_t)L * sizeof(double2) <= 232448;
-    static constexpr size_t bytes = tw_off + (smem_tw ? (size_t)L * sizeof(double2) : 0);
+    static constexpr size_t bytes = tw_off + (smem_tw ? (size_t)L * sizeof(double2) : sizeof(TwoLevelTw));
     static_assert(bytes <= 232448, "slice does not fit in shared memory");
 };
 
@@ -128,14 +128,55 @@ __device__ __forceinline__ double2 *slice_scratch(double *S) {
     return reinterpret_cast<double2 *>(reinterpret_cast<char *>(S) + SliceSmem<NBK>::scr_off);
 }
 
-// the L-point twiddle table staged in shared memory behind the FFT scratch
-// (the first __syncthreads of the kernel publishes it), or the global table
+// The L-point twiddles exp(-2 pi i m / L) staged in shared memory behind the
+// FFT scratch -- the full table, or where that does not fit the two-level
+// table (entry m = hi[m >> 6] lo[m & 63]); the first __syncthreads of the
+// kernel publishes it.
 template <int NBK>
-__device__ __forceinline__ const double2 *slice_twiddles(double *S, const double2 *__restrict__ tw) {
-    if constexpr (!SliceSmem<NBK>::smem_tw) return tw;
-    double2 *t = reinterpret_cast<double2 *>(reinterpret_cast<char *>(S) + SliceSmem<NBK>::tw_off);
-    for (int i = threadIdx.x; i < SliceSmem<NBK>::L; i += blockDim.x) t[i] = __ldg(&tw[i]);
-    return t;
+__device__ __forceinline__ auto slice_twiddles(double *S, const double2 *__restrict__ tw) {
+    constexpr int L = SliceSmem<NBK>::L;
+    char *base = reinterpret_cast<char *>(S) + SliceSmem<NBK>::tw_off;
+    if constexpr (SliceSmem<NBK>::smem_tw) {
+        double2 *t = reinterpret_cast<double2 *>(base);
+        for (int i = threadIdx.x; i < L; i += blockDim.x) t[i] = __ldg(&tw[i]);
+        return (const double2 *)t;
+    } else {
+        TwoLevelTw *t = reinterpret_cast<TwoLevelTw *>(base);
+        for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+            t->hi[i] = 64 * i < L ? __ldg(&tw[64 * i]) : make_double2(1.0, 0.0);
+            t->lo[i] = i < L ? __ldg(&tw[i]) : make_double2(1.0, 0.0);
+        }
+        return (const TwoLevelTw *)t;
+    }
+}
+
+// Fill a symmetric NBK x NBK slice from the octant points: value(o) does all
+// global reads of point o and returns its value.  Each thread takes KB points
+// at a time and issues all their reads before storing any of them, so that
+// KB memory round trips overlap instead of running one after the other.
+template <int NBK, int KB = 8, class T, class Value>
+__device__ __forceinline__ void fill_octant(T *S, const uint32_t *__restrict__ lm, int n8, const Value &value) {
+    for (int base = threadIdx.x; base < n8; base += KB * blockDim.x) {
+        T v[KB];
+        uint32_t p[KB];
+#pragma unroll
+        for (int b = 0; b < KB; ++b) {
+            const int o = base + b * blockDim.x;
+            if (o < n8) {
+                p[b] = __ldg(&lm[o]);
+                v[b] = value(o);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < KB; ++b) {
+            const int o = base + b * blockDim.x;
+            if (o < n8) {
+                const int l = (int)(p[b] >> 16), m = (int)(p[b] & 0xffffu);
+                S[l * NBK + m] = v[b];
+                S[m * NBK + l] = v[b];
+            }
+        }
+    }
 }
 
 // write octant value v of point (l, m) into both triangles of the slice

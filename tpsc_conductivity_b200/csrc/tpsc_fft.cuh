@@ -358,8 +358,8 @@ __device__ void dct2_slice(T *S, C *scr, const TW *tw) {
 // extension of two packed lines, the DST through the odd extension
 // z = [0, X, 0, -reverse(X)], whose transform is -i Y_a + Y_b for the packed
 // pair a + i b.  Same calling rules as dct2_slice.
-template <int NBK>
-__device__ void dst_dct_slice(double *S, double2 *scr, const double2 *tw) {
+template <int NBK, class TW>
+__device__ void dst_dct_slice(double *S, double2 *scr, const TW *tw) {
     constexpr int L = 2 * (NBK - 1);
     constexpr int NR = NBK - 2;
     constexpr int G = FftPlan<L>::G;

@@ -90,18 +90,14 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     k_gslice(const double2 *__restrict__ gk, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
              int n8, int nw0, double T, double *__restrict__ Grt) {
     extern __shared__ __align__(16) double S[];
-    const double2 *tws = slice_twiddles<NBK>(S, tw);
+    const auto *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
     const double t = j / (nw0 * T);
     const double bt = 1.0 / T - t;
-#pragma unroll 4
-    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
-        int l, m;
-        oct_lm(lm, o, l, m);
+    fill_octant<NBK>(S, lm, n8, [&](int o) -> double {
         const double2 c = __ldg(&gk[o]);
-        const double g = c.y * exp((c.x > 0 ? -t : bt) * c.x);
-        put_sym<NBK>(S, l, m, g);
-    }
+        return c.y * exp((c.x > 0 ? -t : bt) * c.x);
+    });
     __syncthreads();
     dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     double *out = Grt + (size_t)j * n8;
@@ -120,14 +116,12 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     k_chi0_slice(const double *__restrict__ Grt, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
                  int n8, int nw0, double *__restrict__ chirt, double *__restrict__ chiq) {
     extern __shared__ __align__(16) double S[];
-    const double2 *tws = slice_twiddles<NBK>(S, tw);
+    const auto *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
     const int nb = nw0 / 2 + 1;
     const double *gp = Grt + (size_t)j * n8;
     const double *gm = Grt + (size_t)(nw0 - j) * n8;
-    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
-        int l, m;
-        oct_lm(lm, o, l, m);
+    fill_octant<NBK>(S, lm, n8, [&](int o) -> double {
         const double a = gp[o];
         double c;
         if (j == 0)
@@ -137,8 +131,8 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
         else
             c = -2.0 * (-gm[o]) * a;
         chirt[bidx(j, o, nb)] = c;
-        put_sym<NBK>(S, l, m, c);
-    }
+        return c;
+    });
     __syncthreads();
     dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
@@ -157,7 +151,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
                     double nk02, double *__restrict__ dG0p, double *__restrict__ dtau_chirt0,
                     double *__restrict__ dtau_chiqt0) {
     extern __shared__ __align__(16) double S[];
-    const double2 *tws = slice_twiddles<NBK>(S, tw);
+    const auto *tws = slice_twiddles<NBK>(S, tw);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
         oct_lm(lm, o, l, m);
@@ -207,16 +201,14 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     k_vertex_q(const double *__restrict__ chiq, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
                int n8, int nb, double normFact, double U, double Usp, double Uch, double *__restrict__ Vr) {
     extern __shared__ __align__(16) double S[];
-    const double2 *tws = slice_twiddles<NBK>(S, tw);
+    const auto *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
-    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
-        int l, m;
-        oct_lm(lm, o, l, m);
+    fill_octant<NBK>(S, lm, n8, [&](int o) -> double {
         const double c0 = chiq[bidx(j, o, nb)];
         const double sp = c0 / (1.0 - Usp * c0 / 2.0);
         const double ch = c0 / (1.0 + Uch * c0 / 2.0);
-        put_sym<NBK>(S, l, m, normFact * U * (3.0 * Usp * (sp - c0) + Uch * (ch - c0)) / 8.0);
-    }
+        return normFact * U * (3.0 * Usp * (sp - c0) + Uch * (ch - c0)) / 8.0;
+    });
     __syncthreads();
     dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
@@ -236,7 +228,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
                      const double *__restrict__ dG0p, int n8, int nw0, int n8p, double mu0, double fact,
                      double *__restrict__ dS) {
     extern __shared__ __align__(16) double S[];
-    const double2 *tws = slice_twiddles<NBK>(S, tw);
+    const auto *tws = slice_twiddles<NBK>(S, tw);
     const int nb = nw0 / 2 + 1;
     {
         const int side = blockIdx.x;
@@ -274,16 +266,12 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     k_sigma_slice(const GT *__restrict__ Grt, const double *__restrict__ V, const uint32_t *__restrict__ lm,
                   const double2 *__restrict__ tw, int n8, int nw0, double *__restrict__ sigt) {
     extern __shared__ __align__(16) double S[];
-    const double2 *tws = slice_twiddles<NBK>(S, tw);
+    const auto *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
     const int nb = nw0 / 2 + 1;
     const int jv = j < nb ? j : nw0 - j;
     const GT *g = Grt + (size_t)j * n8;
-    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
-        int l, m;
-        oct_lm(lm, o, l, m);
-        put_sym<NBK>(S, l, m, (double)g[o] * V[bidx(jv, o, nb)]);
-    }
+    fill_octant<NBK>(S, lm, n8, [&](int o) -> double { return (double)g[o] * V[bidx(jv, o, nb)]; });
     __syncthreads();
     dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {

@@ -48,12 +48,6 @@ __device__ __forceinline__ const float4 *twiddles32(float *S, const float4 *__re
     return t;
 }
 
-template <int NBK>
-__device__ __forceinline__ void put_sym32(float *S, int l, int m, float v) {
-    S[l * NBK + m] = v;
-    S[m * NBK + l] = v;
-}
-
 // G(r, tau_j) = DCT-I[ G0(k, tau_j) / L^2 ] in FP32 (the FP64 k_gslice's
 // stage, src/green.cpp:1830-1841 and src/chi0.cpp:462-495): G0 formed in
 // FP64, rounded once to float; Grt32[j * n8 + o].
@@ -66,13 +60,10 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
     const int j = blockIdx.x;
     const double t = j / (nw0 * T);
     const double bt = 1.0 / T - t;
-#pragma unroll 4
-    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
-        int l, m;
-        oct_lm(lm, o, l, m);
+    fill_octant<NBK>(S32, lm, n8, [&](int o) -> float {
         const double2 c = __ldg(&gk[o]);
-        put_sym32<NBK>(S32, l, m, (float)(c.y * exp((c.x > 0 ? -t : bt) * c.x)));
-    }
+        return (float)(c.y * exp((c.x > 0 ? -t : bt) * c.x));
+    });
     __syncthreads();
     dct2_slice<NBK>(S32, scratch32<NBK>(S32), tws);
     float *out = Grt + (size_t)j * n8;
@@ -96,9 +87,7 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
     const int nb = nw0 / 2 + 1;
     const float *gp = Grt + (size_t)j * n8;
     const float *gm = Grt + (size_t)(nw0 - j) * n8;
-    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
-        int l, m;
-        oct_lm(lm, o, l, m);
+    fill_octant<NBK>(S32, lm, n8, [&](int o) -> float {
         const double a = gp[o];
         double c;
         if (j == 0)
@@ -108,8 +97,8 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
         else
             c = -2.0 * (-(double)gm[o]) * a;
         chirt[bidx(j, o, nb)] = c;
-        put_sym32<NBK>(S32, l, m, (float)c);
-    }
+        return (float)c;
+    });
     __syncthreads();
     dct2_slice<NBK>(S32, scratch32<NBK>(S32), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
@@ -128,14 +117,12 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
     extern __shared__ __align__(16) float S32[];
     const float4 *tws = twiddles32<NBK>(S32, tw);
     const int j = blockIdx.x;
-    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
-        int l, m;
-        oct_lm(lm, o, l, m);
+    fill_octant<NBK>(S32, lm, n8, [&](int o) -> float {
         const double c0 = chiq[bidx(j, o, nb)];
         const double sp = c0 / (1.0 - Usp * c0 / 2.0);
         const double ch = c0 / (1.0 + Uch * c0 / 2.0);
-        put_sym32<NBK>(S32, l, m, (float)(normFact * U * (3.0 * Usp * (sp - c0) + Uch * (ch - c0)) / 8.0));
-    }
+        return (float)(normFact * U * (3.0 * Usp * (sp - c0) + Uch * (ch - c0)) / 8.0);
+    });
     __syncthreads();
     dct2_slice<NBK>(S32, scratch32<NBK>(S32), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
