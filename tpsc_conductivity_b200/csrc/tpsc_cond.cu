@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(CondTauSmem<N>::threads, 1) k_cond_tau(const C
     __shared__ ColState cs[2];
     __shared__ double d0s[2], dNs[2], sums[8], sV[2], sM[2];
     const int tid = threadIdx.x, NT = blockDim.x;
-    const double T = a.T, h = 1.0 / (N * T), beta = 1.0 / T, pT = kPi * T;
+    const double T = a.T, h = 1.0 / (N * T), ih = 1.0 / h, beta = 1.0 / T, pT = kPi * T;
     const double sinf = a.sinf[0], mu = a.mu, nf = a.nf;
     const int PWB = 2 * NJ2;
     double *part = a.partial + (size_t)blockIdx.x * a.pw;
@@ -355,7 +355,7 @@ __global__ void __launch_bounds__(CondTauSmem<N>::threads, 1) k_cond_tau(const C
         if (tid < G) {
             const double *Ma = R, *Mb = R + NJ;
             auto in = [&](int j) -> double2 {
-                return cmul(tw_at(ht2, j), make_double2((Ma[j + 1] - Ma[j]) / h, (Mb[j + 1] - Mb[j]) / h));
+                return cmul(tw_at(ht2, j), make_double2((Ma[j + 1] - Ma[j]) * ih, (Mb[j + 1] - Mb[j]) * ih));
             };
             group_fft_io<N, +1>(X1, tid, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X1});
         }
@@ -558,7 +558,7 @@ __global__ void __launch_bounds__(CondTauSmem<N>::threads, 1) k_cond_tau(const C
         if (tid < G) {
             const double *Ma = R, *Mb = R + NJ;
             auto in = [&](int j) -> double2 {
-                return make_double2((Ma[j + 1] - Ma[j]) / h, (Mb[j + 1] - Mb[j]) / h);
+                return make_double2((Ma[j + 1] - Ma[j]) * ih, (Mb[j + 1] - Mb[j]) * ih);
             };
             group_fft_io<N, -1>(X1, tid, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X1});
         }
@@ -617,7 +617,7 @@ __global__ void __launch_bounds__(CondTauSmem<N>::threads, 1) k_cond_tau(const C
                 const bool lo = j < NO;
                 const int jj = lo ? j : N - 1 - j;
                 const double sg = lo ? 1.0 : -1.0;
-                return make_double2(sg * (Ma[jj + 1] - Ma[jj]) / h, sg * (Mb[jj + 1] - Mb[jj]) / h);
+                return make_double2(sg * (Ma[jj + 1] - Ma[jj]) * ih, sg * (Mb[jj + 1] - Mb[jj]) * ih);
             };
             group_fft_io<N, -1>(X1, tid, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X1});
         }

@@ -19,12 +19,18 @@ namespace {
 constexpr double kPi = 3.141592653589793;  // == acos(-1.0) in double
 constexpr int kSliceThreads = 352;  // 22 groups of 16: the 65 line pairs of a 129-point pass in 3 rounds
 constexpr int kTauThreads = 256;
-constexpr int kWarm = 40;  // spline sweep warm-up: carry error <= 0.268^40
+constexpr int kWarm = 30;  // spline sweep warm-up: carry error <= 0.268^30 < 1e-17
 
-__device__ __forceinline__ void oct_lm(const uint32_t *lm, int o, int &l, int &m) {
-    const uint32_t v = __ldg(&lm[o]);
-    l = (int)(v >> 16);
-    m = (int)(v & 0xffffu);
+// octant index o = m + l (l + 1) / 2, 0 <= m <= l -> (l, m) without a
+// table: 8 o + 1 < 2^24 is exact in float and its square root correctly
+// rounded, so the estimate of l is off by at most one and the two checks
+// correct it
+__device__ __forceinline__ void oct_lm(int o, int &l, int &m) {
+    int a = (int)((sqrtf((float)(8 * o + 1)) - 1.0f) * 0.5f);
+    if ((a + 1) * (a + 2) / 2 <= o) ++a;
+    if (a * (a + 1) / 2 > o) --a;
+    l = a;
+    m = o - a * (a + 1) / 2;
 }
 
 // integer multiplicity weight of octant point (l, m) as in the reference
@@ -155,23 +161,20 @@ __device__ __forceinline__ auto slice_twiddles(double *S, const double2 *__restr
 // at a time and issues all their reads before storing any of them, so that
 // KB memory round trips overlap instead of running one after the other.
 template <int NBK, int KB = 8, class T, class Value>
-__device__ __forceinline__ void fill_octant(T *S, const uint32_t *__restrict__ lm, int n8, const Value &value) {
+__device__ __forceinline__ void fill_octant(T *S, int n8, const Value &value) {
     for (int base = threadIdx.x; base < n8; base += KB * blockDim.x) {
         T v[KB];
-        uint32_t p[KB];
 #pragma unroll
         for (int b = 0; b < KB; ++b) {
             const int o = base + b * blockDim.x;
-            if (o < n8) {
-                p[b] = __ldg(&lm[o]);
-                v[b] = value(o);
-            }
+            if (o < n8) v[b] = value(o);
         }
 #pragma unroll
         for (int b = 0; b < KB; ++b) {
             const int o = base + b * blockDim.x;
             if (o < n8) {
-                const int l = (int)(p[b] >> 16), m = (int)(p[b] & 0xffffu);
+                int l, m;
+                oct_lm(o, l, m);
                 S[l * NBK + m] = v[b];
                 S[m * NBK + l] = v[b];
             }
@@ -199,7 +202,7 @@ __device__ __forceinline__ void put_sym(double *S, int l, int m, double v) {
 // Thomas algorithm with pivots invp = 1/p_i and multipliers cp_i (cp_N = 0)
 // precomputed on the host.  The sweeps are split over TPC threads per column:
 // each chunk starts its carry kWarm rows early from zero; the carry decays
-// by 1/p_i <= 1/(2+sqrt3) per row, so the truncation error is below 1e-22 of
+// by 1/p_i <= 1/(2+sqrt3) per row, so the truncation error is below 1e-17 of
 // the local magnitude.  All threads of the block must call.
 template <int NC = 4>
 __device__ void spline_second_derivatives(double *A, int lda, int NJ, double h, const double *d0, const double *dN,
@@ -210,11 +213,11 @@ __device__ void spline_second_derivatives(double *A, int lda, int NJ, double h, 
     const int C = (NJ + TPC - 1) / TPC;
     const int s = min(k * C, NJ), e = min(s + C, NJ);
     const int N = NJ - 1;
-    const double a6 = 6.0 / (h * h), b6 = 6.0 / h;
+    const double a6 = 6.0 / (h * h), b6 = 6.0 / h, ih = 1.0 / h;
     const double dl = d0[c], dr = dN[c];
     auto rhs = [&](int i, double vm, double v0, double vp) -> double {
-        if (i == 0) return b6 * ((vp - v0) / h - dl);
-        if (i == N) return b6 * (dr - (v0 - vm) / h);
+        if (i == 0) return b6 * ((vp - v0) * ih - dl);
+        if (i == N) return b6 * (dr - (v0 - vm) * ih);
         return a6 * (vp - 2.0 * v0 + vm);
     };
     double carry = 0.0, vm_h = 0.0, vs_h = 0.0, ve_h = 0.0;
@@ -266,20 +269,45 @@ __device__ void spline_second_derivatives(double *A, int lda, int NJ, double h, 
     __syncthreads();
 }
 
-// per-column sum of y[i0..i1) over the TPC threads of each column -> out[c]
+// error-free sum of two doubles (Knuth's TwoSum): a + b = s + e exactly
+__device__ __forceinline__ void two_sum(double a, double b, double &s, double &e) {
+    s = a + b;
+    const double bp = s - a;
+    e = (a - (s - bp)) + (b - bp);
+}
+
+// per-column sum of y[i0..i1) over the TPC threads of each column -> out[c]:
+// compensated per-thread sums, then a fixed shuffle tree that adds the pairs
+// (sum, compensation) with TwoSum, then the column's warps in order.  TPC is
+// a multiple of 32 (blockDim.x = 32 NC k).
 template <int NC = 4>
 __device__ void column_sums(const double *A, int lda, int i0, int i1, double *out) {
     const int TPC = blockDim.x / NC;
     const int c = threadIdx.x / TPC, k = threadIdx.x % TPC;
     KSum acc;
     for (int i = i0 + k; i < i1; i += TPC) acc.add(A[c * lda + i]);
-    __shared__ double part[1024];
-    part[threadIdx.x] = acc.value();
+    double s = acc.s, e = acc.c;
+    for (int off = 16; off > 0; off >>= 1) {
+        const double s2 = __shfl_down_sync(0xffffffffu, s, off);
+        const double e2 = __shfl_down_sync(0xffffffffu, e, off);
+        double t, r;
+        two_sum(s, s2, t, r);
+        s = t;
+        e += e2 + r;
+    }
+    __shared__ double2 part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = make_double2(s, e);
     __syncthreads();
     if (k == 0) {
-        KSum s;
-        for (int q = 0; q < TPC; ++q) s.add(part[c * TPC + q]);
-        out[c] = s.value();
+        const int w0 = threadIdx.x >> 5, nw = TPC >> 5;
+        double S = part[w0].x, E = part[w0].y;
+        for (int q = 1; q < nw; ++q) {
+            double t, r;
+            two_sum(S, part[w0 + q].x, t, r);
+            S = t;
+            E += part[w0 + q].y + r;
+        }
+        out[c] = S + E;
     }
     __syncthreads();
 }

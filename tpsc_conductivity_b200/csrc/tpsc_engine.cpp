@@ -289,11 +289,12 @@ struct Grid {
     // Newton form: moments of chi0 for the high-frequency sum-rule series
     double *mom = nullptr, *cmax = nullptr;  // device [nb][kMomP], [nb]
     bool have_mom = false;
-    std::vector<long double> mom_suf;        // [(nb + 1) kMomP] sums over frequencies >= j
+    bool have_mom_host = false;              // the host copies below are current
+    std::vector<double> mom_suf;             // [(nb + 1) kMomP] sums over frequencies >= j
     std::vector<double> cmax_suf;            // [nb + 1] max |chi| over frequencies >= j
-    long double tail_mom[kMomP] = {0};       // the same moments of the Matsubara tail n > Nw0/2
+    double tail_mom[kMomP] = {0};            // the same moments of the Matsubara tail n > Nw0/2
     double tail_max = 0.0;                   // max |chi| over the tail
-    double *d_mom_suf = nullptr, *d_cmax_suf = nullptr, *d_tailm = nullptr;  // device copies (FP64)
+    double *d_mom_suf = nullptr, *d_cmax_suf = nullptr, *d_tailm = nullptr;  // on the device
     double tailq_T = -1.0;         // temperature the tail power sums were built for
     double tailq_host[kTailQ] = {0};
     std::vector<void *> allocs;
@@ -461,11 +462,9 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
     d.n8p = (d.n8 + 3) & ~3;
     d.nw0 = nw0;
     d.nb = nw0 / 2 + 1;
-    std::vector<uint32_t> lm(d.n8);
     std::vector<double> w16(d.n8p, 0.0);
     for (int l = 0; l < d.nbk; ++l)
         for (int m = 0; m <= l; ++m) {
-            lm[m + l * (l + 1) / 2] = ((uint32_t)l << 16) | (uint32_t)m;
             // multiplicity of octant point (l, m): 16 halved on the l edges, the m
             // edges and the diagonal (src/chi.cpp:755-759)
             int w = 16;
@@ -489,7 +488,6 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
     if (e == cudaSuccess) {                        \
         e = (x);                                   \
     }
-    A(upload(g, &d.lm, lm));
     A(upload(g, &d.w16, w16));
     A(upload(g, &d.tw_k, twk));
     A(upload(g, &d.tw_k32, twk32));
@@ -689,40 +687,40 @@ int run_chi0(tpsc_ctx *ctx) {
     return TPSC_OK;
 }
 
-// Per-frequency moments of chi0 and their sums over the frequencies >= j
-// (long double), for the high-frequency series of the Newton-form sum rule.
+// Per-frequency moments of chi0, their sums over the frequencies >= j and the
+// tail moments, for the high-frequency series of the Newton-form sum rule:
+// formed on the device (tpsc_kernels.cu), queued on the stream without a host
+// round trip.
 int ensure_moments(tpsc_ctx *ctx, Grid *g) {
     if (g->have_mom) return TPSC_OK;
     const GridDev &d = g->d;
-    const int nb = d.nb;
     CK(launch_chi0_moments(d, g->chiq, g->mom, g->cmax, ctx->st));
-    std::vector<double> m((size_t)nb * kMomP), c(nb);
-    CK(cudaMemcpyAsync(m.data(), g->mom, m.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaMemcpyAsync(c.data(), g->cmax, c.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    g->mom_suf.assign((size_t)(nb + 1) * kMomP, 0.0L);
-    g->cmax_suf.assign(nb + 1, 0.0);
-    for (int j = nb - 1; j >= 0; --j) {
-        for (int k = 0; k < kMomP; ++k)
-            g->mom_suf[(size_t)j * kMomP + k] = g->mom_suf[(size_t)(j + 1) * kMomP + k] + m[(size_t)j * kMomP + k];
-        g->cmax_suf[j] = std::max(g->cmax_suf[j + 1], c[j]);
-    }
     CK(launch_tail_moments(d, g->cinf, g->cinf2, ctx->T, ctx->redm, ctx->st));
-    double tm[kMomP + 2];
-    int rc = read_result(ctx, kMomP + 2, tm, ctx->redm.result);
-    if (rc) return rc;
-    for (int k = 0; k < kMomP; ++k) g->tail_mom[k] = tm[k];
-    g->tail_max = tm[kMomP + 1];
-    // FP64 copies for the device root search
-    std::vector<double> ms(g->mom_suf.begin(), g->mom_suf.end()), tl(kMomP + 1);
-    for (int k = 0; k < kMomP; ++k) tl[k] = (double)g->tail_mom[k];
-    tl[kMomP] = g->tail_max;
-    CK(cudaMemcpyAsync(g->d_mom_suf, ms.data(), ms.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(g->d_cmax_suf, g->cmax_suf.data(), g->cmax_suf.size() * sizeof(double),
-                       cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(g->d_tailm, tl.data(), tl.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));  // the host vectors above are released on return
+    CK(launch_moment_suffix(d, g->mom, g->cmax, ctx->redm.result, g->d_mom_suf, g->d_cmax_suf, g->d_tailm,
+                            ctx->st));
     g->have_mom = true;
+    g->have_mom_host = false;
+    return TPSC_OK;
+}
+
+// Host copies of the suffix sums and tail values, for the host-side series
+// of sumrule().
+int ensure_moments_host(tpsc_ctx *ctx, Grid *g) {
+    int rc = ensure_moments(ctx, g);
+    if (rc || g->have_mom_host) return rc;
+    const int nb = g->d.nb;
+    g->mom_suf.resize((size_t)(nb + 1) * kMomP);
+    g->cmax_suf.resize(nb + 1);
+    double tl[kMomP + 1];
+    CK(cudaMemcpyAsync(g->mom_suf.data(), g->d_mom_suf, g->mom_suf.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->st));
+    CK(cudaMemcpyAsync(g->cmax_suf.data(), g->d_cmax_suf, g->cmax_suf.size() * sizeof(double),
+                       cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(tl, g->d_tailm, sizeof(tl), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (int k = 0; k < kMomP; ++k) g->tail_mom[k] = tl[k];
+    g->tail_max = tl[kMomP];
+    g->have_mom_host = true;
     return TPSC_OK;
 }
 
@@ -749,7 +747,7 @@ int sumrule(tpsc_ctx *ctx, int channel, double Uv, double *tr, double *dtr) {
     const bool series = (ctx->form & TPSC_FORM_NEWTON) != 0;
     int jdir = d.nb, tail = 1;
     if (series) {
-        int rc = ensure_moments(ctx, g);
+        int rc = ensure_moments_host(ctx, g);
         if (rc) return rc;
         series_cut(g, Uv, &jdir, &tail);
     }
@@ -788,11 +786,15 @@ int roots_Usp_Uch(tpsc_ctx *ctx, double Usc[2]) {
         if ((rc = ensure_moments(ctx, g))) return rc;
         CK(launch_sumrule_roots(g->d, g->chiq, g->cinf, g->cinf2, g->d_mom_suf, g->d_cmax_suf, g->d_tailm, ctx->T,
                                 n, nsr, U, 2.0 / ctx->scal[TPSC_S_CHI0MAX] - 2 * EPS, ctx->roots, ctx->st));
+        // the results and the barrier's error flag in one readback
+        CK(cudaMemcpyAsync(ctx->h_res, ctx->roots.out, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(ctx->h_res + 6, ctx->roots.bar + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        unsigned err;
+        std::memcpy(&err, ctx->h_res + 6, sizeof(unsigned));
+        if (err) return fail(ctx, TPSC_ERR_CUDA, "device root search: grid barrier timed out");
         double r[6];
-        if ((rc = read_result(ctx, 6, r, ctx->roots.out))) return rc;
-        unsigned flags[4];
-        CK(cudaMemcpy(flags, ctx->roots.bar, sizeof(flags), cudaMemcpyDeviceToHost));
-        if (flags[2]) return fail(ctx, TPSC_ERR_CUDA, "device root search: grid barrier timed out");
+        for (int i = 0; i < 6; ++i) r[i] = ctx->h_res[i];
         if (r[4] != 1.0) return fail(ctx, TPSC_ERR_NO_ROOT, "Usp not found");
         if (r[5] != 1.0) return fail(ctx, TPSC_ERR_NO_ROOT, "Uch not found");
         ctx->Usp = Usc[0] = r[0];
@@ -879,7 +881,9 @@ int run_vertex(tpsc_ctx *ctx) {
     return TPSC_OK;
 }
 
-int run_self(tpsc_ctx *ctx) {
+// settle: read Sigma_inf back now; a Newton-form solve leaves it to the
+// readback of the mu search that follows
+int run_self(tpsc_ctx *ctx, bool settle = true) {
     Grid *g = ctx->cur;
     if (!g || !g->have_V) return fail(ctx, TPSC_ERR_STATE, "the vertex V(r, tau) has not been computed");
     const double fact = ctx->U * (3.0 * ctx->Usp + ctx->Uch) / 8.0;
@@ -899,10 +903,11 @@ int run_self(tpsc_ctx *ctx) {
     }
     if ((rc = join_side(ctx, 1))) return rc;
     CK(launch_sigma_tau(d, g->sigt, g->dS, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->T, ctx->st));
+    g->have_S = true;
+    if (!settle) return TPSC_OK;
     CK(cudaMemcpyAsync(ctx->h_res, g->sinf, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     ctx->scal[TPSC_S_SIGMA_INF] = ctx->h_res[0];
-    g->have_S = true;
     return TPSC_OK;
 }
 
@@ -932,17 +937,16 @@ int trace_diff_G(tpsc_ctx *ctx, double pmu, double *tr, double *dtr = nullptr) {
 }
 
 // The find_mu series covers the frequencies from jc = first n with
-// w_n >= kMomMuRange / kMuSeriesMax (capped at Nw0/2: then only the tail),
-// valid for |mu - mu0| <= dmax = kMuSeriesMax |z|_min, where |z| >= w_n -
-// |Im Sigma| >= w_n - 2 Sigma_inf / w_n bounds |z| on the series set.
-void mu_series_cut(const tpsc_ctx *ctx, int *jc_out, double *dmax) {
+// w_n >= kMomMuRange / kMuSeriesMax (capped at Nw0/2: then only the tail);
+// w_jc is returned for the root search, which takes the series while
+// |mu - mu0| <= kMuSeriesMax |z|_min with |z|_min = w_jc - 2 Sigma_inf / w_jc
+// (|z| >= w_n - |Im Sigma| on the series set).
+void mu_series_cut(const tpsc_ctx *ctx, int *jc_out, double *wc_out) {
     const int NO = ctx->cur->d.nw0 / 2;
     const double pt = PI * ctx->T;
     int jc = (int)std::ceil((kMomMuRange / kMuSeriesMax / pt - 1.0) / 2.0);
     jc = std::max(0, std::min(jc, NO));
-    const double wc = (2 * jc + 1) * pt;
-    const double zmin = wc - 2.0 * std::fabs(ctx->scal[TPSC_S_SIGMA_INF]) / wc;
-    *dmax = zmin > 0 ? kMuSeriesMax * zmin : 0.0;
+    *wc_out = (2 * jc + 1) * pt;
     *jc_out = jc;
 }
 
@@ -954,19 +958,21 @@ int self_traces_and_mu_newton(tpsc_ctx *ctx) {
     Grid *g = ctx->cur;
     const GridDev &d = g->d;
     int jc;
-    double dmax;
-    mu_series_cut(ctx, &jc, &dmax);
+    double wc;
+    mu_series_cut(ctx, &jc, &wc);
     CK(launch_sigma_moments(d, g->S, g->s2, g->s3, g->s4, g->sinf, g->mu0, ctx->T, jc, ctx->redm, ctx->st));
-    CK(launch_mu_roots(d, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->redm.result, g->mu0, ctx->T, jc, dmax, ctx->roots,
+    CK(launch_mu_roots(d, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->redm.result, g->mu0, ctx->T, jc, wc, ctx->roots,
                        ctx->st));
     CK(cudaMemcpyAsync(ctx->h_res, ctx->redm.result, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(ctx->h_res + 2, ctx->roots.out, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaMemcpyAsync(ctx->h_res + 6, ctx->roots.bar + 2, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(ctx->h_res + 7, g->sinf, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     int err;
     std::memcpy(&err, ctx->h_res + 6, sizeof(int));
     if (err) return fail(ctx, TPSC_ERR_CUDA, "device mu search: grid barrier timed out");
     const double *r = ctx->h_res;
+    ctx->scal[TPSC_S_SIGMA_INF] = r[7];
     ctx->scal[TPSC_S_TR_SG] = r[0];
     ctx->scal[TPSC_S_TR_SG_ASYMP] = r[0] + r[1];
     if (r[4] != 1.0) return fail(ctx, TPSC_ERR_NO_ROOT, "mu not found");
@@ -1346,7 +1352,7 @@ int tpsc_solve(tpsc_ctx *ctx) {
     rc = run_vertex(ctx);
     if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[3], ctx->st));
-    rc = run_self(ctx);
+    rc = run_self(ctx, !(ctx->form & TPSC_FORM_NEWTON));
     if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[4], ctx->st));
     // the Newton form computes traceSelfG in the same Sigma pass as the find_mu moments
@@ -1660,7 +1666,7 @@ int tpsc_run_kernel(tpsc_ctx *ctx, int which) {
             break;
         case 10: {
             // one Newton-form sum-rule evaluation at Usp: low frequencies, series above
-            int rc2 = ensure_moments(ctx, g);
+            int rc2 = ensure_moments_host(ctx, g);
             if (rc2) return rc2;
             int jdir, tail;
             series_cut(g, ctx->Usp, &jdir, &tail);
@@ -1670,8 +1676,8 @@ int tpsc_run_kernel(tpsc_ctx *ctx, int which) {
         case 11: {
             // one Newton-form Tr(G - G0) evaluation at mu: frequencies below the series
             int jc;
-            double dmax;
-            mu_series_cut(ctx, &jc, &dmax);
+            double wc;
+            mu_series_cut(ctx, &jc, &wc);
             CK(launch_trace_diff_G(d, g->S, g->s2, g->s3, g->s4, g->sinf, g->mu0, ctx->scal[TPSC_S_MU], ctx->T,
                                    ctx->red, ctx->st, jc));
             break;
@@ -1705,7 +1711,7 @@ int tpsc_kernel_bytes(tpsc_ctx *ctx, int which, double *bytes) {
         case 9: b = gtau + 2 * half + 2 * half; break; // stages 1 and 2
         case 10: {                                     // read chi0(q, iqn), j < jdir
             Grid *g = ctx->cur;
-            int rc2 = ensure_moments(ctx, g);
+            int rc2 = ensure_moments_host(ctx, g);
             if (rc2) return rc2;
             int jdir, tail;
             series_cut(g, ctx->Usp, &jdir, &tail);
@@ -1714,8 +1720,8 @@ int tpsc_kernel_bytes(tpsc_ctx *ctx, int which, double *bytes) {
         }
         case 11: {                                     // read S, j < jc
             int jc;
-            double dmax;
-            mu_series_cut(ctx, &jc, &dmax);
+            double wc;
+            mu_series_cut(ctx, &jc, &wc);
             b = (double)jc * d.n8 * 2 * s;
             break;
         }

@@ -50,12 +50,12 @@ int grid_for(long long total, int threads) {
 // mu0 of the finite lattice: sum_o w 2 f(eps - mu) / L^2 - n
 // (green0::ddensity_mu_PBC, src/green0.cpp:182-203)
 // ---------------------------------------------------------------------------
-__global__ void k_density(const double *__restrict__ ek, const uint32_t *__restrict__ lm, int n8, int nbk,
+__global__ void k_density(const double *__restrict__ ek, int n8, int nbk,
                           double mu, double T, double nk2, double *partial) {
     KSum acc;
     for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n8; o += gridDim.x * blockDim.x) {
         int l, m;
-        oct_lm(lm, o, l, m);
+        oct_lm(o, l, m);
         const int w = oct_weight(8, l, m, nbk);
         acc.add(2 * w / ((exp((ek[o] - mu) / T) + 1.0) * nk2));
     }
@@ -87,14 +87,14 @@ __global__ void k_gk_table(const double *__restrict__ ek, int n8, double mu0, do
 // Grt[j * n8 + o].
 template <int NBK>
 __global__ void __launch_bounds__(kSliceThreads, 1)
-    k_gslice(const double2 *__restrict__ gk, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
+    k_gslice(const double2 *__restrict__ gk, const double2 *__restrict__ tw,
              int n8, int nw0, double T, double *__restrict__ Grt) {
     extern __shared__ __align__(16) double S[];
     const auto *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
     const double t = j / (nw0 * T);
     const double bt = 1.0 / T - t;
-    fill_octant<NBK>(S, lm, n8, [&](int o) -> double {
+    fill_octant<NBK>(S, n8, [&](int o) -> double {
         const double2 c = __ldg(&gk[o]);
         return c.y * exp((c.x > 0 ? -t : bt) * c.x);
     });
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     double *out = Grt + (size_t)j * n8;
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
-        oct_lm(lm, o, l, m);
+        oct_lm(o, l, m);
         out[o] = S[l * NBK + m];
     }
 }
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
 // G(r,0-) = G(r,0+) + delta_r0, tau = beta/2 uses 2 G^2.
 template <int NBK>
 __global__ void __launch_bounds__(kSliceThreads, 1)
-    k_chi0_slice(const double *__restrict__ Grt, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
+    k_chi0_slice(const double *__restrict__ Grt, const double2 *__restrict__ tw,
                  int n8, int nw0, double *__restrict__ chirt, double *__restrict__ chiq) {
     extern __shared__ __align__(16) double S[];
     const auto *tws = slice_twiddles<NBK>(S, tw);
@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     const int nb = nw0 / 2 + 1;
     const double *gp = Grt + (size_t)j * n8;
     const double *gm = Grt + (size_t)(nw0 - j) * n8;
-    fill_octant<NBK>(S, lm, n8, [&](int o) -> double {
+    fill_octant<NBK>(S, n8, [&](int o) -> double {
         const double a = gp[o];
         double c;
         if (j == 0)
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
-        oct_lm(lm, o, l, m);
+        oct_lm(o, l, m);
         chiq[bidx(j, o, nb)] = S[l * NBK + m];
     }
 }
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
 // end condition (src/chi0.cpp:323-367, 420-447).  One CTA.
 template <int NBK, class GT>
 __global__ void __launch_bounds__(kSliceThreads, 1)
-    k_chi0_boundary(const double *__restrict__ ek, const double *__restrict__ er, const uint32_t *__restrict__ lm,
+    k_chi0_boundary(const double *__restrict__ ek, const double *__restrict__ er,
                     const double2 *__restrict__ tw, const GT *__restrict__ Grt, int n8, double mu0, double T,
                     double nk02, double *__restrict__ dG0p, double *__restrict__ dtau_chirt0,
                     double *__restrict__ dtau_chiqt0) {
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     const auto *tws = slice_twiddles<NBK>(S, tw);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
-        oct_lm(lm, o, l, m);
+        oct_lm(o, l, m);
         const double x = ek[o] - mu0;
         const double gkt = -1.0 / (exp(-x / T) + 1.0);
         put_sym<NBK>(S, l, m, -x * gkt / nk02);
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     int k = 0;
     for (int o = threadIdx.x; o < n8; o += blockDim.x, ++k) {
         int l, m;
-        oct_lm(lm, o, l, m);
+        oct_lm(o, l, m);
         const double dp = S[l * NBK + m];
         const double dm = ((o == 0) ? -mu0 : er[o]) - dp;
         const double g0 = Grt[o];
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     k = 0;
     for (int o = threadIdx.x; o < n8; o += blockDim.x, ++k) {
         int l, m;
-        oct_lm(lm, o, l, m);
+        oct_lm(o, l, m);
         dG0p[o] = dp_[k];
         dtau_chirt0[o] = dc_[k];
         put_sym<NBK>(S, l, m, dc_[k]);
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
-        oct_lm(lm, o, l, m);
+        oct_lm(o, l, m);
         dtau_chiqt0[o] = S[l * NBK + m];
     }
 }
@@ -198,12 +198,12 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
 // its DCT-I over q, one bosonic frequency per CTA (src/chi.cpp:89-115).
 template <int NBK>
 __global__ void __launch_bounds__(kSliceThreads, 1)
-    k_vertex_q(const double *__restrict__ chiq, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
+    k_vertex_q(const double *__restrict__ chiq, const double2 *__restrict__ tw,
                int n8, int nb, double normFact, double U, double Usp, double Uch, double *__restrict__ Vr) {
     extern __shared__ __align__(16) double S[];
     const auto *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
-    fill_octant<NBK>(S, lm, n8, [&](int o) -> double {
+    fill_octant<NBK>(S, n8, [&](int o) -> double {
         const double c0 = chiq[bidx(j, o, nb)];
         const double sp = c0 / (1.0 - Usp * c0 / 2.0);
         const double ch = c0 / (1.0 + Uch * c0 / 2.0);
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
-        oct_lm(lm, o, l, m);
+        oct_lm(o, l, m);
         Vr[bidx(j, o, nb)] = S[l * NBK + m];
     }
 }
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
 // (blockIdx.x = 0: tau = 0, 1: tau = beta).
 template <int NBK, class GT>
 __global__ void __launch_bounds__(kSliceThreads, 1)
-    k_sigma_boundary(const double *__restrict__ er, const uint32_t *__restrict__ lm, const double2 *__restrict__ tw,
+    k_sigma_boundary(const double *__restrict__ er, const double2 *__restrict__ tw,
                      const GT *__restrict__ Grt, const double *__restrict__ V, const double *__restrict__ dtau_chirt0,
                      const double *__restrict__ dG0p, int n8, int nw0, int n8p, double mu0, double fact,
                      double *__restrict__ dS) {
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
         const GT *g = Grt + (side == 0 ? 0 : (size_t)nw0 * n8);
         for (int o = threadIdx.x; o < n8; o += blockDim.x) {
             int l, m;
-            oct_lm(lm, o, l, m);
+            oct_lm(o, l, m);
             const double v0 = V[bidx(0, o, nb)];
             double val;
             if (side == 0) {
@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
         dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
         for (int o = threadIdx.x; o < n8; o += blockDim.x) {
             int l, m;
-            oct_lm(lm, o, l, m);
+            oct_lm(o, l, m);
             dS[side * n8p + o] = S[l * NBK + m];
         }
         __syncthreads();
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
 // transform in FP64 either way).
 template <int NBK, class GT>
 __global__ void __launch_bounds__(kSliceThreads, 1)
-    k_sigma_slice(const GT *__restrict__ Grt, const double *__restrict__ V, const uint32_t *__restrict__ lm,
+    k_sigma_slice(const GT *__restrict__ Grt, const double *__restrict__ V,
                   const double2 *__restrict__ tw, int n8, int nw0, double *__restrict__ sigt) {
     extern __shared__ __align__(16) double S[];
     const auto *tws = slice_twiddles<NBK>(S, tw);
@@ -271,12 +271,12 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     const int nb = nw0 / 2 + 1;
     const int jv = j < nb ? j : nw0 - j;
     const GT *g = Grt + (size_t)j * n8;
-    fill_octant<NBK>(S, lm, n8, [&](int o) -> double { return (double)g[o] * V[bidx(jv, o, nb)]; });
+    fill_octant<NBK>(S, n8, [&](int o) -> double { return (double)g[o] * V[bidx(jv, o, nb)]; });
     __syncthreads();
     dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
-        oct_lm(lm, o, l, m);
+        oct_lm(o, l, m);
         sigt[bidx(j, o, nw0 + 1)] = S[l * NBK + m];
     }
 }
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
         VN[threadIdx.x] = A[threadIdx.x * NJ + NJ - 1];
     }
     column_sums(A, NJ, 0, NJ, sV);
-    const double h = 1.0 / (N * T);
+    const double h = 1.0 / (N * T), ih = 1.0 / h;
     spline_second_derivatives(A, NJ, NJ, h, d0, dN, spl, spl + NJ);
     column_sums(A, NJ, 0, NJ, sM);
     if (threadIdx.x < 4) {
@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
             const bool lo = j < N / 2;
             const int jj = lo ? j : N - 1 - j;
             const double sg = lo ? 1.0 : -1.0;
-            return make_double2(sg * (Ma[jj + 1] - Ma[jj]) / h, sg * (Mb[jj + 1] - Mb[jj]) / h);
+            return make_double2(sg * (Ma[jj + 1] - Ma[jj]) * ih, sg * (Mb[jj + 1] - Mb[jj]) * ih);
         };
         if (threadIdx.x < G) group_fft_io<N, +1>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
         __syncthreads();
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
             // split the packed transform: F_a = (Z_n + conj Z_{N-n})/2, F_b = (Z_n - conj Z_{N-n})/(2i)
             const double2 Fa = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
             const double2 Fb = make_double2(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
-            const double wn = 2 * n * kPi * T;
+            const double wn = 2 * n * kPi * T, iw = 1.0 / wn, i2 = iw * iw;
             const double2 w = tw_at(tw2, n);
             const double cth = w.x, sth = -w.y;  // cos, sin of 2 pi n / N
 #pragma unroll
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
                 const int o = o0 + c;
                 const double2 F = q == 0 ? Fa : Fb;
                 const double cinf = -2.0 * d0[c];
-                double val = cinf / (wn * wn) + ((1.0 - cth) * F.x + sth * F.y) / (wn * wn * wn * wn);
+                double val = (cinf + ((1.0 - cth) * F.x + sth * F.y) * i2) * i2;
                 if (o == 0) val = 0.0;
                 A[c * NJ + n] = val;
                 if (n == NJ - 1 && o < n8) chi0_inf2[o] = (o == 0) ? 0.0 : 2.0 * F.x;
@@ -442,7 +442,7 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
         if (o == 0) sinf[0] = -(A[0] + A[NJ - 1]);
         if (o < n8) s2[o] = d0[threadIdx.x] + dN[threadIdx.x];
     }
-    const double h = 1.0 / (N * T);
+    const double h = 1.0 / (N * T), ih = 1.0 / h;
     spline_second_derivatives(A, NJ, NJ, h, d0, dN, spl, spl + NJ);
     if (threadIdx.x < 4) {
         const int o = o0 + threadIdx.x;
@@ -456,8 +456,8 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
         const double *Mb = A + (2 * pr + 1) * NJ;
         // FFT input: exp(i pi j/N) 6 a_j, two columns packed as Re/Im
         auto in = [&](int j) -> double2 {
-            const double fa = (Ma[j + 1] - Ma[j]) / h;
-            const double fb = (Mb[j + 1] - Mb[j]) / h;
+            const double fa = (Ma[j + 1] - Ma[j]) * ih;
+            const double fb = (Mb[j + 1] - Mb[j]) * ih;
             return cmul(tw_at(ht2, j), make_double2(fa, fb));
         };
         if (threadIdx.x < G) group_fft_io<N, +1>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
@@ -532,7 +532,7 @@ __global__ void __launch_bounds__(256, 2)
         if (o == 0) sinf[0] = -(A[0] + A[NJ - 1]);
         if (o < n8) s2[o] = d0[threadIdx.x] + dN[threadIdx.x];
     }
-    const double h = 1.0 / (N * T);
+    const double h = 1.0 / (N * T), ih = 1.0 / h;
     spline_second_derivatives<2>(A, NJ, NJ, h, d0, dN, spl, spl + NJ);
     if (threadIdx.x < 2) {
         const int o = o0 + threadIdx.x;
@@ -542,8 +542,8 @@ __global__ void __launch_bounds__(256, 2)
     if (threadIdx.x < G) {
         const double *Ma = A, *Mb = A + NJ;
         auto in = [&](int j) -> double2 {
-            const double fa = (Ma[j + 1] - Ma[j]) / h;
-            const double fb = (Mb[j + 1] - Mb[j]) / h;
+            const double fa = (Ma[j + 1] - Ma[j]) * ih;
+            const double fb = (Mb[j + 1] - Mb[j]) * ih;
             return cmul(tw_at(ht2, j), make_double2(fa, fb));
         };
         group_fft_io<N, +1, false, true>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
@@ -611,7 +611,7 @@ __global__ void __launch_bounds__(256, 2)
         VN[threadIdx.x] = A[threadIdx.x * NJ + NJ - 1];
     }
     column_sums<2>(A, NJ, 0, NJ, sV);
-    const double h = 1.0 / (N * T);
+    const double h = 1.0 / (N * T), ih = 1.0 / h;
     spline_second_derivatives<2>(A, NJ, NJ, h, d0, dN, spl, spl + NJ);
     column_sums<2>(A, NJ, 0, NJ, sM);
     if (threadIdx.x < 2) {
@@ -626,7 +626,7 @@ __global__ void __launch_bounds__(256, 2)
             const bool lo = j < N / 2;
             const int jj = lo ? j : N - 1 - j;
             const double sg = lo ? 1.0 : -1.0;
-            return make_double2(sg * (Ma[jj + 1] - Ma[jj]) / h, sg * (Mb[jj + 1] - Mb[jj]) / h);
+            return make_double2(sg * (Ma[jj + 1] - Ma[jj]) * ih, sg * (Mb[jj + 1] - Mb[jj]) * ih);
         };
         group_fft_io<N, +1, false, true>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
     }
@@ -636,7 +636,7 @@ __global__ void __launch_bounds__(256, 2)
         const double2 Zc = X[pidx(N - n)];
         const double2 Fa = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
         const double2 Fb = make_double2(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
-        const double wn = 2 * n * kPi * T;
+        const double wn = 2 * n * kPi * T, iw = 1.0 / wn, i2 = iw * iw;
         const double2 w = tw_at(tw2, n);
         const double cth = w.x, sth = -w.y;
 #pragma unroll
@@ -644,7 +644,7 @@ __global__ void __launch_bounds__(256, 2)
             const int o = o0 + q;
             const double2 F = q == 0 ? Fa : Fb;
             const double cinf = -2.0 * d0[q];
-            double val = cinf / (wn * wn) + ((1.0 - cth) * F.x + sth * F.y) / (wn * wn * wn * wn);
+            double val = (cinf + ((1.0 - cth) * F.x + sth * F.y) * i2) * i2;
             if (o == 0) val = 0.0;
             g[4 * n + q] = val;
             if (n == NJ - 1 && o < n8) chi0_inf2[o] = (o == 0) ? 0.0 : 2.0 * F.x;
@@ -1206,12 +1206,12 @@ __device__ __forceinline__ MaxPt max_shfl(MaxPt a, int off) {
     return better(b, a) ? b : a;
 }
 __global__ void __launch_bounds__(1024)
-    k_chi0max(const double *__restrict__ chiq, const uint32_t *__restrict__ lm, int n8, int nb, double *result) {
+    k_chi0max(const double *__restrict__ chiq, int n8, int nb, double *result) {
     // values <= 0 never win: the reference's scan starts from chi0max = 0
     MaxPt best{0.0, -1, -1};
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
-        oct_lm(lm, o, l, m);
+        oct_lm(o, l, m);
         const MaxPt c{chiq[bidx(0, o, nb)], l, m};
         if (c.v > 0.0 && better(c, best)) best = c;
     }
@@ -1238,7 +1238,7 @@ __global__ void __launch_bounds__(1024)
 // bisection otherwise; stops when the step is below 1e-15 (1 + |mu|).
 // The Newton form's replacement of the host root search.
 __global__ void __launch_bounds__(1024)
-    k_mu0_newton(const double *__restrict__ ek, const uint32_t *__restrict__ lm, int n8, int nbk, double n, double T,
+    k_mu0_newton(const double *__restrict__ ek, int n8, int nbk, double n, double T,
                  double nk2, double *result) {
     __shared__ double red[32][2];
     __shared__ double s_mu;
@@ -1254,7 +1254,7 @@ __global__ void __launch_bounds__(1024)
         double v = 0.0, dv = 0.0;
         for (int o = threadIdx.x; o < n8; o += blockDim.x) {
             int l, m;
-            oct_lm(lm, o, l, m);
+            oct_lm(o, l, m);
             const int w = oct_weight(8, l, m, nbk);
             const double f = 1.0 / (exp((ek[o] - mu) / T) + 1.0);
             v += 2 * w * f / nk2;
@@ -1438,7 +1438,7 @@ struct RunGslice {
         const double nk02 = (double)g->nk0 * g->nk0;
         k_gk_table<<<(g->n8 + 255) / 256, 256, 0, st>>>(g->ek, g->n8, mu0, T, nk02, g->gk);
         if ((e = launched()) != cudaSuccess) return e;
-        k_gslice<NBK><<<g->nw0 + 1, kSliceThreads, sm, st>>>(g->gk, g->lm, g->tw_k, g->n8, g->nw0, T, Grt);
+        k_gslice<NBK><<<g->nw0 + 1, kSliceThreads, sm, st>>>(g->gk, g->tw_k, g->n8, g->nw0, T, Grt);
         return launched();
     }
 };
@@ -1451,7 +1451,7 @@ struct RunChi0Boundary {
         cudaError_t e = set_smem(k_chi0_boundary<NBK, GT>, sm);
         if (e != cudaSuccess) return e;
         const double nk02 = (double)g->nk0 * g->nk0;
-        k_chi0_boundary<NBK, GT><<<1, kSliceThreads, sm, st>>>(g->ek, g->er, g->lm, g->tw_k, Grt, g->n8, mu0, T,
+        k_chi0_boundary<NBK, GT><<<1, kSliceThreads, sm, st>>>(g->ek, g->er, g->tw_k, Grt, g->n8, mu0, T,
                                                                 nk02, dG0p, dchirt0, dchiqt0);
         return launched();
     }
@@ -1462,7 +1462,7 @@ struct RunChi0Slice {
         const size_t sm = SliceSmem<NBK>::bytes;
         cudaError_t e = set_smem(k_chi0_slice<NBK>, sm);
         if (e != cudaSuccess) return e;
-        k_chi0_slice<NBK><<<g->nb, kSliceThreads, sm, st>>>(Grt, g->lm, g->tw_k, g->n8, g->nw0, chirt, chiq);
+        k_chi0_slice<NBK><<<g->nb, kSliceThreads, sm, st>>>(Grt, g->tw_k, g->n8, g->nw0, chirt, chiq);
         return launched();
     }
 };
@@ -1474,7 +1474,7 @@ struct RunVertexQ {
         cudaError_t e = set_smem(k_vertex_q<NBK>, sm);
         if (e != cudaSuccess) return e;
         const double normFact = T / ((double)g->nk0 * g->nk0);
-        k_vertex_q<NBK><<<g->nb, kSliceThreads, sm, st>>>(chiq, g->lm, g->tw_k, g->n8, g->nb, normFact, U, Usp, Uch,
+        k_vertex_q<NBK><<<g->nb, kSliceThreads, sm, st>>>(chiq, g->tw_k, g->n8, g->nb, normFact, U, Usp, Uch,
                                                           Vr);
         return launched();
     }
@@ -1487,7 +1487,7 @@ struct RunSigmaBoundary {
         const size_t sm = SliceSmem<NBK>::bytes;
         cudaError_t e = set_smem(k_sigma_boundary<NBK, GT>, sm);
         if (e != cudaSuccess) return e;
-        k_sigma_boundary<NBK, GT><<<2, kSliceThreads, sm, st>>>(g->er, g->lm, g->tw_k, Grt, V, dchirt0, dG0p, g->n8,
+        k_sigma_boundary<NBK, GT><<<2, kSliceThreads, sm, st>>>(g->er, g->tw_k, Grt, V, dchirt0, dG0p, g->n8,
                                                                  g->nw0, g->n8p, mu0, fact, dS);
         return launched();
     }
@@ -1499,7 +1499,7 @@ struct RunSigmaSlice {
         const size_t sm = SliceSmem<NBK>::bytes;
         cudaError_t e = set_smem(k_sigma_slice<NBK, GT>, sm);
         if (e != cudaSuccess) return e;
-        k_sigma_slice<NBK, GT><<<g->nw0 + 1, kSliceThreads, sm, st>>>(Grt, V, g->lm, g->tw_k, g->n8, g->nw0, sigt);
+        k_sigma_slice<NBK, GT><<<g->nw0 + 1, kSliceThreads, sm, st>>>(Grt, V, g->tw_k, g->n8, g->nw0, sigt);
         return launched();
     }
 };
@@ -1574,7 +1574,7 @@ bool supported_grid(int nk0, int nw0) {
 
 cudaError_t launch_density(const GridDev &g, double mu, double n, double T, Reduce r, cudaStream_t st) {
     const int nb = grid_for(g.n8, 256);
-    k_density<<<nb, 256, 0, st>>>(g.ek, g.lm, g.n8, g.nbk, mu, T, 4.0 * (g.nbk - 1) * (g.nbk - 1), r.partial);
+    k_density<<<nb, 256, 0, st>>>(g.ek, g.n8, g.nbk, mu, T, 4.0 * (g.nbk - 1) * (g.nbk - 1), r.partial);
     cudaError_t e = launched();
     if (e != cudaSuccess) return e;
     return finish<1>(r, nb, -n, st);
@@ -1635,6 +1635,94 @@ cudaError_t launch_tail_moments(const GridDev &g, const double *chi0_inf, const 
     if (e != cudaSuccess) return e;
     // the per-block maxima -> result[NV]
     k_max_finish<<<1, 32, 0, st>>>(r.partial + (2 * kMomP + 1) * kMaxBlocks, nblk, r.result + NV);
+    return launched();
+}
+
+namespace {
+
+// double-double value hi + lo, |lo| <= ulp(hi) / 2
+struct DD {
+    double hi, lo;
+};
+__device__ __forceinline__ DD dd_add(DD a, DD b) {
+    double s, e;
+    two_sum(a.hi, b.hi, s, e);
+    e += a.lo + b.lo;
+    const double h = s + e;
+    return DD{h, e - (h - s)};
+}
+__device__ __forceinline__ DD dd_shfl_down(DD a, int off) {
+    return DD{__shfl_down_sync(0xffffffffu, a.hi, off), __shfl_down_sync(0xffffffffu, a.lo, off)};
+}
+
+// Block k < kMomP: suffix sums of moment k over the frequencies; block
+// kMomP: suffix maxima of cmax and the tail values.  Each thread takes a
+// chunk of consecutive frequencies; the chunk totals are combined by a warp
+// suffix scan and the warps' totals in a fixed order, so the sums are
+// deterministic.
+__global__ void __launch_bounds__(256)
+    k_moment_suffix(const double *__restrict__ mom, const double *__restrict__ cmax, const double *__restrict__ tail,
+                    int nb, double *__restrict__ mom_suf, double *__restrict__ cmax_suf, double *__restrict__ tailm) {
+    extern __shared__ double col[];
+    __shared__ DD wtot[32];
+    const int k = blockIdx.x;
+    const bool is_max = k == kMomP;
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) col[j] = is_max ? cmax[j] : mom[(size_t)j * kMomP + k];
+    __syncthreads();
+    const int C = (nb + blockDim.x - 1) / blockDim.x;
+    const int s = min((int)threadIdx.x * C, nb), e = min(s + C, nb);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (is_max) {
+        double m = 0.0;
+        for (int j = e - 1; j >= s; --j) m = fmax(m, col[j]);
+        for (int off = 1; off < 32; off <<= 1) {
+            const double t = __shfl_down_sync(0xffffffffu, m, off);
+            if (lane + off < 32) m = fmax(m, t);
+        }
+        if (lane == 0) wtot[warp].hi = m;
+        double ex = __shfl_down_sync(0xffffffffu, m, 1);
+        __syncthreads();
+        if (lane == 31) ex = 0.0;
+        for (int w = warp + 1; w < nw; ++w) ex = fmax(ex, wtot[w].hi);
+        for (int j = e - 1; j >= s; --j) {
+            ex = fmax(ex, col[j]);
+            cmax_suf[j] = ex;
+        }
+        if (threadIdx.x == 0) {
+            cmax_suf[nb] = 0.0;
+            for (int i = 0; i < kMomP; ++i) tailm[i] = tail[i];
+            tailm[kMomP] = tail[kMomP + 1];
+        }
+    } else {
+        DD c{0.0, 0.0};
+        for (int j = e - 1; j >= s; --j) c = dd_add(c, DD{col[j], 0.0});
+        for (int off = 1; off < 32; off <<= 1) {
+            const DD t = dd_shfl_down(c, off);
+            if (lane + off < 32) c = dd_add(c, t);
+        }
+        if (lane == 0) wtot[warp] = c;
+        DD ex = dd_shfl_down(c, 1);
+        __syncthreads();
+        if (lane == 31) ex = DD{0.0, 0.0};
+        DD above{0.0, 0.0};
+        for (int w = nw - 1; w > warp; --w) above = dd_add(above, wtot[w]);
+        ex = dd_add(ex, above);
+        for (int j = e - 1; j >= s; --j) {
+            ex = dd_add(ex, DD{col[j], 0.0});
+            mom_suf[(size_t)j * kMomP + k] = ex.hi + ex.lo;
+        }
+        if (threadIdx.x == 0) mom_suf[(size_t)nb * kMomP + k] = 0.0;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_moment_suffix(const GridDev &g, const double *mom, const double *cmax, const double *tail_result,
+                                 double *mom_suf, double *cmax_suf, double *tailm, cudaStream_t st) {
+    const size_t sm = (size_t)g.nb * sizeof(double);
+    cudaError_t e = set_smem(k_moment_suffix, sm);
+    if (e != cudaSuccess) return e;
+    k_moment_suffix<<<kMomP + 1, 256, sm, st>>>(mom, cmax, tail_result, g.nb, mom_suf, cmax_suf, tailm);
     return launched();
 }
 
@@ -1730,12 +1818,12 @@ cudaError_t launch_gwn_local(const GridDev &g, const double2 *S, const double *s
 }
 
 cudaError_t launch_mu0_newton(const GridDev &g, double n, double T, Reduce r, cudaStream_t st) {
-    k_mu0_newton<<<1, 1024, 0, st>>>(g.ek, g.lm, g.n8, g.nbk, n, T, 4.0 * (g.nbk - 1) * (g.nbk - 1), r.result);
+    k_mu0_newton<<<1, 1024, 0, st>>>(g.ek, g.n8, g.nbk, n, T, 4.0 * (g.nbk - 1) * (g.nbk - 1), r.result);
     return launched();
 }
 
 cudaError_t launch_chi0max(const GridDev &g, const double *chiq, Reduce r, cudaStream_t st) {
-    k_chi0max<<<1, 1024, 0, st>>>(chiq, g.lm, g.n8, g.nb, r.result);
+    k_chi0max<<<1, 1024, 0, st>>>(chiq, g.n8, g.nb, r.result);
     return launched();
 }
 

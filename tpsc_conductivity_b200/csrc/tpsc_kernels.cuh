@@ -14,7 +14,6 @@ struct GridDev {
     int n8p = 0;        // n8 rounded up to a multiple of 4 (column blocks)
     int nw0 = 0;        // Nw0: fermionic frequencies (+ and -)
     int nb = 0;         // Nw0/2 + 1: bosonic n >= 0 == tau nodes on [0, beta/2]
-    uint32_t *lm = nullptr;        // [n8] (l << 16) | m of octant point o
     double *ek = nullptr;          // [n8] eps_k on the octant
     double2 *gk = nullptr;         // [n8] (eps_k - mu0, G0 prefactor) for the G(r, tau) slices
     double *er = nullptr;          // [n8] real-space hopping table
@@ -83,6 +82,12 @@ constexpr double kMomMuRange = 0.35;     // |mu - mu0| the find_mu series is bui
 constexpr int kMuMomP = 12;              // terms of the find_mu series
 constexpr double kMuSeriesMax = 0.03;    // |mu - mu0| / |z| bound of its terms: 0.03^12 < 1e-18
 cudaError_t launch_chi0_moments(const GridDev &g, const double *chiq, double *mom, double *cmax, cudaStream_t st);
+// sums of mom over the frequencies >= j (double-double, rounded once),
+// j = 0..nb -> mom_suf [(nb + 1)][kMomP]; suffix maxima of cmax -> cmax_suf
+// [nb + 1]; the tail moments and tail maximum of launch_tail_moments' result
+// -> tailm [kMomP + 1].  One launch, no host round trip.
+cudaError_t launch_moment_suffix(const GridDev &g, const double *mom, const double *cmax, const double *tail_result,
+                                 double *mom_suf, double *cmax_suf, double *tailm, cudaStream_t st);
 cudaError_t launch_trace_chi0(const GridDev &g, const double *chiq, const double *chi0_inf,
                               const double *chi0_inf2, double T, Reduce r, cudaStream_t st);
 
@@ -126,11 +131,12 @@ constexpr int kSigmaMomNV = 2 * kMuMomP + 3;
 cudaError_t launch_sigma_moments(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                                  const double *s4, const double *sinf, double mu0, double T, int jc, Reduce r,
                                  cudaStream_t st);
-// mu by safeguarded Newton from mu0 (the series of the moments `mom` for
-// |mu - mu0| <= dmax, the full sum beyond), then Tr Sigma G at mu; one
-// cooperative launch -> rs.out = {mu, evals, ok, Tr Sigma G}
+// mu by safeguarded Newton from mu0 (the series of the moments `mom` while
+// |mu - mu0| <= kMuSeriesMax (wc - 2 |Sigma_inf| / wc), wc = w_jc, the full
+// sum beyond), then Tr Sigma G at mu; one cooperative launch -> rs.out =
+// {mu, evals, ok, Tr Sigma G}
 cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2, const double *s3, const double *s4,
-                            const double *sinf, const double *mom, double mu0, double T, int jc, double dmax,
+                            const double *sinf, const double *mom, double mu0, double T, int jc, double wc,
                             RootScratch rs, cudaStream_t st);
 // Usp then Uch by safeguarded Newton with the moment series, one cooperative
 // launch -> rs.out = {Usp, Uch, evals_sp, evals_ch, ok_sp, ok_ch}

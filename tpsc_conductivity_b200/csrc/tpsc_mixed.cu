@@ -53,14 +53,14 @@ __device__ __forceinline__ const float4 *twiddles32(float *S, const float4 *__re
 // FP64, rounded once to float; Grt32[j * n8 + o].
 template <int NBK>
 __global__ void __launch_bounds__(kSlice32Threads, 2)
-    k_gslice32(const double2 *__restrict__ gk, const uint32_t *__restrict__ lm, const float4 *__restrict__ tw,
+    k_gslice32(const double2 *__restrict__ gk, const float4 *__restrict__ tw,
                int n8, int nw0, double T, float *__restrict__ Grt) {
     extern __shared__ __align__(16) float S32[];
     const float4 *tws = twiddles32<NBK>(S32, tw);
     const int j = blockIdx.x;
     const double t = j / (nw0 * T);
     const double bt = 1.0 / T - t;
-    fill_octant<NBK>(S32, lm, n8, [&](int o) -> float {
+    fill_octant<NBK>(S32, n8, [&](int o) -> float {
         const double2 c = __ldg(&gk[o]);
         return (float)(c.y * exp((c.x > 0 ? -t : bt) * c.x));
     });
@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
     float *out = Grt + (size_t)j * n8;
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
-        oct_lm(lm, o, l, m);
+        oct_lm(o, l, m);
         out[o] = S32[l * NBK + m];
     }
 }
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
 // -> chi0(q, tau_j) in FP64 (src/chi0.cpp:393-418, 497-517, 545-558).
 template <int NBK>
 __global__ void __launch_bounds__(kSlice32Threads, 2)
-    k_chi0_slice32(const float *__restrict__ Grt, const uint32_t *__restrict__ lm, const float4 *__restrict__ tw,
+    k_chi0_slice32(const float *__restrict__ Grt, const float4 *__restrict__ tw,
                    int n8, int nw0, double *__restrict__ chirt, double *__restrict__ chiq) {
     extern __shared__ __align__(16) float S32[];
     const float4 *tws = twiddles32<NBK>(S32, tw);
@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
     const int nb = nw0 / 2 + 1;
     const float *gp = Grt + (size_t)j * n8;
     const float *gm = Grt + (size_t)(nw0 - j) * n8;
-    fill_octant<NBK>(S32, lm, n8, [&](int o) -> float {
+    fill_octant<NBK>(S32, n8, [&](int o) -> float {
         const double a = gp[o];
         double c;
         if (j == 0)
@@ -103,31 +103,34 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
     dct2_slice<NBK>(S32, scratch32<NBK>(S32), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
-        oct_lm(lm, o, l, m);
+        oct_lm(o, l, m);
         chiq[bidx(j, o, nb)] = S32[l * NBK + m];
     }
 }
 
 // V(q, iqn) in FP64 from chi0(q, iqn), its DCT-I over q in FP32
-// (src/chi.cpp:89-115).
+// (src/chi.cpp:89-115).  With a = Usp/2, b = Uch/2,
+//   chi_sp - chi0 = a chi0^2 / (1 - a chi0),  chi_ch - chi0 = -b chi0^2 / (1 + b chi0),
+// so that V takes one FP64 division per point.
 template <int NBK>
 __global__ void __launch_bounds__(kSlice32Threads, 2)
-    k_vertex_q32(const double *__restrict__ chiq, const uint32_t *__restrict__ lm, const float4 *__restrict__ tw,
+    k_vertex_q32(const double *__restrict__ chiq, const float4 *__restrict__ tw,
                  int n8, int nb, double normFact, double U, double Usp, double Uch, double *__restrict__ Vr) {
     extern __shared__ __align__(16) float S32[];
     const float4 *tws = twiddles32<NBK>(S32, tw);
     const int j = blockIdx.x;
-    fill_octant<NBK>(S32, lm, n8, [&](int o) -> float {
+    fill_octant<NBK>(S32, n8, [&](int o) -> float {
         const double c0 = chiq[bidx(j, o, nb)];
-        const double sp = c0 / (1.0 - Usp * c0 / 2.0);
-        const double ch = c0 / (1.0 + Uch * c0 / 2.0);
-        return (float)(normFact * U * (3.0 * Usp * (sp - c0) + Uch * (ch - c0)) / 8.0);
+        const double a = 0.5 * Usp, b = 0.5 * Uch;
+        const double ds = 1.0 - a * c0, dc = 1.0 + b * c0;
+        const double num = 3.0 * Usp * a * dc - Uch * b * ds;
+        return (float)(0.125 * normFact * U * c0 * c0 * num / (ds * dc));
     });
     __syncthreads();
     dct2_slice<NBK>(S32, scratch32<NBK>(S32), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
-        oct_lm(lm, o, l, m);
+        oct_lm(o, l, m);
         Vr[bidx(j, o, nb)] = S32[l * NBK + m];
     }
 }
@@ -139,7 +142,7 @@ struct RunGslice32 {
         cudaError_t e = set_smem(k_gslice32<NBK>, sm);
         if (e != cudaSuccess) return e;
         if ((e = launch_gk_table(*g, mu0, T, st)) != cudaSuccess) return e;
-        k_gslice32<NBK><<<g->nw0 + 1, kSlice32Threads, sm, st>>>(g->gk, g->lm, g->tw_k32, g->n8, g->nw0, T, Grt);
+        k_gslice32<NBK><<<g->nw0 + 1, kSlice32Threads, sm, st>>>(g->gk, g->tw_k32, g->n8, g->nw0, T, Grt);
         return launched();
     }
 };
@@ -149,7 +152,7 @@ struct RunChi0Slice32 {
         const size_t sm = Slice32Smem<NBK>::bytes;
         cudaError_t e = set_smem(k_chi0_slice32<NBK>, sm);
         if (e != cudaSuccess) return e;
-        k_chi0_slice32<NBK><<<g->nb, kSlice32Threads, sm, st>>>(Grt, g->lm, g->tw_k32, g->n8, g->nw0, chirt, chiq);
+        k_chi0_slice32<NBK><<<g->nb, kSlice32Threads, sm, st>>>(Grt, g->tw_k32, g->n8, g->nw0, chirt, chiq);
         return launched();
     }
 };
@@ -161,7 +164,7 @@ struct RunVertexQ32 {
         cudaError_t e = set_smem(k_vertex_q32<NBK>, sm);
         if (e != cudaSuccess) return e;
         const double normFact = T / ((double)g->nk0 * g->nk0);
-        k_vertex_q32<NBK><<<g->nb, kSlice32Threads, sm, st>>>(chiq, g->lm, g->tw_k32, g->n8, g->nb, normFact, U, Usp,
+        k_vertex_q32<NBK><<<g->nb, kSlice32Threads, sm, st>>>(chiq, g->tw_k32, g->n8, g->nb, normFact, U, Usp,
                                                               Uch, Vr);
         return launched();
     }

@@ -281,42 +281,66 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
 //   G0  = sum w Re 1/(i w_n - eps + mu0),
 // so that this part of Tr(G - G0) at mu is Re sum_m (mu0 - mu)^m C_m - G0 to
 // a relative kMuSeriesMax^kMuMomP while |mu - mu0| <= kMuSeriesMax |z|.
+//
+// C_m for m >= kMuMomF64 is formed and summed in FP32 (per thread, ~32 terms;
+// the block and grid sums are FP64): its term (mu0 - mu)^m C_m is at most
+// kMuSeriesMax^m = 8e-7 of the leading one per point, so an FP32 relative
+// error ~1e-6 on it moves Tr(G - G0) by < 1e-12 of its leading term.  The
+// point constants live in shared memory and Tr Sigma G0, its Hartree part and
+// G0 share one reciprocal per (k, n), so that two CTAs fit on an SM.
 // One CTA per column block, per-block partials (block_store).
-__global__ void __launch_bounds__(256)
+constexpr int kMuMomF64 = 4;
+
+__global__ void __launch_bounds__(256, 2)
     k_sigma_moments(const double2 *__restrict__ S, const double *__restrict__ s2, const double *__restrict__ s3,
                     const double *__restrict__ s4, const double *__restrict__ sinfp, const double *__restrict__ ek,
                     const double *__restrict__ w16, int nw0, double mu0, double T, double nk02, int jc,
                     double *partial) {
-    constexpr int NV = kSigmaMomNV;
+    constexpr int NV = kSigmaMomNV, P64 = kMuMomF64, P32 = kMuMomP - kMuMomF64;
+    __shared__ double cw[4], cx[4], c2[4], c3[4], c4[4];
     const int blk = blockIdx.x, o0 = 4 * blk, NO = nw0 / 2;
     const double sinf = sinfp[0];
     const double pt = 3.141592653589793 * T;
-    double acc[NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
-    double ww[4], e[4], c2[4], c3[4], c4[4];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        ww[c] = w16[o0 + c];
-        const bool ok = ww[c] != 0.0;
-        e[c] = ok ? ek[o0 + c] : 0.0;
+    if (threadIdx.x < 4) {
+        const int c = threadIdx.x;
+        const double w = w16[o0 + c];
+        const bool ok = w != 0.0;
+        cw[c] = w;
+        cx[c] = ok ? ek[o0 + c] - mu0 : 0.0;
         c2[c] = ok ? s2[o0 + c] : 0.0;
         c3[c] = ok ? s3[o0 + c] : 0.0;
         c4[c] = ok ? s4[o0 + c] : 0.0;
     }
-    auto moments = [&](double wn, double rS, double iS, double ec, double w) {
-        const double zx = mu0 - ec - rS, zy = wn - iS;
+    __syncthreads();
+    double tsg = 0.0, har = 0.0, g0 = 0.0;
+    double m64[2 * P64];
+    float m32[2 * P32];
+#pragma unroll
+    for (int k = 0; k < 2 * P64; ++k) m64[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 2 * P32; ++k) m32[k] = 0.0f;
+    // z = i w_n - x - Sigma with x = eps - mu0; inv = 1 / (w_n^2 + x^2)
+    auto moments = [&](double wn, double rS, double iS, double x, double w, double inv) {
+        const double zx = -x - rS, zy = wn - iS;
         const double rr = 1.0 / (zx * zx + zy * zy);  // |z| >= w_n > 0
         const double2 zi = make_double2(zx * rr, -zy * rr);
         double2 zp = zi;
 #pragma unroll
-        for (int m = 0; m < kMuMomP; ++m) {
-            acc[2 + 2 * m] += w * zp.x;
-            acc[3 + 2 * m] += w * zp.y;
+        for (int m = 0; m < P64; ++m) {
+            m64[2 * m] += w * zp.x;
+            m64[2 * m + 1] += w * zp.y;
             zp = cmul(zp, zi);
         }
-        const double d = mu0 - ec;
-        acc[2 + 2 * kMuMomP] += w * d / (d * d + wn * wn);
+        const float wf = (float)w;
+        const float2 zf = make_float2((float)zi.x, (float)zi.y);
+        float2 zq = make_float2((float)zp.x, (float)zp.y);
+#pragma unroll
+        for (int m = 0; m < P32; ++m) {
+            m32[2 * m] += wf * zq.x;
+            m32[2 * m + 1] += wf * zq.y;
+            zq = make_float2(zq.x * zf.x - zq.y * zf.y, zq.x * zf.y + zq.y * zf.x);
+        }
+        g0 -= w * x * inv;
     };
     const double4 *row = reinterpret_cast<const double4 *>(S + (size_t)blk * 4 * NO);
     for (int j = threadIdx.x; j < NO; j += blockDim.x) {
@@ -326,30 +350,42 @@ __global__ void __launch_bounds__(256)
                                make_double2(q.z, q.w)};
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            if (ww[c] == 0.0) continue;
+            const double w = cw[c];
+            if (w == 0.0) continue;
             double rS, iS;
             sigma_full(i1, sinf, c2[c], c3[c], sv[c], rS, iS);
-            const double w8 = 0.5 * ww[c], x = e[c] - mu0;
-            const double tmp = w8 * T * 2 / (nk02 * (wn * wn + x * x));
-            acc[0] += tmp * (rS * (-x) + iS * wn);
-            acc[1] += w8 * sinf * T * 2 / (nk02 * (wn * wn + x * x));
-            if (j >= jc) moments(wn, rS, iS, e[c], ww[c]);
+            const double x = cx[c];
+            const double inv = 1.0 / (wn * wn + x * x);
+            tsg += w * inv * (rS * (-x) + iS * wn);
+            har += w * inv;
+            if (j >= jc) moments(wn, rS, iS, x, w, inv);
         }
     }
     for (int t = threadIdx.x; t <= NO; t += blockDim.x) {
         const double wn = (2 * (NO + t) + 1) * pt, i1 = 1.0 / wn, i2 = i1 * i1;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            if (ww[c] == 0.0) continue;
-            moments(wn, -c2[c] * i2 + c4[c] * i2 * i2, -sinf * i1 + c3[c] * i2 * i1, e[c], ww[c]);
+            const double w = cw[c];
+            if (w == 0.0) continue;
+            const double x = cx[c];
+            moments(wn, -c2[c] * i2 + c4[c] * i2 * i2, -sinf * i1 + c3[c] * i2 * i1, x, w,
+                    1.0 / (wn * wn + x * x));
         }
     }
+    double acc[NV];
+    acc[0] = tsg * T / nk02;
+    acc[1] = har * sinf * T / nk02;
+#pragma unroll
+    for (int k = 0; k < 2 * P64; ++k) acc[2 + k] = m64[k];
+#pragma unroll
+    for (int k = 0; k < 2 * P32; ++k) acc[2 + 2 * P64 + k] = (double)m32[k];
+    acc[2 + 2 * kMuMomP] = g0;
     // traceSelfG's Fermi-function term per octant point
     if (threadIdx.x < 4) {
         const int c = threadIdx.x;
-        const double w8 = 0.5 * ww[c];
+        const double w8 = 0.5 * cw[c];
         if (w8 != 0.0) {
-            const double x = e[c] - mu0;
+            const double x = cx[c];
             if (fabs(x) > 1.0e-12) {
                 acc[1] += w8 * sinf * (1.0 / (exp(x / T) + 1.0) - 0.5) / x / nk02;
             } else {
@@ -366,7 +402,7 @@ struct MuRootArgs {
     const double *s2, *s3, *s4, *sinf, *ek, *w16;
     const double *mom;  // the k_sigma_moments results
     int nw0, nblk, jc;
-    double mu0, T, nk02, dmax;
+    double mu0, T, nk02, wc;  // wc = w_jc
     double *partial;  // [2][2 kRootMaxBlocks]
     unsigned *bar;
     int *err;
@@ -381,6 +417,9 @@ __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
     const int NO = a.nw0 / 2;
     const double sinf = a.sinf[0];
     const double pt = 3.141592653589793 * a.T;
+    // the series holds while |mu - mu0| <= kMuSeriesMax |z|_min, |z|_min = w_jc - 2 |Sigma_inf| / w_jc
+    const double zmin = a.wc - 2.0 * fabs(sinf) / a.wc;
+    const double dmax = zmin > 0.0 ? kMuSeriesMax * zmin : 0.0;
     int parity = 0;
     if (threadIdx.x == 0) {
         sc.lo = -10.0;
@@ -393,7 +432,7 @@ __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
 #pragma unroll 1
     while (!sc.done) {
         const double pmu = sc.x, delta = pmu - a.mu0;
-        const bool series = fabs(delta) <= a.dmax;
+        const bool series = fabs(delta) <= dmax;
         const int jhi = series ? a.jc : NO;
         double v = 0.0, dv = 0.0;
         const long long total = (long long)a.nblk * jhi;
@@ -537,7 +576,7 @@ cudaError_t launch_sigma_moments(const GridDev &g, const double2 *S, const doubl
 }
 
 cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2, const double *s3, const double *s4,
-                            const double *sinf, const double *mom, double mu0, double T, int jc, double dmax,
+                            const double *sinf, const double *mom, double mu0, double T, int jc, double wc,
                             RootScratch rs, cudaStream_t st) {
     int grid = 0;
     cudaError_t e = root_grid(k_mu_roots, &grid);
@@ -558,7 +597,7 @@ cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2
     a.mu0 = mu0;
     a.T = T;
     a.nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
-    a.dmax = dmax;
+    a.wc = wc;
     a.partial = rs.partial;
     a.bar = rs.bar;
     a.err = reinterpret_cast<int *>(rs.bar + 2);
