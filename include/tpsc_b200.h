@@ -225,7 +225,10 @@ int tpsc_get_stream(tpsc_ctx *ctx, void **stream);
  *  6 Sigma tau transform  7 one spin sum-rule evaluation at Usp
  *  8 one Tr(G-G0) evaluation at mu   9 stages 1 and 2 back to back
  *  10 one Newton-form sum-rule evaluation at Usp (stored frequencies below
- *     the series cut)   11 one Newton-form Tr(G-G0) evaluation at mu.
+ *     the series cut)   11 one Newton-form Tr(G-G0) evaluation at mu
+ *  12 the Newton-form sum-rule moments (per frequency, tail, suffix sums)
+ *  13 the device Usp/Uch root search   14 the Sigma moment pass (Tr Sigma G0
+ *     and the find_mu series)   15 stage 14 followed by the device mu search.
  * Requires a completed tpsc_solve.  Stages 2 and 4 transform in place and
  * expect stage 1 (resp. 3) to have run just before; launching the stages in
  * increasing order leaves the state as the solve left it. */

@@ -61,7 +61,8 @@ FORM_REFERENCE, FORM_NEWTON, FORM_MIXED = 0, 1, 2
 
 # tpsc_run_kernel stage ids
 KERNELS = ["gslice", "chi0_slice", "chi0_tau", "vertex_q", "vertex_tau", "sigma_slice", "sigma_tau",
-           "sumrule", "trace_diff_G", "chi0_slice+tau", "sumrule_newton", "trace_diff_G_newton"]
+           "sumrule", "trace_diff_G", "chi0_slice+tau", "sumrule_newton", "trace_diff_G_newton",
+           "sumrule_moments", "sumrule_roots", "sigma_moments", "sigma_moments+mu_roots"]
 
 STATUS = {0: "OK", 1: "bad argument", 2: "CUDA error", 3: "out of device memory",
           4: "root not found", 5: "stage prerequisite missing", 6: "non-finite result"}

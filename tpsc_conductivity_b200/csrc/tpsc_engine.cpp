@@ -1682,6 +1682,31 @@ int tpsc_run_kernel(tpsc_ctx *ctx, int which) {
                                    ctx->red, ctx->st, jc));
             break;
         }
+        case 12:
+            // the Newton-form sum-rule moments: per-frequency moments, tail, suffix sums
+            g->have_mom = false;
+            if ((rc = ensure_moments(ctx, g))) return rc;
+            break;
+        case 13:
+            // the device Usp/Uch root search of the Newton form
+            if ((rc = ensure_moments(ctx, g))) return rc;
+            CK(launch_sumrule_roots(d, g->chiq, g->cinf, g->cinf2, g->d_mom_suf, g->d_cmax_suf, g->d_tailm, ctx->T,
+                                    ctx->n, ctx->nsr, ctx->U, 2.0 / ctx->scal[TPSC_S_CHI0MAX] - 2 * EPS, ctx->roots,
+                                    ctx->st));
+            break;
+        case 14:
+        case 15: {
+            // 14: the Sigma moment pass (Tr Sigma G0 and the find_mu series);
+            // 15: that pass followed by the device mu search
+            int jc;
+            double wc;
+            mu_series_cut(ctx, &jc, &wc);
+            CK(launch_sigma_moments(d, g->S, g->s2, g->s3, g->s4, g->sinf, g->mu0, ctx->T, jc, ctx->redm, ctx->st));
+            if (which == 15)
+                CK(launch_mu_roots(d, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->redm.result, g->mu0, ctx->T, jc, wc,
+                                   ctx->roots, ctx->st));
+            break;
+        }
         default: return fail(ctx, TPSC_ERR_ARG, "unknown stage");
     }
     return TPSC_OK;
@@ -1723,6 +1748,25 @@ int tpsc_kernel_bytes(tpsc_ctx *ctx, int which, double *bytes) {
             double wc;
             mu_series_cut(ctx, &jc, &wc);
             b = (double)jc * d.n8 * 2 * s;
+            break;
+        }
+        case 12: b = half + 2 * d.n8 * s; break;       // read chi0(q, iqn), chi0_inf, chi0_inf2
+        case 13: {                                     // every evaluation reads chi0(q, iqn), j < jdir
+            Grid *g = ctx->cur;
+            int rc2 = ensure_moments_host(ctx, g);
+            if (rc2) return rc2;
+            int js, jch, tail;
+            series_cut(g, ctx->Usp, &js, &tail);
+            series_cut(g, ctx->Uch, &jch, &tail);
+            b = (ctx->scal[TPSC_S_EVALS_SP] * js + ctx->scal[TPSC_S_EVALS_CH] * jch) * d.n8 * s;
+            break;
+        }
+        case 14: b = cplx; break;                      // read S
+        case 15: {                                     // the pass, then per evaluation S, j < jc, and one full pass
+            int jc;
+            double wc;
+            mu_series_cut(ctx, &jc, &wc);
+            b = 2 * cplx + ctx->scal[TPSC_S_EVALS_MU] * jc * d.n8 * 2 * s;
             break;
         }
         default: return fail(ctx, TPSC_ERR_ARG, "unknown stage");
