@@ -120,6 +120,14 @@ int tpsc_find_Usp_Uch_grid(tpsc_ctx *ctx, int nq0, int nw0, double Usc[2]);
  * difRel diagnostics and the double occupancy ansatz. */
 int tpsc_find_Usp_Uch(tpsc_ctx *ctx);
 
+/* chi::sp_corr_length (src/chi.cpp:420-718) on the current grid after its
+ * chi0 and Usp: the Fermi velocity at the hot spots of the non-interacting
+ * Fermi surface (green0::find_FS with 10001 lines, src/green0.cpp:626-676)
+ * and the spin correlation lengths from chi_sp(q, 0) = chi0/(1 - Usp chi0/2):
+ * out = {vF, xi_y, xi_x, xiAs_y, xiAs_x, xi0_y, xi0_x} -- half-maximum
+ * lengths along y and x, asymptotic (Ornstein-Zernike) lengths, and xi0. */
+int tpsc_sp_corr_length(tpsc_ctx *ctx, double out[7]);
+
 /* chi::calc_chirt (src/chi.cpp:37-170): V(r, tau) on tau in [0, beta/2]. */
 int tpsc_vertex(tpsc_ctx *ctx);
 

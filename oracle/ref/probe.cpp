@@ -11,7 +11,8 @@
  * usage: tpsc_ref_probe OUTDIR MODE U tp tpp t3 n T nk0 Nw0
  *   MODE chi0   chi0::calc_chiqw_FFT_spline(nk0, Nw0)            (chi0.cpp:279)
  *        solve  green::calc_Self_FFT_spline(); traceSelfG(); find_mu()
- *               (green.cpp:1673, 3001, 3185) -- the full TPSC solve
+ *               (green.cpp:1673, 3001, 3185) -- the full TPSC solve -- then
+ *               chi::sp_corr_length() (chi.cpp:450) on the full-grid chi0
  *        cond   solve + cond_opt::calc_chijj_vertex_corr_all_optim(false,3,N,NULL,0)
  *               (cond_opt.cpp:2537), N = $TPSC_PROBE_NTHETA (default 1) angle bins
  *        post   solve + find_FS_inter, MDC(10 points, w=0, 4 etas), Gwn_local
@@ -61,6 +62,14 @@ public:
         write(dir + "/sigma_inf2.bin", Sigma_inf2, n8);
         write(dir + "/sigma_inf3.bin", Sigma_inf3, n8);
         write(dir + "/sigma_inf4.bin", Sigma_inf4, n8);
+    }
+
+    // chi::sp_corr_length (src/chi.cpp:450-718) on the full-grid chi0 and Usp,
+    // with the Fermi surface green0::find_FS(10001) computed at construction
+    void dump_corr(FILE *meta) {
+        sp_corr_length();
+        fprintf(meta, "vF %.17g\nxi_y %.17g\nxi_x %.17g\nxiAs_y %.17g\nxiAs_x %.17g\nxi0_y %.17g\nxi0_x %.17g\n",
+                vF, spCorrLgth_y, spCorrLgth_x, spCorrLgthAs_y, spCorrLgthAs_x, xi0_y, xi0_x);
     }
 
     void dump_cond(FILE *meta, const std::string &dir) {
@@ -159,6 +168,7 @@ int main(int argc, char **argv) {
         fprintf(meta, "t_self %.6f\nt_traceSelfG %.6f\nt_find_mu %.6f\n", t_self, t_tr, t_mu);
         g->dump_chi0(meta, absdir);
         g->dump_solve(meta, absdir);
+        g->dump_corr(meta);
         if (mode == "post" || mode == "cond") {
             // the post-processing tpsc_main.cpp runs after find_mu (lines 77-114)
             g->find_FS_inter();

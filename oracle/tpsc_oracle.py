@@ -1048,3 +1048,139 @@ def conductivity(sv: Solve, tp, tpp, t3, U, T, ntheta=1) -> CondResult:
         w2 = np.where((mm == 0) | (mm == nbk - 1), 1.0, 2.0)
         k0sum -= np.sum(2.0 * w2 * normFact * d2ek[l, :] * kk)
     return CondResult(chijj1, chijj2, float(k0sum.real), chijj1_k, chijj2_k)
+
+
+# ----------------------------------------------------------------------------
+# spin correlation length (chi::sp_corr_length, src/chi.cpp:450-718) with the
+# Fermi velocity at the hot spots (chi::vF_hot_spots, src/chi.cpp:420-447) on
+# the non-interacting Fermi surface (green0::find_FS, src/green0.cpp:626-676)
+# ----------------------------------------------------------------------------
+def dispk(kx, ky, tp, tpp, t3):
+    """hamiltonien::dispk (src/hamiltonien.cpp:119-122), scalar, libm cos (NaN
+    for a non-finite argument, as C's cos)."""
+
+    def c(x):
+        return math.cos(x) if math.isfinite(x) else math.nan
+
+    return (-2.0 * (c(kx) + c(ky)) - 4.0 * tp * c(kx) * c(ky) - 2.0 * tpp * (c(2 * kx) + c(2 * ky))
+            - 4 * t3 * (c(2 * kx) * c(ky) + c(2 * ky) * c(kx)))
+
+
+def find_fs(mu0, tp, tpp, t3, nk=10001):
+    """green0::find_FS(nk): on each line kx - ky = kx0, kx0 = j pi/(nk-1), the
+    root kx in [kx0, pi] of eps(kx, kx - kx0) - mu0 by the bounded find_zero
+    from init {(kx0 + pi)/2, kx0, pi}; stops at the first line without a root.
+    Returns the list of (kx, ky); lines after a failure are absent."""
+    fs = []
+    for j in range(nk):
+        kx0 = j * PI / (nk - 1)
+        init = (0.5 * (kx0 + PI), kx0, PI)
+        try:
+            root, _ = find_zero(lambda kx: dispk(kx, kx - kx0, tp, tpp, t3) - mu0, init, lims=(kx0, PI))
+        except RootNotFound:
+            break
+        fs.append((root, root - kx0))
+    return fs
+
+
+def vf_hot_spots(fs, tp, tpp, t3, nk=10001):
+    """chi::vF_hot_spots: first pair of consecutive Fermi-surface points whose
+    kx + ky - pi changes sign (or the last pair), |grad eps| at their midpoint.
+    Points of lines without a root read as (-1, -1), as the reference's array."""
+    pts = list(fs) + [(-1.0, -1.0)] * (nk - len(fs))
+    kx1, ky1 = pts[0]
+    kx2, ky2 = pts[1]
+    j = 1
+    while (kx1 + ky1 - PI) * (kx2 + ky2 - PI) > 0 and j < nk - 1:
+        j += 1
+        kx1, ky1 = kx2, ky2
+        kx2, ky2 = pts[j]
+    kx, ky = (kx1 + kx2) / 2, (ky1 + ky2) / 2
+    s, c = math.sin, math.cos
+    gx = 2.0 * s(kx) + 4.0 * tp * s(kx) * c(ky) + 4.0 * tpp * s(2 * kx) + 4 * t3 * (2.0 * s(2 * kx) * c(ky) + c(2 * ky) * s(kx))
+    gy = 2.0 * s(ky) + 4.0 * tp * c(kx) * s(ky) + 4.0 * tpp * s(2 * ky) + 4 * t3 * (c(2 * kx) * s(ky) + 2.0 * s(2 * ky) * c(kx))
+    return math.sqrt(gx * gx + gy * gy)
+
+
+def sp_corr_length(chi0_q0, chi0max, qmax, Usp, nbq, mu0, tp, tpp, t3, nk_fs=10001):
+    """chi::sp_corr_length: the spin correlation lengths along y and x from the
+    half maximum of chi_sp(q, 0) = chi0/(1 - Usp chi0/2) around qmax on the
+    lattice, and from the asymptotic (Ornstein-Zernike) form with the second
+    difference of chi0 at qmax; vF from vF_hot_spots.  chi0_q0 is chi0(q, 0) in
+    the octant layout m + l(l+1)/2.  Returns dict vF, xi_y, xi_x, xiAs_y,
+    xiAs_x, xi0_y, xi0_x."""
+    vF = vf_hot_spots(find_fs(mu0, tp, tpp, t3, nk_fs), tp, tpp, t3, nk_fs)
+    a = np.asarray(chi0_q0, dtype=np.float64)
+
+    def csp(i):
+        return a[i] / (1.0 - Usp * a[i] / 2.0)
+
+    def oi(x, y):
+        return y + (x * (x + 1)) // 2
+
+    q0x, q1x = int(qmax[0]), int(qmax[1])
+    dq = PI / (nbq - 1)
+    half = chi0max / (1.0 - Usp * chi0max / 2.0) / 2.0
+    # along y at kx = qmax_x
+    l, m = q0x, 0
+    base = (l * (l + 1)) // 2
+    cur = csp(base)
+    prev = cur
+    while cur < half and m <= q1x:
+        m += 1
+        prev = cur
+        cur = csp(base + m)
+    q0 = (m - 1) * dq
+    qHM = dq * (half - prev) / (cur - prev) + q0
+    xi_y = 1.0 / (q1x * dq - qHM)
+    # along x at ky = qmax_y, from the diagonal
+    m = q1x
+    l = m
+    cur = csp(oi(l, m))
+    if cur < half:
+        while cur < half and l <= q0x:
+            l += 1
+            prev = cur
+            cur = csp(oi(l, m))
+        q0 = (l - 1) * dq
+        qHM = dq * (half - prev) / (cur - prev) + q0
+        xi_x = 1.0 / (q0x * dq - qHM)
+    else:
+        xi_x = xi_y
+    # asymptotic form
+    fac = (nbq - 1) * (nbq - 1) / (PI * PI)
+    if q0x == nbq - 1 and q1x == nbq - 1:
+        dchi2 = 2.0 * (a[base + nbq - 2] - chi0max) * fac
+        xi0_x = math.sqrt(-0.5 * dchi2 / chi0max)
+        xiAs_x = xi0_x * math.sqrt(Usp / (2.0 / chi0max - Usp))
+        xi0_y, xiAs_y = xi0_x, xiAs_x
+    else:
+        x, y = q0x, q1x - 1
+        if y < 0:
+            y = q1x + 1
+        cl = a[oi(x, y)]
+        y = q1x
+        cm = a[oi(x, y)]
+        y = q1x + 1
+        if y > x:
+            x, y = q1x + 1, q0x
+        cr = a[oi(x, y)]
+        dchi2 = (cr - 2 * cm + cl) * fac
+        xi0_y = math.sqrt(-0.5 * dchi2 / chi0max)
+        xiAs_y = xi0_y * math.sqrt(Usp / (2.0 / chi0max - Usp))
+        x, y = q0x - 1, q1x
+        if y > x:
+            x, y = q1x, q0x - 1
+            if y < 0:
+                y = q0x + 1
+        cl = a[oi(x, y)]
+        x, y = q0x, q1x
+        cm = a[oi(x, y)]
+        x = q0x + 1
+        if x > nbq - 1:
+            x = q0x - 1
+        cr = a[oi(x, y)]
+        dchi2 = (cr - 2 * cm + cl) * fac
+        xi0_x = math.sqrt(-0.5 * dchi2 / chi0max)
+        xiAs_x = xi0_x * math.sqrt(Usp / (2.0 / chi0max - Usp))
+    return dict(vF=vF, xi_y=xi_y, xi_x=xi_x, xiAs_y=xiAs_y, xiAs_x=xiAs_x, xi0_y=xi0_y, xi0_x=xi0_x)

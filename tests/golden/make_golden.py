@@ -88,6 +88,9 @@ def run_case(name, spec, threads):
             "ref_seconds": np.array([float(meta.get(k, 0.0)) for k in
                                      ["t_self", "t_traceSelfG", "t_find_mu"]]),
             "ref_threads": np.array(int(meta["omp_threads"])),
+            # chi::sp_corr_length (src/chi.cpp:450-718) after the solve
+            "corr_names": np.array(["vF", "xi_y", "xi_x", "xiAs_y", "xiAs_x", "xi0_y", "xi0_x"]),
+            "corr": np.array([float(meta[k]) for k in ["vF", "xi_y", "xi_x", "xiAs_y", "xiAs_x", "xi0_y", "xi0_x"]]),
         }
         chiqw = rd("chiqw.bin", (nw, n8))
         V = rd("vertex_rt.bin", (nw, n8))

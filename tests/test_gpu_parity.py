@@ -127,6 +127,37 @@ def test_l256_scalars_match_reference(ctx):
     assert rel(se["S"][:, cols], g["self_cols"]) < 1e-7
 
 
+@pytest.mark.parametrize("name", golden_names())
+def test_sp_corr_length_matches_reference(ctx, name):
+    """chi::sp_corr_length (src/chi.cpp:450-718) after the solve, through the C
+    ABI: vF at the hot spots and the spin correlation lengths vs the
+    reference's; they follow chi0(q, 0) and Usp, so the bound is the solve's."""
+    g = load_golden(name)
+    p = g["p"]
+    gr = make(ctx, p)
+    gr.solve()
+    r = gr.sp_corr_length()
+    for k, v in zip(g["corr_names"], g["corr"]):
+        assert abs(r[str(k)] - v) <= 1e-9 * abs(v), (k, r[str(k)], v)
+    # vF depends on the dispersion and mu0 only: the reference's to rounding
+    assert abs(r["vF"] - g["corr"][0]) <= 1e-13 * g["corr"][0]
+
+
+def test_sp_corr_length_needs_usp(ctx):
+    from tpsc_conductivity_b200 import _lib
+
+    g = load_golden("l16_w64_u2")
+    gr = make(ctx, g["p"])
+    with pytest.raises(_lib.TPSCError):
+        gr.sp_corr_length()
+    gr.calc_chiqw_FFT_spline()
+    with pytest.raises(_lib.TPSCError):
+        gr.sp_corr_length()
+    gr.find_Usp_Uch()
+    r = gr.sp_corr_length()
+    assert abs(r["xi_y"] - g["corr"][1]) <= 1e-9 * g["corr"][1]
+
+
 @pytest.mark.parametrize("name", ["l32_w256_u4_tp", "l16_w128_n110", "l16_w64_half", "l256_w4096_u4"])
 def test_newton_form_same_roots(ctx, name):
     """The Newton form reaches the reference's Usp, Uch and mu (to the

@@ -26,6 +26,7 @@ SIGNATURES = [
     ("tpsc_trace_diff_chi", C.c_int, [C.c_void_p, C.c_int, C.c_double, _dp, _dp]),
     ("tpsc_find_Usp_Uch_grid", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),
     ("tpsc_find_Usp_Uch", C.c_int, [C.c_void_p]),
+    ("tpsc_sp_corr_length", C.c_int, [C.c_void_p, _dp]),
     ("tpsc_vertex", C.c_int, [C.c_void_p]),
     ("tpsc_self_energy", C.c_int, [C.c_void_p]),
     ("tpsc_trace_self_G", C.c_int, [C.c_void_p, _dp]),

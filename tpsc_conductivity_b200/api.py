@@ -89,6 +89,14 @@ class Green:
         """chi::find_Usp_Uch() (src/chi.cpp:210): half grid, full grid, dblOcc."""
         self.ctx.call("tpsc_find_Usp_Uch")
 
+    def sp_corr_length(self):
+        """chi::sp_corr_length (src/chi.cpp:450-718) after find_Usp_Uch: the Fermi
+        velocity at the hot spots and the spin correlation lengths (half maximum
+        of chi_sp(q, 0) along y and x, asymptotic form, xi0)."""
+        out = np.zeros(7)
+        self.ctx.call("tpsc_sp_corr_length", _dptr(out))
+        return dict(zip(["vF", "xi_y", "xi_x", "xiAs_y", "xiAs_x", "xi0_y", "xi0_x"], out.tolist()))
+
     def calc_chirt(self):
         """chi::calc_chirt (src/chi.cpp:37)."""
         self.ctx.call("tpsc_vertex")

@@ -284,6 +284,7 @@ struct Grid {
     double2 *S = nullptr;         // blocked Nw0/2       coefficient of 1/z^4
     double *s2 = nullptr, *s3 = nullptr, *s4 = nullptr, *sinf = nullptr;
     bool have_chi0 = false, have_V = false, have_S = false;
+    bool have_U = false;  // Usp, Uch found from this grid's chi0
     bool g_mixed = false;         // G(r, tau) of the last chi0 stage is Grt32
     long long model_id = -1;      // the model (tpsc_set_model call) the eps_k tables and mu0 belong to
     // Newton form: moments of chi0 for the high-frequency sum-rule series
@@ -624,7 +625,7 @@ int switch_grid(tpsc_ctx *ctx, int nk0, int nw0) {
         if (rc) return rc;
         g->model_id = ctx->model_id;
     }
-    g->have_chi0 = g->have_V = g->have_S = g->have_mom = false;
+    g->have_chi0 = g->have_V = g->have_S = g->have_mom = g->have_U = false;
     ctx->cur = g;
     ctx->scal[TPSC_S_MU0] = g->mu0;
     return TPSC_OK;
@@ -682,7 +683,7 @@ int run_chi0(tpsc_ctx *ctx) {
     ctx->scal[TPSC_S_QMAX0] = r[1];
     ctx->scal[TPSC_S_QMAX1] = r[2];
     g->have_chi0 = true;
-    g->have_V = g->have_S = g->have_mom = false;
+    g->have_V = g->have_S = g->have_mom = g->have_U = false;
     if (!std::isfinite(r[0]) || r[0] <= 0.0) return fail(ctx, TPSC_ERR_NONFINITE, "chi0(q, 0) has no positive maximum");
     return TPSC_OK;
 }
@@ -803,6 +804,7 @@ int roots_Usp_Uch(tpsc_ctx *ctx, double Usc[2]) {
         ctx->scal[TPSC_S_EVALS_CH] = r[3];
         ctx->scal[TPSC_S_USP] = ctx->Usp;
         ctx->scal[TPSC_S_UCH] = ctx->Uch;
+        ctx->cur->have_U = true;
         return TPSC_OK;
     }
     // R_sp(Us) = trace + n - n^2/2 - nsr + Us nsr^2/(2U)  (chi::sum_rule_sp, src/chi.cpp:833-836)
@@ -858,6 +860,7 @@ int roots_Usp_Uch(tpsc_ctx *ctx, double Usc[2]) {
     ctx->Uch = root;
     ctx->scal[TPSC_S_USP] = ctx->Usp;
     ctx->scal[TPSC_S_UCH] = ctx->Uch;
+    ctx->cur->have_U = true;
     return TPSC_OK;
 }
 
@@ -1241,7 +1244,8 @@ int tpsc_set_model(tpsc_ctx *ctx, int nk0, int Nw0, double n, double T, double t
     ctx->nsr = n > 1.0 ? 2.0 - n : n;  // src/chi.cpp:18-19
     ctx->Usp = ctx->Uch = 0.0;
     for (double &s : ctx->scal) s = 0.0;
-    for (auto &kv : ctx->grids) kv.second->have_chi0 = kv.second->have_V = kv.second->have_S = false;
+    for (auto &kv : ctx->grids)
+        kv.second->have_chi0 = kv.second->have_V = kv.second->have_S = kv.second->have_U = false;
     ctx->have_model = true;
     ++ctx->model_id;
     return switch_grid(ctx, nk0, Nw0);
@@ -1286,6 +1290,152 @@ int tpsc_find_Usp_Uch_grid(tpsc_ctx *ctx, int nq0, int nw0, double Usc[2]) {
     int rc = tpsc_chi0(ctx, nq0, nw0);
     if (rc) return rc;
     return roots_Usp_Uch(ctx, Usc);
+}
+
+// ---------------------------------------------------------------------------
+// spin correlation length: host post-processing of chi0(q, 0) and Usp
+// ---------------------------------------------------------------------------
+
+// green0::find_FS(nk) (src/green0.cpp:626-676): on each line kx - ky = kx0,
+// kx0 = j pi/(nk - 1), the root kx in [kx0, pi] of eps(kx, kx - kx0) - mu0 by
+// the bounded find_zero from {(kx0 + pi)/2, kx0, pi}; the first line without
+// a root ends the search and the later points stay (-1, -1).
+void find_fs(const tpsc_ctx *ctx, double mu0, int nk, std::vector<double> &fs) {
+    fs.assign(2 * (size_t)nk, -1.0);
+    for (int j = 0; j < nk; ++j) {
+        const double kx0 = j * PI / (nk - 1);
+        const double init[3] = {0.5 * (kx0 + PI), kx0, PI}, lims[2] = {kx0, PI};
+        auto f = [&](double kx, double &y) -> bool {
+            y = dispk(kx, kx - kx0, ctx->tp, ctx->tpp, ctx->t3) - mu0;
+            return true;
+        };
+        double root = 0.0;
+        int nev;
+        bool derr;
+        if (!find_zero(f, init, &root, lims, &nev, &derr)) break;
+        fs[2 * (size_t)j] = root;
+        fs[2 * (size_t)j + 1] = root - kx0;
+    }
+}
+
+// chi::vF_hot_spots (src/chi.cpp:420-447): the first pair of consecutive
+// Fermi-surface points across kx + ky = pi (or the last pair), |grad eps| at
+// their midpoint (hamiltonien::grad_ek, src/hamiltonien.cpp:125-131).
+double vf_hot_spots(const tpsc_ctx *ctx, const std::vector<double> &fs, int nk) {
+    double kx1 = fs[0], ky1 = fs[1], kx2 = fs[2], ky2 = fs[3];
+    int j = 1;
+    while ((kx1 + ky1 - PI) * (kx2 + ky2 - PI) > 0 && j < nk - 1) {
+        ++j;
+        kx1 = kx2;
+        ky1 = ky2;
+        kx2 = fs[2 * (size_t)j];
+        ky2 = fs[2 * (size_t)j + 1];
+    }
+    const double kx = (kx1 + kx2) / 2, ky = (ky1 + ky2) / 2;
+    const double tp = ctx->tp, tpp = ctx->tpp, t3 = ctx->t3;
+    const double gx = 2.0 * std::sin(kx) + 4.0 * tp * std::sin(kx) * std::cos(ky) + 4.0 * tpp * std::sin(2 * kx) +
+                      4 * t3 * (2.0 * std::sin(2 * kx) * std::cos(ky) + std::cos(2 * ky) * std::sin(kx));
+    const double gy = 2.0 * std::sin(ky) + 4.0 * tp * std::cos(kx) * std::sin(ky) + 4.0 * tpp * std::sin(2 * ky) +
+                      4 * t3 * (std::cos(2 * kx) * std::sin(ky) + 2.0 * std::sin(2 * ky) * std::cos(kx));
+    return std::sqrt(gx * gx + gy * gy);
+}
+
+int tpsc_sp_corr_length(tpsc_ctx *ctx, double out[7]) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    if (!out) return fail(ctx, TPSC_ERR_ARG, "null output");
+    Grid *g = ctx->cur;
+    if (!g || !g->have_chi0 || !g->have_U)
+        return fail(ctx, TPSC_ERR_STATE, "chi0 and Usp have not been computed on the current grid");
+    cudaSetDevice(ctx->device);
+    const GridDev &d = g->d;
+    const int nbq = d.nbk;
+    // chi0(q, 0): row j = 0 of the column-block layout, 4 columns per block
+    std::vector<double> a((size_t)d.n8p);
+    CK(cudaMemcpy2DAsync(a.data(), 4 * sizeof(double), g->chiq, (size_t)d.nb * 4 * sizeof(double),
+                         4 * sizeof(double), d.n8p / 4, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    const int nkfs = 10001;
+    std::vector<double> fs;
+    find_fs(ctx, g->mu0, nkfs, fs);
+    const double vF = vf_hot_spots(ctx, fs, nkfs);
+    // chi::sp_corr_length (src/chi.cpp:450-718): half maximum of
+    // chi_sp(q, 0) = chi0/(1 - Usp chi0/2) around qmax along y and x, and the
+    // asymptotic (Ornstein-Zernike) lengths from the second difference of chi0
+    const double Usp = ctx->Usp, chi0max = ctx->scal[TPSC_S_CHI0MAX];
+    const int qx = (int)ctx->scal[TPSC_S_QMAX0], qy = (int)ctx->scal[TPSC_S_QMAX1];
+    auto csp = [&](size_t i) { return a[i] / (1.0 - Usp * a[i] / 2.0); };
+    auto oi = [](int x, int y) { return (size_t)y + ((size_t)x * (x + 1)) / 2; };
+    const double dq = PI / (nbq - 1), half = chi0max / (1.0 - Usp * chi0max / 2.0) / 2.0;
+    int l = qx, m = 0;
+    const size_t base = ((size_t)l * (l + 1)) / 2;
+    double cur = csp(base), prev = cur;
+    while (cur < half && m <= qy) {
+        ++m;
+        prev = cur;
+        cur = csp(base + m);
+    }
+    double q0 = (m - 1) * dq;
+    double qHM = dq * (half - prev) / (cur - prev) + q0;
+    const double xi_y = 1.0 / (qy * dq - qHM);
+    double xi_x = xi_y;
+    m = qy;
+    l = m;
+    cur = csp(oi(l, m));
+    if (cur < half) {
+        while (cur < half && l <= qx) {
+            ++l;
+            prev = cur;
+            cur = csp(oi(l, m));
+        }
+        q0 = (l - 1) * dq;
+        qHM = dq * (half - prev) / (cur - prev) + q0;
+        xi_x = 1.0 / (qx * dq - qHM);
+    }
+    const double fac = (double)(nbq - 1) * (nbq - 1) / (PI * PI);
+    double xi0_x, xi0_y, xiAs_x, xiAs_y;
+    if (qx == nbq - 1 && qy == nbq - 1) {
+        const double dchi2 = 2.0 * (a[base + nbq - 2] - chi0max) * fac;
+        xi0_x = std::sqrt(-0.5 * dchi2 / chi0max);
+        xiAs_x = xi0_x * std::sqrt(Usp / (2.0 / chi0max - Usp));
+        xi0_y = xi0_x;
+        xiAs_y = xiAs_x;
+    } else {
+        int x = qx, y = qy - 1;
+        if (y < 0) y = qy + 1;
+        const double cl = a[oi(x, y)];
+        y = qy;
+        const double cm = a[oi(x, y)];
+        y = qy + 1;
+        if (y > x) {
+            x = qy + 1;
+            y = qx;
+        }
+        const double cr = a[oi(x, y)];
+        double dchi2 = (cr - 2 * cm + cl) * fac;
+        xi0_y = std::sqrt(-0.5 * dchi2 / chi0max);
+        xiAs_y = xi0_y * std::sqrt(Usp / (2.0 / chi0max - Usp));
+        x = qx - 1;
+        y = qy;
+        if (y > x) {
+            x = qy;
+            y = qx - 1;
+            if (y < 0) y = qx + 1;
+        }
+        const double dl = a[oi(x, y)];
+        x = qx;
+        y = qy;
+        const double dm = a[oi(x, y)];
+        x = qx + 1;
+        if (x > nbq - 1) x = qx - 1;
+        const double dr = a[oi(x, y)];
+        dchi2 = (dr - 2 * dm + dl) * fac;
+        xi0_x = std::sqrt(-0.5 * dchi2 / chi0max);
+        xiAs_x = xi0_x * std::sqrt(Usp / (2.0 / chi0max - Usp));
+    }
+    const double r[7] = {vF, xi_y, xi_x, xiAs_y, xiAs_x, xi0_y, xi0_x};
+    for (int i = 0; i < 7; ++i) out[i] = r[i];
+    return TPSC_OK;
 }
 
 int tpsc_find_Usp_Uch(tpsc_ctx *ctx) {

@@ -239,10 +239,49 @@ void chi::find_Usp_Uch() {
     params.close();
 }
 
+// chi::sp_corr_length (src/chi.cpp:450-718): the lengths from the engine, the
+// reference's lines on stdout and appended to TPSC_infos_*
 void chi::sp_corr_length() {
-    // needs the infinite-lattice Fermi surface (green0::find_FS, adaptive
-    // quadrature), which this build does not reproduce
-    cout << "sp_corr_length(): not available in this build\n";
+    if (!ctx_) return;
+    double r[7];
+    if (!check(tpsc_sp_corr_length(ctx_, r), "sp_corr_length")) return;
+    vF = r[0];
+    spCorrLgth_y = r[1];
+    spCorrLgth_x = r[2];
+    spCorrLgthAs_y = r[3];
+    spCorrLgthAs_x = r[4];
+    xi0_y = r[5];
+    xi0_x = r[6];
+    if (qmax[0] != (nbq - 1) || qmax[1] != (nbq - 1))
+        cout << "chisp incommensurable (formule asymptotique non valable)\n";
+    char name[300];
+    sprintf(name, "./TPSC_infos_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%d_%d.dat", U, tp, tpp, t3, density, tem,
+            2 * (nbq - 1), 2 * nwmax);
+    fstream infos;
+    infos.open(name, ios::out | ios::app);
+    infos << setprecision(16);
+    struct Line {
+        const char *what;
+        double xi;
+        bool th;
+    };
+    const Line lines[] = {
+        {"longueur de correlation de spin (1/(larg.mi-haut.)) (axe y):  ", spCorrLgth_y, true},
+        {"longueur de correlation de spin (1/(larg.mi-haut.)) (axe x):  ", spCorrLgth_x, true},
+        {"longueur de correlation de spin (formule asymptotique) (axe y):  ", spCorrLgthAs_y, false},
+        {"longueur de correlation de spin (formule asymptotique) (axe x):  ", spCorrLgthAs_x, false},
+    };
+    cout << "vitesse de Fermi aux points chauds:  " << vF << endl;
+    infos << "vitesse de Fermi aux points chauds:  " << vF << endl;
+    for (const Line &L : lines) {
+        const char *ratio = L.th ? "xi_sp/xi_th:  " : "xi_sp_As/xi_th:  ";
+        const char *prod = L.th ? "xi_sp*T:  " : "xi_sp_As*T:  ";
+        cout << L.what << L.xi << '\n' << ratio << L.xi * acos(-1.0) * tem / vF << '\n' << prod << L.xi * tem << '\n';
+        infos << L.what << L.xi << '\n' << ratio << L.xi * acos(-1.0) * tem / vF << '\n' << prod << L.xi * tem << '\n';
+    }
+    const double chisp_max = chi0max / (1.0 - Usp * chi0max / 2.0);
+    cout << "(max(chi_sp)/max(chi_0))^0.5:  " << sqrt(chisp_max / chi0max) << endl;
+    infos.close();
 }
 
 void chi::calc_chirt() {

@@ -101,6 +101,7 @@ public:
 protected:
     void calc_chirt();
     double Uch, Usp, dblOcc, nsr;
+    double spCorrLgth_x, spCorrLgth_y, spCorrLgthAs_x, spCorrLgthAs_y, xi0_x, xi0_y, vF;
     char paramsFileName[200];
 };
 
