@@ -304,6 +304,12 @@ def our_arm(a, world, rank, local_rank):
     peak, peak_kind = measured_hbm()
     traffic = profiled_traffic(dom)
 
+    # ---- the batched parameter sweep (512 seeded points, uneven lattices and
+    # cutoffs), mixed + Newton, on the tuned number of solver streams --------
+    batch = None
+    if world == 1 and not a.no_batch:
+        batch = batch_sweep(a.steps)
+
     if rank != 0:
         return
     line = {
@@ -315,7 +321,7 @@ def our_arm(a, world, rank, local_rank):
                            "transforms, tau transforms, sums, roots) + Newton root searches with moment series",
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "512 MB flush before every step; working set ~2.4 GB per solve",
-                   "sumrule_evals": counts["sumrule_newton"], "mu_evals": counts["trace_diff_G_newton"]},
+                   "sumrule_evals": int(sc["evals_sp"] + sc["evals_ch"]), "mu_evals": int(sc["evals_mu"])},
         "forms": {"mixed_newton": {"solves_per_s": value, "ms_per_step": ms / a.steps, "stage_ms": stages,
                                    "max_rel_dSigma_vs_fp64": dsigma},
                   "fp64_newton": {"solves_per_s": value_n64, "ms_per_step": ms_n64 / a.steps,
@@ -338,6 +344,8 @@ def our_arm(a, world, rank, local_rank):
         "clocks": clocks,
         "results": {k: sc[k] for k in ("Usp", "Uch", "dblOcc", "mu", "Sigma_inf")},
     }
+    if batch is not None:
+        line["batch"] = batch
     if world == 1 and not a.no_cpu_baseline:
         try:
             t, raw = run_reference_once(os.cpu_count() or 1)
@@ -349,6 +357,36 @@ def our_arm(a, world, rank, local_rank):
             line["cpu_baseline"] = {"value": None, "unit": "solves/s", "cores": 0, "kind": "reference",
                                     "sample": f"unavailable: {ex}"}
     print(json.dumps(line), flush=True)
+
+
+def batch_sweep(steps):
+    """The 512-point sweep through the batched sweep API: tuned stream count
+    (1, 2, 4, 8, 16 contexts timed on the sweep), then the sweep timed on that
+    count (best of a few calls).  Wall time from a device-idle start to a
+    device-idle end, host work included."""
+    from tpsc_conductivity_b200 import _lib
+    from tpsc_conductivity_b200.api import Batch, sweep_points
+
+    pts = sweep_points(512, seed=20261203)
+    form = _lib.FORM_NEWTON | _lib.FORM_MIXED
+    b = Batch(nstreams=1)
+    tune = b.tune(pts, form, max_streams=16)
+    times = []
+    st = None
+    for _ in range(max(1, min(steps, 5))):
+        _, st, ms = b.solve(pts, form)
+        times.append(ms)
+    nfail = int((st != 0).sum())
+    best = min(times)
+    shapes = sorted({(int(p[0]), int(p[1])) for p in pts})
+    out = {"workload": "512 solves from tpsc_sweep_points(seed 20261203): nk0 in {32,64,128,256}, U~U[1,6], "
+                       "n~U[0.7,1], log T~U[ln .03, ln .5], t'~U[-.3,0], Nw0 = 2 nextpow2(ceil(40/(pi T)))",
+           "form": "mixed + Newton", "shapes": len(shapes), "streams": b.nstreams,
+           "solves_per_s": 512 / (best / 1e3), "ms_per_sweep": best, "ms_per_sweep_all": times,
+           "sequential_solves_per_s": 512 / (tune[1] / 1e3), "tune_ms": tune, "failed_points": nfail,
+           "timing": "host wall clock around the whole call, device idle at both ends"}
+    b.close()
+    return out
 
 
 def profiled_traffic(kernel):
@@ -389,6 +427,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 512-point batched sweep")
     ap.add_argument("--nk0", type=int, default=None, help="lattice side override (profiling only)")
     ap.add_argument("--nw0", type=int, default=None, help="Nw0 override (profiling only)")
     a = ap.parse_args()

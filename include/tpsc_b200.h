@@ -274,6 +274,40 @@ int tpsc_launch_count(tpsc_ctx *ctx, long long *count);
 int tpsc_sumrule_noalloc(const double *chiqw, const double *chi0_inf, const double *chi0_inf2, int nk0, int Nw0,
                          double T, int channel, double Uv, double *out, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Batched sweep (no counterpart in the reference, which solves one parameter
+ * point per run; tpsc_batch.cpp): many independent solves with uneven
+ * lattices and Matsubara cutoffs on one GPU.  A batch owns nstreams solver
+ * contexts (own streams, scratch and per-shape grid cache, kept across
+ * calls) driven by one host thread each; the points of a call run largest
+ * first (nk0^2 Nw0), each on the next free context, so that small solves
+ * overlap on the GPU.  Not thread-safe: one call at a time per batch.
+ * ------------------------------------------------------------------------- */
+typedef struct tpsc_batch tpsc_batch;
+/* 1 <= nstreams <= 32; NULL and *status set on failure. */
+tpsc_batch *tpsc_batch_create(int device, int nstreams, int *status);
+void tpsc_batch_destroy(tpsc_batch *b);
+const char *tpsc_batch_last_error(const tpsc_batch *b);
+int tpsc_batch_streams(const tpsc_batch *b, int *nstreams);
+/* params: npts rows {nk0, Nw0, n, T, tp, tpp, t3, U} (row-major doubles);
+ * form: enum tpsc_form; results: npts rows of TPSC_S_COUNT scalars in the
+ * tpsc_get_scalars order (NaN for a failed point); status[i]: point i's
+ * status -- a failing point does not stop the others; ms (may be NULL): wall
+ * time of the call from a device-idle start to a device-idle end.  Returns
+ * TPSC_OK, or the status of the first failing point. */
+int tpsc_batch_solve(tpsc_batch *b, int form, int npts, const double *params, double *results, int *status,
+                     double *ms);
+/* The tuner: one untimed pass of the sample (allocating every shape on
+ * max_streams contexts), then the sample timed on 1, 2, 4, ... <= max_streams
+ * contexts; later tpsc_batch_solve calls use the fastest count.  ms (may be
+ * NULL) receives each count's time, floor(log2(max_streams)) + 1 entries. */
+int tpsc_batch_tune(tpsc_batch *b, int form, int npts, const double *params, int max_streams, double *ms);
+/* The parameter-sweep workload: npts rows in the tpsc_batch_solve layout
+ * from std::mt19937_64(seed), drawn per point in this order: nk0 uniform in
+ * {32, 64, 128, 256}, U ~ U[1, 6], n ~ U[0.7, 1], log T ~ U[ln 0.03, ln 0.5],
+ * t' ~ U[-0.3, 0]; t'' = t3 = 0 and Nw0 = 2 nextpow2(ceil(40 / (pi T))). */
+int tpsc_sweep_points(int npts, unsigned long long seed, double *params);
+
 #ifdef __cplusplus
 }
 #endif

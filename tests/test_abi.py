@@ -54,3 +54,35 @@ def test_create_without_device_fails_cleanly(lib):
     st = ctypes.c_int(-1)
     h = lib.tpsc_create(0, ctypes.byref(st))
     assert not h and st.value != 0
+
+
+def test_sweep_points_are_the_seeded_workload():
+    """tpsc_sweep_points (host only): deterministic for a seed, every point in
+    the ranges of the sweep, Nw0 = 2 nextpow2(ceil(40 / (pi T)))."""
+    import numpy as np
+
+    from tpsc_conductivity_b200.api import sweep_points
+
+    a = sweep_points(512)
+    b = sweep_points(512)
+    assert np.array_equal(a, b)
+    assert not np.array_equal(a, sweep_points(512, seed=1))
+    nk0, nw0, n, T, tp, tpp, t3, U = a.T
+    assert set(nk0.astype(int)) <= {32, 64, 128, 256} and len(set(nk0.astype(int))) == 4
+    assert np.all((U >= 1) & (U <= 6)) and np.all((n >= 0.7) & (n <= 1.0))
+    assert np.all((T >= 0.03) & (T <= 0.5)) and np.all((tp >= -0.3) & (tp <= 0))
+    assert np.all(tpp == 0) and np.all(t3 == 0)
+    pos = nw0 / 2
+    need = np.ceil(40 / (np.pi * T))
+    assert np.all(pos >= need) and np.all(pos / 2 < need)
+    assert np.all(np.log2(nw0) == np.round(np.log2(nw0)))
+
+
+def test_batch_create_without_device_fails_cleanly(lib):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    lib.tpsc_batch_create.restype = ctypes.c_void_p
+    st = ctypes.c_int(-1)
+    assert not lib.tpsc_batch_create(0, 4, ctypes.byref(st)) and st.value != 0

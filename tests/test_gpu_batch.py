@@ -1,0 +1,91 @@
+"""The batched sweep (tpsc_batch_*): many independent solves with uneven
+lattices and Matsubara cutoffs on one GPU, several solver contexts at once.
+
+Every point's scalars equal those of the same point solved alone through
+tpsc_solve (tolerance 1e-11 relative: the capped cooperative root grids of a
+batch sum their partials in another grouping), a failing point leaves the
+others intact, and the tuner keeps one of the counts it timed."""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ["mu0", "chi0max", "Usp", "Uch", "dblOcc", "Sigma_inf", "mu", "trSG2"]
+
+
+def _single(p, form):
+    from tpsc_conductivity_b200.api import Green
+
+    g = Green(int(p[0]), int(p[1]), p[2], p[3], 0.1, (p[4], p[5], p[6], p[7]))
+    g.set_form(form)
+    g.solve()
+    return g.scalars()
+
+
+@pytest.mark.parametrize("form_name", ["newton", "mixed_newton"])
+def test_batch_points_equal_single_solves(form_name):
+    from tpsc_conductivity_b200 import _lib
+    from tpsc_conductivity_b200.api import Batch, sweep_points
+
+    form = _lib.FORM_NEWTON | (_lib.FORM_MIXED if form_name == "mixed_newton" else 0)
+    pts = sweep_points(12, seed=7)
+    b = Batch(nstreams=4)
+    res, st, ms = b.solve(pts, form)
+    assert np.all(st == 0) and ms > 0
+    names = list(_lib.SCALARS)
+    for i, p in enumerate(pts):
+        ref = _single(p, form)
+        for k in KEYS:
+            v = res[i, names.index(k)]
+            assert abs(v - ref[k]) <= 1e-11 * max(1.0, abs(ref[k])), (i, k, v, ref[k])
+    # the same call again: the contexts and grids are reused, results repeat
+    res2, st2, _ = b.solve(pts, form)
+    assert np.all(st2 == 0)
+    assert np.array_equal(res[:, [names.index(k) for k in KEYS]], res2[:, [names.index(k) for k in KEYS]])
+
+
+def test_batch_reproduces_reference_scalars():
+    """Golden points solved inside one batch match the reference binary."""
+    from tpsc_conductivity_b200 import _lib
+    from tpsc_conductivity_b200.api import Batch
+
+    names = ["l16_w64_u2", "l32_w256_u4_tp", "l16_w128_n110", "l64_w1024_u4", "l32_w512_u2"]
+    rows = []
+    for nm in names:
+        p = load_golden(nm)["p"]
+        rows.append([p["nk0"], p["Nw0"], p["n"], p["T"], p["tp"], p["tpp"], p["t3"], p["U"]])
+    b = Batch(nstreams=3)
+    res, st, _ = b.solve(np.array(rows), _lib.FORM_REFERENCE)
+    assert np.all(st == 0)
+    sn = list(_lib.SCALARS)
+    for i, nm in enumerate(names):
+        s = load_golden(nm)["s"]
+        for k in ("Usp", "Uch", "dblOcc", "mu"):
+            assert abs(res[i, sn.index(k)] - s[k]) <= 1e-9 * max(1.0, abs(s[k])), (nm, k)
+
+
+def test_batch_failing_point_is_isolated():
+    from tpsc_conductivity_b200 import _lib
+    from tpsc_conductivity_b200.api import Batch, sweep_points
+
+    pts = sweep_points(6, seed=3)
+    pts[2, 0] = 48  # not a supported lattice
+    pts[4, 2] = 2.5  # density out of range
+    b = Batch(nstreams=2)
+    res, st, _ = b.solve(pts)
+    assert st[2] == _lib.ERR_ARG and st[4] == _lib.ERR_ARG
+    assert np.all(np.isnan(res[2])) and np.all(np.isnan(res[4]))
+    ok = [i for i in range(6) if i not in (2, 4)]
+    assert np.all(st[ok] == 0) and np.all(np.isfinite(res[ok, list(_lib.SCALARS).index("mu")]))
+
+
+def test_batch_tuner_keeps_a_timed_count():
+    from tpsc_conductivity_b200.api import Batch, sweep_points
+
+    pts = sweep_points(16, seed=11)
+    b = Batch(nstreams=1)
+    t = b.tune(pts, max_streams=4)
+    assert sorted(t) == [1, 2, 4] and all(v > 0 for v in t.values())
+    assert b.nstreams == min(t, key=t.get)

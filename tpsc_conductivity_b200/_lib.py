@@ -27,6 +27,13 @@ SIGNATURES = [
     ("tpsc_find_Usp_Uch_grid", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),
     ("tpsc_find_Usp_Uch", C.c_int, [C.c_void_p]),
     ("tpsc_sp_corr_length", C.c_int, [C.c_void_p, _dp]),
+    ("tpsc_batch_create", C.c_void_p, [C.c_int, C.c_int, _ip]),
+    ("tpsc_batch_destroy", None, [C.c_void_p]),
+    ("tpsc_batch_last_error", C.c_char_p, [C.c_void_p]),
+    ("tpsc_batch_streams", C.c_int, [C.c_void_p, _ip]),
+    ("tpsc_batch_solve", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, _dp, _ip, _dp]),
+    ("tpsc_batch_tune", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, C.c_int, _dp]),
+    ("tpsc_sweep_points", C.c_int, [C.c_int, C.c_ulonglong, _dp]),
     ("tpsc_vertex", C.c_int, [C.c_void_p]),
     ("tpsc_self_energy", C.c_int, [C.c_void_p]),
     ("tpsc_trace_self_G", C.c_int, [C.c_void_p, _dp]),
@@ -67,6 +74,7 @@ KERNELS = ["gslice", "chi0_slice", "chi0_tau", "vertex_q", "vertex_tau", "sigma_
 
 STATUS = {0: "OK", 1: "bad argument", 2: "CUDA error", 3: "out of device memory",
           4: "root not found", 5: "stage prerequisite missing", 6: "non-finite result"}
+OK, ERR_ARG, ERR_CUDA, ERR_OOM, ERR_NO_ROOT, ERR_STATE, ERR_NONFINITE = range(7)
 
 # enum tpsc_scalar
 SCALARS = ["mu0", "chi0max", "qmax0", "qmax1", "Usp", "Uch", "dblOcc", "difRelsp", "difRelch",

@@ -282,3 +282,81 @@ def pade_batch(x, y, z, ctx=None):
     ctx.call("tpsc_pade_batch", nf, Nn, _dptr(x.view(np.float64)), _dptr(y.view(np.float64)), int(z.size),
              _dptr(z.view(np.float64)), _dptr(out.view(np.float64)))
     return out
+
+
+SCALAR_NAMES = None
+
+
+def _scalar_names():
+    global SCALAR_NAMES
+    if SCALAR_NAMES is None:
+        SCALAR_NAMES = list(_lib.SCALARS)
+    return SCALAR_NAMES
+
+
+def sweep_points(npts, seed=20261203):
+    """The parameter-sweep workload (tpsc_sweep_points): npts rows
+    (nk0, Nw0, n, T, tp, tpp, t3, U) from std::mt19937_64(seed)."""
+    lib = _lib.load()
+    out = np.zeros((npts, 8))
+    rc = lib.tpsc_sweep_points(int(npts), C.c_ulonglong(seed), _dptr(out))
+    if rc:
+        raise _lib.TPSCError(rc, "tpsc_sweep_points")
+    return out
+
+
+class Batch:
+    """Many independent solves (uneven lattices and cutoffs) on one GPU through
+    the batched sweep (tpsc_batch_*): ``nstreams`` solver contexts, each fed by
+    a host thread, points largest first."""
+
+    def __init__(self, nstreams=4, device=0):
+        self.lib = _lib.load()
+        st = C.c_int(0)
+        self.h = self.lib.tpsc_batch_create(int(device), int(nstreams), C.byref(st))
+        if not self.h:
+            raise _lib.TPSCError(st.value, "tpsc_batch_create")
+
+    def _err(self, rc):
+        raise _lib.TPSCError(rc, self.lib.tpsc_batch_last_error(self.h).decode())
+
+    def solve(self, params, form=_lib.FORM_NEWTON | _lib.FORM_MIXED):
+        """params: (npts, 8) rows (nk0, Nw0, n, T, tp, tpp, t3, U).  Returns
+        (scalars [npts, TPSC_S_COUNT], status [npts], wall ms); a failing
+        point has NaN scalars and its status, the others are solved."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        n = p.shape[0]
+        res = np.zeros((n, len(_scalar_names())))
+        st = np.zeros(n, dtype=np.int32)
+        ms = C.c_double(0.0)
+        self.lib.tpsc_batch_solve(self.h, int(form), n, _dptr(p), _dptr(res), st.ctypes.data_as(_lib._ip),
+                                  C.byref(ms))
+        return res, st, ms.value
+
+    def tune(self, params, form=_lib.FORM_NEWTON | _lib.FORM_MIXED, max_streams=16):
+        """Times the sample on 1, 2, 4, ... max_streams contexts and keeps the
+        fastest count; returns {count: ms}."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        k = int(np.floor(np.log2(max_streams))) + 1
+        ms = np.zeros(k)
+        rc = self.lib.tpsc_batch_tune(self.h, int(form), p.shape[0], _dptr(p), int(max_streams), _dptr(ms))
+        if rc:
+            self._err(rc)
+        return {2 ** i: float(ms[i]) for i in range(k)}
+
+    @property
+    def nstreams(self):
+        v = C.c_int(0)
+        self.lib.tpsc_batch_streams(self.h, C.byref(v))
+        return v.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tpsc_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

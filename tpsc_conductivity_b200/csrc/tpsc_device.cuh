@@ -14,6 +14,12 @@ namespace tpsc {
 // the launch status
 cudaError_t launched(int n = 1);
 
+// Dynamic shared memory above 48 KB needs the function's opt-in attribute,
+// which is process-wide: it is raised once per kernel and device to the
+// largest size the device allows and never lowered, so that launches from
+// concurrent host threads with different sizes all see a cap they fit under.
+cudaError_t smem_optin(const void *fn);
+
 namespace {
 
 constexpr double kPi = 3.141592653589793;  // == acos(-1.0) in double
@@ -441,7 +447,8 @@ cudaError_t dispatch_nw(int nw0, Args... args) {
 
 template <typename K>
 cudaError_t set_smem(K kernel, size_t bytes) {
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return smem_optin((const void *)kernel);
 }
 
 }  // namespace

@@ -270,6 +270,7 @@ bool newton_root(F &&func, double x0, double lo, double hi, double tol, double *
 // ---------------------------------------------------------------------------
 struct Grid {
     GridDev d;
+    cudaStream_t st = nullptr;    // the owning context's stream: every fill and upload is ordered on it
     std::vector<double> ek_host;  // [nbk * nbk], ek[m + l*nbk]
     double mu0 = 0.0;
     double *Grt = nullptr;        // [(Nw0+1) * n8]      G(r, tau_j)
@@ -366,7 +367,9 @@ cudaError_t dalloc(Grid *g, T **p, size_t count) {
     if (e != cudaSuccess) return e;
     g->allocs.push_back(q);
     *p = static_cast<T *>(q);
-    return cudaMemset(q, 0, count * sizeof(T) + 16);
+    // on the context's (non-blocking) stream, so that the kernels queued there
+    // after it see the zeros: a legacy-stream memset is not ordered with them
+    return cudaMemsetAsync(q, 0, count * sizeof(T) + 16, g->st);
 }
 
 void free_grid(Grid *g) {
@@ -441,7 +444,7 @@ template <typename T>
 cudaError_t upload(Grid *g, T **dst, const std::vector<T> &src) {
     cudaError_t e = dalloc(g, dst, src.size());
     if (e != cudaSuccess) return e;
-    return cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, g->st);
 }
 
 int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
@@ -456,6 +459,7 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
                                            " Nw0=" + std::to_string(nw0) +
                                            " (nk0 in {8,16,32,64,128,256}, Nw0 power of two in [16, 4096])");
     Grid *g = new Grid;
+    g->st = ctx->st;
     GridDev &d = g->d;
     d.nk0 = nk0;
     d.nbk = nk0 / 2 + 1;
@@ -522,6 +526,8 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
     A(dalloc(g, &g->d_cmax_suf, nb + 1));
     A(dalloc(g, &g->d_tailm, (size_t)kMomP + 1));
 #undef A
+    // the host tables above are released on return
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
     if (e != cudaSuccess) {
         free_grid(g);
         return cuda_fail(ctx, e, "grid allocation");
@@ -1183,7 +1189,7 @@ tpsc_ctx *tpsc_create(int device, int *status) {
     if ((e = cudaMalloc(&ctx->red.partial, 4 * kMaxBlocks * sizeof(double))) != cudaSuccess) return bad(e);
     if ((e = cudaMalloc(&ctx->red.result, 8 * sizeof(double))) != cudaSuccess) return bad(e);
     if ((e = cudaMalloc(&ctx->red.ticket, sizeof(unsigned))) != cudaSuccess) return bad(e);
-    if ((e = cudaMemset(ctx->red.ticket, 0, sizeof(unsigned))) != cudaSuccess) return bad(e);
+    if ((e = cudaMemsetAsync(ctx->red.ticket, 0, sizeof(unsigned), ctx->st)) != cudaSuccess) return bad(e);
     if ((e = cudaMalloc(&ctx->redm.partial, (size_t)std::max(2 * kMomP + 2, kSigmaMomNV) * kMaxBlocks *
                                                  sizeof(double))) != cudaSuccess)
         return bad(e);
@@ -1926,3 +1932,9 @@ int tpsc_kernel_bytes(tpsc_ctx *ctx, int which, double *bytes) {
 }
 
 }  // extern "C"
+
+// Cap on the cooperative root-search grids of one context, for callers that
+// run several contexts' solves at once on one GPU (tpsc_batch.cpp).
+void tpsc_ctx_set_coop_cap(tpsc_ctx *ctx, int blocks) {
+    if (ctx) ctx->roots.max_blocks = blocks;
+}

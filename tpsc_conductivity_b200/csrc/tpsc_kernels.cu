@@ -19,6 +19,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
+#include <set>
+#include <utility>
 
 #include "tpsc_device.cuh"
 
@@ -1564,6 +1567,23 @@ struct RunSigmaTau {
 }  // namespace
 
 long long launches_total() { return g_launches.load(); }
+
+cudaError_t smem_optin(const void *fn) {
+    static std::mutex mu;
+    static std::set<std::pair<const void *, int>> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count({fn, dev})) return cudaSuccess;
+    int optin = 0;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return e;
+    cudaFuncAttributes fa;
+    if ((e = cudaFuncGetAttributes(&fa, fn)) != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+    if (e == cudaSuccess) done.insert({fn, dev});
+    return e;
+}
 
 bool supported_grid(int nk0, int nw0) {
     const int nbk = nk0 / 2 + 1;

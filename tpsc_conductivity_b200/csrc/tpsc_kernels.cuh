@@ -120,6 +120,7 @@ struct RootScratch {
     double *partial = nullptr;  // [4 kRootMaxBlocks]
     unsigned *bar = nullptr;    // [4]: barrier arrivals, generation, error flag
     double *out = nullptr;      // [8] results
+    int max_blocks = 0;         // cap on the cooperative grid (0: two blocks per SM)
 };
 // The Newton form's Sigma pass: Tr Sigma G0 (green::traceSelfG) and the
 // find_mu series moments around mu0 over the frequencies n >= jc and the tail

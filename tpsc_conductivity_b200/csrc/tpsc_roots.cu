@@ -550,15 +550,18 @@ __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
     }
 }
 
-// the cooperative grid of the root searches: up to two blocks per SM
+// the cooperative grid of the root searches: up to two blocks per SM, or
+// `cap` blocks when the caller runs several root searches at once (solver
+// streams of a batch), so that all of them fit on the GPU together
 template <typename K>
-cudaError_t root_grid(K kernel, int *grid) {
+cudaError_t root_grid(K kernel, int *grid, int cap) {
     int dev = 0, sms = 0, per = 0;
     cudaError_t e;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kRootThreads, 0)) != cudaSuccess) return e;
     *grid = std::min(sms * std::max(1, std::min(per, 2)), kRootMaxBlocks);
+    if (cap > 0) *grid = std::min(*grid, cap);
     return cudaSuccess;
 }
 
@@ -579,7 +582,7 @@ cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2
                             const double *sinf, const double *mom, double mu0, double T, int jc, double wc,
                             RootScratch rs, cudaStream_t st) {
     int grid = 0;
-    cudaError_t e = root_grid(k_mu_roots, &grid);
+    cudaError_t e = root_grid(k_mu_roots, &grid, rs.max_blocks);
     if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(rs.bar, 0, 2 * sizeof(unsigned) + sizeof(int), st)) != cudaSuccess) return e;
     MuRootArgs a;
@@ -612,7 +615,7 @@ cudaError_t launch_sumrule_roots(const GridDev &g, const double *chiq, const dou
                                  const double *mom_suf, const double *cmax_suf, const double *tailm, double T,
                                  double n, double nsr, double U, double hi_sp, RootScratch rs, cudaStream_t st) {
     int grid = 0;
-    cudaError_t e = root_grid(k_sumrule_roots, &grid);
+    cudaError_t e = root_grid(k_sumrule_roots, &grid, rs.max_blocks);
     if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(rs.bar, 0, 2 * sizeof(unsigned) + sizeof(int), st)) != cudaSuccess) return e;
     SumRootArgs a;
