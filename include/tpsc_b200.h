@@ -120,6 +120,22 @@ int tpsc_find_Usp_Uch_grid(tpsc_ctx *ctx, int nq0, int nw0, double Usc[2]);
  * difRel diagnostics and the double occupancy ansatz. */
 int tpsc_find_Usp_Uch(tpsc_ctx *ctx);
 
+/* Differentiation form, forward half beyond the Newton steps (no counterpart
+ * in the reference): the sensitivities of the sum-rule roots and the double
+ * occupancy on the current grid, after its chi0 and roots (tpsc_chi0 +
+ * tpsc_find_Usp_Uch_grid, or a solve), by forward tangents of
+ * chi0 -> sum rules (FP64, tpsc_tangent.cu) and the implicit derivatives of
+ * R_sp(Usp) = 0, R_ch(Uch) = 0:
+ *   out[3 p + k] = d{Usp, Uch, D}_k / d{U, mu, t'}_p,
+ * with mu a shift of the non-interacting chemical potential mu0 at fixed n
+ * (tpsc_set_mu_shift) and t' at fixed n (mu0 follows the density). */
+int tpsc_sumrule_tangents(tpsc_ctx *ctx, double out[9]);
+/* The backward pair: grad[p] = sum_k cot[k] d{Usp, Uch, D}_k / d{U, mu, t'}_p. */
+int tpsc_sumrule_vjp(tpsc_ctx *ctx, const double cot[3], double grad[3]);
+/* Shift of the non-interacting chemical potential: mu0 = (density root) +
+ * dmu on every grid from the next stage on (default 0). */
+int tpsc_set_mu_shift(tpsc_ctx *ctx, double dmu);
+
 /* chi::sp_corr_length (src/chi.cpp:420-718) on the current grid after its
  * chi0 and Usp: the Fermi velocity at the hot spots of the non-interacting
  * Fermi surface (green0::find_FS with 10001 lines, src/green0.cpp:626-676)

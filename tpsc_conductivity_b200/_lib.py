@@ -27,6 +27,9 @@ SIGNATURES = [
     ("tpsc_find_Usp_Uch_grid", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),
     ("tpsc_find_Usp_Uch", C.c_int, [C.c_void_p]),
     ("tpsc_sp_corr_length", C.c_int, [C.c_void_p, _dp]),
+    ("tpsc_sumrule_tangents", C.c_int, [C.c_void_p, _dp]),
+    ("tpsc_sumrule_vjp", C.c_int, [C.c_void_p, _dp, _dp]),
+    ("tpsc_set_mu_shift", C.c_int, [C.c_void_p, C.c_double]),
     ("tpsc_batch_create", C.c_void_p, [C.c_int, C.c_int, _ip]),
     ("tpsc_batch_destroy", None, [C.c_void_p]),
     ("tpsc_batch_last_error", C.c_char_p, [C.c_void_p]),

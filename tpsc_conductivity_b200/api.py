@@ -97,6 +97,26 @@ class Green:
         self.ctx.call("tpsc_sp_corr_length", _dptr(out))
         return dict(zip(["vF", "xi_y", "xi_x", "xiAs_y", "xiAs_x", "xi0_y", "xi0_x"], out.tolist()))
 
+    def sumrule_tangents(self):
+        """d(Usp, Uch, D)/d(U, mu, t') on the current grid after its chi0 and
+        roots (forward tangents; mu a shift of mu0 at fixed n, t' at fixed n).
+        Returns a dict of dicts: J[param][output]."""
+        out = np.zeros(9)
+        self.ctx.call("tpsc_sumrule_tangents", _dptr(out))
+        return {p: {k: float(out[3 * i + j]) for j, k in enumerate(("Usp", "Uch", "D"))}
+                for i, p in enumerate(("U", "mu", "tp"))}
+
+    def sumrule_vjp(self, cot):
+        """The backward pair: sum_k cot[k] d(Usp, Uch, D)_k/d(U, mu, t')."""
+        c = np.asarray(cot, dtype=np.float64)
+        g = np.zeros(3)
+        self.ctx.call("tpsc_sumrule_vjp", _dptr(c), _dptr(g))
+        return g
+
+    def set_mu_shift(self, dmu):
+        """mu0 = density root + dmu on every grid from the next stage on."""
+        self.ctx.call("tpsc_set_mu_shift", float(dmu))
+
     def calc_chirt(self):
         """chi::calc_chirt (src/chi.cpp:37)."""
         self.ctx.call("tpsc_vertex")

@@ -297,6 +297,10 @@ struct Grid {
     double tail_mom[kMomP] = {0};            // the same moments of the Matsubara tail n > Nw0/2
     double tail_max = 0.0;                   // max |chi| over the tail
     double *d_mom_suf = nullptr, *d_cmax_suf = nullptr, *d_tailm = nullptr;  // on the device
+    // forward tangents (tpsc_sumrule_tangents; allocated on first use)
+    double *t_dGrt = nullptr, *t_dchiq = nullptr, *t_ddq0 = nullptr, *t_dcinf = nullptr, *t_dcinf2 = nullptr;
+    double *t_der = nullptr;
+    double2 *t_fd = nullptr;
     double tailq_T = -1.0;         // temperature the tail power sums were built for
     double tailq_host[kTailQ] = {0};
     std::vector<void *> allocs;
@@ -327,6 +331,7 @@ struct tpsc_ctx {
     int nk0 = 0, Nw0 = 0;
     double n = 0, T = 0, tp = 0, tpp = 0, t3 = 0, U = 0, nsr = 0;
     double Usp = 0, Uch = 0;
+    double mu_shift = 0;  // added to the density root mu0 (tpsc_set_mu_shift)
     std::map<std::pair<int, int>, Grid *> grids;
     Grid *cur = nullptr;
     double scal[TPSC_S_COUNT] = {0};
@@ -585,7 +590,7 @@ int grid_set_model(tpsc_ctx *ctx, Grid *g) {
     CK(cudaStreamSynchronize(ctx->st));
     g->have_chi0 = g->have_V = g->have_S = false;
     if (ctx->n == 1.0 && ctx->tp == 0 && ctx->tpp == 0) {
-        g->mu0 = 0.0;
+        g->mu0 = 0.0 + ctx->mu_shift;
         return TPSC_OK;
     }
     int rc = TPSC_OK;
@@ -594,7 +599,7 @@ int grid_set_model(tpsc_ctx *ctx, Grid *g) {
         double r[2];
         if ((rc = read_result(ctx, 2, r))) return rc;
         if (!std::isfinite(r[0]) || r[1] >= 200) return fail(ctx, TPSC_ERR_NO_ROOT, "mu0 not found");
-        g->mu0 = r[0];
+        g->mu0 = r[0] + ctx->mu_shift;
         return TPSC_OK;
     }
     auto dens = [&](double mu, double &y) -> bool {
@@ -614,7 +619,7 @@ int grid_set_model(tpsc_ctx *ctx, Grid *g) {
         if (derr) return rc;
         return fail(ctx, TPSC_ERR_NO_ROOT, "mu0 not found");
     }
-    g->mu0 = root;
+    g->mu0 = root + ctx->mu_shift;
     return TPSC_OK;
 }
 
@@ -1296,6 +1301,142 @@ int tpsc_find_Usp_Uch_grid(tpsc_ctx *ctx, int nq0, int nw0, double Usc[2]) {
     int rc = tpsc_chi0(ctx, nq0, nw0);
     if (rc) return rc;
     return roots_Usp_Uch(ctx, Usc);
+}
+
+// ---------------------------------------------------------------------------
+// forward tangents of chi0 -> sum rules -> Usp, Uch, D
+// ---------------------------------------------------------------------------
+
+int tpsc_set_mu_shift(tpsc_ctx *ctx, double dmu) {
+    if (!ctx || !std::isfinite(dmu)) return fail(ctx, TPSC_ERR_ARG, "bad mu shift");
+    if (dmu != ctx->mu_shift) {
+        ctx->mu_shift = dmu;
+        ++ctx->model_id;  // every grid re-derives mu0
+    }
+    return TPSC_OK;
+}
+
+int tpsc_sumrule_tangents(tpsc_ctx *ctx, double out[9]) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    if (!out) return fail(ctx, TPSC_ERR_ARG, "null output");
+    Grid *g = ctx->cur;
+    if (!g || !g->have_chi0 || !g->have_U)
+        return fail(ctx, TPSC_ERR_STATE, "chi0 and the sum-rule roots have not been computed on the current grid");
+    cudaSetDevice(ctx->device);
+    const GridDev &d = g->d;
+    const size_t n8 = d.n8, n8p = d.n8p, nb = d.nb, nw = d.nw0;
+    if (!g->t_dGrt) {
+        cudaError_t e = cudaSuccess;
+#define A(x)                                       \
+    if (e == cudaSuccess) {                        \
+        e = (x);                                   \
+    }
+        A(dalloc(g, &g->t_dGrt, (nw + 1) * n8));
+        A(dalloc(g, &g->t_dchiq, nb * n8p));
+        A(dalloc(g, &g->t_ddq0, n8));
+        A(dalloc(g, &g->t_dcinf, n8));
+        A(dalloc(g, &g->t_dcinf2, n8));
+        A(dalloc(g, &g->t_der, n8));
+        A(dalloc(g, &g->t_fd, n8));
+#undef A
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "tangent buffers");
+    }
+    const double T = ctx->T, beta = 1.0 / T, mu0 = g->mu0, U = ctx->U, n = ctx->n, nsr = ctx->nsr;
+    const double Usp = ctx->Usp, Uch = ctx->Uch;
+    // the primal FP64 G(r, tau) (the mixed form keeps only its FP32 copy)
+    CK(launch_gslice(d, g->Grt, mu0, T, ctx->st));
+    // per octant point: xi, beta f(xi), d eps/d t' and the density weight
+    const int nbk = d.nbk;
+    std::vector<double> xi(n8), bf(n8), deps(n8), wf(n8);
+    double sw = 0.0, swd = 0.0;
+    for (int l = 0; l < nbk; ++l)
+        for (int m = 0; m <= l; ++m) {
+            const size_t o = m + (size_t)l * (l + 1) / 2;
+            const double kx = l * PI / (nbk - 1), ky = m * PI / (nbk - 1);
+            xi[o] = g->ek_host[m + (size_t)l * nbk] - mu0;
+            const double z = xi[o] / T;
+            const double f = z > 0 ? std::exp(-z) / (1.0 + std::exp(-z)) : 1.0 / (1.0 + std::exp(z));
+            bf[o] = beta * f;
+            deps[o] = -4.0 * std::cos(kx) * std::cos(ky);
+            // the density's weight (k_density) times df/dxi = -beta f (1 - f)
+            double w = 8;
+            if (l == 0 || l == nbk - 1) w /= 2;
+            if (m == 0 || m == nbk - 1) w /= 2;
+            if (m == l) w /= 2;
+            wf[o] = w * (-beta * f * (1.0 - f));
+            sw += wf[o];
+            swd += wf[o] * deps[o];
+        }
+    // t' moves mu0 so that the density stays n (the reference's finite-lattice
+    // mu0, src/green0.cpp:182-262); the half-filled symmetric point keeps 0,
+    // which is also the density root there
+    const double dmu0_dtp = sw != 0.0 ? swd / sw : 0.0;
+    // d R / d theta at fixed (Usp, Uch) from the chi0 tangent, theta = mu, t'
+    double dRsp[3] = {0, 0, 0}, dRch[3] = {0, 0, 0};
+    for (int p = 1; p < 3; ++p) {
+        std::vector<double2> fd(n8);
+        std::vector<double> der(n8, 0.0);
+        double dmu0;
+        if (p == 1) {  // a shift of mu0: dxi = -1
+            for (size_t o = 0; o < n8; ++o) fd[o] = make_double2(bf[o], -1.0);
+            dmu0 = 1.0;
+        } else {  // t': deps - dmu0/dt'; the hopping table er[2] = -t'
+            for (size_t o = 0; o < n8; ++o) fd[o] = make_double2(bf[o], deps[o] - dmu0_dtp);
+            if (n8 > 2) der[2] = -1.0;
+            dmu0 = dmu0_dtp;
+        }
+        CK(cudaMemcpyAsync(g->t_fd, fd.data(), n8 * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(g->t_der, der.data(), n8 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+        TangentBufs tb;
+        tb.Grt = g->Grt;
+        tb.dG0p = g->dG0p;
+        tb.der = g->t_der;
+        tb.fd = g->t_fd;
+        tb.dGrt = g->t_dGrt;
+        tb.dchiq = g->t_dchiq;
+        tb.ddq0 = g->t_ddq0;
+        CK(launch_chi0_tangent(d, tb, mu0, dmu0, T, ctx->st));
+        CK(launch_chi0_tau(d, g->t_dchiq, g->t_ddq0, g->t_dcinf, g->t_dcinf2, T, ctx->st));
+        CK(launch_sumrule_tan(d, g->chiq, g->t_dchiq, g->cinf, g->cinf2, g->t_dcinf, g->t_dcinf2, Usp, -1.0, T,
+                              ctx->red, ctx->st));
+        if ((rc = read_result(ctx, 1, &dRsp[p]))) return rc;
+        CK(launch_sumrule_tan(d, g->chiq, g->t_dchiq, g->cinf, g->cinf2, g->t_dcinf, g->t_dcinf2, Uch, 1.0, T,
+                              ctx->red, ctx->st));
+        if ((rc = read_result(ctx, 1, &dRch[p]))) return rc;
+    }
+    // the roots' own derivatives (the Newton derivative of each sum rule)
+    double tr, dtr_sp, dtr_ch;
+    if ((rc = sumrule(ctx, 0, Usp, &tr, &dtr_sp))) return rc;
+    if ((rc = sumrule(ctx, 1, Uch, &tr, &dtr_ch))) return rc;
+    // R_sp = tr_sp + n - n^2/2 - nsr + Us nsr^2/(2U),
+    // R_ch = tr_ch + n - n^2/2 - (nsr + Usp nsr^2/(2U) - nsr^2)  (src/chi.cpp:833-843)
+    const double q2 = nsr * nsr;
+    const double dRsp_dUs = dtr_sp + q2 / (2.0 * U), dRch_dUc = dtr_ch, dRch_dUsp = -q2 / (2.0 * U);
+    dRsp[0] = -Usp * q2 / (2.0 * U * U);
+    dRch[0] = Usp * q2 / (2.0 * U * U);
+    for (int p = 0; p < 3; ++p) {
+        const double dUsp = -dRsp[p] / dRsp_dUs;
+        const double dUch = -(dRch[p] + dRch_dUsp * dUsp) / dRch_dUc;
+        // D = Usp nsr^2/(4U) (+ 1 - nsr for n > 1)  (src/chi.cpp:370-371)
+        const double dD = q2 / (4.0 * U) * dUsp - (p == 0 ? Usp * q2 / (4.0 * U * U) : 0.0);
+        out[3 * p] = dUsp;
+        out[3 * p + 1] = dUch;
+        out[3 * p + 2] = dD;
+    }
+    (void)n;
+    for (int i = 0; i < 9; ++i)
+        if (!std::isfinite(out[i])) return fail(ctx, TPSC_ERR_NONFINITE, "non-finite sensitivity");
+    return TPSC_OK;
+}
+
+int tpsc_sumrule_vjp(tpsc_ctx *ctx, const double cot[3], double grad[3]) {
+    if (!ctx || !cot || !grad) return fail(ctx, TPSC_ERR_ARG, "null argument");
+    double J[9];
+    int rc = tpsc_sumrule_tangents(ctx, J);
+    if (rc) return rc;
+    for (int p = 0; p < 3; ++p) grad[p] = cot[0] * J[3 * p] + cot[1] * J[3 * p + 1] + cot[2] * J[3 * p + 2];
+    return TPSC_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -850,6 +850,52 @@ __global__ void __launch_bounds__(kRedThreads)
     grid_finish<2>(out, r, 0.0);
 }
 
+// Directional derivative of k_sumrule's trace at fixed U (jdir = nb, tail
+// term by term) in the direction (dchi, dchi0_inf, dchi0_inf2):
+//   sum w T/Nq [1/(1 + h chi)^2 - 1] dchi,  h = sgn U/2,
+// with the same weights (n = 0 halved) and the same tail frequencies.
+__global__ void __launch_bounds__(kRedThreads)
+    k_sumrule_tan(const double4 *__restrict__ chiq, const double4 *__restrict__ dchiq,
+                  const double *__restrict__ cinf, const double *__restrict__ cinf2, const double *__restrict__ dcinf,
+                  const double *__restrict__ dcinf2, const double *__restrict__ w16, int nb, double Uv, double sgn,
+                  double T, double scale, Reduce r) {
+    const double hu = sgn * Uv / 2.0;
+    double v = 0.0;
+    const int blk = blockIdx.x;
+    const int o0 = 4 * blk;
+    const double4 w = *reinterpret_cast<const double4 *>(w16 + o0);
+    const double ww[4] = {w.x, w.y, w.z, w.w};
+    const double4 *col = chiq + (size_t)blk * nb, *dcol = dchiq + (size_t)blk * nb;
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+        const double4 x = col[j], dx = dcol[j];
+        const double f = j == 0 ? 0.5 : 1.0;
+        const double xs[4] = {x.x, x.y, x.z, x.w}, ds[4] = {dx.x, dx.y, dx.z, dx.w};
+        double s = 0.0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const double q = 1.0 / (1.0 + hu * xs[c]);
+            s += ww[c] * (q * q - 1.0) * ds[c];
+        }
+        v += f * s;
+    }
+    const int nwmax = nb - 1;
+    const double tw = 2.0 * 3.141592653589793 * T;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        if (ww[c] == 0.0) continue;
+        const double a = cinf[o0 + c], b = cinf2[o0 + c], da = dcinf[o0 + c], db = dcinf2[o0 + c];
+        for (int t = threadIdx.x; t < nwmax; t += blockDim.x) {
+            const double wn = (nwmax + 1 + t) * tw;
+            const double i2 = 1.0 / (wn * wn);
+            const double xv = a * i2 + b * i2 * i2, dxv = da * i2 + db * i2 * i2;
+            const double q = 1.0 / (1.0 + hu * xv);
+            v += ww[c] * (q * q - 1.0) * dxv;
+        }
+    }
+    double out[1] = {scale * v};
+    grid_finish<1>(out, r, 0.0);
+}
+
 // The Newton form's sum-rule evaluation: only the stored frequencies
 // j < jdir (the rest enters as the moment series on the host), over a
 // flattened (column block, j) index so that every thread has independent
@@ -1641,6 +1687,16 @@ cudaError_t launch_sumrule(const GridDev &g, const double *chiq, const double *c
     }
     k_sumrule<<<nblk, kRedThreads, 0, st>>>(reinterpret_cast<const double4 *>(chiq), chi0_inf, chi0_inf2, g.w16,
                                             g.tailq, g.nb, jdir, tail, Uv, sign, T, T / Nq, r);
+    return launched();
+}
+
+cudaError_t launch_sumrule_tan(const GridDev &g, const double *chiq, const double *dchiq, const double *chi0_inf,
+                               const double *chi0_inf2, const double *dchi0_inf, const double *dchi0_inf2, double Uv,
+                               double sign, double T, Reduce r, cudaStream_t st) {
+    const double Nq = 4.0 * (g.nbk - 1) * (g.nbk - 1);
+    k_sumrule_tan<<<g.n8p / 4, kRedThreads, 0, st>>>(reinterpret_cast<const double4 *>(chiq),
+                                                     reinterpret_cast<const double4 *>(dchiq), chi0_inf, chi0_inf2,
+                                                     dchi0_inf, dchi0_inf2, g.w16, g.nb, Uv, sign, T, T / Nq, r);
     return launched();
 }
 

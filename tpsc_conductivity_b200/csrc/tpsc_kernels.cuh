@@ -82,6 +82,26 @@ constexpr double kMomMuRange = 0.35;     // |mu - mu0| the find_mu series is bui
 constexpr int kMuMomP = 12;              // terms of the find_mu series
 constexpr double kMuSeriesMax = 0.03;    // |mu - mu0| / |z| bound of its terms: 0.03^12 < 1e-18
 cudaError_t launch_chi0_moments(const GridDev &g, const double *chiq, double *mom, double *cmax, cudaStream_t st);
+// Forward tangents of the chi0 stage (tpsc_tangent.cu): buffers of one
+// direction.  fd[o] = (beta f(xi_o), dxi_o); der[o] the direction of the
+// hopping table; Grt the FP64 G(r, tau) and dG0p the primal d/dtau G(r, 0+).
+struct TangentBufs {
+    const double *Grt = nullptr, *dG0p = nullptr, *der = nullptr;
+    const double2 *fd = nullptr;
+    double *dGrt = nullptr;  // [(Nw0+1) n8]  dG(r, tau)
+    double *dchiq = nullptr; // blocked nb    dchi0(q, tau) -> dchi0(q, iqn) after launch_chi0_tau
+    double *ddq0 = nullptr;  // [n8]          d of d/dtau chi0(q, 0)
+};
+// dG(r, tau), dchi0(q, tau_j) and d(d/dtau chi0(q, 0)) for the direction in t
+// (mu0 the primal chemical potential, dmu0 its direction)
+cudaError_t launch_chi0_tangent(const GridDev &g, const TangentBufs &t, double mu0, double dmu0, double T,
+                                cudaStream_t st);
+// the directional derivative of the full sum-rule trace (k_sumrule with
+// every frequency and the tail term by term) at U = Uv in the direction
+// (dchiq, dchi0_inf, dchi0_inf2) -> r.result[0]
+cudaError_t launch_sumrule_tan(const GridDev &g, const double *chiq, const double *dchiq, const double *chi0_inf,
+                               const double *chi0_inf2, const double *dchi0_inf, const double *dchi0_inf2, double Uv,
+                               double sign, double T, Reduce r, cudaStream_t st);
 // sums of mom over the frequencies >= j (double-double, rounded once),
 // j = 0..nb -> mom_suf [(nb + 1)][kMomP]; suffix maxima of cmax -> cmax_suf
 // [nb + 1]; the tail moments and tail maximum of launch_tail_moments' result
