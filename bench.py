@@ -309,6 +309,9 @@ def our_arm(a, world, rank, local_rank):
     batch = None
     if world == 1 and not a.no_batch:
         batch = batch_sweep(a.steps)
+    extra = None
+    if world == 1 and not a.no_extra:
+        extra = extra_configs()
 
     if rank != 0:
         return
@@ -346,6 +349,8 @@ def our_arm(a, world, rank, local_rank):
     }
     if batch is not None:
         line["batch"] = batch
+    if extra is not None:
+        line["configs"] = extra
     if world == 1 and not a.no_cpu_baseline:
         try:
             t, raw = run_reference_once(os.cpu_count() or 1)
@@ -389,6 +394,84 @@ def batch_sweep(steps):
     return out
 
 
+def extra_configs():
+    """The other workloads of the measurement plan, each timed once after a
+    warm-up run (host wall clock, device idle at both ends, ms):
+    config 1, plain FP64 TPSC at 32^2 x 256 positive iwn with chi_jj for 16
+    bosonic frequencies and the Pade spectral weight of every k on 1000 real
+    frequencies; config 3, the optical conductivity at 128^2 x 1024 positive
+    iwn, mixed + Newton, sigma(iq_n) n = 1..256 against the FP64 form, Pade of
+    sigma on 2000 frequencies; config 4, the sum-rule sensitivities
+    d(Usp, Uch, D)/d(U, mu, t') at 128^2 x 1024."""
+    import numpy as np
+    import torch
+
+    from tpsc_conductivity_b200 import _lib
+    from tpsc_conductivity_b200.api import CondOpt, Green
+
+    def timed(f):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r = f()
+        torch.cuda.synchronize()
+        return r, 1e3 * (time.perf_counter() - t)
+
+    out = {}
+    # config 1
+    c = CondOpt(32, 512, 0.875, 0.25, 0.05, (0.0, 0.0, 0.0, 2.0))
+    c.set_form(_lib.FORM_REFERENCE)
+    w1 = np.linspace(-8.0, 8.0, 1000) + 0.05j
+
+    def c1():
+        ms = {}
+        _, ms["solve"] = timed(c.solve)
+        _, ms["chijj"] = timed(lambda: c.calc_chijj_vertex_corr_all_optim(False, 3, 1))
+        s16, ms["sigma_iqn"] = timed(lambda: c.sigma_qn(16))
+        sa, ms["pade"] = timed(lambda: c.pade_sigma(w1, Nn=32))
+        return s16, sa, ms
+
+    c1()
+    (s16, _), (_, A), ms1 = c1()
+    sc = c.scalars()
+    out["c1_l32_w512_plain_fp64"] = {
+        "ms": ms1, "Usp": sc["Usp"], "Uch": sc["Uch"], "dblOcc": sc["dblOcc"],
+        "sigma_iq1": float(s16[0]), "pade": "Sigma(k, w + 0.05i) and A(k, w) for all 153 octant k, 1000 w in "
+                                              "[-8, 8], 32 Matsubara nodes",
+        "A_finite": bool(np.all(np.isfinite(A)))}
+    # config 3
+    w3 = np.linspace(0.0, 10.0, 2000)
+
+    def c3(g):
+        ms = {}
+        _, ms["solve"] = timed(g.solve)
+        _, ms["chijj"] = timed(lambda: g.calc_chijj_vertex_corr_all_optim(False, 3, 1))
+        sig, ms["sigma_iqn"] = timed(lambda: g.sigma_qn(256)[0])
+        pade, ms["pade"] = timed(lambda: g.sigma_pade(w3, 64, 0.0)[0])
+        return sig, pade, ms
+
+    objs = {}
+    for name, form in (("mixed_newton", _lib.FORM_NEWTON | _lib.FORM_MIXED), ("fp64_newton", _lib.FORM_NEWTON)):
+        objs[name] = CondOpt(128, 2048, 0.9, 0.1, 0.1, (0.0, 0.0, 0.0, 3.0))
+        objs[name].set_form(form)
+        c3(objs[name])
+    sig_m, pade_m, ms3 = c3(objs["mixed_newton"])
+    sig_d, _, ms3d = c3(objs["fp64_newton"])
+    out["c3_l128_w2048_conductivity"] = {
+        "ms_mixed_newton": ms3, "ms_fp64_newton": ms3d,
+        "max_rel_err_sigma_iqn_mixed_vs_fp64": float(np.max(np.abs(sig_m - sig_d)) / np.max(np.abs(sig_d))),
+        "pade": "sigma(w) on 2000 w in [0, 10] from 64 bosonic nodes", "pade_finite": bool(np.all(np.isfinite(pade_m)))}
+    # config 4
+    g4 = Green(128, 2048, 0.85, 0.1, 0.1, (-0.2, 0.0, 0.0, 4.0))
+    g4.set_form(_lib.FORM_NEWTON)
+    g4.find_Usp_Uch_grid(128, 2048)
+    g4.sumrule_tangents()
+    J, t4 = timed(g4.sumrule_tangents)
+    out["c4_l128_w2048_sensitivities"] = {"ms": t4, "d_dU": J["U"], "d_dmu": J["mu"], "d_dtp": J["tp"],
+                                          "checked": "central differences, tests/test_gpu_tangent.py"}
+    out["timing"] = "host wall clock around each call after a warm-up run, device idle at both ends"
+    return out
+
+
 def profiled_traffic(kernel):
     """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
     p = os.path.join(ROOT, "profiles", "dram_traffic.txt")
@@ -428,6 +511,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-point batched sweep")
+    ap.add_argument("--no-extra", action="store_true", help="skip the measurements of the other workloads")
     ap.add_argument("--nk0", type=int, default=None, help="lattice side override (profiling only)")
     ap.add_argument("--nw0", type=int, default=None, help="Nw0 override (profiling only)")
     a = ap.parse_args()

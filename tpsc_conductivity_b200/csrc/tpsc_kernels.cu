@@ -1358,41 +1358,47 @@ constexpr int kPadeMax = 32;
 //  mode 1: Lagrange polynomial through the Nn samples (src/green.cpp:2297-2299).
 // out_sig [N8][Nz] (complex, may be null), out_A [N8][Nz] with
 // A = -Im 1/(z - (eps_k - mu) - Sigma)/pi.
-__global__ void k_pade_sigma(const double2 *__restrict__ S, const double *__restrict__ s2,
-                             const double *__restrict__ s3, const double *__restrict__ sinfp,
-                             const double *__restrict__ ek, const int *__restrict__ nidx, int Nn,
-                             const double2 *__restrict__ z, int Nz, int mode, int n8, int nw0, double mu, double T,
-                             double2 *__restrict__ out_sig, double *__restrict__ out_A) {
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= n8) return;
+// One CTA per octant point: the samples and (mode 0) the continued-fraction
+// coefficients in shared memory -- the recursion runs over l in parallel, one
+// barrier per order m -- then the CTA's threads take the energies z.  Each
+// (k, z) value is the same arithmetic as a one-thread evaluation.
+__global__ void __launch_bounds__(128)
+    k_pade_sigma(const double2 *__restrict__ S, const double *__restrict__ s2, const double *__restrict__ s3,
+                 const double *__restrict__ sinfp, const double *__restrict__ ek, const int *__restrict__ nidx,
+                 int Nn, const double2 *__restrict__ z, int Nz, int mode, int n8, int nw0, double mu, double T,
+                 double2 *__restrict__ out_sig, double *__restrict__ out_A) {
+    const int o = blockIdx.x;
     const int NO = nw0 / 2;
-    const double sinf = sinfp[0];
-    double2 f[kPadeMax], x0[kPadeMax], coef[kPadeMax];
-    for (int j = 0; j < Nn; ++j) {
-        x0[j] = make_double2(0.0, (2 * nidx[j] + 1) * 3.141592653589793 * T);
-        const double wn = (2 * j + 1) * 3.141592653589793 * T;
+    __shared__ double2 f[kPadeMax], x0[kPadeMax], g[kPadeMax], coef[kPadeMax];
+    const int t = threadIdx.x;
+    if (t < Nn) {
+        const double sinf = sinfp[0];
+        x0[t] = make_double2(0.0, (2 * nidx[t] + 1) * 3.141592653589793 * T);
+        const double wn = (2 * t + 1) * 3.141592653589793 * T;
         const double i1 = 1.0 / wn, i2 = i1 * i1, i4 = i2 * i2;
-        const double2 Sv = S[bidx(j, o, NO)];
+        const double2 Sv = S[bidx(t, o, NO)];
         // Sigma(k, i w_j) = Sinf/z + C2/z^2 + C3/z^3 + S/z^4 at z = i w_j
-        f[j] = make_double2(-s2[o] * i2 + Sv.x * i4, -sinf * i1 + s3[o] * i2 * i1 + Sv.y * i4);
+        f[t] = make_double2(-s2[o] * i2 + Sv.x * i4, -sinf * i1 + s3[o] * i2 * i1 + Sv.y * i4);
+        g[t] = f[t];
     }
+    __syncthreads();
     if (mode == 0) {
         // continued-fraction coefficients: g_0(l) = f_l,
         // g_m(l) = (g_{m-1}(m-1) - g_{m-1}(l)) / ((x_l - x_{m-1}) g_{m-1}(l)), coef_m = g_m(m)
-        double2 g[kPadeMax];
-        for (int l = 0; l < Nn; ++l) g[l] = f[l];
-        coef[0] = g[0];
+        if (t == 0) coef[0] = g[0];
         for (int m = 1; m < Nn; ++m) {
             const double2 gm = g[m - 1];
-            for (int l = m; l < Nn; ++l) {
-                const double2 dx = make_double2(x0[l].x - x0[m - 1].x, x0[l].y - x0[m - 1].y);
-                g[l] = cdiv(csub(gm, g[l]), cmul(dx, g[l]));
+            if (t >= m && t < Nn) {
+                const double2 dx = make_double2(x0[t].x - x0[m - 1].x, x0[t].y - x0[m - 1].y);
+                g[t] = cdiv(csub(gm, g[t]), cmul(dx, g[t]));
             }
-            coef[m] = g[m];
+            __syncthreads();
+            if (t == 0) coef[m] = g[m];
         }
+        __syncthreads();
     }
     const double e = ek[o] - mu;
-    for (int iz = 0; iz < Nz; ++iz) {
+    for (int iz = t; iz < Nz; iz += blockDim.x) {
         const double2 zz = z[iz];
         double2 sig;
         if (mode == 0) {
@@ -1400,9 +1406,9 @@ __global__ void k_pade_sigma(const double2 *__restrict__ S, const double *__rest
             double2 B = cadd(make_double2(1.0, 0.0), cmul(csub(zz, x0[0]), coef[1]));
             double2 q = cdiv(A, B);
             for (int j = 3; j <= Nn; ++j) {
-                const double2 t = cmul(csub(zz, x0[j - 2]), coef[j - 1]);
-                A = cadd(make_double2(1.0, 0.0), cdiv(t, A));
-                B = cadd(make_double2(1.0, 0.0), cdiv(t, B));
+                const double2 tj = cmul(csub(zz, x0[j - 2]), coef[j - 1]);
+                A = cadd(make_double2(1.0, 0.0), cdiv(tj, A));
+                B = cadd(make_double2(1.0, 0.0), cdiv(tj, B));
                 q = cdiv(cmul(q, A), B);
             }
             sig = cmul(q, coef[0]);
@@ -1881,7 +1887,7 @@ cudaError_t launch_pade_sigma(const GridDev &g, const double2 *S, const double *
                               const double *sinf, const int *nidx, int Nn, const double2 *z, int Nz, int mode,
                               double mu, double T, double2 *out_sig, double *out_A, cudaStream_t st) {
     if (Nn < 2 || Nn > kPadeMax || Nn > g.nw0 / 2) return cudaErrorInvalidValue;
-    k_pade_sigma<<<(g.n8 + 127) / 128, 128, 0, st>>>(S, s2, s3, sinf, g.ek, nidx, Nn, z, Nz, mode, g.n8, g.nw0, mu, T,
+    k_pade_sigma<<<g.n8, 128, 0, st>>>(S, s2, s3, sinf, g.ek, nidx, Nn, z, Nz, mode, g.n8, g.nw0, mu, T,
                                                       out_sig, out_A);
     return launched();
 }
