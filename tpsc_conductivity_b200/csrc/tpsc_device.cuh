@@ -162,6 +162,32 @@ __device__ __forceinline__ auto slice_twiddles(double *S, const double2 *__restr
     }
 }
 
+// L2 prefetch by the CTA of [p, p + bytes), one request per 128-byte line,
+// every address inside the range
+__device__ __forceinline__ void prefetch_l2_range(const void *p, size_t bytes) {
+    const char *c = static_cast<const char *>(p);
+    for (size_t off = (size_t)threadIdx.x * 128; off < bytes; off += (size_t)blockDim.x * 128)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(c + off));
+}
+// L2 prefetch by the CTA of row j of a four-column-block array (NJ rows per
+// block, nblk blocks): one 32-byte piece per block
+__device__ __forceinline__ void prefetch_l2_blockrow(const double *a, int j, int NJ, int nblk) {
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(a + ((size_t)b * NJ + j) * 4));
+}
+
+// CTAs that one launch of `kernel` holds on the GPU at once: a slice kernel's
+// CTA j prefetches the inputs of slice j + this, which the same launch reaches
+// about one wave later
+template <class K>
+int resident_ctas(K kernel, int threads, size_t smem) {
+    int dev = 0, sms = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess) return 0;
+    return sms * per;
+}
+
 // Fill a symmetric NBK x NBK slice from the octant points: value(o) does all
 // global reads of point o and returns its value.  Each thread takes KB points
 // at a time and issues all their reads before storing any of them, so that

@@ -267,12 +267,17 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
 template <int NBK, class GT>
 __global__ void __launch_bounds__(kSliceThreads, 1)
     k_sigma_slice(const GT *__restrict__ Grt, const double *__restrict__ V,
-                  const double2 *__restrict__ tw, int n8, int nw0, double *__restrict__ sigt) {
+                  const double2 *__restrict__ tw, int n8, int nw0, int ahead, double *__restrict__ sigt) {
     extern __shared__ __align__(16) double S[];
     const auto *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
     const int nb = nw0 / 2 + 1;
     const int jv = j < nb ? j : nw0 - j;
+    if (ahead > 0 && j + ahead <= nw0) {
+        const int jn = j + ahead;
+        prefetch_l2_range(Grt + (size_t)jn * n8, (size_t)n8 * sizeof(GT));
+        prefetch_l2_blockrow(V, jn < nb ? jn : nw0 - jn, nb, (n8 + 3) / 4);
+    }
     const GT *g = Grt + (size_t)j * n8;
     fill_octant<NBK>(S, n8, [&](int o) -> double { return (double)g[o] * V[bidx(jv, o, nb)]; });
     __syncthreads();
@@ -1554,7 +1559,8 @@ struct RunSigmaSlice {
         const size_t sm = SliceSmem<NBK>::bytes;
         cudaError_t e = set_smem(k_sigma_slice<NBK, GT>, sm);
         if (e != cudaSuccess) return e;
-        k_sigma_slice<NBK, GT><<<g->nw0 + 1, kSliceThreads, sm, st>>>(Grt, V, g->tw_k, g->n8, g->nw0, sigt);
+        const int ahead = resident_ctas(k_sigma_slice<NBK, GT>, kSliceThreads, sm);
+        k_sigma_slice<NBK, GT><<<g->nw0 + 1, kSliceThreads, sm, st>>>(Grt, V, g->tw_k, g->n8, g->nw0, ahead, sigt);
         return launched();
     }
 };

@@ -80,11 +80,16 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
 template <int NBK>
 __global__ void __launch_bounds__(kSlice32Threads, 2)
     k_chi0_slice32(const float *__restrict__ Grt, const float4 *__restrict__ tw,
-                   int n8, int nw0, double *__restrict__ chirt, double *__restrict__ chiq) {
+                   int n8, int nw0, int ahead, double *__restrict__ chirt, double *__restrict__ chiq) {
     extern __shared__ __align__(16) float S32[];
     const float4 *tws = twiddles32<NBK>(S32, tw);
     const int j = blockIdx.x;
     const int nb = nw0 / 2 + 1;
+    if (ahead > 0 && j + ahead < nb) {
+        const int jn = j + ahead;
+        prefetch_l2_range(Grt + (size_t)jn * n8, (size_t)n8 * sizeof(float));
+        prefetch_l2_range(Grt + (size_t)(nw0 - jn) * n8, (size_t)n8 * sizeof(float));
+    }
     const float *gp = Grt + (size_t)j * n8;
     const float *gm = Grt + (size_t)(nw0 - j) * n8;
     fill_octant<NBK>(S32, n8, [&](int o) -> float {
@@ -115,10 +120,12 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
 template <int NBK>
 __global__ void __launch_bounds__(kSlice32Threads, 2)
     k_vertex_q32(const double *__restrict__ chiq, const float4 *__restrict__ tw,
-                 int n8, int nb, double normFact, double U, double Usp, double Uch, double *__restrict__ Vr) {
+                 int n8, int nb, int ahead, double normFact, double U, double Usp, double Uch,
+                 double *__restrict__ Vr) {
     extern __shared__ __align__(16) float S32[];
     const float4 *tws = twiddles32<NBK>(S32, tw);
     const int j = blockIdx.x;
+    if (ahead > 0 && j + ahead < nb) prefetch_l2_blockrow(chiq, j + ahead, nb, (n8 + 3) / 4);
     fill_octant<NBK>(S32, n8, [&](int o) -> float {
         const double c0 = chiq[bidx(j, o, nb)];
         const double a = 0.5 * Usp, b = 0.5 * Uch;
@@ -152,7 +159,8 @@ struct RunChi0Slice32 {
         const size_t sm = Slice32Smem<NBK>::bytes;
         cudaError_t e = set_smem(k_chi0_slice32<NBK>, sm);
         if (e != cudaSuccess) return e;
-        k_chi0_slice32<NBK><<<g->nb, kSlice32Threads, sm, st>>>(Grt, g->tw_k32, g->n8, g->nw0, chirt, chiq);
+        const int ahead = resident_ctas(k_chi0_slice32<NBK>, kSlice32Threads, sm);
+        k_chi0_slice32<NBK><<<g->nb, kSlice32Threads, sm, st>>>(Grt, g->tw_k32, g->n8, g->nw0, ahead, chirt, chiq);
         return launched();
     }
 };
@@ -164,8 +172,9 @@ struct RunVertexQ32 {
         cudaError_t e = set_smem(k_vertex_q32<NBK>, sm);
         if (e != cudaSuccess) return e;
         const double normFact = T / ((double)g->nk0 * g->nk0);
-        k_vertex_q32<NBK><<<g->nb, kSlice32Threads, sm, st>>>(chiq, g->tw_k32, g->n8, g->nb, normFact, U, Usp,
-                                                              Uch, Vr);
+        const int ahead = resident_ctas(k_vertex_q32<NBK>, kSlice32Threads, sm);
+        k_vertex_q32<NBK><<<g->nb, kSlice32Threads, sm, st>>>(chiq, g->tw_k32, g->n8, g->nb, ahead, normFact, U,
+                                                              Usp, Uch, Vr);
         return launched();
     }
 };
