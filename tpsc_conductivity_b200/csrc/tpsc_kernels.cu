@@ -491,6 +491,32 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
     }
 }
 
+// Stage the two columns 2 half, 2 half + 1 of a four-column block (NJ rows)
+// column-major into A; columns >= n8 as zeros.  A row of the pair is 16
+// contiguous, 16-byte aligned bytes: each thread issues eight 16-byte
+// streaming loads before storing any.  The caller's barrier publishes them.
+__device__ __forceinline__ void stage_pair4(double *A, const double *blk4, int NJ, int half, int o0, int n8) {
+    const double2 *src = reinterpret_cast<const double2 *>(blk4 + 2 * half);
+    const bool c0 = o0 < n8, c1 = o0 + 1 < n8;
+    constexpr int B = 8;
+    for (int base = threadIdx.x; base < NJ; base += B * blockDim.x) {
+        double2 v[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            const int j = base + b * blockDim.x;
+            if (j < NJ) v[b] = __ldcs(&src[2 * j]);
+        }
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            const int j = base + b * blockDim.x;
+            if (j < NJ) {
+                A[j] = c0 ? v[b].x : 0.0;
+                A[NJ + j] = c1 ? v[b].y : 0.0;
+            }
+        }
+    }
+}
+
 // The same transform for ONE pair of columns per CTA, two CTAs per SM: the
 // pair is staged in a buffer of padded_len(N) complex and the FFT runs in
 // place in it (its first pass reads the spline's third derivatives before the
@@ -518,21 +544,18 @@ __global__ void __launch_bounds__(256, 2)
     __shared__ double d0[2], dN[2];
     const int pair = blockIdx.x, blk = pair >> 1, half = pair & 1;
     const int o0 = 2 * pair;
+    // the end slopes, read before the staging wait
+    double d0r = 0.0, dNr = 0.0;
+    if (threadIdx.x < 2) {
+        d0r = dS[o0 + threadIdx.x];
+        dNr = dS[n8p + o0 + threadIdx.x];
+    }
     tau_tables(tw2, tw2 + 1, tw, ht, N);
     // the pair's two columns of the four-column block, column-major
-    const double *g = sigt + (size_t)blk * 4 * NJ + 2 * half;
-    for (int i = threadIdx.x; i < 2 * NJ; i += blockDim.x) {
-        const int c = i & 1, j = i >> 1;
-        double *dst = &A[c * NJ + j];
-        if (o0 + c < n8)
-            cp_async8(dst, g + 4 * j + c);
-        else
-            *dst = 0.0;
-    }
-    cp_async_wait_all();
+    stage_pair4(A, sigt + (size_t)blk * 4 * NJ, NJ, half, o0, n8);
     if (threadIdx.x < 2) {
-        d0[threadIdx.x] = dS[o0 + threadIdx.x];
-        dN[threadIdx.x] = dS[n8p + o0 + threadIdx.x];
+        d0[threadIdx.x] = d0r;
+        dN[threadIdx.x] = dNr;
     }
     __syncthreads();
     if (threadIdx.x < 2) {
@@ -574,22 +597,6 @@ __global__ void __launch_bounds__(256, 2)
     }
 }
 
-// Stage the two columns 2 half, 2 half + 1 of a four-column block (NJ rows)
-// column-major into A; columns >= n8 as zeros.  The caller's barrier
-// publishes them.
-__device__ __forceinline__ void stage_pair4(double *A, const double *blk4, int NJ, int half, int o0, int n8) {
-    const double *g = blk4 + 2 * half;
-    for (int i = threadIdx.x; i < 2 * NJ; i += blockDim.x) {
-        const int c = i & 1, j = i >> 1;
-        double *dst = &A[c * NJ + j];
-        if (o0 + c < n8)
-            cp_async8(dst, g + 4 * j + c);
-        else
-            *dst = 0.0;
-    }
-    cp_async_wait_all();
-}
-
 // k_chi0_tau for one pair per CTA (in-place FFT, two CTAs per SM); results
 // go straight back to chiq.
 template <int N>
@@ -606,11 +613,12 @@ __global__ void __launch_bounds__(256, 2)
     const int pair = blockIdx.x, blk = pair >> 1, half = pair & 1;
     const int o0 = 2 * pair;
     double *g = chiq + (size_t)blk * 4 * NJ + 2 * half;
+    // the left end slope, read before the staging wait
+    const double d0r = (threadIdx.x < 2 && o0 + (int)threadIdx.x < n8) ? dtau_chiqt0[o0 + threadIdx.x] : 0.0;
     tau_tables(tw2, tw2 + 1, tw, tw, N);
     stage_pair4(A, chiq + (size_t)blk * 4 * NJ, NJ, half, o0, n8);
     if (threadIdx.x < 2) {
-        const int o = o0 + threadIdx.x;
-        d0[threadIdx.x] = o < n8 ? dtau_chiqt0[o] : 0.0;
+        d0[threadIdx.x] = d0r;
         dN[threadIdx.x] = 0.0;
     }
     __syncthreads();
@@ -692,11 +700,13 @@ __global__ void __launch_bounds__(256, 2)
     }
     __syncthreads();
     double *g = Vr + (size_t)blk * 4 * NJ + 2 * half;
-    const double *cr = chirt + (size_t)blk * 4 * NJ + 2 * half;
+    // the pair's chi0(r, tau) values of a row are 16 contiguous bytes
+    const double2 *cr = reinterpret_cast<const double2 *>(chirt + (size_t)blk * 4 * NJ + 2 * half);
     for (int n = threadIdx.x; n < NJ; n += blockDim.x) {
         const double2 Z = X[pidx(n)];
-        g[4 * n] = (o0 < n8) ? Z.x + fact * cr[4 * n] : 0.0;
-        g[4 * n + 1] = (o0 + 1 < n8) ? Z.y + fact * cr[4 * n + 1] : 0.0;
+        const double2 c = __ldcs(&cr[2 * n]);
+        g[4 * n] = (o0 < n8) ? Z.x + fact * c.x : 0.0;
+        g[4 * n + 1] = (o0 + 1 < n8) ? Z.y + fact * c.y : 0.0;
     }
 }
 
