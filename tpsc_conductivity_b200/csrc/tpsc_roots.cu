@@ -143,6 +143,16 @@ __device__ void newton_update(RootCtl &c, double y, double dy, double tol) {
 // partials in the same order and takes the same Newton step on its own copy
 // of the state (identical in every block).  A buffer is rewritten two
 // iterations later, after a barrier that every reader of it has passed.
+//
+// The spin search iterates on s = -ln(1 - Us/hi), hi = 2/chi0max - 2 eps,
+// Us = -hi expm1(-s): R_sp has the AFM pole at hi and behaves like -ln of the
+// distance to it, so Newton in Us overshoots the pole and falls back to
+// bisection step after step, while in s it converges in a few steps.  The
+// root is the same zero of R_sp.
+constexpr double kSpinSMax = 40.0;  // -hi expm1(-40) = hi (1 - 4e-18)
+
+__device__ __forceinline__ double spin_us(double s, double hi) { return -hi * expm1(-s); }
+
 __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
     __shared__ RootCtl sc;
     __shared__ int s_jdir, s_tail;
@@ -154,11 +164,13 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
     for (int phase = 0; phase < 2; ++phase) {
         const double sgn = phase == 0 ? -1.0 : 1.0;
         if (threadIdx.x == 0) {
-            sc.lo = 0.0;
-            sc.hi = phase == 0 ? a.hi_sp : 1000.0 * a.U;
+            const double hi = phase == 0 ? a.hi_sp : 1000.0 * a.U;
             // spin: U/2 (clamped inside the interval); charge: U
             const double x0 = phase == 0 ? a.U / 2.0 : a.U;
-            sc.x = (x0 > sc.lo && x0 < sc.hi) ? x0 : 0.5 * (sc.lo + sc.hi);
+            const double xs = (x0 > 0.0 && x0 < hi) ? x0 : 0.5 * hi;
+            sc.lo = 0.0;
+            sc.hi = phase == 0 ? kSpinSMax : hi;
+            sc.x = phase == 0 ? -log1p(-xs / hi) : xs;
             sc.prev_step = 0.0;
             sc.nev = sc.it = sc.done = sc.ok = 0;
         }
@@ -166,7 +178,7 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
 #pragma unroll 1
         while (!sc.done) {
             if (threadIdx.x == 0) {
-                const double ah = fabs(sc.x) / 2.0;
+                const double ah = fabs(phase == 0 ? spin_us(sc.x, a.hi_sp) : sc.x) / 2.0;
                 // first frequency of the series (cmax_suf does not increase)
                 int lo = 0, hi = a.nb;
                 while (lo < hi) {
@@ -180,7 +192,7 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
                 s_tail = ah * a.tailm[kMomP] >= kMomSeriesMax;
             }
             __syncthreads();
-            const double x = sc.x, hu = sgn * x / 2.0;
+            const double x = phase == 0 ? spin_us(sc.x, a.hi_sp) : sc.x, hu = sgn * x / 2.0;
             const int jdir = s_jdir;
             double v = 0.0, dv = 0.0;
             const long long total = (long long)a.nblk * jdir;
@@ -246,7 +258,8 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
                     if (phase == 0) {
                         // chi::sum_rule_sp (src/chi.cpp:833-836)
                         y = tr + n - n * n / 2.0 - nsr + x * nsr * nsr / (2.0 * U);
-                        dy = dtr + nsr * nsr / (2.0 * U);
+                        // d/ds = d/dUs * dUs/ds, dUs/ds = hi e^-s = hi - Us
+                        dy = (dtr + nsr * nsr / (2.0 * U)) * (a.hi_sp - x);
                     } else {
                         // chi::sum_rule_ch (src/chi.cpp:840-843)
                         y = tr + n - n * n / 2.0 - (nsr + Usp * nsr * nsr / (2.0 * U) - nsr * nsr);
@@ -257,9 +270,10 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
             }
             __syncthreads();
         }
-        if (phase == 0) Usp = sc.root;
+        const double root = phase == 0 ? spin_us(sc.root, a.hi_sp) : sc.root;
+        if (phase == 0) Usp = root;
         if (blockIdx.x == 0 && threadIdx.x == 0) {
-            a.out[phase] = sc.root;
+            a.out[phase] = root;
             a.out[2 + phase] = sc.nev;
             a.out[4 + phase] = sc.ok;
         }
