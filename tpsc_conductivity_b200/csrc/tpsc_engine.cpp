@@ -303,6 +303,7 @@ struct Grid {
     double2 *t_fd = nullptr;
     double tailq_T = -1.0;         // temperature the tail power sums were built for
     double tailq_host[kTailQ] = {0};
+    double tailP_host[kTailP] = {0};
     std::vector<void *> allocs;
     // current-current correlator: device state (allocated on first use) and
     // the last result, [n_theta 2 NB] binned, [2 NB] totals, kx0
@@ -508,6 +509,7 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
     A(dalloc(g, &d.ek, n8));
     A(dalloc(g, &d.gk, n8));
     A(dalloc(g, &d.tailq, (size_t)kTailQ));
+    A(dalloc(g, &d.tailP, (size_t)kTailP));
     A(dalloc(g, &d.er, n8));
     A(dalloc(g, &g->Grt, (nw + 1) * n8));
     A(dalloc(g, &g->chirt, nb * n8p));
@@ -585,6 +587,18 @@ int grid_set_model(tpsc_ctx *ctx, Grid *g) {
         }
         for (int k = 0; k < kTailQ; ++k) g->tailq_host[k] = (double)acc[k];
         CK(cudaMemcpyAsync(d.tailq, g->tailq_host, kTailQ * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+        // P_p = sum_{t=0}^{Nw0/2} w^-p, w = (Nw0 + 2t + 1) pi T: the fermionic tail of
+        // the find_mu moments (largest t first, long double)
+        std::vector<long double> pw(kTailP, 0.0L);
+        const int NO = d.nw0 / 2;
+        for (int t = NO; t >= 0; --t) {
+            const long double x = 1.0L / ((2.0L * (NO + t) + 1.0L) * 3.141592653589793238462643383279502884L *
+                                          (long double)ctx->T);
+            long double xp = 1.0L;
+            for (int k = 0; k < kTailP; ++k, xp *= x) pw[k] += xp;
+        }
+        for (int k = 0; k < kTailP; ++k) g->tailP_host[k] = (double)pw[k];
+        CK(cudaMemcpyAsync(d.tailP, g->tailP_host, kTailP * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
         g->tailq_T = ctx->T;
     }
     CK(cudaStreamSynchronize(ctx->st));

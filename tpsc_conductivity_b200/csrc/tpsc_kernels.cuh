@@ -19,6 +19,7 @@ struct GridDev {
     double *er = nullptr;          // [n8] real-space hopping table
     double *w16 = nullptr;         // [n8p] octant weight: 16 halved on edges and diagonal, 0 on padding
     double *tailq = nullptr;       // [kTailQ] sum-rule tail power sums Q_k = sum_n qn^-2k (T dependent)
+    double *tailP = nullptr;       // [kTailP] P_p = sum over the fermionic tail n = Nw0/2..Nw0 of w_n^-p
     double2 *tw_k = nullptr;       // [L]   exp(-2 pi i m / L)
     float4 *tw_k32 = nullptr;      // [L]   the same as (cos, sin) rounded to float, then the float remainders
     double2 *tw_w = nullptr;       // [Nw0] exp(-2 pi i m / Nw0)
@@ -35,6 +36,7 @@ __host__ __device__ inline size_t bidx(int j, int o, int NJ) {
 }
 
 constexpr int kMaxBlocks = 4096;
+constexpr int kTailP = 41;  // P_p for p < kTailP: the find_mu tail series uses p <= kMuMomP + 28
 constexpr int kTailQ = 20;  // Q_k for k < kTailQ (the series uses k <= 18)  // >= column blocks of the largest grid (2097)
 struct Reduce {
     double *partial = nullptr;   // [4 * kMaxBlocks]

@@ -304,12 +304,15 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
 // G0 share one reciprocal per (k, n), so that two CTAs fit on an SM.
 // One CTA per column block, per-block partials (block_store).
 constexpr int kMuMomF64 = 4;
+constexpr int kTailR = 28;           // terms of the tail power series (needs kMuMomP + kTailR < kTailP)
+constexpr double kTailRatio = 0.05;  // series when rho / w_NO < this: terms below 0.05^28 (~1e-36) relative
+static_assert(kMuMomP + kTailR < kTailP, "tail power sums too short");
 
 __global__ void __launch_bounds__(256, 2)
     k_sigma_moments(const double2 *__restrict__ S, const double *__restrict__ s2, const double *__restrict__ s3,
                     const double *__restrict__ s4, const double *__restrict__ sinfp, const double *__restrict__ ek,
-                    const double *__restrict__ w16, int nw0, double mu0, double T, double nk02, int jc,
-                    double *partial) {
+                    const double *__restrict__ w16, const double *__restrict__ tailP, int nw0, double mu0,
+                    double T, double nk02, int jc, double *partial) {
     constexpr int NV = kSigmaMomNV, P64 = kMuMomF64, P32 = kMuMomP - kMuMomF64;
     __shared__ double cw[4], cx[4], c2[4], c3[4], c4[4];
     const int blk = blockIdx.x, o0 = 4 * blk, NO = nw0 / 2;
@@ -375,15 +378,85 @@ __global__ void __launch_bounds__(256, 2)
             if (j >= jc) moments(wn, rS, iS, x, w, inv);
         }
     }
-    for (int t = threadIdx.x; t <= NO; t += blockDim.x) {
-        const double wn = (2 * (NO + t) + 1) * pt, i1 = 1.0 / wn, i2 = i1 * i1;
+    // The tail n = NO .. 2 NO (asymptotic Sigma), warp c for column c: with
+    // u = 1/(i w_n), z^-1 = u / (1 - q(u)), q(u) = x u + Sinf u^2 + C2 u^3 +
+    // C3 u^4 + C4 u^5 (real coefficients), and h^(p) the coefficients of
+    // (1 - q)^-p,
+    //   sum_tail z^-p = sum_r h^(p)_r (-i)^(p+r) P_(p+r),
+    //   sum_tail Re 1/(i w_n - x) = -x sum_k (-x^2)^k P_(2k+2),
+    // P_p = sum_tail w_n^-p (tailP).  (1 - q)^-p obeys H' (1 - q) = p q' H, so
+    //   R h_R = sum_{s=1..5} q_s h_(R-s) (R - s + p s),   h_0 = 1:
+    // lane p - 1 runs the recurrence of moment m = p - 1 in registers.  The
+    // terms fall like (rho / w_NO)^r, rho a bound on q's root radius; above
+    // kTailRatio the warp sums term by term.
+    {
+        __shared__ double tP[kTailP];
+        for (int k = threadIdx.x; k < kTailP; k += blockDim.x) tP[k] = tailP[k];
+        __syncthreads();
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (warp < 4 && cw[warp] != 0.0) {
+            const int c = warp;
+            const double w = cw[c], x = cx[c];
+            const double q1 = x, q2 = sinf, q3 = c2[c], q4 = c3[c], q5 = c4[c];
+            const double rho = fabs(x) + sqrt(fabs(sinf)) + cbrt(fabs(q3)) + sqrt(sqrt(fabs(q4))) + pow(fabs(q5), 0.2);
+            const double w_no = (2 * NO + 1) * pt;
+            if (rho < kTailRatio * w_no) {
+                double re = 0.0, im = 0.0;
+                if (lane < kMuMomP) {
+                    const double p = lane + 1;
+                    // h_(R-1) .. h_(R-5) in a register window
+                    double h1 = 1.0, h2 = 0.0, h3 = 0.0, h4 = 0.0, h5 = 0.0;
+                    // r = 0 term: (-i)^p P_p
+                    auto add = [&](int k, double h) {
+                        const double t = h * tP[k];
+                        switch (k & 3) {
+                            case 0: re += t; break;
+                            case 1: im -= t; break;
+                            case 2: re -= t; break;
+                            default: im += t; break;
+                        }
+                    };
+                    add(lane + 1, 1.0);
+                    for (int R = 1; R <= kTailR; ++R) {
+                        const double hR = (q1 * h1 * (R - 1 + p) + q2 * h2 * (R - 2 + 2 * p) +
+                                           q3 * h3 * (R - 3 + 3 * p) + q4 * h4 * (R - 4 + 4 * p) +
+                                           q5 * h5 * (R - 5 + 5 * p)) /
+                                          R;
+                        add(lane + 1 + R, hR);
+                        h5 = h4;
+                        h4 = h3;
+                        h3 = h2;
+                        h2 = h1;
+                        h1 = hR;
+                    }
+                } else if (lane == kMuMomP) {
+                    // G0: -x sum_k (-x^2)^k P_(2k+2)
+                    double xp = 1.0;
+                    for (int k = 0; 2 * k + 2 < kTailP; ++k, xp *= -x * x) re += xp * tP[2 * k + 2];
+                    re *= -x;
+                }
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const double w = cw[c];
-            if (w == 0.0) continue;
-            const double x = cx[c];
-            moments(wn, -c2[c] * i2 + c4[c] * i2 * i2, -sinf * i1 + c3[c] * i2 * i1, x, w,
-                    1.0 / (wn * wn + x * x));
+                for (int m = 0; m < kMuMomP; ++m) {
+                    const double rm = __shfl_sync(0xffffffffu, re, m), imm = __shfl_sync(0xffffffffu, im, m);
+                    if (lane == 0) {
+                        if (m < P64) {
+                            m64[2 * m] += w * rm;
+                            m64[2 * m + 1] += w * imm;
+                        } else {
+                            m32[2 * (m - P64)] += (float)(w * rm);
+                            m32[2 * (m - P64) + 1] += (float)(w * imm);
+                        }
+                    }
+                }
+                const double gt = __shfl_sync(0xffffffffu, re, kMuMomP);
+                if (lane == 0) g0 += w * gt;
+            } else {
+                for (int t = lane; t <= NO; t += 32) {
+                    const double wn = (2 * (NO + t) + 1) * pt, i1 = 1.0 / wn, i2 = i1 * i1;
+                    moments(wn, -c2[c] * i2 + c4[c] * i2 * i2, -sinf * i1 + c3[c] * i2 * i1, x, w,
+                            1.0 / (wn * wn + x * x));
+                }
+            }
         }
     }
     double acc[NV];
@@ -586,7 +659,8 @@ cudaError_t launch_sigma_moments(const GridDev &g, const double2 *S, const doubl
                                  cudaStream_t st) {
     const int nblk = g.n8p / 4;
     const double nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
-    k_sigma_moments<<<nblk, 256, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.nw0, mu0, T, nk02, jc, r.partial);
+    k_sigma_moments<<<nblk, 256, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.tailP, g.nw0, mu0, T, nk02, jc,
+                                          r.partial);
     cudaError_t e = launched();
     if (e != cudaSuccess) return e;
     return finish<kSigmaMomNV>(r, nblk, 0.0, st);
