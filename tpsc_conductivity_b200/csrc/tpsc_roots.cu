@@ -337,9 +337,8 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
     for (int k = 0; k < 2 * P32; ++k) m32[k] = 0.0f;
     // z = i w_n - x - Sigma with x = eps - mu0; inv = 1 / (w_n^2 + x^2)
-    auto moments = [&](double wn, double rS, double iS, double x, double w, double inv) {
-        const double zx = -x - rS, zy = wn - iS;
-        const double rr = 1.0 / (zx * zx + zy * zy);  // |z| >= w_n > 0
+    // rr = 1/|z|^2 (|z| >= w_n > 0)
+    auto moments_rr = [&](double zx, double zy, double rr, double x, double w, double inv) {
         const double2 zi = make_double2(zx * rr, -zy * rr);
         double2 zp = zi;
 #pragma unroll
@@ -359,6 +358,10 @@ __global__ void __launch_bounds__(256, 2)
         }
         g0 -= w * x * inv;
     };
+    auto moments = [&](double wn, double rS, double iS, double x, double w, double inv) {
+        const double zx = -x - rS, zy = wn - iS;
+        moments_rr(zx, zy, 1.0 / (zx * zx + zy * zy), x, w, inv);
+    };
     const double4 *row = reinterpret_cast<const double4 *>(S + (size_t)blk * 4 * NO);
     for (int j = threadIdx.x; j < NO; j += blockDim.x) {
         const double wn = (2 * j + 1) * pt, i1 = 1.0 / wn;
@@ -372,10 +375,19 @@ __global__ void __launch_bounds__(256, 2)
             double rS, iS;
             sigma_full(i1, sinf, c2[c], c3[c], sv[c], rS, iS);
             const double x = cx[c];
-            const double inv = 1.0 / (wn * wn + x * x);
-            tsg += w * inv * (rS * (-x) + iS * wn);
-            har += w * inv;
-            if (j >= jc) moments(wn, rS, iS, x, w, inv);
+            const double b = wn * wn + x * x;
+            if (j >= jc) {
+                // one reciprocal for 1/(w_n^2 + x^2) and 1/|z|^2
+                const double zx = -x - rS, zy = wn - iS, a = zx * zx + zy * zy;
+                const double r = 1.0 / (a * b), inv = r * a;
+                tsg += w * inv * (rS * (-x) + iS * wn);
+                har += w * inv;
+                moments_rr(zx, zy, r * b, x, w, inv);
+            } else {
+                const double inv = 1.0 / b;
+                tsg += w * inv * (rS * (-x) + iS * wn);
+                har += w * inv;
+            }
         }
     }
     // The tail n = NO .. 2 NO (asymptotic Sigma), warp c for column c: with
