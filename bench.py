@@ -17,7 +17,8 @@ model parameters (synthetic; no dataset exists for this path).
   data path) and the time is the max over ranks.
 * e2e: the same solve through the public API with the model's lattice tables
   copied host->device and the self-energy Sigma(k, i w_n) (S, C2, C3, C4) and
-  scalars copied device->pinned host inside the timed region.
+  scalars copied device->pinned host inside the timed region; each step's
+  copy overlaps the next step's compute (tpsc_get_self_async).
 * roofline: every stage kernel re-launched alone and timed with CUDA events;
   the dominant one (largest share of a solve) against the measured HBM copy
   bandwidth.
@@ -237,25 +238,41 @@ def our_arm(a, world, rank, local_rank):
     value_ref = world * a.steps / (ms_ref / 1e3)
     value_n64 = world * a.steps / (ms_n64 / 1e3)
 
-    # ---- end to end through the public API ------------------------------------
+    # ---- end to end through the public API: every step sets the model (its
+    # lattice tables go host -> device), solves and copies Sigma (S, C2, C3,
+    # C4: 275 MB) and the scalars back to pinned host memory.  The copy of
+    # step i runs on the library's copy stream while step i + 1 computes
+    # (tpsc_get_self_async, two alternating pinned buffers); the timed region
+    # ends after the last copy.  The working set (~2.4 GB) exceeds L2, so no
+    # flush is needed between steps. ---------------------------------------------
     nk0, nw0, nbk, n8 = g.dims()
-    S_host = torch.empty((nw0 // 2, n8, 2), dtype=torch.float64).pin_memory().numpy()
-    S_c = S_host.view(np.complex128)[..., 0]
+    bufs = []
+    for _ in range(2):
+        S_host = torch.empty((nw0 // 2, n8, 2), dtype=torch.float64).pin_memory().numpy()
+        v = [torch.empty(n8, dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
+        bufs.append((S_host.view(np.complex128)[..., 0], v))
     h2d = 2 * n8 * 8
-    d2h = S_c.nbytes + 3 * n8 * 8 + len(_lib.SCALARS) * 8
-    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
-    for i in range(a.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        ev2[i][0].record(stream)
-        g2 = Green(w["nk0"], w["Nw0"], w["n"], w["T"], 0.1, (w["tp"], w["tpp"], w["t3"], w["U"]), ctx=ctx)
-        g2.set_form(MIXED)
-        g2.solve()
-        g2.self_energy(out=S_c)
-        g2.scalars()
-        ev2[i][1].record(stream)
+    d2h = bufs[0][0].nbytes + 3 * n8 * 8 + len(_lib.SCALARS) * 8
+
+    def e2e_steps(k):
+        for i in range(k):
+            g2 = Green(w["nk0"], w["Nw0"], w["n"], w["T"], 0.1, (w["tp"], w["tpp"], w["t3"], w["U"]), ctx=ctx)
+            g2.set_form(MIXED)
+            g2.solve()
+            S_c, v = bufs[i % 2]
+            g2.self_energy_async(S_c, *v)
+            g2.scalars()
+        g2.wait_copies(join_stream=True)
+
+    e2e_steps(2)
     torch.cuda.synchronize()
-    ms2 = allreduce_max(sum(s.elapsed_time(e) for s, e in ev2), world, dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    e2e_steps(a.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    g.wait_copies()
+    ms2 = allreduce_max(e0.elapsed_time(e1), world, dev)
     e2e = world * a.steps / (ms2 / 1e3)
 
     # ---- per-kernel timing (stages re-launched alone, in order, as the

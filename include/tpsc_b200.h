@@ -182,6 +182,20 @@ int tpsc_get_vertex(tpsc_ctx *ctx, double *vertex_rt);
 /* Self_kw_array [ (Nw0/2) * N8 ] complex (interleaved), Sigma_inf2/3/4 [N8]. */
 int tpsc_get_self(tpsc_ctx *ctx, double *self_kw, double *sigma_inf2, double *sigma_inf3, double *sigma_inf4);
 
+/* The arrays of tpsc_get_self without waiting for them (no counterpart in
+ * the reference): the self-energy is snapshotted on the device, in the
+ * getter's layout, on the context stream, and the snapshot is copied to the
+ * host on a separate copy stream, so that the next stages -- the next solve
+ * included -- run while the copy is in flight.  Two snapshots alternate; a
+ * snapshot is reused only after its previous copy has finished.  The copies
+ * overlap other work only for page-locked (pinned) host buffers.  The host
+ * buffers may be read only after tpsc_wait_copies(ctx, 0). */
+int tpsc_get_self_async(tpsc_ctx *ctx, double *self_kw, double *sigma_inf2, double *sigma_inf3, double *sigma_inf4);
+/* Waits for the copies of tpsc_get_self_async (join_stream = 0), or, with
+ * join_stream = 1, makes the context stream wait for them without blocking
+ * the host (work and events queued on the stream afterwards follow them). */
+int tpsc_wait_copies(tpsc_ctx *ctx, int join_stream);
+
 /* ---- real-frequency continuation (needs tpsc_find_mu) -------------------- */
 /* Sigma(k, z) and A(k, z) = -Im 1/(z - eps_k + mu - Sigma(k, z)) / pi for every
  * octant k at the Nz complex energies z (interleaved re, im), from Sigma

@@ -28,6 +28,8 @@ SIGNATURES = [
     ("tpsc_find_Usp_Uch", C.c_int, [C.c_void_p]),
     ("tpsc_sp_corr_length", C.c_int, [C.c_void_p, _dp]),
     ("tpsc_sumrule_tangents", C.c_int, [C.c_void_p, _dp]),
+    ("tpsc_get_self_async", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    ("tpsc_wait_copies", C.c_int, [C.c_void_p, C.c_int]),
     ("tpsc_sumrule_vjp", C.c_int, [C.c_void_p, _dp, _dp]),
     ("tpsc_set_mu_shift", C.c_int, [C.c_void_p, C.c_double]),
     ("tpsc_batch_create", C.c_void_p, [C.c_int, C.c_int, _ip]),

@@ -193,6 +193,18 @@ class Green:
         self.ctx.call("tpsc_get_self", _dptr(out.view(np.float64)), _dptr(s2), _dptr(s3), _dptr(s4))
         return dict(S=out, Sigma_inf2=s2, Sigma_inf3=s3, Sigma_inf4=s4)
 
+    def self_energy_async(self, out, s2=None, s3=None, s4=None):
+        """The arrays of self_energy() copied to the host without waiting
+        (tpsc_get_self_async): ``out`` complex [Nw0/2, N8] (and the optional
+        float64 [N8] arrays) must stay alive, and should be pinned for the copy
+        to overlap the next stages; read them after wait_copies()."""
+        self.ctx.call("tpsc_get_self_async", _dptr(out.view(np.float64)), _dptr(s2), _dptr(s3), _dptr(s4))
+
+    def wait_copies(self, join_stream=False):
+        """Waits for the copies of self_energy_async (or, with join_stream, makes
+        the context stream wait for them)."""
+        self.ctx.call("tpsc_wait_copies", 1 if join_stream else 0)
+
     def sigma(self):
         """Full Sigma(k, i w_n), n < Nw0/2 (src/green.cpp:3039)."""
         r = self.self_energy()

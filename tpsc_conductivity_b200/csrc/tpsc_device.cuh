@@ -164,6 +164,12 @@ __device__ __forceinline__ auto slice_twiddles(double *S, const double2 *__restr
 
 // L2 prefetch by the CTA of [p, p + bytes), one request per 128-byte line,
 // every address inside the range
+// U (3 Usp + Uch) / 8 from the device pair Usc = (Usp, Uch), rounded as the
+// host expression is (no contraction into an FMA)
+__device__ __forceinline__ double vertex_fact(double U, const double *Usc) {
+    return __dmul_rn(U, __dadd_rn(__dmul_rn(3.0, Usc[0]), Usc[1])) / 8.0;
+}
+
 __device__ __forceinline__ void prefetch_l2_range(const void *p, size_t bytes) {
     const char *c = static_cast<const char *>(p);
     for (size_t off = (size_t)threadIdx.x * 128; off < bytes; off += (size_t)blockDim.x * 128)

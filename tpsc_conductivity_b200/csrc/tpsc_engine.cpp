@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <initializer_list>
 #include <limits>
 #include <map>
 #include <string>
@@ -325,7 +326,11 @@ struct tpsc_ctx {
     Reduce red;
     Reduce redm;              // moment sums: partial [(2 kMomP + 1) kMaxBlocks], result [32]
     RootScratch roots;        // the device root searches' state
-    double *h_res = nullptr;  // pinned, 32 doubles
+    // device results the later stages read without a host round trip:
+    // [0..5] Usp, Uch, evals_sp, evals_ch, ok_sp, ok_ch (the vertex reads [0..1])
+    double *dres = nullptr;
+    double *h_res = nullptr;  // pinned and mapped, 32 doubles
+    unsigned *h_res_dev = nullptr;  // its device address: the readback kernel writes there
     // model
     bool have_model = false;
     long long model_id = 0;   // incremented by every tpsc_set_model
@@ -340,6 +345,13 @@ struct tpsc_ctx {
     cudaEvent_t ev[6] = {};
     void *stage = nullptr;
     size_t stage_bytes = 0;
+    // tpsc_get_self_async: two device snapshots of Sigma, copied out on cst
+    cudaStream_t cst = nullptr;
+    cudaEvent_t snap_ev[2] = {}, copy_ev[2] = {};
+    void *snap[2] = {nullptr, nullptr};
+    size_t snap_bytes[2] = {0, 0};
+    int snap_next = 0;
+    bool copies_pending = false;
     std::string err;
 };
 
@@ -544,11 +556,32 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
     return TPSC_OK;
 }
 
+// Small device ranges (bytes a multiple of 4) copied into ctx->h_res at the
+// given double offsets by one kernel on ctx->st, then a wait on ctx->st.  The
+// kernel writes the mapped pinned buffer directly, so the readback takes no
+// copy engine and never waits behind a Sigma copy-out queued on ctx->cst.
+struct Piece {
+    const void *src;
+    size_t bytes;
+    int at;  // offset in ctx->h_res, doubles
+};
+int read_back(tpsc_ctx *ctx, std::initializer_list<Piece> pieces) {
+    GatherPieces p;
+    for (const Piece &q : pieces) {
+        p.src[p.n] = static_cast<const unsigned *>(q.src);
+        p.words[p.n] = (long long)(q.bytes / sizeof(unsigned));
+        p.dst[p.n] = 2LL * q.at;
+        ++p.n;
+    }
+    CK(launch_gather(p, ctx->h_res_dev, 1, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return TPSC_OK;
+}
+
 // device scalar readback after a reduction launched on ctx->st
 int read_result(tpsc_ctx *ctx, int count, double *out, const double *src = nullptr) {
-    CK(cudaMemcpyAsync(ctx->h_res, src ? src : ctx->red.result, count * sizeof(double), cudaMemcpyDeviceToHost,
-                       ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+    int rc = read_back(ctx, {{src ? src : ctx->red.result, count * sizeof(double), 0}});
+    if (rc) return rc;
     for (int i = 0; i < count; ++i) out[i] = ctx->h_res[i];
     return TPSC_OK;
 }
@@ -677,7 +710,46 @@ int join_side(tpsc_ctx *ctx, int k) {
     return TPSC_OK;
 }
 
-int run_chi0(tpsc_ctx *ctx) {
+// ---- results read back from the device, checked and stored in ctx->scal ----
+// r = (chi0max, qmax0, qmax1)
+int set_chi0max(tpsc_ctx *ctx, const double *r) {
+    ctx->scal[TPSC_S_CHI0MAX] = r[0];
+    ctx->scal[TPSC_S_QMAX0] = r[1];
+    ctx->scal[TPSC_S_QMAX1] = r[2];
+    if (!std::isfinite(r[0]) || r[0] <= 0.0) return fail(ctx, TPSC_ERR_NONFINITE, "chi0(q, 0) has no positive maximum");
+    return TPSC_OK;
+}
+// r = (Usp, Uch, evals_sp, evals_ch, ok_sp, ok_ch) of the device search, err its barrier flag
+int set_roots(tpsc_ctx *ctx, const double *r, unsigned err) {
+    if (err) return fail(ctx, TPSC_ERR_CUDA, "device root search: grid barrier timed out");
+    if (r[4] != 1.0) return fail(ctx, TPSC_ERR_NO_ROOT, "Usp not found");
+    if (r[5] != 1.0) return fail(ctx, TPSC_ERR_NO_ROOT, "Uch not found");
+    ctx->Usp = r[0];
+    ctx->Uch = r[1];
+    ctx->scal[TPSC_S_EVALS_SP] = r[2];
+    ctx->scal[TPSC_S_EVALS_CH] = r[3];
+    ctx->scal[TPSC_S_USP] = ctx->Usp;
+    ctx->scal[TPSC_S_UCH] = ctx->Uch;
+    return TPSC_OK;
+}
+// r = (Tr Sigma G0, its asymptotic part, mu, evals, ok, Tr Sigma G at mu, -, Sigma_inf)
+// of the Newton-form mu search, err its barrier flag
+int set_mu(tpsc_ctx *ctx, const double *r, int err) {
+    if (err) return fail(ctx, TPSC_ERR_CUDA, "device mu search: grid barrier timed out");
+    ctx->scal[TPSC_S_SIGMA_INF] = r[7];
+    ctx->scal[TPSC_S_TR_SG] = r[0];
+    ctx->scal[TPSC_S_TR_SG_ASYMP] = r[0] + r[1];
+    if (r[4] != 1.0) return fail(ctx, TPSC_ERR_NO_ROOT, "mu not found");
+    ctx->scal[TPSC_S_MU] = r[2];
+    ctx->scal[TPSC_S_EVALS_MU] = r[3];
+    ctx->scal[TPSC_S_TR_SG2] = r[5];
+    ctx->scal[TPSC_S_DBLOCC_SG2] = (r[5] + ctx->U * ctx->n * ctx->n / 4.0) / ctx->U;
+    return TPSC_OK;
+}
+
+// read: take chi0max back now and check it; a Newton-form solve leaves that
+// to its one readback at the end (the root search reads the device value)
+int run_chi0(tpsc_ctx *ctx, bool read = true) {
     Grid *g = ctx->cur;
     const GridDev &d = g->d;
     int rc;
@@ -701,16 +773,13 @@ int run_chi0(tpsc_ctx *ctx) {
     g->g_mixed = mixed(ctx);
     CK(launch_chi0_tau(d, g->chiq, g->dchiqt0, g->cinf, g->cinf2, ctx->T, ctx->st));
     CK(launch_chi0max(d, g->chiq, ctx->red, ctx->st));
+    g->have_chi0 = true;
+    g->have_V = g->have_S = g->have_mom = g->have_U = false;
+    if (!read) return TPSC_OK;
     double r[3];
     rc = read_result(ctx, 3, r);
     if (rc) return rc;
-    ctx->scal[TPSC_S_CHI0MAX] = r[0];
-    ctx->scal[TPSC_S_QMAX0] = r[1];
-    ctx->scal[TPSC_S_QMAX1] = r[2];
-    g->have_chi0 = true;
-    g->have_V = g->have_S = g->have_mom = g->have_U = false;
-    if (!std::isfinite(r[0]) || r[0] <= 0.0) return fail(ctx, TPSC_ERR_NONFINITE, "chi0(q, 0) has no positive maximum");
-    return TPSC_OK;
+    return set_chi0max(ctx, r);
 }
 
 // Per-frequency moments of chi0, their sums over the frequencies >= j and the
@@ -802,34 +871,36 @@ int sumrule(tpsc_ctx *ctx, int channel, double Uv, double *tr, double *dtr) {
 }
 
 // chi::find_Usp_Uch(nq0, nw0, Usc) on the current grid after chi0 (src/chi.cpp:850-876)
-int roots_Usp_Uch(tpsc_ctx *ctx, double Usc[2]) {
+// read: take the roots back now; a Newton-form solve defers that to its one
+// readback at the end, the interval's end then coming from the device chi0max
+int roots_Usp_Uch(tpsc_ctx *ctx, double Usc[2], bool read = true) {
     const double n = ctx->n, U = ctx->U, nsr = ctx->nsr;
     const bool newton = (ctx->form & TPSC_FORM_NEWTON) != 0;
     int rc = TPSC_OK;
     if (newton) {
-        // both roots in one cooperative launch (tpsc_roots.cu)
+        // both roots in one cooperative launch (tpsc_roots.cu), into ctx->dres
         Grid *g = ctx->cur;
         if ((rc = ensure_moments(ctx, g))) return rc;
-        CK(launch_sumrule_roots(g->d, g->chiq, g->cinf, g->cinf2, g->d_mom_suf, g->d_cmax_suf, g->d_tailm, ctx->T,
-                                n, nsr, U, 2.0 / ctx->scal[TPSC_S_CHI0MAX] - 2 * EPS, ctx->roots, ctx->st));
+        RootScratch rs = ctx->roots;
+        rs.out = ctx->dres;
+        if (read)
+            CK(launch_sumrule_roots(g->d, g->chiq, g->cinf, g->cinf2, g->d_mom_suf, g->d_cmax_suf, g->d_tailm,
+                                    ctx->T, n, nsr, U, 2.0 / ctx->scal[TPSC_S_CHI0MAX] - 2 * EPS, rs, ctx->st));
+        else
+            CK(launch_sumrule_roots(g->d, g->chiq, g->cinf, g->cinf2, g->d_mom_suf, g->d_cmax_suf, g->d_tailm,
+                                    ctx->T, n, nsr, U, 0.0, rs, ctx->st, ctx->red.result, 2 * EPS));
+        ctx->roots.reset_sr = true;
+        ctx->cur->have_U = true;
+        if (!read) return TPSC_OK;
         // the results and the barrier's error flag in one readback
-        CK(cudaMemcpyAsync(ctx->h_res, ctx->roots.out, 6 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaMemcpyAsync(ctx->h_res + 6, ctx->roots.bar + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaStreamSynchronize(ctx->st));
+        if ((rc = read_back(ctx, {{ctx->dres, 6 * sizeof(double), 0}, {ctx->roots.bar + 2, sizeof(unsigned), 6}})))
+            return rc;
         unsigned err;
         std::memcpy(&err, ctx->h_res + 6, sizeof(unsigned));
-        if (err) return fail(ctx, TPSC_ERR_CUDA, "device root search: grid barrier timed out");
-        double r[6];
-        for (int i = 0; i < 6; ++i) r[i] = ctx->h_res[i];
-        if (r[4] != 1.0) return fail(ctx, TPSC_ERR_NO_ROOT, "Usp not found");
-        if (r[5] != 1.0) return fail(ctx, TPSC_ERR_NO_ROOT, "Uch not found");
-        ctx->Usp = Usc[0] = r[0];
-        ctx->Uch = Usc[1] = r[1];
-        ctx->scal[TPSC_S_EVALS_SP] = r[2];
-        ctx->scal[TPSC_S_EVALS_CH] = r[3];
-        ctx->scal[TPSC_S_USP] = ctx->Usp;
-        ctx->scal[TPSC_S_UCH] = ctx->Uch;
-        ctx->cur->have_U = true;
+        ctx->roots.reset_sr = err != 0;
+        if ((rc = set_roots(ctx, ctx->h_res, err))) return rc;
+        Usc[0] = ctx->Usp;
+        Usc[1] = ctx->Uch;
         return TPSC_OK;
     }
     // R_sp(Us) = trace + n - n^2/2 - nsr + Us nsr^2/(2U)  (chi::sum_rule_sp, src/chi.cpp:833-836)
@@ -886,6 +957,8 @@ int roots_Usp_Uch(tpsc_ctx *ctx, double Usc[2]) {
     ctx->scal[TPSC_S_USP] = ctx->Usp;
     ctx->scal[TPSC_S_UCH] = ctx->Uch;
     ctx->cur->have_U = true;
+    // where the vertex and Sigma kernels read them
+    CK(launch_store(ctx->dres, Usc, 2, ctx->st));
     return TPSC_OK;
 }
 
@@ -899,12 +972,12 @@ void set_dblocc(tpsc_ctx *ctx) {
 int run_vertex(tpsc_ctx *ctx) {
     Grid *g = ctx->cur;
     if (!g || !g->have_chi0) return fail(ctx, TPSC_ERR_STATE, "chi0 has not been computed on the current grid");
-    const double fact = ctx->U * (3.0 * ctx->Usp + ctx->Uch) / 8.0;
+    // Usp, Uch from ctx->dres, where the root search left them
     if (mixed(ctx))
-        CK(launch_vertex_q32(g->d, g->chiq, g->V, ctx->U, ctx->Usp, ctx->Uch, ctx->T, ctx->st));
+        CK(launch_vertex_q32(g->d, g->chiq, g->V, ctx->U, ctx->dres, ctx->T, ctx->st));
     else
-        CK(launch_vertex_q(g->d, g->chiq, g->V, ctx->U, ctx->Usp, ctx->Uch, ctx->T, ctx->st));
-    CK(launch_vertex_tau(g->d, g->V, g->chirt, fact, ctx->st));
+        CK(launch_vertex_q(g->d, g->chiq, g->V, ctx->U, ctx->dres, ctx->T, ctx->st));
+    CK(launch_vertex_tau(g->d, g->V, g->chirt, ctx->U, ctx->dres, ctx->st));
     g->have_V = true;
     return TPSC_OK;
 }
@@ -914,27 +987,25 @@ int run_vertex(tpsc_ctx *ctx) {
 int run_self(tpsc_ctx *ctx, bool settle = true) {
     Grid *g = ctx->cur;
     if (!g || !g->have_V) return fail(ctx, TPSC_ERR_STATE, "the vertex V(r, tau) has not been computed");
-    const double fact = ctx->U * (3.0 * ctx->Usp + ctx->Uch) / 8.0;
     const GridDev &d = g->d;
     // G(r, tau) as the chi0 stage left it (FP32 in the mixed form); the two
     // boundary CTAs run beside the Sigma slices
     int rc = fork_side(ctx, 1);
     if (rc) return rc;
     if (g->g_mixed) {
-        CK(launch_sigma_boundary(d, (const float *)g->Grt32, g->V, g->dchirt0, g->dG0p, g->mu0, fact, g->dS,
-                                 ctx->st2));
+        CK(launch_sigma_boundary(d, (const float *)g->Grt32, g->V, g->dchirt0, g->dG0p, g->mu0, ctx->U, ctx->dres,
+                                 g->dS, ctx->st2));
         CK(launch_sigma_slice(d, (const float *)g->Grt32, g->V, g->sigt, ctx->st));
     } else {
-        CK(launch_sigma_boundary(d, (const double *)g->Grt, g->V, g->dchirt0, g->dG0p, g->mu0, fact, g->dS,
-                                 ctx->st2));
+        CK(launch_sigma_boundary(d, (const double *)g->Grt, g->V, g->dchirt0, g->dG0p, g->mu0, ctx->U, ctx->dres,
+                                 g->dS, ctx->st2));
         CK(launch_sigma_slice(d, (const double *)g->Grt, g->V, g->sigt, ctx->st));
     }
     if ((rc = join_side(ctx, 1))) return rc;
     CK(launch_sigma_tau(d, g->sigt, g->dS, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->T, ctx->st));
     g->have_S = true;
     if (!settle) return TPSC_OK;
-    CK(cudaMemcpyAsync(ctx->h_res, g->sinf, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+    if ((rc = read_back(ctx, {{g->sinf, sizeof(double), 0}}))) return rc;
     ctx->scal[TPSC_S_SIGMA_INF] = ctx->h_res[0];
     return TPSC_OK;
 }
@@ -982,7 +1053,7 @@ void mu_series_cut(const tpsc_ctx *ctx, int *jc_out, double *wc_out) {
 // for Tr Sigma G0 and the series moments (k_sigma_moments), then the Newton
 // search and Tr Sigma G at mu in one cooperative launch (k_mu_roots), one
 // readback for all of it.
-int self_traces_and_mu_newton(tpsc_ctx *ctx) {
+int queue_mu_newton(tpsc_ctx *ctx) {
     Grid *g = ctx->cur;
     const GridDev &d = g->d;
     int jc;
@@ -991,24 +1062,77 @@ int self_traces_and_mu_newton(tpsc_ctx *ctx) {
     CK(launch_sigma_moments(d, g->S, g->s2, g->s3, g->s4, g->sinf, g->mu0, ctx->T, jc, ctx->redm, ctx->st));
     CK(launch_mu_roots(d, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->redm.result, g->mu0, ctx->T, jc, wc, ctx->roots,
                        ctx->st));
-    CK(cudaMemcpyAsync(ctx->h_res, ctx->redm.result, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaMemcpyAsync(ctx->h_res + 2, ctx->roots.out, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaMemcpyAsync(ctx->h_res + 6, ctx->roots.bar + 2, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaMemcpyAsync(ctx->h_res + 7, g->sinf, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+    ctx->roots.reset_mu = true;
+    return TPSC_OK;
+}
+
+int self_traces_and_mu_newton(tpsc_ctx *ctx) {
+    int rc = queue_mu_newton(ctx);
+    if (rc) return rc;
+    if ((rc = read_back(ctx, {{ctx->redm.result, 2 * sizeof(double), 0},
+                              {ctx->roots.out, 4 * sizeof(double), 2},
+                              {ctx->roots.bar + 6, sizeof(int), 6},
+                              {ctx->cur->sinf, sizeof(double), 7}})))
+        return rc;
     int err;
     std::memcpy(&err, ctx->h_res + 6, sizeof(int));
-    if (err) return fail(ctx, TPSC_ERR_CUDA, "device mu search: grid barrier timed out");
-    const double *r = ctx->h_res;
-    ctx->scal[TPSC_S_SIGMA_INF] = r[7];
-    ctx->scal[TPSC_S_TR_SG] = r[0];
-    ctx->scal[TPSC_S_TR_SG_ASYMP] = r[0] + r[1];
-    if (r[4] != 1.0) return fail(ctx, TPSC_ERR_NO_ROOT, "mu not found");
-    ctx->scal[TPSC_S_MU] = r[2];
-    ctx->scal[TPSC_S_EVALS_MU] = r[3];
-    ctx->scal[TPSC_S_TR_SG2] = r[5];
-    ctx->scal[TPSC_S_DBLOCC_SG2] = (r[5] + ctx->U * ctx->n * ctx->n / 4.0) / ctx->U;
+    ctx->roots.reset_mu = err != 0;
+    return set_mu(ctx, ctx->h_res, err);
+}
+
+// stage times from ctx->ev[0..5] and the finiteness check of the scalars
+int finish_solve(tpsc_ctx *ctx) {
+    CK(cudaEventSynchronize(ctx->ev[5]));
+    for (int i = 0; i < 5; ++i) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ctx->ev[i], ctx->ev[i + 1]));
+        ctx->stage_ms[i] = ms;
+    }
+    for (int i = 0; i < TPSC_S_COUNT; ++i)
+        if (!std::isfinite(ctx->scal[i])) return fail(ctx, TPSC_ERR_NONFINITE, "non-finite scalar result");
     return TPSC_OK;
+}
+
+// The Newton-form solve after the chi0 stage, queued without a host round
+// trip (the roots, the vertex and Sigma read their inputs on the device), and
+// its one readback: chi0max, the sum-rule roots, the mu search and their
+// barrier flags, checked in stage order.
+int newton_rest(tpsc_ctx *ctx) {
+    double Usc[2];
+    int rc;
+    if ((rc = roots_Usp_Uch(ctx, Usc, false))) return rc;
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    if ((rc = run_vertex(ctx))) return rc;
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    if ((rc = run_self(ctx, false))) return rc;
+    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    if ((rc = queue_mu_newton(ctx))) return rc;
+    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    // h_res: [0..2] chi0max, qmax; [3..8] the sum-rule roots; [9] their flag;
+    // [10..11] the Sigma traces; [12..15] the mu search; [16] its flag; [17] Sigma_inf
+    if ((rc = read_back(ctx, {{ctx->red.result, 3 * sizeof(double), 0},
+                              {ctx->dres, 6 * sizeof(double), 3},
+                              {ctx->roots.bar + 2, sizeof(unsigned), 9},
+                              {ctx->redm.result, 2 * sizeof(double), 10},
+                              {ctx->roots.out, 4 * sizeof(double), 12},
+                              {ctx->roots.bar + 6, sizeof(int), 16},
+                              {ctx->cur->sinf, sizeof(double), 17}})))
+        return rc;
+    const double *h = ctx->h_res;
+    if ((rc = set_chi0max(ctx, h))) return rc;
+    unsigned err_sr;
+    std::memcpy(&err_sr, h + 9, sizeof(unsigned));
+    int err_mu;
+    std::memcpy(&err_mu, h + 16, sizeof(int));
+    ctx->roots.reset_sr = err_sr != 0;
+    ctx->roots.reset_mu = err_mu != 0;
+    if ((rc = set_roots(ctx, h + 3, err_sr))) return rc;
+    set_dblocc(ctx);
+    double r[8];
+    for (int i = 0; i < 6; ++i) r[i] = h[10 + i];
+    r[6] = 0.0;
+    r[7] = h[17];
+    return set_mu(ctx, r, err_mu);
 }
 
 int find_mu(tpsc_ctx *ctx) {
@@ -1214,9 +1338,14 @@ tpsc_ctx *tpsc_create(int device, int *status) {
         return bad(e);
     if ((e = cudaMalloc(&ctx->redm.result, 32 * sizeof(double))) != cudaSuccess) return bad(e);
     if ((e = cudaMalloc(&ctx->roots.partial, 4 * kRootMaxBlocks * sizeof(double))) != cudaSuccess) return bad(e);
-    if ((e = cudaMalloc(&ctx->roots.bar, 4 * sizeof(unsigned))) != cudaSuccess) return bad(e);
+    if ((e = cudaMalloc(&ctx->roots.bar, 8 * sizeof(unsigned))) != cudaSuccess) return bad(e);
+    if ((e = cudaMemsetAsync(ctx->roots.bar, 0, 8 * sizeof(unsigned), ctx->st)) != cudaSuccess) return bad(e);
+    ctx->roots.reset_sr = ctx->roots.reset_mu = false;
+    if ((e = cudaMalloc(&ctx->dres, 16 * sizeof(double))) != cudaSuccess) return bad(e);
+    if ((e = cudaMemsetAsync(ctx->dres, 0, 16 * sizeof(double), ctx->st)) != cudaSuccess) return bad(e);
     if ((e = cudaMalloc(&ctx->roots.out, 8 * sizeof(double))) != cudaSuccess) return bad(e);
-    if ((e = cudaMallocHost(&ctx->h_res, 32 * sizeof(double))) != cudaSuccess) return bad(e);
+    if ((e = cudaHostAlloc(&ctx->h_res, 32 * sizeof(double), cudaHostAllocMapped)) != cudaSuccess) return bad(e);
+    if ((e = cudaHostGetDevicePointer(&ctx->h_res_dev, ctx->h_res, 0)) != cudaSuccess) return bad(e);
     for (auto &ev : ctx->ev)
         if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bad(e);
     if (status) *status = TPSC_OK;
@@ -1236,8 +1365,16 @@ void tpsc_destroy(tpsc_ctx *ctx) {
     if (ctx->roots.partial) cudaFree(ctx->roots.partial);
     if (ctx->roots.bar) cudaFree(ctx->roots.bar);
     if (ctx->roots.out) cudaFree(ctx->roots.out);
+    if (ctx->dres) cudaFree(ctx->dres);
     if (ctx->h_res) cudaFreeHost(ctx->h_res);
     if (ctx->stage) cudaFree(ctx->stage);
+    if (ctx->cst) cudaStreamSynchronize(ctx->cst);
+    for (int k = 0; k < 2; ++k) {
+        if (ctx->snap[k]) cudaFree(ctx->snap[k]);
+        if (ctx->snap_ev[k]) cudaEventDestroy(ctx->snap_ev[k]);
+        if (ctx->copy_ev[k]) cudaEventDestroy(ctx->copy_ev[k]);
+    }
+    if (ctx->cst) cudaStreamDestroy(ctx->cst);
     for (auto &ev : ctx->ev)
         if (ev) cudaEventDestroy(ev);
     for (auto &ev : ctx->evf)
@@ -1652,9 +1789,14 @@ int tpsc_solve(tpsc_ctx *ctx) {
     CK(cudaEventRecord(ctx->ev[0], ctx->st));
     rc = switch_grid(ctx, ctx->nk0, ctx->Nw0);
     if (rc) return rc;
-    rc = run_chi0(ctx);
+    const bool newton = (ctx->form & TPSC_FORM_NEWTON) != 0;
+    rc = run_chi0(ctx, !newton);
     if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    if (newton) {
+        if ((rc = newton_rest(ctx))) return rc;
+        return finish_solve(ctx);
+    }
     double Usc[2];
     rc = roots_Usp_Uch(ctx, Usc);
     if (rc) return rc;
@@ -1675,15 +1817,7 @@ int tpsc_solve(tpsc_ctx *ctx) {
     rc = find_mu(ctx);
     if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[5], ctx->st));
-    CK(cudaEventSynchronize(ctx->ev[5]));
-    for (int i = 0; i < 5; ++i) {
-        float ms = 0;
-        CK(cudaEventElapsedTime(&ms, ctx->ev[i], ctx->ev[i + 1]));
-        ctx->stage_ms[i] = ms;
-    }
-    for (int i = 0; i < TPSC_S_COUNT; ++i)
-        if (!std::isfinite(ctx->scal[i])) return fail(ctx, TPSC_ERR_NONFINITE, "non-finite scalar result");
-    return TPSC_OK;
+    return finish_solve(ctx);
 }
 
 int tpsc_get_scalars(tpsc_ctx *ctx, double *out, int n) {
@@ -1759,6 +1893,74 @@ int tpsc_get_self(tpsc_ctx *ctx, double *self_kw, double *s2, double *s3, double
     if (s3 && (rc = copy_out(ctx, s3, g->s3, d.n8 * sizeof(double)))) return rc;
     if (s4 && (rc = copy_out(ctx, s4, g->s4, d.n8 * sizeof(double)))) return rc;
     CK(cudaStreamSynchronize(ctx->st));
+    return TPSC_OK;
+}
+
+int tpsc_get_self_async(tpsc_ctx *ctx, double *self_kw, double *s2, double *s3, double *s4) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    Grid *g = ctx->cur;
+    if (!g->have_S) return fail(ctx, TPSC_ERR_STATE, "the self-energy has not been computed");
+    if (!self_kw) return fail(ctx, TPSC_ERR_ARG, "null self_kw");
+    cudaSetDevice(ctx->device);
+    const GridDev &d = g->d;
+    if (!ctx->cst) {
+        CK(cudaStreamCreateWithFlags(&ctx->cst, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k) {
+            CK(cudaEventCreateWithFlags(&ctx->snap_ev[k], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ctx->copy_ev[k], cudaEventDisableTiming));
+        }
+    }
+    const int k = ctx->snap_next;
+    const size_t sbytes = (size_t)(d.nw0 / 2) * d.n8 * sizeof(double2), vbytes = (size_t)d.n8 * sizeof(double);
+    const size_t need = sbytes + 3 * vbytes;
+    // snapshot buffer k is free once its previous copy has finished
+    CK(cudaStreamWaitEvent(ctx->st, ctx->copy_ev[k], 0));
+    if (ctx->snap_bytes[k] < need) {
+        CK(cudaStreamSynchronize(ctx->st));
+        if (ctx->snap[k]) cudaFree(ctx->snap[k]);
+        ctx->snap[k] = nullptr;
+        ctx->snap_bytes[k] = 0;
+        CK(cudaMalloc(&ctx->snap[k], need));
+        ctx->snap_bytes[k] = need;
+    }
+    char *base = static_cast<char *>(ctx->snap[k]);
+    double *vs = reinterpret_cast<double *>(base + sbytes);
+    CK(launch_unblock_c(g->S, reinterpret_cast<double2 *>(base), d.nw0 / 2, d.nw0 / 2, d.n8, ctx->st));
+    // the three vectors by the SMs too: a device-to-device copy may take a
+    // copy engine, where it could wait behind the previous step's copy-out
+    GatherPieces gp;
+    const double *vsrc[3] = {g->s2, g->s3, g->s4};
+    for (int i = 0; i < 3; ++i) {
+        gp.src[i] = reinterpret_cast<const unsigned *>(vsrc[i]);
+        gp.words[i] = 2LL * d.n8;
+        gp.dst[i] = 2LL * i * d.n8;
+    }
+    gp.n = 3;
+    CK(launch_gather(gp, reinterpret_cast<unsigned *>(vs), 32, ctx->st));
+    CK(cudaEventRecord(ctx->snap_ev[k], ctx->st));
+    CK(cudaStreamWaitEvent(ctx->cst, ctx->snap_ev[k], 0));
+    CK(cudaMemcpyAsync(self_kw, base, sbytes, cudaMemcpyDeviceToHost, ctx->cst));
+    if (s2) CK(cudaMemcpyAsync(s2, vs, vbytes, cudaMemcpyDeviceToHost, ctx->cst));
+    if (s3) CK(cudaMemcpyAsync(s3, vs + d.n8, vbytes, cudaMemcpyDeviceToHost, ctx->cst));
+    if (s4) CK(cudaMemcpyAsync(s4, vs + 2 * d.n8, vbytes, cudaMemcpyDeviceToHost, ctx->cst));
+    CK(cudaEventRecord(ctx->copy_ev[k], ctx->cst));
+    ctx->snap_next = k ^ 1;
+    ctx->copies_pending = true;
+    return TPSC_OK;
+}
+
+int tpsc_wait_copies(tpsc_ctx *ctx, int join_stream) {
+    if (!ctx) return fail(nullptr, TPSC_ERR_ARG, "null context");
+    if (!ctx->copies_pending) return TPSC_OK;
+    cudaSetDevice(ctx->device);
+    if (join_stream) {
+        // the last copy recorded copy_ev[snap_next ^ 1]; the stream waits for it
+        CK(cudaStreamWaitEvent(ctx->st, ctx->copy_ev[ctx->snap_next ^ 1], 0));
+        return TPSC_OK;
+    }
+    CK(cudaStreamSynchronize(ctx->cst));
+    ctx->copies_pending = false;
     return TPSC_OK;
 }
 
@@ -1913,6 +2115,12 @@ int tpsc_launch_count(tpsc_ctx *ctx, long long *count) {
 int tpsc_set_form(tpsc_ctx *ctx, int form) {
     if (!ctx) return fail(nullptr, TPSC_ERR_ARG, "null context");
     if (form < 0 || form > (TPSC_FORM_NEWTON | TPSC_FORM_MIXED)) return fail(ctx, TPSC_ERR_ARG, "unknown form");
+    // mu0 comes from the root search of the form (host find_zero or the
+    // device Newton kernel; they agree to an ulp or so): when that changes,
+    // the next grid switch (every solve and chi0 stage) derives it again, so
+    // a result does not depend on whether the form was set before the model
+    if ((ctx->form ^ form) & TPSC_FORM_NEWTON)
+        for (auto &kv : ctx->grids) kv.second->model_id = -1;
     ctx->form = form;
     return TPSC_OK;
 }
@@ -1929,7 +2137,6 @@ int tpsc_run_kernel(tpsc_ctx *ctx, int which) {
     Grid *g = ctx->cur;
     if (!g->have_S) return fail(ctx, TPSC_ERR_STATE, "run tpsc_solve first");
     const GridDev &d = g->d;
-    const double fact = ctx->U * (3.0 * ctx->Usp + ctx->Uch) / 8.0;
     switch (which) {
         case 0:
             if (g->g_mixed)
@@ -1946,11 +2153,11 @@ int tpsc_run_kernel(tpsc_ctx *ctx, int which) {
         case 2: CK(launch_chi0_tau(d, g->chiq, g->dchiqt0, g->cinf, g->cinf2, ctx->T, ctx->st)); break;
         case 3:
             if (g->g_mixed)
-                CK(launch_vertex_q32(d, g->chiq, g->V, ctx->U, ctx->Usp, ctx->Uch, ctx->T, ctx->st));
+                CK(launch_vertex_q32(d, g->chiq, g->V, ctx->U, ctx->dres, ctx->T, ctx->st));
             else
-                CK(launch_vertex_q(d, g->chiq, g->V, ctx->U, ctx->Usp, ctx->Uch, ctx->T, ctx->st));
+                CK(launch_vertex_q(d, g->chiq, g->V, ctx->U, ctx->dres, ctx->T, ctx->st));
             break;
-        case 4: CK(launch_vertex_tau(d, g->V, g->chirt, fact, ctx->st)); break;
+        case 4: CK(launch_vertex_tau(d, g->V, g->chirt, ctx->U, ctx->dres, ctx->st)); break;
         case 5:
             if (g->g_mixed)
                 CK(launch_sigma_slice(d, (const float *)g->Grt32, g->V, g->sigt, ctx->st));
@@ -2004,6 +2211,7 @@ int tpsc_run_kernel(tpsc_ctx *ctx, int which) {
             CK(launch_sumrule_roots(d, g->chiq, g->cinf, g->cinf2, g->d_mom_suf, g->d_cmax_suf, g->d_tailm, ctx->T,
                                     ctx->n, ctx->nsr, ctx->U, 2.0 / ctx->scal[TPSC_S_CHI0MAX] - 2 * EPS, ctx->roots,
                                     ctx->st));
+            ctx->roots.reset_sr = true;
             break;
         case 14:
         case 15: {
@@ -2013,9 +2221,11 @@ int tpsc_run_kernel(tpsc_ctx *ctx, int which) {
             double wc;
             mu_series_cut(ctx, &jc, &wc);
             CK(launch_sigma_moments(d, g->S, g->s2, g->s3, g->s4, g->sinf, g->mu0, ctx->T, jc, ctx->redm, ctx->st));
-            if (which == 15)
+            if (which == 15) {
                 CK(launch_mu_roots(d, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->redm.result, g->mu0, ctx->T, jc, wc,
                                    ctx->roots, ctx->st));
+                ctx->roots.reset_mu = true;
+            }
             break;
         }
         default: return fail(ctx, TPSC_ERR_ARG, "unknown stage");

@@ -202,10 +202,11 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
 template <int NBK>
 __global__ void __launch_bounds__(kSliceThreads, 1)
     k_vertex_q(const double *__restrict__ chiq, const double2 *__restrict__ tw,
-               int n8, int nb, double normFact, double U, double Usp, double Uch, double *__restrict__ Vr) {
+               int n8, int nb, double normFact, double U, const double *__restrict__ Usc, double *__restrict__ Vr) {
     extern __shared__ __align__(16) double S[];
     const auto *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
+    const double Usp = Usc[0], Uch = Usc[1];
     fill_octant<NBK>(S, n8, [&](int o) -> double {
         const double c0 = chiq[bidx(j, o, nb)];
         const double sp = c0 / (1.0 - Usp * c0 / 2.0);
@@ -228,10 +229,11 @@ template <int NBK, class GT>
 __global__ void __launch_bounds__(kSliceThreads, 1)
     k_sigma_boundary(const double *__restrict__ er, const double2 *__restrict__ tw,
                      const GT *__restrict__ Grt, const double *__restrict__ V, const double *__restrict__ dtau_chirt0,
-                     const double *__restrict__ dG0p, int n8, int nw0, int n8p, double mu0, double fact,
-                     double *__restrict__ dS) {
+                     const double *__restrict__ dG0p, int n8, int nw0, int n8p, double mu0, double U,
+                     const double *__restrict__ Usc, double *__restrict__ dS) {
     extern __shared__ __align__(16) double S[];
     const auto *tws = slice_twiddles<NBK>(S, tw);
+    const double fact = vertex_fact(U, Usc);
     const int nb = nw0 / 2 + 1;
     {
         const int side = blockIdx.x;
@@ -383,8 +385,9 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
 template <int N>
 __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
     k_vertex_tau(double *__restrict__ Vr, const double *__restrict__ chirt, const double2 *__restrict__ tw,
-                 double fact, int n8) {
+                 double U, const double *__restrict__ Usc, int n8) {
     constexpr int NJ = N / 2 + 1;
+    const double fact = vertex_fact(U, Usc);
     extern __shared__ __align__(16) double A[];
     double2 *X = reinterpret_cast<double2 *>(A + ((4 * NJ + 1) & ~1));
     TwoLevelTw *tw2 = reinterpret_cast<TwoLevelTw *>(reinterpret_cast<char *>(A) + TauSmem<N>::tables_off(NJ));
@@ -677,8 +680,9 @@ __global__ void __launch_bounds__(256, 2)
 template <int N>
 __global__ void __launch_bounds__(256, 2)
     k_vertex_tau2(double *__restrict__ Vr, const double *__restrict__ chirt, const double2 *__restrict__ tw,
-                  double fact, int n8) {
+                  double U, const double *__restrict__ Usc, int n8) {
     constexpr int NJ = N / 2 + 1;
+    const double fact = vertex_fact(U, Usc);
     static_assert(2 * NJ * sizeof(double) <= Tau2Smem<N>::buf, "pair must fit the FFT buffer");
     extern __shared__ __align__(16) double A[];
     double2 *X = reinterpret_cast<double2 *>(A);
@@ -1496,6 +1500,21 @@ __global__ void k_unblock_c(const double2 *__restrict__ src, double2 *__restrict
     }
 }
 
+__global__ void k_gather(GatherPieces p, unsigned *__restrict__ dst) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (int k = 0; k < p.n; ++k)
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < p.words[k]; i += stride)
+            dst[p.dst[k] + i] = p.src[k][i];
+}
+
+struct StoreVals {
+    double v[4];
+    int n;
+};
+__global__ void k_store(StoreVals s, double *__restrict__ dst) {
+    if ((int)threadIdx.x < s.n) dst[threadIdx.x] = s.v[threadIdx.x];
+}
+
 // ---------------------------------------------------------------------------
 // launch wrappers per compiled size
 // ---------------------------------------------------------------------------
@@ -1538,14 +1557,13 @@ struct RunChi0Slice {
 };
 template <int NBK>
 struct RunVertexQ {
-    static cudaError_t run(const GridDev *g, const double *chiq, double *Vr, double U, double Usp, double Uch, double T,
+    static cudaError_t run(const GridDev *g, const double *chiq, double *Vr, double U, const double *Usc, double T,
                            cudaStream_t st) {
         const size_t sm = SliceSmem<NBK>::bytes;
         cudaError_t e = set_smem(k_vertex_q<NBK>, sm);
         if (e != cudaSuccess) return e;
         const double normFact = T / ((double)g->nk0 * g->nk0);
-        k_vertex_q<NBK><<<g->nb, kSliceThreads, sm, st>>>(chiq, g->tw_k, g->n8, g->nb, normFact, U, Usp, Uch,
-                                                          Vr);
+        k_vertex_q<NBK><<<g->nb, kSliceThreads, sm, st>>>(chiq, g->tw_k, g->n8, g->nb, normFact, U, Usc, Vr);
         return launched();
     }
 };
@@ -1553,12 +1571,13 @@ template <int NBK>
 struct RunSigmaBoundary {
     template <class GT>
     static cudaError_t run(const GridDev *g, const GT *Grt, const double *V, const double *dchirt0,
-                           const double *dG0p, double mu0, double fact, double *dS, cudaStream_t st) {
+                           const double *dG0p, double mu0, double U, const double *Usc, double *dS,
+                           cudaStream_t st) {
         const size_t sm = SliceSmem<NBK>::bytes;
         cudaError_t e = set_smem(k_sigma_boundary<NBK, GT>, sm);
         if (e != cudaSuccess) return e;
         k_sigma_boundary<NBK, GT><<<2, kSliceThreads, sm, st>>>(g->er, g->tw_k, Grt, V, dchirt0, dG0p, g->n8,
-                                                                 g->nw0, g->n8p, mu0, fact, dS);
+                                                                 g->nw0, g->n8p, mu0, U, Usc, dS);
         return launched();
     }
 };
@@ -1596,18 +1615,19 @@ struct RunChi0Tau {
 };
 template <int N>
 struct RunVertexTau {
-    static cudaError_t run(const GridDev *g, double *Vr, const double *chirt, double fact, cudaStream_t st) {
+    static cudaError_t run(const GridDev *g, double *Vr, const double *chirt, double U, const double *Usc,
+                           cudaStream_t st) {
         cudaError_t e;
         if constexpr (N / 16 <= 256) {
             const size_t sm = Tau2Smem<N>::bytes;
             if ((e = set_smem(k_vertex_tau2<N>, sm)) != cudaSuccess) return e;
-            k_vertex_tau2<N><<<g->n8p / 2, 256, sm, st>>>(Vr, chirt, g->tw_w, fact, g->n8);
+            k_vertex_tau2<N><<<g->n8p / 2, 256, sm, st>>>(Vr, chirt, g->tw_w, U, Usc, g->n8);
             return launched();
         }
         const size_t sm = TauSmem<N>::bytes(N / 2 + 1);
         e = set_smem(k_vertex_tau<N>, sm);
         if (e != cudaSuccess) return e;
-        k_vertex_tau<N><<<g->n8p / 4, TauSmem<N>::threads, sm, st>>>(Vr, chirt, g->tw_w, fact, g->n8);
+        k_vertex_tau<N><<<g->n8p / 4, TauSmem<N>::threads, sm, st>>>(Vr, chirt, g->tw_w, U, Usc, g->n8);
         return launched();
     }
 };
@@ -1837,22 +1857,25 @@ cudaError_t launch_trace_chi0(const GridDev &g, const double *chiq, const double
     return launched();
 }
 
-cudaError_t launch_vertex_q(const GridDev &g, const double *chiq, double *Vr, double U, double Usp, double Uch,
-                            double T, cudaStream_t st) {
-    return dispatch_nbk<RunVertexQ>(g.nbk, &g, chiq, Vr, U, Usp, Uch, T, st);
+cudaError_t launch_vertex_q(const GridDev &g, const double *chiq, double *Vr, double U, const double *Usc, double T,
+                            cudaStream_t st) {
+    return dispatch_nbk<RunVertexQ>(g.nbk, &g, chiq, Vr, U, Usc, T, st);
 }
 
-cudaError_t launch_vertex_tau(const GridDev &g, double *Vr, const double *chirt, double fact, cudaStream_t st) {
-    return dispatch_nw<RunVertexTau>(g.nw0, &g, Vr, chirt, fact, st);
+cudaError_t launch_vertex_tau(const GridDev &g, double *Vr, const double *chirt, double U, const double *Usc,
+                              cudaStream_t st) {
+    return dispatch_nw<RunVertexTau>(g.nw0, &g, Vr, chirt, U, Usc, st);
 }
 
 cudaError_t launch_sigma_boundary(const GridDev &g, const double *Grt, const double *V, const double *dtau_chirt0,
-                                  const double *dG0p, double mu0, double fact, double *dS, cudaStream_t st) {
-    return dispatch_nbk<RunSigmaBoundary>(g.nbk, &g, Grt, V, dtau_chirt0, dG0p, mu0, fact, dS, st);
+                                  const double *dG0p, double mu0, double U, const double *Usc, double *dS,
+                                  cudaStream_t st) {
+    return dispatch_nbk<RunSigmaBoundary>(g.nbk, &g, Grt, V, dtau_chirt0, dG0p, mu0, U, Usc, dS, st);
 }
 cudaError_t launch_sigma_boundary(const GridDev &g, const float *Grt, const double *V, const double *dtau_chirt0,
-                                  const double *dG0p, double mu0, double fact, double *dS, cudaStream_t st) {
-    return dispatch_nbk<RunSigmaBoundary>(g.nbk, &g, Grt, V, dtau_chirt0, dG0p, mu0, fact, dS, st);
+                                  const double *dG0p, double mu0, double U, const double *Usc, double *dS,
+                                  cudaStream_t st) {
+    return dispatch_nbk<RunSigmaBoundary>(g.nbk, &g, Grt, V, dtau_chirt0, dG0p, mu0, U, Usc, dS, st);
 }
 
 cudaError_t launch_sigma_slice(const GridDev &g, const double *Grt, const double *V, double *sigt, cudaStream_t st) {
@@ -1934,6 +1957,20 @@ cudaError_t launch_unblock(const double *src, double *dst, int NJ, int nrows, in
 cudaError_t launch_unblock_c(const double2 *src, double2 *dst, int NJ, int nrows, int n8, cudaStream_t st) {
     const int nb = grid_for((long long)nrows * n8, 256);
     k_unblock_c<<<nb, 256, 0, st>>>(src, dst, NJ, nrows, n8);
+    return launched();
+}
+
+cudaError_t launch_gather(const GatherPieces &p, unsigned *dst, int blocks, cudaStream_t st) {
+    k_gather<<<blocks, 256, 0, st>>>(p, dst);
+    return launched();
+}
+
+cudaError_t launch_store(double *dst, const double *v, int n, cudaStream_t st) {
+    if (n < 0 || n > 4) return cudaErrorInvalidValue;
+    StoreVals s;
+    for (int i = 0; i < 4; ++i) s.v[i] = i < n ? v[i] : 0.0;
+    s.n = n;
+    k_store<<<1, 32, 0, st>>>(s, dst);
     return launched();
 }
 

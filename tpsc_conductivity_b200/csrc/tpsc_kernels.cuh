@@ -57,8 +57,9 @@ cudaError_t launch_chi0_boundary(const GridDev &g, const float *Grt, double mu0,
 // the mixed-precision form's FP32 slice transforms (tpsc_mixed.cu)
 cudaError_t launch_gslice32(const GridDev &g, float *Grt, double mu0, double T, cudaStream_t st);
 cudaError_t launch_chi0_slice32(const GridDev &g, const float *Grt, double *chirt, double *chiq, cudaStream_t st);
-cudaError_t launch_vertex_q32(const GridDev &g, const double *chiq, double *Vr, double U, double Usp, double Uch,
-                              double T, cudaStream_t st);
+// Usc: the device pair (Usp, Uch) -- the sum-rule root search leaves it there
+cudaError_t launch_vertex_q32(const GridDev &g, const double *chiq, double *Vr, double U, const double *Usc, double T,
+                              cudaStream_t st);
 cudaError_t launch_chi0_slice(const GridDev &g, const double *Grt, double *chirt, double *chiq, cudaStream_t st);
 cudaError_t launch_chi0_tau(const GridDev &g, double *chiq, const double *dtau_chiqt0, double *chi0_inf,
                             double *chi0_inf2, double T, cudaStream_t st);
@@ -113,14 +114,18 @@ cudaError_t launch_moment_suffix(const GridDev &g, const double *mom, const doub
 cudaError_t launch_trace_chi0(const GridDev &g, const double *chiq, const double *chi0_inf,
                               const double *chi0_inf2, double T, Reduce r, cudaStream_t st);
 
-cudaError_t launch_vertex_q(const GridDev &g, const double *chiq, double *Vr, double U, double Usp, double Uch,
-                            double T, cudaStream_t st);
-cudaError_t launch_vertex_tau(const GridDev &g, double *Vr, const double *chirt, double fact, cudaStream_t st);
+// Usc: the device pair (Usp, Uch); fact = U (3 Usp + Uch) / 8 is formed in the kernels
+cudaError_t launch_vertex_q(const GridDev &g, const double *chiq, double *Vr, double U, const double *Usc, double T,
+                            cudaStream_t st);
+cudaError_t launch_vertex_tau(const GridDev &g, double *Vr, const double *chirt, double U, const double *Usc,
+                              cudaStream_t st);
 
 cudaError_t launch_sigma_boundary(const GridDev &g, const double *Grt, const double *V, const double *dtau_chirt0,
-                                  const double *dG0p, double mu0, double fact, double *dS, cudaStream_t st);
+                                  const double *dG0p, double mu0, double U, const double *Usc, double *dS,
+                                  cudaStream_t st);
 cudaError_t launch_sigma_boundary(const GridDev &g, const float *Grt, const double *V, const double *dtau_chirt0,
-                                  const double *dG0p, double mu0, double fact, double *dS, cudaStream_t st);
+                                  const double *dG0p, double mu0, double U, const double *Usc, double *dS,
+                                  cudaStream_t st);
 cudaError_t launch_sigma_slice(const GridDev &g, const double *Grt, const double *V, double *sigt, cudaStream_t st);
 cudaError_t launch_sigma_slice(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st);
 cudaError_t launch_sigma_tau(const GridDev &g, const double *sigt, const double *dS, double2 *S, double *s2,
@@ -140,9 +145,14 @@ cudaError_t launch_trace_self_G2(const GridDev &g, const double2 *S, const doubl
 constexpr int kRootMaxBlocks = 1024;
 struct RootScratch {
     double *partial = nullptr;  // [4 kRootMaxBlocks]
-    unsigned *bar = nullptr;    // [4]: barrier arrivals, generation, error flag
+    unsigned *bar = nullptr;    // [8]: arrivals, generation, error flag of the sum-rule search (0..2)
+                                //      and of the mu search (4..6)
     double *out = nullptr;      // [8] results
     int max_blocks = 0;         // cap on the cooperative grid (0: two blocks per SM)
+    // Zero the search's barrier words before its launch.  The barrier leaves
+    // them zero after every launch that did not time out, so the host clears
+    // these once it has read a zero error flag after the last launch.
+    bool reset_sr = true, reset_mu = true;
 };
 // The Newton form's Sigma pass: Tr Sigma G0 (green::traceSelfG) and the
 // find_mu series moments around mu0 over the frequencies n >= jc and the tail
@@ -162,10 +172,13 @@ cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2
                             const double *sinf, const double *mom, double mu0, double T, int jc, double wc,
                             RootScratch rs, cudaStream_t st);
 // Usp then Uch by safeguarded Newton with the moment series, one cooperative
-// launch -> rs.out = {Usp, Uch, evals_sp, evals_ch, ok_sp, ok_ch}
+// launch -> rs.out = {Usp, Uch, evals_sp, evals_ch, ok_sp, ok_ch}.  With
+// chi0max (device), the spin interval ends at 2 / chi0max[0] - hi_off and
+// hi_sp is not used.
 cudaError_t launch_sumrule_roots(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
                                  const double *mom_suf, const double *cmax_suf, const double *tailm, double T,
-                                 double n, double nsr, double U, double hi_sp, RootScratch rs, cudaStream_t st);
+                                 double n, double nsr, double U, double hi_sp, RootScratch rs, cudaStream_t st,
+                                 const double *chi0max = nullptr, double hi_off = 0.0);
 
 // ---- real-frequency continuation (Pade / Lagrange) and local G ---------------
 cudaError_t launch_pade_sigma(const GridDev &g, const double2 *S, const double *s2, const double *s3,
@@ -218,6 +231,22 @@ cudaError_t launch_pade_batch(const double2 *x, const double2 *y, int nf, int Nn
 // blocked (NJ rows) -> reference layout [j][o], j < nrows
 cudaError_t launch_unblock(const double *src, double *dst, int NJ, int nrows, int n8, cudaStream_t st);
 cudaError_t launch_unblock_c(const double2 *src, double2 *dst, int NJ, int nrows, int n8, cudaStream_t st);
+
+// ---- gathers done by the SMs instead of a copy engine -----------------------
+// Up to kGatherPieces ranges of 4-byte words, each copied to a word offset of
+// dst.  With dst in mapped pinned host memory this is the solve's scalar
+// readback: no copy engine is involved, so it is not queued behind a large
+// device-to-host copy running on another stream (tpsc_get_self_async).
+constexpr int kGatherPieces = 8;
+struct GatherPieces {
+    const unsigned *src[kGatherPieces] = {};
+    long long words[kGatherPieces] = {};
+    long long dst[kGatherPieces] = {};
+    int n = 0;
+};
+cudaError_t launch_gather(const GatherPieces &p, unsigned *dst, int blocks, cudaStream_t st);
+// up to four host values stored to dst[0..n) in stream order (no copy engine)
+cudaError_t launch_store(double *dst, const double *v, int n, cudaStream_t st);
 
 // kernels launched by the library so far
 long long launches_total();

@@ -120,11 +120,12 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
 template <int NBK>
 __global__ void __launch_bounds__(kSlice32Threads, 2)
     k_vertex_q32(const double *__restrict__ chiq, const float4 *__restrict__ tw,
-                 int n8, int nb, int ahead, double normFact, double U, double Usp, double Uch,
+                 int n8, int nb, int ahead, double normFact, double U, const double *__restrict__ Usc,
                  double *__restrict__ Vr) {
     extern __shared__ __align__(16) float S32[];
     const float4 *tws = twiddles32<NBK>(S32, tw);
     const int j = blockIdx.x;
+    const double Usp = Usc[0], Uch = Usc[1];
     if (ahead > 0 && j + ahead < nb) prefetch_l2_blockrow(chiq, j + ahead, nb, (n8 + 3) / 4);
     fill_octant<NBK>(S32, n8, [&](int o) -> float {
         const double c0 = chiq[bidx(j, o, nb)];
@@ -166,15 +167,15 @@ struct RunChi0Slice32 {
 };
 template <int NBK>
 struct RunVertexQ32 {
-    static cudaError_t run(const GridDev *g, const double *chiq, double *Vr, double U, double Usp, double Uch,
-                           double T, cudaStream_t st) {
+    static cudaError_t run(const GridDev *g, const double *chiq, double *Vr, double U, const double *Usc, double T,
+                           cudaStream_t st) {
         const size_t sm = Slice32Smem<NBK>::bytes;
         cudaError_t e = set_smem(k_vertex_q32<NBK>, sm);
         if (e != cudaSuccess) return e;
         const double normFact = T / ((double)g->nk0 * g->nk0);
         const int ahead = resident_ctas(k_vertex_q32<NBK>, kSlice32Threads, sm);
         k_vertex_q32<NBK><<<g->nb, kSlice32Threads, sm, st>>>(chiq, g->tw_k32, g->n8, g->nb, ahead, normFact, U,
-                                                              Usp, Uch, Vr);
+                                                              Usc, Vr);
         return launched();
     }
 };
@@ -189,9 +190,9 @@ cudaError_t launch_chi0_slice32(const GridDev &g, const float *Grt, double *chir
     return dispatch_nbk<RunChi0Slice32>(g.nbk, &g, Grt, chirt, chiq, st);
 }
 
-cudaError_t launch_vertex_q32(const GridDev &g, const double *chiq, double *Vr, double U, double Usp, double Uch,
-                              double T, cudaStream_t st) {
-    return dispatch_nbk<RunVertexQ32>(g.nbk, &g, chiq, Vr, U, Usp, Uch, T, st);
+cudaError_t launch_vertex_q32(const GridDev &g, const double *chiq, double *Vr, double U, const double *Usc, double T,
+                              cudaStream_t st) {
+    return dispatch_nbk<RunVertexQ32>(g.nbk, &g, chiq, Vr, U, Usc, T, st);
 }
 
 }  // namespace tpsc

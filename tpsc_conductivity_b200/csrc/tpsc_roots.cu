@@ -69,6 +69,8 @@ struct SumRootArgs {
     const double *tailm;     // [kMomP] tail moments, [kMomP] = max |chi| over the tail
     int nb, nblk, n8;
     double T, scale, n, nsr, U, hi_sp;
+    const double *chi0max;  // device max chi0(q, 0), or null: hi_sp as given
+    double hi_off;          // hi_sp = 2 / chi0max - hi_off
     double *partial;  // [2][2 kRootMaxBlocks]: two buffers of (value, derivative) per block
     unsigned *bar;    // [2], zero at launch
     int *err;         // zero at launch
@@ -154,6 +156,9 @@ constexpr double kSpinSMax = 40.0;  // -hi expm1(-40) = hi (1 - 4e-18)
 __device__ __forceinline__ double spin_us(double s, double hi) { return -hi * expm1(-s); }
 
 __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
+    // the spin interval's upper end 2/chi0max - 2 eps, from the device maximum
+    // when the chi0 stage left it there (no host round trip)
+    const double hi_sp = a.chi0max ? 2.0 / a.chi0max[0] - a.hi_off : a.hi_sp;
     __shared__ RootCtl sc;
     __shared__ int s_jdir, s_tail;
     const int nwmax = a.nb - 1;
@@ -164,7 +169,7 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
     for (int phase = 0; phase < 2; ++phase) {
         const double sgn = phase == 0 ? -1.0 : 1.0;
         if (threadIdx.x == 0) {
-            const double hi = phase == 0 ? a.hi_sp : 1000.0 * a.U;
+            const double hi = phase == 0 ? hi_sp : 1000.0 * a.U;
             // spin: U/2 (clamped inside the interval); charge: U
             const double x0 = phase == 0 ? a.U / 2.0 : a.U;
             const double xs = (x0 > 0.0 && x0 < hi) ? x0 : 0.5 * hi;
@@ -178,7 +183,7 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
 #pragma unroll 1
         while (!sc.done) {
             if (threadIdx.x == 0) {
-                const double ah = fabs(phase == 0 ? spin_us(sc.x, a.hi_sp) : sc.x) / 2.0;
+                const double ah = fabs(phase == 0 ? spin_us(sc.x, hi_sp) : sc.x) / 2.0;
                 // first frequency of the series (cmax_suf does not increase)
                 int lo = 0, hi = a.nb;
                 while (lo < hi) {
@@ -192,7 +197,7 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
                 s_tail = ah * a.tailm[kMomP] >= kMomSeriesMax;
             }
             __syncthreads();
-            const double x = phase == 0 ? spin_us(sc.x, a.hi_sp) : sc.x, hu = sgn * x / 2.0;
+            const double x = phase == 0 ? spin_us(sc.x, hi_sp) : sc.x, hu = sgn * x / 2.0;
             const int jdir = s_jdir;
             double v = 0.0, dv = 0.0;
             const long long total = (long long)a.nblk * jdir;
@@ -259,7 +264,7 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
                         // chi::sum_rule_sp (src/chi.cpp:833-836)
                         y = tr + n - n * n / 2.0 - nsr + x * nsr * nsr / (2.0 * U);
                         // d/ds = d/dUs * dUs/ds, dUs/ds = hi e^-s = hi - Us
-                        dy = (dtr + nsr * nsr / (2.0 * U)) * (a.hi_sp - x);
+                        dy = (dtr + nsr * nsr / (2.0 * U)) * (hi_sp - x);
                     } else {
                         // chi::sum_rule_ch (src/chi.cpp:840-843)
                         y = tr + n - n * n / 2.0 - (nsr + Usp * nsr * nsr / (2.0 * U) - nsr * nsr);
@@ -270,7 +275,7 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
             }
             __syncthreads();
         }
-        const double root = phase == 0 ? spin_us(sc.root, a.hi_sp) : sc.root;
+        const double root = phase == 0 ? spin_us(sc.root, hi_sp) : sc.root;
         if (phase == 0) Usp = root;
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             a.out[phase] = root;
@@ -684,7 +689,9 @@ cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2
     int grid = 0;
     cudaError_t e = root_grid(k_mu_roots, &grid, rs.max_blocks);
     if (e != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(rs.bar, 0, 2 * sizeof(unsigned) + sizeof(int), st)) != cudaSuccess) return e;
+    // words 4..6 of rs.bar: the sum-rule search's error flag (word 2) stays readable
+    if (rs.reset_mu && (e = cudaMemsetAsync(rs.bar + 4, 0, 2 * sizeof(unsigned) + sizeof(int), st)) != cudaSuccess)
+        return e;
     MuRootArgs a;
     a.S = S;
     a.s2 = s2;
@@ -702,8 +709,8 @@ cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2
     a.nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
     a.wc = wc;
     a.partial = rs.partial;
-    a.bar = rs.bar;
-    a.err = reinterpret_cast<int *>(rs.bar + 2);
+    a.bar = rs.bar + 4;
+    a.err = reinterpret_cast<int *>(rs.bar + 6);
     a.out = rs.out;
     void *args[] = {&a};
     e = cudaLaunchCooperativeKernel((const void *)k_mu_roots, dim3(grid), dim3(kRootThreads), args, 0, st);
@@ -713,11 +720,13 @@ cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2
 
 cudaError_t launch_sumrule_roots(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
                                  const double *mom_suf, const double *cmax_suf, const double *tailm, double T,
-                                 double n, double nsr, double U, double hi_sp, RootScratch rs, cudaStream_t st) {
+                                 double n, double nsr, double U, double hi_sp, RootScratch rs, cudaStream_t st,
+                                 const double *chi0max, double hi_off) {
     int grid = 0;
     cudaError_t e = root_grid(k_sumrule_roots, &grid, rs.max_blocks);
     if (e != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(rs.bar, 0, 2 * sizeof(unsigned) + sizeof(int), st)) != cudaSuccess) return e;
+    if (rs.reset_sr && (e = cudaMemsetAsync(rs.bar, 0, 2 * sizeof(unsigned) + sizeof(int), st)) != cudaSuccess)
+        return e;
     SumRootArgs a;
     a.chiq = reinterpret_cast<const double4 *>(chiq);
     a.cinf = chi0_inf;
@@ -736,6 +745,8 @@ cudaError_t launch_sumrule_roots(const GridDev &g, const double *chiq, const dou
     a.nsr = nsr;
     a.U = U;
     a.hi_sp = hi_sp;
+    a.chi0max = chi0max;
+    a.hi_off = hi_off;
     a.partial = rs.partial;
     a.bar = rs.bar;
     a.err = reinterpret_cast<int *>(rs.bar + 2);
