@@ -99,6 +99,21 @@ int tpsc_set_model(tpsc_ctx *ctx, int nk0, int Nw0, double n, double T, double t
  * TPSC_FORM_REFERENCE. */
 int tpsc_set_form(tpsc_ctx *ctx, int form);
 
+/* CUDA graphs for Newton-form solves (no counterpart in the reference, whose
+ * solve runs on the host).  A Newton-form tpsc_solve queues its launches with
+ * no host round trip, so the whole solve from the chi0 stage to the final
+ * readback can run as one captured graph.  mode 0: direct launches; 1
+ * (default): a solve whose launches repeat those of the previous solve
+ * (same grid, form, model and mu0) is captured and replayed from then on;
+ * 2: every solve is captured (after the grid's first direct solve in that
+ * form), the executable graph updated in place for the new arguments.  A
+ * capture that fails leaves the context on direct launches. */
+int tpsc_set_graph_mode(tpsc_ctx *ctx, int mode);
+
+/* out = {captures, replays, kernels in the current graph, 1 if a capture
+ * failed and graphs are off}. */
+int tpsc_graph_stats(tpsc_ctx *ctx, long long out[4]);
+
 /* chi0::calc_chiqw_FFT_spline(nq0, nw0) (src/chi0.cpp:279-718): switches the
  * current grid to (nq0, nw0) -- re-deriving eps_k and mu0 as set_grid does --
  * and computes chi0(q, iqn), n = 0..nw0/2, with its tail coefficients. */

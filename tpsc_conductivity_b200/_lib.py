@@ -59,6 +59,8 @@ SIGNATURES = [
     ("tpsc_pade_sigma", C.c_int, [C.c_void_p, _ip, C.c_int, _dp, C.c_int, C.c_int, _dp, _dp]),
     ("tpsc_gwn_local", C.c_int, [C.c_void_p, _dp]),
     ("tpsc_set_form", C.c_int, [C.c_void_p, C.c_int]),
+    ("tpsc_set_graph_mode", C.c_int, [C.c_void_p, C.c_int]),
+    ("tpsc_graph_stats", C.c_int, [C.c_void_p, C.c_void_p]),
     ("tpsc_chijj", C.c_int, [C.c_void_p, C.c_int]),
     ("tpsc_get_chijj", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),
     ("tpsc_sigma_iqn", C.c_int, [C.c_void_p, C.c_int, _dp, _dp]),

@@ -62,6 +62,17 @@ class Green:
         find_zero) or _lib.FORM_NEWTON (safeguarded Newton)."""
         self.ctx.call("tpsc_set_form", int(form))
 
+    def set_graph_mode(self, mode):
+        """CUDA graphs for Newton-form solves of the context: 0 off, 1 replay a
+        repeated solve (default), 2 capture every solve."""
+        self.ctx.call("tpsc_set_graph_mode", int(mode))
+
+    def graph_stats(self):
+        """{captures, replays, kernels per graph, off} of the context's solve graph."""
+        out = np.zeros(4, dtype=np.int64)
+        self.ctx.call("tpsc_graph_stats", out.ctypes.data_as(C.c_void_p))
+        return dict(zip(("captures", "replays", "kernels", "off"), out.tolist()))
+
     # ---- stages (reference method names) ---------------------------------
     def calc_chiqw_FFT_spline(self, nq0=None, nw0=None):
         """chi0::calc_chiqw_FFT_spline (src/chi0.cpp:279)."""

@@ -306,6 +306,7 @@ struct Grid {
     double tailq_host[kTailQ] = {0};
     double tailP_host[kTailP] = {0};
     std::vector<void *> allocs;
+    unsigned warm_forms = 0;  // bit f: a direct (uncaptured) Newton solve in form f ran on this grid
     // current-current correlator: device state (allocated on first use) and
     // the last result, [n_theta 2 NB] binned, [2 NB] totals, kx0
     CondDev cond;
@@ -352,6 +353,26 @@ struct tpsc_ctx {
     size_t snap_bytes[2] = {0, 0};
     int snap_next = 0;
     bool copies_pending = false;
+    // the Newton-form solve as a CUDA graph (tpsc_set_graph_mode): the key of
+    // the captured solve, the executable graph and the kernels in it
+    struct SolveKey {
+        const void *grid = nullptr;
+        int form = -1, cap = -1;
+        long long model_id = -1;
+        double mu0 = 0.0;
+        bool rsr = true, rmu = true;
+        bool operator==(const SolveKey &o) const {
+            return grid == o.grid && form == o.form && cap == o.cap && model_id == o.model_id && mu0 == o.mu0 &&
+                   rsr == o.rsr && rmu == o.rmu;
+        }
+    };
+    int graph_mode = 1;            // 0 off, 1 replay a repeated solve, 2 capture every solve
+    bool graph_off = false;        // a capture failed: direct launches from then on
+    bool capturing = false;
+    cudaGraphExec_t graph_exec = nullptr;
+    SolveKey graph_key, seen_key;  // of the captured solve / of the last direct one
+    long long graph_kernels = 0;
+    long long graph_replays = 0, graph_captures = 0;
     std::string err;
 };
 
@@ -565,7 +586,7 @@ struct Piece {
     size_t bytes;
     int at;  // offset in ctx->h_res, doubles
 };
-int read_back(tpsc_ctx *ctx, std::initializer_list<Piece> pieces) {
+int queue_read_back(tpsc_ctx *ctx, std::initializer_list<Piece> pieces) {
     GatherPieces p;
     for (const Piece &q : pieces) {
         p.src[p.n] = static_cast<const unsigned *>(q.src);
@@ -574,6 +595,11 @@ int read_back(tpsc_ctx *ctx, std::initializer_list<Piece> pieces) {
         ++p.n;
     }
     CK(launch_gather(p, ctx->h_res_dev, 1, ctx->st));
+    return TPSC_OK;
+}
+int read_back(tpsc_ctx *ctx, std::initializer_list<Piece> pieces) {
+    int rc = queue_read_back(ctx, pieces);
+    if (rc) return rc;
     CK(cudaStreamSynchronize(ctx->st));
     return TPSC_OK;
 }
@@ -1093,31 +1119,46 @@ int finish_solve(tpsc_ctx *ctx) {
     return TPSC_OK;
 }
 
-// The Newton-form solve after the chi0 stage, queued without a host round
-// trip (the roots, the vertex and Sigma read their inputs on the device), and
-// its one readback: chi0max, the sum-rule roots, the mu search and their
-// barrier flags, checked in stage order.
-int newton_rest(tpsc_ctx *ctx) {
+// stage boundary i of a solve (ctx->ev[i]); an event record node of the graph
+// while the solve is being captured
+int mark(tpsc_ctx *ctx, int i) {
+    CK(cudaEventRecordWithFlags(ctx->ev[i], ctx->st, ctx->capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
+    return TPSC_OK;
+}
+
+// The Newton-form solve from the chi0 stage on, queued on ctx->st without a
+// host round trip (the roots, the vertex and Sigma read their inputs on the
+// device), ending in the gather of everything the host checks into ctx->h_res;
+// newton_finish waits for it and checks chi0max, the sum-rule roots, the mu
+// search and their barrier flags in stage order.
+int newton_queue(tpsc_ctx *ctx) {
     double Usc[2];
     int rc;
+    if ((rc = mark(ctx, 0))) return rc;
+    if ((rc = run_chi0(ctx, false))) return rc;
+    if ((rc = mark(ctx, 1))) return rc;
     if ((rc = roots_Usp_Uch(ctx, Usc, false))) return rc;
-    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    if ((rc = mark(ctx, 2))) return rc;
     if ((rc = run_vertex(ctx))) return rc;
-    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    if ((rc = mark(ctx, 3))) return rc;
     if ((rc = run_self(ctx, false))) return rc;
-    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    if ((rc = mark(ctx, 4))) return rc;
     if ((rc = queue_mu_newton(ctx))) return rc;
-    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    if ((rc = mark(ctx, 5))) return rc;
     // h_res: [0..2] chi0max, qmax; [3..8] the sum-rule roots; [9] their flag;
     // [10..11] the Sigma traces; [12..15] the mu search; [16] its flag; [17] Sigma_inf
-    if ((rc = read_back(ctx, {{ctx->red.result, 3 * sizeof(double), 0},
-                              {ctx->dres, 6 * sizeof(double), 3},
-                              {ctx->roots.bar + 2, sizeof(unsigned), 9},
-                              {ctx->redm.result, 2 * sizeof(double), 10},
-                              {ctx->roots.out, 4 * sizeof(double), 12},
-                              {ctx->roots.bar + 6, sizeof(int), 16},
-                              {ctx->cur->sinf, sizeof(double), 17}})))
-        return rc;
+    return queue_read_back(ctx, {{ctx->red.result, 3 * sizeof(double), 0},
+                                 {ctx->dres, 6 * sizeof(double), 3},
+                                 {ctx->roots.bar + 2, sizeof(unsigned), 9},
+                                 {ctx->redm.result, 2 * sizeof(double), 10},
+                                 {ctx->roots.out, 4 * sizeof(double), 12},
+                                 {ctx->roots.bar + 6, sizeof(int), 16},
+                                 {ctx->cur->sinf, sizeof(double), 17}});
+}
+
+int newton_finish(tpsc_ctx *ctx) {
+    CK(cudaStreamSynchronize(ctx->st));
+    int rc;
     const double *h = ctx->h_res;
     if ((rc = set_chi0max(ctx, h))) return rc;
     unsigned err_sr;
@@ -1133,6 +1174,89 @@ int newton_rest(tpsc_ctx *ctx) {
     r[6] = 0.0;
     r[7] = h[17];
     return set_mu(ctx, r, err_mu);
+}
+
+// the host state newton_queue leaves behind (a replayed graph only launches)
+void newton_state(tpsc_ctx *ctx) {
+    Grid *g = ctx->cur;
+    g->g_mixed = mixed(ctx);
+    g->have_chi0 = g->have_mom = g->have_U = g->have_V = g->have_S = true;
+    g->have_mom_host = false;
+    ctx->roots.reset_sr = ctx->roots.reset_mu = true;
+}
+
+// The Newton-form solve on the current grid, queued directly or as a CUDA
+// graph (ctx->graph_mode): a solve whose key (grid, form, model, mu0, the
+// root searches' barrier state and grid cap: everything its launches take)
+// equals the captured one replays the executable graph; in mode 1 a key seen
+// twice in a row is captured, in mode 2 every key after the grid's first
+// direct solve in that form (so that the kernels' one-time attribute calls
+// happen outside a capture); a new capture updates the executable graph in
+// place when its topology allows.  A capture that fails turns graphs off for
+// the context and the solve runs as direct launches.
+int newton_solve(tpsc_ctx *ctx) {
+    Grid *g = ctx->cur;
+    const GridDev &d = g->d;
+    if (mixed(ctx) && !g->Grt32) CK(dalloc(g, &g->Grt32, (size_t)(d.nw0 + 1) * d.n8));
+    tpsc_ctx::SolveKey key;
+    key.grid = g;
+    key.form = ctx->form;
+    key.cap = ctx->roots.max_blocks;
+    key.model_id = ctx->model_id;
+    key.mu0 = g->mu0;
+    key.rsr = ctx->roots.reset_sr;
+    key.rmu = ctx->roots.reset_mu;
+    const unsigned fbit = 1u << (ctx->form & 3);
+    const bool graphs = ctx->graph_mode > 0 && !ctx->graph_off && (g->warm_forms & fbit);
+    int rc = TPSC_OK;
+    if (graphs && ctx->graph_exec && key == ctx->graph_key) {
+        CK(cudaGraphLaunch(ctx->graph_exec, ctx->st));
+        add_launches(ctx->graph_kernels);
+        ++ctx->graph_replays;
+        newton_state(ctx);
+        return newton_finish(ctx);
+    }
+    if (graphs && (ctx->graph_mode == 2 || key == ctx->seen_key)) {
+        const long long k0 = launches_thread();
+        CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
+        ctx->capturing = true;
+        rc = newton_queue(ctx);
+        ctx->capturing = false;
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ctx->st, &graph);
+        const long long nk = launches_thread() - k0;
+        add_launches(-nk);
+        if (rc == TPSC_OK && e == cudaSuccess && graph) {
+            if (ctx->graph_exec) {
+                cudaGraphExecUpdateResultInfo info;
+                if (cudaGraphExecUpdate(ctx->graph_exec, graph, &info) != cudaSuccess) {
+                    cudaGetLastError();
+                    cudaGraphExecDestroy(ctx->graph_exec);
+                    ctx->graph_exec = nullptr;
+                }
+            }
+            if (!ctx->graph_exec) e = cudaGraphInstantiate(&ctx->graph_exec, graph, 0);
+        }
+        if (graph) cudaGraphDestroy(graph);
+        if (rc == TPSC_OK && e == cudaSuccess && ctx->graph_exec) {
+            ctx->graph_key = key;
+            ctx->graph_kernels = nk;
+            ++ctx->graph_captures;
+            CK(cudaGraphLaunch(ctx->graph_exec, ctx->st));
+            add_launches(nk);
+            return newton_finish(ctx);
+        }
+        // the capture failed: the same launches, directly, from now on
+        cudaGetLastError();
+        if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+        ctx->graph_exec = nullptr;
+        ctx->graph_off = true;
+        ctx->err.clear();
+    }
+    ctx->seen_key = key;
+    if ((rc = newton_queue(ctx))) return rc;
+    g->warm_forms |= fbit;
+    return newton_finish(ctx);
 }
 
 int find_mu(tpsc_ctx *ctx) {
@@ -1366,6 +1490,7 @@ void tpsc_destroy(tpsc_ctx *ctx) {
     if (ctx->roots.bar) cudaFree(ctx->roots.bar);
     if (ctx->roots.out) cudaFree(ctx->roots.out);
     if (ctx->dres) cudaFree(ctx->dres);
+    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     if (ctx->h_res) cudaFreeHost(ctx->h_res);
     if (ctx->stage) cudaFree(ctx->stage);
     if (ctx->cst) cudaStreamSynchronize(ctx->cst);
@@ -1786,17 +1911,18 @@ int tpsc_solve(tpsc_ctx *ctx) {
     int rc = need_model(ctx);
     if (rc) return rc;
     cudaSetDevice(ctx->device);
+    if (ctx->form & TPSC_FORM_NEWTON) {
+        // no host round trip from the chi0 stage to the one readback at the end
+        if ((rc = switch_grid(ctx, ctx->nk0, ctx->Nw0))) return rc;
+        if ((rc = newton_solve(ctx))) return rc;
+        return finish_solve(ctx);
+    }
     CK(cudaEventRecord(ctx->ev[0], ctx->st));
     rc = switch_grid(ctx, ctx->nk0, ctx->Nw0);
     if (rc) return rc;
-    const bool newton = (ctx->form & TPSC_FORM_NEWTON) != 0;
-    rc = run_chi0(ctx, !newton);
+    rc = run_chi0(ctx);
     if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
-    if (newton) {
-        if ((rc = newton_rest(ctx))) return rc;
-        return finish_solve(ctx);
-    }
     double Usc[2];
     rc = roots_Usp_Uch(ctx, Usc);
     if (rc) return rc;
@@ -2302,4 +2428,20 @@ int tpsc_kernel_bytes(tpsc_ctx *ctx, int which, double *bytes) {
 // run several contexts' solves at once on one GPU (tpsc_batch.cpp).
 void tpsc_ctx_set_coop_cap(tpsc_ctx *ctx, int blocks) {
     if (ctx) ctx->roots.max_blocks = blocks;
+}
+
+int tpsc_set_graph_mode(tpsc_ctx *ctx, int mode) {
+    if (!ctx) return fail(nullptr, TPSC_ERR_ARG, "null context");
+    if (mode < 0 || mode > 2) return fail(ctx, TPSC_ERR_ARG, "graph mode must be 0, 1 or 2");
+    ctx->graph_mode = mode;
+    return TPSC_OK;
+}
+
+int tpsc_graph_stats(tpsc_ctx *ctx, long long out[4]) {
+    if (!ctx || !out) return fail(ctx, TPSC_ERR_ARG, "bad arguments");
+    out[0] = ctx->graph_captures;
+    out[1] = ctx->graph_replays;
+    out[2] = ctx->graph_kernels;
+    out[3] = ctx->graph_off ? 1 : 0;
+    return TPSC_OK;
 }

@@ -29,8 +29,11 @@ namespace tpsc {
 
 // kernels launched by this library (all contexts), for the instrumentation ABI
 static std::atomic<long long> g_launches{0};
+// the same count for the calling host thread (kernels in one stream capture)
+static thread_local long long t_launches = 0;
 cudaError_t launched(int n) {
     g_launches.fetch_add(n, std::memory_order_relaxed);
+    t_launches += n;
     return cudaGetLastError();
 }
 
@@ -1655,6 +1658,8 @@ struct RunSigmaTau {
 }  // namespace
 
 long long launches_total() { return g_launches.load(); }
+long long launches_thread() { return t_launches; }
+void add_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 cudaError_t smem_optin(const void *fn) {
     static std::mutex mu;

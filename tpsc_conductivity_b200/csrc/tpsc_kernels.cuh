@@ -250,6 +250,11 @@ cudaError_t launch_store(double *dst, const double *v, int n, cudaStream_t st);
 
 // kernels launched by the library so far
 long long launches_total();
+// kernels launched (or captured) by the calling host thread so far
+long long launches_thread();
+// adds n to the library's count (kernels replayed by a CUDA graph; negative
+// to take back the kernels that a stream capture only recorded)
+void add_launches(long long n);
 
 // the FFT lengths the build instantiates
 bool supported_grid(int nk0, int nw0);
