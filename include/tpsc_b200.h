@@ -334,6 +334,10 @@ tpsc_batch *tpsc_batch_create(int device, int nstreams, int *status);
 void tpsc_batch_destroy(tpsc_batch *b);
 const char *tpsc_batch_last_error(const tpsc_batch *b);
 int tpsc_batch_streams(const tpsc_batch *b, int *nstreams);
+/* tpsc_set_graph_mode of every context of the batch (default 1); with 2,
+ * each Newton-form point runs as one graph launch, the graph of its grid
+ * updated in place for the point's model. */
+int tpsc_batch_set_graph_mode(tpsc_batch *b, int mode);
 /* params: npts rows {nk0, Nw0, n, T, tp, tpp, t3, U} (row-major doubles);
  * form: enum tpsc_form; results: npts rows of TPSC_S_COUNT scalars in the
  * tpsc_get_scalars order (NaN for a failed point); status[i]: point i's

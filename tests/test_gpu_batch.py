@@ -89,3 +89,25 @@ def test_batch_tuner_keeps_a_timed_count():
     t = b.tune(pts, max_streams=4)
     assert sorted(t) == [1, 2, 4] and all(v > 0 for v in t.values())
     assert b.nstreams == min(t, key=t.get)
+
+
+@pytest.mark.parametrize("form_name", ["newton", "mixed_newton"])
+def test_batch_as_graph_launches_equals_direct_launches(form_name):
+    """Graph mode 2: every point after a grid's first runs as one launch of
+    that grid's graph, updated in place for the point; the scalars are those
+    of the same sweep run as direct launches, bit for bit."""
+    from tpsc_conductivity_b200 import _lib
+    from tpsc_conductivity_b200.api import Batch, sweep_points
+
+    form = _lib.FORM_NEWTON | (_lib.FORM_MIXED if form_name == "mixed_newton" else 0)
+    pts = sweep_points(24, seed=11)
+    direct = Batch(nstreams=3)
+    direct.set_graph_mode(0)
+    ref, st0, _ = direct.solve(pts, form)
+    graphs = Batch(nstreams=3)
+    graphs.set_graph_mode(2)
+    for _ in range(2):
+        res, st, _ = graphs.solve(pts, form)
+        assert np.array_equal(st, st0)
+        ok = st0 == 0
+        assert np.array_equal(res[ok], ref[ok])

@@ -387,6 +387,13 @@ class Batch:
             self._err(rc)
         return {2 ** i: float(ms[i]) for i in range(k)}
 
+    def set_graph_mode(self, mode):
+        """tpsc_set_graph_mode of every solver context (2: each Newton-form
+        point is one graph launch, updated in place per point)."""
+        rc = self.lib.tpsc_batch_set_graph_mode(self.h, int(mode))
+        if rc:
+            self._err(rc)
+
     @property
     def nstreams(self):
         v = C.c_int(0)

@@ -31,6 +31,7 @@ struct tpsc_batch {
     int device = 0;
     int nstreams = 1;
     int sms = 0;
+    int graph_mode = 1;  // tpsc_set_graph_mode of every context
     std::vector<tpsc_ctx *> ctxs;
     std::string err;
 };
@@ -52,7 +53,10 @@ int ensure_contexts(tpsc_batch *b, int n) {
         b->ctxs.push_back(c);
     }
     const int cap = n > 1 ? std::max(8, 2 * b->sms / n) : 0;
-    for (int i = 0; i < n; ++i) tpsc_ctx_set_coop_cap(b->ctxs[i], cap);
+    for (int i = 0; i < n; ++i) {
+        tpsc_ctx_set_coop_cap(b->ctxs[i], cap);
+        tpsc_set_graph_mode(b->ctxs[i], b->graph_mode);
+    }
     return TPSC_OK;
 }
 
@@ -171,6 +175,17 @@ void tpsc_batch_destroy(tpsc_batch *b) {
 }
 
 const char *tpsc_batch_last_error(const tpsc_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+int tpsc_batch_set_graph_mode(tpsc_batch *b, int mode) {
+    if (!b) return TPSC_ERR_ARG;
+    if (mode < 0 || mode > 2) {
+        b->err = "graph mode must be 0, 1 or 2";
+        return TPSC_ERR_ARG;
+    }
+    b->graph_mode = mode;
+    for (tpsc_ctx *c : b->ctxs) tpsc_set_graph_mode(c, mode);
+    return TPSC_OK;
+}
 
 int tpsc_batch_streams(const tpsc_batch *b, int *nstreams) {
     if (!b || !nstreams) return TPSC_ERR_ARG;

@@ -269,6 +269,19 @@ bool newton_root(F &&func, double x0, double lo, double hi, double tol, double *
 // ---------------------------------------------------------------------------
 // one (nk0, Nw0) grid: tables and arrays
 // ---------------------------------------------------------------------------
+// What a Newton-form solve's launches take beyond the grid's buffers: the
+// key of a captured solve graph (tpsc_set_graph_mode)
+struct SolveKey {
+    int form = -1, cap = -1;
+    long long model_id = -1;
+    double mu0 = 0.0;
+    bool rsr = true, rmu = true;
+    bool operator==(const SolveKey &o) const {
+        return form == o.form && cap == o.cap && model_id == o.model_id && mu0 == o.mu0 && rsr == o.rsr &&
+               rmu == o.rmu;
+    }
+};
+
 struct Grid {
     GridDev d;
     cudaStream_t st = nullptr;    // the owning context's stream: every fill and upload is ordered on it
@@ -307,6 +320,11 @@ struct Grid {
     double tailP_host[kTailP] = {0};
     std::vector<void *> allocs;
     unsigned warm_forms = 0;  // bit f: a direct (uncaptured) Newton solve in form f ran on this grid
+    // the Newton-form solve on this grid as an executable CUDA graph, the key
+    // it was captured with and the kernels in it
+    cudaGraphExec_t graph_exec = nullptr;
+    SolveKey graph_key;
+    long long graph_kernels = 0;
     // current-current correlator: device state (allocated on first use) and
     // the last result, [n_theta 2 NB] binned, [2 NB] totals, kx0
     CondDev cond;
@@ -353,25 +371,14 @@ struct tpsc_ctx {
     size_t snap_bytes[2] = {0, 0};
     int snap_next = 0;
     bool copies_pending = false;
-    // the Newton-form solve as a CUDA graph (tpsc_set_graph_mode): the key of
-    // the captured solve, the executable graph and the kernels in it
-    struct SolveKey {
-        const void *grid = nullptr;
-        int form = -1, cap = -1;
-        long long model_id = -1;
-        double mu0 = 0.0;
-        bool rsr = true, rmu = true;
-        bool operator==(const SolveKey &o) const {
-            return grid == o.grid && form == o.form && cap == o.cap && model_id == o.model_id && mu0 == o.mu0 &&
-                   rsr == o.rsr && rmu == o.rmu;
-        }
-    };
-    int graph_mode = 1;            // 0 off, 1 replay a repeated solve, 2 capture every solve
-    bool graph_off = false;        // a capture failed: direct launches from then on
+    // Newton-form solves as CUDA graphs (tpsc_set_graph_mode; the executable
+    // graphs live in the grids)
+    int graph_mode = 1;       // 0 off, 1 replay a repeated solve, 2 capture every solve
+    bool graph_off = false;   // a capture failed: direct launches from then on
     bool capturing = false;
-    cudaGraphExec_t graph_exec = nullptr;
-    SolveKey graph_key, seen_key;  // of the captured solve / of the last direct one
-    long long graph_kernels = 0;
+    const void *seen_grid = nullptr;
+    SolveKey seen_key;        // of the last direct solve
+    long long graph_kernels = 0;  // in the graph of the last captured or replayed solve
     long long graph_replays = 0, graph_captures = 0;
     std::string err;
 };
@@ -412,6 +419,7 @@ cudaError_t dalloc(Grid *g, T **p, size_t count) {
 }
 
 void free_grid(Grid *g) {
+    if (g->graph_exec) cudaGraphExecDestroy(g->graph_exec);
     for (void *p : g->allocs) cudaFree(p);
     if (g->cond.partial) cudaFree(g->cond.partial);
     if (g->cond.out) cudaFree(g->cond.out);
@@ -1198,8 +1206,7 @@ int newton_solve(tpsc_ctx *ctx) {
     Grid *g = ctx->cur;
     const GridDev &d = g->d;
     if (mixed(ctx) && !g->Grt32) CK(dalloc(g, &g->Grt32, (size_t)(d.nw0 + 1) * d.n8));
-    tpsc_ctx::SolveKey key;
-    key.grid = g;
+    SolveKey key;
     key.form = ctx->form;
     key.cap = ctx->roots.max_blocks;
     key.model_id = ctx->model_id;
@@ -1209,14 +1216,15 @@ int newton_solve(tpsc_ctx *ctx) {
     const unsigned fbit = 1u << (ctx->form & 3);
     const bool graphs = ctx->graph_mode > 0 && !ctx->graph_off && (g->warm_forms & fbit);
     int rc = TPSC_OK;
-    if (graphs && ctx->graph_exec && key == ctx->graph_key) {
-        CK(cudaGraphLaunch(ctx->graph_exec, ctx->st));
-        add_launches(ctx->graph_kernels);
+    if (graphs && g->graph_exec && key == g->graph_key) {
+        CK(cudaGraphLaunch(g->graph_exec, ctx->st));
+        add_launches(g->graph_kernels);
+        ctx->graph_kernels = g->graph_kernels;
         ++ctx->graph_replays;
         newton_state(ctx);
         return newton_finish(ctx);
     }
-    if (graphs && (ctx->graph_mode == 2 || key == ctx->seen_key)) {
+    if (graphs && (ctx->graph_mode == 2 || (key == ctx->seen_key && ctx->seen_grid == g))) {
         const long long k0 = launches_thread();
         CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
         ctx->capturing = true;
@@ -1227,33 +1235,34 @@ int newton_solve(tpsc_ctx *ctx) {
         const long long nk = launches_thread() - k0;
         add_launches(-nk);
         if (rc == TPSC_OK && e == cudaSuccess && graph) {
-            if (ctx->graph_exec) {
+            if (g->graph_exec) {
                 cudaGraphExecUpdateResultInfo info;
-                if (cudaGraphExecUpdate(ctx->graph_exec, graph, &info) != cudaSuccess) {
+                if (cudaGraphExecUpdate(g->graph_exec, graph, &info) != cudaSuccess) {
                     cudaGetLastError();
-                    cudaGraphExecDestroy(ctx->graph_exec);
-                    ctx->graph_exec = nullptr;
+                    cudaGraphExecDestroy(g->graph_exec);
+                    g->graph_exec = nullptr;
                 }
             }
-            if (!ctx->graph_exec) e = cudaGraphInstantiate(&ctx->graph_exec, graph, 0);
+            if (!g->graph_exec) e = cudaGraphInstantiate(&g->graph_exec, graph, 0);
         }
         if (graph) cudaGraphDestroy(graph);
-        if (rc == TPSC_OK && e == cudaSuccess && ctx->graph_exec) {
-            ctx->graph_key = key;
-            ctx->graph_kernels = nk;
+        if (rc == TPSC_OK && e == cudaSuccess && g->graph_exec) {
+            g->graph_key = key;
+            g->graph_kernels = ctx->graph_kernels = nk;
             ++ctx->graph_captures;
-            CK(cudaGraphLaunch(ctx->graph_exec, ctx->st));
+            CK(cudaGraphLaunch(g->graph_exec, ctx->st));
             add_launches(nk);
             return newton_finish(ctx);
         }
         // the capture failed: the same launches, directly, from now on
         cudaGetLastError();
-        if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
-        ctx->graph_exec = nullptr;
+        if (g->graph_exec) cudaGraphExecDestroy(g->graph_exec);
+        g->graph_exec = nullptr;
         ctx->graph_off = true;
         ctx->err.clear();
     }
     ctx->seen_key = key;
+    ctx->seen_grid = g;
     if ((rc = newton_queue(ctx))) return rc;
     g->warm_forms |= fbit;
     return newton_finish(ctx);
@@ -1490,7 +1499,6 @@ void tpsc_destroy(tpsc_ctx *ctx) {
     if (ctx->roots.bar) cudaFree(ctx->roots.bar);
     if (ctx->roots.out) cudaFree(ctx->roots.out);
     if (ctx->dres) cudaFree(ctx->dres);
-    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     if (ctx->h_res) cudaFreeHost(ctx->h_res);
     if (ctx->stage) cudaFree(ctx->stage);
     if (ctx->cst) cudaStreamSynchronize(ctx->cst);
