@@ -357,6 +357,55 @@ int tpsc_batch_tune(tpsc_batch *b, int form, int npts, const double *params, int
  * t' ~ U[-0.3, 0]; t'' = t3 = 0 and Nw0 = 2 nextpow2(ceil(40 / (pi T))). */
 int tpsc_sweep_points(int npts, unsigned long long seed, double *params);
 
+/* ---- warm start from saved results ---------------------------------------
+ * tpsc_set_self <- green::load_Self_bin / load_Self (src/green.cpp:1517-1541,
+ * 1637-1670): self_kw [Nw0/2][N8] complex (the Self_kw_array layout) becomes
+ * the current grid's S; sigma_inf2/3/4 [N8] and sigma_inf (one double)
+ * replace the device's only when not NULL, as the reference's loaders leave
+ * them.  find_mu, the traces and chi_jj then run on it. */
+int tpsc_set_self(tpsc_ctx *ctx, const double *self_kw, const double *sigma_inf2, const double *sigma_inf3,
+                  const double *sigma_inf4, const double *sigma_inf);
+/* tpsc_set_chi0 <- chi0::loadChi0 (src/chi0.cpp:99-154): chiqw
+ * [Nw0/2 + 1][N8] becomes the current grid's chi0(q, iqn); chi0max and qmax
+ * are found again (TPSC_S_CHI0MAX, _QMAX0/1); the tail coefficients and
+ * chi0(r, tau) stay those of the last chi0 stage. */
+int tpsc_set_chi0(tpsc_ctx *ctx, const double *chiqw);
+/* Sigma(k, tau_j) [N8], 0 <= j <= Nw0, of the last Sigma stage: the spline
+ * nodes of green::calc_Self_FFT_spline (src/green.cpp:1872-1950). */
+int tpsc_get_sigma_tau(tpsc_ctx *ctx, int j, double *out);
+
+/* ---- the reference's on-disk formats (host only; no context) -------------
+ * Names: the reference's sprintf formats, written into out[cap]. */
+enum tpsc_file_kind {
+    TPSC_FILE_CHI0_BIN = 0,   /* chi0_<tp>_<tpp>_<t3>_<n>_<T>_<nk0>_<nbw>.dat (src/chi0.cpp:63) */
+    TPSC_FILE_SELF_BIN = 1,   /* self_bin_<U>_..._<nk0>_<nbw>.dat (src/green.cpp:1507) */
+    TPSC_FILE_SELF_ASCII = 2, /* self_tpsc_<U>_..._<nk0>_<nbw>.dat (src/green.cpp:1557) */
+    TPSC_FILE_GREEN = 3       /* Green_<U>_..._<nk0>_<nbw>_<l>_<m>.dat (src/green.cpp:1606) */
+};
+int tpsc_file_name(int kind, char *out, int cap, double U, double tp, double tpp, double t3, double n, double T,
+                   int nk0, int nbw, int l, int m);
+/* chi0::save_chi / loadChi0 (src/chi0.cpp:61-154): int nbq, int nwmax, then
+ * nwmax + 1 frames of N8 = nbq (nbq + 1) / 2 doubles.  The reader returns the
+ * header and, when chiqw is not NULL, the frames (cap doubles available). */
+int tpsc_write_chi0_bin(const char *path, int nbq, int nwmax, const double *chiqw);
+int tpsc_read_chi0_bin(const char *path, int *nbq, int *nwmax, double *chiqw, long long cap);
+/* green::save_Self_bin / load_Self_bin (src/green.cpp:1496-1541): nbw/2 + 1
+ * frames of N8 complex.  The first nbw/2 are S; the last is what the
+ * reference's Sigma stage leaves there, (Sigma(k, beta/2), 0) -- pass it as
+ * last [N8] complex (tpsc_get_sigma_tau(ctx, nbw/2, ...)), or NULL for zeros.
+ * The reader fills all nbw/2 + 1 frames. */
+int tpsc_write_self_bin(const char *path, int nbk, int nbw, const double *self_kw, const double *last);
+int tpsc_read_self_bin(const char *path, int nbk, int nbw, double *self_kw);
+/* green::save_Self / load_Self (src/green.cpp:1544-1574, 1637-1670): ascii,
+ * "n l m Re Im" per line; nfreq frames (0 or > nbw/2: all nbw/2). */
+int tpsc_write_self_ascii(const char *path, int nbk, int nbw, int nfreq, const double *self_kw);
+int tpsc_read_self_ascii(const char *path, int nbk, int nbw, double *self_kw);
+/* green::save_Green (src/green.cpp:1577-1633) at one k: G(i w_n) =
+ * 1 / (z - ek_mu - Sigma(z)), Sigma = sigma_inf/z + s2/z^2 + s3/z^3 + S/z^4,
+ * S read at self_col[2 stride j] (complex stride), n < nbw/2. */
+int tpsc_write_green_ascii(const char *path, int nbw, double T, double ek_mu, double sigma_inf, double s2, double s3,
+                           const double *self_col, long long stride);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,6 +18,10 @@
  *        post   solve + find_FS_inter, MDC(10 points, w=0, 4 etas), Gwn_local
  *               (src/tpsc_main.cpp:77-114)
  *        bench  timings only: the half-grid pre-pass alone, then the solve
+ *        files  solve, then the reference's own writers of the saved-run
+ *               formats: chi0::save_chi, green::save_Self(0),
+ *               green::save_Self_bin, green::save_Green({2, 1})
+ *               (src/chi0.cpp:61, src/green.cpp:1496-1633)
  * The reference writes its own text files into the current directory; the
  * probe chdir()s into OUTDIR/work first so they land there.
  */
@@ -70,6 +74,15 @@ public:
         sp_corr_length();
         fprintf(meta, "vF %.17g\nxi_y %.17g\nxi_x %.17g\nxiAs_y %.17g\nxiAs_x %.17g\nxi0_y %.17g\nxi0_x %.17g\n",
                 vF, spCorrLgth_y, spCorrLgth_x, spCorrLgthAs_y, spCorrLgthAs_x, xi0_y, xi0_x);
+    }
+
+    // the saved-run formats, written by the reference's own methods
+    void save_files() {
+        save_chi();
+        save_Self(0);
+        save_Self_bin();
+        int k[2] = {2, 1};
+        save_Green(k);
     }
 
     void dump_cond(FILE *meta, const std::string &dir) {
@@ -152,7 +165,7 @@ int main(int argc, char **argv) {
         t0 = omp_get_wtime();
         g->find_Usp_Uch(nk0 / 2, Nw0 / 2, Usc);
         fprintf(meta, "t_half %.6f\n", omp_get_wtime() - t0);
-    } else if (mode == "solve" || mode == "post" || mode == "cond") {
+    } else if (mode == "solve" || mode == "post" || mode == "cond" || mode == "files") {
         g->set_keep_chiqw(true);
         t0 = omp_get_wtime();
         g->calc_Self_FFT_spline();
@@ -169,6 +182,7 @@ int main(int argc, char **argv) {
         g->dump_chi0(meta, absdir);
         g->dump_solve(meta, absdir);
         g->dump_corr(meta);
+        if (mode == "files") g->save_files();
         if (mode == "post" || mode == "cond") {
             // the post-processing tpsc_main.cpp runs after find_mu (lines 77-114)
             g->find_FS_inter();

@@ -42,7 +42,16 @@ CASES = {
     "l64_w1024_u4": ("solve", 4.0, -0.15, 0.0, 0.0, 0.875, 0.05, 64, 1024, False),
     # the 256x256, 2048 positive iwn case: scalars and sampled columns only
     "l256_w4096_u4": ("solve", 4.0, -0.15, 0.0, 0.0, 0.875, 0.05, 256, 4096, False),
+    # the saved-run files (chi0 binary, self_bin, self_tpsc ascii, Green ascii)
+    # as the reference's own writers leave them, byte for byte, on a 16x16
+    # lattice with 16 positive iwn
+    "files_l16_w32": ("files", 2.0, -0.1, 0.0, 0.0, 0.875, 0.25, 16, 32, True),
 }
+
+# the files the reference's writers leave (src/chi0.cpp:63, src/green.cpp:1507,
+# 1557, 1606); chi0_qmax_wn_* and chi0_wn0_q_* are the chi0 stage's own dumps
+FILE_PREFIXES = ("chi0_", "self_bin_", "self_tpsc_", "Green_")
+FILE_SKIP = ("chi0_qmax_wn_", "chi0_wn0_q_")
 
 
 def read_meta(path):
@@ -132,6 +141,14 @@ def run_case(name, spec, threads):
             out["gwn_local"] = g[:, 1] + 1j * g[:, 2]
             out["fs_inter"] = table("FS_inter_AkF_", exclude="FS_inter_AkF_Pade_")
             out["fs_inter_pade"] = table("FS_inter_AkF_Pade_")
+        if mode == "files":
+            work = os.path.join(d, "work")
+            names = sorted(f for f in os.listdir(work)
+                           if f.startswith(FILE_PREFIXES) and not f.startswith(FILE_SKIP))
+            out["file_names"] = np.array(names)
+            for i, f in enumerate(names):
+                out[f"file_{i}"] = np.fromfile(os.path.join(work, f), dtype=np.uint8)
+            out["ek"] = rd("ek.bin", (nbk, nbk))
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
         print(name, "done", {k: meta.get(k) for k in ("Usp", "Uch", "mu")})
 

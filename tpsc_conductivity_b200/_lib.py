@@ -29,6 +29,19 @@ SIGNATURES = [
     ("tpsc_sp_corr_length", C.c_int, [C.c_void_p, _dp]),
     ("tpsc_sumrule_tangents", C.c_int, [C.c_void_p, _dp]),
     ("tpsc_get_self_async", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    ("tpsc_set_self", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),
+    ("tpsc_set_chi0", C.c_int, [C.c_void_p, _dp]),
+    ("tpsc_get_sigma_tau", C.c_int, [C.c_void_p, C.c_int, _dp]),
+    ("tpsc_file_name", C.c_int, [C.c_int, C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                 C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int]),
+    ("tpsc_write_chi0_bin", C.c_int, [C.c_char_p, C.c_int, C.c_int, _dp]),
+    ("tpsc_read_chi0_bin", C.c_int, [C.c_char_p, _ip, _ip, _dp, C.c_longlong]),
+    ("tpsc_write_self_bin", C.c_int, [C.c_char_p, C.c_int, C.c_int, _dp, _dp]),
+    ("tpsc_read_self_bin", C.c_int, [C.c_char_p, C.c_int, C.c_int, _dp]),
+    ("tpsc_write_self_ascii", C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _dp]),
+    ("tpsc_read_self_ascii", C.c_int, [C.c_char_p, C.c_int, C.c_int, _dp]),
+    ("tpsc_write_green_ascii", C.c_int, [C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                         C.c_double, _dp, C.c_longlong]),
     ("tpsc_wait_copies", C.c_int, [C.c_void_p, C.c_int]),
     ("tpsc_sumrule_vjp", C.c_int, [C.c_void_p, _dp, _dp]),
     ("tpsc_set_mu_shift", C.c_int, [C.c_void_p, C.c_double]),
@@ -74,6 +87,8 @@ SIGNATURES = [
 
 # enum tpsc_form (flags)
 FORM_REFERENCE, FORM_NEWTON, FORM_MIXED = 0, 1, 2
+# enum tpsc_file_kind
+FILE_CHI0_BIN, FILE_SELF_BIN, FILE_SELF_ASCII, FILE_GREEN = 0, 1, 2, 3
 
 # tpsc_run_kernel stage ids
 KERNELS = ["gslice", "chi0_slice", "chi0_tau", "vertex_q", "vertex_tau", "sigma_slice", "sigma_tau",

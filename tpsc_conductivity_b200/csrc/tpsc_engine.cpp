@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../include/tpsc_b200.h"
+#include "tpsc_host.h"
 #include "tpsc_kernels.cuh"
 
 using namespace tpsc;
@@ -1431,6 +1432,10 @@ int copy_out(tpsc_ctx *ctx, void *host, const void *dev, size_t bytes) {
 
 }  // namespace
 
+namespace tpsc {
+int static_fail(int code, const std::string &msg) { return fail(nullptr, code, msg); }
+}  // namespace tpsc
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
@@ -2028,6 +2033,77 @@ int tpsc_get_self(tpsc_ctx *ctx, double *self_kw, double *s2, double *s3, double
     if (s4 && (rc = copy_out(ctx, s4, g->s4, d.n8 * sizeof(double)))) return rc;
     CK(cudaStreamSynchronize(ctx->st));
     return TPSC_OK;
+}
+
+// Sigma(k, tau_j) of the last Sigma stage, j <= Nw0 (the spline nodes of
+// green::calc_Self_FFT_spline, src/green.cpp:1872-1885, 1936-1950)
+int tpsc_get_sigma_tau(tpsc_ctx *ctx, int j, double *out) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    Grid *g = ctx->cur;
+    const GridDev &d = g->d;
+    if (!out || j < 0 || j > d.nw0) return fail(ctx, TPSC_ERR_ARG, "need 0 <= j <= Nw0 and an output array");
+    if (!g->have_S) return fail(ctx, TPSC_ERR_STATE, "the self-energy has not been computed");
+    cudaSetDevice(ctx->device);
+    const size_t bytes = (size_t)d.n8 * sizeof(double);
+    if ((rc = ensure_stage(ctx, bytes))) return rc;
+    CK(launch_take_row(g->sigt, d.nw0 + 1, j, d.n8, (double *)ctx->stage, ctx->st));
+    if ((rc = copy_out(ctx, out, ctx->stage, bytes))) return rc;
+    CK(cudaStreamSynchronize(ctx->st));
+    return TPSC_OK;
+}
+
+// Warm start from saved results (green::load_Self_bin / load_Self,
+// src/green.cpp:1517-1541, 1637-1670): the reference's Self_kw_array layout
+// [Nw0/2][N8] complex into the device's blocked S; each tail array (and
+// Sigma_inf) replaced only when given, as the reference's loaders leave them.
+int tpsc_set_self(tpsc_ctx *ctx, const double *self_kw, const double *s2, const double *s3, const double *s4,
+                  const double *sigma_inf) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    if (!self_kw) return fail(ctx, TPSC_ERR_ARG, "null self_kw");
+    cudaSetDevice(ctx->device);
+    Grid *g = ctx->cur;
+    const GridDev &d = g->d;
+    const size_t bytes = (size_t)(d.nw0 / 2) * d.n8 * sizeof(double2);
+    if ((rc = ensure_stage(ctx, bytes))) return rc;
+    CK(cudaMemcpyAsync(ctx->stage, self_kw, bytes, cudaMemcpyHostToDevice, ctx->st));
+    CK(launch_block_c((const double2 *)ctx->stage, g->S, d.nw0 / 2, d.nw0 / 2, d.n8, ctx->st));
+    const size_t vb = (size_t)d.n8 * sizeof(double);
+    if (s2) CK(cudaMemcpyAsync(g->s2, s2, vb, cudaMemcpyHostToDevice, ctx->st));
+    if (s3) CK(cudaMemcpyAsync(g->s3, s3, vb, cudaMemcpyHostToDevice, ctx->st));
+    if (s4) CK(cudaMemcpyAsync(g->s4, s4, vb, cudaMemcpyHostToDevice, ctx->st));
+    if (sigma_inf) {
+        CK(cudaMemcpyAsync(g->sinf, sigma_inf, sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+        ctx->scal[TPSC_S_SIGMA_INF] = *sigma_inf;
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    g->have_S = true;
+    ctx->scal[TPSC_S_EVALS_MU] = 0;  // mu belongs to the Sigma before this one
+    return TPSC_OK;
+}
+
+// chi0::loadChi0 (src/chi0.cpp:99-154): chi0(q, iqn) [Nw0/2 + 1][N8] of the
+// current grid replaces the device's; chi0max and qmax are found again; the
+// tail coefficients and chi0(r, tau) stay those of the last chi0 stage, as the
+// reference's loader leaves them.
+int tpsc_set_chi0(tpsc_ctx *ctx, const double *chiqw) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    if (!chiqw) return fail(ctx, TPSC_ERR_ARG, "null chiqw");
+    cudaSetDevice(ctx->device);
+    Grid *g = ctx->cur;
+    const GridDev &d = g->d;
+    const size_t bytes = (size_t)d.nb * d.n8 * sizeof(double);
+    if ((rc = ensure_stage(ctx, bytes))) return rc;
+    CK(cudaMemcpyAsync(ctx->stage, chiqw, bytes, cudaMemcpyHostToDevice, ctx->st));
+    CK(launch_block((const double *)ctx->stage, g->chiq, d.nb, d.nb, d.n8, ctx->st));
+    CK(launch_chi0max(d, g->chiq, ctx->red, ctx->st));
+    double r[3];
+    if ((rc = read_result(ctx, 3, r))) return rc;
+    g->have_chi0 = true;
+    g->have_V = g->have_S = g->have_mom = g->have_U = false;
+    return set_chi0max(ctx, r);
 }
 
 int tpsc_get_self_async(tpsc_ctx *ctx, double *self_kw, double *s2, double *s3, double *s4) {

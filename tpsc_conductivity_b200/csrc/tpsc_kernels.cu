@@ -1503,6 +1503,30 @@ __global__ void k_unblock_c(const double2 *__restrict__ src, double2 *__restrict
     }
 }
 
+// [j][o] -> blocked (NJ rows): the setters' inverse of k_unblock
+__global__ void k_block(const double *__restrict__ src, double *__restrict__ dst, int NJ, int nrows, int n8) {
+    const long long total = (long long)nrows * n8;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(i / n8), o = (int)(i % n8);
+        dst[bidx(j, o, NJ)] = src[i];
+    }
+}
+__global__ void k_block_c(const double2 *__restrict__ src, double2 *__restrict__ dst, int NJ, int nrows, int n8) {
+    const long long total = (long long)nrows * n8;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(i / n8), o = (int)(i % n8);
+        dst[bidx(j, o, NJ)] = src[i];
+    }
+}
+
+// row j of a blocked (NJ rows) array -> dst[o]
+__global__ void k_take_row(const double *__restrict__ src, int NJ, int j, int n8, double *__restrict__ dst) {
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n8; o += gridDim.x * blockDim.x)
+        dst[o] = src[bidx(j, o, NJ)];
+}
+
 __global__ void k_gather(GatherPieces p, unsigned *__restrict__ dst) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (int k = 0; k < p.n; ++k)
@@ -1962,6 +1986,23 @@ cudaError_t launch_unblock(const double *src, double *dst, int NJ, int nrows, in
 cudaError_t launch_unblock_c(const double2 *src, double2 *dst, int NJ, int nrows, int n8, cudaStream_t st) {
     const int nb = grid_for((long long)nrows * n8, 256);
     k_unblock_c<<<nb, 256, 0, st>>>(src, dst, NJ, nrows, n8);
+    return launched();
+}
+
+cudaError_t launch_block(const double *src, double *dst, int NJ, int nrows, int n8, cudaStream_t st) {
+    const int nb = grid_for((long long)nrows * n8, 256);
+    k_block<<<nb, 256, 0, st>>>(src, dst, NJ, nrows, n8);
+    return launched();
+}
+
+cudaError_t launch_block_c(const double2 *src, double2 *dst, int NJ, int nrows, int n8, cudaStream_t st) {
+    const int nb = grid_for((long long)nrows * n8, 256);
+    k_block_c<<<nb, 256, 0, st>>>(src, dst, NJ, nrows, n8);
+    return launched();
+}
+
+cudaError_t launch_take_row(const double *src, int NJ, int j, int n8, double *dst, cudaStream_t st) {
+    k_take_row<<<grid_for(n8, 256), 256, 0, st>>>(src, NJ, j, n8, dst);
     return launched();
 }
 

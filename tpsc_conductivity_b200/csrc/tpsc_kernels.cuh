@@ -231,6 +231,11 @@ cudaError_t launch_pade_batch(const double2 *x, const double2 *y, int nf, int Nn
 // blocked (NJ rows) -> reference layout [j][o], j < nrows
 cudaError_t launch_unblock(const double *src, double *dst, int NJ, int nrows, int n8, cudaStream_t st);
 cudaError_t launch_unblock_c(const double2 *src, double2 *dst, int NJ, int nrows, int n8, cudaStream_t st);
+// row j of a blocked (NJ rows) array -> dst[o], o < n8
+cudaError_t launch_take_row(const double *src, int NJ, int j, int n8, double *dst, cudaStream_t st);
+// reference layout [j][o], j < nrows -> blocked (NJ rows): the setters
+cudaError_t launch_block(const double *src, double *dst, int NJ, int nrows, int n8, cudaStream_t st);
+cudaError_t launch_block_c(const double2 *src, double2 *dst, int NJ, int nrows, int n8, cudaStream_t st);
 
 // ---- gathers done by the SMs instead of a copy engine -----------------------
 // Up to kGatherPieces ranges of 4-byte words, each copied to a word offset of

@@ -1,0 +1,57 @@
+// files_main.cpp -- the saved-run formats through the drop-in classes.
+//
+//   files_main_b200 save|load U tp tpp t3 n T nk0 Nw0
+//
+// save: the model is solved as src/tpsc_main.cpp solves it
+// (calc_Self_FFT_spline, traceSelfG, find_mu), then written with the
+// reference's writers chi0::save_chi, green::save_Self(0), green::save_Self_bin
+// and green::save_Green({2, 1}); a second object of the same model then loads
+// the self_bin file back (green::load_Self_bin) and finds mu again.
+// load: only that second part, on a self_bin file already in the directory
+// (for instance one the reference wrote).
+// Prints "mu <value>" per find_mu, 17 significant digits.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "cond_opt.h"
+
+// reaches the protected loader and binary writer, as a program deriving from
+// green would
+class files_green : public green {
+public:
+    files_green(int nk0, int Nw0, double n, double T, double eta, double *p) : green(nk0, Nw0, n, T, eta, p) {}
+    void warm_start() { load_Self_bin(); }
+    void save_bin() { save_Self_bin(); }
+};
+
+int main(int argc, char **argv) {
+    if (argc != 10 || (strcmp(argv[1], "save") && strcmp(argv[1], "load"))) {
+        fprintf(stderr, "usage: %s save|load U tp tpp t3 n T nk0 Nw0\n", argv[0]);
+        return 1;
+    }
+    const bool save = !strcmp(argv[1], "save");
+    double params[] = {atof(argv[3]), atof(argv[4]), atof(argv[5]), atof(argv[2])};
+    const double n = atof(argv[6]), T = atof(argv[7]);
+    const int nk0 = atoi(argv[8]), Nw0 = atoi(argv[9]);
+    if (save) {
+        files_green g(nk0, Nw0, n, T, 0.1, params);
+        g.set_keep_chiqw(true);
+        g.calc_Self_FFT_spline();
+        g.traceSelfG();
+        g.find_mu();
+        printf("mu %.17g\n", g.get_mu());
+        g.save_chi();
+        g.save_Self(0);
+        g.save_bin();
+        int k[2] = {2, 1};
+        g.save_Green(k);
+    }
+    // warm start: the tails come from this object's own Sigma stage, S from the file
+    files_green h(nk0, Nw0, n, T, 0.1, params);
+    h.calc_Self_FFT_spline();
+    h.warm_start();
+    h.find_mu();
+    printf("mu %.17g\n", h.get_mu());
+    return 0;
+}

@@ -136,6 +136,44 @@ void chi0::traceChi0() {
          << "\tdifference relative:  " << (ex - tr[1]) / ex << '\n';
 }
 
+// chi0::save_chi (src/chi0.cpp:61-95): the chi0 binary of the current grid
+void chi0::save_chi() {
+    if (!ctx_) return;
+    const size_t n8 = (size_t)nbq * (nbq + 1) / 2;
+    std::vector<double> chi(n8 * (size_t)(nwmax + 1));
+    if (!check(tpsc_get_chi0(ctx_, chi.data(), NULL, NULL, NULL), "save_chi")) return;
+    char name[200];
+    tpsc_file_name(TPSC_FILE_CHI0_BIN, name, sizeof name, U, tp, tpp, t3, density, tem, 2 * (nbq - 1), 2 * nwmax,
+                   0, 0);
+    if (tpsc_write_chi0_bin(name, nbq, nwmax, chi.data()) != TPSC_OK) std::cout << "Error in chi0::save_chi" << std::endl;
+}
+
+// chi0::loadChi0 (src/chi0.cpp:99-154): the chi0 binary of this grid's name
+// back into the device, chi0max and qmax found again
+void chi0::loadChi0() {
+    char name[200];
+    tpsc_file_name(TPSC_FILE_CHI0_BIN, name, sizeof name, U, tp, tpp, t3, density, tem, 2 * (nbq - 1), 2 * nwmax,
+                   0, 0);
+    int fq = 0, fw = 0;
+    if (tpsc_read_chi0_bin(name, &fq, &fw, NULL, 0) != TPSC_OK) {
+        cout << "chi0::loadChi0():  fichier  " << name << "   inexistant \n";
+        return;
+    }
+    if (fq != nbq || fw != nwmax) {
+        cout << "chi0::loadChi0(): " << name << " holds nbq " << fq << ", nwmax " << fw << ", not this grid's\n";
+        return;
+    }
+    std::vector<double> chi((size_t)fq * (fq + 1) / 2 * (size_t)(fw + 1));
+    if (!check(tpsc_read_chi0_bin(name, &fq, &fw, chi.data(), (long long)chi.size()), "loadChi0")) return;
+    if (!ctx_ || !check(tpsc_set_chi0(ctx_, chi.data()), "loadChi0")) return;
+    refresh();
+    chi0max = scal_[TPSC_S_CHI0MAX];
+    qmax[0] = (int)scal_[TPSC_S_QMAX0];
+    qmax[1] = (int)scal_[TPSC_S_QMAX1];
+    cout << "chi0 charge,  nbq: " << nbq << "  nwmax: " << nwmax << '\n';
+    cout << "qmax: " << qmax[0] << "  " << qmax[1] << "  chi0max: " << chi0max << '\n';
+}
+
 // ---------------------------------------------------------------------------
 chi::chi(int nk0, int Nw0, double n, double T, double *params) : chi0(nk0, Nw0, n, T, params) {
     nsr = n > 1.0 ? 2.0 - n : n;
@@ -528,6 +566,99 @@ void green::save_self_ikn(int *k_save, int nk_save, int Nwn) {
         }
     }
     file.close();
+}
+
+// green::save_Self (src/green.cpp:1544-1574): ascii, Nfreq frequencies
+void green::save_Self(int Nfreq) {
+    if (!have_self) {
+        cout << "save_Self(): Self_kw_array n'existe pas\n";
+        return;
+    }
+    const size_t n8 = (size_t)nbk * (nbk + 1) / 2;
+    std::vector<double> S((size_t)2 * n8 * (nbw / 2));
+    if (!check(tpsc_get_self(ctx_, S.data(), NULL, NULL, NULL), "save_Self")) return;
+    char name[200];
+    tpsc_file_name(TPSC_FILE_SELF_ASCII, name, sizeof name, U, tp, tpp, t3, density, tem, 2 * (nbk - 1), nbw, 0, 0);
+    check(tpsc_write_self_ascii(name, nbk, nbw, Nfreq, S.data()), "save_Self");
+}
+
+// green::save_Self_bin (src/green.cpp:1496-1515): S, then the frame the
+// reference's Sigma stage leaves after it, (Sigma(k, beta/2), 0)
+void green::save_Self_bin() {
+    if (!have_self) {
+        cout << "Self_kw_array n'existe pas\n";
+        return;
+    }
+    const size_t n8 = (size_t)nbk * (nbk + 1) / 2;
+    std::vector<double> S((size_t)2 * n8 * (nbw / 2)), mid(n8), last(2 * n8, 0.0);
+    if (!check(tpsc_get_self(ctx_, S.data(), NULL, NULL, NULL), "save_Self_bin")) return;
+    if (!check(tpsc_get_sigma_tau(ctx_, nbw / 2, mid.data()), "save_Self_bin")) return;
+    for (size_t o = 0; o < n8; ++o) last[2 * o] = mid[o];
+    char name[200];
+    tpsc_file_name(TPSC_FILE_SELF_BIN, name, sizeof name, U, tp, tpp, t3, density, tem, 2 * (nbk - 1), nbw, 0, 0);
+    check(tpsc_write_self_bin(name, nbk, nbw, S.data(), last.data()), "save_Self_bin");
+}
+
+// green::load_Self_bin (src/green.cpp:1517-1541): S from this model's
+// self_bin file; the tails stay as they are
+void green::load_Self_bin() {
+    const size_t n8 = (size_t)nbk * (nbk + 1) / 2;
+    std::vector<double> S((size_t)2 * n8 * (nbw / 2 + 1));
+    char name[200];
+    tpsc_file_name(TPSC_FILE_SELF_BIN, name, sizeof name, U, tp, tpp, t3, density, tem, 2 * (nbk - 1), nbw, 0, 0);
+    if (tpsc_read_self_bin(name, nbk, nbw, S.data()) != TPSC_OK) {
+        cout << "fichier  " << name << "  inexistant\n";
+        return;
+    }
+    if (ctx_ && check(tpsc_set_self(ctx_, S.data(), NULL, NULL, NULL, NULL), "load_Self_bin")) have_self = true;
+}
+
+// green::load_Self (src/green.cpp:1637-1670): S from this model's self_tpsc
+// ascii file; the tails stay as they are
+void green::load_Self() {
+    const size_t n8 = (size_t)nbk * (nbk + 1) / 2;
+    std::vector<double> S((size_t)2 * n8 * (nbw / 2));
+    char name[200];
+    tpsc_file_name(TPSC_FILE_SELF_ASCII, name, sizeof name, U, tp, tpp, t3, density, tem, 2 * (nbk - 1), nbw, 0, 0);
+    if (tpsc_read_self_ascii(name, nbk, nbw, S.data()) != TPSC_OK) {
+        cout << "load_Self():  fichier  " << name << "  inexistant\n";
+        return;
+    }
+    if (ctx_ && check(tpsc_set_self(ctx_, S.data(), NULL, NULL, NULL, NULL), "load_Self")) have_self = true;
+}
+
+// green::save_Green (src/green.cpp:1577-1633): G(k, i w_n) at one k, the
+// lattice point folded into the octant, eps_k - mu with the current mu
+void green::save_Green(int *k) {
+    if (!have_self) {
+        cout << "save_Green(): Self_kw_array n'existe pas\n";
+        return;
+    }
+    const int nk0 = 2 * (nbk - 1);
+    long l = k[0] < 0 ? -k[0] : k[0], m = k[1] < 0 ? -k[1] : k[1];
+    if (l > nk0 || m > nk0) {
+        cout << "save_Green(): k[0] et k[1] doivent etre entre 0 et nk0\n";
+        return;
+    }
+    if (l > nbk - 1) l = nk0 - l;
+    if (m > nbk - 1) m = nk0 - m;
+    if (m > l) std::swap(l, m);
+    // hamiltonien::ek_val (src/hamiltonien.cpp:107-116) on the unfolded k
+    auto fold = [&](int x) {
+        while (x < 0) x += nk0;
+        return x > nbk - 1 ? nk0 - x : x;
+    };
+    std::vector<double> ek((size_t)nbk * nbk);
+    const size_t n8 = (size_t)nbk * (nbk + 1) / 2;
+    std::vector<double> S((size_t)2 * n8 * (nbw / 2)), c2(n8), c3(n8);
+    if (!check(tpsc_get_ek(ctx_, ek.data()), "save_Green")) return;
+    if (!check(tpsc_get_self(ctx_, S.data(), c2.data(), c3.data(), NULL), "save_Green")) return;
+    const double ek_mu = ek[fold(k[1]) + (size_t)fold(k[0]) * nbk] - mu;
+    const size_t o = m + (l * (l + 1)) / 2;
+    char name[200];
+    tpsc_file_name(TPSC_FILE_GREEN, name, sizeof name, U, tp, tpp, t3, density, tem, nk0, nbw, (int)l, (int)m);
+    check(tpsc_write_green_ascii(name, nbw, tem, ek_mu, Sigma_inf, c2[o], c3[o], S.data() + 2 * o, (long long)n8),
+          "save_Green");
 }
 
 // ---------------------------------------------------------------------------

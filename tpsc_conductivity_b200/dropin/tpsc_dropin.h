@@ -81,8 +81,10 @@ public:
     void set_save_chi0_to_file(bool v) { save_chi0_to_file = v; }
     void calc_chiqw_FFT_spline(int nq0, int nw0);
     void traceChi0();
+    void save_chi();
 
 protected:
+    void loadChi0();
     bool keep_chirt, keep_chiqw, save_chi0_q, save_chi0_to_file;
     double chi0max;
     int qmax[2];
@@ -119,8 +121,13 @@ public:
     void MDC(int *n, int Nn, double w, double *eta, int Neta, bool use_Pade = false);
     void Gwn_local();
     void save_self_ikn(int *k_save, int nk_save, int Nwn);
+    void save_Green(int *k);
+    void save_Self(int Nfreq);
 
 protected:
+    void load_Self();
+    void save_Self_bin();
+    void load_Self_bin();
     double eta, mu, Sigma_inf;
     bool mu_calcule, have_self;
 };
