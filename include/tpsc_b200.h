@@ -99,6 +99,13 @@ int tpsc_set_model(tpsc_ctx *ctx, int nk0, int Nw0, double n, double T, double t
  * TPSC_FORM_REFERENCE. */
 int tpsc_set_form(tpsc_ctx *ctx, int form);
 
+/* The sum rules' nsr (src/chi.cpp:18-19: n, or 2 - n for n > 1), which
+ * tpsc_set_model derives from the density; this value holds instead until the
+ * next tpsc_set_model.  The reference sets nsr once, in the chi constructor,
+ * so a chi object whose density changes (set_density, chi::calc_corr_length
+ * src/chi.cpp:931-981) keeps its constructor's nsr. */
+int tpsc_set_nsr(tpsc_ctx *ctx, double nsr);
+
 /* CUDA graphs for Newton-form solves (no counterpart in the reference, whose
  * solve runs on the host).  A Newton-form tpsc_solve queues its launches with
  * no host round trip, so the whole solve from the chi0 stage to the final
@@ -158,6 +165,11 @@ int tpsc_set_mu_shift(tpsc_ctx *ctx, double dmu);
  * out = {vF, xi_y, xi_x, xiAs_y, xiAs_x, xi0_y, xi0_x} -- half-maximum
  * lengths along y and x, asymptotic (Ornstein-Zernike) lengths, and xi0. */
 int tpsc_sp_corr_length(tpsc_ctx *ctx, double out[7]);
+/* The same with the Fermi surface (and so vF and xi0) of mu_fs instead of the
+ * current mu0: the reference computes its Fermi surface once, in the green0
+ * constructor (src/green0.cpp:35), so after set_density / set_tem
+ * (chi::calc_corr_length, src/chi.cpp:931-981) it keeps the constructor's. */
+int tpsc_sp_corr_length_fs(tpsc_ctx *ctx, double mu_fs, double out[7]);
 
 /* chi::calc_chirt (src/chi.cpp:37-170): V(r, tau) on tau in [0, beta/2]. */
 int tpsc_vertex(tpsc_ctx *ctx);

@@ -18,6 +18,9 @@
  *        post   solve + find_FS_inter, MDC(10 points, w=0, 4 etas), Gwn_local
  *               (src/tpsc_main.cpp:77-114)
  *        bench  timings only: the half-grid pre-pass alone, then the solve
+ *        corr   chi::calc_corr_length({n, n + 0.05}, 2, {T, 1.5 T}, 2)
+ *               (src/chi.cpp:931-981): the (n, T) scan of Usp, Uch and the
+ *               correlation lengths; the reference writes its corrLgth file
  *        files  solve, then the reference's own writers of the saved-run
  *               formats: chi0::save_chi, green::save_Self(0),
  *               green::save_Self_bin, green::save_Green({2, 1})
@@ -144,6 +147,11 @@ int main(int argc, char **argv) {
         g->calc_chiqw_FFT_spline(nk0, Nw0);
         fprintf(meta, "t_chi0 %.6f\n", omp_get_wtime() - t0);
         g->dump_chi0(meta, absdir);
+    } else if (mode == "corr") {
+        double dens[2] = {n, n + 0.05}, temp[2] = {T, 1.5 * T};
+        t0 = omp_get_wtime();
+        g->calc_corr_length(dens, 2, temp, 2);
+        fprintf(meta, "t_corr %.6f\n", omp_get_wtime() - t0);
     } else if (mode == "bench") {
         // timing only: the solve exactly as src/tpsc_main.cpp:71-75 runs it, then
         // the half-grid Usp/Uch pass that calc_Self_FFT_spline runs first

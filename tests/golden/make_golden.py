@@ -46,11 +46,14 @@ CASES = {
     # as the reference's own writers leave them, byte for byte, on a 16x16
     # lattice with 16 positive iwn
     "files_l16_w32": ("files", 2.0, -0.1, 0.0, 0.0, 0.875, 0.25, 16, 32, True),
+    # chi::calc_corr_length over n in {0.85, 0.9}, T in {0.2, 0.3} on a 16x16
+    # lattice with 32 positive iwn: the reference's corrLgth file
+    "corr_l16_w64": ("corr", 2.5, -0.1, 0.0, 0.0, 0.85, 0.2, 16, 64, True),
 }
 
 # the files the reference's writers leave (src/chi0.cpp:63, src/green.cpp:1507,
 # 1557, 1606); chi0_qmax_wn_* and chi0_wn0_q_* are the chi0 stage's own dumps
-FILE_PREFIXES = ("chi0_", "self_bin_", "self_tpsc_", "Green_")
+FILE_PREFIXES = ("chi0_", "self_bin_", "self_tpsc_", "Green_", "corrLgth_")
 FILE_SKIP = ("chi0_qmax_wn_", "chi0_wn0_q_")
 
 
@@ -73,6 +76,17 @@ def run_case(name, spec, threads):
         subprocess.run(args, check=True, env=env)
         meta = read_meta(os.path.join(d, "meta.txt"))
         nbk = nk0 // 2 + 1
+        if mode == "corr":
+            work = os.path.join(d, "work")
+            names = sorted(f for f in os.listdir(work) if f.startswith("corrLgth_"))
+            out = {"params": np.array([U, tp, tpp, t3, n, T, nk0, Nw0], dtype=np.float64),
+                   "dens": np.array([n, n + 0.05]), "temp": np.array([T, 1.5 * T]),
+                   "file_names": np.array(names)}
+            for i, f in enumerate(names):
+                out[f"file_{i}"] = np.fromfile(os.path.join(work, f), dtype=np.uint8)
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+            print(name, "done", names)
+            return
         n8 = nbk * (nbk + 1) // 2
         nw = Nw0 // 2 + 1
 

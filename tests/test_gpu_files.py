@@ -121,3 +121,29 @@ def test_abi_warm_start_from_the_references_arrays():
     assert np.array_equal(gr.chi0()["chiqw"], chi)
     # a NULL Sigma is refused
     assert lib.tpsc_set_self(h, None, None, None, None, None) == _lib.ERR_ARG
+
+
+@pytest.mark.skipif(not os.path.exists(BIN), reason="files_main_b200 is built by make -C tpsc_conductivity_b200/dropin")
+def test_dropin_corr_length_scan_writes_the_reference_file(tmp_path):
+    """chi::calc_corr_length over n in {0.85, 0.9}, T in {0.2, 0.3}: the same
+    corrLgth file as the reference's (corr_l16_w64 fixture) -- vF from the
+    constructor's Fermi surface on every line, errUs = errUc = 0 as the
+    reference leaves them, the integer columns exact, the rest to 1e-8."""
+    g = load_golden("corr_l16_w64")
+    name = str(g["file_names"][0])
+    want = bytes(g["file_0"]).decode().splitlines()
+    U, tp, tpp, t3, n, T, nk0, Nw0 = g["params"]
+    args = [repr(float(x)) for x in (U, tp, tpp, t3, n, T)] + [str(int(nk0)), str(int(Nw0))]
+    r = subprocess.run([BIN, "corr"] + args, cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    have = (tmp_path / name).read_text().splitlines()
+    assert len(have) == len(want) == 4
+    for x, y in zip(have, want):
+        assert [m.start() for m in re.finditer(r"\S+", x)] == [m.start() for m in re.finditer(r"\S+", y)]
+    a, b = np.loadtxt(have, ndmin=2), np.loadtxt(want, ndmin=2)
+    ints = [15, 16, 17]
+    assert np.array_equal(a[:, ints], b[:, ints])
+    assert not a[:, [5, 7]].any()
+    assert len(set(a[:, 3])) == 1
+    fl = [c for c in range(a.shape[1]) if c not in ints]
+    assert np.allclose(a[:, fl], b[:, fl], rtol=1e-8, atol=1e-12)

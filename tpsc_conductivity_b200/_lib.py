@@ -27,6 +27,7 @@ SIGNATURES = [
     ("tpsc_find_Usp_Uch_grid", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),
     ("tpsc_find_Usp_Uch", C.c_int, [C.c_void_p]),
     ("tpsc_sp_corr_length", C.c_int, [C.c_void_p, _dp]),
+    ("tpsc_sp_corr_length_fs", C.c_int, [C.c_void_p, C.c_double, _dp]),
     ("tpsc_sumrule_tangents", C.c_int, [C.c_void_p, _dp]),
     ("tpsc_get_self_async", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     ("tpsc_set_self", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),
@@ -74,6 +75,7 @@ SIGNATURES = [
     ("tpsc_gwn_local", C.c_int, [C.c_void_p, _dp]),
     ("tpsc_set_form", C.c_int, [C.c_void_p, C.c_int]),
     ("tpsc_set_graph_mode", C.c_int, [C.c_void_p, C.c_int]),
+    ("tpsc_set_nsr", C.c_int, [C.c_void_p, C.c_double]),
     ("tpsc_graph_stats", C.c_int, [C.c_void_p, C.c_void_p]),
     ("tpsc_chijj", C.c_int, [C.c_void_p, C.c_int]),
     ("tpsc_get_chijj", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),

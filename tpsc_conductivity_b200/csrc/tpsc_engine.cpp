@@ -275,11 +275,11 @@ bool newton_root(F &&func, double x0, double lo, double hi, double tol, double *
 struct SolveKey {
     int form = -1, cap = -1;
     long long model_id = -1;
-    double mu0 = 0.0;
+    double mu0 = 0.0, nsr = -1.0;
     bool rsr = true, rmu = true;
     bool operator==(const SolveKey &o) const {
-        return form == o.form && cap == o.cap && model_id == o.model_id && mu0 == o.mu0 && rsr == o.rsr &&
-               rmu == o.rmu;
+        return form == o.form && cap == o.cap && model_id == o.model_id && mu0 == o.mu0 && nsr == o.nsr &&
+               rsr == o.rsr && rmu == o.rmu;
     }
 };
 
@@ -1212,6 +1212,7 @@ int newton_solve(tpsc_ctx *ctx) {
     key.cap = ctx->roots.max_blocks;
     key.model_id = ctx->model_id;
     key.mu0 = g->mu0;
+    key.nsr = ctx->nsr;
     key.rsr = ctx->roots.reset_sr;
     key.rmu = ctx->roots.reset_mu;
     const unsigned fbit = 1u << (ctx->form & 3);
@@ -1596,6 +1597,19 @@ int tpsc_find_Usp_Uch_grid(tpsc_ctx *ctx, int nq0, int nw0, double Usc[2]) {
 // forward tangents of chi0 -> sum rules -> Usp, Uch, D
 // ---------------------------------------------------------------------------
 
+// the nsr of the sum rules (chi::nsr, src/chi.cpp:18-19): n or 2 - n from
+// the density of tpsc_set_model, or this value until the next tpsc_set_model
+// (the reference sets it once, in the chi constructor)
+int tpsc_set_nsr(tpsc_ctx *ctx, double nsr) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    if (!(nsr > 0.0 && nsr <= 1.0)) return fail(ctx, TPSC_ERR_ARG, "need 0 < nsr <= 1");
+    if (nsr != ctx->nsr)
+        for (auto &kv : ctx->grids) kv.second->have_U = kv.second->have_V = kv.second->have_S = false;
+    ctx->nsr = nsr;
+    return TPSC_OK;
+}
+
 int tpsc_set_mu_shift(tpsc_ctx *ctx, double dmu) {
     if (!ctx || !std::isfinite(dmu)) return fail(ctx, TPSC_ERR_ARG, "bad mu shift");
     if (dmu != ctx->mu_shift) {
@@ -1779,6 +1793,12 @@ double vf_hot_spots(const tpsc_ctx *ctx, const std::vector<double> &fs, int nk) 
 int tpsc_sp_corr_length(tpsc_ctx *ctx, double out[7]) {
     int rc = need_model(ctx);
     if (rc) return rc;
+    return tpsc_sp_corr_length_fs(ctx, ctx->cur->mu0, out);
+}
+
+int tpsc_sp_corr_length_fs(tpsc_ctx *ctx, double mu_fs, double out[7]) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
     if (!out) return fail(ctx, TPSC_ERR_ARG, "null output");
     Grid *g = ctx->cur;
     if (!g || !g->have_chi0 || !g->have_U)
@@ -1793,7 +1813,7 @@ int tpsc_sp_corr_length(tpsc_ctx *ctx, double out[7]) {
     CK(cudaStreamSynchronize(ctx->st));
     const int nkfs = 10001;
     std::vector<double> fs;
-    find_fs(ctx, g->mu0, nkfs, fs);
+    find_fs(ctx, mu_fs, nkfs, fs);
     const double vF = vf_hot_spots(ctx, fs, nkfs);
     // chi::sp_corr_length (src/chi.cpp:450-718): half maximum of
     // chi_sp(q, 0) = chi0/(1 - Usp chi0/2) around qmax along y and x, and the

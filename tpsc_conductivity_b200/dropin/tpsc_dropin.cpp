@@ -58,6 +58,26 @@ green0::green0(int nk0, int Nw0, double n, double T, double params[]) : hamilton
         mu0 = scal_[TPSC_S_MU0];
         cout << "mu0 du systeme fini: " << mu0 << endl;
     }
+    mu0_fs_ = mu0;
+}
+
+// the model of the current members on the current grid; mu0 again
+void green0::set_model() {
+    if (!ctx_ || !check(tpsc_set_model(ctx_, 2 * (nbk - 1), nbw, density, tem, tp, tpp, t3, U), "tpsc_set_model"))
+        return;
+    refresh();
+    mu0 = scal_[TPSC_S_MU0];
+    model_changed();
+}
+
+void green0::set_tem(double T) {
+    tem = T;
+    set_model();
+}
+
+void green0::set_density(double n) {
+    density = n;
+    set_model();
 }
 
 green0::~green0() {
@@ -178,6 +198,7 @@ void chi0::loadChi0() {
 chi::chi(int nk0, int Nw0, double n, double T, double *params) : chi0(nk0, Nw0, n, T, params) {
     nsr = n > 1.0 ? 2.0 - n : n;
     Usp = Uch = dblOcc = 0.0;
+    errUs = errUc = 0.0;
     paramsFileName[0] = 0;
 }
 
@@ -282,7 +303,8 @@ void chi::find_Usp_Uch() {
 void chi::sp_corr_length() {
     if (!ctx_) return;
     double r[7];
-    if (!check(tpsc_sp_corr_length(ctx_, r), "sp_corr_length")) return;
+    // the Fermi surface of the constructor's mu0, as the reference keeps it
+    if (!check(tpsc_sp_corr_length_fs(ctx_, mu0_fs_, r), "sp_corr_length")) return;
     vF = r[0];
     spCorrLgth_y = r[1];
     spCorrLgth_x = r[2];
@@ -320,6 +342,39 @@ void chi::sp_corr_length() {
     const double chisp_max = chi0max / (1.0 - Usp * chi0max / 2.0);
     cout << "(max(chi_sp)/max(chi_0))^0.5:  " << sqrt(chisp_max / chi0max) << endl;
     infos.close();
+}
+
+// the reference's chi computes nsr once, in its constructor (src/chi.cpp:18-19)
+void chi::model_changed() { check(tpsc_set_nsr(ctx_, nsr), "set_density"); }
+
+// chi::calc_corr_length (src/chi.cpp:931-981): Usp, Uch and the spin
+// correlation lengths on the (n, T) grid dens[0]..dens[1] (nD points) x
+// Temp[0]..Temp[1] (nT points), one line per point in the corrLgth file
+void chi::calc_corr_length(double dens[], int nD, double Temp[], int nT) {
+    const double T0 = Temp[0], Tf = Temp[1], dT = (Tf - T0) / (nT - 1);
+    const double n0 = dens[0], nf = dens[1], dn = (nf - n0) / (nD - 1);
+    char name[100];
+    sprintf(name, "./corrLgth_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%7.5f_%6.4f_%6.4f.dat", U, tp, tpp, t3, n0, nf, T0, Tf);
+    fstream file;
+    file.open(name, ios::out);
+    file << setiosflags(ios::left) << setprecision(15);
+    for (int l = 0; l < nD; l++) {
+        set_density(n0 + l * dn);
+        for (int j = 0; j < nT; j++) {
+            set_tem(T0 + j * dT);
+            find_Usp_Uch();
+            sp_corr_length();
+            file << setw(25) << density << setw(25) << tem << setw(25) << mu0;
+            file << setw(25) << vF << setw(25) << Usp << setw(25) << errUs;
+            file << setw(25) << Uch << setw(25) << errUc << setw(25) << dblOcc;
+            file << setw(25) << spCorrLgth_x << setw(25) << spCorrLgth_y;
+            file << setw(25) << spCorrLgthAs_x << setw(25) << spCorrLgthAs_y;
+            file << setw(25) << xi0_x << setw(25) << xi0_y << setw(25) << nbq;
+            file << setw(25) << qmax[0] << setw(25) << qmax[1];
+            file << chi0max << '\n';
+        }
+    }
+    file.close();
 }
 
 void chi::calc_chirt() {

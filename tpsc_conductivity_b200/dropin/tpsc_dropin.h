@@ -61,11 +61,17 @@ public:
     virtual ~green0();
     void get_params() const;
     double get_mu() const { return mu0; }
+    // hamiltonien::set_tem / set_density, then mu0 again (src/green0.h:35-38)
+    void set_tem(double T);
+    void set_density(double n);
 
 protected:
     bool check(int status, const char *what) const;
+    void set_model();
+    virtual void model_changed() {}  // after set_model: the derived classes' own model state
     tpsc_ctx *ctx_;
     double mu0;
+    double mu0_fs_;  // mu0 of the constructor: the Fermi surface's (src/green0.cpp:35)
     int nbw, nwmax;
     double scal_[TPSC_S_COUNT];
     void refresh();
@@ -99,10 +105,13 @@ public:
     void find_Usp_Uch();
     void find_Usp_Uch(int nq0, int nw0, double Usc[]);
     void sp_corr_length();
+    void calc_corr_length(double dens[], int nD, double Temp[], int nT);
 
 protected:
     void calc_chirt();
+    void model_changed() override;  // keeps the constructor's nsr, as the reference does
     double Uch, Usp, dblOcc, nsr;
+    double errUs, errUc;  // never assigned by the reference's find_Usp_Uch (src/chi.cpp:361-362 are commented out)
     double spCorrLgth_x, spCorrLgth_y, spCorrLgthAs_x, spCorrLgthAs_y, xi0_x, xi0_y, vF;
     char paramsFileName[200];
 };
