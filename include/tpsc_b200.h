@@ -368,6 +368,22 @@ int tpsc_batch_tune(tpsc_batch *b, int form, int npts, const double *params, int
  * {32, 64, 128, 256}, U ~ U[1, 6], n ~ U[0.7, 1], log T ~ U[ln 0.03, ln 0.5],
  * t' ~ U[-0.3, 0]; t'' = t3 = 0 and Nw0 = 2 nextpow2(ceil(40 / (pi T))). */
 int tpsc_sweep_points(int npts, unsigned long long seed, double *params);
+/* chi::calc_corr_length (src/chi.cpp:931-981) on the batch's contexts: the
+ * (n, T) grid dens[0]..dens[1] (nD points) x Temp[0]..Temp[1] (nT points),
+ * point i = l nT + j at n = dens[0] + l dn, T = Temp[0] + j dT; per point the
+ * two-grid find_Usp_Uch and sp_corr_length.  rows: nD nT rows of 19 values in
+ * the corrLgth line's order {n, T, mu0, vF, Usp, difRelsp, Uch, difRelch,
+ * dblOcc, xi_x, xi_y, xiAs_x, xiAs_y, xi0_x, xi0_y, nbq, qmax0, qmax1,
+ * chi0max} -- the reference prints 0 in the two error columns (their
+ * assignment is commented out, src/chi.cpp:361-362); here they are the
+ * half-to-full-grid differences.  nsr > 0 fixes the sum rules' nsr for every
+ * point (0: each point's own), mu_fs the Fermi surface's mu (NaN: each
+ * point's mu0); the reference's own scan keeps both from its constructor.
+ * A failing point has status != 0 and a row of NaN; returns the first
+ * failure's status. */
+int tpsc_batch_corr_length(tpsc_batch *b, int form, int nk0, int Nw0, double tp, double tpp, double t3, double U,
+                           const double *dens, int nD, const double *Temp, int nT, double nsr, double mu_fs,
+                           double *rows, int *status, double *ms);
 
 /* ---- warm start from saved results ---------------------------------------
  * tpsc_set_self <- green::load_Self_bin / load_Self (src/green.cpp:1517-1541,

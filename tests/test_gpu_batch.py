@@ -111,3 +111,26 @@ def test_batch_as_graph_launches_equals_direct_launches(form_name):
         assert np.array_equal(st, st0)
         ok = st0 == 0
         assert np.array_equal(res[ok], ref[ok])
+
+
+def test_batch_corr_length_scan_equals_the_references_file():
+    """tpsc_batch_corr_length with the reference's own semantics (the
+    constructor's nsr and Fermi surface for every point) reproduces the
+    reference's corrLgth file (corr_l16_w64) to 1e-8; with each point's own
+    nsr, the n = 0.9 points move."""
+    from tpsc_conductivity_b200.api import Batch
+
+    g = load_golden("corr_l16_w64")
+    ref = np.loadtxt(bytes(g["file_0"]).decode().splitlines(), ndmin=2)
+    U, tp, tpp, t3, n, T, nk0, Nw0 = g["params"]
+    nsr = n if n <= 1.0 else 2.0 - n
+    b = Batch(nstreams=2)
+    rows, st, ms = b.corr_length(int(nk0), int(Nw0), (tp, tpp, t3, U), g["dens"], 2, g["temp"], 2, nsr=nsr,
+                                 mu_fs=ref[0, 2])
+    assert not st.any() and ms > 0
+    cols = [c for c in range(len(Batch.CORR_COLUMNS)) if c not in (5, 7)]
+    assert np.allclose(rows[:, cols], ref[:, cols], rtol=1e-8, atol=1e-12)
+    assert np.all(rows[:, [5, 7]] >= 0)
+    own, st2, _ = b.corr_length(int(nk0), int(Nw0), (tp, tpp, t3, U), g["dens"], 2, g["temp"], 2)
+    assert not st2.any()
+    assert np.allclose(own[:2, 4], rows[:2, 4], rtol=1e-12) and np.all(np.abs(own[2:, 4] - rows[2:, 4]) > 1e-6)

@@ -51,6 +51,9 @@ SIGNATURES = [
     ("tpsc_batch_last_error", C.c_char_p, [C.c_void_p]),
     ("tpsc_batch_streams", C.c_int, [C.c_void_p, _ip]),
     ("tpsc_batch_set_graph_mode", C.c_int, [C.c_void_p, C.c_int]),
+    ("tpsc_batch_corr_length", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                         C.c_double, _dp, C.c_int, _dp, C.c_int, C.c_double, C.c_double, _dp, _ip,
+                                         _dp]),
     ("tpsc_batch_solve", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, _dp, _ip, _dp]),
     ("tpsc_batch_tune", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, C.c_int, _dp]),
     ("tpsc_sweep_points", C.c_int, [C.c_int, C.c_ulonglong, _dp]),

@@ -387,6 +387,29 @@ class Batch:
             self._err(rc)
         return {2 ** i: float(ms[i]) for i in range(k)}
 
+    CORR_COLUMNS = ("n", "T", "mu0", "vF", "Usp", "difRelsp", "Uch", "difRelch", "dblOcc", "xi_x", "xi_y",
+                    "xiAs_x", "xiAs_y", "xi0_x", "xi0_y", "nbq", "qmax0", "qmax1", "chi0max")
+
+    def corr_length(self, nk0, Nw0, params, dens, nD, Temp, nT, nsr=0.0, mu_fs=float("nan"),
+                    form=_lib.FORM_REFERENCE):
+        """chi::calc_corr_length (src/chi.cpp:931-981) on the solver contexts:
+        rows [nD nT, 19] in CORR_COLUMNS order (density-major), per-point
+        status and the wall time (ms).  params = (tp, tpp, t3, U); nsr > 0
+        and mu_fs fix the sum rules' nsr and the Fermi surface's mu for every
+        point, as the reference's own scan keeps its constructor's."""
+        tp, tpp, t3, U = params
+        d = np.ascontiguousarray(dens, dtype=np.float64)
+        t = np.ascontiguousarray(Temp, dtype=np.float64)
+        rows = np.zeros((nD * nT, len(self.CORR_COLUMNS)))
+        st = np.zeros(nD * nT, dtype=np.int32)
+        ms = C.c_double()
+        rc = self.lib.tpsc_batch_corr_length(self.h, int(form), int(nk0), int(Nw0), tp, tpp, t3, U, _dptr(d),
+                                             int(nD), _dptr(t), int(nT), float(nsr), float(mu_fs), _dptr(rows),
+                                             st.ctypes.data_as(_lib._ip), C.byref(ms))
+        if rc and not st.any():
+            self._err(rc)
+        return rows, st, ms.value
+
     def set_graph_mode(self, mode):
         """tpsc_set_graph_mode of every solver context (2: each Newton-form
         point is one graph launch, updated in place per point)."""

@@ -40,6 +40,7 @@ namespace {
 
 constexpr int kParamCols = 8;  // nk0, Nw0, n, T, tp, tpp, t3, U
 constexpr int kMaxStreams = 32;
+constexpr int kCorrCols = 19;  // the columns of a corrLgth line
 
 // contexts 0..n-1 exist, with their root grids capped for n concurrent solvers
 int ensure_contexts(tpsc_batch *b, int n) {
@@ -60,21 +61,17 @@ int ensure_contexts(tpsc_batch *b, int n) {
     return TPSC_OK;
 }
 
-// the points of one call on n contexts; per-point status in status[]; the
-// wall time of the whole call (host clock around the device work) in *ms.
-// Returns a context-level failure only; *first_fail (if given) receives the
-// status of the first failing point, TPSC_OK if none.
-int run_points(tpsc_batch *b, int n, int form, int npts, const double *params, double *results, int *status,
-               double *ms, int *first_fail) {
+// Runs task(ctx, i) for every i < npts on contexts 0..n-1, one host thread
+// per context, in the given order (each point on the next free context);
+// per-point status in status[].  The wall time of the whole call (host clock
+// from a device-idle start to a device-idle end) in *ms.  *first_fail (if
+// given) receives the status of the first failing point in index order, and
+// b->err its message.  Returns a context-level failure only.
+template <class Task>
+int run_tasks(tpsc_batch *b, int n, int npts, const std::vector<int> &order, Task task, int *status, double *ms,
+              int *first_fail) {
     int rc = ensure_contexts(b, n);
     if (rc) return rc;
-    std::vector<int> order(npts);
-    for (int i = 0; i < npts; ++i) order[i] = i;
-    auto cost = [&](int i) {
-        const double *p = params + (size_t)i * kParamCols;
-        return p[0] * p[0] * p[1];
-    };
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
     std::atomic<int> next{0};
     std::mutex err_mu;
     std::string first_msg;
@@ -84,23 +81,11 @@ int run_points(tpsc_batch *b, int n, int form, int npts, const double *params, d
     auto worker = [&](int w) {
         cudaSetDevice(b->device);
         tpsc_ctx *c = b->ctxs[w];
-        tpsc_set_form(c, form);
         for (;;) {
             const int k = next.fetch_add(1);
             if (k >= npts) break;
             const int i = order[k];
-            const double *p = params + (size_t)i * kParamCols;
-            int r = TPSC_ERR_ARG;
-            if (p[0] == std::floor(p[0]) && p[1] == std::floor(p[1]))
-                r = tpsc_set_model(c, (int)p[0], (int)p[1], p[2], p[3], p[4], p[5], p[6], p[7]);
-            if (!r) r = tpsc_solve(c);
-            double *out = results + (size_t)i * TPSC_S_COUNT;
-            if (!r) r = tpsc_get_scalars(c, out, TPSC_S_COUNT);
-            if (r == TPSC_ERR_NONFINITE) {
-                tpsc_get_scalars(c, out, TPSC_S_COUNT);  // keep them: they show which one
-            } else if (r) {
-                for (int q = 0; q < TPSC_S_COUNT; ++q) out[q] = NAN;
-            }
+            const int r = task(c, i);
             if (r) {
                 std::lock_guard<std::mutex> lk(err_mu);
                 if (first_msg.empty()) first_msg = tpsc_last_error(c);
@@ -129,6 +114,35 @@ int run_points(tpsc_batch *b, int n, int form, int npts, const double *params, d
             break;
         }
     return TPSC_OK;
+}
+
+// the solves of one call on n contexts, largest first (nk0^2 Nw0)
+int run_points(tpsc_batch *b, int n, int form, int npts, const double *params, double *results, int *status,
+               double *ms, int *first_fail) {
+    std::vector<int> order(npts);
+    for (int i = 0; i < npts; ++i) order[i] = i;
+    auto cost = [&](int i) {
+        const double *p = params + (size_t)i * kParamCols;
+        return p[0] * p[0] * p[1];
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
+    auto task = [&](tpsc_ctx *c, int i) -> int {
+        tpsc_set_form(c, form);
+        const double *p = params + (size_t)i * kParamCols;
+        int r = TPSC_ERR_ARG;
+        if (p[0] == std::floor(p[0]) && p[1] == std::floor(p[1]))
+            r = tpsc_set_model(c, (int)p[0], (int)p[1], p[2], p[3], p[4], p[5], p[6], p[7]);
+        if (!r) r = tpsc_solve(c);
+        double *out = results + (size_t)i * TPSC_S_COUNT;
+        if (!r) r = tpsc_get_scalars(c, out, TPSC_S_COUNT);
+        if (r == TPSC_ERR_NONFINITE) {
+            tpsc_get_scalars(c, out, TPSC_S_COUNT);  // keep them: they show which one
+        } else if (r) {
+            for (int q = 0; q < TPSC_S_COUNT; ++q) out[q] = NAN;
+        }
+        return r;
+    };
+    return run_tasks(b, n, npts, order, task, status, ms, first_fail);
 }
 
 bool valid_args(tpsc_batch *b, int npts, const double *params, const double *results, const int *status) {
@@ -227,6 +241,46 @@ int tpsc_batch_tune(tpsc_batch *b, int form, int npts, const double *params, int
     }
     b->nstreams = best_n;
     return ensure_contexts(b, best_n);
+}
+
+int tpsc_batch_corr_length(tpsc_batch *b, int form, int nk0, int Nw0, double tp, double tpp, double t3, double U,
+                           const double *dens, int nD, const double *Temp, int nT, double nsr, double mu_fs,
+                           double *rows, int *status, double *ms) {
+    if (!b) return TPSC_ERR_ARG;
+    if (!dens || !Temp || nD < 1 || nT < 1 || !rows || !status) {
+        b->err = "bad arguments";
+        return TPSC_ERR_ARG;
+    }
+    // the grid of chi::calc_corr_length (src/chi.cpp:940-959), density-major
+    const double n0 = dens[0], dn = nD > 1 ? (dens[1] - n0) / (nD - 1) : 0.0;
+    const double T0 = Temp[0], dT = nT > 1 ? (Temp[1] - T0) / (nT - 1) : 0.0;
+    const int npts = nD * nT;
+    std::vector<int> order(npts);
+    for (int i = 0; i < npts; ++i) order[i] = i;
+    auto task = [&](tpsc_ctx *c, int i) -> int {
+        const int l = i / nT, j = i % nT;
+        const double n = n0 + l * dn, T = T0 + j * dT;
+        double *row = rows + (size_t)i * kCorrCols;
+        for (int q = 0; q < kCorrCols; ++q) row[q] = NAN;
+        int r = tpsc_set_form(c, form);
+        if (!r) r = tpsc_set_model(c, nk0, Nw0, n, T, tp, tpp, t3, U);
+        if (!r && nsr > 0.0) r = tpsc_set_nsr(c, nsr);
+        if (!r) r = tpsc_find_Usp_Uch(c);
+        double sc[TPSC_S_COUNT], xi[7];
+        if (!r) r = tpsc_get_scalars(c, sc, TPSC_S_COUNT);
+        if (!r) r = tpsc_sp_corr_length_fs(c, std::isnan(mu_fs) ? sc[TPSC_S_MU0] : mu_fs, xi);
+        if (r) return r;
+        // the columns of the reference's corrLgth line (src/chi.cpp:967-975)
+        const double v[kCorrCols] = {n, T, sc[TPSC_S_MU0], xi[0], sc[TPSC_S_USP], sc[TPSC_S_DIFRELSP],
+                                     sc[TPSC_S_UCH], sc[TPSC_S_DIFRELCH], sc[TPSC_S_DBLOCC], xi[2], xi[1], xi[4],
+                                     xi[3], xi[6], xi[5], (double)(nk0 / 2 + 1), sc[TPSC_S_QMAX0], sc[TPSC_S_QMAX1],
+                                     sc[TPSC_S_CHI0MAX]};
+        std::copy(v, v + kCorrCols, row);
+        return TPSC_OK;
+    };
+    int first = TPSC_OK;
+    const int rc = run_tasks(b, b->nstreams, npts, order, task, status, ms, &first);
+    return rc ? rc : first;
 }
 
 int tpsc_sweep_points(int npts, unsigned long long seed, double *params) {
