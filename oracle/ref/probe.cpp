@@ -21,6 +21,10 @@
  *        corr   chi::calc_corr_length({n, n + 0.05}, 2, {T, 1.5 T}, 2)
  *               (src/chi.cpp:931-981): the (n, T) scan of Usp, Uch and the
  *               correlation lengths; the reference writes its corrLgth file
+ *        rew    solve, then green::calc_Self_Re_w_BZ(n = 0..15, 16, w = -4..4
+ *               (9 points), 9, eta = {0.05, 0.01}, 2) (src/green.cpp:386-542):
+ *               Pade and J-fraction Sigma(k, w + i eta) and A(k, w) files for
+ *               every k of the reduced zone
  *        files  solve, then the reference's own writers of the saved-run
  *               formats: chi0::save_chi, green::save_Self(0),
  *               green::save_Self_bin, green::save_Green({2, 1})
@@ -173,7 +177,7 @@ int main(int argc, char **argv) {
         t0 = omp_get_wtime();
         g->find_Usp_Uch(nk0 / 2, Nw0 / 2, Usc);
         fprintf(meta, "t_half %.6f\n", omp_get_wtime() - t0);
-    } else if (mode == "solve" || mode == "post" || mode == "cond" || mode == "files") {
+    } else if (mode == "solve" || mode == "post" || mode == "cond" || mode == "files" || mode == "rew") {
         g->set_keep_chiqw(true);
         t0 = omp_get_wtime();
         g->calc_Self_FFT_spline();
@@ -191,6 +195,13 @@ int main(int argc, char **argv) {
         g->dump_solve(meta, absdir);
         g->dump_corr(meta);
         if (mode == "files") g->save_files();
+        if (mode == "rew") {
+            int nn[16];
+            for (int j = 0; j < 16; j++) nn[j] = j;
+            double w[9], eta[2] = {0.05, 0.01};
+            for (int j = 0; j < 9; j++) w[j] = -4.0 + j;
+            g->calc_Self_Re_w_BZ(nn, 16, w, 9, eta, 2);
+        }
         if (mode == "post" || mode == "cond") {
             // the post-processing tpsc_main.cpp runs after find_mu (lines 77-114)
             g->find_FS_inter();

@@ -1,6 +1,6 @@
 // files_main.cpp -- the saved-run formats through the drop-in classes.
 //
-//   files_main_b200 save|load|corr U tp tpp t3 n T nk0 Nw0
+//   files_main_b200 save|load|corr|rew U tp tpp t3 n T nk0 Nw0
 //
 // save: the model is solved as src/tpsc_main.cpp solves it
 // (calc_Self_FFT_spline, traceSelfG, find_mu), then written with the
@@ -11,6 +11,9 @@
 // (for instance one the reference wrote).
 // corr: chi::calc_corr_length({n, n + 0.05}, 2, {T, 1.5 T}, 2), the (n, T)
 // scan that writes the corrLgth file.
+// rew: the solve, then green::calc_Self_Re_w_BZ(n = 0..15, 16, w = -4..4
+// (9 points), 9, eta = {0.05, 0.01}, 2): the real-frequency Sigma and A(k, w)
+// files of every k of the reduced zone.
 // Prints "mu <value>" per find_mu, 17 significant digits.
 #include <cstdio>
 #include <cstdlib>
@@ -28,14 +31,27 @@ public:
 };
 
 int main(int argc, char **argv) {
-    if (argc != 10 || (strcmp(argv[1], "save") && strcmp(argv[1], "load") && strcmp(argv[1], "corr"))) {
-        fprintf(stderr, "usage: %s save|load|corr U tp tpp t3 n T nk0 Nw0\n", argv[0]);
+    if (argc != 10 ||
+        (strcmp(argv[1], "save") && strcmp(argv[1], "load") && strcmp(argv[1], "corr") && strcmp(argv[1], "rew"))) {
+        fprintf(stderr, "usage: %s save|load|corr|rew U tp tpp t3 n T nk0 Nw0\n", argv[0]);
         return 1;
     }
     const bool save = !strcmp(argv[1], "save");
     double params[] = {atof(argv[3]), atof(argv[4]), atof(argv[5]), atof(argv[2])};
     const double n = atof(argv[6]), T = atof(argv[7]);
     const int nk0 = atoi(argv[8]), Nw0 = atoi(argv[9]);
+    if (!strcmp(argv[1], "rew")) {
+        files_green g(nk0, Nw0, n, T, 0.1, params);
+        g.calc_Self_FFT_spline();
+        g.traceSelfG();
+        g.find_mu();
+        int nn[16];
+        for (int j = 0; j < 16; j++) nn[j] = j;
+        double w[9], eta[2] = {0.05, 0.01};
+        for (int j = 0; j < 9; j++) w[j] = -4.0 + j;
+        g.calc_Self_Re_w_BZ(nn, 16, w, 9, eta, 2);
+        return 0;
+    }
     if (!strcmp(argv[1], "corr")) {
         files_green c(nk0, Nw0, n, T, 0.1, params);
         double dens[2] = {n, n + 0.05}, temp[2] = {T, 1.5 * T};

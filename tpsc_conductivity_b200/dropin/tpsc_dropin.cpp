@@ -9,6 +9,7 @@
 // dumps (src/chi0.cpp:720-742).
 #include "tpsc_dropin.h"
 
+#include <complex>
 #include <vector>
 
 namespace {
@@ -621,6 +622,128 @@ void green::save_self_ikn(int *k_save, int nk_save, int Nwn) {
         }
     }
     file.close();
+}
+
+// green::calc_Self_Re_w (src/green.cpp:407-542) at one k, and
+// calc_Self_Re_w_BZ (src/green.cpp:386-404) at every k of the reduced zone
+void green::calc_Self_Re_w(int *k, int *n, int Nn, double *w, int Nw, double *eta, int Neta) {
+    self_re_w(k, 1, n, Nn, w, Nw, eta, Neta);
+}
+
+void green::calc_Self_Re_w_BZ(int *n, int Nn, double *w, int Nw, double *eta, int Neta) {
+    std::vector<int> ks;
+    const int nk2 = (nbk - 1) / 2 + 1;
+    for (int l = 0; l < nk2; l++)
+        for (int m = 0; l + m <= nbk - m - 1; m++) {
+            ks.push_back(nbk - m - 1);
+            ks.push_back(l + m);
+        }
+    self_re_w(ks.data(), (int)ks.size() / 2, n, Nn, w, Nw, eta, Neta);
+}
+
+// For the nk points k = (ks[2p], ks[2p+1]): the Pade continuation of
+// Sigma(k, z) = Sigma_inf/z + C2/z^2 + C3/z^3 + S/z^4 from the Nn points
+// z_j = i (2 n[j] + 1) pi T (S read at the stored frequency j, as the
+// reference does) to z = w + i eta, and A(k, w) = -Im 1/(pi (z - eps + mu -
+// Sigma)); then the same from the J-fraction Sigma = a1/(z + b1 + F(z)),
+// a1 = Sigma_inf, b1 = -C2/Sigma_inf, F continued from max(4, Nn/8) points
+// (src/green.cpp:487-540).  All k in two batched Pade launches; the
+// reference's four files per k.
+void green::self_re_w(const int *ks, int nk, int *n, int Nn, double *w, int Nw, double *eta, int Neta) {
+    if (!have_self) {
+        cout << "calc_Self_Re_w(): la self-energie n'a pas ete calculee\n";
+        return;
+    }
+    const int Nn2 = std::max(4, Nn / 8);
+    if (Nn < Nn2 || Nn > nbw / 2 || Neta < 1 || Nw < 1) {
+        cout << "calc_Self_Re_w(): need " << Nn2 << " <= Nn <= " << nbw / 2 << ", Nw >= 1 and Neta >= 1\n";
+        return;
+    }
+    const size_t n8 = (size_t)nbk * (nbk + 1) / 2;
+    std::vector<double> S((size_t)2 * n8 * (nbw / 2)), c2(n8), c3(n8), ek((size_t)nbk * nbk);
+    if (!check(tpsc_get_self(ctx_, S.data(), c2.data(), c3.data(), NULL), "calc_Self_Re_w")) return;
+    if (!check(tpsc_get_ek(ctx_, ek.data()), "calc_Self_Re_w")) return;
+    typedef std::complex<double> cx;
+    const double pi = acos(-1.0);
+    const int nk0 = 2 * (nbk - 1);
+    auto fold = [&](int x) {
+        while (x < 0) x += nk0;
+        return x > nbk - 1 ? nk0 - x : x;
+    };
+    std::vector<cx> z0(Nn), x1((size_t)nk * Nn), y1((size_t)nk * Nn), x2((size_t)nk * Nn2), y2((size_t)nk * Nn2);
+    std::vector<cx> zs((size_t)Nw * Neta);
+    for (int j = 0; j < Nn; j++) z0[j] = cx(0.0, (2 * n[j] + 1) * pi * tem);
+    for (int j = 0; j < Nw; j++)
+        for (int l = 0; l < Neta; l++) zs[(size_t)j * Neta + l] = cx(w[j], eta[l]);
+    std::vector<double> a1(nk), b1(nk), ekmu(nk);
+    for (int p = 0; p < nk; p++) {
+        long x = ks[2 * p], y = ks[2 * p + 1];
+        if (y > x) std::swap(x, y);
+        const size_t o = y + (x * (x + 1)) / 2;
+        auto fk = [&](int j) { return cx(S[2 * (o + j * n8)], S[2 * (o + j * n8) + 1]); };
+        for (int j = 0; j < Nn; j++) {
+            const cx z = z0[j];
+            x1[(size_t)p * Nn + j] = z;
+            y1[(size_t)p * Nn + j] = Sigma_inf / z + c2[o] / (z * z) + c3[o] / (z * z * z) + fk(j) / (z * z * z * z);
+        }
+        const double c1 = Sigma_inf, cc3 = c3[o];
+        a1[p] = c1;
+        b1[p] = -c2[o] / c1;
+        const double b = b1[p];
+        for (int j = 0; j < Nn2; j++) {
+            const cx z = z0[j], f = fk(j);
+            x2[(size_t)p * Nn2 + j] = z;
+            y2[(size_t)p * Nn2 + j] =
+                (b * f + (f + b * cc3) * z + (cc3 - c1 * b * b) * z * z) / (-f - cc3 * z + c1 * b * z * z - c1 * z * z * z);
+        }
+        ekmu[p] = ek[fold(ks[2 * p + 1]) + (size_t)fold(ks[2 * p]) * nbk] - mu;
+    }
+    const int Nz = Nw * Neta;
+    std::vector<cx> s1((size_t)nk * Nz), s2((size_t)nk * Nz);
+    if (!check(tpsc_pade_batch(ctx_, nk, Nn, (double *)x1.data(), (double *)y1.data(), Nz, (double *)zs.data(),
+                               (double *)s1.data()),
+               "calc_Self_Re_w"))
+        return;
+    if (!check(tpsc_pade_batch(ctx_, nk, Nn2, (double *)x2.data(), (double *)y2.data(), Nz, (double *)zs.data(),
+                               (double *)s2.data()),
+               "calc_Self_Re_w"))
+        return;
+    char name[200];
+    for (int p = 0; p < nk; p++) {
+        for (int variant = 0; variant < 2; variant++) {
+            const char *fs = variant ? "Self_Re_w_Jfrac_U%4.2f_tp%5.3f_tpp%5.3f_tt%5.3f_dens%7.5f_tem%6.4f_Nk%1d_Nwn%1d_%1d_%1d.dat"
+                                     : "Self_Re_w_U%4.2f_tp%5.3f_tpp%5.3f_tt%5.3f_dens%7.5f_tem%6.4f_Nk%1d_Nwn%1d_%1d_%1d.dat";
+            const char *fa = variant
+                                 ? "spectr_wgt_Jfrac_U%4.2f_tp%5.3f_tpp%5.3f_tt%5.3f_dens%7.5f_tem%6.4f_Nk%1d_Nwn%1d_%1d_%1d.dat"
+                                 : "spectr_wgt_U%4.2f_tp%5.3f_tpp%5.3f_tt%5.3f_dens%7.5f_tem%6.4f_Nk%1d_Nwn%1d_%1d_%1d.dat";
+            fstream fileSelf, fileAkw;
+            sprintf(name, fs, U, tp, tpp, t3, density, tem, nk0, nbw, ks[2 * p], ks[2 * p + 1]);
+            fileSelf.open(name, ios::out);
+            fileSelf << setiosflags(ios::left) << setprecision(10);
+            sprintf(name, fa, U, tp, tpp, t3, density, tem, nk0, nbw, ks[2 * p], ks[2 * p + 1]);
+            fileAkw.open(name, ios::out);
+            fileAkw << setiosflags(ios::left) << setprecision(10);
+            for (int j = 0; j < Nw; j++) {
+                for (int l = 0; l < Neta; l++) {
+                    const size_t q = (size_t)p * Nz + (size_t)j * Neta + l;
+                    const cx z = zs[(size_t)j * Neta + l];
+                    const cx self_w = variant ? a1[p] / (z + b1[p] + s2[q]) : s1[q];
+                    const double Akw = -imag((1.0 / pi) / (z - ekmu[p] - self_w));
+                    if (l == 0) {
+                        fileSelf << setw(25) << w[j] << setw(20) << real(self_w) << setw(25) << imag(self_w);
+                        fileAkw << setw(25) << w[j] << setw(20) << Akw;
+                    } else {
+                        fileSelf << setw(20) << real(self_w) << setw(25) << imag(self_w);
+                        fileAkw << setw(20) << Akw;
+                    }
+                }
+                fileSelf << endl;
+                fileAkw << endl;
+            }
+            fileSelf.close();
+            fileAkw.close();
+        }
+    }
 }
 
 // green::save_Self (src/green.cpp:1544-1574): ascii, Nfreq frequencies

@@ -132,8 +132,11 @@ public:
     void save_self_ikn(int *k_save, int nk_save, int Nwn);
     void save_Green(int *k);
     void save_Self(int Nfreq);
+    void calc_Self_Re_w(int *k, int *n, int Nn, double *w, int Nw, double *eta, int Neta);
+    void calc_Self_Re_w_BZ(int *n, int Nn, double *w, int Nw, double *eta, int Neta);
 
 protected:
+    void self_re_w(const int *ks, int nk, int *n, int Nn, double *w, int Nw, double *eta, int Neta);
     void load_Self();
     void save_Self_bin();
     void load_Self_bin();
