@@ -25,6 +25,11 @@
  *               (9 points), 9, eta = {0.05, 0.01}, 2) (src/green.cpp:386-542):
  *               Pade and J-fraction Sigma(k, w + i eta) and A(k, w) files for
  *               every k of the reduced zone
+ *        edc    solve, then green::EDC over the reduced zone and over a k list
+ *               (non-uniform grid m = 1, NP_max = 8, w = -2..2 (5 points),
+ *               eta = {0.05, 0.1}) and green::EDC({3}, {1}, 1, "edc2")
+ *               (src/green.cpp:589-812), on one OpenMP thread: the first
+ *               overload shares its Pade buffers (members) between threads
  *        files  solve, then the reference's own writers of the saved-run
  *               formats: chi0::save_chi, green::save_Self(0),
  *               green::save_Self_bin, green::save_Green({2, 1})
@@ -177,7 +182,8 @@ int main(int argc, char **argv) {
         t0 = omp_get_wtime();
         g->find_Usp_Uch(nk0 / 2, Nw0 / 2, Usc);
         fprintf(meta, "t_half %.6f\n", omp_get_wtime() - t0);
-    } else if (mode == "solve" || mode == "post" || mode == "cond" || mode == "files" || mode == "rew") {
+    } else if (mode == "solve" || mode == "post" || mode == "cond" || mode == "files" || mode == "rew" ||
+               mode == "edc") {
         g->set_keep_chiqw(true);
         t0 = omp_get_wtime();
         g->calc_Self_FFT_spline();
@@ -195,6 +201,16 @@ int main(int argc, char **argv) {
         g->dump_solve(meta, absdir);
         g->dump_corr(meta);
         if (mode == "files") g->save_files();
+        if (mode == "edc") {
+            omp_set_num_threads(1);
+            double w[5] = {-2.0, -1.0, 0.0, 1.0, 2.0}, eta[2] = {0.05, 0.1};
+            char f1[] = "edc", f2[] = "edcl", f3[] = "edc2";
+            g->EDC(NULL, NULL, 0, w, 5, 1, 8, eta, 2, f1);
+            int kx[2] = {-3, 10}, ky[2] = {1, 2};
+            g->EDC(kx, ky, 2, w, 5, 1, 8, eta, 2, f2);
+            int kx2[1] = {3}, ky2[1] = {1};
+            g->EDC(kx2, ky2, 1, f3);
+        }
         if (mode == "rew") {
             int nn[16];
             for (int j = 0; j < 16; j++) nn[j] = j;

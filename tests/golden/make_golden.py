@@ -52,11 +52,13 @@ CASES = {
     # green::calc_Self_Re_w_BZ on a 16x16 lattice with 32 positive iwn: the
     # Pade and J-fraction Sigma(k, w + i eta) and A(k, w) files of every k
     "rew_l16_w64": ("rew", 3.0, -0.15, 0.0, 0.0, 0.9, 0.15, 16, 64, True),
+    # green::EDC, both overloads, on a 16x16 lattice with 16 positive iwn
+    "edc_l16_w32": ("edc", 2.5, -0.1, 0.0, 0.0, 0.9, 0.25, 16, 32, True),
 }
 
 # the files the reference's writers leave (src/chi0.cpp:63, src/green.cpp:1507,
 # 1557, 1606); chi0_qmax_wn_* and chi0_wn0_q_* are the chi0 stage's own dumps
-FILE_PREFIXES = ("chi0_", "self_bin_", "self_tpsc_", "Green_", "corrLgth_", "Self_Re_w_", "spectr_wgt_")
+FILE_PREFIXES = ("chi0_", "self_bin_", "self_tpsc_", "Green_", "corrLgth_", "Self_Re_w_", "spectr_wgt_", "edc")
 FILE_SKIP = ("chi0_qmax_wn_", "chi0_wn0_q_")
 
 
@@ -158,7 +160,7 @@ def run_case(name, spec, threads):
             out["gwn_local"] = g[:, 1] + 1j * g[:, 2]
             out["fs_inter"] = table("FS_inter_AkF_", exclude="FS_inter_AkF_Pade_")
             out["fs_inter_pade"] = table("FS_inter_AkF_Pade_")
-        if mode in ("files", "rew"):
+        if mode in ("files", "rew", "edc"):
             work = os.path.join(d, "work")
             names = sorted(f for f in os.listdir(work)
                            if f.startswith(FILE_PREFIXES) and not f.startswith(FILE_SKIP))

@@ -184,3 +184,26 @@ def test_dropin_self_re_w_bz_writes_the_reference_files(tmp_path):
         else:
             pade.append(err)
     assert len(pade) == 38 and np.median(pade) < 1e-5 and max(pade) < 1e-3
+
+
+@pytest.mark.skipif(not os.path.exists(BIN), reason="files_main_b200 is built by make -C tpsc_conductivity_b200/dropin")
+def test_dropin_edc_writes_the_reference_files(tmp_path):
+    """green::EDC, both overloads (edc_l16_w32, written by the reference on
+    one OpenMP thread): the non-uniform-grid Pade over the reduced zone and
+    over a k list (folded into the zone, as the file names show) to 1e-8 of
+    each file's scale, and the 16-point Pade on w = -10..10 to 1e-7; the same
+    file names."""
+    g = load_golden("edc_l16_w32")
+    names = [str(n) for n in g["file_names"]]
+    U, tp, tpp, t3, n, T, nk0, Nw0 = g["params"]
+    args = [repr(float(x)) for x in (U, tp, tpp, t3, n, T)] + [str(int(nk0)), str(int(Nw0))]
+    r = subprocess.run([BIN, "edc"] + args, cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert sorted(f for f in os.listdir(tmp_path) if f.startswith("edc")) == sorted(names)
+    assert any(nm.startswith("edcl_") and nm.endswith("_3_1_-2.0e+00_2.0e+00.dat") for nm in names)
+    for i, name in enumerate(names):
+        b = np.loadtxt(bytes(g[f"file_{i}"]).decode().splitlines(), ndmin=2)
+        a = np.loadtxt((tmp_path / name).read_text().splitlines(), ndmin=2)
+        assert a.shape == b.shape and np.array_equal(a[:, 0], b[:, 0])
+        err = np.abs(a[:, 1:] - b[:, 1:]).max() / np.abs(b[:, 1:]).max()
+        assert err < (1e-7 if name.startswith("edc2") else 1e-8), (name, err)

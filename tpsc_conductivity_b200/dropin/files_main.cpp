@@ -1,6 +1,6 @@
 // files_main.cpp -- the saved-run formats through the drop-in classes.
 //
-//   files_main_b200 save|load|corr|rew U tp tpp t3 n T nk0 Nw0
+//   files_main_b200 save|load|corr|rew|edc U tp tpp t3 n T nk0 Nw0
 //
 // save: the model is solved as src/tpsc_main.cpp solves it
 // (calc_Self_FFT_spline, traceSelfG, find_mu), then written with the
@@ -14,6 +14,9 @@
 // rew: the solve, then green::calc_Self_Re_w_BZ(n = 0..15, 16, w = -4..4
 // (9 points), 9, eta = {0.05, 0.01}, 2): the real-frequency Sigma and A(k, w)
 // files of every k of the reduced zone.
+// edc: the solve, then green::EDC over the reduced zone and over the k list
+// {(-3, 1), (10, 2)} (non-uniform grid m = 1, NP_max = 8, w = -2..2, eta =
+// {0.05, 0.1}; prefixes edc and edcl) and green::EDC({3}, {1}, 1, "edc2").
 // Prints "mu <value>" per find_mu, 17 significant digits.
 #include <cstdio>
 #include <cstdlib>
@@ -32,14 +35,29 @@ public:
 
 int main(int argc, char **argv) {
     if (argc != 10 ||
-        (strcmp(argv[1], "save") && strcmp(argv[1], "load") && strcmp(argv[1], "corr") && strcmp(argv[1], "rew"))) {
-        fprintf(stderr, "usage: %s save|load|corr|rew U tp tpp t3 n T nk0 Nw0\n", argv[0]);
+        (strcmp(argv[1], "save") && strcmp(argv[1], "load") && strcmp(argv[1], "corr") && strcmp(argv[1], "rew") &&
+         strcmp(argv[1], "edc"))) {
+        fprintf(stderr, "usage: %s save|load|corr|rew|edc U tp tpp t3 n T nk0 Nw0\n", argv[0]);
         return 1;
     }
     const bool save = !strcmp(argv[1], "save");
     double params[] = {atof(argv[3]), atof(argv[4]), atof(argv[5]), atof(argv[2])};
     const double n = atof(argv[6]), T = atof(argv[7]);
     const int nk0 = atoi(argv[8]), Nw0 = atoi(argv[9]);
+    if (!strcmp(argv[1], "edc")) {
+        files_green g(nk0, Nw0, n, T, 0.1, params);
+        g.calc_Self_FFT_spline();
+        g.traceSelfG();
+        g.find_mu();
+        double w[5] = {-2.0, -1.0, 0.0, 1.0, 2.0}, eta[2] = {0.05, 0.1};
+        char f1[] = "edc", f2[] = "edcl", f3[] = "edc2";
+        g.EDC(NULL, NULL, 0, w, 5, 1, 8, eta, 2, f1);
+        int kx[2] = {-3, 10}, ky[2] = {1, 2};
+        g.EDC(kx, ky, 2, w, 5, 1, 8, eta, 2, f2);
+        int kx2[1] = {3}, ky2[1] = {1};
+        g.EDC(kx2, ky2, 1, f3);
+        return 0;
+    }
     if (!strcmp(argv[1], "rew")) {
         files_green g(nk0, Nw0, n, T, 0.1, params);
         g.calc_Self_FFT_spline();

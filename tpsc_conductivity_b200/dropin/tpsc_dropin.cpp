@@ -746,6 +746,245 @@ void green::self_re_w(const int *ks, int nk, int *n, int Nn, double *w, int Nw, 
     }
 }
 
+bool green::spectra(const int *ks, int nk, const double *z0, int N, const double *w, int nw0, const double *eta,
+                    int neta, double *out) {
+    typedef std::complex<double> cx;
+    const size_t n8 = (size_t)nbk * (nbk + 1) / 2;
+    std::vector<double> S((size_t)2 * n8 * (nbw / 2)), c2(n8), c3(n8), ek((size_t)nbk * nbk);
+    if (!check(tpsc_get_self(ctx_, S.data(), c2.data(), c3.data(), NULL), "calc_spectral_weight")) return false;
+    if (!check(tpsc_get_ek(ctx_, ek.data()), "calc_spectral_weight")) return false;
+    std::vector<cx> X((size_t)nk * N), Y((size_t)nk * N), Z((size_t)nw0 * neta), F((size_t)nk * nw0 * neta);
+    for (int j = 0; j < nw0; j++)
+        for (int l = 0; l < neta; l++) Z[(size_t)j * neta + l] = cx(w[j], eta[l]);
+    for (int p = 0; p < nk; p++) {
+        int x = ks[2 * p], y = ks[2 * p + 1];
+        if (y > x) std::swap(x, y);
+        const size_t o = y + ((size_t)x * (x + 1)) / 2;
+        for (int n = 0; n < N; n++) {
+            const cx z(z0[2 * n], z0[2 * n + 1]);
+            X[(size_t)p * N + n] = z;
+            Y[(size_t)p * N + n] = Sigma_inf / z + c2[o] / (z * z) + c3[o] / (z * z * z) +
+                                   cx(S[2 * (o + n * n8)], S[2 * (o + n * n8) + 1]) / (z * z * z * z);
+        }
+    }
+    if (!check(tpsc_pade_batch(ctx_, nk, N, (double *)X.data(), (double *)Y.data(), nw0 * neta, (double *)Z.data(),
+                               (double *)F.data()),
+               "calc_spectral_weight"))
+        return false;
+    const double pi = acos(-1.0);
+    for (int p = 0; p < nk; p++) {
+        // hamiltonien::ek_val on the folded point (src/hamiltonien.cpp:107-116)
+        const double ekmu = ek[ks[2 * p + 1] + (size_t)ks[2 * p] * nbk] - mu;
+        for (int j = 0; j < nw0; j++)
+            for (int l = 0; l < neta; l++) {
+                const size_t q = ((size_t)p * nw0 + j) * neta + l;
+                out[q] = -imag(1.0 / (cx(w[j] - ekmu, eta[l]) - F[q])) / pi;
+            }
+    }
+    return true;
+}
+
+// green::calc_spectral_weight (src/green.cpp:1152-1260): A(k, w + i eta) from
+// the N-point Pade through i (2n + 1) pi T, n < N; k folded by |.|
+void green::calc_spectral_weight(int *k, double *w, int nw0, int N, double *spectr_w) {
+    if (w[0] > w[nw0 - 1]) {
+        cout << "calc_spectral_weight: wi>wf!\n";
+        return;
+    }
+    if (N > nbw / 2) {
+        cout << "calc_spectral_weight: Value N larger than nw=" << nbw / 2 << '\n';
+        return;
+    }
+    if (N <= 0) {
+        cout << "calc_spectral_weight: Value N too small: " << N << '\n';
+        return;
+    }
+    if (k[0] < 0) k[0] *= -1;
+    if (k[1] < 0) k[1] *= -1;
+    if (k[0] >= nbk || k[1] >= nbk) {
+        cout << "calc_spectral_weight: invalid wave vector k=(" << k[0] << "," << k[1] << ")" << '\n';
+        return;
+    }
+    if (!have_self) {
+        cout << "calc_spectral_weight: Self-energy not computed" << '\n';
+        return;
+    }
+    const double pi = acos(-1.0);
+    std::vector<double> z0(2 * (size_t)N);
+    for (int n = 0; n < N; n++) {
+        z0[2 * n] = 0.0;
+        z0[2 * n + 1] = (2 * n + 1) * pi * tem;
+    }
+    spectra(k, 1, z0.data(), N, w, nw0, &eta, 1, spectr_w);
+}
+
+// green::calc_spectral_weight with several eta (src/green.cpp:1073-1150): the
+// Pade through the non-uniform points of create_non_uniform_ind_freq; k
+// folded into the zone
+void green::calc_spectral_weight(int *k, double *w, int nw0, int N, double *eta_p, int N_eta, double *spectr_w) {
+    if (w[0] > w[nw0 - 1]) {
+        cout << "calc_spectral_weight: wi>wf!\n";
+        return;
+    }
+    if (N > nbw / 2) {
+        cout << "calc_spectral_weight: Value N larger than nw=" << nbw / 2 << '\n';
+        return;
+    }
+    if (N <= 0) {
+        cout << "calc_spectral_weight: Value N too small: " << N << '\n';
+        return;
+    }
+    const int Nk = 2 * (nbk - 1);
+    while (k[0] < 0) k[0] += Nk;
+    while (k[1] < 0) k[1] += Nk;
+    if (k[0] > nbk - 1) k[0] = Nk - k[0];
+    if (k[1] > nbk - 1) k[1] = Nk - k[1];
+    if (!have_self) {
+        cout << "calc_spectral_weight: Self-energy not computed" << '\n';
+        return;
+    }
+    if ((int)pade_z0.size() < 2 * N) {
+        cout << "calc_spectral_weight: create_non_uniform_ind_freq has not been called\n";
+        return;
+    }
+    spectra(k, 1, pade_z0.data(), N, w, nw0, eta_p, N_eta, spectr_w);
+}
+
+// green::create_non_uniform_ind_freq (src/green.cpp:554-582): the first N1 =
+// nbw / 2^(m+1) indices, then m runs of N1/2 indices spaced 2^(l+1)
+void green::create_non_uniform_ind_freq(int m_freq_p) {
+    m_freq = m_freq_p;
+    const int N1 = nbw / ((int)pow(2, m_freq + 1)), N2 = N1 / 2;
+    N_freq = N1 + m_freq * N2;
+    cout << "non uniform frequency grid parameters:\n";
+    cout << "N1: " << N1 << endl;
+    cout << "N_freq: " << N_freq << endl;
+    ind_freq.assign(N_freq, 0);
+    for (int j = 0; j < N1; j++) ind_freq[j] = j;
+    for (int j = N1; j < N_freq; j++) {
+        const int lj = (j - N1) / N2, p2lj = (int)pow(2, lj);
+        ind_freq[j] = p2lj * N1 + p2lj * 2 * ((j - N1) % N2);
+    }
+    const double pi = acos(-1.0);
+    pade_z0.assign(2 * (size_t)N_freq, 0.0);
+    for (int j = 0; j < N_freq; j++) pade_z0[2 * j + 1] = (2 * ind_freq[j] + 1) * pi * tem;
+}
+
+// green::EDC (src/green.cpp:589-711): A(k, w + i eta_p) from the Pade through
+// up to NP_max points of the non-uniform grid, for the listed k or (kx or ky
+// NULL) every other point of the reduced zone; one file per k.  All k in one
+// batched device Pade.
+void green::EDC(int *kx, int *ky, int Nk, double *w, int nw0, int m_freq_p, int NP_max, double *eta_p, int N_eta,
+                char *fname) {
+    if (!have_self) {
+        cout << "EDC(): la self-energie n'a pas ete calculee\n";
+        return;
+    }
+    create_non_uniform_ind_freq(m_freq_p);
+    const double pi = acos(-1.0);
+    const int NP = N_freq > NP_max ? NP_max : N_freq;
+    cout << setprecision(5);
+    cout << "frequence maximale incluse dans le prolongement analytique: " << (2 * ind_freq[NP - 1] + 1) * pi * tem
+         << endl;
+    std::string form = fname ? fname : "spectral_weight";
+    form += "_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d_%1d_%1d_%3.1e_%3.1e.dat";
+    std::vector<int> ks;
+    if (!kx || !ky) {
+        cout << "calcul du poids spectral dans la zone reduite\n";
+        for (int l = 0; l < nbk; l += 2)
+            for (int m = 0; m <= l; m += 2) {
+                ks.push_back(l);
+                ks.push_back(m);
+            }
+    } else {
+        cout << "calcul du poids spectral pour les vecteurs d'onde entre k=(" << (pi * kx[0]) / (nbk - 1) << ","
+             << (pi * ky[0]) / (nbk - 1) << ") et (" << (pi * kx[Nk - 1]) / (nbk - 1) << ","
+             << (pi * ky[Nk - 1]) / (nbk - 1) << ")\n";
+        const int NK = 2 * (nbk - 1);
+        for (int p = 0; p < Nk; p++) {
+            int k[2] = {kx[p], ky[p]};
+            for (int c = 0; c < 2; c++) {
+                while (k[c] < 0) k[c] += NK;
+                if (k[c] > nbk - 1) k[c] = NK - k[c];
+            }
+            ks.push_back(k[0]);
+            ks.push_back(k[1]);
+        }
+    }
+    const int nk = (int)ks.size() / 2;
+    std::vector<double> A((size_t)nk * nw0 * N_eta);
+    if (NP <= 0 || NP > nbw / 2 || w[0] > w[nw0 - 1] ||
+        !spectra(ks.data(), nk, pade_z0.data(), NP, w, nw0, eta_p, N_eta, A.data()))
+        return;
+    char name[400];
+    for (int p = 0; p < nk; p++) {
+        sprintf(name, form.c_str(), U, tp, tpp, t3, density, tem, 2 * (nbk - 1), nbw, ks[2 * p], ks[2 * p + 1], w[0],
+                w[nw0 - 1]);
+        fstream f;
+        f.open(name, ios::out);
+        f << setprecision(10) << setiosflags(ios::left);
+        for (int j = 0; j < nw0; j++) {
+            f << setw(20) << w[j];
+            for (int n = 0; n < N_eta; n++) f << setw(20) << A[((size_t)p * nw0 + j) * N_eta + n];
+            f << endl;
+        }
+        f.close();
+    }
+}
+
+// green::EDC (src/green.cpp:714-812): A(k, w + i eta) on w = -10..10 (step
+// 0.01) from the nbw/2-point Pade, the object's eta; fname is the prefix
+void green::EDC(int *kx, int *ky, int Nk, char *fname) {
+    if (!have_self) {
+        cout << "EDC(): la self-energie n'a pas ete calculee\n";
+        return;
+    }
+    const double Dw = 10.0, dw = 0.01;
+    const int nw0 = (int)(2 * Dw / dw) + 1;
+    std::vector<double> w(nw0);
+    w[0] = -Dw;
+    for (int j = 1; j < nw0; j++) w[j] = w[0] + j * dw;
+    const int N = nbw / 2;
+    std::vector<int> ks;
+    if (!kx || !ky) {
+        cout << "calcul du poids spectral dans la zone reduite\n";
+        for (int l = 0; l < nbk; l += 2)
+            for (int m = 0; m <= l; m += 2) {
+                ks.push_back(l);
+                ks.push_back(m);
+            }
+    } else {
+        cout << "calcul du poids spectral pour les vecteurs d'onde donnes\n";
+        for (int p = 0; p < Nk; p++) {
+            const int a = kx[p] < 0 ? -kx[p] : kx[p], b = ky[p] < 0 ? -ky[p] : ky[p];
+            if (a >= nbk || b >= nbk) {
+                // the reference would write a file of uninitialised values here
+                cout << "calc_spectral_weight: invalid wave vector k=(" << a << "," << b << ")" << '\n';
+                continue;
+            }
+            ks.push_back(a);
+            ks.push_back(b);
+        }
+    }
+    const int nk = (int)ks.size() / 2;
+    if (!nk) return;
+    const double pi = acos(-1.0);
+    std::vector<double> z0(2 * (size_t)N), A((size_t)nk * nw0);
+    for (int n = 0; n < N; n++) z0[2 * n + 1] = (2 * n + 1) * pi * tem;
+    if (!spectra(ks.data(), nk, z0.data(), N, w.data(), nw0, &eta, 1, A.data())) return;
+    std::string form = fname;
+    form += "_%4.2f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%3.1e_%1d_%1d_%1d_%1d.dat";
+    char name[400];
+    for (int p = 0; p < nk; p++) {
+        sprintf(name, form.c_str(), U, tp, tpp, t3, density, tem, eta, 2 * (nbk - 1), nbw, ks[2 * p], ks[2 * p + 1]);
+        fstream f;
+        f.open(name, ios::out);
+        f << setprecision(15) << setiosflags(ios::left);
+        for (int j = 0; j < nw0; j++) f << setw(30) << w[j] << A[(size_t)p * nw0 + j] << '\n';
+        f.close();
+    }
+}
+
 // green::save_Self (src/green.cpp:1544-1574): ascii, Nfreq frequencies
 void green::save_Self(int Nfreq) {
     if (!have_self) {

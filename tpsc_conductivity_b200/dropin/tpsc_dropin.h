@@ -27,6 +27,7 @@
 #include <iostream>
 #include <limits>
 #include <string>
+#include <vector>
 
 #include "../../include/tpsc_b200.h"
 
@@ -134,9 +135,33 @@ public:
     void save_Self(int Nfreq);
     void calc_Self_Re_w(int *k, int *n, int Nn, double *w, int Nw, double *eta, int Neta);
     void calc_Self_Re_w_BZ(int *n, int Nn, double *w, int Nw, double *eta, int Neta);
+    // spectral weight and energy distribution curves (src/green.cpp:554-812, 1073-1260)
+    void calc_spectral_weight(int *k, double *w, int nw0, int N, double *spectr_w);
+    void calc_spectral_weight(double *x, double *w, int nw0, double *spectr_w) {
+        int k[2];
+        double eps = 0.5 / nbk;
+        double f = (x[0] + eps) * nbk;
+        k[0] = (int)f;
+        f = (x[1] + eps) * nbk;
+        k[1] = (int)f;
+        calc_spectral_weight(k, w, nw0, nbw / 2, spectr_w);
+    }
+    void calc_spectral_weight(int *k, double *w, int nw0, int N, double *eta_p, int N_eta, double *spectr_w);
+    void EDC(int *kx, int *ky, int Nk, char *fname);
+    void create_non_uniform_ind_freq(int m);
+    void EDC(int *kx, int *ky, int Nk, double *w, int nw0, int m_freq, int NP_max, double *eta_p, int N_eta,
+             char *fname);
 
 protected:
     void self_re_w(const int *ks, int nk, int *n, int Nn, double *w, int Nw, double *eta, int Neta);
+    // A(k, w + i eta) at the nk octant points ks (folded pairs) from the N-point
+    // continued fraction through z0[0..N) with Sigma read at the stored
+    // frequencies 0..N-1: out[(p nw0 + j) neta + l]; one batched device Pade
+    bool spectra(const int *ks, int nk, const double *z0, int N, const double *w, int nw0, const double *eta, int neta,
+                 double *out);
+    std::vector<int> ind_freq;   // create_non_uniform_ind_freq
+    std::vector<double> pade_z0; // i (2 ind_freq[j] + 1) pi T, interleaved
+    int N_freq = 0, m_freq = 0;
     void load_Self();
     void save_Self_bin();
     void load_Self_bin();
