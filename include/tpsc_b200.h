@@ -398,6 +398,18 @@ int tpsc_set_self(tpsc_ctx *ctx, const double *self_kw, const double *sigma_inf2
  * are found again (TPSC_S_CHI0MAX, _QMAX0/1); the tail coefficients and
  * chi0(r, tau) stay those of the last chi0 stage. */
 int tpsc_set_chi0(tpsc_ctx *ctx, const double *chiqw);
+/* ---- the infinite lattice (spot checks of the finite-lattice results) ----
+ * green0::find_mu_inf_syst (src/green0.cpp:265-287): mu0 of the infinite
+ * lattice at the model's n and T; chi0::chiqw (src/chi0.cpp:211-276): chi0(q,
+ * i w_n) of the infinite lattice at npts points qw[p] = (qx, qy, w_n) for the
+ * chemical potential mu.  The reference integrates adaptively; here the
+ * integrands, analytic and periodic at T > 0, are summed on L x L grids of
+ * the zone (the trapezoid rule, exponentially convergent), L doubled from 128
+ * until two sums agree to 1e-13; L_used (may be NULL) is the last L.  With
+ * L > 0, tpsc_chi0_infinite sums that lattice only: chi0::chiqw_discret
+ * (src/chi0.cpp:1587-1612) at nq0 = L. */
+int tpsc_mu0_infinite(tpsc_ctx *ctx, double *mu, int *L_used);
+int tpsc_chi0_infinite(tpsc_ctx *ctx, double mu, int npts, const double *qw, int L, double *out, int *L_used);
 /* Sigma(k, tau_j) [N8], 0 <= j <= Nw0, of the last Sigma stage: the spline
  * nodes of green::calc_Self_FFT_spline (src/green.cpp:1872-1950). */
 int tpsc_get_sigma_tau(tpsc_ctx *ctx, int j, double *out);

@@ -30,6 +30,9 @@
  *               eta = {0.05, 0.1}) and green::EDC({3}, {1}, 1, "edc2")
  *               (src/green.cpp:589-812), on one OpenMP thread: the first
  *               overload shares its Pade buffers (members) between threads
+ *        chi0inf  chi0::calc_chi0_qlims(n, {0, 0, pi, pi}, {3, 3}) for n = 0, 1
+ *               (the infinite lattice by adaptive quadrature, src/chi0.cpp:157-276)
+ *               and chi0::chiqw_discret({2, 1}, 1) on the constructor's lattice
  *        files  solve, then the reference's own writers of the saved-run
  *               formats: chi0::save_chi, green::save_Self(0),
  *               green::save_Self_bin, green::save_Green({2, 1})
@@ -86,6 +89,19 @@ public:
         sp_corr_length();
         fprintf(meta, "vF %.17g\nxi_y %.17g\nxi_x %.17g\nxiAs_y %.17g\nxiAs_x %.17g\nxi0_y %.17g\nxi0_x %.17g\n",
                 vF, spCorrLgth_y, spCorrLgth_x, spCorrLgthAs_y, spCorrLgthAs_x, xi0_y, xi0_x);
+    }
+
+    // the infinite-lattice chi0 files, the infinite mu0 they leave in mu0,
+    // and the finite-lattice sum at q = (2, 1), n = 1
+    void chi0_infinite(FILE *meta) {
+        int q[2] = {2, 1};
+        fprintf(meta, "chi_discret %.17g\nmu0_finite %.17g\n", chiqw_discret(q, 1), mu0);
+        const double pi = acos(-1.0);
+        double qlims[4] = {0.0, 0.0, pi, pi};
+        int Nq[2] = {3, 3};
+        calc_chi0_qlims(0, qlims, Nq);
+        calc_chi0_qlims(1, qlims, Nq);
+        fprintf(meta, "mu0_inf %.17g\n", mu0);
     }
 
     // the saved-run formats, written by the reference's own methods
@@ -156,6 +172,10 @@ int main(int argc, char **argv) {
         g->calc_chiqw_FFT_spline(nk0, Nw0);
         fprintf(meta, "t_chi0 %.6f\n", omp_get_wtime() - t0);
         g->dump_chi0(meta, absdir);
+    } else if (mode == "chi0inf") {
+        t0 = omp_get_wtime();
+        g->chi0_infinite(meta);
+        fprintf(meta, "t_chi0inf %.6f\n", omp_get_wtime() - t0);
     } else if (mode == "corr") {
         double dens[2] = {n, n + 0.05}, temp[2] = {T, 1.5 * T};
         t0 = omp_get_wtime();

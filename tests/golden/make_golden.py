@@ -54,6 +54,9 @@ CASES = {
     "rew_l16_w64": ("rew", 3.0, -0.15, 0.0, 0.0, 0.9, 0.15, 16, 64, True),
     # green::EDC, both overloads, on a 16x16 lattice with 16 positive iwn
     "edc_l16_w32": ("edc", 2.5, -0.1, 0.0, 0.0, 0.9, 0.25, 16, 32, True),
+    # the infinite lattice: chi0::calc_chi0_qlims at n = 0, 1 (adaptive
+    # quadrature), the infinite-system mu0, chiqw_discret on the 16x16 lattice
+    "chi0inf_l16": ("chi0inf", 2.0, -0.15, 0.05, 0.0, 0.85, 0.2, 16, 32, True),
 }
 
 # the files the reference's writers leave (src/chi0.cpp:63, src/green.cpp:1507,
@@ -81,6 +84,17 @@ def run_case(name, spec, threads):
         subprocess.run(args, check=True, env=env)
         meta = read_meta(os.path.join(d, "meta.txt"))
         nbk = nk0 // 2 + 1
+        if mode == "chi0inf":
+            work = os.path.join(d, "work")
+            names = sorted(f for f in os.listdir(work) if f.startswith("chi0_q_"))
+            out = {"params": np.array([U, tp, tpp, t3, n, T, nk0, Nw0], dtype=np.float64),
+                   "mu0_inf": np.array(float(meta["mu0_inf"])), "mu0_finite": np.array(float(meta["mu0_finite"])),
+                   "chi_discret": np.array(float(meta["chi_discret"])), "file_names": np.array(names)}
+            for i, f in enumerate(names):
+                out[f"file_{i}"] = np.fromfile(os.path.join(work, f), dtype=np.uint8)
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+            print(name, "done", names, meta.get("t_chi0inf"))
+            return
         if mode == "corr":
             work = os.path.join(d, "work")
             names = sorted(f for f in os.listdir(work) if f.startswith("corrLgth_"))

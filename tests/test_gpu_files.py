@@ -207,3 +207,31 @@ def test_dropin_edc_writes_the_reference_files(tmp_path):
         assert a.shape == b.shape and np.array_equal(a[:, 0], b[:, 0])
         err = np.abs(a[:, 1:] - b[:, 1:]).max() / np.abs(b[:, 1:]).max()
         assert err < (1e-7 if name.startswith("edc2") else 1e-8), (name, err)
+
+
+@pytest.mark.skipif(not os.path.exists(BIN), reason="files_main_b200 is built by make -C tpsc_conductivity_b200/dropin")
+def test_dropin_infinite_lattice_chi0(tmp_path):
+    """chi0::calc_chi0_qlims (the infinite lattice, which the reference
+    integrates adaptively to ~1e-10) from lattice sums doubled until they
+    converge: the same chi0_q files (q columns exact, chi0 to 1e-9), the same
+    infinite-system mu0 (1e-9), and chiqw_discret on the 16x16 lattice
+    (1e-12)."""
+    g = load_golden("chi0inf_l16")
+    names = [str(n) for n in g["file_names"]]
+    U, tp, tpp, t3, n, T, nk0, Nw0 = g["params"]
+    args = [repr(float(x)) for x in (U, tp, tpp, t3, n, T)] + [str(int(nk0)), str(int(Nw0))]
+    r = subprocess.run([BIN, "chi0inf"] + args, cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    val = {k: float(v) for k, v in re.findall(r"^(chi_discret|mu0_finite|mu0_inf) (\S+)$", r.stdout, re.M)}
+    assert abs(val["chi_discret"] - float(g["chi_discret"])) < 1e-12 * abs(float(g["chi_discret"]))
+    assert abs(val["mu0_finite"] - float(g["mu0_finite"])) < 1e-10
+    assert abs(val["mu0_inf"] - float(g["mu0_inf"])) < 1e-9
+    assert sorted(f for f in os.listdir(tmp_path) if f.startswith("chi0_q_")) == sorted(names)
+    for i, name in enumerate(names):
+        want = bytes(g[f"file_{i}"]).decode().splitlines()
+        have = (tmp_path / name).read_text().splitlines()
+        assert len(have) == len(want) == 6
+        for x, y in zip(have, want):
+            assert x.split()[:2] == y.split()[:2]
+        a, b = np.loadtxt(have, ndmin=2), np.loadtxt(want, ndmin=2)
+        assert np.allclose(a[:, 2], b[:, 2], rtol=1e-9, atol=1e-12), (name, a[:, 2] - b[:, 2])

@@ -33,6 +33,8 @@ SIGNATURES = [
     ("tpsc_set_self", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),
     ("tpsc_set_chi0", C.c_int, [C.c_void_p, _dp]),
     ("tpsc_get_sigma_tau", C.c_int, [C.c_void_p, C.c_int, _dp]),
+    ("tpsc_mu0_infinite", C.c_int, [C.c_void_p, _dp, _ip]),
+    ("tpsc_chi0_infinite", C.c_int, [C.c_void_p, C.c_double, C.c_int, _dp, C.c_int, _dp, _ip]),
     ("tpsc_file_name", C.c_int, [C.c_int, C.c_char_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                  C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int]),
     ("tpsc_write_chi0_bin", C.c_int, [C.c_char_p, C.c_int, C.c_int, _dp]),

@@ -2073,6 +2073,30 @@ int tpsc_get_sigma_tau(tpsc_ctx *ctx, int j, double *out) {
     return TPSC_OK;
 }
 
+// green0::find_mu_inf_syst (src/green0.cpp:265-287): mu0 of the infinite
+// lattice at the model's density and temperature (tpsc_lattice.cu)
+int tpsc_mu0_infinite(tpsc_ctx *ctx, double *mu, int *L_used) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    if (!mu) return fail(ctx, TPSC_ERR_ARG, "null output");
+    cudaSetDevice(ctx->device);
+    rc = lattice_mu0(ctx->n, ctx->T, ctx->tp, ctx->tpp, ctx->t3, ctx->st, mu, L_used);
+    return rc ? fail(ctx, rc, g_static_err) : TPSC_OK;
+}
+
+// chi0::chiqw (src/chi0.cpp:211-276): chi0(q, i w_n) of the infinite lattice
+// at npts points qw[p] = (qx, qy, w_n) for the chemical potential mu; L > 0:
+// the L x L lattice's sum (chi0::chiqw_discret, src/chi0.cpp:1587-1612)
+int tpsc_chi0_infinite(tpsc_ctx *ctx, double mu, int npts, const double *qw, int L, double *out, int *L_used) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    if (npts < 1 || npts > 65535 || !qw || !out || L < 0 || L > 65536)
+        return fail(ctx, TPSC_ERR_ARG, "need 1 <= npts <= 65535, 0 <= L <= 65536 and arrays");
+    cudaSetDevice(ctx->device);
+    rc = lattice_chi0(mu, ctx->T, ctx->tp, ctx->tpp, ctx->t3, npts, qw, L, ctx->st, out, L_used);
+    return rc ? fail(ctx, rc, g_static_err) : TPSC_OK;
+}
+
 // Warm start from saved results (green::load_Self_bin / load_Self,
 // src/green.cpp:1517-1541, 1637-1670): the reference's Self_kw_array layout
 // [Nw0/2][N8] complex into the device's blocked S; each tail array (and

@@ -1,6 +1,6 @@
 // files_main.cpp -- the saved-run formats through the drop-in classes.
 //
-//   files_main_b200 save|load|corr|rew|edc U tp tpp t3 n T nk0 Nw0
+//   files_main_b200 save|load|corr|rew|edc|chi0inf U tp tpp t3 n T nk0 Nw0
 //
 // save: the model is solved as src/tpsc_main.cpp solves it
 // (calc_Self_FFT_spline, traceSelfG, find_mu), then written with the
@@ -17,7 +17,11 @@
 // edc: the solve, then green::EDC over the reduced zone and over the k list
 // {(-3, 1), (10, 2)} (non-uniform grid m = 1, NP_max = 8, w = -2..2, eta =
 // {0.05, 0.1}; prefixes edc and edcl) and green::EDC({3}, {1}, 1, "edc2").
+// chi0inf: chi0::chiqw_discret({2, 1}, 1), then chi0::calc_chi0_qlims(n,
+// {0, 0, pi, pi}, {3, 3}) for n = 0, 1 (the infinite lattice); prints
+// "chi_discret", "mu0_finite" and, after the scans, "mu0_inf".
 // Prints "mu <value>" per find_mu, 17 significant digits.
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -31,19 +35,32 @@ public:
     files_green(int nk0, int Nw0, double n, double T, double eta, double *p) : green(nk0, Nw0, n, T, eta, p) {}
     void warm_start() { load_Self_bin(); }
     void save_bin() { save_Self_bin(); }
+    double mu0_now() const { return mu0; }
 };
 
 int main(int argc, char **argv) {
     if (argc != 10 ||
         (strcmp(argv[1], "save") && strcmp(argv[1], "load") && strcmp(argv[1], "corr") && strcmp(argv[1], "rew") &&
-         strcmp(argv[1], "edc"))) {
-        fprintf(stderr, "usage: %s save|load|corr|rew|edc U tp tpp t3 n T nk0 Nw0\n", argv[0]);
+         strcmp(argv[1], "edc") && strcmp(argv[1], "chi0inf"))) {
+        fprintf(stderr, "usage: %s save|load|corr|rew|edc|chi0inf U tp tpp t3 n T nk0 Nw0\n", argv[0]);
         return 1;
     }
     const bool save = !strcmp(argv[1], "save");
     double params[] = {atof(argv[3]), atof(argv[4]), atof(argv[5]), atof(argv[2])};
     const double n = atof(argv[6]), T = atof(argv[7]);
     const int nk0 = atoi(argv[8]), Nw0 = atoi(argv[9]);
+    if (!strcmp(argv[1], "chi0inf")) {
+        files_green g(nk0, Nw0, n, T, 0.1, params);
+        int q[2] = {2, 1};
+        printf("chi_discret %.17g\nmu0_finite %.17g\n", g.chiqw_discret(q, 1), g.mu0_now());
+        const double pi = acos(-1.0);
+        double qlims[4] = {0.0, 0.0, pi, pi};
+        int Nq[2] = {3, 3};
+        g.calc_chi0_qlims(0, qlims, Nq);
+        g.calc_chi0_qlims(1, qlims, Nq);
+        printf("mu0_inf %.17g\n", g.mu0_now());
+        return 0;
+    }
     if (!strcmp(argv[1], "edc")) {
         files_green g(nk0, Nw0, n, T, 0.1, params);
         g.calc_Self_FFT_spline();

@@ -157,6 +157,74 @@ void chi0::traceChi0() {
          << "\tdifference relative:  " << (ex - tr[1]) / ex << '\n';
 }
 
+// green0::find_mu_inf_syst (src/green0.cpp:265-287): mu0 of the infinite
+// lattice becomes the object's mu0, as in the reference (chiqw reads it); the
+// engine's finite-lattice mu0 for the TPSC stages is not changed
+void green0::find_mu_inf_syst() {
+    double mu;
+    if (!ctx_ || tpsc_mu0_infinite(ctx_, &mu, NULL) != TPSC_OK) {
+        cout << "mu0 non trouve\n";
+        return;
+    }
+    mu0 = mu;
+    cout << "mu0 du systeme infini: " << mu0 << endl;
+}
+
+// chi0::chiqw (src/chi0.cpp:211-276): chi0(q, i w_n) of the infinite lattice,
+// q = (qx, par[0]), w_n = par[1], at the object's mu0
+double chi0::chiqw(double qx, double par[]) {
+    double qw[3] = {qx, par[0], par[1]}, out = 0.0;
+    if (ctx_) check(tpsc_chi0_infinite(ctx_, mu0, 1, qw, 0, &out, NULL), "chiqw");
+    return out;
+}
+
+// chi0::chiqw_discret (src/chi0.cpp:1587-1612): the same sum on this object's
+// nq0 x nq0 lattice at q = 2 pi q[] / nq0, w_n = 2 n pi T
+double chi0::chiqw_discret(int *q, int n) {
+    const int nq0 = 2 * (nbq - 1);
+    const double pi = acos(-1.0);
+    double qw[3] = {q[0] * 2 * pi / nq0, q[1] * 2 * pi / nq0, 2 * n * pi * tem}, out = 0.0;
+    if (ctx_) check(tpsc_chi0_infinite(ctx_, mu0, 1, qw, nq0, &out, NULL), "chiqw_discret");
+    return out;
+}
+
+// chi0::calc_chi0_qlims (src/chi0.cpp:157-209): the infinite lattice's chi0 at
+// w_n = 2 n pi T on the q grid from (qlims[0], qlims[1]) to (qlims[2],
+// qlims[3]), Nq points per direction, qy <= qx; all points in one call
+void chi0::calc_chi0_qlims(int n, double qlims[], int Nq[]) {
+    find_mu_inf_syst();
+    const double pi = acos(-1.0), eps = numeric_limits<double>::epsilon();
+    const double wn = 2 * n * pi * tem;
+    const int Nqx = Nq[0], Nqy = Nq[1];
+    const double dqx = Nqx > 1 ? (qlims[2] - qlims[0]) / (Nqx - 1) : 0.0;
+    const double dqy = Nqy > 1 ? (qlims[3] - qlims[1]) / (Nqy - 1) : 0.0;
+    char name[200];
+    sprintf(name, "./chi0_q_%5.3f_%5.3f_%5.3f_%7.5f_%7.5f_%7.5f_%7.5f_%7.5f_%7.5f_%d_%d_%d.dat", tp, tpp, t3, density, tem,
+            qlims[0] / pi, qlims[1] / pi, qlims[2] / pi, qlims[3] / pi, Nqx, Nqy, n);
+    cout << "calcul de chi0(q,wn=" << wn << ")" << '\n';
+    std::vector<double> qw;
+    double qx = qlims[0];
+    for (int jx = 1; qx <= qlims[2] + eps; jx++) {
+        double qy = qlims[1];
+        for (int jy = 1; qy <= qlims[3] + eps && qy <= qx + eps; jy++) {
+            qw.insert(qw.end(), {qx, qy, wn});
+            qy = qlims[1] + jy * dqy;
+            if (dqy == 0.0) break;  // the reference would repeat this point forever
+        }
+        qx = qlims[0] + jx * dqx;
+        if (dqx == 0.0) break;
+    }
+    const int np = (int)qw.size() / 3;
+    std::vector<double> chi(np);
+    if (!np || !ctx_ || !check(tpsc_chi0_infinite(ctx_, mu0, np, qw.data(), 0, chi.data(), NULL), "calc_chi0_qlims"))
+        return;
+    fstream file;
+    file.open(name, ios::out);
+    file << setiosflags(ios::left) << setprecision(16);
+    for (int p = 0; p < np; p++) file << setw(25) << qw[3 * p] << setw(25) << qw[3 * p + 1] << chi[p] << '\n';
+    file.close();
+}
+
 // chi0::save_chi (src/chi0.cpp:61-95): the chi0 binary of the current grid
 void chi0::save_chi() {
     if (!ctx_) return;

@@ -67,6 +67,7 @@ public:
     void set_density(double n);
 
 protected:
+    void find_mu_inf_syst();
     bool check(int status, const char *what) const;
     void set_model();
     virtual void model_changed() {}  // after set_model: the derived classes' own model state
@@ -89,6 +90,9 @@ public:
     void calc_chiqw_FFT_spline(int nq0, int nw0);
     void traceChi0();
     void save_chi();
+    double chiqw(double qx, double par[]);
+    double chiqw_discret(int *q, int n);
+    void calc_chi0_qlims(int n, double qlims[], int Nq[]);
 
 protected:
     void loadChi0();
