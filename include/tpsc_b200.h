@@ -117,6 +117,16 @@ int tpsc_set_nsr(tpsc_ctx *ctx, double nsr);
  * capture that fails leaves the context on direct launches. */
 int tpsc_set_graph_mode(tpsc_ctx *ctx, int mode);
 
+/* Tilings of the three tau transforms (chi0, V, Sigma), process-wide per
+ * Nw0: tile 0 one column pair per CTA (two CTAs per SM, the default), 1 four
+ * columns per CTA.  tpsc_tune_tau_tiles times both on the current grid after
+ * a solve (reps runs each) and keeps the faster of each; ms (may be NULL)
+ * receives the mean times, ms[2 kind + tile].  The transforms run in place,
+ * so the next solve recomputes the grid's stages.  tpsc_set_tau_tile sets
+ * one tiling (kind 0 chi0, 1 V, 2 Sigma). */
+int tpsc_tune_tau_tiles(tpsc_ctx *ctx, int reps, double ms[6]);
+int tpsc_set_tau_tile(int kind, int nw0, int tile);
+
 /* out = {captures, replays, kernels in the current graph, 1 if a capture
  * failed and graphs are off}. */
 int tpsc_graph_stats(tpsc_ctx *ctx, long long out[4]);
@@ -359,9 +369,11 @@ int tpsc_batch_set_graph_mode(tpsc_batch *b, int mode);
 int tpsc_batch_solve(tpsc_batch *b, int form, int npts, const double *params, double *results, int *status,
                      double *ms);
 /* The tuner: one untimed pass of the sample (allocating every shape on
- * max_streams contexts), then the sample timed on 1, 2, 4, ... <= max_streams
- * contexts; later tpsc_batch_solve calls use the fastest count.  ms (may be
- * NULL) receives each count's time, floor(log2(max_streams)) + 1 entries. */
+ * max_streams contexts), the tau transforms' tiling of every shape
+ * (tpsc_tune_tau_tiles on its first good point), then the sample timed on 1,
+ * 2, 4, ... <= max_streams contexts; later tpsc_batch_solve calls use the
+ * fastest count.  ms (may be NULL) receives each count's time,
+ * floor(log2(max_streams)) + 1 entries. */
 int tpsc_batch_tune(tpsc_batch *b, int form, int npts, const double *params, int max_streams, double *ms);
 /* The parameter-sweep workload: npts rows in the tpsc_batch_solve layout
  * from std::mt19937_64(seed), drawn per point in this order: nk0 uniform in

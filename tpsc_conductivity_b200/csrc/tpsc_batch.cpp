@@ -19,6 +19,7 @@
 #include <cmath>
 #include <mutex>
 #include <random>
+#include <set>
 #include <string>
 #include <thread>
 #include <vector>
@@ -227,6 +228,19 @@ int tpsc_batch_tune(tpsc_batch *b, int form, int npts, const double *params, int
     // every count)
     int rc = run_points(b, max_streams, form, npts, params, res.data(), st.data(), nullptr, nullptr);
     if (rc) return rc;
+    // the tau transforms' tiling of every shape, timed on its first good point
+    std::set<std::pair<int, int>> tuned;
+    tpsc_ctx *c0 = b->ctxs[0];
+    for (int i = 0; i < npts; ++i) {
+        const double *p = params + (size_t)i * kParamCols;
+        const std::pair<int, int> shape((int)p[0], (int)p[1]);
+        if (st[i] || tuned.count(shape)) continue;
+        tuned.insert(shape);
+        tpsc_set_form(c0, form);
+        if (tpsc_set_model(c0, shape.first, shape.second, p[2], p[3], p[4], p[5], p[6], p[7]) == TPSC_OK &&
+            tpsc_solve(c0) == TPSC_OK)
+            tpsc_tune_tau_tiles(c0, 3, nullptr);
+    }
     double best = 0.0;
     int best_n = 1, k = 0;
     for (int n = 1; n <= max_streams; n *= 2, ++k) {

@@ -276,10 +276,11 @@ struct SolveKey {
     int form = -1, cap = -1;
     long long model_id = -1;
     double mu0 = 0.0, nsr = -1.0;
+    long long tiles = -1;  // tau_tiles_version(): the tau transforms' tiling
     bool rsr = true, rmu = true;
     bool operator==(const SolveKey &o) const {
         return form == o.form && cap == o.cap && model_id == o.model_id && mu0 == o.mu0 && nsr == o.nsr &&
-               rsr == o.rsr && rmu == o.rmu;
+               tiles == o.tiles && rsr == o.rsr && rmu == o.rmu;
     }
 };
 
@@ -1213,6 +1214,7 @@ int newton_solve(tpsc_ctx *ctx) {
     key.model_id = ctx->model_id;
     key.mu0 = g->mu0;
     key.nsr = ctx->nsr;
+    key.tiles = tau_tiles_version();
     key.rsr = ctx->roots.reset_sr;
     key.rmu = ctx->roots.reset_mu;
     const unsigned fbit = 1u << (ctx->form & 3);
@@ -2070,6 +2072,60 @@ int tpsc_get_sigma_tau(tpsc_ctx *ctx, int j, double *out) {
     CK(launch_take_row(g->sigt, d.nw0 + 1, j, d.n8, (double *)ctx->stage, ctx->st));
     if ((rc = copy_out(ctx, out, ctx->stage, bytes))) return rc;
     CK(cudaStreamSynchronize(ctx->st));
+    return TPSC_OK;
+}
+
+// The tiling of the three tau transforms for the current grid's Nw0, picked
+// by timing: each transform runs in both tilings (one column pair per CTA,
+// four columns per CTA) reps times on this grid's buffers after one warm-up,
+// and the faster stays (process-wide).  ms[2 kind + tile] receives the mean
+// times (kind 0 chi0, 1 V, 2 Sigma).  The transforms run in place, so the
+// grid's stage results are stale afterwards: the next solve recomputes them.
+int tpsc_tune_tau_tiles(tpsc_ctx *ctx, int reps, double ms[6]) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    Grid *g = ctx->cur;
+    if (!g || !g->have_S) return fail(ctx, TPSC_ERR_STATE, "tune after a solve on the current grid");
+    if (reps < 1 || reps > 100) return fail(ctx, TPSC_ERR_ARG, "need 1 <= reps <= 100");
+    cudaSetDevice(ctx->device);
+    const GridDev &d = g->d;
+    cudaEvent_t a = ctx->ev[0], b = ctx->ev[1];
+    for (int kind = 0; kind < 3; ++kind) {
+        double best = 0.0;
+        int pick = 0;
+        for (int tile = 0; tile < 2; ++tile) {
+            set_tau_tile(kind, d.nw0, tile);
+            auto run = [&]() -> cudaError_t {
+                if (kind == kTauChi0) return launch_chi0_tau(d, g->chiq, g->dchiqt0, g->cinf, g->cinf2, ctx->T, ctx->st);
+                if (kind == kTauVertex) return launch_vertex_tau(d, g->V, g->chirt, ctx->U, ctx->dres, ctx->st);
+                return launch_sigma_tau(d, g->sigt, g->dS, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->T, ctx->st);
+            };
+            CK(run());
+            CK(cudaEventRecord(a, ctx->st));
+            for (int r = 0; r < reps; ++r) CK(run());
+            CK(cudaEventRecord(b, ctx->st));
+            CK(cudaEventSynchronize(b));
+            float t = 0;
+            CK(cudaEventElapsedTime(&t, a, b));
+            const double mean = t / reps;
+            if (ms) ms[2 * kind + tile] = mean;
+            if (tile == 0 || mean < best) {
+                best = mean;
+                pick = tile;
+            }
+        }
+        set_tau_tile(kind, d.nw0, pick);
+    }
+    g->have_chi0 = g->have_V = g->have_S = g->have_mom = g->have_U = false;
+    return TPSC_OK;
+}
+
+// the tiling of one tau transform for one Nw0 (kind 0 chi0, 1 V, 2 Sigma;
+// tile 0 one column pair per CTA, 1 four columns per CTA)
+int tpsc_set_tau_tile(int kind, int nw0, int tile) {
+    if (kind < 0 || kind > 2 || tile < 0 || tile > 1 || !supported_grid(8, nw0))
+        return fail(nullptr, TPSC_ERR_ARG, "need kind 0..2, tile 0..1 and a supported Nw0");
+    set_tau_tile(kind, nw0, tile);
     return TPSC_OK;
 }
 

@@ -29,6 +29,21 @@ namespace tpsc {
 
 // kernels launched by this library (all contexts), for the instrumentation ABI
 static std::atomic<long long> g_launches{0};
+
+// tiling of the three tau transforms per N (process-wide; tpsc_tune_tau_tiles):
+// 0 one column pair per CTA (k_*_tau2), 1 four columns per CTA (k_*_tau)
+static std::atomic<int> g_tau_tile[3][13];
+static std::atomic<long long> g_tau_tiles_version{0};
+static int tile_index(int n) {
+    int k = 0;
+    while ((1 << k) < n && k < 12) ++k;
+    return k;
+}
+int tau_tile(int kind, int n) { return g_tau_tile[kind][tile_index(n)].load(std::memory_order_relaxed); }
+void set_tau_tile(int kind, int n, int tile) {
+    if (g_tau_tile[kind][tile_index(n)].exchange(tile) != tile) g_tau_tiles_version.fetch_add(1);
+}
+long long tau_tiles_version() { return g_tau_tiles_version.load(); }
 // the same count for the calling host thread (kernels in one stream capture)
 static thread_local long long t_launches = 0;
 cudaError_t launched(int n) {
@@ -1627,10 +1642,12 @@ struct RunChi0Tau {
                            double T, cudaStream_t st) {
         cudaError_t e;
         if constexpr (N / 16 <= 256) {
-            const size_t sm = Tau2Smem<N>::bytes;
-            if ((e = set_smem(k_chi0_tau2<N>, sm)) != cudaSuccess) return e;
-            k_chi0_tau2<N><<<g->n8p / 2, 256, sm, st>>>(chiq, dchiqt0, cinf, cinf2, g->spl_half, g->tw_w, T, g->n8);
-            return launched();
+            if (tau_tile(kTauChi0, N) == 0) {
+                const size_t sm = Tau2Smem<N>::bytes;
+                if ((e = set_smem(k_chi0_tau2<N>, sm)) != cudaSuccess) return e;
+                k_chi0_tau2<N><<<g->n8p / 2, 256, sm, st>>>(chiq, dchiqt0, cinf, cinf2, g->spl_half, g->tw_w, T, g->n8);
+                return launched();
+            }
         }
         const size_t sm = TauSmem<N>::bytes(N / 2 + 1);
         e = set_smem(k_chi0_tau<N>, sm);
@@ -1646,10 +1663,12 @@ struct RunVertexTau {
                            cudaStream_t st) {
         cudaError_t e;
         if constexpr (N / 16 <= 256) {
-            const size_t sm = Tau2Smem<N>::bytes;
-            if ((e = set_smem(k_vertex_tau2<N>, sm)) != cudaSuccess) return e;
-            k_vertex_tau2<N><<<g->n8p / 2, 256, sm, st>>>(Vr, chirt, g->tw_w, U, Usc, g->n8);
-            return launched();
+            if (tau_tile(kTauVertex, N) == 0) {
+                const size_t sm = Tau2Smem<N>::bytes;
+                if ((e = set_smem(k_vertex_tau2<N>, sm)) != cudaSuccess) return e;
+                k_vertex_tau2<N><<<g->n8p / 2, 256, sm, st>>>(Vr, chirt, g->tw_w, U, Usc, g->n8);
+                return launched();
+            }
         }
         const size_t sm = TauSmem<N>::bytes(N / 2 + 1);
         e = set_smem(k_vertex_tau<N>, sm);
@@ -1664,12 +1683,14 @@ struct RunSigmaTau {
                            double *s4, double *sinf, double T, cudaStream_t st) {
         cudaError_t e;
         if constexpr (N / 16 <= 256) {
-            // one pair per CTA, two CTAs per SM
-            const size_t sm = Tau2Smem<N>::bytes;
-            if ((e = set_smem(k_sigma_tau2<N>, sm)) != cudaSuccess) return e;
-            k_sigma_tau2<N><<<g->n8p / 2, 256, sm, st>>>(sigt, dS, S, s2, s3, s4, sinf, g->spl_full, g->tw_w,
-                                                         g->ht_w, T, g->n8, g->n8p);
-            return launched();
+            if (tau_tile(kTauSigma, N) == 0) {
+                // one pair per CTA, two CTAs per SM
+                const size_t sm = Tau2Smem<N>::bytes;
+                if ((e = set_smem(k_sigma_tau2<N>, sm)) != cudaSuccess) return e;
+                k_sigma_tau2<N><<<g->n8p / 2, 256, sm, st>>>(sigt, dS, S, s2, s3, s4, sinf, g->spl_full, g->tw_w,
+                                                             g->ht_w, T, g->n8, g->n8p);
+                return launched();
+            }
         }
         const size_t sm = TauSmem<N>::bytes(N + 1);
         if ((e = set_smem(k_sigma_tau<N>, sm)) != cudaSuccess) return e;

@@ -253,6 +253,14 @@ cudaError_t launch_gather(const GatherPieces &p, unsigned *dst, int blocks, cuda
 // up to four host values stored to dst[0..n) in stream order (no copy engine)
 cudaError_t launch_store(double *dst, const double *v, int n, cudaStream_t st);
 
+// tiling of the tau transforms (chi0, V, Sigma) per N, process-wide: 0 one
+// column pair per CTA (the default), 1 four columns per CTA; the version
+// counts the changes
+constexpr int kTauChi0 = 0, kTauVertex = 1, kTauSigma = 2;
+int tau_tile(int kind, int n);
+void set_tau_tile(int kind, int n, int tile);
+long long tau_tiles_version();
+
 // kernels launched by the library so far
 long long launches_total();
 // kernels launched (or captured) by the calling host thread so far
