@@ -205,13 +205,16 @@ def our_arm(a, world, rank, local_rank):
         the library stream after an L2 flush; returns total ms (max over
         ranks), kernels launched, the clock record, scalars and stage times."""
         g.set_form(form)
-        for _ in range(a.warmup):
-            g.solve()
-        torch.cuda.synchronize()
-        barrier(world)
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
-        l0 = launches()
+        # the clock sampler starts before the warm-up so that it is running
+        # (nvidia-smi takes a moment to start) when the timed steps begin
         with ClockSampler(dev) as clk:
+            for _ in range(a.warmup):
+                g.solve()
+            torch.cuda.synchronize()
+            barrier(world)
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(a.steps)]
+            l0 = launches()
             torch.cuda.synchronize()
             for i in range(a.steps):
                 flush.zero_()
@@ -223,6 +226,16 @@ def our_arm(a, world, rank, local_rank):
         n = launches() - l0
         t = allreduce_max(sum(s.elapsed_time(e) for s, e in ev), world, dev)
         return t, n, clk.summary(), g.scalars(), g.stage_times()
+
+    # ---- the tau transforms' tiling for this shape, picked by timing both
+    # (tpsc_tune_tau_tiles: one column pair or four columns per CTA) ----------
+    g.set_form(_lib.FORM_NEWTON | _lib.FORM_MIXED)
+    g.solve()
+    tile_ms = np.zeros(6)
+    ctx.call("tpsc_tune_tau_tiles", 5, tile_ms.ctypes.data_as(C.POINTER(C.c_double)))
+    tau_tiles = {kind: {"pair_ms": float(tile_ms[2 * k]), "quad_ms": float(tile_ms[2 * k + 1]),
+                        "picked": "pair" if tile_ms[2 * k] <= tile_ms[2 * k + 1] else "quad"}
+                 for k, kind in enumerate(("chi0_tau", "vertex_tau", "sigma_tau"))}
 
     # ---- device-resident solves: the FP64 drop-in with the reference's root
     # searches, the FP64 Newton form, then mixed precision + Newton (the
@@ -347,6 +360,7 @@ def our_arm(a, world, rank, local_rank):
                              "same kernels and arguments as direct launches); the FP64 drop-in with the "
                              "reference's root searches runs direct launches with its host round trips"},
         "solve_graph": graph_stats,
+        "tau_tiles": tau_tiles,
         "forms": {"mixed_newton": {"solves_per_s": value, "ms_per_step": ms / a.steps, "stage_ms": stages,
                                    "max_rel_dSigma_vs_fp64": dsigma},
                   "fp64_newton": {"solves_per_s": value_n64, "ms_per_step": ms_n64 / a.steps,
