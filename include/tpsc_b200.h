@@ -313,6 +313,10 @@ int tpsc_run_kernel(tpsc_ctx *ctx, int which);
  * grid: every distinct input read once plus every output written once. */
 int tpsc_kernel_bytes(tpsc_ctx *ctx, int which, double *bytes);
 
+/* Instrumentation: the device's FMA throughput (bits 64 or 32), TFLOP/s, by
+ * a kernel of independent FMA chains on every SM -- the arithmetic ceiling of
+ * the transform kernels' roofline beside the HBM copy bandwidth. */
+int tpsc_fma_peak(int bits, double *tflops);
 /* Number of CUDA kernels the library has launched (all contexts) since it was
  * loaded. */
 int tpsc_launch_count(tpsc_ctx *ctx, long long *count);

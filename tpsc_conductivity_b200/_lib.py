@@ -76,6 +76,7 @@ SIGNATURES = [
     ("tpsc_run_kernel", C.c_int, [C.c_void_p, C.c_int]),
     ("tpsc_kernel_bytes", C.c_int, [C.c_void_p, C.c_int, _dp]),
     ("tpsc_launch_count", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    ("tpsc_fma_peak", C.c_int, [C.c_int, _dp]),
     ("tpsc_pade_sigma", C.c_int, [C.c_void_p, _ip, C.c_int, _dp, C.c_int, C.c_int, _dp, _dp]),
     ("tpsc_gwn_local", C.c_int, [C.c_void_p, _dp]),
     ("tpsc_set_form", C.c_int, [C.c_void_p, C.c_int]),
