@@ -627,13 +627,20 @@ int read_result(tpsc_ctx *ctx, int count, double *out, const double *src = nullp
 int grid_set_model(tpsc_ctx *ctx, Grid *g) {
     GridDev &d = g->d;
     g->ek_host.assign((size_t)d.nbk * d.nbk, 0.0);
+    // dispk on the grid from tables of cos(k) and cos(2k): the same values
+    // and the same expression, one pair of cosines per index instead of ten
+    // per point
+    std::vector<double> c1(d.nbk), c2(d.nbk);
     for (int l = 0; l < d.nbk; ++l) {
-        const double kx = l * PI / (d.nbk - 1);
-        for (int m = 0; m < d.nbk; ++m) {
-            const double ky = m * PI / (d.nbk - 1);
-            g->ek_host[m + l * d.nbk] = dispk(kx, ky, ctx->tp, ctx->tpp, ctx->t3);
-        }
+        const double k = l * PI / (d.nbk - 1);
+        c1[l] = std::cos(k);
+        c2[l] = std::cos(2 * k);
     }
+    const double tp = ctx->tp, tpp = ctx->tpp, t3 = ctx->t3;
+    for (int l = 0; l < d.nbk; ++l)
+        for (int m = 0; m < d.nbk; ++m)
+            g->ek_host[m + l * d.nbk] = -2.0 * (c1[l] + c1[m]) - 4.0 * tp * c1[l] * c1[m] -
+                                        2.0 * tpp * (c2[l] + c2[m]) - 4 * t3 * (c2[l] * c1[m] + c2[m] * c1[l]);
     std::vector<double> eo(d.n8), er(d.n8, 0.0);
     for (int l = 0; l < d.nbk; ++l)
         for (int m = 0; m <= l; ++m) eo[m + l * (l + 1) / 2] = g->ek_host[m + l * d.nbk];
