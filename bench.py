@@ -278,16 +278,24 @@ def our_arm(a, world, rank, local_rank):
             g2.scalars()
         g2.wait_copies(join_stream=True)
 
-    e2e_steps(2)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    e2e_steps(a.steps)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    g.wait_copies()
-    ms2 = allreduce_max(e0.elapsed_time(e1), world, dev)
-    e2e = world * a.steps / (ms2 / 1e3)
+    # timed with direct launches (graph mode 1: every step is a new model) and
+    # with every solve captured and its graph updated in place (mode 2); the
+    # faster is the headline, both are reported
+    e2e_modes = {}
+    for mode in (1, 2):
+        g.set_graph_mode(mode)
+        e2e_steps(2)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_steps(a.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        g.wait_copies()
+        e2e_modes[mode] = world * a.steps / (allreduce_max(e0.elapsed_time(e1), world, dev) / 1e3)
+    g.set_graph_mode(1)
+    e2e_mode = max(e2e_modes, key=e2e_modes.get)
+    e2e = e2e_modes[e2e_mode]
 
     # ---- per-kernel timing (stages re-launched alone, in order, as the
     # mixed + Newton solve runs them) -------------------------------------------
@@ -374,7 +382,8 @@ def our_arm(a, world, rank, local_rank):
                                                         for k in ("Usp", "Uch", "mu")),
                   "max_rel_diff_roots_mixed": max(abs(sc[k] - sc_ref[k]) / abs(sc_ref[k])
                                                   for k in ("Usp", "Uch", "mu"))},
-        "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "graph_mode": e2e_mode, "solves_per_s_by_graph_mode": {str(k): v for k, v in e2e_modes.items()}},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                      "algorithmic_bytes": kb.value, "launch_ms": per_ms[dom]},
