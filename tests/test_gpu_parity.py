@@ -7,7 +7,7 @@ Tolerances (relative to the array's max magnitude, or to the scalar):
   Usp, Uch, double occupancy, mu, Sigma_inf vs reference   1e-9
   S (1/z^4 coefficient) vs oracle                           1e-8  (its
       high-frequency end is an alternating sum of spline third derivatives)
-The north-star bound is 1e-7 at FP64."""
+Every one of these is within the 1e-7 FP64 parity bound the path is held to."""
 import numpy as np
 import pytest
 
