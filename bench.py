@@ -518,13 +518,22 @@ def extra_configs():
         "max_rel_err_sigma_iqn_mixed_vs_fp64": float(np.max(np.abs(sig_m - sig_d)) / np.max(np.abs(sig_d))),
         "pade": "sigma(w) on 2000 w in [0, 10] from 64 bosonic nodes", "pade_finite": bool(np.all(np.isfinite(pade_m)))}
     # config 4
-    g4 = Green(128, 2048, 0.85, 0.1, 0.1, (-0.2, 0.0, 0.0, 4.0))
+    g4 = CondOpt(128, 2048, 0.85, 0.1, 0.1, (-0.2, 0.0, 0.0, 4.0))
     g4.set_form(_lib.FORM_NEWTON)
     g4.find_Usp_Uch_grid(128, 2048)
     g4.sumrule_tangents()
     J, t4 = timed(g4.sumrule_tangents)
-    out["c4_l128_w2048_sensitivities"] = {"ms": t4, "d_dU": J["U"], "d_dmu": J["mu"], "d_dtp": J["tp"],
-                                          "checked": "central differences, tests/test_gpu_tangent.py"}
+    # sigma(iq1): central differences of full FP64 solves (no tangent of the
+    # Sigma and chi_jj stages yet)
+    g4.solve()
+    g4.sigma_qn_sensitivities(1)
+    (ds4, dD4), t4s = timed(lambda: g4.sigma_qn_sensitivities(1))
+    out["c4_l128_w2048_sensitivities"] = {
+        "ms": t4, "d_dU": J["U"], "d_dmu": J["mu"], "d_dtp": J["tp"],
+        "checked": "central differences, tests/test_gpu_tangent.py",
+        "sigma_iq1": {"ms": t4s, "d_dU": float(ds4[0, 0]), "d_dmu": float(ds4[1, 0]), "d_dtp": float(ds4[2, 0]),
+                      "method": "central differences of six FP64 Newton solves + chi_jj, h = 1e-5, "
+                                "base point solved again; tests/test_gpu_sigma_fd.py"}}
     out["timing"] = "host wall clock around each call after a warm-up run, device idle at both ends"
     return out
 

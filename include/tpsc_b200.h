@@ -270,6 +270,16 @@ int tpsc_get_chijj(tpsc_ctx *ctx, double *chijj1, double *chijj2, double *kx0, d
  * chi_jj = chijj1 + chijj2 (sigma, with vertex correction) and chi_jj =
  * chijj1 (sigma_bubble).  nq <= Nw0/2; either pointer may be NULL. */
 int tpsc_sigma_iqn(tpsc_ctx *ctx, int nq, double *sigma, double *sigma_bubble);
+/* Sensitivities of sigma(iq_n), n = 1..nq (with vertex correction, one angle
+ * bin), and of the double occupancy D to {U, mu, t'} by central differences of
+ * full FP64 Newton-form device solves with the steps h[3] (no counterpart in
+ * the reference): dsigma[p * nq + n - 1] = d sigma(iq_n) / d theta_p, dD[p]
+ * (may be NULL).  mu is the shift of mu0 at fixed n (tpsc_set_mu_shift), t'
+ * moves at fixed n.  Six solves + tpsc_chijj, then the model, mu shift and
+ * form are restored and the base point solved again.  The forward tangents
+ * of the sum-rule stage (tpsc_sumrule_tangents) give dD exactly; a tangent
+ * of the Sigma and chi_jj stages is not built, so this is the sigma path. */
+int tpsc_sigma_iqn_fd(tpsc_ctx *ctx, int nq, const double h[3], double *dsigma, double dD[3]);
 /* Continued-fraction Pade continuation of sigma(iq_n), n = 1..Nn, and of
  * sigma_bubble to z = w + i eta for the Nw real frequencies w:
  * out [2][Nw] complex interleaved (sigma, then sigma_bubble). */

@@ -303,6 +303,17 @@ class CondOpt(Green):
         self.ctx.call("tpsc_sigma_iqn", nq, _dptr(s), _dptr(sb))
         return s, sb
 
+    def sigma_qn_sensitivities(self, nq=1, h=(1e-5, 1e-5, 1e-5)):
+        """d sigma(iq_n)/d(U, mu, t') for n = 1..nq and dD/d(U, mu, t') by
+        central differences of full FP64 device solves (steps h; mu a shift of
+        mu0 at fixed n, t' at fixed n).  The context is solved again at its
+        own parameters afterwards.  Returns (dsigma [3, nq], dD [3])."""
+        steps = np.ascontiguousarray(np.asarray(h, dtype=np.float64).reshape(3))
+        ds, dD = np.zeros((3, int(nq))), np.zeros(3)
+        self.ctx.call("tpsc_sigma_iqn_fd", int(nq), _dptr(steps), _dptr(ds), _dptr(dD))
+        self._nbins = 1
+        return ds, dD
+
     def sigma_pade(self, w, Nn=64, eta=0.0):
         """Pade continuation of sigma(iq_n), n = 1..Nn, to w + i eta:
         (sigma(w), sigma_bubble(w)) complex arrays."""

@@ -2371,6 +2371,54 @@ int tpsc_sigma_iqn(tpsc_ctx *ctx, int nq, double *sigma, double *sigma_bubble) {
     return TPSC_OK;
 }
 
+// d sigma(iq_n) / d{U, mu, t'} and d D / d{U, mu, t'} by central differences
+// of full device solves (FP64 Newton form), each followed by tpsc_chijj with
+// one angle bin and tpsc_sigma_iqn; mu is the shift of mu0 at fixed n
+// (tpsc_set_mu_shift), t' moves at fixed n.  The model, mu shift and form are
+// put back and the base point solved again, so the context ends as a plain
+// solve + tpsc_chijj(1) of its model would leave it.
+int tpsc_sigma_iqn_fd(tpsc_ctx *ctx, int nq, const double h[3], double *dsigma, double dD[3]) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    if (!h || !dsigma) return fail(ctx, TPSC_ERR_ARG, "null step or output");
+    for (int p = 0; p < 3; ++p)
+        if (!(h[p] > 0.0) || !std::isfinite(h[p])) return fail(ctx, TPSC_ERR_ARG, "steps must be positive");
+    if (nq < 1 || nq > ctx->Nw0 / 2) return fail(ctx, TPSC_ERR_ARG, "need 1 <= nq <= Nw0/2");
+    if (ctx->nk0 < 8) return fail(ctx, TPSC_ERR_ARG, "need nk0 >= 8");
+    const int nk0 = ctx->nk0, Nw0 = ctx->Nw0, form = ctx->form;
+    const double n = ctx->n, T = ctx->T, tp = ctx->tp, tpp = ctx->tpp, t3 = ctx->t3, U = ctx->U;
+    const double dmu0 = ctx->mu_shift;
+    std::vector<double> sp(nq), sm(nq);
+    auto point = [&](double Uv, double dmu, double tpv, double *sig, double *D) -> int {
+        int r = tpsc_set_model(ctx, nk0, Nw0, n, T, tpv, tpp, t3, Uv);
+        if (!r) r = tpsc_set_mu_shift(ctx, dmu);
+        if (!r) r = tpsc_solve(ctx);
+        if (!r) r = tpsc_chijj(ctx, 1);
+        if (!r && sig) r = tpsc_sigma_iqn(ctx, nq, sig, nullptr);
+        if (!r && D) *D = ctx->scal[TPSC_S_DBLOCC];
+        return r;
+    };
+    rc = tpsc_set_form(ctx, form & ~TPSC_FORM_MIXED);
+    for (int p = 0; p < 3 && !rc; ++p) {
+        double Dp = 0.0, Dm = 0.0;
+        const double e[3] = {p == 0 ? h[0] : 0.0, p == 1 ? h[1] : 0.0, p == 2 ? h[2] : 0.0};
+        rc = point(U + e[0], dmu0 + e[1], tp + e[2], sp.data(), &Dp);
+        if (!rc) rc = point(U - e[0], dmu0 - e[1], tp - e[2], sm.data(), &Dm);
+        if (rc) break;
+        for (int k = 0; k < nq; ++k) dsigma[(size_t)p * nq + k] = (sp[k] - sm[k]) / (2.0 * h[p]);
+        if (dD) dD[p] = (Dp - Dm) / (2.0 * h[p]);
+    }
+    // the base point, whatever happened above; the first error is the one reported
+    const std::string err = rc ? ctx->err : std::string();
+    tpsc_set_form(ctx, form);
+    const int rc2 = point(U, dmu0, tp, nullptr, nullptr);
+    if (rc) {
+        ctx->err = err;
+        return rc;
+    }
+    return rc2;
+}
+
 int pade_batch(tpsc_ctx *ctx, int nf, int Nn, const double *x, const double *y, int Nz, const double *z,
                double *out) {
     const size_t bx = (size_t)nf * Nn * sizeof(double2), bz = (size_t)Nz * sizeof(double2),
