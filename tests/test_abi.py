@@ -86,3 +86,27 @@ def test_batch_create_without_device_fails_cleanly(lib):
     lib.tpsc_batch_create.restype = ctypes.c_void_p
     st = ctypes.c_int(-1)
     assert not lib.tpsc_batch_create(0, 4, ctypes.byref(st)) and st.value != 0
+
+
+def test_model_calls_reject_a_null_context(lib):
+    """Entry points that need a model return TPSC_ERR_ARG (1) for a NULL
+    context before any device call, with the reason in tpsc_last_error(NULL)
+    (a null context or argument)."""
+    import numpy as np
+
+    from tpsc_conductivity_b200 import _lib
+
+    lib.tpsc_last_error.restype = ctypes.c_char_p
+    d = np.zeros(64)
+    p = d.ctypes.data_as(ctypes.c_void_p)
+    calls = {
+        "tpsc_solve": (),
+        "tpsc_sumrule_tangents": (p,),
+        "tpsc_sumrule_vjp": (p, p),
+        "tpsc_sigma_iqn": (ctypes.c_int(1), p, p),
+        "tpsc_sigma_iqn_fd": (ctypes.c_int(1), p, p, p),
+        "tpsc_chijj": (ctypes.c_int(1),),
+    }
+    for name, args in calls.items():
+        assert getattr(lib, name)(None, *args) == _lib.ERR_ARG, name
+        assert b"null" in lib.tpsc_last_error(None), name
