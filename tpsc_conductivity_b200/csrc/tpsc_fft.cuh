@@ -183,6 +183,50 @@ __device__ __forceinline__ void group_sync(int grp) {
     }
 }
 
+// The twiddle w_m = exp(-2 pi i m / N) itself, from a FP64 table.
+template <bool SMEM>
+__device__ __forceinline__ double2 tw_value(const double2 *__restrict__ tw, int m) {
+    return SMEM ? tw[m] : __ldg(&tw[m]);
+}
+template <bool SMEM>
+__device__ __forceinline__ double2 tw_value(const TwoLevelTw *__restrict__ tw, int m) {
+    return cmul(tw->hi[m >> 6], tw->lo[m & 63]);
+}
+
+// v[q] *= w^q (conj(w)^q for SIGN > 0), q = 1..15, w = w_step, in FP64: the
+// table gives w, w^2, w^4 and w^8, and every other power is a product of at
+// most four of them (a few ulp), so a radix-16 butterfly reads 4 twiddles
+// instead of 15.  The table entries read are w_{step q mod N}, q = 1, 2, 4, 8.
+template <int N, int SIGN, bool SMEM, class TW>
+__device__ __forceinline__ void twiddle16_powers(double2 *v, const TW *__restrict__ tw, int step) {
+    double2 w1 = tw_value<SMEM>(tw, step & (N - 1)), w2 = tw_value<SMEM>(tw, (2 * step) & (N - 1));
+    double2 w4 = tw_value<SMEM>(tw, (4 * step) & (N - 1)), w8 = tw_value<SMEM>(tw, (8 * step) & (N - 1));
+    if (SIGN > 0) {
+        w1.y = -w1.y;
+        w2.y = -w2.y;
+        w4.y = -w4.y;
+        w8.y = -w8.y;
+    }
+    const double2 w3 = cmul(w2, w1), w5 = cmul(w4, w1), w6 = cmul(w4, w2), w7 = cmul(w4, w3);
+    v[1] = cmul(v[1], w1);
+    v[2] = cmul(v[2], w2);
+    v[3] = cmul(v[3], w3);
+    v[4] = cmul(v[4], w4);
+    v[5] = cmul(v[5], w5);
+    v[6] = cmul(v[6], w6);
+    v[7] = cmul(v[7], w7);
+    v[8] = cmul(v[8], w8);
+    v[9] = cmul(v[9], cmul(w8, w1));
+    v[10] = cmul(v[10], cmul(w8, w2));
+    v[11] = cmul(v[11], cmul(w8, w3));
+    v[12] = cmul(v[12], cmul(w8, w4));
+    v[13] = cmul(v[13], cmul(w8, w5));
+    v[14] = cmul(v[14], cmul(w8, w6));
+    v[15] = cmul(v[15], cmul(w8, w7));
+}
+template <int N, int SIGN, bool SMEM, class TW>
+__device__ __forceinline__ void twiddle16_powers(float2 *, const TW *__restrict__, int) {}
+
 // Loaders / storers for the first and last FFT pass.  `In` returns input
 // element j of the sequence; `Out` receives output element k.
 template <class C>
@@ -224,8 +268,13 @@ __device__ __forceinline__ void stockham_pass(C *x, int t, int Ns, const TW *__r
         if (Ns > 1) {
             // twiddle exp(SIGN 2 pi i k q / (Ns R)) = tw[k q N/(Ns R)] (conjugated for SIGN>0)
             const int step = k * (N / (Ns * R));
+            if constexpr (R == 16 && sizeof(C) == sizeof(double2)) {
+                twiddle16_powers<N, SIGN, SMEM_TW>(&v[u * R], tw, step);
+            } else {
 #pragma unroll
-            for (int q = 1; q < R; ++q) v[u * R + q] = twiddle<SIGN, SMEM_TW>(v[u * R + q], tw, (step * q) & (N - 1));
+                for (int q = 1; q < R; ++q)
+                    v[u * R + q] = twiddle<SIGN, SMEM_TW>(v[u * R + q], tw, (step * q) & (N - 1));
+            }
         }
         C r[R];
 #pragma unroll
