@@ -559,12 +559,14 @@ def barrier(world):
 
 
 def allreduce_max(x, world, dev):
+    """The max of x over the ranks (the replicas' slowest time).  dev: the
+    rank's CUDA device (NCCL), or None for a host tensor (gloo)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+    t = torch.tensor([x], dtype=torch.float64, device="cpu" if dev is None else f"cuda:{dev}")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
