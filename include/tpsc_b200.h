@@ -351,7 +351,10 @@ int tpsc_launch_count(tpsc_ctx *ctx, long long *count);
  * looks up the array's address with that device current; make that first
  * call before any stream capture.  All calls on a device share the array and
  * it keeps the last call's contents; calls whose work overlaps on the GPU
- * race on it, so order them (one stream, or events). */
+ * race on it, so order them (one stream, or events).  The address is looked
+ * up once per device and kept for the life of the process: after a device
+ * reset (cudaDeviceReset) the library's device image may load elsewhere, so
+ * a process that resets a device must not call this entry point again. */
 int tpsc_sumrule_noalloc(const double *chiqw, const double *chi0_inf, const double *chi0_inf2, int nk0, int Nw0,
                          double T, int channel, double Uv, double *out, void *stream);
 

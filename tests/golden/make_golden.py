@@ -1,7 +1,8 @@
 """Regenerate the golden fixtures in this folder from the reference itself.
 
 Runs ``oracle/_ref/tpsc_ref_probe`` -- the UNMODIFIED reference sources
-compiled by ``oracle/ref/Makefile`` (``make -C oracle/ref``) -- on a set of
+compiled by ``oracle/ref/Makefile`` (``TPSC_REFERENCE_SRC=<checkout>/src make -C
+oracle/ref``) -- on a set of
 small lattices and stores what it computed as ``<name>.npz``.  Needs the
 reference checkout to build the probe; the fixtures themselves travel with the
 repository and are all the tests read.
@@ -192,7 +193,7 @@ def main():
     ap.add_argument("--only", nargs="*")
     a = ap.parse_args()
     if not os.path.exists(PROBE):
-        raise SystemExit("build the reference probe first: make -C oracle/ref")
+        raise SystemExit("build the reference probe first: TPSC_REFERENCE_SRC=<reference>/src make -C oracle/ref")
     for name, spec in CASES.items():
         if a.only and name not in a.only:
             continue

@@ -7,16 +7,21 @@ callbacks that forbid allocation, solver loops that must not synchronise the
 device through cudaMalloc/cudaFree).  Its partial sums live in a fixed device
 array shared by all calls, so it is called twice in a row here: a second call
 must not see the first call's leftovers.  This file is collected last so a
-run that stops at the first failure has already run every other test."""
+run that stops at the first failure has already run every other test.
+
+The argument checks return before any device call, so they also run without
+a GPU."""
 import numpy as np
 import pytest
 
 from conftest import load_golden
 
-pytestmark = pytest.mark.gpu
 
-
-@pytest.mark.parametrize("name", ["l32_w256_u4_tp", "l64_w1024_u4"])
+# l256_w4096_u4 is the largest lattice the fixed array accepts: N8 = 8385
+# octant points in 2097 of its 2100 partial-sum slots, the arrival counter
+# right behind them
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["l32_w256_u4_tp", "l64_w1024_u4", "l256_w4096_u4"])
 def test_noalloc_sumrule_matches_context_entry_point(name):
     import torch
 
@@ -49,6 +54,7 @@ def test_noalloc_sumrule_matches_context_entry_point(name):
             out.fill_(float("nan"))
 
 
+@pytest.mark.gpu
 def test_noalloc_rejects_lattices_beyond_its_scratch():
     import torch
 
@@ -58,3 +64,38 @@ def test_noalloc_rejects_lattices_beyond_its_scratch():
     dummy = torch.zeros(8, dtype=torch.float64, device="cuda:0")
     p = dummy.data_ptr()
     assert lib.tpsc_sumrule_noalloc(p, p, p, 512, 64, 0.1, 0, 1.0, p, None) == 1  # TPSC_ERR_ARG
+
+
+# (nk0, Nw0, T, channel): each violates one rule; the pointers are never read
+BAD_ARGS = [
+    (512, 64, 0.1, 0),   # beyond the fixed array (nk0 <= 256)
+    (48, 64, 0.1, 0),    # nk0 not a power of two
+    (4, 64, 0.1, 0),     # nk0 below 8
+    (32, 63, 0.1, 0),    # odd Nw0
+    (32, 2, 0.1, 0),     # Nw0 below 4
+    (32, 64, 0.0, 0),    # T <= 0
+    (32, 64, -0.1, 1),
+    (32, 64, float("nan"), 1),
+    (32, 64, 0.1, 2),    # channel neither 0 (spin) nor 1 (charge)
+    (32, 64, 0.1, -1),
+]
+
+
+@pytest.mark.parametrize("nk0,Nw0,T,channel", BAD_ARGS)
+def test_noalloc_rejects_bad_arguments_before_any_device_call(nk0, Nw0, T, channel):
+    from tpsc_conductivity_b200 import _lib
+
+    lib = _lib.load()
+    fake = 256  # a non-null address that the argument checks never dereference
+    assert lib.tpsc_sumrule_noalloc(fake, fake, fake, nk0, Nw0, T, channel, 1.0, fake, None) == 1  # TPSC_ERR_ARG
+
+
+@pytest.mark.parametrize("which", range(4))
+def test_noalloc_rejects_null_pointers(which):
+    from tpsc_conductivity_b200 import _lib
+
+    lib = _lib.load()
+    ptrs = [256, 256, 256, 256]
+    ptrs[which] = None
+    chi, ci, ci2, out = ptrs
+    assert lib.tpsc_sumrule_noalloc(chi, ci, ci2, 32, 64, 0.1, 0, 1.0, out, None) == 1

@@ -31,7 +31,7 @@ def nvcc_path() -> str:
 
 
 def host_compiler() -> list[str]:
-    # prefer the distribution g++ (the image also has a g++ without libgomp under /opt)
+    # prefer the distribution g++ (another g++ on the image comes without libgomp)
     for cand in ("/usr/bin/g++",):
         if os.path.exists(cand):
             return ["-ccbin", cand]

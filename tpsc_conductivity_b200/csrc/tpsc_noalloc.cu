@@ -32,7 +32,9 @@ constexpr int kScratchDoubles = 2 * kMaxBlocks + 2;
 
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-// device address of g_noalloc_scratch, resolved once per device
+// device address of g_noalloc_scratch, resolved once per device and kept
+// for the life of the process (a device reset would leave it stale; the
+// header says that such a process must not call this entry point again)
 constexpr int kMaxDevices = 64;
 double *g_scratch_addr[kMaxDevices] = {};
 std::mutex g_scratch_mu;
