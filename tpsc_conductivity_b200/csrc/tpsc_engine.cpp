@@ -1038,7 +1038,7 @@ int run_self(tpsc_ctx *ctx, bool settle = true) {
     if (g->g_mixed) {
         CK(launch_sigma_boundary(d, (const float *)g->Grt32, g->V, g->dchirt0, g->dG0p, g->mu0, ctx->U, ctx->dres,
                                  g->dS, ctx->st2));
-        CK(launch_sigma_slice(d, (const float *)g->Grt32, g->V, g->sigt, ctx->st));
+        CK(launch_sigma_slice32(d, g->Grt32, g->V, g->sigt, ctx->st));
     } else {
         CK(launch_sigma_boundary(d, (const double *)g->Grt, g->V, g->dchirt0, g->dG0p, g->mu0, ctx->U, ctx->dres,
                                  g->dS, ctx->st2));
@@ -2525,7 +2525,7 @@ int tpsc_run_kernel(tpsc_ctx *ctx, int which) {
         case 4: CK(launch_vertex_tau(d, g->V, g->chirt, ctx->U, ctx->dres, ctx->st)); break;
         case 5:
             if (g->g_mixed)
-                CK(launch_sigma_slice(d, (const float *)g->Grt32, g->V, g->sigt, ctx->st));
+                CK(launch_sigma_slice32(d, g->Grt32, g->V, g->sigt, ctx->st));
             else
                 CK(launch_sigma_slice(d, (const double *)g->Grt, g->V, g->sigt, ctx->st));
             break;

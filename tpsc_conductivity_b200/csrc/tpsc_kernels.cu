@@ -1931,9 +1931,6 @@ cudaError_t launch_sigma_boundary(const GridDev &g, const float *Grt, const doub
 cudaError_t launch_sigma_slice(const GridDev &g, const double *Grt, const double *V, double *sigt, cudaStream_t st) {
     return dispatch_nbk<RunSigmaSlice>(g.nbk, &g, Grt, V, sigt, st);
 }
-cudaError_t launch_sigma_slice(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st) {
-    return dispatch_nbk<RunSigmaSlice>(g.nbk, &g, Grt, V, sigt, st);
-}
 
 cudaError_t launch_sigma_tau(const GridDev &g, const double *sigt, const double *dS, double2 *S, double *s2,
                              double *s3, double *s4, double *sinf, double T, cudaStream_t st) {

@@ -127,7 +127,8 @@ cudaError_t launch_sigma_boundary(const GridDev &g, const float *Grt, const doub
                                   const double *dG0p, double mu0, double U, const double *Usc, double *dS,
                                   cudaStream_t st);
 cudaError_t launch_sigma_slice(const GridDev &g, const double *Grt, const double *V, double *sigt, cudaStream_t st);
-cudaError_t launch_sigma_slice(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st);
+// the mixed form's Sigma slices: FP32 transform, local term in FP64 (tpsc_mixed.cu)
+cudaError_t launch_sigma_slice32(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st);
 cudaError_t launch_sigma_tau(const GridDev &g, const double *sigt, const double *dS, double2 *S, double *s2,
                              double *s3, double *s4, double *sinf, double T, cudaStream_t st);
 

@@ -1,14 +1,22 @@
 // tpsc_mixed.cu -- the FP32 slice transforms of the mixed-precision form.
 //
-// The G(r, tau), chi0 and V(q) stages of the solve transform in FP32 (the
-// slice and its DCT-I in float, twiddles compensated, see tpsc_fft.cuh);
-// their inputs are formed and their outputs kept in FP64 where the next
-// stage needs it: chi0(r, tau) and chi0(q, tau) feed the FP64 tau
-// transforms and sum rules, V(r, tau) the FP64 self-energy.  G(r, tau) is
-// stored in FP32 (half the bytes) and read by the FP64 Sigma slices.  The
-// Sigma slices, every tau transform, the tail moments, the sum rules, the
-// root searches and the continuation stay FP64: Sigma's own 2D transform in
-// FP32 would cost ~6e-6 of Sigma, the other three stages together ~3e-7.
+// The G(r, tau), chi0, V(q) and Sigma(k, tau) stages of the solve transform
+// in FP32 (the slice and its DCT-I in float, twiddles compensated, see
+// tpsc_fft.cuh); their inputs are formed and their outputs kept in FP64 where
+// the next stage needs it: chi0(r, tau) and chi0(q, tau) feed the FP64 tau
+// transforms and sum rules, V(r, tau) the self-energy, Sigma(k, tau) the
+// FP64 spline and FFT along tau.  G(r, tau) is stored in FP32 (half the
+// bytes).  Every tau transform, the tail moments, the sum rules, the root
+// searches and the continuation stay FP64.
+//
+// The Sigma slice compensates for its size: a plain FP32 transform of
+// G(r, tau) V(r, tau) costs ~6e-6 of Sigma(k, i w_n), because the few
+// points nearest r = 0 dominate the product and their FP32 rounding
+// survives the tau integral.  The slice therefore transforms in FP32 only
+// the product beyond the near field |rx|, |ry| <= kNear and adds the near
+// field's exact DCT-I in FP64: with u_a(k2) = sum_b w_b x(a, b) cos(pi b k2/(nbk-1)),
+// the near field contributes sum_a w_a cos(pi a k1/(nbk-1)) u_a(k2) at
+// (k1, k2), kNear + 1 FMAs per output point.
 //
 // Each FP32 slice needs ~105 KB of shared memory (the 129 x 129 float slice,
 // 16 groups' float2 FFT scratch and the hi/lo twiddles), so two CTAs run on
@@ -143,6 +151,82 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
     }
 }
 
+// near field of the FP32 Sigma slice: the points with both lattice
+// coordinates <= R (R = kNear, or nbk - 2 on the smallest lattices, so that
+// the near field never reaches the slice's last line, whose DCT-I weight
+// is 1), (R + 1)(R + 2)/2 of them in the octant
+constexpr int kNear = 4;
+
+// shared memory of k_sigma_slice32: the FP32 slice plan, then the near
+// field's FP64 values x(o), o < NOCT, and its partial sums u_a(k2)
+template <int NBK>
+struct SigmaSlice32Smem {
+    static constexpr int R = kNear < NBK - 1 ? kNear : NBK - 2;
+    static constexpr int NOCT = (R + 1) * (R + 2) / 2;
+    static constexpr size_t near_off = (Slice32Smem<NBK>::bytes + 15) & ~(size_t)15;
+    static constexpr size_t u_off = near_off + (size_t)NOCT * sizeof(double);
+    static constexpr size_t bytes = u_off + (size_t)(R + 1) * NBK * sizeof(double);
+};
+
+// Sigma(k, tau_j) = DCT-I[ G(r, tau_j) V(r, tau_j) ], j = 0..Nw0, with
+// V(r, tau_j) = V(r, beta - tau_j) for tau_j > beta/2 (src/green.cpp:1822-1885):
+// the product in FP64 from the FP32 G; beyond the near field transformed in
+// FP32, the near field's transform added in FP64 (cosines from the FP64
+// twiddle table tw64[m] = exp(-2 pi i m / L), L = 2 (nbk - 1)).
+template <int NBK>
+__global__ void __launch_bounds__(kSlice32Threads, 2)
+    k_sigma_slice32(const float *__restrict__ Grt, const double *__restrict__ V, const float4 *__restrict__ tw,
+                    const double2 *__restrict__ tw64, int n8, int nw0, int ahead, double *__restrict__ sigt) {
+    constexpr int L = 2 * (NBK - 1);
+    constexpr int R = SigmaSlice32Smem<NBK>::R;
+    constexpr int NOCT = SigmaSlice32Smem<NBK>::NOCT;
+    extern __shared__ __align__(16) float S32[];
+    double *xn = reinterpret_cast<double *>(reinterpret_cast<char *>(S32) + SigmaSlice32Smem<NBK>::near_off);
+    double *u = reinterpret_cast<double *>(reinterpret_cast<char *>(S32) + SigmaSlice32Smem<NBK>::u_off);
+    const float4 *tws = twiddles32<NBK>(S32, tw);
+    const int j = blockIdx.x;
+    const int nb = nw0 / 2 + 1;
+    const int jv = j < nb ? j : nw0 - j;
+    if (ahead > 0 && j + ahead <= nw0) {
+        const int jn = j + ahead;
+        prefetch_l2_range(Grt + (size_t)jn * n8, (size_t)n8 * sizeof(float));
+        prefetch_l2_blockrow(V, jn < nb ? jn : nw0 - jn, nb, (n8 + 3) / 4);
+    }
+    const float *g = Grt + (size_t)j * n8;
+    // octant points o < NOCT are exactly those with l <= R
+    fill_octant<NBK>(S32, n8, [&](int o) -> float {
+        const double x = (double)g[o] * V[bidx(jv, o, nb)];
+        if (o < NOCT) {
+            xn[o] = x;
+            return 0.0f;
+        }
+        return (float)x;
+    });
+    __syncthreads();
+    // u_a(k2) = sum_b w_b x(a, b) cos(pi b k2 / (nbk - 1)), w_0 = 1, w_b = 2
+    for (int i = threadIdx.x; i < (R + 1) * NBK; i += blockDim.x) {
+        const int a = i / NBK, k2 = i % NBK;
+        double acc = 0.0;
+#pragma unroll
+        for (int b = 0; b <= R; ++b) {
+            const int hi = a > b ? a : b, lo = a > b ? b : a;
+            const double wb = b == 0 ? 1.0 : 2.0;
+            acc = fma(wb * xn[lo + hi * (hi + 1) / 2], __ldg(&tw64[(b * k2) % L]).x, acc);
+        }
+        u[i] = acc;
+    }
+    // (the transform's barriers publish u)
+    dct2_slice<NBK>(S32, scratch32<NBK>(S32), tws);
+    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
+        int l, m;
+        oct_lm(o, l, m);
+        double nf = u[m];
+#pragma unroll
+        for (int a = 1; a <= R; ++a) nf = fma(2.0 * __ldg(&tw64[(a * l) % L]).x, u[a * NBK + m], nf);
+        sigt[bidx(j, o, nw0 + 1)] = (double)S32[l * NBK + m] + nf;
+    }
+}
+
 template <int NBK>
 struct RunGslice32 {
     static cudaError_t run(const GridDev *g, float *Grt, double mu0, double T, cudaStream_t st) {
@@ -180,7 +264,24 @@ struct RunVertexQ32 {
     }
 };
 
+template <int NBK>
+struct RunSigmaSlice32 {
+    static cudaError_t run(const GridDev *g, const float *Grt, const double *V, double *sigt, cudaStream_t st) {
+        const size_t sm = SigmaSlice32Smem<NBK>::bytes;
+        cudaError_t e = set_smem(k_sigma_slice32<NBK>, sm);
+        if (e != cudaSuccess) return e;
+        const int ahead = resident_ctas(k_sigma_slice32<NBK>, kSlice32Threads, sm);
+        k_sigma_slice32<NBK><<<g->nw0 + 1, kSlice32Threads, sm, st>>>(Grt, V, g->tw_k32, g->tw_k, g->n8, g->nw0,
+                                                                     ahead, sigt);
+        return launched();
+    }
+};
+
 }  // namespace
+
+cudaError_t launch_sigma_slice32(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st) {
+    return dispatch_nbk<RunSigmaSlice32>(g.nbk, &g, Grt, V, sigt, st);
+}
 
 cudaError_t launch_gslice32(const GridDev &g, float *Grt, double mu0, double T, cudaStream_t st) {
     return dispatch_nbk<RunGslice32>(g.nbk, &g, Grt, mu0, T, st);
