@@ -15,6 +15,9 @@
  *               chi::sp_corr_length() (chi.cpp:450) on the full-grid chi0
  *        cond   solve + cond_opt::calc_chijj_vertex_corr_all_optim(false,3,N,NULL,0)
  *               (cond_opt.cpp:2537), N = $TPSC_PROBE_NTHETA (default 1) angle bins
+ *        cond3  the same with chi3 = true and mmin = $TPSC_PROBE_MMIN (default 3):
+ *               also the Aslamazov-Larkin correction chijj3 on the non-uniform
+ *               iqn grid (cond_opt.cpp:4292-6529)
  *        post   solve + find_FS_inter, MDC(10 points, w=0, 4 etas), Gwn_local
  *               (src/tpsc_main.cpp:77-114)
  *        bench  timings only: the half-grid pre-pass alone, then the solve
@@ -119,6 +122,15 @@ public:
         write(dir + "/chijj2.bin", chijj2_qn, nbw / 2 + 1);
     }
 
+    // chijj3_qn holds the AL correction at the first N entries, N the size of
+    // the non-uniform grid of src/cond_opt.cpp:5123-5126
+    void dump_cond3(FILE *meta, const std::string &dir, int mmin) {
+        const int N0 = nbw / 2 + 1;
+        const int N = mmin * ((N0 - 1) / (1 << (mmin + 1))) + (N0 - 1) / (1 << mmin) + 1;
+        fprintf(meta, "mmin %d\nn_al %d\n", mmin, N);
+        write(dir + "/chijj3.bin", chijj3_qn, N);
+    }
+
 private:
     static void write(const std::string &path, const double *p, long n) {
         if (!p) return;
@@ -202,8 +214,8 @@ int main(int argc, char **argv) {
         t0 = omp_get_wtime();
         g->find_Usp_Uch(nk0 / 2, Nw0 / 2, Usc);
         fprintf(meta, "t_half %.6f\n", omp_get_wtime() - t0);
-    } else if (mode == "solve" || mode == "post" || mode == "cond" || mode == "files" || mode == "rew" ||
-               mode == "edc") {
+    } else if (mode == "solve" || mode == "post" || mode == "cond" || mode == "cond3" || mode == "files" ||
+               mode == "rew" || mode == "edc") {
         g->set_keep_chiqw(true);
         t0 = omp_get_wtime();
         g->calc_Self_FFT_spline();
@@ -238,7 +250,7 @@ int main(int argc, char **argv) {
             for (int j = 0; j < 9; j++) w[j] = -4.0 + j;
             g->calc_Self_Re_w_BZ(nn, 16, w, 9, eta, 2);
         }
-        if (mode == "post" || mode == "cond") {
+        if (mode == "post" || mode == "cond" || mode == "cond3") {
             // the post-processing tpsc_main.cpp runs after find_mu (lines 77-114)
             g->find_FS_inter();
             int NP = 10;
@@ -258,6 +270,19 @@ int main(int argc, char **argv) {
             g->calc_chijj_vertex_corr_all_optim(false, 3, ntheta, NULL, 0);
             fprintf(meta, "t_cond %.6f\n", omp_get_wtime() - t0);
             g->dump_cond(meta, absdir);
+        }
+        if (mode == "cond3") {
+            std::cout << std::setprecision(17);
+            t0 = omp_get_wtime();
+            const char *nt = getenv("TPSC_PROBE_NTHETA");
+            const int ntheta = nt ? atoi(nt) : 1;
+            const char *mm = getenv("TPSC_PROBE_MMIN");
+            const int mmin = mm ? atoi(mm) : 3;
+            fprintf(meta, "ntheta %d\n", ntheta);
+            g->calc_chijj_vertex_corr_all_optim(true, mmin, ntheta, NULL, 0);
+            fprintf(meta, "t_cond %.6f\n", omp_get_wtime() - t0);
+            g->dump_cond(meta, absdir);
+            g->dump_cond3(meta, absdir, mmin);
         }
     } else {
         fprintf(stderr, "unknown mode %s\n", mode.c_str());

@@ -1051,6 +1051,264 @@ def conductivity(sv: Solve, tp, tpp, t3, U, T, ntheta=1) -> CondResult:
 
 
 # ----------------------------------------------------------------------------
+# Aslamazov-Larkin vertex correction chijj3 (cond_opt::calc_chijj_vertex_corr_all_optim
+# with chi3 = true, src/cond_opt.cpp:4292-6529)
+# ----------------------------------------------------------------------------
+def al_frequencies(nbw: int, mmin: int) -> np.ndarray:
+    """The non-uniform bosonic grid of the AL term (src/cond_opt.cpp:5123-5155):
+    every n up to (N0-1)/2^mmin, then mmin blocks of (N0-1)/2^(mmin+1) points
+    whose spacing doubles per block (N0 = nbw/2 + 1)."""
+    N0 = nbw // 2 + 1
+    jf = (N0 - 1) // (2 ** mmin)
+    Nj = (N0 - 1) // (2 ** (mmin + 1))
+    out = list(range(jf + 1))
+    n, d = jf, 1
+    for _ in range(mmin):
+        d *= 2
+        for _ in range(Nj):
+            n += d
+            out.append(n)
+    return np.array(out, dtype=np.int64)
+
+
+@dataclass
+class ALResult:
+    ind_freq: np.ndarray  # [N] the bosonic indices n of the grid
+    chijj3: np.ndarray    # [N] AL correction chi_jj3(iq_n); entry 0 is not computed (0)
+    chijj3_k: np.ndarray  # [N, ntheta] angle-resolved
+
+
+def conductivity_al(sv: Solve, tp, tpp, t3, U, T, mmin=3, ntheta=1) -> ALResult:
+    """The AL branch of cond_opt::calc_chijj_vertex_corr_all_optim
+    (src/cond_opt.cpp:4292-6420), vectorised over the K4 grid of interior kx
+    points; the per-frequency loop follows the reference's order."""
+    nk0, nbw = sv.nk0, sv.Nw0
+    nbk = nk0 // 2 + 1
+    nw = nbw // 2
+    ek = dispersion(nbk, tp, tpp, t3)
+    er = hopping_octant(nbk, tp, tpp, t3)
+    mu0, mu = sv.mu0, sv.mu
+    sr, c0 = sv.sigma, sv.chi0
+    Usp, Uch = sv.U.Usp, sv.U.Uch
+    normFact = 1.0 / (nk0 * nk0)
+    kq = np.arange(nbk) * PI / (nbk - 1)
+    dek = grad_ek_x(kq[1:nbk - 1, None], kq[None, :], tp, tpp, t3)              # [nbk-2, nbk]
+    xk = ek[1:nbk - 1, :] - mu0
+    pos = xk > 0
+    K = (nbk - 2) * nbk
+    lx = np.arange(1, nbk - 1)[:, None] * np.ones((1, nbk), dtype=int)
+    my = np.ones((nbk - 2, 1), dtype=int) * np.arange(nbk)[None, :]
+    xo, yo = np.maximum(lx, my), np.minimum(lx, my)
+    oidx = yo + xo * (xo + 1) // 2                                              # r = (l+1, m) in the octant
+    ok = oidx.reshape(K)
+    # h(r, tau_j) and its tau-derivatives at 0 and beta (:4304-4330, :2744-2783)
+    h = np.empty((nbw + 1, nbk - 2, nbk))
+    for j in range(nbw + 1):
+        t = j / (T * nbw)
+        h[j] = dst_dct(np.where(pos, normFact * dek * np.exp(-xk * t) / (np.exp(-xk / T) + 1.0),
+                                normFact * dek * np.exp(xk * (1.0 / T - t)) / (np.exp(xk / T) + 1.0)))
+    dh0 = dst_dct(np.where(pos, -normFact * dek * xk / (np.exp(-xk / T) + 1.0),
+                           -normFact * dek * xk * np.exp(xk / T) / (np.exp(xk / T) + 1.0)))
+    dhb = dst_dct(np.where(pos, -normFact * dek * xk * np.exp(-xk / T) / (np.exp(-xk / T) + 1.0),
+                           -normFact * dek * xk / (np.exp(xk / T) + 1.0)))
+    # G(r, -tau_j) = DCT-I[G0(k, -tau_j)] / L^2 and its tau-derivative at 0 and beta (:4382-4446)
+    ekm = ek - mu0
+    neg = ek < mu0
+    Grt = np.empty((nbw + 1, nbk * (nbk + 1) // 2))
+    for j in range(nbw + 1):
+        t = j / (T * nbw)
+        fr = np.where(neg, normFact * np.exp(ekm * t) / (np.exp(ekm / T) + 1.0),
+                      normFact * np.exp(ekm * (t - 1.0 / T)) / (np.exp(-ekm / T) + 1.0))
+        Grt[j] = to_octant(dct2(fr))
+    dG0 = to_octant(dct2(np.where(neg, normFact * ekm / (np.exp(ekm / T) + 1.0),
+                                  normFact * ekm * np.exp(-ekm / T) / (np.exp(-ekm / T) + 1.0))))
+    dGb = er.copy()
+    dGb[0] = -mu0
+    dGb = dGb - dG0
+    # h G in q space and its spline over tau -> hG(q, i q_n) (:5158-5330)
+    dhG0 = dst_dct(dh0 * Grt[0][oidx] + h[0] * dG0[oidx]).reshape(K)
+    dhGb = dst_dct(dhb * Grt[nbw][oidx] + h[nbw] * dGb[oidx]).reshape(K)
+    hG = np.empty((nbw + 1, K))
+    for j in range(nbw + 1):
+        hG[j] = dst_dct(h[j] * Grt[j][oidx]).reshape(K)
+    hdt = 1.0 / (nbw * T)
+    a, b, c, d = clamped_spline(hG, hdt, dhG0, dhGb)
+    F = np.fft.fft(6.0 * a, axis=0)
+    integ = np.sum(a * hdt ** 4 / 4.0 + b * hdt ** 3 / 3.0 + c * hdt ** 2 / 2.0 + d * hdt, axis=0)
+    hq = np.empty((nw, K))
+    hq[0] = 2 * integ
+    jq = np.arange(1, nw)[:, None]
+    hq[1:] = 2 * ((1.0 - np.exp(-2j * jq * PI / nbw)) * F[1:nw]).real
+    hg2 = 2 * (dhG0 - dhGb)
+    chiq = c0.chiqw[:, ok]                                                      # [nw+1, K]
+    cinf, cinf2 = c0.chi0_inf[ok], c0.chi0_inf2[ok]
+
+    def chi0_at(p):
+        p = np.abs(p)
+        wn = 2 * PI * p * T
+        if p <= nw:
+            return chiq[p]
+        return cinf / wn ** 2 + cinf2 / wn ** 4
+
+    def hg_at(p):
+        p = abs(p)
+        wn = 2 * PI * p * T
+        if p == 0:
+            return hq[0]
+        return -hg2 / wn ** 2 + hq[min(p, nw - 1)] / wn ** 4
+
+    ind_freq = al_frequencies(nbw, mmin)
+    N = ind_freq.size
+    chijj3 = np.zeros(N)
+    chijj3_k = np.zeros((N, ntheta))
+    e = ek[1:nbk - 1, :].reshape(K)
+    dk = dek.reshape(K)
+    wt = np.where((my == 0) | (my == nbk - 1), 2.0, 4.0).reshape(K)
+    theta = np.arctan((nk0 / 2 - my) / (nk0 / 2 - lx)).reshape(K)
+    ib = np.floor(theta / (PI / (2.0 * ntheta))).astype(int)
+    C2, C3 = sr.Sigma_inf2[ok], sr.Sigma_inf3[ok]
+    Sk = sr.S[:, ok]                                                            # [nw, K] 1/z^4 coefficient
+    jj = np.arange(nbw)[:, None]
+    zsp0 = 1j * np.sqrt(Usp * cinf / 2.0)
+    zsp1 = -zsp0
+    zch0 = np.sqrt(Uch * cinf / 2.0) + 0j
+    zch1 = -zch0
+
+    for n in range(1, N):
+        nn = int(ind_freq[n])
+        qn = 2.0 * nn * PI * T
+        nc = nn // 2
+        # I_n(q, i q_m): the difference quotient of hG against chi0 (:5351-5493)
+        # at q_m = -q_n/2 (n even) both ends of the quotient meet: the
+        # reference extrapolates from the two previous m, (4 D(m-1) - D(m-2))/3
+        HG = np.empty((nbw, K))
+        D1 = np.zeros(K)
+        D2 = np.zeros(K)
+        for j in range(nbw):
+            first = j < nw - nc
+            p1, p2 = (j, j + nn) if first else (j - nbw, j - nbw + nn)
+            ch1 = chi0_at(p1)
+            pre = 3 * Usp * ch1 / (1.0 - Usp * ch1 / 2) + Uch * ch1 / (1.0 + Uch * ch1 / 2)
+            if not first and nn % 2 == 0 and j - nbw == -(nn // 2):
+                HG[j] = pre * (4 * D1 - D2) / 3.0
+                continue
+            q = (hg_at(p1) - hg_at(p2)) / (ch1 - chi0_at(p2))
+            if not first and nn % 2 == 0:
+                D2, D1 = D1, q
+            HG[j] = pre * q
+        # to tau: minus the asymptote, FFT, plus its closed form (:5500-5622)
+        wn = np.where(jj < nw - nc, 2 * jj * PI * T, 2 * (jj - nbw) * PI * T)
+        cq = -cinf
+        Hinf = hg2 * (3.0 * Usp / (-wn * wn - Usp * cq / 2.0) + Uch / (-wn * wn + Uch * cq / 2.0))
+        ft = T * (HG - Hinf)
+        dtauH0 = -np.sum(wn * ft, axis=0)
+        ft = np.fft.fft(ft, axis=0)
+        tt = jj / (nbw * T)
+        tmp_sp = (np.exp(-zsp0 * tt) / ((np.exp(-zsp0 / T) - 1.0) * (zsp0 - zsp1))
+                  + np.exp(-zsp1 * tt) / ((np.exp(-zsp1 / T) - 1.0) * (zsp1 - zsp0)))
+        tmp_ch = (np.exp(-zch0 * tt) / ((np.exp(-zch0 / T) - 1.0) * (zch0 - zch1))
+                  + np.exp(zch1 * (1.0 / T - tt)) / ((1.0 - np.exp(zch1 / T)) * (zch1 - zch0)))
+        Hq = np.empty((nbw + 1, K), dtype=np.complex128)
+        Hq[:nbw] = ft + hg2 * (3.0 * Usp * tmp_sp + Uch * tmp_ch)
+        tsp = (1.0 / ((1.0 - np.exp(zsp0 / T)) * (zsp0 - zsp1)) + 1.0 / ((1.0 - np.exp(zsp1 / T)) * (zsp1 - zsp0)))
+        tch = (np.exp(-zch0 / T) / ((np.exp(-zch0 / T) - 1.0) * (zch0 - zch1))
+               + 1.0 / ((1.0 - np.exp(zch1 / T)) * (zch1 - zch0)))
+        Hq[nbw] = ft[0] + hg2 * (3.0 * Usp * tsp + Uch * tch)
+        tsp = (-zsp0 / ((np.exp(-zsp0 / T) - 1.0) * (zsp0 - zsp1)) - zsp1 / ((np.exp(-zsp1 / T) - 1.0) * (zsp1 - zsp0)))
+        tch = (-zch0 / ((np.exp(-zch0 / T) - 1.0) * (zch0 - zch1))
+               - zch1 * np.exp(zch1 / T) / ((1.0 - np.exp(zch1 / T)) * (zch1 - zch0)))
+        dH0 = 1j * dtauH0 + hg2 * (3.0 * Usp * tsp + Uch * tch)
+        tsp = (-zsp0 * np.exp(-zsp0 / T) / ((np.exp(-zsp0 / T) - 1.0) * (zsp0 - zsp1))
+               - zsp1 * np.exp(-zsp1 / T) / ((np.exp(-zsp1 / T) - 1.0) * (zsp1 - zsp0)))
+        tch = (-zch0 * np.exp(-zch0 / T) / ((np.exp(-zch0 / T) - 1.0) * (zch0 - zch1))
+               - zch1 / ((1.0 - np.exp(zch1 / T)) * (zch1 - zch0)))
+        dHb = 1j * dtauH0 + hg2 * (3.0 * Usp * tsp + Uch * tch)
+
+        def dd(z):
+            """DST x DCT of the real and imaginary parts (q -> r or r -> k)."""
+            z = z.reshape(z.shape[:-1] + (nbk - 2, nbk))
+            return (dst_dct(z.real) + 1j * dst_dct(z.imag)).reshape(z.shape[:-2] + (K,))
+
+        # q -> r (:5628-5716), then the mirror H2(tau) = H(beta - tau) (:5718-5727)
+        Hr = dd(normFact * Hq)
+        dH0r, dHbr = dd(normFact * dH0), dd(normFact * dHb)
+        H2r = Hr[::-1]
+        dH20r, dH2br = -dHbr, -dH0r
+        Gk = Grt[:, ok]                                                         # G(r, -tau_j) on the K4 r grid
+        dG0k, dGbk = dG0[ok], dGb[ok]
+
+        def to_k(Hr_, d0r, dbr):
+            """times G(r, -tau) and DST x DCT back to k (:5729-5900)."""
+            d0 = dd(Hr_[0].real * dG0k + d0r.real * Gk[0]) + 1j * dd(Hr_[0].imag * dG0k + d0r.imag * Gk[0])
+            db = (dd(Hr_[nbw].real * dGbk + dbr.real * Gk[nbw])
+                  + 1j * dd(Hr_[nbw].imag * dGbk + dbr.imag * Gk[nbw]))
+            Hk = dd(Hr_.real * Gk) + 1j * dd(Hr_.imag * Gk)
+            return Hk, d0, db
+
+        Hk, d0k, dbk = to_k(Hr, dH0r, dHbr)
+        H2k, d20k, d2bk = to_k(H2r, dH20r, dH2br)
+
+        def to_matsubara(Hk_, d0, db):
+            """two splines (Re, Im) over tau, pre-twiddled FFT (:5906-5985)."""
+            ar, br, _, _ = clamped_spline(Hk_.real, hdt, d0.real, db.real)
+            ai, bi, _, _ = clamped_spline(Hk_.imag, hdt, d0.imag, db.imag)
+            d2S0 = 2 * br[0] + 1j * 2 * bi[0]
+            d2Sb = (6.0 * ar[nbw - 1] / (nbw * T) + 2.0 * br[nbw - 1]
+                    + 1j * (6.0 * ai[nbw - 1] / (nbw * T) + 2.0 * bi[nbw - 1]))
+            ph = np.exp(-1j * PI * jj / nbw)
+            Fq = np.fft.fft(ph * 6.0 * ar + 1j * ph * 6.0 * ai, axis=0)
+            return Fq, Hk_[0] + Hk_[nbw], d0 + db, d2S0 + d2Sb
+
+        F1, cw1, dsum1, d2sum1 = to_matsubara(Hk, d0k, dbk)
+        F2, cw2, dsum2, d2sum2 = to_matsubara(H2k, d20k, d2bk)
+        HGf = np.empty((nbw, K), dtype=np.complex128)
+        HG2f = np.empty((nbw, K), dtype=np.complex128)
+        for j in range(nbw):
+            if j < nw - nc:
+                w1 = (2 * (j + nn) + 1) * PI * T
+                idx = j + nn if j + nn < nbw else None
+            else:
+                w1 = (2 * (j + nn - nbw) + 1) * PI * T
+                if j + nn - nbw < 0:
+                    idx = j + nn
+                elif j + nn - nbw < nbw:
+                    idx = j + nn - nbw
+                else:
+                    idx = None
+            v = -1j * cw1 / w1 - dsum1 / w1 ** 2 + 1j * d2sum1 / w1 ** 3
+            if idx is not None:
+                v = v + (1.0 - np.exp(-1j * (2 * (j + nn) + 1) * PI / nbw)) * F1[idx] / w1 ** 4
+            HGf[j] = v
+            w2 = (2 * j + 1) * PI * T if j < nw - nc else (2 * (j - nbw) + 1) * PI * T
+            HG2f[j] = (-1j * cw2 / w2 - dsum2 / w2 ** 2 + 1j * d2sum2 / w2 ** 3
+                       + (1.0 - np.exp(-1j * (2 * j + 1) * PI / nbw)) * F2[j] / w2 ** 4)
+
+        # accumulate with G(k, i k_j) G(k, i k_{j+n}) (:6253-6398)
+        def green(f):
+            """G(k, i k_f) for the fermionic index f (k_f = (2f+1) pi T, any sign)."""
+            kn = (2 * f + 1) * PI * T
+            if f >= 0:
+                s = (-C2 / kn ** 2 + 1j * (-sr.Sigma_inf / kn + C3 / kn ** 3))
+                if f < nw:
+                    s = s + Sk[f] / kn ** 4
+            else:
+                s = (-C2 / kn ** 2 + 1j * (-sr.Sigma_inf / kn + C3 / kn ** 3))
+                if -f - 1 < nw:
+                    s = s + np.conj(Sk[-f - 1]) / kn ** 4
+            return 1.0 / (1j * kn - e + mu - s)
+
+        acc = np.zeros(K, dtype=np.complex128)
+        for j in range(nbw):
+            f1 = j if j < nw - nc else j - nbw
+            acc += green(f1) * green(f1 + nn) * (HGf[j] - HG2f[j])
+        term = -1j * U * T * normFact * wt * dk * acc / (2 * qn)
+        chijj3[n] = term.real.sum()
+        for b in range(ntheta):
+            chijj3_k[n, b] = term.real[ib == b].sum()
+    return ALResult(ind_freq, chijj3, chijj3_k)
+
+
+# ----------------------------------------------------------------------------
 # spin correlation length (chi::sp_corr_length, src/chi.cpp:450-718) with the
 # Fermi velocity at the hot spots (chi::vF_hot_spots, src/chi.cpp:420-447) on
 # the non-interacting Fermi surface (green0::find_FS, src/green0.cpp:626-676)

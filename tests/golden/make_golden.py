@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 PROBE = os.path.join(ROOT, "oracle", "_ref", "tpsc_ref_probe")
 
-# name: (mode, U, tp, tpp, t3, n, T, nk0, Nw0, keep_full_arrays[, angle bins of chi_jj])
+# name: (mode, U, tp, tpp, t3, n, T, nk0, Nw0, keep_full_arrays[, angle bins of chi_jj[, mmin]])
 CASES = {
     # tiny lattice, half-grid pre-pass exercised, conductivity too
     "l16_w64_u2": ("cond", 2.0, 0.0, 0.0, 0.0, 0.875, 0.25, 16, 64, True),
@@ -39,6 +39,15 @@ CASES = {
     # the optical-conductivity case: 128x128, U=3, n=0.9, T=0.1, 1024 positive
     # fermionic frequencies; scalars, sampled columns, chi_jj and 4 angle bins
     "l128_w2048_cond": ("cond", 3.0, 0.0, 0.0, 0.0, 0.9, 0.1, 128, 2048, False, 4),
+    # chi_jj (bubble + Maki-Thompson, kx0) at 256x256 with 2048 positive iwn
+    "l256_w4096_cond": ("cond", 4.0, -0.15, 0.0, 0.0, 0.875, 0.05, 256, 4096, False),
+    # the Aslamazov-Larkin correction chijj3 on the non-uniform iqn grid of
+    # mmin (src/cond_opt.cpp:4292-6529), with the reference's chijj3_qn_*,
+    # chijj_with_all_vc_qn_* and (angle bins) chijj3_k_qn_* files
+    "al_l16_w64": ("cond3", 2.0, -0.1, 0.0, 0.0, 0.875, 0.25, 16, 64, True, 1, 3),
+    "al_l32_w256_theta3": ("cond3", 4.0, -0.15, 0.0, 0.0, 0.875, 0.2, 32, 256, True, 3, 3),
+    "al_l16_w128_n110": ("cond3", 2.5, -0.2, 0.05, 0.0, 1.1, 0.3, 16, 128, True, 1, 2),
+    "al_l32_w512_n1": ("cond3", 3.0, -0.1, 0.0, 0.0, 1.0, 0.15, 32, 512, True, 1, 4),
     # larger lattice, lower temperature
     "l64_w1024_u4": ("solve", 4.0, -0.15, 0.0, 0.0, 0.875, 0.05, 64, 1024, False),
     # the 256x256, 2048 positive iwn case: scalars and sampled columns only
@@ -79,8 +88,10 @@ def read_meta(path):
 def run_case(name, spec, threads):
     mode, U, tp, tpp, t3, n, T, nk0, Nw0, full = spec[:10]
     ntheta = spec[10] if len(spec) > 10 else 1
+    mmin = spec[11] if len(spec) > 11 else 3
     with tempfile.TemporaryDirectory() as d:
-        env = dict(os.environ, OMP_NUM_THREADS=str(threads), TPSC_PROBE_NTHETA=str(ntheta))
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), TPSC_PROBE_NTHETA=str(ntheta),
+                   TPSC_PROBE_MMIN=str(mmin))
         args = [PROBE, d, mode] + [repr(v) for v in (U, tp, tpp, t3, n, T)] + [str(nk0), str(Nw0)]
         subprocess.run(args, check=True, env=env)
         meta = read_meta(os.path.join(d, "meta.txt"))
@@ -149,7 +160,7 @@ def run_case(name, spec, threads):
             out["vertex_rt_cols"] = V[:, cols]
             out["self_cols"] = S[:, cols]
             out["chiqw_w0"] = chiqw[0]
-        if mode == "cond":
+        if mode in ("cond", "cond3"):
             out["kx0"] = np.array(float(meta["kx0"]))
             out["chijj1"] = rd("chijj1.bin")
             out["chijj2"] = rd("chijj2.bin")
@@ -175,6 +186,20 @@ def run_case(name, spec, threads):
             out["gwn_local"] = g[:, 1] + 1j * g[:, 2]
             out["fs_inter"] = table("FS_inter_AkF_", exclude="FS_inter_AkF_Pade_")
             out["fs_inter_pade"] = table("FS_inter_AkF_Pade_")
+        if mode == "cond3":
+            work = os.path.join(d, "work")
+            out["mmin"] = np.array(mmin)
+            out["chijj3"] = rd("chijj3.bin")
+            names = sorted(f for f in os.listdir(work)
+                           if f.startswith(("chijj3_qn_", "chijj_with_all_vc_qn_", "chijj3_k_qn_", "chijj3_k_tot_qn_")))
+            out["file_names"] = np.array(names)
+            for i, f in enumerate(names):
+                out[f"file_{i}"] = np.fromfile(os.path.join(work, f), dtype=np.uint8)
+            t = np.loadtxt(os.path.join(work, [f for f in names if f.startswith("chijj3_qn_")][0]), ndmin=2)
+            out["ind_freq"] = t[:, 0].astype(np.int64)
+            if ntheta > 1:
+                t = np.loadtxt(os.path.join(work, [f for f in names if f.startswith("chijj3_k_qn_")][0]), ndmin=2)
+                out["chijj3_k"] = t[:, 2].reshape(-1, ntheta)
         if mode in ("files", "rew", "edc"):
             work = os.path.join(d, "work")
             names = sorted(f for f in os.listdir(work)

@@ -150,3 +150,24 @@ def test_oracle_sp_corr_length_matches_reference(name):
                          s["mu0"], p["tp"], p["tpp"], p["t3"])
     for k, v in zip(g["corr_names"], g["corr"]):
         assert abs(r[str(k)] - v) <= 1e-13 * abs(v), (k, r[str(k)], v)
+
+
+AL = [n for n in golden_names() if n.startswith("al_")]
+
+
+@pytest.mark.parametrize("name", AL)
+def test_oracle_al_matches_reference(name):
+    """The Aslamazov-Larkin correction chijj3 on the non-uniform iqn grid
+    (cond_opt::calc_chijj_vertex_corr_all_optim with chi3 = true,
+    src/cond_opt.cpp:4292-6529) against the reference's own array: mmin 2, 3
+    and 4, n < 1, n = 1 and n > 1, angle bins."""
+    g = load_golden(name)
+    p = g["p"]
+    ntheta = g["chijj3_k"].shape[1] if "chijj3_k" in g else 1
+    r = O.solve(p["U"], p["tp"], p["tpp"], p["t3"], p["n"], p["T"], p["nk0"], p["Nw0"])
+    a = O.conductivity_al(r, p["tp"], p["tpp"], p["t3"], p["U"], p["T"], int(g["mmin"]), ntheta)
+    assert np.array_equal(a.ind_freq, g["ind_freq"])
+    scale = np.max(np.abs(g["chijj3"]))
+    assert np.max(np.abs(a.chijj3 - g["chijj3"])) <= 1e-10 * scale
+    if ntheta > 1:
+        assert np.max(np.abs(a.chijj3_k[1:] - g["chijj3_k"])) <= 1e-10 * scale
