@@ -264,6 +264,22 @@ int tpsc_chijj(tpsc_ctx *ctx, int n_theta);
 int tpsc_get_chijj(tpsc_ctx *ctx, double *chijj1, double *chijj2, double *kx0, double *chijj1_k,
                    double *chijj2_k);
 
+/* The Aslamazov-Larkin vertex correction chijj3(iq_n) -- the chi3 = true
+ * branch of cond_opt::calc_chijj_vertex_corr_all_optim
+ * (src/cond_opt.cpp:4292-6529) -- on the current grid after the self-energy
+ * and mu, in FP64.  It is computed on the reference's non-uniform bosonic
+ * grid of mmin (src/cond_opt.cpp:5123-5155): every n up to (Nw0/2)/2^mmin,
+ * then mmin blocks of (Nw0/2)/2^(mmin+1) points whose spacing doubles; the
+ * entry n = 0 is not computed and stays 0, as in the reference.  n_theta >= 1
+ * angle bins as in tpsc_chijj; 0 <= mmin <= 24.  Each grid frequency costs
+ * about one and a half tpsc_chijj. */
+int tpsc_chijj3(tpsc_ctx *ctx, int mmin, int n_theta);
+/* Results of the last tpsc_chijj3: *n_freq = N, the grid size; then, where the
+ * pointer is not NULL (cap >= N is required for those), ind_freq [N] the
+ * bosonic indices n of the grid, chijj3 [N] and chijj3_k [N * n_theta] in the
+ * layout p + j * n_theta (row j for grid entry j). */
+int tpsc_get_chijj3(tpsc_ctx *ctx, int cap, int *n_freq, int *ind_freq, double *chijj3, double *chijj3_k);
+
 /* Optical conductivity on the bosonic Matsubara axis from the last tpsc_chijj
  * (no counterpart in the reference, which stops at chi_jj and kx0):
  * sigma(iq_n) = (-kx0 - chi_jj(iq_n)) / q_n, q_n = 2 pi n T, n = 1..nq, with

@@ -96,3 +96,48 @@ def test_conductivity_block_writes_the_reference_files(tmp_path):
     assert np.allclose(t1[:, 1], t1[:, 2], rtol=1e-12, atol=0)
     # the Fermi-surface files of find_FS_inter come first, as in the reference
     assert glob.glob(str(run / "FS_inter_AkF_Pade_*"))
+
+
+@pytest.mark.gpu
+def test_conductivity_block_with_the_al_correction_writes_its_files(tmp_path):
+    """The same block with chijj3 = 1 in input.dat: the Aslamazov-Larkin
+    correction on the non-uniform grid of mmin, and the reference's
+    chijj3_qn_*, chijj_with_all_vc_qn_*, chijj3_k_qn_* and chijj3_k_tot_qn_*
+    files (src/cond_opt.cpp:6448-6521) with the reference's grid and numbers."""
+    import io
+
+    if not os.path.exists(COND_BIN):
+        pytest.skip("cond_main_b200 is built by make -C tpsc_conductivity_b200/dropin")
+    g = load_golden("al_l32_w256_theta3")
+    p = g["p"]
+    nt = g["chijj3_k"].shape[1]
+    mmin = int(g["mmin"])
+    run = tmp_path / "a" / "b"
+    run.mkdir(parents=True)
+    (tmp_path / "input.dat").write_text(
+        f"{p['U']} {p['tp']} {p['tpp']} {p['t3']} {p['n']} {p['T']} {p['nk0']} {p['Nw0']} 1 {mmin} {nt}\n")
+    r = subprocess.run([COND_BIN], cwd=run, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "calcul de la seconde correction de vertex" in r.stdout
+    names = [str(n) for n in g["file_names"]]
+    scale = np.max(np.abs(g["chijj3"]))
+    for prefix in ("chijj3_qn_", "chijj_with_all_vc_qn_", "chijj3_k_qn_", "chijj3_k_tot_qn_"):
+        i = [k for k, n in enumerate(names) if n.startswith(prefix)]
+        assert len(i) == 1, prefix
+        ref_name = names[i[0]]
+        mine = run / ref_name
+        assert mine.exists(), ref_name  # same file name (parameters, nk0, Nw0, mmin)
+        a = np.loadtxt(mine, ndmin=2)
+        b = np.loadtxt(io.BytesIO(g[f"file_{i[0]}"].tobytes()), ndmin=2)
+        assert a.shape == b.shape, prefix
+        assert np.array_equal(a[:, 0], b[:, 0]), prefix  # the grid indices
+        if prefix == "chijj3_k_tot_qn_":
+            # total of the bins, total, their ratio
+            assert np.max(np.abs(a[:, 1:3] - b[:, 1:3])) <= 1e-10 * scale
+            assert np.allclose(a[:, 3], b[:, 3], rtol=1e-8, atol=0)
+        elif prefix == "chijj3_k_qn_":
+            assert np.array_equal(a[:, 1], b[:, 1])
+            assert np.max(np.abs(a[:, 2] - b[:, 2])) <= 1e-10 * scale
+        else:
+            s = np.max(np.abs(b[:, 1]))
+            assert np.max(np.abs(a[:, 1] - b[:, 1])) <= 1e-10 * s, prefix

@@ -94,8 +94,6 @@ def test_chijj_bad_arguments():
     c.solve()
     with pytest.raises(_lib.TPSCError):
         c.ctx.call("tpsc_chijj", 0)
-    with pytest.raises(NotImplementedError):
-        c.calc_chijj_vertex_corr_all_optim(True)
 
 
 def test_sigma_iqn_is_the_kubo_form_of_chijj():

@@ -260,15 +260,15 @@ class CondOpt(Green):
         super().__init__(nk0, Nw0, n, T, eta, params, device, ctx)
 
     def calc_chijj_vertex_corr_all_optim(self, chi3=False, mmin=3, N_theta_k=1, k_chijj=None, nk_chijj=0):
-        """cond_opt::calc_chijj_vertex_corr_all_optim (src/cond_opt.cpp:2537-4286),
-        bubble + Maki-Thompson branch.  Computes Sigma and mu first when they are
-        missing, as the reference does (src/cond_opt.cpp:2550-2560).  ``mmin``,
-        ``k_chijj`` and ``nk_chijj`` do not change chi_jj in the reference and
-        are accepted for the signature's sake.  Returns chijj1, chijj2
-        [Nw0/2+1], kx0 and the angle-resolved chijj1_k, chijj2_k [Nw0/2+1,
-        N_theta_k]."""
-        if chi3:
-            raise NotImplementedError("the second vertex correction (chi3 = true) is not part of this build")
+        """cond_opt::calc_chijj_vertex_corr_all_optim (src/cond_opt.cpp:2537-6529):
+        the bubble and the Maki-Thompson correction, and with ``chi3`` the
+        Aslamazov-Larkin correction on the non-uniform grid of ``mmin``.
+        Computes Sigma and mu first when they are missing, as the reference
+        does (src/cond_opt.cpp:2550-2560).  ``k_chijj`` and ``nk_chijj`` do not
+        change chi_jj in the reference and are accepted for the signature's
+        sake.  Returns chijj1, chijj2 [Nw0/2+1], kx0, the angle-resolved
+        chijj1_k, chijj2_k [Nw0/2+1, N_theta_k] and, with ``chi3``, the AL
+        grid ind_freq [N], chijj3 [N] and chijj3_k [N, N_theta_k]."""
         self._nbins = int(N_theta_k)
         try:
             self.ctx.call("tpsc_chijj", int(N_theta_k))
@@ -279,7 +279,24 @@ class CondOpt(Green):
             self.traceSelfG()
             self.find_mu()
             self.ctx.call("tpsc_chijj", int(N_theta_k))
-        return self.chijj()
+        out = self.chijj()
+        if chi3:
+            self.ctx.call("tpsc_chijj3", int(mmin), int(N_theta_k))
+            out.update(self.chijj3())
+        return out
+
+    def chijj3(self):
+        """Results of the last Aslamazov-Larkin evaluation: the grid ind_freq,
+        chijj3 and the angle-resolved chijj3_k."""
+        n = np.zeros(1, dtype=np.int32)
+        self.ctx.call("tpsc_get_chijj3", 0, n.ctypes.data_as(_lib._ip), None, None, None)
+        N = int(n[0])
+        nb = getattr(self, "_nbins", 1)
+        ind = np.zeros(N, dtype=np.int32)
+        c3, k3 = np.zeros(N), np.zeros(N * nb)
+        self.ctx.call("tpsc_get_chijj3", N, n.ctypes.data_as(_lib._ip), ind.ctypes.data_as(_lib._ip), _dptr(c3),
+                      _dptr(k3))
+        return {"ind_freq": ind.astype(np.int64), "chijj3": c3, "chijj3_k": k3.reshape(N, nb)}
 
     def chijj(self):
         """Results of the last calc_chijj_vertex_corr_all_optim."""

@@ -33,24 +33,6 @@ namespace tpsc {
 
 namespace {
 
-// two-column-block layout of the h V and f0 V tau arrays: element (j, c)
-__host__ __device__ __forceinline__ size_t bidx2(int j, int c, int NJ) {
-    return ((size_t)(c >> 1) * NJ + j) * 2 + (c & 1);
-}
-
-// octant index of lattice point (x, y), 0 <= x, y < nbk
-__device__ __forceinline__ int oct_index(int x, int y) {
-    const int a = max(x, y), b = min(x, y);
-    return b + a * (a + 1) / 2;
-}
-
-__device__ __forceinline__ double2 cexp2(double2 z) {
-    const double ea = exp(z.x);
-    if (z.y == 0.0) return make_double2(ea, 0.0);
-    double s, c;
-    sincos(z.y, &s, &c);
-    return make_double2(ea * c, ea * s);
-}
 
 __device__ __forceinline__ double cabs2(double2 z) { return hypot(z.x, z.y); }
 
@@ -63,7 +45,6 @@ __device__ __forceinline__ double2 csqrt2(double2 z) {
     return make_double2(fabs(z.y) / (2.0 * t), copysign(t, z.y));
 }
 
-__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
 
 // z^2 + B z + C at x and its derivative
 __device__ __forceinline__ void quad_eval(double2 x, double2 B, double2 C, double2 &y, double2 &p) {
@@ -263,33 +244,6 @@ struct ColState {
     double CJ1b, CJ3b;
 };
 
-// block-wide sum of NV values per thread -> out[0..NV) (all threads must call;
-// out visible to every thread on return)
-template <int NV>
-__device__ void block_sum(double (&v)[NV], double *out) {
-    __shared__ double red[32][NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k)
-        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0)
-#pragma unroll
-        for (int k = 0; k < NV; ++k) red[warp][k] = v[k];
-    __syncthreads();
-    if (threadIdx.x < NV) {
-        const int nw = (blockDim.x + 31) >> 5;
-        double s = 0.0;
-        for (int w = 0; w < nw; ++w) s += red[w][threadIdx.x];
-        out[threadIdx.x] = s;
-    }
-    __syncthreads();
-}
-
-// split of a packed FFT of two real sequences at bins n and N - n
-__device__ __forceinline__ void split_real(double2 Z, double2 Zc, double2 &Fa, double2 &Fb) {
-    Fa = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
-    Fb = make_double2(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
-}
 
 // full Sigma(k, i k_n) at octant o, n >= 0
 __device__ __forceinline__ double2 sigma_at(const CondTauArgs &a, int n, int o, int NO, double ik, double sinf) {
@@ -310,18 +264,6 @@ __device__ __forceinline__ void tails(const ColState &q, double tau, double beta
     jinf = cmul(q.v1, j1).x + cmul(q.v2, j2).x;
 }
 
-// Stage the two columns of pair p (contiguous in the two-column-block layout)
-// column-major into R; a padding column loads zeros.
-__device__ __forceinline__ void stage_pair(double *R, const double *g, int NJ, bool two) {
-    for (int i = threadIdx.x; i < 2 * NJ; i += blockDim.x) {
-        double *dst = &R[(i & 1) * NJ + (i >> 1)];
-        if ((i & 1) && !two)
-            *dst = 0.0;
-        else
-            cp_async8(dst, g + i);
-    }
-    cp_async_wait_all();
-}
 
 template <int N>
 __global__ void __launch_bounds__(CondTauSmem<N>::threads, 1) k_cond_tau(const CondTauArgs a) {
@@ -832,6 +774,12 @@ struct CondBlocks {
 }  // namespace
 
 cudaError_t cond_blocks(const GridDev &g, int *blocks) { return dispatch_nw<CondBlocks>(g.nw0, blocks); }
+
+cudaError_t launch_cond_table(const GridDev &g, const CondDev &c, double mu0, double T, cudaStream_t st) {
+    const double nf = 1.0 / ((double)g.nk0 * g.nk0);
+    k_cond_table<<<(c.K4 + 255) / 256, 256, 0, st>>>(g.ek, c.dek, c.K4, g.nbk, mu0, T, nf, c.tab);
+    return launched();
+}
 
 cudaError_t launch_cond_slices(const GridDev &g, const CondDev &c, const double *V, const double *dtau_chirt0,
                                double mu0, double T, double fact, cudaStream_t st) {

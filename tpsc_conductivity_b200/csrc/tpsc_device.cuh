@@ -447,6 +447,71 @@ __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
 }
 
 // ---------------------------------------------------------------------------
+// helpers of the current-current correlator kernels (tpsc_cond.cu, tpsc_al.cu)
+// ---------------------------------------------------------------------------
+// two-column-block layout of the h V and f0 V tau arrays: element (j, c)
+__host__ __device__ __forceinline__ size_t bidx2(int j, int c, int NJ) {
+    return ((size_t)(c >> 1) * NJ + j) * 2 + (c & 1);
+}
+
+// octant index of lattice point (x, y), 0 <= x, y < nbk
+__device__ __forceinline__ int oct_index(int x, int y) {
+    const int a = max(x, y), b = min(x, y);
+    return b + a * (a + 1) / 2;
+}
+
+__device__ __forceinline__ double2 cexp2(double2 z) {
+    const double ea = exp(z.x);
+    if (z.y == 0.0) return make_double2(ea, 0.0);
+    double s, c;
+    sincos(z.y, &s, &c);
+    return make_double2(ea * c, ea * s);
+}
+
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+
+// block-wide sum of NV values per thread -> out[0..NV) (all threads must call;
+// out visible to every thread on return)
+template <int NV>
+__device__ void block_sum(double (&v)[NV], double *out) {
+    __shared__ double red[32][NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) red[warp][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += red[w][threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+// split of a packed FFT of two real sequences at bins n and N - n
+__device__ __forceinline__ void split_real(double2 Z, double2 Zc, double2 &Fa, double2 &Fb) {
+    Fa = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
+    Fb = make_double2(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
+}
+
+// Stage the two columns of pair p (contiguous in the two-column-block layout)
+// column-major into R; a padding column loads zeros.
+__device__ __forceinline__ void stage_pair(double *R, const double *g, int NJ, bool two) {
+    for (int i = threadIdx.x; i < 2 * NJ; i += blockDim.x) {
+        double *dst = &R[(i & 1) * NJ + (i >> 1)];
+        if ((i & 1) && !two)
+            *dst = 0.0;
+        else
+            cp_async8(dst, g + i);
+    }
+    cp_async_wait_all();
+}
+
+// ---------------------------------------------------------------------------
 // dispatch over the compiled sizes
 // ---------------------------------------------------------------------------
 template <template <int> class F, typename... Args>

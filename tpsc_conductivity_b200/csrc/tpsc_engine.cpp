@@ -334,6 +334,14 @@ struct Grid {
     size_t cond_part_cap = 0, cond_out_cap = 0;  // doubles in cond.partial, cond.out
     std::vector<double> cond_host;
     int cond_bins = 0;                            // n_theta of cond_host (0: none yet)
+    // Aslamazov-Larkin correction: device state (allocated on first use) and
+    // the last result, [N (1 + n_theta)] on the grid al_ind
+    AlDev al;
+    bool al_alloc = false;
+    size_t al_out_cap = 0;                        // doubles in al.out
+    std::vector<double> al_host;
+    std::vector<int> al_ind;
+    int al_bins = 0;                              // n_theta of al_host (0: none yet)
 };
 
 }  // namespace
@@ -425,6 +433,7 @@ void free_grid(Grid *g) {
     for (void *p : g->allocs) cudaFree(p);
     if (g->cond.partial) cudaFree(g->cond.partial);
     if (g->cond.out) cudaFree(g->cond.out);
+    if (g->al.out) cudaFree(g->al.out);
     delete g;
 }
 
@@ -1425,6 +1434,88 @@ int run_cond(tpsc_ctx *ctx, int nbins) {
     return TPSC_OK;
 }
 
+// The non-uniform bosonic grid of the AL correction (src/cond_opt.cpp:5123-5155):
+// every n up to (N0-1)/2^mmin, then mmin blocks of (N0-1)/2^(mmin+1) points
+// whose spacing doubles from block to block (N0 = Nw0/2 + 1).
+std::vector<int> al_frequencies(int nw0, int mmin) {
+    const int n0 = nw0 / 2;
+    const int jf = n0 >> mmin, nj = n0 >> (mmin + 1);
+    std::vector<int> ind;
+    for (int j = 0; j <= jf; ++j) ind.push_back(j);
+    int n = jf, d = 1;
+    for (int b = 0; b < mmin; ++b) {
+        d *= 2;
+        for (int j = 0; j < nj; ++j) ind.push_back(n += d);
+    }
+    return ind;
+}
+
+// cond_opt::calc_chijj_vertex_corr_all_optim, Aslamazov-Larkin branch
+// (chi3 = true), on the current grid after Sigma and mu
+// (src/cond_opt.cpp:4292-6529): one setup, then the per-frequency pipeline
+// for every grid frequency n >= 1 (entry 0 stays 0, as in the reference)
+int run_al(tpsc_ctx *ctx, int mmin, int nbins) {
+    Grid *g = ctx->cur;
+    int rc = ensure_cond(ctx, g, nbins);  // the K4 tables and the angle bins
+    if (rc) return rc;
+    const GridDev &d = g->d;
+    const CondDev &c = g->cond;
+    AlDev &a = g->al;
+    const std::vector<int> ind = al_frequencies(d.nw0, mmin);
+    const int N = (int)ind.size();
+    if (!g->al_alloc) {
+        a.K4 = c.K4;
+        a.K4p = c.K4p;
+        const size_t K4 = a.K4, K4p = a.K4p, NJ = d.nw0 + 1, NO = d.nw0 / 2;
+        cudaError_t e = cudaSuccess;
+#define A(x)                \
+    if (e == cudaSuccess) { \
+        e = (x);            \
+    }
+        A(dalloc(g, &a.Grt, NJ * d.n8));
+        A(dalloc(g, &a.hGt, K4p * NJ));
+        A(dalloc(g, &a.pre, 2 * K4));
+        A(dalloc(g, &a.dhG, 2 * K4));
+        A(dalloc(g, &a.hgq, K4 * (NO + 1)));
+        A(dalloc(g, &a.HQ, NJ * K4));
+        A(dalloc(g, &a.dHQ, 2 * K4));
+        A(dalloc(g, &a.HR, NJ * K4));
+        A(dalloc(g, &a.dHR, 2 * K4));
+        A(dalloc(g, &a.HK, K4p * NJ));
+        A(dalloc(g, &a.H2K, K4p * NJ));
+        A(dalloc(g, &a.dHK, 4 * K4));
+        A(dalloc(g, &a.colv, K4));
+#undef A
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "Aslamazov-Larkin allocation");
+        g->al_alloc = true;
+    }
+    a.nbins = nbins;
+    a.nrows = N;
+    const size_t need_out = (size_t)N * (1 + nbins);
+    if (need_out > g->al_out_cap) {
+        if (a.out) cudaFree(a.out);
+        a.out = nullptr;
+        g->al_out_cap = 0;
+        CK(cudaMalloc(&a.out, need_out * sizeof(double)));
+        g->al_out_cap = need_out;
+    }
+    CK(cudaMemsetAsync(a.out, 0, need_out * sizeof(double), ctx->st));
+    const double mu = ctx->scal[TPSC_S_MU];
+    CK(launch_cond_table(d, c, g->mu0, ctx->T, ctx->st));
+    CK(launch_al_setup(d, c, a, g->dG0p, g->mu0, ctx->T, ctx->st));
+    for (int n = 1; n < N; ++n)
+        CK(launch_al_freq(d, c, a, g->chiq, g->cinf, g->cinf2, g->S, g->s2, g->s3, g->sinf, g->dG0p, ind[n], n,
+                          ctx->U, ctx->Usp, ctx->Uch, mu, g->mu0, ctx->T, ctx->st));
+    g->al_host.assign(need_out, 0.0);
+    CK(cudaMemcpyAsync(g->al_host.data(), a.out, need_out * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    g->al_ind = ind;
+    g->al_bins = nbins;
+    for (double v : g->al_host)
+        if (!std::isfinite(v)) return fail(ctx, TPSC_ERR_NONFINITE, "non-finite chijj3");
+    return TPSC_OK;
+}
+
 int ensure_stage(tpsc_ctx *ctx, size_t bytes) {
     if (ctx->stage_bytes >= bytes) return TPSC_OK;
     if (ctx->stage) cudaFree(ctx->stage);
@@ -2334,6 +2425,37 @@ int tpsc_chijj(tpsc_ctx *ctx, int n_theta) {
     if (g->d.nk0 < 8) return fail(ctx, TPSC_ERR_ARG, "need nk0 >= 8");
     g->cond_bins = 0;
     return run_cond(ctx, n_theta);
+}
+
+int tpsc_chijj3(tpsc_ctx *ctx, int mmin, int n_theta) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    Grid *g = ctx->cur;
+    if (!g->have_S || ctx->scal[TPSC_S_EVALS_MU] == 0)
+        return fail(ctx, TPSC_ERR_STATE, "the self-energy and mu must be computed first");
+    if (n_theta < 1 || n_theta > 64) return fail(ctx, TPSC_ERR_ARG, "need 1 <= n_theta <= 64");
+    if (mmin < 0 || mmin > 24) return fail(ctx, TPSC_ERR_ARG, "need 0 <= mmin <= 24");
+    if (g->d.nk0 < 8) return fail(ctx, TPSC_ERR_ARG, "need nk0 >= 8");
+    g->al_bins = 0;
+    return run_al(ctx, mmin, n_theta);
+}
+
+int tpsc_get_chijj3(tpsc_ctx *ctx, int cap, int *n_freq, int *ind_freq, double *chijj3, double *chijj3_k) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    const Grid *g = ctx->cur;
+    if (g->al_bins == 0) return fail(ctx, TPSC_ERR_STATE, "tpsc_chijj3 has not been run on the current grid");
+    const int N = (int)g->al_ind.size(), nb = g->al_bins;
+    if (n_freq) *n_freq = N;
+    if ((ind_freq || chijj3 || chijj3_k) && cap < N) return fail(ctx, TPSC_ERR_ARG, "cap is below the grid size");
+    for (int j = 0; j < N; ++j) {
+        if (ind_freq) ind_freq[j] = g->al_ind[j];
+        if (chijj3) chijj3[j] = g->al_host[(size_t)j * (1 + nb)];
+        for (int p = 0; p < nb; ++p)
+            if (chijj3_k) chijj3_k[p + j * nb] = g->al_host[(size_t)j * (1 + nb) + 1 + p];
+    }
+    return TPSC_OK;
 }
 
 int tpsc_get_chijj(tpsc_ctx *ctx, double *chijj1, double *chijj2, double *kx0, double *chijj1_k, double *chijj2_k) {

@@ -212,6 +212,8 @@ struct CondDev {
 };
 
 cudaError_t cond_blocks(const GridDev &g, int *blocks);
+// the (eps - mu0, A, B) table of the h and f0 slices into c.tab
+cudaError_t launch_cond_table(const GridDev &g, const CondDev &c, double mu0, double T, cudaStream_t st);
 // table + h V, f0 V slices + end conditions (fact = U (3 Usp + Uch)/4)
 cudaError_t launch_cond_slices(const GridDev &g, const CondDev &c, const double *V, const double *dtau_chirt0,
                                double mu0, double T, double fact, cudaStream_t st);
@@ -221,6 +223,38 @@ cudaError_t launch_cond_tau(const GridDev &g, const CondDev &c, const double2 *S
 // kx = 0, pi lines and the ordered sum of the partial rows -> c.out
 cudaError_t launch_cond_finish(const GridDev &g, const CondDev &c, const double2 *S, const double *s2,
                                const double *s3, const double *sinf, double mu, double T, cudaStream_t st);
+
+// ---- Aslamazov-Larkin correction chijj3 on the non-uniform iqn grid --------
+// (tpsc_al.cu).  Arrays on the K4 grid of the correlator; NJ = Nw0 + 1 tau
+// nodes, NO = Nw0 / 2.
+struct AlDev {
+    int K4 = 0, K4p = 0;        // as CondDev
+    int nrows = 0;              // rows of out (grid frequencies)
+    int nbins = 1;              // angular bins
+    double *Grt = nullptr;      // [NJ n8]   FP64 G(r, tau_j) (the G(r, -tau) of the AL branch by symmetry)
+    double *hGt = nullptr;      // [K4p NJ]  h G(q, tau), two-column blocks
+    double *pre = nullptr;      // [2 K4]    h(r, 0), h(r, beta)
+    double *dhG = nullptr;      // [2 K4]    d/dtau h G(q) at 0, beta
+    double *hgq = nullptr;      // [K4 (NO+1)] h G(q, i q_p), p < NO, then its 1/q^2 coefficient hg2
+    double2 *HQ = nullptr;      // [NJ K4]   H(q, tau_j) of the current frequency
+    double2 *dHQ = nullptr;     // [2 K4]    d/dtau H(q) at 0, beta
+    double2 *HR = nullptr;      // [NJ K4]   H(r, tau_j)
+    double2 *dHR = nullptr;     // [2 K4]
+    double2 *HK = nullptr;      // [K4p NJ]  G H(k, tau), two-column blocks
+    double2 *H2K = nullptr;     // [K4p NJ]  G H2(k, tau), H2(r, tau) = H(r, beta - tau)
+    double2 *dHK = nullptr;     // [4 K4]    end slopes: H at 0, beta; H2 at 0, beta
+    double *colv = nullptr;     // [K4]      per-point term of the current frequency
+    double *out = nullptr;      // [nrows (1 + nbins)] chijj3, then its angular bins
+};
+// once per call: G(r, tau) in FP64, h G(q, tau), its end slopes and h G(q, i q_p)
+// (c.tab, c.dek must be current)
+cudaError_t launch_al_setup(const GridDev &g, const CondDev &c, const AlDev &a, const double *dG0p, double mu0,
+                            double T, cudaStream_t st);
+// one grid frequency q_nn -> row `row` of a.out
+cudaError_t launch_al_freq(const GridDev &g, const CondDev &c, const AlDev &a, const double *chiq, const double *cinf,
+                           const double *cinf2, const double2 *S, const double *s2, const double *s3,
+                           const double *sinf, const double *dG0p, int nn, int row, double U, double Usp, double Uch,
+                           double mu, double mu0, double T, cudaStream_t st);
 
 // Batched continued-fraction Pade of nf functions sampled at Nn points
 // (x, y: [nf][Nn]) evaluated at Nz shared points: out [nf][Nz].

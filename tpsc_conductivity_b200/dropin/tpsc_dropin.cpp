@@ -1148,21 +1148,23 @@ void green::save_Green(int *k) {
 
 // ---------------------------------------------------------------------------
 cond_opt::cond_opt(int nk0, int Nw0, double n, double T, double eta0, double *params)
-    : green(nk0, Nw0, n, T, eta0, params), chijj1_qn(NULL), chijj2_qn(NULL), kx0(0.0) {}
+    : green(nk0, Nw0, n, T, eta0, params), chijj1_qn(NULL), chijj2_qn(NULL), chijj3_qn(NULL), kx0(0.0) {}
 
 cond_opt::~cond_opt() {
     delete[] chijj1_qn;
     delete[] chijj2_qn;
+    delete[] chijj3_qn;
 }
 
-// cond_opt::calc_chijj_vertex_corr_all_optim (src/cond_opt.cpp:2537-4286):
+// cond_opt::calc_chijj_vertex_corr_all_optim (src/cond_opt.cpp:2537-6529):
 // Sigma and mu first when missing, Sigma at the listed k points, the Fermi
 // surface files, then chi_jj on the device and the reference's result files
 // (chijj*_k_qn_*, chijj*_k_tot_qn_*, kx0_*, kx0_bin_*, chijj1_qn_*,
 // chijj_with_vc1_qn_*, chijj2_qn_*) with its column layouts and stdout lines.
-// mmin does not enter the bubble + Maki-Thompson result in the reference.
+// With chi3, the Aslamazov-Larkin correction on the non-uniform grid of mmin
+// and its files (chijj3_qn_*, chijj_with_all_vc_qn_*, and with angle bins
+// chijj3_k_qn_*, chijj3_k_tot_qn_*; src/cond_opt.cpp:6448-6521).
 void cond_opt::calc_chijj_vertex_corr_all_optim(bool chi3, int mmin, int N_theta_k, int *k_chijj, int nk_chijj) {
-    (void)mmin;
     cout << "calcul de chijj par calc_chijj_vertex_corr_all_optim()\n";
     const int nw = nbw / 2, nk0 = 2 * (nbk - 1);
     if (!have_self) {
@@ -1258,5 +1260,65 @@ void cond_opt::calc_chijj_vertex_corr_all_optim(bool chi3, int mmin, int N_theta
     cout << "chijj2(iqn=0):  " << chijj2_qn[0] << '\n';
     cout << "chijj1(iqn=0)+chijj2(iqn=0):  " << chijj1_qn[0] + chijj2_qn[0] << '\n';
     cout << "difference relative avec -k0:  " << (chijj1_qn[0] + chijj2_qn[0] + kx0) / kx0 << '\n';
-    if (chi3) cout << "calc_chijj_vertex_corr_all_optim(): la seconde correction de vertex (chi3) n'est pas disponible\n";
+    if (chi3) calc_chijj3(mmin, N_theta_k);
+}
+
+// The chi3 branch of calc_chijj_vertex_corr_all_optim (src/cond_opt.cpp:4292-6529)
+// after chijj1, chijj2: the AL correction on the device, then the reference's
+// files with their formats.
+void cond_opt::calc_chijj3(int mmin, int N_theta_k) {
+    cout << "calcul de la seconde correction de vertex\n";
+    const int nw = nbw / 2, nk0 = 2 * (nbk - 1);
+    if (!check(tpsc_chijj3(ctx_, mmin, N_theta_k), "calc_chijj_vertex_corr_all_optim")) return;
+    int N = 0;
+    if (!check(tpsc_get_chijj3(ctx_, 0, &N, NULL, NULL, NULL), "tpsc_get_chijj3")) return;
+    std::vector<int> ind(N);
+    std::vector<double> c3(N), k3((size_t)N * N_theta_k);
+    if (!check(tpsc_get_chijj3(ctx_, N, &N, ind.data(), c3.data(), k3.data()), "tpsc_get_chijj3")) return;
+    cout << "2^M:  " << (1 << mmin) << "  (N0-1)/((int)pow(2.0,M)):  " << (nw >> mmin) << "   N:  " << N << '\n';
+    delete[] chijj3_qn;
+    chijj3_qn = new double[nw + 1];
+    for (int j = 0; j <= nw; j++) chijj3_qn[j] = j < N ? c3[j] : 0.0;
+
+    char name[200];
+    fstream file, file2;
+    const double dn = density;
+    sprintf(name, "./chijj3_qn_%5.3f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d_%1d.dat", U, tp, tpp, t3, dn, tem, nk0, nbw,
+            mmin);
+    file.open(name, ios::out);
+    file << setprecision(16) << setiosflags(ios::left) << setiosflags(ios::scientific);
+    for (int j = 0; j < N; j++) file << setw(10) << (long)ind[j] << chijj3_qn[j] << '\n';
+    file.close();
+
+    sprintf(name, "./chijj_with_all_vc_qn_%5.3f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d_%1d.dat", U, tp, tpp, t3, dn, tem,
+            nk0, nbw, mmin);
+    file.open(name, ios::out);
+    file << setprecision(16) << setiosflags(ios::left) << setiosflags(ios::scientific);
+    for (int j = 0; j < N; j++) {
+        const double v = j == 0 ? chijj1_qn[0] + chijj2_qn[0]
+                                : chijj1_qn[ind[j]] + chijj2_qn[ind[j]] + chijj3_qn[j];
+        file << setw(10) << (long)ind[j] << v << '\n';
+    }
+    file.close();
+
+    if (N_theta_k > 1) {
+        sprintf(name, "./chijj3_k_qn_%5.3f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d_%1d.dat", U, tp, tpp, t3, dn, tem, nk0,
+                nbw, mmin);
+        file.open(name, ios::out);
+        file << setprecision(16) << setiosflags(ios::left) << setiosflags(ios::scientific);
+        sprintf(name, "./chijj3_k_tot_qn_%5.3f_%5.3f_%5.3f_%5.3f_%7.5f_%6.4f_%1d_%1d_%1d.dat", U, tp, tpp, t3, dn, tem,
+                nk0, nbw, mmin);
+        file2.open(name, ios::out);
+        file2 << setprecision(16) << setiosflags(ios::left) << setiosflags(ios::scientific);
+        for (int j = 1; j < N; j++) {
+            double tot = 0;
+            for (int p = 0; p < N_theta_k; p++) tot += k3[p + (size_t)j * N_theta_k];
+            file2 << setw(10) << (long)ind[j] << setw(30) << tot << setw(30) << chijj3_qn[j] << tot / chijj3_qn[j]
+                  << '\n';
+            for (int p = 0; p < N_theta_k; p++)
+                file << setw(10) << (long)ind[j] << setw(10) << (p + 1) << k3[p + (size_t)j * N_theta_k] << '\n';
+        }
+        file.close();
+        file2.close();
+    }
 }

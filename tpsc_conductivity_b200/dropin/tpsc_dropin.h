@@ -178,12 +178,15 @@ class cond_opt : public green {
 public:
     cond_opt(int nk0 = 8, int Nw0 = 256, double n = 1.0, double T = 1.0, double eta = 0.1, double *params = NULL);
     virtual ~cond_opt();
-    // bubble + Maki-Thompson branch; chi3 = true (second vertex correction)
-    // prints that it is not available after the bubble + Maki-Thompson files
+    // the bubble and the Maki-Thompson correction; with chi3 also the
+    // Aslamazov-Larkin correction on the non-uniform iqn grid of mmin
     void calc_chijj_vertex_corr_all_optim(bool chi3, int mmin, int N_theta_k, int *k_chijj, int nk_chijj);
 
 protected:
+    // the chi3 branch (device AL correction and its files)
+    void calc_chijj3(int mmin, int N_theta_k);
     double *chijj1_qn, *chijj2_qn;  // [Nw0/2 + 1]
+    double *chijj3_qn;              // [Nw0/2 + 1]: the AL correction at the first N entries (grid order)
     double kx0;
 };
 
