@@ -512,11 +512,31 @@ def extra_configs():
         c3(objs[name])
         c3(objs[name])
     sig_m, pade_m, ms3 = c3(objs["mixed_newton"])
+    st3 = objs["mixed_newton"].stage_times()
     sig_d, _, ms3d = c3(objs["fp64_newton"])
+    # the chi_jj stage against the HBM roofline: device time of its kernels
+    # (CUDA events around the slices, the tau kernel and the finish) and the
+    # minimal-traffic model 8 K4 (Nw0+1) s + N8 Nb s + N8 (Nw0/2) 2s, s = 8 B
+    nbk3, nw3 = 128 // 2 + 1, 2048
+    K4, N8, Nb = (nbk3 - 2) * nbk3, nbk3 * (nbk3 + 1) // 2, nw3 // 2 + 1
+    alg3 = 8.0 * (8 * K4 * (nw3 + 1) + N8 * Nb + N8 * (nw3 // 2) * 2)
+    dev3 = st3["cond_slices"] + st3["cond_tau"] + st3["cond_finish"]
+    peak3, _ = measured_hbm()
+    # the Aslamazov-Larkin correction on the non-uniform grid of mmin = 3
+    g3 = objs["fp64_newton"]
+    g3.calc_chijj_vertex_corr_all_optim(True, 3, 1)
+    al3, t_al = timed(lambda: g3.calc_chijj_vertex_corr_all_optim(True, 3, 1))
     out["c3_l128_w2048_conductivity"] = {
         "ms_mixed_newton": ms3, "ms_fp64_newton": ms3d,
         "max_rel_err_sigma_iqn_mixed_vs_fp64": float(np.max(np.abs(sig_m - sig_d)) / np.max(np.abs(sig_d))),
-        "pade": "sigma(w) on 2000 w in [0, 10] from 64 bosonic nodes", "pade_finite": bool(np.all(np.isfinite(pade_m)))}
+        "pade": "sigma(w) on 2000 w in [0, 10] from 64 bosonic nodes", "pade_finite": bool(np.all(np.isfinite(pade_m))),
+        "chijj_roofline": {"bound": "hbm", "device_ms": dev3, "stage_ms": {k: st3[k] for k in
+                                                                        ("cond_slices", "cond_tau", "cond_finish")},
+                           "algorithmic_bytes": alg3, "achieved": alg3 / (dev3 * 1e-3) / 1e9, "peak": peak3,
+                           "unit": "GB/s", "frac": alg3 / (dev3 * 1e-3) / 1e9 / peak3},
+        "aslamazov_larkin": {"ms": t_al, "mmin": 3, "grid_frequencies": int(len(al3["ind_freq"])),
+                             "ms_per_frequency": t_al / max(1, len(al3["ind_freq"]) - 1),
+                             "note": "includes the bubble + Maki-Thompson call before it (FP64)"}}
     # config 4
     g4 = CondOpt(128, 2048, 0.85, 0.1, 0.1, (-0.2, 0.0, 0.0, 4.0))
     g4.set_form(_lib.FORM_NEWTON)

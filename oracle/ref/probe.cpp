@@ -36,6 +36,10 @@
  *        chi0inf  chi0::calc_chi0_qlims(n, {0, 0, pi, pi}, {3, 3}) for n = 0, 1
  *               (the infinite lattice by adaptive quadrature, src/chi0.cpp:157-276)
  *               and chi0::chiqw_discret({2, 1}, 1) on the constructor's lattice
+ *        fftbench  timings of the FFTW shim alone, single thread, on the
+ *               transforms the reference runs: 2D REDFT00 of nk0/2+1 points
+ *               square, 2D RODFT00 x REDFT00 of (nk0/2-1) x (nk0/2+1), 1D
+ *               complex DFT of Nw0 points (seconds per transform in meta.txt)
  *        files  solve, then the reference's own writers of the saved-run
  *               formats: chi0::save_chi, green::save_Self(0),
  *               green::save_Self_bin, green::save_Green({2, 1})
@@ -53,6 +57,7 @@
 #include <cstring>
 #include <sstream>
 #include <string>
+#include <vector>
 
 class tpsc_probe : public cond_opt {
 public:
@@ -188,6 +193,34 @@ int main(int argc, char **argv) {
         t0 = omp_get_wtime();
         g->chi0_infinite(meta);
         fprintf(meta, "t_chi0inf %.6f\n", omp_get_wtime() - t0);
+    } else if (mode == "fftbench") {
+        const int nb = nk0 / 2 + 1;
+        std::vector<double> a((size_t)nb * nb, 0.5), b((size_t)(nb - 2) * nb, 0.5);
+        std::vector<fftw_complex> c(Nw0);
+        for (int j = 0; j < Nw0; j++) c[j][0] = c[j][1] = 1.0 / (j + 1);
+        for (size_t j = 0; j < a.size(); j++) a[j] = 1.0 / (j + 1);
+        for (size_t j = 0; j < b.size(); j++) b[j] = 1.0 / (j + 2);
+        fftw_plan p1 = fftw_plan_r2r_2d(nb, nb, a.data(), a.data(), FFTW_REDFT00, FFTW_REDFT00, FFTW_MEASURE);
+        fftw_plan p2 = fftw_plan_r2r_2d(nb - 2, nb, b.data(), b.data(), FFTW_RODFT00, FFTW_REDFT00, FFTW_MEASURE);
+        fftw_plan p3 = fftw_plan_dft_1d(Nw0, c.data(), c.data(), FFTW_FORWARD, FFTW_MEASURE);
+        auto time_it = [&](fftw_plan p, const char *key) {
+            int reps = 1;
+            double dt = 0.0;
+            for (;;) {
+                t0 = omp_get_wtime();
+                for (int r = 0; r < reps; r++) fftw_execute(p);
+                dt = omp_get_wtime() - t0;
+                if (dt > 0.5) break;
+                reps *= 2;
+            }
+            fprintf(meta, "%s %.9g\n", key, dt / reps);
+        };
+        time_it(p1, "t_dct2d");
+        time_it(p2, "t_dstdct2d");
+        time_it(p3, "t_dft1d");
+        fftw_destroy_plan(p1);
+        fftw_destroy_plan(p2);
+        fftw_destroy_plan(p3);
     } else if (mode == "corr") {
         double dens[2] = {n, n + 0.05}, temp[2] = {T, 1.5 * T};
         t0 = omp_get_wtime();
