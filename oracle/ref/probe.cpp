@@ -59,6 +59,9 @@
 #include <string>
 #include <vector>
 
+// transforms the FFTW shim has executed, per kind (fftw_shim.cpp)
+extern "C" void oracle_fftw_counts(long out[4]);
+
 class tpsc_probe : public cond_opt {
 public:
     tpsc_probe(int nk0, int Nw0, double n, double T, double eta, double *p)
@@ -244,6 +247,9 @@ int main(int argc, char **argv) {
         double t_mu = omp_get_wtime() - t0;
         fprintf(meta, "t_self %.6f\nt_traceSelfG %.6f\nt_find_mu %.6f\n", t_self, t_tr, t_mu);
         fprintf(meta, "mu %.17g\n", g->get_mu());
+        long cnt[4];
+        oracle_fftw_counts(cnt);
+        fprintf(meta, "n_r2r_2d %ld\nn_r2r_1d %ld\nn_dft_1d %ld\nn_dft_2d %ld\n", cnt[0], cnt[1], cnt[2], cnt[3]);
         t0 = omp_get_wtime();
         g->find_Usp_Uch(nk0 / 2, Nw0 / 2, Usc);
         fprintf(meta, "t_half %.6f\n", omp_get_wtime() - t0);
