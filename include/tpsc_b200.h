@@ -228,6 +228,14 @@ int tpsc_get_self(tpsc_ctx *ctx, double *self_kw, double *sigma_inf2, double *si
  * overlap other work only for page-locked (pinned) host buffers.  The host
  * buffers may be read only after tpsc_wait_copies(ctx, 0). */
 int tpsc_get_self_async(tpsc_ctx *ctx, double *self_kw, double *sigma_inf2, double *sigma_inf3, double *sigma_inf4);
+/* The full self-energy Sigma(k, i w_n) = Sigma_inf/z + C2/z^2 + C3/z^3 +
+ * S/z^4, z = i (2n+1) pi T, n < Nw0/2, formed in FP64 on the device, rounded
+ * to FP32 and copied out the same way ([Nw0/2][N8] complex float, interleaved
+ * re, im); no counterpart in the reference.  Half the bytes of S over the
+ * host link, for the mixed-precision form, whose bound (1e-6 of Sigma) it
+ * keeps: each element moves by at most 6e-8 of itself.  (S itself cannot be
+ * rounded: at low n its 1/z^4 term cancels against the others.) */
+int tpsc_get_sigma32_async(tpsc_ctx *ctx, float *sigma_kw);
 /* Waits for the copies of tpsc_get_self_async (join_stream = 0), or, with
  * join_stream = 1, makes the context stream wait for them without blocking
  * the host (work and events queued on the stream afterwards follow them). */

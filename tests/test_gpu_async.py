@@ -36,3 +36,39 @@ def test_async_copies_equal_the_synchronous_getter():
     for (a, b) in zip(outs, refs):
         for x, y in zip(a, b):
             assert np.array_equal(x, y)
+
+
+def test_fp32_sigma_copy_out_keeps_the_mixed_form_within_its_bound():
+    """tpsc_get_sigma32_async: the full Sigma(k, i w_n) formed in FP64 on the
+    device, rounded to FP32 and copied to the host.  Every element is within
+    6e-8 of itself of the same solve's FP64 Sigma, and the mixed form's Sigma
+    so delivered stays within its 1e-6 bound of the FP64 form at 256 x 256
+    with 2048 positive frequencies."""
+    import torch
+
+    from tpsc_conductivity_b200 import _lib
+    from tpsc_conductivity_b200.api import Green
+
+    p = load_golden("l256_w4096_u4")["p"]
+
+    def solve(form):
+        g = Green(int(p["nk0"]), int(p["Nw0"]), p["n"], p["T"], 0.1, (p["tp"], p["tpp"], p["t3"], p["U"]))
+        g.set_form(form)
+        g.solve()
+        return g
+
+    g64 = solve(_lib.FORM_NEWTON)
+    sig64 = g64.sigma()
+    del g64
+    g = solve(_lib.FORM_NEWTON | _lib.FORM_MIXED)
+    n8 = g.dims()[3]
+    buf = torch.empty((int(p["Nw0"]) // 2, n8, 2), dtype=torch.float32).pin_memory().numpy()
+    sig32 = buf.view(np.complex64)[..., 0]
+    g.sigma_async32(sig32)
+    g.wait_copies()
+    mine = g.sigma()
+    d = np.abs(sig32.astype(np.complex128) - mine)
+    assert np.all(d <= 6e-8 * np.abs(mine) + 1e-300)
+    err = float(np.max(np.abs(sig32.astype(np.complex128) - sig64)) / np.max(np.abs(sig64)))
+    print("mixed form, FP32 Sigma copy-out: rel err %.3g" % err)
+    assert err <= 1e-6

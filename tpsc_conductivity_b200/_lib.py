@@ -30,6 +30,7 @@ SIGNATURES = [
     ("tpsc_sp_corr_length_fs", C.c_int, [C.c_void_p, C.c_double, _dp]),
     ("tpsc_sumrule_tangents", C.c_int, [C.c_void_p, _dp]),
     ("tpsc_get_self_async", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    ("tpsc_get_sigma32_async", C.c_int, [C.c_void_p, C.c_void_p]),
     ("tpsc_set_self", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),
     ("tpsc_set_chi0", C.c_int, [C.c_void_p, _dp]),
     ("tpsc_get_sigma_tau", C.c_int, [C.c_void_p, C.c_int, _dp]),

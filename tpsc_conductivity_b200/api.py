@@ -211,6 +211,17 @@ class Green:
         to overlap the next stages; read them after wait_copies()."""
         self.ctx.call("tpsc_get_self_async", _dptr(out.view(np.float64)), _dptr(s2), _dptr(s3), _dptr(s4))
 
+    def sigma_async32(self, out):
+        """The full Sigma(k, i w_n), n < Nw0/2, formed in FP64 on the device and
+        copied to the host in FP32 without waiting (tpsc_get_sigma32_async):
+        ``out`` complex64 [Nw0/2, N8], half the bytes of S over the host link;
+        the mixed-precision form's result in its own precision.  Read after
+        wait_copies()."""
+        out = np.asarray(out)
+        if out.dtype != np.complex64 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous complex64 array")
+        self.ctx.call("tpsc_get_sigma32_async", out.ctypes.data_as(C.c_void_p))
+
     def wait_copies(self, join_stream=False):
         """Waits for the copies of self_energy_async (or, with join_stream, makes
         the context stream wait for them)."""

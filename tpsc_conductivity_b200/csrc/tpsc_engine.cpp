@@ -2304,7 +2304,11 @@ int tpsc_set_chi0(tpsc_ctx *ctx, const double *chiqw) {
     return set_chi0max(ctx, r);
 }
 
-int tpsc_get_self_async(tpsc_ctx *ctx, double *self_kw, double *s2, double *s3, double *s4) {
+namespace {
+// The asynchronous copy-out of S and the three tail vectors (FP64), or, with
+// f32, of the full Sigma(k, i w_n) formed in FP64 and rounded to FP32: a
+// device snapshot, then copies on the copy stream.
+int get_self_async(tpsc_ctx *ctx, void *self_kw, bool f32, double *s2, double *s3, double *s4) {
     int rc = need_model(ctx);
     if (rc) return rc;
     Grid *g = ctx->cur;
@@ -2320,8 +2324,9 @@ int tpsc_get_self_async(tpsc_ctx *ctx, double *self_kw, double *s2, double *s3, 
         }
     }
     const int k = ctx->snap_next;
-    const size_t sbytes = (size_t)(d.nw0 / 2) * d.n8 * sizeof(double2), vbytes = (size_t)d.n8 * sizeof(double);
-    const size_t need = sbytes + 3 * vbytes;
+    const size_t sbytes = (size_t)(d.nw0 / 2) * d.n8 * (f32 ? sizeof(float2) : sizeof(double2));
+    const size_t vbytes = (size_t)d.n8 * sizeof(double);
+    const size_t need = ((sbytes + 15) & ~(size_t)15) + 3 * vbytes;
     // snapshot buffer k is free once its previous copy has finished
     CK(cudaStreamWaitEvent(ctx->st, ctx->copy_ev[k], 0));
     if (ctx->snap_bytes[k] < need) {
@@ -2333,8 +2338,11 @@ int tpsc_get_self_async(tpsc_ctx *ctx, double *self_kw, double *s2, double *s3, 
         ctx->snap_bytes[k] = need;
     }
     char *base = static_cast<char *>(ctx->snap[k]);
-    double *vs = reinterpret_cast<double *>(base + sbytes);
-    CK(launch_unblock_c(g->S, reinterpret_cast<double2 *>(base), d.nw0 / 2, d.nw0 / 2, d.n8, ctx->st));
+    double *vs = reinterpret_cast<double *>(base + ((sbytes + 15) & ~(size_t)15));
+    if (f32)
+        CK(launch_sigma_full32(d, g->S, g->s2, g->s3, g->sinf, ctx->T, reinterpret_cast<float2 *>(base), ctx->st));
+    else
+        CK(launch_unblock_c(g->S, reinterpret_cast<double2 *>(base), d.nw0 / 2, d.nw0 / 2, d.n8, ctx->st));
     // the three vectors by the SMs too: a device-to-device copy may take a
     // copy engine, where it could wait behind the previous step's copy-out
     GatherPieces gp;
@@ -2356,6 +2364,15 @@ int tpsc_get_self_async(tpsc_ctx *ctx, double *self_kw, double *s2, double *s3, 
     ctx->snap_next = k ^ 1;
     ctx->copies_pending = true;
     return TPSC_OK;
+}
+}  // namespace
+
+int tpsc_get_self_async(tpsc_ctx *ctx, double *self_kw, double *s2, double *s3, double *s4) {
+    return get_self_async(ctx, self_kw, false, s2, s3, s4);
+}
+
+int tpsc_get_sigma32_async(tpsc_ctx *ctx, float *sigma_kw) {
+    return get_self_async(ctx, sigma_kw, true, nullptr, nullptr, nullptr);
 }
 
 int tpsc_wait_copies(tpsc_ctx *ctx, int join_stream) {

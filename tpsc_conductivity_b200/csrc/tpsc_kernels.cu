@@ -513,29 +513,21 @@ __global__ void __launch_bounds__(TauSmem<N>::threads, 1)
 }
 
 // Stage the two columns 2 half, 2 half + 1 of a four-column block (NJ rows)
-// column-major into A; columns >= n8 as zeros.  A row of the pair is 16
-// contiguous, 16-byte aligned bytes: each thread issues eight 16-byte
-// streaming loads before storing any.  The caller's barrier publishes them.
+// column-major into A; columns >= n8 as zeros.  Every element is an
+// asynchronous 8-byte copy, all of a thread's copies in flight at once (the
+// thread waits for its own; the caller's barrier publishes them).
 __device__ __forceinline__ void stage_pair4(double *A, const double *blk4, int NJ, int half, int o0, int n8) {
-    const double2 *src = reinterpret_cast<const double2 *>(blk4 + 2 * half);
     const bool c0 = o0 < n8, c1 = o0 + 1 < n8;
-    constexpr int B = 8;
-    for (int base = threadIdx.x; base < NJ; base += B * blockDim.x) {
-        double2 v[B];
-#pragma unroll
-        for (int b = 0; b < B; ++b) {
-            const int j = base + b * blockDim.x;
-            if (j < NJ) v[b] = __ldcs(&src[2 * j]);
-        }
-#pragma unroll
-        for (int b = 0; b < B; ++b) {
-            const int j = base + b * blockDim.x;
-            if (j < NJ) {
-                A[j] = c0 ? v[b].x : 0.0;
-                A[NJ + j] = c1 ? v[b].y : 0.0;
-            }
-        }
+    const double *src = blk4 + 2 * half;
+    for (int i = threadIdx.x; i < 2 * NJ; i += blockDim.x) {
+        const int j = i >> 1, q = i & 1;
+        double *dst = &A[q * NJ + j];
+        if (q == 0 ? c0 : c1)
+            cp_async8(dst, src + 4 * j + q);
+        else
+            *dst = 0.0;
     }
+    cp_async_wait_all();
 }
 
 // The same transform for ONE pair of columns per CTA, two CTAs per SM: the
@@ -1518,6 +1510,24 @@ __global__ void k_unblock_c(const double2 *__restrict__ src, double2 *__restrict
     }
 }
 
+// The full Sigma(k, i w_n) = Sinf/z + C2/z^2 + C3/z^3 + S/z^4, z = i w_n,
+// w_n = (2n+1) pi T, n < NO, formed in FP64 and rounded to FP32, [n][o]
+// (the mixed form's copy-out: S alone could not be rounded, its 1/z^4 term
+// cancels against the others at low n)
+__global__ void k_sigma_full32(const double2 *__restrict__ S, const double *__restrict__ s2,
+                               const double *__restrict__ s3, const double *__restrict__ sinfp, int NO, int n8,
+                               double T, float2 *__restrict__ dst) {
+    const long long total = (long long)NO * n8;
+    const double sinf = sinfp[0];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int n = (int)(i / n8), o = (int)(i % n8);
+        double rS, iS;
+        sigma_full(1.0 / ((2 * n + 1) * kPi * T), sinf, s2[o], s3[o], S[bidx(n, o, NO)], rS, iS);
+        dst[i] = make_float2((float)rS, (float)iS);
+    }
+}
+
 // [j][o] -> blocked (NJ rows): the setters' inverse of k_unblock
 __global__ void k_block(const double *__restrict__ src, double *__restrict__ dst, int NJ, int nrows, int n8) {
     const long long total = (long long)nrows * n8;
@@ -2004,6 +2014,14 @@ cudaError_t launch_unblock(const double *src, double *dst, int NJ, int nrows, in
 cudaError_t launch_unblock_c(const double2 *src, double2 *dst, int NJ, int nrows, int n8, cudaStream_t st) {
     const int nb = grid_for((long long)nrows * n8, 256);
     k_unblock_c<<<nb, 256, 0, st>>>(src, dst, NJ, nrows, n8);
+    return launched();
+}
+
+cudaError_t launch_sigma_full32(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                                const double *sinf, double T, float2 *dst, cudaStream_t st) {
+    const int NO = g.nw0 / 2;
+    const int nb = grid_for((long long)NO * g.n8, 256);
+    k_sigma_full32<<<nb, 256, 0, st>>>(S, s2, s3, sinf, NO, g.n8, T, dst);
     return launched();
 }
 

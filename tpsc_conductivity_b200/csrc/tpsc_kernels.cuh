@@ -266,6 +266,9 @@ cudaError_t launch_pade_batch(const double2 *x, const double2 *y, int nf, int Nn
 // blocked (NJ rows) -> reference layout [j][o], j < nrows
 cudaError_t launch_unblock(const double *src, double *dst, int NJ, int nrows, int n8, cudaStream_t st);
 cudaError_t launch_unblock_c(const double2 *src, double2 *dst, int NJ, int nrows, int n8, cudaStream_t st);
+// the full Sigma(k, i w_n), n < Nw0/2, in FP32, [n][o]
+cudaError_t launch_sigma_full32(const GridDev &g, const double2 *S, const double *s2, const double *s3,
+                                const double *sinf, double T, float2 *dst, cudaStream_t st);
 // row j of a blocked (NJ rows) array -> dst[o], o < n8
 cudaError_t launch_take_row(const double *src, int NJ, int j, int n8, double *dst, cudaStream_t st);
 // reference layout [j][o], j < nrows -> blocked (NJ rows): the setters
