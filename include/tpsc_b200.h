@@ -351,6 +351,16 @@ int tpsc_kernel_bytes(tpsc_ctx *ctx, int which, double *bytes);
  * a kernel of independent FMA chains on every SM -- the arithmetic ceiling of
  * the transform kernels' roofline beside the HBM copy bandwidth. */
 int tpsc_fma_peak(int bits, double *tflops);
+/* Check of the bounded grid barrier of the device root searches (no
+ * counterpart in the reference): their barrier in a cooperative launch of
+ * their grid (*blocks), where block `withhold` never arrives (negative: every
+ * block does).  Every other block's wait then runs out after about a second,
+ * sets the error flag and leaves, so the kernel ends and the context stays
+ * usable.  *err_flag: the flag after the launch; *timed_out: blocks that left
+ * with it; *ms: the kernel's time.  Returns TPSC_OK when the launch itself
+ * ran (the flag reports the barrier). */
+int tpsc_barrier_probe(tpsc_ctx *ctx, int withhold, int *err_flag, int *timed_out, int *blocks, double *ms);
+
 /* Number of CUDA kernels the library has launched (all contexts) since it was
  * loaded. */
 int tpsc_launch_count(tpsc_ctx *ctx, long long *count);

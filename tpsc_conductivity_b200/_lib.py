@@ -89,6 +89,7 @@ SIGNATURES = [
     ("tpsc_chijj", C.c_int, [C.c_void_p, C.c_int]),
     ("tpsc_get_chijj", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),
     ("tpsc_chijj3", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("tpsc_barrier_probe", C.c_int, [C.c_void_p, C.c_int, _ip, _ip, _ip, _dp]),
     ("tpsc_get_chijj3", C.c_int, [C.c_void_p, C.c_int, _ip, _ip, _dp, _dp]),
     ("tpsc_sigma_iqn", C.c_int, [C.c_void_p, C.c_int, _dp, _dp]),
     ("tpsc_sigma_iqn_fd", C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp]),

@@ -2444,6 +2444,29 @@ int tpsc_chijj(tpsc_ctx *ctx, int n_theta) {
     return run_cond(ctx, n_theta);
 }
 
+int tpsc_barrier_probe(tpsc_ctx *ctx, int withhold, int *err_flag, int *timed_out, int *blocks, double *ms) {
+    if (!ctx) return fail(nullptr, TPSC_ERR_ARG, "null context");
+    cudaSetDevice(ctx->device);
+    unsigned *words = nullptr;
+    CK(cudaMallocAsync(reinterpret_cast<void **>(&words), 4 * sizeof(unsigned), ctx->st));
+    int nblk = 0;
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    cudaError_t e = launch_barrier_probe(words, withhold, &nblk, ctx->st);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[1], ctx->st);
+    unsigned h[4] = {0, 0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, words, sizeof(h), cudaMemcpyDeviceToHost, ctx->st);
+    cudaFreeAsync(words, ctx->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "barrier probe");
+    float t = 0.0f;
+    CK(cudaEventElapsedTime(&t, ctx->ev[0], ctx->ev[1]));
+    if (err_flag) *err_flag = (int)h[2];
+    if (timed_out) *timed_out = (int)h[3];
+    if (blocks) *blocks = nblk;
+    if (ms) *ms = t;
+    return TPSC_OK;
+}
+
 int tpsc_chijj3(tpsc_ctx *ctx, int mmin, int n_theta) {
     int rc = need_model(ctx);
     if (rc) return rc;

@@ -268,7 +268,16 @@ __device__ __forceinline__ void stockham_pass(C *x, int t, int Ns, const TW *__r
         if (Ns > 1) {
             // twiddle exp(SIGN 2 pi i k q / (Ns R)) = tw[k q N/(Ns R)] (conjugated for SIGN>0)
             const int step = k * (N / (Ns * R));
-            if constexpr (R == 16 && sizeof(C) == sizeof(double2)) {
+            if constexpr (N == 256 && R == 16 && !FIRST && sizeof(C) == sizeof(float2)) {
+                // the FP32 256-point transform's second pass (Ns = 16, step = k):
+                // its twiddles tw[k q], q = 1..15, are read from the transposed
+                // copy behind the table, entry 256 + (q - 1) 16 + k, so that the
+                // 16 threads of a group read 16 consecutive entries (no bank
+                // conflicts; strided reads tw[k q] are up to 16-way for even q)
+#pragma unroll
+                for (int q = 1; q < R; ++q)
+                    v[u * R + q] = twiddle<SIGN, SMEM_TW>(v[u * R + q], tw, 256 + (q - 1) * 16 + k);
+            } else if constexpr (R == 16 && sizeof(C) == sizeof(double2)) {
                 twiddle16_powers<N, SIGN, SMEM_TW>(&v[u * R], tw, step);
             } else {
 #pragma unroll

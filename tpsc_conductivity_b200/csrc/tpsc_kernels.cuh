@@ -256,6 +256,12 @@ cudaError_t launch_al_freq(const GridDev &g, const CondDev &c, const AlDev &a, c
                            const double *sinf, const double *dG0p, int nn, int row, double U, double Usp, double Uch,
                            double mu, double mu0, double T, cudaStream_t st);
 
+// The root searches' bounded grid barrier on its own, in a cooperative launch
+// of their grid (returned in *blocks): block `withhold` never arrives
+// (negative: all do).  words [4], zeroed here: barrier, generation, error
+// flag, blocks that left the barrier with the error.
+cudaError_t launch_barrier_probe(unsigned *words, int withhold, int *blocks, cudaStream_t st);
+
 // Batched continued-fraction Pade of nf functions sampled at Nn points
 // (x, y: [nf][Nn]) evaluated at Nz shared points: out [nf][Nz].
 constexpr int kPadeBatchMax = 4096;

@@ -23,7 +23,9 @@ namespace tpsc {
 namespace {
 
 constexpr int kRootThreads = 256;
-constexpr long long kBarrierSpins = 1LL << 24;  // x ~64 ns: ~1 s before giving up
+// spins of a barrier wait before it gives up: each spin sleeps __nanosleep(64),
+// which takes ~0.4 us on a B200 (2^24 spins measured 6.4 s), so ~1.6 s
+constexpr long long kBarrierSpins = 1LL << 22;
 
 // bar[0]: arrivals, bar[1]: generation.  Returns false (and sets *err) when
 // the wait ran out or another block had already failed.
@@ -654,6 +656,17 @@ __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
     }
 }
 
+// The barrier's bound, exercised: block `withhold` never arrives (negative:
+// every block does), so every other block's wait runs out after
+// kBarrierSpins and leaves with the error flag set.  words[0..1] the barrier,
+// words[2] the error flag, words[3] the number of blocks that left with it;
+// all zero at launch.
+__global__ void __launch_bounds__(kRootThreads) k_barrier_probe(unsigned *words, int withhold) {
+    if ((int)blockIdx.x == withhold) return;
+    const bool ok = grid_sync(words, reinterpret_cast<int *>(words + 2));
+    if (threadIdx.x == 0 && !ok) atomicAdd(words + 3, 1u);
+}
+
 // the cooperative grid of the root searches: up to two blocks per SM, or
 // `cap` blocks when the caller runs several root searches at once (solver
 // streams of a batch), so that all of them fit on the GPU together
@@ -753,6 +766,18 @@ cudaError_t launch_sumrule_roots(const GridDev &g, const double *chiq, const dou
     a.out = rs.out;
     void *args[] = {&a};
     e = cudaLaunchCooperativeKernel((const void *)k_sumrule_roots, dim3(grid), dim3(kRootThreads), args, 0, st);
+    if (e != cudaSuccess) return e;
+    return launched();
+}
+
+cudaError_t launch_barrier_probe(unsigned *words, int withhold, int *blocks, cudaStream_t st) {
+    int grid = 0;
+    cudaError_t e = root_grid(k_barrier_probe, &grid, 0);
+    if (e != cudaSuccess) return e;
+    *blocks = grid;
+    if ((e = cudaMemsetAsync(words, 0, 4 * sizeof(unsigned), st)) != cudaSuccess) return e;
+    void *args[] = {&words, &withhold};
+    e = cudaLaunchCooperativeKernel((const void *)k_barrier_probe, dim3(grid), dim3(kRootThreads), args, 0, st);
     if (e != cudaSuccess) return e;
     return launched();
 }
