@@ -386,6 +386,71 @@ __device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// ---------------------------------------------------------------------------
+// input staging of the slice kernels whose inputs are rows of global arrays:
+// the slice and the FFT scratch are idle until the fill, so a CTA first copies
+// its input rows there with asynchronous copies (all in flight at once: one
+// memory latency per slice instead of one per batch of loads), waits for its
+// own copies, and forms the slice from shared memory
+// ---------------------------------------------------------------------------
+template <int NBK>
+struct StageRows {
+    static constexpr int N8 = NBK * (NBK + 1) / 2;
+    static constexpr int N8P = (N8 + 3) & ~3;
+    static constexpr size_t blockrow_bytes = (size_t)N8P * sizeof(double);  // one row of a column-block array
+    static constexpr size_t drow_bytes = ((size_t)N8 * sizeof(double) + 15) & ~(size_t)15;  // one FP64 row
+};
+
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+// row j of a column-block array a (NJ rows) -> dst[o], o < N8P (16-byte copies)
+template <int NBK>
+__device__ __forceinline__ void stage_blockrow(double *dst, const double *__restrict__ a, int j, int NJ) {
+    for (int i = threadIdx.x; i < StageRows<NBK>::N8P / 2; i += blockDim.x) {
+        const int b = i >> 1, h = i & 1;
+        cp_async16(dst + 4 * b + 2 * h, a + ((size_t)b * NJ + j) * 4 + 2 * h);
+    }
+}
+// n8 doubles from src -> dst (8-byte copies: rows of an [j][o] array are
+// 16-byte aligned only for even j)
+template <int NBK>
+__device__ __forceinline__ void stage_drow(double *dst, const double *__restrict__ src) {
+    for (int o = threadIdx.x; o < StageRows<NBK>::N8; o += blockDim.x) cp_async8(dst + o, src + o);
+}
+// Form the symmetric slice from value(o), which reads the staged inputs:
+// every thread computes its octant points into registers, then a barrier (the
+// staging area overlaps the slice), then the writes of both triangles.
+// THREADS: the block size the kernel is launched with.
+template <int NBK, int THREADS, class T, class Value>
+__device__ __forceinline__ void fill_from_staged(T *S, const Value &value) {
+    constexpr int N8 = StageRows<NBK>::N8, PER = (N8 + THREADS - 1) / THREADS;
+    T v[PER];
+#pragma unroll
+    for (int b = 0; b < PER; ++b) {
+        const int o = threadIdx.x + b * THREADS;
+        if (o < N8) v[b] = value(o);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < PER; ++b) {
+        const int o = threadIdx.x + b * THREADS;
+        if (o < N8) {
+            int l, m;
+            oct_lm(o, l, m);
+            S[l * NBK + m] = v[b];
+            S[m * NBK + l] = v[b];
+        }
+    }
+}
+
+
 // Load one column block into shared memory, column-major (the caller's next
 // __syncthreads publishes it).  Padding columns (octant index >= n8, present
 // because N8 is rounded up to a multiple of 4) load as zeros: they share

@@ -140,9 +140,15 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     const auto *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
     const int nb = nw0 / 2 + 1;
-    const double *gp = Grt + (size_t)j * n8;
-    const double *gm = Grt + (size_t)(nw0 - j) * n8;
-    fill_octant<NBK>(S, n8, [&](int o) -> double {
+    // G(r, tau_j) and G(r, beta - tau_j) staged in the slice / scratch area
+    static_assert(2 * StageRows<NBK>::drow_bytes <= SliceSmem<NBK>::tw_off, "inputs must fit");
+    double *gp = S;
+    double *gm = S + StageRows<NBK>::drow_bytes / sizeof(double);
+    stage_drow<NBK>(gp, Grt + (size_t)j * n8);
+    stage_drow<NBK>(gm, Grt + (size_t)(nw0 - j) * n8);
+    cp_async_wait_all();
+    __syncthreads();
+    fill_from_staged<NBK, kSliceThreads>(S, [&](int o) -> double {
         const double a = gp[o];
         double c;
         if (j == 0)
@@ -225,8 +231,14 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     const auto *tws = slice_twiddles<NBK>(S, tw);
     const int j = blockIdx.x;
     const double Usp = Usc[0], Uch = Usc[1];
-    fill_octant<NBK>(S, n8, [&](int o) -> double {
-        const double c0 = chiq[bidx(j, o, nb)];
+    // chi0(q, iq_j) staged in the slice / scratch area
+    static_assert(StageRows<NBK>::blockrow_bytes <= SliceSmem<NBK>::tw_off, "inputs must fit");
+    double *cs = S;
+    stage_blockrow<NBK>(cs, chiq, j, nb);
+    cp_async_wait_all();
+    __syncthreads();
+    fill_from_staged<NBK, kSliceThreads>(S, [&](int o) -> double {
+        const double c0 = cs[o];
         const double sp = c0 / (1.0 - Usp * c0 / 2.0);
         const double ch = c0 / (1.0 + Uch * c0 / 2.0);
         return normFact * U * (3.0 * Usp * (sp - c0) + Uch * (ch - c0)) / 8.0;
@@ -281,12 +293,11 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
 }
 
 // Sigma(k, tau_j) = DCT-I[ G(r, tau_j) V(r, tau_j) ], j = 0..Nw0, with
-// V(r, tau_j) = V(r, beta - tau_j) for tau_j > beta/2 (src/green.cpp:1822-1885).
-// G in FP64, or in FP32 in the mixed-precision form (the product and the
-// transform in FP64 either way).
-template <int NBK, class GT>
+// V(r, tau_j) = V(r, beta - tau_j) for tau_j > beta/2 (src/green.cpp:1822-1885),
+// in FP64 (the mixed form's FP32 slice is k_sigma_slice32).
+template <int NBK>
 __global__ void __launch_bounds__(kSliceThreads, 1)
-    k_sigma_slice(const GT *__restrict__ Grt, const double *__restrict__ V,
+    k_sigma_slice(const double *__restrict__ Grt, const double *__restrict__ V,
                   const double2 *__restrict__ tw, int n8, int nw0, int ahead, double *__restrict__ sigt) {
     extern __shared__ __align__(16) double S[];
     const auto *tws = slice_twiddles<NBK>(S, tw);
@@ -295,11 +306,19 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     const int jv = j < nb ? j : nw0 - j;
     if (ahead > 0 && j + ahead <= nw0) {
         const int jn = j + ahead;
-        prefetch_l2_range(Grt + (size_t)jn * n8, (size_t)n8 * sizeof(GT));
+        prefetch_l2_range(Grt + (size_t)jn * n8, (size_t)n8 * sizeof(double));
         prefetch_l2_blockrow(V, jn < nb ? jn : nw0 - jn, nb, (n8 + 3) / 4);
     }
-    const GT *g = Grt + (size_t)j * n8;
-    fill_octant<NBK>(S, n8, [&](int o) -> double { return (double)g[o] * V[bidx(jv, o, nb)]; });
+    // V(r, tau_j) and G(r, tau_j) staged in the slice / scratch area
+    static_assert(StageRows<NBK>::blockrow_bytes + StageRows<NBK>::drow_bytes <= SliceSmem<NBK>::tw_off,
+                  "inputs must fit");
+    double *vs = S;
+    double *gs = S + StageRows<NBK>::blockrow_bytes / sizeof(double);
+    stage_blockrow<NBK>(vs, V, jv, nb);
+    stage_drow<NBK>(gs, Grt + (size_t)j * n8);
+    cp_async_wait_all();
+    __syncthreads();
+    fill_from_staged<NBK, kSliceThreads>(S, [&](int o) -> double { return gs[o] * vs[o]; });
     __syncthreads();
     dct2_slice<NBK>(S, slice_scratch<NBK>(S), tws);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
@@ -1635,13 +1654,12 @@ struct RunSigmaBoundary {
 };
 template <int NBK>
 struct RunSigmaSlice {
-    template <class GT>
-    static cudaError_t run(const GridDev *g, const GT *Grt, const double *V, double *sigt, cudaStream_t st) {
+    static cudaError_t run(const GridDev *g, const double *Grt, const double *V, double *sigt, cudaStream_t st) {
         const size_t sm = SliceSmem<NBK>::bytes;
-        cudaError_t e = set_smem(k_sigma_slice<NBK, GT>, sm);
+        cudaError_t e = set_smem(k_sigma_slice<NBK>, sm);
         if (e != cudaSuccess) return e;
-        const int ahead = resident_ctas(k_sigma_slice<NBK, GT>, kSliceThreads, sm);
-        k_sigma_slice<NBK, GT><<<g->nw0 + 1, kSliceThreads, sm, st>>>(Grt, V, g->tw_k, g->n8, g->nw0, ahead, sigt);
+        const int ahead = resident_ctas(k_sigma_slice<NBK>, kSliceThreads, sm);
+        k_sigma_slice<NBK><<<g->nw0 + 1, kSliceThreads, sm, st>>>(Grt, V, g->tw_k, g->n8, g->nw0, ahead, sigt);
         return launched();
     }
 };

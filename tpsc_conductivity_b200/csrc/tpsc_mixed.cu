@@ -40,69 +40,27 @@ struct Slice32Smem {
     static constexpr size_t slice_bytes = (size_t)NBK * NBK * sizeof(float);
     static constexpr size_t scr_off = (slice_bytes + 15) & ~(size_t)15;
     static constexpr size_t tw_off = scr_off + (size_t)NGRP * padded_len(L) * sizeof(float2);
-    static constexpr size_t bytes = tw_off + (size_t)L * sizeof(float4);
+    // the L twiddles, and for L = 256 the second pass's twiddles transposed
+    // behind them (15 x 16, see stockham_pass)
+    static constexpr int NTW = L + (L == 256 ? 15 * 16 : 0);
+    static constexpr size_t bytes = tw_off + (size_t)NTW * sizeof(float4);
 };
 
-// Input staging of the slice kernels whose inputs are rows of global arrays
-// (chi0, V, Sigma): the slice and the FFT scratch are idle until the fill, so
-// a CTA first copies its input rows there with asynchronous copies (all in
-// flight at once: one memory latency per slice instead of one per batch of
-// loads), waits for its own copies, and forms the slice from shared memory.
+// Input staging (see stage_blockrow / fill_from_staged): the FP32 slices'
+// input rows fit in the slice and FFT scratch, which are idle until the fill
 template <int NBK>
 struct Stage32 {
     static constexpr int N8 = NBK * (NBK + 1) / 2;
-    static constexpr int N8P = (N8 + 3) & ~3;
-    static constexpr int PER = (N8 + kSlice32Threads - 1) / kSlice32Threads;  // octant points per thread
-    static constexpr size_t blockrow_bytes = (size_t)N8P * sizeof(double);      // one row of a column-block array
+    static constexpr size_t blockrow_bytes = StageRows<NBK>::blockrow_bytes;
     static constexpr size_t frow_bytes = ((size_t)N8 * sizeof(float) + 15) & ~(size_t)15;  // one FP32 G row
     static_assert(blockrow_bytes + frow_bytes <= Slice32Smem<NBK>::tw_off, "inputs must fit before the twiddles");
     static_assert(2 * frow_bytes <= Slice32Smem<NBK>::tw_off, "inputs must fit before the twiddles");
 };
 
-__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-// row j of a column-block array a (NJ rows) -> dst[o], o < N8P (16-byte copies)
-template <int NBK>
-__device__ __forceinline__ void stage_blockrow(double *dst, const double *__restrict__ a, int j, int NJ) {
-    for (int i = threadIdx.x; i < Stage32<NBK>::N8P / 2; i += blockDim.x) {
-        const int b = i >> 1, h = i & 1;
-        cp_async16(dst + 4 * b + 2 * h, a + ((size_t)b * NJ + j) * 4 + 2 * h);
-    }
-}
 // n8 floats from src -> dst (4-byte copies: the FP32 G rows are not 16-byte aligned)
 template <int NBK>
 __device__ __forceinline__ void stage_frow(float *dst, const float *__restrict__ src) {
-    for (int o = threadIdx.x; o < Stage32<NBK>::N8; o += blockDim.x) cp_async4(dst + o, src + o);
-}
-// Form the symmetric slice from value(o), which reads the staged inputs:
-// every thread computes its octant points into registers, then a barrier (the
-// staging area overlaps the slice), then the writes of both triangles.
-template <int NBK, class Value>
-__device__ __forceinline__ void fill_from_staged(float *S, const Value &value) {
-    constexpr int N8 = Stage32<NBK>::N8, PER = Stage32<NBK>::PER;
-    float v[PER];
-#pragma unroll
-    for (int b = 0; b < PER; ++b) {
-        const int o = threadIdx.x + b * kSlice32Threads;
-        if (o < N8) v[b] = value(o);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int b = 0; b < PER; ++b) {
-        const int o = threadIdx.x + b * kSlice32Threads;
-        if (o < N8) {
-            int l, m;
-            oct_lm(o, l, m);
-            S[l * NBK + m] = v[b];
-            S[m * NBK + l] = v[b];
-        }
-    }
+    for (int o = threadIdx.x; o < StageRows<NBK>::N8; o += blockDim.x) cp_async4(dst + o, src + o);
 }
 
 template <int NBK>
@@ -110,11 +68,16 @@ __device__ __forceinline__ float2 *scratch32(float *S) {
     return reinterpret_cast<float2 *>(reinterpret_cast<char *>(S) + Slice32Smem<NBK>::scr_off);
 }
 
-// the hi/lo twiddles in shared memory; the kernel's first barrier publishes them
+// the hi/lo twiddles in shared memory, and for L = 256 entry 256 + (q-1) 16 + k
+// = tw[k q] (q = 1..15, k < 16); the kernel's first barrier publishes them
 template <int NBK>
 __device__ __forceinline__ const float4 *twiddles32(float *S, const float4 *__restrict__ tw) {
+    constexpr int L = Slice32Smem<NBK>::L;
     float4 *t = reinterpret_cast<float4 *>(reinterpret_cast<char *>(S) + Slice32Smem<NBK>::tw_off);
-    for (int i = threadIdx.x; i < Slice32Smem<NBK>::L; i += blockDim.x) t[i] = __ldg(&tw[i]);
+    for (int i = threadIdx.x; i < Slice32Smem<NBK>::NTW; i += blockDim.x) {
+        const int m = i < L ? i : (((i - L) & 15) * ((i - L) / 16 + 1)) & (L - 1);
+        t[i] = __ldg(&tw[m]);
+    }
     return t;
 }
 
@@ -167,7 +130,7 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
     stage_frow<NBK>(gm, Grt + (size_t)(nw0 - j) * n8);
     cp_async_wait_all();
     __syncthreads();
-    fill_from_staged<NBK>(S32, [&](int o) -> float {
+    fill_from_staged<NBK, kSlice32Threads>(S32, [&](int o) -> float {
         const double a = gp[o];
         double c;
         if (j == 0)
@@ -207,7 +170,7 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
     stage_blockrow<NBK>(cs, chiq, j, nb);
     cp_async_wait_all();
     __syncthreads();
-    fill_from_staged<NBK>(S32, [&](int o) -> float {
+    fill_from_staged<NBK, kSlice32Threads>(S32, [&](int o) -> float {
         const double c0 = cs[o];
         const double a = 0.5 * Usp, b = 0.5 * Uch;
         const double ds = 1.0 - a * c0, dc = 1.0 + b * c0;
@@ -272,7 +235,7 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
     cp_async_wait_all();
     __syncthreads();
     // octant points o < NOCT are exactly those with l <= R
-    fill_from_staged<NBK>(S32, [&](int o) -> float {
+    fill_from_staged<NBK, kSlice32Threads>(S32, [&](int o) -> float {
         const double x = (double)gs[o] * vs[o];
         if (o < NOCT) {
             xn[o] = x;
