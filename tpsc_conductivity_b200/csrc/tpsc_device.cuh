@@ -253,6 +253,11 @@ __device__ void spline_second_derivatives(double *A, int lda, int NJ, double h, 
     const int N = NJ - 1;
     const double a6 = 6.0 / (h * h), b6 = 6.0 / h, ih = 1.0 / h;
     const double dl = d0[c], dr = dN[c];
+    // interior rows kSplinePivotConst <= i < N share one pivot, 1/p = cp: a
+    // register instead of a load in the sweeps' dependent chains
+    const double cpiv = N > kSplinePivotConst ? __ldg(&invp[kSplinePivotConst]) : 0.0;
+    auto piv = [&](int i) -> double { return (i >= kSplinePivotConst && i < N) ? cpiv : __ldg(&invp[i]); };
+    auto sup = [&](int i) -> double { return (i >= kSplinePivotConst && i < N) ? cpiv : __ldg(&cp[i]); };
     auto rhs = [&](int i, double vm, double v0, double vp) -> double {
         if (i == 0) return b6 * ((vp - v0) * ih - dl);
         if (i == N) return b6 * (dr - (v0 - vm) * ih);
@@ -266,7 +271,7 @@ __device__ void spline_second_derivatives(double *A, int lda, int NJ, double h, 
             double vm = i0 > 0 ? y[i0 - 1] : 0.0, v0 = y[i0];
             for (int i = i0; i < s; ++i) {
                 const double vp = y[i + 1];
-                cc = (rhs(i, vm, v0, vp) - cc) * __ldg(&invp[i]);
+                cc = (rhs(i, vm, v0, vp) - cc) * piv(i);
                 vm = v0;
                 v0 = vp;
             }
@@ -281,7 +286,7 @@ __device__ void spline_second_derivatives(double *A, int lda, int NJ, double h, 
         double vm = vm_h, v0 = vs_h;
         for (int i = s; i < e; ++i) {
             const double vp = (i + 1 < e) ? y[i + 1] : ve_h;
-            const double dp = (rhs(i, vm, v0, vp) - carry) * __ldg(&invp[i]);
+            const double dp = (rhs(i, vm, v0, vp) - carry) * piv(i);
             y[i] = dp;
             carry = dp;
             vm = v0;
@@ -293,14 +298,14 @@ __device__ void spline_second_derivatives(double *A, int lda, int NJ, double h, 
     if (s < e && e < NJ) {
         const int i1 = min(N, e - 1 + kWarm);
         double mm = 0.0;
-        for (int i = i1; i >= e; --i) mm = y[i] - __ldg(&cp[i]) * mm;
+        for (int i = i1; i >= e; --i) mm = y[i] - sup(i) * mm;
         mc = mm;
     }
     __syncthreads();
     if (s < e) {
         double mm = mc;
         for (int i = e - 1; i >= s; --i) {
-            mm = y[i] - __ldg(&cp[i]) * mm;
+            mm = y[i] - sup(i) * mm;
             y[i] = mm;
         }
     }

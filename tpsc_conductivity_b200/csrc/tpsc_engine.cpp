@@ -9,7 +9,6 @@
 
 #include <algorithm>
 #include <cmath>
-#include <cstdio>
 #include <cstring>
 #include <initializer_list>
 #include <limits>
@@ -458,7 +457,7 @@ double hessian_ek_xx(double kx, double ky, double tp, double tpp, double t3) {
 
 // Thomas-algorithm tables of the clamped-spline system with NJ nodes:
 // invp[i] = 1/pivot_i, cp[i] = superdiagonal / pivot (cp[NJ-1] = 0).
-void spline_tables(int NJ, std::vector<double> &out) {
+bool spline_tables(int NJ, std::vector<double> &out) {
     out.assign(2 * NJ, 0.0);
     const int N = NJ - 1;
     long double cpv = 0.0L;
@@ -474,6 +473,11 @@ void spline_tables(int NJ, std::vector<double> &out) {
         cpv = (i < N) ? 1.0L / p : 0.0L;
         out[NJ + i] = (double)cpv;
     }
+    // the device sweeps take rows kSplinePivotConst..N-1 as one constant: the
+    // pivots converge to 2 + sqrt(3) within ~15 rows, so this always holds
+    for (int i = kSplinePivotConst; i < N; ++i)
+        if (out[i] != out[kSplinePivotConst] || out[NJ + i] != out[kSplinePivotConst]) return false;
+    return true;
 }
 
 void twiddles(int N, long double sign, long double scale, std::vector<double2> &out) {
@@ -543,8 +547,10 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
     twiddles(nw0, -2.0L, 1.0L, tww);
     twiddles(nw0, 1.0L, 1.0L, htw);
     std::vector<double> sh, sf;
-    spline_tables(d.nb, sh);
-    spline_tables(nw0 + 1, sf);
+    if (!spline_tables(d.nb, sh) || !spline_tables(nw0 + 1, sf)) {
+        delete g;
+        return fail(ctx, TPSC_ERR_ARG, "spline pivot tables are not constant from the interior row on");
+    }
     cudaError_t e = cudaSuccess;
     const size_t n8 = d.n8, n8p = d.n8p, nb = d.nb, nw = nw0;
 #define A(x)                                       \

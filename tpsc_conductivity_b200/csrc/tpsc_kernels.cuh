@@ -35,6 +35,12 @@ __host__ __device__ inline size_t bidx(int j, int o, int NJ) {
     return ((size_t)(o >> 2) * NJ + j) * 4 + (o & 3);
 }
 
+// The clamped-spline system's Thomas pivots converge to 2 + sqrt(3): from this
+// row on (up to the last row) the pivot tables hold one constant, which the
+// spline sweeps use instead of loading the entry (the host checks the tables
+// where it builds them)
+constexpr int kSplinePivotConst = 32;
+
 constexpr int kMaxBlocks = 4096;
 constexpr int kTailP = 41;  // P_p for p < kTailP: the find_mu tail series uses p <= kMuMomP + 28
 constexpr int kTailQ = 20;  // Q_k for k < kTailQ (the series uses k <= 18)  // >= column blocks of the largest grid (2097)
