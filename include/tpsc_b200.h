@@ -304,6 +304,16 @@ int tpsc_sigma_iqn(tpsc_ctx *ctx, int nq, double *sigma, double *sigma_bubble);
  * of the sum-rule stage (tpsc_sumrule_tangents) give dD exactly; a tangent
  * of the Sigma and chi_jj stages is not built, so this is the sigma path. */
 int tpsc_sigma_iqn_fd(tpsc_ctx *ctx, int nq, const double h[3], double *dsigma, double dD[3]);
+/* The backward pair of tpsc_sigma_iqn (no counterpart in the reference): for
+ * the cotangent cot[n - 1] on sigma(iq_n), n = 1..nq (with vertex correction,
+ * one angle bin), grad[p] = sum_n cot[n-1] d sigma(iq_n) / d theta_p,
+ * theta = {U, mu, t'} as in tpsc_sigma_iqn_fd, by one reverse pass through
+ * chi_jj, mu (an implicit root), Sigma and V in FP64 on the device, chained
+ * with the forward tangents of chi0 and of the sum-rule roots
+ * (tpsc_sumrule_tangents, which it runs).  dD (may be NULL) = d D / d theta.
+ * Needs the self-energy and mu of the current grid (a solve); the point is
+ * not re-solved. */
+int tpsc_sigma_iqn_bwd(tpsc_ctx *ctx, int nq, const double *cot, double grad[3], double dD[3]);
 /* Continued-fraction Pade continuation of sigma(iq_n), n = 1..Nn, and of
  * sigma_bubble to z = w + i eta for the Nw real frequencies w:
  * out [2][Nw] complex interleaved (sigma, then sigma_bubble). */

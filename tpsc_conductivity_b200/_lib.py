@@ -93,6 +93,7 @@ SIGNATURES = [
     ("tpsc_get_chijj3", C.c_int, [C.c_void_p, C.c_int, _ip, _ip, _dp, _dp]),
     ("tpsc_sigma_iqn", C.c_int, [C.c_void_p, C.c_int, _dp, _dp]),
     ("tpsc_sigma_iqn_fd", C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp]),
+    ("tpsc_sigma_iqn_bwd", C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp]),
     ("tpsc_sigma_pade", C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int, C.c_double, _dp]),
     ("tpsc_pade_batch", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _dp]),
     ("tpsc_sumrule_noalloc", C.c_int,

@@ -342,6 +342,16 @@ class CondOpt(Green):
         self._nbins = 1
         return ds, dD
 
+    def sigma_qn_vjp(self, cot):
+        """The backward pair of sigma_qn: grad[p] = sum_n cot[n-1] d sigma(iq_n)
+        / d theta_p, theta = (U, mu, t'), by one reverse pass on the device
+        (mu a shift of mu0 at fixed n, t' at fixed n).  Needs a solve of the
+        current grid.  Returns (grad [3], dD [3])."""
+        c = np.ascontiguousarray(np.atleast_1d(np.asarray(cot, dtype=np.float64)))
+        grad, dD = np.zeros(3), np.zeros(3)
+        self.ctx.call("tpsc_sigma_iqn_bwd", int(c.size), _dptr(c), _dptr(grad), _dptr(dD))
+        return grad, dD
+
     def sigma_pade(self, w, Nn=64, eta=0.0):
         """Pade continuation of sigma(iq_n), n = 1..Nn, to w + i eta:
         (sigma(w), sigma_bubble(w)) complex arrays."""

@@ -242,7 +242,9 @@ __device__ __forceinline__ void put_sym(double *S, int l, int m, double v) {
 // each chunk starts its carry kWarm rows early from zero; the carry decays
 // by 1/p_i <= 1/(2+sqrt3) per row, so the truncation error is below 1e-17 of
 // the local magnitude.  All threads of the block must call.
-template <int NC = 4>
+// RAW: y already holds the right-hand side (the adjoint of the spline solves
+// the same symmetric system); h, d0 and dN are not used.
+template <int NC = 4, bool RAW = false>
 __device__ void spline_second_derivatives(double *A, int lda, int NJ, double h, const double *d0, const double *dN,
                                           const double *__restrict__ invp, const double *__restrict__ cp) {
     const int TPC = blockDim.x / NC;
@@ -252,13 +254,14 @@ __device__ void spline_second_derivatives(double *A, int lda, int NJ, double h, 
     const int s = min(k * C, NJ), e = min(s + C, NJ);
     const int N = NJ - 1;
     const double a6 = 6.0 / (h * h), b6 = 6.0 / h, ih = 1.0 / h;
-    const double dl = d0[c], dr = dN[c];
+    const double dl = RAW ? 0.0 : d0[c], dr = RAW ? 0.0 : dN[c];
     // interior rows kSplinePivotConst <= i < N share one pivot, 1/p = cp: a
     // register instead of a load in the sweeps' dependent chains
     const double cpiv = N > kSplinePivotConst ? __ldg(&invp[kSplinePivotConst]) : 0.0;
     auto piv = [&](int i) -> double { return (i >= kSplinePivotConst && i < N) ? cpiv : __ldg(&invp[i]); };
     auto sup = [&](int i) -> double { return (i >= kSplinePivotConst && i < N) ? cpiv : __ldg(&cp[i]); };
     auto rhs = [&](int i, double vm, double v0, double vp) -> double {
+        if (RAW) return v0;
         if (i == 0) return b6 * ((vp - v0) * ih - dl);
         if (i == N) return b6 * (dr - (v0 - vm) * ih);
         return a6 * (vp - 2.0 * v0 + vm);

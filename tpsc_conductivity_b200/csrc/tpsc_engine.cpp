@@ -313,9 +313,15 @@ struct Grid {
     double tail_max = 0.0;                   // max |chi| over the tail
     double *d_mom_suf = nullptr, *d_cmax_suf = nullptr, *d_tailm = nullptr;  // on the device
     // forward tangents (tpsc_sumrule_tangents; allocated on first use)
-    double *t_dGrt = nullptr, *t_dchiq = nullptr, *t_ddq0 = nullptr, *t_dcinf = nullptr, *t_dcinf2 = nullptr;
+    // (the two directions' dG(r, tau), dchi0(q, iqn) and end tables are kept
+    // in adj for the reverse pass)
+    double *t_ddq0 = nullptr, *t_dcinf = nullptr, *t_dcinf2 = nullptr;
     double *t_der = nullptr;
     double2 *t_fd = nullptr;
+    double t_dmu0_tp = 0.0;   // d mu0 / d t' at fixed density of the last tangents
+    // the reverse pass of sigma(iq_n) (tpsc_sigma_iqn_bwd; allocated on first use)
+    AdjDev adj;
+    bool adj_alloc = false;
     double tailq_T = -1.0;         // temperature the tail power sums were built for
     double tailq_host[kTailQ] = {0};
     double tailP_host[kTailP] = {0};
@@ -1735,14 +1741,19 @@ int tpsc_sumrule_tangents(tpsc_ctx *ctx, double out[9]) {
     cudaSetDevice(ctx->device);
     const GridDev &d = g->d;
     const size_t n8 = d.n8, n8p = d.n8p, nb = d.nb, nw = d.nw0;
-    if (!g->t_dGrt) {
+    if (!g->adj.dGrt[0]) {
         cudaError_t e = cudaSuccess;
 #define A(x)                                       \
     if (e == cudaSuccess) {                        \
         e = (x);                                   \
     }
-        A(dalloc(g, &g->t_dGrt, (nw + 1) * n8));
-        A(dalloc(g, &g->t_dchiq, nb * n8p));
+        for (int q = 0; q < 2; ++q) {
+            A(dalloc(g, &g->adj.dGrt[q], (nw + 1) * n8));
+            A(dalloc(g, &g->adj.dchiq[q], nb * n8p));
+            A(dalloc(g, &g->adj.ddG0p[q], n8));
+            A(dalloc(g, &g->adj.ddchir[q], n8));
+        }
+        A(dalloc(g, &g->adj.der2, n8));
         A(dalloc(g, &g->t_ddq0, n8));
         A(dalloc(g, &g->t_dcinf, n8));
         A(dalloc(g, &g->t_dcinf2, n8));
@@ -1781,6 +1792,7 @@ int tpsc_sumrule_tangents(tpsc_ctx *ctx, double out[9]) {
     // mu0, src/green0.cpp:182-262); the half-filled symmetric point keeps 0,
     // which is also the density root there
     const double dmu0_dtp = sw != 0.0 ? swd / sw : 0.0;
+    g->t_dmu0_tp = dmu0_dtp;
     // d R / d theta at fixed (Usp, Uch) from the chi0 tangent, theta = mu, t'
     double dRsp[3] = {0, 0, 0}, dRch[3] = {0, 0, 0};
     for (int p = 1; p < 3; ++p) {
@@ -1797,20 +1809,25 @@ int tpsc_sumrule_tangents(tpsc_ctx *ctx, double out[9]) {
         }
         CK(cudaMemcpyAsync(g->t_fd, fd.data(), n8 * sizeof(double2), cudaMemcpyHostToDevice, ctx->st));
         CK(cudaMemcpyAsync(g->t_der, der.data(), n8 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+        if (p == 2)
+            CK(cudaMemcpyAsync(g->adj.der2, der.data(), n8 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+        double *dchiq = g->adj.dchiq[p - 1];
         TangentBufs tb;
         tb.Grt = g->Grt;
         tb.dG0p = g->dG0p;
         tb.der = g->t_der;
         tb.fd = g->t_fd;
-        tb.dGrt = g->t_dGrt;
-        tb.dchiq = g->t_dchiq;
+        tb.dGrt = g->adj.dGrt[p - 1];
+        tb.dchiq = dchiq;
         tb.ddq0 = g->t_ddq0;
+        tb.ddG0p = g->adj.ddG0p[p - 1];
+        tb.ddchir = g->adj.ddchir[p - 1];
         CK(launch_chi0_tangent(d, tb, mu0, dmu0, T, ctx->st));
-        CK(launch_chi0_tau(d, g->t_dchiq, g->t_ddq0, g->t_dcinf, g->t_dcinf2, T, ctx->st));
-        CK(launch_sumrule_tan(d, g->chiq, g->t_dchiq, g->cinf, g->cinf2, g->t_dcinf, g->t_dcinf2, Usp, -1.0, T,
+        CK(launch_chi0_tau(d, dchiq, g->t_ddq0, g->t_dcinf, g->t_dcinf2, T, ctx->st));
+        CK(launch_sumrule_tan(d, g->chiq, dchiq, g->cinf, g->cinf2, g->t_dcinf, g->t_dcinf2, Usp, -1.0, T,
                               ctx->red, ctx->st));
         if ((rc = read_result(ctx, 1, &dRsp[p]))) return rc;
-        CK(launch_sumrule_tan(d, g->chiq, g->t_dchiq, g->cinf, g->cinf2, g->t_dcinf, g->t_dcinf2, Uch, 1.0, T,
+        CK(launch_sumrule_tan(d, g->chiq, dchiq, g->cinf, g->cinf2, g->t_dcinf, g->t_dcinf2, Uch, 1.0, T,
                               ctx->red, ctx->st));
         if ((rc = read_result(ctx, 1, &dRch[p]))) return rc;
     }
@@ -2585,6 +2602,172 @@ int tpsc_sigma_iqn_fd(tpsc_ctx *ctx, int nq, const double h[3], double *dsigma, 
         return rc;
     }
     return rc2;
+}
+
+// buffers of the reverse pass, on first use per grid (the cond tables first)
+int ensure_adj(tpsc_ctx *ctx, Grid *g) {
+    if (g->adj_alloc) return TPSC_OK;
+    const GridDev &d = g->d;
+    const CondDev &c = g->cond;
+    AdjDev &a = g->adj;
+    int nblk = 0;
+    CK(cond_bwd_blocks(d, &nblk));
+    a.nblk = std::max(1, std::min(nblk, c.K4));
+    const size_t NO = d.nw0 / 2, NJ = d.nw0 + 1, nb = d.nb, K4 = c.K4, K4p = c.K4p, n8 = d.n8, n8p = d.n8p;
+    a.row_ct = 0;
+    a.row_cl = a.row_ct + a.nblk;
+    a.row_cb = a.row_cl + 2 * d.nbk;
+    a.row_cs = a.row_cb + 2;
+    a.row_sg = a.row_cs + (int)nb;
+    a.row_ss = a.row_sg + (int)n8;
+    a.row_sb = a.row_ss + (int)nb;
+    a.row_vt = a.row_sb + 1;
+    a.row_vq = a.row_vt + (int)n8;
+    a.rows = a.row_vq + (int)nb;
+    cudaError_t e = cudaSuccess;
+#define A(x)                \
+    if (e == cudaSuccess) { \
+        e = (x);            \
+    }
+    A(dalloc(g, &a.cw, NO + 1));
+    A(dalloc(g, &a.ws, (size_t)a.nblk * 2 * NO));
+    A(dalloc(g, &a.hVb, K4p * NJ));
+    A(dalloc(g, &a.dbb, 2 * K4p));
+    A(dalloc(g, &a.sigc, K4 * NO));
+    A(dalloc(g, &a.sigl, (size_t)2 * d.nbk * NO));
+    A(dalloc(g, &a.tmpB, 2 * K4p));
+    A(dalloc(g, &a.vbk, 2 * K4p));
+    A(dalloc(g, &a.preb, 2 * K4p));
+    A(dalloc(g, &a.dchb, 2 * K4p));
+    A(dalloc(g, &a.tmpU, nb * K4p));
+    A(dalloc(g, &a.vcond, nb * K4p));
+    A(dalloc(g, &a.Sb, n8 * NO));
+    A(dalloc(g, &a.s2b, n8));
+    A(dalloc(g, &a.s3b, n8));
+    A(dalloc(g, &a.stb, NJ * n8p));
+    A(dalloc(g, &a.dSb, 2 * n8p));
+    A(dalloc(g, &a.Vb, nb * n8p));
+    A(dalloc(g, &a.part, (size_t)a.rows * kAdjW));
+#undef A
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "reverse-pass allocation");
+    g->adj_alloc = true;
+    return TPSC_OK;
+}
+
+// sums of the partial-row slots over rows [r0, r1) of the reverse pass, in row order
+int adj_rows(tpsc_ctx *ctx, const AdjDev &a, int r0, int r1, std::vector<double> &rows) {
+    rows.assign((size_t)(r1 - r0) * kAdjW, 0.0);
+    CK(cudaMemcpyAsync(rows.data(), a.part + (size_t)r0 * kAdjW, rows.size() * sizeof(double),
+                       cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return TPSC_OK;
+}
+double adj_slot(const std::vector<double> &rows, int slot) {
+    double s = 0.0, c = 0.0;  // compensated, in row order
+    for (size_t i = slot; i < rows.size(); i += kAdjW) {
+        const double y = rows[i] - c, t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    return s;
+}
+
+int tpsc_sigma_iqn_bwd(tpsc_ctx *ctx, int nq, const double *cot, double grad[3], double dD[3]) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    if (!cot || !grad) return fail(ctx, TPSC_ERR_ARG, "null cotangent or gradient");
+    Grid *g = ctx->cur;
+    if (!g->have_S || ctx->scal[TPSC_S_EVALS_MU] == 0)
+        return fail(ctx, TPSC_ERR_STATE, "the self-energy and mu must be computed first");
+    if (nq < 1 || nq > ctx->Nw0 / 2) return fail(ctx, TPSC_ERR_ARG, "need 1 <= nq <= Nw0/2");
+    if (ctx->nk0 < 8) return fail(ctx, TPSC_ERR_ARG, "need nk0 >= 8");
+    for (int n = 0; n < nq; ++n)
+        if (!std::isfinite(cot[n])) return fail(ctx, TPSC_ERR_ARG, "non-finite cotangent");
+    cudaSetDevice(ctx->device);
+    // forward tangents of the chi0 stage and the roots' sensitivities (also
+    // leaves the FP64 G(r, tau) in g->Grt)
+    double J[9];
+    if ((rc = tpsc_sumrule_tangents(ctx, J))) return rc;
+    if ((rc = ensure_cond(ctx, g, std::max(1, g->cond_bins)))) return rc;
+    if ((rc = ensure_adj(ctx, g))) return rc;
+    const GridDev &d = g->d;
+    const CondDev &c = g->cond;
+    AdjDev &a = g->adj;
+    const double T = ctx->T, U = ctx->U, Usp = ctx->Usp, Uch = ctx->Uch, mu = ctx->scal[TPSC_S_MU], mu0 = g->mu0;
+    const double fact4 = U * (3.0 * Usp + Uch) / 4.0, fact8 = U * (3.0 * Usp + Uch) / 8.0;
+    const double dmu0_2 = g->t_dmu0_tp;
+    const int NO = d.nw0 / 2;
+    // d L / d chi_jj(iq_n) and d L / d kx0 for L = sum_n cot_n sigma(iq_n)
+    std::vector<double> cw(NO + 1, 0.0);
+    double kx0b = 0.0;
+    for (int n = 1; n <= nq; ++n) {
+        cw[n] = -cot[n - 1] / (2.0 * PI * n * T);
+        kx0b += cw[n];
+    }
+    CK(cudaMemcpyAsync(a.cw, cw.data(), cw.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    // the h slices at the solved point, then chi_jj backward
+    CK(launch_cond_slices(d, c, g->V, g->dchirt0, mu0, T, fact4, ctx->st));
+    CondBwdArgs ca;
+    ca.hV = c.hV;
+    ca.dbound = c.dbound;
+    ca.S = g->S;
+    ca.s2 = g->s2;
+    ca.s3 = g->s3;
+    ca.sinf = g->sinf;
+    ca.ek = d.ek;
+    ca.dek = c.dek;
+    ca.d2ek = c.d2ek;
+    ca.spl_full = d.spl_full;
+    ca.spl_half = d.spl_half;
+    ca.tw = d.tw_w;
+    ca.ht = d.ht_w;
+    ca.cw = a.cw;
+    ca.kx0b = kx0b;
+    ca.ws = a.ws;
+    ca.hVb = a.hVb;
+    ca.dbb = a.dbb;
+    ca.sigc = a.sigc;
+    ca.part = a.part + (size_t)a.row_ct * kAdjW;
+    ca.K4 = c.K4;
+    ca.K4p = c.K4p;
+    ca.nbk = d.nbk;
+    ca.mu = mu;
+    ca.T = T;
+    ca.nf = 1.0 / ((double)d.nk0 * d.nk0);
+    CK(launch_cond_tau_bwd(d, ca, a.nblk, ctx->st));
+    CK(launch_cond_lines_bwd(d, c, a, g->S, g->s2, g->s3, g->sinf, mu, T, kx0b, ctx->st));
+    // mu is the root of traceDiffG: its cotangent moves to Sigma, eps and mu0
+    // through lam = -(d L / d mu) / (d traceDiffG / d mu)
+    std::vector<double> rows;
+    if ((rc = adj_rows(ctx, a, a.row_ct, a.row_cb, rows))) return rc;
+    const double mub = adj_slot(rows, kAdjMu);
+    const double sinfb_c = adj_slot(rows, kAdjSinf);
+    CK(launch_trace_diff_G(d, g->S, g->s2, g->s3, g->s4, g->sinf, mu0, mu, T, ctx->red, ctx->st));
+    double fr[2];
+    if ((rc = read_result(ctx, 2, fr))) return rc;
+    if (!(fr[1] != 0.0) || !std::isfinite(fr[1])) return fail(ctx, TPSC_ERR_NONFINITE, "d traceDiffG / d mu is zero");
+    const double lam = -mub / fr[1];
+    CK(launch_cond_slices_bwd(d, c, a, g->V, g->dchirt0, mu0, T, fact4, dmu0_2, ctx->st));
+    CK(launch_sigbar(d, c, a, g->S, g->s2, g->s3, g->s4, g->sinf, mu0, mu, lam, T, dmu0_2, ctx->st));
+    if ((rc = adj_rows(ctx, a, a.row_sg, a.row_sg + d.n8, rows))) return rc;
+    const double sinfb = sinfb_c + adj_slot(rows, kAdjSinf);
+    CK(launch_sigma_tau_bwd(d, a, sinfb, T, ctx->st));
+    CK(launch_sigma_slices_bwd(d, c, a, g->Grt, g->V, g->dchirt0, g->dG0p, mu0, fact8, dmu0_2, ctx->st));
+    CK(launch_vertex_bwd(d, a, g->chirt, g->chiq, g->Grt, U, Usp, Uch, T, ctx->st));
+    if ((rc = adj_rows(ctx, a, 0, a.rows, rows))) return rc;
+    // assembly: the mu0-shift and t' directions from the contractions; U, and
+    // the roots' sensitivities d{Usp, Uch}/d theta (J) for every direction
+    const double f4b = adj_slot(rows, kAdjFact4), f8b = adj_slot(rows, kAdjFact8);
+    const double Uspb = adj_slot(rows, kAdjUsp) + f4b * 3.0 * U / 4.0 + f8b * 3.0 * U / 8.0;
+    const double Uchb = adj_slot(rows, kAdjUch) + f4b * U / 4.0 + f8b * U / 8.0;
+    const double Ub = adj_slot(rows, kAdjU) + f4b * (3.0 * Usp + Uch) / 4.0 + f8b * (3.0 * Usp + Uch) / 8.0;
+    const double th[3] = {Ub, adj_slot(rows, kAdjTh1), adj_slot(rows, kAdjTh2)};
+    for (int p = 0; p < 3; ++p) {
+        grad[p] = th[p] + Uspb * J[3 * p] + Uchb * J[3 * p + 1];
+        if (dD) dD[p] = J[3 * p + 2];
+        if (!std::isfinite(grad[p])) return fail(ctx, TPSC_ERR_NONFINITE, "non-finite gradient");
+    }
+    return TPSC_OK;
 }
 
 int pade_batch(tpsc_ctx *ctx, int nf, int Nn, const double *x, const double *y, int Nz, const double *z,

@@ -100,6 +100,8 @@ struct TangentBufs {
     double *dGrt = nullptr;  // [(Nw0+1) n8]  dG(r, tau)
     double *dchiq = nullptr; // blocked nb    dchi0(q, tau) -> dchi0(q, iqn) after launch_chi0_tau
     double *ddq0 = nullptr;  // [n8]          d of d/dtau chi0(q, 0)
+    double *ddG0p = nullptr; // [n8] or null  d of d/dtau G(r, 0+)
+    double *ddchir = nullptr; // [n8] or null d of d/dtau chi0(r, 0)
 };
 // dG(r, tau), dchi0(q, tau_j) and d(d/dtau chi0(q, 0)) for the direction in t
 // (mu0 the primal chemical potential, dmu0 its direction)
@@ -229,6 +231,74 @@ cudaError_t launch_cond_tau(const GridDev &g, const CondDev &c, const double2 *S
 // kx = 0, pi lines and the ordered sum of the partial rows -> c.out
 cudaError_t launch_cond_finish(const GridDev &g, const CondDev &c, const double2 *S, const double *s2,
                                const double *s3, const double *sinf, double mu, double T, cudaStream_t st);
+
+// ---- the reverse pass of V -> Sigma -> mu -> chi_jj -> sigma(iq_n) (tpsc_adjoint.cu)
+// Every backward kernel leaves per-CTA rows of kAdjW partial sums: the loss
+// derivative along mu, Sigma_inf, the mu0-shift and t' directions (through
+// the tangents), and along fact4 = U(3Usp+Uch)/4, fact8 = U(3Usp+Uch)/8,
+// Usp, Uch and U held fixed elsewhere.  The host adds the rows in order.
+constexpr int kAdjW = 12;
+enum AdjSlot { kAdjMu = 0, kAdjSinf, kAdjTh1, kAdjTh2, kAdjFact4, kAdjFact8, kAdjUsp, kAdjUch, kAdjU };
+struct AdjDev {
+    // forward tangents of the chi0 stage along the mu0 shift [0] and t' [1]
+    double *dGrt[2] = {nullptr, nullptr};   // [(Nw0+1) n8]
+    double *dchiq[2] = {nullptr, nullptr};  // blocked nb: dchi0(q, iqn)
+    double *ddG0p[2] = {nullptr, nullptr};  // [n8] d of d/dtau G(r, 0+)
+    double *ddchir[2] = {nullptr, nullptr}; // [n8] d of d/dtau chi0(r, 0)
+    double *der2 = nullptr;                 // [n8] the hopping table's direction along t'
+    double *cw = nullptr;                   // [Nw0/2 + 1] d L / d chi_jj(iq_n)
+    double2 *ws = nullptr;                  // [nblk 2 (Nw0/2)] per-CTA G(ik_n), J(ik_n)
+    double *hVb = nullptr;                  // [K4p (Nw0+1)] two-column blocks: d L / d hV
+    double *dbb = nullptr;                  // [2 K4p] d L / d dhV(0), dhV(beta)
+    double2 *sigc = nullptr;                // [K4 (Nw0/2)] d L / d Sigma per K4 column
+    double2 *sigl = nullptr;                // [2 nbk (Nw0/2)] the same on the kx = 0, pi lines
+    double *tmpB = nullptr, *vbk = nullptr, *preb = nullptr, *dchb = nullptr;  // [2 K4p] each
+    double *tmpU = nullptr, *vcond = nullptr;                                  // [nb K4p] each
+    double2 *Sb = nullptr;                  // [n8 (Nw0/2)] d L / d S, column-major
+    double *s2b = nullptr, *s3b = nullptr;  // [n8]
+    double *stb = nullptr;                  // blocked Nw0+1: d L / d Sigma(k, tau)
+    double *dSb = nullptr;                  // [2 n8p]
+    double *Vb = nullptr;                   // blocked nb: d L / d V(r, tau), then d L / d V(r, iqn)
+    double *part = nullptr;                 // [rows kAdjW]
+    int nblk = 0;
+    int row_ct = 0, row_cl = 0, row_cb = 0, row_cs = 0, row_sg = 0, row_ss = 0, row_sb = 0, row_vt = 0, row_vq = 0;
+    int rows = 0;
+};
+struct CondBwdArgs {
+    const double *hV = nullptr, *dbound = nullptr;
+    const double2 *S = nullptr;
+    const double *s2 = nullptr, *s3 = nullptr, *sinf = nullptr;
+    const double *ek = nullptr, *dek = nullptr, *d2ek = nullptr;
+    const double *spl_full = nullptr, *spl_half = nullptr;
+    const double2 *tw = nullptr, *ht = nullptr;
+    const double *cw = nullptr;
+    double kx0b = 0.0;
+    double2 *ws = nullptr;
+    double *hVb = nullptr, *dbb = nullptr;
+    double2 *sigc = nullptr;
+    double *part = nullptr;
+    int K4 = 0, K4p = 0, nbk = 0;
+    double mu = 0.0, T = 0.0, nf = 0.0;
+};
+cudaError_t cond_bwd_blocks(const GridDev &g, int *blocks);
+cudaError_t launch_cond_tau_bwd(const GridDev &g, const CondBwdArgs &a, int nblk, cudaStream_t st);
+cudaError_t launch_cond_lines_bwd(const GridDev &g, const CondDev &c, const AdjDev &a, const double2 *S,
+                                  const double *s2, const double *s3, const double *sinf, double mu, double T,
+                                  double kx0b, cudaStream_t st);
+// the chi_jj boundary (two CTAs) and h slices (one CTA per tau pair) backward
+cudaError_t launch_cond_slices_bwd(const GridDev &g, const CondDev &c, const AdjDev &a, const double *V,
+                                   const double *dchirt0, double mu0, double T, double fact4, double dmu0_2,
+                                   cudaStream_t st);
+// lam = -(d L / d mu) / (d traceDiffG / d mu)
+cudaError_t launch_sigbar(const GridDev &g, const CondDev &c, const AdjDev &a, const double2 *S, const double *s2,
+                          const double *s3, const double *s4, const double *sinf, double mu0, double mu, double lam,
+                          double T, double dmu0_2, cudaStream_t st);
+cudaError_t launch_sigma_tau_bwd(const GridDev &g, const AdjDev &a, double sinfb, double T, cudaStream_t st);
+cudaError_t launch_sigma_slices_bwd(const GridDev &g, const CondDev &c, const AdjDev &a, const double *Grt,
+                                    const double *V, const double *dchirt0, const double *dG0p, double mu0,
+                                    double fact8, double dmu0_2, cudaStream_t st);
+cudaError_t launch_vertex_bwd(const GridDev &g, const AdjDev &a, const double *chirt, const double *chiq,
+                              const double *Grt, double U, double Usp, double Uch, double T, cudaStream_t st);
 
 // ---- Aslamazov-Larkin correction chijj3 on the non-uniform iqn grid --------
 // (tpsc_al.cu).  Arrays on the K4 grid of the correlator; NJ = Nw0 + 1 tau

@@ -82,7 +82,8 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     k_chi0_boundary_tan(const double *__restrict__ ek, const double *__restrict__ er, const double *__restrict__ der,
                         const double2 *__restrict__ fd, const double2 *__restrict__ tw, const double *__restrict__ Grt,
                         const double *__restrict__ dGrt, const double *__restrict__ dG0p, int n8, double mu0,
-                        double dmu0, double T, double nk02, double *__restrict__ d_dtau_chiqt0) {
+                        double dmu0, double T, double nk02, double *__restrict__ d_dtau_chiqt0,
+                        double *__restrict__ out_ddG0p, double *__restrict__ out_ddchir) {
     extern __shared__ __align__(16) double S[];
     const auto *tws = slice_twiddles<NBK>(S, tw);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
@@ -108,6 +109,8 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
         const double g0 = Grt[o], dg0 = dGrt[o];
         dc_[k] = (o == 0) ? -2.0 * (ddp * (1.0 + g0) + dp * dg0 + ddm * g0 + dm * dg0)
                           : -2.0 * (ddp * g0 + dp * dg0 + ddm * g0 + dm * dg0);
+        if (out_ddG0p) out_ddG0p[o] = ddp;
+        if (out_ddchir) out_ddchir[o] = dc_[k];
     }
     __syncthreads();
     k = 0;
@@ -140,7 +143,8 @@ struct RunChi0Tan {
         k_chi0_slice_tan<NBK><<<g->nb, kSliceThreads, sm, st>>>(t->Grt, t->dGrt, g->tw_k, g->n8, g->nw0, t->dchiq);
         if ((e = launched()) != cudaSuccess) return e;
         k_chi0_boundary_tan<NBK><<<1, kSliceThreads, sm, st>>>(g->ek, g->er, t->der, t->fd, g->tw_k, t->Grt, t->dGrt,
-                                                               t->dG0p, g->n8, mu0, dmu0, T, nk02, t->ddq0);
+                                                               t->dG0p, g->n8, mu0, dmu0, T, nk02, t->ddq0,
+                                                               t->ddG0p, t->ddchir);
         return launched();
     }
 };
