@@ -566,17 +566,29 @@ def extra_configs():
     g4.find_Usp_Uch_grid(128, 2048)
     g4.sumrule_tangents()
     J, t4 = timed(g4.sumrule_tangents)
-    # sigma(iq1): central differences of full FP64 solves (no tangent of the
-    # Sigma and chi_jj stages yet)
+    # sigma(iq1): the reverse pass (tpsc_sigma_iqn_bwd) after one solve +
+    # chi_jj, and the central differences of full FP64 solves beside it
     g4.solve()
+    g4.ctx.call("tpsc_chijj", 1)
+    _, t4f = timed(lambda: (g4.solve(), g4.ctx.call("tpsc_chijj", 1)))
+    g4.sigma_qn_vjp([1.0])
+    (gr4, _), t4b = timed(lambda: g4.sigma_qn_vjp([1.0]))
     g4.sigma_qn_sensitivities(1)
     (ds4, dD4), t4s = timed(lambda: g4.sigma_qn_sensitivities(1))
     out["c4_l128_w2048_sensitivities"] = {
         "ms": t4, "d_dU": J["U"], "d_dmu": J["mu"], "d_dtp": J["tp"],
         "checked": "central differences, tests/test_gpu_tangent.py",
-        "sigma_iq1": {"ms": t4s, "d_dU": float(ds4[0, 0]), "d_dmu": float(ds4[1, 0]), "d_dtp": float(ds4[2, 0]),
-                      "method": "central differences of six FP64 Newton solves + chi_jj, h = 1e-5, "
-                                "base point solved again; tests/test_gpu_sigma_fd.py"}}
+        "sigma_iq1": {"reverse_pass": {"ms": t4b, "d_dU": float(gr4[0]), "d_dmu": float(gr4[1]),
+                                       "d_dtp": float(gr4[2]),
+                                       "method": "tpsc_sigma_iqn_bwd: chi_jj, mu, Sigma, V backward (FP64) chained "
+                                                 "with the chi0 and sum-rule forward tangents; "
+                                                 "tests/test_gpu_adjoint.py"},
+                      "forward_ms": t4f, "reverse_over_forward": t4b / t4f,
+                      "central_differences": {"ms": t4s, "d_dU": float(ds4[0, 0]), "d_dmu": float(ds4[1, 0]),
+                                              "d_dtp": float(ds4[2, 0]),
+                                              "method": "six FP64 Newton solves + chi_jj, h = 1e-5, base point "
+                                                        "solved again; tests/test_gpu_sigma_fd.py"},
+                      "max_rel_diff": float(np.max(np.abs(gr4 - ds4[:, 0])) / np.max(np.abs(ds4[:, 0])))}}
     out["timing"] = "host wall clock around each call after a warm-up run, device idle at both ends"
     return out
 

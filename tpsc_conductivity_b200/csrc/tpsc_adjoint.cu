@@ -115,8 +115,15 @@ struct CondBwdCol {
     double k0sb, dGsb, dJsb, C1bs, mub, eb, sinfb;
 };
 
+// threads of the backward tau kernel: one FFT group (N/16) from N = 2048 on,
+// so that every thread works in the FFTs and two CTAs share an SM up to 2048
 template <int N>
-__global__ void __launch_bounds__(256, 1) k_cond_tau_bwd(const CondBwdArgs a) {
+constexpr int cond_bwd_threads() {
+    return N >= 4096 ? 256 : 128;
+}
+
+template <int N>
+__global__ void __launch_bounds__(cond_bwd_threads<N>(), N >= 4096 ? 1 : 2) k_cond_tau_bwd(const CondBwdArgs a) {
     constexpr int NJ = N + 1, NO = N / 2, NJ2 = NO + 1;
     constexpr int G = FftPlan<N>::G;
     using SM = CondBwdSmem<N>;
@@ -680,16 +687,36 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     }
 }
 
+// per-K4-point table of the h slices' backward: (x, A, dA/dx, dA/d dek,
+// dx/dt', d dek/dt') with x = eps - mu0, A = nf dek (1 - f) or nf dek f
+// (the branch of k_cond_table), the t' direction at fixed density
+__global__ void k_hbwd_table(const double *__restrict__ ek, const double *__restrict__ dek, int K4, int nbk,
+                             double mu0, double T, double nf, double dmu0_2, double *__restrict__ tab) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= K4) return;
+    const HPoint p = h_point(ek, dek, c, nbk, mu0, T, nf);
+    double de, ddek, dd2;
+    tp_dirs(c / nbk + 1, c % nbk, nbk, de, ddek, dd2);
+    double *t = tab + 8 * (size_t)c;
+    t[0] = p.x;
+    t[1] = p.A;
+    t[2] = nf * dek[c] * p.dbase;
+    t[3] = nf * p.base;
+    t[4] = de - dmu0_2;
+    t[5] = ddek;
+    t[6] = 0.0;
+    t[7] = 0.0;
+}
+
 // CTA jv = 0..Nw0/2 takes tau_j and tau_{Nw0 - j} (j = jv): u_j = T^T hVb(j);
 // V-bar(jv) in the K4 layout (2 h_j u_j summed over the pair) -> vcond; the
 // cotangent of h_j (2 V u_j, plus the boundary's at tau = 0, beta) through
 // T^T into the parameter directions.  tmpU: [nb][K4p] scratch.
 template <int NBK>
 __global__ void __launch_bounds__(kSliceThreads, 1)
-    k_cond_slice_bwd(const double *__restrict__ ek, const double *__restrict__ dek, const double *__restrict__ V,
-                     const double *__restrict__ hVb, const double *__restrict__ preb, const double2 *__restrict__ tw,
-                     int nw0, int K4p, double mu0, double T, double nf, double dmu0_2, double *__restrict__ tmpU,
-                     double *__restrict__ vcond, double *__restrict__ part) {
+    k_cond_slice_bwd(const double *__restrict__ htab, const double *__restrict__ V, const double *__restrict__ hVb,
+                     const double *__restrict__ preb, const double2 *__restrict__ tw, int nw0, int K4p, double T,
+                     double *__restrict__ tmpU, double *__restrict__ vcond, double *__restrict__ part) {
     constexpr int K4 = (NBK - 2) * NBK;
     extern __shared__ __align__(16) double S[];
     const auto *tws = slice_twiddles<NBK>(S, tw);
@@ -711,8 +738,8 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
         __syncthreads();
         // h_j = T (A E(t))
         for (int c = threadIdx.x; c < K4; c += blockDim.x) {
-            const HPoint p = h_point(ek, dek, c, NBK, mu0, T, nf);
-            S[c] = p.A * h_E(p.x, t, beta);
+            const double2 xa = *reinterpret_cast<const double2 *>(htab + 8 * (size_t)c);
+            S[c] = xa.y * h_E(xa.x, t, beta);
         }
         __syncthreads();
         dst_dct_slice<NBK>(S, slice_scratch<NBK>(S), tws);
@@ -729,16 +756,16 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
         __syncthreads();
         dst_dct_slice<NBK>(S, slice_scratch<NBK>(S), tws);
         for (int c = threadIdx.x; c < K4; c += blockDim.x) {
-            const int l = c / NBK, m = c % NBK;
-            const double s = S[c] * edge_w(m, NBK);
-            const HPoint p = h_point(ek, dek, c, NBK, mu0, T, nf);
-            const double E = h_E(p.x, t, beta), dEx = h_dEdx(p.x, t, beta) * E;
-            double de, ddek, dd2;
-            tp_dirs(l + 1, m, NBK, de, ddek, dd2);
-            // d(A E) = (nf dk dbase E + A dE/dx) dx + nf base E ddek
-            const double gx = nf * dek[c] * p.dbase * E + p.A * dEx;
+            const double s = S[c] * edge_w(c % NBK, NBK);
+            const double *tc = htab + 8 * (size_t)c;
+            const double2 xa = *reinterpret_cast<const double2 *>(tc);
+            const double2 gb = *reinterpret_cast<const double2 *>(tc + 2);
+            const double2 dd = *reinterpret_cast<const double2 *>(tc + 4);
+            const double E = h_E(xa.x, t, beta), dEx = h_dEdx(xa.x, t, beta) * E;
+            // d(A E) = (dA/dx E + A dE/dx) dx + dA/d dek E d dek
+            const double gx = gb.x * E + xa.y * dEx;
             th1 += s * (-gx);
-            th2 += s * (gx * (de - dmu0_2) + nf * p.base * E * ddek);
+            th2 += s * (gx * dd.x + gb.y * E * dd.y);
         }
         __syncthreads();
     }
@@ -1157,7 +1184,7 @@ struct RunCondTauBwd {
         const size_t sm = CondBwdSmem<N>::bytes;
         cudaError_t e = set_smem(k_cond_tau_bwd<N>, sm);
         if (e != cudaSuccess) return e;
-        k_cond_tau_bwd<N><<<nblk, 256, sm, st>>>(*a);
+        k_cond_tau_bwd<N><<<nblk, cond_bwd_threads<N>(), sm, st>>>(*a);
         return launched();
     }
 };
@@ -1170,7 +1197,8 @@ struct CondBwdBlocks {
         int dev = 0, sms = 0, per = 0;
         if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
         if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cond_tau_bwd<N>, 256, sm)) != cudaSuccess)
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cond_tau_bwd<N>, cond_bwd_threads<N>(), sm)) !=
+            cudaSuccess)
             return e;
         *blocks = sms * (per > 0 ? per : 1);
         return cudaSuccess;
@@ -1189,9 +1217,10 @@ struct RunCondSliceBwd {
                                                                 g->nw0, c->K4p, mu0, T, nf, fact4, dmu0_2, a->tmpB,
                                                                 a->vbk, a->preb, a->dchb, a->part + a->row_cb * kAdjW);
         if ((e = launched()) != cudaSuccess) return e;
-        k_cond_slice_bwd<NBK><<<g->nb, kSliceThreads, sm, st>>>(g->ek, c->dek, V, a->hVb, a->preb, g->tw_k, g->nw0,
-                                                                 c->K4p, mu0, T, nf, dmu0_2, a->tmpU, a->vcond,
-                                                                 a->part + a->row_cs * kAdjW);
+        k_hbwd_table<<<(c->K4 + 255) / 256, 256, 0, st>>>(g->ek, c->dek, c->K4, g->nbk, mu0, T, nf, dmu0_2, a->htab);
+        if ((e = launched()) != cudaSuccess) return e;
+        k_cond_slice_bwd<NBK><<<g->nb, kSliceThreads, sm, st>>>(a->htab, V, a->hVb, a->preb, g->tw_k, g->nw0, c->K4p,
+                                                                 T, a->tmpU, a->vcond, a->part + a->row_cs * kAdjW);
         return launched();
     }
 };

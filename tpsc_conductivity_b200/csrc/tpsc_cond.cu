@@ -699,8 +699,9 @@ __global__ void __launch_bounds__(256)
 // ---------------------------------------------------------------------------
 template <int NBK>
 struct RunCondSlices {
+    // ny = 2: the h and f0 slices and all four end conditions; ny = 1: h only
     static cudaError_t run(const GridDev *g, const CondDev *c, const double *V, const double *dchirt0, double mu0,
-                           double T, double fact, cudaStream_t st) {
+                           double T, double fact, int ny, cudaStream_t st) {
         const size_t sm = SliceSmem<NBK>::bytes;
         cudaError_t e = set_smem(k_cond_slice<NBK>, sm);
         if (e != cudaSuccess) return e;
@@ -708,10 +709,10 @@ struct RunCondSlices {
         const double nf = 1.0 / ((double)g->nk0 * g->nk0);
         k_cond_table<<<(c->K4 + 255) / 256, 256, 0, st>>>(g->ek, c->dek, c->K4, g->nbk, mu0, T, nf, c->tab);
         if ((e = launched()) != cudaSuccess) return e;
-        k_cond_slice<NBK><<<dim3(g->nw0 + 1, 2), kSliceThreads, sm, st>>>(c->tab, V, g->tw_k, g->nw0, T, c->K4p,
-                                                                           c->hV, c->f0V, c->pre);
+        k_cond_slice<NBK><<<dim3(g->nw0 + 1, ny), kSliceThreads, sm, st>>>(c->tab, V, g->tw_k, g->nw0, T, c->K4p,
+                                                                            c->hV, c->f0V, c->pre);
         if ((e = launched()) != cudaSuccess) return e;
-        k_cond_boundary<NBK><<<4, kSliceThreads, sm, st>>>(g->ek, c->dek, V, dchirt0, g->tw_k, c->pre, g->nw0, c->K4p,
+        k_cond_boundary<NBK><<<2 * ny, kSliceThreads, sm, st>>>(g->ek, c->dek, V, dchirt0, g->tw_k, c->pre, g->nw0, c->K4p,
                                                             mu0, T, nf, fact, c->dbound);
         return launched();
     }
@@ -783,7 +784,12 @@ cudaError_t launch_cond_table(const GridDev &g, const CondDev &c, double mu0, do
 
 cudaError_t launch_cond_slices(const GridDev &g, const CondDev &c, const double *V, const double *dtau_chirt0,
                                double mu0, double T, double fact, cudaStream_t st) {
-    return dispatch_nbk<RunCondSlices>(g.nbk, &g, &c, V, dtau_chirt0, mu0, T, fact, st);
+    return dispatch_nbk<RunCondSlices>(g.nbk, &g, &c, V, dtau_chirt0, mu0, T, fact, 2, st);
+}
+
+cudaError_t launch_cond_slices_h(const GridDev &g, const CondDev &c, const double *V, const double *dtau_chirt0,
+                                 double mu0, double T, double fact, cudaStream_t st) {
+    return dispatch_nbk<RunCondSlices>(g.nbk, &g, &c, V, dtau_chirt0, mu0, T, fact, 1, st);
 }
 
 cudaError_t launch_cond_tau(const GridDev &g, const CondDev &c, const double2 *S, const double *s2, const double *s3,

@@ -2641,6 +2641,7 @@ int ensure_adj(tpsc_ctx *ctx, Grid *g) {
     A(dalloc(g, &a.dchb, 2 * K4p));
     A(dalloc(g, &a.tmpU, nb * K4p));
     A(dalloc(g, &a.vcond, nb * K4p));
+    A(dalloc(g, &a.htab, 8 * K4));
     A(dalloc(g, &a.Sb, n8 * NO));
     A(dalloc(g, &a.s2b, n8));
     A(dalloc(g, &a.s3b, n8));
@@ -2706,7 +2707,7 @@ int tpsc_sigma_iqn_bwd(tpsc_ctx *ctx, int nq, const double *cot, double grad[3],
     }
     CK(cudaMemcpyAsync(a.cw, cw.data(), cw.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
     // the h slices at the solved point, then chi_jj backward
-    CK(launch_cond_slices(d, c, g->V, g->dchirt0, mu0, T, fact4, ctx->st));
+    CK(launch_cond_slices_h(d, c, g->V, g->dchirt0, mu0, T, fact4, ctx->st));
     CondBwdArgs ca;
     ca.hV = c.hV;
     ca.dbound = c.dbound;

@@ -225,6 +225,9 @@ cudaError_t launch_cond_table(const GridDev &g, const CondDev &c, double mu0, do
 // table + h V, f0 V slices + end conditions (fact = U (3 Usp + Uch)/4)
 cudaError_t launch_cond_slices(const GridDev &g, const CondDev &c, const double *V, const double *dtau_chirt0,
                                double mu0, double T, double fact, cudaStream_t st);
+// the h slices and their two end conditions only (the reverse pass's forward values)
+cudaError_t launch_cond_slices_h(const GridDev &g, const CondDev &c, const double *V, const double *dtau_chirt0,
+                                 double mu0, double T, double fact, cudaStream_t st);
 // per-k pairs -> c.partial (zeroed first)
 cudaError_t launch_cond_tau(const GridDev &g, const CondDev &c, const double2 *S, const double *s2, const double *s3,
                             const double *sinf, double mu, double T, cudaStream_t st);
@@ -254,6 +257,7 @@ struct AdjDev {
     double2 *sigl = nullptr;                // [2 nbk (Nw0/2)] the same on the kx = 0, pi lines
     double *tmpB = nullptr, *vbk = nullptr, *preb = nullptr, *dchb = nullptr;  // [2 K4p] each
     double *tmpU = nullptr, *vcond = nullptr;                                  // [nb K4p] each
+    double *htab = nullptr;                 // [8 K4] the h slices' point table of the reverse pass
     double2 *Sb = nullptr;                  // [n8 (Nw0/2)] d L / d S, column-major
     double *s2b = nullptr, *s3b = nullptr;  // [n8]
     double *stb = nullptr;                  // blocked Nw0+1: d L / d Sigma(k, tau)
