@@ -210,7 +210,11 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
 // ---------------------------------------------------------------------------
 template <int N>
 struct CondTauSmem {
-    static constexpr int threads = TauSmem<N>::threads;
+    // one FFT group (N/16 threads) up to N = 2048, so that every thread works
+    // in the FFTs and two CTAs share an SM (the kernel needs ~240 registers
+    // a thread, which holds a 256-thread CTA to one per SM); 256 beyond
+    static constexpr int threads = N >= 4096 ? TauSmem<N>::threads : 128;
+    static constexpr int min_blocks = N >= 4096 ? 1 : 2;
     static constexpr size_t r_bytes = ((size_t)2 * (N + 1) * sizeof(double) + 15) & ~(size_t)15;
     static constexpr size_t x_bytes = (size_t)padded_len(N) * sizeof(double2);
     static constexpr size_t tables_off = r_bytes + 2 * x_bytes;
@@ -266,7 +270,7 @@ __device__ __forceinline__ void tails(const ColState &q, double tau, double beta
 
 
 template <int N>
-__global__ void __launch_bounds__(CondTauSmem<N>::threads, 1) k_cond_tau(const CondTauArgs a) {
+__global__ void __launch_bounds__(CondTauSmem<N>::threads, CondTauSmem<N>::min_blocks) k_cond_tau(const CondTauArgs a) {
     constexpr int NJ = N + 1, NO = N / 2, NJ2 = NO + 1;
     constexpr int G = FftPlan<N>::G;
     extern __shared__ __align__(16) double R[];
@@ -645,8 +649,24 @@ __global__ void k_cond_finish(const double *__restrict__ partial, int nblk, int 
     }
     KSum tot;
     for (int bin = 0; bin < nbins; ++bin) {
+        // eight independent compensated sums over the rows b = r mod 8 (their
+        // loads overlap), added in a fixed order: deterministic
+        constexpr int NS = 8;
+        KSum s8[NS];
+        int b = 0;
+        for (; b + NS <= nblk; b += NS) {
+            double v[NS];
+#pragma unroll
+            for (int r = 0; r < NS; ++r) v[r] = partial[(size_t)(b + r) * pw + bin * PWB + i];
+#pragma unroll
+            for (int r = 0; r < NS; ++r) s8[r].add(v[r]);
+        }
+        for (; b < nblk; ++b) s8[b % NS].add(partial[(size_t)b * pw + bin * PWB + i]);
         KSum s;
-        for (int b = 0; b < nblk; ++b) s.add(partial[(size_t)b * pw + bin * PWB + i]);
+        for (int r = 0; r < NS; ++r) {
+            s.add(s8[r].s);
+            s.add(s8[r].c);
+        }
         const double v = s.value();
         out[(size_t)bin * PWB + i] = v;
         tot.add(v);
@@ -701,7 +721,7 @@ template <int NBK>
 struct RunCondSlices {
     // ny = 2: the h and f0 slices and all four end conditions; ny = 1: h only
     static cudaError_t run(const GridDev *g, const CondDev *c, const double *V, const double *dchirt0, double mu0,
-                           double T, double fact, int ny, cudaStream_t st) {
+                           double T, double fact, int ny, bool f32, cudaStream_t st) {
         const size_t sm = SliceSmem<NBK>::bytes;
         cudaError_t e = set_smem(k_cond_slice<NBK>, sm);
         if (e != cudaSuccess) return e;
@@ -709,9 +729,13 @@ struct RunCondSlices {
         const double nf = 1.0 / ((double)g->nk0 * g->nk0);
         k_cond_table<<<(c->K4 + 255) / 256, 256, 0, st>>>(g->ek, c->dek, c->K4, g->nbk, mu0, T, nf, c->tab);
         if ((e = launched()) != cudaSuccess) return e;
-        k_cond_slice<NBK><<<dim3(g->nw0 + 1, ny), kSliceThreads, sm, st>>>(c->tab, V, g->tw_k, g->nw0, T, c->K4p,
-                                                                            c->hV, c->f0V, c->pre);
-        if ((e = launched()) != cudaSuccess) return e;
+        if (f32) {
+            if ((e = launch_cond_slice32(*g, *c, V, T, ny, st)) != cudaSuccess) return e;
+        } else {
+            k_cond_slice<NBK><<<dim3(g->nw0 + 1, ny), kSliceThreads, sm, st>>>(c->tab, V, g->tw_k, g->nw0, T,
+                                                                                c->K4p, c->hV, c->f0V, c->pre);
+            if ((e = launched()) != cudaSuccess) return e;
+        }
         k_cond_boundary<NBK><<<2 * ny, kSliceThreads, sm, st>>>(g->ek, c->dek, V, dchirt0, g->tw_k, c->pre, g->nw0, c->K4p,
                                                             mu0, T, nf, fact, c->dbound);
         return launched();
@@ -784,12 +808,17 @@ cudaError_t launch_cond_table(const GridDev &g, const CondDev &c, double mu0, do
 
 cudaError_t launch_cond_slices(const GridDev &g, const CondDev &c, const double *V, const double *dtau_chirt0,
                                double mu0, double T, double fact, cudaStream_t st) {
-    return dispatch_nbk<RunCondSlices>(g.nbk, &g, &c, V, dtau_chirt0, mu0, T, fact, 2, st);
+    return dispatch_nbk<RunCondSlices>(g.nbk, &g, &c, V, dtau_chirt0, mu0, T, fact, 2, false, st);
+}
+
+cudaError_t launch_cond_slices32(const GridDev &g, const CondDev &c, const double *V, const double *dtau_chirt0,
+                                 double mu0, double T, double fact, cudaStream_t st) {
+    return dispatch_nbk<RunCondSlices>(g.nbk, &g, &c, V, dtau_chirt0, mu0, T, fact, 2, true, st);
 }
 
 cudaError_t launch_cond_slices_h(const GridDev &g, const CondDev &c, const double *V, const double *dtau_chirt0,
                                  double mu0, double T, double fact, cudaStream_t st) {
-    return dispatch_nbk<RunCondSlices>(g.nbk, &g, &c, V, dtau_chirt0, mu0, T, fact, 1, st);
+    return dispatch_nbk<RunCondSlices>(g.nbk, &g, &c, V, dtau_chirt0, mu0, T, fact, 1, false, st);
 }
 
 cudaError_t launch_cond_tau(const GridDev &g, const CondDev &c, const double2 *S, const double *s2, const double *s3,

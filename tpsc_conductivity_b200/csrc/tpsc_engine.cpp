@@ -1424,7 +1424,10 @@ int run_cond(tpsc_ctx *ctx, int nbins) {
     const double mu = ctx->scal[TPSC_S_MU];
     const double fact = ctx->U * (3.0 * ctx->Usp + ctx->Uch) / 4.0;  // TPSC_fact (src/cond_opt.cpp:2892)
     CK(cudaEventRecord(ctx->ev[0], ctx->st));
-    CK(launch_cond_slices(d, c, g->V, g->dchirt0, g->mu0, ctx->T, fact, ctx->st));
+    if (ctx->form & TPSC_FORM_MIXED)
+        CK(launch_cond_slices32(d, c, g->V, g->dchirt0, g->mu0, ctx->T, fact, ctx->st));
+    else
+        CK(launch_cond_slices(d, c, g->V, g->dchirt0, g->mu0, ctx->T, fact, ctx->st));
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
     CK(launch_cond_tau(d, c, g->S, g->s2, g->s3, g->sinf, mu, ctx->T, ctx->st));
     CK(cudaEventRecord(ctx->ev[2], ctx->st));

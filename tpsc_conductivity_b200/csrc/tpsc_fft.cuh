@@ -416,8 +416,8 @@ __device__ void dct2_slice(T *S, C *scr, const TW *tw) {
 // extension of two packed lines, the DST through the odd extension
 // z = [0, X, 0, -reverse(X)], whose transform is -i Y_a + Y_b for the packed
 // pair a + i b.  Same calling rules as dct2_slice.
-template <int NBK, class TW>
-__device__ void dst_dct_slice(double *S, double2 *scr, const TW *tw) {
+template <int NBK, class T, class C, class TW>
+__device__ void dst_dct_slice(T *S, C *scr, const TW *tw) {
     constexpr int L = 2 * (NBK - 1);
     constexpr int NR = NBK - 2;
     constexpr int G = FftPlan<L>::G;
@@ -425,19 +425,19 @@ __device__ void dst_dct_slice(double *S, double2 *scr, const TW *tw) {
     const int grp = tid / G;
     const int t = tid % G;
     const int ngrp = blockDim.x / G;
-    double2 *x = scr + grp * padded_len(L);
+    C *x = scr + grp * padded_len(L);
     // rows: DCT-I along m, NR lines
 #pragma unroll 1
     for (int p = grp; p < (NR + 1) / 2; p += ngrp) {
         const int r0 = 2 * p, r1 = 2 * p + 1;
         const bool two = r1 < NR;
-        double *a = S + r0 * NBK;
-        double *b = S + (two ? r1 : r0) * NBK;
-        auto in = [&](int j) -> double2 {
+        T *a = S + r0 * NBK;
+        T *b = S + (two ? r1 : r0) * NBK;
+        auto in = [&](int j) -> C {
             const int c = j < NBK ? j : L - j;
-            return make_double2(a[c], two ? b[c] : 0.0);
+            return C{a[c], two ? b[c] : (T)0};
         };
-        auto out = [&](int k, double2 z) {
+        auto out = [&](int k, C z) {
             if (k < NBK) {
                 a[k] = z.x;
                 if (two) b[k] = z.y;
@@ -452,15 +452,15 @@ __device__ void dst_dct_slice(double *S, double2 *scr, const TW *tw) {
     for (int p = grp; p < (NBK + 1) / 2; p += ngrp) {
         const int c0 = 2 * p, c1 = 2 * p + 1;
         const bool two = c1 < NBK;
-        double *a = S + c0;
-        double *b = S + (two ? c1 : c0);
-        auto in = [&](int j) -> double2 {
-            if (j == 0 || j == NR + 1) return make_double2(0.0, 0.0);
-            if (j <= NR) return make_double2(a[(j - 1) * NBK], two ? b[(j - 1) * NBK] : 0.0);
+        T *a = S + c0;
+        T *b = S + (two ? c1 : c0);
+        auto in = [&](int j) -> C {
+            if (j == 0 || j == NR + 1) return C{(T)0, (T)0};
+            if (j <= NR) return C{a[(j - 1) * NBK], two ? b[(j - 1) * NBK] : (T)0};
             const int r = L - j - 1;
-            return make_double2(-a[r * NBK], two ? -b[r * NBK] : 0.0);
+            return C{-a[r * NBK], two ? -b[r * NBK] : (T)0};
         };
-        auto out = [&](int k, double2 z) {
+        auto out = [&](int k, C z) {
             if (k >= 1 && k <= NR) {
                 a[(k - 1) * NBK] = -z.y;
                 if (two) b[(k - 1) * NBK] = z.x;

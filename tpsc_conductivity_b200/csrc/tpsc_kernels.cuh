@@ -225,6 +225,13 @@ cudaError_t launch_cond_table(const GridDev &g, const CondDev &c, double mu0, do
 // table + h V, f0 V slices + end conditions (fact = U (3 Usp + Uch)/4)
 cudaError_t launch_cond_slices(const GridDev &g, const CondDev &c, const double *V, const double *dtau_chirt0,
                                double mu0, double T, double fact, cudaStream_t st);
+// the mixed form's slices: both transforms of the h and f0 slices in FP32
+// (tpsc_mixed.cu), the table and the end conditions in FP64
+cudaError_t launch_cond_slices32(const GridDev &g, const CondDev &c, const double *V, const double *dtau_chirt0,
+                                 double mu0, double T, double fact, cudaStream_t st);
+// the FP32 slice kernel alone (after the table), ny = 2: h and f0, 1: h
+cudaError_t launch_cond_slice32(const GridDev &g, const CondDev &c, const double *V, double T, int ny,
+                                cudaStream_t st);
 // the h slices and their two end conditions only (the reverse pass's forward values)
 cudaError_t launch_cond_slices_h(const GridDev &g, const CondDev &c, const double *V, const double *dtau_chirt0,
                                  double mu0, double T, double fact, cudaStream_t st);

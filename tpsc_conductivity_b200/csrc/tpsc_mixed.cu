@@ -268,6 +268,59 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
     }
 }
 
+// h V(r, tau) and f0 V(r, tau) of the correlator (k_cond_slice's stage,
+// src/cond_opt.cpp:2696-2908) with both DST x DCT transforms in FP32: the
+// slice formed in FP64 from the (x, A, B) table and rounded once, the
+// product with 2 V(r, tau) formed in FP64 from the FP32 transform and rounded
+// once; outputs kept in FP64 for the FP64 tau kernel.  h V enters only the
+// Maki-Thompson part of chi_jj and f0 V only its q_n = 0 value.
+template <int NBK>
+__global__ void __launch_bounds__(kSlice32Threads, 2)
+    k_cond_slice32(const double *__restrict__ tab, const double *__restrict__ V, const float4 *__restrict__ tw,
+                   int nw0, double T, int K4p, double *__restrict__ hV, double *__restrict__ f0V,
+                   double *__restrict__ pre) {
+    constexpr int K4 = (NBK - 2) * NBK;
+    extern __shared__ __align__(16) float S32[];
+    const float4 *tws = twiddles32<NBK>(S32, tw);
+    const int j = blockIdx.x, y = blockIdx.y;
+    const int nb = nw0 / 2 + 1;
+    const double t = j / (nw0 * T);
+    const double bt = 1.0 / T - t;
+    for (int c = threadIdx.x; c < K4; c += blockDim.x) {
+        const double2 xa = *reinterpret_cast<const double2 *>(tab + 4 * c);
+        const double b = tab[4 * c + 2];
+        const double E = exp(xa.x > 0 ? -xa.x * t : xa.x * bt);
+        S32[c] = (float)((y == 0) ? xa.y * E : (xa.y * t + b) * E);
+    }
+    __syncthreads();
+    dst_dct_slice<NBK>(S32, scratch32<NBK>(S32), tws);
+    const int jv = j < nb ? j : nw0 - j;
+    const bool edge = (j == 0 || j == nw0);
+    double *pe = pre + (size_t)(2 * y + (j == nw0 ? 1 : 0)) * K4p;
+    for (int c = threadIdx.x; c < K4; c += blockDim.x) {
+        const int l = c / NBK, m = c % NBK;
+        const double v = S32[c];
+        if (edge) pe[c] = v;
+        S32[c] = (float)(v * (2.0 * V[bidx(jv, oct_index(l + 1, m), nb)]));
+    }
+    __syncthreads();
+    dst_dct_slice<NBK>(S32, scratch32<NBK>(S32), tws);
+    double *out = (y == 0) ? hV : f0V;
+    for (int c = threadIdx.x; c < K4; c += blockDim.x) out[bidx2(j, c, nw0 + 1)] = S32[c];
+}
+
+template <int NBK>
+struct RunCondSlice32 {
+    static cudaError_t run(const GridDev *g, const CondDev *c, const double *V, double T, int ny, cudaStream_t st) {
+        const size_t sm = Slice32Smem<NBK>::bytes;
+        cudaError_t e = set_smem(k_cond_slice32<NBK>, sm);
+        if (e != cudaSuccess) return e;
+        k_cond_slice32<NBK><<<dim3(g->nw0 + 1, ny), kSlice32Threads, sm, st>>>(c->tab, V, g->tw_k32, g->nw0, T,
+                                                                               c->K4p, c->hV, c->f0V, c->pre);
+        return launched();
+    }
+};
+
 template <int NBK>
 struct RunGslice32 {
     static cudaError_t run(const GridDev *g, float *Grt, double mu0, double T, cudaStream_t st) {
@@ -319,6 +372,11 @@ struct RunSigmaSlice32 {
 };
 
 }  // namespace
+
+cudaError_t launch_cond_slice32(const GridDev &g, const CondDev &c, const double *V, double T, int ny,
+                                cudaStream_t st) {
+    return dispatch_nbk<RunCondSlice32>(g.nbk, &g, &c, V, T, ny, st);
+}
 
 cudaError_t launch_sigma_slice32(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st) {
     return dispatch_nbk<RunSigmaSlice32>(g.nbk, &g, Grt, V, sigt, st);
