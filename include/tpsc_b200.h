@@ -301,8 +301,9 @@ int tpsc_sigma_iqn(tpsc_ctx *ctx, int nq, double *sigma, double *sigma_bubble);
  * (may be NULL).  mu is the shift of mu0 at fixed n (tpsc_set_mu_shift), t'
  * moves at fixed n.  Six solves + tpsc_chijj, then the model, mu shift and
  * form are restored and the base point solved again.  The forward tangents
- * of the sum-rule stage (tpsc_sumrule_tangents) give dD exactly; a tangent
- * of the Sigma and chi_jj stages is not built, so this is the sigma path. */
+ * of the sum-rule stage (tpsc_sumrule_tangents) give dD exactly; the reverse
+ * pass tpsc_sigma_iqn_bwd gives the sigma derivatives exactly and is checked
+ * against this. */
 int tpsc_sigma_iqn_fd(tpsc_ctx *ctx, int nq, const double h[3], double *dsigma, double dD[3]);
 /* The backward pair of tpsc_sigma_iqn (no counterpart in the reference): for
  * the cotangent cot[n - 1] on sigma(iq_n), n = 1..nq (with vertex correction,
@@ -325,6 +326,23 @@ int tpsc_sigma_pade(tpsc_ctx *ctx, int Nn, const double *w, int Nw, double eta, 
  * complex points z: out [nf][Nz] complex interleaved. */
 int tpsc_pade_batch(tpsc_ctx *ctx, int nf, int Nn, const double *x, const double *y, int Nz, const double *z,
                     double *out);
+
+/* Many points at once, by shape (no counterpart in the reference, which
+ * solves one model at a time): the rows params[i] = {nk0, Nw0, n, T, tp, tpp,
+ * t3, U} are grouped by (nk0, Nw0), and each group (up to 128 points) is
+ * solved by ONE launch per stage of the Newton-form mixed-precision solve
+ * over all its points -- every point's arrays in its own arena, its scalars
+ * read on the device -- captured as one CUDA graph per group shape and size
+ * and replayed on later calls.  results: npts rows of TPSC_S_COUNT scalars
+ * (those of tpsc_solve in that form); status[i] per point (a failing point
+ * gets NaN or its partial scalars and does not stop the others).  *ms (may
+ * be NULL): host wall time of the solves, device idle at both ends.  The
+ * context's own model and grids are not changed. */
+int tpsc_solve_points(tpsc_ctx *ctx, int npts, const double *params, double *results, int *status, double *ms);
+/* Streams tpsc_solve_points spreads its groups over (1..4, default 2), the
+ * largest first onto the least loaded; each group's cooperative root searches
+ * then take 2 blocks per SM / n. */
+int tpsc_set_group_streams(tpsc_ctx *ctx, int n);
 
 /* Device time of the last tpsc_solve per stage in ms:
  * {chi0, sum rules, vertex, self energy, traces + mu}, then of the last
@@ -419,7 +437,9 @@ const char *tpsc_batch_last_error(const tpsc_batch *b);
 int tpsc_batch_streams(const tpsc_batch *b, int *nstreams);
 /* tpsc_set_graph_mode of every context of the batch (default 1); with 2,
  * each Newton-form point runs as one graph launch, the graph of its grid
- * updated in place for the point's model. */
+ * updated in place for the point's model; with 3, a Newton + mixed sweep runs
+ * by shape groups, one launch per stage over every point of a group, one
+ * graph launch per group (tpsc_solve_points on the first context). */
 int tpsc_batch_set_graph_mode(tpsc_batch *b, int mode);
 /* params: npts rows {nk0, Nw0, n, T, tp, tpp, t3, U} (row-major doubles);
  * form: enum tpsc_form; results: npts rows of TPSC_S_COUNT scalars in the

@@ -94,6 +94,8 @@ SIGNATURES = [
     ("tpsc_sigma_iqn", C.c_int, [C.c_void_p, C.c_int, _dp, _dp]),
     ("tpsc_sigma_iqn_fd", C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp]),
     ("tpsc_sigma_iqn_bwd", C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp]),
+    ("tpsc_solve_points", C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _ip, _dp]),
+    ("tpsc_set_group_streams", C.c_int, [C.c_void_p, C.c_int]),
     ("tpsc_sigma_pade", C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int, C.c_double, _dp]),
     ("tpsc_pade_batch", C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _dp]),
     ("tpsc_sumrule_noalloc", C.c_int,

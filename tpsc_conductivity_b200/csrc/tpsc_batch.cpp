@@ -193,12 +193,12 @@ const char *tpsc_batch_last_error(const tpsc_batch *b) { return b ? b->err.c_str
 
 int tpsc_batch_set_graph_mode(tpsc_batch *b, int mode) {
     if (!b) return TPSC_ERR_ARG;
-    if (mode < 0 || mode > 2) {
-        b->err = "graph mode must be 0, 1 or 2";
+    if (mode < 0 || mode > 3) {
+        b->err = "graph mode must be 0, 1, 2 or 3";
         return TPSC_ERR_ARG;
     }
     b->graph_mode = mode;
-    for (tpsc_ctx *c : b->ctxs) tpsc_set_graph_mode(c, mode);
+    for (tpsc_ctx *c : b->ctxs) tpsc_set_graph_mode(c, mode == 3 ? 2 : mode);
     return TPSC_OK;
 }
 
@@ -211,6 +211,22 @@ int tpsc_batch_streams(const tpsc_batch *b, int *nstreams) {
 int tpsc_batch_solve(tpsc_batch *b, int form, int npts, const double *params, double *results, int *status,
                      double *ms) {
     if (!valid_args(b, npts, params, results, status)) return TPSC_ERR_ARG;
+    if (b->graph_mode == 3 && form == (TPSC_FORM_NEWTON | TPSC_FORM_MIXED)) {
+        // every shape group in one launch per stage (tpsc_solve_points)
+        cudaSetDevice(b->device);
+        int rc = tpsc_solve_points(b->ctxs[0], npts, params, results, status, ms);
+        if (rc) {
+            b->err = tpsc_last_error(b->ctxs[0]);
+            return rc;
+        }
+        for (int i = 0; i < npts; ++i)
+            if (status[i]) {
+                b->err = "point " + std::to_string(i) + " failed with status " + std::to_string(status[i]) + " (" +
+                         tpsc_last_error(b->ctxs[0]) + ")";
+                return status[i];
+            }
+        return TPSC_OK;
+    }
     int first = TPSC_OK;
     const int rc = run_points(b, b->nstreams, form, npts, params, results, status, ms, &first);
     return rc ? rc : first;

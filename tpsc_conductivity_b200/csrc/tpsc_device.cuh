@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "tpsc_fft.cuh"
 #include "tpsc_kernels.cuh"
 
@@ -23,6 +25,17 @@ cudaError_t smem_optin(const void *fn);
 namespace {
 
 constexpr double kPi = 3.141592653589793;  // == acos(-1.0) in double
+
+// point blockIdx.z's copy of a per-point array (see Bp)
+template <class T>
+__device__ __forceinline__ T *at(T *ptr, long long arena) {
+    using Ch = typename std::conditional<std::is_const<T>::value, const char, char>::type;
+    return ptr ? reinterpret_cast<T *>(reinterpret_cast<Ch *>(ptr) + (long long)blockIdx.z * arena) : ptr;
+}
+// the point's scalar `slot`, or v for a plain launch
+__device__ __forceinline__ double bpar(const Bp &b, int slot, double v) {
+    return b.pp ? at(b.pp, b.arena)[slot] : v;
+}
 constexpr int kSliceThreads = 352;  // 22 groups of 16: the 65 line pairs of a 129-point pass in 3 rounds
 constexpr int kTauThreads = 256;
 constexpr int kWarm = 30;  // spline sweep warm-up: carry error <= 0.268^30 < 1e-17
@@ -93,8 +106,10 @@ __device__ void block_store(double (&v)[NV], double *partial) {
 // Sum of the per-block partials in a fixed order: warp k adds value k with
 // lane-strided compensated sums and a shuffle tree (deterministic).
 template <int NV>
-__global__ void k_finish(const double *partial, int nblocks, double *result, double offset0) {
+__global__ void k_finish(const double *partial, int nblocks, double *result, double offset0, Bp bp) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    partial = at(partial, bp.arena);
+    result = at(result, bp.arena);
     for (int k = warp; k < NV; k += blockDim.x >> 5) {
         KSum acc;
         for (int b = lane; b < nblocks; b += 32) acc.add(partial[k * kMaxBlocks + b]);
@@ -104,7 +119,9 @@ __global__ void k_finish(const double *partial, int nblocks, double *result, dou
     }
 }
 
-__global__ void k_max_finish(const double *partial, int nblocks, double *result) {
+__global__ void k_max_finish(const double *partial, int nblocks, double *result, Bp bp) {
+    partial = at(partial, bp.arena);
+    result = at(result, bp.arena);
     double m = 0.0;
     for (int b = threadIdx.x; b < nblocks; b += 32) m = fmax(m, partial[b]);
     for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
@@ -112,8 +129,8 @@ __global__ void k_max_finish(const double *partial, int nblocks, double *result)
 }
 
 template <int NV>
-cudaError_t finish(Reduce r, int nblocks, double offset0, cudaStream_t st) {
-    k_finish<NV><<<1, 32 * (NV < 32 ? NV : 32), 0, st>>>(r.partial, nblocks, r.result, offset0);
+cudaError_t finish(Reduce r, int nblocks, double offset0, cudaStream_t st, const Bp &b = Bp{}) {
+    k_finish<NV><<<dim3(1, 1, b.P), 32 * (NV < 32 ? NV : 32), 0, st>>>(r.partial, nblocks, r.result, offset0, b);
     return launched();
 }
 

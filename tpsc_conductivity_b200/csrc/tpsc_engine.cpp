@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <initializer_list>
@@ -349,6 +350,39 @@ struct Grid {
     int al_bins = 0;                              // n_theta of al_host (0: none yet)
 };
 
+// The points of one shape (nk0, Nw0) of a batched sweep, solved together:
+// every point's arrays live in its own arena (see Bp), point p's at
+// base + p * arena, and each stage of the Newton-form mixed solve is one
+// launch over all of them.  The group's solve -- upload of the points' tables
+// and scalars, the launches, the readback -- is one CUDA graph, replayed
+// while the group's point count stays the same.
+struct Group {
+    int nk0 = 0, nw0 = 0, cap = 0;  // cap: points the arenas are allocated for
+    GridDev d;                      // the shape's tables; ek, er, gk, tailq, tailP of point 0
+    char *base = nullptr;           // cap * arena bytes
+    long long arena = 0;
+    size_t in_bytes = 0;            // the per-point inputs at arena offset 0: ek, er, tailq, tailP, scalars
+    size_t res_off = 0;             // the results block: kGroupRes doubles
+    double *pp = nullptr;           // point 0's scalars [kPP]
+    float *Grt32 = nullptr;
+    double *chirt = nullptr, *chiq = nullptr, *V = nullptr, *sigt = nullptr, *dS = nullptr;
+    double *dG0p = nullptr, *dchirt0 = nullptr, *dchiqt0 = nullptr, *cinf = nullptr, *cinf2 = nullptr;
+    double2 *S = nullptr;
+    double *s2 = nullptr, *s3 = nullptr, *s4 = nullptr, *sinf = nullptr;
+    double *mom = nullptr, *cmax = nullptr, *msuf = nullptr, *csuf = nullptr, *tailm = nullptr;
+    double *dres = nullptr, *mu_out = nullptr;
+    Reduce red, redm, mu0r;
+    RootScratch roots;
+    char *h_in = nullptr;    // pinned, cap * in_bytes
+    double *h_res = nullptr; // pinned, cap * kGroupRes
+    cudaGraphExec_t gexec = nullptr;
+    int gexec_P = 0;
+};
+// results block of a point (doubles): [0, 3) chi0max, qmax; [8, 14) the
+// sum-rule roots; [16, 20) the root searches' barrier words; [20, 24) the mu
+// search; [28] Sigma_inf; [32, 64) the moment sums (Tr Sigma G0 at 32, 33)
+constexpr int kGroupRes = 64;
+
 }  // namespace
 
 struct tpsc_ctx {
@@ -395,6 +429,9 @@ struct tpsc_ctx {
     SolveKey seen_key;        // of the last direct solve
     long long graph_kernels = 0;  // in the graph of the last captured or replayed solve
     long long graph_replays = 0, graph_captures = 0;
+    std::map<std::pair<int, int>, Group *> groups;  // tpsc_solve_points' shape groups
+    int group_streams = 2;                          // streams the groups are spread over (1..4)
+    cudaStream_t gst[2] = {nullptr, nullptr};       // the third and fourth (st, st2 are the first two)
     std::string err;
 };
 
@@ -431,6 +468,14 @@ cudaError_t dalloc(Grid *g, T **p, size_t count) {
     // on the context's (non-blocking) stream, so that the kernels queued there
     // after it see the zeros: a legacy-stream memset is not ordered with them
     return cudaMemsetAsync(q, 0, count * sizeof(T) + 16, g->st);
+}
+
+void free_group(Group *q) {
+    if (q->gexec) cudaGraphExecDestroy(q->gexec);
+    if (q->base) cudaFree(q->base);
+    if (q->h_in) cudaFreeHost(q->h_in);
+    if (q->h_res) cudaFreeHost(q->h_res);
+    delete q;
 }
 
 void free_grid(Grid *g) {
@@ -645,56 +690,64 @@ int read_result(tpsc_ctx *ctx, int count, double *out, const double *src = nullp
 
 // eps_k tables of the grid for the current model, then mu0 by the density
 // root of green0::find_mu (src/green0.cpp:240-262)
-int grid_set_model(tpsc_ctx *ctx, Grid *g) {
-    GridDev &d = g->d;
-    g->ek_host.assign((size_t)d.nbk * d.nbk, 0.0);
-    // dispk on the grid from tables of cos(k) and cos(2k): the same values
-    // and the same expression, one pair of cosines per index instead of ten
-    // per point
-    std::vector<double> c1(d.nbk), c2(d.nbk);
-    for (int l = 0; l < d.nbk; ++l) {
-        const double k = l * PI / (d.nbk - 1);
+// power sums Q_k = sum_{n = Nw0/2+1}^{Nw0} qn^(-2k), qn = 2 pi n T, for the
+// sum-rule tail series (smallest terms first, long double), and
+// P_p = sum_{t=0}^{Nw0/2} w^-p, w = (Nw0 + 2t + 1) pi T: the fermionic tail of
+// the find_mu moments (largest t first, long double)
+void tail_power_sums(int nw0, double T, double tailq[kTailQ], double tailP[kTailP]) {
+    std::vector<long double> acc(kTailQ, 0.0L);
+    const int nwmax = nw0 / 2;
+    for (int j = 2 * nwmax; j > nwmax; --j) {
+        const long double wn = 2.0L * 3.141592653589793238462643383279502884L * j * (long double)T;
+        const long double x = 1.0L / (wn * wn);
+        long double xp = x;
+        for (int k = 1; k < kTailQ; ++k, xp *= x) acc[k] += xp;
+    }
+    for (int k = 0; k < kTailQ; ++k) tailq[k] = (double)acc[k];
+    std::vector<long double> pw(kTailP, 0.0L);
+    const int NO = nw0 / 2;
+    for (int t = NO; t >= 0; --t) {
+        const long double x =
+            1.0L / ((2.0L * (NO + t) + 1.0L) * 3.141592653589793238462643383279502884L * (long double)T);
+        long double xp = 1.0L;
+        for (int k = 0; k < kTailP; ++k, xp *= x) pw[k] += xp;
+    }
+    for (int k = 0; k < kTailP; ++k) tailP[k] = (double)pw[k];
+}
+
+// eps_k on the octant of the nbk x nbk quadrant (dispk from tables of cos(k)
+// and cos(2k): the same values and expression as the reference's, one pair
+// of cosines per index instead of ten per point); full = the quadrant, or null
+void octant_eps(int nbk, double tp, double tpp, double t3, double *eo, std::vector<double> *full) {
+    std::vector<double> c1(nbk), c2(nbk);
+    for (int l = 0; l < nbk; ++l) {
+        const double k = l * PI / (nbk - 1);
         c1[l] = std::cos(k);
         c2[l] = std::cos(2 * k);
     }
-    const double tp = ctx->tp, tpp = ctx->tpp, t3 = ctx->t3;
-    for (int l = 0; l < d.nbk; ++l)
-        for (int m = 0; m < d.nbk; ++m)
-            g->ek_host[m + l * d.nbk] = -2.0 * (c1[l] + c1[m]) - 4.0 * tp * c1[l] * c1[m] -
-                                        2.0 * tpp * (c2[l] + c2[m]) - 4 * t3 * (c2[l] * c1[m] + c2[m] * c1[l]);
+    if (full) full->assign((size_t)nbk * nbk, 0.0);
+    for (int l = 0; l < nbk; ++l)
+        for (int m = 0; m < nbk; ++m) {
+            const double e = -2.0 * (c1[l] + c1[m]) - 4.0 * tp * c1[l] * c1[m] - 2.0 * tpp * (c2[l] + c2[m]) -
+                             4 * t3 * (c2[l] * c1[m] + c2[m] * c1[l]);
+            if (full) (*full)[m + (size_t)l * nbk] = e;
+            if (m <= l) eo[m + (size_t)l * (l + 1) / 2] = e;
+        }
+}
+
+int grid_set_model(tpsc_ctx *ctx, Grid *g) {
+    GridDev &d = g->d;
     std::vector<double> eo(d.n8), er(d.n8, 0.0);
-    for (int l = 0; l < d.nbk; ++l)
-        for (int m = 0; m <= l; ++m) eo[m + l * (l + 1) / 2] = g->ek_host[m + l * d.nbk];
+    octant_eps(d.nbk, ctx->tp, ctx->tpp, ctx->t3, eo.data(), &g->ek_host);
     er[1] = -1;
     er[2] = -ctx->tp;
     er[3] = -ctx->tpp;
     er[4] = -ctx->t3;
     CK(cudaMemcpyAsync(d.ek, eo.data(), d.n8 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(d.er, er.data(), d.n8 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
-    // power sums Q_k = sum_{n = Nw0/2+1}^{Nw0} qn^(-2k), qn = 2 pi n T, for the
-    // sum-rule tail series (smallest terms first, long double)
     if (g->tailq_T != ctx->T) {
-        std::vector<long double> acc(kTailQ, 0.0L);
-        const int nwmax = d.nb - 1;
-        for (int j = 2 * nwmax; j > nwmax; --j) {
-            const long double wn = 2.0L * 3.141592653589793238462643383279502884L * j * (long double)ctx->T;
-            const long double x = 1.0L / (wn * wn);
-            long double xp = x;
-            for (int k = 1; k < kTailQ; ++k, xp *= x) acc[k] += xp;
-        }
-        for (int k = 0; k < kTailQ; ++k) g->tailq_host[k] = (double)acc[k];
+        tail_power_sums(d.nw0, ctx->T, g->tailq_host, g->tailP_host);
         CK(cudaMemcpyAsync(d.tailq, g->tailq_host, kTailQ * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
-        // P_p = sum_{t=0}^{Nw0/2} w^-p, w = (Nw0 + 2t + 1) pi T: the fermionic tail of
-        // the find_mu moments (largest t first, long double)
-        std::vector<long double> pw(kTailP, 0.0L);
-        const int NO = d.nw0 / 2;
-        for (int t = NO; t >= 0; --t) {
-            const long double x = 1.0L / ((2.0L * (NO + t) + 1.0L) * 3.141592653589793238462643383279502884L *
-                                          (long double)ctx->T);
-            long double xp = 1.0L;
-            for (int k = 0; k < kTailP; ++k, xp *= x) pw[k] += xp;
-        }
-        for (int k = 0; k < kTailP; ++k) g->tailP_host[k] = (double)pw[k];
         CK(cudaMemcpyAsync(d.tailP, g->tailP_host, kTailP * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
         g->tailq_T = ctx->T;
     }
@@ -1104,13 +1157,16 @@ int trace_diff_G(tpsc_ctx *ctx, double pmu, double *tr, double *dtr = nullptr) {
 // w_jc is returned for the root search, which takes the series while
 // |mu - mu0| <= kMuSeriesMax |z|_min with |z|_min = w_jc - 2 Sigma_inf / w_jc
 // (|z| >= w_n - |Im Sigma| on the series set).
-void mu_series_cut(const tpsc_ctx *ctx, int *jc_out, double *wc_out) {
-    const int NO = ctx->cur->d.nw0 / 2;
-    const double pt = PI * ctx->T;
+void mu_series_cut(int nw0, double T, int *jc_out, double *wc_out) {
+    const int NO = nw0 / 2;
+    const double pt = PI * T;
     int jc = (int)std::ceil((kMomMuRange / kMuSeriesMax / pt - 1.0) / 2.0);
     jc = std::max(0, std::min(jc, NO));
     *wc_out = (2 * jc + 1) * pt;
     *jc_out = jc;
+}
+void mu_series_cut(const tpsc_ctx *ctx, int *jc_out, double *wc_out) {
+    mu_series_cut(ctx->cur->d.nw0, ctx->T, jc_out, wc_out);
 }
 
 // The Newton form of traceSelfG + find_mu + traceSelfG2: one pass over Sigma
@@ -1611,6 +1667,9 @@ void tpsc_destroy(tpsc_ctx *ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->st) cudaStreamSynchronize(ctx->st);
     for (auto &kv : ctx->grids) free_grid(kv.second);
+    for (auto &kv : ctx->groups) free_group(kv.second);
+    for (cudaStream_t s : ctx->gst)
+        if (s) cudaStreamDestroy(s);
     if (ctx->red.partial) cudaFree(ctx->red.partial);
     if (ctx->red.result) cudaFree(ctx->red.result);
     if (ctx->red.ticket) cudaFree(ctx->red.ticket);
@@ -2103,6 +2162,380 @@ int tpsc_solve(tpsc_ctx *ctx) {
     if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[5], ctx->st));
     return finish_solve(ctx);
+}
+
+namespace {
+// ---------------------------------------------------------------------------
+// many points of one shape at once: one launch per stage (tpsc_solve_points)
+// ---------------------------------------------------------------------------
+constexpr int kGroupMax = 128;  // points per group launch (the root searches' grid is shared out)
+
+// the group of shape (nk0, nw0) with arenas for at least P points
+int group_alloc(tpsc_ctx *ctx, int nk0, int nw0, int P, Group **out) {
+    const auto key = std::make_pair(nk0, nw0);
+    auto it = ctx->groups.find(key);
+    if (it != ctx->groups.end()) {
+        if (it->second->cap >= P) {
+            *out = it->second;
+            return TPSC_OK;
+        }
+        CK(cudaStreamSynchronize(ctx->st));
+        free_group(it->second);
+        ctx->groups.erase(it);
+    }
+    Grid *g = nullptr;
+    int rc = build_grid(ctx, nk0, nw0, &g);  // the shape tables
+    if (rc) return rc;
+    Group *q = new Group;
+    q->nk0 = nk0;
+    q->nw0 = nw0;
+    q->cap = P;
+    q->d = g->d;
+    const GridDev &d = q->d;
+    const size_t n8 = d.n8, n8p = d.n8p, nb = d.nb, nw = nw0, NO = nw0 / 2;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off += (bytes + 255) & ~(size_t)255;
+        return o;
+    };
+    const size_t o_ek = take(n8 * 8), o_er = take(n8 * 8), o_tq = take(kTailQ * 8), o_tp = take(kTailP * 8),
+                 o_pp = take(kPP * 8);
+    q->in_bytes = off;
+    q->res_off = take(kGroupRes * 8);
+    const size_t o_gk = take(n8 * 16), o_grt = take((nw + 1) * n8 * 4), o_chirt = take(nb * n8p * 8),
+                 o_chiq = take(nb * n8p * 8), o_V = take(nb * n8p * 8), o_dG0p = take(n8 * 8),
+                 o_dchirt0 = take(n8 * 8), o_dchiqt0 = take(n8 * 8), o_cinf = take(n8 * 8), o_cinf2 = take(n8 * 8),
+                 o_dS = take(2 * n8p * 8), o_sigt = take((nw + 1) * n8p * 8), o_S = take(NO * n8p * 16),
+                 o_s2 = take(n8 * 8), o_s3 = take(n8 * 8), o_s4 = take(n8 * 8), o_mom = take(nb * kMomP * 8),
+                 o_cmax = take(nb * 8), o_msuf = take((nb + 1) * kMomP * 8), o_csuf = take((nb + 1) * 8),
+                 o_tailm = take((kMomP + 1) * 8), o_redp = take(4 * kMaxBlocks * 8), o_redt = take(16),
+                 o_redmp = take((size_t)std::max(2 * kMomP + 2, kSigmaMomNV) * kMaxBlocks * 8),
+                 o_redmt = take(16), o_rootp = take(4 * kRootMaxBlocks * 8);
+    q->arena = (long long)off;
+    cudaError_t e = cudaMalloc(&q->base, (size_t)P * off);
+    if (e == cudaSuccess) e = cudaMemsetAsync(q->base, 0, (size_t)P * off, ctx->st);
+    if (e == cudaSuccess) e = cudaHostAlloc(&q->h_in, (size_t)P * q->in_bytes, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc(&q->h_res, (size_t)P * kGroupRes * sizeof(double), cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        free_group(q);
+        return cuda_fail(ctx, e, "group allocation");
+    }
+    char *b0 = q->base;
+    auto P0 = [&](size_t o) { return b0 + o; };
+    q->d.ek = reinterpret_cast<double *>(P0(o_ek));
+    q->d.er = reinterpret_cast<double *>(P0(o_er));
+    q->d.tailq = reinterpret_cast<double *>(P0(o_tq));
+    q->d.tailP = reinterpret_cast<double *>(P0(o_tp));
+    q->d.gk = reinterpret_cast<double2 *>(P0(o_gk));
+    q->pp = reinterpret_cast<double *>(P0(o_pp));
+    double *res = reinterpret_cast<double *>(P0(q->res_off));
+    q->red.result = res;                  // [0, 8)
+    q->dres = res + 8;                    // [8, 16)
+    q->roots.bar = reinterpret_cast<unsigned *>(res + 16);  // [16, 20): 8 words
+    q->mu_out = res + 20;                 // [20, 28)
+    q->sinf = res + 28;                   // [28]
+    q->redm.result = res + 32;            // [32, 64)
+    q->Grt32 = reinterpret_cast<float *>(P0(o_grt));
+    q->chirt = reinterpret_cast<double *>(P0(o_chirt));
+    q->chiq = reinterpret_cast<double *>(P0(o_chiq));
+    q->V = reinterpret_cast<double *>(P0(o_V));
+    q->dG0p = reinterpret_cast<double *>(P0(o_dG0p));
+    q->dchirt0 = reinterpret_cast<double *>(P0(o_dchirt0));
+    q->dchiqt0 = reinterpret_cast<double *>(P0(o_dchiqt0));
+    q->cinf = reinterpret_cast<double *>(P0(o_cinf));
+    q->cinf2 = reinterpret_cast<double *>(P0(o_cinf2));
+    q->dS = reinterpret_cast<double *>(P0(o_dS));
+    q->sigt = reinterpret_cast<double *>(P0(o_sigt));
+    q->S = reinterpret_cast<double2 *>(P0(o_S));
+    q->s2 = reinterpret_cast<double *>(P0(o_s2));
+    q->s3 = reinterpret_cast<double *>(P0(o_s3));
+    q->s4 = reinterpret_cast<double *>(P0(o_s4));
+    q->mom = reinterpret_cast<double *>(P0(o_mom));
+    q->cmax = reinterpret_cast<double *>(P0(o_cmax));
+    q->msuf = reinterpret_cast<double *>(P0(o_msuf));
+    q->csuf = reinterpret_cast<double *>(P0(o_csuf));
+    q->tailm = reinterpret_cast<double *>(P0(o_tailm));
+    q->red.partial = reinterpret_cast<double *>(P0(o_redp));
+    q->red.ticket = reinterpret_cast<unsigned *>(P0(o_redt));
+    q->redm.partial = reinterpret_cast<double *>(P0(o_redmp));
+    q->redm.ticket = reinterpret_cast<unsigned *>(P0(o_redmt));
+    q->roots.partial = reinterpret_cast<double *>(P0(o_rootp));
+    // the density root's result in the scalars' spare slots 10, 11
+    q->mu0r.result = q->pp + 10;
+    ctx->groups[key] = q;
+    *out = q;
+    return TPSC_OK;
+}
+
+// the input block of one point (params row nk0, Nw0, n, T, t', t'', t3, U):
+// eps_k on the octant, the hopping table, the tail power sums, the scalars
+void group_point_inputs(const Group *q, const double *p, char *dst) {
+    const GridDev &d = q->d;
+    const double n = p[2], T = p[3], tp = p[4], tpp = p[5], t3 = p[6], U = p[7];
+    size_t off = 0;
+    auto next = [&](size_t bytes) {
+        double *r = reinterpret_cast<double *>(dst + off);
+        off += (bytes + 255) & ~(size_t)255;
+        return r;
+    };
+    double *ek = next((size_t)d.n8 * 8), *er = next((size_t)d.n8 * 8), *tq = next(kTailQ * 8),
+           *tpw = next(kTailP * 8), *pp = next(kPP * 8);
+    octant_eps(d.nbk, tp, tpp, t3, ek, nullptr);
+    std::fill(er, er + d.n8, 0.0);
+    er[1] = -1;
+    er[2] = -tp;
+    er[3] = -tpp;
+    er[4] = -t3;
+    tail_power_sums(q->nw0, T, tq, tpw);
+    std::fill(pp, pp + kPP, 0.0);
+    pp[kPpT] = T;
+    pp[kPpU] = U;
+    pp[kPpN] = n;
+    pp[kPpNsr] = n > 1.0 ? 2.0 - n : n;  // src/chi.cpp:18-19
+    pp[kPpNormFact] = T / ((double)q->nk0 * q->nk0);
+    int jc;
+    double wc;
+    mu_series_cut(q->nw0, T, &jc, &wc);
+    pp[kPpJc] = jc;
+    pp[kPpWc] = wc;
+    // the reference's shortcut for mu0 (green0::find_mu): half filling without t', t''
+    pp[kPpMu0Fixed] = (n == 1.0 && tp == 0 && tpp == 0) ? 1.0 : 0.0;
+}
+
+// the Newton-form mixed solve of the group's first P points, queued on
+// ctx->st: inputs up, one launch per stage over the P points, results down
+int group_queue(tpsc_ctx *ctx, Group *q, int P, cudaStream_t st, int root_cap) {
+    const GridDev &d = q->d;
+    Bp b;
+    b.P = P;
+    b.arena = q->arena;
+    b.pp = q->pp;
+    CK(cudaMemcpy2DAsync(q->base, (size_t)q->arena, q->h_in, q->in_bytes, q->in_bytes, P, cudaMemcpyHostToDevice,
+                         st));
+    CK(launch_mu0_newton(d, 0.0, 0.0, q->mu0r, st, b));
+    CK(launch_gslice32(d, q->Grt32, 0.0, 0.0, st, b));
+    CK(launch_chi0_boundary(d, (const float *)q->Grt32, 0.0, 0.0, q->dG0p, q->dchirt0, q->dchiqt0, st, b));
+    CK(launch_chi0_slice32(d, q->Grt32, q->chirt, q->chiq, st, b));
+    CK(launch_chi0_tau(d, q->chiq, q->dchiqt0, q->cinf, q->cinf2, 0.0, st, b));
+    CK(launch_chi0max(d, q->chiq, q->red, st, b));
+    CK(launch_chi0_moments(d, q->chiq, q->mom, q->cmax, st, b));
+    CK(launch_tail_moments(d, q->cinf, q->cinf2, 0.0, q->redm, st, b));
+    CK(launch_moment_suffix(d, q->mom, q->cmax, q->redm.result, q->msuf, q->csuf, q->tailm, st, b));
+    RootScratch rs = q->roots;
+    rs.max_blocks = root_cap;
+    rs.reset_sr = rs.reset_mu = true;
+    rs.out = q->dres;
+    CK(launch_sumrule_roots(d, q->chiq, q->cinf, q->cinf2, q->msuf, q->csuf, q->tailm, 0.0, 0.0, 0.0, 0.0, 0.0, rs,
+                            st, q->red.result, 2 * EPS, b));
+    CK(launch_vertex_q32(d, q->chiq, q->V, 0.0, q->dres, 0.0, st, b));
+    CK(launch_vertex_tau(d, q->V, q->chirt, 0.0, q->dres, st, b));
+    CK(launch_sigma_boundary(d, (const float *)q->Grt32, q->V, q->dchirt0, q->dG0p, 0.0, 0.0, q->dres, q->dS, st,
+                             b));
+    CK(launch_sigma_slice32(d, q->Grt32, q->V, q->sigt, st, b));
+    CK(launch_sigma_tau(d, q->sigt, q->dS, q->S, q->s2, q->s3, q->s4, q->sinf, 0.0, st, b));
+    CK(launch_sigma_moments(d, q->S, q->s2, q->s3, q->s4, q->sinf, 0.0, 0.0, 0, q->redm, st, b));
+    rs.out = q->mu_out;
+    CK(launch_mu_roots(d, q->S, q->s2, q->s3, q->s4, q->sinf, q->redm.result, 0.0, 0.0, 0, 0.0, rs, st, b));
+    // the results block and the scalars (mu0 and its search) of every point
+    CK(cudaMemcpy2DAsync(q->h_res, kGroupRes * sizeof(double), q->base + q->res_off, (size_t)q->arena,
+                         kGroupRes * sizeof(double), P, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpy2DAsync(q->h_in + (q->in_bytes - ((kPP * 8 + 255) & ~(size_t)255)), q->in_bytes, q->pp,
+                         (size_t)q->arena, kPP * sizeof(double), P, cudaMemcpyDeviceToHost, st));
+    return TPSC_OK;
+}
+
+// the group's solve as one graph launch: captured on the first call after a
+// direct one (the kernels' one-time attribute calls happen outside a
+// capture), replayed while P stays the same
+int group_run(tpsc_ctx *ctx, Group *q, int P, cudaStream_t st, int root_cap) {
+    if (q->gexec && q->gexec_P == P) {
+        CK(cudaGraphLaunch(q->gexec, st));
+        return TPSC_OK;
+    }
+    if (q->gexec_P != -P) {
+        // first call with this P: direct launches
+        int rc = group_queue(ctx, q, P, st, root_cap);
+        if (rc) return rc;
+        q->gexec_P = -P;
+        return TPSC_OK;
+    }
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int rc = group_queue(ctx, q, P, st, root_cap);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "group capture");
+    if (q->gexec) cudaGraphExecDestroy(q->gexec);
+    q->gexec = nullptr;
+    e = cudaGraphInstantiate(&q->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "group graph instantiation");
+    q->gexec_P = P;
+    CK(cudaGraphLaunch(q->gexec, st));
+    return TPSC_OK;
+}
+
+// the scalars of point p of the group (the Newton-form solve's checks and
+// results, as newton_finish and switch_grid leave them) -> out; its status
+int group_point_result(const Group *q, int p, const double *prm, double *out, std::string &msg) {
+    const double *r = q->h_res + (size_t)p * kGroupRes;
+    const double *pp = reinterpret_cast<const double *>(q->h_in + (size_t)p * q->in_bytes +
+                                                        (q->in_bytes - ((kPP * 8 + 255) & ~(size_t)255)));
+    const double n = prm[2], U = prm[7], nsr = n > 1.0 ? 2.0 - n : n;
+    for (int k = 0; k < TPSC_S_COUNT; ++k) out[k] = 0.0;
+    out[TPSC_S_MU0] = pp[kPpMu0];
+    if (!std::isfinite(pp[kPpMu0]) || pp[11] >= 200) {
+        msg = "mu0 not found";
+        return TPSC_ERR_NO_ROOT;
+    }
+    out[TPSC_S_CHI0MAX] = r[0];
+    out[TPSC_S_QMAX0] = r[1];
+    out[TPSC_S_QMAX1] = r[2];
+    if (!std::isfinite(r[0]) || r[0] <= 0.0) {
+        msg = "chi0(q, 0) has no positive maximum";
+        return TPSC_ERR_NONFINITE;
+    }
+    unsigned bar[8];
+    std::memcpy(bar, r + 16, sizeof(bar));
+    if (bar[2]) {
+        msg = "device root search: grid barrier timed out";
+        return TPSC_ERR_CUDA;
+    }
+    if (r[12] != 1.0 || r[13] != 1.0) {
+        msg = r[12] != 1.0 ? "Usp not found" : "Uch not found";
+        return TPSC_ERR_NO_ROOT;
+    }
+    out[TPSC_S_USP] = r[8];
+    out[TPSC_S_UCH] = r[9];
+    out[TPSC_S_EVALS_SP] = r[10];
+    out[TPSC_S_EVALS_CH] = r[11];
+    double D = r[8] / U * nsr * nsr / 4.0;  // src/chi.cpp:370-371
+    if (n > 1.0) D += 1.0 - nsr;
+    out[TPSC_S_DBLOCC] = D;
+    if (bar[6]) {
+        msg = "device mu search: grid barrier timed out";
+        return TPSC_ERR_CUDA;
+    }
+    out[TPSC_S_SIGMA_INF] = r[28];
+    out[TPSC_S_TR_SG] = r[32];
+    out[TPSC_S_TR_SG_ASYMP] = r[32] + r[33];
+    if (r[22] != 1.0) {
+        msg = "mu not found";
+        return TPSC_ERR_NO_ROOT;
+    }
+    out[TPSC_S_MU] = r[20];
+    out[TPSC_S_EVALS_MU] = r[21];
+    out[TPSC_S_TR_SG2] = r[23];
+    out[TPSC_S_DBLOCC_SG2] = (r[23] + U * n * n / 4.0) / U;
+    for (int k = 0; k < TPSC_S_COUNT; ++k)
+        if (!std::isfinite(out[k])) {
+            msg = "non-finite scalar result";
+            return TPSC_ERR_NONFINITE;
+        }
+    return TPSC_OK;
+}
+}  // namespace
+
+int tpsc_solve_points(tpsc_ctx *ctx, int npts, const double *params, double *results, int *status, double *ms) {
+    if (!ctx) return fail(nullptr, TPSC_ERR_ARG, "null context");
+    if (npts < 0 || (npts > 0 && (!params || !results || !status))) return fail(ctx, TPSC_ERR_ARG, "bad arguments");
+    cudaSetDevice(ctx->device);
+    // valid points by shape, in input order
+    std::map<std::pair<int, int>, std::vector<int>> shapes;
+    for (int i = 0; i < npts; ++i) {
+        const double *p = params + (size_t)i * 8;
+        double *out = results + (size_t)i * TPSC_S_COUNT;
+        for (int k = 0; k < TPSC_S_COUNT; ++k) out[k] = NAN;
+        const bool ok = p[0] == std::floor(p[0]) && p[1] == std::floor(p[1]) && p[0] >= 8 && p[0] <= 256 &&
+                        p[1] >= 16 && p[1] <= 4096 && supported_grid((int)p[0], (int)p[1]) && p[2] > 0.0 &&
+                        p[2] < 2.0 && p[3] > 0.0 && p[7] > 0.0 && std::isfinite(p[7]) && std::isfinite(p[4]) &&
+                        std::isfinite(p[5]) && std::isfinite(p[6]);
+        status[i] = ok ? TPSC_OK : TPSC_ERR_ARG;
+        if (ok) shapes[std::make_pair((int)p[0], (int)p[1])].push_back(i);
+    }
+    // the groups' arenas first (allocation waits for the device)
+    for (auto &kv : shapes) {
+        Group *q = nullptr;
+        const int P = (int)std::min<size_t>(kGroupMax, kv.second.size());
+        int rc = group_alloc(ctx, kv.first.first, kv.first.second, P, &q);
+        if (rc) return rc;
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    const auto t0 = std::chrono::steady_clock::now();
+    std::string first_msg;
+    // every group queued without a wait (the host builds the next group's
+    // tables while the device runs the previous ones), largest first, on two
+    // streams by least queued work (a group's root searches then take half
+    // of the resident grid, so that both streams' fit on the GPU together); a
+    // shape with more than kGroupMax points waits for its previous chunk
+    // before its staging buffers are refilled
+    struct Chunk {
+        Group *q;
+        size_t c0;
+        int P;
+        const std::vector<int> *idx;
+    };
+    std::vector<Chunk> done;
+    std::vector<std::pair<double, const std::pair<const std::pair<int, int>, std::vector<int>> *>> order;
+    for (auto &kv : shapes)
+        order.push_back({-(double)kv.first.first * kv.first.first * kv.first.second * kv.second.size(), &kv});
+    std::sort(order.begin(), order.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+    const int ns = ctx->group_streams;
+    for (int k = 0; k + 2 < ns; ++k)
+        if (!ctx->gst[k]) CK(cudaStreamCreateWithFlags(&ctx->gst[k], cudaStreamNonBlocking));
+    cudaStream_t streams[4] = {ctx->st, ctx->st2, ctx->gst[0], ctx->gst[1]};
+    double load[4] = {0.0, 0.0, 0.0, 0.0};
+    int dev_sms = 0;
+    CK(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    const int root_cap = std::max(8, 2 * dev_sms / ns);  // two blocks per SM, shared out
+    auto collect = [&](const Chunk &ch) {
+        for (int k = 0; k < ch.P; ++k) {
+            const int i = (*ch.idx)[ch.c0 + k];
+            std::string msg;
+            status[i] = group_point_result(ch.q, k, params + (size_t)i * 8, results + (size_t)i * TPSC_S_COUNT, msg);
+            if (status[i] && first_msg.empty()) first_msg = "point " + std::to_string(i) + ": " + msg;
+        }
+    };
+    for (const auto &o : order) {
+        const std::vector<int> &idx = o.second->second;
+        Group *q = ctx->groups[o.second->first];
+        int s = 0;
+        for (int k = 1; k < ns; ++k)
+            if (load[k] < load[s]) s = k;
+        load[s] += -o.first;
+        for (size_t c0 = 0; c0 < idx.size(); c0 += kGroupMax) {
+            const int P = (int)std::min<size_t>(kGroupMax, idx.size() - c0);
+            if (c0 > 0) {
+                CK(cudaStreamSynchronize(streams[s]));
+                collect(done.back());
+                done.pop_back();
+            }
+            for (int k = 0; k < P; ++k)
+                group_point_inputs(q, params + (size_t)idx[c0 + k] * 8, q->h_in + (size_t)k * q->in_bytes);
+            int rc = group_run(ctx, q, P, streams[s], root_cap);
+            if (rc) return rc;
+            done.push_back({q, c0, P, &idx});
+        }
+    }
+    for (int k = 0; k < ns; ++k) CK(cudaStreamSynchronize(streams[k]));
+    for (const Chunk &ch : done) collect(ch);
+    const auto t1 = std::chrono::steady_clock::now();
+    if (ms) *ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    ctx->err = first_msg;
+    return TPSC_OK;
+}
+
+int tpsc_set_group_streams(tpsc_ctx *ctx, int n) {
+    if (!ctx) return fail(nullptr, TPSC_ERR_ARG, "null context");
+    if (n < 1 || n > 4) return fail(ctx, TPSC_ERR_ARG, "need 1 <= n <= 4");
+    if (n != ctx->group_streams)
+        for (auto &kv : ctx->groups) kv.second->gexec_P = 0;  // the root grids' cap changes: capture again
+    ctx->group_streams = n;
+    return TPSC_OK;
 }
 
 int tpsc_get_scalars(tpsc_ctx *ctx, double *out, int n) {

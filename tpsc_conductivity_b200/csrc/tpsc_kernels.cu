@@ -93,9 +93,13 @@ __global__ void k_density(const double *__restrict__ ek, int n8, int nbk,
 //   x <= 0:               -exp((beta - tau) x) / (exp(x/T) + 1) / L^2
 // gk[o] = (x, prefactor), so one exp per element remains per slice.
 __global__ void k_gk_table(const double *__restrict__ ek, int n8, double mu0, double T, double nk02,
-                           double2 *__restrict__ gk) {
+                           double2 *__restrict__ gk, Bp b) {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n8) return;
+    ek = at(ek, b.arena);
+    gk = at(gk, b.arena);
+    mu0 = bpar(b, kPpMu0, mu0);
+    T = bpar(b, kPpT, T);
     const double x = ek[o] - mu0;
     const double pre = x > 0 ? -1.0 / (exp(-x / T) + 1.0) / nk02 : -1.0 / (exp(x / T) + 1.0) / nk02;
     gk[o] = make_double2(x, pre);
@@ -176,9 +180,17 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     k_chi0_boundary(const double *__restrict__ ek, const double *__restrict__ er,
                     const double2 *__restrict__ tw, const GT *__restrict__ Grt, int n8, double mu0, double T,
                     double nk02, double *__restrict__ dG0p, double *__restrict__ dtau_chirt0,
-                    double *__restrict__ dtau_chiqt0) {
+                    double *__restrict__ dtau_chiqt0, Bp b) {
     extern __shared__ __align__(16) double S[];
     const auto *tws = slice_twiddles<NBK>(S, tw);
+    ek = at(ek, b.arena);
+    er = at(er, b.arena);
+    Grt = at(Grt, b.arena);
+    dG0p = at(dG0p, b.arena);
+    dtau_chirt0 = at(dtau_chirt0, b.arena);
+    dtau_chiqt0 = at(dtau_chiqt0, b.arena);
+    mu0 = bpar(b, kPpMu0, mu0);
+    T = bpar(b, kPpT, T);
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
         oct_lm(o, l, m);
@@ -260,9 +272,18 @@ __global__ void __launch_bounds__(kSliceThreads, 1)
     k_sigma_boundary(const double *__restrict__ er, const double2 *__restrict__ tw,
                      const GT *__restrict__ Grt, const double *__restrict__ V, const double *__restrict__ dtau_chirt0,
                      const double *__restrict__ dG0p, int n8, int nw0, int n8p, double mu0, double U,
-                     const double *__restrict__ Usc, double *__restrict__ dS) {
+                     const double *__restrict__ Usc, double *__restrict__ dS, Bp b) {
     extern __shared__ __align__(16) double S[];
     const auto *tws = slice_twiddles<NBK>(S, tw);
+    er = at(er, b.arena);
+    Grt = at(Grt, b.arena);
+    V = at(V, b.arena);
+    dtau_chirt0 = at(dtau_chirt0, b.arena);
+    dG0p = at(dG0p, b.arena);
+    Usc = at(Usc, b.arena);
+    dS = at(dS, b.arena);
+    mu0 = bpar(b, kPpMu0, mu0);
+    U = bpar(b, kPpU, U);
     const double fact = vertex_fact(U, Usc);
     const int nb = nw0 / 2 + 1;
     {
@@ -565,10 +586,18 @@ __global__ void __launch_bounds__(256, 2)
     k_sigma_tau2(const double *__restrict__ sigt, const double *__restrict__ dS, double2 *__restrict__ Sout,
                  double *__restrict__ s2, double *__restrict__ s3, double *__restrict__ s4, double *__restrict__ sinf,
                  const double *__restrict__ spl, const double2 *__restrict__ tw, const double2 *__restrict__ ht,
-                 double T, int n8, int n8p) {
+                 double T, int n8, int n8p, Bp b) {
     constexpr int NJ = N + 1;
     constexpr int NO = N / 2;
     static_assert(2 * NJ * sizeof(double) <= Tau2Smem<N>::buf, "pair must fit the FFT buffer");
+    sigt = at(sigt, b.arena);
+    dS = at(dS, b.arena);
+    Sout = at(Sout, b.arena);
+    s2 = at(s2, b.arena);
+    s3 = at(s3, b.arena);
+    s4 = at(s4, b.arena);
+    sinf = at(sinf, b.arena);
+    T = bpar(b, kPpT, T);
     extern __shared__ __align__(16) double A[];
     double2 *X = reinterpret_cast<double2 *>(A);
     TwoLevelTw *tw2 = reinterpret_cast<TwoLevelTw *>(reinterpret_cast<char *>(A) + Tau2Smem<N>::buf);
@@ -635,8 +664,13 @@ template <int N>
 __global__ void __launch_bounds__(256, 2)
     k_chi0_tau2(double *__restrict__ chiq, const double *__restrict__ dtau_chiqt0, double *__restrict__ chi0_inf,
                 double *__restrict__ chi0_inf2, const double *__restrict__ spl, const double2 *__restrict__ tw,
-                double T, int n8) {
+                double T, int n8, Bp b) {
     constexpr int NJ = N / 2 + 1;
+    chiq = at(chiq, b.arena);
+    dtau_chiqt0 = at(dtau_chiqt0, b.arena);
+    chi0_inf = at(chi0_inf, b.arena);
+    chi0_inf2 = at(chi0_inf2, b.arena);
+    T = bpar(b, kPpT, T);
     static_assert(2 * NJ * sizeof(double) <= Tau2Smem<N>::buf, "pair must fit the FFT buffer");
     extern __shared__ __align__(16) double A[];
     double2 *X = reinterpret_cast<double2 *>(A);
@@ -709,8 +743,12 @@ __global__ void __launch_bounds__(256, 2)
 template <int N>
 __global__ void __launch_bounds__(256, 2)
     k_vertex_tau2(double *__restrict__ Vr, const double *__restrict__ chirt, const double2 *__restrict__ tw,
-                  double U, const double *__restrict__ Usc, int n8) {
+                  double U, const double *__restrict__ Usc, int n8, Bp b) {
     constexpr int NJ = N / 2 + 1;
+    Vr = at(Vr, b.arena);
+    chirt = at(chirt, b.arena);
+    Usc = at(Usc, b.arena);
+    U = bpar(b, kPpU, U);
     const double fact = vertex_fact(U, Usc);
     static_assert(2 * NJ * sizeof(double) <= Tau2Smem<N>::buf, "pair must fit the FFT buffer");
     extern __shared__ __align__(16) double A[];
@@ -982,8 +1020,11 @@ __global__ void __launch_bounds__(kRedThreads)
 // up to a relative (kTailSeriesMax)^kMomP.
 __global__ void __launch_bounds__(256)
     k_chi0_moments(const double4 *__restrict__ chiq, const double *__restrict__ w16, int nb, int nblk,
-                   double *__restrict__ mom, double *__restrict__ cmax) {
+                   double *__restrict__ mom, double *__restrict__ cmax, Bp b) {
     const int j = blockIdx.x;
+    chiq = at(chiq, b.arena);
+    mom = at(mom, b.arena);
+    cmax = at(cmax, b.arena);
     const double f = j == 0 ? 0.5 : 1.0;
     double acc[kMomP + 1];
 #pragma unroll
@@ -1038,8 +1079,13 @@ __global__ void __launch_bounds__(256)
 // value kMomP = max over columns of |chi| at the first tail frequency.
 __global__ void __launch_bounds__(256)
     k_tail_moments(const double *__restrict__ cinf, const double *__restrict__ cinf2, const double *__restrict__ w16,
-                   const double *__restrict__ tailq, int n8, int nb, double T, double *partial) {
+                   const double *__restrict__ tailq, int n8, int nb, double T, double *partial, Bp b) {
     constexpr int NV = kMomP + 1;
+    cinf = at(cinf, b.arena);
+    cinf2 = at(cinf2, b.arena);
+    tailq = at(tailq, b.arena);
+    partial = at(partial, b.arena);
+    T = bpar(b, kPpT, T);
     double acc[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k) acc[k] = 0.0;
@@ -1303,7 +1349,9 @@ __device__ __forceinline__ MaxPt max_shfl(MaxPt a, int off) {
     return better(b, a) ? b : a;
 }
 __global__ void __launch_bounds__(1024)
-    k_chi0max(const double *__restrict__ chiq, int n8, int nb, double *result) {
+    k_chi0max(const double *__restrict__ chiq, int n8, int nb, double *result, Bp b) {
+    chiq = at(chiq, b.arena);
+    result = at(result, b.arena);
     // values <= 0 never win: the reference's scan starts from chi0max = 0
     MaxPt best{0.0, -1, -1};
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
@@ -1336,10 +1384,25 @@ __global__ void __launch_bounds__(1024)
 // The Newton form's replacement of the host root search.
 __global__ void __launch_bounds__(1024)
     k_mu0_newton(const double *__restrict__ ek, int n8, int nbk, double n, double T,
-                 double nk2, double *result) {
+                 double nk2, double *result, Bp b) {
     __shared__ double red[32][2];
     __shared__ double s_mu;
     __shared__ int s_done, s_it;
+    ek = at(ek, b.arena);
+    result = at(result, b.arena);
+    n = bpar(b, kPpN, n);
+    T = bpar(b, kPpT, T);
+    // a batched launch writes the point's mu0 into its scalars (half filling
+    // without t', t'': 0, no search)
+    double *mu0_out = b.pp ? at(const_cast<double *>(b.pp), b.arena) + kPpMu0 : nullptr;
+    if (mu0_out && at(b.pp, b.arena)[kPpMu0Fixed] != 0.0) {
+        if (threadIdx.x == 0) {
+            *mu0_out = 0.0;
+            result[0] = 0.0;
+            result[1] = 0.0;
+        }
+        return;
+    }
     double lo = -8.0, hi = 8.0, mu = 0.0;
     if (threadIdx.x == 0) {
         s_mu = 0.0;
@@ -1390,6 +1453,7 @@ __global__ void __launch_bounds__(1024)
     if (threadIdx.x == 0) {
         result[0] = s_mu;
         result[1] = s_it;
+        if (mu0_out) *mu0_out = s_mu;
     }
 }
 
@@ -1596,7 +1660,7 @@ struct RunGslice {
         cudaError_t e = set_smem(k_gslice<NBK>, sm);
         if (e != cudaSuccess) return e;
         const double nk02 = (double)g->nk0 * g->nk0;
-        k_gk_table<<<(g->n8 + 255) / 256, 256, 0, st>>>(g->ek, g->n8, mu0, T, nk02, g->gk);
+        k_gk_table<<<(g->n8 + 255) / 256, 256, 0, st>>>(g->ek, g->n8, mu0, T, nk02, g->gk, Bp{});
         if ((e = launched()) != cudaSuccess) return e;
         k_gslice<NBK><<<g->nw0 + 1, kSliceThreads, sm, st>>>(g->gk, g->tw_k, g->n8, g->nw0, T, Grt);
         return launched();
@@ -1606,13 +1670,13 @@ template <int NBK>
 struct RunChi0Boundary {
     template <class GT>
     static cudaError_t run(const GridDev *g, const GT *Grt, double mu0, double T, double *dG0p, double *dchirt0,
-                           double *dchiqt0, cudaStream_t st) {
+                           double *dchiqt0, const Bp *b, cudaStream_t st) {
         const size_t sm = SliceSmem<NBK>::bytes;
         cudaError_t e = set_smem(k_chi0_boundary<NBK, GT>, sm);
         if (e != cudaSuccess) return e;
         const double nk02 = (double)g->nk0 * g->nk0;
-        k_chi0_boundary<NBK, GT><<<1, kSliceThreads, sm, st>>>(g->ek, g->er, g->tw_k, Grt, g->n8, mu0, T,
-                                                                nk02, dG0p, dchirt0, dchiqt0);
+        k_chi0_boundary<NBK, GT><<<dim3(1, 1, b->P), kSliceThreads, sm, st>>>(g->ek, g->er, g->tw_k, Grt, g->n8, mu0,
+                                                                               T, nk02, dG0p, dchirt0, dchiqt0, *b);
         return launched();
     }
 };
@@ -1642,13 +1706,14 @@ template <int NBK>
 struct RunSigmaBoundary {
     template <class GT>
     static cudaError_t run(const GridDev *g, const GT *Grt, const double *V, const double *dchirt0,
-                           const double *dG0p, double mu0, double U, const double *Usc, double *dS,
+                           const double *dG0p, double mu0, double U, const double *Usc, double *dS, const Bp *b,
                            cudaStream_t st) {
         const size_t sm = SliceSmem<NBK>::bytes;
         cudaError_t e = set_smem(k_sigma_boundary<NBK, GT>, sm);
         if (e != cudaSuccess) return e;
-        k_sigma_boundary<NBK, GT><<<2, kSliceThreads, sm, st>>>(g->er, g->tw_k, Grt, V, dchirt0, dG0p, g->n8,
-                                                                 g->nw0, g->n8p, mu0, U, Usc, dS);
+        k_sigma_boundary<NBK, GT><<<dim3(2, 1, b->P), kSliceThreads, sm, st>>>(g->er, g->tw_k, Grt, V, dchirt0, dG0p,
+                                                                                g->n8, g->nw0, g->n8p, mu0, U, Usc, dS,
+                                                                                *b);
         return launched();
     }
 };
@@ -1666,14 +1731,16 @@ struct RunSigmaSlice {
 
 template <int N>
 struct RunChi0Tau {
+    // (a batched launch, b->pp set, always takes the pair-per-CTA kernel)
     static cudaError_t run(const GridDev *g, double *chiq, const double *dchiqt0, double *cinf, double *cinf2,
-                           double T, cudaStream_t st) {
+                           double T, const Bp *b, cudaStream_t st) {
         cudaError_t e;
         if constexpr (N / 16 <= 256) {
-            if (tau_tile(kTauChi0, N) == 0) {
+            if (tau_tile(kTauChi0, N) == 0 || b->pp) {
                 const size_t sm = Tau2Smem<N>::bytes;
                 if ((e = set_smem(k_chi0_tau2<N>, sm)) != cudaSuccess) return e;
-                k_chi0_tau2<N><<<g->n8p / 2, 256, sm, st>>>(chiq, dchiqt0, cinf, cinf2, g->spl_half, g->tw_w, T, g->n8);
+                k_chi0_tau2<N><<<dim3(g->n8p / 2, 1, b->P), 256, sm, st>>>(chiq, dchiqt0, cinf, cinf2, g->spl_half,
+                                                                          g->tw_w, T, g->n8, *b);
                 return launched();
             }
         }
@@ -1688,13 +1755,13 @@ struct RunChi0Tau {
 template <int N>
 struct RunVertexTau {
     static cudaError_t run(const GridDev *g, double *Vr, const double *chirt, double U, const double *Usc,
-                           cudaStream_t st) {
+                           const Bp *b, cudaStream_t st) {
         cudaError_t e;
         if constexpr (N / 16 <= 256) {
-            if (tau_tile(kTauVertex, N) == 0) {
+            if (tau_tile(kTauVertex, N) == 0 || b->pp) {
                 const size_t sm = Tau2Smem<N>::bytes;
                 if ((e = set_smem(k_vertex_tau2<N>, sm)) != cudaSuccess) return e;
-                k_vertex_tau2<N><<<g->n8p / 2, 256, sm, st>>>(Vr, chirt, g->tw_w, U, Usc, g->n8);
+                k_vertex_tau2<N><<<dim3(g->n8p / 2, 1, b->P), 256, sm, st>>>(Vr, chirt, g->tw_w, U, Usc, g->n8, *b);
                 return launched();
             }
         }
@@ -1708,15 +1775,15 @@ struct RunVertexTau {
 template <int N>
 struct RunSigmaTau {
     static cudaError_t run(const GridDev *g, const double *sigt, const double *dS, double2 *S, double *s2, double *s3,
-                           double *s4, double *sinf, double T, cudaStream_t st) {
+                           double *s4, double *sinf, double T, const Bp *b, cudaStream_t st) {
         cudaError_t e;
         if constexpr (N / 16 <= 256) {
-            if (tau_tile(kTauSigma, N) == 0) {
+            if (tau_tile(kTauSigma, N) == 0 || b->pp) {
                 // one pair per CTA, two CTAs per SM
                 const size_t sm = Tau2Smem<N>::bytes;
                 if ((e = set_smem(k_sigma_tau2<N>, sm)) != cudaSuccess) return e;
-                k_sigma_tau2<N><<<g->n8p / 2, 256, sm, st>>>(sigt, dS, S, s2, s3, s4, sinf, g->spl_full, g->tw_w,
-                                                             g->ht_w, T, g->n8, g->n8p);
+                k_sigma_tau2<N><<<dim3(g->n8p / 2, 1, b->P), 256, sm, st>>>(sigt, dS, S, s2, s3, s4, sinf, g->spl_full,
+                                                                           g->tw_w, g->ht_w, T, g->n8, g->n8p, *b);
                 return launched();
             }
         }
@@ -1772,15 +1839,16 @@ cudaError_t launch_gslice(const GridDev &g, double *Grt, double mu0, double T, c
 
 cudaError_t launch_chi0_boundary(const GridDev &g, const double *Grt, double mu0, double T, double *dG0p,
                                  double *dtau_chirt0, double *dtau_chiqt0, cudaStream_t st) {
-    return dispatch_nbk<RunChi0Boundary>(g.nbk, &g, Grt, mu0, T, dG0p, dtau_chirt0, dtau_chiqt0, st);
+    const Bp b;
+    return dispatch_nbk<RunChi0Boundary>(g.nbk, &g, Grt, mu0, T, dG0p, dtau_chirt0, dtau_chiqt0, &b, st);
 }
 cudaError_t launch_chi0_boundary(const GridDev &g, const float *Grt, double mu0, double T, double *dG0p,
-                                 double *dtau_chirt0, double *dtau_chiqt0, cudaStream_t st) {
-    return dispatch_nbk<RunChi0Boundary>(g.nbk, &g, Grt, mu0, T, dG0p, dtau_chirt0, dtau_chiqt0, st);
+                                 double *dtau_chirt0, double *dtau_chiqt0, cudaStream_t st, const Bp &b) {
+    return dispatch_nbk<RunChi0Boundary>(g.nbk, &g, Grt, mu0, T, dG0p, dtau_chirt0, dtau_chiqt0, &b, st);
 }
 
-cudaError_t launch_gk_table(const GridDev &g, double mu0, double T, cudaStream_t st) {
-    k_gk_table<<<(g.n8 + 255) / 256, 256, 0, st>>>(g.ek, g.n8, mu0, T, (double)g.nk0 * g.nk0, g.gk);
+cudaError_t launch_gk_table(const GridDev &g, double mu0, double T, cudaStream_t st, const Bp &b) {
+    k_gk_table<<<dim3((g.n8 + 255) / 256, 1, b.P), 256, 0, st>>>(g.ek, g.n8, mu0, T, (double)g.nk0 * g.nk0, g.gk, b);
     return launched();
 }
 
@@ -1789,8 +1857,8 @@ cudaError_t launch_chi0_slice(const GridDev &g, const double *Grt, double *chirt
 }
 
 cudaError_t launch_chi0_tau(const GridDev &g, double *chiq, const double *dtau_chiqt0, double *chi0_inf,
-                            double *chi0_inf2, double T, cudaStream_t st) {
-    return dispatch_nw<RunChi0Tau>(g.nw0, &g, chiq, dtau_chiqt0, chi0_inf, chi0_inf2, T, st);
+                            double *chi0_inf2, double T, cudaStream_t st, const Bp &b) {
+    return dispatch_nw<RunChi0Tau>(g.nw0, &g, chiq, dtau_chiqt0, chi0_inf, chi0_inf2, T, &b, st);
 }
 
 cudaError_t launch_sumrule(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
@@ -1821,16 +1889,17 @@ cudaError_t launch_sumrule_tan(const GridDev &g, const double *chiq, const doubl
 }
 
 cudaError_t launch_tail_moments(const GridDev &g, const double *chi0_inf, const double *chi0_inf2, double T,
-                                Reduce r, cudaStream_t st) {
+                                Reduce r, cudaStream_t st, const Bp &b) {
     constexpr int NV = kMomP + 1;
     const int nblk = grid_for(g.n8, 256);
-    k_tail_moments<<<nblk, 256, 0, st>>>(chi0_inf, chi0_inf2, g.w16, g.tailq, g.n8, g.nb, T, r.partial);
+    k_tail_moments<<<dim3(nblk, 1, b.P), 256, 0, st>>>(chi0_inf, chi0_inf2, g.w16, g.tailq, g.n8, g.nb, T, r.partial,
+                                                        b);
     cudaError_t e = launched();
     if (e != cudaSuccess) return e;
-    e = finish<NV>(r, nblk, 0.0, st);
+    e = finish<NV>(r, nblk, 0.0, st, b);
     if (e != cudaSuccess) return e;
     // the per-block maxima -> result[NV]
-    k_max_finish<<<1, 32, 0, st>>>(r.partial + (2 * kMomP + 1) * kMaxBlocks, nblk, r.result + NV);
+    k_max_finish<<<dim3(1, 1, b.P), 32, 0, st>>>(r.partial + (2 * kMomP + 1) * kMaxBlocks, nblk, r.result + NV, b);
     return launched();
 }
 
@@ -1858,7 +1927,14 @@ __device__ __forceinline__ DD dd_shfl_down(DD a, int off) {
 // deterministic.
 __global__ void __launch_bounds__(256)
     k_moment_suffix(const double *__restrict__ mom, const double *__restrict__ cmax, const double *__restrict__ tail,
-                    int nb, double *__restrict__ mom_suf, double *__restrict__ cmax_suf, double *__restrict__ tailm) {
+                    int nb, double *__restrict__ mom_suf, double *__restrict__ cmax_suf, double *__restrict__ tailm,
+                    Bp b) {
+    mom = at(mom, b.arena);
+    cmax = at(cmax, b.arena);
+    tail = at(tail, b.arena);
+    mom_suf = at(mom_suf, b.arena);
+    cmax_suf = at(cmax_suf, b.arena);
+    tailm = at(tailm, b.arena);
     extern __shared__ double col[];
     __shared__ DD wtot[32];
     const int k = blockIdx.x;
@@ -1914,16 +1990,19 @@ __global__ void __launch_bounds__(256)
 }  // namespace
 
 cudaError_t launch_moment_suffix(const GridDev &g, const double *mom, const double *cmax, const double *tail_result,
-                                 double *mom_suf, double *cmax_suf, double *tailm, cudaStream_t st) {
+                                 double *mom_suf, double *cmax_suf, double *tailm, cudaStream_t st, const Bp &b) {
     const size_t sm = (size_t)g.nb * sizeof(double);
     cudaError_t e = set_smem(k_moment_suffix, sm);
     if (e != cudaSuccess) return e;
-    k_moment_suffix<<<kMomP + 1, 256, sm, st>>>(mom, cmax, tail_result, g.nb, mom_suf, cmax_suf, tailm);
+    k_moment_suffix<<<dim3(kMomP + 1, 1, b.P), 256, sm, st>>>(mom, cmax, tail_result, g.nb, mom_suf, cmax_suf, tailm,
+                                                               b);
     return launched();
 }
 
-cudaError_t launch_chi0_moments(const GridDev &g, const double *chiq, double *mom, double *cmax, cudaStream_t st) {
-    k_chi0_moments<<<g.nb, 256, 0, st>>>(reinterpret_cast<const double4 *>(chiq), g.w16, g.nb, g.n8p / 4, mom, cmax);
+cudaError_t launch_chi0_moments(const GridDev &g, const double *chiq, double *mom, double *cmax, cudaStream_t st,
+                                const Bp &b) {
+    k_chi0_moments<<<dim3(g.nb, 1, b.P), 256, 0, st>>>(reinterpret_cast<const double4 *>(chiq), g.w16, g.nb,
+                                                        g.n8p / 4, mom, cmax, b);
     return launched();
 }
 
@@ -1941,19 +2020,20 @@ cudaError_t launch_vertex_q(const GridDev &g, const double *chiq, double *Vr, do
 }
 
 cudaError_t launch_vertex_tau(const GridDev &g, double *Vr, const double *chirt, double U, const double *Usc,
-                              cudaStream_t st) {
-    return dispatch_nw<RunVertexTau>(g.nw0, &g, Vr, chirt, U, Usc, st);
+                              cudaStream_t st, const Bp &b) {
+    return dispatch_nw<RunVertexTau>(g.nw0, &g, Vr, chirt, U, Usc, &b, st);
 }
 
 cudaError_t launch_sigma_boundary(const GridDev &g, const double *Grt, const double *V, const double *dtau_chirt0,
                                   const double *dG0p, double mu0, double U, const double *Usc, double *dS,
                                   cudaStream_t st) {
-    return dispatch_nbk<RunSigmaBoundary>(g.nbk, &g, Grt, V, dtau_chirt0, dG0p, mu0, U, Usc, dS, st);
+    const Bp b;
+    return dispatch_nbk<RunSigmaBoundary>(g.nbk, &g, Grt, V, dtau_chirt0, dG0p, mu0, U, Usc, dS, &b, st);
 }
 cudaError_t launch_sigma_boundary(const GridDev &g, const float *Grt, const double *V, const double *dtau_chirt0,
                                   const double *dG0p, double mu0, double U, const double *Usc, double *dS,
-                                  cudaStream_t st) {
-    return dispatch_nbk<RunSigmaBoundary>(g.nbk, &g, Grt, V, dtau_chirt0, dG0p, mu0, U, Usc, dS, st);
+                                  cudaStream_t st, const Bp &b) {
+    return dispatch_nbk<RunSigmaBoundary>(g.nbk, &g, Grt, V, dtau_chirt0, dG0p, mu0, U, Usc, dS, &b, st);
 }
 
 cudaError_t launch_sigma_slice(const GridDev &g, const double *Grt, const double *V, double *sigt, cudaStream_t st) {
@@ -1961,8 +2041,8 @@ cudaError_t launch_sigma_slice(const GridDev &g, const double *Grt, const double
 }
 
 cudaError_t launch_sigma_tau(const GridDev &g, const double *sigt, const double *dS, double2 *S, double *s2,
-                             double *s3, double *s4, double *sinf, double T, cudaStream_t st) {
-    return dispatch_nw<RunSigmaTau>(g.nw0, &g, sigt, dS, S, s2, s3, s4, sinf, T, st);
+                             double *s3, double *s4, double *sinf, double T, cudaStream_t st, const Bp &b) {
+    return dispatch_nw<RunSigmaTau>(g.nw0, &g, sigt, dS, S, s2, s3, s4, sinf, T, &b, st);
 }
 
 cudaError_t launch_trace_diff_G(const GridDev &g, const double2 *S, const double *s2, const double *s3,
@@ -2013,13 +2093,14 @@ cudaError_t launch_gwn_local(const GridDev &g, const double2 *S, const double *s
     return launched();
 }
 
-cudaError_t launch_mu0_newton(const GridDev &g, double n, double T, Reduce r, cudaStream_t st) {
-    k_mu0_newton<<<1, 1024, 0, st>>>(g.ek, g.n8, g.nbk, n, T, 4.0 * (g.nbk - 1) * (g.nbk - 1), r.result);
+cudaError_t launch_mu0_newton(const GridDev &g, double n, double T, Reduce r, cudaStream_t st, const Bp &b) {
+    k_mu0_newton<<<dim3(1, 1, b.P), 1024, 0, st>>>(g.ek, g.n8, g.nbk, n, T, 4.0 * (g.nbk - 1) * (g.nbk - 1),
+                                                    r.result, b);
     return launched();
 }
 
-cudaError_t launch_chi0max(const GridDev &g, const double *chiq, Reduce r, cudaStream_t st) {
-    k_chi0max<<<1, 1024, 0, st>>>(chiq, g.n8, g.nb, r.result);
+cudaError_t launch_chi0max(const GridDev &g, const double *chiq, Reduce r, cudaStream_t st, const Bp &b) {
+    k_chi0max<<<dim3(1, 1, b.P), 1024, 0, st>>>(chiq, g.n8, g.nb, r.result, b);
     return launched();
 }
 

@@ -50,30 +50,58 @@ struct Reduce {
     unsigned *ticket = nullptr;  // arrival counter of the last-block finish (0 between launches)
 };
 
+// ---- one launch over the points of a shape group (the batched sweep) -------
+// Every point of a group keeps its arrays at the same offsets inside its own
+// arena of `arena` bytes, point p's at p * arena from point 0's; a batched
+// launch passes point 0's pointers, P = gridDim.z and the arena, and each
+// block works on point p = blockIdx.z (at() below).  The shape tables
+// (twiddles, spline pivots, octant weights) are shared.  The point's scalars
+// are pp[slot] in its arena (pp non-null): they replace the launch's
+// by-value arguments.  Bp{} (P = 1, arena 0, pp null) is a plain launch.
+constexpr int kPP = 16;
+enum PpSlot {
+    kPpT = 0,       // temperature
+    kPpMu0,         // mu0 (written on the device by the batched density root)
+    kPpU,           // U
+    kPpN,           // density n
+    kPpNsr,         // nsr of the sum rules
+    kPpNormFact,    // T / L^2
+    kPpJc,          // first frequency of the find_mu series
+    kPpWc,          // w_jc
+    kPpMu0Fixed,    // 1: mu0 = 0 (half filling with t' = t'' = 0), no root search
+};
+struct Bp {
+    int P = 1;
+    long long arena = 0;       // bytes between consecutive points' arrays
+    const double *pp = nullptr;  // point 0's scalars [kPP]
+};
+
 // ---- launchers (all asynchronous on `st`) ---------------------------------
 cudaError_t launch_density(const GridDev &g, double mu, double n, double T, Reduce r, cudaStream_t st);
 
 // per-octant (eps - mu0, G0 prefactor) into g.gk
-cudaError_t launch_gk_table(const GridDev &g, double mu0, double T, cudaStream_t st);
+cudaError_t launch_gk_table(const GridDev &g, double mu0, double T, cudaStream_t st, const Bp &b = Bp{});
 cudaError_t launch_gslice(const GridDev &g, double *Grt, double mu0, double T, cudaStream_t st);
 cudaError_t launch_chi0_boundary(const GridDev &g, const double *Grt, double mu0, double T,
                                  double *dG0p, double *dtau_chirt0, double *dtau_chiqt0, cudaStream_t st);
 cudaError_t launch_chi0_boundary(const GridDev &g, const float *Grt, double mu0, double T,
-                                 double *dG0p, double *dtau_chirt0, double *dtau_chiqt0, cudaStream_t st);
+                                 double *dG0p, double *dtau_chirt0, double *dtau_chiqt0, cudaStream_t st,
+                                 const Bp &b = Bp{});
 // the mixed-precision form's FP32 slice transforms (tpsc_mixed.cu)
-cudaError_t launch_gslice32(const GridDev &g, float *Grt, double mu0, double T, cudaStream_t st);
-cudaError_t launch_chi0_slice32(const GridDev &g, const float *Grt, double *chirt, double *chiq, cudaStream_t st);
+cudaError_t launch_gslice32(const GridDev &g, float *Grt, double mu0, double T, cudaStream_t st, const Bp &b = Bp{});
+cudaError_t launch_chi0_slice32(const GridDev &g, const float *Grt, double *chirt, double *chiq, cudaStream_t st,
+                                const Bp &b = Bp{});
 // Usc: the device pair (Usp, Uch) -- the sum-rule root search leaves it there
 cudaError_t launch_vertex_q32(const GridDev &g, const double *chiq, double *Vr, double U, const double *Usc, double T,
-                              cudaStream_t st);
+                              cudaStream_t st, const Bp &b = Bp{});
 cudaError_t launch_chi0_slice(const GridDev &g, const double *Grt, double *chirt, double *chiq, cudaStream_t st);
 cudaError_t launch_chi0_tau(const GridDev &g, double *chiq, const double *dtau_chiqt0, double *chi0_inf,
-                            double *chi0_inf2, double T, cudaStream_t st);
+                            double *chi0_inf2, double T, cudaStream_t st, const Bp &b = Bp{});
 
 // mu0 by safeguarded Newton in one block -> r.result[0] (iterations in r.result[1])
-cudaError_t launch_mu0_newton(const GridDev &g, double n, double T, Reduce r, cudaStream_t st);
+cudaError_t launch_mu0_newton(const GridDev &g, double n, double T, Reduce r, cudaStream_t st, const Bp &b = Bp{});
 // chi0max, qmax -> r.result[0..2]
-cudaError_t launch_chi0max(const GridDev &g, const double *chiq, Reduce r, cudaStream_t st);
+cudaError_t launch_chi0max(const GridDev &g, const double *chiq, Reduce r, cudaStream_t st, const Bp &b = Bp{});
 
 // sum-rule trace and its U derivative -> r.result[0..1]; stored frequencies
 // j < jdir term by term (jdir = -1: all)
@@ -83,14 +111,15 @@ cudaError_t launch_sumrule(const GridDev &g, const double *chiq, const double *c
 // Matsubara-tail moments sum_q w S_(k+2) -> r.result[0..kMomP), max tail |chi| ->
 // r.result[kMomP + 1] (r.partial must hold (2 kMomP + 2) kMaxBlocks doubles)
 cudaError_t launch_tail_moments(const GridDev &g, const double *chi0_inf, const double *chi0_inf2, double T,
-                                Reduce r, cudaStream_t st);
+                                Reduce r, cudaStream_t st, const Bp &b = Bp{});
 // per-frequency moments sum_q w f chi^(k+2), k < kMomP -> mom [nb][kMomP]; max_q |chi| -> cmax [nb]
 constexpr int kMomP = 8;
 constexpr double kMomSeriesMax = 0.004;  // |h chi| bound of the series terms: 0.004^8 < 1e-19
 constexpr double kMomMuRange = 0.35;     // |mu - mu0| the find_mu series is built to cover
 constexpr int kMuMomP = 12;              // terms of the find_mu series
 constexpr double kMuSeriesMax = 0.03;    // |mu - mu0| / |z| bound of its terms: 0.03^12 < 1e-18
-cudaError_t launch_chi0_moments(const GridDev &g, const double *chiq, double *mom, double *cmax, cudaStream_t st);
+cudaError_t launch_chi0_moments(const GridDev &g, const double *chiq, double *mom, double *cmax, cudaStream_t st,
+                                const Bp &b = Bp{});
 // Forward tangents of the chi0 stage (tpsc_tangent.cu): buffers of one
 // direction.  fd[o] = (beta f(xi_o), dxi_o); der[o] the direction of the
 // hopping table; Grt the FP64 G(r, tau) and dG0p the primal d/dtau G(r, 0+).
@@ -118,7 +147,8 @@ cudaError_t launch_sumrule_tan(const GridDev &g, const double *chiq, const doubl
 // [nb + 1]; the tail moments and tail maximum of launch_tail_moments' result
 // -> tailm [kMomP + 1].  One launch, no host round trip.
 cudaError_t launch_moment_suffix(const GridDev &g, const double *mom, const double *cmax, const double *tail_result,
-                                 double *mom_suf, double *cmax_suf, double *tailm, cudaStream_t st);
+                                 double *mom_suf, double *cmax_suf, double *tailm, cudaStream_t st,
+                                 const Bp &b = Bp{});
 cudaError_t launch_trace_chi0(const GridDev &g, const double *chiq, const double *chi0_inf,
                               const double *chi0_inf2, double T, Reduce r, cudaStream_t st);
 
@@ -126,19 +156,20 @@ cudaError_t launch_trace_chi0(const GridDev &g, const double *chiq, const double
 cudaError_t launch_vertex_q(const GridDev &g, const double *chiq, double *Vr, double U, const double *Usc, double T,
                             cudaStream_t st);
 cudaError_t launch_vertex_tau(const GridDev &g, double *Vr, const double *chirt, double U, const double *Usc,
-                              cudaStream_t st);
+                              cudaStream_t st, const Bp &b = Bp{});
 
 cudaError_t launch_sigma_boundary(const GridDev &g, const double *Grt, const double *V, const double *dtau_chirt0,
                                   const double *dG0p, double mu0, double U, const double *Usc, double *dS,
                                   cudaStream_t st);
 cudaError_t launch_sigma_boundary(const GridDev &g, const float *Grt, const double *V, const double *dtau_chirt0,
                                   const double *dG0p, double mu0, double U, const double *Usc, double *dS,
-                                  cudaStream_t st);
+                                  cudaStream_t st, const Bp &b = Bp{});
 cudaError_t launch_sigma_slice(const GridDev &g, const double *Grt, const double *V, double *sigt, cudaStream_t st);
 // the mixed form's Sigma slices: FP32 transform, local term in FP64 (tpsc_mixed.cu)
-cudaError_t launch_sigma_slice32(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st);
+cudaError_t launch_sigma_slice32(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st,
+                                 const Bp &b = Bp{});
 cudaError_t launch_sigma_tau(const GridDev &g, const double *sigt, const double *dS, double2 *S, double *s2,
-                             double *s3, double *s4, double *sinf, double T, cudaStream_t st);
+                             double *s3, double *s4, double *sinf, double T, cudaStream_t st, const Bp &b = Bp{});
 
 // Tr(G - G0) at pmu and its pmu derivative -> r.result[0..1]; jdir = -1: all
 // frequencies (stored and tail), else stored j < jdir only
@@ -172,14 +203,14 @@ struct RootScratch {
 constexpr int kSigmaMomNV = 2 * kMuMomP + 3;
 cudaError_t launch_sigma_moments(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                                  const double *s4, const double *sinf, double mu0, double T, int jc, Reduce r,
-                                 cudaStream_t st);
+                                 cudaStream_t st, const Bp &b = Bp{});
 // mu by safeguarded Newton from mu0 (the series of the moments `mom` while
 // |mu - mu0| <= kMuSeriesMax (wc - 2 |Sigma_inf| / wc), wc = w_jc, the full
 // sum beyond), then Tr Sigma G at mu; one cooperative launch -> rs.out =
 // {mu, evals, ok, Tr Sigma G}
 cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2, const double *s3, const double *s4,
                             const double *sinf, const double *mom, double mu0, double T, int jc, double wc,
-                            RootScratch rs, cudaStream_t st);
+                            RootScratch rs, cudaStream_t st, const Bp &b = Bp{});
 // Usp then Uch by safeguarded Newton with the moment series, one cooperative
 // launch -> rs.out = {Usp, Uch, evals_sp, evals_ch, ok_sp, ok_ch}.  With
 // chi0max (device), the spin interval ends at 2 / chi0max[0] - hi_off and
@@ -187,7 +218,7 @@ cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2
 cudaError_t launch_sumrule_roots(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
                                  const double *mom_suf, const double *cmax_suf, const double *tailm, double T,
                                  double n, double nsr, double U, double hi_sp, RootScratch rs, cudaStream_t st,
-                                 const double *chi0max = nullptr, double hi_off = 0.0);
+                                 const double *chi0max = nullptr, double hi_off = 0.0, const Bp &b = Bp{});
 
 // ---- real-frequency continuation (Pade / Lagrange) and local G ---------------
 cudaError_t launch_pade_sigma(const GridDev &g, const double2 *S, const double *s2, const double *s3,

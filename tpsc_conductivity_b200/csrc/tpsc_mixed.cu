@@ -87,9 +87,12 @@ __device__ __forceinline__ const float4 *twiddles32(float *S, const float4 *__re
 template <int NBK>
 __global__ void __launch_bounds__(kSlice32Threads, 2)
     k_gslice32(const double2 *__restrict__ gk, const float4 *__restrict__ tw,
-               int n8, int nw0, double T, float *__restrict__ Grt) {
+               int n8, int nw0, double T, float *__restrict__ Grt, Bp b) {
     extern __shared__ __align__(16) float S32[];
     const float4 *tws = twiddles32<NBK>(S32, tw);
+    gk = at(gk, b.arena);
+    Grt = at(Grt, b.arena);
+    T = bpar(b, kPpT, T);
     const int j = blockIdx.x;
     const double t = j / (nw0 * T);
     const double bt = 1.0 / T - t;
@@ -113,9 +116,12 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
 template <int NBK>
 __global__ void __launch_bounds__(kSlice32Threads, 2)
     k_chi0_slice32(const float *__restrict__ Grt, const float4 *__restrict__ tw,
-                   int n8, int nw0, int ahead, double *__restrict__ chirt, double *__restrict__ chiq) {
+                   int n8, int nw0, int ahead, double *__restrict__ chirt, double *__restrict__ chiq, Bp b) {
     extern __shared__ __align__(16) float S32[];
     const float4 *tws = twiddles32<NBK>(S32, tw);
+    Grt = at(Grt, b.arena);
+    chirt = at(chirt, b.arena);
+    chiq = at(chiq, b.arena);
     const int j = blockIdx.x;
     const int nb = nw0 / 2 + 1;
     if (ahead > 0 && j + ahead < nb) {
@@ -159,9 +165,14 @@ template <int NBK>
 __global__ void __launch_bounds__(kSlice32Threads, 2)
     k_vertex_q32(const double *__restrict__ chiq, const float4 *__restrict__ tw,
                  int n8, int nb, int ahead, double normFact, double U, const double *__restrict__ Usc,
-                 double *__restrict__ Vr) {
+                 double *__restrict__ Vr, Bp b) {
     extern __shared__ __align__(16) float S32[];
     const float4 *tws = twiddles32<NBK>(S32, tw);
+    chiq = at(chiq, b.arena);
+    Usc = at(Usc, b.arena);
+    Vr = at(Vr, b.arena);
+    normFact = bpar(b, kPpNormFact, normFact);
+    U = bpar(b, kPpU, U);
     const int j = blockIdx.x;
     const double Usp = Usc[0], Uch = Usc[1];
     if (ahead > 0 && j + ahead < nb) prefetch_l2_blockrow(chiq, j + ahead, nb, (n8 + 3) / 4);
@@ -211,7 +222,10 @@ struct SigmaSlice32Smem {
 template <int NBK>
 __global__ void __launch_bounds__(kSlice32Threads, 2)
     k_sigma_slice32(const float *__restrict__ Grt, const double *__restrict__ V, const float4 *__restrict__ tw,
-                    const double2 *__restrict__ tw64, int n8, int nw0, int ahead, double *__restrict__ sigt) {
+                    const double2 *__restrict__ tw64, int n8, int nw0, int ahead, double *__restrict__ sigt, Bp b) {
+    Grt = at(Grt, b.arena);
+    V = at(V, b.arena);
+    sigt = at(sigt, b.arena);
     constexpr int L = 2 * (NBK - 1);
     constexpr int R = SigmaSlice32Smem<NBK>::R;
     constexpr int NOCT = SigmaSlice32Smem<NBK>::NOCT;
@@ -321,52 +335,58 @@ struct RunCondSlice32 {
     }
 };
 
+// (a batched launch, b.P > 1, skips the L2 prefetch of the slice ahead: its
+// blocks of one slice index belong to different points)
 template <int NBK>
 struct RunGslice32 {
-    static cudaError_t run(const GridDev *g, float *Grt, double mu0, double T, cudaStream_t st) {
+    static cudaError_t run(const GridDev *g, float *Grt, double mu0, double T, const Bp *b, cudaStream_t st) {
         const size_t sm = Slice32Smem<NBK>::bytes;
         cudaError_t e = set_smem(k_gslice32<NBK>, sm);
         if (e != cudaSuccess) return e;
-        if ((e = launch_gk_table(*g, mu0, T, st)) != cudaSuccess) return e;
-        k_gslice32<NBK><<<g->nw0 + 1, kSlice32Threads, sm, st>>>(g->gk, g->tw_k32, g->n8, g->nw0, T, Grt);
+        if ((e = launch_gk_table(*g, mu0, T, st, *b)) != cudaSuccess) return e;
+        k_gslice32<NBK><<<dim3(g->nw0 + 1, 1, b->P), kSlice32Threads, sm, st>>>(g->gk, g->tw_k32, g->n8, g->nw0, T,
+                                                                               Grt, *b);
         return launched();
     }
 };
 template <int NBK>
 struct RunChi0Slice32 {
-    static cudaError_t run(const GridDev *g, const float *Grt, double *chirt, double *chiq, cudaStream_t st) {
+    static cudaError_t run(const GridDev *g, const float *Grt, double *chirt, double *chiq, const Bp *b,
+                           cudaStream_t st) {
         const size_t sm = Slice32Smem<NBK>::bytes;
         cudaError_t e = set_smem(k_chi0_slice32<NBK>, sm);
         if (e != cudaSuccess) return e;
-        const int ahead = resident_ctas(k_chi0_slice32<NBK>, kSlice32Threads, sm);
-        k_chi0_slice32<NBK><<<g->nb, kSlice32Threads, sm, st>>>(Grt, g->tw_k32, g->n8, g->nw0, ahead, chirt, chiq);
+        const int ahead = b->P > 1 ? 0 : resident_ctas(k_chi0_slice32<NBK>, kSlice32Threads, sm);
+        k_chi0_slice32<NBK><<<dim3(g->nb, 1, b->P), kSlice32Threads, sm, st>>>(Grt, g->tw_k32, g->n8, g->nw0, ahead,
+                                                                              chirt, chiq, *b);
         return launched();
     }
 };
 template <int NBK>
 struct RunVertexQ32 {
     static cudaError_t run(const GridDev *g, const double *chiq, double *Vr, double U, const double *Usc, double T,
-                           cudaStream_t st) {
+                           const Bp *b, cudaStream_t st) {
         const size_t sm = Slice32Smem<NBK>::bytes;
         cudaError_t e = set_smem(k_vertex_q32<NBK>, sm);
         if (e != cudaSuccess) return e;
         const double normFact = T / ((double)g->nk0 * g->nk0);
-        const int ahead = resident_ctas(k_vertex_q32<NBK>, kSlice32Threads, sm);
-        k_vertex_q32<NBK><<<g->nb, kSlice32Threads, sm, st>>>(chiq, g->tw_k32, g->n8, g->nb, ahead, normFact, U,
-                                                              Usc, Vr);
+        const int ahead = b->P > 1 ? 0 : resident_ctas(k_vertex_q32<NBK>, kSlice32Threads, sm);
+        k_vertex_q32<NBK><<<dim3(g->nb, 1, b->P), kSlice32Threads, sm, st>>>(chiq, g->tw_k32, g->n8, g->nb, ahead,
+                                                                            normFact, U, Usc, Vr, *b);
         return launched();
     }
 };
 
 template <int NBK>
 struct RunSigmaSlice32 {
-    static cudaError_t run(const GridDev *g, const float *Grt, const double *V, double *sigt, cudaStream_t st) {
+    static cudaError_t run(const GridDev *g, const float *Grt, const double *V, double *sigt, const Bp *b,
+                           cudaStream_t st) {
         const size_t sm = SigmaSlice32Smem<NBK>::bytes;
         cudaError_t e = set_smem(k_sigma_slice32<NBK>, sm);
         if (e != cudaSuccess) return e;
-        const int ahead = resident_ctas(k_sigma_slice32<NBK>, kSlice32Threads, sm);
-        k_sigma_slice32<NBK><<<g->nw0 + 1, kSlice32Threads, sm, st>>>(Grt, V, g->tw_k32, g->tw_k, g->n8, g->nw0,
-                                                                     ahead, sigt);
+        const int ahead = b->P > 1 ? 0 : resident_ctas(k_sigma_slice32<NBK>, kSlice32Threads, sm);
+        k_sigma_slice32<NBK><<<dim3(g->nw0 + 1, 1, b->P), kSlice32Threads, sm, st>>>(Grt, V, g->tw_k32, g->tw_k, g->n8,
+                                                                                    g->nw0, ahead, sigt, *b);
         return launched();
     }
 };
@@ -378,21 +398,23 @@ cudaError_t launch_cond_slice32(const GridDev &g, const CondDev &c, const double
     return dispatch_nbk<RunCondSlice32>(g.nbk, &g, &c, V, T, ny, st);
 }
 
-cudaError_t launch_sigma_slice32(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st) {
-    return dispatch_nbk<RunSigmaSlice32>(g.nbk, &g, Grt, V, sigt, st);
+cudaError_t launch_sigma_slice32(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st,
+                                 const Bp &b) {
+    return dispatch_nbk<RunSigmaSlice32>(g.nbk, &g, Grt, V, sigt, &b, st);
 }
 
-cudaError_t launch_gslice32(const GridDev &g, float *Grt, double mu0, double T, cudaStream_t st) {
-    return dispatch_nbk<RunGslice32>(g.nbk, &g, Grt, mu0, T, st);
+cudaError_t launch_gslice32(const GridDev &g, float *Grt, double mu0, double T, cudaStream_t st, const Bp &b) {
+    return dispatch_nbk<RunGslice32>(g.nbk, &g, Grt, mu0, T, &b, st);
 }
 
-cudaError_t launch_chi0_slice32(const GridDev &g, const float *Grt, double *chirt, double *chiq, cudaStream_t st) {
-    return dispatch_nbk<RunChi0Slice32>(g.nbk, &g, Grt, chirt, chiq, st);
+cudaError_t launch_chi0_slice32(const GridDev &g, const float *Grt, double *chirt, double *chiq, cudaStream_t st,
+                                const Bp &b) {
+    return dispatch_nbk<RunChi0Slice32>(g.nbk, &g, Grt, chirt, chiq, &b, st);
 }
 
 cudaError_t launch_vertex_q32(const GridDev &g, const double *chiq, double *Vr, double U, const double *Usc, double T,
-                              cudaStream_t st) {
-    return dispatch_nbk<RunVertexQ32>(g.nbk, &g, chiq, Vr, U, Usc, T, st);
+                              cudaStream_t st, const Bp &b) {
+    return dispatch_nbk<RunVertexQ32>(g.nbk, &g, chiq, Vr, U, Usc, T, &b, st);
 }
 
 }  // namespace tpsc

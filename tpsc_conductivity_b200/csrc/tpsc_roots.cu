@@ -77,6 +77,7 @@ struct SumRootArgs {
     unsigned *bar;    // [2], zero at launch
     int *err;         // zero at launch
     double *out;      // Usp, Uch, evals_sp, evals_ch, ok_sp, ok_ch
+    Bp b;             // batched launch: point blockIdx.z, blocks blockIdx.x of gridDim.x per point
 };
 
 // the (value, derivative) pair, summed in a fixed order
@@ -158,6 +159,26 @@ constexpr double kSpinSMax = 40.0;  // -hi expm1(-40) = hi (1 - 4e-18)
 __device__ __forceinline__ double spin_us(double s, double hi) { return -hi * expm1(-s); }
 
 __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
+    {
+        const long long ar = a.b.arena;
+        a.chiq = at(a.chiq, ar);
+        a.cinf = at(a.cinf, ar);
+        a.cinf2 = at(a.cinf2, ar);
+        a.tailq = at(a.tailq, ar);
+        a.mom_suf = at(a.mom_suf, ar);
+        a.cmax_suf = at(a.cmax_suf, ar);
+        a.tailm = at(a.tailm, ar);
+        a.chi0max = at(a.chi0max, ar);
+        a.partial = at(a.partial, ar);
+        a.bar = at(a.bar, ar);
+        a.err = at(a.err, ar);
+        a.out = at(a.out, ar);
+        a.T = bpar(a.b, kPpT, a.T);
+        a.scale = bpar(a.b, kPpNormFact, a.scale);
+        a.n = bpar(a.b, kPpN, a.n);
+        a.nsr = bpar(a.b, kPpNsr, a.nsr);
+        a.U = bpar(a.b, kPpU, a.U);
+    }
     // the spin interval's upper end 2/chi0max - 2 eps, from the device maximum
     // when the chi0 stage left it there (no host round trip)
     const double hi_sp = a.chi0max ? 2.0 / a.chi0max[0] - a.hi_off : a.hi_sp;
@@ -319,9 +340,20 @@ __global__ void __launch_bounds__(256, 2)
     k_sigma_moments(const double2 *__restrict__ S, const double *__restrict__ s2, const double *__restrict__ s3,
                     const double *__restrict__ s4, const double *__restrict__ sinfp, const double *__restrict__ ek,
                     const double *__restrict__ w16, const double *__restrict__ tailP, int nw0, double mu0,
-                    double T, double nk02, int jc, double *partial) {
+                    double T, double nk02, int jc, double *partial, Bp b) {
     constexpr int NV = kSigmaMomNV, P64 = kMuMomF64, P32 = kMuMomP - kMuMomF64;
     __shared__ double cw[4], cx[4], c2[4], c3[4], c4[4];
+    S = at(S, b.arena);
+    s2 = at(s2, b.arena);
+    s3 = at(s3, b.arena);
+    s4 = at(s4, b.arena);
+    sinfp = at(sinfp, b.arena);
+    ek = at(ek, b.arena);
+    tailP = at(tailP, b.arena);
+    partial = at(partial, b.arena);
+    mu0 = bpar(b, kPpMu0, mu0);
+    T = bpar(b, kPpT, T);
+    jc = (int)bpar(b, kPpJc, (double)jc);
     const int blk = blockIdx.x, o0 = 4 * blk, NO = nw0 / 2;
     const double sinf = sinfp[0];
     const double pt = 3.141592653589793 * T;
@@ -513,12 +545,31 @@ struct MuRootArgs {
     unsigned *bar;
     int *err;
     double *out;  // mu, evals, ok, Tr Sigma G at mu
+    Bp b;         // batched launch: point blockIdx.z
 };
 
 // find_mu by safeguarded Newton (the host routine newton_root's steps) from
 // mu0 inside [-10, 10] with tolerance 1e-15, one barrier per evaluation as in
 // k_sumrule_roots; then green::traceSelfG2 (src/green.cpp:2929-2976) at mu.
 __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
+    {
+        const long long ar = a.b.arena;
+        a.S = at(a.S, ar);
+        a.s2 = at(a.s2, ar);
+        a.s3 = at(a.s3, ar);
+        a.s4 = at(a.s4, ar);
+        a.sinf = at(a.sinf, ar);
+        a.ek = at(a.ek, ar);
+        a.mom = at(a.mom, ar);
+        a.partial = at(a.partial, ar);
+        a.bar = at(a.bar, ar);
+        a.err = at(a.err, ar);
+        a.out = at(a.out, ar);
+        a.mu0 = bpar(a.b, kPpMu0, a.mu0);
+        a.T = bpar(a.b, kPpT, a.T);
+        a.jc = (int)bpar(a.b, kPpJc, (double)a.jc);
+        a.wc = bpar(a.b, kPpWc, a.wc);
+    }
     __shared__ RootCtl sc;
     const int NO = a.nw0 / 2;
     const double sinf = a.sinf[0];
@@ -686,25 +737,31 @@ cudaError_t root_grid(K kernel, int *grid, int cap) {
 
 cudaError_t launch_sigma_moments(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                                  const double *s4, const double *sinf, double mu0, double T, int jc, Reduce r,
-                                 cudaStream_t st) {
+                                 cudaStream_t st, const Bp &b) {
     const int nblk = g.n8p / 4;
     const double nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
-    k_sigma_moments<<<nblk, 256, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.tailP, g.nw0, mu0, T, nk02, jc,
-                                          r.partial);
+    k_sigma_moments<<<dim3(nblk, 1, b.P), 256, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.tailP, g.nw0, mu0, T,
+                                                         nk02, jc, r.partial, b);
     cudaError_t e = launched();
     if (e != cudaSuccess) return e;
-    return finish<kSigmaMomNV>(r, nblk, 0.0, st);
+    return finish<kSigmaMomNV>(r, nblk, 0.0, st, b);
 }
 
 cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2, const double *s3, const double *s4,
                             const double *sinf, const double *mom, double mu0, double T, int jc, double wc,
-                            RootScratch rs, cudaStream_t st) {
+                            RootScratch rs, cudaStream_t st, const Bp &b) {
     int grid = 0;
     cudaError_t e = root_grid(k_mu_roots, &grid, rs.max_blocks);
     if (e != cudaSuccess) return e;
+    // a batched search: the resident grid shared out between the points
+    // (the caller keeps P at most the resident grid)
+    if (b.P > 1) grid = std::max(1, grid / b.P);
     // words 4..6 of rs.bar: the sum-rule search's error flag (word 2) stays readable
-    if (rs.reset_mu && (e = cudaMemsetAsync(rs.bar + 4, 0, 2 * sizeof(unsigned) + sizeof(int), st)) != cudaSuccess)
-        return e;
+    if (rs.reset_mu) {
+        e = b.P > 1 ? cudaMemset2DAsync(rs.bar + 4, (size_t)b.arena, 0, 2 * sizeof(unsigned) + sizeof(int), b.P, st)
+                    : cudaMemsetAsync(rs.bar + 4, 0, 2 * sizeof(unsigned) + sizeof(int), st);
+        if (e != cudaSuccess) return e;
+    }
     MuRootArgs a;
     a.S = S;
     a.s2 = s2;
@@ -725,8 +782,9 @@ cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2
     a.bar = rs.bar + 4;
     a.err = reinterpret_cast<int *>(rs.bar + 6);
     a.out = rs.out;
+    a.b = b;
     void *args[] = {&a};
-    e = cudaLaunchCooperativeKernel((const void *)k_mu_roots, dim3(grid), dim3(kRootThreads), args, 0, st);
+    e = cudaLaunchCooperativeKernel((const void *)k_mu_roots, dim3(grid, 1, b.P), dim3(kRootThreads), args, 0, st);
     if (e != cudaSuccess) return e;
     return launched();
 }
@@ -734,12 +792,16 @@ cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2
 cudaError_t launch_sumrule_roots(const GridDev &g, const double *chiq, const double *chi0_inf, const double *chi0_inf2,
                                  const double *mom_suf, const double *cmax_suf, const double *tailm, double T,
                                  double n, double nsr, double U, double hi_sp, RootScratch rs, cudaStream_t st,
-                                 const double *chi0max, double hi_off) {
+                                 const double *chi0max, double hi_off, const Bp &b) {
     int grid = 0;
     cudaError_t e = root_grid(k_sumrule_roots, &grid, rs.max_blocks);
     if (e != cudaSuccess) return e;
-    if (rs.reset_sr && (e = cudaMemsetAsync(rs.bar, 0, 2 * sizeof(unsigned) + sizeof(int), st)) != cudaSuccess)
-        return e;
+    if (b.P > 1) grid = std::max(1, grid / b.P);
+    if (rs.reset_sr) {
+        e = b.P > 1 ? cudaMemset2DAsync(rs.bar, (size_t)b.arena, 0, 2 * sizeof(unsigned) + sizeof(int), b.P, st)
+                    : cudaMemsetAsync(rs.bar, 0, 2 * sizeof(unsigned) + sizeof(int), st);
+        if (e != cudaSuccess) return e;
+    }
     SumRootArgs a;
     a.chiq = reinterpret_cast<const double4 *>(chiq);
     a.cinf = chi0_inf;
@@ -764,8 +826,10 @@ cudaError_t launch_sumrule_roots(const GridDev &g, const double *chiq, const dou
     a.bar = rs.bar;
     a.err = reinterpret_cast<int *>(rs.bar + 2);
     a.out = rs.out;
+    a.b = b;
     void *args[] = {&a};
-    e = cudaLaunchCooperativeKernel((const void *)k_sumrule_roots, dim3(grid), dim3(kRootThreads), args, 0, st);
+    e = cudaLaunchCooperativeKernel((const void *)k_sumrule_roots, dim3(grid, 1, b.P), dim3(kRootThreads), args, 0,
+                                    st);
     if (e != cudaSuccess) return e;
     return launched();
 }
