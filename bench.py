@@ -444,11 +444,13 @@ def batch_sweep(steps):
     form = _lib.FORM_NEWTON | _lib.FORM_MIXED
     b = Batch(nstreams=1)
     tune = b.tune(pts, form, max_streams=16)
-    # the sweep as direct launches (graph mode 0) and as one graph launch per
-    # point (mode 2: each grid's graph updated in place for the point)
+    # the sweep as direct launches (graph mode 0), as one graph launch per
+    # point (mode 2: each grid's graph updated in place for the point) and by
+    # shape groups (mode 3: one launch per stage over every point of a
+    # (nk0, Nw0) group, one graph launch per group, tpsc_solve_points)
     per_mode = {}
     st = None
-    for mode in (0, 2):
+    for mode in (0, 2, 3):
         b.set_graph_mode(mode)
         b.solve(pts, form)  # mode 2: every grid captured once before timing
         times = []
@@ -465,6 +467,9 @@ def batch_sweep(steps):
            "form": "mixed + Newton", "shapes": len(shapes), "streams": b.nstreams,
            "solves_per_s": 512 / (best / 1e3), "ms_per_sweep": best, "graph_mode": mode,
            "ms_per_sweep_direct": per_mode[0], "ms_per_sweep_graphs": per_mode[2],
+           "ms_per_sweep_shape_groups": per_mode[3],
+           "launches": {"0": "every kernel of every point", "2": "one graph per point",
+                        "3": "one graph per (nk0, Nw0) group, each kernel over all its points"},
            "sequential_solves_per_s": 512 / (tune[1] / 1e3), "tune_ms": tune, "failed_points": nfail,
            "timing": "host wall clock around the whole call, device idle at both ends"}
     b.close()

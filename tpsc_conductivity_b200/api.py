@@ -386,6 +386,21 @@ def _scalar_names():
     return SCALAR_NAMES
 
 
+def solve_points(params, ctx=None, streams=2):
+    """tpsc_solve_points: the rows (nk0, Nw0, n, T, tp, tpp, t3, U) solved by
+    shape groups in the Newton-form mixed solve, one graph launch per group.
+    Returns (scalars [npts, TPSC_S_COUNT], status [npts], wall ms)."""
+    ctx = ctx or Context()
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    n = p.shape[0]
+    res = np.zeros((n, len(_scalar_names())))
+    st = np.zeros(n, dtype=np.int32)
+    ms = np.zeros(1)
+    ctx.call("tpsc_set_group_streams", int(streams))
+    ctx.call("tpsc_solve_points", n, _dptr(p), _dptr(res), st.ctypes.data_as(_lib._ip), _dptr(ms))
+    return res, st, float(ms[0])
+
+
 def sweep_points(npts, seed=20261203):
     """The parameter-sweep workload (tpsc_sweep_points): npts rows
     (nk0, Nw0, n, T, tp, tpp, t3, U) from std::mt19937_64(seed)."""
@@ -461,7 +476,9 @@ class Batch:
 
     def set_graph_mode(self, mode):
         """tpsc_set_graph_mode of every solver context (2: each Newton-form
-        point is one graph launch, updated in place per point)."""
+        point is one graph launch, updated in place per point; 3: a Newton +
+        mixed sweep by shape groups, one graph launch per (nk0, Nw0) group
+        whose kernels each run over all its points)."""
         rc = self.lib.tpsc_batch_set_graph_mode(self.h, int(mode))
         if rc:
             self._err(rc)
