@@ -125,6 +125,10 @@ int tpsc_set_graph_mode(tpsc_ctx *ctx, int mode);
  * so the next solve recomputes the grid's stages.  tpsc_set_tau_tile sets
  * one tiling (kind 0 chi0, 1 V, 2 Sigma). */
 int tpsc_tune_tau_tiles(tpsc_ctx *ctx, int reps, double ms[6]);
+/* The same tuner over the FFT plan as well: tile 2 = one column pair per CTA
+ * with radix-8 FFT passes (twice the threads in the FFT; Nw0 <= 2048), timed
+ * beside tiles 0 and 1; ms[3 kind + plan] (0 where plan 2 does not apply). */
+int tpsc_tune_tau_plans(tpsc_ctx *ctx, int reps, double ms[9]);
 int tpsc_set_tau_tile(int kind, int nw0, int tile);
 
 /* out = {captures, replays, kernels in the current graph, 1 if a capture

@@ -84,6 +84,7 @@ SIGNATURES = [
     ("tpsc_set_graph_mode", C.c_int, [C.c_void_p, C.c_int]),
     ("tpsc_set_nsr", C.c_int, [C.c_void_p, C.c_double]),
     ("tpsc_tune_tau_tiles", C.c_int, [C.c_void_p, C.c_int, _dp]),
+    ("tpsc_tune_tau_plans", C.c_int, [C.c_void_p, C.c_int, _dp]),
     ("tpsc_set_tau_tile", C.c_int, [C.c_int, C.c_int, C.c_int]),
     ("tpsc_graph_stats", C.c_int, [C.c_void_p, C.c_void_p]),
     ("tpsc_chijj", C.c_int, [C.c_void_p, C.c_int]),

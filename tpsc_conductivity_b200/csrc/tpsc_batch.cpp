@@ -255,7 +255,7 @@ int tpsc_batch_tune(tpsc_batch *b, int form, int npts, const double *params, int
         tpsc_set_form(c0, form);
         if (tpsc_set_model(c0, shape.first, shape.second, p[2], p[3], p[4], p[5], p[6], p[7]) == TPSC_OK &&
             tpsc_solve(c0) == TPSC_OK)
-            tpsc_tune_tau_tiles(c0, 3, nullptr);
+            tpsc_tune_tau_plans(c0, 3, nullptr);
     }
     double best = 0.0;
     int best_n = 1, k = 0;

@@ -377,6 +377,7 @@ struct Group {
     double *h_res = nullptr; // pinned, cap * kGroupRes
     cudaGraphExec_t gexec = nullptr;
     int gexec_P = 0;
+    long long gexec_tiles = -1;  // tau_tiles_version() the graph was captured with
 };
 // results block of a point (doubles): [0, 3) chi0max, qmax; [8, 14) the
 // sum-rule roots; [16, 20) the root searches' barrier words; [20, 24) the mu
@@ -2349,6 +2350,11 @@ int group_queue(tpsc_ctx *ctx, Group *q, int P, cudaStream_t st, int root_cap) {
 // direct one (the kernels' one-time attribute calls happen outside a
 // capture), replayed while P stays the same
 int group_run(tpsc_ctx *ctx, Group *q, int P, cudaStream_t st, int root_cap) {
+    if (q->gexec_tiles != tau_tiles_version()) {
+        // the tau transforms' plans changed: launch directly, then capture again
+        q->gexec_P = 0;
+        q->gexec_tiles = tau_tiles_version();
+    }
     if (q->gexec && q->gexec_P == P) {
         CK(cudaGraphLaunch(q->gexec, st));
         return TPSC_OK;
@@ -2677,11 +2683,60 @@ int tpsc_tune_tau_tiles(tpsc_ctx *ctx, int reps, double ms[6]) {
     return TPSC_OK;
 }
 
+// The FFT plan and tiling of the three tau transforms for the current grid's
+// Nw0: one column pair per CTA with radix-16 passes (0), four columns per CTA
+// (1), one pair per CTA with radix-8 passes (2, Nw0 <= 2048: twice the
+// threads in the FFT, one more pass) -- each timed as in
+// tpsc_tune_tau_tiles, the fastest kept; ms[3 kind + plan] (plan 2 is 0
+// where it does not apply).
+int tpsc_tune_tau_plans(tpsc_ctx *ctx, int reps, double ms[9]) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    Grid *g = ctx->cur;
+    if (!g || !g->have_S) return fail(ctx, TPSC_ERR_STATE, "tune after a solve on the current grid");
+    if (reps < 1 || reps > 100) return fail(ctx, TPSC_ERR_ARG, "need 1 <= reps <= 100");
+    cudaSetDevice(ctx->device);
+    const GridDev &d = g->d;
+    cudaEvent_t a = ctx->ev[0], b = ctx->ev[1];
+    const int nplans = d.nw0 <= 2048 ? 3 : 2;
+    for (int kind = 0; kind < 3; ++kind) {
+        double best = 0.0;
+        int pick = 0;
+        for (int plan = 0; plan < 3; ++plan) {
+            if (ms) ms[3 * kind + plan] = 0.0;
+            if (plan >= nplans) continue;
+            set_tau_tile(kind, d.nw0, plan);
+            auto run = [&]() -> cudaError_t {
+                if (kind == kTauChi0) return launch_chi0_tau(d, g->chiq, g->dchiqt0, g->cinf, g->cinf2, ctx->T, ctx->st);
+                if (kind == kTauVertex) return launch_vertex_tau(d, g->V, g->chirt, ctx->U, ctx->dres, ctx->st);
+                return launch_sigma_tau(d, g->sigt, g->dS, g->S, g->s2, g->s3, g->s4, g->sinf, ctx->T, ctx->st);
+            };
+            CK(run());
+            CK(cudaEventRecord(a, ctx->st));
+            for (int r = 0; r < reps; ++r) CK(run());
+            CK(cudaEventRecord(b, ctx->st));
+            CK(cudaEventSynchronize(b));
+            float t = 0;
+            CK(cudaEventElapsedTime(&t, a, b));
+            const double mean = t / reps;
+            if (ms) ms[3 * kind + plan] = mean;
+            if (plan == 0 || mean < best) {
+                best = mean;
+                pick = plan;
+            }
+        }
+        set_tau_tile(kind, d.nw0, pick);
+    }
+    g->have_chi0 = g->have_V = g->have_S = g->have_mom = g->have_U = false;
+    return TPSC_OK;
+}
+
 // the tiling of one tau transform for one Nw0 (kind 0 chi0, 1 V, 2 Sigma;
-// tile 0 one column pair per CTA, 1 four columns per CTA)
+// tile 0 one column pair per CTA, 1 four columns per CTA, 2 one pair per CTA
+// with radix-8 FFT passes, Nw0 <= 2048)
 int tpsc_set_tau_tile(int kind, int nw0, int tile) {
-    if (kind < 0 || kind > 2 || tile < 0 || tile > 1 || !supported_grid(8, nw0))
-        return fail(nullptr, TPSC_ERR_ARG, "need kind 0..2, tile 0..1 and a supported Nw0");
+    if (kind < 0 || kind > 2 || tile < 0 || tile > 2 || !supported_grid(8, nw0) || (tile == 2 && nw0 > 2048))
+        return fail(nullptr, TPSC_ERR_ARG, "need kind 0..2, tile 0..2 (2: Nw0 <= 2048) and a supported Nw0");
     set_tau_tile(kind, nw0, tile);
     return TPSC_OK;
 }

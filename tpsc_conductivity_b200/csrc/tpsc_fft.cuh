@@ -308,36 +308,40 @@ __device__ __forceinline__ void stockham_pass(C *x, int t, int Ns, const TW *__r
     if (!LAST) group_sync<G>(grp);
 }
 
-template <int N>
+// EP points per thread (16 or 8): radix-EP passes followed by one pass of
+// radix N / EP^P16 (if > 1); each of the G threads holds E = min(EP, N)
+// points.  EP = 8 takes twice the threads and one more pass for N >= 512.
+template <int N, int EP = 16>
 struct FftPlan {
-    // radix-16 passes followed by one pass of radix N / 16^P16 (if > 1);
-    // each of the G threads holds E = min(16, N) points
+    static_assert(EP == 16 || EP == 8, "16 or 8 points per thread");
     static constexpr int log2n() {
         int l = 0;
         while ((1 << l) < N) ++l;
         return l;
     }
-    static constexpr int P16 = log2n() / 4;
-    static constexpr int RLAST = 1 << (log2n() % 4);
-    static constexpr int E = N < 16 ? N : 16;
+    static constexpr int LE = EP == 16 ? 4 : 3;
+    static constexpr int P16 = log2n() / LE;
+    static constexpr int RLAST = 1 << (log2n() % LE);
+    static constexpr int E = N < EP ? N : EP;
     static constexpr int G = N / E;
     static constexpr int NPASS = P16 + (RLAST > 1 ? 1 : 0);
 };
 
-template <int N, int SIGN, bool SMEM_TW, bool INPLACE, int P, class In, class Out, class C, class TW>
+template <int N, int SIGN, bool SMEM_TW, bool INPLACE, int P, int EP, class In, class Out, class C, class TW>
 __device__ __forceinline__ void fft_passes(C *x, int t, int Ns, const TW *__restrict__ tw, int grp, const In &in,
                                            const Out &out) {
-    constexpr int G = FftPlan<N>::G;
-    constexpr int E = FftPlan<N>::E;
-    constexpr int NP = FftPlan<N>::NPASS;
-    constexpr int R = (P < FftPlan<N>::P16) ? 16 : FftPlan<N>::RLAST;
-    if constexpr (N <= 16) {
+    using Plan = FftPlan<N, EP>;
+    constexpr int G = Plan::G;
+    constexpr int E = Plan::E;
+    constexpr int NP = Plan::NPASS;
+    constexpr int R = (P < Plan::P16) ? EP : Plan::RLAST;
+    if constexpr (N <= EP) {
         // one in-register DFT, single pass
         stockham_pass<N, G, N, SIGN, E, SMEM_TW, true, true, INPLACE>(x, t, 1, tw, grp, in, out);
     } else {
         stockham_pass<N, G, R, SIGN, E, SMEM_TW, P == 0, P == NP - 1, INPLACE && P == 0>(x, t, Ns, tw, grp, in,
                                                                                         out);
-        if constexpr (P + 1 < NP) fft_passes<N, SIGN, SMEM_TW, INPLACE, P + 1>(x, t, Ns * R, tw, grp, in, out);
+        if constexpr (P + 1 < NP) fft_passes<N, SIGN, SMEM_TW, INPLACE, P + 1, EP>(x, t, Ns * R, tw, grp, in, out);
     }
 }
 
@@ -347,12 +351,13 @@ __device__ __forceinline__ void fft_passes(C *x, int t, int Ns, const TW *__rest
 // the FFT has more than one pass, x is free again when the call returns.
 // INPLACE: `in` reads x (the first pass then holds its writes back until
 // every thread of the group has read its inputs).
-template <int N, int SIGN, bool SMEM_TW = false, bool INPLACE = false, class In, class Out, class C, class TW>
+template <int N, int SIGN, bool SMEM_TW = false, bool INPLACE = false, int EP = 16, class In, class Out, class C,
+          class TW>
 __device__ __forceinline__ void group_fft_io(C *x, int t, const TW *__restrict__ tw, int grp, const In &in,
                                              const Out &out) {
     static_assert(N >= 4 && (N & (N - 1)) == 0, "power of two >= 4");
-    fft_passes<N, SIGN, SMEM_TW, INPLACE, 0>(x, t, 1, tw, grp, in, out);
-    if constexpr (FftPlan<N>::NPASS > 1) group_sync<FftPlan<N>::G>(grp);
+    fft_passes<N, SIGN, SMEM_TW, INPLACE, 0, EP>(x, t, 1, tw, grp, in, out);
+    if constexpr (FftPlan<N, EP>::NPASS > 1) group_sync<FftPlan<N, EP>::G>(grp);
 }
 
 // In-place FFT of x[0..N) (padded layout).

@@ -30,8 +30,10 @@ namespace tpsc {
 // kernels launched by this library (all contexts), for the instrumentation ABI
 static std::atomic<long long> g_launches{0};
 
-// tiling of the three tau transforms per N (process-wide; tpsc_tune_tau_tiles):
-// 0 one column pair per CTA (k_*_tau2), 1 four columns per CTA (k_*_tau)
+// tiling of the three tau transforms per N (process-wide; tpsc_tune_tau_tiles,
+// tpsc_tune_tau_plans): 0 one column pair per CTA, radix-16 FFT passes;
+// 1 four columns per CTA (k_*_tau); 2 one pair per CTA with radix-8 passes
+// (k_*_tau2<N, 8>, N <= 2048; 0 elsewhere)
 static std::atomic<int> g_tau_tile[3][13];
 static std::atomic<long long> g_tau_tiles_version{0};
 static int tile_index(int n) {
@@ -581,7 +583,7 @@ struct Tau2Smem {
     static constexpr size_t bytes = buf + 2 * sizeof(TwoLevelTw);
 };
 
-template <int N>
+template <int N, int EP = 16>
 __global__ void __launch_bounds__(256, 2)
     k_sigma_tau2(const double *__restrict__ sigt, const double *__restrict__ dS, double2 *__restrict__ Sout,
                  double *__restrict__ s2, double *__restrict__ s3, double *__restrict__ s4, double *__restrict__ sinf,
@@ -630,7 +632,8 @@ __global__ void __launch_bounds__(256, 2)
         const int o = o0 + threadIdx.x;
         if (o < n8) s3[o] = -(A[threadIdx.x * NJ] + A[threadIdx.x * NJ + N]);
     }
-    constexpr int G = FftPlan<N>::G;
+    constexpr int G = FftPlan<N, EP>::G;
+    static_assert(G <= 256, "one FFT group of at most 256 threads");
     if (threadIdx.x < G) {
         const double *Ma = A, *Mb = A + NJ;
         auto in = [&](int j) -> double2 {
@@ -638,7 +641,7 @@ __global__ void __launch_bounds__(256, 2)
             const double fb = (Mb[j + 1] - Mb[j]) * ih;
             return cmul(tw_at(ht2, j), make_double2(fa, fb));
         };
-        group_fft_io<N, +1, false, true>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
+        group_fft_io<N, +1, false, true, EP>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
     }
     __syncthreads();
     for (int n = threadIdx.x; n < NO; n += blockDim.x) {
@@ -660,7 +663,7 @@ __global__ void __launch_bounds__(256, 2)
 
 // k_chi0_tau for one pair per CTA (in-place FFT, two CTAs per SM); results
 // go straight back to chiq.
-template <int N>
+template <int N, int EP = 16>
 __global__ void __launch_bounds__(256, 2)
     k_chi0_tau2(double *__restrict__ chiq, const double *__restrict__ dtau_chiqt0, double *__restrict__ chi0_inf,
                 double *__restrict__ chi0_inf2, const double *__restrict__ spl, const double2 *__restrict__ tw,
@@ -701,7 +704,8 @@ __global__ void __launch_bounds__(256, 2)
         const double M0 = A[c * NJ], MN = A[c * NJ + NJ - 1];
         integ[c] = h * (sV[c] - 0.5 * (V0[c] + VN[c])) - h * h * h / 24.0 * (2.0 * sM[c] - M0 - MN);
     }
-    constexpr int G = FftPlan<N>::G;
+    constexpr int G = FftPlan<N, EP>::G;
+    static_assert(G <= 256, "one FFT group of at most 256 threads");
     if (threadIdx.x < G) {
         const double *Ma = A, *Mb = A + NJ;
         auto in = [&](int j) -> double2 {
@@ -710,7 +714,7 @@ __global__ void __launch_bounds__(256, 2)
             const double sg = lo ? 1.0 : -1.0;
             return make_double2(sg * (Ma[jj + 1] - Ma[jj]) * ih, sg * (Mb[jj + 1] - Mb[jj]) * ih);
         };
-        group_fft_io<N, +1, false, true>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
+        group_fft_io<N, +1, false, true, EP>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
     }
     __syncthreads();
     for (int n = threadIdx.x + 1; n < NJ; n += blockDim.x) {
@@ -740,7 +744,7 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 // k_vertex_tau for one pair per CTA (in-place FFT, two CTAs per SM).
-template <int N>
+template <int N, int EP = 16>
 __global__ void __launch_bounds__(256, 2)
     k_vertex_tau2(double *__restrict__ Vr, const double *__restrict__ chirt, const double2 *__restrict__ tw,
                   double U, const double *__restrict__ Usc, int n8, Bp b) {
@@ -759,7 +763,8 @@ __global__ void __launch_bounds__(256, 2)
     tau_tables(tw2, tw2 + 1, tw, tw, N);
     stage_pair4(A, Vr + (size_t)blk * 4 * NJ, NJ, half, o0, n8);
     __syncthreads();
-    constexpr int G = FftPlan<N>::G;
+    constexpr int G = FftPlan<N, EP>::G;
+    static_assert(G <= 256, "one FFT group of at most 256 threads");
     if (threadIdx.x < G) {
         const double *a = A, *b = A + NJ;
         // even extension of the two columns: a DCT-I each, packed as Re/Im
@@ -767,7 +772,7 @@ __global__ void __launch_bounds__(256, 2)
             const int jj = j < NJ ? j : N - j;
             return make_double2(a[jj], b[jj]);
         };
-        group_fft_io<N, -1, false, true>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
+        group_fft_io<N, -1, false, true, EP>(X, threadIdx.x, (const TwoLevelTw *)tw2, 0, in, ScratchIO{X});
     }
     __syncthreads();
     double *g = Vr + (size_t)blk * 4 * NJ + 2 * half;
@@ -1735,8 +1740,18 @@ struct RunChi0Tau {
     static cudaError_t run(const GridDev *g, double *chiq, const double *dchiqt0, double *cinf, double *cinf2,
                            double T, const Bp *b, cudaStream_t st) {
         cudaError_t e;
+        const int tile = tau_tile(kTauChi0, N);
+        if constexpr (N / 8 <= 256) {
+            if (tile == 2) {
+                const size_t sm = Tau2Smem<N>::bytes;
+                if ((e = set_smem(k_chi0_tau2<N, 8>, sm)) != cudaSuccess) return e;
+                k_chi0_tau2<N, 8><<<dim3(g->n8p / 2, 1, b->P), 256, sm, st>>>(chiq, dchiqt0, cinf, cinf2,
+                                                                             g->spl_half, g->tw_w, T, g->n8, *b);
+                return launched();
+            }
+        }
         if constexpr (N / 16 <= 256) {
-            if (tau_tile(kTauChi0, N) == 0 || b->pp) {
+            if (tile != 1 || b->pp) {
                 const size_t sm = Tau2Smem<N>::bytes;
                 if ((e = set_smem(k_chi0_tau2<N>, sm)) != cudaSuccess) return e;
                 k_chi0_tau2<N><<<dim3(g->n8p / 2, 1, b->P), 256, sm, st>>>(chiq, dchiqt0, cinf, cinf2, g->spl_half,
@@ -1757,8 +1772,18 @@ struct RunVertexTau {
     static cudaError_t run(const GridDev *g, double *Vr, const double *chirt, double U, const double *Usc,
                            const Bp *b, cudaStream_t st) {
         cudaError_t e;
+        const int tile = tau_tile(kTauVertex, N);
+        if constexpr (N / 8 <= 256) {
+            if (tile == 2) {
+                const size_t sm = Tau2Smem<N>::bytes;
+                if ((e = set_smem(k_vertex_tau2<N, 8>, sm)) != cudaSuccess) return e;
+                k_vertex_tau2<N, 8><<<dim3(g->n8p / 2, 1, b->P), 256, sm, st>>>(Vr, chirt, g->tw_w, U, Usc, g->n8,
+                                                                               *b);
+                return launched();
+            }
+        }
         if constexpr (N / 16 <= 256) {
-            if (tau_tile(kTauVertex, N) == 0 || b->pp) {
+            if (tile != 1 || b->pp) {
                 const size_t sm = Tau2Smem<N>::bytes;
                 if ((e = set_smem(k_vertex_tau2<N>, sm)) != cudaSuccess) return e;
                 k_vertex_tau2<N><<<dim3(g->n8p / 2, 1, b->P), 256, sm, st>>>(Vr, chirt, g->tw_w, U, Usc, g->n8, *b);
@@ -1777,8 +1802,18 @@ struct RunSigmaTau {
     static cudaError_t run(const GridDev *g, const double *sigt, const double *dS, double2 *S, double *s2, double *s3,
                            double *s4, double *sinf, double T, const Bp *b, cudaStream_t st) {
         cudaError_t e;
+        const int tile = tau_tile(kTauSigma, N);
+        if constexpr (N / 8 <= 256) {
+            if (tile == 2) {
+                const size_t sm = Tau2Smem<N>::bytes;
+                if ((e = set_smem(k_sigma_tau2<N, 8>, sm)) != cudaSuccess) return e;
+                k_sigma_tau2<N, 8><<<dim3(g->n8p / 2, 1, b->P), 256, sm, st>>>(
+                    sigt, dS, S, s2, s3, s4, sinf, g->spl_full, g->tw_w, g->ht_w, T, g->n8, g->n8p, *b);
+                return launched();
+            }
+        }
         if constexpr (N / 16 <= 256) {
-            if (tau_tile(kTauSigma, N) == 0 || b->pp) {
+            if (tile != 1 || b->pp) {
                 // one pair per CTA, two CTAs per SM
                 const size_t sm = Tau2Smem<N>::bytes;
                 if ((e = set_smem(k_sigma_tau2<N>, sm)) != cudaSuccess) return e;
