@@ -131,6 +131,31 @@ int tpsc_tune_tau_tiles(tpsc_ctx *ctx, int reps, double ms[6]);
 int tpsc_tune_tau_plans(tpsc_ctx *ctx, int reps, double ms[9]);
 int tpsc_set_tau_tile(int kind, int nw0, int tile);
 
+/* Plan of the mixed form's FP32 slice transforms (2D DCT-I of symmetric
+ * slices; the reference runs them as FFTW REDFT00 x REDFT00 plans,
+ * src/chi0.cpp:462-517, src/chi.cpp:89-115, src/green.cpp:1830-1885),
+ * process-wide per slice kind (0 G(r, tau), 1 chi0, 2 V, 3 Sigma) and
+ * lattice side nk0: plan 0 packed radix-16 FFTs of the even extension,
+ * 1 folded matrix DCT-I on the FP32 pipe (nk0 64, 128, 256), 2 the same on
+ * the tensor cores (below).  Graphs captured
+ * with another plan are captured again.  tpsc_get_slice_plan returns the
+ * plan in use (the library's default until one is set), or -TPSC_ERR_ARG. */
+int tpsc_set_slice_plan(int kind, int nk0, int plan);
+int tpsc_get_slice_plan(int kind, int nk0);
+/* Plan 2 (kind 3, nk0 256) runs the Sigma slice's folded matrix DCT-I on the
+ * tcgen05 tensor cores (3xTF32, FP32 accumulation in tensor memory).  Its
+ * kernels wait on the tensor cores with a 2 s bound; a wait that runs out
+ * sets a process-wide error word (the results of that launch are not valid,
+ * the context stays usable).  tpsc_tensor_plan_errors reads the word of the
+ * current device into *word and clears it when clear != 0. */
+int tpsc_tensor_plan_errors(unsigned *word, int clear);
+/* The autotuner over the slice plans: after a mixed-form solve, times every
+ * plan each slice kind supports on the current grid (reps launches each),
+ * keeps the fastest per kind (process-wide, for this nk0) and leaves the
+ * grid to be recomputed by the next solve.  ms (may be NULL) receives the
+ * mean times, ms[3 kind + plan], 0 where a plan does not apply. */
+int tpsc_tune_slice_plans(tpsc_ctx *ctx, int reps, double ms[12]);
+
 /* out = {captures, replays, kernels in the current graph, 1 if a capture
  * failed and graphs are off}. */
 int tpsc_graph_stats(tpsc_ctx *ctx, long long out[4]);

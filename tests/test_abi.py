@@ -110,3 +110,28 @@ def test_model_calls_reject_a_null_context(lib):
     for name, args in calls.items():
         assert getattr(lib, name)(None, *args) == _lib.ERR_ARG, name
         assert b"null" in lib.tpsc_last_error(None), name
+
+
+def test_slice_plan_arguments_and_defaults(lib):
+    """tpsc_set_slice_plan / tpsc_get_slice_plan are host-side settings: bad
+    kinds, plans and lattices are rejected with TPSC_ERR_ARG, the folded
+    matrix plan only where its tables exist (nk0 64, 128, 256), and the
+    defaults are the FFT plan except the Sigma slice at nk0 = 256."""
+    from tpsc_conductivity_b200 import _lib
+
+    for kind, nk0, plan in [(4, 256, 1), (-1, 256, 0), (3, 256, 3), (3, 32, 1), (3, 100, 0), (0, 16, 1),
+                            (0, 256, 2), (3, 128, 2)]:
+        assert lib.tpsc_set_slice_plan(kind, nk0, plan) == _lib.ERR_ARG, (kind, nk0, plan)
+    assert lib.tpsc_get_slice_plan(4, 256) < 0
+    assert lib.tpsc_get_slice_plan(3, 100) < 0
+    assert lib.tpsc_get_slice_plan(3, 256) in (0, 1, 2)
+    for kind in range(3):
+        assert lib.tpsc_get_slice_plan(kind, 256) in (0, 1)
+    for nk0 in (8, 16, 32):
+        for kind in range(4):
+            assert lib.tpsc_get_slice_plan(kind, nk0) == 0
+    # a set plan reads back, and the default can be put back
+    assert lib.tpsc_set_slice_plan(3, 128, 1) == 0
+    assert lib.tpsc_get_slice_plan(3, 128) == 1
+    assert lib.tpsc_set_slice_plan(3, 128, 0) == 0
+    assert lib.tpsc_get_slice_plan(3, 128) == 0

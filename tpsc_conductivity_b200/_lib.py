@@ -86,6 +86,10 @@ SIGNATURES = [
     ("tpsc_tune_tau_tiles", C.c_int, [C.c_void_p, C.c_int, _dp]),
     ("tpsc_tune_tau_plans", C.c_int, [C.c_void_p, C.c_int, _dp]),
     ("tpsc_set_tau_tile", C.c_int, [C.c_int, C.c_int, C.c_int]),
+    ("tpsc_set_slice_plan", C.c_int, [C.c_int, C.c_int, C.c_int]),
+    ("tpsc_get_slice_plan", C.c_int, [C.c_int, C.c_int]),
+    ("tpsc_tensor_plan_errors", C.c_int, [C.c_void_p, C.c_int]),
+    ("tpsc_tune_slice_plans", C.c_int, [C.c_void_p, C.c_int, _dp]),
     ("tpsc_graph_stats", C.c_int, [C.c_void_p, C.c_void_p]),
     ("tpsc_chijj", C.c_int, [C.c_void_p, C.c_int]),
     ("tpsc_get_chijj", C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),

@@ -18,8 +18,8 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libtpsc_b200.so")
 SOURCES = ["tpsc_kernels.cu", "tpsc_cond.cu", "tpsc_al.cu", "tpsc_mixed.cu", "tpsc_roots.cu", "tpsc_engine.cpp",
            "tpsc_batch.cpp", "tpsc_tangent.cu", "tpsc_noalloc.cu", "tpsc_files.cpp",
-           "tpsc_lattice.cu", "tpsc_peaks.cu", "tpsc_adjoint.cu"]
-HEADERS = ["tpsc_fft.cuh", "tpsc_kernels.cuh", "tpsc_device.cuh", "tpsc_host.h"]
+           "tpsc_lattice.cu", "tpsc_peaks.cu", "tpsc_adjoint.cu", "tpsc_direct.cu", "tpsc_tcdct.cu"]
+HEADERS = ["tpsc_fft.cuh", "tpsc_kernels.cuh", "tpsc_device.cuh", "tpsc_dct.cuh", "tpsc_tc.cuh", "tpsc_host.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -612,6 +612,11 @@ int build_grid(tpsc_ctx *ctx, int nk0, int nw0, Grid **out) {
     A(upload(g, &d.w16, w16));
     A(upload(g, &d.tw_k, twk));
     A(upload(g, &d.tw_k32, twk32));
+    std::vector<float> dct;
+    dct_table(d.nbk, dct);
+    if (!dct.empty()) A(upload(g, &d.dct32, dct));
+    dct_tc_table(d.nbk, dct);
+    if (!dct.empty()) A(upload(g, &d.dct_tc, dct));
     A(upload(g, &d.tw_w, tww));
     A(upload(g, &d.ht_w, htw));
     A(upload(g, &d.spl_half, sh));
@@ -2739,6 +2744,78 @@ int tpsc_set_tau_tile(int kind, int nw0, int tile) {
         return fail(nullptr, TPSC_ERR_ARG, "need kind 0..2, tile 0..2 (2: Nw0 <= 2048) and a supported Nw0");
     set_tau_tile(kind, nw0, tile);
     return TPSC_OK;
+}
+
+int tpsc_set_slice_plan(int kind, int nk0, int plan) {
+    const int nbk = nk0 / 2 + 1;
+    if (kind < 0 || kind > 3 || plan < 0 || plan > 2 || !supported_grid(nk0, 16) ||
+        !slice_plan_supported(kind, plan, nbk))
+        return fail(nullptr, TPSC_ERR_ARG,
+                    "need kind 0..3, plan 0, 1 (nk0 64, 128, 256) or 2 (kind 3, nk0 256) and a supported nk0");
+    set_slice_plan(kind, nbk, plan);
+    return TPSC_OK;
+}
+
+// Times every supported plan of the four FP32 slice transforms on the
+// current grid (after a mixed-form solve) and keeps the fastest per kind.
+int tpsc_tune_slice_plans(tpsc_ctx *ctx, int reps, double ms[12]) {
+    int rc = need_model(ctx);
+    if (rc) return rc;
+    Grid *g = ctx->cur;
+    if (!g || !g->have_S || !g->g_mixed || !g->Grt32)
+        return fail(ctx, TPSC_ERR_STATE, "tune after a mixed-form solve on the current grid");
+    if (reps < 1 || reps > 100) return fail(ctx, TPSC_ERR_ARG, "need 1 <= reps <= 100");
+    cudaSetDevice(ctx->device);
+    const GridDev &d = g->d;
+    cudaEvent_t a = ctx->ev[0], b = ctx->ev[1];
+    for (int kind = 0; kind < 4; ++kind) {
+        double best = 0.0;
+        int pick = -1;
+        for (int plan = 0; plan < 3; ++plan) {
+            if (ms) ms[3 * kind + plan] = 0.0;
+            if (!slice_plan_supported(kind, plan, d.nbk)) continue;
+            set_slice_plan(kind, d.nbk, plan);
+            auto run = [&]() -> cudaError_t {
+                if (kind == kSliceG) return launch_gslice32(d, g->Grt32, g->mu0, ctx->T, ctx->st);
+                if (kind == kSliceChi0) return launch_chi0_slice32(d, g->Grt32, g->chirt, g->chiq, ctx->st);
+                if (kind == kSliceVertex)
+                    return launch_vertex_q32(d, g->chiq, g->V, ctx->U, ctx->dres, ctx->T, ctx->st);
+                return launch_sigma_slice32(d, g->Grt32, g->V, g->sigt, ctx->st);
+            };
+            CK(run());
+            CK(cudaEventRecord(a, ctx->st));
+            for (int r = 0; r < reps; ++r) CK(run());
+            CK(cudaEventRecord(b, ctx->st));
+            CK(cudaEventSynchronize(b));
+            float t = 0;
+            CK(cudaEventElapsedTime(&t, a, b));
+            const double mean = t / reps;
+            if (ms) ms[3 * kind + plan] = mean;
+            if (pick < 0 || mean < best) {
+                best = mean;
+                pick = plan;
+            }
+        }
+        set_slice_plan(kind, d.nbk, pick);
+    }
+    unsigned word = 0;
+    if (tensor_plan_errors(&word, false) == 0 && word)
+        return fail(ctx, TPSC_ERR_CUDA, "a tensor-plan kernel gave up waiting on the tensor cores");
+    // the transforms overwrote the grid's stages: the next solve recomputes them
+    g->have_chi0 = g->have_V = g->have_S = g->have_mom = g->have_U = false;
+    return TPSC_OK;
+}
+
+int tpsc_tensor_plan_errors(unsigned *word, int clear) {
+    if (!word) return fail(nullptr, TPSC_ERR_ARG, "null output");
+    if (tensor_plan_errors(word, clear != 0)) return fail(nullptr, TPSC_ERR_CUDA, "reading the error word failed");
+    return TPSC_OK;
+}
+
+int tpsc_get_slice_plan(int kind, int nk0) {
+    if (kind < 0 || kind > 3 || !supported_grid(nk0, 16))
+        return -fail(nullptr, TPSC_ERR_ARG, "need kind 0..3 and a supported nk0");
+    return slice_plan(kind, nk0 / 2 + 1);
 }
 
 // green0::find_mu_inf_syst (src/green0.cpp:265-287): mu0 of the infinite

@@ -46,6 +46,7 @@ void set_tau_tile(int kind, int n, int tile) {
     if (g_tau_tile[kind][tile_index(n)].exchange(tile) != tile) g_tau_tiles_version.fetch_add(1);
 }
 long long tau_tiles_version() { return g_tau_tiles_version.load(); }
+void bump_plans_version() { g_tau_tiles_version.fetch_add(1); }
 // the same count for the calling host thread (kernels in one stream capture)
 static thread_local long long t_launches = 0;
 cudaError_t launched(int n) {

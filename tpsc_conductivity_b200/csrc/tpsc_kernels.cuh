@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 namespace tpsc {
 
 // Device tables of one lattice / frequency grid.
@@ -22,6 +24,8 @@ struct GridDev {
     double *tailP = nullptr;       // [kTailP] P_p = sum over the fermionic tail n = Nw0/2..Nw0 of w_n^-p
     double2 *tw_k = nullptr;       // [L]   exp(-2 pi i m / L)
     float4 *tw_k32 = nullptr;      // [L]   the same as (cos, sin) rounded to float, then the float remainders
+    float *dct32 = nullptr;        // [(nk0 + 1)(nk0/4 + 4)] folded DCT-I tables of the direct slice plan (nk0 >= 64)
+    float *dct_tc = nullptr;       // A-operand tables of the tensor slice plan (nk0 = 256)
     double2 *tw_w = nullptr;       // [Nw0] exp(-2 pi i m / Nw0)
     double2 *ht_w = nullptr;       // [Nw0] exp(+i pi m / Nw0)
     double *spl_half = nullptr;    // [2 nb]       spline LU tables, nb nodes
@@ -422,6 +426,33 @@ constexpr int kTauChi0 = 0, kTauVertex = 1, kTauSigma = 2;
 int tau_tile(int kind, int n);
 void set_tau_tile(int kind, int n, int tile);
 long long tau_tiles_version();
+// adds one to the version above (a plan changed: captured graphs are stale)
+void bump_plans_version();
+
+// plan of the mixed form's FP32 slice transforms per kind and lattice,
+// process-wide: kSliceFft the packed radix-16 FFTs (tpsc_fft.cuh),
+// kSliceDirect the folded matrix DCT-I (tpsc_dct.cuh; nbk 33, 65, 129)
+constexpr int kSliceG = 0, kSliceChi0 = 1, kSliceVertex = 2, kSliceSigma = 3;
+constexpr int kSliceFft = 0, kSliceDirect = 1, kSliceTensor = 2;
+int slice_plan(int kind, int nbk);
+void set_slice_plan(int kind, int nbk, int plan);
+bool slice_plan_supported(int kind, int plan, int nbk);
+// the table of the direct plan for a quadrant side nbk (empty where it does not apply)
+void dct_table(int nbk, std::vector<float> &out);
+// the tensor plan (tpsc_tcdct.cu): Sigma slices of the 256 x 256 lattice
+void dct_tc_table(int nbk, std::vector<float> &out);
+cudaError_t launch_sigma_slice_tc(const GridDev &g, const float *Grt, const double *V, double *sigt,
+                                  cudaStream_t st, const Bp &b = Bp{});
+// the tensor plan's error word (nonzero after a bounded wait ran out); 0 on success
+int tensor_plan_errors(unsigned *out, bool clear);
+cudaError_t launch_sigma_slice_dct(const GridDev &g, const float *Grt, const double *V, double *sigt,
+                                   cudaStream_t st, const Bp &b = Bp{});
+cudaError_t launch_gslice_dct(const GridDev &g, float *Grt, double mu0, double T, cudaStream_t st,
+                              const Bp &b = Bp{});
+cudaError_t launch_chi0_slice_dct(const GridDev &g, const float *Grt, double *chirt, double *chiq, cudaStream_t st,
+                                  const Bp &b = Bp{});
+cudaError_t launch_vertex_q_dct(const GridDev &g, const double *chiq, double *Vr, double U, const double *Usc,
+                                double T, cudaStream_t st, const Bp &b = Bp{});
 
 // kernels launched by the library so far
 long long launches_total();

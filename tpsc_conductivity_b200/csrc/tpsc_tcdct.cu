@@ -1,0 +1,471 @@
+// tpsc_tcdct.cu -- the "tensor" slice plan: the folded matrix DCT-I of the
+// mixed form's Sigma slice (tpsc_dct.cuh) with both matrix products on the
+// tcgen05 tensor cores, 3xTF32 (each FP32 operand split into a TF32 high part
+// and its remainder; hi*hi + hi*lo + lo*hi accumulated in FP32 in tensor
+// memory).  Lattice 256 x 256 (nbk = 129, H = 64).
+//
+// One slice at a time per CTA (persistent, one CTA per SM, 384 threads):
+//   1. stage the V(r, tau_j) block row and the FP32 G(r, tau_j) row (async copies);
+//   2. x = G V in FP64: the near field |rx|, |ry| <= 4 kept in FP64, the rest rounded to FP32;
+//   3. fold x into SS, SD, DD (tpsc_dct.cuh) as K-major hi/lo TF32 operands;
+//   4. T = K . fold^T on the tensor cores (M = 64 output rows of the DCT
+//      tables Ks, Kd; N = the fold's rows; K = its columns);
+//   5. T from tensor memory into the second products' operands (hi/lo);
+//   6. Z = K . T^T on the tensor cores; Z from tensor memory into shared memory;
+//   7. Sigma(k, tau_j) = Z + the near field's FP64 transform, to HBM.
+// Row and column H = 64 of the blocks, which the M = 64 products leave out,
+// are alternating sums (Ks[H][k] = w_k (-1)^k) formed on the CUDA cores while
+// the tensor cores run.  Every mbarrier wait is bounded: a wait that runs
+// out sets the error word, the CTA waits (bounded) once more, frees its
+// tensor memory and returns.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <cstring>
+#include <vector>
+
+#include "tpsc_dct.cuh"
+#include "tpsc_tc.cuh"
+
+namespace tpsc {
+
+// the A-operand tables of the tensor plan for H = 64 (host side): Ks rows
+// n < 64 (K = 72, k > 64 zero) and Kd (64 x 64) as K-major TF32 hi / lo
+// pairs, then Ks[64][k] = w_k (-1)^k (72 floats); 69,920 bytes
+void dct_tc_table(int nbk, std::vector<float> &out) {
+    out.clear();
+    if (nbk != 129) return;
+    constexpr int H = 64, N = 128, KS = 72;
+    const long double pi = 3.141592653589793238462643383279502884L;
+    out.assign((2 * 64 * KS + 2 * 64 * 64 + KS), 0.0f);
+    auto rna = [](float x) {
+        uint32_t b;
+        memcpy(&b, &x, 4);
+        b = (b + 0x1000u) & ~0x1FFFu;
+        float y;
+        memcpy(&y, &b, 4);
+        return y;
+    };
+    auto put = [&](size_t base_hi, size_t base_lo, int r, int k, int R, long double v) {
+        const float hi = rna((float)v);
+        const float lo = (float)(v - (long double)hi);
+        out[base_hi + kmaj_off(r, k, R) / 4] = hi;
+        out[base_lo + kmaj_off(r, k, R) / 4] = lo;
+    };
+    const size_t ks_hi = 0, ks_lo = 64 * KS, kd_hi = 2 * 64 * KS, kd_lo = kd_hi + 64 * 64, k64 = kd_lo + 64 * 64;
+    for (int n = 0; n < 64; ++n)
+        for (int k = 0; k <= H; ++k)
+            put(ks_hi, ks_lo, n, k, 64, (k == 0 ? 1.0L : 2.0L) * cosl(pi * ((k * n) % (2 * H)) / H));
+    for (int n = 0; n < 64; ++n)
+        for (int k = 0; k < H; ++k)
+            put(kd_hi, kd_lo, n, k, 64, (k == 0 ? 1.0L : 2.0L) * cosl(pi * ((k * (2 * n + 1)) % (2 * N)) / N));
+    for (int k = 0; k <= H; ++k) out[k64 + k] = (k == 0 ? 1.0f : 2.0f) * ((k & 1) ? -1.0f : 1.0f);
+}
+
+namespace {
+
+__device__ unsigned g_tc_err;  // set by a wait that ran out (never cleared by the kernel)
+
+template <class T>
+__device__ __forceinline__ T *tc_point(T *ptr, long long arena, int p) {
+    using Ch = typename std::conditional<std::is_const<T>::value, const char, char>::type;
+    return reinterpret_cast<T *>(reinterpret_cast<Ch *>(ptr) + (long long)p * arena);
+}
+
+// shared memory of k_sigma_slice_tc (bytes)
+struct TcSmem {
+    static constexpr int N8 = 8385, N8P = 8388, NBK = 129, KS = 72;
+    // A tables: Ks hi | Ks lo (64 x 72) | Kd hi | Kd lo (64 x 64) | Ks row 64
+    static constexpr uint32_t ks_hi = 0, ks_lo = 64 * KS * 4, kd_hi = 2 * 64 * KS * 4, kd_lo = kd_hi + 64 * 64 * 4;
+    static constexpr uint32_t k64 = kd_lo + 64 * 64 * 4;  // 72 floats
+    static constexpr uint32_t tab_bytes = k64 + KS * 4;   // 69,920
+    // B operands: ee (72 x 72), eo (72 x 64 first products, 64 x 72 second), oo (64 x 64), hi | lo each
+    static constexpr uint32_t b0 = tab_bytes;
+    static constexpr uint32_t ee_hi = b0, ee_lo = ee_hi + 72 * 72 * 4;
+    static constexpr uint32_t eo_hi = ee_lo + 72 * 72 * 4, eo_lo = eo_hi + 72 * 64 * 4;
+    static constexpr uint32_t oo_hi = eo_lo + 72 * 64 * 4, oo_lo = oo_hi + 64 * 64 * 4;
+    static constexpr uint32_t b_end = oo_lo + 64 * 64 * 4;  // b0 + 111,104
+    static constexpr uint32_t xs = b_end;                    // N8 floats
+    static constexpr uint32_t xn = xs + ((N8 * 4 + 15) & ~15);
+    static constexpr uint32_t u = xn + 16 * 8;
+    static constexpr int R = 4, NOCT = 15;
+    static constexpr uint32_t zx = u + (R + 1) * NBK * 8;  // 129 floats: rows 64 of Z_ee, Z_eo
+    static constexpr uint32_t t64 = zx + 132 * 4;          // 72 floats: column 64 of T_ee
+    static constexpr uint32_t bar = t64 + 72 * 4;           // mbarrier (8-byte aligned)
+    static constexpr uint32_t misc = bar + 8;               // tensor-memory base, error flag
+    static constexpr uint32_t cf = misc + 16;               // 2 cos(pi a l / N), a = 1..R, l < NBK (doubles)
+    static constexpr uint32_t bytes = cf + R * NBK * 8;
+    static_assert(bar % 8 == 0, "mbarrier alignment");
+    static_assert(N8P * 8 + N8 * 4 <= b_end - b0, "raw inputs fit over the B operands");
+    static_assert(DctPlan<64>::REG * 4 <= b_end - b0, "Z fits over the B operands");
+};
+
+constexpr int kTcThreads = 384;
+constexpr uint32_t kTmemCols = 256;
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s: the products of one slice take microseconds
+
+// The butterfly at position (r, k) of the three blocks at once, from the
+// octant values xs: with A = X(r, k), B = X(N-r, k), C = X(r, N-k),
+// D = X(N-r, N-k),
+//   SS = A + B + C + D,  SD = (A - C) + (B - D),  DD = (A - C) - (B - D),
+// row or column H taking its point once (s_H = x_H, no d_H); positions
+// beyond the blocks are the operands' zero padding.
+__device__ __forceinline__ void fold_at(const float *__restrict__ xs, int r, int k, float &ss, float &sd, float &dd) {
+    constexpr int H = 64, N = 128;
+    auto X = [&](int p, int q) -> float {
+        const int l = p > q ? p : q, m = p > q ? q : p;
+        return xs[l * (l + 1) / 2 + m];
+    };
+    ss = sd = dd = 0.0f;
+    if (r > H || k > H) return;
+    const float a = X(r, k);
+    if (r < H && k < H) {
+        const float bq = X(N - r, k), c = X(r, N - k), d = X(N - r, N - k);
+        ss = (a + bq) + (c + d);
+        sd = (a - c) + (bq - d);
+        dd = (a - c) - (bq - d);
+    } else if (r < H) {  // k = H
+        ss = a + X(N - r, k);
+    } else if (k < H) {  // r = H
+        const float c = X(r, N - k);
+        ss = a + c;
+        sd = a - c;
+    } else {
+        ss = a;
+    }
+}
+
+// The MMAs of one block: D (tensor-memory column COL) = A B^T over KSTEPS
+// steps of K = 8, 3xTF32 (the two cross terms first, then hi * hi); A is a
+// table of 64 rows, B has BROWS rows (= N).  Fully unrolled: every
+// descriptor is the base descriptor plus a constant start-address offset.
+template <uint32_t A_HI, uint32_t A_LO, uint32_t B_HI, uint32_t B_LO, int BROWS, int KSTEPS, int COL>
+__device__ __forceinline__ void issue_block(uint64_t dbase_a, uint64_t dbase_b, uint32_t tmem) {
+    constexpr uint32_t a_lbo = 64 * 16, b_lbo = BROWS * 16;
+    constexpr uint32_t id = idesc_tf32(64, BROWS);
+    const uint64_t a0 = dbase_a | ((uint64_t)(a_lbo >> 4) << 16), b0 = dbase_b | ((uint64_t)(b_lbo >> 4) << 16);
+#pragma unroll
+    for (int pass = 0; pass < 3; ++pass) {
+        const uint32_t a = pass == 1 ? A_LO : A_HI;
+        const uint32_t bb = pass == 0 ? B_LO : B_HI;
+#pragma unroll
+        for (int s = 0; s < KSTEPS; ++s)
+            mma_tf32(tmem + COL, a0 + ((a + 2 * a_lbo * s) >> 4), b0 + ((bb + 2 * b_lbo * s) >> 4), id,
+                     (pass | s) != 0);
+    }
+}
+
+// the first products (T = K . fold^T) or the second (Z = K . T^T); sdesc: the
+// descriptor of shared-memory offset 0 (start address field only, SBO 128)
+template <bool SECOND>
+__device__ __forceinline__ void issue_stage(uint64_t sdesc, uint32_t tmem) {
+    using S = TcSmem;
+    issue_block<S::ks_hi, S::ks_lo, S::ee_hi, S::ee_lo, 72, 9, 0>(sdesc, sdesc, tmem);
+    if constexpr (SECOND) {
+        issue_block<S::ks_hi, S::ks_lo, S::eo_hi, S::eo_lo, 64, 9, 72>(sdesc, sdesc, tmem);
+        issue_block<S::kd_hi, S::kd_lo, S::oo_hi, S::oo_lo, 64, 8, 136>(sdesc, sdesc, tmem);
+    } else {
+        issue_block<S::kd_hi, S::kd_lo, S::eo_hi, S::eo_lo, 72, 8, 72>(sdesc, sdesc, tmem);
+        issue_block<S::kd_hi, S::kd_lo, S::oo_hi, S::oo_lo, 64, 8, 144>(sdesc, sdesc, tmem);
+    }
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_sigma_slice_tc(const float *__restrict__ Grt, const double *__restrict__ V, const float *__restrict__ tab,
+                     const double2 *__restrict__ tw64, int nw0, double *__restrict__ sigt, Bp b) {
+    using S = TcSmem;
+    constexpr int H = 64, N8 = S::N8, NBK = S::NBK, L = 256, R = S::R, NOCT = S::NOCT;
+    constexpr int PER = (N8 + kTcThreads - 1) / kTcThreads;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const uint32_t sbase = smem_u32(smem);
+    const uint64_t sdesc0 = smem_desc(sbase, 0, 128);
+    float *xs = reinterpret_cast<float *>(smem + S::xs);
+    double *xn = reinterpret_cast<double *>(smem + S::xn);
+    double *u = reinterpret_cast<double *>(smem + S::u);
+    float *zx = reinterpret_cast<float *>(smem + S::zx);
+    float *t64 = reinterpret_cast<float *>(smem + S::t64);
+    const float *k64 = reinterpret_cast<const float *>(smem + S::k64);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::bar);
+    uint32_t *s_tmem = reinterpret_cast<uint32_t *>(smem + S::misc);
+    volatile uint32_t *s_err = reinterpret_cast<volatile uint32_t *>(smem + S::misc + 4);
+    float *Z = reinterpret_cast<float *>(smem + S::b0);  // the transformed slice, DctPlan<64> layout
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    if (warp == 0) {
+        tmem_alloc(s_tmem, kTmemCols);
+        tmem_relinquish();
+    }
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        *s_err = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = tid; i < (int)(S::tab_bytes / 16); i += blockDim.x)
+        cp_async16(smem + 16 * i, reinterpret_cast<const unsigned char *>(tab) + 16 * i);
+    double *cf = reinterpret_cast<double *>(smem + S::cf);
+    for (int i = tid; i < R * NBK; i += blockDim.x) cf[i] = 2.0 * __ldg(&tw64[((i / NBK + 1) * (i % NBK)) % L]).x;
+    cp_async_wait_all();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *s_tmem;
+    uint32_t phase = 0;
+
+    const int nb = nw0 / 2 + 1;
+    const long long items = (long long)(nw0 + 1) * b.P;
+    for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+        const int p = (int)(it / (nw0 + 1)), j = (int)(it % (nw0 + 1));
+        const int jv = j < nb ? j : nw0 - j;
+        const float *G = tc_point(Grt, b.arena, p);
+        const double *Vp = tc_point(V, b.arena, p);
+        double *out = tc_point(sigt, b.arena, p);
+        const long long nx = it + gridDim.x;
+        if (nx < items) {
+            const int pn = (int)(nx / (nw0 + 1)), jn = (int)(nx % (nw0 + 1));
+            prefetch_l2_blockrow(tc_point(V, b.arena, pn), jn < nb ? jn : nw0 - jn, nb, S::N8P / 4);
+            prefetch_l2_range(tc_point(Grt, b.arena, pn) + (size_t)jn * N8, (size_t)N8 * sizeof(float));
+        }
+        __syncthreads();  // the previous slice's reads of Z are done
+        // 1. raw inputs over the B operands
+        double *vs = reinterpret_cast<double *>(smem + S::b0);
+        float *gs = reinterpret_cast<float *>(smem + S::b0 + S::N8P * 8);
+        stage_blockrow<NBK>(vs, Vp, jv, nb);
+        for (int o = tid; o < N8; o += blockDim.x) cp_async4(gs + o, G + (size_t)j * N8 + o);
+        cp_async_wait_all();
+        __syncthreads();
+        // 2. x = G V
+        float r1[PER];
+#pragma unroll
+        for (int i = 0; i < PER; ++i) {
+            const int o = tid + i * kTcThreads;
+            r1[i] = 0.0f;
+            if (o < N8) {
+                const double x = (double)gs[o] * vs[o];
+                if (o < NOCT)
+                    xn[o] = x;
+                else
+                    r1[i] = (float)x;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < PER; ++i) {
+            const int o = tid + i * kTcThreads;
+            if (o < N8) xs[o] = r1[i];
+        }
+        __syncthreads();
+        // 3. the fold as K-major hi/lo operands, 8 rows x 4 columns per warp pass
+        for (int un = warp; un < 9 * 18; un += kTcThreads / 32) {
+            const int r = 8 * (un / 18) + (lane >> 2), k = 4 * (un % 18) + (lane & 3);
+            float v[3];
+            fold_at(xs, r, k, v[0], v[1], v[2]);
+            const uint32_t off72 = kmaj_off(r, k, 72);
+            float h = tf32_hi(v[0]);
+            *reinterpret_cast<float *>(smem + S::ee_hi + off72) = h;
+            *reinterpret_cast<float *>(smem + S::ee_lo + off72) = v[0] - h;
+            if (k < 64) {
+                h = tf32_hi(v[1]);
+                *reinterpret_cast<float *>(smem + S::eo_hi + off72) = h;
+                *reinterpret_cast<float *>(smem + S::eo_lo + off72) = v[1] - h;
+                if (r < 64) {
+                    const uint32_t off64 = kmaj_off(r, k, 64);
+                    h = tf32_hi(v[2]);
+                    *reinterpret_cast<float *>(smem + S::oo_hi + off64) = h;
+                    *reinterpret_cast<float *>(smem + S::oo_lo + off64) = v[2] - h;
+                }
+            }
+        }
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        // 4. first products
+        if (tid == 0) {
+            tc_fence_after();
+            issue_stage<false>(sdesc0, tmem);
+            mma_commit(bar);
+        }
+        // (while the tensor cores run) near field: u_a(k2) = sum_c w_c x(a, c) cos(pi c k2 / N)
+        for (int i = tid; i < (R + 1) * NBK; i += blockDim.x) {
+            const int a = i / NBK, k2 = i % NBK;
+            double acc = 0.0;
+#pragma unroll
+            for (int c = 0; c <= R; ++c) {
+                const int hi = a > c ? a : c, lo = a > c ? c : a;
+                acc = fma((c == 0 ? 1.0 : 2.0) * xn[lo + hi * (hi + 1) / 2], __ldg(&tw64[(c * k2) % L]).x, acc);
+            }
+            u[i] = acc;
+        }
+        // column 64 of T_ee: t64[m] = sum_{k<=64} SS[m][k] Ks[64][k], m <= 64 (warps 4..6)
+        if (tid >= 128 && tid < 128 + H + 1) {
+            const int m = tid - 128;
+            float acc = 0.0f;
+            for (int k = 0; k <= H; ++k) {
+                const uint32_t off = kmaj_off(m, k, 72);
+                const float sv = *reinterpret_cast<const float *>(smem + S::ee_hi + off) +
+                                 *reinterpret_cast<const float *>(smem + S::ee_lo + off);
+                acc = fmaf(sv, k64[k], acc);
+            }
+            t64[m] = acc;
+        }
+        if (!mbar_wait(bar, phase, kWaitNs)) *s_err = 1;
+        tc_fence_after();
+        __syncthreads();
+        if (*s_err) break;
+        phase ^= 1;
+        // 5. T from tensor memory into the second products' B operands:
+        // B2_ee[n][k] = T_ee[k][n] (n < 64 from the accumulator, row 64 = t64),
+        // B2_eo[n][k] = T_eo[k][n], B2_oo[n][k] = T_oo[k][n]
+        {
+            const int q = warp & 3, blk = warp >> 2;
+            const int n = 16 * q + (lane & 15);
+            const int col0 = blk == 0 ? 0 : (blk == 1 ? 72 : 144);
+            const int ncol = blk == 2 ? 64 : 72;
+            const uint32_t hi_off = blk == 0 ? S::ee_hi : (blk == 1 ? S::eo_hi : S::oo_hi);
+            const uint32_t lo_off = blk == 0 ? S::ee_lo : (blk == 1 ? S::eo_lo : S::oo_lo);
+            const int R2 = blk == 0 ? 72 : 64;
+            uint32_t rr[72];
+            tmem_ld_row72(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)col0, rr, ncol == 72);
+            if (lane < 16) {
+#pragma unroll
+                for (int c = 0; c < 72; c += 4) {
+                    if (c < ncol) {
+                        float4 hv, lv;
+                        float *hp = &hv.x, *lp = &lv.x;
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) {
+                            const float v = __uint_as_float(rr[c + e]);
+                            hp[e] = tf32_hi(v);
+                            lp[e] = v - hp[e];
+                        }
+                        const uint32_t off = kmaj_off(n, c, R2);
+                        *reinterpret_cast<float4 *>(smem + hi_off + off) = hv;
+                        *reinterpret_cast<float4 *>(smem + lo_off + off) = lv;
+                    }
+                }
+            }
+        }
+        // rows 64..71 of B2_ee: row 64 = t64 (k <= 64), the rest zero
+        for (int i = tid; i < 8 * 72; i += blockDim.x) {
+            const int n = 64 + i / 72, k = i % 72;
+            const float v = (n == 64 && k <= H) ? t64[k] : 0.0f;
+            const float h = tf32_hi(v);
+            const uint32_t off = kmaj_off(n, k, 72);
+            *reinterpret_cast<float *>(smem + S::ee_hi + off) = h;
+            *reinterpret_cast<float *>(smem + S::ee_lo + off) = v - h;
+        }
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        // 6. second products
+        if (tid == 0) {
+            tc_fence_after();
+            issue_stage<true>(sdesc0, tmem);
+            mma_commit(bar);
+        }
+        // rows 64 of Z_ee (n <= 64) and Z_eo (n < 64): sum_{k<=64} Ks[64][k] T[k][n]
+        if (tid >= 128 && tid < 128 + 2 * H + 1) {
+            const int i = tid - 128;
+            const bool ee = i <= H;
+            const int n = ee ? i : i - H - 1;
+            const uint32_t hi_off = ee ? S::ee_hi : S::eo_hi, lo_off = ee ? S::ee_lo : S::eo_lo;
+            const int R2 = ee ? 72 : 64;
+            float acc = 0.0f;
+            for (int k = 0; k <= H; ++k) {
+                const uint32_t off = kmaj_off(n, k, R2);
+                const float tv = *reinterpret_cast<const float *>(smem + hi_off + off) +
+                                 *reinterpret_cast<const float *>(smem + lo_off + off);
+                acc = fmaf(k64[k], tv, acc);
+            }
+            zx[i] = acc;
+        }
+        if (!mbar_wait(bar, phase, kWaitNs)) *s_err = 1;
+        tc_fence_after();
+        __syncthreads();
+        if (*s_err) break;
+        phase ^= 1;
+        // Z from tensor memory (rows m < 64) over the B operands, rows 64 from zx
+        {
+            using P = DctPlan<64>;
+            const int q = warp & 3, blk = warp >> 2;
+            const int m = 16 * q + (lane & 15);
+            const int col0 = blk == 0 ? 0 : (blk == 1 ? 72 : 136);
+            const int zoff = blk == 0 ? P::EE : (blk == 1 ? P::EO : P::OO);
+            uint32_t rr[72];
+            tmem_ld_row72(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)col0, rr, blk == 0);
+            if (lane < 16) {
+                float *zr = Z + zoff + m * P::LD;
+#pragma unroll
+                for (int c = 0; c < 68; c += 4)
+                    if (blk == 0 || c < 64)
+                        *reinterpret_cast<float4 *>(zr + c) = make_float4(
+                            __uint_as_float(rr[c]), __uint_as_float(rr[c + 1]), __uint_as_float(rr[c + 2]),
+                            __uint_as_float(rr[c + 3]));
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+        for (int i = tid; i < 2 * H + 1; i += blockDim.x) {
+            using P = DctPlan<64>;
+            if (i <= H)
+                Z[P::EE + H * P::LD + i] = zx[i];
+            else
+                Z[P::EO + H * P::LD + (i - H - 1)] = zx[i];
+        }
+        __syncthreads();
+        // 7. output
+        for (int o = tid; o < N8; o += blockDim.x) {
+            int l, m;
+            oct_lm(o, l, m);
+            double nf = u[m];
+#pragma unroll
+            for (int a = 1; a <= R; ++a) nf = fma(cf[(a - 1) * NBK + l], u[a * NBK + m], nf);
+            out[bidx(j, o, nw0 + 1)] = (double)dct_z<64>(Z, l, m) + nf;
+        }
+    }
+    if (*s_err) {
+        // let the MMAs in flight (the phase whose wait ran out) finish, bounded,
+        // before the tensor memory is freed
+        if (tid == 0) {
+            atomicOr(&g_tc_err, 1u);
+            mbar_wait(bar, phase, kWaitNs);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kTmemCols);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_sigma_slice_tc(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st,
+                                  const Bp &b) {
+    if (g.nbk != 129 || !g.dct_tc) return cudaErrorInvalidValue;
+    const size_t sm = TcSmem::bytes;
+    cudaError_t e = set_smem(k_sigma_slice_tc, sm);
+    if (e != cudaSuccess) return e;
+    const int ctas = resident_ctas(k_sigma_slice_tc, kTcThreads, sm);
+    if (ctas <= 0) return cudaErrorInvalidConfiguration;
+    const long long items = (long long)(g.nw0 + 1) * b.P;
+    const int grid = (int)(items < ctas ? items : ctas);
+    k_sigma_slice_tc<<<grid, kTcThreads, sm, st>>>(Grt, V, g.dct_tc, g.tw_k, g.nw0, sigt, b);
+    return launched();
+}
+
+// the error word of the tensor plan's kernels: nonzero once an mbarrier wait
+// ran out (the context stays usable; the affected outputs are not valid)
+int tensor_plan_errors(unsigned *out, bool clear) {
+    unsigned v = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, g_tc_err, sizeof(v));
+    if (e != cudaSuccess) return -1;
+    if (clear && v) {
+        const unsigned z = 0;
+        if (cudaMemcpyToSymbol(g_tc_err, &z, sizeof(z)) != cudaSuccess) return -1;
+    }
+    *out = v;
+    return 0;
+}
+
+}  // namespace tpsc
