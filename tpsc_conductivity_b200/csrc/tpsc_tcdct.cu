@@ -11,7 +11,8 @@
 //   4. T = K . fold^T on the tensor cores (M = 64 output rows of the DCT
 //      tables Ks, Kd; N = the fold's rows; K = its columns);
 //   5. T from tensor memory into the second products' operands (hi/lo);
-//   6. Z = K . T^T on the tensor cores; Z from tensor memory into shared memory;
+//   6. Z = K . T^T on the tensor cores; Z from tensor memory into shared memory
+//      in octant order; the next slice's inputs are staged from here on;
 //   7. Sigma(k, tau_j) = Z + the near field's FP64 transform, to HBM.
 // Row and column H = 64 of the blocks, which the M = 64 products leave out,
 // are alternating sums (Ks[H][k] = w_k (-1)^k) formed on the CUDA cores while
@@ -171,6 +172,21 @@ __device__ __forceinline__ void issue_stage(uint64_t sdesc, uint32_t tmem) {
     }
 }
 
+// stage the raw inputs of slice j of point p (the V block row, the FP32 G
+// row) over the B operands with asynchronous copies (waited for by the caller)
+__device__ __forceinline__ void tc_stage(unsigned char *smem, const float *__restrict__ Grt,
+                                         const double *__restrict__ V, int nw0, int p, int j, long long arena) {
+    using S = TcSmem;
+    const int nb = nw0 / 2 + 1;
+    const int jv = j < nb ? j : nw0 - j;
+    const float *G = tc_point(Grt, arena, p) + (size_t)j * S::N8;
+    stage_blockrow<S::NBK>(reinterpret_cast<double *>(smem + S::b0), tc_point(V, arena, p), jv, nb);
+    float *gs = reinterpret_cast<float *>(smem + S::b0 + S::N8P * 8);
+    for (int o = threadIdx.x; o < S::N8; o += blockDim.x) cp_async4(gs + o, G + o);
+}
+
+__device__ __forceinline__ int oct_of(int l, int m) { return l * (l + 1) / 2 + m; }
+
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_sigma_slice_tc(const float *__restrict__ Grt, const double *__restrict__ V, const float *__restrict__ tab,
                      const double2 *__restrict__ tw64, int nw0, double *__restrict__ sigt, Bp b) {
@@ -180,7 +196,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     extern __shared__ __align__(1024) unsigned char smem[];
     const uint32_t sbase = smem_u32(smem);
     const uint64_t sdesc0 = smem_desc(sbase, 0, 128);
-    float *xs = reinterpret_cast<float *>(smem + S::xs);
+    float *xs = reinterpret_cast<float *>(smem + S::xs);  // the slice's octant values, later its transform
     double *xn = reinterpret_cast<double *>(smem + S::xn);
     double *u = reinterpret_cast<double *>(smem + S::u);
     float *zx = reinterpret_cast<float *>(smem + S::zx);
@@ -189,7 +205,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::bar);
     uint32_t *s_tmem = reinterpret_cast<uint32_t *>(smem + S::misc);
     volatile uint32_t *s_err = reinterpret_cast<volatile uint32_t *>(smem + S::misc + 4);
-    float *Z = reinterpret_cast<float *>(smem + S::b0);  // the transformed slice, DctPlan<64> layout
+    double *cf = reinterpret_cast<double *>(smem + S::cf);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
     if (warp == 0) {
@@ -203,55 +219,43 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     for (int i = tid; i < (int)(S::tab_bytes / 16); i += blockDim.x)
         cp_async16(smem + 16 * i, reinterpret_cast<const unsigned char *>(tab) + 16 * i);
-    double *cf = reinterpret_cast<double *>(smem + S::cf);
     for (int i = tid; i < R * NBK; i += blockDim.x) cf[i] = 2.0 * __ldg(&tw64[((i / NBK + 1) * (i % NBK)) % L]).x;
-    cp_async_wait_all();
+    const int nb = nw0 / 2 + 1;
+    const long long items = (long long)(nw0 + 1) * b.P;
+    if (blockIdx.x < items)
+        tc_stage(smem, Grt, V, nw0, (int)(blockIdx.x / (nw0 + 1)), (int)(blockIdx.x % (nw0 + 1)), b.arena);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *s_tmem;
     uint32_t phase = 0;
 
-    const int nb = nw0 / 2 + 1;
-    const long long items = (long long)(nw0 + 1) * b.P;
     for (long long it = blockIdx.x; it < items; it += gridDim.x) {
         const int p = (int)(it / (nw0 + 1)), j = (int)(it % (nw0 + 1));
-        const int jv = j < nb ? j : nw0 - j;
-        const float *G = tc_point(Grt, b.arena, p);
-        const double *Vp = tc_point(V, b.arena, p);
         double *out = tc_point(sigt, b.arena, p);
         const long long nx = it + gridDim.x;
+        __syncthreads();  // the previous slice's reads of xs are done
+        // 1. this slice's raw inputs (staged during the previous slice's output)
+        cp_async_wait_all();
+        __syncthreads();
         if (nx < items) {
             const int pn = (int)(nx / (nw0 + 1)), jn = (int)(nx % (nw0 + 1));
             prefetch_l2_blockrow(tc_point(V, b.arena, pn), jn < nb ? jn : nw0 - jn, nb, S::N8P / 4);
             prefetch_l2_range(tc_point(Grt, b.arena, pn) + (size_t)jn * N8, (size_t)N8 * sizeof(float));
         }
-        __syncthreads();  // the previous slice's reads of Z are done
-        // 1. raw inputs over the B operands
-        double *vs = reinterpret_cast<double *>(smem + S::b0);
-        float *gs = reinterpret_cast<float *>(smem + S::b0 + S::N8P * 8);
-        stage_blockrow<NBK>(vs, Vp, jv, nb);
-        for (int o = tid; o < N8; o += blockDim.x) cp_async4(gs + o, G + (size_t)j * N8 + o);
-        cp_async_wait_all();
-        __syncthreads();
         // 2. x = G V
-        float r1[PER];
+        {
+            const double *vs = reinterpret_cast<const double *>(smem + S::b0);
+            const float *gs = reinterpret_cast<const float *>(smem + S::b0 + S::N8P * 8);
 #pragma unroll
-        for (int i = 0; i < PER; ++i) {
-            const int o = tid + i * kTcThreads;
-            r1[i] = 0.0f;
-            if (o < N8) {
-                const double x = (double)gs[o] * vs[o];
-                if (o < NOCT)
-                    xn[o] = x;
-                else
-                    r1[i] = (float)x;
+            for (int i = 0; i < PER; ++i) {
+                const int o = tid + i * kTcThreads;
+                if (o < N8) {
+                    const double x = (double)gs[o] * vs[o];
+                    if (o < NOCT) xn[o] = x;
+                    xs[o] = o < NOCT ? 0.0f : (float)x;
+                }
             }
-        }
-#pragma unroll
-        for (int i = 0; i < PER; ++i) {
-            const int o = tid + i * kTcThreads;
-            if (o < N8) xs[o] = r1[i];
         }
         __syncthreads();
         // 3. the fold as K-major hi/lo operands, 8 rows x 4 columns per warp pass
@@ -383,35 +387,36 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         __syncthreads();
         if (*s_err) break;
         phase ^= 1;
-        // Z from tensor memory (rows m < 64) over the B operands, rows 64 from zx
+        // Z from tensor memory straight into octant order over xs:
+        //   Z_ee[m][n] -> (2m, 2n), n <= m;  Z_oo[m][n] -> (2m+1, 2n+1), n <= m;
+        //   Z_eo[m][n] -> (2m, 2n+1) for n < m, (2n+1, 2m) for n >= m
+        // rows 64 of Z_ee and Z_eo (zx) -> (128, 2n) and (128, 2n+1)
         {
-            using P = DctPlan<64>;
             const int q = warp & 3, blk = warp >> 2;
             const int m = 16 * q + (lane & 15);
             const int col0 = blk == 0 ? 0 : (blk == 1 ? 72 : 136);
-            const int zoff = blk == 0 ? P::EE : (blk == 1 ? P::EO : P::OO);
             uint32_t rr[72];
             tmem_ld_row72(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)col0, rr, blk == 0);
             if (lane < 16) {
-                float *zr = Z + zoff + m * P::LD;
 #pragma unroll
-                for (int c = 0; c < 68; c += 4)
-                    if (blk == 0 || c < 64)
-                        *reinterpret_cast<float4 *>(zr + c) = make_float4(
-                            __uint_as_float(rr[c]), __uint_as_float(rr[c + 1]), __uint_as_float(rr[c + 2]),
-                            __uint_as_float(rr[c + 3]));
+                for (int n = 0; n < 64; ++n) {
+                    const float v = __uint_as_float(rr[n]);
+                    if (blk == 0) {
+                        if (n <= m) xs[oct_of(2 * m, 2 * n)] = v;
+                    } else if (blk == 1) {
+                        xs[n < m ? oct_of(2 * m, 2 * n + 1) : oct_of(2 * n + 1, 2 * m)] = v;
+                    } else {
+                        if (n <= m) xs[oct_of(2 * m + 1, 2 * n + 1)] = v;
+                    }
+                }
             }
         }
+        for (int i = tid; i < 2 * H + 1; i += blockDim.x)
+            xs[oct_of(2 * H, i <= H ? 2 * i : 2 * (i - H - 1) + 1)] = zx[i];
         tc_fence_before();
         __syncthreads();
-        for (int i = tid; i < 2 * H + 1; i += blockDim.x) {
-            using P = DctPlan<64>;
-            if (i <= H)
-                Z[P::EE + H * P::LD + i] = zx[i];
-            else
-                Z[P::EO + H * P::LD + (i - H - 1)] = zx[i];
-        }
-        __syncthreads();
+        // the next slice's raw inputs (the B operands are free again)
+        if (nx < items) tc_stage(smem, Grt, V, nw0, (int)(nx / (nw0 + 1)), (int)(nx % (nw0 + 1)), b.arena);
         // 7. output
         for (int o = tid; o < N8; o += blockDim.x) {
             int l, m;
@@ -419,9 +424,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             double nf = u[m];
 #pragma unroll
             for (int a = 1; a <= R; ++a) nf = fma(cf[(a - 1) * NBK + l], u[a * NBK + m], nf);
-            out[bidx(j, o, nw0 + 1)] = (double)dct_z<64>(Z, l, m) + nf;
+            out[bidx(j, o, nw0 + 1)] = (double)xs[o] + nf;
         }
     }
+    cp_async_wait_all();  // no copy may land after the CTA leaves
     if (*s_err) {
         // let the MMAs in flight (the phase whose wait ran out) finish, bounded,
         // before the tensor memory is freed
