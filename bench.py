@@ -239,6 +239,17 @@ def our_arm(a, world, rank, local_rank):
     tau_tiles = {kind: {"pair_ms": float(tile_ms[2 * k]), "quad_ms": float(tile_ms[2 * k + 1]),
                         "picked": "pair" if tile_ms[2 * k] <= tile_ms[2 * k + 1] else "quad"}
                  for k, kind in enumerate(("chi0_tau", "vertex_tau", "sigma_tau"))}
+    # ---- the FP32 slice transforms' plan for this lattice, picked by timing
+    # every plan each kind supports (tpsc_tune_slice_plans: packed FFTs, the
+    # folded matrix DCT-I on the FP32 pipe, the same on the tensor cores) ------
+    g.solve()
+    plan_ms = np.zeros(12)
+    ctx.call("tpsc_tune_slice_plans", 5, plan_ms.ctypes.data_as(C.POINTER(C.c_double)))
+    plan_names = ("fft", "matrix_fp32", "matrix_tensor_3xtf32")
+    slice_plans = {}
+    for k, kind in enumerate(("gslice", "chi0_slice", "vertex_q", "sigma_slice")):
+        slice_plans[kind] = {plan_names[pl] + "_ms": float(plan_ms[3 * k + pl]) for pl in range(3) if plan_ms[3 * k + pl] > 0}
+        slice_plans[kind]["picked"] = plan_names[_lib.load().tpsc_get_slice_plan(k, w["nk0"])]
 
     # ---- device-resident solves: the FP64 drop-in with the reference's root
     # searches, the FP64 Newton form, then mixed precision + Newton (the
@@ -378,8 +389,9 @@ def our_arm(a, world, rank, local_rank):
         "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (model parameters; no dataset)",
         "config": {"workload": WORKLOAD_NAME,
-                   "form": "mixed precision (FP32 G/chi0/V slice transforms, compensated twiddles; FP64 Sigma "
-                           "transforms, tau transforms, sums, roots) + Newton root searches with moment series",
+                   "form": "mixed precision (FP32 slice transforms of G, chi0, V and Sigma on the autotuned "
+                           "slice plan, Sigma's near field |r| <= 4 in FP64; FP64 tau transforms, sums, roots) "
+                           "+ Newton root searches with moment series",
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "512 MB flush before every step; working set ~2.4 GB per solve",
                    "sumrule_evals": int(sc["evals_sp"] + sc["evals_ch"]), "mu_evals": int(sc["evals_mu"]),
@@ -388,6 +400,7 @@ def our_arm(a, world, rank, local_rank):
                              "reference's root searches runs direct launches with its host round trips"},
         "solve_graph": graph_stats,
         "tau_tiles": tau_tiles,
+        "slice_plans": slice_plans,
         "forms": {"mixed_newton": {"solves_per_s": value, "ms_per_step": ms / a.steps, "stage_ms": stages,
                                    "max_rel_dSigma_vs_fp64": dsigma},
                   "fp64_newton": {"solves_per_s": value_n64, "ms_per_step": ms_n64 / a.steps,

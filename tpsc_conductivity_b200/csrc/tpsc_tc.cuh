@@ -141,6 +141,29 @@ __device__ __forceinline__ void tmem_ld_row72(uint32_t taddr, uint32_t (&r)[72],
     for (int i = 0; i < 72; ++i) asm volatile("" : "+r"(r[i]));
 }
 
+// the mbarrier's current phase expects `bytes` more bytes from asynchronous copies
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// TMA: one box of a 4-D tensor map (this GPU's memory, no multicast) into
+// shared memory, counted on bar
+__device__ __forceinline__ void tma_load_4d(void *dst, const void *tmap, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(smem_u32(dst)),
+        "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+// bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned) into shared memory, counted on bar
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
 // x = hi + lo with hi rounded to TF32 (nearest, ties away); lo = x - hi is
 // exact in FP32 and enters the MMA truncated to TF32
 __device__ __forceinline__ float tf32_hi(float x) {

@@ -5,7 +5,8 @@
 // memory).  Lattice 256 x 256 (nbk = 129, H = 64).
 //
 // One slice at a time per CTA (persistent, one CTA per SM, 384 threads):
-//   1. stage the V(r, tau_j) block row and the FP32 G(r, tau_j) row (async copies);
+//   1. the V(r, tau_j) block row by TMA (a 4-D tensor map over this GPU's
+//      V), the FP32 G(r, tau_j) row by one bulk copy, both on an mbarrier;
 //   2. x = G V in FP64: the near field |rx|, |ry| <= 4 kept in FP64, the rest rounded to FP32;
 //   3. fold x into SS, SD, DD (tpsc_dct.cuh) as K-major hi/lo TF32 operands;
 //   4. T = K . fold^T on the tensor cores (M = 64 output rows of the DCT
@@ -19,11 +20,14 @@
 // the tensor cores run.  Every mbarrier wait is bounded: a wait that runs
 // out sets the error word, the CTA waits (bounded) once more, frees its
 // tensor memory and returns.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <math.h>
 #include <stdint.h>
 
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "tpsc_dct.cuh"
@@ -96,9 +100,18 @@ struct TcSmem {
     static constexpr uint32_t bar = t64 + 72 * 4;           // mbarrier (8-byte aligned)
     static constexpr uint32_t misc = bar + 8;               // tensor-memory base, error flag
     static constexpr uint32_t cf = misc + 16;               // 2 cos(pi a l / N), a = 1..R, l < NBK (doubles)
-    static constexpr uint32_t bytes = cf + R * NBK * 8;
+    static constexpr uint32_t tbar = cf + R * NBK * 8;      // mbarrier of the input copies
+    static constexpr uint32_t bytes = tbar + 8;
+    // the raw inputs over the B operands: the V block row as 9 TMA boxes of
+    // 256 four-double blocks (the last one partly beyond the row, filled with
+    // zeros), then the FP32 G row as one bulk copy of its 16-byte-aligned cover
+    static constexpr int VBOX = 256, NVBOX = (N8P / 4 + VBOX - 1) / VBOX;
+    static constexpr uint32_t vst = (b0 + 127) & ~127u;
+    static constexpr uint32_t gst = vst + NVBOX * VBOX * 32;
+    static constexpr uint32_t gmax = ((N8 * 4 + 15) & ~15) + 16;  // the cover of a row: at most 12 bytes each side
+    static_assert(gst + gmax <= b_end, "raw inputs fit over the B operands");
+    static_assert(tbar % 8 == 0, "mbarrier alignment");
     static_assert(bar % 8 == 0, "mbarrier alignment");
-    static_assert(N8P * 8 + N8 * 4 <= b_end - b0, "raw inputs fit over the B operands");
     static_assert(DctPlan<64>::REG * 4 <= b_end - b0, "Z fits over the B operands");
 };
 
@@ -172,24 +185,41 @@ __device__ __forceinline__ void issue_stage(uint64_t sdesc, uint32_t tmem) {
     }
 }
 
-// stage the raw inputs of slice j of point p (the V block row, the FP32 G
-// row) over the B operands with asynchronous copies (waited for by the caller)
-__device__ __forceinline__ void tc_stage(unsigned char *smem, const float *__restrict__ Grt,
-                                         const double *__restrict__ V, int nw0, int p, int j, long long arena) {
+// the 16-byte-aligned cover of the FP32 G row j of point p: its start and
+// bytes, and the row's offset in floats inside it
+struct GCover {
+    const unsigned char *src;
+    uint32_t bytes;
+    int shift;
+};
+__device__ __forceinline__ GCover g_cover(const float *__restrict__ Grt, int p, int j, long long arena) {
+    using S = TcSmem;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(tc_point(Grt, arena, p) + (size_t)j * S::N8);
+    const uintptr_t a0 = a & ~(uintptr_t)15, a1 = (a + S::N8 * 4 + 15) & ~(uintptr_t)15;
+    return GCover{reinterpret_cast<const unsigned char *>(a0), (uint32_t)(a1 - a0), (int)((a - a0) >> 2)};
+}
+// (one thread) the raw inputs of slice j of point p into shared memory, on tbar:
+// V(r, tau_jv) block row by TMA, G(r, tau_j) by one bulk copy
+__device__ __forceinline__ void tc_stage(unsigned char *smem, const void *tmV, const float *__restrict__ Grt,
+                                         int nw0, int p, int j, long long arena) {
     using S = TcSmem;
     const int nb = nw0 / 2 + 1;
     const int jv = j < nb ? j : nw0 - j;
-    const float *G = tc_point(Grt, arena, p) + (size_t)j * S::N8;
-    stage_blockrow<S::NBK>(reinterpret_cast<double *>(smem + S::b0), tc_point(V, arena, p), jv, nb);
-    float *gs = reinterpret_cast<float *>(smem + S::b0 + S::N8P * 8);
-    for (int o = threadIdx.x; o < S::N8; o += blockDim.x) cp_async4(gs + o, G + o);
+    uint64_t *tbar = reinterpret_cast<uint64_t *>(smem + S::tbar);
+    const GCover gc = g_cover(Grt, p, j, arena);
+    fence_async_smem();
+    mbar_expect_tx(tbar, (uint32_t)(S::NVBOX * S::VBOX * 32) + gc.bytes);
+#pragma unroll 1
+    for (int c = 0; c < S::NVBOX; ++c) tma_load_4d(smem + S::vst + c * S::VBOX * 32, tmV, 0, jv, c * S::VBOX, p, tbar);
+    bulk_load(smem + S::gst, gc.src, gc.bytes, tbar);
 }
 
 __device__ __forceinline__ int oct_of(int l, int m) { return l * (l + 1) / 2 + m; }
 
 __global__ void __launch_bounds__(kTcThreads, 1)
-    k_sigma_slice_tc(const float *__restrict__ Grt, const double *__restrict__ V, const float *__restrict__ tab,
-                     const double2 *__restrict__ tw64, int nw0, double *__restrict__ sigt, Bp b) {
+    k_sigma_slice_tc(const __grid_constant__ CUtensorMap tmV, const float *__restrict__ Grt,
+                     const float *__restrict__ tab, const double2 *__restrict__ tw64, int nw0,
+                     double *__restrict__ sigt, Bp b) {
     using S = TcSmem;
     constexpr int H = 64, N8 = S::N8, NBK = S::NBK, L = 256, R = S::R, NOCT = S::NOCT;
     constexpr int PER = (N8 + kTcThreads - 1) / kTcThreads;
@@ -203,6 +233,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     float *t64 = reinterpret_cast<float *>(smem + S::t64);
     const float *k64 = reinterpret_cast<const float *>(smem + S::k64);
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + S::bar);
+    uint64_t *tbar = reinterpret_cast<uint64_t *>(smem + S::tbar);
     uint32_t *s_tmem = reinterpret_cast<uint32_t *>(smem + S::misc);
     volatile uint32_t *s_err = reinterpret_cast<volatile uint32_t *>(smem + S::misc + 4);
     double *cf = reinterpret_cast<double *>(smem + S::cf);
@@ -214,39 +245,41 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     if (tid == 0) {
         mbar_init(bar, 1);
+        mbar_init(tbar, 1);
         *s_err = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = tid; i < (int)(S::tab_bytes / 16); i += blockDim.x)
         cp_async16(smem + 16 * i, reinterpret_cast<const unsigned char *>(tab) + 16 * i);
     for (int i = tid; i < R * NBK; i += blockDim.x) cf[i] = 2.0 * __ldg(&tw64[((i / NBK + 1) * (i % NBK)) % L]).x;
-    const int nb = nw0 / 2 + 1;
+    cp_async_wait_all();
     const long long items = (long long)(nw0 + 1) * b.P;
-    if (blockIdx.x < items)
-        tc_stage(smem, Grt, V, nw0, (int)(blockIdx.x / (nw0 + 1)), (int)(blockIdx.x % (nw0 + 1)), b.arena);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    if (tid == 0 && blockIdx.x < items)
+        tc_stage(smem, &tmV, Grt, nw0, (int)(blockIdx.x / (nw0 + 1)), (int)(blockIdx.x % (nw0 + 1)), b.arena);
     const uint32_t tmem = *s_tmem;
-    uint32_t phase = 0;
+    uint32_t phase = 0, tphase = 0;
 
     for (long long it = blockIdx.x; it < items; it += gridDim.x) {
         const int p = (int)(it / (nw0 + 1)), j = (int)(it % (nw0 + 1));
         double *out = tc_point(sigt, b.arena, p);
         const long long nx = it + gridDim.x;
         __syncthreads();  // the previous slice's reads of xs are done
-        // 1. this slice's raw inputs (staged during the previous slice's output)
-        cp_async_wait_all();
+        // 1. this slice's raw inputs (copied in during the previous slice's output)
+        if (!mbar_wait(tbar, tphase, kWaitNs)) *s_err = 1;
         __syncthreads();
+        if (*s_err) break;
+        tphase ^= 1;
         if (nx < items) {
             const int pn = (int)(nx / (nw0 + 1)), jn = (int)(nx % (nw0 + 1));
-            prefetch_l2_blockrow(tc_point(V, b.arena, pn), jn < nb ? jn : nw0 - jn, nb, S::N8P / 4);
             prefetch_l2_range(tc_point(Grt, b.arena, pn) + (size_t)jn * N8, (size_t)N8 * sizeof(float));
         }
         // 2. x = G V
         {
-            const double *vs = reinterpret_cast<const double *>(smem + S::b0);
-            const float *gs = reinterpret_cast<const float *>(smem + S::b0 + S::N8P * 8);
+            const double *vs = reinterpret_cast<const double *>(smem + S::vst);
+            const float *gs = reinterpret_cast<const float *>(smem + S::gst) + g_cover(Grt, p, j, b.arena).shift;
 #pragma unroll
             for (int i = 0; i < PER; ++i) {
                 const int o = tid + i * kTcThreads;
@@ -299,17 +332,21 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
             u[i] = acc;
         }
-        // column 64 of T_ee: t64[m] = sum_{k<=64} SS[m][k] Ks[64][k], m <= 64 (warps 4..6)
-        if (tid >= 128 && tid < 128 + H + 1) {
-            const int m = tid - 128;
+        // column 64 of T_ee: t64[m] = sum_{k<=64} SS[m][k] Ks[64][k], m <= 64;
+        // four threads per m (warps 2..10), k = sub, sub + 4, ...
+        if (warp >= 2 && warp <= 10) {
+            const int i = tid - 64, m = i >> 2, sub = i & 3;
             float acc = 0.0f;
-            for (int k = 0; k <= H; ++k) {
-                const uint32_t off = kmaj_off(m, k, 72);
-                const float sv = *reinterpret_cast<const float *>(smem + S::ee_hi + off) +
-                                 *reinterpret_cast<const float *>(smem + S::ee_lo + off);
-                acc = fmaf(sv, k64[k], acc);
-            }
-            t64[m] = acc;
+            if (m <= H)
+                for (int k = sub; k <= H; k += 4) {
+                    const uint32_t off = kmaj_off(m, k, 72);
+                    const float sv = *reinterpret_cast<const float *>(smem + S::ee_hi + off) +
+                                     *reinterpret_cast<const float *>(smem + S::ee_lo + off);
+                    acc = fmaf(sv, k64[k], acc);
+                }
+            acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+            acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+            if (sub == 0 && m <= H) t64[m] = acc;
         }
         if (!mbar_wait(bar, phase, kWaitNs)) *s_err = 1;
         tc_fence_after();
@@ -366,21 +403,24 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             issue_stage<true>(sdesc0, tmem);
             mma_commit(bar);
         }
-        // rows 64 of Z_ee (n <= 64) and Z_eo (n < 64): sum_{k<=64} Ks[64][k] T[k][n]
-        if (tid >= 128 && tid < 128 + 2 * H + 1) {
-            const int i = tid - 128;
-            const bool ee = i <= H;
-            const int n = ee ? i : i - H - 1;
+        // rows 64 of Z_ee (n <= 64) and Z_eo (n < 64): sum_{k<=64} Ks[64][k] T[k][n];
+        // two threads per sum (warps 2..10), k = sub, sub + 2, ...
+        if (warp >= 2 && warp <= 10) {
+            const int i = tid - 64, d = i >> 1, sub = i & 1;
+            const bool ee = d <= H;
+            const int n = ee ? d : d - H - 1;
             const uint32_t hi_off = ee ? S::ee_hi : S::eo_hi, lo_off = ee ? S::ee_lo : S::eo_lo;
             const int R2 = ee ? 72 : 64;
             float acc = 0.0f;
-            for (int k = 0; k <= H; ++k) {
-                const uint32_t off = kmaj_off(n, k, R2);
-                const float tv = *reinterpret_cast<const float *>(smem + hi_off + off) +
-                                 *reinterpret_cast<const float *>(smem + lo_off + off);
-                acc = fmaf(k64[k], tv, acc);
-            }
-            zx[i] = acc;
+            if (d <= 2 * H)
+                for (int k = sub; k <= H; k += 2) {
+                    const uint32_t off = kmaj_off(n, k, R2);
+                    const float tv = *reinterpret_cast<const float *>(smem + hi_off + off) +
+                                     *reinterpret_cast<const float *>(smem + lo_off + off);
+                    acc = fmaf(k64[k], tv, acc);
+                }
+            acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+            if (sub == 0 && d <= 2 * H) zx[d] = acc;
         }
         if (!mbar_wait(bar, phase, kWaitNs)) *s_err = 1;
         tc_fence_after();
@@ -413,27 +453,45 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         for (int i = tid; i < 2 * H + 1; i += blockDim.x)
             xs[oct_of(2 * H, i <= H ? 2 * i : 2 * (i - H - 1) + 1)] = zx[i];
+        fence_async_smem();  // this slice's accesses to the B operands come before the next copies
         tc_fence_before();
         __syncthreads();
         // the next slice's raw inputs (the B operands are free again)
-        if (nx < items) tc_stage(smem, Grt, V, nw0, (int)(nx / (nw0 + 1)), (int)(nx % (nw0 + 1)), b.arena);
-        // 7. output
-        for (int o = tid; o < N8; o += blockDim.x) {
+        if (tid == 0 && nx < items)
+            tc_stage(smem, &tmV, Grt, nw0, (int)(nx / (nw0 + 1)), (int)(nx % (nw0 + 1)), b.arena);
+        // 7. output: four consecutive octant points (one 32-byte block of the
+        // column-block layout) per thread and pass
+        for (int g = tid; g < S::N8P / 4; g += blockDim.x) {
             int l, m;
-            oct_lm(o, l, m);
-            double nf = u[m];
+            oct_lm(4 * g, l, m);
+            double v[4];
 #pragma unroll
-            for (int a = 1; a <= R; ++a) nf = fma(cf[(a - 1) * NBK + l], u[a * NBK + m], nf);
-            out[bidx(j, o, nw0 + 1)] = (double)xs[o] + nf;
+            for (int e = 0; e < 4; ++e) {
+                const int o = 4 * g + e;
+                v[e] = 0.0;
+                if (o < N8) {
+                    double nf = u[m];
+#pragma unroll
+                    for (int a = 1; a <= R; ++a) nf = fma(cf[(a - 1) * NBK + l], u[a * NBK + m], nf);
+                    v[e] = (double)xs[o] + nf;
+                }
+                if (++m > l) {
+                    ++l;
+                    m = 0;
+                }
+            }
+            double2 *dst = reinterpret_cast<double2 *>(out + bidx(j, 4 * g, nw0 + 1));
+            dst[0] = make_double2(v[0], v[1]);
+            dst[1] = make_double2(v[2], v[3]);
         }
     }
-    cp_async_wait_all();  // no copy may land after the CTA leaves
     if (*s_err) {
-        // let the MMAs in flight (the phase whose wait ran out) finish, bounded,
-        // before the tensor memory is freed
+        // let the MMAs and copies in flight (the phases whose wait ran out)
+        // finish, bounded, before the tensor memory is freed and the CTA leaves
         if (tid == 0) {
             atomicOr(&g_tc_err, 1u);
             mbar_wait(bar, phase, kWaitNs);
+            mbar_wait(tbar, tphase, kWaitNs);
         }
     }
     tc_fence_before();
@@ -446,9 +504,39 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
 }  // namespace
 
+namespace {
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+}  // namespace
+
 cudaError_t launch_sigma_slice_tc(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st,
                                   const Bp &b) {
     if (g.nbk != 129 || !g.dct_tc) return cudaErrorInvalidValue;
+    // V as (4 doubles of a column block, row j, column block, point): box
+    // (4, 1, 256, 1) = one row of 256 column blocks, 8 KB
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode) return cudaErrorNotSupported;
+    const cuuint64_t nblk = (cuuint64_t)g.n8p / 4;
+    const cuuint64_t dims[4] = {4, (cuuint64_t)g.nb, nblk, (cuuint64_t)b.P};
+    const cuuint64_t strides[3] = {32, (cuuint64_t)g.nb * 32,
+                                   b.P > 1 ? (cuuint64_t)b.arena : (cuuint64_t)g.nb * 32 * nblk};
+    const cuuint32_t box[4] = {4, 1, TcSmem::VBOX, 1}, estr[4] = {1, 1, 1, 1};
+    CUtensorMap tmV;
+    if (encode(&tmV, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double *>(V), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return cudaErrorInvalidValue;
     const size_t sm = TcSmem::bytes;
     cudaError_t e = set_smem(k_sigma_slice_tc, sm);
     if (e != cudaSuccess) return e;
@@ -456,7 +544,7 @@ cudaError_t launch_sigma_slice_tc(const GridDev &g, const float *Grt, const doub
     if (ctas <= 0) return cudaErrorInvalidConfiguration;
     const long long items = (long long)(g.nw0 + 1) * b.P;
     const int grid = (int)(items < ctas ? items : ctas);
-    k_sigma_slice_tc<<<grid, kTcThreads, sm, st>>>(Grt, V, g.dct_tc, g.tw_k, g.nw0, sigt, b);
+    k_sigma_slice_tc<<<grid, kTcThreads, sm, st>>>(tmV, Grt, g.dct_tc, g.tw_k, g.nw0, sigt, b);
     return launched();
 }
 
