@@ -10,7 +10,9 @@ line.  Under a kernel profiler, the launches of the last solve start at its
 k_gk_table launch.  With --cond, every solve is followed by the
 current-current correlator (bubble + Maki-Thompson, N_theta_k = 1), whose
 stage times are in the same line.  --model takes the lattice parameters
-"tp,U,n,T" (default the bench's -0.15,4,0.875,0.05).
+"tp,U,n,T" (default the bench's -0.15,4,0.875,0.05).  --slice-plans sets the
+plan of the four FP32 slice transforms (G, chi0, V, Sigma) for this lattice
+before the first solve, e.g. 0,0,0,2 for the tensor-core Sigma slice.
 """
 import argparse
 import json
@@ -33,7 +35,13 @@ def main(argv=None):
     ap.add_argument("--solves", type=int, default=3)
     ap.add_argument("--cond", action="store_true")
     ap.add_argument("--model", default="-0.15,4,0.875,0.05")
+    ap.add_argument("--slice-plans", default=None, help="plans of the G, chi0, V and Sigma slices, e.g. 0,0,0,2")
     a = ap.parse_args(argv)
+    if a.slice_plans:
+        lib = _lib.load()
+        for kind, plan in enumerate(int(x) for x in a.slice_plans.split(",")):
+            if lib.tpsc_set_slice_plan(kind, a.nk0, plan) != 0:
+                raise SystemExit(f"slice plan {plan} is not available for kind {kind} at nk0 = {a.nk0}")
     tp, U, n, T = (float(x) for x in a.model.split(","))
     g = CondOpt(a.nk0, a.nw0, n, T, 0.1, (tp, 0.0, 0.0, U))
     g.set_form(FORMS[a.form])
@@ -42,7 +50,8 @@ def main(argv=None):
         if a.cond:
             g.calc_chijj_vertex_corr_all_optim(False, 3, 1)
     s = g.scalars()
-    print(json.dumps({"nk0": a.nk0, "nw0": a.nw0, "form": a.form, "stage_ms": g.stage_times(),
+    print(json.dumps({"nk0": a.nk0, "nw0": a.nw0, "form": a.form, "slice_plans": a.slice_plans,
+                      "stage_ms": g.stage_times(),
                       "evals": {"sp": s["evals_sp"], "ch": s["evals_ch"], "mu": s["evals_mu"]}}))
 
 
