@@ -187,6 +187,18 @@ __device__ __forceinline__ double vertex_fact(double U, const double *Usc) {
     return __dmul_rn(U, __dadd_rn(__dmul_rn(3.0, Usc[0]), Usc[1])) / 8.0;
 }
 
+// c[a] = cos(pi a t / N), a = 0..R, from c1 = cos(pi t / N) (tw64[t].x of the
+// table tw64[m] = exp(-2 pi i m / 2N)) by the Chebyshev recurrence
+// c[a + 1] = 2 c1 c[a] - c[a - 1]: one table read for all R + 1 cosines, a
+// few ulp for R <= 4
+template <int R>
+__device__ __forceinline__ void cheb_cos(double c1, double (&c)[R + 1]) {
+    c[0] = 1.0;
+    if constexpr (R >= 1) c[1] = c1;
+#pragma unroll
+    for (int a = 2; a <= R; ++a) c[a] = fma(2.0 * c1, c[a - 1], -c[a - 2]);
+}
+
 __device__ __forceinline__ void prefetch_l2_range(const void *p, size_t bytes) {
     const char *c = static_cast<const char *>(p);
     for (size_t off = (size_t)threadIdx.x * 128; off < bytes; off += (size_t)blockDim.x * 128)

@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(kDctThreads, 1)
                       const double2 *__restrict__ tw64, int nw0, double *__restrict__ sigt, Bp b) {
     using P = DctPlan<H>;
     using SM = SigmaDctSmem<H>;
-    constexpr int NBK = P::NBK, N8 = P::N8, L = 2 * P::N, R = SM::R, NOCT = SM::NOCT;
+    constexpr int NBK = P::NBK, N8 = P::N8, R = SM::R, NOCT = SM::NOCT;
     constexpr int PER = (N8 + kDctThreads - 1) / kDctThreads;
     extern __shared__ __align__(16) unsigned char smem[];
     float *tabs = reinterpret_cast<float *>(smem);
@@ -201,12 +201,14 @@ __global__ void __launch_bounds__(kDctThreads, 1)
             // near field: u_a(k2) = sum_b w_b x(a, b) cos(pi b k2 / N), w_0 = 1, w_b = 2
             for (int i = tid; i < (R + 1) * NBK; i += blockDim.x) {
                 const int a = i / NBK, k2 = i % NBK;
+                double cs[R + 1];
+                cheb_cos<R>(__ldg(&tw64[k2]).x, cs);
                 double acc = 0.0;
 #pragma unroll
                 for (int c = 0; c <= R; ++c) {
                     const int hi = a > c ? a : c, lo = a > c ? c : a;
                     const double wb = c == 0 ? 1.0 : 2.0;
-                    acc = fma(wb * xns[lo + hi * (hi + 1) / 2], __ldg(&tw64[(c * k2) % L]).x, acc);
+                    acc = fma(wb * xns[lo + hi * (hi + 1) / 2], cs[c], acc);
                 }
                 us[i] = acc;
             }
@@ -216,9 +218,11 @@ __global__ void __launch_bounds__(kDctThreads, 1)
             for (int o = tid; o < N8; o += blockDim.x) {
                 int l, m;
                 oct_lm(o, l, m);
+                double cs[R + 1];
+                cheb_cos<R>(__ldg(&tw64[l]).x, cs);
                 double nf = us[m];
 #pragma unroll
-                for (int a = 1; a <= R; ++a) nf = fma(2.0 * __ldg(&tw64[(a * l) % L]).x, us[a * NBK + m], nf);
+                for (int a = 1; a <= R; ++a) nf = fma(2.0 * cs[a], us[a * NBK + m], nf);
                 out[bidx(js, o, nw0 + 1)] = (double)dct_z<H>(F, l, m) + nf;
             }
             if (s == 0 && two) __syncthreads();  // the next fold overwrites F

@@ -217,8 +217,9 @@ struct SigmaSlice32Smem {
 // Sigma(k, tau_j) = DCT-I[ G(r, tau_j) V(r, tau_j) ], j = 0..Nw0, with
 // V(r, tau_j) = V(r, beta - tau_j) for tau_j > beta/2 (src/green.cpp:1822-1885):
 // the product in FP64 from the FP32 G; beyond the near field transformed in
-// FP32, the near field's transform added in FP64 (cosines from the FP64
-// twiddle table tw64[m] = exp(-2 pi i m / L), L = 2 (nbk - 1)).
+// FP32, the near field's transform added in FP64 (cos(pi a t / (nbk - 1)) by
+// the Chebyshev recurrence from the FP64 twiddle table entry tw64[t],
+// tw64[m] = exp(-2 pi i m / L), L = 2 (nbk - 1)).
 template <int NBK>
 __global__ void __launch_bounds__(kSlice32Threads, 2)
     k_sigma_slice32(const float *__restrict__ Grt, const double *__restrict__ V, const float4 *__restrict__ tw,
@@ -226,7 +227,6 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
     Grt = at(Grt, b.arena);
     V = at(V, b.arena);
     sigt = at(sigt, b.arena);
-    constexpr int L = 2 * (NBK - 1);
     constexpr int R = SigmaSlice32Smem<NBK>::R;
     constexpr int NOCT = SigmaSlice32Smem<NBK>::NOCT;
     extern __shared__ __align__(16) float S32[];
@@ -261,12 +261,14 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
     // u_a(k2) = sum_b w_b x(a, b) cos(pi b k2 / (nbk - 1)), w_0 = 1, w_b = 2
     for (int i = threadIdx.x; i < (R + 1) * NBK; i += blockDim.x) {
         const int a = i / NBK, k2 = i % NBK;
+        double cs[R + 1];
+        cheb_cos<R>(__ldg(&tw64[k2]).x, cs);
         double acc = 0.0;
 #pragma unroll
         for (int b = 0; b <= R; ++b) {
             const int hi = a > b ? a : b, lo = a > b ? b : a;
             const double wb = b == 0 ? 1.0 : 2.0;
-            acc = fma(wb * xn[lo + hi * (hi + 1) / 2], __ldg(&tw64[(b * k2) % L]).x, acc);
+            acc = fma(wb * xn[lo + hi * (hi + 1) / 2], cs[b], acc);
         }
         u[i] = acc;
     }
@@ -275,9 +277,11 @@ __global__ void __launch_bounds__(kSlice32Threads, 2)
     for (int o = threadIdx.x; o < n8; o += blockDim.x) {
         int l, m;
         oct_lm(o, l, m);
+        double cs[R + 1];
+        cheb_cos<R>(__ldg(&tw64[l]).x, cs);
         double nf = u[m];
 #pragma unroll
-        for (int a = 1; a <= R; ++a) nf = fma(2.0 * __ldg(&tw64[(a * l) % L]).x, u[a * NBK + m], nf);
+        for (int a = 1; a <= R; ++a) nf = fma(2.0 * cs[a], u[a * NBK + m], nf);
         sigt[bidx(j, o, nw0 + 1)] = (double)S32[l * NBK + m] + nf;
     }
 }

@@ -292,6 +292,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         __syncthreads();
         // 3. the fold as K-major hi/lo operands, 8 rows x 4 columns per warp pass
+#pragma unroll 2
         for (int un = warp; un < 9 * 18; un += kTcThreads / 32) {
             const int r = 8 * (un / 18) + (lane >> 2), k = 4 * (un % 18) + (lane & 3);
             float v[3];
@@ -324,11 +325,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // (while the tensor cores run) near field: u_a(k2) = sum_c w_c x(a, c) cos(pi c k2 / N)
         for (int i = tid; i < (R + 1) * NBK; i += blockDim.x) {
             const int a = i / NBK, k2 = i % NBK;
+            double cs[R + 1];
+            cheb_cos<R>(__ldg(&tw64[k2]).x, cs);
             double acc = 0.0;
 #pragma unroll
             for (int c = 0; c <= R; ++c) {
                 const int hi = a > c ? a : c, lo = a > c ? c : a;
-                acc = fma((c == 0 ? 1.0 : 2.0) * xn[lo + hi * (hi + 1) / 2], __ldg(&tw64[(c * k2) % L]).x, acc);
+                acc = fma((c == 0 ? 1.0 : 2.0) * xn[lo + hi * (hi + 1) / 2], cs[c], acc);
             }
             u[i] = acc;
         }
@@ -459,30 +462,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // the next slice's raw inputs (the B operands are free again)
         if (tid == 0 && nx < items)
             tc_stage(smem, &tmV, Grt, nw0, (int)(nx / (nw0 + 1)), (int)(nx % (nw0 + 1)), b.arena);
-        // 7. output: four consecutive octant points (one 32-byte block of the
-        // column-block layout) per thread and pass
-        for (int g = tid; g < S::N8P / 4; g += blockDim.x) {
+        // 7. output (consecutive lanes on consecutive octant points: a warp
+        // writes whole 32-byte blocks of the column-block layout)
+        for (int o = tid; o < N8; o += blockDim.x) {
             int l, m;
-            oct_lm(4 * g, l, m);
-            double v[4];
+            oct_lm(o, l, m);
+            double nf = u[m];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int o = 4 * g + e;
-                v[e] = 0.0;
-                if (o < N8) {
-                    double nf = u[m];
-#pragma unroll
-                    for (int a = 1; a <= R; ++a) nf = fma(cf[(a - 1) * NBK + l], u[a * NBK + m], nf);
-                    v[e] = (double)xs[o] + nf;
-                }
-                if (++m > l) {
-                    ++l;
-                    m = 0;
-                }
-            }
-            double2 *dst = reinterpret_cast<double2 *>(out + bidx(j, 4 * g, nw0 + 1));
-            dst[0] = make_double2(v[0], v[1]);
-            dst[1] = make_double2(v[2], v[3]);
+            for (int a = 1; a <= R; ++a) nf = fma(cf[(a - 1) * NBK + l], u[a * NBK + m], nf);
+            out[bidx(j, o, nw0 + 1)] = (double)xs[o] + nf;
         }
     }
     if (*s_err) {
