@@ -85,12 +85,17 @@ struct TcSmem {
     static constexpr uint32_t ks_hi = 0, ks_lo = 64 * KS * 4, kd_hi = 2 * 64 * KS * 4, kd_lo = kd_hi + 64 * 64 * 4;
     static constexpr uint32_t k64 = kd_lo + 64 * 64 * 4;  // 72 floats
     static constexpr uint32_t tab_bytes = k64 + KS * 4;   // 69,920
-    // B operands: ee (72 x 72), eo (72 x 64 first products, 64 x 72 second), oo (64 x 64), hi | lo each
+    // B operands, hi | lo each.  First products: SS (72 rows x K 72) and
+    // [SD; DD] (72 + 64 rows x K 64, one MMA for both, A = Kd).  Second
+    // products: [T_ee^T; T_eo^T] (72 + 64 rows x K 72, one MMA, A = Ks) and
+    // T_oo^T (64 x 64).  Both stages span the same 111,104 bytes.
     static constexpr uint32_t b0 = tab_bytes;
-    static constexpr uint32_t ee_hi = b0, ee_lo = ee_hi + 72 * 72 * 4;
-    static constexpr uint32_t eo_hi = ee_lo + 72 * 72 * 4, eo_lo = eo_hi + 72 * 64 * 4;
-    static constexpr uint32_t oo_hi = eo_lo + 72 * 64 * 4, oo_lo = oo_hi + 64 * 64 * 4;
-    static constexpr uint32_t b_end = oo_lo + 64 * 64 * 4;  // b0 + 111,104
+    static constexpr uint32_t ss_hi = b0, ss_lo = ss_hi + 72 * 72 * 4;
+    static constexpr uint32_t sddd_hi = ss_lo + 72 * 72 * 4, sddd_lo = sddd_hi + 136 * 64 * 4;
+    static constexpr uint32_t b_end = sddd_lo + 136 * 64 * 4;  // b0 + 111,104
+    static constexpr uint32_t t_hi = b0, t_lo = t_hi + 136 * 72 * 4;
+    static constexpr uint32_t too_hi = t_lo + 136 * 72 * 4, too_lo = too_hi + 64 * 64 * 4;
+    static_assert(too_lo + 64 * 64 * 4 == b_end, "both stages' operands span the same bytes");
     static constexpr uint32_t xs = b_end;                    // N8 floats
     static constexpr uint32_t xn = xs + ((N8 * 4 + 15) & ~15);
     static constexpr uint32_t u = xn + 16 * 8;
@@ -175,13 +180,14 @@ __device__ __forceinline__ void issue_block(uint64_t dbase_a, uint64_t dbase_b, 
 template <bool SECOND>
 __device__ __forceinline__ void issue_stage(uint64_t sdesc, uint32_t tmem) {
     using S = TcSmem;
-    issue_block<S::ks_hi, S::ks_lo, S::ee_hi, S::ee_lo, 72, 9, 0>(sdesc, sdesc, tmem);
     if constexpr (SECOND) {
-        issue_block<S::ks_hi, S::ks_lo, S::eo_hi, S::eo_lo, 64, 9, 72>(sdesc, sdesc, tmem);
-        issue_block<S::kd_hi, S::kd_lo, S::oo_hi, S::oo_lo, 64, 8, 136>(sdesc, sdesc, tmem);
+        // Z_ee and Z_eo in one MMA chain (columns 0..71 and 72..135), Z_oo (136..199)
+        issue_block<S::ks_hi, S::ks_lo, S::t_hi, S::t_lo, 136, 9, 0>(sdesc, sdesc, tmem);
+        issue_block<S::kd_hi, S::kd_lo, S::too_hi, S::too_lo, 64, 8, 136>(sdesc, sdesc, tmem);
     } else {
-        issue_block<S::kd_hi, S::kd_lo, S::eo_hi, S::eo_lo, 72, 8, 72>(sdesc, sdesc, tmem);
-        issue_block<S::kd_hi, S::kd_lo, S::oo_hi, S::oo_lo, 64, 8, 144>(sdesc, sdesc, tmem);
+        // T_ee (columns 0..71), then T_eo and T_oo in one MMA chain (72..143 and 144..207)
+        issue_block<S::ks_hi, S::ks_lo, S::ss_hi, S::ss_lo, 72, 9, 0>(sdesc, sdesc, tmem);
+        issue_block<S::kd_hi, S::kd_lo, S::sddd_hi, S::sddd_lo, 136, 8, 72>(sdesc, sdesc, tmem);
     }
 }
 
@@ -299,17 +305,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             fold_at(xs, r, k, v[0], v[1], v[2]);
             const uint32_t off72 = kmaj_off(r, k, 72);
             float h = tf32_hi(v[0]);
-            *reinterpret_cast<float *>(smem + S::ee_hi + off72) = h;
-            *reinterpret_cast<float *>(smem + S::ee_lo + off72) = v[0] - h;
+            *reinterpret_cast<float *>(smem + S::ss_hi + off72) = h;
+            *reinterpret_cast<float *>(smem + S::ss_lo + off72) = v[0] - h;
             if (k < 64) {
+                const uint32_t offsd = kmaj_off(r, k, 136);
                 h = tf32_hi(v[1]);
-                *reinterpret_cast<float *>(smem + S::eo_hi + off72) = h;
-                *reinterpret_cast<float *>(smem + S::eo_lo + off72) = v[1] - h;
+                *reinterpret_cast<float *>(smem + S::sddd_hi + offsd) = h;
+                *reinterpret_cast<float *>(smem + S::sddd_lo + offsd) = v[1] - h;
                 if (r < 64) {
-                    const uint32_t off64 = kmaj_off(r, k, 64);
+                    const uint32_t offdd = kmaj_off(72 + r, k, 136);
                     h = tf32_hi(v[2]);
-                    *reinterpret_cast<float *>(smem + S::oo_hi + off64) = h;
-                    *reinterpret_cast<float *>(smem + S::oo_lo + off64) = v[2] - h;
+                    *reinterpret_cast<float *>(smem + S::sddd_hi + offdd) = h;
+                    *reinterpret_cast<float *>(smem + S::sddd_lo + offdd) = v[2] - h;
                 }
             }
         }
@@ -343,8 +350,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (m <= H)
                 for (int k = sub; k <= H; k += 4) {
                     const uint32_t off = kmaj_off(m, k, 72);
-                    const float sv = *reinterpret_cast<const float *>(smem + S::ee_hi + off) +
-                                     *reinterpret_cast<const float *>(smem + S::ee_lo + off);
+                    const float sv = *reinterpret_cast<const float *>(smem + S::ss_hi + off) +
+                                     *reinterpret_cast<const float *>(smem + S::ss_lo + off);
                     acc = fmaf(sv, k64[k], acc);
                 }
             acc += __shfl_xor_sync(0xffffffffu, acc, 1);
@@ -357,16 +364,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (*s_err) break;
         phase ^= 1;
         // 5. T from tensor memory into the second products' B operands:
-        // B2_ee[n][k] = T_ee[k][n] (n < 64 from the accumulator, row 64 = t64),
-        // B2_eo[n][k] = T_eo[k][n], B2_oo[n][k] = T_oo[k][n]
+        // rows n of [T_ee^T; T_eo^T] (row n: T_ee[.][n], n < 64 from the
+        // accumulator, row 64 = t64; row 72 + n: T_eo[.][n]) and of T_oo^T
         {
             const int q = warp & 3, blk = warp >> 2;
-            const int n = 16 * q + (lane & 15);
+            const int n = 16 * q + (lane & 15) + (blk == 1 ? 72 : 0);
             const int col0 = blk == 0 ? 0 : (blk == 1 ? 72 : 144);
             const int ncol = blk == 2 ? 64 : 72;
-            const uint32_t hi_off = blk == 0 ? S::ee_hi : (blk == 1 ? S::eo_hi : S::oo_hi);
-            const uint32_t lo_off = blk == 0 ? S::ee_lo : (blk == 1 ? S::eo_lo : S::oo_lo);
-            const int R2 = blk == 0 ? 72 : 64;
+            const uint32_t hi_off = blk == 2 ? S::too_hi : S::t_hi;
+            const uint32_t lo_off = blk == 2 ? S::too_lo : S::t_lo;
+            const int R2 = blk == 2 ? 64 : 136;
             uint32_t rr[72];
             tmem_ld_row72(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)col0, rr, ncol == 72);
             if (lane < 16) {
@@ -388,14 +395,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 }
             }
         }
-        // rows 64..71 of B2_ee: row 64 = t64 (k <= 64), the rest zero
+        // rows 64..71 of the T_ee^T part: row 64 = t64 (k <= 64), the rest zero
         for (int i = tid; i < 8 * 72; i += blockDim.x) {
             const int n = 64 + i / 72, k = i % 72;
             const float v = (n == 64 && k <= H) ? t64[k] : 0.0f;
             const float h = tf32_hi(v);
-            const uint32_t off = kmaj_off(n, k, 72);
-            *reinterpret_cast<float *>(smem + S::ee_hi + off) = h;
-            *reinterpret_cast<float *>(smem + S::ee_lo + off) = v - h;
+            const uint32_t off = kmaj_off(n, k, 136);
+            *reinterpret_cast<float *>(smem + S::t_hi + off) = h;
+            *reinterpret_cast<float *>(smem + S::t_lo + off) = v - h;
         }
         fence_async_smem();
         tc_fence_before();
@@ -411,15 +418,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (warp >= 2 && warp <= 10) {
             const int i = tid - 64, d = i >> 1, sub = i & 1;
             const bool ee = d <= H;
-            const int n = ee ? d : d - H - 1;
-            const uint32_t hi_off = ee ? S::ee_hi : S::eo_hi, lo_off = ee ? S::ee_lo : S::eo_lo;
-            const int R2 = ee ? 72 : 64;
+            const int row = ee ? d : 72 + (d - H - 1);  // T_ee^T row d, T_eo^T row d - 65
             float acc = 0.0f;
             if (d <= 2 * H)
                 for (int k = sub; k <= H; k += 2) {
-                    const uint32_t off = kmaj_off(n, k, R2);
-                    const float tv = *reinterpret_cast<const float *>(smem + hi_off + off) +
-                                     *reinterpret_cast<const float *>(smem + lo_off + off);
+                    const uint32_t off = kmaj_off(row, k, 136);
+                    const float tv = *reinterpret_cast<const float *>(smem + S::t_hi + off) +
+                                     *reinterpret_cast<const float *>(smem + S::t_lo + off);
                     acc = fmaf(k64[k], tv, acc);
                 }
             acc += __shfl_xor_sync(0xffffffffu, acc, 1);
