@@ -142,8 +142,9 @@ int tpsc_set_tau_tile(int kind, int nw0, int tile);
  * plan in use (the library's default until one is set), or -TPSC_ERR_ARG. */
 int tpsc_set_slice_plan(int kind, int nk0, int plan);
 int tpsc_get_slice_plan(int kind, int nk0);
-/* Plan 2 (kind 3, nk0 256) runs the Sigma slice's folded matrix DCT-I on the
- * tcgen05 tensor cores (3xTF32, FP32 accumulation in tensor memory).  Its
+/* Plan 2 (nk0 256, kinds 2 and 3) runs the V or Sigma slice's folded matrix
+ * DCT-I on the tcgen05 tensor cores (3xTF32, FP32 accumulation in tensor
+ * memory).  Its
  * kernels wait on the tensor cores with a 2 s bound; a wait that runs out
  * sets a process-wide error word (the results of that launch are not valid,
  * the context stays usable).  tpsc_tensor_plan_errors reads the word of the

@@ -120,7 +120,7 @@ def test_slice_plan_arguments_and_defaults(lib):
     from tpsc_conductivity_b200 import _lib
 
     for kind, nk0, plan in [(4, 256, 1), (-1, 256, 0), (3, 256, 3), (3, 32, 1), (3, 100, 0), (0, 16, 1),
-                            (0, 256, 2), (3, 128, 2)]:
+                            (0, 256, 2), (1, 256, 2), (3, 128, 2)]:
         assert lib.tpsc_set_slice_plan(kind, nk0, plan) == _lib.ERR_ARG, (kind, nk0, plan)
     assert lib.tpsc_get_slice_plan(4, 256) < 0
     assert lib.tpsc_get_slice_plan(3, 100) < 0

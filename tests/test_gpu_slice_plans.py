@@ -1,8 +1,8 @@
 """The plans of the mixed form's FP32 slice transforms (tpsc_set_slice_plan):
 packed radix-16 FFTs of the even extension (plan 0), the folded matrix
-DCT-I on the FP32 pipe (plan 1) and, for the Sigma slice of the 256 x 256
-lattice, the same matrix DCT-I on the tcgen05 tensor cores in 3xTF32 (plan
-2).  All compute the reference's REDFT00 x REDFT00 of the same slices, so a
+DCT-I on the FP32 pipe (plan 1) and, for the V and Sigma slices of the
+256 x 256 lattice, the same matrix DCT-I on the tcgen05 tensor cores in
+3xTF32 (plan 2).  All compute the reference's REDFT00 x REDFT00 of the same slices, so a
 mixed + Newton solve with any plan is within the mixed form's bound of the
 FP64 Newton solve (Sigma, chi0, V and the scalars to 1e-6), and the plans
 agree with each other to the same bound.  Settings are process-wide; every
@@ -72,10 +72,12 @@ def test_plans_agree_within_the_mixed_bound(shape):
         assert v <= TOL, ("between", k, v)
 
 
+@pytest.mark.parametrize("kinds", [(3,), (2, 3)], ids=["sigma", "vertex_sigma"])
 @pytest.mark.parametrize("nw0", [512, 4096])
-def test_tensor_plan_sigma_slice(nw0):
-    """Plan 2 (tensor cores) for the Sigma slice against plan 0 and the FP64
-    solve, with the tensor plan's error word checked clear."""
+def test_tensor_plan(nw0, kinds):
+    """Plan 2 (tensor cores) for the Sigma slice alone and for the V and
+    Sigma slices, against plan 0 and the FP64 solve, with the tensor plan's
+    error word checked clear."""
     import ctypes as C
 
     from tpsc_conductivity_b200 import _lib
@@ -88,10 +90,9 @@ def test_tensor_plan_sigma_slice(nw0):
     ref = _solve(shape, _lib.FORM_NEWTON)
     out = {}
     try:
-        for kind in range(3):
-            assert lib.tpsc_set_slice_plan(kind, 256, 0) == 0
         for plan in (0, 2):
-            assert lib.tpsc_set_slice_plan(3, 256, plan) == 0
+            for kind in range(4):
+                assert lib.tpsc_set_slice_plan(kind, 256, plan if kind in kinds else 0) == 0
             out[plan] = _solve(shape, _lib.FORM_NEWTON | _lib.FORM_MIXED)
     finally:
         for kind in range(4):
@@ -100,7 +101,7 @@ def test_tensor_plan_sigma_slice(nw0):
     assert word.value == 0
     errs = {plan: _errors(out[plan], ref) for plan in (0, 2)}
     between = _errors(out[2], out[0])
-    print("tensor plan", nw0, json.dumps({str(k): {a: float("%.3g" % b) for a, b in v.items()}
+    print("tensor plan", nw0, kinds, json.dumps({str(k): {a: float("%.3g" % b) for a, b in v.items()}
                                          for k, v in {**errs, "2v0": between}.items()}))
     for plan in (0, 2):
         for k, v in errs[plan].items():

@@ -41,7 +41,11 @@ void set_slice_plan(int kind, int nbk, int plan) {
 bool slice_plan_supported(int kind, int plan, int nbk) {
     if (plan == kSliceFft) return true;
     if (plan == kSliceDirect) return nbk == 33 || nbk == 65 || nbk == 129;
-    return plan == kSliceTensor && kind == kSliceSigma && nbk == 129;
+    // the tensor plan for the Sigma and V slices only: on the G and chi0
+    // slices, whose values have no large near field split off, its 3xTF32
+    // products leave chi0 8e-7 and Sigma 1e-6 to 3e-6 from FP64 (the FFT
+    // plan: 1e-7, 5e-7), outside the mixed form's bound
+    return plan == kSliceTensor && (kind == kSliceSigma || kind == kSliceVertex) && nbk == 129;
 }
 
 // KsT[k][n] = w_k cos(pi k n / H) (rows k <= H) and KdT[k][n] = w_k cos(pi k (2n + 1) / N)

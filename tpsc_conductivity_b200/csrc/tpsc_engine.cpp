@@ -2751,7 +2751,7 @@ int tpsc_set_slice_plan(int kind, int nk0, int plan) {
     if (kind < 0 || kind > 3 || plan < 0 || plan > 2 || !supported_grid(nk0, 16) ||
         !slice_plan_supported(kind, plan, nbk))
         return fail(nullptr, TPSC_ERR_ARG,
-                    "need kind 0..3, plan 0, 1 (nk0 64, 128, 256) or 2 (kind 3, nk0 256) and a supported nk0");
+                    "need kind 0..3, plan 0, 1 (nk0 64, 128, 256) or 2 (kinds 2, 3 at nk0 256) and a supported nk0");
     set_slice_plan(kind, nbk, plan);
     return TPSC_OK;
 }

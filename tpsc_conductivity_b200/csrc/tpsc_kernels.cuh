@@ -439,10 +439,12 @@ void set_slice_plan(int kind, int nbk, int plan);
 bool slice_plan_supported(int kind, int plan, int nbk);
 // the table of the direct plan for a quadrant side nbk (empty where it does not apply)
 void dct_table(int nbk, std::vector<float> &out);
-// the tensor plan (tpsc_tcdct.cu): Sigma slices of the 256 x 256 lattice
+// the tensor plan (tpsc_tcdct.cu): the Sigma and V slices of the 256 x 256 lattice
 void dct_tc_table(int nbk, std::vector<float> &out);
 cudaError_t launch_sigma_slice_tc(const GridDev &g, const float *Grt, const double *V, double *sigt,
                                   cudaStream_t st, const Bp &b = Bp{});
+cudaError_t launch_vertex_q_tc(const GridDev &g, const double *chiq, double *Vr, double U, const double *Usc,
+                               double T, cudaStream_t st, const Bp &b = Bp{});
 // the tensor plan's error word (nonzero after a bounded wait ran out); 0 on success
 int tensor_plan_errors(unsigned *out, bool clear);
 cudaError_t launch_sigma_slice_dct(const GridDev &g, const float *Grt, const double *V, double *sigt,

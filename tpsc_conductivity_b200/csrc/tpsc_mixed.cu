@@ -344,7 +344,8 @@ struct RunCondSlice32 {
 template <int NBK>
 struct RunGslice32 {
     static cudaError_t run(const GridDev *g, float *Grt, double mu0, double T, const Bp *b, cudaStream_t st) {
-        if (slice_plan(kSliceG, NBK) == kSliceDirect && g->dct32) return launch_gslice_dct(*g, Grt, mu0, T, st, *b);
+        const int plan = slice_plan(kSliceG, NBK);
+        if (plan == kSliceDirect && g->dct32) return launch_gslice_dct(*g, Grt, mu0, T, st, *b);
         const size_t sm = Slice32Smem<NBK>::bytes;
         cudaError_t e = set_smem(k_gslice32<NBK>, sm);
         if (e != cudaSuccess) return e;
@@ -358,8 +359,8 @@ template <int NBK>
 struct RunChi0Slice32 {
     static cudaError_t run(const GridDev *g, const float *Grt, double *chirt, double *chiq, const Bp *b,
                            cudaStream_t st) {
-        if (slice_plan(kSliceChi0, NBK) == kSliceDirect && g->dct32)
-            return launch_chi0_slice_dct(*g, Grt, chirt, chiq, st, *b);
+        const int plan = slice_plan(kSliceChi0, NBK);
+        if (plan == kSliceDirect && g->dct32) return launch_chi0_slice_dct(*g, Grt, chirt, chiq, st, *b);
         const size_t sm = Slice32Smem<NBK>::bytes;
         cudaError_t e = set_smem(k_chi0_slice32<NBK>, sm);
         if (e != cudaSuccess) return e;
@@ -373,8 +374,9 @@ template <int NBK>
 struct RunVertexQ32 {
     static cudaError_t run(const GridDev *g, const double *chiq, double *Vr, double U, const double *Usc, double T,
                            const Bp *b, cudaStream_t st) {
-        if (slice_plan(kSliceVertex, NBK) == kSliceDirect && g->dct32)
-            return launch_vertex_q_dct(*g, chiq, Vr, U, Usc, T, st, *b);
+        const int plan = slice_plan(kSliceVertex, NBK);
+        if (plan == kSliceTensor && g->dct_tc) return launch_vertex_q_tc(*g, chiq, Vr, U, Usc, T, st, *b);
+        if (plan == kSliceDirect && g->dct32) return launch_vertex_q_dct(*g, chiq, Vr, U, Usc, T, st, *b);
         const size_t sm = Slice32Smem<NBK>::bytes;
         cudaError_t e = set_smem(k_vertex_q32<NBK>, sm);
         if (e != cudaSuccess) return e;

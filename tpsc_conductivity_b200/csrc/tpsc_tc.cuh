@@ -164,8 +164,8 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
                  : "memory");
 }
 
-// x = hi + lo with hi rounded to TF32 (nearest, ties away); lo = x - hi is
-// exact in FP32 and enters the MMA truncated to TF32
+// x rounded to TF32 (nearest, ties away): the high part of x, and applied to
+// x - hi (exact in FP32) its remainder as the MMA reads it
 __device__ __forceinline__ float tf32_hi(float x) {
     uint32_t h;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));

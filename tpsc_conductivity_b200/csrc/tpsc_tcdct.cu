@@ -115,6 +115,7 @@ struct TcSmem {
     static constexpr uint32_t gst = vst + NVBOX * VBOX * 32;
     static constexpr uint32_t gmax = ((N8 * 4 + 15) & ~15) + 16;  // the cover of a row: at most 12 bytes each side
     static_assert(gst + gmax <= b_end, "raw inputs fit over the B operands");
+    static_assert(vst + 2 * gmax <= b_end && gmax % 16 == 0, "two G rows fit over the B operands");
     static_assert(tbar % 8 == 0, "mbarrier alignment");
     static_assert(bar % 8 == 0, "mbarrier alignment");
     static_assert(DctPlan<64>::REG * 4 <= b_end - b0, "Z fits over the B operands");
@@ -204,28 +205,58 @@ __device__ __forceinline__ GCover g_cover(const float *__restrict__ Grt, int p, 
     const uintptr_t a0 = a & ~(uintptr_t)15, a1 = (a + S::N8 * 4 + 15) & ~(uintptr_t)15;
     return GCover{reinterpret_cast<const unsigned char *>(a0), (uint32_t)(a1 - a0), (int)((a - a0) >> 2)};
 }
+// the kinds of slice the tensor plan transforms (kSliceVertex, kSliceSigma) and
+// their arguments (the pointers are point 0's; a batched launch adds
+// p * arena for point p)
+struct TcArgs {
+    const float *Grt = nullptr;     // Sigma: G(r, tau) in FP32, [j][o]
+    const double *Usc = nullptr;    // V: the device pair (Usp, Uch)
+    const double2 *tw64 = nullptr;  // Sigma: exp(-2 pi i m / 2N), m < 2N
+    double *out = nullptr;          // Sigma: Sigma(k, tau); V: V(r, tau) (column blocks)
+    double normFact = 0.0, U = 0.0;
+    int nw0 = 0;
+};
+template <int KIND>
+__host__ __device__ constexpr int tc_slices(int nw0) {
+    static_assert(KIND == kSliceSigma || KIND == kSliceVertex, "the tensor plan's slice kinds");
+    return KIND == kSliceSigma ? nw0 + 1 : nw0 / 2 + 1;
+}
 // (one thread) the raw inputs of slice j of point p into shared memory, on tbar:
-// V(r, tau_jv) block row by TMA, G(r, tau_j) by one bulk copy
-__device__ __forceinline__ void tc_stage(unsigned char *smem, const void *tmV, const float *__restrict__ Grt,
-                                         int nw0, int p, int j, long long arena) {
+//   Sigma: the V(r, tau_jv) block row by TMA and the G(r, tau_j) row by one bulk copy;
+//   V:     the chi0(q, iq_j) block row by TMA.
+template <int KIND>
+__device__ __forceinline__ void tc_stage(unsigned char *smem, const void *tmIn, const TcArgs &a, int p, int j,
+                                         long long arena) {
     using S = TcSmem;
-    const int nb = nw0 / 2 + 1;
-    const int jv = j < nb ? j : nw0 - j;
+    const int nb = a.nw0 / 2 + 1;
     uint64_t *tbar = reinterpret_cast<uint64_t *>(smem + S::tbar);
-    const GCover gc = g_cover(Grt, p, j, arena);
     fence_async_smem();
-    mbar_expect_tx(tbar, (uint32_t)(S::NVBOX * S::VBOX * 32) + gc.bytes);
+    if constexpr (KIND == kSliceSigma) {
+        const int jv = j < nb ? j : a.nw0 - j;
+        const GCover gc = g_cover(a.Grt, p, j, arena);
+        mbar_expect_tx(tbar, (uint32_t)(S::NVBOX * S::VBOX * 32) + gc.bytes);
 #pragma unroll 1
-    for (int c = 0; c < S::NVBOX; ++c) tma_load_4d(smem + S::vst + c * S::VBOX * 32, tmV, 0, jv, c * S::VBOX, p, tbar);
-    bulk_load(smem + S::gst, gc.src, gc.bytes, tbar);
+        for (int c = 0; c < S::NVBOX; ++c)
+            tma_load_4d(smem + S::vst + c * S::VBOX * 32, tmIn, 0, jv, c * S::VBOX, p, tbar);
+        bulk_load(smem + S::gst, gc.src, gc.bytes, tbar);
+    } else if constexpr (KIND == kSliceVertex) {
+        mbar_expect_tx(tbar, (uint32_t)(S::NVBOX * S::VBOX * 32));
+#pragma unroll 1
+        for (int c = 0; c < S::NVBOX; ++c)
+            tma_load_4d(smem + S::vst + c * S::VBOX * 32, tmIn, 0, j, c * S::VBOX, p, tbar);
+    }
 }
 
 __device__ __forceinline__ int oct_of(int l, int m) { return l * (l + 1) / 2 + m; }
 
+// point p's scalar `slot` of a batched launch, or v for a plain launch
+__device__ __forceinline__ double tc_par(const Bp &b, int slot, double v, int p) {
+    return b.pp ? tc_point(b.pp, b.arena, p)[slot] : v;
+}
+
+template <int KIND>
 __global__ void __launch_bounds__(kTcThreads, 1)
-    k_sigma_slice_tc(const __grid_constant__ CUtensorMap tmV, const float *__restrict__ Grt,
-                     const float *__restrict__ tab, const double2 *__restrict__ tw64, int nw0,
-                     double *__restrict__ sigt, Bp b) {
+    k_slice_tc(const __grid_constant__ CUtensorMap tmIn, const float *__restrict__ tab, const TcArgs a, Bp b) {
     using S = TcSmem;
     constexpr int H = 64, N8 = S::N8, NBK = S::NBK, L = 256, R = S::R, NOCT = S::NOCT;
     constexpr int PER = (N8 + kTcThreads - 1) / kTcThreads;
@@ -257,20 +288,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     for (int i = tid; i < (int)(S::tab_bytes / 16); i += blockDim.x)
         cp_async16(smem + 16 * i, reinterpret_cast<const unsigned char *>(tab) + 16 * i);
-    for (int i = tid; i < R * NBK; i += blockDim.x) cf[i] = 2.0 * __ldg(&tw64[((i / NBK + 1) * (i % NBK)) % L]).x;
+    if constexpr (KIND == kSliceSigma)
+        for (int i = tid; i < R * NBK; i += blockDim.x)
+            cf[i] = 2.0 * __ldg(&a.tw64[((i / NBK + 1) * (i % NBK)) % L]).x;
     cp_async_wait_all();
-    const long long items = (long long)(nw0 + 1) * b.P;
+    const int nw0 = a.nw0, nb = nw0 / 2 + 1, ns = tc_slices<KIND>(nw0);
+    const long long items = (long long)ns * b.P;
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     if (tid == 0 && blockIdx.x < items)
-        tc_stage(smem, &tmV, Grt, nw0, (int)(blockIdx.x / (nw0 + 1)), (int)(blockIdx.x % (nw0 + 1)), b.arena);
+        tc_stage<KIND>(smem, &tmIn, a, (int)(blockIdx.x / ns), (int)(blockIdx.x % ns), b.arena);
     const uint32_t tmem = *s_tmem;
     uint32_t phase = 0, tphase = 0;
 
     for (long long it = blockIdx.x; it < items; it += gridDim.x) {
-        const int p = (int)(it / (nw0 + 1)), j = (int)(it % (nw0 + 1));
-        double *out = tc_point(sigt, b.arena, p);
+        const int p = (int)(it / ns), j = (int)(it % ns);
         const long long nx = it + gridDim.x;
         __syncthreads();  // the previous slice's reads of xs are done
         // 1. this slice's raw inputs (copied in during the previous slice's output)
@@ -278,14 +311,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         __syncthreads();
         if (*s_err) break;
         tphase ^= 1;
-        if (nx < items) {
-            const int pn = (int)(nx / (nw0 + 1)), jn = (int)(nx % (nw0 + 1));
-            prefetch_l2_range(tc_point(Grt, b.arena, pn) + (size_t)jn * N8, (size_t)N8 * sizeof(float));
+        if (KIND == kSliceSigma && nx < items) {
+            const int pn = (int)(nx / ns), jn = (int)(nx % ns);
+            prefetch_l2_range(tc_point(a.Grt, b.arena, pn) + (size_t)jn * N8, (size_t)N8 * sizeof(float));
         }
-        // 2. x = G V
-        {
+        // 2. the slice's octant values, formed in FP64 and rounded once
+        if constexpr (KIND == kSliceSigma) {
+            // x = G V; the near field stays in FP64
             const double *vs = reinterpret_cast<const double *>(smem + S::vst);
-            const float *gs = reinterpret_cast<const float *>(smem + S::gst) + g_cover(Grt, p, j, b.arena).shift;
+            const float *gs = reinterpret_cast<const float *>(smem + S::gst) + g_cover(a.Grt, p, j, b.arena).shift;
 #pragma unroll
             for (int i = 0; i < PER; ++i) {
                 const int o = tid + i * kTcThreads;
@@ -293,6 +327,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const double x = (double)gs[o] * vs[o];
                     if (o < NOCT) xn[o] = x;
                     xs[o] = o < NOCT ? 0.0f : (float)x;
+                }
+            }
+        } else if constexpr (KIND == kSliceVertex) {
+            // V(q, iq_j) from chi0(q, iq_j): with a = Usp/2, b = Uch/2 one division per point
+            const double *cs = reinterpret_cast<const double *>(smem + S::vst);
+            const double *us = tc_point(a.Usc, b.arena, p);
+            const double Usp = us[0], Uch = us[1];
+            const double nf = tc_par(b, kPpNormFact, a.normFact, p), Up = tc_par(b, kPpU, a.U, p);
+#pragma unroll
+            for (int i = 0; i < PER; ++i) {
+                const int o = tid + i * kTcThreads;
+                if (o < N8) {
+                    const double c0 = cs[o];
+                    const double as = 0.5 * Usp, bc = 0.5 * Uch;
+                    const double ds = 1.0 - as * c0, dc = 1.0 + bc * c0;
+                    const double num = 3.0 * Usp * as * dc - Uch * bc * ds;
+                    xs[o] = (float)(0.125 * nf * Up * c0 * c0 * num / (ds * dc));
                 }
             }
         }
@@ -329,19 +380,21 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             issue_stage<false>(sdesc0, tmem);
             mma_commit(bar);
         }
-        // (while the tensor cores run) near field: u_a(k2) = sum_c w_c x(a, c) cos(pi c k2 / N)
-        for (int i = tid; i < (R + 1) * NBK; i += blockDim.x) {
-            const int a = i / NBK, k2 = i % NBK;
-            double cs[R + 1];
-            cheb_cos<R>(__ldg(&tw64[k2]).x, cs);
-            double acc = 0.0;
+        // (while the tensor cores run) near field of the Sigma slice:
+        // u_r(k2) = sum_c w_c x(r, c) cos(pi c k2 / N)
+        if constexpr (KIND == kSliceSigma)
+            for (int i = tid; i < (R + 1) * NBK; i += blockDim.x) {
+                const int r = i / NBK, k2 = i % NBK;
+                double cs[R + 1];
+                cheb_cos<R>(__ldg(&a.tw64[k2]).x, cs);
+                double acc = 0.0;
 #pragma unroll
-            for (int c = 0; c <= R; ++c) {
-                const int hi = a > c ? a : c, lo = a > c ? c : a;
-                acc = fma((c == 0 ? 1.0 : 2.0) * xn[lo + hi * (hi + 1) / 2], cs[c], acc);
+                for (int c = 0; c <= R; ++c) {
+                    const int hi = r > c ? r : c, lo = r > c ? c : r;
+                    acc = fma((c == 0 ? 1.0 : 2.0) * xn[lo + hi * (hi + 1) / 2], cs[c], acc);
+                }
+                u[i] = acc;
             }
-            u[i] = acc;
-        }
         // column 64 of T_ee: t64[m] = sum_{k<=64} SS[m][k] Ks[64][k], m <= 64;
         // four threads per m (warps 2..10), k = sub, sub + 4, ...
         if (warp >= 2 && warp <= 10) {
@@ -466,16 +519,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         __syncthreads();
         // the next slice's raw inputs (the B operands are free again)
         if (tid == 0 && nx < items)
-            tc_stage(smem, &tmV, Grt, nw0, (int)(nx / (nw0 + 1)), (int)(nx % (nw0 + 1)), b.arena);
+            tc_stage<KIND>(smem, &tmIn, a, (int)(nx / ns), (int)(nx % ns), b.arena);
         // 7. output (consecutive lanes on consecutive octant points: a warp
         // writes whole 32-byte blocks of the column-block layout)
-        for (int o = tid; o < N8; o += blockDim.x) {
-            int l, m;
-            oct_lm(o, l, m);
-            double nf = u[m];
+        if constexpr (KIND == kSliceSigma) {
+            double *out = tc_point(a.out, b.arena, p);
+            for (int o = tid; o < N8; o += blockDim.x) {
+                int l, m;
+                oct_lm(o, l, m);
+                double nf = u[m];
 #pragma unroll
-            for (int a = 1; a <= R; ++a) nf = fma(cf[(a - 1) * NBK + l], u[a * NBK + m], nf);
-            out[bidx(j, o, nw0 + 1)] = (double)xs[o] + nf;
+                for (int r = 1; r <= R; ++r) nf = fma(cf[(r - 1) * NBK + l], u[r * NBK + m], nf);
+                out[bidx(j, o, nw0 + 1)] = (double)xs[o] + nf;
+            }
+        } else {
+            double *out = tc_point(a.out, b.arena, p);
+            for (int o = tid; o < N8; o += blockDim.x) out[bidx(j, o, nb)] = xs[o];
         }
     }
     if (*s_err) {
@@ -511,13 +570,10 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     });
     return fn;
 }
-}  // namespace
 
-cudaError_t launch_sigma_slice_tc(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st,
-                                  const Bp &b) {
-    if (g.nbk != 129 || !g.dct_tc) return cudaErrorInvalidValue;
-    // V as (4 doubles of a column block, row j, column block, point): box
-    // (4, 1, 256, 1) = one row of 256 column blocks, 8 KB
+// a 4-D tensor map over a column-block array of nb rows (4 doubles of a block,
+// row, block, point): box (4, 1, 256, 1) = one row of 256 column blocks, 8 KB
+cudaError_t block_row_map(const double *base, const GridDev &g, const Bp &b, CUtensorMap *m) {
     PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
     if (!encode) return cudaErrorNotSupported;
     const cuuint64_t nblk = (cuuint64_t)g.n8p / 4;
@@ -525,20 +581,53 @@ cudaError_t launch_sigma_slice_tc(const GridDev &g, const float *Grt, const doub
     const cuuint64_t strides[3] = {32, (cuuint64_t)g.nb * 32,
                                    b.P > 1 ? (cuuint64_t)b.arena : (cuuint64_t)g.nb * 32 * nblk};
     const cuuint32_t box[4] = {4, 1, TcSmem::VBOX, 1}, estr[4] = {1, 1, 1, 1};
-    CUtensorMap tmV;
-    if (encode(&tmV, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double *>(V), dims, strides, box, estr,
+    if (encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double *>(base), dims, strides, box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return cudaErrorInvalidValue;
+    return cudaSuccess;
+}
+
+template <int KIND>
+cudaError_t run_slice_tc(const GridDev &g, const CUtensorMap &m, const TcArgs &a, const Bp &b, cudaStream_t st) {
+    if (g.nbk != 129 || !g.dct_tc) return cudaErrorInvalidValue;
     const size_t sm = TcSmem::bytes;
-    cudaError_t e = set_smem(k_sigma_slice_tc, sm);
+    cudaError_t e = set_smem(k_slice_tc<KIND>, sm);
     if (e != cudaSuccess) return e;
-    const int ctas = resident_ctas(k_sigma_slice_tc, kTcThreads, sm);
+    const int ctas = resident_ctas(k_slice_tc<KIND>, kTcThreads, sm);
     if (ctas <= 0) return cudaErrorInvalidConfiguration;
-    const long long items = (long long)(g.nw0 + 1) * b.P;
+    const long long items = (long long)tc_slices<KIND>(g.nw0) * b.P;
     const int grid = (int)(items < ctas ? items : ctas);
-    k_sigma_slice_tc<<<grid, kTcThreads, sm, st>>>(tmV, Grt, g.dct_tc, g.tw_k, g.nw0, sigt, b);
+    k_slice_tc<KIND><<<grid, kTcThreads, sm, st>>>(m, g.dct_tc, a, b);
     return launched();
+}
+}  // namespace
+
+cudaError_t launch_sigma_slice_tc(const GridDev &g, const float *Grt, const double *V, double *sigt, cudaStream_t st,
+                                  const Bp &b) {
+    CUtensorMap m;
+    cudaError_t e = block_row_map(V, g, b, &m);
+    if (e != cudaSuccess) return e;
+    TcArgs a;
+    a.Grt = Grt;
+    a.tw64 = g.tw_k;
+    a.out = sigt;
+    a.nw0 = g.nw0;
+    return run_slice_tc<kSliceSigma>(g, m, a, b, st);
+}
+
+cudaError_t launch_vertex_q_tc(const GridDev &g, const double *chiq, double *Vr, double U, const double *Usc,
+                               double T, cudaStream_t st, const Bp &b) {
+    CUtensorMap m;
+    cudaError_t e = block_row_map(chiq, g, b, &m);
+    if (e != cudaSuccess) return e;
+    TcArgs a;
+    a.Usc = Usc;
+    a.normFact = T / ((double)g.nk0 * g.nk0);
+    a.U = U;
+    a.out = Vr;
+    a.nw0 = g.nw0;
+    return run_slice_tc<kSliceVertex>(g, m, a, b, st);
 }
 
 // the error word of the tensor plan's kernels: nonzero once an mbarrier wait
