@@ -144,3 +144,49 @@ def test_slice_plan_tuner_keeps_the_fastest_and_the_results():
             assert lib.tpsc_set_slice_plan(kind, nk0, defaults[kind]) == 0
     for k, v in _errors(out, ref).items():
         assert v <= TOL, (k, v)
+
+
+def test_tensor_plan_in_batched_points():
+    """The tensor plan's kernels over the points of a batched launch (one
+    launch per stage over every point of a shape group, the TMA tensor maps
+    spanning the points' arenas) give each point's one-point solve with the
+    same plans to 1e-11."""
+    import ctypes as C
+
+    from tpsc_conductivity_b200 import _lib
+    from tpsc_conductivity_b200.api import Context, Green
+
+    lib = _lib.load()
+    defaults = [lib.tpsc_get_slice_plan(k, 256) for k in range(4)]
+    P = np.array([[256, 512, 0.875, 0.05, -0.15, 0.0, 0.0, 4.0],
+                  [256, 512, 0.9, 0.08, -0.1, 0.0, 0.0, 3.0],
+                  [256, 512, 0.8, 0.06, -0.2, 0.0, 0.0, 5.0]], dtype=np.float64)
+    names = list(_lib.SCALARS)
+    try:
+        for kind in range(4):
+            assert lib.tpsc_set_slice_plan(kind, 256, 2 if kind >= 2 else 0) == 0
+        ctx = Context()
+        n = P.shape[0]
+        res = np.zeros((n, len(names)))
+        st = np.zeros(n, dtype=np.int32)
+        ms = np.zeros(1)
+        ctx.call("tpsc_solve_points", n, P.ctypes.data_as(C.POINTER(C.c_double)),
+                 res.ctypes.data_as(C.POINTER(C.c_double)), st.ctypes.data_as(C.POINTER(C.c_int)),
+                 ms.ctypes.data_as(C.POINTER(C.c_double)))
+        ctx.close()
+        assert np.all(st == 0), st
+        for i in range(n):
+            nk0, Nw0, dn, T, tp, tpp, t3, U = P[i]
+            g = Green(int(nk0), int(Nw0), dn, T, 0.1, (tp, tpp, t3, U))
+            g.set_form(_lib.FORM_NEWTON | _lib.FORM_MIXED)
+            g.solve()
+            ref = g.scalars()
+            g.ctx.close()
+            for k in ("Usp", "Uch", "mu", "dblOcc", "Sigma_inf", "trSG"):
+                a, b = res[i, names.index(k)], ref[k]
+                assert abs(a - b) <= 1e-11 * max(abs(b), 1e-3), (i, k, a, b)
+        word = C.c_uint(0)
+        assert lib.tpsc_tensor_plan_errors(C.byref(word), 1) == 0 and word.value == 0
+    finally:
+        for kind in range(4):
+            assert lib.tpsc_set_slice_plan(kind, 256, defaults[kind]) == 0
