@@ -7,7 +7,7 @@
 // same safeguarded Newton step, until both roots have converged.  One launch
 // and one readback replace a host round trip per evaluation.
 //
-// The grid barrier spins on a generation counter with an iteration bound:
+// The grid barrier spins on a generation counter with a wall-time bound:
 // the launch is cooperative (every block resident), so the bound only ends
 // a wait that could not otherwise end; it then sets the error flag, every
 // block leaves, and the host reports the failure.
@@ -23,12 +23,19 @@ namespace tpsc {
 namespace {
 
 constexpr int kRootThreads = 256;
-// spins of a barrier wait before it gives up: each spin sleeps __nanosleep(64),
-// which takes ~0.4 us on a B200 (2^24 spins measured 6.4 s), so ~1.6 s
-constexpr long long kBarrierSpins = 1LL << 22;
+// wall time a barrier wait spins before it gives up (%globaltimer, ns)
+constexpr unsigned long long kBarrierNs = 1500000000ull;
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
 
 // bar[0]: arrivals, bar[1]: generation.  Returns false (and sets *err) when
-// the wait ran out or another block had already failed.
+// the wait ran out or another block had already failed.  The waiting thread
+// polls the generation word without sleeping: a poll is one L2 round trip,
+// so the barrier opens within about that of the last arrival.
 __device__ bool grid_sync(unsigned *bar, int *err) {
     __shared__ int s_ok;
     __syncthreads();
@@ -42,13 +49,13 @@ __device__ bool grid_sync(unsigned *bar, int *err) {
             __threadfence();
             atomicAdd(bar + 1, 1u);
         } else {
-            for (long long spin = 0; *gen == g0; ++spin) {
-                if (spin > kBarrierSpins || *(volatile int *)err) {
+            const unsigned long long t0 = globaltimer_ns();
+            while (*gen == g0) {
+                if (*(volatile int *)err || globaltimer_ns() - t0 > kBarrierNs) {
                     atomicExch(err, 1);
                     ok = 0;
                     break;
                 }
-                __nanosleep(64);
             }
         }
         __threadfence();
@@ -57,6 +64,35 @@ __device__ bool grid_sync(unsigned *bar, int *err) {
     __syncthreads();
     return s_ok;
 }
+
+// Grid-stride walk over the items it = blk * nj + j (blk a column block,
+// j < nj a frequency): both indices are stepped by the stride's quotient and
+// remainder, so that no item pays a 64-bit division.  nj <= 0: no items.
+struct GridWalk {
+    int blk, j, dblk, dj, nj;
+    __device__ explicit GridWalk(int nj_) : nj(nj_) {
+        if (nj <= 0) {
+            blk = 0x7fffffff;
+            j = dblk = dj = 0;
+            return;
+        }
+        const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        const long long stride = (long long)gridDim.x * blockDim.x;
+        blk = (int)(first / nj);
+        j = (int)(first - (long long)blk * nj);
+        dblk = (int)(stride / nj);
+        dj = (int)(stride - (long long)dblk * nj);
+    }
+    // the item after (b, jj) in this thread's walk
+    __device__ void after(int b, int jj, int &nb, int &nj2) const {
+        nb = b + dblk;
+        nj2 = jj + dj;
+        if (nj2 >= nj) {
+            nj2 -= nj;
+            ++nb;
+        }
+    }
+};
 
 struct RootCtl {
     double x, lo, hi, prev_step, root;
@@ -205,29 +241,39 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
         __syncthreads();
 #pragma unroll 1
         while (!sc.done) {
-            if (threadIdx.x == 0) {
+            if (threadIdx.x < 32) {
                 const double ah = fabs(phase == 0 ? spin_us(sc.x, hi_sp) : sc.x) / 2.0;
-                // first frequency of the series (cmax_suf does not increase)
+                // first frequency of the series (cmax_suf does not increase):
+                // every j < lo is below the cut and every j >= hi above it;
+                // a round probes 32 points of [lo, hi) and keeps one step of it
                 int lo = 0, hi = a.nb;
-                while (lo < hi) {
-                    const int mid = (lo + hi) / 2;
-                    if (ah * a.cmax_suf[mid] >= kMomSeriesMax)
-                        lo = mid + 1;
-                    else
-                        hi = mid;
+                while (hi > lo) {
+                    const int step = (hi - lo + 31) / 32;
+                    const int q = lo + ((int)threadIdx.x + 1) * step - 1;
+                    const bool below = q < hi && ah * a.cmax_suf[q] >= kMomSeriesMax;
+                    const int t = __popc(__ballot_sync(0xffffffffu, below));
+                    const int qt = lo + (t + 1) * step - 1;
+                    if (t < 32 && qt < hi) hi = qt;
+                    lo += t * step;
                 }
-                s_jdir = lo;
-                s_tail = ah * a.tailm[kMomP] >= kMomSeriesMax;
+                if (threadIdx.x == 0) {
+                    s_jdir = lo;
+                    s_tail = ah * a.tailm[kMomP] >= kMomSeriesMax;
+                }
             }
             __syncthreads();
             const double x = phase == 0 ? spin_us(sc.x, hi_sp) : sc.x, hu = sgn * x / 2.0;
             const int jdir = s_jdir;
             double v = 0.0, dv = 0.0;
-            const long long total = (long long)a.nblk * jdir;
-            for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < total;
-                 it += (long long)gridDim.x * blockDim.x) {
-                const int blk = (int)(it / jdir), j = (int)(it - (long long)blk * jdir);
-                const double4 xq = a.chiq[(size_t)blk * a.nb + j];
+            // the next item's chi0 row is loaded before this item's arithmetic
+            const GridWalk walk(jdir);
+            int blk = walk.blk, j = walk.j;
+            double4 xn = blk < a.nblk ? a.chiq[(size_t)blk * a.nb + j] : make_double4(0.0, 0.0, 0.0, 0.0);
+            while (blk < a.nblk) {
+                const double4 xq = xn;
+                int nb, nj;
+                walk.after(blk, j, nb, nj);
+                if (nb < a.nblk) xn = a.chiq[(size_t)nb * a.nb + nj];
                 const double4 w = reinterpret_cast<const double4 *>(a.w16)[blk];
                 const double f = j == 0 ? 0.5 : 1.0;
                 const double xs[4] = {xq.x, xq.y, xq.z, xq.w}, ws[4] = {w.x, w.y, w.z, w.w};
@@ -237,6 +283,8 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
                     v += f * ws[c] * (q - xs[c]);
                     dv += f * ws[c] * q * q;
                 }
+                blk = nb;
+                j = nj;
             }
             dv *= -0.5 * sgn;
             if (s_tail) {
@@ -330,19 +378,30 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
 // error ~1e-6 on it moves Tr(G - G0) by < 1e-12 of its leading term.  The
 // point constants live in shared memory and Tr Sigma G0, its Hartree part and
 // G0 share one reciprocal per (k, n), so that two CTAs fit on an SM.
-// One CTA per column block, per-block partials (block_store).
+//
+// Blocks 0 .. nblk-1 take one column block each over the stored frequencies;
+// the four columns of a row are formed without a branch (a padding column
+// has weight 0 and finite stand-in values), so that their chains interleave.
+// Blocks nblk .. nblk + ceil(nblk / 2) - 1 take the tail, one warp per
+// column, away from the Sigma stream.  Per-block partials (block_store).
 constexpr int kMuMomF64 = 4;
 constexpr int kTailR = 28;           // terms of the tail power series (needs kMuMomP + kTailR < kTailP)
 constexpr double kTailRatio = 0.05;  // series when rho / w_NO < this: terms below 0.05^28 (~1e-36) relative
 static_assert(kMuMomP + kTailR < kTailP, "tail power sums too short");
+constexpr int kMomThreads = 256;
+constexpr int kMomTailCols = kMomThreads / 32;  // columns of a tail block
 
-__global__ void __launch_bounds__(256, 2)
+__host__ __device__ constexpr int sigma_moment_tail_blocks(int nblk) {
+    return (4 * nblk + kMomTailCols - 1) / kMomTailCols;
+}
+
+__global__ void __launch_bounds__(kMomThreads, 2)
     k_sigma_moments(const double2 *__restrict__ S, const double *__restrict__ s2, const double *__restrict__ s3,
                     const double *__restrict__ s4, const double *__restrict__ sinfp, const double *__restrict__ ek,
                     const double *__restrict__ w16, const double *__restrict__ tailP, int nw0, double mu0,
-                    double T, double nk02, int jc, double *partial, Bp b) {
+                    double T, double nk02, int jc, int nblk, double *partial, Bp b) {
     constexpr int NV = kSigmaMomNV, P64 = kMuMomF64, P32 = kMuMomP - kMuMomF64;
-    __shared__ double cw[4], cx[4], c2[4], c3[4], c4[4];
+    __shared__ double cw[4], cx[4], c2[4], c3[4];
     S = at(S, b.arena);
     s2 = at(s2, b.arena);
     s3 = at(s3, b.arena);
@@ -354,20 +413,9 @@ __global__ void __launch_bounds__(256, 2)
     mu0 = bpar(b, kPpMu0, mu0);
     T = bpar(b, kPpT, T);
     jc = (int)bpar(b, kPpJc, (double)jc);
-    const int blk = blockIdx.x, o0 = 4 * blk, NO = nw0 / 2;
+    const int blk = blockIdx.x, NO = nw0 / 2;
     const double sinf = sinfp[0];
     const double pt = 3.141592653589793 * T;
-    if (threadIdx.x < 4) {
-        const int c = threadIdx.x;
-        const double w = w16[o0 + c];
-        const bool ok = w != 0.0;
-        cw[c] = w;
-        cx[c] = ok ? ek[o0 + c] - mu0 : 0.0;
-        c2[c] = ok ? s2[o0 + c] : 0.0;
-        c3[c] = ok ? s3[o0 + c] : 0.0;
-        c4[c] = ok ? s4[o0 + c] : 0.0;
-    }
-    __syncthreads();
     double tsg = 0.0, har = 0.0, g0 = 0.0;
     double m64[2 * P64];
     float m32[2 * P32];
@@ -401,54 +449,87 @@ __global__ void __launch_bounds__(256, 2)
         const double zx = -x - rS, zy = wn - iS;
         moments_rr(zx, zy, 1.0 / (zx * zx + zy * zy), x, w, inv);
     };
-    const double4 *row = reinterpret_cast<const double4 *>(S + (size_t)blk * 4 * NO);
-    for (int j = threadIdx.x; j < NO; j += blockDim.x) {
-        const double wn = (2 * j + 1) * pt, i1 = 1.0 / wn;
-        const double4 p = ld_stream4(&row[2 * j]), q = ld_stream4(&row[2 * j + 1]);
-        const double2 sv[4] = {make_double2(p.x, p.y), make_double2(p.z, p.w), make_double2(q.x, q.y),
-                               make_double2(q.z, q.w)};
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const double w = cw[c];
-            if (w == 0.0) continue;
-            double rS, iS;
-            sigma_full(i1, sinf, c2[c], c3[c], sv[c], rS, iS);
-            const double x = cx[c];
-            const double b = wn * wn + x * x;
+    double fermi = 0.0;  // traceSelfG's Fermi-function term, threads 0..3 of a stored-frequency block
+    if (blk < nblk) {
+        const int o0 = 4 * blk;
+        if (threadIdx.x < 4) {
+            // a padding column: weight 0, x = 1 and Sigma's coefficients 0,
+            // so that |z| and w_n^2 + x^2 stay away from 0 and its terms are 0
+            const int c = threadIdx.x;
+            const double w = w16[o0 + c];
+            const bool ok = w != 0.0;
+            cw[c] = w;
+            cx[c] = ok ? ek[o0 + c] - mu0 : 1.0;
+            c2[c] = ok ? s2[o0 + c] : 0.0;
+            c3[c] = ok ? s3[o0 + c] : 0.0;
+        }
+        __syncthreads();
+        const double4 *row = reinterpret_cast<const double4 *>(S + (size_t)blk * 4 * NO);
+        for (int j = threadIdx.x; j < NO; j += blockDim.x) {
+            const double wn = (2 * j + 1) * pt, i1 = 1.0 / wn;
+            const double4 p = ld_stream4(&row[2 * j]), q = ld_stream4(&row[2 * j + 1]);
+            const double2 sv[4] = {make_double2(p.x, p.y), make_double2(p.z, p.w), make_double2(q.x, q.y),
+                                   make_double2(q.z, q.w)};
             if (j >= jc) {
-                // one reciprocal for 1/(w_n^2 + x^2) and 1/|z|^2
-                const double zx = -x - rS, zy = wn - iS, a = zx * zx + zy * zy;
-                const double r = 1.0 / (a * b), inv = r * a;
-                tsg += w * inv * (rS * (-x) + iS * wn);
-                har += w * inv;
-                moments_rr(zx, zy, r * b, x, w, inv);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const double w = cw[c], x = cx[c];
+                    const double2 s = w != 0.0 ? sv[c] : make_double2(0.0, 0.0);
+                    double rS, iS;
+                    sigma_full(i1, sinf, c2[c], c3[c], s, rS, iS);
+                    // one reciprocal for 1/(w_n^2 + x^2) and 1/|z|^2
+                    const double b = wn * wn + x * x;
+                    const double zx = -x - rS, zy = wn - iS, a = zx * zx + zy * zy;
+                    const double r = 1.0 / (a * b), inv = r * a;
+                    tsg += w * inv * (rS * (-x) + iS * wn);
+                    har += w * inv;
+                    moments_rr(zx, zy, r * b, x, w, inv);
+                }
             } else {
-                const double inv = 1.0 / b;
-                tsg += w * inv * (rS * (-x) + iS * wn);
-                har += w * inv;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const double w = cw[c], x = cx[c];
+                    const double2 s = w != 0.0 ? sv[c] : make_double2(0.0, 0.0);
+                    double rS, iS;
+                    sigma_full(i1, sinf, c2[c], c3[c], s, rS, iS);
+                    const double inv = 1.0 / (wn * wn + x * x);
+                    tsg += w * inv * (rS * (-x) + iS * wn);
+                    har += w * inv;
+                }
             }
         }
-    }
-    // The tail n = NO .. 2 NO (asymptotic Sigma), warp c for column c: with
-    // u = 1/(i w_n), z^-1 = u / (1 - q(u)), q(u) = x u + Sinf u^2 + C2 u^3 +
-    // C3 u^4 + C4 u^5 (real coefficients), and h^(p) the coefficients of
-    // (1 - q)^-p,
-    //   sum_tail z^-p = sum_r h^(p)_r (-i)^(p+r) P_(p+r),
-    //   sum_tail Re 1/(i w_n - x) = -x sum_k (-x^2)^k P_(2k+2),
-    // P_p = sum_tail w_n^-p (tailP).  (1 - q)^-p obeys H' (1 - q) = p q' H, so
-    //   R h_R = sum_{s=1..5} q_s h_(R-s) (R - s + p s),   h_0 = 1:
-    // lane p - 1 runs the recurrence of moment m = p - 1 in registers.  The
-    // terms fall like (rho / w_NO)^r, rho a bound on q's root radius; above
-    // kTailRatio the warp sums term by term.
-    {
-        __shared__ double tP[kTailP];
-        for (int k = threadIdx.x; k < kTailP; k += blockDim.x) tP[k] = tailP[k];
-        __syncthreads();
+        // traceSelfG's Fermi-function term per octant point
+        if (threadIdx.x < 4) {
+            const int c = threadIdx.x;
+            const double w8 = 0.5 * cw[c];
+            if (w8 != 0.0) {
+                const double x = cx[c];
+                if (fabs(x) > 1.0e-12) {
+                    fermi = w8 * sinf * (1.0 / (exp(x / T) + 1.0) - 0.5) / x / nk02;
+                } else {
+                    const double ex = (x < 0) ? exp(x / T) : exp(-x / T);
+                    fermi = -w8 * sinf * ex / ((ex + 1.0) * (ex + 1.0) * nk02 * T);
+                }
+            }
+        }
+    } else {
+        // The tail n = NO .. 2 NO (asymptotic Sigma), warp `warp` for column o:
+        // with u = 1/(i w_n), z^-1 = u / (1 - q(u)), q(u) = x u + Sinf u^2 +
+        // C2 u^3 + C3 u^4 + C4 u^5 (real coefficients), and h^(p) the
+        // coefficients of (1 - q)^-p,
+        //   sum_tail z^-p = sum_r h^(p)_r (-i)^(p+r) P_(p+r),
+        //   sum_tail Re 1/(i w_n - x) = -x sum_k (-x^2)^k P_(2k+2),
+        // P_p = sum_tail w_n^-p (tailP).  (1 - q)^-p obeys H' (1 - q) = p q' H,
+        // so R h_R = sum_{s=1..5} q_s h_(R-s) (R - s + p s),   h_0 = 1:
+        // lane p - 1 runs the recurrence of moment m = p - 1 in registers.  The
+        // terms fall like (rho / w_NO)^r, rho a bound on q's root radius; above
+        // kTailRatio the warp sums term by term.
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if (warp < 4 && cw[warp] != 0.0) {
-            const int c = warp;
-            const double w = cw[c], x = cx[c];
-            const double q1 = x, q2 = sinf, q3 = c2[c], q4 = c3[c], q5 = c4[c];
+        const int o = (blk - nblk) * kMomTailCols + warp;
+        const double w = o < 4 * nblk ? __ldg(&w16[o]) : 0.0;
+        if (w != 0.0) {
+            const double x = __ldg(&ek[o]) - mu0;
+            const double q1 = x, q2 = sinf, q3 = __ldg(&s2[o]), q4 = __ldg(&s3[o]), q5 = __ldg(&s4[o]);
             const double rho = fabs(x) + sqrt(fabs(sinf)) + cbrt(fabs(q3)) + sqrt(sqrt(fabs(q4))) + pow(fabs(q5), 0.2);
             const double w_no = (2 * NO + 1) * pt;
             if (rho < kTailRatio * w_no) {
@@ -459,7 +540,7 @@ __global__ void __launch_bounds__(256, 2)
                     double h1 = 1.0, h2 = 0.0, h3 = 0.0, h4 = 0.0, h5 = 0.0;
                     // r = 0 term: (-i)^p P_p
                     auto add = [&](int k, double h) {
-                        const double t = h * tP[k];
+                        const double t = h * __ldg(&tailP[k]);
                         switch (k & 3) {
                             case 0: re += t; break;
                             case 1: im -= t; break;
@@ -468,11 +549,13 @@ __global__ void __launch_bounds__(256, 2)
                         }
                     };
                     add(lane + 1, 1.0);
+                    // unrolled: 1 / R is a constant of each step
+#pragma unroll
                     for (int R = 1; R <= kTailR; ++R) {
                         const double hR = (q1 * h1 * (R - 1 + p) + q2 * h2 * (R - 2 + 2 * p) +
                                            q3 * h3 * (R - 3 + 3 * p) + q4 * h4 * (R - 4 + 4 * p) +
-                                           q5 * h5 * (R - 5 + 5 * p)) /
-                                          R;
+                                           q5 * h5 * (R - 5 + 5 * p)) *
+                                          (1.0 / R);
                         add(lane + 1 + R, hR);
                         h5 = h4;
                         h4 = h3;
@@ -483,7 +566,7 @@ __global__ void __launch_bounds__(256, 2)
                 } else if (lane == kMuMomP) {
                     // G0: -x sum_k (-x^2)^k P_(2k+2)
                     double xp = 1.0;
-                    for (int k = 0; 2 * k + 2 < kTailP; ++k, xp *= -x * x) re += xp * tP[2 * k + 2];
+                    for (int k = 0; 2 * k + 2 < kTailP; ++k, xp *= -x * x) re += xp * __ldg(&tailP[2 * k + 2]);
                     re *= -x;
                 }
 #pragma unroll
@@ -504,34 +587,19 @@ __global__ void __launch_bounds__(256, 2)
             } else {
                 for (int t = lane; t <= NO; t += 32) {
                     const double wn = (2 * (NO + t) + 1) * pt, i1 = 1.0 / wn, i2 = i1 * i1;
-                    moments(wn, -c2[c] * i2 + c4[c] * i2 * i2, -sinf * i1 + c3[c] * i2 * i1, x, w,
-                            1.0 / (wn * wn + x * x));
+                    moments(wn, -q3 * i2 + q5 * i2 * i2, -sinf * i1 + q4 * i2 * i1, x, w, 1.0 / (wn * wn + x * x));
                 }
             }
         }
     }
     double acc[NV];
     acc[0] = tsg * T / nk02;
-    acc[1] = har * sinf * T / nk02;
+    acc[1] = har * sinf * T / nk02 + fermi;
 #pragma unroll
     for (int k = 0; k < 2 * P64; ++k) acc[2 + k] = m64[k];
 #pragma unroll
     for (int k = 0; k < 2 * P32; ++k) acc[2 + 2 * P64 + k] = (double)m32[k];
     acc[2 + 2 * kMuMomP] = g0;
-    // traceSelfG's Fermi-function term per octant point
-    if (threadIdx.x < 4) {
-        const int c = threadIdx.x;
-        const double w8 = 0.5 * cw[c];
-        if (w8 != 0.0) {
-            const double x = cx[c];
-            if (fabs(x) > 1.0e-12) {
-                acc[1] += w8 * sinf * (1.0 / (exp(x / T) + 1.0) - 0.5) / x / nk02;
-            } else {
-                const double ex = (x < 0) ? exp(x / T) : exp(-x / T);
-                acc[1] += -w8 * sinf * ex / ((ex + 1.0) * (ex + 1.0) * nk02 * T);
-            }
-        }
-    }
     block_store<NV>(acc, partial);
 }
 
@@ -547,6 +615,30 @@ struct MuRootArgs {
     double *out;  // mu, evals, ok, Tr Sigma G at mu
     Bp b;         // batched launch: point blockIdx.z
 };
+
+// the four octant points of column block blk at frequency j of
+// green::traceSelfG2 (src/green.cpp:2929-2976): sum w8 2T/nk02 Re[Sigma G]
+// with G = 1/(i w_n - e + mu - Sigma); p, q the block's Sigma row at j
+__device__ __forceinline__ double trsg_row(const MuRootArgs &a, int blk, int j, double4 p, double4 q, double mu,
+                                           double sinf, double pt) {
+    const int o0 = 4 * blk;
+    const double2 sv[4] = {make_double2(p.x, p.y), make_double2(p.z, p.w), make_double2(q.x, q.y),
+                           make_double2(q.z, q.w)};
+    const double wn = (2 * j + 1) * pt, i1 = 1.0 / wn;
+    double v = 0.0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const double w8 = 0.5 * __ldg(&a.w16[o0 + c]);
+        if (w8 == 0.0) continue;
+        double rS, iS;
+        sigma_full(i1, sinf, __ldg(&a.s2[o0 + c]), __ldg(&a.s3[o0 + c]), sv[c], rS, iS);
+        const double ec = __ldg(&a.ek[o0 + c]);
+        const double aa = ec - mu + rS;
+        const double tmp = w8 * a.T * 2 / (a.nk02 * ((wn - iS) * (wn - iS) + aa * aa));
+        v += tmp * (iS * wn - iS * iS - (ec - mu) * rS - rS * rS);
+    }
+    return v;
+}
 
 // find_mu by safeguarded Newton (the host routine newton_root's steps) from
 // mu0 inside [-10, 10] with tolerance 1e-15, one barrier per evaluation as in
@@ -592,10 +684,8 @@ __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
         const bool series = fabs(delta) <= dmax;
         const int jhi = series ? a.jc : NO;
         double v = 0.0, dv = 0.0;
-        const long long total = (long long)a.nblk * jhi;
-        for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < total;
-             it += (long long)gridDim.x * blockDim.x) {
-            const int blk = (int)(it / jhi), j = (int)(it - (long long)blk * jhi);
+        const GridWalk walk(jhi);
+        for (int blk = walk.blk, j = walk.j; blk < a.nblk; walk.after(blk, j, blk, j)) {
             const int o0 = 4 * blk;
             const double4 *row = reinterpret_cast<const double4 *>(a.S + (size_t)blk * 4 * NO);
             const double4 p = ld_stream4(&row[2 * j]), q = ld_stream4(&row[2 * j + 1]);
@@ -666,29 +756,30 @@ __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
         }
         return;
     }
-    // Tr Sigma G at mu over the stored frequencies
+    // Tr Sigma G at mu over the stored frequencies; the next item's Sigma
+    // row is loaded before this item's arithmetic.
     const double mu = sc.root;
     double v = 0.0, dummy = 0.0;
-    const long long total = (long long)a.nblk * NO;
-    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < total;
-         it += (long long)gridDim.x * blockDim.x) {
-        const int blk = (int)(it / NO), j = (int)(it - (long long)blk * NO);
-        const int o0 = 4 * blk;
-        const double4 *row = reinterpret_cast<const double4 *>(a.S + (size_t)blk * 4 * NO);
-        const double4 p = ld_stream4(&row[2 * j]), q = ld_stream4(&row[2 * j + 1]);
-        const double2 sv[4] = {make_double2(p.x, p.y), make_double2(p.z, p.w), make_double2(q.x, q.y),
-                               make_double2(q.z, q.w)};
-        const double wn = (2 * j + 1) * pt, i1 = 1.0 / wn;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const double w8 = 0.5 * __ldg(&a.w16[o0 + c]);
-            if (w8 == 0.0) continue;
-            double rS, iS;
-            sigma_full(i1, sinf, __ldg(&a.s2[o0 + c]), __ldg(&a.s3[o0 + c]), sv[c], rS, iS);
-            const double ec = __ldg(&a.ek[o0 + c]);
-            const double aa = ec - mu + rS;
-            const double tmp = w8 * a.T * 2 / (a.nk02 * ((wn - iS) * (wn - iS) + aa * aa));
-            v += tmp * (iS * wn - iS * iS - (ec - mu) * rS - rS * rS);
+    {
+        const GridWalk walk(NO);
+        int blk = walk.blk, j = walk.j;
+        auto load = [&](int bk, int jj, double4 &p, double4 &q) {
+            const double4 *row = reinterpret_cast<const double4 *>(a.S + (size_t)bk * 4 * NO);
+            p = ld_stream4(&row[2 * jj]);
+            q = ld_stream4(&row[2 * jj + 1]);
+        };
+        double4 p = make_double4(0.0, 0.0, 0.0, 0.0), q = p;
+        if (blk < a.nblk) load(blk, j, p, q);
+        while (blk < a.nblk) {
+            int nb, nj;
+            walk.after(blk, j, nb, nj);
+            double4 pn = p, qn = q;
+            if (nb < a.nblk) load(nb, nj, pn, qn);
+            v += trsg_row(a, blk, j, p, q, mu, sinf, pt);
+            blk = nb;
+            j = nj;
+            p = pn;
+            q = qn;
         }
     }
     double *part = a.partial + (size_t)parity * 2 * kRootMaxBlocks;
@@ -709,7 +800,7 @@ __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
 
 // The barrier's bound, exercised: block `withhold` never arrives (negative:
 // every block does), so every other block's wait runs out after
-// kBarrierSpins and leaves with the error flag set.  words[0..1] the barrier,
+// kBarrierNs and leaves with the error flag set.  words[0..1] the barrier,
 // words[2] the error flag, words[3] the number of blocks that left with it;
 // all zero at launch.
 __global__ void __launch_bounds__(kRootThreads) k_barrier_probe(unsigned *words, int withhold) {
@@ -738,13 +829,14 @@ cudaError_t root_grid(K kernel, int *grid, int cap) {
 cudaError_t launch_sigma_moments(const GridDev &g, const double2 *S, const double *s2, const double *s3,
                                  const double *s4, const double *sinf, double mu0, double T, int jc, Reduce r,
                                  cudaStream_t st, const Bp &b) {
-    const int nblk = g.n8p / 4;
+    const int nblk = g.n8p / 4, nb = nblk + sigma_moment_tail_blocks(nblk);
+    if (nb > kMaxBlocks) return cudaErrorInvalidValue;
     const double nk02 = 4.0 * (g.nbk - 1) * (g.nbk - 1);
-    k_sigma_moments<<<dim3(nblk, 1, b.P), 256, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.tailP, g.nw0, mu0, T,
-                                                         nk02, jc, r.partial, b);
+    k_sigma_moments<<<dim3(nb, 1, b.P), kMomThreads, 0, st>>>(S, s2, s3, s4, sinf, g.ek, g.w16, g.tailP, g.nw0, mu0,
+                                                               T, nk02, jc, nblk, r.partial, b);
     cudaError_t e = launched();
     if (e != cudaSuccess) return e;
-    return finish<kSigmaMomNV>(r, nblk, 0.0, st, b);
+    return finish<kSigmaMomNV>(r, nb, 0.0, st, b);
 }
 
 cudaError_t launch_mu_roots(const GridDev &g, const double2 *S, const double *s2, const double *s3, const double *s4,
