@@ -618,26 +618,40 @@ struct MuRootArgs {
 
 // the four octant points of column block blk at frequency j of
 // green::traceSelfG2 (src/green.cpp:2929-2976): sum w8 2T/nk02 Re[Sigma G]
-// with G = 1/(i w_n - e + mu - Sigma); p, q the block's Sigma row at j
+// with G = 1/(i w_n - e + mu - Sigma); p, q the block's Sigma row at j.  The
+// four fractions K N / A share one division: sum K_c N_c / A_c =
+// [(K0 N0 A1 + K1 N1 A0) A2 A3 + (K2 N2 A3 + K3 N3 A2) A0 A1] / (A0 A1 A2 A3),
+// A_c lies between w_n^2 and ~w_max^2, so the products stay far inside FP64's range.
 __device__ __forceinline__ double trsg_row(const MuRootArgs &a, int blk, int j, double4 p, double4 q, double mu,
                                            double sinf, double pt) {
     const int o0 = 4 * blk;
     const double2 sv[4] = {make_double2(p.x, p.y), make_double2(p.z, p.w), make_double2(q.x, q.y),
                            make_double2(q.z, q.w)};
-    const double wn = (2 * j + 1) * pt, i1 = 1.0 / wn;
-    double v = 0.0;
+    const double wn = (2 * j + 1) * pt, i1 = 1.0 / wn, kT = 2.0 * a.T / a.nk02;
+    double K[4], N[4], A[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
         const double w8 = 0.5 * __ldg(&a.w16[o0 + c]);
-        if (w8 == 0.0) continue;
+        // a padding column: weight 0, and e - mu = 1 with Sigma's
+        // coefficients 0, so that its A >= 1 and its term is 0
+        double e = 1.0, c2 = 0.0, c3 = 0.0;
+        double2 s = make_double2(0.0, 0.0);
+        if (w8 != 0.0) {
+            e = __ldg(&a.ek[o0 + c]) - mu;
+            c2 = __ldg(&a.s2[o0 + c]);
+            c3 = __ldg(&a.s3[o0 + c]);
+            s = sv[c];
+        }
         double rS, iS;
-        sigma_full(i1, sinf, __ldg(&a.s2[o0 + c]), __ldg(&a.s3[o0 + c]), sv[c], rS, iS);
-        const double ec = __ldg(&a.ek[o0 + c]);
-        const double aa = ec - mu + rS;
-        const double tmp = w8 * a.T * 2 / (a.nk02 * ((wn - iS) * (wn - iS) + aa * aa));
-        v += tmp * (iS * wn - iS * iS - (ec - mu) * rS - rS * rS);
+        sigma_full(i1, sinf, c2, c3, s, rS, iS);
+        const double aa = e + rS;
+        A[c] = (wn - iS) * (wn - iS) + aa * aa;
+        N[c] = iS * wn - iS * iS - e * rS - rS * rS;
+        K[c] = w8 * kT;
     }
-    return v;
+    const double P01 = A[0] * A[1], P23 = A[2] * A[3];
+    return ((K[0] * N[0] * A[1] + K[1] * N[1] * A[0]) * P23 + (K[2] * N[2] * A[3] + K[3] * N[3] * A[2]) * P01) /
+           (P01 * P23);
 }
 
 // find_mu by safeguarded Newton (the host routine newton_root's steps) from
