@@ -23,6 +23,7 @@ namespace tpsc {
 namespace {
 
 constexpr int kRootThreads = 256;
+constexpr int kRootMaxNb = 2049;  // bosonic frequencies of Nw0 = 4096
 // wall time a barrier wait spins before it gives up (%globaltimer, ns)
 constexpr unsigned long long kBarrierNs = 1500000000ull;
 
@@ -220,6 +221,11 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
     const double hi_sp = a.chi0max ? 2.0 / a.chi0max[0] - a.hi_off : a.hi_sp;
     __shared__ RootCtl sc;
     __shared__ int s_jdir, s_tail;
+    // cmax_suf and tailm staged once; the series moments of an evaluation's
+    // cut are fetched before its pass and read after the barrier
+    __shared__ double s_cmax[kRootMaxNb], s_tailm[kMomP + 1], s_M[kMomP];
+    for (int j = threadIdx.x; j < a.nb; j += blockDim.x) s_cmax[j] = a.cmax_suf[j];
+    for (int m = threadIdx.x; m <= kMomP; m += blockDim.x) s_tailm[m] = a.tailm[m];
     const int nwmax = a.nb - 1;
     const double tw = 2.0 * 3.141592653589793 * a.T;
     double Usp = 0.0;
@@ -250,15 +256,19 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
                 while (hi > lo) {
                     const int step = (hi - lo + 31) / 32;
                     const int q = lo + ((int)threadIdx.x + 1) * step - 1;
-                    const bool below = q < hi && ah * a.cmax_suf[q] >= kMomSeriesMax;
+                    const bool below = q < hi && ah * s_cmax[q] >= kMomSeriesMax;
                     const int t = __popc(__ballot_sync(0xffffffffu, below));
                     const int qt = lo + (t + 1) * step - 1;
                     if (t < 32 && qt < hi) hi = qt;
                     lo += t * step;
                 }
+                const bool tail = ah * s_tailm[kMomP] >= kMomSeriesMax;
+                if (threadIdx.x < kMomP)
+                    s_M[threadIdx.x] = (lo < a.nb ? a.mom_suf[(size_t)lo * kMomP + threadIdx.x] : 0.0) +
+                                       (tail ? 0.0 : s_tailm[threadIdx.x]);
                 if (threadIdx.x == 0) {
                     s_jdir = lo;
-                    s_tail = ah * a.tailm[kMomP] >= kMomSeriesMax;
+                    s_tail = tail;
                 }
             }
             __syncthreads();
@@ -322,8 +332,7 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
                     double S = 0.0, dS = 0.0, hm1 = 1.0;  // hm1 = (-h)^(m-1)
                     const double h = hu;
                     for (int m = 1; m <= kMomP; ++m) {
-                        const double M = (jdir < a.nb ? a.mom_suf[(size_t)jdir * kMomP + m - 1] : 0.0) +
-                                         (s_tail ? 0.0 : a.tailm[m - 1]);
+                        const double M = s_M[m - 1];
                         S += -h * hm1 * M;
                         dS += -m * hm1 * M;
                         hm1 *= -h;
@@ -899,6 +908,7 @@ cudaError_t launch_sumrule_roots(const GridDev &g, const double *chiq, const dou
                                  const double *mom_suf, const double *cmax_suf, const double *tailm, double T,
                                  double n, double nsr, double U, double hi_sp, RootScratch rs, cudaStream_t st,
                                  const double *chi0max, double hi_off, const Bp &b) {
+    if (g.nb > kRootMaxNb) return cudaErrorInvalidValue;
     int grid = 0;
     cudaError_t e = root_grid(k_sumrule_roots, &grid, rs.max_blocks);
     if (e != cudaSuccess) return e;
