@@ -103,19 +103,27 @@ __device__ void block_store(double (&v)[NV], double *partial) {
     }
 }
 
-// Sum of the per-block partials in a fixed order: warp k adds value k with
-// lane-strided compensated sums and a shuffle tree (deterministic).
+// Sum of the per-block partials in a fixed order: block k adds value k, each
+// thread a lane-strided compensated sum, then a shuffle tree per warp and the
+// warps' totals in order (deterministic).
+constexpr int kFinishThreads = 256;
 template <int NV>
-__global__ void k_finish(const double *partial, int nblocks, double *result, double offset0, Bp bp) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(kFinishThreads) k_finish(const double *partial, int nblocks, double *result,
+                                                           double offset0, Bp bp) {
+    __shared__ double wsum[kFinishThreads / 32];
+    const int k = blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     partial = at(partial, bp.arena);
     result = at(result, bp.arena);
-    for (int k = warp; k < NV; k += blockDim.x >> 5) {
-        KSum acc;
-        for (int b = lane; b < nblocks; b += 32) acc.add(partial[k * kMaxBlocks + b]);
-        double v = acc.value();
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        if (lane == 0) result[k] = v + (k == 0 ? offset0 : 0.0);
+    KSum acc;
+    for (int b = threadIdx.x; b < nblocks; b += kFinishThreads) acc.add(partial[k * kMaxBlocks + b]);
+    double v = acc.value();
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (lane == 0) wsum[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kFinishThreads / 32; ++w) t += wsum[w];
+        result[k] = t + (k == 0 ? offset0 : 0.0);
     }
 }
 
@@ -130,7 +138,7 @@ __global__ void k_max_finish(const double *partial, int nblocks, double *result,
 
 template <int NV>
 cudaError_t finish(Reduce r, int nblocks, double offset0, cudaStream_t st, const Bp &b = Bp{}) {
-    k_finish<NV><<<dim3(1, 1, b.P), 32 * (NV < 32 ? NV : 32), 0, st>>>(r.partial, nblocks, r.result, offset0, b);
+    k_finish<NV><<<dim3(NV, 1, b.P), kFinishThreads, 0, st>>>(r.partial, nblocks, r.result, offset0, b);
     return launched();
 }
 

@@ -1358,13 +1358,27 @@ __global__ void __launch_bounds__(1024)
     k_chi0max(const double *__restrict__ chiq, int n8, int nb, double *result, Bp b) {
     chiq = at(chiq, b.arena);
     result = at(result, b.arena);
-    // values <= 0 never win: the reference's scan starts from chi0max = 0
+    // values <= 0 never win: the reference's scan starts from chi0max = 0.
+    // Each round issues its U loads before any comparison (one latency per
+    // round instead of one per point).
+    constexpr int U = 4;
     MaxPt best{0.0, -1, -1};
-    for (int o = threadIdx.x; o < n8; o += blockDim.x) {
-        int l, m;
-        oct_lm(o, l, m);
-        const MaxPt c{chiq[bidx(0, o, nb)], l, m};
-        if (c.v > 0.0 && better(c, best)) best = c;
+    for (int o0 = threadIdx.x; o0 < n8; o0 += U * blockDim.x) {
+        double v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int o = o0 + u * (int)blockDim.x;
+            v[u] = o < n8 ? chiq[bidx(0, o, nb)] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int o = o0 + u * (int)blockDim.x;
+            if (o >= n8) continue;
+            int l, m;
+            oct_lm(o, l, m);
+            const MaxPt c{v[u], l, m};
+            if (c.v > 0.0 && better(c, best)) best = c;
+        }
     }
     for (int off = 16; off > 0; off >>= 1) best = max_shfl(best, off);
     __shared__ MaxPt w[32];
