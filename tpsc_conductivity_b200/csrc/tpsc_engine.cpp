@@ -1653,7 +1653,8 @@ tpsc_ctx *tpsc_create(int device, int *status) {
                                                  sizeof(double))) != cudaSuccess)
         return bad(e);
     if ((e = cudaMalloc(&ctx->redm.result, 32 * sizeof(double))) != cudaSuccess) return bad(e);
-    if ((e = cudaMalloc(&ctx->roots.partial, 4 * kRootMaxBlocks * sizeof(double))) != cudaSuccess) return bad(e);
+    if ((e = cudaMalloc(&ctx->roots.partial, 2 * kRootVals * kRootMaxBlocks * sizeof(double))) != cudaSuccess)
+        return bad(e);
     if ((e = cudaMalloc(&ctx->roots.bar, 8 * sizeof(unsigned))) != cudaSuccess) return bad(e);
     if ((e = cudaMemsetAsync(ctx->roots.bar, 0, 8 * sizeof(unsigned), ctx->st)) != cudaSuccess) return bad(e);
     ctx->roots.reset_sr = ctx->roots.reset_mu = false;
@@ -2217,7 +2218,7 @@ int group_alloc(tpsc_ctx *ctx, int nk0, int nw0, int P, Group **out) {
                  o_cmax = take(nb * 8), o_msuf = take((nb + 1) * kMomP * 8), o_csuf = take((nb + 1) * 8),
                  o_tailm = take((kMomP + 1) * 8), o_redp = take(4 * kMaxBlocks * 8), o_redt = take(16),
                  o_redmp = take((size_t)std::max(2 * kMomP + 2, kSigmaMomNV) * kMaxBlocks * 8),
-                 o_redmt = take(16), o_rootp = take(4 * kRootMaxBlocks * 8);
+                 o_redmt = take(16), o_rootp = take(2 * kRootVals * kRootMaxBlocks * 8);
     q->arena = (long long)off;
     cudaError_t e = cudaMalloc(&q->base, (size_t)P * off);
     if (e == cudaSuccess) e = cudaMemsetAsync(q->base, 0, (size_t)P * off, ctx->st);

@@ -187,8 +187,9 @@ cudaError_t launch_trace_self_G2(const GridDev &g, const double2 *S, const doubl
 
 // ---- the Newton form's root searches on the device (tpsc_roots.cu) ----------
 constexpr int kRootMaxBlocks = 1024;
+constexpr int kRootVals = 3;  // per-block partials of an evaluation: value and two derivatives
 struct RootScratch {
-    double *partial = nullptr;  // [4 kRootMaxBlocks]
+    double *partial = nullptr;  // [2 kRootVals kRootMaxBlocks]: two parities
     unsigned *bar = nullptr;    // [8]: arrivals, generation, error flag of the sum-rule search (0..2)
                                 //      and of the mu search (4..6)
     double *out = nullptr;      // [8] results

@@ -4,8 +4,9 @@
 // src/chi.cpp:846-876) as one cooperative kernel: every block sums its share
 // of the stored frequencies below the series cut, a grid barrier, then every
 // block adds the partials and the high-frequency moment series and takes the
-// same safeguarded Newton step, until both roots have converged.  One launch
-// and one readback replace a host round trip per evaluation.
+// same safeguarded Halley step (the pass also sums the second derivative),
+// until both roots have converged.  One launch and one readback replace a
+// host round trip per evaluation.
 //
 // The grid barrier spins on a generation counter with a wall-time bound:
 // the launch is cooperative (every block resident), so the bound only ends
@@ -117,32 +118,55 @@ struct SumRootArgs {
     Bp b;             // batched launch: point blockIdx.z, blocks blockIdx.x of gridDim.x per point
 };
 
-// the (value, derivative) pair, summed in a fixed order
-__device__ void block_pair_sum(double &v, double &dv, double *dst) {
-    __shared__ double red[32][2];
+// the value and its derivatives, each summed in a fixed order, into
+// dst[0..kRootVals)
+__device__ void block_root_sums(double v, double dv, double d2v, double *dst) {
+    __shared__ double red[32][kRootVals];
     for (int off = 16; off > 0; off >>= 1) {
         v += __shfl_down_sync(0xffffffffu, v, off);
         dv += __shfl_down_sync(0xffffffffu, dv, off);
+        d2v += __shfl_down_sync(0xffffffffu, d2v, off);
     }
     if ((threadIdx.x & 31) == 0) {
         red[threadIdx.x >> 5][0] = v;
         red[threadIdx.x >> 5][1] = dv;
+        red[threadIdx.x >> 5][2] = d2v;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double a = 0.0, b = 0.0;
+        double a = 0.0, b = 0.0, c = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
             a += red[w][0];
             b += red[w][1];
+            c += red[w][2];
         }
         dst[0] = a;
         dst[1] = b;
+        dst[2] = c;
     }
     __syncthreads();
 }
 
-// one safeguarded Newton update of the host routine newton_root (tpsc_engine.cpp)
-__device__ void newton_update(RootCtl &c, double y, double dy, double tol) {
+// warp 0 adds every block's partials of one evaluation in the same order
+__device__ void grid_root_sums(const double *part, double &pv, double &pd, double &p2) {
+    pv = pd = p2 = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) {
+        pv += __ldcg(&part[kRootVals * b]);
+        pd += __ldcg(&part[kRootVals * b + 1]);
+        p2 += __ldcg(&part[kRootVals * b + 2]);
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        pv += __shfl_down_sync(0xffffffffu, pv, off);
+        pd += __shfl_down_sync(0xffffffffu, pd, off);
+        p2 += __shfl_down_sync(0xffffffffu, p2, off);
+    }
+}
+
+// One safeguarded update with the bracket, bisection fallback and stopping
+// tests of the host routine newton_root (tpsc_engine.cpp).  The step is
+// Halley's, x - 2 y y' / (2 y'^2 - y y''), while |y y''| <= y'^2 (it is then
+// between 2/3 and 2 Newton steps); else, and with d2y = 0, Newton's.
+__device__ void newton_update(RootCtl &c, double y, double dy, double tol, double d2y = 0.0) {
     ++c.nev;
     if (!isfinite(y) || !isfinite(dy)) {
         c.done = 1;
@@ -159,7 +183,11 @@ __device__ void newton_update(RootCtl &c, double y, double dy, double tol) {
     else
         c.lo = fmax(c.lo, c.x);
     const double scale = fmax(1.0, fabs(c.x));
-    double xn = (dy != 0.0) ? c.x - y / dy : 0.5 * (c.lo + c.hi);
+    double xn = 0.5 * (c.lo + c.hi);
+    if (dy != 0.0) {
+        const double yy = y * d2y, dd = dy * dy;
+        xn = (d2y != 0.0 && fabs(yy) <= dd) ? c.x - 2.0 * y * dy / (2.0 * dd - yy) : c.x - y / dy;
+    }
     if (dy != 0.0 && fabs(xn - c.x) <= 1e-14 * scale) {
         c.root = xn;
         c.done = c.ok = 1;
@@ -274,7 +302,9 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
             __syncthreads();
             const double x = phase == 0 ? spin_us(sc.x, hi_sp) : sc.x, hu = sgn * x / 2.0;
             const int jdir = s_jdir;
-            double v = 0.0, dv = 0.0;
+            // v = sum f w (q - x), q = x / (1 + h x), h = sgn U / 2; its U
+            // derivatives: dq/dU = -sgn q^2 / 2, d2q/dU2 = q^3 / 2
+            double v = 0.0, dv = 0.0, d2v = 0.0;
             // the next item's chi0 row is loaded before this item's arithmetic
             const GridWalk walk(jdir);
             int blk = walk.blk, j = walk.j;
@@ -289,14 +319,16 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
                 const double xs[4] = {xq.x, xq.y, xq.z, xq.w}, ws[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
-                    const double q = xs[c] / (1.0 + hu * xs[c]);
-                    v += f * ws[c] * (q - xs[c]);
-                    dv += f * ws[c] * q * q;
+                    const double q = xs[c] / (1.0 + hu * xs[c]), fw = f * ws[c];
+                    v += fw * (q - xs[c]);
+                    dv += fw * q * q;
+                    d2v += fw * q * q * q;
                 }
                 blk = nb;
                 j = nj;
             }
             dv *= -0.5 * sgn;
+            d2v *= 0.5;
             if (s_tail) {
                 // the Matsubara tail term by term (the series does not converge there)
                 for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < a.n8; o += gridDim.x * blockDim.x) {
@@ -310,47 +342,49 @@ __global__ void __launch_bounds__(kRootThreads) k_sumrule_roots(SumRootArgs a) {
                         const double q = xv / (1.0 + hu * xv);
                         v += w * (q - xv);
                         dv += w * (-0.5 * sgn) * q * q;
+                        d2v += w * 0.5 * q * q * q;
                     }
                 }
             }
-            double *part = a.partial + (size_t)parity * 2 * kRootMaxBlocks;
-            block_pair_sum(v, dv, part + 2 * blockIdx.x);
+            double *part = a.partial + (size_t)parity * kRootVals * kRootMaxBlocks;
+            block_root_sums(v, dv, d2v, part + kRootVals * blockIdx.x);
             if (!grid_sync(a.bar, a.err)) return;
             parity ^= 1;
             if (threadIdx.x < 32) {
-                double pv = 0.0, pd = 0.0;
-                for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) {
-                    pv += __ldcg(&part[2 * b]);
-                    pd += __ldcg(&part[2 * b + 1]);
-                }
-                for (int off = 16; off > 0; off >>= 1) {
-                    pv += __shfl_down_sync(0xffffffffu, pv, off);
-                    pd += __shfl_down_sync(0xffffffffu, pd, off);
-                }
+                double pv, pd, p2;
+                grid_root_sums(part, pv, pd, p2);
                 if (threadIdx.x == 0) {
-                    // the series over the frequencies from jdir (and over the tail)
-                    double S = 0.0, dS = 0.0, hm1 = 1.0;  // hm1 = (-h)^(m-1)
+                    // the series over the frequencies from jdir (and over the
+                    // tail), S = sum_m (-h)^m M_m, and its h derivatives
+                    double S = 0.0, dS = 0.0, d2S = 0.0, hm1 = 1.0, hm2 = 0.0;  // (-h)^(m-1), (-h)^(m-2)
                     const double h = hu;
                     for (int m = 1; m <= kMomP; ++m) {
                         const double M = s_M[m - 1];
                         S += -h * hm1 * M;
                         dS += -m * hm1 * M;
+                        d2S += m * (m - 1) * hm2 * M;
+                        hm2 = hm1;
                         hm1 *= -h;
                     }
-                    const double tr = a.scale * (pv + S), dtr = a.scale * (pd + 0.5 * sgn * dS);
+                    // dh/dU = sgn / 2
+                    const double tr = a.scale * (pv + S), dtr = a.scale * (pd + 0.5 * sgn * dS),
+                                 d2tr = a.scale * (p2 + 0.25 * d2S);
                     const double n = a.n, nsr = a.nsr, U = a.U;
-                    double y, dy;
+                    double y, dy, d2y;
                     if (phase == 0) {
                         // chi::sum_rule_sp (src/chi.cpp:833-836)
                         y = tr + n - n * n / 2.0 - nsr + x * nsr * nsr / (2.0 * U);
-                        // d/ds = d/dUs * dUs/ds, dUs/ds = hi e^-s = hi - Us
+                        // d/ds = d/dUs * dUs/ds, dUs/ds = hi e^-s = hi - Us,
+                        // d2Us/ds2 = -(hi - Us)
                         dy = (dtr + nsr * nsr / (2.0 * U)) * (hi_sp - x);
+                        d2y = d2tr * (hi_sp - x) * (hi_sp - x) - dy;
                     } else {
                         // chi::sum_rule_ch (src/chi.cpp:840-843)
                         y = tr + n - n * n / 2.0 - (nsr + Usp * nsr * nsr / (2.0 * U) - nsr * nsr);
                         dy = dtr;
+                        d2y = d2tr;
                     }
-                    newton_update(sc, y, dy, 1e-16);
+                    newton_update(sc, y, dy, 1e-16, d2y);
                 }
             }
             __syncthreads();
@@ -738,20 +772,13 @@ __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
                 trdiff_term(wn, rS, iS, __ldg(&a.ek[o]), a.mu0, pmu, w, v, dv);
             }
         }
-        double *part = a.partial + (size_t)parity * 2 * kRootMaxBlocks;
-        block_pair_sum(v, dv, part + 2 * blockIdx.x);
+        double *part = a.partial + (size_t)parity * kRootVals * kRootMaxBlocks;
+        block_root_sums(v, dv, 0.0, part + kRootVals * blockIdx.x);
         if (!grid_sync(a.bar, a.err)) return;
         parity ^= 1;
         if (threadIdx.x < 32) {
-            double pv = 0.0, pd = 0.0;
-            for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) {
-                pv += __ldcg(&part[2 * b]);
-                pd += __ldcg(&part[2 * b + 1]);
-            }
-            for (int off = 16; off > 0; off >>= 1) {
-                pv += __shfl_down_sync(0xffffffffu, pv, off);
-                pd += __shfl_down_sync(0xffffffffu, pd, off);
-            }
+            double pv, pd, p2;
+            grid_root_sums(part, pv, pd, p2);
             if (threadIdx.x == 0) {
                 if (series) {
                     // Re sum_m (-delta)^m C_m - G0 and its delta derivative
@@ -782,7 +809,7 @@ __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
     // Tr Sigma G at mu over the stored frequencies; the next item's Sigma
     // row is loaded before this item's arithmetic.
     const double mu = sc.root;
-    double v = 0.0, dummy = 0.0;
+    double v = 0.0;
     {
         const GridWalk walk(NO);
         int blk = walk.blk, j = walk.j;
@@ -805,13 +832,12 @@ __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
             q = qn;
         }
     }
-    double *part = a.partial + (size_t)parity * 2 * kRootMaxBlocks;
-    block_pair_sum(v, dummy, part + 2 * blockIdx.x);
+    double *part = a.partial + (size_t)parity * kRootVals * kRootMaxBlocks;
+    block_root_sums(v, 0.0, 0.0, part + kRootVals * blockIdx.x);
     if (!grid_sync(a.bar, a.err)) return;
     if (blockIdx.x == 0 && threadIdx.x < 32) {
-        double pv = 0.0;
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) pv += __ldcg(&part[2 * b]);
-        for (int off = 16; off > 0; off >>= 1) pv += __shfl_down_sync(0xffffffffu, pv, off);
+        double pv, pd, p2;
+        grid_root_sums(part, pv, pd, p2);
         if (threadIdx.x == 0) {
             a.out[0] = mu;
             a.out[1] = sc.nev;
