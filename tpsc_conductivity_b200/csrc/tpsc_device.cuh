@@ -543,6 +543,14 @@ __device__ __forceinline__ void trdiff_term(double wn, double rS, double iS, dou
     v += inv * num;
     dv += inv * (wn * wn - (a + g) * d + num * 2.0 * a / A2);
 }
+// the same with the second derivative: d2/dpmu2 w Re G = 2 w Re G^3, and
+// with z = x + i y (x = -a, y = w_n - Im Sigma), Re conj(z)^3 = x^3 - 3 x y^2
+__device__ __forceinline__ void trdiff_term(double wn, double rS, double iS, double e, double mu0, double pmu,
+                                            double w, double &v, double &dv, double &d2v) {
+    trdiff_term(wn, rS, iS, e, mu0, pmu, w, v, dv);
+    const double x = pmu - e - rS, y = wn - iS, r = 1.0 / (x * x + y * y);
+    d2v += 2.0 * w * x * (x * x - 3.0 * y * y) * (r * r * r);
+}
 
 // complex division
 __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {

@@ -697,7 +697,7 @@ __device__ __forceinline__ double trsg_row(const MuRootArgs &a, int blk, int j, 
            (P01 * P23);
 }
 
-// find_mu by safeguarded Newton (the host routine newton_root's steps) from
+// find_mu by safeguarded Halley steps (newton_update) from
 // mu0 inside [-10, 10] with tolerance 1e-15, one barrier per evaluation as in
 // k_sumrule_roots; then green::traceSelfG2 (src/green.cpp:2929-2976) at mu.
 __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
@@ -740,7 +740,7 @@ __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
         const double pmu = sc.x, delta = pmu - a.mu0;
         const bool series = fabs(delta) <= dmax;
         const int jhi = series ? a.jc : NO;
-        double v = 0.0, dv = 0.0;
+        double v = 0.0, dv = 0.0, d2v = 0.0;
         const GridWalk walk(jhi);
         for (int blk = walk.blk, j = walk.j; blk < a.nblk; walk.after(blk, j, blk, j)) {
             const int o0 = 4 * blk;
@@ -755,7 +755,7 @@ __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
                 if (w == 0.0) continue;
                 double rS, iS;
                 sigma_full(i1, sinf, __ldg(&a.s2[o0 + c]), __ldg(&a.s3[o0 + c]), sv[c], rS, iS);
-                trdiff_term(wn, rS, iS, __ldg(&a.ek[o0 + c]), a.mu0, pmu, w, v, dv);
+                trdiff_term(wn, rS, iS, __ldg(&a.ek[o0 + c]), a.mu0, pmu, w, v, dv, d2v);
             }
         }
         if (!series) {
@@ -769,11 +769,11 @@ __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
                 const double wn = (2 * (NO + t) + 1) * pt, i1 = 1.0 / wn, i2 = i1 * i1;
                 const double rS = -__ldg(&a.s2[o]) * i2 + __ldg(&a.s4[o]) * i2 * i2;
                 const double iS = -sinf * i1 + __ldg(&a.s3[o]) * i2 * i1;
-                trdiff_term(wn, rS, iS, __ldg(&a.ek[o]), a.mu0, pmu, w, v, dv);
+                trdiff_term(wn, rS, iS, __ldg(&a.ek[o]), a.mu0, pmu, w, v, dv, d2v);
             }
         }
         double *part = a.partial + (size_t)parity * kRootVals * kRootMaxBlocks;
-        block_root_sums(v, dv, 0.0, part + kRootVals * blockIdx.x);
+        block_root_sums(v, dv, d2v, part + kRootVals * blockIdx.x);
         if (!grid_sync(a.bar, a.err)) return;
         parity ^= 1;
         if (threadIdx.x < 32) {
@@ -781,18 +781,22 @@ __global__ void __launch_bounds__(kRootThreads) k_mu_roots(MuRootArgs a) {
             grid_root_sums(part, pv, pd, p2);
             if (threadIdx.x == 0) {
                 if (series) {
-                    // Re sum_m (-delta)^m C_m - G0 and its delta derivative
-                    double sr = 0.0, dsr = 0.0, pr = 1.0, pm = 0.0;  // (-delta)^m, (-delta)^(m-1)
-                    for (int m = 0; m < kMuMomP; ++m) {
-                        sr += pr * a.mom[2 + 2 * m];
-                        if (m > 0) dsr += -m * pm * a.mom[2 + 2 * m];
+                    // Re sum_m (-delta)^m C_m - G0 and its first two mu derivatives
+                    double sr = 0.0, dsr = 0.0, d2sr = 0.0, pr = 1.0, pm = 0.0, pmm = 0.0;
+                    for (int m = 0; m < kMuMomP; ++m) {  // pr, pm, pmm = (-delta)^(m, m-1, m-2)
+                        const double C = a.mom[2 + 2 * m];
+                        sr += pr * C;
+                        dsr += -m * pm * C;
+                        d2sr += m * (m - 1) * pmm * C;
+                        pmm = pm;
                         pm = pr;
                         pr *= -delta;
                     }
                     pv += sr - a.mom[2 + 2 * kMuMomP];
                     pd += dsr;
+                    p2 += d2sr;
                 }
-                newton_update(sc, pv, pd, 1e-15);
+                newton_update(sc, pv, pd, 1e-15, p2);
             }
         }
         __syncthreads();
