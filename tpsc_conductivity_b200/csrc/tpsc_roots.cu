@@ -445,6 +445,7 @@ __global__ void __launch_bounds__(kMomThreads, 2)
                     double T, double nk02, int jc, int nblk, double *partial, Bp b) {
     constexpr int NV = kSigmaMomNV, P64 = kMuMomF64, P32 = kMuMomP - kMuMomF64;
     __shared__ double cw[4], cx[4], c2[4], c3[4];
+    __shared__ __align__(16) double2 s_row[2][kMomThreads][4];  // two stages of 64-byte Sigma rows
     S = at(S, b.arena);
     s2 = at(s2, b.arena);
     s3 = at(s3, b.arena);
@@ -507,12 +508,26 @@ __global__ void __launch_bounds__(kMomThreads, 2)
             c3[c] = ok ? s3[o0 + c] : 0.0;
         }
         __syncthreads();
-        const double4 *row = reinterpret_cast<const double4 *>(S + (size_t)blk * 4 * NO);
-        for (int j = threadIdx.x; j < NO; j += blockDim.x) {
+        // this thread's Sigma rows j = tid + 256 i through two shared-memory
+        // stages: row i + 1 is copied (cp.async, 4 x 16 bytes) while row i is
+        // formed; each thread reads back only its own copies
+        const double2 *row = S + (size_t)blk * 4 * NO;
+        auto issue = [&](int jj, int st) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) cp_async16(&s_row[st][threadIdx.x][c], row + 4 * (size_t)jj + c);
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+        };
+        if ((int)threadIdx.x < NO) issue(threadIdx.x, 0);
+        for (int j = threadIdx.x, st = 0; j < NO; j += blockDim.x, st ^= 1) {
             const double wn = (2 * j + 1) * pt, i1 = 1.0 / wn;
-            const double4 p = ld_stream4(&row[2 * j]), q = ld_stream4(&row[2 * j + 1]);
-            const double2 sv[4] = {make_double2(p.x, p.y), make_double2(p.z, p.w), make_double2(q.x, q.y),
-                                   make_double2(q.z, q.w)};
+            if (j + (int)blockDim.x < NO) {
+                issue(j + blockDim.x, st ^ 1);
+                asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+            } else {
+                asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+            }
+            const double2 sv[4] = {s_row[st][threadIdx.x][0], s_row[st][threadIdx.x][1], s_row[st][threadIdx.x][2],
+                                   s_row[st][threadIdx.x][3]};
             if (j >= jc) {
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
